@@ -1,0 +1,274 @@
+"""ctypes bindings to the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  Two checkers are exposed with the same driving interface:
+
+  * ``OracleRun``  the C restatement (oracle/liboracle.so, vh_oracle.c)
+  * ``RefRun``     the reference's own hot-path sources compiled unmodified
+                   into oracle/_ref/libvhlle_ref.so (present only where the
+                   reference tree was available at build time)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libvhlle_ref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+class _Grid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
+                ("zmin", ctypes.c_double), ("zmax", ctypes.c_double)]
+
+
+class _Eos(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
+                ("ne", ctypes.c_int), ("nn", ctypes.c_int),
+                ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp)]
+
+
+class _Trc(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin",
+        "etaSShiftMuB", "etaSScaleMuB", "zetaSPeakEpsilon", "zetaSScaleBeta",
+        "zetaSSigmaMinus", "zetaSSigmaPlus")] + [
+        ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int)]
+
+
+class _State(ctypes.Structure):
+    _fields_ = [(n, _dp) for n in ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")]
+
+
+_lib_oracle = None
+_lib_ref = None
+
+
+def oracle_lib():
+    global _lib_oracle
+    if _lib_oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError("oracle not built: run `make -C oracle liboracle.so`")
+        lib = ctypes.CDLL(ORACLE_SO)
+        lib.or_step.restype = ctypes.c_int
+        lib.or_step.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_Trc),
+                                ctypes.POINTER(_State), _dp, ctypes.c_double]
+        lib.or_transform_pv.argtypes = [ctypes.POINTER(_Eos), _dp, ctypes.c_int, _dp]
+        lib.or_eos_eval.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
+        lib.or_eos_s.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
+        lib.or_update_m.argtypes = [ctypes.POINTER(_Grid), _dp, ctypes.c_double, ctypes.c_double]
+        _lib_oracle = lib
+    return _lib_oracle
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _lib_ref
+    if _lib_ref is None:
+        if not ref_available():
+            raise RuntimeError("compiled reference not present (oracle/_ref)")
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_create.restype = ctypes.c_void_p
+        lib.ref_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                   ctypes.c_char_p, _dp, ctypes.c_int, ctypes.c_int]
+        lib.ref_destroy.argtypes = [ctypes.c_void_p]
+        lib.ref_set_state.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp, _dp, _dp]
+        lib.ref_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.ref_tau.restype = ctypes.c_double
+        lib.ref_tau.argtypes = [ctypes.c_void_p]
+        lib.ref_set_dtau.restype = ctypes.c_int
+        lib.ref_set_dtau.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        lib.ref_get_state.argtypes = [ctypes.c_void_p] + [_dp] * 9
+        lib.ref_transform_pv.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
+        lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        _lib_ref = lib
+    return _lib_ref
+
+
+FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")
+FIELD_NCOMP = dict(Q=7, Qh=7, Qprev=7, pi=10, piH=10, Pi=1, PiH=1, m=3, vcc=1)
+
+
+def empty_state(N):
+    return {k: np.zeros((FIELD_NCOMP[k], N)) for k in FIELDS}
+
+
+def initial_state(setup):
+    """Cell contents right after the initial condition: Q, Qprev = Q,
+    m = setAllM(value), pi = Pi = 0, viscCorrCut = 1 (src/cll.cpp:33-52)."""
+    N = setup.grid.ncells
+    st = empty_state(N)
+    Q = np.array(setup.Q, dtype=np.float64).reshape(7, N)
+    # Cell::setQ zeroing (src/cll.h:75-86)
+    neg = Q[0] < 0
+    Q[:, neg] = 0.0
+    st["Q"][:] = Q
+    st["Qprev"][:] = Q
+    st["m"][:] = np.asarray(setup.m, dtype=np.float64).reshape(1, N)
+    if setup.pi is not None:
+        st["pi"][:] = setup.pi
+    if setup.Pi is not None:
+        st["Pi"][0] = setup.Pi
+    st["vcc"][:] = 1.0
+    return st
+
+
+class _EosHolder:
+    def __init__(self, eos):
+        self.keep = []
+        self.s = _Eos()
+        self.s.kind = eos.kind
+        self.s.conf_cnst = eos.conf_cnst
+        if eos.kind == 1:
+            arrs = [np.ascontiguousarray(a, dtype=np.float64)
+                    for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub)]
+            self.keep = arrs
+            self.s.ne = len(arrs[0])
+            self.s.nn = len(arrs[1])
+            self.s.egrid, self.s.ngrid, self.s.p, self.s.T, self.s.mub = (_ptr(a) for a in arrs)
+
+
+def _trc(setup):
+    t = _Trc()
+    for k, v in setup.tr.items():
+        setattr(t, k, float(v))
+    t.etaSparam = setup.etaSparam
+    t.zetaSparam = setup.zetaSparam
+    return t
+
+
+class OracleRun:
+    """The C restatement driven like Hydro: step() == performStep()."""
+
+    def __init__(self, setup):
+        self.setup = setup
+        g = setup.grid
+        self.grid = _Grid(g.nx, g.ny, g.nz, *g.bounds())
+        self.eos = _EosHolder(setup.eos)
+        self.trc = _trc(setup)
+        self.state = initial_state(setup)
+        self.tau = ctypes.c_double(setup.tau0)
+        self.dt = setup.dt
+        self.lib = oracle_lib()
+        self.errors = 0
+
+    def _sview(self):
+        s = _State()
+        for k in FIELDS:
+            setattr(s, k, _ptr(self.state[k]))
+        return s
+
+    def step(self, n=1):
+        sv = self._sview()
+        for _ in range(n):
+            self.errors |= self.lib.or_step(ctypes.byref(self.grid), ctypes.byref(self.eos.s),
+                                            ctypes.byref(self.trc), ctypes.byref(sv),
+                                            ctypes.byref(self.tau), self.dt)
+        return self.errors
+
+    @property
+    def tau_now(self):
+        return self.tau.value
+
+    def get_state(self):
+        return {k: v.copy() for k, v in self.state.items()}
+
+    def transform_pv(self, Q):
+        Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
+        out = np.zeros((len(Q), 8))
+        self.lib.or_transform_pv(ctypes.byref(self.eos.s), _ptr(Q), len(Q), _ptr(out))
+        return out
+
+    def eos_eval(self, e, nb):
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.float64)
+        out = np.zeros((len(e), 3))
+        s = np.zeros(len(e))
+        self.lib.or_eos_eval(ctypes.byref(self.eos.s), _ptr(e), _ptr(nb), len(e), _ptr(out))
+        self.lib.or_eos_s(ctypes.byref(self.eos.s), _ptr(e), _ptr(nb), len(e), _ptr(s))
+        return out, s
+
+
+class RefRun:
+    """The compiled reference (Fluid/Hydro objects) behind the same interface."""
+
+    def __init__(self, setup, eos_file=None):
+        self.setup = setup
+        self.lib = ref_lib()
+        g = setup.grid
+        self._tmp = None
+        if setup.eos.kind == 1 and eos_file is None:
+            self._tmp = tempfile.TemporaryDirectory()
+            eos_file = os.path.join(self._tmp.name, "eos1f.dat")
+            setup.eos.write_eos1f(eos_file)
+        bounds = np.array(g.bounds(), dtype=np.float64)
+        tr = np.array(setup.tr_vector(), dtype=np.float64)
+        self.h = self.lib.ref_create(g.nx, g.ny, g.nz, _ptr(bounds), setup.tau0, setup.dt,
+                                     setup.ecrit, setup.eos.kind, setup.eos.conf_cnst,
+                                     (eos_file or "").encode(), _ptr(tr), setup.etaSparam,
+                                     setup.zetaSparam)
+        st = initial_state(setup)
+        self.lib.ref_set_state(self.h, _ptr(st["Q"]), _ptr(st["pi"]), _ptr(st["piH"]),
+                               _ptr(st["Pi"][0]), _ptr(st["PiH"][0]), _ptr(st["m"][0].copy()))
+
+    def close(self):
+        if self.h:
+            self.lib.ref_destroy(self.h)
+            self.h = None
+        if self._tmp is not None:
+            self._tmp.cleanup()
+            self._tmp = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n=1):
+        self.lib.ref_step(self.h, n)
+        return 0
+
+    @property
+    def tau_now(self):
+        return self.lib.ref_tau(self.h)
+
+    def get_state(self):
+        N = self.setup.grid.ncells
+        st = empty_state(N)
+        self.lib.ref_get_state(self.h, *[_ptr(st[k]) for k in FIELDS])
+        return st
+
+    def transform_pv(self, Q):
+        Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
+        out = np.zeros((len(Q), 8))
+        self.lib.ref_transform_pv(self.h, _ptr(Q), len(Q), _ptr(out))
+        return out
+
+    def eos_eval(self, e, nb):
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.float64)
+        out = np.zeros((len(e), 3))
+        s = np.zeros(len(e))
+        self.lib.ref_eos(self.h, _ptr(e), _ptr(nb), len(e), _ptr(out), _ptr(s))
+        return out, s

@@ -1,0 +1,218 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// A thin extern "C" driver around the reference's own, unmodified classes
+// (Fluid, Hydro, Cell, EoS1f, TransportCoeff from src/), compiled together
+// with them into oracle/_ref/libvhlle_ref.so by oracle/Makefile.  It is the
+// pin for the C restatement in vh_oracle.c and the timed CPU baseline.
+//
+// Harness-owned pieces (not in the reference):
+//  * ConformalEoS: p = e/3, T = (e/cnst)^(1/4) evaluated as sqrt(sqrt(.)),
+//    muB = 0, the conformal gas of the Gubser-flow workload.  It plays the
+//    role of EoSs in its SIMPLE variant (src/eos.cpp:90-110), which the
+//    reference only offers at compile time.
+//  * The driver loop: performStep is called directly, as the reference main
+//    loop does (src/main.cpp:399-428), without the surface-based loop exit.
+//  * The initial state is uploaded as conserved Q arrays through Cell::setQ
+//    + saveQprev + setAllM, the pattern every reference IC ends with
+//    (e.g. src/icGubser.cpp:50-57).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "eos.h"  // must precede eo1.h, which only forward-declares EoS
+#include "cll.h"
+#include "eo1.h"
+#include "fld.h"
+#include "hdo.h"
+#include "inc.h"
+#include "rmn.h"
+#include "trancoeff.h"
+
+namespace {
+
+class ConformalEoS : public EoS {
+ public:
+  explicit ConformalEoS(double cnst) : cnst_(cnst) {}
+  void eos(double e, double nb, double nq, double ns, double &T, double &mub,
+           double &muq, double &mus, double &p) override {
+    (void)nb;
+    (void)nq;
+    (void)ns;
+    p = e / 3.;
+    T = e > 0. ? std::sqrt(std::sqrt(e / cnst_)) : 0.;
+    mub = muq = mus = 0.;
+  }
+  double p(double e, double nb, double ns, double nq) override {
+    (void)nb;
+    (void)ns;
+    (void)nq;
+    return e / 3.;
+  }
+
+ private:
+  double cnst_;
+};
+
+struct RefRun {
+  EoS *eos = nullptr;
+  TransportCoeff *tr = nullptr;
+  Fluid *f = nullptr;
+  Hydro *h = nullptr;
+  int nx = 0, ny = 0, nz = 0;
+  double dx = 0, dy = 0;
+};
+
+}  // namespace
+
+extern "C" {
+
+int ref_abi_version(void) { return 1; }
+
+// tr[14] = etaS0, zetaS0, ah, al, aRho, T0, etaSMin, etaSEpsilonMin,
+//          etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
+//          zetaSSigmaMinus, zetaSSigmaPlus
+void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
+                 double tau0, double dt, double ecrit, int eos_kind,
+                 double conf_cnst, const char *eos_file, const double *tr,
+                 int etaSparam, int zetaSparam) {
+  RefRun *r = new RefRun;
+  if (eos_kind == 0)
+    r->eos = new ConformalEoS(conf_cnst);
+  else
+    r->eos = new EoS1f(const_cast<char *>(eos_file));
+  r->tr = new TransportCoeff(tr[0], tr[1], tr[2], tr[3], tr[4], tr[5], tr[6],
+                             tr[7], tr[8], tr[9], tr[10], tr[11], tr[12],
+                             tr[13], r->eos, etaSparam, zetaSparam);
+  r->f = new Fluid(r->eos, r->eos, r->tr, nx, ny, nz, bounds[0], bounds[1],
+                   bounds[2], bounds[3], bounds[4], bounds[5], dt, ecrit);
+  r->h = new Hydro(r->f, r->eos, r->tr, tau0, dt);
+  r->nx = nx;
+  r->ny = ny;
+  r->nz = nz;
+  r->dx = r->f->getDx();
+  r->dy = r->f->getDy();
+  return r;
+}
+
+void ref_destroy(void *p) {
+  RefRun *r = static_cast<RefRun *>(p);
+  delete r->h;
+  delete r->f;
+  delete r->tr;
+  delete r->eos;
+  delete r;
+}
+
+// Q[7][N], pi[10][N], piH[10][N], Pi[N], PiH[N], m[N] (uniform per cell);
+// any of pi/piH/Pi/PiH may be null (then zero).
+void ref_set_state(void *p, const double *Q, const double *pi,
+                   const double *piH, const double *Pi, const double *PiH,
+                   const double *m) {
+  RefRun *r = static_cast<RefRun *>(p);
+  const long N = (long)r->nx * r->ny * r->nz;
+  for (int iz = 0; iz < r->nz; iz++)
+    for (int iy = 0; iy < r->ny; iy++)
+      for (int ix = 0; ix < r->nx; ix++) {
+        const long i = ix + (long)r->nx * (iy + (long)r->ny * iz);
+        Cell *c = r->f->getCell(ix, iy, iz);
+        double q[7];
+        for (int k = 0; k < 7; k++) q[k] = Q[k * N + i];
+        c->setQ(q);
+        c->saveQprev();
+        c->setAllM(m[i]);
+        for (int a = 0; a < 4; a++)
+          for (int b = 0; b <= a; b++) {
+            const int k = index44(a, b);
+            c->setpi(a, b, pi ? pi[k * N + i] : 0.);
+            c->setpiH(a, b, piH ? piH[k * N + i] : 0.);
+          }
+        c->setPi(Pi ? Pi[i] : 0.);
+        c->setPiH(PiH ? PiH[i] : 0.);
+      }
+}
+
+void ref_step(void *p, int nsteps) {
+  RefRun *r = static_cast<RefRun *>(p);
+  for (int s = 0; s < nsteps; s++) r->h->performStep();
+}
+
+double ref_tau(void *p) { return static_cast<RefRun *>(p)->h->getTau(); }
+
+// Hydro::setDtau exits when dt > dx/2; refuse that here instead.
+int ref_set_dtau(void *p, double dt) {
+  RefRun *r = static_cast<RefRun *>(p);
+  if (dt > r->dx / 2. || dt > r->dy / 2.) return 1;
+  r->h->setDtau(dt);
+  return 0;
+}
+
+// out arrays: component-major, any may be null.
+void ref_get_state(void *p, double *Q, double *Qh, double *Qprev, double *pi,
+                   double *piH, double *Pi, double *PiH, double *m,
+                   double *vcc) {
+  RefRun *r = static_cast<RefRun *>(p);
+  const long N = (long)r->nx * r->ny * r->nz;
+  for (int iz = 0; iz < r->nz; iz++)
+    for (int iy = 0; iy < r->ny; iy++)
+      for (int ix = 0; ix < r->nx; ix++) {
+        const long i = ix + (long)r->nx * (iy + (long)r->ny * iz);
+        Cell *c = r->f->getCell(ix, iy, iz);
+        double q[7];
+        if (Q) {
+          c->getQ(q);
+          for (int k = 0; k < 7; k++) Q[k * N + i] = q[k];
+        }
+        if (Qh) {
+          c->getQh(q);
+          for (int k = 0; k < 7; k++) Qh[k * N + i] = q[k];
+        }
+        if (Qprev) {
+          c->getQprev(q);
+          for (int k = 0; k < 7; k++) Qprev[k * N + i] = q[k];
+        }
+        for (int a = 0; a < 4; a++)
+          for (int b = 0; b <= a; b++) {
+            const int k = index44(a, b);
+            if (pi) pi[k * N + i] = c->getpi(a, b);
+            if (piH) piH[k * N + i] = c->getpiH(a, b);
+          }
+        if (Pi) Pi[i] = c->getPi();
+        if (PiH) PiH[i] = c->getPiH();
+        if (m)
+          for (int d = 0; d < 3; d++) m[d * N + i] = c->getM(d + 1);
+        if (vcc) vcc[i] = c->getViscCorrCutFlag();
+      }
+}
+
+// transformPV on n row-major states Q[n][7] -> out[n][8]
+void ref_transform_pv(void *p, const double *Q, int n, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  for (int i = 0; i < n; i++) {
+    double q[7];
+    for (int k = 0; k < 7; k++) q[k] = Q[7 * i + k];
+    double *o = out + 8 * i;
+    transformPV(r->eos, q, o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7]);
+  }
+}
+
+// EoS::eos -> out[n][3] = p, T, mub ; s_out[n] = EoS::s
+void ref_eos(void *p, const double *e, const double *nb, int n, double *out,
+             double *s_out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  for (int i = 0; i < n; i++) {
+    double T, mub, muq, mus, pp;
+    r->eos->eos(e[i], nb[i], 0., 0., T, mub, muq, mus, pp);
+    out[3 * i] = pp;
+    out[3 * i + 1] = T;
+    out[3 * i + 2] = mub;
+    if (s_out) s_out[i] = r->eos->s(e[i], nb[i], 0., 0.);
+  }
+}
+
+// Fluid::updateM alone (test of the vacuum-front rule)
+void ref_update_m(void *p, double tau, double dt) {
+  static_cast<RefRun *>(p)->f->updateM(tau, dt);
+}
+
+}  // extern "C"

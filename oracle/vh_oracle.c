@@ -1,0 +1,1370 @@
+/*
+ * vh_oracle.c -- CPU oracle (test infrastructure only) for the vHLLE
+ * per-timestep hydro update.  See vh_oracle.h for the contract.
+ *
+ * Each function restates the reference function named in its comment, in
+ * the reference's own loop and operation order, so that a build with
+ * -ffp-contract=off reproduces the reference's FP64 results bit for bit.
+ * The restatement is sequential on purpose: the cumulative per-cell flux
+ * order it produces (x faces, y faces, z faces, source) is the order the
+ * CUDA path has to match.
+ */
+#include "vh_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum { T_ = 0, X_ = 1, Y_ = 2, Z_ = 3, NB_ = 4, NQ_ = 5, NS_ = 6 };
+enum { PREDICT = 0, CORRECT = 1 };
+
+int or_abi_version(void) { return 1; }
+
+/* ---------------------------------------------------------------- helpers */
+
+/* minmod slope limiter, src/cll.cpp:12-19 */
+static double minmod(double a, double b) {
+  if (a * b <= 0.) return 0.;
+  if (fabs(a) > fabs(b))
+    return b;
+  else
+    return a;
+}
+
+/* index44, src/cll.cpp:22-31 (indices are always in range here) */
+static int index44(int i, int j) {
+  if (j < i)
+    return (i * (i + 1)) / 2 + j;
+  else
+    return (j * (j + 1)) / 2 + i;
+}
+
+/* std::min / std::max semantics (return the first argument on ties/NaN) */
+static double smin(double a, double b) { return (b < a) ? b : a; }
+static double smax(double a, double b) { return (a < b) ? b : a; }
+
+/* sign(), src/hdo.cpp:34-41 */
+static double sgn(double x) {
+  if (x > 0)
+    return 1.;
+  else if (x < 0.)
+    return -1.;
+  else
+    return 0.;
+}
+
+/* ------------------------------------------------------------------- EoS */
+
+/* EoS1f::getue / getun / eos, src/eo1.cpp:63-123 */
+static void eos1f(const or_eos *E, double e, double nb, double *T, double *mub,
+                  double *p) {
+  const int ne = E->ne, nn = E->nn;
+  int k, k1, k2;
+  k1 = 0;
+  k2 = ne - 1;
+  while (k2 - k1 > 1) {
+    k = (k1 + k2) / 2;
+    if (e < E->egrid[k])
+      k2 = k;
+    else
+      k1 = k;
+  }
+  int ixe = k1;
+  if (ixe > ne - 2) ixe = ne - 2;
+  const double ue = (e - E->egrid[k1]) / (E->egrid[k2] - E->egrid[k1]);
+  k1 = 0;
+  k2 = nn - 1;
+  while (k2 - k1 > 1) {
+    k = (k1 + k2) / 2;
+    if (nb < E->ngrid[k])
+      k2 = k;
+    else
+      k1 = k;
+  }
+  int ixn = k1;
+  if (ixn > nn - 2) ixn = nn - 2;
+  if (ixn < 0) ixn = 0;
+  const double un = (nb - E->ngrid[k1]) / (E->ngrid[k2] - E->ngrid[k1]);
+  const double we[2] = {1. - ue, ue};
+  const double wn[2] = {1. - un, un};
+  double sp = 0., sT = 0., smu = 0.;
+  for (int je = 0; je < 2; je++)
+    for (int jn = 0; jn < 2; jn++) {
+      const int id = (ixe + je) + ne * (ixn + jn);
+      sp += we[je] * wn[jn] * E->p[id];
+      sT += we[je] * wn[jn] * E->T[id];
+      smu += we[je] * wn[jn] * E->mub[id];
+    }
+  if (sp < 0.) sp = 0.;
+  *p = sp;
+  *T = sT;
+  *mub = smu;
+}
+
+/* EoS::eos(); muq = mus = 0 for both supported kinds */
+static void eos_eval(const or_eos *E, double e, double nb, double *T,
+                     double *mub, double *p) {
+  if (E->kind == 0) {
+    *p = e / 3.;
+    *T = e > 0. ? sqrt(sqrt(e / E->conf_cnst)) : 0.;
+    *mub = 0.;
+  } else {
+    eos1f(E, e, nb, T, mub, p);
+  }
+}
+
+static double eos_p(const or_eos *E, double e, double nb) {
+  double T, mub, p;
+  if (E->kind == 0) return e / 3.;
+  eos1f(E, e, nb, &T, &mub, &p);
+  return p;
+}
+
+/* EoS::s, src/eos.cpp:18-25 */
+static double eos_s(const or_eos *E, double e, double nb, double nq,
+                    double ns) {
+  double T, mub, p;
+  const double muq = 0., mus = 0.;
+  eos_eval(E, e, nb, &T, &mub, &p);
+  if (T > 0.0)
+    return (e + p - mub * nb - muq * nq - mus * ns) / T;
+  else
+    return 0.;
+}
+
+/* ------------------------------------------------------- transformPV */
+
+/* transformPV, src/rmn.cpp:28-139.  Q is modified in place exactly as the
+ * reference does when |M| > Q_t (the caller's copy). */
+static void transform_pv(const or_eos *E, double Q[7], double *e, double *p,
+                         double *nb, double *nq, double *ns, double *vx,
+                         double *vy, double *vz) {
+  const int MAXIT = 100;
+  const double dpe = 1. / 3.;
+  const double corrf = 0.9999;
+  double v, vl = 0., vh = 1., dvold, dv, f, df;
+  double M = sqrt(Q[X_] * Q[X_] + Q[Y_] * Q[Y_] + Q[Z_] * Q[Z_]);
+  if (Q[T_] <= 0.) {
+    *e = 0.;
+    *p = 0.;
+    *vx = *vy = *vz = 0.;
+    *nb = *nq = *ns = 0.;
+    return;
+  }
+  if (M == 0.) {
+    *e = Q[T_];
+    *vx = 0.;
+    *vy = 0.;
+    *vz = 0.;
+    *nb = Q[NB_];
+    *nq = Q[NQ_];
+    *ns = Q[NS_];
+    *p = eos_p(E, *e, *nb);
+    return;
+  }
+  if (M > Q[T_]) {
+    Q[X_] *= corrf * Q[T_] / M;
+    Q[Y_] *= corrf * Q[T_] / M;
+    Q[Z_] *= corrf * Q[T_] / M;
+    M = Q[T_] * corrf;
+  }
+  v = 0.5 * (vl + vh);
+  *e = Q[T_] - M * v;
+  if (*e < 0.) *e = 0.;
+  *nb = Q[NB_] * sqrt(1 - v * v);
+  *nq = Q[NQ_] * sqrt(1 - v * v);
+  *ns = Q[NS_] * sqrt(1 - v * v);
+  *p = eos_p(E, *e, *nb);
+  f = (Q[T_] + *p) * v - M;
+  df = (Q[T_] + *p) - M * v * dpe;
+  dvold = vh - vl;
+  dv = dvold;
+  for (int i = 0; i < MAXIT; i++) {
+    if ((f + df * (vh - v)) * (f + df * (vl - v)) >= 0. ||
+        fabs(2. * f) > fabs(dvold * df)) {
+      dvold = dv;
+      dv = 0.5 * (vh - vl);
+      v = vl + dv;
+    } else {
+      dvold = dv;
+      dv = f / df;
+      v -= dv;
+    }
+    if (fabs(dv) < 0.00001) break;
+    *e = Q[T_] - M * v;
+    if (*e < 0.) *e = 0.;
+    *nb = Q[NB_] * sqrt(1 - v * v);
+    *nq = Q[NQ_] * sqrt(1 - v * v);
+    *ns = Q[NS_] * sqrt(1 - v * v);
+    *p = eos_p(E, *e, *nb);
+    f = (Q[T_] + *p) * v - M;
+    df = (Q[T_] + *p) - M * v * dpe;
+    if (f > 0.)
+      vh = v;
+    else
+      vl = v;
+  }
+  *vx = v * Q[X_] / M;
+  *vy = v * Q[Y_] / M;
+  *vz = v * Q[Z_] / M;
+  *e = Q[T_] - M * v;
+  *p = eos_p(E, *e, *nb); /* stale nb, as in the reference */
+  *nb = Q[NB_] * sqrt(1 - *vx * *vx - *vy * *vy - *vz * *vz);
+  *nq = Q[NQ_] * sqrt(1 - *vx * *vx - *vy * *vy - *vz * *vz);
+  *ns = Q[NS_] * sqrt(1 - *vx * *vx - *vy * *vy - *vz * *vz);
+}
+
+/* ------------------------------------------------ transport coefficients */
+
+/* TransportCoeff::zetaS, src/trancoeff.cpp:19-66.  cs2(e) is the EoS base
+ * class value 1/3 for both supported EoS kinds (src/eos.h:37). */
+static double tr_zetaS(const or_trc *t, double e, double T, double s,
+                       double P) {
+  const double cs2e = 1. / 3.;
+  const double T_p = 0.180, T_peak = 0.165, T_width = 0.010, B_norm = 0.24,
+               B_width = 1.5, T_peak2 = 0.160, B_norm2 = 0.13, B1 = 0.01,
+               B2 = 0.12;
+  if (t->zetaSparam == 0)
+    return t->zetaS0 * (1. / 3. - cs2e) / (exp((0.16 - T) / 0.001) + 1.);
+  else if (t->zetaSparam == 1) {
+    if (T < 0.180)
+      return 0.03 + (0.08 * exp(((T / T_p) - 1.) / (0.0025))) +
+             (0.22 * exp(((T / T_p) - 1) / (0.022)));
+    else if (T >= 0.180 && T < 0.200)
+      return 27.55 * (T / T_p) - 13.45 - (13.77 * (T / T_p) * (T / T_p));
+    else if (T >= 0.200)
+      return 0.001 + (0.9 * exp(-((T / T_p) - 1.) / (0.0025))) +
+             (0.25 * exp(-((T / T_p) - 1.) / (0.13)));
+  } else if (t->zetaSparam == 2) {
+    if (T > T_peak)
+      return B_norm * ((B_width * B_width) /
+                       ((((T / T_peak) - 1.) * ((T / T_peak) - 1.)) +
+                        (B_width * B_width)));
+    else if (T <= T_peak)
+      return B_norm *
+             (exp(-((T - T_peak) / T_width) * ((T - T_peak) / T_width)));
+  } else if (t->zetaSparam == 3) {
+    if (T < T_peak2)
+      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B1 * B1)));
+    else if (T >= T_peak2)
+      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B2 * B2)));
+  } else if (t->zetaSparam == 4) {
+    /* abs() binds to int abs(int) in the reference: |s| < 1 reads as 0 */
+    if (!(fabs(s) >= 1.0) || T < 1e-1) return 0;
+    const double d =
+        t->zetaSScaleBeta * (pow(e, 0.25) - pow(t->zetaSPeakEpsilon, 0.25));
+    const double sig =
+        e < t->zetaSPeakEpsilon ? t->zetaSSigmaMinus : t->zetaSSigmaPlus;
+    return ((e + P) / (s * T)) * t->zetaS0 * exp(d * d / 2.0 * (sig * sig));
+  }
+  return 0.;
+}
+
+/* TransportCoeff::etaS, src/trancoeff.cpp:73-90 */
+static double tr_etaS(const or_trc *t, double e, double rho, double T,
+                      double muB, double s, double P) {
+  if (t->etaSparam == 0) {
+    return t->etaS0;
+  } else if (t->etaSparam == 1) {
+    return t->etaSMin + ((T > t->T0) ? t->ah * (T - t->T0) : t->al * (T - t->T0));
+  } else if (t->etaSparam == 2) {
+    return smax(0.0, t->etaSMin + ((e > t->etaSEpsilonMin)
+                                       ? ((t->ah * (e - t->etaSEpsilonMin) +
+                                           t->aRho * rho))
+                                       : t->al * (e - t->etaSEpsilonMin) +
+                                             t->aRho * rho));
+  } else if (t->etaSparam == 3) {
+    if (!(fabs(s) >= 1.0) || T < 1e-1) return 0;
+    const double Tc = t->T0 + t->etaSShiftMuB * (muB / 0.938);
+    return ((e + P) / (s * T)) *
+           smax(0.0, (t->etaSMin + ((T > Tc) ? t->ah * (T - Tc)
+                                             : t->al * (T - Tc))) *
+                         (1 + t->etaSScaleMuB * (muB / 0.938)));
+  }
+  return 0.;
+}
+
+/* TransportCoeff::getTau, src/trancoeff.cpp:92-100.  The reference's
+ * abs(e + P) resolves to int abs(int): the test is trunc(e + P) != 0. */
+static void tr_getTau(const or_trc *t, double e, double rho, double T,
+                      double muB, double s, double P, double *taupi,
+                      double *tauPi) {
+  if (T > 1e-1 && !(fabs(e + P) < 1.0)) {
+    *taupi = (5. / 5.068) * s * tr_etaS(t, e, rho, T, muB, s, P) / (e + P);
+    *tauPi = (6. / 5.068) * tr_zetaS(t, e, T, s, P) * s / (e + P);
+  } else {
+    *taupi = *tauPi = 0.;
+  }
+}
+
+static int tr_isViscous(const or_trc *t) {
+  return (t->etaS0 > 0. || t->zetaS0 > 0. || t->etaSparam > 0 ||
+          t->zetaSparam > 0);
+}
+
+/* ------------------------------------------------------------ the step */
+
+typedef struct Ctx {
+  const or_grid *g;
+  const or_eos *E;
+  const or_trc *tr;
+  or_state *s;
+  long N;
+  int nx, ny, nz;
+  double dx, dy, dz;
+  double tau, dt;
+  double *flux, *dm, *pi0, *piH0, *Pi0, *PiH0;
+  int err;
+} Ctx;
+
+static long cell(const Ctx *c, int ix, int iy, int iz) {
+  ix = ix > 0 ? ix : 0;
+  ix = ix < c->nx ? ix : c->nx - 1;
+  iy = iy > 0 ? iy : 0;
+  iy = iy < c->ny ? iy : c->ny - 1;
+  iz = iz > 0 ? iz : 0;
+  iz = iz < c->nz ? iz : c->nz - 1;
+  return (long)ix + (long)c->nx * iy + (long)c->nx * c->ny * iz;
+}
+
+static void coords(const Ctx *c, long i, int *ix, int *iy, int *iz) {
+  *ix = (int)(i % c->nx);
+  *iy = (int)((i / c->nx) % c->ny);
+  *iz = (int)(i / ((long)c->nx * c->ny));
+}
+
+static long neighbour(const Ctx *c, long i, int dir, int step) {
+  int ix, iy, iz;
+  coords(c, i, &ix, &iy, &iz);
+  if (dir == X_) ix += step;
+  if (dir == Y_) iy += step;
+  if (dir == Z_) iz += step;
+  return cell(c, ix, iy, iz);
+}
+
+#define F(a, comp, i) ((a)[(long)(comp) * c->N + (i)])
+
+static double getM(const Ctx *c, long i, int dir) {
+  return c->s->m[(long)(dir - 1) * c->N + i];
+}
+static double getMaxM(const Ctx *c, long i) {
+  const double *m = c->s->m;
+  return smax(m[i], smax(m[c->N + i], m[2 * c->N + i]));
+}
+
+static void addFlux(Ctx *c, long i, const double f[7]) {
+  for (int k = 0; k < 7; k++) F(c->flux, k, i) += f[k];
+}
+
+/* Cell::getPrimVar / getPrimVarHCenter / getPrimVarPrev,
+ * src/cll.cpp:90-104,206-220: con2prim of (field / tau) */
+static void primCenter(Ctx *c, const double *field, long i, double tau,
+                       double *e, double *p, double *nb, double *nq,
+                       double *ns, double *vx, double *vy, double *vz) {
+  double q[7];
+  for (int k = 0; k < 7; k++) q[k] = F(field, k, i) / tau;
+  transform_pv(c->E, q, e, p, nb, nq, ns, vx, vy, vz);
+}
+
+/* getPrimVarLeft/Right and the H variants, src/cll.cpp:106-204.
+ * side = -1: left boundary of cell i; +1: right boundary. */
+static void primFace(Ctx *c, const double *field, long i, int dir, int side,
+                     double tau, double *e, double *p, double *nb, double *nq,
+                     double *ns, double *vx, double *vy, double *vz) {
+  const long inext = neighbour(c, i, dir, +1), iprev = neighbour(c, i, dir, -1);
+  double Qr[7], Ql[7], Q[7], dQ[7], q[7];
+  for (int k = 0; k < 7; k++) {
+    Qr[k] = F(field, k, inext);
+    Ql[k] = F(field, k, iprev);
+    Q[k] = F(field, k, i);
+  }
+  for (int k = 0; k < 7; k++)
+    dQ[k] = minmod((Qr[k] - Q[k]) / 2., (Q[k] - Ql[k]) / 2.);
+  if (side < 0)
+    for (int k = 0; k < 7; k++) q[k] = (Q[k] - dQ[k]) / tau;
+  else
+    for (int k = 0; k < 7; k++) q[k] = (Q[k] + dQ[k]) / tau;
+  transform_pv(c->E, q, e, p, nb, nq, ns, vx, vy, vz);
+}
+
+/* Hydro::hlle_flux, src/hdo.cpp:77-305 */
+static void hlle_flux(Ctx *c, long L, long R, int direction, int mode) {
+  double el, er, pl, pr, nbl, nql, nsl, nbr, nqr, nsr, vxl, vxr, vyl, vyr, vzl,
+      vzr, bl = 0., br = 0., csb, vb, El, Er, dx = 0.;
+  double Ftl = 0., Fxl = 0., Fyl = 0., Fzl = 0., Fbl = 0., Fql = 0., Fsl = 0.,
+         Ftr = 0., Fxr = 0., Fyr = 0., Fzr = 0., Fbr = 0., Fqr = 0., Fsr = 0.;
+  double U1l, U2l, U3l, U4l, Ubl, Uql, Usl, U1r, U2r, U3r, U4r, Ubr, Uqr, Usr;
+  double flux[7];
+  const double dt = c->dt, tau = c->tau;
+  const double dta = mode == 0 ? dt / 2. : dt;
+  double tauFactor;
+  const double *QQ = (mode == PREDICT) ? c->s->Q : c->s->Qh;
+  primFace(c, QQ, L, direction, +1, tau, &el, &pl, &nbl, &nql, &nsl, &vxl,
+           &vyl, &vzl);
+  primFace(c, QQ, R, direction, -1, tau, &er, &pr, &nbr, &nqr, &nsr, &vxr,
+           &vyr, &vzr);
+  El = (el + pl) / (1 - vxl * vxl - vyl * vyl - vzl * vzl);
+  Er = (er + pr) / (1 - vxr * vxr - vyr * vyr - vzr * vzr);
+  if (mode == PREDICT)
+    tauFactor = tau + 0.25 * dt;
+  else
+    tauFactor = tau + 0.5 * dt;
+
+  if (el < 0.) {
+    el = 0.;
+    pl = 0.;
+  }
+  if (er < 0.) {
+    er = 0.;
+    pr = 0.;
+  }
+  if (el > 1e10) { /* the reference dumps the cell and exits */
+    c->err |= OR_ERR_E_HUGE;
+    return;
+  }
+  if (el == 0. && er == 0.) return;
+  /* pr < 0: the reference re-evaluates the same two calls; no effect */
+  if (getM(c, L, direction) < 1. && getM(c, R, direction) < 1.) return;
+
+  const double cs2 = 1. / 3.;
+  const double cs = sqrt(1. / 3.);
+  double gammal = 1. / sqrt(1 - vxl * vxl - vyl * vyl - vzl * vzl);
+  double gammar = 1. / sqrt(1 - vxr * vxr - vyr * vyr - vzr * vzr);
+  U1l = gammal * gammal * (el + pl) * vxl;
+  U2l = gammal * gammal * (el + pl) * vyl;
+  U3l = gammal * gammal * (el + pl) * vzl;
+  U4l = gammal * gammal * (el + pl) - pl;
+  Ubl = gammal * nbl;
+  Uql = gammal * nql;
+  Usl = gammal * nsl;
+  U1r = gammar * gammar * (er + pr) * vxr;
+  U2r = gammar * gammar * (er + pr) * vyr;
+  U3r = gammar * gammar * (er + pr) * vzr;
+  U4r = gammar * gammar * (er + pr) - pr;
+  Ubr = gammar * nbr;
+  Uqr = gammar * nqr;
+  Usr = gammar * nsr;
+
+  const double sEl = sqrt(El), sEr = sqrt(Er);
+  if (direction == X_) {
+    Ftl = U4l * vxl + pl * vxl;
+    Fxl = U1l * vxl + pl;
+    Fyl = U2l * vxl;
+    Fzl = U3l * vxl;
+    Fbl = Ubl * vxl;
+    Fql = Uql * vxl;
+    Fsl = Usl * vxl;
+    Ftr = U4r * vxr + pr * vxr;
+    Fxr = U1r * vxr + pr;
+    Fyr = U2r * vxr;
+    Fzr = U3r * vxr;
+    Fbr = Ubr * vxr;
+    Fqr = Uqr * vxr;
+    Fsr = Usr * vxr;
+    const double ss = sEl + sEr, dv = vxl - vxr;
+    csb = sqrt(cs2 + 0.5 * sqrt(El * Er) / (ss * ss) * (dv * dv));
+    vb = (sEl * vxl + sEr * vxr) / (sEl + sEr);
+    bl = smin(0., smin((vb - csb) / (1 - vb * csb), (vxl - cs) / (1 - vxl * cs)));
+    br = smax(0., smax((vb + csb) / (1 + vb * csb), (vxr + cs) / (1 + vxr * cs)));
+    dx = c->dx;
+    if (el == 0.) bl = -1.;
+    if (er == 0.) br = 1.;
+  }
+  if (direction == Y_) {
+    Ftl = U4l * vyl + pl * vyl;
+    Fxl = U1l * vyl;
+    Fyl = U2l * vyl + pl;
+    Fzl = U3l * vyl;
+    Fbl = Ubl * vyl;
+    Fql = Uql * vyl;
+    Fsl = Usl * vyl;
+    Ftr = U4r * vyr + pr * vyr;
+    Fxr = U1r * vyr;
+    Fyr = U2r * vyr + pr;
+    Fzr = U3r * vyr;
+    Fbr = Ubr * vyr;
+    Fqr = Uqr * vyr;
+    Fsr = Usr * vyr;
+    const double ss = sEl + sEr, dv = vyl - vyr;
+    csb = sqrt(cs2 + 0.5 * sqrt(El * Er) / (ss * ss) * (dv * dv));
+    vb = (sEl * vyl + sEr * vyr) / (sEl + sEr);
+    bl = smin(0., smin((vb - csb) / (1 - vb * csb), (vyl - cs) / (1 - vyl * cs)));
+    br = smax(0., smax((vb + csb) / (1 + vb * csb), (vyr + cs) / (1 + vyr * cs)));
+    dx = c->dy;
+    if (el == 0.) bl = -1.;
+    if (er == 0.) br = 1.;
+  }
+  if (direction == Z_) {
+    const double tau1 = tauFactor;
+    Ftl = U4l * vzl / tau1 + pl * vzl / tau1;
+    Fxl = U1l * vzl / tau1;
+    Fyl = U2l * vzl / tau1;
+    Fzl = U3l * vzl / tau1 + pl / tau1;
+    Fbl = Ubl * vzl / tau1;
+    Fql = Uql * vzl / tau1;
+    Fsl = Usl * vzl / tau1;
+    Ftr = U4r * vzr / tau1 + pr * vzr / tau1;
+    Fxr = U1r * vzr / tau1;
+    Fyr = U2r * vzr / tau1;
+    Fzr = U3r * vzr / tau1 + pr / tau1;
+    Fbr = Ubr * vzr / tau1;
+    Fqr = Uqr * vzr / tau1;
+    Fsr = Usr * vzr / tau1;
+    const double ss = sEl + sEr, dv = vzl - vzr;
+    csb = sqrt(cs2 + 0.5 * sqrt(El * Er) / (ss * ss) * (dv * dv));
+    vb = (sEl * vzl + sEr * vzr) / (sEl + sEr);
+    bl = 1. / tau *
+         smin(0., smin((vb - csb) / (1 - vb * csb), (vzl - cs) / (1 - vzl * cs)));
+    br = 1. / tau *
+         smax(0., smax((vb + csb) / (1 + vb * csb), (vzr + cs) / (1 + vzr * cs)));
+    dx = c->dz;
+    if (el == 0.) bl = -1. / tau;
+    if (er == 0.) br = 1. / tau;
+  }
+  if (bl == 0. && br == 0.) return;
+
+  flux[T_] = tauFactor * dta / dx *
+             (-bl * br * (U4l - U4r) + br * Ftl - bl * Ftr) / (-bl + br);
+  flux[X_] = tauFactor * dta / dx *
+             (-bl * br * (U1l - U1r) + br * Fxl - bl * Fxr) / (-bl + br);
+  flux[Y_] = tauFactor * dta / dx *
+             (-bl * br * (U2l - U2r) + br * Fyl - bl * Fyr) / (-bl + br);
+  flux[Z_] = tauFactor * dta / dx *
+             (-bl * br * (U3l - U3r) + br * Fzl - bl * Fzr) / (-bl + br);
+  flux[NB_] = tauFactor * dta / dx *
+              (-bl * br * (Ubl - Ubr) + br * Fbl - bl * Fbr) / (-bl + br);
+  flux[NQ_] = tauFactor * dta / dx *
+              (-bl * br * (Uql - Uqr) + br * Fql - bl * Fqr) / (-bl + br);
+  flux[NS_] = tauFactor * dta / dx *
+              (-bl * br * (Usl - Usr) + br * Fsl - bl * Fsr) / (-bl + br);
+  if (flux[NB_] != flux[NB_]) {
+    c->err |= OR_ERR_FLUX_NAN;
+    return;
+  }
+  double mf[7];
+  for (int k = 0; k < 7; k++) mf[k] = -flux[k];
+  addFlux(c, L, mf);
+  addFlux(c, R, flux);
+}
+
+/* Hydro::source + source_step, src/hdo.cpp:307-353 */
+static void source_step(Ctx *c, long i, int mode) {
+  const double dt = c->dt, tau = c->tau;
+  const double _dt = (mode == PREDICT) ? dt / 2. : dt;
+  double tau1, Q[7], k[7], _Q[7];
+  const double *field = (mode == PREDICT) ? c->s->Q : c->s->Qh;
+  for (int j = 0; j < 7; j++) Q[j] = F(field, j, i);
+  tau1 = (mode == PREDICT) ? tau : tau + 0.5 * dt;
+  double e, p, nb, nq, ns, vx, vy, vz;
+  for (int j = 0; j < 7; j++) _Q[j] = Q[j] / tau1;
+  transform_pv(c->E, _Q, &e, &p, &nb, &nq, &ns, &vx, &vy, &vz);
+  k[T_] = -_Q[T_] * vz * vz - p * (1. + vz * vz);
+  k[X_] = 0.;
+  k[Y_] = 0.;
+  k[Z_] = -_Q[Z_];
+  k[NB_] = 0.;
+  k[NQ_] = 0.;
+  k[NS_] = 0.;
+  for (int j = 0; j < 7; j++) k[j] *= _dt;
+  if (k[NB_] != k[NB_]) {
+    c->err |= OR_ERR_SOURCE_NAN;
+    return;
+  }
+  addFlux(c, i, k);
+}
+
+/* Cell::setQ / setQh zeroing copy, src/cll.h:75-86 (Q) */
+static void copyQ(Ctx *c, double *field, long dst, long src) {
+  double q[7];
+  for (int k = 0; k < 7; k++) q[k] = F(field, k, src);
+  if (q[T_] < 0.)
+    for (int k = 0; k < 7; k++) q[k] = 0.;
+  for (int k = 0; k < 7; k++) F(field, k, dst) = q[k];
+}
+
+static void copyVisc(Ctx *c, long dst, long src) {
+  double p[10];
+  for (int k = 0; k < 10; k++) p[k] = F(c->s->pi, k, src);
+  const double P = c->s->Pi[src];
+  for (int k = 0; k < 10; k++) F(c->s->pi, k, dst) = p[k];
+  c->s->Pi[dst] = P;
+}
+
+/* Fluid::correctImagCells (full = 0) and correctImagCellsFull (full = 1),
+ * src/fld.cpp:211-382 */
+static void correctImagCells(Ctx *c, int full) {
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+  double *Q = c->s->Q, *Qh = c->s->Qh;
+  /* Z */
+  for (int ix = 0; ix < nx; ix++)
+    for (int iy = 0; iy < ny; iy++) {
+      long s = cell(c, ix, iy, 2);
+      copyQ(c, Q, cell(c, ix, iy, 1), s);
+      copyQ(c, Q, cell(c, ix, iy, 0), s);
+      if (!full) {
+        copyQ(c, Qh, cell(c, ix, iy, 1), s);
+        copyQ(c, Qh, cell(c, ix, iy, 0), s);
+      } else {
+        double p[10];
+        for (int k = 0; k < 10; k++) p[k] = F(c->s->pi, k, s);
+        const double P = c->s->Pi[s];
+        long d0 = cell(c, ix, iy, 0), d1 = cell(c, ix, iy, 1);
+        for (int k = 0; k < 10; k++) F(c->s->pi, k, d0) = p[k];
+        for (int k = 0; k < 10; k++) F(c->s->pi, k, d1) = p[k];
+        c->s->Pi[d0] = P;
+        c->s->Pi[d1] = P;
+      }
+      s = cell(c, ix, iy, nz - 3);
+      copyQ(c, Q, cell(c, ix, iy, nz - 2), s);
+      copyQ(c, Q, cell(c, ix, iy, nz - 1), s);
+      if (!full) {
+        copyQ(c, Qh, cell(c, ix, iy, nz - 2), s);
+        copyQ(c, Qh, cell(c, ix, iy, nz - 1), s);
+      } else {
+        double p[10];
+        for (int k = 0; k < 10; k++) p[k] = F(c->s->pi, k, s);
+        const double P = c->s->Pi[s];
+        long d0 = cell(c, ix, iy, nz - 2), d1 = cell(c, ix, iy, nz - 1);
+        for (int k = 0; k < 10; k++) F(c->s->pi, k, d0) = p[k];
+        for (int k = 0; k < 10; k++) F(c->s->pi, k, d1) = p[k];
+        c->s->Pi[d0] = P;
+        c->s->Pi[d1] = P;
+      }
+    }
+  /* Y */
+  for (int ix = 0; ix < nx; ix++)
+    for (int iz = 0; iz < nz; iz++) {
+      long s = cell(c, ix, 2, iz);
+      copyQ(c, Q, cell(c, ix, 1, iz), s);
+      copyQ(c, Q, cell(c, ix, 0, iz), s);
+      if (!full) {
+        copyQ(c, Qh, cell(c, ix, 1, iz), s);
+        copyQ(c, Qh, cell(c, ix, 0, iz), s);
+      } else {
+        copyVisc(c, cell(c, ix, 0, iz), s);
+        copyVisc(c, cell(c, ix, 1, iz), s);
+      }
+      s = cell(c, ix, ny - 3, iz);
+      copyQ(c, Q, cell(c, ix, ny - 2, iz), s);
+      copyQ(c, Q, cell(c, ix, ny - 1, iz), s);
+      if (!full) {
+        copyQ(c, Qh, cell(c, ix, ny - 2, iz), s);
+        copyQ(c, Qh, cell(c, ix, ny - 1, iz), s);
+      } else {
+        copyVisc(c, cell(c, ix, ny - 2, iz), s);
+        copyVisc(c, cell(c, ix, ny - 1, iz), s);
+      }
+    }
+  /* X */
+  for (int iy = 0; iy < ny; iy++)
+    for (int iz = 0; iz < nz; iz++) {
+      long s = cell(c, 2, iy, iz);
+      copyQ(c, Q, cell(c, 1, iy, iz), s);
+      copyQ(c, Q, cell(c, 0, iy, iz), s);
+      if (!full) {
+        copyQ(c, Qh, cell(c, 1, iy, iz), s);
+        copyQ(c, Qh, cell(c, 0, iy, iz), s);
+      } else {
+        copyVisc(c, cell(c, 0, iy, iz), s);
+        copyVisc(c, cell(c, 1, iy, iz), s);
+      }
+      s = cell(c, nx - 3, iy, iz);
+      copyQ(c, Q, cell(c, nx - 2, iy, iz), s);
+      copyQ(c, Q, cell(c, nx - 1, iy, iz), s);
+      if (!full) {
+        copyQ(c, Qh, cell(c, nx - 2, iy, iz), s);
+        copyQ(c, Qh, cell(c, nx - 1, iy, iz), s);
+      } else {
+        copyVisc(c, cell(c, nx - 2, iy, iz), s);
+        copyVisc(c, cell(c, nx - 1, iy, iz), s);
+      }
+    }
+}
+
+/* Cell::addM, src/cll.h:147-151 */
+static void addM(Ctx *c, long i, int dir, double inc) {
+  double *m = c->s->m;
+  m[(long)(dir - 1) * c->N + i] += inc;
+  if (m[(long)(dir - 1) * c->N + i] > 0.9)
+    for (int k = 0; k < 3; k++) m[(long)k * c->N + i] = 1.;
+}
+
+/* Fluid::updateM, src/fld.cpp:384-423 */
+static void updateM(Ctx *c, double tau, double dt) {
+  const long N = c->N;
+  double *dm = c->dm;
+  for (int ix = 0; ix < c->nx; ix++)
+    for (int iy = 0; iy < c->ny; iy++)
+      for (int iz = 0; iz < c->nz; iz++) {
+        const long i = cell(c, ix, iy, iz);
+        dm[i] = dm[N + i] = dm[2 * N + i] = 0.;
+        if (getMaxM(c, i) < 1.) {
+          if (getM(c, cell(c, ix + 1, iy, iz), X_) >= 1. ||
+              getM(c, cell(c, ix - 1, iy, iz), X_) >= 1.)
+            dm[i] = dt / c->dx;
+          if (getM(c, cell(c, ix, iy + 1, iz), Y_) >= 1. ||
+              getM(c, cell(c, ix, iy - 1, iz), Y_) >= 1.)
+            dm[N + i] = dt / c->dy;
+          if (getM(c, cell(c, ix, iy, iz + 1), Z_) >= 1. ||
+              getM(c, cell(c, ix, iy, iz - 1), Z_) >= 1.)
+            dm[2 * N + i] = dt / c->dz / tau;
+          if (dm[i] == 0. && dm[N + i] == 0.) {
+            if (getMaxM(c, cell(c, ix + 1, iy + 1, iz)) >= 1. ||
+                getMaxM(c, cell(c, ix + 1, iy - 1, iz)) >= 1. ||
+                getMaxM(c, cell(c, ix - 1, iy + 1, iz)) >= 1. ||
+                getMaxM(c, cell(c, ix - 1, iy - 1, iz)) >= 1.) {
+              dm[i] = 0.707 * dt / c->dx;
+              dm[N + i] = 0.707 * dt / c->dy;
+            }
+          }
+        }
+      }
+  for (int ix = 0; ix < c->nx; ix++)
+    for (int iy = 0; iy < c->ny; iy++)
+      for (int iz = 0; iz < c->nz; iz++) {
+        const long i = cell(c, ix, iy, iz);
+        addM(c, i, X_, dm[i]);
+        addM(c, i, Y_, dm[N + i]);
+        addM(c, i, Z_, dm[2 * N + i]);
+      }
+}
+
+static double getpi(const Ctx *c, const double *a, long i, int mu, int nu) {
+  return a[(long)index44(mu, nu) * c->N + i];
+}
+
+/* Hydro::NSquant, src/hdo.cpp:381-652 (vorticity off) */
+static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
+                    double *Pi, double dmu[4][4], double *du) {
+  const double VMIN = 1e-2;
+  const double UDIFF = 3.0;
+  const double tau = c->tau, dt = c->dt;
+  double e0, e1, p, nb, nq, ns, vx1, vy1, vz1, vx0, vy0, vz0, vxH, vyH, vzH;
+  double T, mub;
+  double ut0, ux0, uy0, uz0, ut1, ux1, uy1, uz1;
+  double uuu[4];
+  const double gmunu[4][4] = {
+      {1, 0, 0, 0}, {0, -1, 0, 0}, {0, 0, -1, 0}, {0, 0, 0, -1}};
+  const long ic = cell(c, ix, iy, iz);
+  const double dx = c->dx, dy = c->dy, dz = c->dz;
+  if (getMaxM(c, cell(c, ix + 1, iy, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix, iy + 1, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix - 1, iy, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix, iy - 1, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix + 1, iy + 1, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix + 1, iy - 1, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix - 1, iy + 1, iz)) <= 0.9 ||
+      getMaxM(c, cell(c, ix - 1, iy - 1, iz)) <= 0.9) {
+    for (int i = 0; i < 4; i++)
+      for (int j = 0; j < 4; j++) {
+        pi[i][j] = 0.;
+        dmu[i][j] = 0.;
+      }
+    *Pi = *du = 0.;
+    return;
+  }
+  primCenter(c, c->s->Qprev, ic, tau - dt, &e0, &p, &nb, &nq, &ns, &vx0, &vy0,
+             &vz0);
+  primCenter(c, c->s->Q, ic, tau, &e1, &p, &nb, &nq, &ns, &vx1, &vy1, &vz1);
+  primCenter(c, c->s->Qh, ic, tau - 0.5 * dt, &e1, &p, &nb, &nq, &ns, &vxH,
+             &vyH, &vzH);
+  double etaS, zetaS;
+  double s = eos_s(c->E, e1, nb, nq, ns);
+  eos_eval(c->E, e1, nb, &T, &mub, &p);
+  etaS = tr_etaS(c->tr, e1, nb, T, mub, s, p);
+  zetaS = tr_zetaS(c->tr, e1, T, s, p);
+  ut0 = 1.0 / sqrt(1.0 - vx0 * vx0 - vy0 * vy0 - vz0 * vz0);
+  ux0 = ut0 * vx0;
+  uy0 = ut0 * vy0;
+  uz0 = ut0 * vz0;
+  ut1 = 1.0 / sqrt(1.0 - vx1 * vx1 - vy1 * vy1 - vz1 * vz1);
+  ux1 = ut1 * vx1;
+  uy1 = ut1 * vy1;
+  uz1 = ut1 * vz1;
+  uuu[0] = 1.0 / sqrt(1.0 - vxH * vxH - vyH * vyH - vzH * vzH);
+  uuu[1] = uuu[0] * vxH;
+  uuu[2] = uuu[0] * vyH;
+  uuu[3] = uuu[0] * vzH;
+
+  dmu[0][0] = (ut1 * ut1 - ut0 * ut0) / 2. / uuu[0] / dt;
+  dmu[0][1] = (ux1 * ux1 - ux0 * ux0) / 2. / uuu[1] / dt;
+  dmu[0][2] = (uy1 * uy1 - uy0 * uy0) / 2. / uuu[2] / dt;
+  dmu[0][3] = (uz1 * uz1 - uz0 * uz0) / 2. / uuu[3] / dt;
+  if (fabs(0.5 * (ut1 + ut0) / ut1) > UDIFF) dmu[0][0] = (ut1 - ut0) / dt;
+  if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / ux1) > UDIFF)
+    dmu[0][1] = (ux1 - ux0) / dt;
+  if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uy1) > UDIFF)
+    dmu[0][2] = (uy1 - uy0) / dt;
+  if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uz1) > UDIFF)
+    dmu[0][3] = (uz1 - uz0) / dt;
+  if (e1 <= 0. || e0 <= 0.) {
+    dmu[0][0] = dmu[0][1] = dmu[0][2] = dmu[0][3] = 0.;
+  }
+  /* spatial derivatives: d = 1 (x), 2 (y), 3 (eta) */
+  for (int d = 1; d <= 3; d++) {
+    long ip, im;
+    if (d == 1) {
+      ip = cell(c, ix + 1, iy, iz);
+      im = cell(c, ix - 1, iy, iz);
+    } else if (d == 2) {
+      ip = cell(c, ix, iy + 1, iz);
+      im = cell(c, ix, iy - 1, iz);
+    } else {
+      ip = cell(c, ix, iy, iz + 1);
+      im = cell(c, ix, iy, iz - 1);
+    }
+    primCenter(c, c->s->Qh, ip, tau, &e1, &p, &nb, &nq, &ns, &vx1, &vy1, &vz1);
+    primCenter(c, c->s->Qh, im, tau, &e0, &p, &nb, &nq, &ns, &vx0, &vy0, &vz0);
+    if (e1 > 0. && e0 > 0.) {
+      ut0 = 1.0 / sqrt(1.0 - vx0 * vx0 - vy0 * vy0 - vz0 * vz0);
+      ux0 = ut0 * vx0;
+      uy0 = ut0 * vy0;
+      uz0 = ut0 * vz0;
+      ut1 = 1.0 / sqrt(1.0 - vx1 * vx1 - vy1 * vy1 - vz1 * vz1);
+      ux1 = ut1 * vx1;
+      uy1 = ut1 * vy1;
+      uz1 = ut1 * vz1;
+      if (d == 1 || d == 2) {
+        const double h = (d == 1) ? dx : dy;
+        dmu[d][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / h;
+        dmu[d][1] = 0.25 * (ux1 * ux1 - ux0 * ux0) / uuu[1] / h;
+        dmu[d][2] = 0.25 * (uy1 * uy1 - uy0 * uy0) / uuu[2] / h;
+        dmu[d][3] = 0.25 * (uz1 * uz1 - uz0 * uz0) / uuu[3] / h;
+        if (fabs(0.5 * (ut1 + ut0) / uuu[0]) > UDIFF)
+          dmu[d][0] = 0.5 * (ut1 - ut0) / h;
+        if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / uuu[1]) > UDIFF)
+          dmu[d][1] = 0.5 * (ux1 - ux0) / h;
+        if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uuu[2]) > UDIFF)
+          dmu[d][2] = 0.5 * (uy1 - uy0) / h;
+        if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uuu[3]) > UDIFF)
+          dmu[d][3] = 0.5 * (uz1 - uz0) / h;
+      } else {
+        const double th = tau + 0.5 * dt;
+        dmu[3][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / dz / th;
+        dmu[3][1] = 0.25 * (ux1 * ux1 - ux0 * ux0) / uuu[1] / dz / th;
+        dmu[3][2] = 0.25 * (uy1 * uy1 - uy0 * uy0) / uuu[2] / dz / th;
+        dmu[3][3] = 0.25 * (uz1 * uz1 - uz0 * uz0) / uuu[3] / dz / th;
+        if (fabs(0.5 * (ut1 + ut0) / uuu[0]) > UDIFF)
+          dmu[3][0] = 0.5 * (ut1 - ut0) / dz / th;
+        if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / uuu[1]) > UDIFF)
+          dmu[3][1] = 0.5 * (ux1 - ux0) / dz / th;
+        if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uuu[2]) > UDIFF)
+          dmu[3][2] = 0.5 * (uy1 - uy0) / dz / th;
+        if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uuu[3]) > UDIFF)
+          dmu[3][3] = 0.5 * (uz1 - uz0) / dz / th;
+      }
+    } else {
+      dmu[d][0] = dmu[d][1] = dmu[d][2] = dmu[d][3] = 0.;
+    }
+  }
+  dmu[3][0] += uuu[3] / (tau - 0.5 * dt);
+  dmu[3][3] += uuu[0] / (tau - 0.5 * dt);
+  /* Z^{mu nu lambda rho} contraction, element by element */
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++) {
+      double acc = 0.0;
+      for (int k = 0; k < 4; k++)
+        for (int l = 0; l < 4; l++) {
+          double Z = 0.0;
+          if (j == l) Z += 0.5 * (gmunu[i][k] - uuu[i] * uuu[k]);
+          if (i == l) Z += 0.5 * (gmunu[j][k] - uuu[j] * uuu[k]);
+          if (k == l) Z -= (gmunu[i][j] - uuu[i] * uuu[j]) / 3.0;
+          acc += Z * dmu[k][l] * 2.0 * etaS * s / 5.068;
+        }
+      pi[i][j] = acc;
+    }
+  *Pi = -zetaS * s * (dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3]) / 5.068;
+  *du = dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3];
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 4; j++)
+      if (isinf(pi[i][j]) || isnan(pi[i][j])) c->err |= OR_ERR_NSQUANT_NAN;
+}
+
+/* Hydro::ISformal, src/hdo.cpp:682-963 (first-order relaxation, no
+ * FORMAL_SOLUTION, vorticity off) */
+static void ISformal(Ctx *c) {
+  const double tau = c->tau, dt = c->dt;
+  const double gmumu[4] = {1., -1., -1., -1.};
+  const long N = c->N;
+  double *pi0 = c->pi0, *piH0 = c->piH0, *Pi0 = c->Pi0, *PiH0 = c->PiH0;
+  const double *cpi = c->s->pi;
+  const double *cPi = c->s->Pi;
+#define PI(i, j) cpi[(long)index44(i, j) * N + ic]
+#define PIH0(i, j) piH0[(long)index44(i, j) * N + ic]
+#define PI0(i, j) pi0[(long)index44(i, j) * N + ic]
+  /* loop #1 */
+  for (int ix = 0; ix < c->nx; ix++)
+    for (int iy = 0; iy < c->ny; iy++)
+      for (int iz = 0; iz < c->nz; iz++) {
+        const long ic = cell(c, ix, iy, iz);
+        double e, p, nb, nq, ns, vx, vy, vz, T, mub;
+        double piNS[4][4], sigNS[4][4], PiNS, dmu[4][4], du;
+        primCenter(c, c->s->Qh, ic, tau - dt / 2., &e, &p, &nb, &nq, &ns, &vx,
+                   &vy, &vz);
+        if (e <= 0.) {
+          for (int i = 0; i < 4; i++)
+            for (int j = 0; j <= i; j++) {
+              PIH0(i, j) = 0.0;
+              PI0(i, j) = 0.0;
+            }
+          PiH0[ic] = 0.0;
+          Pi0[ic] = 0.0;
+          continue;
+        }
+        double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
+        double u[4];
+        u[0] = gamma;
+        u[1] = u[0] * vx;
+        u[2] = u[0] * vy;
+        u[3] = u[0] * vz;
+        double flux[7] = {0., 0., 0., 0., 0., 0., 0.};
+        for (int i = 0; i < 4; i++)
+          flux[i] = (tau - dt) * (PI(0, i) + cPi[ic] * u[0] * u[i]);
+        flux[0] += -(tau - dt) * cPi[ic];
+        addFlux(c, ic, flux);
+        NSquant(c, ix, iy, iz, piNS, &PiNS, dmu, &du);
+        eos_eval(c->E, e, nb, &T, &mub, &p);
+        double etaS, zetaS;
+        const double s = eos_s(c->E, e, nb, nq, ns);
+        etaS = tr_etaS(c->tr, e, nb, T, mub, s, p);
+        zetaS = tr_zetaS(c->tr, e, T, s, p);
+        (void)zetaS;
+        const double eta = etaS * s;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) {
+            sigNS[i][j] = 0.5 * piNS[i][j] / eta * 5.068;
+            if (eta <= 0.0) sigNS[i][j] = 0.0;
+          }
+        double taupi, tauPi;
+        tr_getTau(c->tr, e, nb, T, mub, s, p, &taupi, &tauPi);
+        double deltapipi, taupipi, lambdapiPi, phi7, delPiPi, lamPipi;
+        /* TransportCoeff::getOther / getOtherBulk, src/trancoeff.h:28-37 */
+        deltapipi = 4. / 3.;
+        taupipi = 10. / 7.;
+        lambdapiPi = 6. / 5.;
+        phi7 = 9. / 70. / eos_p(c->E, e, nb);
+        if (isinf(phi7)) phi7 = 0.0;
+        phi7 = phi7 / taupi;
+        if (taupi < 0.5 * dt) deltapipi = taupipi = lambdapiPi = phi7 = 0.0;
+        delPiPi = 2. / 3.;
+        lamPipi = 8. / 5. * (1. / 3. - 1. / 3.);
+        if (tauPi < 0.5 * dt) delPiPi = lamPipi = 0.0;
+        double Delta[10];
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j <= i; j++) {
+            Delta[index44(i, j)] = -u[i] * u[j];
+            if (i == j) Delta[index44(i, j)] += gmumu[i];
+            if (taupi > 0.5 * dt)
+              PIH0(i, j) = PI(i, j) - (PI(i, j) - piNS[i][j]) * dt / 2.0 /
+                                          gamma / taupi;
+            else
+              PIH0(i, j) = piNS[i][j];
+          }
+        if (tauPi > 0.5 * dt)
+          PiH0[ic] = cPi[ic] - (cPi[ic] - PiNS) * dt / 2.0 / gamma / tauPi;
+        else
+          PiH0[ic] = PiNS;
+        double tau1 = tau - dt * 0.75;
+        PIH0(0, 0) += -2. * vz * PI(0, 3) / tau1 * dt / 2.;
+        PIH0(3, 3) += -(2. * vz / tau1 * PI(0, 3)) * dt / 2.;
+        PIH0(3, 0) += -(vz / tau1 * PI(0, 0) + vz / tau1 * PI(3, 3)) * dt / 2.;
+        PIH0(1, 0) += -vz / tau1 * PI(1, 3) * dt / 2.;
+        PIH0(2, 0) += -vz / tau1 * PI(2, 3) * dt / 2.;
+        PIH0(3, 1) += -(vz / tau1 * PI(0, 1)) * dt / 2.;
+        PIH0(3, 2) += -(vz / tau1 * PI(0, 2)) * dt / 2.;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j <= i; j++) {
+            PIH0(i, j) += (-deltapipi * PI(i, j) * du +
+                           lambdapiPi * cPi[ic] * sigNS[i][j]) /
+                          gamma * 0.5 * dt;
+            for (int k = 0; k < 4; k++) {
+              PIH0(i, j) += (phi7 * PI(i, k) * PI(j, k) * gmumu[k] -
+                             taupipi * 0.5 *
+                                 (PI(i, k) * sigNS[j][k] * gmumu[k] +
+                                  PI(j, k) * sigNS[i][k] * gmumu[k])) /
+                            gamma * 0.5 * dt;
+              for (int l = 0; l < 4; l++) {
+                PIH0(i, j) +=
+                    (-PI(i, k) * u[j] - PI(j, k) * u[i]) * u[l] * dmu[l][k] *
+                        gmumu[k] / gamma * 0.5 * dt -
+                    1. / 3. * Delta[index44(i, j)] * PI(k, l) *
+                        (phi7 * PI(k, l) - taupipi * sigNS[k][l]) * gmumu[k] *
+                        gmumu[l] / gamma * 0.5 * dt;
+              }
+            }
+          }
+        for (int k = 0; k < 4; k++)
+          for (int l = 0; l < 4; l++)
+            PiH0[ic] += lamPipi * PI(k, l) * sigNS[k][l] * gmumu[k] *
+                        gmumu[l] / gamma * 0.5 * dt;
+        PiH0[ic] += -delPiPi * cPi[ic] * du / gamma * 0.5 * dt;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j <= i; j++) {
+            if (taupi > 0.5 * dt)
+              PI0(i, j) =
+                  PI(i, j) - (PIH0(i, j) - piNS[i][j]) * dt / gamma / taupi;
+            else
+              PI0(i, j) = piNS[i][j];
+          }
+        if (tauPi > 0.5 * dt)
+          Pi0[ic] = cPi[ic] - (PiH0[ic] - PiNS) * dt / gamma / tauPi;
+        else
+          Pi0[ic] = PiNS;
+        tau1 = tau - dt * 0.5;
+        PI0(0, 0) += -2. * vz / tau1 * PIH0(0, 3) * dt;
+        PI0(3, 3) += -(2. * vz / tau1 * PIH0(0, 3)) * dt;
+        PI0(3, 0) += -(vz / tau1 * PIH0(0, 0) + vz / tau1 * PIH0(3, 3)) * dt;
+        PI0(1, 0) += -vz / tau1 * PIH0(1, 3) * dt;
+        PI0(2, 0) += -vz / tau1 * PIH0(2, 3) * dt;
+        PI0(3, 1) += -(vz / tau1 * PIH0(0, 1)) * dt;
+        PI0(3, 2) += -(vz / tau1 * PIH0(0, 2)) * dt;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j <= i; j++) {
+            PI0(i, j) += (-deltapipi * PIH0(i, j) * du +
+                          lambdapiPi * PiH0[ic] * sigNS[i][j]) /
+                         gamma * dt;
+            for (int k = 0; k < 4; k++) {
+              PI0(i, j) += (phi7 * PI(i, k) * PIH0(j, k) * gmumu[k] -
+                            taupipi * 0.5 *
+                                (PIH0(i, k) * sigNS[j][k] * gmumu[k] +
+                                 PIH0(j, k) * sigNS[i][k] * gmumu[k])) /
+                           gamma * dt;
+              for (int l = 0; l < 4; l++) {
+                PI0(i, j) +=
+                    ((-PIH0(i, k) * u[j] - PIH0(j, k) * u[i]) * u[l] *
+                         dmu[l][k] * gmumu[k] -
+                     1. / 3. * Delta[index44(i, j)] * PIH0(k, l) *
+                         (phi7 * PIH0(k, l) - taupipi * sigNS[k][l]) *
+                         gmumu[k] * gmumu[l]) /
+                    gamma * dt;
+              }
+            }
+          }
+        for (int k = 0; k < 4; k++)
+          for (int l = 0; l < 4; l++)
+            Pi0[ic] += lamPipi * PIH0(k, l) * sigNS[k][l] * gmumu[k] *
+                       gmumu[l] / gamma * dt;
+        Pi0[ic] += -delPiPi * PiH0[ic] * du / gamma * dt;
+      }
+#undef PI
+#undef PIH0
+#undef PI0
+
+  /* loop #2: advection, limiter, -(tau)*delta Q_{n+1} source */
+  double *spi = c->s->pi, *spiH = c->s->piH, *sPi = c->s->Pi,
+         *sPiH = c->s->PiH;
+  for (int ix = 0; ix < c->nx; ix++)
+    for (int iy = 0; iy < c->ny; iy++)
+      for (int iz = 0; iz < c->nz; iz++) {
+        const long ic = cell(c, ix, iy, iz);
+        double e, p, nb, nq, ns, vx, vy, vz;
+        double pi[4][4], piH[4][4], Pi, PiH;
+        primCenter(c, c->s->Qh, ic, tau - 0.5 * dt, &e, &p, &nb, &nq, &ns, &vx,
+                   &vy, &vz);
+        if (e <= 0.) continue;
+        double xm = -vx * dt / c->dx;
+        double ym = -vy * dt / c->dy;
+        double zm = -vz * dt / c->dz / (tau - 0.5 * dt);
+        double xmH = -vx * dt / c->dx / 2.0;
+        double ymH = -vy * dt / c->dy / 2.0;
+        double zmH = -vz * dt / c->dz / (tau - 0.5 * dt) / 2.0;
+        double wx[2] = {(1. - fabs(xm)), fabs(xm)};
+        double wy[2] = {(1. - fabs(ym)), fabs(ym)};
+        double wz[2] = {(1. - fabs(zm)), fabs(zm)};
+        double wxH[2] = {(1. - fabs(xmH)), fabs(xmH)};
+        double wyH[2] = {(1. - fabs(ymH)), fabs(ymH)};
+        double wzH[2] = {(1. - fabs(zmH)), fabs(zmH)};
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++) pi[i][j] = piH[i][j] = 0.0;
+        Pi = PiH = 0.0;
+        for (int jx = 0; jx < 2; jx++)
+          for (int jy = 0; jy < 2; jy++)
+            for (int jz = 0; jz < 2; jz++) {
+              const long c1 =
+                  cell(c, (int)(ix + jx * sgn(xm)), (int)(iy + jy * sgn(ym)),
+                       (int)(iz + jz * sgn(zm)));
+              for (int i = 0; i < 4; i++)
+                for (int j = 0; j < 4; j++) {
+                  pi[i][j] += wx[jx] * wy[jy] * wz[jz] *
+                              pi0[(long)index44(i, j) * N + c1];
+                  piH[i][j] += wxH[jx] * wyH[jy] * wzH[jz] *
+                               piH0[(long)index44(i, j) * N + c1];
+                }
+              Pi += wx[jx] * wy[jy] * wz[jz] * Pi0[c1];
+              PiH += wxH[jx] * wyH[jy] * wzH[jz] * PiH0[c1];
+            }
+        double maxT0 = smax((e + p) / (1. - vx * vx - vy * vy - vz * vz) - p,
+                            (e + p) * (vx * vx + vy * vy + vz * vz) /
+                                    (1. - vx * vx - vy * vy - vz * vz) +
+                                p);
+        double maxpi = 0.;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j < 4; j++)
+            if (fabs(pi[i][j]) > maxpi) maxpi = fabs(pi[i][j]);
+        int rescaled = 0;
+        if (maxT0 / maxpi < 1.0) {
+          for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++) {
+              pi[i][j] = 0.1 * pi[i][j] * maxT0 / maxpi;
+              piH[i][j] = 0.1 * piH[i][j] * maxT0 / maxpi;
+            }
+          rescaled = 1;
+        }
+        if (fabs(Pi) > p) {
+          if (Pi != 0.) Pi = 1 * Pi / fabs(Pi) * p;
+          if (PiH != 0.) PiH = 1 * PiH / fabs(PiH) * p;
+          rescaled = 1;
+        }
+        c->s->vcc[ic] = rescaled ? maxT0 / maxpi : 1.;
+        for (int i = 0; i < 4; i++)
+          for (int j = 0; j <= i; j++) {
+            spi[(long)index44(i, j) * N + ic] = pi[i][j];
+            spiH[(long)index44(i, j) * N + ic] = piH[i][j];
+          }
+        sPi[ic] = Pi;
+        sPiH[ic] = PiH;
+        double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
+        double u[4];
+        u[0] = gamma;
+        u[1] = u[0] * vx;
+        u[2] = u[0] * vy;
+        u[3] = u[0] * vz;
+        double flux[7] = {0., 0., 0., 0., 0., 0., 0.};
+        for (int i = 0; i < 4; i++)
+          flux[i] = -tau * (getpi(c, spi, ic, 0, i) + sPi[ic] * u[0] * u[i]);
+        flux[0] += tau * sPi[ic];
+        addFlux(c, ic, flux);
+      }
+}
+
+/* Hydro::visc_flux, src/hdo.cpp:966-1014 */
+static void visc_flux(Ctx *c, long L, long R, int direction) {
+  const double tau = c->tau, dt = c->dt;
+  double flux[4];
+  int ind2 = 0;
+  double dxa = 0.;
+  if (getM(c, L, direction) < 1. && getM(c, R, direction) < 1.) return;
+  if (direction == X_)
+    dxa = c->dx;
+  else if (direction == Y_)
+    dxa = c->dy;
+  else if (direction == Z_)
+    dxa = c->dz * (tau + 0.5 * dt);
+  double e, p, nb, nq, ns, vxl, vyl, vzl, vxr, vyr, vzr;
+  primCenter(c, c->s->Qh, L, tau - dt / 2., &e, &p, &nb, &nq, &ns, &vxl, &vyl,
+             &vzl);
+  primCenter(c, c->s->Qh, R, tau - dt / 2., &e, &p, &nb, &nq, &ns, &vxr, &vyr,
+             &vzr);
+  vxl = 0.5 * (vxl + vxr);
+  vyl = 0.5 * (vyl + vyr);
+  vzl = 0.5 * (vzl + vzr);
+  double v = sqrt(vxl * vxl + vyl * vyl + vzl * vzl);
+  if (v > 1.) {
+    vxl = 0.99 * vxl / v;
+    vyl = 0.99 * vyl / v;
+    vzl = 0.99 * vzl / v;
+  }
+  double gamma = 1. / sqrt(1. - v * v);
+  double uuu[4] = {gamma, gamma * vxl, gamma * vyl, gamma * vzl};
+  const double gmumu[4] = {1., -1., -1., -1.};
+  ind2 = direction;
+  const double *piH = c->s->piH, *PiH = c->s->PiH;
+  for (int ind1 = 0; ind1 < 4; ind1++) {
+    flux[ind1] = 0.5 * (getpi(c, piH, L, ind1, ind2) + getpi(c, piH, R, ind1, ind2));
+    if (ind1 == ind2) flux[ind1] += -0.5 * (PiH[L] + PiH[R]) * gmumu[ind1];
+    flux[ind1] += 0.5 * (PiH[L] + PiH[R]) * uuu[ind1] * uuu[ind2];
+  }
+  for (int i = 0; i < 4; i++) flux[i] = flux[i] * (tau - 0.5 * dt) * dt / dxa;
+  double fl[7] = {-flux[0], -flux[1], -flux[2], -flux[3], 0., 0., 0.};
+  double fr[7] = {flux[0], flux[1], flux[2], flux[3], 0., 0., 0.};
+  addFlux(c, L, fl);
+  addFlux(c, R, fr);
+}
+
+/* Hydro::visc_source_step, src/hdo.cpp:355-375 */
+static void visc_source_step(Ctx *c, long i) {
+  const double tau = c->tau, dt = c->dt;
+  double e, p, nb, nq, ns, vx, vy, vz, uuu[4], k[7];
+  primCenter(c, c->s->Qh, i, tau - dt / 2., &e, &p, &nb, &nq, &ns, &vx, &vy,
+             &vz);
+  if (e <= 0.) return;
+  uuu[0] = 1. / sqrt(1. - vx * vx - vy * vy - vz * vz);
+  uuu[1] = uuu[0] * vx;
+  uuu[2] = uuu[0] * vy;
+  uuu[3] = uuu[0] * vz;
+  const double piH33 = getpi(c, c->s->piH, i, 3, 3);
+  const double piH03 = getpi(c, c->s->piH, i, 0, 3);
+  const double PiH = c->s->PiH[i];
+  k[T_] = -piH33 + PiH * (-1.0 - uuu[3] * uuu[3]);
+  k[X_] = 0.;
+  k[Y_] = 0.;
+  k[Z_] = -(piH03 + PiH * uuu[0] * uuu[3]);
+  for (int j = 0; j < 4; j++) k[j] *= dt;
+  k[NB_] = k[NQ_] = k[NS_] = 0.;
+  addFlux(c, i, k);
+}
+
+/* Cell::updateByViscFlux, src/cll.cpp:76-84 */
+static void updateByViscFlux(Ctx *c, long i) {
+  double *Q = c->s->Q;
+  const double q0 = F(Q, 0, i), f0 = F(c->flux, 0, i);
+  if (fabs(f0) <= 0.5 * q0) {
+    for (int k = 0; k < 7; k++) F(Q, k, i) += F(c->flux, k, i);
+  } else if (f0 != 0.) {
+    const double fac = fabs(0.5 * q0 / f0);
+    for (int k = 0; k < 7; k++) F(Q, k, i) += fac * F(c->flux, k, i);
+  }
+}
+
+static void clearFlux(Ctx *c, long i) {
+  for (int k = 0; k < 7; k++) F(c->flux, k, i) = 0.;
+}
+
+/* Hydro::performStep, src/hdo.cpp:1016-1134 */
+int or_step(const or_grid *g, const or_eos *eos, const or_trc *tr,
+            or_state *s, double *tau, double dt) {
+  Ctx cx;
+  Ctx *c = &cx;
+  memset(c, 0, sizeof(*c));
+  c->g = g;
+  c->E = eos;
+  c->tr = tr;
+  c->s = s;
+  c->nx = g->nx;
+  c->ny = g->ny;
+  c->nz = g->nz;
+  c->N = (long)g->nx * g->ny * g->nz;
+  c->dx = (g->xmax - g->xmin) / (g->nx - 1);
+  c->dy = (g->ymax - g->ymin) / (g->ny - 1);
+  c->dz = (g->zmax - g->zmin) / (g->nz - 1);
+  c->tau = *tau;
+  c->dt = dt;
+  const long N = c->N;
+  c->flux = (double *)calloc((size_t)(7 * N), sizeof(double));
+  c->dm = (double *)calloc((size_t)(3 * N), sizeof(double));
+  c->pi0 = (double *)calloc((size_t)(10 * N), sizeof(double));
+  c->piH0 = (double *)calloc((size_t)(10 * N), sizeof(double));
+  c->Pi0 = (double *)calloc((size_t)N, sizeof(double));
+  c->PiH0 = (double *)calloc((size_t)N, sizeof(double));
+  const int nx = c->nx, ny = c->ny, nz = c->nz;
+
+  updateM(c, c->tau, dt);
+
+  /* predictor */
+  for (long i = 0; i < N; i++) {
+    for (int k = 0; k < 7; k++) F(s->Qprev, k, i) = F(s->Q, k, i);
+    clearFlux(c, i);
+  }
+  for (int mode = PREDICT; mode <= CORRECT; mode++) {
+    for (int iy = 0; iy < ny; iy++)
+      for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx - 1; ix++)
+          hlle_flux(c, cell(c, ix, iy, iz), cell(c, ix + 1, iy, iz), X_, mode);
+    for (int iz = 0; iz < nz; iz++)
+      for (int ix = 0; ix < nx; ix++)
+        for (int iy = 0; iy < ny - 1; iy++)
+          hlle_flux(c, cell(c, ix, iy, iz), cell(c, ix, iy + 1, iz), Y_, mode);
+    for (int ix = 0; ix < nx; ix++)
+      for (int iy = 0; iy < ny; iy++)
+        for (int iz = 0; iz < nz - 1; iz++)
+          hlle_flux(c, cell(c, ix, iy, iz), cell(c, ix, iy, iz + 1), Z_, mode);
+    for (int iy = 0; iy < ny; iy++)
+      for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++) {
+          const long i = cell(c, ix, iy, iz);
+          source_step(c, i, mode);
+          if (mode == PREDICT) {
+            /* Cell::updateQtoQhByFlux, src/cll.cpp:86-88 */
+            for (int k = 0; k < 7; k++)
+              F(s->Qh, k, i) = F(s->Q, k, i) + F(c->flux, k, i);
+          } else {
+            /* Cell::updateByFlux, src/cll.cpp:70-74 */
+            if (!(F(s->Q, 0, i) + F(c->flux, 0, i) < 0.))
+              for (int k = 0; k < 7; k++) F(s->Q, k, i) += F(c->flux, k, i);
+          }
+          clearFlux(c, i);
+        }
+  }
+  c->tau += dt;
+  correctImagCells(c, 0);
+
+  if (tr_isViscous(tr)) {
+    ISformal(c);
+    for (int iy = 0; iy < ny; iy++)
+      for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx - 1; ix++)
+          visc_flux(c, cell(c, ix, iy, iz), cell(c, ix + 1, iy, iz), X_);
+    for (int iz = 0; iz < nz; iz++)
+      for (int ix = 0; ix < nx; ix++)
+        for (int iy = 0; iy < ny - 1; iy++)
+          visc_flux(c, cell(c, ix, iy, iz), cell(c, ix, iy + 1, iz), Y_);
+    for (int ix = 0; ix < nx; ix++)
+      for (int iy = 0; iy < ny; iy++)
+        for (int iz = 0; iz < nz - 1; iz++)
+          visc_flux(c, cell(c, ix, iy, iz), cell(c, ix, iy, iz + 1), Z_);
+    for (int iy = 0; iy < ny; iy++)
+      for (int iz = 0; iz < nz; iz++)
+        for (int ix = 0; ix < nx; ix++) {
+          const long i = cell(c, ix, iy, iz);
+          visc_source_step(c, i);
+          updateByViscFlux(c, i);
+          clearFlux(c, i);
+        }
+  }
+  correctImagCells(c, 1);
+  *tau = c->tau;
+  free(c->flux);
+  free(c->dm);
+  free(c->pi0);
+  free(c->piH0);
+  free(c->Pi0);
+  free(c->PiH0);
+  return c->err;
+}
+
+/* ----------------------------------------------------- test entry points */
+
+void or_transform_pv(const or_eos *eos, const double *Q, int n, double *out) {
+  for (int i = 0; i < n; i++) {
+    double q[7];
+    for (int k = 0; k < 7; k++) q[k] = Q[7 * i + k];
+    double *o = out + 8 * i;
+    transform_pv(eos, q, &o[0], &o[1], &o[2], &o[3], &o[4], &o[5], &o[6], &o[7]);
+  }
+}
+
+void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
+                 double *out) {
+  for (int i = 0; i < n; i++) {
+    double T, mub, p;
+    eos_eval(eos, e[i], nb[i], &T, &mub, &p);
+    out[3 * i] = p;
+    out[3 * i + 1] = T;
+    out[3 * i + 2] = mub;
+  }
+}
+
+void or_eos_s(const or_eos *eos, const double *e, const double *nb, int n,
+              double *out) {
+  for (int i = 0; i < n; i++) out[i] = eos_s(eos, e[i], nb[i], 0., 0.);
+}
+
+void or_update_m(const or_grid *g, double *m, double tau, double dt) {
+  Ctx cx;
+  memset(&cx, 0, sizeof(cx));
+  or_state st;
+  memset(&st, 0, sizeof(st));
+  st.m = m;
+  cx.g = g;
+  cx.s = &st;
+  cx.nx = g->nx;
+  cx.ny = g->ny;
+  cx.nz = g->nz;
+  cx.N = (long)g->nx * g->ny * g->nz;
+  cx.dx = (g->xmax - g->xmin) / (g->nx - 1);
+  cx.dy = (g->ymax - g->ymin) / (g->ny - 1);
+  cx.dz = (g->zmax - g->zmin) / (g->nz - 1);
+  cx.dm = (double *)calloc((size_t)(3 * cx.N), sizeof(double));
+  updateM(&cx, tau, dt);
+  free(cx.dm);
+}

@@ -1,0 +1,92 @@
+/*
+ * vh_oracle.h -- CPU oracle for the vHLLE per-timestep hydro update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C, single-threaded restatement
+ * of the reference's Hydro::performStep (src/hdo.cpp:1016-1134) and of the
+ * functions it calls, written over structure-of-arrays state.  It exists so
+ * that tests, the smoke check and the CPU-baseline leg of the benchmark can
+ * check the CUDA path; the product never links, loads or calls it.
+ *
+ * Parity pin: the restatement is compared bit-for-bit against the reference
+ * C++ sources themselves, compiled unmodified into oracle/_ref by
+ * oracle/Makefile (see tests/test_oracle_vs_ref.py), and against the golden
+ * fixtures in tests/golden/ that the compiled reference generated.
+ *
+ * Layout: every field is component-major, field[c * N + i] with
+ * i = ix + nx * (iy + ny * iz) (x fastest, as Fluid::getCell, src/fld.h:70-78).
+ * The 10 stored pi^{mu nu} components follow index44 (src/cll.cpp:22-31):
+ * (0,0)=0 (1,0)=1 (1,1)=2 (2,0)=3 (2,1)=4 (2,2)=5 (3,0)=6 (3,1)=7 (3,2)=8 (3,3)=9.
+ */
+#ifndef VH_ORACLE_H
+#define VH_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_grid {
+  int nx, ny, nz;
+  double xmin, xmax, ymin, ymax, zmin, zmax; /* zmin/zmax = eta range */
+} or_grid;
+
+/* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)
+ * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb] */
+typedef struct or_eos {
+  int kind;
+  double conf_cnst;
+  int ne, nn;
+  const double *egrid, *ngrid, *p, *T, *mub;
+} or_eos;
+
+/* TransportCoeff (src/trancoeff.h:6-45) public constants */
+typedef struct or_trc {
+  double etaS0, zetaS0, ah, al, aRho, T0, etaSMin, etaSEpsilonMin,
+      etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
+      zetaSSigmaMinus, zetaSSigmaPlus;
+  int etaSparam, zetaSparam;
+} or_trc;
+
+/* Persistent + inspected cell fields (all caller-owned, component-major). */
+typedef struct or_state {
+  double *Q;     /* [7][N]  tau-weighted conserved T^{0mu}, J^0 */
+  double *Qh;    /* [7][N]  half-step values                   */
+  double *Qprev; /* [7][N]  values at the start of the step    */
+  double *pi;    /* [10][N] pi^{mu nu}                          */
+  double *piH;   /* [10][N] half-step pi^{mu nu}                */
+  double *Pi;    /* [N]     bulk pressure                        */
+  double *PiH;   /* [N]                                          */
+  double *m;     /* [3][N]  matter fill fraction per direction   */
+  double *vcc;   /* [N]     viscCorrCut flag                      */
+} or_state;
+
+/* error bits returned by or_step (the reference calls exit() on these) */
+#define OR_ERR_E_HUGE 1      /* e > 1e10 in hlle_flux, src/hdo.cpp:118-130 */
+#define OR_ERR_FLUX_NAN 2    /* src/hdo.cpp:285-298 */
+#define OR_ERR_SOURCE_NAN 4  /* src/hdo.cpp:345-351 */
+#define OR_ERR_NSQUANT_NAN 8 /* src/hdo.cpp:643-651 */
+
+/* One Hydro::performStep.  *tau advances by dt.  Returns error bits. */
+int or_step(const or_grid *g, const or_eos *eos, const or_trc *tr,
+            or_state *s, double *tau, double dt);
+
+/* transformPV (src/rmn.cpp:28-139) on n states Q[n][7] (row-major);
+ * out[n][8] = e, p, nb, nq, ns, vx, vy, vz.  Q is not modified. */
+void or_transform_pv(const or_eos *eos, const double *Q, int n, double *out);
+
+/* EoS::eos for n points; out[n][3] = p, T, mub. */
+void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
+                 double *out);
+
+/* EoS::s for n points (nq = ns = 0). */
+void or_eos_s(const or_eos *eos, const double *e, const double *nb, int n,
+              double *out);
+
+/* Fluid::updateM (src/fld.cpp:384-423) alone, for unit tests. */
+void or_update_m(const or_grid *g, double *m, double tau, double dt);
+
+int or_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,344 @@
+"""Seeded synthetic inputs for the hydro step: grids, EoS tables, initial states.
+
+Everything here runs once on the host, off the timed path.  The same FP64
+arrays are handed to the CUDA path and to the CPU checkers, so the initial
+state never has to be reproduced bit-for-bit by two implementations.
+
+Workloads (sizes and physics as the benchmark configurations state them):
+  * ``gubser``   Gubser flow, ideal, conformal EoS, 101x101x1 on [-5,5]^2,
+                 tau0 = 1, dtau = 0.025.  The initial state follows the
+                 reference's analytic Gubser IC (src/icGubser.cpp:17-62:
+                 q = 1, t = 1, e = (...)^(4/3), transverse flow k(r)).
+  * ``glauber3d`` 3D viscous single event, 101x101x51 on [-15,15]^2 x
+                 [-7.5,7.5], tau0 = 0.5, dtau = 0.05, eta/s = 0.08,
+                 zeta/s = 0, 2000-point log e-table from
+                 c_s^2(e) = 1/3 - 0.18 exp(-(ln(e/0.45))^2/1.5); seeded
+                 Monte-Carlo Glauber Pb+Pb (WS R = 6.62, a = 0.546, b = 7,
+                 sigma_NN = 6.4 fm^2, 0.4 fm smearing, peak e = 50 GeV/fm^3,
+                 plateau |eta_s| < 2.5 with Gaussian tails of width 1.0).
+  Smaller grids of the same physics are produced with ``scale_grid``.
+
+The reference publishes no input files for these workloads (its data
+repository is separate), so seeded synthetic inputs stand in for them.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional
+
+import numpy as np
+
+HBARC = 0.1973269804  # GeV fm
+# conformal gas with g = 16 + 31.5 (src/eos.cpp:12 uses the same degeneracy)
+CONF_DEG = 16.0 + 3.0 * 12.0 * (7.0 / 8.0)
+CONF_CNST = 3.0 * CONF_DEG * math.pi ** 2 / 90.0 / HBARC ** 3  # e = cnst T^4
+
+# transport-coefficient parameter order of TransportCoeff's constructor
+# (src/trancoeff.h:14-20)
+TR_FIELDS = ("etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin",
+             "etaSEpsilonMin", "etaSShiftMuB", "etaSScaleMuB",
+             "zetaSPeakEpsilon", "zetaSScaleBeta", "zetaSSigmaMinus",
+             "zetaSSigmaPlus")
+# defaults of the reference driver (src/main.cpp:70-78)
+TR_DEFAULTS = dict(etaS0=0.08, zetaS0=0.0, ah=0.0, al=0.0, aRho=0.0, T0=0.15,
+                   etaSMin=0.08, etaSEpsilonMin=5.0, etaSShiftMuB=0.0,
+                   etaSScaleMuB=0.0, zetaSPeakEpsilon=5.0,
+                   zetaSScaleBeta=0.103, zetaSSigmaMinus=0.1,
+                   zetaSSigmaPlus=0.1)
+
+
+@dataclasses.dataclass
+class Grid:
+    nx: int
+    ny: int
+    nz: int
+    xmin: float
+    xmax: float
+    ymin: float
+    ymax: float
+    etamin: float
+    etamax: float
+
+    @property
+    def ncells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def dx(self) -> float:  # src/fld.cpp:77-79
+        return (self.xmax - self.xmin) / (self.nx - 1)
+
+    @property
+    def dy(self) -> float:
+        return (self.ymax - self.ymin) / (self.ny - 1)
+
+    @property
+    def dz(self) -> float:
+        # nz = 1 gives an infinite cell, as the reference's FP64 division does
+        span = self.etamax - self.etamin
+        if self.nz == 1:
+            return math.copysign(math.inf, span) if span != 0 else math.nan
+        return span / (self.nz - 1)
+
+    def bounds(self):
+        return (self.xmin, self.xmax, self.ymin, self.ymax, self.etamin,
+                self.etamax)
+
+    def coords(self):
+        """Cell-centre coordinates x[ix], y[iy], eta[iz] (Fluid::getX etc.)."""
+        ix = np.arange(self.nx)
+        iy = np.arange(self.ny)
+        iz = np.arange(self.nz)
+        with np.errstate(invalid="ignore"):
+            return (self.xmin + ix * self.dx, self.ymin + iy * self.dy,
+                    self.etamin + iz * self.dz)
+
+
+@dataclasses.dataclass
+class EosTable:
+    """EoS descriptor.  kind 0: conformal gas; kind 1: EoS1f (e, nb) table
+    with p/T/mub stored [ie + ne*inb] (src/eo1.cpp:21-45)."""
+    kind: int
+    conf_cnst: float = CONF_CNST
+    egrid: Optional[np.ndarray] = None
+    ngrid: Optional[np.ndarray] = None
+    p: Optional[np.ndarray] = None
+    T: Optional[np.ndarray] = None
+    mub: Optional[np.ndarray] = None
+
+    @property
+    def ne(self) -> int:
+        return 0 if self.egrid is None else len(self.egrid)
+
+    @property
+    def nn(self) -> int:
+        return 0 if self.ngrid is None else len(self.ngrid)
+
+    def write_eos1f(self, path: str) -> None:
+        """Write the table in the reference's EoS1f text format: header
+        ``emax e0 nmax n0 ne nn``, the e grid, the n grid, then ``p T mub``
+        rows with ie outer and inb inner (src/eo1.cpp:24-43).  Values are
+        written with 17 significant digits so that they read back exactly."""
+        assert self.kind == 1
+        ne, nn = self.ne, self.nn
+        with open(path, "w") as f:
+            f.write("%r %r %r %r %d %d\n" % (float(self.egrid[-1]), float(self.egrid[0]),
+                                            float(self.ngrid[-1]), float(self.ngrid[0]), ne, nn))
+            f.write(" ".join(repr(float(v)) for v in self.egrid) + "\n")
+            f.write(" ".join(repr(float(v)) for v in self.ngrid) + "\n")
+            for ie in range(ne):
+                for inb in range(nn):
+                    k = ie + ne * inb
+                    f.write("%r %r %r\n" % (float(self.p[k]), float(self.T[k]), float(self.mub[k])))
+
+    @staticmethod
+    def read_eos1f(path: str) -> "EosTable":
+        """Parse an EoS1f file the way the reference constructor does; values
+        below 1e-18 in the pressure column read as 0 (src/eo1.cpp:42)."""
+        with open(path) as f:
+            tok = f.read().split()
+        emax, e0, nmax, n0 = (float(t) for t in tok[:4])
+        ne, nn = int(tok[4]), int(tok[5])
+        pos = 6
+        egrid = np.array([float(t) for t in tok[pos:pos + ne]]); pos += ne
+        ngrid = np.array([float(t) for t in tok[pos:pos + nn]]); pos += nn
+        p = np.zeros(ne * nn); T = np.zeros(ne * nn); mub = np.zeros(ne * nn)
+        for ie in range(ne):
+            for inb in range(nn):
+                k = ie + ne * inb
+                p[k] = float(tok[pos]); T[k] = float(tok[pos + 1]); mub[k] = float(tok[pos + 2])
+                if p[k] < 1e-18:
+                    p[k] = 0.0
+                pos += 3
+        return EosTable(kind=1, egrid=egrid, ngrid=ngrid, p=p, T=T, mub=mub)
+
+
+def cs2_model(e):
+    """c_s^2(e) = 1/3 - 0.18 exp(-(ln(e/0.45))^2/1.5) of the 3D workloads."""
+    e = np.asarray(e, dtype=np.float64)
+    return 1.0 / 3.0 - 0.18 * np.exp(-np.log(e / 0.45) ** 2 / 1.5)
+
+
+def make_cs2_table(ne: int = 2000, emin: float = 1e-4, emax: float = 1e3,
+                   nn: int = 2, nbmax: float = 1.0, mub_slope: float = 0.0,
+                   sub: int = 64) -> EosTable:
+    """Log-spaced e-table with p and T integrated consistently from c_s^2(e).
+
+    p(e) = p(emin) + int c_s^2 de with p(emin) = emin/3 (conformal at the low
+    end, where c_s^2 -> 1/3), and d ln T = dp/(e+p) at mu_B = 0, anchored to
+    the Stefan-Boltzmann gas of CONF_DEG degrees of freedom at emax.  The nb
+    axis has ``nn`` points on [0, nbmax]; for nn = 2 and mub_slope = 0 the
+    table is nb independent (the reference's EoS1f needs nn >= 2).  A nonzero
+    ``mub_slope`` adds mu_B = mub_slope * nb (GeV per fm^-3) and the matching
+    first-order pressure shift dp = nb * mu_B / 2 (thermodynamically
+    consistent to that order)."""
+    egrid = np.exp(np.linspace(math.log(emin), math.log(emax), ne))
+    # fine composite Simpson integration between grid points
+    p = np.empty(ne)
+    lnT_rel = np.empty(ne)
+    p[0] = emin / 3.0
+    lnT_rel[0] = 0.0
+    for i in range(1, ne):
+        a, b = egrid[i - 1], egrid[i]
+        xs = np.linspace(a, b, 2 * sub + 1)
+        w = np.ones_like(xs); w[1:-1:2] = 4.0; w[2:-1:2] = 2.0
+        h = (b - a) / (2 * sub)
+        cs = cs2_model(xs)
+        pseg = p[i - 1] + np.concatenate(([0.0], np.cumsum((cs[1:] + cs[:-1]) * 0.5 * np.diff(xs))))
+        p[i] = p[i - 1] + h / 3.0 * np.sum(w * cs)
+        lnT_rel[i] = lnT_rel[i - 1] + h / 3.0 * np.sum(w * cs / (xs + pseg))
+    T_top = (emax / CONF_CNST) ** 0.25
+    T = T_top * np.exp(lnT_rel - lnT_rel[-1])
+    ngrid = np.linspace(0.0, nbmax, nn)
+    P = np.empty(ne * nn); TT = np.empty(ne * nn); MU = np.empty(ne * nn)
+    for inb in range(nn):
+        nb = ngrid[inb]
+        mu = mub_slope * nb
+        P[inb * ne:(inb + 1) * ne] = p + 0.5 * nb * mu
+        TT[inb * ne:(inb + 1) * ne] = T
+        MU[inb * ne:(inb + 1) * ne] = mu
+    return EosTable(kind=1, egrid=egrid, ngrid=ngrid, p=P, T=TT, mub=MU)
+
+
+@dataclasses.dataclass
+class Setup:
+    """One hydro problem: grid, EoS, transport, clock and initial state."""
+    name: str
+    grid: Grid
+    eos: EosTable
+    tr: dict
+    etaSparam: int
+    zetaSparam: int
+    tau0: float
+    dt: float
+    ecrit: float
+    Q: np.ndarray          # [7][N] tau-weighted conserved variables
+    m: np.ndarray          # [N] initial fill fraction (setAllM value)
+    pi: Optional[np.ndarray] = None   # [10][N]
+    Pi: Optional[np.ndarray] = None   # [N]
+
+    @property
+    def viscous(self) -> bool:  # TransportCoeff::isViscous, src/trancoeff.h:39-45
+        t = self.tr
+        return (t["etaS0"] > 0 or t["zetaS0"] > 0 or self.etaSparam > 0
+                or self.zetaSparam > 0)
+
+    def tr_vector(self):
+        return [float(self.tr[k]) for k in TR_FIELDS]
+
+
+def conserved_from_primitive(tau, e, p, nb, vx, vy, vz):
+    """Cell::setPrimVar arithmetic (src/cll.cpp:222-241) on arrays."""
+    gamma2 = 1.0 / (1 - vx * vx - vy * vy - vz * vz)
+    v2 = vx * vx + vy * vy + vz * vz
+    Q = np.zeros((7,) + np.shape(e))
+    Q[0] = tau * (e + p * v2) * gamma2
+    Q[1] = tau * (e + p) * vx * gamma2
+    Q[2] = tau * (e + p) * vy * gamma2
+    Q[3] = tau * (e + p) * vz * gamma2
+    Q[4] = tau * nb * np.sqrt(gamma2)
+    return Q
+
+
+def gubser_setup(nx: int = 101, ny: int = 101, xmax: float = 5.0,
+                 tau0: float = 1.0, dt: float = 0.025) -> Setup:
+    """Gubser flow initial state on an nz = 1 grid (eta in [-0.5, 0.5], so
+    that dz is finite), following src/icGubser.cpp:24-57."""
+    g = Grid(nx, ny, 1, -xmax, xmax, -xmax, xmax, -0.5, 0.5)
+    x, y, _ = g.coords()
+    X, Y = np.meshgrid(x, y, indexing="xy")  # [iy][ix]
+    t, q = 1.0, 1.0
+    r = np.sqrt(X * X + Y * Y)
+    k = 2. * q * q * t * r / (1. + q * q * t * t + q * q * r * r)
+    e = 4. * q * q / (1. + 2. * q * q * (t * t + r * r) + (q * q * (t * t - r * r)) ** 2) / t
+    e = np.where(e < 0., 0., e)
+    e = e ** (4. / 3.)
+    vx = X / (r + 1e-50) * k
+    vy = Y / (r + 1e-50) * k
+    vz = np.zeros_like(e)
+    nb = np.zeros_like(e)
+    p = e / 3.
+    Q = conserved_from_primitive(tau0, e, p, nb, vx, vy, vz).reshape(7, -1)
+    m = (e.reshape(-1) > 0).astype(np.float64)
+    tr = dict(TR_DEFAULTS, etaS0=0.0, etaSMin=0.0)
+    return Setup("gubser", g, EosTable(kind=0), tr, 0, 0, tau0, dt, 0.5, Q, m)
+
+
+def _woods_saxon(rng, A, R, a):
+    out = np.empty((A, 3))
+    n = 0
+    rmax = R + 10 * a
+    while n < A:
+        r = rng.uniform(0, rmax, size=4 * A)
+        acc = rng.uniform(0, 1, size=4 * A) < (r * r / (rmax * rmax)) / (1 + np.exp((r - R) / a))
+        r = r[acc]
+        cth = rng.uniform(-1, 1, size=r.size)
+        ph = rng.uniform(0, 2 * math.pi, size=r.size)
+        sth = np.sqrt(1 - cth * cth)
+        pts = np.stack([r * sth * np.cos(ph), r * sth * np.sin(ph), r * cth], 1)
+        take = min(A - n, len(pts))
+        out[n:n + take] = pts[:take]
+        n += take
+    return out
+
+
+def glauber_profile(seed: int, b: float, x: np.ndarray, y: np.ndarray,
+                    A: int = 208, R: float = 6.62, a: float = 0.546,
+                    sigma_nn: float = 6.4, smear: float = 0.4):
+    """Participant density of one seeded MC-Glauber event on the (x, y) grid,
+    normalised to a maximum of 1; returns (profile[iy][ix], n_participants)."""
+    rng = np.random.default_rng(seed)
+    na = _woods_saxon(rng, A, R, a)
+    nbn = _woods_saxon(rng, A, R, a)
+    na[:, 0] += b / 2
+    nbn[:, 0] -= b / 2
+    d2 = ((na[:, None, 0] - nbn[None, :, 0]) ** 2 + (na[:, None, 1] - nbn[None, :, 1]) ** 2)
+    hit = d2 < sigma_nn / math.pi
+    parts = np.concatenate([na[hit.any(1), :2], nbn[hit.any(0), :2]], 0)
+    X, Y = np.meshgrid(x, y, indexing="xy")
+    prof = np.zeros_like(X)
+    for px, py in parts:
+        prof += np.exp(-((X - px) ** 2 + (Y - py) ** 2) / (2 * smear * smear))
+    if prof.max() > 0:
+        prof /= prof.max()
+    return prof, len(parts)
+
+
+def eta_profile(eta, plateau=2.5, width=1.0):
+    ae = np.abs(eta)
+    return np.where(ae < plateau, 1.0, np.exp(-(ae - plateau) ** 2 / (2 * width * width)))
+
+
+def glauber3d_setup(nx: int = 101, ny: int = 101, nz: int = 51,
+                    xmax: float = 15.0, etamax: float = 7.5,
+                    tau0: float = 0.5, dt: float = 0.05, seed: int = 20260001,
+                    b: float = 7.0, epeak: float = 50.0, etaS: float = 0.08,
+                    eos: Optional[EosTable] = None, ecut: float = 1e-3,
+                    nb_peak: float = 0.0) -> Setup:
+    """3D viscous single event (seeded MC-Glauber).  Cells whose energy
+    density falls below ``ecut`` GeV/fm^3 start as vacuum (e = 0, m = 0), so
+    the vacuum-front machinery (Fluid::updateM) is exercised as in real runs."""
+    g = Grid(nx, ny, nz, -xmax, xmax, -xmax, xmax, -etamax, etamax)
+    x, y, eta = g.coords()
+    prof, _ = glauber_profile(seed, b, x, y)
+    H = eta_profile(eta)
+    e = epeak * H[:, None, None] * prof[None, :, :]  # [iz][iy][ix]
+    e = np.where(e < ecut, 0.0, e)
+    nb = nb_peak * H[:, None, None] * prof[None, :, :]
+    nb = np.where(e > 0, nb, 0.0)
+    zero = np.zeros_like(e)
+    if eos is None:
+        eos = make_cs2_table()
+    # v = 0: Q_T = tau e and Q_NB = tau nb, independent of p
+    Q = conserved_from_primitive(tau0, e, zero, nb, zero, zero, zero).reshape(7, -1)
+    m = (e.reshape(-1) > 0).astype(np.float64)
+    tr = dict(TR_DEFAULTS, etaS0=etaS, zetaS0=0.0)
+    return Setup("glauber3d", g, eos, tr, 0, 0, tau0, dt, 0.5, Q, m)
+
+
+def small_glauber3d(n: int = 17, nz: int = 9, seed: int = 20260001, **kw) -> Setup:
+    """The 3D viscous physics on a reduced grid that the CPU checkers finish
+    in seconds (same physical extent, coarser cells, smaller dt)."""
+    kw.setdefault("dt", 0.05)
+    kw.setdefault("xmax", 15.0)
+    return glauber3d_setup(nx=n, ny=n, nz=nz, seed=seed, **kw)
