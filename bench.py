@@ -1,0 +1,368 @@
+"""Benchmark: cell-updates/s of the hydro step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload (one "step" = one Hydro::performStep over the whole grid): the 3D
+viscous single event, 101x101x51 cells (x, y in [-15, 15] fm, eta_s in
+[-7.5, 7.5]), tau0 = 0.5 fm/c, dtau = 0.05 fm/c, eta/s = 0.08, zeta/s = 0,
+2000-point c_s^2(e) EoS table, seeded Monte-Carlo Glauber Pb+Pb event at
+b = 7 fm (synthetic: the reference ships no input data).  The timed K steps
+are the first K steps of the event (warm-up runs on a throw-away copy).
+
+Multi-GPU (torchrun, N ranks): events are independent, so every rank runs
+its own event (seed + rank) with no collective on the data path; the time is
+the max over ranks (weak scaling).
+
+The JSON line carries, besides the contract keys:
+  roofline      the dominant kernel's algorithmic bytes per launch over its
+                CUDA-event time, against the measured HBM copy bandwidth;
+  step_roofline the whole step against the compulsory 288 B per
+                cell-update (Q, pi, Pi read and written once);
+  e2e           the same metric through the C ABI with host-resident state:
+                every step uploads the state from pinned host memory, steps,
+                and reads the updated state back;
+  cpu_baseline  the reference's own C++ step (compiled from its sources,
+                single-threaded) timed on this host over a bounded sample.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s per B200: batched+MLP-guess vs plain GPU at ≤1e-8 rel err"
+UNIT = "cell-updates/s"
+WORKLOAD = ("3D viscous single event 101x101x51 (x,y in [-15,15] fm, eta_s in [-7.5,7.5]), "
+            "tau0=0.5, dtau=0.05, eta/s=0.08, zeta/s=0, c_s^2(e) 2000-point EoS table, "
+            "seeded MC-Glauber Pb+Pb b=7 fm, peak e=50 GeV/fm^3")
+COMPULSORY_B = 288  # bytes per cell-update: Q[7] + pi[10] + Pi, read + write
+
+# Algorithmic bytes per cell per launch of each kernel (fields each launch
+# must read and write once; stencil neighbours come from cache).
+KERNEL_BYTES = {
+    "k_update_m": 48,       # m[3] in, m[3] out
+    "k_face_x": 120,        # Q or Qh [7] + m in, face flux [7] out
+    "k_face_y": 120,
+    "k_face_z": 120,
+    "k_update": 336,        # 3 face fluxes [21] + Q/Qh [7] in, 2 x [7] out
+    "k_ghost": 0,           # boundary planes only
+    "k_visc_prims": 152,    # Qh [7] in, prims [8] + [4] out
+    "k_is_relax": 528,      # Q, Qprev [14], m [3], prims [12], pi, Pi [11] in; pi0, piH0, Pi0, PiH0 [22], flux [4] out
+    "k_is_advect": 496,     # prims [5], pi0, piH0, Pi0, PiH0 [22], flux [4] in; pi, piH, Pi, PiH, vcc [23], flux [4] out
+    "k_visc_update": 288,   # prims [4], piH [10], PiH, m [3], flux [4], Q [7] in; Q [7] out
+}
+
+STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")  # persistent per-cell state
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Dist:
+    """Barrier and max-reduce over ranks (gloo over the host; timings only)."""
+
+    def __init__(self, ws):
+        self.ws = ws
+        self.dist = None
+        if ws > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x):
+        if not self.dist:
+            return x
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.p = None
+        self.out = os.path.join(ROOT, "gpurun_out", "clocks_rank%s.csv" % os.environ.get("RANK", "0"))
+        try:
+            os.makedirs(os.path.dirname(self.out), exist_ok=True)
+            self.f = open(self.out, "w")
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in open(self.out):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def gpu_index_for(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids) and ids[local_rank].isdigit():
+            return ids[local_rank]
+    return str(local_rank)
+
+
+def traffic_per_cell(kernel):
+    """DRAM bytes per cell of one launch of `kernel` from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    v = d.get(kernel)
+    return None if v is None else float(v["bytes_per_cell"])
+
+
+def cpu_baseline_sample(setup, steps=2):
+    """The reference C++ step (oracle/_ref, single-threaded) on the same
+    event; falls back to the C restatement if the reference is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    kind = "reference" if P.ref_available() else "port"
+    run = P.RefRun(setup) if kind == "reference" else P.OracleRun(setup)
+    run.step(1)  # warm-up step, as the reference timing plan asks
+    t0 = time.perf_counter()
+    run.step(steps)
+    dt = time.perf_counter() - t0
+    if kind == "reference":
+        run.close()
+    cells = setup.grid.ncells
+    return {"value": cells * steps / dt, "unit": UNIT, "cores": 1, "kind": kind,
+            "sample": "%d performStep calls of the full 101x101x51 event after 1 warm-up "
+                      "step, one thread, %.1f s" % (steps, dt)}
+
+
+def _ref_worker(args):
+    seed, steps, budget = args
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from vhlle_b200 import workloads as W
+    import pyoracle as P
+    setup = W.glauber3d_setup(seed=seed)
+    run = P.RefRun(setup) if P.ref_available() else P.OracleRun(setup)
+    done = 0
+    t0 = time.perf_counter()
+    while done < steps:
+        run.step(1)
+        done += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    return done * setup.grid.ncells, dt, P.ref_available()
+
+
+def run_reference_arm(args):
+    """--impl reference: the reference's CPU step on all host cores, one
+    independent copy of the event per process, time-boxed."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    ncores = os.cpu_count() or 1
+    nproc = max(1, min(ncores, 32))
+    budget = float(os.environ.get("VH_REF_BUDGET_S", "60"))
+    steps = max(1, args.steps)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_ref_worker, [(20260001 + k, steps, budget) for k in range(nproc)])
+    wall = time.perf_counter() - t0
+    total = sum(r[0] for r in res)
+    slowest = max(r[1] for r in res)
+    kind = "reference" if all(r[2] for r in res) else "port"
+    value = total / slowest
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "path": "reference C++ Hydro::performStep"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": kind,
+                         "sample": "%d processes, each stepping its own copy of the event for up "
+                                   "to %d steps or %.0f s; %.1f s wall" % (nproc, steps, budget, wall)},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+
+    from vhlle_b200 import capi
+    from vhlle_b200 import workloads as W
+
+    ws, rank, local = dist_env()
+    dist = Dist(ws)
+    setup = W.glauber3d_setup(seed=20260001 + rank)
+    cells = setup.grid.ncells
+    h = capi.GpuHydro(setup, device=local)
+    lps = h.launches_per_step()
+
+    # warm-up on the event itself, then restart the event for the timed run
+    h.step(args.warmup)
+    h.sync()
+    h.upload_initial()
+    h.L.vh_set_tau(h.h, setup.tau0)
+
+    sampler = ClockSampler(gpu_index_for(local))
+    time.sleep(0.3)
+    dist.barrier()
+    h.profile(True)
+    h.timer_start()
+    h.step(args.steps)
+    ms = h.timer_stop()
+    dist.barrier()
+    clocks = sampler.stop()
+    h.sync()
+    prof = h.profile_read()
+    h.profile(False)
+    ms_max = dist.max(ms)
+    value = ws * cells * args.steps / (ms_max / 1e3)
+
+    # dominant kernel roofline
+    peak, peak_kind = measured_peaks()
+    dom = max(prof.items(), key=lambda kv: kv[1][1])
+    dname, (dn, dms) = dom
+    avg_s = dms / dn / 1e3
+    alg = KERNEL_BYTES.get(dname, 0) * cells
+    achieved = alg / avg_s / 1e9
+    tpc = traffic_per_cell(dname)
+    roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
+                "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                "traffic": None if tpc is None else tpc * cells,
+                "alg_bytes_per_launch": alg, "avg_launch_ms": avg_s * 1e3}
+    step_bw = COMPULSORY_B * cells * args.steps / (ms / 1e3) / 1e9
+    step_roofline = {"bound": "hbm", "achieved": step_bw, "peak": peak, "unit": "GB/s",
+                     "frac": step_bw / peak, "bytes_per_cell_update": COMPULSORY_B}
+    kernels = {k: {"launches": n, "total_ms": t, "share": t / ms} for k, (n, t) in prof.items()}
+
+    # end to end through the C ABI with host-resident state
+    e2e = None
+    if not args.no_e2e:
+        nE = args.e2e_steps or min(args.steps, 50)
+        L = h.L
+        bufs = {}
+        view = capi.VhStateView()
+        nbytes = 0
+        for k in STATE_IO:
+            n = capi.STATE_NCOMP[k] * cells * 8
+            p = ctypes.c_void_p()
+            h._check(L.vh_alloc_pinned(n, ctypes.byref(p)))
+            bufs[k] = (p, n)
+            setattr(view, k, p.value)
+            nbytes += n
+        h.upload_initial()
+        L.vh_set_tau(h.h, setup.tau0)
+        h._check(L.vh_download_async(h.h, ctypes.byref(view)))
+        h.sync()
+        dist.barrier()
+        h.timer_start()
+        for _ in range(nE):
+            h._check(L.vh_upload_async(h.h, ctypes.byref(view)))
+            h._check(L.vh_step(h.h))
+            h._check(L.vh_download_async(h.h, ctypes.byref(view)))
+        ems = h.timer_stop()
+        h.sync()
+        ems = dist.max(ems)
+        for p, _ in bufs.values():
+            L.vh_free_pinned(p)
+        e2e = {"value": ws * cells * nE / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": nE}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(W.glauber3d_setup(seed=20260001))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": cells,
+                       "path": "plain FP64 step (no MLP guess, single event per GPU)",
+                       "parallelism": "events%d" % ws,
+                       "l2": "inputs larger than L2 (%.0f MB of resident fields)" % (
+                           cells * 8 * 109 / 1e6)},
+            "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
+            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": lps * args.steps, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    h.close()
+    dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,165 @@
+/*
+ * vhlle_b200.h -- C ABI of the B200 hydro step (libvhlle_b200.so).
+ *
+ * The library replaces the per-timestep update of the vHLLE hydro code,
+ * Hydro::performStep (reference src/hdo.h:55, src/hdo.cpp:1016-1134), and
+ * the pieces it calls, with FP64 CUDA kernels for sm_100a that run on a
+ * structure-of-arrays grid resident in device memory.  The host keeps the
+ * reference's class surface (Hydro / Fluid / EoS / TransportCoeff) and calls
+ * down through these entry points; there is no CPU fallback: every entry
+ * point that needs the GPU returns VH_ERR_CUDA when there is none.
+ *
+ * Conventions
+ *  - Plain C types, pointers and sizes only.  All functions return a
+ *    vh_status; 0 is success.  vh_last_error() gives the message of the last
+ *    failure on a context (or of vh_create when ctx is NULL).
+ *  - Cell index i = ix + nx*(iy + ny*iz) (x fastest, Fluid::getCell,
+ *    src/fld.h:70-78).  Fields are component-major: field[c*N + i].
+ *  - pi^{mu nu} is stored as 10 components in index44 order
+ *    (src/cll.cpp:22-31): 00,10,11,20,21,22,30,31,32,33.
+ *  - Calls on one context are not thread-safe; use one context per thread.
+ *  - Device work is enqueued on the context's stream and is asynchronous;
+ *    vh_sync() waits and reports numerical failures that the reference
+ *    would have stopped on with exit() (NaN fluxes, e > 1e10, ...).
+ */
+#ifndef VHLLE_B200_H
+#define VHLLE_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VH_ABI_VERSION 1
+
+typedef int vh_status;
+#define VH_OK 0
+#define VH_ERR_ARG 1      /* invalid argument (the reference would exit) */
+#define VH_ERR_CUDA 2     /* CUDA runtime failure or no usable GPU        */
+#define VH_ERR_NUMERIC 3  /* device error word set during a step          */
+#define VH_ERR_STATE 4    /* call out of order (e.g. step before upload)  */
+
+/* device error-word bits, returned by vh_error_bits() */
+#define VH_NUM_E_HUGE 1u       /* e > 1e10 in hlle_flux, src/hdo.cpp:118-130 */
+#define VH_NUM_FLUX_NAN 2u     /* NaN HLLE flux, src/hdo.cpp:285-298        */
+#define VH_NUM_SOURCE_NAN 4u   /* NaN source, src/hdo.cpp:345-351           */
+#define VH_NUM_NSQUANT_NAN 8u  /* inf/NaN shear, src/hdo.cpp:643-651        */
+
+typedef struct vh_ctx vh_ctx;
+
+/* Fluid geometry (Fluid ctor arguments, src/fld.h:29-31; dx = (xmax-xmin)/(nx-1)). */
+typedef struct vh_grid {
+  int nx, ny, nz;
+  double xmin, xmax, ymin, ymax, etamin, etamax;
+} vh_grid;
+
+/* EoS descriptor.  Device code cannot call the host EoS virtuals
+ * (src/eos.h:21-38), so the EoS is lowered to data:
+ *  kind VH_EOS_CONFORMAL: p = e/3, T = (e/conf_cnst)^(1/4), muB = 0;
+ *  kind VH_EOS_TABLE:     EoS1f (e, nb) table (src/eo1.cpp:21-123): sorted
+ *                         egrid[ne], ngrid[nn] (nn >= 2), p/T/mub[ie + ne*inb].
+ * Host arrays are copied at vh_create. */
+#define VH_EOS_CONFORMAL 0
+#define VH_EOS_TABLE 1
+typedef struct vh_eos {
+  int kind;
+  double conf_cnst;
+  int ne, nn;
+  const double *egrid, *ngrid, *p, *T, *mub;
+} vh_eos;
+
+/* TransportCoeff public constants (src/trancoeff.h:8-11, ctor :14-20). */
+typedef struct vh_trcoeff {
+  double etaS0, zetaS0, ah, al, aRho, T0, etaSMin, etaSEpsilonMin,
+      etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
+      zetaSSigmaMinus, zetaSSigmaPlus;
+  int etaSparam, zetaSparam;
+} vh_trcoeff;
+
+/* A view of the per-cell fields (host or device pointers depending on the
+ * call).  Any pointer may be NULL to skip that field.  Sizes in doubles:
+ * Q, Qh, Qprev 7N; pi, piH 10N; Pi, PiH, viscCorrCut N; m 3N. */
+typedef struct vh_state_view {
+  double *Q, *Qh, *Qprev, *pi, *piH, *Pi, *PiH, *m, *viscCorrCut;
+} vh_state_view;
+
+/* Creates a context on CUDA device `device`, allocates the grid in device
+ * memory and uploads the EoS tables.  Replaces the Fluid + Hydro
+ * constructors (src/fld.cpp:62-112, src/hdo.cpp:50-57); rejects dt > dx/2 or
+ * dt > dy/2 like Hydro::setDtau (src/hdo.cpp:67-75). */
+vh_status vh_create(const vh_grid *grid, const vh_eos *eos,
+                    const vh_trcoeff *tr, double tau0, double dt, int device,
+                    vh_ctx **out);
+vh_status vh_destroy(vh_ctx *ctx);
+
+/* Uses `stream` (a cudaStream_t, NULL = legacy default) for all later work. */
+vh_status vh_set_stream(vh_ctx *ctx, void *stream);
+
+/* Copies cell fields from host memory and synchronises.  Fields left NULL
+ * take the values of a freshly initialised cell (src/cll.cpp:33-52) except
+ * Qprev, which defaults to Q as after Cell::saveQprev.  Q rows with Q_t < 0
+ * are zeroed as by Cell::setQ (src/cll.h:75-80). */
+vh_status vh_upload_state(vh_ctx *ctx, const vh_state_view *host);
+/* Copies cell fields to host memory and synchronises. */
+vh_status vh_download_state(vh_ctx *ctx, const vh_state_view *host);
+/* Asynchronous variants on the context stream; host buffers should be
+ * pinned (cudaHostAlloc) for the copies to overlap.  No defaults applied:
+ * NULL fields are left untouched. */
+vh_status vh_upload_async(vh_ctx *ctx, const vh_state_view *host);
+vh_status vh_download_async(vh_ctx *ctx, const vh_state_view *host);
+/* Device pointers of the resident fields (valid until vh_destroy). */
+vh_status vh_device_state(vh_ctx *ctx, vh_state_view *dev);
+
+/* Hydro::performStep (src/hdo.cpp:1016-1134): one timestep of the whole
+ * grid; tau advances by dt.  Asynchronous. */
+vh_status vh_step(vh_ctx *ctx);
+/* n successive performStep calls. */
+vh_status vh_steps(vh_ctx *ctx, int n);
+
+/* Hydro::setDtau / getDtau / getTau (src/hdo.h:24-26,57). */
+vh_status vh_set_dtau(vh_ctx *ctx, double dt);
+vh_status vh_get_dtau(vh_ctx *ctx, double *dt);
+vh_status vh_get_tau(vh_ctx *ctx, double *tau);
+vh_status vh_set_tau(vh_ctx *ctx, double tau);
+
+/* Waits for the context's work; returns VH_ERR_NUMERIC if a step set the
+ * device error word (then vh_error_bits tells which check fired). */
+vh_status vh_sync(vh_ctx *ctx);
+vh_status vh_error_bits(vh_ctx *ctx, unsigned *bits);
+vh_status vh_clear_errors(vh_ctx *ctx);
+
+/* Number of kernel launches one vh_step issues for this context. */
+vh_status vh_launches_per_step(vh_ctx *ctx, int *n);
+
+/* Device timing with CUDA events recorded on the context's stream.
+ * vh_timer_stop waits for the stop event and returns the elapsed time. */
+vh_status vh_timer_start(vh_ctx *ctx);
+vh_status vh_timer_stop(vh_ctx *ctx, double *ms);
+
+/* Per-kernel timing: while enabled, vh_step records an event after every
+ * launch.  vh_profile_read waits for the context's work and returns, for
+ * kernel kind `kind` (0 <= kind < vh_profile_kinds()), its name, the number
+ * of launches and their summed device time since profiling was enabled. */
+vh_status vh_profile_enable(vh_ctx *ctx, int on);
+vh_status vh_profile_read(vh_ctx *ctx, int kind, const char **name,
+                          long *launches, double *total_ms);
+int vh_profile_kinds(void);
+
+/* Page-locked host memory for the asynchronous copies. */
+vh_status vh_alloc_pinned(size_t bytes, void **p);
+vh_status vh_free_pinned(void *p);
+
+const char *vh_last_error(vh_ctx *ctx);
+int vh_abi_version(void);
+
+/* Batched con2prim + EoS on device arrays (transformPV, src/rmn.cpp:28-139):
+ * Q[7][n] (component-major) -> prim[8][n] = e, p, nb, nq, ns, vx, vy, vz.
+ * Uses the context's EoS and stream. */
+vh_status vh_transform_pv(vh_ctx *ctx, const double *Q_dev, long n,
+                          double *prim_dev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VHLLE_B200_H */

@@ -1,0 +1,118 @@
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Run from the repository root, where oracle/_ref/libvhlle_ref.so has been
+built from the reference sources (``make -C oracle``):
+
+    python tests/golden/make_golden.py
+
+Each fixture is self-contained: the grid, EoS table, transport constants,
+clock, initial state and the reference's state after ``nsteps`` calls of
+Hydro::performStep.  A second set holds transformPV and EoS known answers.
+The generator is the only thing that needs the reference; the fixtures are
+committed so that tests on machines without it still pin the oracle and the
+CUDA path.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+from vhlle_b200 import workloads as W  # noqa: E402
+import pyoracle as P  # noqa: E402
+
+CASES = {
+    # name: (setup factory, steps)
+    "gubser_21x21": (lambda: W.gubser_setup(nx=21, ny=21), 5),
+    "glauber_17x17x9": (lambda: W.small_glauber3d(17, 9), 4),
+    "glauber_13x13x7_b3": (lambda: W.small_glauber3d(13, 7, b=3.0, seed=5, etaS=0.2), 6),
+}
+
+
+def save_case(name, setup, nsteps):
+    r = P.RefRun(setup)
+    r.step(nsteps)
+    st = r.get_state()
+    g = setup.grid
+    eos = setup.eos
+    arrays = dict(
+        grid_n=np.array([g.nx, g.ny, g.nz]), grid_b=np.array(g.bounds()),
+        eos_kind=np.array(eos.kind), eos_cnst=np.array(eos.conf_cnst),
+        tr=np.array(setup.tr_vector()), tr_params=np.array([setup.etaSparam, setup.zetaSparam]),
+        clock=np.array([setup.tau0, setup.dt, setup.ecrit]), nsteps=np.array(nsteps),
+        Q0=setup.Q, m0=setup.m, tau_end=np.array(r.tau_now),
+    )
+    if eos.kind == 1:
+        arrays.update(eos_egrid=eos.egrid, eos_ngrid=eos.ngrid, eos_p=eos.p, eos_T=eos.T,
+                      eos_mub=eos.mub)
+    for k, v in st.items():
+        arrays["out_" + k] = v
+    r.close()
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+
+
+def known_answers():
+    """transformPV / EoS known answers over regimes the step meets: empty
+    (Q_t <= 0), at rest (M = 0), superluminal (M > Q_t), dilute, dense."""
+    rng = np.random.default_rng(12345)
+    n = 2000
+    Qt = 10 ** rng.uniform(-5, 2.5, n)
+    frac = np.concatenate([rng.uniform(0, 0.999, n - 400), rng.uniform(1.0, 1.3, 200),
+                           np.zeros(100), rng.uniform(0, 0.5, 100)])
+    dirs = rng.normal(size=(n, 3))
+    dirs /= np.linalg.norm(dirs, axis=1)[:, None]
+    Q = np.zeros((n, 7))
+    Q[:, 0] = Qt
+    Q[:, 1:4] = dirs * (frac * Qt)[:, None]
+    Q[:, 4] = Qt * rng.uniform(0, 0.02, n)
+    Q[-50:, 0] = -np.abs(Q[-50:, 0])  # empty cells
+    out = {"kpv_Q": Q}
+    for kind, setup in (("conf", W.gubser_setup(nx=5, ny=5)), ("table", W.small_glauber3d(5, 5))):
+        r = P.RefRun(setup)
+        out["kpv_%s" % kind] = r.transform_pv(Q)
+        e = 10 ** rng.uniform(-4.5, 3.2, 1000)
+        nb = rng.uniform(0, 0.9, 1000)
+        pT, s = r.eos_eval(e, nb)
+        out["keos_%s_in" % kind] = np.stack([e, nb])
+        out["keos_%s_out" % kind] = pT
+        out["keos_%s_s" % kind] = s
+        if kind == "table":
+            ee = setup.eos
+            out.update(keos_table_egrid=ee.egrid, keos_table_ngrid=ee.ngrid, keos_table_p=ee.p,
+                       keos_table_T=ee.T, keos_table_mub=ee.mub)
+        r.close()
+    np.savez_compressed(os.path.join(HERE, "known_answers.npz"), **out)
+
+
+def load_case(path):
+    """Rebuilds the Setup and the expected end state from a fixture."""
+    z = np.load(path)
+    nx, ny, nz = (int(v) for v in z["grid_n"])
+    g = W.Grid(nx, ny, nz, *(float(v) for v in z["grid_b"]))
+    if int(z["eos_kind"]) == 1:
+        eos = W.EosTable(kind=1, egrid=z["eos_egrid"], ngrid=z["eos_ngrid"], p=z["eos_p"],
+                         T=z["eos_T"], mub=z["eos_mub"])
+    else:
+        eos = W.EosTable(kind=0, conf_cnst=float(z["eos_cnst"]))
+    tr = dict(zip(W.TR_FIELDS, (float(v) for v in z["tr"])))
+    tau0, dt, ecrit = (float(v) for v in z["clock"])
+    setup = W.Setup(os.path.basename(path), g, eos, tr, int(z["tr_params"][0]),
+                    int(z["tr_params"][1]), tau0, dt, ecrit, z["Q0"], z["m0"])
+    expect = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
+    return setup, int(z["nsteps"]), float(z["tau_end"]), expect
+
+
+if __name__ == "__main__":
+    if not P.ref_available():
+        sys.exit("oracle/_ref/libvhlle_ref.so missing: run `make -C oracle` first")
+    for name, (fac, n) in CASES.items():
+        save_case(name, fac(), n)
+        print("wrote", name)
+    known_answers()
+    print("wrote known_answers")

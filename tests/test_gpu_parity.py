@@ -1,0 +1,180 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Pins, in order of strength:
+  * the golden fixtures written by the compiled reference itself;
+  * the C restatement (oracle), step by step, on seeded inputs up to the
+    full-size workloads (the 101x101x1 Gubser run end to end, the
+    101x101x51 viscous event for its first steps);
+  * size-independent properties at full size: determinism, exact boost
+    invariance of an eta-independent event, the reflection symmetry of the
+    Gubser flow.
+The required agreement is bit-for-bit (FP64, -fmad=false); the tolerance
+named in the contract for the hydro fields (1e-12 relative after one step,
+1e-8 after a full run) is checked as well so that a failure says which
+bound broke.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as P
+from helpers import compare_states, gpu_state_as_oracle
+from make_golden import load_case
+from vhlle_b200 import capi
+from vhlle_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(glob.glob(os.path.join(GOLDEN, "*_*x*.npz")))
+FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")
+
+
+def gpu_state(h):
+    return gpu_state_as_oracle(h.get_state())
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
+def test_gpu_matches_reference_fixture(path):
+    setup, nsteps, tau_end, expect = load_case(path)
+    h = capi.GpuHydro(setup)
+    h.step(nsteps)
+    h.sync()
+    assert h.tau == tau_end
+    got = gpu_state(h)
+    assert not compare_states(got, expect, rtol=1e-12), compare_states(got, expect, rtol=1e-12)
+    assert not compare_states(got, expect), compare_states(got, expect)
+
+
+def _check_every_step(setup, nsteps, every=1):
+    h = capi.GpuHydro(setup)
+    o = P.OracleRun(setup)
+    for s in range(nsteps):
+        h.step(1)
+        assert o.step(1) == 0
+        if (s + 1) % every == 0 or s == nsteps - 1:
+            h.sync()
+            assert h.tau == o.tau_now
+            bad = compare_states(gpu_state(h), o.get_state(), FIELDS)
+            assert not bad, (s + 1, bad)
+    return h, o
+
+
+def test_gubser_full_size_full_run_bitwise():
+    """101x101x1 ideal Gubser flow, all 200 steps, checked every 20 steps."""
+    _check_every_step(W.gubser_setup(), 200, every=20)
+
+
+@pytest.mark.parametrize("case", [
+    ("glauber_41x41x21", lambda: W.small_glauber3d(41, 21), 12),
+    ("glauber_35x35x17_b11", lambda: W.small_glauber3d(35, 17, b=11.0, seed=31, etaS=0.2), 12),
+], ids=lambda c: c[0])
+def test_viscous_every_step_bitwise(case):
+    _check_every_step(case[1](), case[2])
+
+
+def test_viscous_full_size_first_steps_bitwise():
+    """The 101x101x51 viscous event itself, first 3 steps (about 3 s of CPU
+    per oracle step)."""
+    _check_every_step(W.glauber3d_setup(), 3)
+
+
+def test_full_size_run_is_deterministic():
+    s = W.glauber3d_setup()
+    a = capi.GpuHydro(s)
+    b = capi.GpuHydro(s)
+    a.step(20)
+    b.step(20)
+    a.sync()
+    b.sync()
+    sa, sb = a.get_state(), b.get_state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k], equal_nan=True), k
+
+
+def test_full_size_boost_invariant_event_stays_boost_invariant():
+    """With an eta-independent initial state every eta slice of the 3+1D
+    update does identical arithmetic, so after any number of steps all eta
+    slices must be bit-identical (Bjorken boost invariance)."""
+    s = W.glauber3d_setup()
+    g = s.grid
+    Q = s.Q.reshape(7, g.nz, g.ny * g.nx)
+    m = s.m.reshape(g.nz, -1)
+    mid = g.nz // 2
+    s.Q = np.ascontiguousarray(np.repeat(Q[:, mid:mid + 1, :], g.nz, axis=1).reshape(7, -1))
+    s.m = np.ascontiguousarray(np.repeat(m[mid:mid + 1], g.nz, axis=0).reshape(-1))
+    h = capi.GpuHydro(s)
+    h.step(40)
+    h.sync()
+    st = h.get_state(["Q", "pi", "Pi"])
+    for k, a in st.items():
+        a = a.reshape(a.shape[0], g.nz, -1)
+        assert np.all(np.isfinite(a)), k
+        for iz in range(g.nz):
+            assert np.array_equal(a[:, iz], a[:, mid]), (k, iz)
+    assert np.all(st["pi"].reshape(10, g.nz, -1)[[6, 7, 8]] == 0.0)  # pi^{eta x}, ... stay 0
+
+
+def test_gubser_reflection_symmetry_at_full_size():
+    s = W.gubser_setup()
+    h = capi.GpuHydro(s)
+    h.step(100)
+    h.sync()
+    Q = h.get_state(["Q"])["Q"].reshape(7, s.grid.ny, s.grid.nx)
+    assert np.allclose(Q[0], Q[0][:, ::-1], rtol=1e-10, atol=1e-14)
+    assert np.allclose(Q[1], -Q[1][:, ::-1], rtol=1e-10, atol=1e-14)
+    assert np.allclose(Q[0], Q[0].T, rtol=1e-10, atol=1e-14)
+
+
+def test_transform_pv_known_answers_on_device():
+    torch = pytest.importorskip("torch")
+    z = np.load(os.path.join(GOLDEN, "known_answers.npz"))
+    Q = np.ascontiguousarray(z["kpv_Q"].T)  # [7][n]
+    n = Q.shape[1]
+    for kind, setup in (("conf", W.gubser_setup(nx=5, ny=5)), ("table", W.small_glauber3d(5, 5))):
+        if kind == "table":
+            setup.eos = W.EosTable(kind=1, egrid=z["keos_table_egrid"], ngrid=z["keos_table_ngrid"],
+                                   p=z["keos_table_p"], T=z["keos_table_T"], mub=z["keos_table_mub"])
+        h = capi.GpuHydro(setup)
+        dQ = torch.from_numpy(Q).cuda()
+        out = torch.empty((8, n), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        st = h.L.vh_transform_pv(h.h, dQ.data_ptr(), n, out.data_ptr())
+        assert st == capi.VH_OK
+        h.sync()
+        got = out.cpu().numpy().T
+        assert np.array_equal(got, z["kpv_%s" % kind], equal_nan=True), kind
+
+
+def test_numerical_failure_is_reported_not_fatal():
+    """A NaN planted in the uploaded state (host-side fault injection) makes
+    the HLLE flux NaN; the reference would exit(1), here vh_sync reports
+    VH_ERR_NUMERIC and the context stays usable."""
+    s = W.small_glauber3d(17, 9)
+    Q = s.Q.copy()
+    c = np.argmax(Q[0])
+    Q[1, c] = np.nan
+    s.Q = Q
+    h = capi.GpuHydro(s)
+    h.step(1)
+    with pytest.raises(capi.VhError) as ei:
+        h.sync()
+    assert ei.value.status == capi.VH_ERR_NUMERIC
+    assert h.error_bits() & 2  # VH_NUM_FLUX_NAN
+    h.L.vh_clear_errors(h.h)
+    h2 = capi.GpuHydro(W.small_glauber3d(17, 9))
+    h2.step(2)
+    h2.sync()
+
+
+def test_setdtau_rules_follow_the_reference():
+    h = capi.GpuHydro(W.gubser_setup(nx=21, ny=21))
+    with pytest.raises(capi.VhError) as ei:
+        h.set_dtau(0.3)  # > dx/2 = 0.25
+    assert ei.value.status == capi.VH_ERR_ARG
+    h.set_dtau(0.0125)
+    h.step(2)
+    h.sync()
+    assert abs(h.tau - (1.0 + 0.025)) < 1e-15

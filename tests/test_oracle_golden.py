@@ -1,0 +1,56 @@
+"""The C restatement (oracle) against the golden fixtures that the compiled
+reference generated (tests/golden/make_golden.py): bit-for-bit."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as P
+from helpers import compare_states
+from make_golden import load_case
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CASES = sorted(glob.glob(os.path.join(GOLDEN, "*_*x*.npz")))
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
+def test_oracle_matches_reference_fixture(path):
+    setup, nsteps, tau_end, expect = load_case(path)
+    o = P.OracleRun(setup)
+    err = o.step(nsteps)
+    assert err == 0
+    assert o.tau_now == tau_end
+    bad = compare_states(o.get_state(), expect)
+    assert not bad, bad
+
+
+@pytest.fixture(scope="module")
+def known():
+    return np.load(os.path.join(GOLDEN, "known_answers.npz"))
+
+
+def _setup_for(kind, z):
+    from vhlle_b200 import workloads as W
+    if kind == "conf":
+        return W.gubser_setup(nx=5, ny=5)
+    s = W.small_glauber3d(5, 5)
+    s.eos = W.EosTable(kind=1, egrid=z["keos_table_egrid"], ngrid=z["keos_table_ngrid"],
+                       p=z["keos_table_p"], T=z["keos_table_T"], mub=z["keos_table_mub"])
+    return s
+
+
+@pytest.mark.parametrize("kind", ["conf", "table"])
+def test_oracle_transform_pv_known_answers(known, kind):
+    o = P.OracleRun(_setup_for(kind, known))
+    got = o.transform_pv(known["kpv_Q"])
+    assert np.array_equal(got, known["kpv_%s" % kind], equal_nan=True)
+
+
+@pytest.mark.parametrize("kind", ["conf", "table"])
+def test_oracle_eos_known_answers(known, kind):
+    o = P.OracleRun(_setup_for(kind, known))
+    e, nb = known["keos_%s_in" % kind]
+    pT, s = o.eos_eval(e, nb)
+    assert np.array_equal(pT, known["keos_%s_out" % kind])
+    assert np.array_equal(s, known["keos_%s_s" % kind])

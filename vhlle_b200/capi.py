@@ -1,0 +1,261 @@
+"""ctypes binding of the C ABI in include/vhlle_b200.h (libvhlle_b200.so).
+
+``GpuHydro`` drives one device-resident grid through the C entry points the
+way the reference's driver drives Hydro (src/main.cpp:399-428): upload the
+initial state, call ``step()`` (== Hydro::performStep) and read fields back.
+There is no CPU fallback: constructing a GpuHydro without the built library
+or without a GPU raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvhlle_b200.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+VH_OK, VH_ERR_ARG, VH_ERR_CUDA, VH_ERR_NUMERIC, VH_ERR_STATE = 0, 1, 2, 3, 4
+
+# symbols the header declares (checked by the CPU test suite)
+EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_download_state",
+           "vh_upload_async", "vh_download_async", "vh_device_state", "vh_step", "vh_steps",
+           "vh_set_dtau", "vh_get_dtau", "vh_get_tau", "vh_set_tau", "vh_sync",
+           "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
+           "vh_abi_version", "vh_transform_pv", "vh_timer_start", "vh_timer_stop",
+           "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
+           "vh_free_pinned")
+
+
+class VhError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("vhlle_b200 status %d: %s" % (status, msg))
+        self.status = status
+
+
+class VhGrid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
+                ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
+                ("etamin", ctypes.c_double), ("etamax", ctypes.c_double)]
+
+
+class VhEos(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
+                ("ne", ctypes.c_int), ("nn", ctypes.c_int),
+                ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp)]
+
+
+class VhTrcoeff(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in (
+        "etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin",
+        "etaSShiftMuB", "etaSScaleMuB", "zetaSPeakEpsilon", "zetaSScaleBeta",
+        "zetaSSigmaMinus", "zetaSSigmaPlus")] + [
+        ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int)]
+
+
+STATE_FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "viscCorrCut")
+STATE_NCOMP = dict(Q=7, Qh=7, Qprev=7, pi=10, piH=10, Pi=1, PiH=1, m=3, viscCorrCut=1)
+
+
+class VhStateView(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in STATE_FIELDS]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libvhlle_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libvhlle_b200.so is not built (run `python -m vhlle_b200.build`); "
+                           "there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    L.vh_create.argtypes = [ctypes.POINTER(VhGrid), ctypes.POINTER(VhEos),
+                            ctypes.POINTER(VhTrcoeff), ctypes.c_double, ctypes.c_double,
+                            ctypes.c_int, ctypes.POINTER(vp)]
+    L.vh_destroy.argtypes = [vp]
+    L.vh_set_stream.argtypes = [vp, vp]
+    for n in ("vh_upload_state", "vh_download_state", "vh_upload_async", "vh_download_async",
+              "vh_device_state"):
+        getattr(L, n).argtypes = [vp, ctypes.POINTER(VhStateView)]
+    L.vh_step.argtypes = [vp]
+    L.vh_steps.argtypes = [vp, ctypes.c_int]
+    L.vh_set_dtau.argtypes = [vp, ctypes.c_double]
+    L.vh_get_dtau.argtypes = [vp, _dp]
+    L.vh_get_tau.argtypes = [vp, _dp]
+    L.vh_set_tau.argtypes = [vp, ctypes.c_double]
+    L.vh_sync.argtypes = [vp]
+    L.vh_error_bits.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
+    L.vh_clear_errors.argtypes = [vp]
+    L.vh_launches_per_step.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.vh_last_error.argtypes = [vp]
+    L.vh_last_error.restype = ctypes.c_char_p
+    L.vh_abi_version.restype = ctypes.c_int
+    L.vh_transform_pv.argtypes = [vp, vp, ctypes.c_long, vp]
+    L.vh_timer_start.argtypes = [vp]
+    L.vh_timer_stop.argtypes = [vp, _dp]
+    L.vh_profile_enable.argtypes = [vp, ctypes.c_int]
+    L.vh_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                  ctypes.POINTER(ctypes.c_long), _dp]
+    L.vh_profile_kinds.restype = ctypes.c_int
+    L.vh_alloc_pinned.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
+    L.vh_free_pinned.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def make_eos(eos):
+    """Lowers a workloads.EosTable into the vh_eos descriptor (arrays kept alive)."""
+    d = VhEos()
+    d.kind = eos.kind
+    d.conf_cnst = eos.conf_cnst
+    keep = []
+    if eos.kind == 1:
+        keep = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub)]
+        d.ne, d.nn = len(keep[0]), len(keep[1])
+        d.egrid, d.ngrid, d.p, d.T, d.mub = (_ptr(a) for a in keep)
+    return d, keep
+
+
+def make_trcoeff(setup):
+    t = VhTrcoeff()
+    for k, v in setup.tr.items():
+        setattr(t, k, float(v))
+    t.etaSparam = setup.etaSparam
+    t.zetaSparam = setup.zetaSparam
+    return t
+
+
+class GpuHydro:
+    """One grid on one GPU behind the C ABI (Fluid + Hydro of the reference)."""
+
+    def __init__(self, setup, device: int = 0, upload: bool = True):
+        self.L = lib()
+        self.setup = setup
+        g = setup.grid
+        self.N = g.ncells
+        grid = VhGrid(g.nx, g.ny, g.nz, *g.bounds())
+        eos, self._eos_keep = make_eos(setup.eos)
+        tr = make_trcoeff(setup)
+        h = ctypes.c_void_p()
+        st = self.L.vh_create(ctypes.byref(grid), ctypes.byref(eos), ctypes.byref(tr),
+                              setup.tau0, setup.dt, device, ctypes.byref(h))
+        if st != VH_OK:
+            raise VhError(st, self.L.vh_last_error(None).decode())
+        self.h = h
+        if upload:
+            self.upload_initial()
+
+    def _check(self, st):
+        if st != VH_OK:
+            raise VhError(st, self.L.vh_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_initial(self):
+        """Initial state as the reference ICs leave it: Q, Qprev = Q, all m
+        set to the given value, viscous fields zero (src/icGubser.cpp:50-57)."""
+        s = self.setup
+        Q = np.ascontiguousarray(s.Q, dtype=np.float64).reshape(7, self.N)
+        m = np.ascontiguousarray(np.repeat(np.asarray(s.m, dtype=np.float64).reshape(1, self.N), 3, 0))
+        fields = dict(Q=Q, m=m)
+        if s.pi is not None:
+            fields["pi"] = np.ascontiguousarray(s.pi, dtype=np.float64)
+        if s.Pi is not None:
+            fields["Pi"] = np.ascontiguousarray(s.Pi, dtype=np.float64)
+        self.upload(fields)
+
+    def upload(self, fields: dict):
+        v = VhStateView()
+        keep = []
+        for k, a in fields.items():
+            a = np.ascontiguousarray(a, dtype=np.float64).reshape(STATE_NCOMP[k], self.N)
+            keep.append(a)
+            setattr(v, k, a.ctypes.data)
+        self._check(self.L.vh_upload_state(self.h, ctypes.byref(v)))
+
+    def step(self, n: int = 1):
+        self._check(self.L.vh_steps(self.h, n))
+
+    def sync(self):
+        self._check(self.L.vh_sync(self.h))
+
+    def error_bits(self) -> int:
+        b = ctypes.c_uint(0)
+        self._check(self.L.vh_error_bits(self.h, ctypes.byref(b)))
+        return b.value
+
+    @property
+    def tau(self) -> float:
+        t = ctypes.c_double()
+        self._check(self.L.vh_get_tau(self.h, ctypes.byref(t)))
+        return t.value
+
+    def set_dtau(self, dt: float):
+        self._check(self.L.vh_set_dtau(self.h, dt))
+
+    def launches_per_step(self) -> int:
+        n = ctypes.c_int()
+        self._check(self.L.vh_launches_per_step(self.h, ctypes.byref(n)))
+        return n.value
+
+    def get_state(self, fields=STATE_FIELDS) -> dict:
+        v = VhStateView()
+        out = {}
+        for k in fields:
+            out[k] = np.empty((STATE_NCOMP[k], self.N))
+            setattr(v, k, out[k].ctypes.data)
+        self._check(self.L.vh_download_state(self.h, ctypes.byref(v)))
+        return out
+
+    def timer_start(self):
+        self._check(self.L.vh_timer_start(self.h))
+
+    def timer_stop(self) -> float:
+        ms = ctypes.c_double()
+        self._check(self.L.vh_timer_stop(self.h, ctypes.byref(ms)))
+        return ms.value
+
+    def profile(self, on: bool):
+        self._check(self.L.vh_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self) -> dict:
+        """{kernel name: (launches, total device ms)} since profiling started."""
+        out = {}
+        for k in range(self.L.vh_profile_kinds()):
+            name = ctypes.c_char_p()
+            n = ctypes.c_long()
+            ms = ctypes.c_double()
+            self._check(self.L.vh_profile_read(self.h, k, ctypes.byref(name), ctypes.byref(n),
+                                               ctypes.byref(ms)))
+            if n.value:
+                out[name.value.decode()] = (n.value, ms.value)
+        return out
+
+    def device_state(self) -> dict:
+        v = VhStateView()
+        self._check(self.L.vh_device_state(self.h, ctypes.byref(v)))
+        return {k: getattr(v, k) for k in STATE_FIELDS}

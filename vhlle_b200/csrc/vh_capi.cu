@@ -1,0 +1,527 @@
+// vh_capi.cu -- the C ABI declared in include/vhlle_b200.h.
+//
+// A context owns one fluid grid resident in device memory (the role of the
+// reference's Fluid + Hydro pair, src/fld.cpp:62-112, src/hdo.cpp:50-57):
+// every field is a component-major FP64 array, the EoS table is copied to
+// the device once, and vh_step enqueues the kernels of one performStep on
+// the context's stream.  Errors are returned as status codes; nothing in
+// here exits or traps.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/vhlle_b200.h"
+#include "vh_step.cuh"
+
+namespace vh {
+void launch_fill(double* p, long long n, double v, cudaStream_t s);
+void launch_zero_negative_rows(double* Q, long long N, cudaStream_t s);
+}  // namespace vh
+
+struct vh_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  vh::Geo g{};
+  vh::EosDev eos{};
+  vh::TrDev tr{};
+  vh::Fields f{};
+  double tau = 0., dt = 0.;
+  bool viscous = false;
+  bool uploaded = false;
+  int launches = 0;
+  std::string err;
+  std::vector<void*> allocs;
+  // timers and per-kernel profiling
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  bool prof = false;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  struct Seg {
+    int kind;
+    size_t ev0, ev1;
+  };
+  std::vector<Seg> segs;
+};
+
+namespace {
+struct EventMarker : vh::LaunchMarker {
+  vh_ctx* c;
+  size_t prev;
+  cudaError_t err = cudaSuccess;
+  EventMarker(vh_ctx* ctx, size_t start) : c(ctx), prev(start) {}
+  void after(int kind) override {
+    if (c->evused == c->evpool.size()) {
+      cudaEvent_t e;
+      cudaError_t r = cudaEventCreate(&e);
+      if (r != cudaSuccess) {
+        err = r;
+        return;
+      }
+      c->evpool.push_back(e);
+    }
+    const size_t k = c->evused++;
+    cudaError_t r = cudaEventRecord(c->evpool[k], c->stream);
+    if (r != cudaSuccess) err = r;
+    c->segs.push_back({kind, prev, k});
+    prev = k;
+  }
+};
+}  // namespace
+
+static thread_local std::string g_create_error;
+
+static vh_status fail(vh_ctx* c, vh_status st, const std::string& msg) {
+  if (c)
+    c->err = msg;
+  else
+    g_create_error = msg;
+  return st;
+}
+
+static vh_status cuda_fail(vh_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, VH_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define VH_CUDA(c, call)                                 \
+  do {                                                   \
+    cudaError_t e_ = (call);                             \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call); \
+  } while (0)
+
+template <typename T>
+static vh_status dalloc(vh_ctx* c, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMalloc");
+  c->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return VH_OK;
+}
+
+// Per-dimension source map of the ghost-cell copies: the reference copies
+// cell 2 into 1 and 0, then cell n-3 into n-2 and n-1, each index clamped
+// into [0, n-1] (src/fld.cpp:211-273).  Simulating that sequence gives, for
+// every index, the original cell its final value comes from.
+static void ghost_map(int n, int* src, unsigned char* dst) {
+  for (int i = 0; i < n; i++) {
+    src[i] = i;
+    dst[i] = 0;
+  }
+  auto cl = [n](int i) { return std::min(std::max(i, 0), n - 1); };
+  int s = cl(2);
+  for (int d : {cl(1), cl(0)}) {
+    src[d] = src[s];
+    dst[d] = 1;
+  }
+  s = cl(n - 3);
+  for (int d : {cl(n - 2), cl(n - 1)}) {
+    src[d] = src[s];
+    dst[d] = 1;
+  }
+}
+
+extern "C" {
+
+int vh_abi_version(void) { return VH_ABI_VERSION; }
+
+const char* vh_last_error(vh_ctx* ctx) {
+  return ctx ? ctx->err.c_str() : g_create_error.c_str();
+}
+
+vh_status vh_destroy(vh_ctx* ctx) {
+  if (!ctx) return VH_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (void* p : ctx->allocs) cudaFree(p);
+  for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->t0) cudaEventDestroy(ctx->t0);
+  if (ctx->t1) cudaEventDestroy(ctx->t1);
+  delete ctx;
+  return VH_OK;
+}
+
+vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr, double tau0,
+                    double dt, int device, vh_ctx** out) {
+  if (!out) return fail(nullptr, VH_ERR_ARG, "vh_create: out is NULL");
+  *out = nullptr;
+  if (!grid || !eos || !tr) return fail(nullptr, VH_ERR_ARG, "vh_create: NULL argument");
+  if (grid->nx < 2 || grid->ny < 2 || grid->nz < 1)
+    return fail(nullptr, VH_ERR_ARG, "vh_create: need nx >= 2, ny >= 2, nz >= 1");
+  if (eos->kind != VH_EOS_CONFORMAL && eos->kind != VH_EOS_TABLE)
+    return fail(nullptr, VH_ERR_ARG, "vh_create: unsupported EoS kind (no device lowering)");
+  if (eos->kind == VH_EOS_TABLE) {
+    if (eos->ne < 2 || eos->nn < 2 || !eos->egrid || !eos->ngrid || !eos->p || !eos->T || !eos->mub)
+      return fail(nullptr, VH_ERR_ARG,
+                  "vh_create: EoS table needs ne >= 2, nn >= 2 and all five arrays");
+  }
+  const double dx = (grid->xmax - grid->xmin) / (grid->nx - 1);
+  const double dy = (grid->ymax - grid->ymin) / (grid->ny - 1);
+  if (!(dt > 0.) || dt > dx / 2. || dt > dy / 2.)
+    return fail(nullptr, VH_ERR_ARG, "vh_create: too big delta_tau (dt > dx/2 or dy/2)");
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(nullptr, VH_ERR_CUDA, std::string("vh_create: no CUDA device: ") +
+                                          (e != cudaSuccess ? cudaGetErrorString(e) : "count 0"));
+  if (device < 0 || device >= ndev) return fail(nullptr, VH_ERR_ARG, "vh_create: bad device index");
+
+  vh_ctx* c = new vh_ctx;
+  c->err.clear();
+  c->device = device;
+  if ((e = cudaSetDevice(device)) != cudaSuccess) {
+    g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+    delete c;
+    return VH_ERR_CUDA;
+  }
+  auto bail = [&](vh_status st) {
+    g_create_error = c->err;
+    vh_destroy(c);
+    return st;
+  };
+  vh::Geo& g = c->g;
+  g.nx = grid->nx;
+  g.ny = grid->ny;
+  g.nz = grid->nz;
+  g.N = (long long)grid->nx * grid->ny * grid->nz;
+  g.dx = dx;
+  g.dy = dy;
+  g.dz = (grid->etamax - grid->etamin) / (grid->nz - 1);
+  c->tau = tau0;
+  c->dt = dt;
+  c->tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
+                    tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
+                    tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,
+                    tr->zetaSSigmaPlus, tr->etaSparam, tr->zetaSparam};
+  // TransportCoeff::isViscous, src/trancoeff.h:39-45
+  c->viscous = tr->etaS0 > 0. || tr->zetaS0 > 0. || tr->etaSparam > 0 || tr->zetaSparam > 0;
+
+  const long long N = g.N;
+  vh::Fields& f = c->f;
+  vh_status st = VH_OK;
+#define ALLOC(p, n) \
+  if ((st = dalloc(c, &(p), (size_t)(n))) != VH_OK) return bail(st)
+  ALLOC(f.Q, 7 * N);
+  ALLOC(f.Qh, 7 * N);
+  ALLOC(f.Qprev, 7 * N);
+  ALLOC(f.pi, 10 * N);
+  ALLOC(f.piH, 10 * N);
+  ALLOC(f.Pi, N);
+  ALLOC(f.PiH, N);
+  ALLOC(f.vcc, N);
+  ALLOC(f.m, 3 * N);
+  ALLOC(f.m2, 3 * N);
+  ALLOC(f.Fx, 7 * N);
+  ALLOC(f.Fy, 7 * N);
+  ALLOC(f.Fz, 7 * N);
+  if (c->viscous) {
+    ALLOC(f.flux, 4 * N);
+    ALLOC(f.pA, 8 * N);
+    ALLOC(f.pD, 4 * N);
+    ALLOC(f.pi0, 10 * N);
+    ALLOC(f.piH0, 10 * N);
+    ALLOC(f.Pi0, N);
+    ALLOC(f.PiH0, N);
+  }
+  const int ng = g.nx + g.ny + g.nz;
+  ALLOC(f.gsrc, ng);
+  ALLOC(f.gdst, ng);
+  ALLOC(f.err, 1);
+  std::vector<int> hsrc(ng);
+  std::vector<unsigned char> hdst(ng);
+  ghost_map(g.nx, hsrc.data(), hdst.data());
+  ghost_map(g.ny, hsrc.data() + g.nx, hdst.data() + g.nx);
+  ghost_map(g.nz, hsrc.data() + g.nx + g.ny, hdst.data() + g.nx + g.ny);
+  if ((e = cudaMemcpy(f.gsrc, hsrc.data(), ng * sizeof(int), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(f.gdst, hdst.data(), ng, cudaMemcpyHostToDevice)) ||
+      (e = cudaMemset(f.err, 0, sizeof(unsigned)))) {
+    cuda_fail(c, e, "vh_create: upload");
+    return bail(VH_ERR_CUDA);
+  }
+  c->eos.kind = eos->kind;
+  c->eos.conf_cnst = eos->conf_cnst;
+  if (eos->kind == VH_EOS_TABLE) {
+    const int ne = eos->ne, nn = eos->nn;
+    double* buf = nullptr;
+    ALLOC(buf, (size_t)ne + nn + 3 * (size_t)ne * nn);
+    c->eos.ne = ne;
+    c->eos.nn = nn;
+    c->eos.egrid = buf;
+    c->eos.ngrid = buf + ne;
+    c->eos.p = buf + ne + nn;
+    c->eos.T = c->eos.p + (size_t)ne * nn;
+    c->eos.mub = c->eos.T + (size_t)ne * nn;
+    const size_t tb = (size_t)ne * nn * sizeof(double);
+    if ((e = cudaMemcpy((void*)c->eos.egrid, eos->egrid, ne * sizeof(double), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)c->eos.ngrid, eos->ngrid, nn * sizeof(double), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)c->eos.p, eos->p, tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)c->eos.T, eos->T, tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)c->eos.mub, eos->mub, tb, cudaMemcpyHostToDevice))) {
+      cuda_fail(c, e, "vh_create: EoS upload");
+      return bail(VH_ERR_CUDA);
+    }
+  }
+#undef ALLOC
+  *out = c;
+  return VH_OK;
+}
+
+vh_status vh_set_stream(vh_ctx* ctx, void* stream) {
+  if (!ctx) return VH_ERR_ARG;
+  ctx->stream = static_cast<cudaStream_t>(stream);
+  return VH_OK;
+}
+
+struct FieldSpec {
+  double* vh_state_view::*host;
+  double* vh::Fields::*dev;
+  int ncomp;
+};
+
+static const FieldSpec kFields[] = {
+    {&vh_state_view::Q, &vh::Fields::Q, 7},       {&vh_state_view::Qh, &vh::Fields::Qh, 7},
+    {&vh_state_view::Qprev, &vh::Fields::Qprev, 7}, {&vh_state_view::pi, &vh::Fields::pi, 10},
+    {&vh_state_view::piH, &vh::Fields::piH, 10},  {&vh_state_view::Pi, &vh::Fields::Pi, 1},
+    {&vh_state_view::PiH, &vh::Fields::PiH, 1},   {&vh_state_view::m, &vh::Fields::m, 3},
+    {&vh_state_view::viscCorrCut, &vh::Fields::vcc, 1},
+};
+
+vh_status vh_upload_async(vh_ctx* ctx, const vh_state_view* h) {
+  if (!ctx || !h) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  for (const FieldSpec& fs : kFields) {
+    const double* src = h->*(fs.host);
+    if (!src) continue;
+    VH_CUDA(ctx, cudaMemcpyAsync(ctx->f.*(fs.dev), src, sizeof(double) * fs.ncomp * ctx->g.N,
+                                 cudaMemcpyHostToDevice, ctx->stream));
+  }
+  ctx->uploaded = true;
+  return VH_OK;
+}
+
+vh_status vh_download_async(vh_ctx* ctx, const vh_state_view* h) {
+  if (!ctx || !h) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  for (const FieldSpec& fs : kFields) {
+    double* dst = h->*(fs.host);
+    if (!dst) continue;
+    VH_CUDA(ctx, cudaMemcpyAsync(dst, ctx->f.*(fs.dev), sizeof(double) * fs.ncomp * ctx->g.N,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  return VH_OK;
+}
+
+vh_status vh_upload_state(vh_ctx* ctx, const vh_state_view* h) {
+  if (!ctx || !h) return VH_ERR_ARG;
+  if (!h->Q) return fail(ctx, VH_ERR_ARG, "vh_upload_state: Q is required");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  const long long N = ctx->g.N;
+  vh::Fields& f = ctx->f;
+  cudaStream_t s = ctx->stream;
+  vh_status st = vh_upload_async(ctx, h);
+  if (st != VH_OK) return st;
+  vh::launch_zero_negative_rows(f.Q, N, s);  // Cell::setQ
+  if (!h->Qprev)
+    VH_CUDA(ctx, cudaMemcpyAsync(f.Qprev, f.Q, 7 * N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (!h->Qh) VH_CUDA(ctx, cudaMemsetAsync(f.Qh, 0, 7 * N * sizeof(double), s));
+  if (!h->pi) VH_CUDA(ctx, cudaMemsetAsync(f.pi, 0, 10 * N * sizeof(double), s));
+  if (!h->piH) VH_CUDA(ctx, cudaMemsetAsync(f.piH, 0, 10 * N * sizeof(double), s));
+  if (!h->Pi) VH_CUDA(ctx, cudaMemsetAsync(f.Pi, 0, N * sizeof(double), s));
+  if (!h->PiH) VH_CUDA(ctx, cudaMemsetAsync(f.PiH, 0, N * sizeof(double), s));
+  if (!h->m) VH_CUDA(ctx, cudaMemsetAsync(f.m, 0, 3 * N * sizeof(double), s));
+  if (!h->viscCorrCut) vh::launch_fill(f.vcc, N, 1.0, s);
+  VH_CUDA(ctx, cudaGetLastError());
+  VH_CUDA(ctx, cudaStreamSynchronize(s));
+  return VH_OK;
+}
+
+vh_status vh_download_state(vh_ctx* ctx, const vh_state_view* h) {
+  vh_status st = vh_download_async(ctx, h);
+  if (st != VH_OK) return st;
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return VH_OK;
+}
+
+vh_status vh_device_state(vh_ctx* ctx, vh_state_view* d) {
+  if (!ctx || !d) return VH_ERR_ARG;
+  for (const FieldSpec& fs : kFields) d->*(fs.host) = ctx->f.*(fs.dev);
+  return VH_OK;
+}
+
+vh_status vh_step(vh_ctx* ctx) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_step: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::StepArgs a;
+  a.g = ctx->g;
+  a.eos = ctx->eos;
+  a.tr = ctx->tr;
+  a.f = ctx->f;
+  a.tau = ctx->tau;
+  a.dt = ctx->dt;
+  a.viscous = ctx->viscous;
+  if (ctx->prof) {
+    EventMarker mk(ctx, 0);
+    mk.after(-1);  // start event of this step
+    mk.prev = ctx->segs.back().ev1;
+    ctx->segs.pop_back();
+    ctx->launches = vh::launch_step(a, ctx->stream, &mk);
+    if (mk.err != cudaSuccess) return cuda_fail(ctx, mk.err, "vh_step: profiling event");
+  } else {
+    ctx->launches = vh::launch_step(a, ctx->stream);
+  }
+  VH_CUDA(ctx, cudaGetLastError());
+  std::swap(ctx->f.m, ctx->f.m2);
+  ctx->tau += ctx->dt;  // src/hdo.cpp:1095
+  return VH_OK;
+}
+
+vh_status vh_steps(vh_ctx* ctx, int n) {
+  for (int k = 0; k < n; k++) {
+    vh_status st = vh_step(ctx);
+    if (st != VH_OK) return st;
+  }
+  return VH_OK;
+}
+
+vh_status vh_set_dtau(vh_ctx* ctx, double dt) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!(dt > 0.) || dt > ctx->g.dx / 2. || dt > ctx->g.dy / 2.)
+    return fail(ctx, VH_ERR_ARG, "vh_set_dtau: too big delta_tau (dt > dx/2 or dy/2)");
+  ctx->dt = dt;
+  return VH_OK;
+}
+
+vh_status vh_get_dtau(vh_ctx* ctx, double* dt) {
+  if (!ctx || !dt) return VH_ERR_ARG;
+  *dt = ctx->dt;
+  return VH_OK;
+}
+
+vh_status vh_get_tau(vh_ctx* ctx, double* tau) {
+  if (!ctx || !tau) return VH_ERR_ARG;
+  *tau = ctx->tau;
+  return VH_OK;
+}
+
+vh_status vh_set_tau(vh_ctx* ctx, double tau) {
+  if (!ctx) return VH_ERR_ARG;
+  ctx->tau = tau;
+  return VH_OK;
+}
+
+vh_status vh_error_bits(vh_ctx* ctx, unsigned* bits) {
+  if (!ctx || !bits) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  VH_CUDA(ctx, cudaMemcpyAsync(bits, ctx->f.err, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return VH_OK;
+}
+
+vh_status vh_clear_errors(vh_ctx* ctx) {
+  if (!ctx) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  VH_CUDA(ctx, cudaMemsetAsync(ctx->f.err, 0, sizeof(unsigned), ctx->stream));
+  return VH_OK;
+}
+
+vh_status vh_sync(vh_ctx* ctx) {
+  unsigned bits = 0;
+  vh_status st = vh_error_bits(ctx, &bits);
+  if (st != VH_OK) return st;
+  if (bits) {
+    char buf[160];
+    snprintf(buf, sizeof buf,
+             "numerical failure during a step (error bits 0x%x: 1 e>1e10, 2 NaN flux, "
+             "4 NaN source, 8 inf/NaN shear)",
+             bits);
+    return fail(ctx, VH_ERR_NUMERIC, buf);
+  }
+  return VH_OK;
+}
+
+vh_status vh_launches_per_step(vh_ctx* ctx, int* n) {
+  if (!ctx || !n) return VH_ERR_ARG;
+  int k = 1 + 2 * (2 + (ctx->g.nz > 1 ? 1 : 0) + 1) + 1 + (ctx->viscous ? 4 : 0) + 1;
+  *n = k;
+  return VH_OK;
+}
+
+vh_status vh_timer_start(vh_ctx* ctx) {
+  if (!ctx) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->t0) VH_CUDA(ctx, cudaEventCreate(&ctx->t0));
+  if (!ctx->t1) VH_CUDA(ctx, cudaEventCreate(&ctx->t1));
+  VH_CUDA(ctx, cudaEventRecord(ctx->t0, ctx->stream));
+  return VH_OK;
+}
+
+vh_status vh_timer_stop(vh_ctx* ctx, double* ms) {
+  if (!ctx || !ms || !ctx->t0) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  VH_CUDA(ctx, cudaEventRecord(ctx->t1, ctx->stream));
+  VH_CUDA(ctx, cudaEventSynchronize(ctx->t1));
+  float f = 0.f;
+  VH_CUDA(ctx, cudaEventElapsedTime(&f, ctx->t0, ctx->t1));
+  *ms = f;
+  return VH_OK;
+}
+
+int vh_profile_kinds(void) { return vh::KK_COUNT; }
+
+vh_status vh_profile_enable(vh_ctx* ctx, int on) {
+  if (!ctx) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->prof = on != 0;
+  ctx->segs.clear();
+  ctx->evused = 0;
+  return VH_OK;
+}
+
+vh_status vh_profile_read(vh_ctx* ctx, int kind, const char** name, long* launches,
+                          double* total_ms) {
+  if (!ctx || kind < 0 || kind >= vh::KK_COUNT) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  long n = 0;
+  double tot = 0.;
+  for (const auto& sg : ctx->segs) {
+    if (sg.kind != kind) continue;
+    float f = 0.f;
+    VH_CUDA(ctx, cudaEventElapsedTime(&f, ctx->evpool[sg.ev0], ctx->evpool[sg.ev1]));
+    tot += f;
+    n++;
+  }
+  if (name) *name = vh::kKernelNames[kind];
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = tot;
+  return VH_OK;
+}
+
+vh_status vh_alloc_pinned(size_t bytes, void** p) {
+  if (!p) return VH_ERR_ARG;
+  cudaError_t e = cudaHostAlloc(p, bytes, cudaHostAllocDefault);
+  if (e != cudaSuccess) return fail(nullptr, VH_ERR_CUDA, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+  return VH_OK;
+}
+
+vh_status vh_free_pinned(void* p) {
+  if (p) cudaFreeHost(p);
+  return VH_OK;
+}
+
+vh_status vh_transform_pv(vh_ctx* ctx, const double* Q_dev, long n, double* prim_dev) {
+  if (!ctx || !Q_dev || !prim_dev || n < 0) return VH_ERR_ARG;
+  if (n == 0) return VH_OK;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::launch_transform_pv(ctx->eos, Q_dev, (long long)n, prim_dev, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
+  return VH_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,388 @@
+// vh_physics.cuh -- per-cell / per-face FP64 physics of the vHLLE step,
+// as device functions.
+//
+// Every function keeps the operation order of the reference function cited
+// in its comment, and the library is compiled with -fmad=false, so that
+// IEEE-754 double arithmetic gives the reference's results bit for bit
+// (division and square root are correctly rounded on both sides).
+#pragma once
+
+#include <cstdint>
+
+namespace vh {
+
+enum { T_ = 0, X_ = 1, Y_ = 2, Z_ = 3, NB_ = 4, NQ_ = 5, NS_ = 6 };
+
+// error bits (the reference exits on these conditions)
+enum : unsigned {
+  ERR_E_HUGE = 1u,       // e > 1e10 in hlle_flux, src/hdo.cpp:118-130
+  ERR_FLUX_NAN = 2u,     // src/hdo.cpp:285-298
+  ERR_SOURCE_NAN = 4u,   // src/hdo.cpp:345-351
+  ERR_NSQUANT_NAN = 8u,  // src/hdo.cpp:643-651
+};
+
+struct EosDev {
+  int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table
+  double conf_cnst;  // e = cnst T^4 for kind 0
+  int ne, nn;
+  const double* __restrict__ egrid;
+  const double* __restrict__ ngrid;
+  const double* __restrict__ p;  // [ie + ne*inb]
+  const double* __restrict__ T;
+  const double* __restrict__ mub;
+};
+
+struct TrDev {
+  double etaS0, zetaS0, ah, al, aRho, T0, etaSMin, etaSEpsilonMin,
+      etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
+      zetaSSigmaMinus, zetaSSigmaPlus;
+  int etaSparam, zetaSparam;
+};
+
+struct Prim {
+  double e, p, nb, nq, ns, vx, vy, vz;
+};
+
+__device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
+__device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+
+// index44, src/cll.cpp:22-31
+__host__ __device__ __forceinline__ int index44(int i, int j) {
+  return (j < i) ? (i * (i + 1)) / 2 + j : (j * (j + 1)) / 2 + i;
+}
+
+// minmod, src/cll.cpp:12-19
+__device__ __forceinline__ double minmod(double a, double b) {
+  if (a * b <= 0.) return 0.;
+  return (fabs(a) > fabs(b)) ? b : a;
+}
+
+// ------------------------------------------------------------------ EoS
+// EoS1f binary search over a sorted grid (getue / getun, src/eo1.cpp:63-98);
+// returns k1 of the bracketing pair and k2.
+__device__ __forceinline__ void bsearch_grid(const double* __restrict__ g, int n,
+                                             double x, int& k1, int& k2) {
+  k1 = 0;
+  k2 = n - 1;
+  while (k2 - k1 > 1) {
+    const int k = (k1 + k2) / 2;
+    if (x < __ldg(g + k))
+      k2 = k;
+    else
+      k1 = k;
+  }
+}
+
+// EoS1f::eos, src/eo1.cpp:100-123
+template <bool WANT_T>
+__device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
+                                      double& T, double& mub, double& p) {
+  int k1, k2;
+  bsearch_grid(E.egrid, E.ne, e, k1, k2);
+  int ixe = k1;
+  if (ixe > E.ne - 2) ixe = E.ne - 2;
+  const double ue = (e - __ldg(E.egrid + k1)) / (__ldg(E.egrid + k2) - __ldg(E.egrid + k1));
+  bsearch_grid(E.ngrid, E.nn, nb, k1, k2);
+  int ixn = k1;
+  if (ixn > E.nn - 2) ixn = E.nn - 2;
+  if (ixn < 0) ixn = 0;
+  const double un = (nb - __ldg(E.ngrid + k1)) / (__ldg(E.ngrid + k2) - __ldg(E.ngrid + k1));
+  const double we0 = 1. - ue, we1 = ue;
+  const double wn0 = 1. - un, wn1 = un;
+  const int b00 = ixe + E.ne * ixn, b01 = ixe + E.ne * (ixn + 1);
+  double sp = 0.;
+  sp += we0 * wn0 * __ldg(E.p + b00);
+  sp += we0 * wn1 * __ldg(E.p + b01);
+  sp += we1 * wn0 * __ldg(E.p + b00 + 1);
+  sp += we1 * wn1 * __ldg(E.p + b01 + 1);
+  if (sp < 0.) sp = 0.;
+  p = sp;
+  if (WANT_T) {
+    double sT = 0., sm = 0.;
+    sT += we0 * wn0 * __ldg(E.T + b00);
+    sT += we0 * wn1 * __ldg(E.T + b01);
+    sT += we1 * wn0 * __ldg(E.T + b00 + 1);
+    sT += we1 * wn1 * __ldg(E.T + b01 + 1);
+    sm += we0 * wn0 * __ldg(E.mub + b00);
+    sm += we0 * wn1 * __ldg(E.mub + b01);
+    sm += we1 * wn0 * __ldg(E.mub + b00 + 1);
+    sm += we1 * wn1 * __ldg(E.mub + b01 + 1);
+    T = sT;
+    mub = sm;
+  }
+}
+
+__device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
+  if (E.kind == 0) return e / 3.;
+  double T, mub, p;
+  eos1f<false>(E, e, nb, T, mub, p);
+  return p;
+}
+
+__device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
+                                         double& T, double& mub, double& p) {
+  if (E.kind == 0) {
+    p = e / 3.;
+    T = e > 0. ? sqrt(sqrt(e / E.conf_cnst)) : 0.;
+    mub = 0.;
+  } else {
+    eos1f<true>(E, e, nb, T, mub, p);
+  }
+}
+
+// EoS::s, src/eos.cpp:18-25 (muq = mus = 0)
+__device__ __forceinline__ double eos_s(const EosDev& E, double e, double nb,
+                                        double nq, double ns) {
+  double T, mub, p;
+  const double muq = 0., mus = 0.;
+  eos_eval(E, e, nb, T, mub, p);
+  if (T > 0.0) return (e + p - mub * nb - muq * nq - mus * ns) / T;
+  return 0.;
+}
+
+// ----------------------------------------------------------- transformPV
+// src/rmn.cpp:28-139.  Q is the caller's copy and is rescaled in place when
+// |M| > Q_t, exactly as the reference does.
+__device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim& o) {
+  const int MAXIT = 100;
+  const double dpe = 1. / 3.;
+  const double corrf = 0.9999;
+  double v, vl = 0., vh = 1., dvold, dv, f, df;
+  double M = sqrt(Q[X_] * Q[X_] + Q[Y_] * Q[Y_] + Q[Z_] * Q[Z_]);
+  if (Q[T_] <= 0.) {
+    o.e = 0.; o.p = 0.;
+    o.vx = o.vy = o.vz = 0.;
+    o.nb = o.nq = o.ns = 0.;
+    return;
+  }
+  if (M == 0.) {
+    o.e = Q[T_];
+    o.vx = 0.; o.vy = 0.; o.vz = 0.;
+    o.nb = Q[NB_]; o.nq = Q[NQ_]; o.ns = Q[NS_];
+    o.p = eos_p(E, o.e, o.nb);
+    return;
+  }
+  if (M > Q[T_]) {
+    Q[X_] *= corrf * Q[T_] / M;
+    Q[Y_] *= corrf * Q[T_] / M;
+    Q[Z_] *= corrf * Q[T_] / M;
+    M = Q[T_] * corrf;
+  }
+  double e, p, nb, nq, ns;
+  v = 0.5 * (vl + vh);
+  e = Q[T_] - M * v;
+  if (e < 0.) e = 0.;
+  {
+    const double sq = sqrt(1 - v * v);
+    nb = Q[NB_] * sq;
+    nq = Q[NQ_] * sq;
+    ns = Q[NS_] * sq;
+  }
+  p = eos_p(E, e, nb);
+  f = (Q[T_] + p) * v - M;
+  df = (Q[T_] + p) - M * v * dpe;
+  dvold = vh - vl;
+  dv = dvold;
+  for (int i = 0; i < MAXIT; i++) {
+    if ((f + df * (vh - v)) * (f + df * (vl - v)) >= 0. ||
+        fabs(2. * f) > fabs(dvold * df)) {
+      dvold = dv;
+      dv = 0.5 * (vh - vl);
+      v = vl + dv;
+    } else {
+      dvold = dv;
+      dv = f / df;
+      v -= dv;
+    }
+    if (fabs(dv) < 0.00001) break;
+    e = Q[T_] - M * v;
+    if (e < 0.) e = 0.;
+    const double sq = sqrt(1 - v * v);
+    nb = Q[NB_] * sq;
+    nq = Q[NQ_] * sq;
+    ns = Q[NS_] * sq;
+    p = eos_p(E, e, nb);
+    f = (Q[T_] + p) * v - M;
+    df = (Q[T_] + p) - M * v * dpe;
+    if (f > 0.)
+      vh = v;
+    else
+      vl = v;
+  }
+  o.vx = v * Q[X_] / M;
+  o.vy = v * Q[Y_] / M;
+  o.vz = v * Q[Z_] / M;
+  o.e = Q[T_] - M * v;
+  o.p = eos_p(E, o.e, nb);  // the last iterate's nb, as the reference
+  const double sq = sqrt(1 - o.vx * o.vx - o.vy * o.vy - o.vz * o.vz);
+  o.nb = Q[NB_] * sq;
+  o.nq = Q[NQ_] * sq;
+  o.ns = Q[NS_] * sq;
+}
+
+// ------------------------------------------------- transport coefficients
+// TransportCoeff::zetaS, src/trancoeff.cpp:19-66; cs2(e) = 1/3 (src/eos.h:37)
+__device__ __forceinline__ double tr_zetaS(const TrDev& t, double e, double T,
+                                           double s, double P) {
+  const double cs2e = 1. / 3.;
+  const double T_p = 0.180, T_peak = 0.165, T_width = 0.010, B_norm = 0.24,
+               B_width = 1.5, T_peak2 = 0.160, B_norm2 = 0.13, B1 = 0.01, B2 = 0.12;
+  if (t.zetaSparam == 0) {
+    return t.zetaS0 * (1. / 3. - cs2e) / (exp((0.16 - T) / 0.001) + 1.);
+  } else if (t.zetaSparam == 1) {
+    if (T < 0.180)
+      return 0.03 + (0.08 * exp(((T / T_p) - 1.) / (0.0025))) +
+             (0.22 * exp(((T / T_p) - 1) / (0.022)));
+    else if (T >= 0.180 && T < 0.200)
+      return 27.55 * (T / T_p) - 13.45 - (13.77 * (T / T_p) * (T / T_p));
+    else if (T >= 0.200)
+      return 0.001 + (0.9 * exp(-((T / T_p) - 1.) / (0.0025))) +
+             (0.25 * exp(-((T / T_p) - 1.) / (0.13)));
+  } else if (t.zetaSparam == 2) {
+    if (T > T_peak)
+      return B_norm * ((B_width * B_width) /
+                       ((((T / T_peak) - 1.) * ((T / T_peak) - 1.)) + (B_width * B_width)));
+    else if (T <= T_peak)
+      return B_norm * (exp(-((T - T_peak) / T_width) * ((T - T_peak) / T_width)));
+  } else if (t.zetaSparam == 3) {
+    if (T < T_peak2)
+      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B1 * B1)));
+    else if (T >= T_peak2)
+      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B2 * B2)));
+  } else if (t.zetaSparam == 4) {
+    // abs(s) binds to int abs(int) in the reference: |s| < 1 reads as 0
+    if (!(fabs(s) >= 1.0) || T < 1e-1) return 0;
+    const double d = t.zetaSScaleBeta * (pow(e, 0.25) - pow(t.zetaSPeakEpsilon, 0.25));
+    const double sig = e < t.zetaSPeakEpsilon ? t.zetaSSigmaMinus : t.zetaSSigmaPlus;
+    return ((e + P) / (s * T)) * t.zetaS0 * exp(d * d / 2.0 * (sig * sig));
+  }
+  return 0.;
+}
+
+// TransportCoeff::etaS, src/trancoeff.cpp:73-90
+__device__ __forceinline__ double tr_etaS(const TrDev& t, double e, double rho,
+                                          double T, double muB, double s, double P) {
+  if (t.etaSparam == 0) {
+    return t.etaS0;
+  } else if (t.etaSparam == 1) {
+    return t.etaSMin + ((T > t.T0) ? t.ah * (T - t.T0) : t.al * (T - t.T0));
+  } else if (t.etaSparam == 2) {
+    return smax(0.0, t.etaSMin + ((e > t.etaSEpsilonMin)
+                                      ? ((t.ah * (e - t.etaSEpsilonMin) + t.aRho * rho))
+                                      : t.al * (e - t.etaSEpsilonMin) + t.aRho * rho));
+  } else if (t.etaSparam == 3) {
+    if (!(fabs(s) >= 1.0) || T < 1e-1) return 0;
+    const double Tc = t.T0 + t.etaSShiftMuB * (muB / 0.938);
+    return ((e + P) / (s * T)) *
+           smax(0.0, (t.etaSMin + ((T > Tc) ? t.ah * (T - Tc) : t.al * (T - Tc))) *
+                         (1 + t.etaSScaleMuB * (muB / 0.938)));
+  }
+  return 0.;
+}
+
+// TransportCoeff::getTau, src/trancoeff.cpp:92-100.  abs(e + P) binds to
+// int abs(int) in the reference: the test is trunc(e + P) != 0.
+__device__ __forceinline__ void tr_getTau(const TrDev& t, double e, double rho,
+                                          double T, double muB, double s, double P,
+                                          double& taupi, double& tauPi) {
+  if (T > 1e-1 && !(fabs(e + P) < 1.0)) {
+    taupi = (5. / 5.068) * s * tr_etaS(t, e, rho, T, muB, s, P) / (e + P);
+    tauPi = (6. / 5.068) * tr_zetaS(t, e, T, s, P) * s / (e + P);
+  } else {
+    taupi = tauPi = 0.;
+  }
+}
+
+// ---------------------------------------------------------- HLLE face flux
+// Hydro::hlle_flux, src/hdo.cpp:77-305, for one face given the two
+// reconstructed states (L = right edge of the left cell, R = left edge of
+// the right cell) and the fill fractions of the two cells in `dir`.
+// Returns false when the reference returns without adding a flux.
+__device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, double dt,
+                                          double dxdir, Prim l, Prim r, double mL,
+                                          double mR, double flux[7], unsigned& err) {
+  const double dta = predict ? dt / 2. : dt;
+  const double El = (l.e + l.p) / (1 - l.vx * l.vx - l.vy * l.vy - l.vz * l.vz);
+  const double Er = (r.e + r.p) / (1 - r.vx * r.vx - r.vy * r.vy - r.vz * r.vz);
+  const double tauFactor = predict ? tau + 0.25 * dt : tau + 0.5 * dt;
+  if (l.e < 0.) { l.e = 0.; l.p = 0.; }
+  if (r.e < 0.) { r.e = 0.; r.p = 0.; }
+  if (l.e > 1e10) { err |= ERR_E_HUGE; return false; }
+  if (l.e == 0. && r.e == 0.) return false;
+  if (mL < 1. && mR < 1.) return false;
+  const double cs2 = 1. / 3.;
+  const double cs = sqrt(1. / 3.);
+  const double gammal = 1. / sqrt(1 - l.vx * l.vx - l.vy * l.vy - l.vz * l.vz);
+  const double gammar = 1. / sqrt(1 - r.vx * r.vx - r.vy * r.vy - r.vz * r.vz);
+  const double U1l = gammal * gammal * (l.e + l.p) * l.vx;
+  const double U2l = gammal * gammal * (l.e + l.p) * l.vy;
+  const double U3l = gammal * gammal * (l.e + l.p) * l.vz;
+  const double U4l = gammal * gammal * (l.e + l.p) - l.p;
+  const double Ubl = gammal * l.nb, Uql = gammal * l.nq, Usl = gammal * l.ns;
+  const double U1r = gammar * gammar * (r.e + r.p) * r.vx;
+  const double U2r = gammar * gammar * (r.e + r.p) * r.vy;
+  const double U3r = gammar * gammar * (r.e + r.p) * r.vz;
+  const double U4r = gammar * gammar * (r.e + r.p) - r.p;
+  const double Ubr = gammar * r.nb, Uqr = gammar * r.nq, Usr = gammar * r.ns;
+  double Ftl, Fxl, Fyl, Fzl, Fbl, Fql, Fsl, Ftr, Fxr, Fyr, Fzr, Fbr, Fqr, Fsr;
+  double bl, br;
+  const double sEl = sqrt(El), sEr = sqrt(Er);
+  const double vnl = dir == X_ ? l.vx : (dir == Y_ ? l.vy : l.vz);
+  const double vnr = dir == X_ ? r.vx : (dir == Y_ ? r.vy : r.vz);
+  if (dir != Z_) {
+    Ftl = U4l * vnl + l.p * vnl;
+    Fxl = U1l * vnl;
+    Fyl = U2l * vnl;
+    Fzl = U3l * vnl;
+    Fbl = Ubl * vnl; Fql = Uql * vnl; Fsl = Usl * vnl;
+    Ftr = U4r * vnr + r.p * vnr;
+    Fxr = U1r * vnr;
+    Fyr = U2r * vnr;
+    Fzr = U3r * vnr;
+    Fbr = Ubr * vnr; Fqr = Uqr * vnr; Fsr = Usr * vnr;
+    if (dir == X_) { Fxl = Fxl + l.p; Fxr = Fxr + r.p; }
+    else { Fyl = Fyl + l.p; Fyr = Fyr + r.p; }
+  } else {
+    const double tau1 = tauFactor;
+    Ftl = U4l * vnl / tau1 + l.p * vnl / tau1;
+    Fxl = U1l * vnl / tau1;
+    Fyl = U2l * vnl / tau1;
+    Fzl = U3l * vnl / tau1 + l.p / tau1;
+    Fbl = Ubl * vnl / tau1; Fql = Uql * vnl / tau1; Fsl = Usl * vnl / tau1;
+    Ftr = U4r * vnr / tau1 + r.p * vnr / tau1;
+    Fxr = U1r * vnr / tau1;
+    Fyr = U2r * vnr / tau1;
+    Fzr = U3r * vnr / tau1 + r.p / tau1;
+    Fbr = Ubr * vnr / tau1; Fqr = Uqr * vnr / tau1; Fsr = Usr * vnr / tau1;
+  }
+  {
+    const double ss = sEl + sEr, dv = vnl - vnr;
+    const double csb = sqrt(cs2 + 0.5 * sqrt(El * Er) / (ss * ss) * (dv * dv));
+    const double vb = (sEl * vnl + sEr * vnr) / (sEl + sEr);
+    bl = smin(0., smin((vb - csb) / (1 - vb * csb), (vnl - cs) / (1 - vnl * cs)));
+    br = smax(0., smax((vb + csb) / (1 + vb * csb), (vnr + cs) / (1 + vnr * cs)));
+    if (dir == Z_) {
+      bl = 1. / tau * bl;
+      br = 1. / tau * br;
+      if (l.e == 0.) bl = -1. / tau;
+      if (r.e == 0.) br = 1. / tau;
+    } else {
+      if (l.e == 0.) bl = -1.;
+      if (r.e == 0.) br = 1.;
+    }
+  }
+  if (bl == 0. && br == 0.) return false;
+  const double pre = tauFactor * dta / dxdir;
+  const double den = -bl + br;
+  flux[T_] = pre * (-bl * br * (U4l - U4r) + br * Ftl - bl * Ftr) / den;
+  flux[X_] = pre * (-bl * br * (U1l - U1r) + br * Fxl - bl * Fxr) / den;
+  flux[Y_] = pre * (-bl * br * (U2l - U2r) + br * Fyl - bl * Fyr) / den;
+  flux[Z_] = pre * (-bl * br * (U3l - U3r) + br * Fzl - bl * Fzr) / den;
+  flux[NB_] = pre * (-bl * br * (Ubl - Ubr) + br * Fbl - bl * Fbr) / den;
+  flux[NQ_] = pre * (-bl * br * (Uql - Uqr) + br * Fql - bl * Fqr) / den;
+  flux[NS_] = pre * (-bl * br * (Usl - Usr) + br * Fsl - bl * Fsr) / den;
+  if (flux[NB_] != flux[NB_]) { err |= ERR_FLUX_NAN; return false; }
+  return true;
+}
+
+}  // namespace vh

@@ -1,0 +1,975 @@
+// vh_step.cu -- the kernels of one hydro timestep (Hydro::performStep,
+// src/hdo.cpp:1016-1134) on a structure-of-arrays FP64 grid.
+//
+// Data-parallel restructuring of the reference's sequential loops:
+//  * face kernels compute each HLLE face flux once (two con2prims per face)
+//    into a per-direction face array; a cell kernel then gathers the six
+//    faces in the reference's accumulation order (x-, x+, y-, y+, z-, z+,
+//    source), which keeps every cell's FP64 sum identical to the reference;
+//  * the viscous part stores the two cell-centred con2prims that every
+//    viscous stage re-derives (Qh at tau_n + dt/2 and Qh at tau_{n+1}) once
+//    per cell and reuses them, which is exact because the reference
+//    recomputes them from identical inputs;
+//  * ghost cells are a gather from a per-dimension source map simulated on
+//    the host from the reference's copy sequence (z, then y, then x).
+#include <cuda_runtime.h>
+
+#include "vh_physics.cuh"
+#include "vh_step.cuh"
+
+namespace vh {
+
+__device__ __forceinline__ long long cidx(const Geo& g, int ix, int iy, int iz) {
+  ix = ix > 0 ? ix : 0;
+  ix = ix < g.nx ? ix : g.nx - 1;
+  iy = iy > 0 ? iy : 0;
+  iy = iy < g.ny ? iy : g.ny - 1;
+  iz = iz > 0 ? iz : 0;
+  iz = iz < g.nz ? iz : g.nz - 1;
+  return (long long)ix + (long long)g.nx * iy + (long long)g.nx * g.ny * iz;
+}
+
+__device__ __forceinline__ void coords(const Geo& g, long long i, int& ix, int& iy, int& iz) {
+  ix = (int)(i % g.nx);
+  const long long r = i / g.nx;
+  iy = (int)(r % g.ny);
+  iz = (int)(r / g.ny);
+}
+
+__device__ __forceinline__ double maxM(const double* __restrict__ m, long long N, long long i) {
+  return smax(m[i], smax(m[N + i], m[2 * N + i]));
+}
+
+// -------------------------------------------------------------- updateM
+// Fluid::updateM, src/fld.cpp:384-423 (both passes; out of place).
+__global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restrict__ mo,
+                           double tau, double dt) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const long long N = g.N;
+  double d0 = 0., d1 = 0., d2 = 0.;
+  if (maxM(m, N, i) < 1.) {
+    if (m[cidx(g, ix + 1, iy, iz)] >= 1. || m[cidx(g, ix - 1, iy, iz)] >= 1.) d0 = dt / g.dx;
+    if (m[N + cidx(g, ix, iy + 1, iz)] >= 1. || m[N + cidx(g, ix, iy - 1, iz)] >= 1.)
+      d1 = dt / g.dy;
+    if (m[2 * N + cidx(g, ix, iy, iz + 1)] >= 1. || m[2 * N + cidx(g, ix, iy, iz - 1)] >= 1.)
+      d2 = dt / g.dz / tau;
+    if (d0 == 0. && d1 == 0.) {
+      if (maxM(m, N, cidx(g, ix + 1, iy + 1, iz)) >= 1. ||
+          maxM(m, N, cidx(g, ix + 1, iy - 1, iz)) >= 1. ||
+          maxM(m, N, cidx(g, ix - 1, iy + 1, iz)) >= 1. ||
+          maxM(m, N, cidx(g, ix - 1, iy - 1, iz)) >= 1.) {
+        d0 = 0.707 * dt / g.dx;
+        d1 = 0.707 * dt / g.dy;
+      }
+    }
+  }
+  // Cell::addM, src/cll.h:147-151, for X, Y, Z in turn
+  double a0 = m[i], a1 = m[N + i], a2 = m[2 * N + i];
+  a0 += d0;
+  if (a0 > 0.9) a0 = a1 = a2 = 1.;
+  a1 += d1;
+  if (a1 > 0.9) a0 = a1 = a2 = 1.;
+  a2 += d2;
+  if (a2 > 0.9) a0 = a1 = a2 = 1.;
+  mo[i] = a0;
+  mo[N + i] = a1;
+  mo[2 * N + i] = a2;
+}
+
+// ------------------------------------------------------------ face flux
+// One HLLE face between cell i and its +DIR neighbour (Hydro::hlle_flux with
+// Cell::getPrimVarRight / getPrimVarLeft or their H variants,
+// src/cll.cpp:106-204).  F[c*N + i] holds the flux of the face on the +DIR
+// side of cell i (0 where the reference adds nothing).
+template <int DIR, bool PRED>
+__global__ void __launch_bounds__(128) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
+                                              const double* __restrict__ m,
+                                              double* __restrict__ F, double tau, double dt,
+                                              unsigned* err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const long long N = g.N;
+  long long L = i, Lm, R, Rp;
+  if (DIR == X_) {
+    if (ix >= g.nx - 1) return;
+    Lm = cidx(g, ix - 1, iy, iz);
+    R = cidx(g, ix + 1, iy, iz);
+    Rp = cidx(g, ix + 2, iy, iz);
+  } else if (DIR == Y_) {
+    if (iy >= g.ny - 1) return;
+    Lm = cidx(g, ix, iy - 1, iz);
+    R = cidx(g, ix, iy + 1, iz);
+    Rp = cidx(g, ix, iy + 2, iz);
+  } else {
+    if (iz >= g.nz - 1) return;
+    Lm = cidx(g, ix, iy, iz - 1);
+    R = cidx(g, ix, iy, iz + 1);
+    Rp = cidx(g, ix, iy, iz + 2);
+  }
+  double ql[7], qr[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    const double a = QQ[k * N + Lm], b = QQ[k * N + L], c = QQ[k * N + R], d = QQ[k * N + Rp];
+    const double dQl = minmod((c - b) / 2., (b - a) / 2.);
+    ql[k] = (b + dQl) / tau;
+    const double dQr = minmod((d - c) / 2., (c - b) / 2.);
+    qr[k] = (c - dQr) / tau;
+  }
+  Prim pl, pr;
+  transform_pv(E, ql, pl);
+  transform_pv(E, qr, pr);
+  const double dxdir = DIR == X_ ? g.dx : (DIR == Y_ ? g.dy : g.dz);
+  double fl[7];
+  unsigned e = 0;
+  const bool ok = hlle_face(DIR, PRED, tau, dt, dxdir, pl, pr, m[(DIR - 1) * N + L],
+                            m[(DIR - 1) * N + R], fl, e);
+  if (e) atomicOr(err, e);
+#pragma unroll
+  for (int k = 0; k < 7; k++) F[k * N + i] = ok ? fl[k] : 0.;
+}
+
+// --------------------------------------------------- ideal cell update
+// Gathers the six face fluxes and the Milne source (Hydro::source_step,
+// src/hdo.cpp:307-353), then Cell::updateQtoQhByFlux (predictor) or
+// Cell::updateByFlux (corrector), src/cll.cpp:70-88.
+template <bool PRED>
+__global__ void __launch_bounds__(128) k_update(Geo g, EosDev E, double* __restrict__ Q,
+                                                double* __restrict__ Qh,
+                                                double* __restrict__ Qprev,
+                                                const double* __restrict__ Fx,
+                                                const double* __restrict__ Fy,
+                                                const double* __restrict__ Fz, double tau,
+                                                double dt, unsigned* err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const long long N = g.N;
+  const long long sy = g.nx, sz = (long long)g.nx * g.ny;
+  double fl[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    double a = 0.;
+    if (ix > 0) a += Fx[k * N + i - 1];
+    if (ix < g.nx - 1) a += -Fx[k * N + i];
+    if (iy > 0) a += Fy[k * N + i - sy];
+    if (iy < g.ny - 1) a += -Fy[k * N + i - 0];
+    if (iz > 0) a += Fz[k * N + i - sz];
+    if (iz < g.nz - 1) a += -Fz[k * N + i];
+    fl[k] = a;
+  }
+  const double* field = PRED ? Q : Qh;
+  const double tau1 = PRED ? tau : tau + 0.5 * dt;
+  const double _dt = PRED ? dt / 2. : dt;
+  double q[7], qin[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    qin[k] = field[k * N + i];
+    q[k] = qin[k] / tau1;
+  }
+  Prim pp;
+  transform_pv(E, q, pp);
+  double kk[7];
+  kk[T_] = -q[T_] * pp.vz * pp.vz - pp.p * (1. + pp.vz * pp.vz);
+  kk[X_] = 0.;
+  kk[Y_] = 0.;
+  kk[Z_] = -q[Z_];
+  kk[NB_] = 0.;
+  kk[NQ_] = 0.;
+  kk[NS_] = 0.;
+#pragma unroll
+  for (int k = 0; k < 7; k++) kk[k] *= _dt;
+  if (kk[NB_] != kk[NB_]) {
+    atomicOr(err, (unsigned)ERR_SOURCE_NAN);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 7; k++) fl[k] += kk[k];
+  }
+  if (PRED) {
+#pragma unroll
+    for (int k = 0; k < 7; k++) {
+      const double qk = Q[k * N + i];
+      Qprev[k * N + i] = qk;
+      Qh[k * N + i] = qk + fl[k];
+    }
+  } else {
+    if (!(Q[i] + fl[0] < 0.)) {
+#pragma unroll
+      for (int k = 0; k < 7; k++) Q[k * N + i] += fl[k];
+    }
+  }
+}
+
+// ------------------------------------------------------------- ghosts
+// Fluid::correctImagCells (FULL = false: Q and Qh) and correctImagCellsFull
+// (FULL = true: Q, pi, Pi), src/fld.cpp:211-382, as a gather from the
+// per-dimension source maps; copies into a ghost zero the row when Q_t < 0
+// (Cell::setQ / setQh).
+template <bool FULL>
+__global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char* __restrict__ isdst,
+                        double* __restrict__ Q, double* __restrict__ Qh,
+                        double* __restrict__ pi, double* __restrict__ Pi) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const int* sx = src;
+  const int* sy = src + g.nx;
+  const int* sz = src + g.nx + g.ny;
+  if (!(isdst[ix] | isdst[g.nx + iy] | isdst[g.nx + g.ny + iz])) return;
+  const long long N = g.N;
+  const long long s = (long long)sx[ix] + (long long)g.nx * (sy[iy] + (long long)g.ny * sz[iz]);
+  {
+    double q[7];
+#pragma unroll
+    for (int k = 0; k < 7; k++) q[k] = Q[k * N + s];
+    const bool neg = q[0] < 0.;
+#pragma unroll
+    for (int k = 0; k < 7; k++) Q[k * N + i] = neg ? 0. : q[k];
+  }
+  if (!FULL) {
+    double q[7];
+#pragma unroll
+    for (int k = 0; k < 7; k++) q[k] = Qh[k * N + s];
+    const bool neg = q[0] < 0.;
+#pragma unroll
+    for (int k = 0; k < 7; k++) Qh[k * N + i] = neg ? 0. : q[k];
+  } else {
+    double p[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) p[k] = pi[k * N + s];
+    const double P = Pi[s];
+#pragma unroll
+    for (int k = 0; k < 10; k++) pi[k * N + i] = p[k];
+    Pi[i] = P;
+  }
+}
+
+// ------------------------------------------------ viscous cell prims
+// The two cell-centred con2prims of the viscous stages:
+//  A = Qh / (tau - dt/2)  (getPrimVarHCenter in ISformal, NSquant, visc_flux,
+//                          visc_source_step),
+//  D = Qh / tau           (getPrimVarHCenter of the six NSquant neighbours).
+__global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, const double* __restrict__ Qh,
+                                                    double* __restrict__ pA,
+                                                    double* __restrict__ pD, double tau,
+                                                    double dt) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  const long long N = g.N;
+  double q[7], qh[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) qh[k] = Qh[k * N + i];
+  const double tA = tau - dt / 2.;
+#pragma unroll
+  for (int k = 0; k < 7; k++) q[k] = qh[k] / tA;
+  Prim a;
+  transform_pv(E, q, a);
+  pA[0 * N + i] = a.e;
+  pA[1 * N + i] = a.p;
+  pA[2 * N + i] = a.nb;
+  pA[3 * N + i] = a.nq;
+  pA[4 * N + i] = a.ns;
+  pA[5 * N + i] = a.vx;
+  pA[6 * N + i] = a.vy;
+  pA[7 * N + i] = a.vz;
+#pragma unroll
+  for (int k = 0; k < 7; k++) q[k] = qh[k] / tau;
+  Prim d;
+  transform_pv(E, q, d);
+  pD[0 * N + i] = d.e;
+  pD[1 * N + i] = d.vx;
+  pD[2 * N + i] = d.vy;
+  pD[3 * N + i] = d.vz;
+}
+
+__device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N, long long i) {
+  Prim a;
+  a.e = pA[i];
+  a.p = pA[N + i];
+  a.nb = pA[2 * N + i];
+  a.nq = pA[3 * N + i];
+  a.ns = pA[4 * N + i];
+  a.vx = pA[5 * N + i];
+  a.vy = pA[6 * N + i];
+  a.vz = pA[7 * N + i];
+  return a;
+}
+
+// ------------------------------------------------ ISformal, loop #1
+// Hydro::ISformal loop 1 with Hydro::NSquant inlined (src/hdo.cpp:381-652,
+// 690-864): Navier-Stokes shear/bulk from the velocity gradients, then the
+// two-stage Israel-Stewart relaxation with Christoffel and cross terms.
+// Writes pi0/piH0/Pi0/PiH0 and the first flux contribution
+// (+(tau-dt) * delta Q_n).
+__global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
+                                                  const double* __restrict__ Q,
+                                                  const double* __restrict__ Qprev,
+                                                  const double* __restrict__ m,
+                                                  const double* __restrict__ pA,
+                                                  const double* __restrict__ pD,
+                                                  const double* __restrict__ pi,
+                                                  const double* __restrict__ Pi,
+                                                  double* __restrict__ pi0,
+                                                  double* __restrict__ piH0,
+                                                  double* __restrict__ Pi0,
+                                                  double* __restrict__ PiH0,
+                                                  double* __restrict__ flux, double tau,
+                                                  double dt, unsigned* err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const long long N = g.N;
+  const Prim A = loadA(pA, N, i);
+  if (A.e <= 0.) {
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+      piH0[k * N + i] = 0.0;
+      pi0[k * N + i] = 0.0;
+    }
+    PiH0[i] = 0.0;
+    Pi0[i] = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) flux[k * N + i] = 0.;
+    return;
+  }
+  const double gmumu[4] = {1., -1., -1., -1.};
+  double cpi[10];
+#pragma unroll
+  for (int k = 0; k < 10; k++) cpi[k] = pi[k * N + i];
+  const double cPi = Pi[i];
+#define PI(a, b) cpi[index44(a, b)]
+  const double vx = A.vx, vy = A.vy, vz = A.vz;
+  const double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
+  double u[4];
+  u[0] = gamma;
+  u[1] = u[0] * vx;
+  u[2] = u[0] * vy;
+  u[3] = u[0] * vz;
+  {
+    double f[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) f[k] = (tau - dt) * (PI(0, k) + cPi * u[0] * u[k]);
+    f[0] += -(tau - dt) * cPi;
+#pragma unroll
+    for (int k = 0; k < 4; k++) flux[k * N + i] = 0. + f[k];
+  }
+  // thermodynamics at the cell (shared by NSquant and ISformal)
+  double T, mub, p;
+  eos_eval(E, A.e, A.nb, T, mub, p);
+  const double s = eos_s(E, A.e, A.nb, A.nq, A.ns);
+  const double etaS = tr_etaS(tr, A.e, A.nb, T, mub, s, p);
+  const double zetaS = tr_zetaS(tr, A.e, T, s, p);
+
+  // ------------------------------------------------------ NSquant
+  double piNS[10], PiNS, du;
+  double dmu[4][4];
+  const bool vac = maxM(m, N, cidx(g, ix + 1, iy, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix, iy + 1, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix - 1, iy, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix, iy - 1, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix + 1, iy + 1, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix + 1, iy - 1, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix - 1, iy + 1, iz)) <= 0.9 ||
+                   maxM(m, N, cidx(g, ix - 1, iy - 1, iz)) <= 0.9;
+  if (vac) {
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b < 4; b++) dmu[a][b] = 0.;
+#pragma unroll
+    for (int k = 0; k < 10; k++) piNS[k] = 0.;
+    PiNS = du = 0.;
+  } else {
+    const double VMIN = 1e-2;
+    const double UDIFF = 3.0;
+    double q[7];
+    Prim P0, P1;
+#pragma unroll
+    for (int k = 0; k < 7; k++) q[k] = Qprev[k * N + i] / (tau - dt);
+    transform_pv(E, q, P0);
+#pragma unroll
+    for (int k = 0; k < 7; k++) q[k] = Q[k * N + i] / tau;
+    transform_pv(E, q, P1);
+    const double e0 = P0.e, e1 = A.e;
+    double ut0 = 1.0 / sqrt(1.0 - P0.vx * P0.vx - P0.vy * P0.vy - P0.vz * P0.vz);
+    double ux0 = ut0 * P0.vx, uy0 = ut0 * P0.vy, uz0 = ut0 * P0.vz;
+    double ut1 = 1.0 / sqrt(1.0 - P1.vx * P1.vx - P1.vy * P1.vy - P1.vz * P1.vz);
+    double ux1 = ut1 * P1.vx, uy1 = ut1 * P1.vy, uz1 = ut1 * P1.vz;
+    double uuu[4];
+    uuu[0] = u[0];
+    uuu[1] = u[1];
+    uuu[2] = u[2];
+    uuu[3] = u[3];
+    dmu[0][0] = (ut1 * ut1 - ut0 * ut0) / 2. / uuu[0] / dt;
+    dmu[0][1] = (ux1 * ux1 - ux0 * ux0) / 2. / uuu[1] / dt;
+    dmu[0][2] = (uy1 * uy1 - uy0 * uy0) / 2. / uuu[2] / dt;
+    dmu[0][3] = (uz1 * uz1 - uz0 * uz0) / 2. / uuu[3] / dt;
+    if (fabs(0.5 * (ut1 + ut0) / ut1) > UDIFF) dmu[0][0] = (ut1 - ut0) / dt;
+    if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / ux1) > UDIFF) dmu[0][1] = (ux1 - ux0) / dt;
+    if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uy1) > UDIFF) dmu[0][2] = (uy1 - uy0) / dt;
+    if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uz1) > UDIFF) dmu[0][3] = (uz1 - uz0) / dt;
+    if (e1 <= 0. || e0 <= 0.) dmu[0][0] = dmu[0][1] = dmu[0][2] = dmu[0][3] = 0.;
+#pragma unroll
+    for (int d = 1; d <= 3; d++) {
+      long long ip, im;
+      if (d == 1) {
+        ip = cidx(g, ix + 1, iy, iz);
+        im = cidx(g, ix - 1, iy, iz);
+      } else if (d == 2) {
+        ip = cidx(g, ix, iy + 1, iz);
+        im = cidx(g, ix, iy - 1, iz);
+      } else {
+        ip = cidx(g, ix, iy, iz + 1);
+        im = cidx(g, ix, iy, iz - 1);
+      }
+      const double ep = pD[ip], em = pD[im];
+      if (ep > 0. && em > 0.) {
+        const double vx1 = pD[N + ip], vy1 = pD[2 * N + ip], vz1 = pD[3 * N + ip];
+        const double vx0 = pD[N + im], vy0 = pD[2 * N + im], vz0 = pD[3 * N + im];
+        ut0 = 1.0 / sqrt(1.0 - vx0 * vx0 - vy0 * vy0 - vz0 * vz0);
+        ux0 = ut0 * vx0;
+        uy0 = ut0 * vy0;
+        uz0 = ut0 * vz0;
+        ut1 = 1.0 / sqrt(1.0 - vx1 * vx1 - vy1 * vy1 - vz1 * vz1);
+        ux1 = ut1 * vx1;
+        uy1 = ut1 * vy1;
+        uz1 = ut1 * vz1;
+        if (d < 3) {
+          const double h = d == 1 ? g.dx : g.dy;
+          dmu[d][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / h;
+          dmu[d][1] = 0.25 * (ux1 * ux1 - ux0 * ux0) / uuu[1] / h;
+          dmu[d][2] = 0.25 * (uy1 * uy1 - uy0 * uy0) / uuu[2] / h;
+          dmu[d][3] = 0.25 * (uz1 * uz1 - uz0 * uz0) / uuu[3] / h;
+          if (fabs(0.5 * (ut1 + ut0) / uuu[0]) > UDIFF) dmu[d][0] = 0.5 * (ut1 - ut0) / h;
+          if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / uuu[1]) > UDIFF)
+            dmu[d][1] = 0.5 * (ux1 - ux0) / h;
+          if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uuu[2]) > UDIFF)
+            dmu[d][2] = 0.5 * (uy1 - uy0) / h;
+          if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uuu[3]) > UDIFF)
+            dmu[d][3] = 0.5 * (uz1 - uz0) / h;
+        } else {
+          const double dz = g.dz, th = tau + 0.5 * dt;
+          dmu[3][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / dz / th;
+          dmu[3][1] = 0.25 * (ux1 * ux1 - ux0 * ux0) / uuu[1] / dz / th;
+          dmu[3][2] = 0.25 * (uy1 * uy1 - uy0 * uy0) / uuu[2] / dz / th;
+          dmu[3][3] = 0.25 * (uz1 * uz1 - uz0 * uz0) / uuu[3] / dz / th;
+          if (fabs(0.5 * (ut1 + ut0) / uuu[0]) > UDIFF) dmu[3][0] = 0.5 * (ut1 - ut0) / dz / th;
+          if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / uuu[1]) > UDIFF)
+            dmu[3][1] = 0.5 * (ux1 - ux0) / dz / th;
+          if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uuu[2]) > UDIFF)
+            dmu[3][2] = 0.5 * (uy1 - uy0) / dz / th;
+          if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uuu[3]) > UDIFF)
+            dmu[3][3] = 0.5 * (uz1 - uz0) / dz / th;
+        }
+      } else {
+        dmu[d][0] = dmu[d][1] = dmu[d][2] = dmu[d][3] = 0.;
+      }
+    }
+    dmu[3][0] += uuu[3] / (tau - 0.5 * dt);
+    dmu[3][3] += uuu[0] / (tau - 0.5 * dt);
+    const double gdiag[4] = {1., -1., -1., -1.};
+    // sigma contraction with Z^{mu nu lambda rho} (src/hdo.cpp:613-637);
+    // the result is symmetric in (mu, nu), so only a <= b... b <= a is formed.
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int b = 0; b <= a; b++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+#pragma unroll
+          for (int l = 0; l < 4; l++) {
+            double Z = 0.0;
+            const double gak = (a == k) ? gdiag[a] : 0.;
+            const double gbk = (b == k) ? gdiag[b] : 0.;
+            const double gab = (a == b) ? gdiag[a] : 0.;
+            if (b == l) Z += 0.5 * (gak - uuu[a] * uuu[k]);
+            if (a == l) Z += 0.5 * (gbk - uuu[b] * uuu[k]);
+            if (k == l) Z -= (gab - uuu[a] * uuu[b]) / 3.0;
+            acc += Z * dmu[k][l] * 2.0 * etaS * s / 5.068;
+          }
+        piNS[index44(a, b)] = acc;
+      }
+    PiNS = -zetaS * s * (dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3]) / 5.068;
+    du = dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3];
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < 10; k++) bad |= isinf(piNS[k]) || isnan(piNS[k]);
+    if (bad) atomicOr(err, (unsigned)ERR_NSQUANT_NAN);
+  }
+#define PINS(a, b) piNS[index44(a, b)]
+
+  // ------------------------------------------------ ISformal loop 1 body
+  const double eta = etaS * s;
+  double sig[10];
+#pragma unroll
+  for (int k = 0; k < 10; k++) {
+    sig[k] = 0.5 * piNS[k] / eta * 5.068;
+    if (eta <= 0.0) sig[k] = 0.0;
+  }
+#define SIG(a, b) sig[index44(a, b)]
+  double taupi, tauPi;
+  tr_getTau(tr, A.e, A.nb, T, mub, s, p, taupi, tauPi);
+  double deltapipi = 4. / 3., taupipi = 10. / 7., lambdapiPi = 6. / 5.;
+  double phi7 = 9. / 70. / eos_p(E, A.e, A.nb);
+  if (isinf(phi7)) phi7 = 0.0;
+  phi7 = phi7 / taupi;
+  if (taupi < 0.5 * dt) deltapipi = taupipi = lambdapiPi = phi7 = 0.0;
+  double delPiPi = 2. / 3.;
+  double lamPipi = 8. / 5. * (1. / 3. - 1. / 3.);
+  if (tauPi < 0.5 * dt) delPiPi = lamPipi = 0.0;
+  double Delta[10];
+  double h0[10];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b <= a; b++) {
+      const int k = index44(a, b);
+      Delta[k] = -u[a] * u[b];
+      if (a == b) Delta[k] += gmumu[a];
+      if (taupi > 0.5 * dt)
+        h0[k] = PI(a, b) - (PI(a, b) - PINS(a, b)) * dt / 2.0 / gamma / taupi;
+      else
+        h0[k] = PINS(a, b);
+    }
+  double H0;
+  if (tauPi > 0.5 * dt)
+    H0 = cPi - (cPi - PiNS) * dt / 2.0 / gamma / tauPi;
+  else
+    H0 = PiNS;
+  double tau1 = tau - dt * 0.75;
+  h0[index44(0, 0)] += -2. * vz * PI(0, 3) / tau1 * dt / 2.;
+  h0[index44(3, 3)] += -(2. * vz / tau1 * PI(0, 3)) * dt / 2.;
+  h0[index44(3, 0)] += -(vz / tau1 * PI(0, 0) + vz / tau1 * PI(3, 3)) * dt / 2.;
+  h0[index44(1, 0)] += -vz / tau1 * PI(1, 3) * dt / 2.;
+  h0[index44(2, 0)] += -vz / tau1 * PI(2, 3) * dt / 2.;
+  h0[index44(3, 1)] += -(vz / tau1 * PI(0, 1)) * dt / 2.;
+  h0[index44(3, 2)] += -(vz / tau1 * PI(0, 2)) * dt / 2.;
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b <= a; b++) {
+      double acc = h0[index44(a, b)];
+      acc += (-deltapipi * PI(a, b) * du + lambdapiPi * cPi * SIG(a, b)) / gamma * 0.5 * dt;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        acc += (phi7 * PI(a, k) * PI(b, k) * gmumu[k] -
+                taupipi * 0.5 * (PI(a, k) * SIG(b, k) * gmumu[k] + PI(b, k) * SIG(a, k) * gmumu[k])) /
+               gamma * 0.5 * dt;
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          acc += (-PI(a, k) * u[b] - PI(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k] / gamma * 0.5 * dt -
+                 1. / 3. * Delta[index44(a, b)] * PI(k, l) * (phi7 * PI(k, l) - taupipi * SIG(k, l)) *
+                     gmumu[k] * gmumu[l] / gamma * 0.5 * dt;
+        }
+      }
+      h0[index44(a, b)] = acc;
+    }
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      H0 += lamPipi * PI(k, l) * SIG(k, l) * gmumu[k] * gmumu[l] / gamma * 0.5 * dt;
+  H0 += -delPiPi * cPi * du / gamma * 0.5 * dt;
+#define H(a, b) h0[index44(a, b)]
+  double f0[10];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b <= a; b++) {
+      if (taupi > 0.5 * dt)
+        f0[index44(a, b)] = PI(a, b) - (H(a, b) - PINS(a, b)) * dt / gamma / taupi;
+      else
+        f0[index44(a, b)] = PINS(a, b);
+    }
+  double F0;
+  if (tauPi > 0.5 * dt)
+    F0 = cPi - (H0 - PiNS) * dt / gamma / tauPi;
+  else
+    F0 = PiNS;
+  tau1 = tau - dt * 0.5;
+  f0[index44(0, 0)] += -2. * vz / tau1 * H(0, 3) * dt;
+  f0[index44(3, 3)] += -(2. * vz / tau1 * H(0, 3)) * dt;
+  f0[index44(3, 0)] += -(vz / tau1 * H(0, 0) + vz / tau1 * H(3, 3)) * dt;
+  f0[index44(1, 0)] += -vz / tau1 * H(1, 3) * dt;
+  f0[index44(2, 0)] += -vz / tau1 * H(2, 3) * dt;
+  f0[index44(3, 1)] += -(vz / tau1 * H(0, 1)) * dt;
+  f0[index44(3, 2)] += -(vz / tau1 * H(0, 2)) * dt;
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b <= a; b++) {
+      double acc = f0[index44(a, b)];
+      acc += (-deltapipi * H(a, b) * du + lambdapiPi * H0 * SIG(a, b)) / gamma * dt;
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        acc += (phi7 * PI(a, k) * H(b, k) * gmumu[k] -
+                taupipi * 0.5 * (H(a, k) * SIG(b, k) * gmumu[k] + H(b, k) * SIG(a, k) * gmumu[k])) /
+               gamma * dt;
+#pragma unroll
+        for (int l = 0; l < 4; l++) {
+          acc += ((-H(a, k) * u[b] - H(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k] -
+                  1. / 3. * Delta[index44(a, b)] * H(k, l) * (phi7 * H(k, l) - taupipi * SIG(k, l)) *
+                      gmumu[k] * gmumu[l]) /
+                 gamma * dt;
+        }
+      }
+      f0[index44(a, b)] = acc;
+    }
+#pragma unroll
+  for (int k = 0; k < 4; k++)
+#pragma unroll
+    for (int l = 0; l < 4; l++)
+      F0 += lamPipi * H(k, l) * SIG(k, l) * gmumu[k] * gmumu[l] / gamma * dt;
+  F0 += -delPiPi * H0 * du / gamma * dt;
+#pragma unroll
+  for (int k = 0; k < 10; k++) {
+    piH0[k * N + i] = h0[k];
+    pi0[k * N + i] = f0[k];
+  }
+  PiH0[i] = H0;
+  Pi0[i] = F0;
+#undef PI
+#undef PINS
+#undef SIG
+#undef H
+}
+
+// ------------------------------------------------ ISformal, loop #2
+// Semi-Lagrangian advection of pi0/piH0 from the 2x2x2 upwind cells, the
+// viscous-correction limiter and the -(tau) * delta Q_{n+1} flux
+// (src/hdo.cpp:866-962).
+__device__ __forceinline__ double sgn(double x) {
+  if (x > 0) return 1.;
+  if (x < 0.) return -1.;
+  return 0.;
+}
+
+__global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restrict__ pA,
+                                                   const double* __restrict__ pi0,
+                                                   const double* __restrict__ piH0,
+                                                   const double* __restrict__ Pi0,
+                                                   const double* __restrict__ PiH0,
+                                                   double* __restrict__ pi, double* __restrict__ piH,
+                                                   double* __restrict__ Pi, double* __restrict__ PiH,
+                                                   double* __restrict__ vcc,
+                                                   double* __restrict__ flux, double tau,
+                                                   double dt) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const long long N = g.N;
+  const Prim A = loadA(pA, N, i);
+  if (A.e <= 0.) return;
+  const double e = A.e, p = A.p, vx = A.vx, vy = A.vy, vz = A.vz;
+  const double xm = -vx * dt / g.dx;
+  const double ym = -vy * dt / g.dy;
+  const double zm = -vz * dt / g.dz / (tau - 0.5 * dt);
+  const double xmH = -vx * dt / g.dx / 2.0;
+  const double ymH = -vy * dt / g.dy / 2.0;
+  const double zmH = -vz * dt / g.dz / (tau - 0.5 * dt) / 2.0;
+  const double wx[2] = {(1. - fabs(xm)), fabs(xm)};
+  const double wy[2] = {(1. - fabs(ym)), fabs(ym)};
+  const double wz[2] = {(1. - fabs(zm)), fabs(zm)};
+  const double wxH[2] = {(1. - fabs(xmH)), fabs(xmH)};
+  const double wyH[2] = {(1. - fabs(ymH)), fabs(ymH)};
+  const double wzH[2] = {(1. - fabs(zmH)), fabs(zmH)};
+  const int sx = (int)sgn(xm), sy = (int)sgn(ym), sz = (int)sgn(zm);
+  double a[10], aH[10], P = 0.0, PH = 0.0;
+#pragma unroll
+  for (int k = 0; k < 10; k++) a[k] = aH[k] = 0.0;
+#pragma unroll
+  for (int jx = 0; jx < 2; jx++)
+#pragma unroll
+    for (int jy = 0; jy < 2; jy++)
+#pragma unroll
+      for (int jz = 0; jz < 2; jz++) {
+        const long long c1 = cidx(g, ix + jx * sx, iy + jy * sy, iz + jz * sz);
+        const double w = wx[jx] * wy[jy] * wz[jz];
+        const double wH = wxH[jx] * wyH[jy] * wzH[jz];
+#pragma unroll
+        for (int k = 0; k < 10; k++) {
+          a[k] += w * pi0[k * N + c1];
+          aH[k] += wH * piH0[k * N + c1];
+        }
+        P += w * Pi0[c1];
+        PH += wH * PiH0[c1];
+      }
+  const double maxT0 = smax((e + p) / (1. - vx * vx - vy * vy - vz * vz) - p,
+                            (e + p) * (vx * vx + vy * vy + vz * vz) / (1. - vx * vx - vy * vy - vz * vz) + p);
+  double maxpi = 0.;
+#pragma unroll
+  for (int k = 0; k < 10; k++)
+    if (fabs(a[k]) > maxpi) maxpi = fabs(a[k]);
+  bool rescaled = false;
+  if (maxT0 / maxpi < 1.0) {
+#pragma unroll
+    for (int k = 0; k < 10; k++) {
+      a[k] = 0.1 * a[k] * maxT0 / maxpi;
+      aH[k] = 0.1 * aH[k] * maxT0 / maxpi;
+    }
+    rescaled = true;
+  }
+  if (fabs(P) > p) {
+    if (P != 0.) P = 1 * P / fabs(P) * p;
+    if (PH != 0.) PH = 1 * PH / fabs(PH) * p;
+    rescaled = true;
+  }
+  vcc[i] = rescaled ? maxT0 / maxpi : 1.;
+#pragma unroll
+  for (int k = 0; k < 10; k++) {
+    pi[k * N + i] = a[k];
+    piH[k * N + i] = aH[k];
+  }
+  Pi[i] = P;
+  PiH[i] = PH;
+  const double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
+  double u[4];
+  u[0] = gamma;
+  u[1] = u[0] * vx;
+  u[2] = u[0] * vy;
+  u[3] = u[0] * vz;
+  double f[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) f[k] = -tau * (a[index44(0, k)] + P * u[0] * u[k]);
+  f[0] += tau * P;
+#pragma unroll
+  for (int k = 0; k < 4; k++) flux[k * N + i] += f[k];
+}
+
+// --------------------------------------------- viscous flux + update
+// Hydro::visc_flux (src/hdo.cpp:966-1014) for the six faces of the cell,
+// visc_source_step (src/hdo.cpp:355-375) and Cell::updateByViscFlux
+// (src/cll.cpp:76-84).
+__device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const Geo& g,
+                                          const double* __restrict__ pA,
+                                          const double* __restrict__ piH,
+                                          const double* __restrict__ PiH,
+                                          const double* __restrict__ m, long long L, long long R,
+                                          double f[4]) {
+  const long long N = g.N;
+  if (m[(dir - 1) * N + L] < 1. && m[(dir - 1) * N + R] < 1.) return false;
+  double dxa;
+  if (dir == X_)
+    dxa = g.dx;
+  else if (dir == Y_)
+    dxa = g.dy;
+  else
+    dxa = g.dz * (tau + 0.5 * dt);
+  double vxl = pA[5 * N + L], vyl = pA[6 * N + L], vzl = pA[7 * N + L];
+  const double vxr = pA[5 * N + R], vyr = pA[6 * N + R], vzr = pA[7 * N + R];
+  vxl = 0.5 * (vxl + vxr);
+  vyl = 0.5 * (vyl + vyr);
+  vzl = 0.5 * (vzl + vzr);
+  const double v = sqrt(vxl * vxl + vyl * vyl + vzl * vzl);
+  if (v > 1.) {
+    vxl = 0.99 * vxl / v;
+    vyl = 0.99 * vyl / v;
+    vzl = 0.99 * vzl / v;
+  }
+  const double gamma = 1. / sqrt(1. - v * v);
+  const double uuu[4] = {gamma, gamma * vxl, gamma * vyl, gamma * vzl};
+  const double gmumu[4] = {1., -1., -1., -1.};
+  const double PL = PiH[L], PR = PiH[R];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    const int k = index44(a, dir);
+    double x = 0.5 * (piH[k * N + L] + piH[k * N + R]);
+    if (a == dir) x += -0.5 * (PL + PR) * gmumu[a];
+    x += 0.5 * (PL + PR) * uuu[a] * uuu[dir];
+    f[a] = x * (tau - 0.5 * dt) * dt / dxa;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(128) k_visc_update(Geo g, const double* __restrict__ pA,
+                                                     const double* __restrict__ piH,
+                                                     const double* __restrict__ PiH,
+                                                     const double* __restrict__ m,
+                                                     const double* __restrict__ flux,
+                                                     double* __restrict__ Q, double tau,
+                                                     double dt) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const long long N = g.N;
+  double fl[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) fl[k] = flux[k * N + i];
+  double f[4];
+  const long long st[3] = {1, g.nx, (long long)g.nx * g.ny};
+  const int cc[3] = {ix, iy, iz};
+  const int nn[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    if (cc[d] > 0 && visc_face(d + 1, tau, dt, g, pA, piH, PiH, m, i - st[d], i, f)) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) fl[k] += f[k];
+    }
+    if (cc[d] < nn[d] - 1 && visc_face(d + 1, tau, dt, g, pA, piH, PiH, m, i, i + st[d], f)) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) fl[k] += -f[k];
+    }
+  }
+  const double e = pA[i];
+  if (!(e <= 0.)) {
+    const double vx = pA[5 * N + i], vy = pA[6 * N + i], vz = pA[7 * N + i];
+    double uuu[4];
+    uuu[0] = 1. / sqrt(1. - vx * vx - vy * vy - vz * vz);
+    uuu[1] = uuu[0] * vx;
+    uuu[2] = uuu[0] * vy;
+    uuu[3] = uuu[0] * vz;
+    const double PH = PiH[i];
+    double k0 = -piH[index44(3, 3) * N + i] + PH * (-1.0 - uuu[3] * uuu[3]);
+    double k3 = -(piH[index44(0, 3) * N + i] + PH * uuu[0] * uuu[3]);
+    k0 *= dt;
+    k3 *= dt;
+    fl[0] += k0;
+    fl[1] += 0. * dt;
+    fl[2] += 0. * dt;
+    fl[3] += k3;
+  }
+  const double q0 = Q[i];
+  if (fabs(fl[0]) <= 0.5 * q0) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) Q[k * N + i] += fl[k];
+#pragma unroll
+    for (int k = 4; k < 7; k++) Q[k * N + i] += 0.;
+  } else if (fl[0] != 0.) {
+    const double fac = fabs(0.5 * q0 / fl[0]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) Q[k * N + i] += fac * fl[k];
+#pragma unroll
+    for (int k = 4; k < 7; k++) Q[k * N + i] += fac * 0.;
+  }
+}
+
+// --------------------------------------------------- batched transformPV
+__global__ void k_transform_pv(EosDev E, const double* __restrict__ Q, long long n,
+                               double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double q[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) q[k] = Q[k * n + i];
+  Prim o;
+  transform_pv(E, q, o);
+  out[0 * n + i] = o.e;
+  out[1 * n + i] = o.p;
+  out[2 * n + i] = o.nb;
+  out[3 * n + i] = o.nq;
+  out[4 * n + i] = o.ns;
+  out[5 * n + i] = o.vx;
+  out[6 * n + i] = o.vy;
+  out[7 * n + i] = o.vz;
+}
+
+// ------------------------------------------------------------ launcher
+static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+const char* const kKernelNames[KK_COUNT] = {
+    "k_update_m", "k_face_x", "k_face_y", "k_face_z", "k_update", "k_ghost",
+    "k_visc_prims", "k_is_relax", "k_is_advect", "k_visc_update"};
+
+int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
+  const Geo& g = a.g;
+  const int bs = 128;
+  const unsigned nb = nblk(g.N, bs);
+  int launches = 0;
+  const Fields& F = a.f;
+  auto done = [&](int kind) {
+    launches++;
+    if (mk) mk->after(kind);
+  };
+  k_update_m<<<nb, bs, 0, s>>>(g, F.m, F.m2, a.tau, a.dt);
+  done(KK_UPDATE_M);
+  const double* m = F.m2;  // the updated fill fractions
+  // predictor (src/hdo.cpp:1023-1060) and corrector (src/hdo.cpp:1062-1094)
+  for (int pass = 0; pass < 2; pass++) {
+    const bool pred = pass == 0;
+    const double* QQ = pred ? F.Q : F.Qh;
+    if (pred) {
+      k_face<X_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.tau, a.dt, F.err);
+      done(KK_FACE_X);
+      k_face<Y_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.tau, a.dt, F.err);
+      done(KK_FACE_Y);
+      if (g.nz > 1) {
+        k_face<Z_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.tau, a.dt, F.err);
+        done(KK_FACE_Z);
+      }
+      k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.tau,
+                                       a.dt, F.err);
+      done(KK_UPDATE);
+    } else {
+      k_face<X_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.tau, a.dt, F.err);
+      done(KK_FACE_X);
+      k_face<Y_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.tau, a.dt, F.err);
+      done(KK_FACE_Y);
+      if (g.nz > 1) {
+        k_face<Z_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.tau, a.dt, F.err);
+        done(KK_FACE_Z);
+      }
+      k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.tau,
+                                        a.dt, F.err);
+      done(KK_UPDATE);
+    }
+  }
+  const double tau1 = a.tau + a.dt;  // tau += dt (src/hdo.cpp:1095)
+  k_ghost<false><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
+  done(KK_GHOST);
+  if (a.viscous) {
+    k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, F.Qh, F.pA, F.pD, tau1, a.dt);
+    done(KK_VISC_PRIMS);
+    k_is_relax<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pi, F.Pi, F.pi0,
+                                 F.piH0, F.Pi0, F.PiH0, F.flux, tau1, a.dt, F.err);
+    done(KK_IS_RELAX);
+    k_is_advect<<<nb, bs, 0, s>>>(g, F.pA, F.pi0, F.piH0, F.Pi0, F.PiH0, F.pi, F.piH, F.Pi, F.PiH,
+                                  F.vcc, F.flux, tau1, a.dt);
+    done(KK_IS_ADVECT);
+    k_visc_update<<<nb, bs, 0, s>>>(g, F.pA, F.piH, F.PiH, m, F.flux, F.Q, tau1, a.dt);
+    done(KK_VISC_UPDATE);
+  }
+  k_ghost<true><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
+  done(KK_GHOST);
+  return launches;
+}
+
+void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
+                         cudaStream_t s) {
+  k_transform_pv<<<nblk(n, 128), 128, 0, s>>>(E, Q, n, out);
+}
+
+// ------------------------------------------------------- small helpers
+__global__ void k_fill(double* __restrict__ p, long long n, double v) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// Cell::setQ (src/cll.h:75-80): a row with Q_t < 0 becomes zero.
+__global__ void k_zero_negative_rows(double* __restrict__ Q, long long N) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  if (Q[i] < 0.) {
+#pragma unroll
+    for (int k = 0; k < 7; k++) Q[k * N + i] = 0.;
+  }
+}
+
+void launch_fill(double* p, long long n, double v, cudaStream_t s) {
+  if (n > 0) k_fill<<<nblk(n, 256), 256, 0, s>>>(p, n, v);
+}
+
+void launch_zero_negative_rows(double* Q, long long N, cudaStream_t s) {
+  if (N > 0) k_zero_negative_rows<<<nblk(N, 256), 256, 0, s>>>(Q, N);
+}
+
+}  // namespace vh

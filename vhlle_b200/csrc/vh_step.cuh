@@ -1,0 +1,63 @@
+// vh_step.cuh -- internal interface between the C ABI (vh_capi.cu) and the
+// step kernels (vh_step.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "vh_physics.cuh"
+
+namespace vh {
+
+struct Geo {
+  int nx, ny, nz;
+  long long N;
+  double dx, dy, dz;
+};
+
+// Device pointers of every field the step touches (component-major).
+struct Fields {
+  double *Q, *Qh, *Qprev;        // [7][N]
+  double *pi, *piH;              // [10][N]
+  double *Pi, *PiH, *vcc;        // [N]
+  double *m, *m2;                // [3][N] fill fractions (double-buffered)
+  double *Fx, *Fy, *Fz;          // [7][N] face fluxes on the +dir side
+  double *flux;                  // [4][N] viscous flux accumulator
+  double *pA;                    // [8][N] prims of Qh at tau_{n+1} - dt/2
+  double *pD;                    // [4][N] e, v of Qh at tau_{n+1}
+  double *pi0, *piH0;            // [10][N] IS relaxation results
+  double *Pi0, *PiH0;            // [N]
+  int *gsrc;                     // [nx+ny+nz] ghost-cell source map
+  unsigned char *gdst;           // [nx+ny+nz] ghost-cell destination flags
+  unsigned *err;                 // device error word
+};
+
+struct StepArgs {
+  Geo g;
+  EosDev eos;
+  TrDev tr;
+  Fields f;
+  double tau, dt;
+  bool viscous;
+};
+
+// Kernel kinds, for per-kernel timing.
+enum KernelKind {
+  KK_UPDATE_M = 0, KK_FACE_X, KK_FACE_Y, KK_FACE_Z, KK_UPDATE, KK_GHOST, KK_VISC_PRIMS,
+  KK_IS_RELAX, KK_IS_ADVECT, KK_VISC_UPDATE, KK_COUNT
+};
+extern const char* const kKernelNames[KK_COUNT];
+
+// Called after each launch with its kind (used to record timing events).
+struct LaunchMarker {
+  virtual void after(int kind) = 0;
+  virtual ~LaunchMarker() {}
+};
+
+// Enqueues one performStep on stream s; returns the number of launches.
+// Leaves the updated fill fractions in f.m2 (the caller swaps m and m2).
+int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk = nullptr);
+
+void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
+                         cudaStream_t s);
+
+}  // namespace vh
