@@ -159,6 +159,33 @@ int vh_abi_version(void);
 vh_status vh_transform_pv(vh_ctx *ctx, const double *Q_dev, long n,
                           double *prim_dev);
 
+/* Allocation-free step.  No counterpart in the reference: this entry point
+ * exists for callers that cannot let a library allocate -- host codes whose
+ * device memory is reserved up front by their own pool or by another
+ * framework's caching allocator, or that forbid cudaMalloc once their time
+ * loop runs.  It performs one Hydro::performStep on caller-owned DEVICE
+ * arrays: every field of `state` is required (sizes as in vh_state_view),
+ * and the EoS table pointers in `eos_dev` are device pointers.  `tau` is the
+ * time at the start of the step; the caller advances it by dt.
+ * All scratch lives in one static device array sized for at most
+ * VH_NOALLOC_MAX_CELLS cells and VH_NOALLOC_MAX_DIM cells per dimension
+ * (about 16 MB held on every GPU that loads the library until exit); larger
+ * grids are rejected with VH_ERR_ARG.  Nothing is allocated: no cudaMalloc,
+ * cudaFree, host malloc or library allocator is called.  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress), so make
+ * that first call before any stream capture on the device.  Every call on a
+ * device shares the array: calls whose GPU work overlaps race, so serialise
+ * them.  The call waits for `stream`, writes the device error word to
+ * *error_bits (if not NULL) and returns VH_ERR_NUMERIC when it is nonzero;
+ * vh_noalloc_last_error() describes the last failure on this thread. */
+#define VH_NOALLOC_MAX_CELLS 32768
+#define VH_NOALLOC_MAX_DIM 1024
+vh_status vh_step_noalloc(const vh_grid *grid, const vh_eos *eos_dev,
+                          const vh_trcoeff *tr, double tau, double dt,
+                          const vh_state_view *state, void *stream,
+                          unsigned *error_bits);
+const char *vh_noalloc_last_error(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -27,7 +27,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
            "vh_abi_version", "vh_transform_pv", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
-           "vh_free_pinned")
+           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error")
 
 
 class VhError(RuntimeError):
@@ -108,6 +108,10 @@ def lib():
     L.vh_profile_kinds.restype = ctypes.c_int
     L.vh_alloc_pinned.argtypes = [ctypes.c_size_t, ctypes.POINTER(vp)]
     L.vh_free_pinned.argtypes = [vp]
+    L.vh_step_noalloc.argtypes = [ctypes.POINTER(VhGrid), ctypes.POINTER(VhEos),
+                                  ctypes.POINTER(VhTrcoeff), ctypes.c_double, ctypes.c_double,
+                                  ctypes.POINTER(VhStateView), vp, ctypes.POINTER(ctypes.c_uint)]
+    L.vh_noalloc_last_error.restype = ctypes.c_char_p
     _lib = L
     return L
 
