@@ -169,7 +169,7 @@ vh_status vh_transform_pv(vh_ctx *ctx, const double *Q_dev, long n,
  * time at the start of the step; the caller advances it by dt.
  * All scratch lives in one static device array sized for at most
  * VH_NOALLOC_MAX_CELLS cells and VH_NOALLOC_MAX_DIM cells per dimension
- * (about 16 MB held on every GPU that loads the library until exit); larger
+ * (about 21 MB held on every GPU that loads the library until exit); larger
  * grids are rejected with VH_ERR_ARG.  Nothing is allocated: no cudaMalloc,
  * cudaFree, host malloc or library allocator is called.  The first call on a
  * device looks up the array's device address (cudaGetSymbolAddress), so make

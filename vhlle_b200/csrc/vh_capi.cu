@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -124,6 +125,45 @@ static void ghost_map(int n, int* src, unsigned char* dst) {
   }
 }
 
+// Chooses how the device searches a table axis: the index guess of a log
+// or linear fit when every grid point is predicted within two places (and
+// the axis is strictly increasing), else the reference's binary search.
+// Results are identical in every mode; only the number of loads differs.
+static void choose_axis_mode(const double* g, int n, int* mode, float* x0, float* inv) {
+  *mode = vh::GRID_BSEARCH;
+  *x0 = 0.f;
+  *inv = 0.f;
+  if (n < 3) return;
+  for (int k = 1; k < n; k++)
+    if (!(g[k] > g[k - 1])) return;
+  auto worst = [&](int m, float a0, float ainv) {
+    float w = 0.f;
+    for (int k = 0; k < n; k++) {
+      const float fx = (float)g[k];
+      const float t = (m == vh::GRID_LOG ? std::log2(fx) - a0 : fx - a0) * ainv;
+      w = std::max(w, std::fabs(t - (float)k));
+    }
+    return w;
+  };
+  if (g[0] > 0.) {
+    const float a0 = std::log2((float)g[0]);
+    const float ainv = (float)(n - 1) / (std::log2((float)g[n - 1]) - a0);
+    if (std::isfinite(ainv) && worst(vh::GRID_LOG, a0, ainv) <= 2.f) {
+      *mode = vh::GRID_LOG;
+      *x0 = a0;
+      *inv = ainv;
+      return;
+    }
+  }
+  const float a0 = (float)g[0];
+  const float ainv = (float)(n - 1) / ((float)g[n - 1] - a0);
+  if (std::isfinite(ainv) && worst(vh::GRID_LIN, a0, ainv) <= 2.f) {
+    *mode = vh::GRID_LIN;
+    *x0 = a0;
+    *inv = ainv;
+  }
+}
+
 extern "C" {
 
 int vh_abi_version(void) { return VH_ABI_VERSION; }
@@ -151,6 +191,10 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   if (!grid || !eos || !tr) return fail(nullptr, VH_ERR_ARG, "vh_create: NULL argument");
   if (grid->nx < 2 || grid->ny < 2 || grid->nz < 1)
     return fail(nullptr, VH_ERR_ARG, "vh_create: need nx >= 2, ny >= 2, nz >= 1");
+  // src/main.cpp:153-155 (checkGridBorders) requires min < max on every axis
+  if (!(grid->xmin < grid->xmax) || !(grid->ymin < grid->ymax) || !(grid->etamin < grid->etamax))
+    return fail(nullptr, VH_ERR_ARG, "vh_create: the grid needs min < max on every axis");
+  if (!(tau0 > 0.)) return fail(nullptr, VH_ERR_ARG, "vh_create: tau0 must be positive");
   if (eos->kind != VH_EOS_CONFORMAL && eos->kind != VH_EOS_TABLE)
     return fail(nullptr, VH_ERR_ARG, "vh_create: unsupported EoS kind (no device lowering)");
   if (eos->kind == VH_EOS_TABLE) {
@@ -221,6 +265,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     ALLOC(f.flux, 4 * N);
     ALLOC(f.pA, 8 * N);
     ALLOC(f.pD, 4 * N);
+    ALLOC(f.pTh, 9 * N);
+    ALLOC(f.pBC, 9 * N);
     ALLOC(f.pi0, 10 * N);
     ALLOC(f.piH0, 10 * N);
     ALLOC(f.Pi0, N);
@@ -249,6 +295,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     ALLOC(buf, (size_t)ne + nn + 3 * (size_t)ne * nn);
     c->eos.ne = ne;
     c->eos.nn = nn;
+    choose_axis_mode(eos->egrid, ne, &c->eos.emode, &c->eos.e0, &c->eos.einv);
+    choose_axis_mode(eos->ngrid, nn, &c->eos.nmode, &c->eos.n0, &c->eos.ninv);
     c->eos.egrid = buf;
     c->eos.ngrid = buf + ne;
     c->eos.p = buf + ne + nn;

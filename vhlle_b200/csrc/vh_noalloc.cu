@@ -12,7 +12,7 @@
 // or host allocation.
 //
 // Limits and sharing: the scratch array is sized for VH_NOALLOC_MAX_CELLS
-// cells (about 16 MB, held on every GPU that loads this library until the
+// cells (about 21 MB, held on every GPU that loads this library until the
 // process exits), and every call on a device uses the same array.  Calls
 // whose work overlaps on one GPU (concurrent streams or threads) race on it
 // and must be serialised by the caller.  The array keeps the previous call's
@@ -31,8 +31,8 @@ namespace {
 
 constexpr long long kMaxCells = VH_NOALLOC_MAX_CELLS;
 constexpr int kMaxDim = VH_NOALLOC_MAX_DIM;
-constexpr long long kDoublesPerCell = 62;  // m2 3, Fx/Fy/Fz 21, flux 4, pA 8, pD 4,
-                                           // pi0/piH0 20, Pi0/PiH0 2
+constexpr long long kDoublesPerCell = 80;  // m2 3, Fx/Fy/Fz 21, flux 4, pA 8, pD 4,
+                                           // pTh 9, pBC 9, pi0/piH0 20, Pi0/PiH0 2
 constexpr size_t kHeaderBytes = 256 + 3 * kMaxDim * sizeof(int) + 3 * kMaxDim;  // err, maps
 constexpr size_t kHeaderAligned = (kHeaderBytes + 255) / 256 * 256;
 constexpr size_t kScratchBytes = kHeaderAligned + (size_t)kDoublesPerCell * kMaxCells * sizeof(double);
@@ -115,6 +115,9 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
     return nfail(VH_ERR_ARG, "vh_step_noalloc: every field of the state view is required");
   if (grid->nx < 2 || grid->ny < 2 || grid->nz < 1)
     return nfail(VH_ERR_ARG, "vh_step_noalloc: need nx >= 2, ny >= 2, nz >= 1");
+  if (!(grid->xmin < grid->xmax) || !(grid->ymin < grid->ymax) || !(grid->etamin < grid->etamax))
+    return nfail(VH_ERR_ARG, "vh_step_noalloc: the grid needs min < max on every axis");
+  if (!(tau > 0.)) return nfail(VH_ERR_ARG, "vh_step_noalloc: tau must be positive");
   if (grid->nx > kMaxDim || grid->ny > kMaxDim || grid->nz > kMaxDim)
     return nfail(VH_ERR_ARG,
                  "vh_step_noalloc: a grid dimension exceeds VH_NOALLOC_MAX_DIM (1024)");
@@ -157,6 +160,8 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.eos.p = eos_dev->p;
   a.eos.T = eos_dev->T;
   a.eos.mub = eos_dev->mub;
+  a.eos.emode = a.eos.nmode = vh::GRID_BSEARCH;  // the table stays on the device
+  a.eos.e0 = a.eos.einv = a.eos.n0 = a.eos.ninv = 0.f;
   a.tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
                    tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
                    tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,
@@ -185,6 +190,10 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   d += 8 * N;
   f.pD = d;
   d += 4 * N;
+  f.pTh = d;
+  d += 9 * N;
+  f.pBC = d;
+  d += 9 * N;
   f.pi0 = d;
   d += 10 * N;
   f.piH0 = d;

@@ -21,6 +21,11 @@ enum : unsigned {
   ERR_NSQUANT_NAN = 8u,  // src/hdo.cpp:643-651
 };
 
+// How a table axis is searched: a binary search as the reference does, or
+// an index guess from the axis' log or linear spacing followed by a walk to
+// the same bracket (GRID_LOG / GRID_LIN need a strictly increasing axis).
+enum : int { GRID_BSEARCH = 0, GRID_LOG = 1, GRID_LIN = 2 };
+
 struct EosDev {
   int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table
   double conf_cnst;  // e = cnst T^4 for kind 0
@@ -30,6 +35,9 @@ struct EosDev {
   const double* __restrict__ p;  // [ie + ne*inb]
   const double* __restrict__ T;
   const double* __restrict__ mub;
+  int emode, nmode;    // GRID_* per axis
+  float e0, einv;      // guess: (f(x) - e0) * einv, f = log2 or identity
+  float n0, ninv;
 };
 
 struct TrDev {
@@ -57,6 +65,46 @@ __device__ __forceinline__ double minmod(double a, double b) {
   return (fabs(a) > fabs(b)) ? b : a;
 }
 
+// ---------------------------------------------- zero-safe FP64 division
+// On B200 an FP64 division (or square root) of zero leaves the operation's
+// fast path and costs about three times a regular one, and one such lane
+// holds up its whole warp.  This step divides zeros all the time (nb = 0 in
+// every EoS lookup of a baryon-free run, vanishing velocity components, zero
+// tensor entries and coefficients).  The helpers below return exactly the
+// IEEE-754 result, but never hand the hardware a zero operand: the operand
+// is swapped for 1.0 by a PTX select, which the compiler cannot see through
+// (a plain C select would be folded back into the original division), and
+// the result for a zero operand is formed from the signs.
+__device__ __forceinline__ double one_if(bool z, double y) {
+  double r;
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.s32 p, %2, 0;\n\tselp.f64 %0, 0d3FF0000000000000, %1, p;\n\t}"
+      : "=d"(r)
+      : "d"(y), "r"((int)z));
+  return r;
+}
+
+// y / b
+__device__ __forceinline__ double ddiv(double y, double b) {
+  const bool z = (y == 0.);
+  const double q = one_if(z, y) / b;
+  if (!z) return q;
+  return (b == 0. || b != b) ? q * y : (signbit(b) ? -y : y);
+}
+
+// y / b for a divisor known to be positive (finite or +inf)
+__device__ __forceinline__ double ddivp(double y, double b) {
+  const bool z = (y == 0.);
+  const double q = one_if(z, y) / b;
+  return z ? y : q;
+}
+
+// sqrt(x) (sqrt(+-0) = +-0)
+__device__ __forceinline__ double sqrtz(double x) {
+  const bool z = (x == 0.);
+  const double r = sqrt(one_if(z, x));
+  return z ? x : r;
+}
+
 // ------------------------------------------------------------------ EoS
 // EoS1f binary search over a sorted grid (getue / getun, src/eo1.cpp:63-98);
 // returns k1 of the bracketing pair and k2.
@@ -73,20 +121,45 @@ __device__ __forceinline__ void bsearch_grid(const double* __restrict__ g, int n
   }
 }
 
+// The bracket the binary search above returns, found from an index guess.
+// For a strictly increasing axis g[0..n-1] the search yields the unique k in
+// [0, n-2] with (k == 0 or g[k] <= x) and (k == n-2 or x < g[k+1]) (and
+// n-2 for NaN); the two walks below stop exactly there, from any start, so
+// the guess only decides how many steps they take (usually none or one).
+__device__ __forceinline__ void bracket_guess(const double* __restrict__ g, int n, double x,
+                                              int mode, float x0, float inv, int& k1, int& k2) {
+  if (mode == GRID_BSEARCH || n <= 2) {
+    bsearch_grid(g, n, x, k1, k2);
+    return;
+  }
+  int k;
+  if (x != x) {
+    k = n - 2;
+  } else {
+    const float fx = (float)x;
+    const float t = (mode == GRID_LOG ? __log2f(fx) - x0 : fx - x0) * inv;
+    k = !(t > 0.f) ? 0 : (t >= (float)(n - 2) ? n - 2 : (int)t);
+    while (k > 0 && x < __ldg(g + k)) k--;
+    while (k < n - 2 && !(x < __ldg(g + k + 1))) k++;
+  }
+  k1 = k;
+  k2 = k + 1;
+}
+
 // EoS1f::eos, src/eo1.cpp:100-123
 template <bool WANT_T>
 __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
                                       double& T, double& mub, double& p) {
   int k1, k2;
-  bsearch_grid(E.egrid, E.ne, e, k1, k2);
+  bracket_guess(E.egrid, E.ne, e, E.emode, E.e0, E.einv, k1, k2);
   int ixe = k1;
   if (ixe > E.ne - 2) ixe = E.ne - 2;
-  const double ue = (e - __ldg(E.egrid + k1)) / (__ldg(E.egrid + k2) - __ldg(E.egrid + k1));
-  bsearch_grid(E.ngrid, E.nn, nb, k1, k2);
+  const double ue = ddiv(e - __ldg(E.egrid + k1), __ldg(E.egrid + k2) - __ldg(E.egrid + k1));
+  bracket_guess(E.ngrid, E.nn, nb, E.nmode, E.n0, E.ninv, k1, k2);
   int ixn = k1;
   if (ixn > E.nn - 2) ixn = E.nn - 2;
   if (ixn < 0) ixn = 0;
-  const double un = (nb - __ldg(E.ngrid + k1)) / (__ldg(E.ngrid + k2) - __ldg(E.ngrid + k1));
+  const double un = ddiv(nb - __ldg(E.ngrid + k1), __ldg(E.ngrid + k2) - __ldg(E.ngrid + k1));
   const double we0 = 1. - ue, we1 = ue;
   const double wn0 = 1. - un, wn1 = un;
   const int b00 = ixe + E.ne * ixn, b01 = ixe + E.ne * (ixn + 1);
@@ -113,7 +186,7 @@ __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
 }
 
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
-  if (E.kind == 0) return e / 3.;
+  if (E.kind == 0) return ddivp(e, 3.);
   double T, mub, p;
   eos1f<false>(E, e, nb, T, mub, p);
   return p;
@@ -122,7 +195,7 @@ __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
                                          double& T, double& mub, double& p) {
   if (E.kind == 0) {
-    p = e / 3.;
+    p = ddivp(e, 3.);
     T = e > 0. ? sqrt(sqrt(e / E.conf_cnst)) : 0.;
     mub = 0.;
   } else {
@@ -136,7 +209,7 @@ __device__ __forceinline__ double eos_s(const EosDev& E, double e, double nb,
   double T, mub, p;
   const double muq = 0., mus = 0.;
   eos_eval(E, e, nb, T, mub, p);
-  if (T > 0.0) return (e + p - mub * nb - muq * nq - mus * ns) / T;
+  if (T > 0.0) return ddivp(e + p - mub * nb - muq * nq - mus * ns, T);
   return 0.;
 }
 
@@ -148,7 +221,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
   const double dpe = 1. / 3.;
   const double corrf = 0.9999;
   double v, vl = 0., vh = 1., dvold, dv, f, df;
-  double M = sqrt(Q[X_] * Q[X_] + Q[Y_] * Q[Y_] + Q[Z_] * Q[Z_]);
+  double M = sqrtz(Q[X_] * Q[X_] + Q[Y_] * Q[Y_] + Q[Z_] * Q[Z_]);
   if (Q[T_] <= 0.) {
     o.e = 0.; o.p = 0.;
     o.vx = o.vy = o.vz = 0.;
@@ -191,7 +264,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
       v = vl + dv;
     } else {
       dvold = dv;
-      dv = f / df;
+      dv = ddiv(f, df);
       v -= dv;
     }
     if (fabs(dv) < 0.00001) break;
@@ -209,9 +282,9 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     else
       vl = v;
   }
-  o.vx = v * Q[X_] / M;
-  o.vy = v * Q[Y_] / M;
-  o.vz = v * Q[Z_] / M;
+  o.vx = ddivp(v * Q[X_], M);
+  o.vy = ddivp(v * Q[Y_], M);
+  o.vz = ddivp(v * Q[Z_], M);
   o.e = Q[T_] - M * v;
   o.p = eos_p(E, o.e, nb);  // the last iterate's nb, as the reference
   const double sq = sqrt(1 - o.vx * o.vx - o.vy * o.vy - o.vz * o.vz);
@@ -286,8 +359,8 @@ __device__ __forceinline__ void tr_getTau(const TrDev& t, double e, double rho,
                                           double T, double muB, double s, double P,
                                           double& taupi, double& tauPi) {
   if (T > 1e-1 && !(fabs(e + P) < 1.0)) {
-    taupi = (5. / 5.068) * s * tr_etaS(t, e, rho, T, muB, s, P) / (e + P);
-    tauPi = (6. / 5.068) * tr_zetaS(t, e, T, s, P) * s / (e + P);
+    taupi = ddiv((5. / 5.068) * s * tr_etaS(t, e, rho, T, muB, s, P), e + P);
+    tauPi = ddiv((6. / 5.068) * tr_zetaS(t, e, T, s, P) * s, e + P);
   } else {
     taupi = tauPi = 0.;
   }
@@ -302,8 +375,8 @@ __device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, dou
                                           double dxdir, Prim l, Prim r, double mL,
                                           double mR, double flux[7], unsigned& err) {
   const double dta = predict ? dt / 2. : dt;
-  const double El = (l.e + l.p) / (1 - l.vx * l.vx - l.vy * l.vy - l.vz * l.vz);
-  const double Er = (r.e + r.p) / (1 - r.vx * r.vx - r.vy * r.vy - r.vz * r.vz);
+  const double El = ddiv(l.e + l.p, 1 - l.vx * l.vx - l.vy * l.vy - l.vz * l.vz);
+  const double Er = ddiv(r.e + r.p, 1 - r.vx * r.vx - r.vy * r.vy - r.vz * r.vz);
   const double tauFactor = predict ? tau + 0.25 * dt : tau + 0.5 * dt;
   if (l.e < 0.) { l.e = 0.; l.p = 0.; }
   if (r.e < 0.) { r.e = 0.; r.p = 0.; }
@@ -326,7 +399,7 @@ __device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, dou
   const double Ubr = gammar * r.nb, Uqr = gammar * r.nq, Usr = gammar * r.ns;
   double Ftl, Fxl, Fyl, Fzl, Fbl, Fql, Fsl, Ftr, Fxr, Fyr, Fzr, Fbr, Fqr, Fsr;
   double bl, br;
-  const double sEl = sqrt(El), sEr = sqrt(Er);
+  const double sEl = sqrtz(El), sEr = sqrtz(Er);
   const double vnl = dir == X_ ? l.vx : (dir == Y_ ? l.vy : l.vz);
   const double vnr = dir == X_ ? r.vx : (dir == Y_ ? r.vy : r.vz);
   if (dir != Z_) {
@@ -344,21 +417,21 @@ __device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, dou
     else { Fyl = Fyl + l.p; Fyr = Fyr + r.p; }
   } else {
     const double tau1 = tauFactor;
-    Ftl = U4l * vnl / tau1 + l.p * vnl / tau1;
-    Fxl = U1l * vnl / tau1;
-    Fyl = U2l * vnl / tau1;
-    Fzl = U3l * vnl / tau1 + l.p / tau1;
-    Fbl = Ubl * vnl / tau1; Fql = Uql * vnl / tau1; Fsl = Usl * vnl / tau1;
-    Ftr = U4r * vnr / tau1 + r.p * vnr / tau1;
-    Fxr = U1r * vnr / tau1;
-    Fyr = U2r * vnr / tau1;
-    Fzr = U3r * vnr / tau1 + r.p / tau1;
-    Fbr = Ubr * vnr / tau1; Fqr = Uqr * vnr / tau1; Fsr = Usr * vnr / tau1;
+    Ftl = ddivp(U4l * vnl, tau1) + ddivp(l.p * vnl, tau1);
+    Fxl = ddivp(U1l * vnl, tau1);
+    Fyl = ddivp(U2l * vnl, tau1);
+    Fzl = ddivp(U3l * vnl, tau1) + ddivp(l.p, tau1);
+    Fbl = ddivp(Ubl * vnl, tau1); Fql = ddivp(Uql * vnl, tau1); Fsl = ddivp(Usl * vnl, tau1);
+    Ftr = ddivp(U4r * vnr, tau1) + ddivp(r.p * vnr, tau1);
+    Fxr = ddivp(U1r * vnr, tau1);
+    Fyr = ddivp(U2r * vnr, tau1);
+    Fzr = ddivp(U3r * vnr, tau1) + ddivp(r.p, tau1);
+    Fbr = ddivp(Ubr * vnr, tau1); Fqr = ddivp(Uqr * vnr, tau1); Fsr = ddivp(Usr * vnr, tau1);
   }
   {
     const double ss = sEl + sEr, dv = vnl - vnr;
-    const double csb = sqrt(cs2 + 0.5 * sqrt(El * Er) / (ss * ss) * (dv * dv));
-    const double vb = (sEl * vnl + sEr * vnr) / (sEl + sEr);
+    const double csb = sqrt(cs2 + ddiv(0.5 * sqrtz(El * Er), ss * ss) * (dv * dv));
+    const double vb = ddiv(sEl * vnl + sEr * vnr, sEl + sEr);
     bl = smin(0., smin((vb - csb) / (1 - vb * csb), (vnl - cs) / (1 - vnl * cs)));
     br = smax(0., smax((vb + csb) / (1 + vb * csb), (vnr + cs) / (1 + vnr * cs)));
     if (dir == Z_) {
@@ -374,13 +447,13 @@ __device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, dou
   if (bl == 0. && br == 0.) return false;
   const double pre = tauFactor * dta / dxdir;
   const double den = -bl + br;
-  flux[T_] = pre * (-bl * br * (U4l - U4r) + br * Ftl - bl * Ftr) / den;
-  flux[X_] = pre * (-bl * br * (U1l - U1r) + br * Fxl - bl * Fxr) / den;
-  flux[Y_] = pre * (-bl * br * (U2l - U2r) + br * Fyl - bl * Fyr) / den;
-  flux[Z_] = pre * (-bl * br * (U3l - U3r) + br * Fzl - bl * Fzr) / den;
-  flux[NB_] = pre * (-bl * br * (Ubl - Ubr) + br * Fbl - bl * Fbr) / den;
-  flux[NQ_] = pre * (-bl * br * (Uql - Uqr) + br * Fql - bl * Fqr) / den;
-  flux[NS_] = pre * (-bl * br * (Usl - Usr) + br * Fsl - bl * Fsr) / den;
+  flux[T_] = ddiv(pre * (-bl * br * (U4l - U4r) + br * Ftl - bl * Ftr), den);
+  flux[X_] = ddiv(pre * (-bl * br * (U1l - U1r) + br * Fxl - bl * Fxr), den);
+  flux[Y_] = ddiv(pre * (-bl * br * (U2l - U2r) + br * Fyl - bl * Fyr), den);
+  flux[Z_] = ddiv(pre * (-bl * br * (U3l - U3r) + br * Fzl - bl * Fzr), den);
+  flux[NB_] = ddiv(pre * (-bl * br * (Ubl - Ubr) + br * Fbl - bl * Fbr), den);
+  flux[NQ_] = ddiv(pre * (-bl * br * (Uql - Uqr) + br * Fql - bl * Fqr), den);
+  flux[NS_] = ddiv(pre * (-bl * br * (Usl - Usr) + br * Fsl - bl * Fsr), den);
   if (flux[NB_] != flux[NB_]) { err |= ERR_FLUX_NAN; return false; }
   return true;
 }

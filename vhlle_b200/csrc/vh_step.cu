@@ -116,9 +116,9 @@ __global__ void __launch_bounds__(128) k_face(Geo g, EosDev E, const double* __r
   for (int k = 0; k < 7; k++) {
     const double a = QQ[k * N + Lm], b = QQ[k * N + L], c = QQ[k * N + R], d = QQ[k * N + Rp];
     const double dQl = minmod((c - b) / 2., (b - a) / 2.);
-    ql[k] = (b + dQl) / tau;
+    ql[k] = ddivp(b + dQl, tau);
     const double dQr = minmod((d - c) / 2., (c - b) / 2.);
-    qr[k] = (c - dQr) / tau;
+    qr[k] = ddivp(c - dQr, tau);
   }
   Prim pl, pr;
   transform_pv(E, ql, pl);
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(128) k_update(Geo g, EosDev E, double* __restr
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     qin[k] = field[k * N + i];
-    q[k] = qin[k] / tau1;
+    q[k] = ddivp(qin[k], tau1);
   }
   Prim pp;
   transform_pv(E, q, pp);
@@ -251,13 +251,29 @@ __global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char*
 }
 
 // ------------------------------------------------ viscous cell prims
-// The two cell-centred con2prims of the viscous stages:
-//  A = Qh / (tau - dt/2)  (getPrimVarHCenter in ISformal, NSquant, visc_flux,
-//                          visc_source_step),
-//  D = Qh / tau           (getPrimVarHCenter of the six NSquant neighbours).
-__global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, const double* __restrict__ Qh,
+// Per-cell inputs of the viscous stages, one thread per cell:
+//  A  = con2prim(Qh / (tau - dt/2))  (getPrimVarHCenter in ISformal, NSquant,
+//                                     visc_flux, visc_source_step),
+//  D  = con2prim(Qh / tau)           (the six NSquant neighbour velocities),
+//  thermodynamics at A: T, muB, p, s, eta/s, zeta/s, tau_pi, tau_Pi, 9/70/p
+//                                    (src/hdo.cpp:427-432, 727-749),
+//  B  = con2prim(Qprev / (tau - dt)), C = con2prim(Q / tau) as four-velocities
+//                                    (NSquant's time derivative,
+//                                     src/hdo.cpp:419-446), only where
+//                                     NSquant reaches them (matter, no vacuum
+//                                     neighbour).
+__device__ __forceinline__ double maxM_at(const Geo& g, const double* __restrict__ m, int ix,
+                                          int iy, int iz);
+
+__global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, TrDev tr,
+                                                    const double* __restrict__ Q,
+                                                    const double* __restrict__ Qprev,
+                                                    const double* __restrict__ Qh,
+                                                    const double* __restrict__ m,
                                                     double* __restrict__ pA,
-                                                    double* __restrict__ pD, double tau,
+                                                    double* __restrict__ pD,
+                                                    double* __restrict__ pTh,
+                                                    double* __restrict__ pBC, double tau,
                                                     double dt) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
@@ -267,7 +283,7 @@ __global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, const doubl
   for (int k = 0; k < 7; k++) qh[k] = Qh[k * N + i];
   const double tA = tau - dt / 2.;
 #pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = qh[k] / tA;
+  for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tA);
   Prim a;
   transform_pv(E, q, a);
   pA[0 * N + i] = a.e;
@@ -279,13 +295,60 @@ __global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, const doubl
   pA[6 * N + i] = a.vy;
   pA[7 * N + i] = a.vz;
 #pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = qh[k] / tau;
+  for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tau);
   Prim d;
   transform_pv(E, q, d);
   pD[0 * N + i] = d.e;
   pD[1 * N + i] = d.vx;
   pD[2 * N + i] = d.vy;
   pD[3 * N + i] = d.vz;
+  if (a.e <= 0.) return;
+  {
+    double T, mub, p;
+    eos_eval(E, a.e, a.nb, T, mub, p);
+    const double s = eos_s(E, a.e, a.nb, a.nq, a.ns);
+    double taupi, tauPi;
+    tr_getTau(tr, a.e, a.nb, T, mub, s, p, taupi, tauPi);
+    pTh[0 * N + i] = T;
+    pTh[1 * N + i] = mub;
+    pTh[2 * N + i] = p;
+    pTh[3 * N + i] = s;
+    pTh[4 * N + i] = tr_etaS(tr, a.e, a.nb, T, mub, s, p);
+    pTh[5 * N + i] = tr_zetaS(tr, a.e, T, s, p);
+    pTh[6 * N + i] = taupi;
+    pTh[7 * N + i] = tauPi;
+    pTh[8 * N + i] = 9. / 70. / eos_p(E, a.e, a.nb);
+  }
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  const bool vac = maxM_at(g, m, ix + 1, iy, iz) <= 0.9 || maxM_at(g, m, ix, iy + 1, iz) <= 0.9 ||
+                   maxM_at(g, m, ix - 1, iy, iz) <= 0.9 || maxM_at(g, m, ix, iy - 1, iz) <= 0.9 ||
+                   maxM_at(g, m, ix + 1, iy + 1, iz) <= 0.9 ||
+                   maxM_at(g, m, ix + 1, iy - 1, iz) <= 0.9 ||
+                   maxM_at(g, m, ix - 1, iy + 1, iz) <= 0.9 ||
+                   maxM_at(g, m, ix - 1, iy - 1, iz) <= 0.9;
+  if (vac) return;
+#pragma unroll 1
+  for (int w = 0; w < 2; w++) {
+    const double* src = w == 0 ? Qprev : Q;
+    const double tt = w == 0 ? tau - dt : tau;
+#pragma unroll
+    for (int k = 0; k < 7; k++) q[k] = ddivp(src[k * N + i], tt);
+    Prim P;
+    transform_pv(E, q, P);
+    const double ut = 1.0 / sqrt(1.0 - P.vx * P.vx - P.vy * P.vy - P.vz * P.vz);
+    const int o = w == 0 ? 0 : 5;
+    pBC[(o + 0) * N + i] = ut;
+    pBC[(o + 1) * N + i] = ut * P.vx;
+    pBC[(o + 2) * N + i] = ut * P.vy;
+    pBC[(o + 3) * N + i] = ut * P.vz;
+    if (w == 0) pBC[4 * N + i] = P.e;
+  }
+}
+
+__device__ __forceinline__ double maxM_at(const Geo& g, const double* __restrict__ m, int ix,
+                                          int iy, int iz) {
+  return maxM(m, g.N, cidx(g, ix, iy, iz));
 }
 
 __device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N, long long i) {
@@ -302,32 +365,29 @@ __device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N
 }
 
 // ------------------------------------------------ ISformal, loop #1
-// Hydro::ISformal loop 1 with Hydro::NSquant inlined (src/hdo.cpp:381-652,
+// Hydro::ISformal loop 1 with Hydro::NSquant (src/hdo.cpp:381-652,
 // 690-864): Navier-Stokes shear/bulk from the velocity gradients, then the
 // two-stage Israel-Stewart relaxation with Christoffel and cross terms.
 // Writes pi0/piH0/Pi0/PiH0 and the first flux contribution
-// (+(tau-dt) * delta Q_n).
-__global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
-                                                  const double* __restrict__ Q,
-                                                  const double* __restrict__ Qprev,
-                                                  const double* __restrict__ m,
-                                                  const double* __restrict__ pA,
-                                                  const double* __restrict__ pD,
-                                                  const double* __restrict__ pi,
-                                                  const double* __restrict__ Pi,
-                                                  double* __restrict__ pi0,
-                                                  double* __restrict__ piH0,
-                                                  double* __restrict__ Pi0,
-                                                  double* __restrict__ PiH0,
-                                                  double* __restrict__ flux, double tau,
-                                                  double dt, unsigned* err) {
+// (+(tau-dt) * delta Q_n).  One thread per cell, every index a compile-time
+// constant; the con2prims and the thermodynamics come precomputed from
+// k_visc_prims.  Four 128-thread blocks per SM (128 registers) hide the FP64
+// latency better than fewer, spill-free ones (measured: 3 and 2 blocks per SM
+// are 7 % and 35 % slower, 5 and 6 are 9 % and 3 % slower).
+constexpr int kRelaxMinBlocks = 4;
+
+__global__ void __launch_bounds__(128, kRelaxMinBlocks) k_is_relax(
+    Geo g, EosDev E, TrDev tr, const double* __restrict__ Q, const double* __restrict__ Qprev,
+    const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
+    const double* __restrict__ pTh, const double* __restrict__ pBC,
+    const double* __restrict__ pi, const double* __restrict__ Pi, double* __restrict__ pi0,
+    double* __restrict__ piH0, double* __restrict__ Pi0, double* __restrict__ PiH0,
+    double* __restrict__ flux, double tau, double dt, unsigned* err) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
-  int ix, iy, iz;
-  coords(g, i, ix, iy, iz);
   const long long N = g.N;
-  const Prim A = loadA(pA, N, i);
-  if (A.e <= 0.) {
+  const double e = pA[i];
+  if (e <= 0.) {
 #pragma unroll
     for (int k = 0; k < 10; k++) {
       piH0[k * N + i] = 0.0;
@@ -339,13 +399,15 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
     for (int k = 0; k < 4; k++) flux[k * N + i] = 0.;
     return;
   }
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
   const double gmumu[4] = {1., -1., -1., -1.};
   double cpi[10];
 #pragma unroll
   for (int k = 0; k < 10; k++) cpi[k] = pi[k * N + i];
   const double cPi = Pi[i];
 #define PI(a, b) cpi[index44(a, b)]
-  const double vx = A.vx, vy = A.vy, vz = A.vz;
+  const double vx = pA[5 * N + i], vy = pA[6 * N + i], vz = pA[7 * N + i];
   const double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
   double u[4];
   u[0] = gamma;
@@ -360,12 +422,9 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
 #pragma unroll
     for (int k = 0; k < 4; k++) flux[k * N + i] = 0. + f[k];
   }
-  // thermodynamics at the cell (shared by NSquant and ISformal)
-  double T, mub, p;
-  eos_eval(E, A.e, A.nb, T, mub, p);
-  const double s = eos_s(E, A.e, A.nb, A.nq, A.ns);
-  const double etaS = tr_etaS(tr, A.e, A.nb, T, mub, s, p);
-  const double zetaS = tr_zetaS(tr, A.e, T, s, p);
+  const double s = pTh[3 * N + i];
+  const double etaS = pTh[4 * N + i];
+  const double zetaS = pTh[5 * N + i];
 
   // ------------------------------------------------------ NSquant
   double piNS[10], PiNS, du;
@@ -389,32 +448,21 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
   } else {
     const double VMIN = 1e-2;
     const double UDIFF = 3.0;
-    double q[7];
-    Prim P0, P1;
-#pragma unroll
-    for (int k = 0; k < 7; k++) q[k] = Qprev[k * N + i] / (tau - dt);
-    transform_pv(E, q, P0);
-#pragma unroll
-    for (int k = 0; k < 7; k++) q[k] = Q[k * N + i] / tau;
-    transform_pv(E, q, P1);
-    const double e0 = P0.e, e1 = A.e;
-    double ut0 = 1.0 / sqrt(1.0 - P0.vx * P0.vx - P0.vy * P0.vy - P0.vz * P0.vz);
-    double ux0 = ut0 * P0.vx, uy0 = ut0 * P0.vy, uz0 = ut0 * P0.vz;
-    double ut1 = 1.0 / sqrt(1.0 - P1.vx * P1.vx - P1.vy * P1.vy - P1.vz * P1.vz);
-    double ux1 = ut1 * P1.vx, uy1 = ut1 * P1.vy, uz1 = ut1 * P1.vz;
-    double uuu[4];
-    uuu[0] = u[0];
-    uuu[1] = u[1];
-    uuu[2] = u[2];
-    uuu[3] = u[3];
-    dmu[0][0] = (ut1 * ut1 - ut0 * ut0) / 2. / uuu[0] / dt;
-    dmu[0][1] = (ux1 * ux1 - ux0 * ux0) / 2. / uuu[1] / dt;
-    dmu[0][2] = (uy1 * uy1 - uy0 * uy0) / 2. / uuu[2] / dt;
-    dmu[0][3] = (uz1 * uz1 - uz0 * uz0) / 2. / uuu[3] / dt;
-    if (fabs(0.5 * (ut1 + ut0) / ut1) > UDIFF) dmu[0][0] = (ut1 - ut0) / dt;
-    if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / ux1) > UDIFF) dmu[0][1] = (ux1 - ux0) / dt;
-    if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uy1) > UDIFF) dmu[0][2] = (uy1 - uy0) / dt;
-    if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uz1) > UDIFF) dmu[0][3] = (uz1 - uz0) / dt;
+    const double e0 = pBC[4 * N + i], e1 = e;
+    double ut0 = pBC[0 * N + i], ux0 = pBC[1 * N + i], uy0 = pBC[2 * N + i], uz0 = pBC[3 * N + i];
+    double ut1 = pBC[5 * N + i], ux1 = pBC[6 * N + i], uy1 = pBC[7 * N + i], uz1 = pBC[8 * N + i];
+    const double* uuu = u;
+    dmu[0][0] = ddivp(ddivp((ut1 * ut1 - ut0 * ut0) / 2., uuu[0]), dt);
+    dmu[0][1] = ddivp(ddiv((ux1 * ux1 - ux0 * ux0) / 2., uuu[1]), dt);
+    dmu[0][2] = ddivp(ddiv((uy1 * uy1 - uy0 * uy0) / 2., uuu[2]), dt);
+    dmu[0][3] = ddivp(ddiv((uz1 * uz1 - uz0 * uz0) / 2., uuu[3]), dt);
+    if (fabs(ddivp(0.5 * (ut1 + ut0), ut1)) > UDIFF) dmu[0][0] = ddivp(ut1 - ut0, dt);
+    if (fabs(uuu[1]) < VMIN || fabs(ddiv(0.5 * (ux1 + ux0), ux1)) > UDIFF)
+      dmu[0][1] = ddivp(ux1 - ux0, dt);
+    if (fabs(uuu[2]) < VMIN || fabs(ddiv(0.5 * (uy1 + uy0), uy1)) > UDIFF)
+      dmu[0][2] = ddivp(uy1 - uy0, dt);
+    if (fabs(uuu[3]) < VMIN || fabs(ddiv(0.5 * (uz1 + uz0), uz1)) > UDIFF)
+      dmu[0][3] = ddivp(uz1 - uz0, dt);
     if (e1 <= 0. || e0 <= 0.) dmu[0][0] = dmu[0][1] = dmu[0][2] = dmu[0][3] = 0.;
 #pragma unroll
     for (int d = 1; d <= 3; d++) {
@@ -443,40 +491,39 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
         uz1 = ut1 * vz1;
         if (d < 3) {
           const double h = d == 1 ? g.dx : g.dy;
-          dmu[d][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / h;
-          dmu[d][1] = 0.25 * (ux1 * ux1 - ux0 * ux0) / uuu[1] / h;
-          dmu[d][2] = 0.25 * (uy1 * uy1 - uy0 * uy0) / uuu[2] / h;
-          dmu[d][3] = 0.25 * (uz1 * uz1 - uz0 * uz0) / uuu[3] / h;
-          if (fabs(0.5 * (ut1 + ut0) / uuu[0]) > UDIFF) dmu[d][0] = 0.5 * (ut1 - ut0) / h;
-          if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / uuu[1]) > UDIFF)
-            dmu[d][1] = 0.5 * (ux1 - ux0) / h;
-          if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uuu[2]) > UDIFF)
-            dmu[d][2] = 0.5 * (uy1 - uy0) / h;
-          if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uuu[3]) > UDIFF)
-            dmu[d][3] = 0.5 * (uz1 - uz0) / h;
+          dmu[d][0] = ddivp(ddivp(0.25 * (ut1 * ut1 - ut0 * ut0), uuu[0]), h);
+          dmu[d][1] = ddivp(ddiv(0.25 * (ux1 * ux1 - ux0 * ux0), uuu[1]), h);
+          dmu[d][2] = ddivp(ddiv(0.25 * (uy1 * uy1 - uy0 * uy0), uuu[2]), h);
+          dmu[d][3] = ddivp(ddiv(0.25 * (uz1 * uz1 - uz0 * uz0), uuu[3]), h);
+          if (fabs(ddivp(0.5 * (ut1 + ut0), uuu[0])) > UDIFF) dmu[d][0] = ddivp(0.5 * (ut1 - ut0), h);
+          if (fabs(uuu[1]) < VMIN || fabs(ddiv(0.5 * (ux1 + ux0), uuu[1])) > UDIFF)
+            dmu[d][1] = ddivp(0.5 * (ux1 - ux0), h);
+          if (fabs(uuu[2]) < VMIN || fabs(ddiv(0.5 * (uy1 + uy0), uuu[2])) > UDIFF)
+            dmu[d][2] = ddivp(0.5 * (uy1 - uy0), h);
+          if (fabs(uuu[3]) < VMIN || fabs(ddiv(0.5 * (uz1 + uz0), uuu[3])) > UDIFF)
+            dmu[d][3] = ddivp(0.5 * (uz1 - uz0), h);
         } else {
           const double dz = g.dz, th = tau + 0.5 * dt;
-          dmu[3][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / dz / th;
-          dmu[3][1] = 0.25 * (ux1 * ux1 - ux0 * ux0) / uuu[1] / dz / th;
-          dmu[3][2] = 0.25 * (uy1 * uy1 - uy0 * uy0) / uuu[2] / dz / th;
-          dmu[3][3] = 0.25 * (uz1 * uz1 - uz0 * uz0) / uuu[3] / dz / th;
-          if (fabs(0.5 * (ut1 + ut0) / uuu[0]) > UDIFF) dmu[3][0] = 0.5 * (ut1 - ut0) / dz / th;
-          if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / uuu[1]) > UDIFF)
-            dmu[3][1] = 0.5 * (ux1 - ux0) / dz / th;
-          if (fabs(uuu[2]) < VMIN || fabs(0.5 * (uy1 + uy0) / uuu[2]) > UDIFF)
-            dmu[3][2] = 0.5 * (uy1 - uy0) / dz / th;
-          if (fabs(uuu[3]) < VMIN || fabs(0.5 * (uz1 + uz0) / uuu[3]) > UDIFF)
-            dmu[3][3] = 0.5 * (uz1 - uz0) / dz / th;
+          dmu[3][0] = ddivp(ddivp(ddivp(0.25 * (ut1 * ut1 - ut0 * ut0), uuu[0]), dz), th);
+          dmu[3][1] = ddivp(ddivp(ddiv(0.25 * (ux1 * ux1 - ux0 * ux0), uuu[1]), dz), th);
+          dmu[3][2] = ddivp(ddivp(ddiv(0.25 * (uy1 * uy1 - uy0 * uy0), uuu[2]), dz), th);
+          dmu[3][3] = ddivp(ddivp(ddiv(0.25 * (uz1 * uz1 - uz0 * uz0), uuu[3]), dz), th);
+          if (fabs(ddivp(0.5 * (ut1 + ut0), uuu[0])) > UDIFF)
+            dmu[3][0] = ddivp(ddivp(0.5 * (ut1 - ut0), dz), th);
+          if (fabs(uuu[1]) < VMIN || fabs(ddiv(0.5 * (ux1 + ux0), uuu[1])) > UDIFF)
+            dmu[3][1] = ddivp(ddivp(0.5 * (ux1 - ux0), dz), th);
+          if (fabs(uuu[2]) < VMIN || fabs(ddiv(0.5 * (uy1 + uy0), uuu[2])) > UDIFF)
+            dmu[3][2] = ddivp(ddivp(0.5 * (uy1 - uy0), dz), th);
+          if (fabs(uuu[3]) < VMIN || fabs(ddiv(0.5 * (uz1 + uz0), uuu[3])) > UDIFF)
+            dmu[3][3] = ddivp(ddivp(0.5 * (uz1 - uz0), dz), th);
         }
       } else {
         dmu[d][0] = dmu[d][1] = dmu[d][2] = dmu[d][3] = 0.;
       }
     }
-    dmu[3][0] += uuu[3] / (tau - 0.5 * dt);
-    dmu[3][3] += uuu[0] / (tau - 0.5 * dt);
+    dmu[3][0] += ddivp(uuu[3], tau - 0.5 * dt);
+    dmu[3][3] += ddivp(uuu[0], tau - 0.5 * dt);
     const double gdiag[4] = {1., -1., -1., -1.};
-    // sigma contraction with Z^{mu nu lambda rho} (src/hdo.cpp:613-637);
-    // the result is symmetric in (mu, nu), so only a <= b... b <= a is formed.
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -492,12 +539,12 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
             const double gab = (a == b) ? gdiag[a] : 0.;
             if (b == l) Z += 0.5 * (gak - uuu[a] * uuu[k]);
             if (a == l) Z += 0.5 * (gbk - uuu[b] * uuu[k]);
-            if (k == l) Z -= (gab - uuu[a] * uuu[b]) / 3.0;
-            acc += Z * dmu[k][l] * 2.0 * etaS * s / 5.068;
+            if (k == l) Z -= ddivp(gab - uuu[a] * uuu[b], 3.0);
+            acc += ddivp(Z * dmu[k][l] * 2.0 * etaS * s, 5.068);
           }
         piNS[index44(a, b)] = acc;
       }
-    PiNS = -zetaS * s * (dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3]) / 5.068;
+    PiNS = ddivp(-zetaS * s * (dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3]), 5.068);
     du = dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3];
     bool bad = false;
 #pragma unroll
@@ -511,16 +558,15 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
   double sig[10];
 #pragma unroll
   for (int k = 0; k < 10; k++) {
-    sig[k] = 0.5 * piNS[k] / eta * 5.068;
+    sig[k] = ddiv(0.5 * piNS[k], eta) * 5.068;
     if (eta <= 0.0) sig[k] = 0.0;
   }
 #define SIG(a, b) sig[index44(a, b)]
-  double taupi, tauPi;
-  tr_getTau(tr, A.e, A.nb, T, mub, s, p, taupi, tauPi);
+  const double taupi = pTh[6 * N + i], tauPi = pTh[7 * N + i];
   double deltapipi = 4. / 3., taupipi = 10. / 7., lambdapiPi = 6. / 5.;
-  double phi7 = 9. / 70. / eos_p(E, A.e, A.nb);
+  double phi7 = pTh[8 * N + i];
   if (isinf(phi7)) phi7 = 0.0;
-  phi7 = phi7 / taupi;
+  phi7 = ddiv(phi7, taupi);
   if (taupi < 0.5 * dt) deltapipi = taupipi = lambdapiPi = phi7 = 0.0;
   double delPiPi = 2. / 3.;
   double lamPipi = 8. / 5. * (1. / 3. - 1. / 3.);
@@ -535,39 +581,44 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
       Delta[k] = -u[a] * u[b];
       if (a == b) Delta[k] += gmumu[a];
       if (taupi > 0.5 * dt)
-        h0[k] = PI(a, b) - (PI(a, b) - PINS(a, b)) * dt / 2.0 / gamma / taupi;
+        h0[k] = PI(a, b) - ddivp(ddivp((PI(a, b) - PINS(a, b)) * dt / 2.0, gamma), taupi);
       else
         h0[k] = PINS(a, b);
     }
   double H0;
   if (tauPi > 0.5 * dt)
-    H0 = cPi - (cPi - PiNS) * dt / 2.0 / gamma / tauPi;
+    H0 = cPi - ddivp(ddivp((cPi - PiNS) * dt / 2.0, gamma), tauPi);
   else
     H0 = PiNS;
   double tau1 = tau - dt * 0.75;
-  h0[index44(0, 0)] += -2. * vz * PI(0, 3) / tau1 * dt / 2.;
-  h0[index44(3, 3)] += -(2. * vz / tau1 * PI(0, 3)) * dt / 2.;
-  h0[index44(3, 0)] += -(vz / tau1 * PI(0, 0) + vz / tau1 * PI(3, 3)) * dt / 2.;
-  h0[index44(1, 0)] += -vz / tau1 * PI(1, 3) * dt / 2.;
-  h0[index44(2, 0)] += -vz / tau1 * PI(2, 3) * dt / 2.;
-  h0[index44(3, 1)] += -(vz / tau1 * PI(0, 1)) * dt / 2.;
-  h0[index44(3, 2)] += -(vz / tau1 * PI(0, 2)) * dt / 2.;
+  h0[index44(0, 0)] += ddivp(-2. * vz * PI(0, 3), tau1) * dt / 2.;
+  h0[index44(3, 3)] += -(ddivp(2. * vz, tau1) * PI(0, 3)) * dt / 2.;
+  h0[index44(3, 0)] += -(ddivp(vz, tau1) * PI(0, 0) + ddivp(vz, tau1) * PI(3, 3)) * dt / 2.;
+  h0[index44(1, 0)] += ddivp(-vz, tau1) * PI(1, 3) * dt / 2.;
+  h0[index44(2, 0)] += ddivp(-vz, tau1) * PI(2, 3) * dt / 2.;
+  h0[index44(3, 1)] += -(ddivp(vz, tau1) * PI(0, 1)) * dt / 2.;
+  h0[index44(3, 2)] += -(ddivp(vz, tau1) * PI(0, 2)) * dt / 2.;
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b <= a; b++) {
       double acc = h0[index44(a, b)];
-      acc += (-deltapipi * PI(a, b) * du + lambdapiPi * cPi * SIG(a, b)) / gamma * 0.5 * dt;
+      acc += ddivp(-deltapipi * PI(a, b) * du + lambdapiPi * cPi * SIG(a, b), gamma) * 0.5 * dt;
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        acc += (phi7 * PI(a, k) * PI(b, k) * gmumu[k] -
-                taupipi * 0.5 * (PI(a, k) * SIG(b, k) * gmumu[k] + PI(b, k) * SIG(a, k) * gmumu[k])) /
-               gamma * 0.5 * dt;
+        acc += ddivp(phi7 * PI(a, k) * PI(b, k) * gmumu[k] -
+                         taupipi * 0.5 *
+                             (PI(a, k) * SIG(b, k) * gmumu[k] + PI(b, k) * SIG(a, k) * gmumu[k]),
+                     gamma) *
+               0.5 * dt;
 #pragma unroll
         for (int l = 0; l < 4; l++) {
-          acc += (-PI(a, k) * u[b] - PI(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k] / gamma * 0.5 * dt -
-                 1. / 3. * Delta[index44(a, b)] * PI(k, l) * (phi7 * PI(k, l) - taupipi * SIG(k, l)) *
-                     gmumu[k] * gmumu[l] / gamma * 0.5 * dt;
+          acc += ddivp((-PI(a, k) * u[b] - PI(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k], gamma) *
+                     0.5 * dt -
+                 ddivp(1. / 3. * Delta[index44(a, b)] * PI(k, l) *
+                           (phi7 * PI(k, l) - taupipi * SIG(k, l)) * gmumu[k] * gmumu[l],
+                       gamma) *
+                     0.5 * dt;
         }
       }
       h0[index44(a, b)] = acc;
@@ -576,8 +627,8 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
   for (int k = 0; k < 4; k++)
 #pragma unroll
     for (int l = 0; l < 4; l++)
-      H0 += lamPipi * PI(k, l) * SIG(k, l) * gmumu[k] * gmumu[l] / gamma * 0.5 * dt;
-  H0 += -delPiPi * cPi * du / gamma * 0.5 * dt;
+      H0 += ddivp(lamPipi * PI(k, l) * SIG(k, l) * gmumu[k] * gmumu[l], gamma) * 0.5 * dt;
+  H0 += ddivp(-delPiPi * cPi * du, gamma) * 0.5 * dt;
 #define H(a, b) h0[index44(a, b)]
   double f0[10];
 #pragma unroll
@@ -585,40 +636,43 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
 #pragma unroll
     for (int b = 0; b <= a; b++) {
       if (taupi > 0.5 * dt)
-        f0[index44(a, b)] = PI(a, b) - (H(a, b) - PINS(a, b)) * dt / gamma / taupi;
+        f0[index44(a, b)] = PI(a, b) - ddivp(ddivp((H(a, b) - PINS(a, b)) * dt, gamma), taupi);
       else
         f0[index44(a, b)] = PINS(a, b);
     }
   double F0;
   if (tauPi > 0.5 * dt)
-    F0 = cPi - (H0 - PiNS) * dt / gamma / tauPi;
+    F0 = cPi - ddivp(ddivp((H0 - PiNS) * dt, gamma), tauPi);
   else
     F0 = PiNS;
   tau1 = tau - dt * 0.5;
-  f0[index44(0, 0)] += -2. * vz / tau1 * H(0, 3) * dt;
-  f0[index44(3, 3)] += -(2. * vz / tau1 * H(0, 3)) * dt;
-  f0[index44(3, 0)] += -(vz / tau1 * H(0, 0) + vz / tau1 * H(3, 3)) * dt;
-  f0[index44(1, 0)] += -vz / tau1 * H(1, 3) * dt;
-  f0[index44(2, 0)] += -vz / tau1 * H(2, 3) * dt;
-  f0[index44(3, 1)] += -(vz / tau1 * H(0, 1)) * dt;
-  f0[index44(3, 2)] += -(vz / tau1 * H(0, 2)) * dt;
+  f0[index44(0, 0)] += ddivp(-2. * vz, tau1) * H(0, 3) * dt;
+  f0[index44(3, 3)] += -(ddivp(2. * vz, tau1) * H(0, 3)) * dt;
+  f0[index44(3, 0)] += -(ddivp(vz, tau1) * H(0, 0) + ddivp(vz, tau1) * H(3, 3)) * dt;
+  f0[index44(1, 0)] += ddivp(-vz, tau1) * H(1, 3) * dt;
+  f0[index44(2, 0)] += ddivp(-vz, tau1) * H(2, 3) * dt;
+  f0[index44(3, 1)] += -(ddivp(vz, tau1) * H(0, 1)) * dt;
+  f0[index44(3, 2)] += -(ddivp(vz, tau1) * H(0, 2)) * dt;
 #pragma unroll
   for (int a = 0; a < 4; a++)
 #pragma unroll
     for (int b = 0; b <= a; b++) {
       double acc = f0[index44(a, b)];
-      acc += (-deltapipi * H(a, b) * du + lambdapiPi * H0 * SIG(a, b)) / gamma * dt;
+      acc += ddivp(-deltapipi * H(a, b) * du + lambdapiPi * H0 * SIG(a, b), gamma) * dt;
 #pragma unroll
       for (int k = 0; k < 4; k++) {
-        acc += (phi7 * PI(a, k) * H(b, k) * gmumu[k] -
-                taupipi * 0.5 * (H(a, k) * SIG(b, k) * gmumu[k] + H(b, k) * SIG(a, k) * gmumu[k])) /
-               gamma * dt;
+        acc += ddivp(phi7 * PI(a, k) * H(b, k) * gmumu[k] -
+                         taupipi * 0.5 *
+                             (H(a, k) * SIG(b, k) * gmumu[k] + H(b, k) * SIG(a, k) * gmumu[k]),
+                     gamma) *
+               dt;
 #pragma unroll
         for (int l = 0; l < 4; l++) {
-          acc += ((-H(a, k) * u[b] - H(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k] -
-                  1. / 3. * Delta[index44(a, b)] * H(k, l) * (phi7 * H(k, l) - taupipi * SIG(k, l)) *
-                      gmumu[k] * gmumu[l]) /
-                 gamma * dt;
+          acc += ddivp((-H(a, k) * u[b] - H(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k] -
+                           1. / 3. * Delta[index44(a, b)] * H(k, l) *
+                               (phi7 * H(k, l) - taupipi * SIG(k, l)) * gmumu[k] * gmumu[l],
+                       gamma) *
+                 dt;
         }
       }
       f0[index44(a, b)] = acc;
@@ -627,8 +681,8 @@ __global__ void __launch_bounds__(128) k_is_relax(Geo g, EosDev E, TrDev tr,
   for (int k = 0; k < 4; k++)
 #pragma unroll
     for (int l = 0; l < 4; l++)
-      F0 += lamPipi * H(k, l) * SIG(k, l) * gmumu[k] * gmumu[l] / gamma * dt;
-  F0 += -delPiPi * H0 * du / gamma * dt;
+      F0 += ddivp(lamPipi * H(k, l) * SIG(k, l) * gmumu[k] * gmumu[l], gamma) * dt;
+  F0 += ddivp(-delPiPi * H0 * du, gamma) * dt;
 #pragma unroll
   for (int k = 0; k < 10; k++) {
     piH0[k * N + i] = h0[k];
@@ -670,12 +724,12 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
   const Prim A = loadA(pA, N, i);
   if (A.e <= 0.) return;
   const double e = A.e, p = A.p, vx = A.vx, vy = A.vy, vz = A.vz;
-  const double xm = -vx * dt / g.dx;
-  const double ym = -vy * dt / g.dy;
-  const double zm = -vz * dt / g.dz / (tau - 0.5 * dt);
-  const double xmH = -vx * dt / g.dx / 2.0;
-  const double ymH = -vy * dt / g.dy / 2.0;
-  const double zmH = -vz * dt / g.dz / (tau - 0.5 * dt) / 2.0;
+  const double xm = ddivp(-vx * dt, g.dx);
+  const double ym = ddivp(-vy * dt, g.dy);
+  const double zm = ddivp(ddivp(-vz * dt, g.dz), tau - 0.5 * dt);
+  const double xmH = ddivp(-vx * dt, g.dx) / 2.0;
+  const double ymH = ddivp(-vy * dt, g.dy) / 2.0;
+  const double zmH = ddivp(ddivp(-vz * dt, g.dz), tau - 0.5 * dt) / 2.0;
   const double wx[2] = {(1. - fabs(xm)), fabs(xm)};
   const double wy[2] = {(1. - fabs(ym)), fabs(ym)};
   const double wz[2] = {(1. - fabs(zm)), fabs(zm)};
@@ -703,18 +757,18 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
         P += w * Pi0[c1];
         PH += wH * PiH0[c1];
       }
-  const double maxT0 = smax((e + p) / (1. - vx * vx - vy * vy - vz * vz) - p,
-                            (e + p) * (vx * vx + vy * vy + vz * vz) / (1. - vx * vx - vy * vy - vz * vz) + p);
+  const double maxT0 = smax(ddivp(e + p, 1. - vx * vx - vy * vy - vz * vz) - p,
+                            ddivp((e + p) * (vx * vx + vy * vy + vz * vz), 1. - vx * vx - vy * vy - vz * vz) + p);
   double maxpi = 0.;
 #pragma unroll
   for (int k = 0; k < 10; k++)
     if (fabs(a[k]) > maxpi) maxpi = fabs(a[k]);
   bool rescaled = false;
-  if (maxT0 / maxpi < 1.0) {
+  if (ddiv(maxT0, maxpi) < 1.0) {
 #pragma unroll
     for (int k = 0; k < 10; k++) {
-      a[k] = 0.1 * a[k] * maxT0 / maxpi;
-      aH[k] = 0.1 * aH[k] * maxT0 / maxpi;
+      a[k] = ddiv(0.1 * a[k] * maxT0, maxpi);
+      aH[k] = ddiv(0.1 * aH[k] * maxT0, maxpi);
     }
     rescaled = true;
   }
@@ -723,7 +777,7 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
     if (PH != 0.) PH = 1 * PH / fabs(PH) * p;
     rescaled = true;
   }
-  vcc[i] = rescaled ? maxT0 / maxpi : 1.;
+  vcc[i] = rescaled ? ddiv(maxT0, maxpi) : 1.;
 #pragma unroll
   for (int k = 0; k < 10; k++) {
     pi[k * N + i] = a[k];
@@ -771,9 +825,9 @@ __device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const 
   vzl = 0.5 * (vzl + vzr);
   const double v = sqrt(vxl * vxl + vyl * vyl + vzl * vzl);
   if (v > 1.) {
-    vxl = 0.99 * vxl / v;
-    vyl = 0.99 * vyl / v;
-    vzl = 0.99 * vzl / v;
+    vxl = ddivp(0.99 * vxl, v);
+    vyl = ddivp(0.99 * vyl, v);
+    vzl = ddivp(0.99 * vzl, v);
   }
   const double gamma = 1. / sqrt(1. - v * v);
   const double uuu[4] = {gamma, gamma * vxl, gamma * vyl, gamma * vzl};
@@ -785,7 +839,7 @@ __device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const 
     double x = 0.5 * (piH[k * N + L] + piH[k * N + R]);
     if (a == dir) x += -0.5 * (PL + PR) * gmumu[a];
     x += 0.5 * (PL + PR) * uuu[a] * uuu[dir];
-    f[a] = x * (tau - 0.5 * dt) * dt / dxa;
+    f[a] = ddivp(x * (tau - 0.5 * dt) * dt, dxa);
   }
   return true;
 }
@@ -845,7 +899,7 @@ __global__ void __launch_bounds__(128) k_visc_update(Geo g, const double* __rest
 #pragma unroll
     for (int k = 4; k < 7; k++) Q[k * N + i] += 0.;
   } else if (fl[0] != 0.) {
-    const double fac = fabs(0.5 * q0 / fl[0]);
+    const double fac = fabs(ddiv(0.5 * q0, fl[0]));
 #pragma unroll
     for (int k = 0; k < 4; k++) Q[k * N + i] += fac * fl[k];
 #pragma unroll
@@ -927,10 +981,11 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   k_ghost<false><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
   done(KK_GHOST);
   if (a.viscous) {
-    k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, F.Qh, F.pA, F.pD, tau1, a.dt);
+    k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
+                                   F.pBC, tau1, a.dt);
     done(KK_VISC_PRIMS);
-    k_is_relax<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pi, F.Pi, F.pi0,
-                                 F.piH0, F.Pi0, F.PiH0, F.flux, tau1, a.dt, F.err);
+    k_is_relax<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh, F.pBC, F.pi,
+                                 F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0, F.flux, tau1, a.dt, F.err);
     done(KK_IS_RELAX);
     k_is_advect<<<nb, bs, 0, s>>>(g, F.pA, F.pi0, F.piH0, F.Pi0, F.PiH0, F.pi, F.piH, F.Pi, F.PiH,
                                   F.vcc, F.flux, tau1, a.dt);

@@ -24,6 +24,8 @@ struct Fields {
   double *flux;                  // [4][N] viscous flux accumulator
   double *pA;                    // [8][N] prims of Qh at tau_{n+1} - dt/2
   double *pD;                    // [4][N] e, v of Qh at tau_{n+1}
+  double *pTh;                   // [9][N] thermodynamics and transport at pA
+  double *pBC;                   // [9][N] four-velocities for NSquant's d/dtau
   double *pi0, *piH0;            // [10][N] IS relaxation results
   double *Pi0, *PiH0;            // [N]
   int *gsrc;                     // [nx+ny+nz] ghost-cell source map
