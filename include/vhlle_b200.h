@@ -132,6 +132,16 @@ vh_status vh_clear_errors(vh_ctx *ctx);
 /* Number of kernel launches one vh_step issues for this context. */
 vh_status vh_launches_per_step(vh_ctx *ctx, int *n);
 
+/* Interior totals that Fluid::outputSurface accumulates and prints after a
+ * step (src/fld.cpp:544-604, 846-857), for the current state and tau:
+ * out[VH_TOTALS_N] = E, Efull, Nb1, Nb2, S (each already multiplied by
+ * dx*dy*dz, as the reference does), Px, vt_num, vt_den, vxvy_num,
+ * vxvy_den, pi0x_num, pi0x_den, txxyy_num, txxyy_den, nCoreCells,
+ * nCoreCutCells.  e_crit is the freeze-out energy density of the core-cell
+ * count.  Waits for the result. */
+#define VH_TOTALS_N 16
+vh_status vh_totals(vh_ctx *ctx, double ecrit, double *out);
+
 /* Device timing with CUDA events recorded on the context's stream.
  * vh_timer_stop waits for the stop event and returns the elapsed time. */
 vh_status vh_timer_start(vh_ctx *ctx);

@@ -72,6 +72,8 @@ def oracle_lib():
         lib.or_eos_eval.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_eos_s.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_update_m.argtypes = [ctypes.POINTER(_Grid), _dp, ctypes.c_double, ctypes.c_double]
+        lib.or_totals.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_Trc),
+                                  ctypes.POINTER(_State), ctypes.c_double, ctypes.c_double, _dp]
         _lib_oracle = lib
     return _lib_oracle
 
@@ -101,11 +103,17 @@ def ref_lib():
         lib.ref_transform_pv.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
+        lib.ref_output_surface.restype = ctypes.c_int
+        lib.ref_output_surface.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
+                                           ctypes.c_int]
         _lib_ref = lib
     return _lib_ref
 
 
 FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")
+TOTALS = ("E", "Efull", "Nb1", "Nb2", "S", "Px", "vt_num", "vt_den", "vxvy_num", "vxvy_den",
+          "pi0x_num", "pi0x_den", "txxyy_num", "txxyy_den", "nCoreCells", "nCoreCutCells")
 FIELD_NCOMP = dict(Q=7, Qh=7, Qprev=7, pi=10, piH=10, Pi=1, PiH=1, m=3, vcc=1)
 
 
@@ -193,6 +201,13 @@ class OracleRun:
     def get_state(self):
         return {k: v.copy() for k, v in self.state.items()}
 
+    def totals(self):
+        out = np.zeros(len(TOTALS))
+        sv = self._sview()
+        self.lib.or_totals(ctypes.byref(self.grid), ctypes.byref(self.eos.s), ctypes.byref(self.trc),
+                           ctypes.byref(sv), self.tau.value, self.setup.ecrit, _ptr(out))
+        return dict(zip(TOTALS, out))
+
     def transform_pv(self, Q):
         Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
         out = np.zeros((len(Q), 8))
@@ -264,6 +279,17 @@ class RefRun:
         out = np.zeros((len(Q), 8))
         self.lib.ref_transform_pv(self.h, _ptr(Q), len(Q), _ptr(out))
         return out
+
+    def totals(self):
+        out = np.zeros(len(TOTALS))
+        self.lib.ref_totals(self.h, self.tau_now, _ptr(out))
+        return dict(zip(TOTALS, out))
+
+    def output_surface(self, outdir):
+        """Fluid::outputSurface: returns (nelements, printed totals line)."""
+        buf = ctypes.create_string_buffer(512)
+        n = self.lib.ref_output_surface(self.h, outdir.encode(), buf, 512)
+        return n, buf.value.decode()
 
     def eos_eval(self, e, nb):
         e = np.ascontiguousarray(e, dtype=np.float64)

@@ -18,6 +18,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
 #include <string>
 
 #include "eos.h"  // must precede eo1.h, which only forward-declares EoS
@@ -28,6 +31,11 @@
 #include "inc.h"
 #include "rmn.h"
 #include "trancoeff.h"
+
+// the freeze-out stream Fluid::outputSurface writes to (src/fld.cpp:43-46)
+namespace output {
+extern std::ofstream ffreeze;
+}
 
 namespace {
 
@@ -61,6 +69,8 @@ struct RefRun {
   Hydro *h = nullptr;
   int nx = 0, ny = 0, nz = 0;
   double dx = 0, dy = 0;
+  double tau0 = 0, ecrit = 0;
+  bool output_open = false;
 };
 
 }  // namespace
@@ -92,6 +102,8 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
   r->nz = nz;
   r->dx = r->f->getDx();
   r->dy = r->f->getDy();
+  r->tau0 = tau0;
+  r->ecrit = ecrit;
   return r;
 }
 
@@ -208,6 +220,115 @@ void ref_eos(void *p, const double *e, const double *nb, int n, double *out,
     out[3 * i + 2] = mub;
     if (s_out) s_out[i] = r->eos->s(e[i], nb[i], 0., 0.);
   }
+}
+
+// The interior totals of Fluid::outputSurface (src/fld.cpp:544-604, scaled
+// at :846-851), accumulated here with the reference's own Fluid/Cell/EoS
+// methods in its loop order, at full precision (outputSurface itself prints
+// them with 6 digits).  out[16]: E, Efull, Nb1, Nb2, S, Px, vt_num, vt_den,
+// vxvy_num, vxvy_den, pi0x_num, pi0x_den, txxyy_num, txxyy_den,
+// nCoreCells, nCoreCutCells.
+void ref_totals(void *p, double tau, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  Fluid *f = r->f;
+  const int nx = r->nx, ny = r->ny, nz = r->nz;
+  const double dx = f->getDx(), dy = f->getDy(), dz = f->getDz();
+  const bool visc = r->tr->isViscous();
+  double E = 0., Efull = 0., S = 0., Px = 0., vt_num = 0., vt_den = 0.,
+         vxvy_num = 0., vxvy_den = 0., pi0x_num = 0., pi0x_den = 0.,
+         txxyy_num = 0., txxyy_den = 0., Nb1 = 0., Nb2 = 0.;
+  int nCoreCells = 0, nCoreCutCells = 0;
+  for (int ix = 2; ix < nx - 2; ix++)
+    for (int iy = 2; iy < ny - 2; iy++)
+      for (int iz = 2; iz < nz - 2; iz++) {
+        Cell *c = f->getCell(ix, iy, iz);
+        double e, nb, nq, ns, vx, vy, vz, t, mub, muq, mus, p, Q[7];
+        f->getCMFvariables(c, tau, e, nb, nq, ns, vx, vy, vz);
+        c->getQ(Q);
+        r->eos->eos(e, nb, nq, ns, t, mub, muq, mus, p);
+        double s = r->eos->s(e, nb, nq, ns);
+        const double eta = f->getZ(iz);
+        const double cosh_int = (sinh(eta + 0.5 * dz) - sinh(eta - 0.5 * dz)) / dz;
+        const double sinh_int = (cosh(eta + 0.5 * dz) - cosh(eta - 0.5 * dz)) / dz;
+        E += tau * (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                 (cosh_int - tanh(vz) * sinh_int) -
+             tau * p * cosh_int;
+        Nb1 += Q[NB_];
+        Nb2 += tau * nb * (cosh_int - tanh(vz) * sinh_int) /
+               sqrt(1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+        Efull += tau * (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                     (cosh(eta) - tanh(vz) * sinh(eta)) -
+                 tau * p * cosh(eta);
+        if (visc) Efull += tau * c->getpi(0, 0) * cosh(eta) + tau * c->getpi(0, 3) * sinh(eta);
+        if (e > r->ecrit) {
+          nCoreCells++;
+          if (c->getViscCorrCutFlag() < 0.9) nCoreCutCells++;
+        }
+        const double gmumu[4] = {1., -1., -1., -1.};
+        double deltas = 0.;
+        if (visc)
+          for (int i = 0; i < 4; i++)
+            for (int j = 0; j < 4; j++)
+              deltas += pow(c->getpi(i, j), 2) * gmumu[i] * gmumu[j];
+        if (t > 0.02) {
+          s += 1.5 * deltas / ((e + p) * t);
+          S += tau * s * (cosh_int - tanh(vz) * sinh_int) /
+               sqrt(1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+        }
+        Px += tau * (e + p) * vx / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+        if (iz > nz / 2 - 3 and iz < nz / 2 + 3) {
+          vxvy_num += e * (fabs(vx) - fabs(vy));
+          vxvy_den += e;
+          vt_den += e / sqrt(1. - vx * vx - vy * vy);
+          vt_num += e / sqrt(1. - vx * vx - vy * vy) * sqrt(vx * vx + vy * vy);
+          txxyy_num += (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                       (vx * vx - vy * vy);
+          txxyy_den += (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                           (vx * vx + vy * vy) +
+                       2. * p;
+        }
+        pi0x_num += e / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) * fabs(c->getpi(0, 1));
+        pi0x_den += e / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+      }
+  E = E * dx * dy * dz;
+  Efull = Efull * dx * dy * dz;
+  S = S * dx * dy * dz;
+  Nb1 *= dx * dy * dz;
+  Nb2 *= dx * dy * dz;
+  const double v[16] = {E, Efull, Nb1, Nb2, S, Px, vt_num, vt_den, vxvy_num, vxvy_den,
+                        pi0x_num, pi0x_den, txxyy_num, txxyy_den, (double)nCoreCells,
+                        (double)nCoreCutCells};
+  for (int k = 0; k < 16; k++) out[k] = v[k];
+}
+
+// Fluid::outputSurface itself (src/fld.cpp:517-874).  The first call opens
+// `dir`/freezeout.dat.unfinished (Fluid::initOutput with hsOnly = true).
+// Returns the number of surface elements; the line outputSurface prints
+// (tau E Efull nbSurf S EtotSurf nelements nsusp cut-fraction, 6 digits) is
+// copied into `line`.
+int ref_output_surface(void *p, const char *dir, char *line, int linelen) {
+  RefRun *r = static_cast<RefRun *>(p);
+  std::streambuf *old = std::cout.rdbuf();
+  std::ostringstream cap;
+  std::cout.rdbuf(cap.rdbuf());
+  if (!r->output_open) {
+    r->f->initOutput(dir, r->tau0, true);
+    r->output_open = true;
+  }
+  const int n = r->f->outputSurface(r->h->getTau(), false);
+  output::ffreeze.flush();
+  std::cout.rdbuf(old);
+  const std::string all = cap.str();
+  // the totals line is the last non-empty line
+  std::string last;
+  std::istringstream in(all);
+  for (std::string l; std::getline(in, l);)
+    if (!l.empty()) last = l;
+  if (line && linelen > 0) {
+    strncpy(line, last.c_str(), linelen - 1);
+    line[linelen - 1] = 0;
+  }
+  return n;
 }
 
 // Fluid::updateM alone (test of the vacuum-front rule)

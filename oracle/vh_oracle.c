@@ -1368,3 +1368,106 @@ void or_update_m(const or_grid *g, double *m, double tau, double dt) {
   updateM(&cx, tau, dt);
   free(cx.dm);
 }
+
+/* ------------------------------------------------------------- totals */
+
+/* Fluid::getCMFvariables, src/fld.cpp:50-60: con2prim of Q/tau, then the
+ * fluid rapidity Y and the velocities in the fireball rest frame. */
+static void cmf_variables(const or_eos *E, const or_state *s, long N, long i,
+                          double eta, double tau, double *e, double *nb,
+                          double *nq, double *ns, double *vx, double *vy,
+                          double *Y) {
+  double q[7], p, vz;
+  for (int k = 0; k < 7; k++) q[k] = s->Q[(long)k * N + i] / tau;
+  transform_pv(E, q, e, &p, nb, nq, ns, vx, vy, &vz);
+  *Y = eta + 1. / 2. * log((1. + vz) / (1. - vz));
+  *vx = *vx * cosh(*Y - eta) / cosh(*Y);
+  *vy = *vy * cosh(*Y - eta) / cosh(*Y);
+}
+
+void or_totals(const or_grid *g, const or_eos *E, const or_trc *tr,
+               const or_state *s, double tau, double ecrit, double *out) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const long N = (long)nx * ny * nz;
+  const double dx = (g->xmax - g->xmin) / (nx - 1);
+  const double dy = (g->ymax - g->ymin) / (ny - 1);
+  const double dz = (g->zmax - g->zmin) / (nz - 1);
+  const int visc = tr_isViscous(tr);
+  double E_ = 0., Efull = 0., S = 0., Px = 0., vt_num = 0., vt_den = 0.,
+         vxvy_num = 0., vxvy_den = 0., pi0x_num = 0., pi0x_den = 0.,
+         txxyy_num = 0., txxyy_den = 0., Nb1 = 0., Nb2 = 0.;
+  int nCore = 0, nCoreCut = 0;
+  const double gmumu[4] = {1., -1., -1., -1.};
+  for (int ix = 2; ix < nx - 2; ix++)
+    for (int iy = 2; iy < ny - 2; iy++)
+      for (int iz = 2; iz < nz - 2; iz++) {
+        const long i = ix + (long)nx * iy + (long)nx * ny * iz;
+        const double etaz = g->zmin + iz * dz;
+        double e, nb, nq, ns, vx, vy, vz, t, mub, p;
+        cmf_variables(E, s, N, i, etaz, tau, &e, &nb, &nq, &ns, &vx, &vy, &vz);
+        eos_eval(E, e, nb, &t, &mub, &p);
+        double sd = eos_s(E, e, nb, nq, ns);
+        const double eta = etaz;
+        const double cosh_int = (sinh(eta + 0.5 * dz) - sinh(eta - 0.5 * dz)) / dz;
+        const double sinh_int = (cosh(eta + 0.5 * dz) - cosh(eta - 0.5 * dz)) / dz;
+        E_ += tau * (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                  (cosh_int - tanh(vz) * sinh_int) -
+              tau * p * cosh_int;
+        Nb1 += s->Q[(long)NB_ * N + i];
+        Nb2 += tau * nb * (cosh_int - tanh(vz) * sinh_int) /
+               sqrt(1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+        Efull += tau * (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                     (cosh(eta) - tanh(vz) * sinh(eta)) -
+                 tau * p * cosh(eta);
+        const double pi00 = s->pi[(long)index44(0, 0) * N + i];
+        const double pi03 = s->pi[(long)index44(0, 3) * N + i];
+        const double pi01 = s->pi[(long)index44(0, 1) * N + i];
+        if (visc) Efull += tau * pi00 * cosh(eta) + tau * pi03 * sinh(eta);
+        if (e > ecrit) {
+          nCore++;
+          if (s->vcc[i] < 0.9) nCoreCut++;
+        }
+        double deltas = 0.;
+        if (visc)
+          for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++) {
+              const double pab = s->pi[(long)index44(a, b) * N + i];
+              deltas += pab * pab * gmumu[a] * gmumu[b];
+            }
+        if (t > 0.02) {
+          sd += 1.5 * deltas / ((e + p) * t);
+          S += tau * sd * (cosh_int - tanh(vz) * sinh_int) /
+               sqrt(1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+        }
+        Px += tau * (e + p) * vx / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+        if (iz > nz / 2 - 3 && iz < nz / 2 + 3) {
+          vxvy_num += e * (fabs(vx) - fabs(vy));
+          vxvy_den += e;
+          vt_den += e / sqrt(1. - vx * vx - vy * vy);
+          vt_num += e / sqrt(1. - vx * vx - vy * vy) * sqrt(vx * vx + vy * vy);
+          txxyy_num += (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                       (vx * vx - vy * vy);
+          txxyy_den += (e + p) / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) *
+                           (vx * vx + vy * vy) +
+                       2. * p;
+        }
+        pi0x_num += e / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz)) * fabs(pi01);
+        pi0x_den += e / (1. - vx * vx - vy * vy - tanh(vz) * tanh(vz));
+      }
+  out[0] = E_ * dx * dy * dz;
+  out[1] = Efull * dx * dy * dz;
+  out[2] = Nb1 * (dx * dy * dz);
+  out[3] = Nb2 * (dx * dy * dz);
+  out[4] = S * dx * dy * dz;
+  out[5] = Px;
+  out[6] = vt_num;
+  out[7] = vt_den;
+  out[8] = vxvy_num;
+  out[9] = vxvy_den;
+  out[10] = pi0x_num;
+  out[11] = pi0x_den;
+  out[12] = txxyy_num;
+  out[13] = txxyy_den;
+  out[14] = nCore;
+  out[15] = nCoreCut;
+}

@@ -81,6 +81,14 @@ void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
 void or_eos_s(const or_eos *eos, const double *e, const double *nb, int n,
               double *out);
 
+/* The grid totals Fluid::outputSurface accumulates over the interior cells
+ * [2, n-2)^3 (src/fld.cpp:544-604, scaled at :846-851).  out[OR_TOT_N]:
+ * E, Efull, Nb1, Nb2, S, Px, vt_num, vt_den, vxvy_num, vxvy_den, pi0x_num,
+ * pi0x_den, txxyy_num, txxyy_den, nCoreCells, nCoreCutCells. */
+#define OR_TOT_N 16
+void or_totals(const or_grid *g, const or_eos *eos, const or_trc *tr,
+               const or_state *s, double tau, double ecrit, double *out);
+
 /* Fluid::updateM (src/fld.cpp:384-423) alone, for unit tests. */
 void or_update_m(const or_grid *g, double *m, double tau, double dt);
 

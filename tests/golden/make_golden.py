@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import os
 import sys
+import tempfile
 
 import numpy as np
 
@@ -39,6 +40,9 @@ def save_case(name, setup, nsteps):
     r = P.RefRun(setup)
     r.step(nsteps)
     st = r.get_state()
+    tot = r.totals()
+    with tempfile.TemporaryDirectory() as d:
+        nelem, line = r.output_surface(d)
     g = setup.grid
     eos = setup.eos
     arrays = dict(
@@ -47,6 +51,8 @@ def save_case(name, setup, nsteps):
         tr=np.array(setup.tr_vector()), tr_params=np.array([setup.etaSparam, setup.zetaSparam]),
         clock=np.array([setup.tau0, setup.dt, setup.ecrit]), nsteps=np.array(nsteps),
         Q0=setup.Q, m0=setup.m, tau_end=np.array(r.tau_now),
+        tot_ref=np.array([tot[k] for k in P.TOTALS]),
+        surface_line=np.array(line), surface_nelements=np.array(nelem),
     )
     if eos.kind == 1:
         arrays.update(eos_egrid=eos.egrid, eos_ngrid=eos.ngrid, eos_p=eos.p, eos_T=eos.T,
@@ -106,6 +112,13 @@ def load_case(path):
                     int(z["tr_params"][1]), tau0, dt, ecrit, z["Q0"], z["m0"])
     expect = {k[4:]: z[k] for k in z.files if k.startswith("out_")}
     return setup, int(z["nsteps"]), float(z["tau_end"]), expect
+
+
+def load_totals(path):
+    """The reference's interior totals after the fixture's steps, and the
+    line Fluid::outputSurface printed (6 significant digits)."""
+    z = np.load(path)
+    return dict(zip(P.TOTALS, z["tot_ref"])), str(z["surface_line"]), int(z["surface_nelements"])
 
 
 if __name__ == "__main__":

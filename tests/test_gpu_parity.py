@@ -178,3 +178,39 @@ def test_setdtau_rules_follow_the_reference():
     h.step(2)
     h.sync()
     assert abs(h.tau - (1.0 + 0.025)) < 1e-15
+
+
+TOTALS_RTOL = 1e-10  # energy and baryon number: 1e-10 relative (summation order, libm ulps)
+
+
+def _assert_totals_close(got, exp):
+    for k, v in exp.items():
+        g = got[k]
+        if np.isnan(v):
+            assert np.isnan(g), k
+        else:
+            assert g == pytest.approx(v, rel=TOTALS_RTOL, abs=1e-10 * max(1.0, abs(exp["E"]))), k
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
+def test_gpu_totals_match_reference_fixture(path):
+    from make_golden import load_totals
+    setup, nsteps, tau_end, expect = load_case(path)
+    tot_ref, line, nelem = load_totals(path)
+    h = capi.GpuHydro(setup)
+    h.step(nsteps)
+    h.sync()
+    _assert_totals_close(h.totals(), tot_ref)
+
+
+def test_gpu_totals_full_size_event():
+    s = W.glauber3d_setup()
+    h = capi.GpuHydro(s)
+    o = P.OracleRun(s)
+    h.step(2)
+    o.step(2)
+    h.sync()
+    _assert_totals_close(h.totals(), o.totals())
+    # repeated reductions are bit-identical (fixed reduction tree)
+    t1, t2 = h.totals(), h.totals()
+    assert all(t1[k] == t2[k] for k in t1)

@@ -54,3 +54,20 @@ def test_oracle_eos_known_answers(known, kind):
     pT, s = o.eos_eval(e, nb)
     assert np.array_equal(pT, known["keos_%s_out" % kind])
     assert np.array_equal(s, known["keos_%s_s" % kind])
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
+def test_oracle_totals_match_reference_fixture(path):
+    from make_golden import load_totals
+    setup, nsteps, tau_end, expect = load_case(path)
+    tot_ref, line, nelem = load_totals(path)
+    o = P.OracleRun(setup)
+    o.step(nsteps)
+    tot = o.totals()
+    for k in tot_ref:  # nz = 1 gives 0 * dz = NaN, in the reference too
+        assert tot[k] == tot_ref[k] or (np.isnan(tot[k]) and np.isnan(tot_ref[k])), k
+    # and the 6-digit line the reference printed: tau E Efull nbSurf S ...
+    printed = [float(x) for x in line.split()]
+    assert printed[0] == pytest.approx(tau_end, rel=1e-5)
+    for val, k in ((printed[1], "E"), (printed[2], "Efull"), (printed[4], "S")):
+        assert val == pytest.approx(tot[k], rel=1e-5, abs=1e-6, nan_ok=True), k

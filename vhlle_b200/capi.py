@@ -27,7 +27,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
            "vh_abi_version", "vh_transform_pv", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
-           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error")
+           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals")
 
 
 class VhError(RuntimeError):
@@ -58,6 +58,8 @@ class VhTrcoeff(ctypes.Structure):
 
 
 STATE_FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "viscCorrCut")
+TOTALS = ("E", "Efull", "Nb1", "Nb2", "S", "Px", "vt_num", "vt_den", "vxvy_num", "vxvy_den",
+          "pi0x_num", "pi0x_den", "txxyy_num", "txxyy_den", "nCoreCells", "nCoreCutCells")
 STATE_NCOMP = dict(Q=7, Qh=7, Qprev=7, pi=10, piH=10, Pi=1, PiH=1, m=3, viscCorrCut=1)
 
 
@@ -112,6 +114,7 @@ def lib():
                                   ctypes.POINTER(VhTrcoeff), ctypes.c_double, ctypes.c_double,
                                   ctypes.POINTER(VhStateView), vp, ctypes.POINTER(ctypes.c_uint)]
     L.vh_noalloc_last_error.restype = ctypes.c_char_p
+    L.vh_totals.argtypes = [vp, ctypes.c_double, _dp]
     _lib = L
     return L
 
@@ -258,6 +261,13 @@ class GpuHydro:
             if n.value:
                 out[name.value.decode()] = (n.value, ms.value)
         return out
+
+    def totals(self, ecrit=None) -> dict:
+        """Interior totals of Fluid::outputSurface for the current state."""
+        out = np.zeros(len(TOTALS))
+        ec = self.setup.ecrit if ecrit is None else ecrit
+        self._check(self.L.vh_totals(self.h, ec, _ptr(out)))
+        return dict(zip(TOTALS, out))
 
     def device_state(self) -> dict:
         v = VhStateView()

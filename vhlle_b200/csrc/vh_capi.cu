@@ -17,6 +17,7 @@
 
 #include "../../include/vhlle_b200.h"
 #include "vh_step.cuh"
+#include "vh_surface.cuh"
 
 namespace vh {
 void launch_fill(double* p, long long n, double v, cudaStream_t s);
@@ -34,6 +35,9 @@ struct vh_ctx {
   bool viscous = false;
   bool uploaded = false;
   int launches = 0;
+  vh_grid grid{};
+  double* tot_partial = nullptr;  // [blocks][16] block sums of the totals
+  double* tot_out = nullptr;      // [16]
   std::string err;
   std::vector<void*> allocs;
   // timers and per-kernel profiling
@@ -234,6 +238,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   g.dx = dx;
   g.dy = dy;
   g.dz = (grid->etamax - grid->etamin) / (grid->nz - 1);
+  c->grid = *grid;
   c->tau = tau0;
   c->dt = dt;
   c->tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
@@ -272,6 +277,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     ALLOC(f.Pi0, N);
     ALLOC(f.PiH0, N);
   }
+  ALLOC(c->tot_partial, (size_t)vh::totals_blocks(g) * vh::kTotals);
+  ALLOC(c->tot_out, vh::kTotals);
   const int ng = g.nx + g.ny + g.nz;
   ALLOC(f.gsrc, ng);
   ALLOC(f.gdst, ng);
@@ -496,6 +503,27 @@ vh_status vh_launches_per_step(vh_ctx* ctx, int* n) {
   if (!ctx || !n) return VH_ERR_ARG;
   int k = 1 + 2 * (2 + (ctx->g.nz > 1 ? 1 : 0) + 1) + 1 + (ctx->viscous ? 4 : 0) + 1;
   *n = k;
+  return VH_OK;
+}
+
+vh_status vh_totals(vh_ctx* ctx, double ecrit, double* out) {
+  if (!ctx || !out) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_totals: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::launch_totals(ctx->g, ctx->eos, ctx->f, ctx->tau, ecrit, ctx->grid.etamin, ctx->viscous,
+                    ctx->tot_partial, ctx->tot_out, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
+  double h[vh::kTotals];
+  VH_CUDA(ctx, cudaMemcpyAsync(h, ctx->tot_out, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  const double dx = ctx->g.dx, dy = ctx->g.dy, dz = ctx->g.dz;
+  // src/fld.cpp:846-851
+  h[0] = h[0] * dx * dy * dz;
+  h[1] = h[1] * dx * dy * dz;
+  h[2] *= dx * dy * dz;
+  h[3] *= dx * dy * dz;
+  h[4] = h[4] * dx * dy * dz;
+  for (int k = 0; k < vh::kTotals; k++) out[k] = h[k];
   return VH_OK;
 }
 

@@ -14,6 +14,28 @@ struct Geo {
   double dx, dy, dz;
 };
 
+// Fluid::getCell index with clamping (src/fld.h:70-78)
+__device__ __forceinline__ long long cidx(const Geo& g, int ix, int iy, int iz) {
+  ix = ix > 0 ? ix : 0;
+  ix = ix < g.nx ? ix : g.nx - 1;
+  iy = iy > 0 ? iy : 0;
+  iy = iy < g.ny ? iy : g.ny - 1;
+  iz = iz > 0 ? iz : 0;
+  iz = iz < g.nz ? iz : g.nz - 1;
+  return (long long)ix + (long long)g.nx * iy + (long long)g.nx * g.ny * iz;
+}
+
+__device__ __forceinline__ void coords(const Geo& g, long long i, int& ix, int& iy, int& iz) {
+  ix = (int)(i % g.nx);
+  const long long r = i / g.nx;
+  iy = (int)(r % g.ny);
+  iz = (int)(r / g.ny);
+}
+
+__device__ __forceinline__ double maxM(const double* __restrict__ m, long long N, long long i) {
+  return smax(m[i], smax(m[N + i], m[2 * N + i]));
+}
+
 // Device pointers of every field the step touches (component-major).
 struct Fields {
   double *Q, *Qh, *Qprev;        // [7][N]
