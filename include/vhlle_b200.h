@@ -123,6 +123,28 @@ vh_status vh_get_dtau(vh_ctx *ctx, double *dt);
 vh_status vh_get_tau(vh_ctx *ctx, double *tau);
 vh_status vh_set_tau(vh_ctx *ctx, double tau);
 
+/* The grid the context currently evolves: the creation grid, or the one
+ * vh_resize2x made, whose bounds are derived from the old grid's first and
+ * last cell coordinates exactly as expandGrid2x does. */
+vh_status vh_get_grid(vh_ctx *ctx, vh_grid *out);
+
+/* The substep block of the driver loop (src/main.cpp:405-419): while
+ * dtau / n > tau * (etamax - etamin) / (nz - 1) the count n doubles; with
+ * n > 1 the step is divided by n for n performStep calls and restored, else
+ * one performStep runs.  dtau, etamin, etamax and nz are the run
+ * parameters (not the resized grid).  *nsub (may be NULL) receives n. */
+vh_status vh_advance(vh_ctx *ctx, double dtau, double etamin, double etamax,
+                     int nz, int *nsub);
+
+/* expandGrid2x (src/main.cpp:246-271) on the device: same nx, ny, nz over
+ * twice the transverse range; every cell imports all variables of the old
+ * cell at 2*(i - n/2) + n/2 in x and y (clamped to the grid), and the time
+ * step doubles.  A grid whose x or y range is not symmetric is kept
+ * (*resized = 0, VH_OK) as the reference does; a doubled step above half
+ * the new cell size returns VH_ERR_ARG with nothing changed (the reference
+ * exits).  *resized may be NULL. */
+vh_status vh_resize2x(vh_ctx *ctx, int *resized);
+
 /* Waits for the context's work; returns VH_ERR_NUMERIC if a step set the
  * device error word (then vh_error_bits tells which check fired). */
 vh_status vh_sync(vh_ctx *ctx);

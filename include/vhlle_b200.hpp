@@ -1,0 +1,518 @@
+// vhlle_b200.hpp -- C++ host layer over the C ABI (vhlle_b200.h), keeping
+// the reference's class surface so that a vHLLE-style driver changes only
+// its includes: EoS1f (src/eo1.h), TransportCoeff (src/trancoeff.h), Fluid
+// (src/fld.h) with Cell-level accessors (src/cll.h), Hydro (src/hdo.h) and
+// the params-file reader (src/main.cpp:70-156).
+//
+// Differences a caller sees:
+//  * Hydro owns a device copy of the Fluid's cells.  performStep() runs on
+//    the GPU; the Fluid's host arrays are refreshed by Hydro::sync() (and
+//    uploaded again by setFluid or after the caller edits cells and calls
+//    upload()).
+//  * Conditions the reference stops on with exit() throw vhb::Error.
+//  * EoS objects must be lowerable to the device (conformal gas or an EoS1f
+//    table); their host p()/eos() follow the reference for initial states.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <functional>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "vhlle_b200.h"
+
+namespace vhb {
+
+enum { T_ = 0, X_ = 1, Y_ = 2, Z_ = 3, NB_ = 4, NQ_ = 5, NS_ = 6 };
+
+struct Error : std::runtime_error {
+  int status;
+  Error(int st, const std::string& m) : std::runtime_error(m), status(st) {}
+};
+
+inline void check(vh_status st, vh_ctx* ctx) {
+  if (st != VH_OK) throw Error(st, vh_last_error(ctx));
+}
+
+// index44, src/cll.cpp:22-31
+inline int index44(int i, int j) { return (j < i) ? (i * (i + 1)) / 2 + j : (j * (j + 1)) / 2 + i; }
+
+// ------------------------------------------------------------------- EoS
+// Abstract EoS (src/eos.h:21-38) restricted to what the device can evaluate.
+class EoS {
+ public:
+  virtual ~EoS() {}
+  virtual void eos(double e, double nb, double nq, double ns, double& T, double& mub,
+                   double& muq, double& mus, double& p) const = 0;
+  virtual double p(double e, double nb, double nq, double ns) const {
+    double T, mub, muq, mus, pp;
+    eos(e, nb, nq, ns, T, mub, muq, mus, pp);
+    return pp;
+  }
+  // EoS::s, src/eos.cpp:18-25
+  double s(double e, double nb, double nq, double ns) const {
+    double T, mub, muq, mus, p;
+    eos(e, nb, nq, ns, T, mub, muq, mus, p);
+    return T > 0.0 ? (e + p - mub * nb - muq * nq - mus * ns) / T : 0.;
+  }
+  virtual vh_eos descriptor() const = 0;
+};
+
+// Conformal gas p = e/3, e = cnst T^4.
+class EoSConformal : public EoS {
+  double cnst_;
+
+ public:
+  explicit EoSConformal(double cnst) : cnst_(cnst) {}
+  void eos(double e, double, double, double, double& T, double& mub, double& muq, double& mus,
+           double& p) const override {
+    p = e / 3.;
+    T = e > 0. ? std::sqrt(std::sqrt(e / cnst_)) : 0.;
+    mub = muq = mus = 0.;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_CONFORMAL;
+    d.conf_cnst = cnst_;
+    return d;
+  }
+};
+
+// EoS1f (src/eo1.cpp:21-123): (e, nb) table read from the same file format.
+class EoS1f : public EoS {
+  int ne_ = 0, nn_ = 0;
+  std::vector<double> eg_, ng_, p_, T_, mub_;
+
+  static void bracket(const std::vector<double>& g, double x, int& k1, double& u) {
+    int n = (int)g.size(), lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+      const int k = (lo + hi) / 2;
+      if (x < g[k])
+        hi = k;
+      else
+        lo = k;
+    }
+    k1 = lo;
+    if (k1 > n - 2) k1 = n - 2;
+    if (k1 < 0) k1 = 0;
+    u = (x - g[lo]) / (g[hi] - g[lo]);
+  }
+
+ public:
+  explicit EoS1f(const char* filename) {
+    std::ifstream fin(filename);
+    if (!fin) throw Error(VH_ERR_ARG, std::string("EoS1f: cannot open ") + filename);
+    double emax, e0, nmax, n0;
+    fin >> emax >> e0 >> nmax >> n0 >> ne_ >> nn_;
+    if (!fin || ne_ < 2 || nn_ < 2) throw Error(VH_ERR_ARG, "EoS1f: bad table header");
+    eg_.resize(ne_);
+    ng_.resize(nn_);
+    for (double& v : eg_) fin >> v;
+    for (double& v : ng_) fin >> v;
+    p_.resize((size_t)ne_ * nn_);
+    T_.resize(p_.size());
+    mub_.resize(p_.size());
+    for (int ie = 0; ie < ne_; ie++)
+      for (int inb = 0; inb < nn_; inb++) {
+        const size_t k = ie + (size_t)ne_ * inb;
+        fin >> p_[k] >> T_[k] >> mub_[k];
+        if (p_[k] < 1e-18) p_[k] = 0.;
+      }
+    if (!fin) throw Error(VH_ERR_ARG, "EoS1f: truncated table");
+  }
+  void eos(double e, double nb, double, double, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    int ie, inb;
+    double ue, un;
+    bracket(eg_, e, ie, ue);
+    bracket(ng_, nb, inb, un);
+    const double we[2] = {1. - ue, ue}, wn[2] = {1. - un, un};
+    T = mub = muq = mus = p = 0.;
+    for (int je = 0; je < 2; je++)
+      for (int jn = 0; jn < 2; jn++) {
+        const size_t k = (ie + je) + (size_t)ne_ * (inb + jn);
+        p += we[je] * wn[jn] * p_[k];
+        T += we[je] * wn[jn] * T_[k];
+        mub += we[je] * wn[jn] * mub_[k];
+      }
+    if (p < 0.) p = 0.;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_TABLE;
+    d.ne = ne_;
+    d.nn = nn_;
+    d.egrid = eg_.data();
+    d.ngrid = ng_.data();
+    d.p = p_.data();
+    d.T = T_.data();
+    d.mub = mub_.data();
+    return d;
+  }
+};
+
+// -------------------------------------------------------- TransportCoeff
+// src/trancoeff.h:6-45: the same public constants and constructor.
+class TransportCoeff {
+ public:
+  const double etaS0, zetaS0, ah, al, aRho, T0, etaSMin, etaSEpsilonMin, etaSShiftMuB,
+      etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta, zetaSSigmaMinus, zetaSSigmaPlus;
+  EoS* eos;
+  const int etaSparam, zetaSparam;
+  TransportCoeff(double _etaS0, double _zetaS0, double _ah, double _al, double _aRho, double _T0,
+                 double _etaSMin, double _etaSEpsilonMin, double _etaSShiftMuB,
+                 double _etaSScaleMuB, double _zetaSPeakEpsilon, double _zetaSScaleBeta,
+                 double _zetaSSigmaMinus, double _zetaSSigmaPlus, EoS* _eos, int _etaSparam,
+                 int _zetaSparam)
+      : etaS0(_etaS0), zetaS0(_zetaS0), ah(_ah), al(_al), aRho(_aRho), T0(_T0),
+        etaSMin(_etaSMin), etaSEpsilonMin(_etaSEpsilonMin), etaSShiftMuB(_etaSShiftMuB),
+        etaSScaleMuB(_etaSScaleMuB), zetaSPeakEpsilon(_zetaSPeakEpsilon),
+        zetaSScaleBeta(_zetaSScaleBeta), zetaSSigmaMinus(_zetaSSigmaMinus),
+        zetaSSigmaPlus(_zetaSSigmaPlus), eos(_eos), etaSparam(_etaSparam),
+        zetaSparam(_zetaSparam) {}
+  bool isViscous() const {
+    return etaS0 > 0. || zetaS0 > 0. || etaSparam > 0 || zetaSparam > 0;
+  }
+  vh_trcoeff descriptor() const {
+    return vh_trcoeff{etaS0,         zetaS0,         ah,           al,
+                      aRho,          T0,             etaSMin,      etaSEpsilonMin,
+                      etaSShiftMuB,  etaSScaleMuB,   zetaSPeakEpsilon, zetaSScaleBeta,
+                      zetaSSigmaMinus, zetaSSigmaPlus, etaSparam,   zetaSparam};
+  }
+};
+
+// ------------------------------------------------------------------ Fluid
+// src/fld.h: the grid and a host copy of every cell (structure of arrays).
+class Fluid {
+  EoS *eos_, *eosH_;
+  TransportCoeff* tr_;
+  int nx_, ny_, nz_;
+  double minx_, maxx_, miny_, maxy_, minz_, maxz_, dx_, dy_, dz_, dt_, ecrit_;
+  long long N_;
+
+ public:
+  std::vector<double> Q, Qh, Qprev, pi, piH, Pi, PiH, m, vcc;
+
+  Fluid(EoS* eos, EoS* eosH, TransportCoeff* tr, int nx, int ny, int nz, double minx,
+        double maxx, double miny, double maxy, double minz, double maxz, double dt, double eCrit)
+      : eos_(eos), eosH_(eosH), tr_(tr), nx_(nx), ny_(ny), nz_(nz), minx_(minx), maxx_(maxx),
+        miny_(miny), maxy_(maxy), minz_(minz), maxz_(maxz), dt_(dt), ecrit_(eCrit) {
+    dx_ = (maxx - minx) / (nx - 1);  // src/fld.cpp:77-79
+    dy_ = (maxy - miny) / (ny - 1);
+    dz_ = (maxz - minz) / (nz - 1);
+    N_ = (long long)nx * ny * nz;
+    Q.assign(7 * N_, 0.);
+    Qh.assign(7 * N_, 0.);
+    Qprev.assign(7 * N_, 0.);
+    pi.assign(10 * N_, 0.);
+    piH.assign(10 * N_, 0.);
+    Pi.assign(N_, 0.);
+    PiH.assign(N_, 0.);
+    m.assign(3 * N_, 0.);
+    vcc.assign(N_, 1.);
+  }
+  int getNX() const { return nx_; }
+  int getNY() const { return ny_; }
+  int getNZ() const { return nz_; }
+  double getDx() const { return dx_; }
+  double getDy() const { return dy_; }
+  double getDz() const { return dz_; }
+  double getX(int ix) const { return minx_ + ix * dx_; }
+  double getY(int iy) const { return miny_ + iy * dy_; }
+  double getZ(int iz) const { return minz_ + iz * dz_; }
+  double geteCrit() const { return ecrit_; }
+  EoS* getEoS() const { return eos_; }
+  long long ncells() const { return N_; }
+  vh_grid grid() const { return vh_grid{nx_, ny_, nz_, minx_, maxx_, miny_, maxy_, minz_, maxz_}; }
+  // Fluid::getCell clamping (src/fld.h:70-78)
+  long long index(int ix, int iy, int iz) const {
+    ix = std::min(std::max(ix, 0), nx_ - 1);
+    iy = std::min(std::max(iy, 0), ny_ - 1);
+    iz = std::min(std::max(iz, 0), nz_ - 1);
+    return ix + (long long)nx_ * iy + (long long)nx_ * ny_ * iz;
+  }
+  // Cell accessors (src/cll.h)
+  void getQ(int ix, int iy, int iz, double* q) const {
+    const long long i = index(ix, iy, iz);
+    for (int k = 0; k < 7; k++) q[k] = Q[k * N_ + i];
+  }
+  void setQ(int ix, int iy, int iz, const double* q) {  // Cell::setQ zeroing, src/cll.h:75-80
+    const long long i = index(ix, iy, iz);
+    const bool neg = q[T_] < 0.;
+    for (int k = 0; k < 7; k++) Q[k * N_ + i] = neg ? 0. : q[k];
+  }
+  void saveQprev(int ix, int iy, int iz) {
+    const long long i = index(ix, iy, iz);
+    for (int k = 0; k < 7; k++) Qprev[k * N_ + i] = Q[k * N_ + i];
+  }
+  void setAllM(int ix, int iy, int iz, double v) {
+    const long long i = index(ix, iy, iz);
+    for (int d = 0; d < 3; d++) m[d * N_ + i] = v;
+  }
+  double getM(int ix, int iy, int iz, int dir) const { return m[(dir - 1) * N_ + index(ix, iy, iz)]; }
+  double getpi(int ix, int iy, int iz, int a, int b) const {
+    return pi[index44(a, b) * N_ + index(ix, iy, iz)];
+  }
+  double getPi(int ix, int iy, int iz) const { return Pi[index(ix, iy, iz)]; }
+  double getViscCorrCutFlag(int ix, int iy, int iz) const { return vcc[index(ix, iy, iz)]; }
+  // Cell::setPrimVar, src/cll.cpp:222-241
+  void setPrimVar(int ix, int iy, int iz, double tau, double e, double nb, double nq, double ns,
+                  double vx, double vy, double vz) {
+    const double gamma2 = 1. / (1 - vx * vx - vy * vy - vz * vz);
+    const double p = eos_->p(e, nb, nq, ns);
+    double q[7];
+    q[T_] = tau * (e + p * (vx * vx + vy * vy + vz * vz)) * gamma2;
+    q[X_] = tau * (e + p) * vx * gamma2;
+    q[Y_] = tau * (e + p) * vy * gamma2;
+    q[Z_] = tau * (e + p) * vz * gamma2;
+    q[NB_] = tau * nb * std::sqrt(gamma2);
+    q[NQ_] = tau * nq * std::sqrt(gamma2);
+    q[NS_] = tau * ns * std::sqrt(gamma2);
+    const long long i = index(ix, iy, iz);
+    for (int k = 0; k < 7; k++) Q[k * N_ + i] = q[k];
+  }
+  vh_state_view view() {
+    return vh_state_view{Q.data(), Qh.data(), Qprev.data(), pi.data(), piH.data(),
+                         Pi.data(), PiH.data(), m.data(), vcc.data()};
+  }
+
+  // Grid snapshot (initial state or checkpoint): 8-byte tag "VHBSNAP1",
+  // int32 nx ny nz 0, float64 xmin xmax ymin ymax etamin etamax tau dt, then
+  // the planes Q Qh Qprev pi piH Pi PiH m viscCorrCut as raw float64.
+  struct SnapshotHeader {
+    vh_grid grid;
+    double tau, dt;
+  };
+  static SnapshotHeader readSnapshotHeader(const char* path) {
+    std::ifstream in(path, std::ios::binary);
+    char tag[8];
+    int32_t n[4];
+    double b[8];
+    in.read(tag, 8);
+    in.read(reinterpret_cast<char*>(n), sizeof n);
+    in.read(reinterpret_cast<char*>(b), sizeof b);
+    if (!in || std::memcmp(tag, "VHBSNAP1", 8) != 0)
+      throw Error(VH_ERR_ARG, std::string("not a grid snapshot: ") + path);
+    return SnapshotHeader{vh_grid{n[0], n[1], n[2], b[0], b[1], b[2], b[3], b[4], b[5]}, b[6],
+                          b[7]};
+  }
+  void loadSnapshot(const char* path) {
+    const SnapshotHeader h = readSnapshotHeader(path);
+    if (h.grid.nx != nx_ || h.grid.ny != ny_ || h.grid.nz != nz_)
+      throw Error(VH_ERR_ARG, "snapshot grid size differs from the fluid's");
+    std::ifstream in(path, std::ios::binary);
+    in.seekg(8 + 4 * 4 + 8 * 8);
+    for (std::vector<double>* v : planes())
+      in.read(reinterpret_cast<char*>(v->data()), (std::streamsize)(v->size() * sizeof(double)));
+    if (!in) throw Error(VH_ERR_ARG, std::string("truncated snapshot: ") + path);
+  }
+  void saveSnapshot(const char* path, double tau, double dt) {
+    std::ofstream out(path, std::ios::binary);
+    const int32_t n[4] = {nx_, ny_, nz_, 0};
+    const double b[8] = {minx_, maxx_, miny_, maxy_, minz_, maxz_, tau, dt};
+    out.write("VHBSNAP1", 8);
+    out.write(reinterpret_cast<const char*>(n), sizeof n);
+    out.write(reinterpret_cast<const char*>(b), sizeof b);
+    for (std::vector<double>* v : planes())
+      out.write(reinterpret_cast<const char*>(v->data()), (std::streamsize)(v->size() * sizeof(double)));
+    if (!out) throw Error(VH_ERR_ARG, std::string("cannot write snapshot: ") + path);
+  }
+
+ private:
+  std::vector<std::vector<double>*> planes() {
+    return {&Q, &Qh, &Qprev, &pi, &piH, &Pi, &PiH, &m, &vcc};
+  }
+};
+
+// Interior totals printed by Fluid::outputSurface (src/fld.cpp:544-604).
+struct Totals {
+  double E, Efull, Nb1, Nb2, S, Px, vt_num, vt_den, vxvy_num, vxvy_den, pi0x_num, pi0x_den,
+      txxyy_num, txxyy_den, nCoreCells, nCoreCutCells;
+};
+
+// ------------------------------------------------------------------ Hydro
+// src/hdo.h: one timestep of the whole grid per performStep(), on the GPU.
+class Hydro {
+  Fluid* f_;
+  EoS* eos_;
+  TransportCoeff* tr_;
+  vh_ctx* ctx_ = nullptr;
+  int device_;
+  double t0_, dt0_;
+  bool uploaded_ = false;
+
+  void create() {
+    const vh_grid g = f_->grid();
+    const vh_eos e = eos_->descriptor();
+    const vh_trcoeff t = tr_->descriptor();
+    check(vh_create(&g, &e, &t, t0_, dt0_, device_, &ctx_), nullptr);
+  }
+
+ public:
+  Hydro(Fluid* f, EoS* eos, TransportCoeff* tr, double t0, double dt, int device = 0)
+      : f_(f), eos_(eos), tr_(tr), device_(device), t0_(t0), dt0_(dt) {
+    create();
+  }
+  ~Hydro() { vh_destroy(ctx_); }
+  Hydro(const Hydro&) = delete;
+  Hydro& operator=(const Hydro&) = delete;
+
+  // Hydro::setDtau (src/hdo.cpp:67-75); the reference exits on dt > dx/2.
+  void setDtau(double dt) { check(vh_set_dtau(ctx_, dt), ctx_); }
+  double getDtau() const {
+    double d;
+    check(vh_get_dtau(ctx_, &d), ctx_);
+    return d;
+  }
+  double getTau() const {
+    double t;
+    check(vh_get_tau(ctx_, &t), ctx_);
+    return t;
+  }
+  Fluid* getFluid() const { return f_; }
+  // Hydro::setFluid: the new Fluid's cells replace the device grid.
+  void setFluid(Fluid* f) {
+    const double tau = getTau(), dt = getDtau();
+    vh_destroy(ctx_);
+    ctx_ = nullptr;
+    f_ = f;
+    t0_ = tau;
+    dt0_ = dt;
+    create();
+    uploaded_ = false;
+  }
+  // Copies the Fluid's host cells to the device (done by the first step).
+  void upload() {
+    vh_state_view v = f_->view();
+    check(vh_upload_state(ctx_, &v), ctx_);
+    uploaded_ = true;
+  }
+  // Hydro::performStep (src/hdo.cpp:1016-1134)
+  void performStep() {
+    if (!uploaded_) upload();
+    check(vh_step(ctx_), ctx_);
+  }
+  // Waits for the device and copies every cell back into the Fluid.
+  void sync() {
+    check(vh_sync(ctx_), ctx_);
+    vh_state_view v = f_->view();
+    check(vh_download_state(ctx_, &v), ctx_);
+  }
+  Totals totals() {
+    Totals t;
+    check(vh_totals(ctx_, f_->geteCrit(), &t.E), ctx_);
+    return t;
+  }
+  // The driver's substep block (src/main.cpp:405-419); returns the count.
+  int advance(double dtau, double etamin, double etamax, int nz) {
+    if (!uploaded_) upload();
+    int n = 1;
+    check(vh_advance(ctx_, dtau, etamin, etamax, nz, &n), ctx_);
+    return n;
+  }
+  vh_ctx* context() const { return ctx_; }
+
+  // expandGrid2x (src/main.cpp:246-271): the device grid doubles its
+  // transverse range and the step doubles.  Returns the new host Fluid (its
+  // cells are filled by the next sync()) and deletes the old one, or
+  // returns the old Fluid when the grid is not symmetric.
+  friend Fluid* expandGrid2x(Hydro* h, EoS* eos, EoS* eosH, TransportCoeff* tr);
+};
+
+inline Fluid* expandGrid2x(Hydro* h, EoS* eos, EoS* eosH, TransportCoeff* tr) {
+  Fluid* f = h->getFluid();
+  int resized = 0;
+  check(vh_resize2x(h->ctx_, &resized), h->ctx_);
+  if (!resized) {
+    std::cout << "this grid expansion works only with symmetric min/max ranges\n";
+    return f;
+  }
+  vh_grid g;
+  check(vh_get_grid(h->ctx_, &g), h->ctx_);
+  Fluid* fnew = new Fluid(eos, eosH, tr, g.nx, g.ny, g.nz, g.xmin, g.xmax, g.ymin, g.ymax,
+                          g.etamin, g.etamax, h->getDtau(), f->geteCrit());
+  h->f_ = fnew;
+  delete f;
+  return fnew;
+}
+
+// ------------------------------------------------------------- parameters
+// The reference driver's parameters with their defaults (src/main.cpp:70-81)
+// and its params-file reader (src/main.cpp:83-156): "name value" lines;
+// lines starting with '!' are comments echoed as "CCC", unknown names are
+// echoed as "UUU"; the grid must have min < max on every axis.
+struct Params {
+  int nx = 100, ny = 100, nz = 100, eosType = 1, etaSparam = 0, zetaSparam = 0,
+      eosTypeHadron = 0;
+  bool freezeoutOnly = false, freezeoutExtend = false, vorticityOn = false;
+  double xmin = -5.0, xmax = 5.0, ymin = -5.0, ymax = 5.0, etamin = -5.0, etamax = 5.0,
+         tau0 = 1.0, tauMax = 20.0, tauResize = 4.0, dtau = 0.05, etaS = 0.08, zetaS = 0.0,
+         eCrit = 0.5, etaSEpsilonMin = 5., al = 0., ah = 0., aRho = 0., T0 = 0.15,
+         etaSMin = 0.08, etaSShiftMuB = 0., etaSScaleMuB = 0., zetaSPeakEpsilon = 5.,
+         zetaSScaleBeta = 0.103, zetaSSigmaMinus = 0.1, zetaSSigmaPlus = 0.1, epsilon0 = 0.,
+         Rgt = 1.0, Rgz = 1.0, impactPar = 0., s0ScaleFactor = 0.;
+  std::string collSystem, outputDir = "data", isInputFile, vtk_values;
+  int icModel = 1, glauberVariable = 1, smoothingType = 0;
+  // extension of this build: an EoS1f table for the hydro EoS (the
+  // reference selects compiled-in EoS classes with eosType instead)
+  std::string eos1fFile;
+
+  void read(const char* parFile, std::ostream& log) {
+    std::ifstream fin(parFile);
+    if (!fin.is_open()) throw Error(VH_ERR_ARG, std::string("cannot open parameters file ") + parFile);
+    auto I = [](int& v) { return [&v](const std::string& s) { v = atoi(s.c_str()); }; };
+    auto D = [](double& v) { return [&v](const std::string& s) { v = atof(s.c_str()); }; };
+    auto B = [](bool& v) { return [&v](const std::string& s) { v = atoi(s.c_str()); }; };
+    auto S = [](std::string& v) { return [&v](const std::string& s) { v = s; }; };
+    std::map<std::string, std::function<void(const std::string&)>> h = {
+        {"eosType", I(eosType)}, {"eosTypeHadron", I(eosTypeHadron)}, {"nx", I(nx)},
+        {"ny", I(ny)}, {"nz", I(nz)}, {"icModel", I(icModel)},
+        {"glauberVar", I(glauberVariable)}, {"xmin", D(xmin)}, {"xmax", D(xmax)},
+        {"ymin", D(ymin)}, {"ymax", D(ymax)}, {"etamin", D(etamin)}, {"etamax", D(etamax)},
+        {"tau0", D(tau0)}, {"tauMax", D(tauMax)}, {"tauGridResize", D(tauResize)},
+        {"dtau", D(dtau)}, {"e_crit", D(eCrit)}, {"etaS", D(etaS)}, {"zetaS", D(zetaS)},
+        {"zetaSparam", I(zetaSparam)}, {"zetaSScaleBeta", D(zetaSScaleBeta)},
+        {"zetaSPeakEpsilon", D(zetaSPeakEpsilon)}, {"zetaSSigmaMinus", D(zetaSSigmaMinus)},
+        {"zetaSSigmaPlus", D(zetaSSigmaPlus)}, {"epsilon0", D(epsilon0)}, {"Rg", D(Rgt)},
+        {"Rgz", D(Rgz)}, {"impactPar", D(impactPar)}, {"s0ScaleFactor", D(s0ScaleFactor)},
+        {"VTK_output_values", S(vtk_values)}, {"etaSparam", I(etaSparam)}, {"aRho", D(aRho)},
+        {"ah", D(ah)}, {"al", D(al)}, {"T0", D(T0)}, {"etaSEpsilonMin", D(etaSEpsilonMin)},
+        {"etaSMin", D(etaSMin)}, {"etaSShiftMuB", D(etaSShiftMuB)},
+        {"etaSScaleMuB", D(etaSScaleMuB)}, {"freezeoutOnly", B(freezeoutOnly)},
+        {"freezeoutExtend", B(freezeoutExtend)}, {"vorticity", B(vorticityOn)},
+        {"smoothingType", I(smoothingType)}, {"eos1fFile", S(eos1fFile)},
+    };
+    // as in the reference, a line's name and value go through fixed
+    // buffers that keep their previous contents when a line has fewer words
+    std::string name, value;
+    while (fin.good()) {
+      std::string line;
+      std::getline(fin, line);
+      std::istringstream sline(line);
+      std::string a, b;
+      if (sline >> a) name = a;
+      if (sline >> b) value = b;
+      auto it = h.find(name);
+      if (it != h.end())
+        it->second(value);
+      else if (!name.empty() && name[0] == '!')
+        log << "CCC " << line << "\n";
+      else
+        log << "UUU " << line << "\n";
+    }
+    if (!(xmin < xmax)) throw Error(VH_ERR_ARG, "The hydrodynamic grid is not set up correctly: xmin >= xmax");
+    if (!(ymin < ymax)) throw Error(VH_ERR_ARG, "The hydrodynamic grid is not set up correctly: ymin >= ymax");
+    if (!(etamin < etamax)) throw Error(VH_ERR_ARG, "The hydrodynamic grid is not set up correctly: etamin >= etamax");
+  }
+};
+
+}  // namespace vhb

@@ -72,6 +72,12 @@ def oracle_lib():
         lib.or_eos_eval.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_eos_s.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_update_m.argtypes = [ctypes.POINTER(_Grid), _dp, ctypes.c_double, ctypes.c_double]
+        lib.or_resize2x.restype = ctypes.c_int
+        lib.or_resize2x.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_State),
+                                    ctypes.POINTER(_Grid), ctypes.POINTER(_State)]
+        lib.or_substeps.restype = ctypes.c_int
+        lib.or_substeps.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int]
         lib.or_totals.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_Trc),
                                   ctypes.POINTER(_State), ctypes.c_double, ctypes.c_double, _dp]
         _lib_oracle = lib
@@ -104,6 +110,14 @@ def ref_lib():
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
+        lib.ref_resize2x.restype = ctypes.c_int
+        lib.ref_resize2x.argtypes = [ctypes.c_void_p]
+        lib.ref_advance.restype = ctypes.c_int
+        lib.ref_advance.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int]
+        lib.ref_dtau.restype = ctypes.c_double
+        lib.ref_dtau.argtypes = [ctypes.c_void_p]
+        lib.ref_grid.argtypes = [ctypes.c_void_p, _dp]
         lib.ref_output_surface.restype = ctypes.c_int
         lib.ref_output_surface.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
                                            ctypes.c_int]
@@ -198,6 +212,62 @@ class OracleRun:
     def tau_now(self):
         return self.tau.value
 
+    def set_dtau(self, dt):
+        """Hydro::setDtau (src/hdo.cpp:67-75); returns False instead of exiting."""
+        g = self.grid
+        dx = (g.xmax - g.xmin) / (g.nx - 1)
+        dy = (g.ymax - g.ymin) / (g.ny - 1)
+        if dt > dx / 2. or dt > dy / 2.:
+            return False
+        self.dt = dt
+        return True
+
+    def advance(self, dtau, etamin, etamax, nz):
+        """The driver's substep block (src/main.cpp:405-419); returns the count."""
+        n = self.lib.or_substeps(dtau, self.tau.value, etamin, etamax, nz)
+        if n < 0:
+            raise RuntimeError("substep count overflow")
+        if n > 1:
+            self.dt = self.dt / n
+            self.step(n)
+            self.dt = self.dt * n
+        else:
+            self.step(1)
+        return n
+
+    def resize2x(self):
+        """expandGrid2x (src/main.cpp:246-271): 1 resized, 0 not symmetric,
+        -1 the doubled step fails the dx/2 check."""
+        out = {k: np.empty_like(v) for k, v in self.state.items()}
+        so = _State()
+        for k in FIELDS:
+            setattr(so, k, _ptr(out[k]))
+        gout = _Grid()
+        si = self._sview()
+        if not self.lib.or_resize2x(ctypes.byref(self.grid), ctypes.byref(si), ctypes.byref(gout),
+                                    ctypes.byref(so)):
+            return 0
+        dt2 = 2.0 * self.dt
+        dx = (gout.xmax - gout.xmin) / (gout.nx - 1)
+        dy = (gout.ymax - gout.ymin) / (gout.ny - 1)
+        if dt2 > dx / 2. or dt2 > dy / 2.:
+            return -1
+        self.grid = gout
+        self.state = out
+        self.dt = dt2
+        return 1
+
+    def grid_coords(self):
+        """getX(0), getX(nx-1), getY(0), getY(ny-1), getZ(0), getZ(nz-1), dx, dy, dz."""
+        g = self.grid
+        with np.errstate(all="ignore"):
+            a = np.array([g.xmin, g.xmax, g.ymin, g.ymax, g.zmin, g.zmax], dtype=np.float64)
+            n = np.array([g.nx - 1, g.ny - 1, g.nz - 1], dtype=np.float64)
+            d = (a[1::2] - a[0::2]) / n
+            out = np.array([a[0] + 0 * d[0], a[0] + n[0] * d[0], a[2] + 0 * d[1], a[2] + n[1] * d[1],
+                            a[4] + 0 * d[2], a[4] + n[2] * d[2], d[0], d[1], d[2]])
+        return out
+
     def get_state(self):
         return {k: v.copy() for k, v in self.state.items()}
 
@@ -267,6 +337,21 @@ class RefRun:
     @property
     def tau_now(self):
         return self.lib.ref_tau(self.h)
+
+    @property
+    def dtau(self):
+        return self.lib.ref_dtau(self.h)
+
+    def advance(self, dtau, etamin, etamax, nz):
+        return self.lib.ref_advance(self.h, dtau, etamin, etamax, nz)
+
+    def resize2x(self):
+        return self.lib.ref_resize2x(self.h)
+
+    def grid_coords(self):
+        out = np.zeros(9)
+        self.lib.ref_grid(self.h, _ptr(out))
+        return out
 
     def get_state(self):
         N = self.setup.grid.ncells

@@ -151,6 +151,73 @@ void ref_step(void *p, int nsteps) {
 
 double ref_tau(void *p) { return static_cast<RefRun *>(p)->h->getTau(); }
 
+// expandGrid2x (src/main.cpp:246-271) restated over the reference's own
+// Fluid/Cell/Hydro objects (main.cpp is not compiled into the harness since
+// it holds main()).  Returns 1 when resized, 0 when the grid is not
+// symmetric, -1 when the doubled step would fail Hydro::setDtau's check.
+int ref_resize2x(void *p) {
+  RefRun *r = static_cast<RefRun *>(p);
+  Fluid *f = r->f;
+  if (f->getX(0) + f->getX(f->getNX() - 1) > 0.001 ||
+      f->getY(0) + f->getY(f->getNY() - 1) > 0.001)
+    return 0;
+  Fluid *fnew = new Fluid(r->eos, r->eos, r->tr, f->getNX(), f->getNY(), f->getNZ(),
+                          2.0 * f->getX(0), 2.0 * f->getX(f->getNX() - 1),
+                          2.0 * f->getY(0), 2.0 * f->getY(f->getNY() - 1), f->getZ(0),
+                          f->getZ(f->getNZ() - 1), 2.0 * r->h->getDtau(), f->geteCrit());
+  const double dt2 = 2.0 * r->h->getDtau();
+  if (dt2 > fnew->getDx() / 2. || dt2 > fnew->getDy() / 2.) {
+    delete fnew;
+    return -1;
+  }
+  for (int ix = 0; ix < f->getNX(); ix++)
+    for (int iy = 0; iy < f->getNY(); iy++)
+      for (int iz = 0; iz < f->getNZ(); iz++)
+        fnew->getCell(ix, iy, iz)->importVars(f->getCell(2 * (ix - f->getNX() / 2) + f->getNX() / 2,
+                                                         2 * (iy - f->getNY() / 2) + f->getNY() / 2, iz));
+  r->h->setFluid(fnew);
+  r->h->setDtau(dt2);
+  delete f;
+  r->f = fnew;
+  r->dx = fnew->getDx();
+  r->dy = fnew->getDy();
+  return 1;
+}
+
+// The substep block of the driver loop (src/main.cpp:405-419) with
+// performStep; returns the substep count.
+int ref_advance(void *p, double dtau, double etamin, double etamax, int nz) {
+  RefRun *r = static_cast<RefRun *>(p);
+  Hydro *h = r->h;
+  int nSubSteps = 1;
+  while (dtau / nSubSteps > 1.0 * h->getTau() * (etamax - etamin) / (nz - 1)) nSubSteps *= 2;
+  if (nSubSteps > 1) {
+    h->setDtau(h->getDtau() / nSubSteps);
+    for (int j = 0; j < nSubSteps; j++) h->performStep();
+    h->setDtau(h->getDtau() * nSubSteps);
+  } else {
+    h->performStep();
+  }
+  return nSubSteps;
+}
+
+double ref_dtau(void *p) { return static_cast<RefRun *>(p)->h->getDtau(); }
+
+// out[9] = getX(0), getX(nx-1), getY(0), getY(ny-1), getZ(0), getZ(nz-1),
+//          dx, dy, dz of the current fluid
+void ref_grid(void *p, double *out) {
+  Fluid *f = static_cast<RefRun *>(p)->f;
+  out[0] = f->getX(0);
+  out[1] = f->getX(f->getNX() - 1);
+  out[2] = f->getY(0);
+  out[3] = f->getY(f->getNY() - 1);
+  out[4] = f->getZ(0);
+  out[5] = f->getZ(f->getNZ() - 1);
+  out[6] = f->getDx();
+  out[7] = f->getDy();
+  out[8] = f->getDz();
+}
+
 // Hydro::setDtau exits when dt > dx/2; refuse that here instead.
 int ref_set_dtau(void *p, double dt) {
   RefRun *r = static_cast<RefRun *>(p);

@@ -1471,3 +1471,66 @@ void or_totals(const or_grid *g, const or_eos *E, const or_trc *tr,
   out[14] = nCore;
   out[15] = nCoreCut;
 }
+
+/* expandGrid2x, src/main.cpp:246-271.  The new grid keeps nx, ny, nz and
+ * spans twice the transverse range, its bounds taken from the old grid's
+ * first and last cell coordinates (Fluid::getX = minx + ix*dx, src/fld.h);
+ * each new cell imports every variable of the old cell at
+ * 2*(i - n/2) + n/2 (clamped like Fluid::getCell) in x and y and the same iz
+ * (Cell::importVars, src/cll.cpp:54-68). */
+int or_resize2x(const or_grid *g, const or_state *in, or_grid *gout,
+                or_state *out) {
+  const double dx = (g->xmax - g->xmin) / (g->nx - 1);
+  const double dy = (g->ymax - g->ymin) / (g->ny - 1);
+  const double dz = (g->zmax - g->zmin) / (g->nz - 1);
+  const double x0 = g->xmin + 0 * dx, x1 = g->xmin + (g->nx - 1) * dx;
+  const double y0 = g->ymin + 0 * dy, y1 = g->ymin + (g->ny - 1) * dy;
+  if (x0 + x1 > 0.001 || y0 + y1 > 0.001) return 0;
+  or_grid ng = *g;
+  ng.xmin = 2.0 * x0;
+  ng.xmax = 2.0 * x1;
+  ng.ymin = 2.0 * y0;
+  ng.ymax = 2.0 * y1;
+  ng.zmin = g->zmin + 0 * dz;
+  ng.zmax = g->zmin + (g->nz - 1) * dz;
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const long N = (long)nx * ny * nz;
+  for (int iz = 0; iz < nz; iz++)
+    for (int iy = 0; iy < ny; iy++)
+      for (int ix = 0; ix < nx; ix++) {
+        int sx = 2 * (ix - nx / 2) + nx / 2, sy = 2 * (iy - ny / 2) + ny / 2;
+        sx = sx > 0 ? sx : 0;
+        sx = sx < nx ? sx : nx - 1;
+        sy = sy > 0 ? sy : 0;
+        sy = sy < ny ? sy : ny - 1;
+        const long i = ix + (long)nx * (iy + (long)ny * iz);
+        const long j = sx + (long)nx * (sy + (long)ny * iz);
+        for (int k = 0; k < 7; k++) {
+          out->Q[k * N + i] = in->Q[k * N + j];
+          out->Qh[k * N + i] = in->Qh[k * N + j];
+          out->Qprev[k * N + i] = in->Qprev[k * N + j];
+        }
+        for (int k = 0; k < 10; k++) {
+          out->pi[k * N + i] = in->pi[k * N + j];
+          out->piH[k * N + i] = in->piH[k * N + j];
+        }
+        out->Pi[i] = in->Pi[j];
+        out->PiH[i] = in->PiH[j];
+        for (int k = 0; k < 3; k++) out->m[k * N + i] = in->m[k * N + j];
+        out->vcc[i] = in->vcc[j];
+      }
+  *gout = ng;
+  return 1;
+}
+
+/* The driver's substep count, src/main.cpp:405-409: halve the step until
+ * it is below tau times the eta cell size of the parameters' grid.  Returns
+ * -1 when the count would pass 2^30. */
+int or_substeps(double dtau, double tau, double etamin, double etamax, int nz) {
+  int n = 1;
+  while (dtau / n > 1.0 * tau * (etamax - etamin) / (nz - 1)) {
+    if (n >= (1 << 30)) return -1;
+    n *= 2;
+  }
+  return n;
+}

@@ -89,6 +89,15 @@ void or_eos_s(const or_eos *eos, const double *e, const double *nb, int n,
 void or_totals(const or_grid *g, const or_eos *eos, const or_trc *tr,
                const or_state *s, double tau, double ecrit, double *out);
 
+/* expandGrid2x (src/main.cpp:246-271): fills *gout and out (caller-owned,
+ * same sizes as in) and returns 1, or returns 0 when the transverse grid is
+ * not symmetric (the reference then keeps the old grid). */
+int or_resize2x(const or_grid *g, const or_state *in, or_grid *gout,
+                or_state *out);
+
+/* Substep count of the driver loop (src/main.cpp:405-409); -1 past 2^30. */
+int or_substeps(double dtau, double tau, double etamin, double etamax, int nz);
+
 /* Fluid::updateM (src/fld.cpp:384-423) alone, for unit tests. */
 void or_update_m(const or_grid *g, double *m, double tau, double dt);
 

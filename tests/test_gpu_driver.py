@@ -1,0 +1,131 @@
+"""Device driver-loop pieces through the C ABI against the oracle: the
+eta-CFL substeps (vh_advance, src/main.cpp:405-419) and the x2 transverse
+resize (vh_resize2x, expandGrid2x src/main.cpp:246-271), bit-for-bit."""
+import numpy as np
+import pytest
+
+import pyoracle as P
+from helpers import compare_states, gpu_state_as_oracle
+from vhlle_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _drive(run, setup, nloops, dtau, tau_resize):
+    g = setup.grid
+    counts, resized = [], False
+    for _ in range(nloops):
+        counts.append(run.advance(dtau, g.etamin, g.etamax, g.nz))
+        if run_tau(run) >= tau_resize and not resized:
+            assert run.resize2x() == 1
+            resized = True
+    return counts, resized
+
+
+def run_tau(run):
+    return run.tau_now if hasattr(run, "tau_now") else run.tau
+
+
+@pytest.mark.parametrize("case", [
+    ("glauber_17x17x9_tau005", lambda: W.small_glauber3d(17, 9, tau0=0.05, dt=0.1), 0.1, 8, 0.3),
+    ("glauber_16x16x7_even", lambda: W.small_glauber3d(16, 7, tau0=0.04, dt=0.1, b=4.0), 0.1, 7,
+     0.2),
+    ("glauber_33x33x17", lambda: W.small_glauber3d(33, 17, tau0=0.1, dt=0.1), 0.1, 10, 0.5),
+], ids=lambda c: c[0])
+def test_gpu_substeps_and_resize_equal_oracle(case):
+    from vhlle_b200.capi import GpuHydro
+    name, fac, dtau, nloops, tres = case
+    setup = fac()
+    o = P.OracleRun(setup)
+    d = GpuHydro(setup)
+    co, ro = _drive(o, setup, nloops, dtau, tres)
+    cd, rd = _drive(d, setup, nloops, dtau, tres)
+    assert co == cd and ro and rd
+    assert max(co) > 1
+    assert o.tau_now == d.tau
+    assert o.dt == d.dtau
+    assert np.array_equal(o.grid_coords(), d.grid_coords())
+    d.sync()
+    assert d.error_bits() == 0
+    bad = compare_states(gpu_state_as_oracle(d.get_state()), o.get_state())
+    assert not bad, bad
+    # totals on the resized grid (reduction order differs: 1e-10)
+    to, td = o.totals(), d.totals()
+    for k in P.TOTALS:
+        a, b = to[k], td[k]
+        assert abs(a - b) <= 1e-10 * max(abs(a), abs(b)) + 1e-300, (k, a, b)
+    d.close()
+
+
+def test_gpu_resize_2d_nan_eta_bounds():
+    """nz = 1: the reference's getZ(0) = etamin + 0*inf is NaN, and the
+    resized 2D grid carries it; evolution continues as in the oracle."""
+    from vhlle_b200.capi import GpuHydro
+    setup = W.gubser_setup(nx=21, ny=21)
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    o.step(2)
+    d.step(2)
+    assert o.resize2x() == 1 and d.resize2x() == 1
+    go, gd = o.grid_coords(), d.grid_coords()
+    assert ((go == gd) | (np.isnan(go) & np.isnan(gd))).all(), (go, gd)
+    o.step(3)
+    d.step(3)
+    bad = compare_states(gpu_state_as_oracle(d.get_state()), o.get_state())
+    assert not bad, bad
+    d.close()
+
+
+def test_gpu_resize_keeps_asymmetric_grid():
+    from vhlle_b200.capi import GpuHydro
+    setup = W.small_glauber3d(13, 5)
+    g = setup.grid
+    setup.grid = W.Grid(g.nx, g.ny, g.nz, g.xmin + 1.0, g.xmax + 1.0, g.ymin, g.ymax, g.etamin,
+                        g.etamax)
+    d = GpuHydro(setup)
+    before = d.get_state()
+    dt0 = d.dtau
+    assert d.resize2x() == 0
+    assert d.dtau == dt0
+    assert not compare_states(d.get_state(), before)
+    d.close()
+
+
+def test_cpp_driver_loop_equals_oracle(tmp_path):
+    """vhlle_run (C++ host layer over the C ABI) runs the reference driver
+    loop -- substeps at small tau, the x2 resize at tauGridResize, stop at
+    tauMax -- from a snapshot; its final grid equals the oracle driven
+    through the same loop, bit-for-bit."""
+    import subprocess
+    from vhlle_b200 import build as B
+    drv = B.build_driver()
+    setup = W.small_glauber3d(17, 9, tau0=0.05, dt=0.1)
+    ic = str(tmp_path / "ic.vhb")
+    W.write_snapshot(ic, setup.grid, setup.tau0, setup.dt, W.initial_snapshot_state(setup))
+    params = str(tmp_path / "params.txt")
+    tau_max, tau_resize = 0.75, 0.3
+    W.write_params(params, setup, tauMax=tau_max, tauGridResize=tau_resize, eos1fFile=str(
+        tmp_path / "eos.dat"))
+    setup.eos.write_eos1f(str(tmp_path / "eos.dat"))
+    out = tmp_path / "out"
+    r = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", str(out)],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
+    assert "grid resize" in r.stdout and "timestep reduced by 2" in r.stdout
+
+    o = P.OracleRun(setup)
+    g = setup.grid
+    resized = False
+    while True:
+        o.advance(setup.dt, g.etamin, g.etamax, g.nz)
+        if o.tau_now >= tau_resize and not resized:
+            assert o.resize2x() == 1
+            resized = True
+        if not o.tau_now < tau_max + 0.0001:
+            break
+    nx, ny, nz, b, tau, dt, st = W.read_snapshot(str(out / "final.vhb"))
+    assert tau == o.tau_now and dt == o.dt
+    og = o.grid
+    assert np.array_equal(b, [og.xmin, og.xmax, og.ymin, og.ymax, og.zmin, og.zmax])
+    exp = o.get_state()
+    bad = compare_states(st, exp)
+    assert not bad, bad

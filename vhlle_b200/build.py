@@ -20,6 +20,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvhlle_b200.so")
 SOURCES = ["vh_step.cu", "vh_capi.cu", "vh_noalloc.cu", "vh_surface.cu"]
 HEADERS = ["vh_physics.cuh", "vh_step.cuh", "vh_surface.cuh"]
+DRIVER_SRC = os.path.join(HERE, "driver", "vhlle_run.cpp")
+DRIVER = os.path.join(HERE, "driver", "vhlle_run")
 
 
 def nvcc_path() -> str:
@@ -77,6 +79,23 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     return LIB
 
 
+def build_driver(force: bool = False) -> str:
+    """Compiles the C++ driver program (vhlle_run) against the library."""
+    build()
+    hpp = os.path.join(ROOT, "include", "vhlle_b200.hpp")
+    if (not force and os.path.exists(DRIVER)
+            and os.path.getmtime(DRIVER) >= max(os.path.getmtime(p) for p in (DRIVER_SRC, hpp, LIB))):
+        return DRIVER
+    cmd = [host_cxx(), "-O2", "-std=c++17", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+           DRIVER_SRC, "-L", HERE, "-lvhlle_b200", "-Wl,-rpath,$ORIGIN/..", "-o", DRIVER + ".tmp"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("driver build failed:\n%s%s" % (r.stdout, r.stderr))
+    os.replace(DRIVER + ".tmp", DRIVER)
+    return DRIVER
+
+
 if __name__ == "__main__":
     out = build(force=True, verbose=True, ptxas_v="--check" in sys.argv)
     print(out)
+    print(build_driver(force=True))

@@ -27,7 +27,8 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
            "vh_abi_version", "vh_transform_pv", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
-           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals")
+           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
+           "vh_get_grid", "vh_advance", "vh_resize2x")
 
 
 class VhError(RuntimeError):
@@ -115,6 +116,10 @@ def lib():
                                   ctypes.POINTER(VhStateView), vp, ctypes.POINTER(ctypes.c_uint)]
     L.vh_noalloc_last_error.restype = ctypes.c_char_p
     L.vh_totals.argtypes = [vp, ctypes.c_double, _dp]
+    L.vh_get_grid.argtypes = [vp, ctypes.POINTER(VhGrid)]
+    L.vh_advance.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                             ctypes.POINTER(ctypes.c_int)]
+    L.vh_resize2x.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     _lib = L
     return L
 
@@ -223,6 +228,40 @@ class GpuHydro:
 
     def set_dtau(self, dt: float):
         self._check(self.L.vh_set_dtau(self.h, dt))
+
+    @property
+    def dtau(self) -> float:
+        d = ctypes.c_double()
+        self._check(self.L.vh_get_dtau(self.h, ctypes.byref(d)))
+        return d.value
+
+    def advance(self, dtau: float, etamin: float, etamax: float, nz: int) -> int:
+        """The driver's substep block (src/main.cpp:405-419); returns the count."""
+        n = ctypes.c_int(0)
+        self._check(self.L.vh_advance(self.h, dtau, etamin, etamax, nz, ctypes.byref(n)))
+        return n.value
+
+    def resize2x(self) -> int:
+        """expandGrid2x (src/main.cpp:246-271): 1 resized, 0 grid not symmetric."""
+        r = ctypes.c_int(0)
+        self._check(self.L.vh_resize2x(self.h, ctypes.byref(r)))
+        return r.value
+
+    def grid(self):
+        g = VhGrid()
+        self._check(self.L.vh_get_grid(self.h, ctypes.byref(g)))
+        return g
+
+    def grid_coords(self):
+        """getX(0), getX(nx-1), getY(0), getY(ny-1), getZ(0), getZ(nz-1), dx, dy, dz."""
+        g = self.grid()
+        with np.errstate(all="ignore"):
+            a = np.array([g.xmin, g.xmax, g.ymin, g.ymax, g.etamin, g.etamax], dtype=np.float64)
+            n = np.array([g.nx - 1, g.ny - 1, g.nz - 1], dtype=np.float64)
+            d = (a[1::2] - a[0::2]) / n
+            return np.array([a[0] + 0 * d[0], a[0] + n[0] * d[0], a[2] + 0 * d[1],
+                             a[2] + n[1] * d[1], a[4] + 0 * d[2], a[4] + n[2] * d[2],
+                             d[0], d[1], d[2]])
 
     def launches_per_step(self) -> int:
         n = ctypes.c_int()

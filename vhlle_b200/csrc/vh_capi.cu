@@ -38,6 +38,7 @@ struct vh_ctx {
   vh_grid grid{};
   double* tot_partial = nullptr;  // [blocks][16] block sums of the totals
   double* tot_out = nullptr;      // [16]
+  double* resize_tmp = nullptr;   // [10][N] staging of the resize gather
   std::string err;
   std::vector<void*> allocs;
   // timers and per-kernel profiling
@@ -465,6 +466,78 @@ vh_status vh_get_tau(vh_ctx* ctx, double* tau) {
 vh_status vh_set_tau(vh_ctx* ctx, double tau) {
   if (!ctx) return VH_ERR_ARG;
   ctx->tau = tau;
+  return VH_OK;
+}
+
+vh_status vh_get_grid(vh_ctx* ctx, vh_grid* out) {
+  if (!ctx || !out) return VH_ERR_ARG;
+  *out = ctx->grid;
+  return VH_OK;
+}
+
+vh_status vh_advance(vh_ctx* ctx, double dtau, double etamin, double etamax, int nz, int* nsub) {
+  if (!ctx) return VH_ERR_ARG;
+  int n = 1;
+  while (dtau / n > 1.0 * ctx->tau * (etamax - etamin) / (nz - 1)) {
+    if (n >= (1 << 30)) return fail(ctx, VH_ERR_ARG, "vh_advance: substep count overflow");
+    n *= 2;
+  }
+  if (nsub) *nsub = n;
+  if (n == 1) return vh_step(ctx);
+  vh_status st = vh_set_dtau(ctx, ctx->dt / n);
+  if (st != VH_OK) return st;
+  for (int j = 0; j < n && st == VH_OK; j++) st = vh_step(ctx);
+  const vh_status st2 = vh_set_dtau(ctx, ctx->dt * n);
+  return st != VH_OK ? st : st2;
+}
+
+vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
+  if (resized) *resized = 0;
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_resize2x: no state uploaded");
+  const vh_grid& gr = ctx->grid;
+  vh::Geo& g = ctx->g;
+  // Fluid::getX / getY / getZ, src/fld.h:62-64
+  const double x0 = gr.xmin + 0 * g.dx, x1 = gr.xmin + (g.nx - 1) * g.dx;
+  const double y0 = gr.ymin + 0 * g.dy, y1 = gr.ymin + (g.ny - 1) * g.dy;
+  if (x0 + x1 > 0.001 || y0 + y1 > 0.001) return VH_OK;
+  vh_grid ng = gr;
+  ng.xmin = 2.0 * x0;
+  ng.xmax = 2.0 * x1;
+  ng.ymin = 2.0 * y0;
+  ng.ymax = 2.0 * y1;
+  ng.etamin = gr.etamin + 0 * g.dz;
+  ng.etamax = gr.etamin + (g.nz - 1) * g.dz;
+  // Fluid::Fluid, src/fld.cpp:77-79
+  const double ndx = (ng.xmax - ng.xmin) / (g.nx - 1);
+  const double ndy = (ng.ymax - ng.ymin) / (g.ny - 1);
+  const double ndz = (ng.etamax - ng.etamin) / (g.nz - 1);
+  const double dt2 = 2.0 * ctx->dt;
+  if (dt2 > ndx / 2. || dt2 > ndy / 2.)
+    return fail(ctx, VH_ERR_ARG, "vh_resize2x: too big delta_tau for the resized grid");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->resize_tmp) {
+    vh_status st = dalloc(ctx, &ctx->resize_tmp, (size_t)10 * g.N);
+    if (st != VH_OK) return st;
+  }
+  vh::Fields& f = ctx->f;
+  struct Plane {
+    double* p;
+    int n;
+  } planes[] = {{f.Q, 7}, {f.Qh, 7}, {f.Qprev, 7}, {f.pi, 10}, {f.piH, 10},
+                {f.Pi, 1}, {f.PiH, 1}, {f.m, 3},  {f.vcc, 1}};
+  for (const Plane& pl : planes) {
+    vh::launch_resize_gather(g, pl.p, ctx->resize_tmp, pl.n, ctx->stream);
+    VH_CUDA(ctx, cudaGetLastError());
+    VH_CUDA(ctx, cudaMemcpyAsync(pl.p, ctx->resize_tmp, sizeof(double) * pl.n * g.N,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  ctx->grid = ng;
+  g.dx = ndx;
+  g.dy = ndy;
+  g.dz = ndz;
+  ctx->dt = dt2;  // src/main.cpp:268
+  if (resized) *resized = 1;
   return VH_OK;
 }
 

@@ -1006,4 +1006,27 @@ void launch_zero_negative_rows(double* Q, long long N, cudaStream_t s) {
   if (N > 0) k_zero_negative_rows<<<nblk(N, 256), 256, 0, s>>>(Q, N);
 }
 
+// expandGrid2x decimation (src/main.cpp:259-266): new cell (ix, iy, iz) takes
+// the old cell 2*(i - n/2) + n/2 in x and y, clamped like Fluid::getCell, and
+// the same iz.  ncomp component planes of N cells each.
+__global__ void k_resize_gather(Geo g, const double* __restrict__ src, double* __restrict__ dst,
+                                int ncomp) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  int sx = 2 * (ix - g.nx / 2) + g.nx / 2, sy = 2 * (iy - g.ny / 2) + g.ny / 2;
+  sx = sx > 0 ? sx : 0;
+  sx = sx < g.nx ? sx : g.nx - 1;
+  sy = sy > 0 ? sy : 0;
+  sy = sy < g.ny ? sy : g.ny - 1;
+  const long long j = cidx(g, sx, sy, iz);
+  for (int k = 0; k < ncomp; k++) dst[k * g.N + i] = src[k * g.N + j];
+}
+
+void launch_resize_gather(const Geo& g, const double* src, double* dst, int ncomp,
+                          cudaStream_t s) {
+  if (g.N > 0) k_resize_gather<<<nblk(g.N, 256), 256, 0, s>>>(g, src, dst, ncomp);
+}
+
 }  // namespace vh

@@ -80,6 +80,9 @@ struct LaunchMarker {
 // Enqueues one performStep on stream s; returns the number of launches.
 // Leaves the updated fill fractions in f.m2 (the caller swaps m and m2).
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk = nullptr);
+// gathers ncomp planes of the x2 resized grid from src into dst
+void launch_resize_gather(const Geo& g, const double* src, double* dst, int ncomp,
+                          cudaStream_t s);
 
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
                          cudaStream_t s);

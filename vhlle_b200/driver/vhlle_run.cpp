@@ -1,0 +1,151 @@
+// vhlle_run -- the reference driver's evolution loop (src/main.cpp:273-441)
+// over the device hydro: parameters file, substeps, one-shot x2 resize,
+// termination at tauMax, with the initial grid read from a snapshot instead
+// of the reference's initial-state models.
+//
+//   vhlle_run -params FILE -ISinput SNAPSHOT [-outputDir DIR] [-system S]
+//             [-printParams]
+//
+// Parameters are read exactly as the reference reads them (same keys,
+// defaults, "CCC"/"UUU" echo).  The hydro EoS is the EoS1f table named by
+// the extra key eos1fFile, else the conformal gas of 47.5 degrees of
+// freedom.  Each loop iteration prints tau and the interior totals of
+// Fluid::outputSurface; the final grid is written to DIR/final.vhb.
+#include <sys/stat.h>
+
+#include <cmath>
+#include <cstring>
+#include <iomanip>
+#include <iostream>
+#include <string>
+
+#include "vhlle_b200.hpp"
+
+namespace {
+
+struct CommandLine {
+  std::string collSystem, isInputFile, outputDir = "data", params;
+  bool printParams = false;
+};
+
+// readCommandLine, src/main.cpp:226-243 (same flags, value after the flag)
+CommandLine readCommandLine(int argc, char** argv, vhb::Params& P) {
+  CommandLine c;
+  if (argc == 1) throw vhb::Error(VH_ERR_ARG, "no CL params - exiting.");
+  for (int i = 1; i < argc; i++)
+    if (std::strcmp(argv[i], "-printParams") == 0) c.printParams = true;
+  for (int i = 1; i < argc - 1; i++) {
+    if (std::strcmp(argv[i], "-system") == 0) c.collSystem = argv[i + 1];
+    if (std::strcmp(argv[i], "-params") == 0) {
+      c.params = argv[i + 1];
+      std::cout << "vhlle: reading parameters from " << c.params << std::endl;
+      P.read(argv[i + 1], std::cout);
+    }
+    if (std::strcmp(argv[i], "-ISinput") == 0) c.isInputFile = argv[i + 1];
+    if (std::strcmp(argv[i], "-outputDir") == 0) c.outputDir = argv[i + 1];
+  }
+  P.outputDir = c.outputDir;
+  P.isInputFile = c.isInputFile;
+  P.collSystem = c.collSystem;
+  return c;
+}
+
+void printParameters(const vhb::Params& P) {
+  std::cout << std::setprecision(17);
+  std::cout << "====== parameters ======\n"
+            << "outputDir = " << P.outputDir << "\n"
+            << "eos1fFile = " << P.eos1fFile << "\n"
+            << "nx = " << P.nx << "\nny = " << P.ny << "\nnz = " << P.nz << "\n"
+            << "xmin = " << P.xmin << "\nxmax = " << P.xmax << "\n"
+            << "ymin = " << P.ymin << "\nymax = " << P.ymax << "\n"
+            << "etamin = " << P.etamin << "\netamax = " << P.etamax << "\n"
+            << "tau0 = " << P.tau0 << "\ntauMax = " << P.tauMax << "\n"
+            << "tauGridResize = " << P.tauResize << "\ndtau = " << P.dtau << "\n"
+            << "e_crit = " << P.eCrit << "\n"
+            << "zetaSparam = " << P.zetaSparam << "\netaSparam = " << P.etaSparam << "\n"
+            << "etaS = " << P.etaS << "\nzetaS = " << P.zetaS << "\n"
+            << "al = " << P.al << "\nah = " << P.ah << "\naRho = " << P.aRho << "\n"
+            << "T0 = " << P.T0 << "\netaSMin = " << P.etaSMin << "\n"
+            << "etaSEpsilonMin = " << P.etaSEpsilonMin << "\n"
+            << "etaSShiftMuB = " << P.etaSShiftMuB << "\netaSScaleMuB = " << P.etaSScaleMuB
+            << "\n"
+            << "zetaSPeakEpsilon = " << P.zetaSPeakEpsilon << "\n"
+            << "zetaSScaleBeta = " << P.zetaSScaleBeta << "\n"
+            << "zetaSSigmaMinus = " << P.zetaSSigmaMinus << "\n"
+            << "zetaSSigmaPlus = " << P.zetaSSigmaPlus << "\n"
+            << "VTK_output_values = " << P.vtk_values << "\n"
+            << "======= end parameters =======" << std::endl;
+}
+
+int run(int argc, char** argv) {
+  vhb::Params P;
+  const CommandLine cl = readCommandLine(argc, argv, P);
+  printParameters(P);
+  if (cl.printParams) return 0;
+  if (cl.isInputFile.empty()) throw vhb::Error(VH_ERR_ARG, "no -ISinput snapshot given");
+
+  const double hbarc = 0.1973269804, deg = 16.0 + 3.0 * 12.0 * (7.0 / 8.0);
+  vhb::EoS* eos = P.eos1fFile.empty()
+                      ? static_cast<vhb::EoS*>(new vhb::EoSConformal(3.0 * deg * M_PI * M_PI / 90.0 /
+                                                                     (hbarc * hbarc * hbarc)))
+                      : static_cast<vhb::EoS*>(new vhb::EoS1f(P.eos1fFile.c_str()));
+  vhb::EoS* eosH = eos;
+  vhb::TransportCoeff* trcoeff = new vhb::TransportCoeff(
+      P.etaS, P.zetaS, P.ah, P.al, P.aRho, P.T0, P.etaSMin, P.etaSEpsilonMin, P.etaSShiftMuB,
+      P.etaSScaleMuB, P.zetaSPeakEpsilon, P.zetaSScaleBeta, P.zetaSSigmaMinus,
+      P.zetaSSigmaPlus, eos, P.etaSparam, P.zetaSparam);
+
+  const auto hdr = vhb::Fluid::readSnapshotHeader(cl.isInputFile.c_str());
+  if (hdr.grid.nx != P.nx || hdr.grid.ny != P.ny || hdr.grid.nz != P.nz ||
+      hdr.grid.xmin != P.xmin || hdr.grid.xmax != P.xmax || hdr.grid.ymin != P.ymin ||
+      hdr.grid.ymax != P.ymax || hdr.grid.etamin != P.etamin || hdr.grid.etamax != P.etamax)
+    throw vhb::Error(VH_ERR_ARG, "the snapshot's grid differs from the parameters' grid");
+  vhb::Fluid* f = new vhb::Fluid(eos, eosH, trcoeff, P.nx, P.ny, P.nz, P.xmin, P.xmax, P.ymin,
+                                 P.ymax, P.etamin, P.etamax, P.dtau, P.eCrit);
+  f->loadSnapshot(cl.isInputFile.c_str());
+  const double tau0 = hdr.tau;  // the snapshot fixes the start time
+  std::cout << "fluid allocation done\nIC done (tau0 = " << tau0 << ")\n";
+
+  vhb::Hydro* h = new vhb::Hydro(f, eos, trcoeff, tau0, P.dtau);
+  bool resized = false;
+  int nloops = 0;
+  std::cout << std::setprecision(6);
+  do {
+    const int nSubSteps = h->advance(P.dtau, P.etamin, P.etamax, P.nz);
+    if (nSubSteps > 1) std::cout << "timestep reduced by " << nSubSteps << std::endl;
+    const vhb::Totals t = h->totals();
+    std::cout << std::setw(10) << h->getTau() << std::setw(13) << t.E << std::setw(13) << t.Efull
+              << std::setw(13) << t.Nb2 << std::setw(13) << t.S << std::setw(13)
+              << (float)t.nCoreCutCells / (float)t.nCoreCells << std::endl;
+    nloops++;
+    if (h->getTau() >= P.tauResize && !resized) {
+      std::cout << "grid resize\n";
+      f = vhb::expandGrid2x(h, eos, eosH, trcoeff);
+      resized = true;
+    }
+  } while (h->getTau() < P.tauMax + 0.0001);
+
+  h->sync();
+  unsigned bits = 0;
+  vhb::check(vh_error_bits(h->context(), &bits), h->context());
+  mkdir(cl.outputDir.c_str(), 0755);
+  const std::string out = cl.outputDir + "/final.vhb";
+  f->saveSnapshot(out.c_str(), h->getTau(), h->getDtau());
+  std::cout << "loops " << nloops << " error_bits " << bits << " final " << out << std::endl;
+  delete h;
+  delete f;
+  delete trcoeff;
+  delete eos;
+  return bits ? 3 : 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+  try {
+    return run(argc, argv);
+  } catch (const vhb::Error& e) {
+    std::cerr << "vhlle_run: " << e.what() << std::endl;
+    return 1;
+  }
+}

@@ -342,3 +342,80 @@ def small_glauber3d(n: int = 17, nz: int = 9, seed: int = 20260001, **kw) -> Set
     kw.setdefault("dt", 0.05)
     kw.setdefault("xmax", 15.0)
     return glauber3d_setup(nx=n, ny=n, nz=nz, seed=seed, **kw)
+
+
+# --------------------------------------------------------------- snapshots
+SNAPSHOT_TAG = b"VHBSNAP1"
+SNAPSHOT_FIELDS = (("Q", 7), ("Qh", 7), ("Qprev", 7), ("pi", 10), ("piH", 10), ("Pi", 1),
+                   ("PiH", 1), ("m", 3), ("vcc", 1))
+
+
+def write_snapshot(path: str, grid: Grid, tau: float, dt: float, state: dict) -> None:
+    """Grid snapshot read by the C++ driver (Fluid::loadSnapshot): tag
+    "VHBSNAP1", int32 nx ny nz 0, float64 bounds tau dt, then the planes
+    Q Qh Qprev pi piH Pi PiH m vcc as raw float64 (component-major)."""
+    N = grid.ncells
+    with open(path, "wb") as f:
+        f.write(SNAPSHOT_TAG)
+        f.write(np.array([grid.nx, grid.ny, grid.nz, 0], dtype="<i4").tobytes())
+        f.write(np.array(list(grid.bounds()) + [tau, dt], dtype="<f8").tobytes())
+        for k, nc in SNAPSHOT_FIELDS:
+            a = state.get(k)
+            if a is None:
+                a = np.ones(N) if k == "vcc" else np.zeros((nc, N))
+            f.write(np.ascontiguousarray(a, dtype="<f8").reshape(nc, N).tobytes())
+
+
+def read_snapshot(path: str):
+    """(nx, ny, nz, bounds[6], tau, dt, state) of a snapshot file."""
+    with open(path, "rb") as f:
+        raw = f.read()
+    if raw[:8] != SNAPSHOT_TAG:
+        raise ValueError("not a grid snapshot: %s" % path)
+    nx, ny, nz, _ = np.frombuffer(raw, dtype="<i4", count=4, offset=8)
+    hdr = np.frombuffer(raw, dtype="<f8", count=8, offset=24)
+    N = int(nx) * int(ny) * int(nz)
+    off, state = 88, {}
+    for k, nc in SNAPSHOT_FIELDS:
+        state[k] = np.frombuffer(raw, dtype="<f8", count=nc * N, offset=off).reshape(nc, N).copy()
+        off += nc * N * 8
+    if off != len(raw):
+        raise ValueError("snapshot size mismatch: %s" % path)
+    return int(nx), int(ny), int(nz), hdr[:6].copy(), float(hdr[6]), float(hdr[7]), state
+
+
+def initial_snapshot_state(setup: "Setup") -> dict:
+    """The state an initial-condition model leaves in the cells: Q, Qprev = Q,
+    m on all three axes, optional pi/Pi, other fields zero, vcc = 1."""
+    N = setup.grid.ncells
+    Q = np.array(setup.Q, dtype=np.float64).reshape(7, N)
+    Q[:, Q[0] < 0] = 0.0  # Cell::setQ, src/cll.h:75-80
+    m = np.repeat(np.asarray(setup.m, dtype=np.float64).reshape(1, N), 3, 0)
+    st = dict(Q=Q, Qh=np.zeros((7, N)), Qprev=Q.copy(), m=m, vcc=np.ones((1, N)))
+    if setup.pi is not None:
+        st["pi"] = np.asarray(setup.pi, dtype=np.float64).reshape(10, N)
+    if setup.Pi is not None:
+        st["Pi"] = np.asarray(setup.Pi, dtype=np.float64).reshape(1, N)
+    return st
+
+
+def write_params(path: str, setup: "Setup", **extra) -> None:
+    """A parameters file in the reference's "name value" format for the
+    setup's grid, step and transport coefficients (src/main.cpp:83-156)."""
+    g = setup.grid
+    tr = dict(zip(TR_FIELDS, setup.tr_vector()))
+    lines = ["! written by vhlle_b200.workloads.write_params",
+             "nx %d" % g.nx, "ny %d" % g.ny, "nz %d" % g.nz,
+             "xmin %r" % g.xmin, "xmax %r" % g.xmax, "ymin %r" % g.ymin, "ymax %r" % g.ymax,
+             "etamin %r" % g.etamin, "etamax %r" % g.etamax,
+             "tau0 %r" % setup.tau0, "dtau %r" % setup.dt, "e_crit %r" % setup.ecrit,
+             "etaS %r" % tr["etaS0"], "zetaS %r" % tr["zetaS0"],
+             "etaSparam %d" % setup.etaSparam, "zetaSparam %d" % setup.zetaSparam]
+    for k in ("ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin", "etaSShiftMuB",
+              "etaSScaleMuB", "zetaSPeakEpsilon", "zetaSScaleBeta", "zetaSSigmaMinus",
+              "zetaSSigmaPlus"):
+        lines.append("%s %r" % (k, tr[k]))
+    for k, v in extra.items():
+        lines.append("%s %s" % (k, v if isinstance(v, str) else repr(v)))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
