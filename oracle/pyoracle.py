@@ -75,6 +75,12 @@ def oracle_lib():
         lib.or_resize2x.restype = ctypes.c_int
         lib.or_resize2x.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_State),
                                     ctypes.POINTER(_Grid), ctypes.POINTER(_State)]
+        lib.or_surface.restype = ctypes.c_long
+        lib.or_surface.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_State),
+                                   ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_long,
+                                   _dp]
+        lib.or_cornelius4d.restype = ctypes.c_int
+        lib.or_cornelius4d.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp]
         lib.or_substeps.restype = ctypes.c_int
         lib.or_substeps.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                     ctypes.c_double, ctypes.c_int]
@@ -110,6 +116,8 @@ def ref_lib():
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
+        lib.ref_cornelius4d.restype = ctypes.c_int
+        lib.ref_cornelius4d.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp]
         lib.ref_resize2x.restype = ctypes.c_int
         lib.ref_resize2x.argtypes = [ctypes.c_void_p]
         lib.ref_advance.restype = ctypes.c_int
@@ -119,13 +127,46 @@ def ref_lib():
         lib.ref_dtau.argtypes = [ctypes.c_void_p]
         lib.ref_grid.argtypes = [ctypes.c_void_p, _dp]
         lib.ref_output_surface.restype = ctypes.c_int
-        lib.ref_output_surface.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p,
+        lib.ref_output_surface.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_char_p,
                                            ctypes.c_int]
         _lib_ref = lib
     return _lib_ref
 
 
 FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")
+# one freeze-out element record (Fluid::outputSurface, src/fld.cpp:656-797)
+SURF_REC = 29
+SURF_COLS = ("tau", "x", "y", "eta", "ds0", "ds1", "ds2", "ds3", "u0", "u1", "u2", "u3", "T",
+             "mub", "muq", "mus", "pi00", "pi01", "pi11", "pi02", "pi12", "pi22", "pi03", "pi13",
+             "pi23", "pi33", "Pi", "e", "nb")
+SURF_ACC = ("nsusp", "EtotSurf", "nbSurf", "vEff", "highT")
+
+
+def cornelius4d(cube, dx, e0, reference=False):
+    """One hypercube through the oracle's Cornelius (or the reference's):
+    (centroids [n][4], normals [n][4]); n = -1 where the reference stops."""
+    cube = np.ascontiguousarray(cube, dtype=np.float64).reshape(16)
+    dx = np.ascontiguousarray(dx, dtype=np.float64)
+    cent = np.zeros((10, 4))
+    norm = np.zeros((10, 4))
+    if reference:
+        n = ref_lib().ref_cornelius4d(_ptr(cube), _ptr(dx), e0, _ptr(cent), _ptr(norm))
+    else:
+        n = oracle_lib().or_cornelius4d(_ptr(cube), _ptr(dx), e0, _ptr(cent), _ptr(norm))
+    return (cent[:n].copy(), norm[:n].copy()) if n >= 0 else (None, None)
+
+
+def read_freezeout(path, extend=False):
+    """Element records of a freezeout.dat written by the reference
+    (src/fld.cpp:658-797: 15 significant digits, OUTPI layout)."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            v = line.split()
+            if v:
+                rows.append([float(x) for x in v])
+    a = np.array(rows, dtype=np.float64).reshape(-1, 29 if extend else 27)
+    return a
 TOTALS = ("E", "Efull", "Nb1", "Nb2", "S", "Px", "vt_num", "vt_den", "vxvy_num", "vxvy_den",
           "pi0x_num", "pi0x_den", "txxyy_num", "txxyy_den", "nCoreCells", "nCoreCutCells")
 FIELD_NCOMP = dict(Q=7, Qh=7, Qprev=7, pi=10, piH=10, Pi=1, PiH=1, m=3, vcc=1)
@@ -278,6 +319,20 @@ class OracleRun:
                            ctypes.byref(sv), self.tau.value, self.setup.ecrit, _ptr(out))
         return dict(zip(TOTALS, out))
 
+    def surface(self, dtf=None, cap=200000):
+        """Freeze-out elements of outputSurface at the current tau: (records
+        [n][29], acc dict).  dtf is the Fluid's step (default: the setup's)."""
+        dtf = self.setup.dt if dtf is None else dtf
+        rec = np.zeros((cap, SURF_REC))
+        acc = np.zeros(5)
+        sv = self._sview()
+        n = self.lib.or_surface(ctypes.byref(self.grid), ctypes.byref(self.eos.s), ctypes.byref(sv),
+                                self.tau.value, dtf, self.setup.ecrit, _ptr(rec), cap, _ptr(acc))
+        if n < 0:
+            raise RuntimeError("Cornelius stopped (the reference would exit)")
+        assert n <= cap
+        return rec[:n].copy(), dict(zip(SURF_ACC, acc))
+
     def transform_pv(self, Q):
         Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
         out = np.zeros((len(Q), 8))
@@ -370,10 +425,11 @@ class RefRun:
         self.lib.ref_totals(self.h, self.tau_now, _ptr(out))
         return dict(zip(TOTALS, out))
 
-    def output_surface(self, outdir):
-        """Fluid::outputSurface: returns (nelements, printed totals line)."""
+    def output_surface(self, outdir, extend=False):
+        """Fluid::outputSurface: returns (nelements, printed totals line).
+        Element lines go to outdir/freezeout.dat.unfinished."""
         buf = ctypes.create_string_buffer(512)
-        n = self.lib.ref_output_surface(self.h, outdir.encode(), buf, 512)
+        n = self.lib.ref_output_surface(self.h, outdir.encode(), int(extend), buf, 512)
         return n, buf.value.decode()
 
     def eos_eval(self, e, nb):

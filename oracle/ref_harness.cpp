@@ -25,6 +25,7 @@
 
 #include "eos.h"  // must precede eo1.h, which only forward-declares EoS
 #include "cll.h"
+#include "cornelius.h"
 #include "eo1.h"
 #include "fld.h"
 #include "hdo.h"
@@ -109,6 +110,7 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
 
 void ref_destroy(void *p) {
   RefRun *r = static_cast<RefRun *>(p);
+  if (r->output_open && output::ffreeze.is_open()) output::ffreeze.close();
   delete r->h;
   delete r->f;
   delete r->tr;
@@ -373,16 +375,18 @@ void ref_totals(void *p, double tau, double *out) {
 // Returns the number of surface elements; the line outputSurface prints
 // (tau E Efull nbSurf S EtotSurf nelements nsusp cut-fraction, 6 digits) is
 // copied into `line`.
-int ref_output_surface(void *p, const char *dir, char *line, int linelen) {
+int ref_output_surface(void *p, const char *dir, int extendFO, char *line, int linelen) {
   RefRun *r = static_cast<RefRun *>(p);
   std::streambuf *old = std::cout.rdbuf();
   std::ostringstream cap;
   std::cout.rdbuf(cap.rdbuf());
   if (!r->output_open) {
+    // the freeze-out stream is a process-wide global: one run at a time
+    if (output::ffreeze.is_open()) output::ffreeze.close();
     r->f->initOutput(dir, r->tau0, true);
     r->output_open = true;
   }
-  const int n = r->f->outputSurface(r->h->getTau(), false);
+  const int n = r->f->outputSurface(r->h->getTau(), extendFO != 0);
   output::ffreeze.flush();
   std::cout.rdbuf(old);
   const std::string all = cap.str();
@@ -395,6 +399,43 @@ int ref_output_surface(void *p, const char *dir, char *line, int linelen) {
     strncpy(line, last.c_str(), linelen - 1);
     line[linelen - 1] = 0;
   }
+  return n;
+}
+
+// The reference's Cornelius class on one hypercube: cube[it*8+jx*4+jy*2+jz],
+// dx[4]; writes up to 10 centroids and normals, returns the element count.
+int ref_cornelius4d(const double *cube, const double *dx, double E0, double *cent,
+                    double *norm) {
+  static Cornelius *cor = nullptr;
+  if (!cor) cor = new Cornelius;
+  double arrayDx[4] = {dx[0], dx[1], dx[2], dx[3]};
+  cor->init(4, E0, arrayDx);
+  double ****c = new double ***[2];
+  for (int i = 0; i < 2; i++) {
+    c[i] = new double **[2];
+    for (int j = 0; j < 2; j++) {
+      c[i][j] = new double *[2];
+      for (int k = 0; k < 2; k++) {
+        c[i][j][k] = new double[2];
+        for (int l = 0; l < 2; l++) c[i][j][k][l] = cube[i * 8 + j * 4 + k * 2 + l];
+      }
+    }
+  }
+  cor->find_surface_4d(c);
+  const int n = cor->get_Nelements();
+  for (int e = 0; e < n; e++)
+    for (int d = 0; d < 4; d++) {
+      cent[e * 4 + d] = cor->get_centroid_elem(e, d);
+      norm[e * 4 + d] = cor->get_normal_elem(e, d);
+    }
+  for (int i = 0; i < 2; i++) {
+    for (int j = 0; j < 2; j++) {
+      for (int k = 0; k < 2; k++) delete[] c[i][j][k];
+      delete[] c[i][j];
+    }
+    delete[] c[i];
+  }
+  delete[] c;
   return n;
 }
 

@@ -1534,3 +1534,602 @@ int or_substeps(double dtau, double tau, double etamin, double etamax, int nz) {
   }
   return n;
 }
+
+/* ===================================================================
+ * Freeze-out hypersurface: Cornelius 4D (P. Huovinen and H. Petersen,
+ * Eur. Phys. J. A 48 (2012) 171, arXiv:1206.3371) as the reference's
+ * cornelius.cpp implements it, restated over flat arrays.
+ *
+ * Hypercube corner values cube[it*8 + jx*4 + jy*2 + jz] (dimension 0 is
+ * time).  The 4-cube splits into 8 3-cubes (constant dimension i at j = 0, 1,
+ * Hypercube::split_to_cubes, cornelius.cpp:1733-1774), each 3-cube into 6
+ * squares (Cube::split_to_squares, :1436-1482).  A square yields 0-2 line
+ * elements (Square::construct_lines / ends_of_edge / find_outside,
+ * :1083-1313), a 3-cube joins its lines into polygons (:1484-1578), the
+ * 4-cube joins polygons into polyhedra (:1776-1878); each polyhedron is one
+ * surface element whose centroid and normal come from its tetrahedra
+ * (:761-1000).
+ * =================================================================== */
+#define CN_MAX_LINES 96
+#define CN_MAX_POLY 32
+#define CN_MAX_ELEM 10
+#define CN_EPS 1e-10
+
+typedef struct cn_line {
+  double p[2][4]; /* the two end points */
+  double o[4];    /* a point outside the surface */
+  int start;      /* index of the start point in p (flip_start_end swaps) */
+} cn_line;
+
+typedef struct cn_poly {
+  int n, cdim;
+  int li[12];
+  double cen[4];
+} cn_poly;
+
+typedef struct cn_work {
+  cn_line L[CN_MAX_LINES];
+  int nl;
+  cn_poly P[CN_MAX_POLY];
+  int np;
+  int err;
+} cn_work;
+
+static const double *ln_start(const cn_line *l) { return l->p[l->start]; }
+static const double *ln_end(const cn_line *l) { return l->p[1 - l->start]; }
+
+static double hv(const double *cube, const int b[4]) {
+  return cube[b[0] * 8 + b[1] * 4 + b[2] * 2 + b[3]];
+}
+
+/* Square::construct_lines (cornelius.cpp:1083-1133) for the square whose
+ * constant dimensions are c0, c1 (values v0, v1) and whose corner values
+ * are p[a][b] (a along x1, b along x2, x1 < x2).  Appends its lines to w
+ * and returns 1 when the square is ambiguous (4 cuts). */
+static int cn_square(cn_work *w, const double p[2][2], int c0, int c1, double v0,
+                     double v1, int x1, int x2, const double *dx, double E0) {
+  int above = 0;
+  for (int i = 0; i < 2; i++)
+    for (int j = 0; j < 2; j++)
+      if (p[i][j] >= E0) above++;
+  if (above == 0 || above == 4) return 0;
+  double cuts[4][2], out[2][2];
+  int nc = 0, amb = 0;
+  /* ends_of_edge, :1147-1221 */
+  if ((p[0][0] - E0) * (p[1][0] - E0) < 0) {
+    cuts[nc][0] = (p[0][0] - E0) / (p[0][0] - p[1][0]) * dx[x1];
+    cuts[nc++][1] = 0;
+  } else if (p[0][0] == E0 && p[1][0] < E0) {
+    cuts[nc][0] = 1e-9 * dx[x1];
+    cuts[nc++][1] = 0;
+  } else if (p[1][0] == E0 && p[0][0] < E0) {
+    cuts[nc][0] = (1.0 - 1e-9) * dx[x1];
+    cuts[nc++][1] = 0;
+  }
+  if ((p[0][0] - E0) * (p[0][1] - E0) < 0) {
+    cuts[nc][0] = 0;
+    cuts[nc++][1] = (p[0][0] - E0) / (p[0][0] - p[0][1]) * dx[x2];
+  } else if (p[0][0] == E0 && p[0][1] < E0) {
+    cuts[nc][0] = 0;
+    cuts[nc++][1] = 1e-9 * dx[x2];
+  } else if (p[0][1] == E0 && p[0][0] < E0) {
+    cuts[nc][0] = 0;
+    cuts[nc++][1] = (1.0 - 1e-9) * dx[x2];
+  }
+  if ((p[1][0] - E0) * (p[1][1] - E0) < 0) {
+    cuts[nc][0] = dx[x1];
+    cuts[nc++][1] = (p[1][0] - E0) / (p[1][0] - p[1][1]) * dx[x2];
+  } else if (p[1][0] == E0 && p[1][1] < E0) {
+    cuts[nc][0] = dx[x1];
+    cuts[nc++][1] = 1e-9 * dx[x2];
+  } else if (p[1][1] == E0 && p[1][0] < E0) {
+    cuts[nc][0] = dx[x1];
+    cuts[nc++][1] = (1.0 - 1e-9) * dx[x2];
+  }
+  if ((p[0][1] - E0) * (p[1][1] - E0) < 0) {
+    cuts[nc][0] = (p[0][1] - E0) / (p[0][1] - p[1][1]) * dx[x1];
+    cuts[nc++][1] = dx[x2];
+  } else if (p[0][1] == E0 && p[1][1] < E0) {
+    cuts[nc][0] = 1e-9 * dx[x1];
+    cuts[nc++][1] = dx[x2];
+  } else if (p[1][1] == E0 && p[0][1] < E0) {
+    cuts[nc][0] = (1.0 - 1e-9) * dx[x1];
+    cuts[nc++][1] = dx[x2];
+  }
+  if (nc != 0 && nc != 2 && nc != 4) { /* the reference exits */
+    w->err |= 1;
+    return 0;
+  }
+  if (nc == 0) return 0;
+  /* find_outside, :1223-1298 */
+  if (nc == 4) {
+    amb = 1;
+    double Emid = 0;
+    for (int i = 0; i < 2; i++)
+      for (int j = 0; j < 2; j++) Emid += 0.25 * p[i][j];
+    if ((p[0][0] < E0 && Emid < E0) || (p[0][0] > E0 && Emid > E0)) {
+      for (int i = 0; i < 2; i++) {
+        const double t = cuts[1][i];
+        cuts[1][i] = cuts[2][i];
+        cuts[2][i] = t;
+      }
+    }
+    if ((Emid - E0) < 0) {
+      out[0][0] = out[1][0] = 0.5 * dx[x1];
+      out[0][1] = out[1][1] = 0.5 * dx[x2];
+    } else if ((p[0][0] - E0) < 0) {
+      out[0][0] = 0;
+      out[0][1] = 0;
+      out[1][0] = dx[x1];
+      out[1][1] = dx[x2];
+    } else {
+      out[0][0] = dx[x1];
+      out[0][1] = 0;
+      out[1][0] = 0;
+      out[1][1] = dx[x2];
+    }
+  } else {
+    for (int i = 0; i < 2; i++)
+      for (int j = 0; j < 2; j++) out[i][j] = 0;
+    int nout = 0;
+    for (int i = 0; i < 2; i++)
+      for (int j = 0; j < 2; j++)
+        if (p[i][j] < E0) {
+          out[0][0] += i * dx[x1];
+          out[0][1] += j * dx[x2];
+          nout++;
+        }
+    if (nout > 0)
+      for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) out[i][j] = out[i][j] / (double)nout;
+  }
+  for (int k = 0; k < nc / 2; k++) {
+    if (w->nl >= CN_MAX_LINES) {
+      w->err |= 2;
+      return amb;
+    }
+    cn_line *l = &w->L[w->nl++];
+    for (int e = 0; e < 2; e++) {
+      l->p[e][x1] = cuts[2 * k + e][0];
+      l->p[e][x2] = cuts[2 * k + e][1];
+      l->p[e][c0] = v0;
+      l->p[e][c1] = v1;
+    }
+    l->o[x1] = out[k][0];
+    l->o[x2] = out[k][1];
+    l->o[c0] = v0;
+    l->o[c1] = v1;
+    l->start = 0;
+  }
+  return amb;
+}
+
+/* Polygon::add_line (cornelius.cpp:404-438) */
+static int cn_add_line(cn_work *w, cn_poly *pg, int li, int donotcheck) {
+  if (donotcheck || pg->n == 0) {
+    pg->li[pg->n++] = li;
+    return 1;
+  }
+  cn_line *l = &w->L[li];
+  const double *p1 = ln_start(l), *p2 = ln_end(l), *p3 = ln_end(&w->L[pg->li[pg->n - 1]]);
+  double d1 = 0, d2 = 0;
+  for (int j = 0; j < 4; j++) {
+    d1 += fabs(p1[j] - p3[j]);
+    d2 += fabs(p2[j] - p3[j]);
+  }
+  if (d1 < CN_EPS || d2 < CN_EPS) {
+    if (d2 < CN_EPS) l->start = 1 - l->start;
+    pg->li[pg->n++] = li;
+    return 1;
+  }
+  return 0;
+}
+
+/* Cube::construct_polygons (cornelius.cpp:1484-1578) for the 3-cube with
+ * constant dimension ci at corner bit jc.  Returns its line count. */
+static int cn_cube(cn_work *w, const double *cube, int ci, int jc, const double *dx,
+                   double E0, int *cube_amb) {
+  const int l0 = w->nl;
+  const double cv = jc * dx[ci];
+  int namb = 0;
+  for (int i = 0; i < 4; i++) {
+    if (i == ci) continue;
+    int x1 = -1, x2 = -1;
+    for (int d = 0; d < 4; d++)
+      if (d != ci && d != i) {
+        if (x1 < 0)
+          x1 = d;
+        else
+          x2 = d;
+      }
+    for (int j = 0; j < 2; j++) {
+      double sq[2][2];
+      for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) {
+          int bits[4];
+          bits[ci] = jc;
+          bits[i] = j;
+          bits[x1] = a;
+          bits[x2] = b;
+          sq[a][b] = hv(cube, bits);
+        }
+      namb += cn_square(w, sq, ci, i, cv, j * dx[i], x1, x2, dx, E0);
+    }
+  }
+  const int nl = w->nl - l0;
+  *cube_amb = 0;
+  if (nl == 0) return 0;
+  /* Cube::check_ambiguous, :1580-1595 */
+  int amb = namb;
+  if (amb == 0 && nl == 6) amb = 1;
+  *cube_amb = amb;
+  if (amb > 0) {
+    int not_used[CN_MAX_LINES];
+    for (int i = 0; i < nl; i++) not_used[i] = 1;
+    int used = 0;
+    do {
+      if (nl - used < 3 || w->np >= CN_MAX_POLY) { /* the reference exits */
+        w->err |= 4;
+        return nl;
+      }
+      cn_poly *pg = &w->P[w->np];
+      pg->n = 0;
+      pg->cdim = ci;
+      for (int i = 0; i < nl; i++) {
+        if (not_used[i]) {
+          if (cn_add_line(w, pg, l0 + i, 0)) {
+            not_used[i] = 0;
+            used++;
+            i = 0;
+          }
+        }
+      }
+      w->np++;
+    } while (used < nl);
+  } else {
+    if (w->np >= CN_MAX_POLY) {
+      w->err |= 4;
+      return nl;
+    }
+    cn_poly *pg = &w->P[w->np];
+    pg->n = 0;
+    pg->cdim = ci;
+    for (int i = 0; i < nl; i++) cn_add_line(w, pg, l0 + i, 1);
+    w->np++;
+  }
+  return nl;
+}
+
+/* Polygon::calculate_centroid (cornelius.cpp:440-516) */
+static void cn_poly_centroid(const cn_work *w, cn_poly *pg) {
+  int x[3], k = 0;
+  for (int d = 0; d < 4; d++)
+    if (d != pg->cdim) x[k++] = d;
+  const int x1 = x[0], x2 = x[1], x3 = x[2];
+  double mean[4] = {0, 0, 0, 0};
+  for (int i = 0; i < pg->n; i++) {
+    const cn_line *l = &w->L[pg->li[i]];
+    const double *p1 = ln_start(l), *p2 = ln_end(l);
+    for (int j = 0; j < 4; j++) mean[j] += p1[j] + p2[j];
+  }
+  for (int j = 0; j < 4; j++) mean[j] = mean[j] / (double)(2.0 * pg->n);
+  if (pg->n == 3) {
+    for (int j = 0; j < 4; j++) pg->cen[j] = mean[j];
+    return;
+  }
+  double up[4] = {0, 0, 0, 0}, down = 0, a[4], b[4], cm[4];
+  for (int i = 0; i < pg->n; i++) {
+    const cn_line *l = &w->L[pg->li[i]];
+    const double *p1 = ln_start(l), *p2 = ln_end(l);
+    for (int j = 0; j < 4; j++) cm[j] = (p1[j] + p2[j] + mean[j]) / 3.0;
+    for (int j = 0; j < 4; j++) {
+      a[j] = p1[j] - mean[j];
+      b[j] = p2[j] - mean[j];
+    }
+    const double c1 = a[x2] * b[x3] - a[x3] * b[x2];
+    const double c2 = a[x1] * b[x3] - a[x3] * b[x1];
+    const double c3 = a[x2] * b[x1] - a[x1] * b[x2];
+    const double A = 0.5 * sqrt(c1 * c1 + c2 * c2 + c3 * c3);
+    for (int j = 0; j < 4; j++) up[j] += cm[j] * A;
+    down += A;
+  }
+  for (int j = 0; j < 4; j++) pg->cen[j] = up[j] / down;
+}
+
+/* Polyhedron::tetravolume (cornelius.cpp:771-788) */
+static void cn_tetra(const double *a, const double *b, const double *c, double *n) {
+  const double bc01 = b[0] * c[1] - b[1] * c[0];
+  const double bc02 = b[0] * c[2] - b[2] * c[0];
+  const double bc03 = b[0] * c[3] - b[3] * c[0];
+  const double bc12 = b[1] * c[2] - b[2] * c[1];
+  const double bc13 = b[1] * c[3] - b[3] * c[1];
+  const double bc23 = b[2] * c[3] - b[3] * c[2];
+  n[0] = 1.0 / 6.0 * (a[1] * bc23 - a[2] * bc13 + a[3] * bc12);
+  n[1] = -1.0 / 6.0 * (a[0] * bc23 - a[2] * bc03 + a[3] * bc02);
+  n[2] = 1.0 / 6.0 * (a[0] * bc13 - a[1] * bc03 + a[3] * bc01);
+  n[3] = -1.0 / 6.0 * (a[0] * bc12 - a[1] * bc02 + a[2] * bc01);
+}
+
+/* Polyhedron::lines_equal (cornelius.cpp:749-765) */
+static int cn_lines_equal(const cn_line *l1, const cn_line *l2) {
+  const double *p11 = ln_start(l1), *p12 = ln_end(l1), *p21 = ln_start(l2);
+  double d1 = 0, d2 = 0;
+  for (int i = 0; i < 4; i++) {
+    d1 += fabs(p11[i] - p21[i]);
+    d2 += fabs(p12[i] - p21[i]);
+    if (d1 > CN_EPS && d2 > CN_EPS) return 0;
+  }
+  return 1;
+}
+
+/* Cornelius::find_surface_4d (cornelius.cpp:2247-2285) with Hypercube
+ * construct_polyhedrons / check_ambiguous (:1776-1878): returns the number
+ * of elements (centroid, normal relative to the cube's low corner), or -1
+ * when the reference would have stopped (exit or overflow). */
+int or_cornelius4d(const double cube[16], const double dx[4], double E0, double cent[][4],
+                   double norm[][4]) {
+  int above = 0;
+  for (int k = 0; k < 16; k++)
+    if (cube[k] >= E0) above++;
+  if (above == 0 || above == 16) return 0;
+  static cn_work w; /* single-threaded oracle */
+  w.nl = w.np = w.err = 0;
+  int namb = 0, nlines = 0;
+  for (int i = 0; i < 4; i++)
+    for (int j = 0; j < 2; j++) {
+      int ca;
+      nlines += cn_cube(&w, cube, i, j, dx, E0, &ca);
+      if (ca) namb++;
+    }
+  if (w.err) return -1;
+  int amb = namb;
+  if (amb == 0) {
+    int pts = 0;
+    for (int k = 0; k < 16; k++)
+      if (cube[k] < E0) pts++;
+    if (pts > 8) pts = 16 - pts;
+    if (nlines == 24 && pts == 2) amb++;
+  }
+  int ph[CN_MAX_ELEM][CN_MAX_POLY], nph[CN_MAX_ELEM], nel = 0;
+  if (amb > 0) {
+    int not_used[CN_MAX_POLY], used = 0;
+    for (int i = 0; i < w.np; i++) not_used[i] = 1;
+    do {
+      if (nel >= CN_MAX_ELEM) return -1;
+      nph[nel] = 0;
+      for (int i = 0; i < w.np; i++) {
+        if (!not_used[i]) continue;
+        int add = 0;
+        if (nph[nel] == 0) {
+          add = 1;
+        } else {
+          const cn_poly *p = &w.P[i];
+          for (int q = 0; q < nph[nel] && !add; q++) {
+            const cn_poly *pq = &w.P[ph[nel][q]];
+            for (int j = 0; j < p->n && !add; j++)
+              for (int k = 0; k < pq->n && !add; k++)
+                if (cn_lines_equal(&w.L[p->li[j]], &w.L[pq->li[k]])) add = 1;
+          }
+        }
+        if (add) {
+          ph[nel][nph[nel]++] = i;
+          not_used[i] = 0;
+          used++;
+          i = 0;
+        }
+      }
+      nel++;
+    } while (used < w.np);
+  } else {
+    nph[0] = 0;
+    for (int i = 0; i < w.np; i++) ph[0][nph[0]++] = i;
+    nel = 1;
+  }
+  for (int i = 0; i < w.np; i++) cn_poly_centroid(&w, &w.P[i]);
+  for (int e = 0; e < nel; e++) {
+    /* Polyhedron::calculate_centroid, :790-870 */
+    int ntet = 0;
+    double mean[4] = {0, 0, 0, 0};
+    for (int q = 0; q < nph[e]; q++) {
+      const cn_poly *pg = &w.P[ph[e][q]];
+      ntet += pg->n;
+      for (int j = 0; j < pg->n; j++) {
+        const cn_line *l = &w.L[pg->li[j]];
+        const double *p1 = ln_start(l), *p2 = ln_end(l);
+        for (int k = 0; k < 4; k++) mean[k] += p1[k] + p2[k];
+      }
+    }
+    for (int k = 0; k < 4; k++) mean[k] = mean[k] / (double)(2.0 * ntet);
+    double up[4] = {0, 0, 0, 0}, down = 0, a[4], b[4], c[4], n[4], cm[4];
+    for (int q = 0; q < nph[e]; q++) {
+      const cn_poly *pg = &w.P[ph[e][q]];
+      for (int j = 0; j < pg->n; j++) {
+        const cn_line *l = &w.L[pg->li[j]];
+        const double *p1 = ln_start(l), *p2 = ln_end(l);
+        for (int k = 0; k < 4; k++) cm[k] = (p1[k] + p2[k] + pg->cen[k] + mean[k]) / 4.0;
+        for (int k = 0; k < 4; k++) {
+          a[k] = p1[k] - mean[k];
+          b[k] = p2[k] - mean[k];
+          c[k] = pg->cen[k] - mean[k];
+        }
+        cn_tetra(a, b, c, n);
+        double V = 0;
+        for (int k = 0; k < 4; k++) V += n[k] * n[k];
+        V = sqrt(V);
+        for (int k = 0; k < 4; k++) up[k] += cm[k] * V;
+        down += V;
+      }
+    }
+    double *C = cent[e];
+    for (int k = 0; k < 4; k++) C[k] = up[k] / down;
+    /* Polyhedron::calculate_normal, :872-935 */
+    double *Nn = norm[e];
+    for (int k = 0; k < 4; k++) Nn[k] = 0;
+    for (int q = 0; q < nph[e]; q++) {
+      const cn_poly *pg = &w.P[ph[e][q]];
+      for (int j = 0; j < pg->n; j++) {
+        const cn_line *l = &w.L[pg->li[j]];
+        const double *p1 = ln_start(l), *p2 = ln_end(l);
+        for (int k = 0; k < 4; k++) {
+          a[k] = p1[k] - C[k];
+          b[k] = p2[k] - C[k];
+          c[k] = pg->cen[k] - C[k];
+        }
+        cn_tetra(a, b, c, n);
+        double dot = 0;
+        for (int k = 0; k < 4; k++) dot += (l->o[k] - C[k]) * n[k];
+        if (dot < 0)
+          for (int k = 0; k < 4; k++) n[k] = -n[k];
+        for (int k = 0; k < 4; k++) Nn[k] += n[k];
+      }
+    }
+  }
+  return nel;
+}
+
+/* transformToLab, src/fld.cpp:508-513 */
+static void to_lab(double eta, double *vx, double *vy, double *vz) {
+  const double Y = eta + 1. / 2. * log((1. + *vz) / (1. - *vz));
+  *vx = *vx * cosh(Y - eta) / cosh(Y);
+  *vy = *vy * cosh(Y - eta) / cosh(Y);
+  *vz = tanh(Y);
+}
+
+/* The freeze-out part of Fluid::outputSurface (src/fld.cpp:544-842): for
+ * every interior cube [ix, ix+1] x [iy, iy+1] x [iz, iz+1] x [tau - dt,
+ * tau] (ix, iy, iz in [2, n-2), iz fastest) the energy densities at the
+ * 16 corners (getPrimVar of Q at tau, getPrimVarPrev of Qprev at tau - dt,
+ * dt = the Fluid's construction-time step) go to Cornelius; each element
+ * gets the interpolated state and one record of OR_SURF_REC doubles:
+ * position (4), dSigma_mu (4, from the normal of the cube's FIRST element
+ * for every element, as the reference does), u^mu (4), T, muB, muQ, muS,
+ * pi^{mu nu} in Cartesian components (10, index44 order), Pi, e, nb.
+ * acc[OR_SURF_ACC] += nsusp, EtotSurf, nbSurf, vEff increments and the
+ * count of elements with T > 0.4 or |muB| > 0.85.  Returns the number of
+ * elements (records beyond cap are counted but not written), or -1 when
+ * Cornelius would have stopped the reference. */
+long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau,
+                double dtf, double ecrit, double *rec, long cap, double *acc) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const long N = (long)nx * ny * nz;
+  const double dx = (g->xmax - g->xmin) / (nx - 1);
+  const double dy = (g->ymax - g->ymin) / (ny - 1);
+  const double dz = (g->zmax - g->zmin) / (nz - 1);
+  const double arrayDx[4] = {dtf, dx, dy, dz};
+  long nel = 0;
+  for (int ix = 2; ix < nx - 2; ix++)
+    for (int iy = 2; iy < ny - 2; iy++)
+      for (int iz = 2; iz < nz - 2; iz++) {
+        double cube[16], QCube[2][8][7], piS[8][10], PiS[8];
+        for (int jx = 0; jx < 2; jx++)
+          for (int jy = 0; jy < 2; jy++)
+            for (int jz = 0; jz < 2; jz++) {
+              const int c = jx * 4 + jy * 2 + jz;
+              const long i = (ix + jx) + (long)nx * (iy + jy) + (long)nx * ny * (iz + jz);
+              double q[7], e, p, nb, nq, ns, vx, vy, vz;
+              for (int k = 0; k < 7; k++) q[k] = s->Q[(long)k * N + i] / tau;
+              transform_pv(E, q, &e, &p, &nb, &nq, &ns, &vx, &vy, &vz);
+              cube[8 + c] = e;
+              for (int k = 0; k < 7; k++) q[k] = s->Qprev[(long)k * N + i] / (tau - dtf);
+              transform_pv(E, q, &e, &p, &nb, &nq, &ns, &vx, &vy, &vz);
+              cube[c] = e;
+              for (int k = 0; k < 7; k++) {
+                QCube[1][c][k] = s->Q[(long)k * N + i];
+                QCube[0][c][k] = s->Qprev[(long)k * N + i];
+              }
+              for (int k = 0; k < 10; k++) piS[c][k] = s->pi[(long)k * N + i];
+              PiS[c] = s->Pi[i];
+            }
+        double cen[CN_MAX_ELEM][4], nrm[CN_MAX_ELEM][4];
+        const int ne = or_cornelius4d(cube, arrayDx, ecrit, cen, nrm);
+        if (ne < 0) return -1;
+        for (int el = 0; el < ne; el++) {
+          const double *C = cen[el];
+          double QC[7] = {0., 0., 0., 0., 0., 0., 0.}, piC[10], PiC = 0.;
+          for (int k = 0; k < 10; k++) piC[k] = 0.;
+          const double wT[2] = {1. - C[0] / dtf, C[0] / dtf};
+          const double wX[2] = {1. - C[1] / dx, C[1] / dx};
+          const double wY[2] = {1. - C[2] / dy, C[2] / dy};
+          const double wZ[2] = {1. - C[3] / dz, C[3] / dz};
+          for (int jt = 0; jt < 2; jt++)
+            for (int jx = 0; jx < 2; jx++)
+              for (int jy = 0; jy < 2; jy++)
+                for (int jz = 0; jz < 2; jz++)
+                  for (int k = 0; k < 7; k++)
+                    QC[k] += QCube[jt][jx * 4 + jy * 2 + jz][k] * wT[jt] * wX[jx] * wY[jy] * wZ[jz];
+          for (int k = 0; k < 7; k++) QC[k] = QC[k] / (tau + C[0]);
+          double eC, pC, nbC, nqC, nsC = 0.0, vxC, vyC, vzC, TC, mubC;
+          transform_pv(E, QC, &eC, &pC, &nbC, &nqC, &nsC, &vxC, &vyC, &vzC);
+          eos_eval(E, eC, nbC, &TC, &mubC, &pC);
+          const double muqC = 0., musC = 0.;
+          if (TC > 0.4 || fabs(mubC) > 0.85) acc[4] += 1.;
+          if (eC > ecrit * 2.0 || eC < ecrit * 0.5) acc[0] += 1.;
+          for (int jx = 0; jx < 2; jx++)
+            for (int jy = 0; jy < 2; jy++)
+              for (int jz = 0; jz < 2; jz++) {
+                const int c = jx * 4 + jy * 2 + jz;
+                for (int k = 0; k < 10; k++) piC[k] += piS[c][k] * wX[jx] * wY[jy] * wZ[jz];
+                PiC += PiS[c] * wX[jx] * wY[jy] * wZ[jz];
+              }
+          double v2C = vxC * vxC + vyC * vyC + vzC * vzC;
+          if (v2C > 1.) {
+            vxC *= sqrt(0.99 / v2C);
+            vyC *= sqrt(0.99 / v2C);
+            vzC *= sqrt(0.99 / v2C);
+            v2C = 0.99;
+          }
+          const double etaC = (g->zmin + iz * dz) + C[3];
+          to_lab(etaC, &vxC, &vyC, &vzC);
+          const double gammaC = 1. / sqrt(1. - vxC * vxC - vyC * vyC - vzC * vzC);
+          const double uC[4] = {gammaC, gammaC * vxC, gammaC * vyC, gammaC * vzC};
+          const double tauC = tau + C[0];
+          const double ch = cosh(etaC), sh = sinh(etaC);
+          const double *n0 = nrm[0];
+          double ds[4];
+          ds[0] = tauC * (ch * n0[0] - sh / tauC * n0[3]);
+          ds[3] = tauC * (-sh * n0[0] + ch / tauC * n0[3]);
+          ds[1] = tauC * n0[1];
+          ds[2] = tauC * n0[2];
+          double dVEff = 0.0;
+          for (int k = 0; k < 4; k++) dVEff += ds[k] * uC[k];
+          double pc[10];
+          pc[0] = ch * ch * piC[0] + 2. * ch * sh * piC[6] + sh * sh * piC[9];
+          pc[1] = ch * piC[1] + sh * piC[7];
+          pc[3] = ch * piC[3] + sh * piC[8];
+          pc[6] = ch * sh * (piC[0] + piC[9]) + (ch * ch + sh * sh) * piC[6];
+          pc[2] = piC[2];
+          pc[4] = piC[4];
+          pc[7] = sh * piC[1] + ch * piC[7];
+          pc[5] = piC[5];
+          pc[8] = sh * piC[3] + ch * piC[8];
+          pc[9] = sh * sh * piC[0] + ch * ch * piC[9] + 2. * sh * ch * piC[6];
+          const int i0k[4] = {0, 1, 3, 6}; /* index44(0, k) */
+          double dEsurfVisc = 0.;
+          for (int k = 0; k < 4; k++) dEsurfVisc += pc[i0k[k]] * ds[k];
+          acc[1] += (eC + pC) * uC[0] * dVEff - pC * ds[0] + dEsurfVisc;
+          acc[2] += nbC * dVEff;
+          acc[3] += dVEff;
+          if (nel < cap) {
+            double *r = rec + nel * OR_SURF_REC;
+            r[0] = tau + C[0];
+            r[1] = (g->xmin + ix * dx) + C[1];
+            r[2] = (g->ymin + iy * dy) + C[2];
+            r[3] = (g->zmin + iz * dz) + C[3];
+            for (int k = 0; k < 4; k++) {
+              r[4 + k] = ds[k];
+              r[8 + k] = uC[k];
+            }
+            r[12] = TC;
+            r[13] = mubC;
+            r[14] = muqC;
+            r[15] = musC;
+            for (int k = 0; k < 10; k++) r[16 + k] = pc[k];
+            r[26] = PiC;
+            r[27] = eC;
+            r[28] = nbC;
+          }
+          nel++;
+        }
+      }
+  return nel;
+}

@@ -101,6 +101,26 @@ int or_substeps(double dtau, double tau, double etamin, double etamax, int nz);
 /* Fluid::updateM (src/fld.cpp:384-423) alone, for unit tests. */
 void or_update_m(const or_grid *g, double *m, double tau, double dt);
 
+/* Cornelius 4D on one hypercube (cornelius.cpp:2247-2285): cube[it*8 +
+ * jx*4 + jy*2 + jz], cell sizes dx[4] = dt, dx, dy, dz, iso-value E0.
+ * Returns the number of elements (<= 10) with centroid and normal
+ * relative to the low corner, or -1 where the reference stops. */
+int or_cornelius4d(const double cube[16], const double dx[4], double E0,
+                   double cent[][4], double norm[][4]);
+
+/* The freeze-out elements of Fluid::outputSurface (src/fld.cpp:544-842)
+ * at tau (the previous layer is Qprev at tau - dtf, dtf = the Fluid's
+ * construction-time step).  Records of OR_SURF_REC doubles: tau, x, y, eta,
+ * dSigma[4], u[4], T, muB, muQ, muS, pi_cart[10] (index44 order), Pi, e, nb.
+ * acc[OR_SURF_ACC] += nsusp, EtotSurf, nbSurf, vEff increments and the
+ * high-T/muB warning count.  Returns the element count (records past cap
+ * are not written) or -1 where the reference stops. */
+#define OR_SURF_REC 29
+#define OR_SURF_ACC 5
+long or_surface(const or_grid *g, const or_eos *eos, const or_state *s,
+                double tau, double dtf, double ecrit, double *rec, long cap,
+                double *acc);
+
 int or_abi_version(void);
 
 #ifdef __cplusplus

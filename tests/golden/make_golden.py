@@ -63,6 +63,84 @@ def save_case(name, setup, nsteps):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
 
 
+SURFACE_CASES = {
+    # name: (setup factory, steps; Fluid::outputSurface after every step)
+    "surface_glauber_21x21x11_b9": (lambda: W.small_glauber3d(21, 11, b=9.0, seed=5), 8),
+}
+
+
+def save_surface_case(name, setup, nsteps):
+    """Per-step freeze-out elements as the reference writes them
+    (freezeout.dat, extended records with e and nb) and the printed lines."""
+    r = P.RefRun(setup)
+    counts, lines = [], []
+    with tempfile.TemporaryDirectory() as d:
+        for _ in range(nsteps):
+            r.step(1)
+            n, line = r.output_surface(d, extend=True)
+            counts.append(n)
+            lines.append(line)
+        r.close()
+        rec = P.read_freezeout(os.path.join(d, "freezeout.dat.unfinished"), extend=True)
+    g = setup.grid
+    eos = setup.eos
+    arrays = dict(
+        grid_n=np.array([g.nx, g.ny, g.nz]), grid_b=np.array(g.bounds()),
+        eos_kind=np.array(eos.kind), eos_cnst=np.array(eos.conf_cnst),
+        tr=np.array(setup.tr_vector()), tr_params=np.array([setup.etaSparam, setup.zetaSparam]),
+        clock=np.array([setup.tau0, setup.dt, setup.ecrit]), nsteps=np.array(nsteps),
+        Q0=setup.Q, m0=setup.m, tau_end=np.array(0.0),
+        surf_counts=np.array(counts), surf_rec=rec, surf_lines=np.array(lines),
+    )
+    if eos.kind == 1:
+        arrays.update(eos_egrid=eos.egrid, eos_ngrid=eos.ngrid, eos_p=eos.p, eos_T=eos.T,
+                      eos_mub=eos.mub)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+
+
+def cornelius_cubes():
+    """Hypercubes (random, near-binary and exact hits of the iso-value) with
+    the reference Cornelius' elements."""
+    rng = np.random.default_rng(2024)
+    dx = np.array([0.05, 0.3, 0.3, 0.25])
+    cubes, counts, cent, norm = [], [], [], []
+    while len(cubes) < 1200:
+        mode = len(cubes) % 4
+        if mode == 0:
+            c = rng.uniform(0, 1, 16)
+        elif mode == 1:
+            c = rng.choice([0.2, 0.8], 16) + rng.uniform(-0.01, 0.01, 16)
+        elif mode == 2:
+            c = rng.choice([0.2, 0.5, 0.8], 16)
+        else:
+            c = 0.5 + rng.normal(0, 0.3, 16) * (rng.uniform(0, 1, 16) < 0.5)
+        co, _ = P.cornelius4d(c, dx, 0.5)  # the oracle first: skips cubes the reference exits on
+        if co is None:
+            continue
+        cr, nr = P.cornelius4d(c, dx, 0.5, reference=True)
+        cubes.append(c)
+        counts.append(len(cr))
+        cent.append(cr)
+        norm.append(nr)
+    np.savez_compressed(os.path.join(HERE, "cornelius_cubes.npz"), dx=dx, e0=np.array(0.5),
+                        cubes=np.array(cubes), counts=np.array(counts),
+                        cent=np.concatenate(cent), norm=np.concatenate(norm))
+
+
+def load_surface_case(path):
+    """(Setup, steps, per-step element counts, records [n][29], lines)."""
+    z = np.load(path)
+    nx, ny, nz = (int(v) for v in z["grid_n"])
+    g = W.Grid(nx, ny, nz, *(float(v) for v in z["grid_b"]))
+    eos = W.EosTable(kind=1, egrid=z["eos_egrid"], ngrid=z["eos_ngrid"], p=z["eos_p"],
+                     T=z["eos_T"], mub=z["eos_mub"])
+    tr = dict(zip(W.TR_FIELDS, (float(v) for v in z["tr"])))
+    tau0, dt, ecrit = (float(v) for v in z["clock"])
+    setup = W.Setup(os.path.basename(path), g, eos, tr, int(z["tr_params"][0]),
+                    int(z["tr_params"][1]), tau0, dt, ecrit, z["Q0"], z["m0"])
+    return setup, int(z["nsteps"]), z["surf_counts"], z["surf_rec"], [str(v) for v in z["surf_lines"]]
+
+
 def known_answers():
     """transformPV / EoS known answers over regimes the step meets: empty
     (Q_t <= 0), at rest (M = 0), superluminal (M > Q_t), dilute, dense."""
@@ -127,5 +205,10 @@ if __name__ == "__main__":
     for name, (fac, n) in CASES.items():
         save_case(name, fac(), n)
         print("wrote", name)
+    for name, (fac, n) in SURFACE_CASES.items():
+        save_surface_case(name, fac(), n)
+        print("wrote", name)
+    cornelius_cubes()
+    print("wrote cornelius_cubes")
     known_answers()
     print("wrote known_answers")
