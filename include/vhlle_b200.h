@@ -45,6 +45,8 @@ typedef int vh_status;
 #define VH_NUM_FLUX_NAN 2u     /* NaN HLLE flux, src/hdo.cpp:285-298        */
 #define VH_NUM_SOURCE_NAN 4u   /* NaN source, src/hdo.cpp:345-351           */
 #define VH_NUM_NSQUANT_NAN 8u  /* inf/NaN shear, src/hdo.cpp:643-651        */
+#define VH_NUM_SURFACE 16u     /* a hypercube on which Cornelius stops the
+                                  reference (src/cornelius.cpp:1217,1534) */
 
 typedef struct vh_ctx vh_ctx;
 
@@ -163,6 +165,54 @@ vh_status vh_launches_per_step(vh_ctx *ctx, int *n);
  * count.  Waits for the result. */
 #define VH_TOTALS_N 16
 vh_status vh_totals(vh_ctx *ctx, double ecrit, double *out);
+
+/* The freeze-out hypersurface of Fluid::outputSurface (src/fld.cpp:606-842)
+ * at the current tau: every interior cube [ix,ix+1]x[iy,iy+1]x[iz,iz+1]
+ * (indices in [2, n-2)) spanning [tau - dt_fluid, tau], with the energy
+ * densities of Q at tau and Qprev at tau - dt_fluid at its 16 corners, goes
+ * through Cornelius 4D at e_crit; each element gets the 4-linearly
+ * interpolated state (con2prim, EoS), its dSigma_mu (built, as in the
+ * reference, from the normal of its cube's first element), u^mu, pi^{mu nu}
+ * in Cartesian components and Pi.  dt_fluid is the step the grid was
+ * created with (doubled by vh_resize2x), not the substep.  Elements are
+ * kept on the device in the reference's loop order (ix, iy, iz with iz
+ * fastest, then element index) until the next call.  Waits for the result;
+ * VH_ERR_NUMERIC if a hypercube would stop the reference (VH_NUM_SURFACE). */
+typedef struct vh_surface_info {
+  long nelements; /* elements of this call */
+  long nsusp;     /* elements with e > 2 e_crit or e < e_crit / 2 */
+  long high_T;    /* elements with T > 0.4 or |muB| > 0.85 (the reference
+                     prints a warning for each) */
+  double EtotSurf; /* energy through the surface, summed over the calls on
+                      this grid (a Fluid member: a resize restarts it) */
+  double nbSurf;   /* baryon number through the surface, summed over all
+                      calls of the context (a function static there) */
+  double vEff;     /* effective volume, summed like EtotSurf */
+} vh_surface_info;
+vh_status vh_surface(vh_ctx *ctx, double ecrit, vh_surface_info *info);
+
+/* Element records of the last vh_surface call, VH_SURF_REC doubles each:
+ * tau, x, y, eta, dSigma_0..3, u^0..3, T, muB, muQ, muS, pi^{mu nu}
+ * (10, index44 order: 00 01 11 02 12 22 03 13 23 33), Pi, e, nb.
+ * vh_surface_records copies min(n, max) of them to host memory and sets
+ * *n (may be NULL) to n; vh_surface_device gives the device array (valid
+ * until the next vh_surface or vh_destroy). */
+#define VH_SURF_REC 29
+vh_status vh_surface_records(vh_ctx *ctx, double *out, long max, long *n);
+vh_status vh_surface_device(vh_ctx *ctx, const double **rec, long *n);
+/* Appends the last call's elements to a text file as freezeout.dat lines
+ * (src/fld.cpp:658-797: 15 significant digits, width 24; e and nb only
+ * when extendFO). */
+vh_status vh_surface_write(vh_ctx *ctx, const char *path, int extendFO);
+
+/* Cornelius::find_surface_4d (src/cornelius.cpp:2247-2285) on n independent
+ * hypercubes, on the device: cubes[k][16] corner values (index it*8 + jx*4 +
+ * jy*2 + jz, dimension 0 is time), cell sizes dx[4], iso-value e0.
+ * counts[k] = element count (-1 where the reference stops), cent and norm
+ * [k][10][4] the elements' centroids and normals.  Synchronous; for tests
+ * and for callers with their own cubes. */
+vh_status vh_cornelius4d(const double *cubes, long n, const double *dx, double e0,
+                         int device, int *counts, double *cent, double *norm);
 
 /* Device timing with CUDA events recorded on the context's stream.
  * vh_timer_stop waits for the stop event and returns the elapsed time. */

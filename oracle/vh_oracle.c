@@ -1551,7 +1551,8 @@ int or_substeps(double dtau, double tau, double etamin, double etamax, int nz) {
  * (:761-1000).
  * =================================================================== */
 #define CN_MAX_LINES 96
-#define CN_MAX_POLY 32
+#define CN_MAX_POLY 64
+#define CN_MAX_POLY_PER_CUBE 8
 #define CN_MAX_ELEM 10
 #define CN_EPS 1e-10
 
@@ -1729,7 +1730,7 @@ static int cn_add_line(cn_work *w, cn_poly *pg, int li, int donotcheck) {
  * constant dimension ci at corner bit jc.  Returns its line count. */
 static int cn_cube(cn_work *w, const double *cube, int ci, int jc, const double *dx,
                    double E0, int *cube_amb) {
-  const int l0 = w->nl;
+  const int l0 = w->nl, p0 = w->np;
   const double cv = jc * dx[ci];
   int namb = 0;
   for (int i = 0; i < 4; i++) {
@@ -1768,7 +1769,8 @@ static int cn_cube(cn_work *w, const double *cube, int ci, int jc, const double 
     for (int i = 0; i < nl; i++) not_used[i] = 1;
     int used = 0;
     do {
-      if (nl - used < 3 || w->np >= CN_MAX_POLY) { /* the reference exits */
+      /* the reference exits (too few lines) or overflows its polygon array */
+      if (nl - used < 3 || w->np >= CN_MAX_POLY || w->np - p0 >= CN_MAX_POLY_PER_CUBE) {
         w->err |= 4;
         return nl;
       }

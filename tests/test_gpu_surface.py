@@ -1,0 +1,139 @@
+"""The device freeze-out surface (Cornelius 4D per hypercube and the element
+records of Fluid::outputSurface, src/fld.cpp:606-842) against the
+reference's own outputs (golden fixtures) and the oracle.
+
+Tolerances: element counts, nsusp and the element order are exact; records
+within 1e-12 relative (the fixtures hold the reference's 15-digit text, and
+the device's cosh/sinh/log/tanh may differ from the host's in the last bit);
+Cornelius centroids and normals on given hypercubes bit-exact; the summed
+EtotSurf / nbSurf / vEff within 1e-10 of the sum of their magnitudes
+(summation order differs)."""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as P
+from make_golden import load_surface_case
+from vhlle_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+REC_RTOL = 1e-12
+
+
+def rec_close(a, b, rtol=REC_RTOL):
+    return np.abs(a - b) <= rtol * np.maximum(np.abs(a), np.abs(b)) + 1e-300
+
+
+def test_gpu_cornelius_equals_reference_cubes():
+    from vhlle_b200.capi import cornelius4d
+    z = np.load(os.path.join(GOLDEN, "cornelius_cubes.npz"))
+    counts, cent, norm = cornelius4d(z["cubes"], z["dx"], float(z["e0"]))
+    assert np.array_equal(counts, z["counts"])
+    k = 0
+    for i, n in enumerate(z["counts"]):
+        assert np.array_equal(cent[i, :n], z["cent"][k:k + n]), i
+        assert np.array_equal(norm[i, :n], z["norm"][k:k + n]), i
+        k += n
+
+
+def test_gpu_cornelius_equals_oracle_random():
+    from vhlle_b200.capi import cornelius4d
+    rng = np.random.default_rng(31)
+    cubes = np.concatenate([rng.uniform(0, 1, (3000, 16)),
+                            rng.choice([0.1, 0.9], (3000, 16)) + rng.uniform(-0.02, 0.02, (3000, 16)),
+                            rng.choice([0.2, 0.5, 0.8], (2000, 16))])
+    dx = np.array([0.05, 0.6, 0.6, 0.3])
+    counts, cent, norm = cornelius4d(cubes, dx, 0.5)
+    for i, c in enumerate(cubes):
+        co, no = P.cornelius4d(c, dx, 0.5)
+        if co is None:
+            assert counts[i] == -1
+            continue
+        assert counts[i] == len(co), i
+        assert np.array_equal(cent[i, :len(co)], co) and np.array_equal(norm[i, :len(co)], no), i
+
+
+def test_gpu_surface_equals_reference_fixture():
+    from vhlle_b200.capi import GpuHydro
+    setup, nsteps, counts, rec, lines = load_surface_case(
+        os.path.join(GOLDEN, "surface_glauber_21x21x11_b9.npz"))
+    d = GpuHydro(setup)
+    got = []
+    for s in range(nsteps):
+        d.step(1)
+        r, info = d.surface()
+        assert info["nelements"] == counts[s], s
+        words = lines[s].split()
+        assert int(words[7]) == info["nsusp"], s
+        assert abs(info["EtotSurf"] - float(words[5])) <= 5e-6 * abs(info["EtotSurf"]) + 1e-9
+        got.append(r)
+    got = np.concatenate(got)
+    ok = rec_close(got, rec)
+    assert ok.all(), (np.argwhere(~ok)[:5], got[~ok][:5], rec[~ok][:5])
+    d.close()
+
+
+@pytest.mark.parametrize("case", [
+    ("glauber_33x33x17", lambda: W.small_glauber3d(33, 17, seed=11, b=6.0), 6),
+    ("gubser_2d_no_interior", lambda: W.gubser_setup(nx=21, ny=21), 2),
+], ids=lambda c: c[0])
+def test_gpu_surface_equals_oracle(case):
+    from vhlle_b200.capi import GpuHydro
+    name, fac, nsteps = case
+    setup = fac()
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    sums = {"EtotSurf": 0., "nbSurf": 0., "vEff": 0.}
+    mags = {"EtotSurf": 0., "nbSurf": 0., "vEff": 0.}
+    for s in range(nsteps):
+        o.step(1)
+        d.step(1)
+        ro, acc = o.surface()
+        rd, info = d.surface()
+        assert len(ro) == info["nelements"] and int(acc["nsusp"]) == info["nsusp"], s
+        ok = rec_close(rd, ro)
+        assert ok.all(), (s, np.argwhere(~ok)[:5])
+        for k in sums:
+            sums[k] += acc[k]
+            mags[k] += np.abs(acc[k])
+            assert abs(info[k] - sums[k]) <= 1e-10 * (mags[k] + 1e-30) + 1e-300, (k, info[k], sums[k])
+    d.close()
+
+
+def test_gpu_surface_full_size_event():
+    """The 101x101x51 event after 3 steps: every element and the sums as
+    the oracle's."""
+    from vhlle_b200.capi import GpuHydro
+    setup = W.glauber3d_setup()
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    o.step(3)
+    d.step(3)
+    ro, acc = o.surface(cap=2000000)
+    rd, info = d.surface()
+    assert len(ro) == info["nelements"] > 1000
+    ok = rec_close(rd, ro)
+    assert ok.all(), np.argwhere(~ok)[:5]
+    assert int(acc["nsusp"]) == info["nsusp"]
+    assert abs(info["EtotSurf"] - acc["EtotSurf"]) <= 1e-10 * abs(acc["EtotSurf"]) + 1e-6
+    d.close()
+
+
+def test_gpu_surface_writer_matches_reference_text(tmp_path):
+    """vh_surface_write emits the reference's freezeout.dat layout."""
+    from vhlle_b200.capi import GpuHydro
+    setup, nsteps, counts, rec, lines = load_surface_case(
+        os.path.join(GOLDEN, "surface_glauber_21x21x11_b9.npz"))
+    d = GpuHydro(setup)
+    path = str(tmp_path / "freezeout.dat")
+    for _ in range(nsteps):
+        d.step(1)
+        d.surface()
+        d.surface_write(path, extend=True)
+    back = P.read_freezeout(path, extend=True)
+    assert back.shape == rec.shape
+    assert rec_close(back, rec, 1e-13).all()
+    with open(path) as f:
+        first = f.readline()
+    assert len(first.rstrip("\n")) == 24 * 29
+    d.close()

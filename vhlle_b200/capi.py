@@ -28,13 +28,40 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_abi_version", "vh_transform_pv", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
-           "vh_get_grid", "vh_advance", "vh_resize2x")
+           "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_records",
+           "vh_surface_device", "vh_surface_write", "vh_cornelius4d")
 
 
 class VhError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__("vhlle_b200 status %d: %s" % (status, msg))
         self.status = status
+
+
+class VhSurfaceInfo(ctypes.Structure):
+    _fields_ = [("nelements", ctypes.c_long), ("nsusp", ctypes.c_long), ("high_T", ctypes.c_long),
+                ("EtotSurf", ctypes.c_double), ("nbSurf", ctypes.c_double),
+                ("vEff", ctypes.c_double)]
+
+
+SURF_REC = 29
+
+
+def cornelius4d(cubes, dx, e0, device=0):
+    """Device Cornelius on hypercubes [n][16]: (counts[n], cent[n][10][4], norm[n][10][4])."""
+    L = lib()
+    cubes = np.ascontiguousarray(cubes, dtype=np.float64).reshape(-1, 16)
+    n = len(cubes)
+    counts = np.zeros(n, dtype=np.int32)
+    cent = np.zeros((n, 10, 4))
+    norm = np.zeros((n, 10, 4))
+    dx = np.ascontiguousarray(dx, dtype=np.float64)
+    st = L.vh_cornelius4d(cubes.ctypes.data_as(_dp), n, dx.ctypes.data_as(_dp), e0, device,
+                          counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                          cent.ctypes.data_as(_dp), norm.ctypes.data_as(_dp))
+    if st != VH_OK:
+        raise VhError(st, L.vh_last_error(None).decode())
+    return counts, cent, norm
 
 
 class VhGrid(ctypes.Structure):
@@ -120,6 +147,12 @@ def lib():
     L.vh_advance.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                              ctypes.POINTER(ctypes.c_int)]
     L.vh_resize2x.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.vh_surface.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
+    L.vh_surface_records.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
+    L.vh_surface_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long)]
+    L.vh_surface_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.vh_cornelius4d.argtypes = [_dp, ctypes.c_long, _dp, ctypes.c_double, ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_int), _dp, _dp]
     _lib = L
     return L
 
@@ -246,6 +279,23 @@ class GpuHydro:
         r = ctypes.c_int(0)
         self._check(self.L.vh_resize2x(self.h, ctypes.byref(r)))
         return r.value
+
+    def surface(self, ecrit=None):
+        """Fluid::outputSurface's freeze-out elements at the current tau:
+        (records [n][29], info dict)."""
+        info = VhSurfaceInfo()
+        ec = self.setup.ecrit if ecrit is None else ecrit
+        self._check(self.L.vh_surface(self.h, ec, ctypes.byref(info)))
+        n = info.nelements
+        rec = np.zeros((n, SURF_REC))
+        if n:
+            got = ctypes.c_long()
+            self._check(self.L.vh_surface_records(self.h, rec.ctypes.data_as(_dp), n,
+                                                  ctypes.byref(got)))
+        return rec, {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+
+    def surface_write(self, path, extend=False):
+        self._check(self.L.vh_surface_write(self.h, path.encode(), int(extend)))
 
     def grid(self):
         g = VhGrid()

@@ -12,6 +12,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <iomanip>
 #include <string>
 #include <vector>
 
@@ -39,6 +41,19 @@ struct vh_ctx {
   double* tot_partial = nullptr;  // [blocks][16] block sums of the totals
   double* tot_out = nullptr;      // [16]
   double* resize_tmp = nullptr;   // [10][N] staging of the resize gather
+  // the Fluid's construction-time step: the time side of the freeze-out
+  // hypercubes (src/fld.cpp:106-108); set at creation, doubled by the resize
+  double fluid_dt = 0.;
+  // surface sums: EtotSurf and vEff are Fluid members (reset by the resize's
+  // new Fluid), nbSurf is a function static in the reference (never reset)
+  double EtotSurf = 0., vEff = 0., nbSurf = 0.;
+  struct Surf {
+    double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
+           *partial = nullptr;
+    int *blk = nullptr, *cubes = nullptr, *cnt = nullptr, *counters = nullptr;
+    size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
+    long long nel = 0;
+  } surf;
   std::string err;
   std::vector<void*> allocs;
   // timers and per-kernel profiling
@@ -106,6 +121,25 @@ static vh_status dalloc(vh_ctx* c, T** p, size_t count) {
   c->allocs.push_back(q);
   *p = static_cast<T*>(q);
   return VH_OK;
+}
+
+// Replaces *p by an allocation of at least `need` elements (no copy).
+template <typename T>
+static vh_status dgrow(vh_ctx* c, T** p, size_t* cap, size_t need) {
+  if (*p && *cap >= need) return VH_OK;
+  if (*p) {
+    for (auto it = c->allocs.begin(); it != c->allocs.end(); ++it)
+      if (*it == (void*)*p) {
+        c->allocs.erase(it);
+        break;
+      }
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  const size_t n = std::max<size_t>(need, 2 * *cap);
+  vh_status st = dalloc(c, p, n);
+  if (st == VH_OK) *cap = n;
+  return st;
 }
 
 // Per-dimension source map of the ghost-cell copies: the reference copies
@@ -242,6 +276,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   c->grid = *grid;
   c->tau = tau0;
   c->dt = dt;
+  c->fluid_dt = dt;
   c->tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
                     tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
                     tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,
@@ -537,6 +572,8 @@ vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
   g.dy = ndy;
   g.dz = ndz;
   ctx->dt = dt2;  // src/main.cpp:268
+  ctx->fluid_dt = dt2;  // the new Fluid's step, src/main.cpp:254-256
+  ctx->EtotSurf = ctx->vEff = 0.;  // members of the new Fluid, src/fld.cpp:110-111
   if (resized) *resized = 1;
   return VH_OK;
 }
@@ -597,6 +634,149 @@ vh_status vh_totals(vh_ctx* ctx, double ecrit, double* out) {
   h[3] *= dx * dy * dz;
   h[4] = h[4] * dx * dy * dz;
   for (int k = 0; k < vh::kTotals; k++) out[k] = h[k];
+  return VH_OK;
+}
+
+// block partials of the surface sums (a fixed count keeps them deterministic)
+static const int kSurfPartials = 296;
+
+vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_surface: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  const vh::Geo& g = ctx->g;
+  vh_ctx::Surf& S = ctx->surf;
+  vh_status st;
+  if (!S.eN) {
+    if ((st = dalloc(ctx, &S.eN, g.N)) || (st = dalloc(ctx, &S.eP, g.N)) ||
+        (st = dalloc(ctx, &S.blk, std::max(1, vh::surf_count_blocks(g)))) ||
+        (st = dalloc(ctx, &S.counters, 2)) ||
+        (st = dalloc(ctx, &S.partial, (size_t)(kSurfPartials + 1) * vh::kSurfAcc)))
+      return st;
+  }
+  cudaStream_t s = ctx->stream;
+  const double taup = ctx->tau - ctx->fluid_dt;
+  vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, taup, S.eN, S.eP, s);
+  vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
+  VH_CUDA(ctx, cudaGetLastError());
+  int ncubes = 0, nel = 0;
+  VH_CUDA(ctx, cudaMemcpyAsync(&ncubes, S.counters, sizeof(int), cudaMemcpyDeviceToHost, s));
+  VH_CUDA(ctx, cudaStreamSynchronize(s));
+  if (ncubes > 0) {
+    if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, (size_t)ncubes)) ||
+        (st = dgrow(ctx, &S.geo, &S.cap_geo,
+                    (size_t)ncubes * vh::kSurfMaxElemPerCube * vh::kSurfGeo)) ||
+        (st = dgrow(ctx, &S.cnt, &S.cap_cnt, (size_t)ncubes + 1)))
+      return st;
+    vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, s);
+    vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, ncubes, S.geo, S.cnt,
+                              S.counters + 1, ctx->f.err, s);
+    VH_CUDA(ctx, cudaGetLastError());
+    VH_CUDA(ctx, cudaMemcpyAsync(&nel, S.counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaStreamSynchronize(s));
+  }
+  double acc[vh::kSurfAcc] = {0., 0., 0., 0., 0.};
+  if (nel > 0) {
+    if ((st = dgrow(ctx, &S.rec, &S.cap_rec, (size_t)nel * vh::kSurfRec)) ||
+        (st = dgrow(ctx, &S.contrib, &S.cap_contrib, (size_t)nel * vh::kSurfAcc)))
+      return st;
+    const int npart = std::max(1, std::min(kSurfPartials, (nel + 255) / 256));
+    vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
+                             ctx->grid.ymin, ctx->grid.etamin, S.cubes, ncubes, S.geo, S.cnt, nel,
+                             S.rec, S.contrib, S.partial, npart, s);
+    VH_CUDA(ctx, cudaGetLastError());
+    VH_CUDA(ctx, cudaMemcpyAsync(acc, S.partial + (size_t)npart * vh::kSurfAcc, sizeof acc,
+                                 cudaMemcpyDeviceToHost, s));
+  }
+  unsigned bits = 0;
+  VH_CUDA(ctx, cudaMemcpyAsync(&bits, ctx->f.err, sizeof bits, cudaMemcpyDeviceToHost, s));
+  VH_CUDA(ctx, cudaStreamSynchronize(s));
+  S.nel = nel;
+  ctx->EtotSurf += acc[1];
+  ctx->nbSurf += acc[2];
+  ctx->vEff += acc[3];
+  if (info) {
+    info->nelements = nel;
+    info->nsusp = (long)acc[0];
+    info->high_T = (long)acc[4];
+    info->EtotSurf = ctx->EtotSurf;
+    info->nbSurf = ctx->nbSurf;
+    info->vEff = ctx->vEff;
+  }
+  if (bits & vh::ERR_SURFACE)
+    return fail(ctx, VH_ERR_NUMERIC, "vh_surface: a hypercube on which the reference stops");
+  return VH_OK;
+}
+
+vh_status vh_surface_records(vh_ctx* ctx, double* out, long max, long* n) {
+  if (!ctx || (!out && max > 0)) return VH_ERR_ARG;
+  const long k = (long)std::min<long long>(ctx->surf.nel, std::max(0L, max));
+  if (n) *n = (long)ctx->surf.nel;
+  if (k > 0) {
+    VH_CUDA(ctx, cudaSetDevice(ctx->device));
+    VH_CUDA(ctx, cudaMemcpyAsync(out, ctx->surf.rec, sizeof(double) * vh::kSurfRec * k,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return VH_OK;
+}
+
+vh_status vh_surface_device(vh_ctx* ctx, const double** rec, long* n) {
+  if (!ctx || !rec || !n) return VH_ERR_ARG;
+  *rec = ctx->surf.rec;
+  *n = (long)ctx->surf.nel;
+  return VH_OK;
+}
+
+vh_status vh_surface_write(vh_ctx* ctx, const char* path, int extendFO) {
+  if (!ctx || !path) return VH_ERR_ARG;
+  const long n = (long)ctx->surf.nel;
+  std::vector<double> h((size_t)n * vh::kSurfRec);
+  vh_status st = vh_surface_records(ctx, h.data(), n, nullptr);
+  if (st != VH_OK) return st;
+  std::ofstream out(path, std::ios::app);
+  if (!out) return fail(ctx, VH_ERR_ARG, std::string("vh_surface_write: cannot open ") + path);
+  // src/fld.cpp:658-797: precision 15, width 24, OUTPI layout
+  out.precision(15);
+  const int ncol = extendFO ? vh::kSurfRec : vh::kSurfRec - 2;
+  for (long i = 0; i < n; i++) {
+    const double* r = h.data() + (size_t)i * vh::kSurfRec;
+    for (int c = 0; c < ncol; c++) out << std::setw(24) << r[c];
+    out << std::endl;
+  }
+  return out ? VH_OK : fail(ctx, VH_ERR_ARG, "vh_surface_write: write failed");
+}
+
+vh_status vh_cornelius4d(const double* cubes, long n, const double* dx, double e0, int device,
+                         int* counts, double* cent, double* norm) {
+  if (n < 0 || n > (1L << 24) || (n > 0 && (!cubes || !dx || !counts || !cent || !norm)))
+    return fail(nullptr, VH_ERR_ARG, "vh_cornelius4d: bad arguments");
+  if (n == 0) return VH_OK;
+  cudaError_t e;
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_fail(nullptr, e, "cudaSetDevice");
+  double *dc = nullptr, *dg = nullptr;
+  int* dn = nullptr;
+  const size_t G = (size_t)vh::kSurfMaxElemPerCube * vh::kSurfGeo;
+  std::vector<double> hg((size_t)n * G);
+  if ((e = cudaMalloc(&dc, sizeof(double) * 16 * n)) == cudaSuccess &&
+      (e = cudaMalloc(&dg, sizeof(double) * G * n)) == cudaSuccess &&
+      (e = cudaMalloc(&dn, sizeof(int) * n)) == cudaSuccess &&
+      (e = cudaMemcpy(dc, cubes, sizeof(double) * 16 * n, cudaMemcpyHostToDevice)) == cudaSuccess) {
+    vh::launch_cornelius_batch(dc, (int)n, dx, e0, dn, dg, 0);
+    if ((e = cudaGetLastError()) == cudaSuccess &&
+        (e = cudaMemcpy(counts, dn, sizeof(int) * n, cudaMemcpyDeviceToHost)) == cudaSuccess)
+      e = cudaMemcpy(hg.data(), dg, sizeof(double) * G * n, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(dc);
+  cudaFree(dg);
+  cudaFree(dn);
+  if (e != cudaSuccess) return cuda_fail(nullptr, e, "vh_cornelius4d");
+  for (long k = 0; k < n; k++)
+    for (int el = 0; el < vh::kSurfMaxElemPerCube; el++)
+      for (int d = 0; d < 4; d++) {
+        cent[(k * vh::kSurfMaxElemPerCube + el) * 4 + d] = hg[k * G + el * vh::kSurfGeo + d];
+        norm[(k * vh::kSurfMaxElemPerCube + el) * 4 + d] = hg[k * G + el * vh::kSurfGeo + 4 + d];
+      }
   return VH_OK;
 }
 

@@ -1,0 +1,496 @@
+// vh_cornelius.cuh -- Cornelius 4D iso-surface elements of one hypercube on
+// the device (P. Huovinen and H. Petersen, Eur. Phys. J. A 48 (2012) 171,
+// arXiv:1206.3371, as the reference's src/cornelius.cpp implements it).
+//
+// One thread handles one hypercube.  The 4-cube splits into 8 3-cubes
+// (constant dimension i at j = 0, 1; cornelius.cpp:1733-1774), each 3-cube
+// into 6 squares (:1436-1482).  A square gives 0-2 line elements from the
+// cuts of its edges (:1083-1313), a 3-cube joins its lines into polygons
+// (:1484-1578) and the 4-cube joins the polygons into polyhedra
+// (:1776-1878).  Every polyhedron is one element; its centroid and normal
+// come from the tetrahedra (line, polygon centroid, polyhedron mean) as in
+// :761-935.  Every decision (cut tests, ambiguity rules, the line and
+// polygon joining order, the 1e-10 point matching) and every floating-point
+// operation follows the reference's order, so the elements are
+// bit-identical to it.  Capacities: 96 lines, 64 polygons (8 per 3-cube),
+// 10 elements, as the reference's arrays; a hypercube that would exceed
+// them, or on which the reference stops (an odd number of cuts on a square,
+// too few lines for a polygon), returns -1.
+#pragma once
+
+namespace vh {
+namespace cn {
+
+constexpr int kMaxLines = 96;
+constexpr int kMaxPoly = 64;
+constexpr int kMaxPolyPerCube = 8;
+constexpr int kMaxElem = 10;
+constexpr double kEps = 1e-10;
+
+struct Line {
+  double p[2][4];  // end points
+  double o[4];     // a point outside the surface
+  int start;       // which of p is the start point (flip_start_end swaps)
+};
+
+struct Poly {
+  unsigned char li[12];
+  int n, cdim;
+  double cen[4];
+};
+
+struct Work {
+  Line L[kMaxLines];
+  Poly P[kMaxPoly];
+  int nl, np, err;
+};
+
+__device__ __forceinline__ const double* lstart(const Line& l) { return l.p[l.start]; }
+__device__ __forceinline__ const double* lend(const Line& l) { return l.p[1 - l.start]; }
+
+// Square::construct_lines with ends_of_edge and find_outside.  The square's
+// constant dimensions are c0, c1 (values v0, v1), its corner values p[a][b]
+// (a along x1, b along x2, x1 < x2).  Returns 1 when it is ambiguous.
+__device__ int square(Work& w, const double p[2][2], int c0, int c1, double v0, double v1,
+                      int x1, int x2, const double* dx, double E0) {
+  int above = 0;
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+      if (p[i][j] >= E0) above++;
+  if (above == 0 || above == 4) return 0;
+  double cx[4], cy[4];
+  int nc = 0;
+  if ((p[0][0] - E0) * (p[1][0] - E0) < 0) {
+    cx[nc] = (p[0][0] - E0) / (p[0][0] - p[1][0]) * dx[x1];
+    cy[nc++] = 0;
+  } else if (p[0][0] == E0 && p[1][0] < E0) {
+    cx[nc] = 1e-9 * dx[x1];
+    cy[nc++] = 0;
+  } else if (p[1][0] == E0 && p[0][0] < E0) {
+    cx[nc] = (1.0 - 1e-9) * dx[x1];
+    cy[nc++] = 0;
+  }
+  if ((p[0][0] - E0) * (p[0][1] - E0) < 0) {
+    cx[nc] = 0;
+    cy[nc++] = (p[0][0] - E0) / (p[0][0] - p[0][1]) * dx[x2];
+  } else if (p[0][0] == E0 && p[0][1] < E0) {
+    cx[nc] = 0;
+    cy[nc++] = 1e-9 * dx[x2];
+  } else if (p[0][1] == E0 && p[0][0] < E0) {
+    cx[nc] = 0;
+    cy[nc++] = (1.0 - 1e-9) * dx[x2];
+  }
+  if ((p[1][0] - E0) * (p[1][1] - E0) < 0) {
+    cx[nc] = dx[x1];
+    cy[nc++] = (p[1][0] - E0) / (p[1][0] - p[1][1]) * dx[x2];
+  } else if (p[1][0] == E0 && p[1][1] < E0) {
+    cx[nc] = dx[x1];
+    cy[nc++] = 1e-9 * dx[x2];
+  } else if (p[1][1] == E0 && p[1][0] < E0) {
+    cx[nc] = dx[x1];
+    cy[nc++] = (1.0 - 1e-9) * dx[x2];
+  }
+  if ((p[0][1] - E0) * (p[1][1] - E0) < 0) {
+    cx[nc] = (p[0][1] - E0) / (p[0][1] - p[1][1]) * dx[x1];
+    cy[nc++] = dx[x2];
+  } else if (p[0][1] == E0 && p[1][1] < E0) {
+    cx[nc] = 1e-9 * dx[x1];
+    cy[nc++] = dx[x2];
+  } else if (p[1][1] == E0 && p[0][1] < E0) {
+    cx[nc] = (1.0 - 1e-9) * dx[x1];
+    cy[nc++] = dx[x2];
+  }
+  if (nc != 0 && nc != 2 && nc != 4) {
+    w.err |= 1;
+    return 0;
+  }
+  if (nc == 0) return 0;
+  double ox[2], oy[2];
+  int amb = 0;
+  if (nc == 4) {
+    amb = 1;
+    double Emid = 0;
+    Emid += 0.25 * p[0][0];
+    Emid += 0.25 * p[0][1];
+    Emid += 0.25 * p[1][0];
+    Emid += 0.25 * p[1][1];
+    if ((p[0][0] < E0 && Emid < E0) || (p[0][0] > E0 && Emid > E0)) {
+      double t = cx[1];
+      cx[1] = cx[2];
+      cx[2] = t;
+      t = cy[1];
+      cy[1] = cy[2];
+      cy[2] = t;
+    }
+    if ((Emid - E0) < 0) {
+      ox[0] = ox[1] = 0.5 * dx[x1];
+      oy[0] = oy[1] = 0.5 * dx[x2];
+    } else if ((p[0][0] - E0) < 0) {
+      ox[0] = 0;
+      oy[0] = 0;
+      ox[1] = dx[x1];
+      oy[1] = dx[x2];
+    } else {
+      ox[0] = dx[x1];
+      oy[0] = 0;
+      ox[1] = 0;
+      oy[1] = dx[x2];
+    }
+  } else {
+    double sx = 0, sy = 0;
+    int nout = 0;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+        if (p[i][j] < E0) {
+          sx += i * dx[x1];
+          sy += j * dx[x2];
+          nout++;
+        }
+    ox[0] = sx;
+    oy[0] = sy;
+    ox[1] = oy[1] = 0;
+    if (nout > 0) {
+      ox[0] = ox[0] / (double)nout;
+      oy[0] = oy[0] / (double)nout;
+    }
+  }
+  for (int k = 0; k < nc / 2; k++) {
+    if (w.nl >= kMaxLines) {
+      w.err |= 2;
+      return amb;
+    }
+    Line& l = w.L[w.nl++];
+#pragma unroll
+    for (int e = 0; e < 2; e++) {
+      l.p[e][x1] = cx[2 * k + e];
+      l.p[e][x2] = cy[2 * k + e];
+      l.p[e][c0] = v0;
+      l.p[e][c1] = v1;
+    }
+    l.o[x1] = ox[k];
+    l.o[x2] = oy[k];
+    l.o[c0] = v0;
+    l.o[c1] = v1;
+    l.start = 0;
+  }
+  return amb;
+}
+
+// Polygon::add_line
+__device__ bool add_line(Work& w, Poly& pg, int li, bool donotcheck) {
+  if (donotcheck || pg.n == 0) {
+    pg.li[pg.n++] = (unsigned char)li;
+    return true;
+  }
+  Line& l = w.L[li];
+  const double *p1 = lstart(l), *p2 = lend(l), *p3 = lend(w.L[pg.li[pg.n - 1]]);
+  double d1 = 0, d2 = 0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    d1 += fabs(p1[j] - p3[j]);
+    d2 += fabs(p2[j] - p3[j]);
+  }
+  if (d1 < kEps || d2 < kEps) {
+    if (d2 < kEps) l.start = 1 - l.start;
+    pg.li[pg.n++] = (unsigned char)li;
+    return true;
+  }
+  return false;
+}
+
+// Cube::construct_polygons + check_ambiguous for the 3-cube with constant
+// dimension ci at corner bit jc.  Returns its number of lines.
+__device__ int cube3(Work& w, const double* hc, int ci, int jc, const double* dx, double E0,
+                     int& cube_amb) {
+  const int l0 = w.nl, p0 = w.np;
+  const double cv = jc * dx[ci];
+  int namb = 0;
+#pragma unroll 1
+  for (int i = 0; i < 4; i++) {
+    if (i == ci) continue;
+    int x1 = -1, x2 = -1;
+    for (int d = 0; d < 4; d++)
+      if (d != ci && d != i) {
+        if (x1 < 0)
+          x1 = d;
+        else
+          x2 = d;
+      }
+#pragma unroll 1
+    for (int j = 0; j < 2; j++) {
+      double sq[2][2];
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+          // corner bit of dimension d: ci -> jc, i -> j, x1 -> a, x2 -> b
+          const int bt = (jc << (3 - ci)) | (j << (3 - i)) | (a << (3 - x1)) | (b << (3 - x2));
+          sq[a][b] = hc[bt];
+        }
+      namb += square(w, sq, ci, i, cv, j * dx[i], x1, x2, dx, E0);
+    }
+  }
+  const int nl = w.nl - l0;
+  cube_amb = 0;
+  if (nl == 0) return 0;
+  int amb = namb;
+  if (amb == 0 && nl == 6) amb = 1;
+  cube_amb = amb;
+  if (amb > 0) {
+    unsigned long long unused_lo = 0, unused_hi = 0;  // bits of the cube's lines
+    for (int i = 0; i < nl; i++) {
+      if (i < 64)
+        unused_lo |= 1ull << i;
+      else
+        unused_hi |= 1ull << (i - 64);
+    }
+    int used = 0;
+    do {
+      if (nl - used < 3 || w.np >= kMaxPoly || w.np - p0 >= kMaxPolyPerCube) {
+        w.err |= 4;
+        return nl;
+      }
+      Poly& pg = w.P[w.np];
+      pg.n = 0;
+      pg.cdim = ci;
+      for (int i = 0; i < nl; i++) {
+        const bool un = i < 64 ? (unused_lo >> i) & 1 : (unused_hi >> (i - 64)) & 1;
+        if (un && pg.n < 12) {
+          if (add_line(w, pg, l0 + i, false)) {
+            if (i < 64)
+              unused_lo &= ~(1ull << i);
+            else
+              unused_hi &= ~(1ull << (i - 64));
+            used++;
+            i = 0;
+          }
+        }
+      }
+      w.np++;
+    } while (used < nl);
+  } else {
+    if (w.np >= kMaxPoly || nl > 12) {
+      w.err |= 4;
+      return nl;
+    }
+    Poly& pg = w.P[w.np];
+    pg.n = 0;
+    pg.cdim = ci;
+    for (int i = 0; i < nl; i++) add_line(w, pg, l0 + i, true);
+    w.np++;
+  }
+  return nl;
+}
+
+// Polygon::calculate_centroid
+__device__ void poly_centroid(const Work& w, Poly& pg) {
+  int x[3], k = 0;
+  for (int d = 0; d < 4; d++)
+    if (d != pg.cdim) x[k++] = d;
+  const int x1 = x[0], x2 = x[1], x3 = x[2];
+  double mean[4] = {0, 0, 0, 0};
+  for (int i = 0; i < pg.n; i++) {
+    const Line& l = w.L[pg.li[i]];
+    const double *p1 = lstart(l), *p2 = lend(l);
+#pragma unroll
+    for (int j = 0; j < 4; j++) mean[j] += p1[j] + p2[j];
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) mean[j] = mean[j] / (double)(2.0 * pg.n);
+  if (pg.n == 3) {
+#pragma unroll
+    for (int j = 0; j < 4; j++) pg.cen[j] = mean[j];
+    return;
+  }
+  double up[4] = {0, 0, 0, 0}, down = 0, a[4], b[4];
+  for (int i = 0; i < pg.n; i++) {
+    const Line& l = w.L[pg.li[i]];
+    const double *p1 = lstart(l), *p2 = lend(l);
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      a[j] = p1[j] - mean[j];
+      b[j] = p2[j] - mean[j];
+    }
+    const double c1 = a[x2] * b[x3] - a[x3] * b[x2];
+    const double c2 = a[x1] * b[x3] - a[x3] * b[x1];
+    const double c3 = a[x2] * b[x1] - a[x1] * b[x2];
+    const double A = 0.5 * sqrt(c1 * c1 + c2 * c2 + c3 * c3);
+#pragma unroll
+    for (int j = 0; j < 4; j++) up[j] += (p1[j] + p2[j] + mean[j]) / 3.0 * A;
+    down += A;
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) pg.cen[j] = up[j] / down;
+}
+
+// Polyhedron::tetravolume
+__device__ __forceinline__ void tetra(const double* a, const double* b, const double* c,
+                                      double* n) {
+  const double bc01 = b[0] * c[1] - b[1] * c[0];
+  const double bc02 = b[0] * c[2] - b[2] * c[0];
+  const double bc03 = b[0] * c[3] - b[3] * c[0];
+  const double bc12 = b[1] * c[2] - b[2] * c[1];
+  const double bc13 = b[1] * c[3] - b[3] * c[1];
+  const double bc23 = b[2] * c[3] - b[3] * c[2];
+  n[0] = 1.0 / 6.0 * (a[1] * bc23 - a[2] * bc13 + a[3] * bc12);
+  n[1] = -1.0 / 6.0 * (a[0] * bc23 - a[2] * bc03 + a[3] * bc02);
+  n[2] = 1.0 / 6.0 * (a[0] * bc13 - a[1] * bc03 + a[3] * bc01);
+  n[3] = -1.0 / 6.0 * (a[0] * bc12 - a[1] * bc02 + a[2] * bc01);
+}
+
+// Polyhedron::lines_equal
+__device__ bool lines_equal(const Line& l1, const Line& l2) {
+  const double *p11 = lstart(l1), *p12 = lend(l1), *p21 = lstart(l2);
+  double d1 = 0, d2 = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    d1 += fabs(p11[i] - p21[i]);
+    d2 += fabs(p12[i] - p21[i]);
+    if (d1 > kEps && d2 > kEps) return false;
+  }
+  return true;
+}
+
+// Cornelius::find_surface_4d.  hc[it*8 + jx*4 + jy*2 + jz]; dx = dt, dx, dy,
+// dz.  Writes up to kMaxElem centroids and normals (relative to the low
+// corner); returns the element count or -1.
+__device__ int find_surface_4d(Work& w, const double* hc, const double* dx, double E0,
+                               double (*cent)[4], double (*norm)[4]) {
+  int above = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++)
+    if (hc[k] >= E0) above++;
+  if (above == 0 || above == 16) return 0;
+  w.nl = w.np = w.err = 0;
+  int namb = 0, nlines = 0;
+#pragma unroll 1
+  for (int i = 0; i < 4; i++)
+#pragma unroll 1
+    for (int j = 0; j < 2; j++) {
+      int ca;
+      nlines += cube3(w, hc, i, j, dx, E0, ca);
+      if (ca) namb++;
+    }
+  if (w.err) return -1;
+  int amb = namb;
+  if (amb == 0) {
+    int pts = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++)
+      if (hc[k] < E0) pts++;
+    if (pts > 8) pts = 16 - pts;
+    if (nlines == 24 && pts == 2) amb++;
+  }
+  // polyhedra as lists of polygon indices
+  unsigned char ph[kMaxElem][kMaxPoly];
+  int nph[kMaxElem], nel = 0;
+  if (amb > 0) {
+    unsigned long long unused = w.np >= 64 ? ~0ull : ((1ull << w.np) - 1);
+    int used = 0;
+    do {
+      if (nel >= kMaxElem) return -1;
+      nph[nel] = 0;
+      for (int i = 0; i < w.np; i++) {
+        if (!((unused >> i) & 1)) continue;
+        bool add = nph[nel] == 0;
+        if (!add) {
+          const Poly& p = w.P[i];
+          for (int q = 0; q < nph[nel] && !add; q++) {
+            const Poly& pq = w.P[ph[nel][q]];
+            for (int j = 0; j < p.n && !add; j++)
+              for (int k = 0; k < pq.n && !add; k++)
+                if (lines_equal(w.L[p.li[j]], w.L[pq.li[k]])) add = true;
+          }
+        }
+        if (add) {
+          ph[nel][nph[nel]++] = (unsigned char)i;
+          unused &= ~(1ull << i);
+          used++;
+          i = 0;
+        }
+      }
+      nel++;
+    } while (used < w.np);
+  } else {
+    nph[0] = 0;
+    for (int i = 0; i < w.np; i++) ph[0][nph[0]++] = (unsigned char)i;
+    nel = 1;
+  }
+  for (int i = 0; i < w.np; i++) poly_centroid(w, w.P[i]);
+#pragma unroll 1
+  for (int e = 0; e < nel; e++) {
+    int ntet = 0;
+    double mean[4] = {0, 0, 0, 0};
+    for (int q = 0; q < nph[e]; q++) {
+      const Poly& pg = w.P[ph[e][q]];
+      ntet += pg.n;
+      for (int j = 0; j < pg.n; j++) {
+        const Line& l = w.L[pg.li[j]];
+        const double *p1 = lstart(l), *p2 = lend(l);
+#pragma unroll
+        for (int k = 0; k < 4; k++) mean[k] += p1[k] + p2[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) mean[k] = mean[k] / (double)(2.0 * ntet);
+    double up[4] = {0, 0, 0, 0}, down = 0, a[4], b[4], c[4], n[4];
+    for (int q = 0; q < nph[e]; q++) {
+      const Poly& pg = w.P[ph[e][q]];
+      for (int j = 0; j < pg.n; j++) {
+        const Line& l = w.L[pg.li[j]];
+        const double *p1 = lstart(l), *p2 = lend(l);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          a[k] = p1[k] - mean[k];
+          b[k] = p2[k] - mean[k];
+          c[k] = pg.cen[k] - mean[k];
+        }
+        tetra(a, b, c, n);
+        double V = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) V += n[k] * n[k];
+        V = sqrt(V);
+#pragma unroll
+        for (int k = 0; k < 4; k++) up[k] += (p1[k] + p2[k] + pg.cen[k] + mean[k]) / 4.0 * V;
+        down += V;
+      }
+    }
+    double* C = cent[e];
+#pragma unroll
+    for (int k = 0; k < 4; k++) C[k] = up[k] / down;
+    double* Nn = norm[e];
+#pragma unroll
+    for (int k = 0; k < 4; k++) Nn[k] = 0;
+    for (int q = 0; q < nph[e]; q++) {
+      const Poly& pg = w.P[ph[e][q]];
+      for (int j = 0; j < pg.n; j++) {
+        const Line& l = w.L[pg.li[j]];
+        const double *p1 = lstart(l), *p2 = lend(l);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          a[k] = p1[k] - C[k];
+          b[k] = p2[k] - C[k];
+          c[k] = pg.cen[k] - C[k];
+        }
+        tetra(a, b, c, n);
+        double dot = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) dot += (l.o[k] - C[k]) * n[k];
+        if (dot < 0) {
+#pragma unroll
+          for (int k = 0; k < 4; k++) n[k] = -n[k];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) Nn[k] += n[k];
+      }
+    }
+  }
+  return nel;
+}
+
+}  // namespace cn
+}  // namespace vh

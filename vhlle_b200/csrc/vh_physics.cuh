@@ -19,6 +19,7 @@ enum : unsigned {
   ERR_FLUX_NAN = 2u,     // src/hdo.cpp:285-298
   ERR_SOURCE_NAN = 4u,   // src/hdo.cpp:345-351
   ERR_NSQUANT_NAN = 8u,  // src/hdo.cpp:643-651
+  ERR_SURFACE = 16u,     // Cornelius would stop the reference (src/cornelius.cpp:1217,1534)
 };
 
 // How a table axis is searched: a binary search as the reference does, or

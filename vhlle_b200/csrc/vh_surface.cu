@@ -1,6 +1,7 @@
 // vh_surface.cu -- what Fluid::outputSurface (src/fld.cpp:517-874) computes
 // from the grid after a step: the interior totals (energy, baryon number,
-// entropy, momentum, flow anisotropy sums).
+// entropy, momentum, flow anisotropy sums) and the freeze-out hypersurface
+// elements (Cornelius 4D, vh_cornelius.cuh) with their interpolated state.
 //
 // The totals are a deterministic two-level reduction: every thread forms its
 // cell's 16 contributions exactly as the reference does (src/fld.cpp:544-604),
@@ -11,6 +12,7 @@
 // summation order and by the last bits of log/cosh/sinh/tanh.
 #include <cuda_runtime.h>
 
+#include "vh_cornelius.cuh"
 #include "vh_physics.cuh"
 #include "vh_step.cuh"
 #include "vh_surface.cuh"
@@ -164,6 +166,430 @@ void launch_totals(const Geo& g, const EosDev& E, const Fields& f, double tau, d
   const int nb = totals_blocks(g);
   k_totals<<<nb, kTotBlock, 0, s>>>(g, E, f.Q, f.pi, f.vcc, tau, ecrit, etamin, viscous, partial);
   k_totals_final<<<1, kTotBlock, 0, s>>>(partial, nb, out);
+}
+
+}  // namespace vh
+
+// ===================================================================
+// Freeze-out hypersurface: the element part of Fluid::outputSurface
+// (src/fld.cpp:606-842).  Stages, all on the context's stream:
+//   1. k_surf_energy     e at tau (Q) and at tau - dt (Qprev) per cell
+//   2. k_surf_count      straddling interior cubes per block
+//   3. k_scan_excl       block offsets (one block)
+//   4. k_surf_compact    straddling cube list in the reference's loop order
+//   5. k_surf_cornelius  Cornelius per cube -> centroids, normals, counts
+//   6. k_scan_excl       element offsets
+//   7. k_surf_elements   one record per element (+ its sums' contributions)
+//   8. k_sum_cols        deterministic sums of the contributions
+// ===================================================================
+namespace vh {
+
+__global__ void k_surf_energy(Geo g, EosDev E, const double* __restrict__ Q,
+                              const double* __restrict__ Qprev, double tau, double taup,
+                              double* __restrict__ eN, double* __restrict__ eP) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  int ix, iy, iz;
+  coords(g, i, ix, iy, iz);
+  // only corners of interior cubes: [2, n-2] on every axis
+  if (ix < 2 || iy < 2 || iz < 2 || ix > g.nx - 2 || iy > g.ny - 2 || iz > g.nz - 2) return;
+  const long long N = g.N;
+  double q[7];
+  Prim P;
+  // Cell::getPrimVar / getPrimVarPrev, src/cll.cpp:90-95,214-220
+#pragma unroll
+  for (int k = 0; k < 7; k++) q[k] = ddivp(Q[k * N + i], tau);
+  transform_pv(E, q, P);
+  eN[i] = P.e;
+#pragma unroll
+  for (int k = 0; k < 7; k++) q[k] = ddivp(Qprev[k * N + i], taup);
+  transform_pv(E, q, P);
+  eP[i] = P.e;
+}
+
+__device__ __forceinline__ void cube_cell(const Geo& g, long long t, int& ix, int& iy, int& iz) {
+  const int niz = g.nz - 4, niy = g.ny - 4;
+  iz = 2 + (int)(t % niz);
+  iy = 2 + (int)((t / niz) % niy);
+  ix = 2 + (int)(t / ((long long)niz * niy));
+}
+
+__device__ __forceinline__ void load_cube(const Geo& g, const double* __restrict__ eN,
+                                          const double* __restrict__ eP, int ix, int iy, int iz,
+                                          double* hc) {
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const long long i = cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1));
+    hc[8 + c] = eN[i];
+    hc[c] = eP[i];
+  }
+}
+
+__device__ __forceinline__ bool straddles(const double* hc, double e0) {
+  int above = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++) above += hc[k] >= e0;
+  return above != 0 && above != 16;
+}
+
+constexpr int kSurfBlock = 256;
+
+__global__ void __launch_bounds__(kSurfBlock) k_surf_count(Geo g, const double* __restrict__ eN,
+                                                           const double* __restrict__ eP,
+                                                           double e0, long long ncube,
+                                                           int* __restrict__ blk) {
+  const long long t = (long long)blockIdx.x * kSurfBlock + threadIdx.x;
+  int flag = 0;
+  if (t < ncube) {
+    int ix, iy, iz;
+    double hc[16];
+    cube_cell(g, t, ix, iy, iz);
+    load_cube(g, eN, eP, ix, iy, iz, hc);
+    flag = straddles(hc, e0);
+  }
+  const int c = __syncthreads_count(flag);
+  if (threadIdx.x == 0) blk[blockIdx.x] = c;
+}
+
+// Exclusive prefix sum of a[0..n) in place by one block; *total = the sum.
+constexpr int kScanBlock = 1024;
+__global__ void __launch_bounds__(kScanBlock) k_scan_excl(int* __restrict__ a, int n,
+                                                          int* __restrict__ total) {
+  __shared__ long long part[kScanBlock];
+  const int per = (n + kScanBlock - 1) / kScanBlock;
+  const int b = threadIdx.x * per, e = min(n, b + per);
+  long long s = 0;
+  for (int i = b; i < e; i++) s += a[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  // Hillis-Steele inclusive scan of the chunk sums
+  for (int o = 1; o < kScanBlock; o <<= 1) {
+    const long long v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+  for (int i = b; i < e; i++) {
+    const int v = a[i];
+    a[i] = (int)run;
+    run += v;
+  }
+  if (threadIdx.x == kScanBlock - 1) *total = (int)part[kScanBlock - 1];
+}
+
+__global__ void __launch_bounds__(kSurfBlock) k_surf_compact(Geo g, const double* __restrict__ eN,
+                                                             const double* __restrict__ eP,
+                                                             double e0, long long ncube,
+                                                             const int* __restrict__ blkoff,
+                                                             int* __restrict__ cubes) {
+  __shared__ int woff[kSurfBlock / 32];
+  const long long t = (long long)blockIdx.x * kSurfBlock + threadIdx.x;
+  bool flag = false;
+  if (t < ncube) {
+    int ix, iy, iz;
+    double hc[16];
+    cube_cell(g, t, ix, iy, iz);
+    load_cube(g, eN, eP, ix, iy, iz, hc);
+    flag = straddles(hc, e0);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(0xffffffffu, flag);
+  if (lane == 0) woff[w] = __popc(bal);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int k = 0; k < kSurfBlock / 32; k++) {
+      const int v = woff[k];
+      woff[k] = s;
+      s += v;
+    }
+  }
+  __syncthreads();
+  if (flag)
+    cubes[blkoff[blockIdx.x] + woff[w] + __popc(bal & ((1u << lane) - 1u))] = (int)t;
+}
+
+constexpr int kCornBlock = 64;
+constexpr int kGeo = 8;  // centroid[4], normal[4] per element
+
+__global__ void __launch_bounds__(kCornBlock) k_surf_cornelius(
+    Geo g, const double* __restrict__ eN, const double* __restrict__ eP, double e0, double dt4,
+    const int* __restrict__ cubes, int ncubes, double* __restrict__ geo, int* __restrict__ cnt,
+    unsigned* err) {
+  const int k = blockIdx.x * kCornBlock + threadIdx.x;
+  if (k >= ncubes) return;
+  int ix, iy, iz;
+  double hc[16];
+  cube_cell(g, cubes[k], ix, iy, iz);
+  load_cube(g, eN, eP, ix, iy, iz, hc);
+  // Fluid::Fluid's Cornelius cell sizes {dt, dx, dy, dz}, src/fld.cpp:106-108
+  const double dx4[4] = {dt4, g.dx, g.dy, g.dz};
+  cn::Work w;
+  double cent[cn::kMaxElem][4], norm[cn::kMaxElem][4];
+  int n = cn::find_surface_4d(w, hc, dx4, e0, cent, norm);
+  if (n < 0) {
+    atomicOr(err, ERR_SURFACE);
+    n = 0;
+  }
+  double* o = geo + (long long)k * cn::kMaxElem * kGeo;
+  for (int e = 0; e < n; e++) {
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      o[e * kGeo + d] = cent[e][d];
+      o[e * kGeo + 4 + d] = norm[e][d];
+    }
+  }
+  cnt[k] = n;
+}
+
+// transformToLab, src/fld.cpp:508-513
+__device__ __forceinline__ void to_lab(double eta, double& vx, double& vy, double& vz) {
+  const double Y = eta + 1. / 2. * log((1. + vz) / (1. - vz));
+  vx = vx * cosh(Y - eta) / cosh(Y);
+  vy = vy * cosh(Y - eta) / cosh(Y);
+  vz = tanh(Y);
+}
+
+struct SurfArgs {
+  Geo g;
+  EosDev E;
+  const double *Q, *Qprev, *pi, *Pi;
+  double tau, dtf, ecrit, xmin, ymin, zmin;
+  const int* cubes;
+  int ncubes;
+  const double* geo;
+  const int* off;
+  int nel;
+  double* rec;
+  double* contrib;
+};
+
+__global__ void __launch_bounds__(128) k_surf_elements(SurfArgs a) {
+  const int el = blockIdx.x * blockDim.x + threadIdx.x;
+  if (el >= a.nel) return;
+  // the cube whose element range holds el: the last k with off[k] <= el
+  int lo = 0, hi = a.ncubes;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (a.off[mid] <= el)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  const int k = lo, e = el - a.off[k];
+  const Geo& g = a.g;
+  int ix, iy, iz;
+  cube_cell(g, a.cubes[k], ix, iy, iz);
+  const double* G = a.geo + (long long)k * cn::kMaxElem * kGeo;
+  const double C[4] = {G[e * kGeo], G[e * kGeo + 1], G[e * kGeo + 2], G[e * kGeo + 3]};
+  const double n0[4] = {G[4], G[5], G[6], G[7]};  // the cube's first element (src/fld.cpp:743-751)
+  const double dx = g.dx, dy = g.dy, dz = g.dz, dtf = a.dtf, tau = a.tau;
+  const long long N = g.N;
+  const double wT[2] = {1. - C[0] / dtf, C[0] / dtf};
+  const double wX[2] = {1. - C[1] / dx, C[1] / dx};
+  const double wY[2] = {1. - C[2] / dy, C[2] / dy};
+  const double wZ[2] = {1. - C[3] / dz, C[3] / dz};
+  double QC[7] = {0., 0., 0., 0., 0., 0., 0.};
+  const double* lay[2] = {a.Qprev, a.Q};
+#pragma unroll 1
+  for (int jt = 0; jt < 2; jt++)
+#pragma unroll 1
+    for (int c = 0; c < 8; c++) {
+      const int jx = c >> 2, jy = (c >> 1) & 1, jz = c & 1;
+      const long long i = cidx(g, ix + jx, iy + jy, iz + jz);
+#pragma unroll
+      for (int q = 0; q < 7; q++) QC[q] += lay[jt][q * N + i] * wT[jt] * wX[jx] * wY[jy] * wZ[jz];
+    }
+#pragma unroll
+  for (int q = 0; q < 7; q++) QC[q] = QC[q] / (tau + C[0]);
+  Prim P;
+  transform_pv(a.E, QC, P);
+  double TC, mubC, pC;
+  eos_eval(a.E, P.e, P.nb, TC, mubC, pC);
+  const double eC = P.e, nbC = P.nb;
+  double vxC = P.vx, vyC = P.vy, vzC = P.vz;
+  double* ct = a.contrib + (long long)el * 5;
+  ct[4] = (TC > 0.4 || fabs(mubC) > 0.85) ? 1. : 0.;
+  ct[0] = (eC > a.ecrit * 2.0 || eC < a.ecrit * 0.5) ? 1. : 0.;
+  double piC[10], PiC = 0.;
+#pragma unroll
+  for (int q = 0; q < 10; q++) piC[q] = 0.;
+#pragma unroll 1
+  for (int c = 0; c < 8; c++) {
+    const int jx = c >> 2, jy = (c >> 1) & 1, jz = c & 1;
+    const long long i = cidx(g, ix + jx, iy + jy, iz + jz);
+#pragma unroll
+    for (int q = 0; q < 10; q++) piC[q] += a.pi[q * N + i] * wX[jx] * wY[jy] * wZ[jz];
+    PiC += a.Pi[i] * wX[jx] * wY[jy] * wZ[jz];
+  }
+  const double v2C = vxC * vxC + vyC * vyC + vzC * vzC;
+  if (v2C > 1.) {
+    vxC *= sqrt(0.99 / v2C);
+    vyC *= sqrt(0.99 / v2C);
+    vzC *= sqrt(0.99 / v2C);
+  }
+  const double etaC = (a.zmin + iz * dz) + C[3];
+  to_lab(etaC, vxC, vyC, vzC);
+  const double gammaC = 1. / sqrt(1. - vxC * vxC - vyC * vyC - vzC * vzC);
+  const double uC[4] = {gammaC, gammaC * vxC, gammaC * vyC, gammaC * vzC};
+  const double tauC = tau + C[0];
+  const double ch = cosh(etaC), sh = sinh(etaC);
+  double ds[4];
+  ds[0] = tauC * (ch * n0[0] - sh / tauC * n0[3]);
+  ds[3] = tauC * (-sh * n0[0] + ch / tauC * n0[3]);
+  ds[1] = tauC * n0[1];
+  ds[2] = tauC * n0[2];
+  double dVEff = 0.0;
+#pragma unroll
+  for (int q = 0; q < 4; q++) dVEff += ds[q] * uC[q];
+  // pi^{mu nu} to Cartesian components, src/fld.cpp:767-786 (index44 order)
+  double pc[10];
+  pc[0] = ch * ch * piC[0] + 2. * ch * sh * piC[6] + sh * sh * piC[9];
+  pc[1] = ch * piC[1] + sh * piC[7];
+  pc[3] = ch * piC[3] + sh * piC[8];
+  pc[6] = ch * sh * (piC[0] + piC[9]) + (ch * ch + sh * sh) * piC[6];
+  pc[2] = piC[2];
+  pc[4] = piC[4];
+  pc[7] = sh * piC[1] + ch * piC[7];
+  pc[5] = piC[5];
+  pc[8] = sh * piC[3] + ch * piC[8];
+  pc[9] = sh * sh * piC[0] + ch * ch * piC[9] + 2. * sh * ch * piC[6];
+  double dEsurfVisc = 0.;
+  dEsurfVisc += pc[0] * ds[0];
+  dEsurfVisc += pc[1] * ds[1];
+  dEsurfVisc += pc[3] * ds[2];
+  dEsurfVisc += pc[6] * ds[3];
+  ct[1] = (eC + pC) * uC[0] * dVEff - pC * ds[0] + dEsurfVisc;
+  ct[2] = nbC * dVEff;
+  ct[3] = dVEff;
+  double* r = a.rec + (long long)el * kSurfRec;
+  r[0] = tau + C[0];
+  r[1] = (a.xmin + ix * dx) + C[1];
+  r[2] = (a.ymin + iy * dy) + C[2];
+  r[3] = (a.zmin + iz * dz) + C[3];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    r[4 + q] = ds[q];
+    r[8 + q] = uC[q];
+  }
+  r[12] = TC;
+  r[13] = mubC;
+  r[14] = 0.;
+  r[15] = 0.;
+#pragma unroll
+  for (int q = 0; q < 10; q++) r[16 + q] = pc[q];
+  r[26] = PiC;
+  r[27] = eC;
+  r[28] = nbC;
+}
+
+// Column sums of x[n][kSurfAcc] in a fixed tree: block partials, then one
+// block over the partials in index order.
+__global__ void __launch_bounds__(kTotBlock) k_sum_cols(const double* __restrict__ x, int n,
+                                                        int ncol, double* __restrict__ out) {
+  __shared__ double red[kTotBlock / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int c = 0; c < ncol; c++) {
+    double s = 0.;
+    for (int i = blockIdx.x * kTotBlock + threadIdx.x; i < n; i += gridDim.x * kTotBlock)
+      s += x[(long long)i * ncol + c];
+    s = warp_sum(s);
+    if (lane == 0) red[w] = s;
+    __syncthreads();
+    if (w == 0) {
+      double v = lane < kTotBlock / 32 ? red[lane] : 0.;
+      v = warp_sum(v);
+      if (lane == 0) out[blockIdx.x * ncol + c] = v;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double tau, double taup,
+                        double* eN, double* eP, cudaStream_t s) {
+  k_surf_energy<<<(unsigned)((g.N + 127) / 128), 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN,
+                                                               eP);
+}
+
+long long surf_ncube(const Geo& g) {
+  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.nz - 4;
+  return (nix > 0 && niy > 0 && niz > 0) ? (long long)nix * niy * niz : 0;
+}
+
+int surf_count_blocks(const Geo& g) {
+  return (int)((surf_ncube(g) + kSurfBlock - 1) / kSurfBlock);
+}
+
+void launch_surf_count(const Geo& g, const double* eN, const double* eP, double e0, int* blk,
+                       int* total, cudaStream_t s) {
+  const int nb = surf_count_blocks(g);
+  if (nb == 0) {
+    cudaMemsetAsync(total, 0, sizeof(int), s);
+    return;
+  }
+  k_surf_count<<<nb, kSurfBlock, 0, s>>>(g, eN, eP, e0, surf_ncube(g), blk);
+  k_scan_excl<<<1, kScanBlock, 0, s>>>(blk, nb, total);
+}
+
+void launch_surf_compact(const Geo& g, const double* eN, const double* eP, double e0,
+                         const int* blkoff, int* cubes, cudaStream_t s) {
+  const int nb = surf_count_blocks(g);
+  if (nb) k_surf_compact<<<nb, kSurfBlock, 0, s>>>(g, eN, eP, e0, surf_ncube(g), blkoff, cubes);
+}
+
+void launch_surf_cornelius(const Geo& g, const double* eN, const double* eP, double e0, double dtf,
+                           const int* cubes, int ncubes, double* geo, int* cnt, int* nel,
+                           unsigned* err, cudaStream_t s) {
+  k_surf_cornelius<<<(ncubes + kCornBlock - 1) / kCornBlock, kCornBlock, 0, s>>>(
+      g, eN, eP, e0, dtf, cubes, ncubes, geo, cnt, err);
+  k_scan_excl<<<1, kScanBlock, 0, s>>>(cnt, ncubes, nel);
+}
+
+void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double tau, double dtf,
+                          double ecrit, double xmin, double ymin, double zmin, const int* cubes,
+                          int ncubes, const double* geo, const int* off, int nel, double* rec,
+                          double* contrib, double* partial, int npartial, cudaStream_t s) {
+  SurfArgs a{g,     E,    f.Q,  f.Qprev, f.pi,  f.Pi, tau, dtf,     ecrit,   xmin, ymin,
+             zmin,  cubes, ncubes, geo,  off,   nel,  rec, contrib};
+  k_surf_elements<<<(nel + 127) / 128, 128, 0, s>>>(a);
+  k_sum_cols<<<npartial, kTotBlock, 0, s>>>(contrib, nel, kSurfAcc, partial);
+  k_sum_cols<<<1, kTotBlock, 0, s>>>(partial, npartial, kSurfAcc, partial + npartial * kSurfAcc);
+}
+
+}  // namespace vh
+
+namespace vh {
+
+__global__ void __launch_bounds__(kCornBlock) k_cornelius_batch(const double* __restrict__ cubes,
+                                                                int n, double d0, double d1,
+                                                                double d2, double d3, double e0,
+                                                                int* __restrict__ counts,
+                                                                double* __restrict__ geo) {
+  const int k = blockIdx.x * kCornBlock + threadIdx.x;
+  if (k >= n) return;
+  double hc[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) hc[q] = cubes[(long long)k * 16 + q];
+  const double dx4[4] = {d0, d1, d2, d3};
+  cn::Work w;
+  double cent[cn::kMaxElem][4], norm[cn::kMaxElem][4];
+  const int m = cn::find_surface_4d(w, hc, dx4, e0, cent, norm);
+  counts[k] = m;
+  double* o = geo + (long long)k * cn::kMaxElem * kGeo;
+  for (int e = 0; e < m; e++)
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+      o[e * kGeo + d] = cent[e][d];
+      o[e * kGeo + 4 + d] = norm[e][d];
+    }
+}
+
+void launch_cornelius_batch(const double* cubes, int n, const double* dx, double e0, int* counts,
+                            double* geo, cudaStream_t s) {
+  if (n > 0)
+    k_cornelius_batch<<<(n + kCornBlock - 1) / kCornBlock, kCornBlock, 0, s>>>(
+        cubes, n, dx[0], dx[1], dx[2], dx[3], e0, counts, geo);
 }
 
 }  // namespace vh

@@ -11,8 +11,40 @@ namespace vh {
 // pi0x_den, txxyy_num, txxyy_den, nCoreCells, nCoreCutCells (unscaled sums)
 constexpr int kTotals = 16;
 
+// freeze-out element record: tau, x, y, eta, dSigma[4], u[4], T, muB, muQ,
+// muS, pi_cart[10] (index44 order), Pi, e, nb
+constexpr int kSurfRec = 29;
+// per-element contributions: nsusp, EtotSurf, nbSurf, vEff, high-T/muB flag
+constexpr int kSurfAcc = 5;
+constexpr int kSurfMaxElemPerCube = 10;
+constexpr int kSurfGeo = 8;
+
 int totals_blocks(const Geo& g);
 void launch_totals(const Geo& g, const EosDev& E, const Fields& f, double tau, double ecrit,
                    double etamin, bool viscous, double* partial, double* out, cudaStream_t s);
+
+long long surf_ncube(const Geo& g);
+int surf_count_blocks(const Geo& g);
+void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double tau, double taup,
+                        double* eN, double* eP, cudaStream_t s);
+// per-block counts into blk[], exclusive offsets in place, the sum to *total
+void launch_surf_count(const Geo& g, const double* eN, const double* eP, double e0, int* blk,
+                       int* total, cudaStream_t s);
+void launch_surf_compact(const Geo& g, const double* eN, const double* eP, double e0,
+                         const int* blkoff, int* cubes, cudaStream_t s);
+// Cornelius on ncubes cubes; cnt[] becomes the element offsets, *nel the total
+void launch_surf_cornelius(const Geo& g, const double* eN, const double* eP, double e0, double dtf,
+                           const int* cubes, int ncubes, double* geo, int* cnt, int* nel,
+                           unsigned* err, cudaStream_t s);
+// records and per-element sums; the sums land in partial[npartial*kSurfAcc ..]
+void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double tau, double dtf,
+                          double ecrit, double xmin, double ymin, double zmin, const int* cubes,
+                          int ncubes, const double* geo, const int* off, int nel, double* rec,
+                          double* contrib, double* partial, int npartial, cudaStream_t s);
+
+// Cornelius on n independent hypercubes (16 corner values each): counts[k]
+// elements (-1 where the reference stops), geo[k][10][8] centroid + normal
+void launch_cornelius_batch(const double* cubes, int n, const double* dx, double e0, int* counts,
+                            double* geo, cudaStream_t s);
 
 }  // namespace vh
