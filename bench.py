@@ -6,8 +6,10 @@ Workload (one "step" = one Hydro::performStep over the whole grid): the 3D
 viscous single event, 101x101x51 cells (x, y in [-15, 15] fm, eta_s in
 [-7.5, 7.5]), tau0 = 0.5 fm/c, dtau = 0.05 fm/c, eta/s = 0.08, zeta/s = 0,
 2000-point c_s^2(e) EoS table, seeded Monte-Carlo Glauber Pb+Pb event at
-b = 7 fm (synthetic: the reference ships no input data).  The timed K steps
-are the first K steps of the event (warm-up runs on a throw-away copy).
+b = 7 fm (synthetic: the reference ships no input data), with the Cornelius
+freeze-out surface at e_f = 0.5 GeV/fm^3 after every second step.  The timed
+K steps are the first K steps of the event (warm-up runs on a throw-away
+copy) and include those surface calls.
 
 Multi-GPU (torchrun, N ranks): events are independent, so every rank runs
 its own event (seed + rank) with no collective on the data path; the time is
@@ -40,11 +42,15 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+from vhlle_b200.sharding import Ranks, dist_env  # noqa: E402
+
 METRIC = "cell-updates/s per B200: batched+MLP-guess vs plain GPU at ≤1e-8 rel err"
 UNIT = "cell-updates/s"
-WORKLOAD = ("3D viscous single event 101x101x51 (x,y in [-15,15] fm, eta_s in [-7.5,7.5]), "
+WORKLOAD = ("3D viscous single event %s (x,y in [-15,15] fm, eta_s in [-7.5,7.5]), "
             "tau0=0.5, dtau=0.05, eta/s=0.08, zeta/s=0, c_s^2(e) 2000-point EoS table, "
-            "seeded MC-Glauber Pb+Pb b=7 fm, peak e=50 GeV/fm^3")
+            "seeded MC-Glauber Pb+Pb b=7 fm, peak e=50 GeV/fm^3, Cornelius surface at "
+            "e_f=0.5 GeV/fm^3 every 2 steps")
+SURF_EVERY = 2
 COMPULSORY_B = 288  # bytes per cell-update: Q[7] + pi[10] + Pi, read + write
 
 # Algorithmic bytes per cell per launch of each kernel (fields each launch
@@ -71,42 +77,6 @@ def measured_peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
-
-
-def dist_env():
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return ws, rank, local
-
-
-class Dist:
-    """Barrier and max-reduce over ranks (gloo over the host; timings only)."""
-
-    def __init__(self, ws):
-        self.ws = ws
-        self.dist = None
-        if ws > 1:
-            import datetime
-            import torch.distributed as dist
-            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-            self.dist = dist
-
-    def barrier(self):
-        if self.dist:
-            self.dist.barrier()
-
-    def max(self, x):
-        if not self.dist:
-            return x
-        import torch
-        t = torch.tensor([float(x)], dtype=torch.float64)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def close(self):
-        if self.dist:
-            self.dist.destroy_process_group()
 
 
 class ClockSampler:
@@ -180,18 +150,24 @@ def cpu_baseline_sample(setup, steps=2):
     event; falls back to the C restatement if the reference is not built."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as P
+    import tempfile
     kind = "reference" if P.ref_available() else "port"
     run = P.RefRun(setup) if kind == "reference" else P.OracleRun(setup)
     run.step(1)  # warm-up step, as the reference timing plan asks
-    t0 = time.perf_counter()
-    run.step(steps)
-    dt = time.perf_counter() - t0
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        for k in range(1, steps + 1):
+            run.step(1)
+            if k % SURF_EVERY == 0:
+                run.output_surface(d) if kind == "reference" else run.surface()
+        dt = time.perf_counter() - t0
     if kind == "reference":
         run.close()
     cells = setup.grid.ncells
     return {"value": cells * steps / dt, "unit": UNIT, "cores": 1, "kind": kind,
-            "sample": "%d performStep calls of the full 101x101x51 event after 1 warm-up "
-                      "step, one thread, %.1f s" % (steps, dt)}
+            "sample": "%d performStep calls of the %dx%dx%d event with the freeze-out "
+                      "surface after every %d, after 1 warm-up step, one thread, %.1f s"
+                      % (steps, setup.grid.nx, setup.grid.ny, setup.grid.nz, SURF_EVERY, dt)}
 
 
 def _ref_worker(args):
@@ -200,17 +176,22 @@ def _ref_worker(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from vhlle_b200 import workloads as W
     import pyoracle as P
+    import tempfile
     setup = W.glauber3d_setup(seed=seed)
-    run = P.RefRun(setup) if P.ref_available() else P.OracleRun(setup)
+    ref = P.ref_available()
+    run = P.RefRun(setup) if ref else P.OracleRun(setup)
     done = 0
-    t0 = time.perf_counter()
-    while done < steps:
-        run.step(1)
-        done += 1
-        if time.perf_counter() - t0 > budget:
-            break
-    dt = time.perf_counter() - t0
-    return done * setup.grid.ncells, dt, P.ref_available()
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        while done < steps:
+            run.step(1)
+            done += 1
+            if done % SURF_EVERY == 0:
+                run.output_surface(d) if ref else run.surface()
+            if time.perf_counter() - t0 > budget:
+                break
+        dt = time.perf_counter() - t0
+    return done * setup.grid.ncells, dt, ref
 
 
 def run_reference_arm(args):
@@ -237,10 +218,13 @@ def run_reference_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "path": "reference C++ Hydro::performStep"},
+        "config": {"workload": WORKLOAD % "101x101x51",
+                   "path": "reference C++ Hydro::performStep + Fluid::outputSurface every %d steps"
+                           % SURF_EVERY},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": kind,
-                         "sample": "%d processes, each stepping its own copy of the event for up "
-                                   "to %d steps or %.0f s; %.1f s wall" % (nproc, steps, budget, wall)},
+                         "sample": "%d processes, each stepping its own copy of the event (surface every "
+                                   "%d steps) for up to %d steps or %.0f s; %.1f s wall"
+                                   % (nproc, SURF_EVERY, steps, budget, wall)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -256,7 +240,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--grid", default="101,101,51",
+                    help="nx,ny,nz of the event (smaller grids only for profiler captures)")
     args = ap.parse_args()
+    args.grid = tuple(int(v) for v in args.grid.split(","))
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -264,8 +251,9 @@ def main():
     from vhlle_b200 import workloads as W
 
     ws, rank, local = dist_env()
-    dist = Dist(ws)
-    setup = W.glauber3d_setup(seed=20260001 + rank)
+    dist = Ranks(ws)
+    nx, ny, nz = args.grid
+    setup = W.glauber3d_setup(nx, ny, nz, seed=20260001 + rank)
     cells = setup.grid.ncells
     h = capi.GpuHydro(setup, device=local)
     lps = h.launches_per_step()
@@ -281,13 +269,29 @@ def main():
     dist.barrier()
     h.profile(True)
     h.timer_start()
-    h.step(args.steps)
+    nel = 0
+    for k in range(1, args.steps + 1):
+        h.step(1)
+        if k % SURF_EVERY == 0:
+            nel += h.surface_only()["nelements"]
     ms = h.timer_stop()
     dist.barrier()
     clocks = sampler.stop()
     h.sync()
     prof = h.profile_read()
     h.profile(False)
+    # the surface calls' own share: the same loop again with a CUDA-event
+    # pair around every surface call (vh_surface waits for its result, so
+    # the pair spans the call's kernels and its host round trips)
+    h.upload_initial()
+    h.L.vh_set_tau(h.h, setup.tau0)
+    surf_ms_tot = 0.0
+    for k in range(1, args.steps + 1):
+        h.step(1)
+        if k % SURF_EVERY == 0:
+            h.timer_start()
+            h.surface_only()
+            surf_ms_tot += h.timer_stop()
     ms_max = dist.max(ms)
     value = ws * cells * args.steps / (ms_max / 1e3)
 
@@ -307,6 +311,9 @@ def main():
     step_roofline = {"bound": "hbm", "achieved": step_bw, "peak": peak, "unit": "GB/s",
                      "frac": step_bw / peak, "bytes_per_cell_update": COMPULSORY_B}
     kernels = {k: {"launches": n, "total_ms": t, "share": t / ms} for k, (n, t) in prof.items()}
+    nsurf = args.steps // SURF_EVERY
+    kernels["surface (vh_surface, 9 kernels)"] = {"launches": nsurf, "total_ms": surf_ms_tot,
+                                                   "share": surf_ms_tot / ms, "elements": nel}
 
     # end to end through the C ABI with host-resident state
     e2e = None
@@ -328,35 +335,50 @@ def main():
         h._check(L.vh_download_async(h.h, ctypes.byref(view)))
         h.sync()
         dist.barrier()
+        rec_cap = 400000
+        rec_p = ctypes.c_void_p()
+        h._check(L.vh_alloc_pinned(rec_cap * capi.SURF_REC * 8, ctypes.byref(rec_p)))
+        rec_ptr = ctypes.cast(rec_p, ctypes.POINTER(ctypes.c_double))
+        rec_bytes = 0
         h.timer_start()
-        for _ in range(nE):
+        for k in range(1, nE + 1):
             h._check(L.vh_upload_async(h.h, ctypes.byref(view)))
             h._check(L.vh_step(h.h))
             h._check(L.vh_download_async(h.h, ctypes.byref(view)))
+            if k % SURF_EVERY == 0:
+                n = h.surface_only()["nelements"]
+                got = ctypes.c_long()
+                h._check(L.vh_surface_records(h.h, rec_ptr, rec_cap, ctypes.byref(got)))
+                rec_bytes += min(n, rec_cap) * capi.SURF_REC * 8
         ems = h.timer_stop()
         h.sync()
         ems = dist.max(ems)
         for p, _ in bufs.values():
             L.vh_free_pinned(p)
+        L.vh_free_pinned(rec_p)
         e2e = {"value": ws * cells * nE / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes, "steps": nE}
+               "d2h_bytes_per_step": nbytes + rec_bytes // nE, "steps": nE,
+               "note": "state uploaded and downloaded every step, surface records every %d"
+                       % SURF_EVERY}
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(W.glauber3d_setup(seed=20260001))
+        cpu = cpu_baseline_sample(W.glauber3d_setup(nx, ny, nz, seed=20260001))
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "cells": cells,
-                       "path": "plain FP64 step (no MLP guess, single event per GPU)",
+            "config": {"workload": WORKLOAD % ("x".join(map(str, args.grid))), "cells": cells,
+                       "path": "plain FP64 step + device freeze-out surface every %d steps "
+                               "(no MLP guess, single event per GPU)" % SURF_EVERY,
                        "parallelism": "events%d" % ws,
                        "l2": "inputs larger than L2 (%.0f MB of resident fields)" % (
-                           cells * 8 * 109 / 1e6)},
+                           cells * 8 * 127 / 1e6)},
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
-            "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": lps * args.steps, "clocks": clocks,
+            "e2e": e2e, "cpu_baseline": cpu,
+            "gpu_launches": lps * args.steps + 9 * (args.steps // SURF_EVERY), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     h.close()

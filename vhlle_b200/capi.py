@@ -294,6 +294,13 @@ class GpuHydro:
                                                   ctypes.byref(got)))
         return rec, {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
 
+    def surface_only(self, ecrit=None):
+        """vh_surface without copying the records: the info dict."""
+        info = VhSurfaceInfo()
+        ec = self.setup.ecrit if ecrit is None else ecrit
+        self._check(self.L.vh_surface(self.h, ec, ctypes.byref(info)))
+        return {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+
     def surface_write(self, path, extend=False):
         self._check(self.L.vh_surface_write(self.h, path.encode(), int(extend)))
 
