@@ -125,6 +125,59 @@ vh_status vh_get_dtau(vh_ctx *ctx, double *dt);
 vh_status vh_get_tau(vh_ctx *ctx, double *tau);
 vh_status vh_set_tau(vh_ctx *ctx, double tau);
 
+/* The con2prim (transformPV, src/rmn.cpp:28-139) stopping tolerance on
+ * |dv| for every root find of the context: the reference's 1e-5 by default.
+ * A tighter value (down to round-off, e.g. 1e-13) makes the result
+ * independent of the start point, which is what a learned start point
+ * (vh_set_con2prim_guess) needs to stay within 1e-8 of the tight oracle.
+ * No counterpart in the reference (its tolerance is a literal). */
+vh_status vh_set_con2prim(vh_ctx *ctx, double tol);
+
+/* The learned con2prim start point.  A vh_mlp is a 4 -> 64 -> 64 -> 3
+ * network (SiLU; BF16 weights and activations, FP32 accumulation) from the
+ * features x = (0.1 ln T^00, min(|T^0i|/T^00, 1.5), J^0/T^00,
+ * [|T^0i| > T^00]) of T^0mu = Q/tau to (e/T^00, |v|, nb/T^00).  Attached to
+ * a context, it runs once per step over every cell (tensor-core tiles) and
+ * its |v| becomes the start point of every con2prim root find of that cell
+ * in the step; the FP64 safeguarded Newton / bisection still finishes each
+ * solve to the context's tolerance, so only the iteration count changes.
+ * Use it with a tight tolerance (vh_set_con2prim): at the reference's 1e-5
+ * the result depends on the start point.  No counterpart in the reference.
+ *
+ * Parameters (VH_MLP_PARAMS floats): W1[64][4], b1[64], W2[64][64], b2[64],
+ * W3[3][64], b3[3].  vh_mlp_samples writes features X[n][4] and labels
+ * Y[n][3] (from the root converged to 1e-13) of every cell of a context
+ * with a state into device arrays; vh_mlp_train runs epochs of Adam with a
+ * cosine-decayed step on the weighted squared error (weights 1, 4, 1) with
+ * the project's own forward / backward kernels and writes each epoch's mean
+ * loss to epoch_loss[epochs] (may be NULL); vh_mlp_grad gives the gradient
+ * of the mean loss over n samples (for checks); vh_mlp_forward evaluates
+ * the inference path.  X, Y are device pointers.  Errors of the vh_mlp_*
+ * calls that take no context are described by vh_mlp_last_error(). */
+#define VH_MLP_PARAMS 4675
+typedef struct vh_mlp vh_mlp;
+vh_status vh_mlp_create(int device, unsigned long long seed, vh_mlp **out);
+vh_status vh_mlp_destroy(vh_mlp *mlp);
+vh_status vh_mlp_set_params(vh_mlp *mlp, const float *params);
+vh_status vh_mlp_get_params(vh_mlp *mlp, float *params);
+vh_status vh_mlp_forward(vh_mlp *mlp, const float *X, long n, float *Y);
+vh_status vh_mlp_grad(vh_mlp *mlp, const float *X, const float *Y, long n,
+                      float *grad, float *loss);
+vh_status vh_mlp_train(vh_mlp *mlp, const float *X, const float *Y, long n,
+                       int batch, int epochs, float lr, unsigned long long seed,
+                       float *epoch_loss);
+const char *vh_mlp_last_error(void);
+vh_status vh_mlp_samples(vh_ctx *ctx, float *X, float *Y, long cap, long *n);
+/* Attaches (mlp != NULL) or detaches the start-point network; the context
+ * does not own it (destroy it after the context stops using it). */
+vh_status vh_set_con2prim_guess(vh_ctx *ctx, vh_mlp *mlp);
+
+/* Counts of con2prim root finds and their iterations since the previous
+ * call (read, then reset); enable = 1 keeps counting (slower: two atomics
+ * per root find), 0 stops.  For measurements, not production steps. */
+vh_status vh_con2prim_stats(vh_ctx *ctx, int enable, unsigned long long *calls,
+                            unsigned long long *iters);
+
 /* The grid the context currently evolves: the creation grid, or the one
  * vh_resize2x made, whose bounds are derived from the old grid's first and
  * last cell coordinates exactly as expandGrid2x does. */

@@ -40,7 +40,8 @@ class _Grid(ctypes.Structure):
 class _Eos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
-                ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp)]
+                ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
+                ("tol", ctypes.c_double)]
 
 
 class _Trc(ctypes.Structure):
@@ -223,11 +224,14 @@ def _trc(setup):
 class OracleRun:
     """The C restatement driven like Hydro: step() == performStep()."""
 
-    def __init__(self, setup):
+    def __init__(self, setup, tol=None):
+        """tol: the transformPV stopping tolerance (None: the reference's
+        1e-5; a smaller value gives the tight-tolerance oracle)."""
         self.setup = setup
         g = setup.grid
         self.grid = _Grid(g.nx, g.ny, g.nz, *g.bounds())
         self.eos = _EosHolder(setup.eos)
+        self.eos.s.tol = 0.0 if tol is None else float(tol)
         self.trc = _trc(setup)
         self.state = initial_state(setup)
         self.tau = ctypes.c_double(setup.tau0)

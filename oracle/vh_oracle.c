@@ -190,7 +190,7 @@ static void transform_pv(const or_eos *E, double Q[7], double *e, double *p,
       dv = f / df;
       v -= dv;
     }
-    if (fabs(dv) < 0.00001) break;
+    if (fabs(dv) < (E->tol > 0. ? E->tol : 0.00001)) break;
     *e = Q[T_] - M * v;
     if (*e < 0.) *e = 0.;
     *nb = Q[NB_] * sqrt(1 - v * v);

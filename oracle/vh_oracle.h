@@ -36,6 +36,10 @@ typedef struct or_eos {
   double conf_cnst;
   int ne, nn;
   const double *egrid, *ngrid, *p, *T, *mub;
+  /* transformPV stopping tolerance on |dv|; 0 means the reference's 1e-5
+   * (src/rmn.cpp:96).  A smaller value gives the tight-tolerance oracle the
+   * learned-guess path is checked against. */
+  double tol;
 } or_eos;
 
 /* TransportCoeff (src/trancoeff.h:6-45) public constants */

@@ -29,7 +29,10 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_records",
-           "vh_surface_device", "vh_surface_write", "vh_cornelius4d")
+           "vh_surface_device", "vh_surface_write", "vh_cornelius4d", "vh_set_con2prim",
+           "vh_con2prim_stats", "vh_mlp_create", "vh_mlp_destroy", "vh_mlp_set_params",
+           "vh_mlp_get_params", "vh_mlp_forward", "vh_mlp_grad", "vh_mlp_train",
+           "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess")
 
 
 class VhError(RuntimeError):
@@ -62,6 +65,83 @@ def cornelius4d(cubes, dx, e0, device=0):
     if st != VH_OK:
         raise VhError(st, L.vh_last_error(None).decode())
     return counts, cent, norm
+
+
+MLP_PARAMS = 4675
+
+
+def _tensor_ptr(t, dtype_name, shape):
+    """Device pointer of a contiguous CUDA tensor of the given dtype and shape."""
+    import torch
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.is_contiguous()):
+        raise ValueError("need a contiguous CUDA tensor")
+    if str(t.dtype) != "torch." + dtype_name or tuple(t.shape[1:]) != tuple(shape[1:]):
+        raise ValueError("need a %s tensor of shape %s" % (dtype_name, shape))
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class Mlp:
+    """The learned con2prim start point (vh_mlp_*): 4 -> 64 -> 64 -> 3."""
+
+    def __init__(self, device: int = 0, seed: int = 1):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        st = self.L.vh_mlp_create(device, seed, ctypes.byref(h))
+        if st != VH_OK:
+            raise VhError(st, self.L.vh_mlp_last_error().decode())
+        self.h = h
+        self.device = device
+
+    def _check(self, st):
+        if st != VH_OK:
+            raise VhError(st, self.L.vh_mlp_last_error().decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.vh_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(MLP_PARAMS, dtype=np.float32)
+        self._check(self.L.vh_mlp_get_params(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32).reshape(MLP_PARAMS)
+        self._check(self.L.vh_mlp_set_params(self.h, p.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+
+    def forward(self, X):
+        """X: CUDA float32 [n, 4] -> CUDA float32 [n, 3] (tensor-core path)."""
+        import torch
+        n = X.shape[0]
+        Y = torch.empty((n, 3), dtype=torch.float32, device=X.device)
+        self._check(self.L.vh_mlp_forward(self.h, _tensor_ptr(X, "float32", (n, 4)), n,
+                                          _tensor_ptr(Y, "float32", (n, 3))))
+        return Y
+
+    def grad(self, X, Y):
+        n = X.shape[0]
+        g = np.zeros(MLP_PARAMS, dtype=np.float32)
+        loss = ctypes.c_float()
+        fp = ctypes.POINTER(ctypes.c_float)
+        self._check(self.L.vh_mlp_grad(self.h, _tensor_ptr(X, "float32", (n, 4)),
+                                       _tensor_ptr(Y, "float32", (n, 3)), n, g.ctypes.data_as(fp),
+                                       ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, X, Y, batch=16384, epochs=10, lr=3e-3, seed=1):
+        n = X.shape[0]
+        losses = np.zeros(epochs, dtype=np.float32)
+        self._check(self.L.vh_mlp_train(self.h, _tensor_ptr(X, "float32", (n, 4)),
+                                        _tensor_ptr(Y, "float32", (n, 3)), n, batch, epochs, lr,
+                                        seed, losses.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return losses
 
 
 class VhGrid(ctypes.Structure):
@@ -151,6 +231,21 @@ def lib():
     L.vh_surface_records.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.vh_set_con2prim.argtypes = [vp, ctypes.c_double]
+    L.vh_con2prim_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
+                                    ctypes.POINTER(ctypes.c_ulonglong)]
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.vh_mlp_create.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(vp)]
+    L.vh_mlp_destroy.argtypes = [vp]
+    L.vh_mlp_set_params.argtypes = [vp, fp]
+    L.vh_mlp_get_params.argtypes = [vp, fp]
+    L.vh_mlp_forward.argtypes = [vp, vp, ctypes.c_long, vp]
+    L.vh_mlp_grad.argtypes = [vp, vp, vp, ctypes.c_long, fp, fp]
+    L.vh_mlp_train.argtypes = [vp, vp, vp, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                               ctypes.c_float, ctypes.c_ulonglong, fp]
+    L.vh_mlp_last_error.restype = ctypes.c_char_p
+    L.vh_mlp_samples.argtypes = [vp, vp, vp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
+    L.vh_set_con2prim_guess.argtypes = [vp, vp]
     L.vh_cornelius4d.argtypes = [_dp, ctypes.c_long, _dp, ctypes.c_double, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), _dp, _dp]
     _lib = L
@@ -293,6 +388,27 @@ class GpuHydro:
             self._check(self.L.vh_surface_records(self.h, rec.ctypes.data_as(_dp), n,
                                                   ctypes.byref(got)))
         return rec, {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+
+    def set_con2prim(self, tol):
+        self._check(self.L.vh_set_con2prim(self.h, tol))
+
+    def con2prim_stats(self, enable=True):
+        """(calls, iterations) since the last call; keeps counting if enable."""
+        c, it = ctypes.c_ulonglong(), ctypes.c_ulonglong()
+        self._check(self.L.vh_con2prim_stats(self.h, int(enable), ctypes.byref(c), ctypes.byref(it)))
+        return c.value, it.value
+
+    def mlp_samples(self, X, Y):
+        """Features and tight labels of every cell into CUDA tensors X [cap, 4],
+        Y [cap, 3]; returns the number written."""
+        cap = X.shape[0]
+        n = ctypes.c_long()
+        self._check(self.L.vh_mlp_samples(self.h, _tensor_ptr(X, "float32", (cap, 4)),
+                                          _tensor_ptr(Y, "float32", (cap, 3)), cap, ctypes.byref(n)))
+        return n.value
+
+    def set_con2prim_guess(self, mlp):
+        self._check(self.L.vh_set_con2prim_guess(self.h, mlp.h if mlp is not None else None))
 
     def surface_only(self, ecrit=None):
         """vh_surface without copying the records: the info dict."""

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/vhlle_b200.h"
+#include "vh_mlp.cuh"
 #include "vh_step.cuh"
 #include "vh_surface.cuh"
 
@@ -41,6 +42,10 @@ struct vh_ctx {
   double* tot_partial = nullptr;  // [blocks][16] block sums of the totals
   double* tot_out = nullptr;      // [16]
   double* resize_tmp = nullptr;   // [10][N] staging of the resize gather
+  unsigned long long* c2p_stats = nullptr;  // [2] con2prim calls, iterations
+  vh_mlp* mlp = nullptr;           // learned con2prim start point (not owned)
+  float* vguess = nullptr;         // [N] per-cell start points of the step
+  unsigned long long* ucount = nullptr;
   // the Fluid's construction-time step: the time side of the freeze-out
   // hypercubes (src/fld.cpp:106-108); set at creation, doubled by the resize
   double fluid_dt = 0.;
@@ -332,6 +337,9 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   }
   c->eos.kind = eos->kind;
   c->eos.conf_cnst = eos->conf_cnst;
+  c->eos.tol = 0.00001;  // src/rmn.cpp:96
+  c->eos.vguess = nullptr;
+  c->eos.stats = nullptr;
   if (eos->kind == VH_EOS_TABLE) {
     const int ne = eos->ne, nn = eos->nn;
     double* buf = nullptr;
@@ -449,6 +457,11 @@ vh_status vh_step(vh_ctx* ctx) {
   vh::StepArgs a;
   a.g = ctx->g;
   a.eos = ctx->eos;
+  a.eos.vguess = nullptr;
+  if (ctx->mlp) {  // start points for this step's root finds from Q at tau
+    vh::launch_mlp_guess(ctx->mlp->packed, ctx->f.Q, ctx->g.N, ctx->tau, ctx->vguess, ctx->stream);
+    a.eos.vguess = ctx->vguess;
+  }
   a.tr = ctx->tr;
   a.f = ctx->f;
   a.tau = ctx->tau;
@@ -501,6 +514,68 @@ vh_status vh_get_tau(vh_ctx* ctx, double* tau) {
 vh_status vh_set_tau(vh_ctx* ctx, double tau) {
   if (!ctx) return VH_ERR_ARG;
   ctx->tau = tau;
+  return VH_OK;
+}
+
+vh_status vh_set_con2prim(vh_ctx* ctx, double tol) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!(tol > 0.) || !(tol <= 0.00001))
+    return fail(ctx, VH_ERR_ARG, "vh_set_con2prim: tol must be in (0, 1e-5]");
+  ctx->eos.tol = tol;
+  return VH_OK;
+}
+
+vh_status vh_set_con2prim_guess(vh_ctx* ctx, vh_mlp* mlp) {
+  if (!ctx) return VH_ERR_ARG;
+  if (mlp && mlp->device != ctx->device)
+    return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_guess: the network lives on another device");
+  if (mlp && !ctx->vguess) {
+    VH_CUDA(ctx, cudaSetDevice(ctx->device));
+    vh_status st = dalloc(ctx, &ctx->vguess, (size_t)ctx->g.N);
+    if (st != VH_OK) return st;
+  }
+  ctx->mlp = mlp;
+  return VH_OK;
+}
+
+vh_status vh_mlp_samples(vh_ctx* ctx, float* X, float* Y, long cap, long* n) {
+  if (!ctx || cap < 0 || (cap > 0 && (!X || !Y))) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_mlp_samples: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->ucount) {
+    vh_status st = dalloc(ctx, &ctx->ucount, 1);
+    if (st != VH_OK) return st;
+  }
+  VH_CUDA(ctx, cudaMemsetAsync(ctx->ucount, 0, sizeof(unsigned long long), ctx->stream));
+  vh::EosDev E = ctx->eos;
+  E.tol = 1e-13;  // labels from the root converged to round-off
+  E.vguess = nullptr;
+  E.stats = nullptr;
+  vh::launch_mlp_samples(E, ctx->f.Q, ctx->g.N, ctx->tau, X, Y, cap, ctx->ucount, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
+  unsigned long long h = 0;
+  VH_CUDA(ctx, cudaMemcpyAsync(&h, ctx->ucount, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (n) *n = (long)std::min<unsigned long long>(h, (unsigned long long)cap);
+  return VH_OK;
+}
+
+vh_status vh_con2prim_stats(vh_ctx* ctx, int enable, unsigned long long* calls,
+                            unsigned long long* iters) {
+  if (!ctx) return VH_ERR_ARG;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->c2p_stats) {
+    vh_status st = dalloc(ctx, &ctx->c2p_stats, 2);
+    if (st != VH_OK) return st;
+    VH_CUDA(ctx, cudaMemsetAsync(ctx->c2p_stats, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  }
+  unsigned long long h[2] = {0, 0};
+  VH_CUDA(ctx, cudaMemcpyAsync(h, ctx->c2p_stats, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (calls) *calls = h[0];
+  if (iters) *iters = h[1];
+  VH_CUDA(ctx, cudaMemsetAsync(ctx->c2p_stats, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  ctx->eos.stats = enable ? ctx->c2p_stats : nullptr;
   return VH_OK;
 }
 
@@ -611,7 +686,8 @@ vh_status vh_sync(vh_ctx* ctx) {
 
 vh_status vh_launches_per_step(vh_ctx* ctx, int* n) {
   if (!ctx || !n) return VH_ERR_ARG;
-  int k = 1 + 2 * (2 + (ctx->g.nz > 1 ? 1 : 0) + 1) + 1 + (ctx->viscous ? 4 : 0) + 1;
+  int k = 1 + 2 * (2 + (ctx->g.nz > 1 ? 1 : 0) + 1) + 1 + (ctx->viscous ? 4 : 0) + 1 +
+          (ctx->mlp ? 1 : 0);
   *n = k;
   return VH_OK;
 }

@@ -162,6 +162,9 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.eos.mub = eos_dev->mub;
   a.eos.emode = a.eos.nmode = vh::GRID_BSEARCH;  // the table stays on the device
   a.eos.e0 = a.eos.einv = a.eos.n0 = a.eos.ninv = 0.f;
+  a.eos.tol = 0.00001;  // src/rmn.cpp:96
+  a.eos.vguess = nullptr;
+  a.eos.stats = nullptr;
   a.tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
                    tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
                    tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,

@@ -39,7 +39,18 @@ struct EosDev {
   int emode, nmode;    // GRID_* per axis
   float e0, einv;      // guess: (f(x) - e0) * einv, f = log2 or identity
   float n0, ninv;
+  // con2prim policy (not part of the EoS proper, but passed everywhere with
+  // it): stop when |dv| < tol (the reference's 0.00001 by default); vguess,
+  // when set, holds a start point in (0, 1) per cell for the root find; stats,
+  // when set, counts calls [0] and iterations [1].
+  double tol;
+  const float* __restrict__ vguess;
+  unsigned long long* stats;
 };
+
+__device__ __forceinline__ float c2p_guess(const EosDev& E, long long i) {
+  return E.vguess ? E.vguess[i] : -1.f;
+}
 
 struct TrDev {
   double etaS0, zetaS0, ah, al, aRho, T0, etaSMin, etaSEpsilonMin,
@@ -216,8 +227,12 @@ __device__ __forceinline__ double eos_s(const EosDev& E, double e, double nb,
 
 // ----------------------------------------------------------- transformPV
 // src/rmn.cpp:28-139.  Q is the caller's copy and is rescaled in place when
-// |M| > Q_t, exactly as the reference does.
-__device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim& o) {
+// |M| > Q_t, exactly as the reference does.  With a start point g in (0, 1)
+// (a learned guess) the iteration starts there instead of at 0.5 and the
+// bracket is narrowed by the sign of f at g; the safeguarded Newton /
+// bisection then runs as in the reference until |dv| < E.tol.
+__device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim& o,
+                                             float g = -1.f) {
   const int MAXIT = 100;
   const double dpe = 1. / 3.;
   const double corrf = 0.9999;
@@ -243,7 +258,8 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     M = Q[T_] * corrf;
   }
   double e, p, nb, nq, ns;
-  v = 0.5 * (vl + vh);
+  const bool guessed = g > 0.f && g < 1.f;
+  v = guessed ? (double)g : 0.5 * (vl + vh);
   e = Q[T_] - M * v;
   if (e < 0.) e = 0.;
   {
@@ -255,9 +271,17 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
   p = eos_p(E, e, nb);
   f = (Q[T_] + p) * v - M;
   df = (Q[T_] + p) - M * v * dpe;
+  if (guessed) {
+    if (f > 0.)
+      vh = v;
+    else
+      vl = v;
+  }
   dvold = vh - vl;
   dv = dvold;
+  int it = 0;
   for (int i = 0; i < MAXIT; i++) {
+    it = i + 1;
     if ((f + df * (vh - v)) * (f + df * (vl - v)) >= 0. ||
         fabs(2. * f) > fabs(dvold * df)) {
       dvold = dv;
@@ -268,7 +292,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
       dv = ddiv(f, df);
       v -= dv;
     }
-    if (fabs(dv) < 0.00001) break;
+    if (fabs(dv) < E.tol) break;
     e = Q[T_] - M * v;
     if (e < 0.) e = 0.;
     const double sq = sqrt(1 - v * v);
@@ -282,6 +306,10 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
       vh = v;
     else
       vl = v;
+  }
+  if (E.stats) {
+    atomicAdd(&E.stats[0], 1ull);
+    atomicAdd(&E.stats[1], (unsigned long long)it);
   }
   o.vx = ddivp(v * Q[X_], M);
   o.vy = ddivp(v * Q[Y_], M);

@@ -100,8 +100,8 @@ __global__ void __launch_bounds__(128) k_face(Geo g, EosDev E, const double* __r
     qr[k] = ddivp(c - dQr, tau);
   }
   Prim pl, pr;
-  transform_pv(E, ql, pl);
-  transform_pv(E, qr, pr);
+  transform_pv(E, ql, pl, c2p_guess(E, L));
+  transform_pv(E, qr, pr, c2p_guess(E, R));
   const double dxdir = DIR == X_ ? g.dx : (DIR == Y_ ? g.dy : g.dz);
   double fl[7];
   unsigned e = 0;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(128) k_update(Geo g, EosDev E, double* __restr
     q[k] = ddivp(qin[k], tau1);
   }
   Prim pp;
-  transform_pv(E, q, pp);
+  transform_pv(E, q, pp, c2p_guess(E, i));
   double kk[7];
   kk[T_] = -q[T_] * pp.vz * pp.vz - pp.p * (1. + pp.vz * pp.vz);
   kk[X_] = 0.;
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, TrDev tr,
 #pragma unroll
   for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tA);
   Prim a;
-  transform_pv(E, q, a);
+  transform_pv(E, q, a, c2p_guess(E, i));
   pA[0 * N + i] = a.e;
   pA[1 * N + i] = a.p;
   pA[2 * N + i] = a.nb;
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, TrDev tr,
 #pragma unroll
   for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tau);
   Prim d;
-  transform_pv(E, q, d);
+  transform_pv(E, q, d, c2p_guess(E, i));
   pD[0 * N + i] = d.e;
   pD[1 * N + i] = d.vx;
   pD[2 * N + i] = d.vy;
@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, TrDev tr,
 #pragma unroll
     for (int k = 0; k < 7; k++) q[k] = ddivp(src[k * N + i], tt);
     Prim P;
-    transform_pv(E, q, P);
+    transform_pv(E, q, P, c2p_guess(E, i));
     const double ut = 1.0 / sqrt(1.0 - P.vx * P.vx - P.vy * P.vy - P.vz * P.vz);
     const int o = w == 0 ? 0 : 5;
     pBC[(o + 0) * N + i] = ut;
