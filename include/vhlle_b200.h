@@ -267,6 +267,35 @@ vh_status vh_surface_write(vh_ctx *ctx, const char *path, int extendFO);
 vh_status vh_cornelius4d(const double *cubes, long n, const double *dx, double e0,
                          int device, int *counts, double *cent, double *norm);
 
+/* Many independent events advanced together (no counterpart in the
+ * reference, which runs one event per process).  The batch holds contexts
+ * it does not own, all on one device and uploaded; vh_batch_advance runs
+ * one iteration of the driver loop for every event -- its substep block
+ * (src/main.cpp:405-419, from the event's driver parameters) and, once tau
+ * reaches the event's tau_resize, the x2 resize (src/main.cpp:423-427) --
+ * as one CUDA graph in which every event is an independent branch.  The
+ * graph is captured once per shape (substep counts, buffer parity, launch
+ * configuration, context settings) and replayed; results are bit-identical
+ * to advancing each context alone with vh_advance / vh_resize2x.
+ * vh_batch_set_driver sets an event's (k >= 0) or every event's (k < 0)
+ * dtau, eta range, nz and tau_resize (defaults: the context's step and grid,
+ * no resize).  vh_batch_tune(b, 1) times the next iterations under each
+ * launch configuration (capture streams, block size) and keeps the fastest.
+ * Set every context (tolerance, network, stream counters) before advancing;
+ * a change is picked up by re-capturing.  vh_batch_sync waits and ORs the
+ * events' device error words (VH_ERR_NUMERIC if any is set).  Errors of
+ * batch calls are described by vh_batch_last_error(). */
+typedef struct vh_batch vh_batch;
+vh_status vh_batch_create(vh_ctx *const *ctxs, int n, vh_batch **out);
+vh_status vh_batch_destroy(vh_batch *batch);
+vh_status vh_batch_set_driver(vh_batch *batch, int k, double dtau, double etamin,
+                              double etamax, int nz, double tau_resize);
+vh_status vh_batch_tune(vh_batch *batch, int enable);
+vh_status vh_batch_advance(vh_batch *batch, int *nsub_max);
+vh_status vh_batch_sync(vh_batch *batch, unsigned *error_bits);
+vh_status vh_batch_info(vh_batch *batch, int *captures, int *nstreams, int *block);
+const char *vh_batch_last_error(void);
+
 /* Device timing with CUDA events recorded on the context's stream.
  * vh_timer_stop waits for the stop event and returns the elapsed time. */
 vh_status vh_timer_start(vh_ctx *ctx);

@@ -32,7 +32,9 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_surface_device", "vh_surface_write", "vh_cornelius4d", "vh_set_con2prim",
            "vh_con2prim_stats", "vh_mlp_create", "vh_mlp_destroy", "vh_mlp_set_params",
            "vh_mlp_get_params", "vh_mlp_forward", "vh_mlp_grad", "vh_mlp_train",
-           "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess")
+           "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
+           "vh_batch_destroy", "vh_batch_set_driver", "vh_batch_tune", "vh_batch_advance",
+           "vh_batch_sync", "vh_batch_info", "vh_batch_last_error")
 
 
 class VhError(RuntimeError):
@@ -144,6 +146,56 @@ class Mlp:
         return losses
 
 
+class Batch:
+    """Independent events advanced together (vh_batch_*): one CUDA graph per
+    driver-loop iteration, every event an independent branch."""
+
+    def __init__(self, hydros):
+        self.L = lib()
+        self.hydros = list(hydros)
+        arr = (ctypes.c_void_p * len(self.hydros))(*[h.h.value for h in self.hydros])
+        b = ctypes.c_void_p()
+        self._check(self.L.vh_batch_create(arr, len(self.hydros), ctypes.byref(b)))
+        self.b = b
+
+    def _check(self, st):
+        if st != VH_OK:
+            raise VhError(st, self.L.vh_batch_last_error().decode())
+
+    def set_driver(self, k, dtau, etamin, etamax, nz, tau_resize=float("inf")):
+        self._check(self.L.vh_batch_set_driver(self.b, k, dtau, etamin, etamax, nz, tau_resize))
+
+    def tune(self, enable=True):
+        self._check(self.L.vh_batch_tune(self.b, int(enable)))
+
+    def advance(self, n=1):
+        m = ctypes.c_int()
+        for _ in range(n):
+            self._check(self.L.vh_batch_advance(self.b, ctypes.byref(m)))
+        return m.value
+
+    def sync(self):
+        bits = ctypes.c_uint()
+        self._check(self.L.vh_batch_sync(self.b, ctypes.byref(bits)))
+        return bits.value
+
+    def info(self):
+        c, s, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.L.vh_batch_info(self.b, ctypes.byref(c), ctypes.byref(s), ctypes.byref(b)))
+        return {"captures": c.value, "nstreams": s.value, "block": b.value}
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.L.vh_batch_destroy(self.b)
+            self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class VhGrid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
@@ -246,6 +298,15 @@ def lib():
     L.vh_mlp_last_error.restype = ctypes.c_char_p
     L.vh_mlp_samples.argtypes = [vp, vp, vp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.vh_set_con2prim_guess.argtypes = [vp, vp]
+    L.vh_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+    L.vh_batch_destroy.argtypes = [vp]
+    L.vh_batch_set_driver.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_double]
+    L.vh_batch_tune.argtypes = [vp, ctypes.c_int]
+    L.vh_batch_advance.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    L.vh_batch_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
+    L.vh_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3
+    L.vh_batch_last_error.restype = ctypes.c_char_p
     L.vh_cornelius4d.argtypes = [_dp, ctypes.c_long, _dp, ctypes.c_double, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), _dp, _dp]
     _lib = L

@@ -27,51 +27,7 @@ void launch_fill(double* p, long long n, double v, cudaStream_t s);
 void launch_zero_negative_rows(double* Q, long long N, cudaStream_t s);
 }  // namespace vh
 
-struct vh_ctx {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  vh::Geo g{};
-  vh::EosDev eos{};
-  vh::TrDev tr{};
-  vh::Fields f{};
-  double tau = 0., dt = 0.;
-  bool viscous = false;
-  bool uploaded = false;
-  int launches = 0;
-  vh_grid grid{};
-  double* tot_partial = nullptr;  // [blocks][16] block sums of the totals
-  double* tot_out = nullptr;      // [16]
-  double* resize_tmp = nullptr;   // [10][N] staging of the resize gather
-  unsigned long long* c2p_stats = nullptr;  // [2] con2prim calls, iterations
-  vh_mlp* mlp = nullptr;           // learned con2prim start point (not owned)
-  float* vguess = nullptr;         // [N] per-cell start points of the step
-  unsigned long long* ucount = nullptr;
-  // the Fluid's construction-time step: the time side of the freeze-out
-  // hypercubes (src/fld.cpp:106-108); set at creation, doubled by the resize
-  double fluid_dt = 0.;
-  // surface sums: EtotSurf and vEff are Fluid members (reset by the resize's
-  // new Fluid), nbSurf is a function static in the reference (never reset)
-  double EtotSurf = 0., vEff = 0., nbSurf = 0.;
-  struct Surf {
-    double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
-           *partial = nullptr;
-    int *blk = nullptr, *cubes = nullptr, *cnt = nullptr, *counters = nullptr;
-    size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
-    long long nel = 0;
-  } surf;
-  std::string err;
-  std::vector<void*> allocs;
-  // timers and per-kernel profiling
-  cudaEvent_t t0 = nullptr, t1 = nullptr;
-  bool prof = false;
-  std::vector<cudaEvent_t> evpool;
-  size_t evused = 0;
-  struct Seg {
-    int kind;
-    size_t ev0, ev1;
-  };
-  std::vector<Seg> segs;
-};
+#include "vh_ctx.cuh"
 
 namespace {
 struct EventMarker : vh::LaunchMarker {
@@ -318,6 +274,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     ALLOC(f.Pi0, N);
     ALLOC(f.PiH0, N);
   }
+  ALLOC(c->clk, 2);
   ALLOC(c->tot_partial, (size_t)vh::totals_blocks(g) * vh::kTotals);
   ALLOC(c->tot_out, vh::kTotals);
   const int ng = g.nx + g.ny + g.nz;
@@ -331,7 +288,9 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   ghost_map(g.nz, hsrc.data() + g.nx + g.ny, hdst.data() + g.nx + g.ny);
   if ((e = cudaMemcpy(f.gsrc, hsrc.data(), ng * sizeof(int), cudaMemcpyHostToDevice)) ||
       (e = cudaMemcpy(f.gdst, hdst.data(), ng, cudaMemcpyHostToDevice)) ||
-      (e = cudaMemset(f.err, 0, sizeof(unsigned)))) {
+      (e = cudaMemset(f.err, 0, sizeof(unsigned))) ||
+      (e = cudaMemcpy(c->clk, std::vector<double>{tau0, dt}.data(), 2 * sizeof(double),
+                      cudaMemcpyHostToDevice))) {
     cuda_fail(c, e, "vh_create: upload");
     return bail(VH_ERR_CUDA);
   }
@@ -459,13 +418,12 @@ vh_status vh_step(vh_ctx* ctx) {
   a.eos = ctx->eos;
   a.eos.vguess = nullptr;
   if (ctx->mlp) {  // start points for this step's root finds from Q at tau
-    vh::launch_mlp_guess(ctx->mlp->packed, ctx->f.Q, ctx->g.N, ctx->tau, ctx->vguess, ctx->stream);
+    vh::launch_mlp_guess(ctx->mlp->packed, ctx->f.Q, ctx->g.N, ctx->clk, ctx->vguess, ctx->stream);
     a.eos.vguess = ctx->vguess;
   }
   a.tr = ctx->tr;
   a.f = ctx->f;
-  a.tau = ctx->tau;
-  a.dt = ctx->dt;
+  a.clk = ctx->clk;  // holds (tau, dt): set when the host changes them, advanced per step
   a.viscous = ctx->viscous;
   if (ctx->prof) {
     EventMarker mk(ctx, 0);
@@ -477,6 +435,7 @@ vh_status vh_step(vh_ctx* ctx) {
   } else {
     ctx->launches = vh::launch_step(a, ctx->stream);
   }
+  vh::launch_clock_op(ctx->clk, 0, 0, ctx->stream);  // tau += dt on the device
   VH_CUDA(ctx, cudaGetLastError());
   std::swap(ctx->f.m, ctx->f.m2);
   ctx->tau += ctx->dt;  // src/hdo.cpp:1095
@@ -496,6 +455,9 @@ vh_status vh_set_dtau(vh_ctx* ctx, double dt) {
   if (!(dt > 0.) || dt > ctx->g.dx / 2. || dt > ctx->g.dy / 2.)
     return fail(ctx, VH_ERR_ARG, "vh_set_dtau: too big delta_tau (dt > dx/2 or dy/2)");
   ctx->dt = dt;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::launch_clock_set(ctx->clk, ctx->tau, ctx->dt, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
   return VH_OK;
 }
 
@@ -514,6 +476,9 @@ vh_status vh_get_tau(vh_ctx* ctx, double* tau) {
 vh_status vh_set_tau(vh_ctx* ctx, double tau) {
   if (!ctx) return VH_ERR_ARG;
   ctx->tau = tau;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::launch_clock_set(ctx->clk, ctx->tau, ctx->dt, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
   return VH_OK;
 }
 
@@ -522,6 +487,7 @@ vh_status vh_set_con2prim(vh_ctx* ctx, double tol) {
   if (!(tol > 0.) || !(tol <= 0.00001))
     return fail(ctx, VH_ERR_ARG, "vh_set_con2prim: tol must be in (0, 1e-5]");
   ctx->eos.tol = tol;
+  ctx->version++;
   return VH_OK;
 }
 
@@ -535,6 +501,7 @@ vh_status vh_set_con2prim_guess(vh_ctx* ctx, vh_mlp* mlp) {
     if (st != VH_OK) return st;
   }
   ctx->mlp = mlp;
+  ctx->version++;
   return VH_OK;
 }
 
@@ -576,6 +543,7 @@ vh_status vh_con2prim_stats(vh_ctx* ctx, int enable, unsigned long long* calls,
   if (iters) *iters = h[1];
   VH_CUDA(ctx, cudaMemsetAsync(ctx->c2p_stats, 0, 2 * sizeof(unsigned long long), ctx->stream));
   ctx->eos.stats = enable ? ctx->c2p_stats : nullptr;
+  ctx->version++;
   return VH_OK;
 }
 
@@ -647,8 +615,11 @@ vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
   g.dy = ndy;
   g.dz = ndz;
   ctx->dt = dt2;  // src/main.cpp:268
+  vh::launch_clock_set(ctx->clk, ctx->tau, ctx->dt, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
   ctx->fluid_dt = dt2;  // the new Fluid's step, src/main.cpp:254-256
   ctx->EtotSurf = ctx->vEff = 0.;  // members of the new Fluid, src/fld.cpp:110-111
+  ctx->version++;
   if (resized) *resized = 1;
   return VH_OK;
 }
@@ -687,7 +658,7 @@ vh_status vh_sync(vh_ctx* ctx) {
 vh_status vh_launches_per_step(vh_ctx* ctx, int* n) {
   if (!ctx || !n) return VH_ERR_ARG;
   int k = 1 + 2 * (2 + (ctx->g.nz > 1 ? 1 : 0) + 1) + 1 + (ctx->viscous ? 4 : 0) + 1 +
-          (ctx->mlp ? 1 : 0);
+          (ctx->mlp ? 1 : 0) + 1;  // + the clock
   *n = k;
   return VH_OK;
 }

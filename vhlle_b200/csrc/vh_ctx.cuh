@@ -1,0 +1,60 @@
+// vh_ctx.cuh -- the context behind the C ABI's opaque vh_ctx (one grid on
+// one GPU), shared by the ABI implementation files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/vhlle_b200.h"
+#include "vh_mlp.cuh"
+#include "vh_step.cuh"
+
+struct vh_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  vh::Geo g{};
+  vh::EosDev eos{};
+  vh::TrDev tr{};
+  vh::Fields f{};
+  double tau = 0., dt = 0.;
+  bool viscous = false;
+  bool uploaded = false;
+  int launches = 0;
+  vh_grid grid{};
+  double* tot_partial = nullptr;  // [blocks][16] block sums of the totals
+  double* tot_out = nullptr;      // [16]
+  double* resize_tmp = nullptr;   // [10][N] staging of the resize gather
+  double* clk = nullptr;          // [2] device clock (tau, dt) the step kernels read
+  unsigned long long* c2p_stats = nullptr;  // [2] con2prim calls, iterations
+  int version = 0;  // bumped by every change a captured step bakes in
+  vh_mlp* mlp = nullptr;           // learned con2prim start point (not owned)
+  float* vguess = nullptr;         // [N] per-cell start points of the step
+  unsigned long long* ucount = nullptr;
+  // the Fluid's construction-time step: the time side of the freeze-out
+  // hypercubes (src/fld.cpp:106-108); set at creation, doubled by the resize
+  double fluid_dt = 0.;
+  // surface sums: EtotSurf and vEff are Fluid members (reset by the resize's
+  // new Fluid), nbSurf is a function static in the reference (never reset)
+  double EtotSurf = 0., vEff = 0., nbSurf = 0.;
+  struct Surf {
+    double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
+           *partial = nullptr;
+    int *blk = nullptr, *cubes = nullptr, *cnt = nullptr, *counters = nullptr;
+    size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
+    long long nel = 0;
+  } surf;
+  std::string err;
+  std::vector<void*> allocs;
+  // timers and per-kernel profiling
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  bool prof = false;
+  std::vector<cudaEvent_t> evpool;
+  size_t evused = 0;
+  struct Seg {
+    int kind;
+    size_t ev0, ev1;
+  };
+  std::vector<Seg> segs;
+};

@@ -209,7 +209,9 @@ __global__ void __launch_bounds__(kMlpBlock) k_mlp_forward(const uint32_t* __res
 // into (0, 1); -1 (no guess) where the state has no root to find.
 __global__ void __launch_bounds__(kMlpBlock) k_mlp_guess(const uint32_t* __restrict__ Wg,
                                                          const double* __restrict__ Q, long long N,
-                                                         double tau, float* __restrict__ vg) {
+                                                         const double* __restrict__ clk,
+                                                         float* __restrict__ vg) {
+  const double tau = clk[0];
   __shared__ uint32_t W[kPackWords];
   __shared__ float feat[kMlpBlock / 32][16][4];
   __shared__ unsigned char okv[kMlpBlock / 32][16];
@@ -409,12 +411,12 @@ void launch_mlp_forward(const uint32_t* W, const float* X, long long n, float* Y
   if (blocks > 0) k_mlp_forward<<<(unsigned)blocks, kMlpBlock, 0, s>>>(W, X, n, Y);
 }
 
-void launch_mlp_guess(const uint32_t* W, const double* Q, long long N, double tau, float* vg,
+void launch_mlp_guess(const uint32_t* W, const double* Q, long long N, const double* clk, float* vg,
                       cudaStream_t s) {
   const long long tiles = (N + 15) / 16;
   long long blocks = (tiles + 3) / 4;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  if (blocks > 0) k_mlp_guess<<<(unsigned)blocks, kMlpBlock, 0, s>>>(W, Q, N, tau, vg);
+  if (blocks > 0) k_mlp_guess<<<(unsigned)blocks, kMlpBlock, 0, s>>>(W, Q, N, clk, vg);
 }
 
 void launch_mlp_samples(const EosDev& E, const double* Q, long long N, double tau, float* X,

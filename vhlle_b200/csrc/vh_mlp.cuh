@@ -16,7 +16,8 @@ int mlp_pack_words();
 size_t mlp_grad_smem();
 void launch_mlp_pack(const float* P, uint32_t* packed, cudaStream_t s);
 void launch_mlp_forward(const uint32_t* W, const float* X, long long n, float* Y, cudaStream_t s);
-void launch_mlp_guess(const uint32_t* W, const double* Q, long long N, double tau, float* vg,
+// tau from the device clock clk[0]
+void launch_mlp_guess(const uint32_t* W, const double* Q, long long N, const double* clk, float* vg,
                       cudaStream_t s);
 void launch_mlp_samples(const EosDev& E, const double* Q, long long N, double tau, float* X,
                         float* Y, long long cap, unsigned long long* count, cudaStream_t s);

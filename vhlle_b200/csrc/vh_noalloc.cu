@@ -170,12 +170,12 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
                    tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,
                    tr->zetaSSigmaPlus, tr->etaSparam, tr->zetaSparam};
   a.viscous = tr->etaS0 > 0. || tr->zetaS0 > 0. || tr->etaSparam > 0 || tr->zetaSparam > 0;
-  a.tau = tau;
-  a.dt = dt;
 
-  // scratch layout: [err | ghost src maps | ghost dst flags | pad][doubles...]
+  // scratch layout: [err, clock | ghost src maps | ghost dst flags | pad][doubles...]
   vh::Fields& f = a.f;
   f.err = reinterpret_cast<unsigned*>(base);
+  double* clk = reinterpret_cast<double*>(base + 16);
+  a.clk = clk;
   f.gsrc = reinterpret_cast<int*>(base + 256);
   f.gdst = base + 256 + 3 * kMaxDim * sizeof(int);
   double* d = reinterpret_cast<double*>(base + kHeaderAligned);
@@ -226,6 +226,7 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
       (e = cudaMemsetAsync(f.err, 0, sizeof(unsigned), st)))
     return cfail(e, "scratch initialisation");
 
+  vh::launch_clock_set(clk, tau, dt, st);
   vh::launch_step(a, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cfail(e, "kernel launch");
   // the updated fill fractions go back into the caller's array

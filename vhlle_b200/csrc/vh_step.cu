@@ -22,7 +22,8 @@ namespace vh {
 // -------------------------------------------------------------- updateM
 // Fluid::updateM, src/fld.cpp:384-423 (both passes; out of place).
 __global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restrict__ mo,
-                           double tau, double dt) {
+                           const double* __restrict__ clk) {
+  const double tau = clk[0], dt = clk[1];  // the step's clock (device)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
@@ -66,8 +67,9 @@ __global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restri
 template <int DIR, bool PRED>
 __global__ void __launch_bounds__(128) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
                                               const double* __restrict__ m,
-                                              double* __restrict__ F, double tau, double dt,
+                                              double* __restrict__ F, const double* __restrict__ clk,
                                               unsigned* err) {
+  const double tau = clk[0], dt = clk[1];  // the step's clock (device)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
@@ -122,8 +124,8 @@ __global__ void __launch_bounds__(128) k_update(Geo g, EosDev E, double* __restr
                                                 double* __restrict__ Qprev,
                                                 const double* __restrict__ Fx,
                                                 const double* __restrict__ Fy,
-                                                const double* __restrict__ Fz, double tau,
-                                                double dt, unsigned* err) {
+                                                const double* __restrict__ Fz, const double* __restrict__ clk, unsigned* err) {
+  const double tau = clk[0], dt = clk[1];  // the step's clock (device)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
@@ -252,8 +254,8 @@ __global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, TrDev tr,
                                                     double* __restrict__ pA,
                                                     double* __restrict__ pD,
                                                     double* __restrict__ pTh,
-                                                    double* __restrict__ pBC, double tau,
-                                                    double dt) {
+                                                    double* __restrict__ pBC, const double* __restrict__ clk) {
+  const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   const long long N = g.N;
@@ -361,7 +363,8 @@ __global__ void __launch_bounds__(128, kRelaxMinBlocks) k_is_relax(
     const double* __restrict__ pTh, const double* __restrict__ pBC,
     const double* __restrict__ pi, const double* __restrict__ Pi, double* __restrict__ pi0,
     double* __restrict__ piH0, double* __restrict__ Pi0, double* __restrict__ PiH0,
-    double* __restrict__ flux, double tau, double dt, unsigned* err) {
+    double* __restrict__ flux, const double* __restrict__ clk, unsigned* err) {
+  const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   const long long N = g.N;
@@ -693,8 +696,8 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
                                                    double* __restrict__ pi, double* __restrict__ piH,
                                                    double* __restrict__ Pi, double* __restrict__ PiH,
                                                    double* __restrict__ vcc,
-                                                   double* __restrict__ flux, double tau,
-                                                   double dt) {
+                                                   double* __restrict__ flux, const double* __restrict__ clk) {
+  const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
@@ -828,8 +831,8 @@ __global__ void __launch_bounds__(128) k_visc_update(Geo g, const double* __rest
                                                      const double* __restrict__ PiH,
                                                      const double* __restrict__ m,
                                                      const double* __restrict__ flux,
-                                                     double* __restrict__ Q, double tau,
-                                                     double dt) {
+                                                     double* __restrict__ Q, const double* __restrict__ clk) {
+  const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
@@ -915,15 +918,16 @@ const char* const kKernelNames[KK_COUNT] = {
 
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   const Geo& g = a.g;
-  const int bs = 128;
+  const int bs = a.block == 64 ? 64 : 128;
   const unsigned nb = nblk(g.N, bs);
+  const unsigned nb128 = nblk(g.N, 128);
   int launches = 0;
   const Fields& F = a.f;
   auto done = [&](int kind) {
     launches++;
     if (mk) mk->after(kind);
   };
-  k_update_m<<<nb, bs, 0, s>>>(g, F.m, F.m2, a.tau, a.dt);
+  k_update_m<<<nb, bs, 0, s>>>(g, F.m, F.m2, a.clk);
   done(KK_UPDATE_M);
   const double* m = F.m2;  // the updated fill fractions
   // predictor (src/hdo.cpp:1023-1060) and corrector (src/hdo.cpp:1062-1094)
@@ -931,45 +935,42 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
     const bool pred = pass == 0;
     const double* QQ = pred ? F.Q : F.Qh;
     if (pred) {
-      k_face<X_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.tau, a.dt, F.err);
+      k_face<X_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
       done(KK_FACE_X);
-      k_face<Y_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.tau, a.dt, F.err);
+      k_face<Y_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.clk, F.err);
       done(KK_FACE_Y);
       if (g.nz > 1) {
-        k_face<Z_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.tau, a.dt, F.err);
+        k_face<Z_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
         done(KK_FACE_Z);
       }
-      k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.tau,
-                                       a.dt, F.err);
+      k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err);
       done(KK_UPDATE);
     } else {
-      k_face<X_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.tau, a.dt, F.err);
+      k_face<X_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
       done(KK_FACE_X);
-      k_face<Y_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.tau, a.dt, F.err);
+      k_face<Y_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.clk, F.err);
       done(KK_FACE_Y);
       if (g.nz > 1) {
-        k_face<Z_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.tau, a.dt, F.err);
+        k_face<Z_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
         done(KK_FACE_Z);
       }
-      k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.tau,
-                                        a.dt, F.err);
+      k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err);
       done(KK_UPDATE);
     }
   }
-  const double tau1 = a.tau + a.dt;  // tau += dt (src/hdo.cpp:1095)
   k_ghost<false><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
   done(KK_GHOST);
   if (a.viscous) {
     k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
-                                   F.pBC, tau1, a.dt);
+                                   F.pBC, a.clk);
     done(KK_VISC_PRIMS);
-    k_is_relax<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh, F.pBC, F.pi,
-                                 F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0, F.flux, tau1, a.dt, F.err);
+    k_is_relax<<<nb128, 128, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh, F.pBC, F.pi,
+                                 F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0, F.flux, a.clk, F.err);
     done(KK_IS_RELAX);
     k_is_advect<<<nb, bs, 0, s>>>(g, F.pA, F.pi0, F.piH0, F.Pi0, F.PiH0, F.pi, F.piH, F.Pi, F.PiH,
-                                  F.vcc, F.flux, tau1, a.dt);
+                                  F.vcc, F.flux, a.clk);
     done(KK_IS_ADVECT);
-    k_visc_update<<<nb, bs, 0, s>>>(g, F.pA, F.piH, F.PiH, m, F.flux, F.Q, tau1, a.dt);
+    k_visc_update<<<nb, bs, 0, s>>>(g, F.pA, F.piH, F.PiH, m, F.flux, F.Q, a.clk);
     done(KK_VISC_UPDATE);
   }
   k_ghost<true><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
@@ -980,6 +981,31 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
                          cudaStream_t s) {
   k_transform_pv<<<nblk(n, 128), 128, 0, s>>>(E, Q, n, out);
+}
+
+// ------------------------------------------------------------ clock
+// The step kernels read (tau, dt) from a two-double device clock, so that a
+// captured step stays valid from one step to the next.
+__global__ void k_clock_set(double* clk, double tau, double dt) {
+  clk[0] = tau;
+  clk[1] = dt;
+}
+// tau += dt (src/hdo.cpp:1095), the substep divide (dt / n) and restore
+// (dt * n) of the driver loop (src/main.cpp:411,415), in the host's order
+__global__ void k_clock_op(double* clk, int op, int n) {
+  if (op == 0)
+    clk[0] += clk[1];
+  else if (op == 1)
+    clk[1] = clk[1] / n;
+  else
+    clk[1] = clk[1] * n;
+}
+
+void launch_clock_set(double* clk, double tau, double dt, cudaStream_t s) {
+  k_clock_set<<<1, 1, 0, s>>>(clk, tau, dt);
+}
+void launch_clock_op(double* clk, int op, int n, cudaStream_t s) {
+  k_clock_op<<<1, 1, 0, s>>>(clk, op, n);
 }
 
 // ------------------------------------------------------- small helpers

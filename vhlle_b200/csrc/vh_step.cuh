@@ -60,8 +60,10 @@ struct StepArgs {
   EosDev eos;
   TrDev tr;
   Fields f;
-  double tau, dt;
+  const double* clk;  // device [tau, dt] of the step (launch_clock_set)
   bool viscous;
+  int block = 128;    // threads per block of the step kernels (64 or 128; the
+                      // relaxation kernel always uses 128)
 };
 
 // Kernel kinds, for per-kernel timing.
@@ -80,6 +82,9 @@ struct LaunchMarker {
 // Enqueues one performStep on stream s; returns the number of launches.
 // Leaves the updated fill fractions in f.m2 (the caller swaps m and m2).
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk = nullptr);
+void launch_clock_set(double* clk, double tau, double dt, cudaStream_t s);
+// op 0: tau += dt; 1: dt = dt / n; 2: dt = dt * n
+void launch_clock_op(double* clk, int op, int n, cudaStream_t s);
 // gathers ncomp planes of the x2 resized grid from src into dst
 void launch_resize_gather(const Geo& g, const double* src, double* dst, int ncomp,
                           cudaStream_t s);
