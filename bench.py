@@ -231,6 +231,132 @@ def run_reference_arm(args):
     return 0
 
 
+def _reset(h, setup):
+    h.upload_initial()
+    h.L.vh_set_tau(h.h, setup.tau0)
+    h.set_dtau(setup.dt)
+
+
+def batch_measure(capi, W, n_events, steps, device):
+    """Event-by-event batch (the 256-event configuration's generator, its
+    first n_events): every event stepped alone through vh_advance, one after
+    another on the default stream, against the same events advanced by one
+    vh_batch graph per iteration after the online tuning.  Device time with
+    CUDA events; the same states are reset between the two runs."""
+    evs = W.batch_events(n_events)
+    cells = sum(s.grid.ncells for s in evs)
+    hs = [capi.GpuHydro(s, device=device) for s in evs]
+    drv = [(s.dt, s.grid.etamin, s.grid.etamax, s.grid.nz) for s in evs]
+    for h, d in zip(hs, drv):  # warm-up
+        h.advance(*d)
+    for h, s in zip(hs, evs):
+        _reset(h, s)
+    for h in hs:
+        h.sync()
+    hs[0].timer_start()
+    for _ in range(steps):
+        for h, d in zip(hs, drv):
+            h.advance(*d)
+    plain_ms = hs[0].timer_stop()
+    for h in hs:
+        h.sync()
+    b = capi.Batch(hs)
+    for k, d in enumerate(drv):
+        b.set_driver(k, *d, 4.0)
+    b.tune(True)
+    b.advance(16)  # 7 configurations x 2 timed iterations, then the chosen one
+    b.sync()
+    for h, s in zip(hs, evs):
+        _reset(h, s)
+    for h in hs:
+        h.sync()
+    b.advance(2)  # graphs of the reset parity
+    b.sync()
+    for h, s in zip(hs, evs):
+        _reset(h, s)
+    for h in hs:
+        h.sync()
+    b.timer_start()
+    b.advance(steps)
+    batch_ms = b.timer_stop()
+    bits = b.sync()
+    info = b.info()
+    b.close()
+    for h in hs:
+        h.close()
+    return {"events": n_events, "steps": steps, "cells": cells,
+            "grids": "%d..%d cells (61x61x1 .. 121x121x61 family)" % (
+                min(s.grid.ncells for s in evs), max(s.grid.ncells for s in evs)),
+            "plain_per_event": cells * steps / (plain_ms / 1e3),
+            "batched_graph": cells * steps / (batch_ms / 1e3),
+            "speedup": plain_ms / batch_ms, "unit": UNIT, "error_bits": bits,
+            "tuned": {"nstreams": info["nstreams"], "block": info["block"],
+                      "captures": info["captures"]},
+            "physics": "eta/s=0.12, zeta/s Gaussian bump 0.05 at T=0.175 GeV (width 0.02)"}
+
+
+def learned_guess_measure(capi, W, setup, steps, device):
+    """The learned con2prim start point on the same event: root-find
+    iterations and throughput at the tight tolerance (1e-13, where results
+    are start-point independent) without and with the trained network, and
+    at the reference tolerance for context."""
+    import torch
+    tight = 1e-13
+    cells = setup.grid.ncells
+    h = capi.GpuHydro(setup, device=device)
+    out = {"tolerance": tight}
+    # iterations per root find
+    iters = {}
+    for name, tol in (("reference_tol", None), ("tight", tight)):
+        _reset(h, setup)
+        if tol:
+            h.set_con2prim(tol)
+        h.con2prim_stats(True)
+        h.step(10)
+        c, it = h.con2prim_stats(False)
+        iters[name] = it / c
+    # training data from the event itself, then training
+    t0 = time.perf_counter()
+    _reset(h, setup)
+    cap = 24 * cells
+    X = torch.empty((cap, 4), dtype=torch.float32, device="cuda:%d" % device)
+    Y = torch.empty((cap, 3), dtype=torch.float32, device="cuda:%d" % device)
+    n = 0
+    for _ in range(20):
+        h.step(5)
+        n += h.mlp_samples(X[n:], Y[n:])
+    X, Y = X[:n].contiguous(), Y[:n].contiguous()
+    m = capi.Mlp(device=device, seed=17)
+    losses = m.train(X, Y, batch=16384, epochs=8, lr=3e-3, seed=5)
+    torch.cuda.synchronize()
+    out["train"] = {"samples": n, "epochs": 8, "first_loss": float(losses[0]),
+                    "final_loss": float(losses[-1]), "seconds": time.perf_counter() - t0}
+    for name, guess in (("tight", None), ("tight_mlp", m)):
+        _reset(h, setup)
+        h.set_con2prim(tight)
+        h.set_con2prim_guess(guess)
+        h.step(3)
+        h.sync()
+        _reset(h, setup)
+        h.set_con2prim(tight)
+        h.timer_start()
+        h.step(steps)
+        ms = h.timer_stop()
+        out[name] = cells * steps / (ms / 1e3)
+        h.con2prim_stats(True)
+        h.step(5)
+        c, it = h.con2prim_stats(False)
+        if guess is not None:
+            iters["tight_mlp"] = it / c
+    h.set_con2prim_guess(None)
+    out["iters_per_root_find"] = iters
+    out["speedup_mlp_vs_tight"] = out["tight_mlp"] / out["tight"]
+    out["unit"] = UNIT
+    h.close()
+    m.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -240,6 +366,10 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--batch-events", type=int, default=32,
+                    help="events of the batched-vs-plain measurement (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--no-learned-guess", action="store_true")
     ap.add_argument("--grid", default="101,101,51",
                     help="nx,ny,nz of the event (smaller grids only for profiler captures)")
     args = ap.parse_args()
@@ -361,6 +491,13 @@ def main():
                "note": "state uploaded and downloaded every step, surface records every %d"
                        % SURF_EVERY}
 
+    batch = None
+    if args.batch_events > 0:
+        batch = batch_measure(capi, W, args.batch_events, args.batch_steps, local)
+    learned = None
+    if not args.no_learned_guess:
+        learned = learned_guess_measure(capi, W, setup, 30, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(W.glauber3d_setup(nx, ny, nz, seed=20260001))
@@ -377,7 +514,7 @@ def main():
                        "l2": "inputs larger than L2 (%.0f MB of resident fields)" % (
                            cells * 8 * 127 / 1e6)},
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
-            "e2e": e2e, "cpu_baseline": cpu,
+            "e2e": e2e, "cpu_baseline": cpu, "batch": batch, "learned_guess": learned,
             "gpu_launches": lps * args.steps + 9 * (args.steps // SURF_EVERY), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

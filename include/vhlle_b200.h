@@ -77,6 +77,10 @@ typedef struct vh_trcoeff {
       etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
       zetaSSigmaMinus, zetaSSigmaPlus;
   int etaSparam, zetaSparam;
+  /* zetaSparam 5 (no counterpart in the reference's src/trancoeff.cpp:32-65):
+   * zeta/s = zetaS0 exp(-(T - zetaSPeakT)^2 / (2 zetaSWidthT^2)), a Gaussian
+   * bump in T (GeV); unused by the other parameterisations. */
+  double zetaSPeakT, zetaSWidthT;
 } vh_trcoeff;
 
 /* A view of the per-cell fields (host or device pointers depending on the
@@ -294,6 +298,9 @@ vh_status vh_batch_tune(vh_batch *batch, int enable);
 vh_status vh_batch_advance(vh_batch *batch, int *nsub_max);
 vh_status vh_batch_sync(vh_batch *batch, unsigned *error_bits);
 vh_status vh_batch_info(vh_batch *batch, int *captures, int *nstreams, int *block);
+/* CUDA-event timing of the batch's stream (stop waits for the stop event). */
+vh_status vh_batch_timer_start(vh_batch *batch);
+vh_status vh_batch_timer_stop(vh_batch *batch, double *ms);
 const char *vh_batch_last_error(void);
 
 /* Device timing with CUDA events recorded on the context's stream.

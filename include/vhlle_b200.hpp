@@ -168,6 +168,8 @@ class TransportCoeff {
       etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta, zetaSSigmaMinus, zetaSSigmaPlus;
   EoS* eos;
   const int etaSparam, zetaSparam;
+  // zetaSparam 5 (this build's Gaussian bump in T; not in the reference)
+  double zetaSPeakT = 0.175, zetaSWidthT = 0.02;
   TransportCoeff(double _etaS0, double _zetaS0, double _ah, double _al, double _aRho, double _T0,
                  double _etaSMin, double _etaSEpsilonMin, double _etaSShiftMuB,
                  double _etaSScaleMuB, double _zetaSPeakEpsilon, double _zetaSScaleBeta,
@@ -186,7 +188,8 @@ class TransportCoeff {
     return vh_trcoeff{etaS0,         zetaS0,         ah,           al,
                       aRho,          T0,             etaSMin,      etaSEpsilonMin,
                       etaSShiftMuB,  etaSScaleMuB,   zetaSPeakEpsilon, zetaSScaleBeta,
-                      zetaSSigmaMinus, zetaSSigmaPlus, etaSparam,   zetaSparam};
+                      zetaSSigmaMinus, zetaSSigmaPlus, etaSparam,   zetaSparam,
+                      zetaSPeakT,      zetaSWidthT};
   }
 };
 

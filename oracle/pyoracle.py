@@ -49,7 +49,8 @@ class _Trc(ctypes.Structure):
         "etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin",
         "etaSShiftMuB", "etaSScaleMuB", "zetaSPeakEpsilon", "zetaSScaleBeta",
         "zetaSSigmaMinus", "zetaSSigmaPlus")] + [
-        ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int)]
+        ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int),
+        ("zetaSPeakT", ctypes.c_double), ("zetaSWidthT", ctypes.c_double)]
 
 
 class _State(ctypes.Structure):

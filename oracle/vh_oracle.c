@@ -256,6 +256,10 @@ static double tr_zetaS(const or_trc *t, double e, double T, double s,
     const double sig =
         e < t->zetaSPeakEpsilon ? t->zetaSSigmaMinus : t->zetaSSigmaPlus;
     return ((e + P) / (s * T)) * t->zetaS0 * exp(d * d / 2.0 * (sig * sig));
+  } else if (t->zetaSparam == 5) {
+    /* a Gaussian bump in T: this build's addition, not in the reference */
+    const double x = T - t->zetaSPeakT;
+    return t->zetaS0 * exp(-x * x / (2. * t->zetaSWidthT * t->zetaSWidthT));
   }
   return 0.;
 }

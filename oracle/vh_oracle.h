@@ -48,6 +48,9 @@ typedef struct or_trc {
       etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
       zetaSSigmaMinus, zetaSSigmaPlus;
   int etaSparam, zetaSparam;
+  /* zetaSparam 5, an addition of this build (no reference counterpart):
+   * zeta/s = zetaS0 exp(-(T - zetaSPeakT)^2 / (2 zetaSWidthT^2)) */
+  double zetaSPeakT, zetaSWidthT;
 } or_trc;
 
 /* Persistent + inspected cell fields (all caller-owned, component-major). */

@@ -5,7 +5,7 @@ substep block and the resize (vh_advance, vh_resize2x): bit for bit."""
 import numpy as np
 import pytest
 
-from helpers import compare_states
+from helpers import compare_states, gpu_state_as_oracle
 from vhlle_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
@@ -68,3 +68,52 @@ def test_gpu_batch_rejects_bad_input():
     with pytest.raises(VhError):
         Batch([h, h])
     h.close()
+
+
+def test_gpu_zeta_bump_event_against_oracle():
+    """A batch event with the zeta/s bump (zetaSparam 5) against the oracle.
+    The bump uses exp, where the device and glibc may differ in the last bit;
+    the oracle alone, with the bump height moved by one ulp, differs from
+    itself by ~1e-16 of each field's scale after 5 steps (more at the vacuum
+    edge later on).  Tolerance: 1e-10 relative plus 1e-12 of the field's
+    largest magnitude, after one step and after five."""
+    import pyoracle as P
+    from vhlle_b200.capi import GpuHydro
+    setup = W.batch_event(1, nz=9)
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+
+    def check():
+        got, exp = gpu_state_as_oracle(d.get_state()), o.get_state()
+        for k in exp:
+            a = np.asarray(got[k], dtype=np.float64).reshape(-1)
+            b = np.asarray(exp[k], dtype=np.float64).reshape(-1)
+            scale = np.abs(b).max()
+            ok = np.abs(a - b) <= 1e-10 * np.maximum(np.abs(a), np.abs(b)) + 1e-12 * scale
+            assert ok.all(), (k, np.argwhere(~ok)[:5])
+        return exp
+
+    o.step(1)
+    d.step(1)
+    check()
+    o.step(4)
+    d.step(4)
+    exp = check()
+    assert np.abs(exp["Pi"]).max() > 0  # the bump drives bulk pressure
+    d.close()
+
+
+def test_gpu_batch_of_c3_events_runs_and_tunes():
+    from vhlle_b200.capi import Batch, GpuHydro
+    evs = W.batch_events(12)
+    hs = [GpuHydro(s) for s in evs]
+    b = Batch(hs)
+    for k, s in enumerate(evs):
+        g = s.grid
+        b.set_driver(k, s.dt, g.etamin, g.etamax, g.nz, 4.0)
+    b.tune(True)
+    b.advance(20)
+    assert b.sync() == 0
+    assert all(abs(h.tau - (0.5 + 20 * 0.05)) < 1e-12 for h in hs)
+    b.close()
+    for h in hs:
+        h.close()

@@ -52,3 +52,21 @@ def test_full_size_configs_have_the_stated_shapes():
     assert math.isclose(g.dx, 0.3) and math.isclose(g.dz, 0.3)
     g1 = W.gubser_setup().grid
     assert (g1.nx, g1.ny, g1.nz) == (101, 101, 1) and math.isclose(g1.dx, 0.1)
+
+
+def test_batch_events_shape_and_physics():
+    evs = W.batch_events(8)
+    bs = np.random.default_rng(W.BATCH_SEED0).uniform(0, 12, 8)
+    for k, s in enumerate(evs):
+        g = s.grid
+        assert 61 <= g.nx <= 121 and g.nx == g.ny and g.nx % 2 == 1
+        assert g.nz == W.BATCH_NZ[k % 4]
+        assert s.zetaSparam == 5 and s.tr["etaS0"] == 0.12 and s.tr["zetaS0"] == 0.05
+        assert s.tr["zetaSPeakT"] == 0.175 and s.tr["zetaSWidthT"] == 0.02
+        assert s.viscous
+        nt = 121 - 2 * int(round(30 * bs[k] / 12))
+        assert g.nx == nt
+        assert np.asarray(s.Q).shape == (7, g.ncells)
+        assert np.isfinite(np.asarray(s.Q)).all() and np.asarray(s.Q)[0].max() > 0
+    # the same event regardless of how many are generated
+    assert np.array_equal(np.asarray(W.batch_event(5).Q), np.asarray(evs[5].Q))

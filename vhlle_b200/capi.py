@@ -34,7 +34,8 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_mlp_get_params", "vh_mlp_forward", "vh_mlp_grad", "vh_mlp_train",
            "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
            "vh_batch_destroy", "vh_batch_set_driver", "vh_batch_tune", "vh_batch_advance",
-           "vh_batch_sync", "vh_batch_info", "vh_batch_last_error")
+           "vh_batch_sync", "vh_batch_info", "vh_batch_last_error", "vh_batch_timer_start",
+           "vh_batch_timer_stop")
 
 
 class VhError(RuntimeError):
@@ -179,6 +180,14 @@ class Batch:
         self._check(self.L.vh_batch_sync(self.b, ctypes.byref(bits)))
         return bits.value
 
+    def timer_start(self):
+        self._check(self.L.vh_batch_timer_start(self.b))
+
+    def timer_stop(self) -> float:
+        ms = ctypes.c_double()
+        self._check(self.L.vh_batch_timer_stop(self.b, ctypes.byref(ms)))
+        return ms.value
+
     def info(self):
         c, s, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         self._check(self.L.vh_batch_info(self.b, ctypes.byref(c), ctypes.byref(s), ctypes.byref(b)))
@@ -214,7 +223,8 @@ class VhTrcoeff(ctypes.Structure):
         "etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin",
         "etaSShiftMuB", "etaSScaleMuB", "zetaSPeakEpsilon", "zetaSScaleBeta",
         "zetaSSigmaMinus", "zetaSSigmaPlus")] + [
-        ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int)]
+        ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int),
+        ("zetaSPeakT", ctypes.c_double), ("zetaSWidthT", ctypes.c_double)]
 
 
 STATE_FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "viscCorrCut")
@@ -307,6 +317,8 @@ def lib():
     L.vh_batch_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
     L.vh_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3
     L.vh_batch_last_error.restype = ctypes.c_char_p
+    L.vh_batch_timer_start.argtypes = [vp]
+    L.vh_batch_timer_stop.argtypes = [vp, _dp]
     L.vh_cornelius4d.argtypes = [_dp, ctypes.c_long, _dp, ctypes.c_double, ctypes.c_int,
                                  ctypes.POINTER(ctypes.c_int), _dp, _dp]
     _lib = L

@@ -59,7 +59,7 @@ struct vh_batch {
   std::vector<double*> bufA;  // each event's first fill-fraction buffer (parity 0)
   cudaStream_t origin = nullptr;
   std::vector<cudaStream_t> streams;
-  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr, ts = nullptr, te = nullptr;
   std::vector<cudaEvent_t> join;
   std::map<std::vector<int>, cudaGraphExec_t> graphs;
   int captures = 0;
@@ -170,6 +170,8 @@ vh_status vh_batch_destroy(vh_batch* b) {
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->t0) cudaEventDestroy(b->t0);
   if (b->t1) cudaEventDestroy(b->t1);
+  if (b->ts) cudaEventDestroy(b->ts);
+  if (b->te) cudaEventDestroy(b->te);
   if (b->origin) cudaStreamDestroy(b->origin);
   delete b;
   return VH_OK;
@@ -209,7 +211,8 @@ vh_status vh_batch_create(vh_ctx* const* ctxs, int n, vh_batch** out) {
   }
   if ((e = cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess ||
-      (e = cudaEventCreate(&b->t0)) != cudaSuccess || (e = cudaEventCreate(&b->t1)) != cudaSuccess) {
+      (e = cudaEventCreate(&b->t0)) != cudaSuccess || (e = cudaEventCreate(&b->t1)) != cudaSuccess ||
+      (e = cudaEventCreate(&b->ts)) != cudaSuccess || (e = cudaEventCreate(&b->te)) != cudaSuccess) {
     vh_batch_destroy(b);
     return bfail(VH_ERR_CUDA, cudaGetErrorString(e));
   }
@@ -346,6 +349,26 @@ vh_status vh_batch_sync(vh_batch* b, unsigned* error_bits) {
   }
   if (error_bits) *error_bits = all;
   return all ? bfail(VH_ERR_NUMERIC, "vh_batch_sync: a step set the device error word") : VH_OK;
+}
+
+vh_status vh_batch_timer_start(vh_batch* b) {
+  if (!b) return VH_ERR_ARG;
+  cudaSetDevice(b->device);
+  cudaError_t e = cudaEventRecord(b->ts, b->origin);
+  return e == cudaSuccess ? VH_OK : bfail(VH_ERR_CUDA, cudaGetErrorString(e));
+}
+
+vh_status vh_batch_timer_stop(vh_batch* b, double* ms) {
+  if (!b || !ms) return VH_ERR_ARG;
+  cudaSetDevice(b->device);
+  float f = 0.f;
+  cudaError_t e;
+  if ((e = cudaEventRecord(b->te, b->origin)) != cudaSuccess ||
+      (e = cudaEventSynchronize(b->te)) != cudaSuccess ||
+      (e = cudaEventElapsedTime(&f, b->ts, b->te)) != cudaSuccess)
+    return bfail(VH_ERR_CUDA, cudaGetErrorString(e));
+  *ms = f;
+  return VH_OK;
 }
 
 vh_status vh_batch_info(vh_batch* b, int* captures, int* nstreams, int* block) {

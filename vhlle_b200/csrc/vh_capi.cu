@@ -241,7 +241,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   c->tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
                     tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
                     tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,
-                    tr->zetaSSigmaPlus, tr->etaSparam, tr->zetaSparam};
+                    tr->zetaSSigmaPlus, tr->etaSparam, tr->zetaSparam, tr->zetaSPeakT,
+                    tr->zetaSWidthT};
   // TransportCoeff::isViscous, src/trancoeff.h:39-45
   c->viscous = tr->etaS0 > 0. || tr->zetaS0 > 0. || tr->etaSparam > 0 || tr->zetaSparam > 0;
 

@@ -168,7 +168,8 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
                    tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
                    tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,
-                   tr->zetaSSigmaPlus, tr->etaSparam, tr->zetaSparam};
+                   tr->zetaSSigmaPlus, tr->etaSparam, tr->zetaSparam, tr->zetaSPeakT,
+                   tr->zetaSWidthT};
   a.viscous = tr->etaS0 > 0. || tr->zetaS0 > 0. || tr->etaSparam > 0 || tr->zetaSparam > 0;
 
   // scratch layout: [err, clock | ghost src maps | ghost dst flags | pad][doubles...]

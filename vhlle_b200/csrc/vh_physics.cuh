@@ -57,6 +57,7 @@ struct TrDev {
       etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
       zetaSSigmaMinus, zetaSSigmaPlus;
   int etaSparam, zetaSparam;
+  double zetaSPeakT, zetaSWidthT;  // zetaSparam 5
 };
 
 struct Prim {
@@ -357,6 +358,10 @@ __device__ __forceinline__ double tr_zetaS(const TrDev& t, double e, double T,
     const double d = t.zetaSScaleBeta * (pow(e, 0.25) - pow(t.zetaSPeakEpsilon, 0.25));
     const double sig = e < t.zetaSPeakEpsilon ? t.zetaSSigmaMinus : t.zetaSSigmaPlus;
     return ((e + P) / (s * T)) * t.zetaS0 * exp(d * d / 2.0 * (sig * sig));
+  } else if (t.zetaSparam == 5) {
+    // a Gaussian bump in T (this build's addition; not in the reference)
+    const double x = T - t.zetaSPeakT;
+    return t.zetaS0 * exp(-x * x / (2. * t.zetaSWidthT * t.zetaSWidthT));
   }
   return 0.;
 }

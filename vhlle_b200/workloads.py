@@ -419,3 +419,50 @@ def write_params(path: str, setup: "Setup", **extra) -> None:
         lines.append("%s %s" % (k, v if isinstance(v, str) else repr(v)))
     with open(path, "w") as f:
         f.write("\n".join(lines) + "\n")
+
+
+# ------------------------------------------------- event-by-event batches
+BATCH_SEED0 = 20263000
+BATCH_NZ = (1, 21, 41, 61)
+
+
+def batch_event(k: int, seed0: int = BATCH_SEED0, nz: Optional[int] = None,
+                eos: Optional[EosTable] = None, etaS: float = 0.12, zeta_height: float = 0.05,
+                zeta_peak_T: float = 0.175, zeta_width_T: float = 0.02, tau0: float = 0.5,
+                dt: float = 0.05) -> Setup:
+    """Event k of the event-by-event batch: seed seed0 + k; impact parameter
+    uniform on [0, 12] fm from one seeded stream shared by the batch; the
+    transverse grid sized to the event's extent (121 cells at b = 0 down to
+    61 at b = 12, x, y in [-15, 15] * n / 121 fm); eta cells cycling through
+    1, 21, 41, 61 (eta_s in [-7.5, 7.5], or [-0.5, 0.5] boost-invariant for
+    one cell); eta/s = 0.12 and a zeta/s Gaussian bump in T (height 0.05 at
+    T = 0.175 GeV, width 0.02 GeV: zetaSparam 5)."""
+    bs = np.random.default_rng(seed0).uniform(0.0, 12.0, k + 1)
+    b = float(bs[k])
+    nt = 121 - 2 * int(round(30.0 * b / 12.0))
+    nz = BATCH_NZ[k % len(BATCH_NZ)] if nz is None else nz
+    xmax = 15.0 * nt / 121.0
+    if nz > 1:
+        s = glauber3d_setup(nt, nt, nz, xmax=xmax, etamax=7.5, tau0=tau0, dt=dt, seed=seed0 + k,
+                            b=b, etaS=etaS, eos=eos)
+    else:
+        g = Grid(nt, nt, 1, -xmax, xmax, -xmax, xmax, -0.5, 0.5)
+        x, y, _ = g.coords()
+        prof, _ = glauber_profile(seed0 + k, b, x, y)
+        e = 50.0 * prof[None, :, :]
+        e = np.where(e < 1e-3, 0.0, e)
+        zero = np.zeros_like(e)
+        Q = conserved_from_primitive(tau0, e, zero, zero, zero, zero, zero).reshape(7, -1)
+        m = (e.reshape(-1) > 0).astype(np.float64)
+        tr = dict(TR_DEFAULTS, etaS0=etaS, zetaS0=0.0)
+        s = Setup("glauber2d", g, eos or make_cs2_table(), tr, 0, 0, tau0, dt, 0.5, Q, m)
+    s.name = "batch_event_%d" % k
+    s.tr = dict(s.tr, zetaS0=zeta_height, zetaSPeakT=zeta_peak_T, zetaSWidthT=zeta_width_T)
+    s.zetaSparam = 5
+    return s
+
+
+def batch_events(n: int = 256, seed0: int = BATCH_SEED0, **kw):
+    """The first n events of the batch (one EoS table shared by all)."""
+    eos = kw.pop("eos", None) or make_cs2_table()
+    return [batch_event(k, seed0, eos=eos, **kw) for k in range(n)]
