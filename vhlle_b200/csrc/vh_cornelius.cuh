@@ -2,7 +2,7 @@
 // the device (P. Huovinen and H. Petersen, Eur. Phys. J. A 48 (2012) 171,
 // arXiv:1206.3371, as the reference's src/cornelius.cpp implements it).
 //
-// One thread handles one hypercube.  The 4-cube splits into 8 3-cubes
+// One warp handles one hypercube.  The 4-cube splits into 8 3-cubes
 // (constant dimension i at j = 0, 1; cornelius.cpp:1733-1774), each 3-cube
 // into 6 squares (:1436-1482).  A square gives 0-2 line elements from the
 // cuts of its edges (:1083-1313), a 3-cube joins its lines into polygons
@@ -15,7 +15,11 @@
 // bit-identical to it.  Capacities: 96 lines, 64 polygons (8 per 3-cube),
 // 10 elements, as the reference's arrays; a hypercube that would exceed
 // them, or on which the reference stops (an odd number of cuts on a square,
-// too few lines for a polygon), returns -1.
+// too few lines for a polygon), returns -1.  The squares go across the
+// lanes, the 3-cubes across 8 lanes, and the joining into polyhedra and the
+// reference-ordered sums run in one lane, all over shared memory (a thread
+// per hypercube left ~2 warps per SM on a typical surface, each running the
+// whole construction serially out of L2-resident local memory).
 #pragma once
 
 namespace vh {
@@ -33,26 +37,18 @@ struct Line {
   int start;       // which of p is the start point (flip_start_end swaps)
 };
 
-struct Poly {
-  unsigned char li[12];
-  int n, cdim;
-  double cen[4];
-};
-
-struct Work {
-  Line L[kMaxLines];
-  Poly P[kMaxPoly];
-  int nl, np, err;
-};
-
 __device__ __forceinline__ const double* lstart(const Line& l) { return l.p[l.start]; }
 __device__ __forceinline__ const double* lend(const Line& l) { return l.p[1 - l.start]; }
 
 // Square::construct_lines with ends_of_edge and find_outside.  The square's
 // constant dimensions are c0, c1 (values v0, v1), its corner values p[a][b]
-// (a along x1, b along x2, x1 < x2).  Returns 1 when it is ambiguous.
-__device__ int square(Work& w, const double p[2][2], int c0, int c1, double v0, double v1,
-                      int x1, int x2, const double* dx, double E0) {
+// (a along x1, b along x2, x1 < x2).  Writes its 0-2 lines to out[0..n) and
+// returns n; *amb_out = 1 when it is ambiguous, *err = 1 when the reference
+// would stop (an odd number of cuts).
+__device__ int square_lines(const double p[2][2], int c0, int c1, double v0, double v1, int x1,
+                            int x2, const double* dx, double E0, Line* out, int* amb_out,
+                            int* err) {
+  *amb_out = 0;
   int above = 0;
 #pragma unroll
   for (int i = 0; i < 2; i++)
@@ -103,7 +99,7 @@ __device__ int square(Work& w, const double p[2][2], int c0, int c1, double v0, 
     cy[nc++] = dx[x2];
   }
   if (nc != 0 && nc != 2 && nc != 4) {
-    w.err |= 1;
+    *err = 1;
     return 0;
   }
   if (nc == 0) return 0;
@@ -159,11 +155,7 @@ __device__ int square(Work& w, const double p[2][2], int c0, int c1, double v0, 
     }
   }
   for (int k = 0; k < nc / 2; k++) {
-    if (w.nl >= kMaxLines) {
-      w.err |= 2;
-      return amb;
-    }
-    Line& l = w.L[w.nl++];
+    Line& l = out[k];
 #pragma unroll
     for (int e = 0; e < 2; e++) {
       l.p[e][x1] = cx[2 * k + e];
@@ -177,11 +169,100 @@ __device__ int square(Work& w, const double p[2][2], int c0, int c1, double v0, 
     l.o[c1] = v1;
     l.start = 0;
   }
-  return amb;
+  *amb_out = amb;
+  return nc / 2;
 }
 
-// Polygon::add_line
-__device__ bool add_line(Work& w, Poly& pg, int li, bool donotcheck) {
+// Polyhedron::tetravolume
+__device__ __forceinline__ void tetra(const double* a, const double* b, const double* c,
+                                      double* n) {
+  const double bc01 = b[0] * c[1] - b[1] * c[0];
+  const double bc02 = b[0] * c[2] - b[2] * c[0];
+  const double bc03 = b[0] * c[3] - b[3] * c[0];
+  const double bc12 = b[1] * c[2] - b[2] * c[1];
+  const double bc13 = b[1] * c[3] - b[3] * c[1];
+  const double bc23 = b[2] * c[3] - b[3] * c[2];
+  n[0] = 1.0 / 6.0 * (a[1] * bc23 - a[2] * bc13 + a[3] * bc12);
+  n[1] = -1.0 / 6.0 * (a[0] * bc23 - a[2] * bc03 + a[3] * bc02);
+  n[2] = 1.0 / 6.0 * (a[0] * bc13 - a[1] * bc03 + a[3] * bc01);
+  n[3] = -1.0 / 6.0 * (a[0] * bc12 - a[1] * bc02 + a[2] * bc01);
+}
+
+// Polyhedron::lines_equal
+__device__ bool lines_equal(const Line& l1, const Line& l2) {
+  const double *p11 = lstart(l1), *p12 = lend(l1), *p21 = lstart(l2);
+  double d1 = 0, d2 = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    d1 += fabs(p11[i] - p21[i]);
+    d2 += fabs(p12[i] - p21[i]);
+    if (d1 > kEps && d2 > kEps) return false;
+  }
+  return true;
+}
+
+}  // namespace cn
+
+// ---------------------------------------------------------------------
+// The warp's part: 48 square instances (8 3-cubes x 6 squares) across the
+// lanes, each 3-cube's polygons in one of 8 lanes, the polyhedra in lane 0.
+namespace cnw {
+
+using cn::kEps;
+using cn::kMaxElem;
+using cn::Line;
+using cn::lend;
+using cn::lstart;
+
+struct Poly {
+  unsigned char li[12];  // line ids: 2 * square instance + line
+  int n;
+  double cen[4];
+};
+
+struct WarpWork {
+  Line L[96];  // lines of square instance t at 2t, 2t + 1
+  unsigned char sqn[48], sqamb[48];
+  Poly P[8][8];  // polygons of each 3-cube
+  int np[8], nl[8], camb[8];
+  double hc[16];
+  int err;
+};
+
+// Square instance t = 6 c + s: 3-cube c (constant dimension c / 2 at corner
+// bit c % 2), square s (its constant dimension the (s / 2)-th free dimension
+// of the 3-cube, at bit s % 2) -- the order Cube::split_to_squares and
+// Hypercube::split_to_cubes produce (src/cornelius.cpp:1436-1482,1733-1774).
+__device__ __forceinline__ void square_instance(WarpWork& w, int t, const double* dx, double E0) {
+  const int c = t / 6, s = t % 6, ci = c >> 1, jc = c & 1, j = s & 1;
+  int fr[3], k = 0;
+  for (int d = 0; d < 4; d++)
+    if (d != ci) fr[k++] = d;
+  const int i = fr[s >> 1];
+  int x1 = -1, x2 = -1;
+  for (int d = 0; d < 4; d++)
+    if (d != ci && d != i) {
+      if (x1 < 0)
+        x1 = d;
+      else
+        x2 = d;
+    }
+  double sq[2][2];
+#pragma unroll
+  for (int a = 0; a < 2; a++)
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+      sq[a][b] = w.hc[(jc << (3 - ci)) | (j << (3 - i)) | (a << (3 - x1)) | (b << (3 - x2))];
+  int amb = 0, err = 0;
+  const int n = cn::square_lines(sq, ci, i, jc * dx[ci], j * dx[i], x1, x2, dx, E0, &w.L[2 * t],
+                                 &amb, &err);
+  w.sqn[t] = (unsigned char)n;
+  w.sqamb[t] = (unsigned char)amb;
+  if (err) atomicOr(&w.err, 1);
+}
+
+// Polygon::add_line (src/cornelius.cpp:404-438)
+__device__ bool add_line(WarpWork& w, Poly& pg, int li, bool donotcheck) {
   if (donotcheck || pg.n == 0) {
     pg.li[pg.n++] = (unsigned char)li;
     return true;
@@ -202,95 +283,11 @@ __device__ bool add_line(Work& w, Poly& pg, int li, bool donotcheck) {
   return false;
 }
 
-// Cube::construct_polygons + check_ambiguous for the 3-cube with constant
-// dimension ci at corner bit jc.  Returns its number of lines.
-__device__ int cube3(Work& w, const double* hc, int ci, int jc, const double* dx, double E0,
-                     int& cube_amb) {
-  const int l0 = w.nl, p0 = w.np;
-  const double cv = jc * dx[ci];
-  int namb = 0;
-#pragma unroll 1
-  for (int i = 0; i < 4; i++) {
-    if (i == ci) continue;
-    int x1 = -1, x2 = -1;
-    for (int d = 0; d < 4; d++)
-      if (d != ci && d != i) {
-        if (x1 < 0)
-          x1 = d;
-        else
-          x2 = d;
-      }
-#pragma unroll 1
-    for (int j = 0; j < 2; j++) {
-      double sq[2][2];
-#pragma unroll
-      for (int a = 0; a < 2; a++)
-#pragma unroll
-        for (int b = 0; b < 2; b++) {
-          // corner bit of dimension d: ci -> jc, i -> j, x1 -> a, x2 -> b
-          const int bt = (jc << (3 - ci)) | (j << (3 - i)) | (a << (3 - x1)) | (b << (3 - x2));
-          sq[a][b] = hc[bt];
-        }
-      namb += square(w, sq, ci, i, cv, j * dx[i], x1, x2, dx, E0);
-    }
-  }
-  const int nl = w.nl - l0;
-  cube_amb = 0;
-  if (nl == 0) return 0;
-  int amb = namb;
-  if (amb == 0 && nl == 6) amb = 1;
-  cube_amb = amb;
-  if (amb > 0) {
-    unsigned long long unused_lo = 0, unused_hi = 0;  // bits of the cube's lines
-    for (int i = 0; i < nl; i++) {
-      if (i < 64)
-        unused_lo |= 1ull << i;
-      else
-        unused_hi |= 1ull << (i - 64);
-    }
-    int used = 0;
-    do {
-      if (nl - used < 3 || w.np >= kMaxPoly || w.np - p0 >= kMaxPolyPerCube) {
-        w.err |= 4;
-        return nl;
-      }
-      Poly& pg = w.P[w.np];
-      pg.n = 0;
-      pg.cdim = ci;
-      for (int i = 0; i < nl; i++) {
-        const bool un = i < 64 ? (unused_lo >> i) & 1 : (unused_hi >> (i - 64)) & 1;
-        if (un && pg.n < 12) {
-          if (add_line(w, pg, l0 + i, false)) {
-            if (i < 64)
-              unused_lo &= ~(1ull << i);
-            else
-              unused_hi &= ~(1ull << (i - 64));
-            used++;
-            i = 0;
-          }
-        }
-      }
-      w.np++;
-    } while (used < nl);
-  } else {
-    if (w.np >= kMaxPoly || nl > 12) {
-      w.err |= 4;
-      return nl;
-    }
-    Poly& pg = w.P[w.np];
-    pg.n = 0;
-    pg.cdim = ci;
-    for (int i = 0; i < nl; i++) add_line(w, pg, l0 + i, true);
-    w.np++;
-  }
-  return nl;
-}
-
-// Polygon::calculate_centroid
-__device__ void poly_centroid(const Work& w, Poly& pg) {
+// Polygon::calculate_centroid (src/cornelius.cpp:440-516)
+__device__ void poly_centroid(const WarpWork& w, Poly& pg, int cdim) {
   int x[3], k = 0;
   for (int d = 0; d < 4; d++)
-    if (d != pg.cdim) x[k++] = d;
+    if (d != cdim) x[k++] = d;
   const int x1 = x[0], x2 = x[1], x3 = x[2];
   double mean[4] = {0, 0, 0, 0};
   for (int i = 0; i < pg.n; i++) {
@@ -327,106 +324,116 @@ __device__ void poly_centroid(const Work& w, Poly& pg) {
   for (int j = 0; j < 4; j++) pg.cen[j] = up[j] / down;
 }
 
-// Polyhedron::tetravolume
-__device__ __forceinline__ void tetra(const double* a, const double* b, const double* c,
-                                      double* n) {
-  const double bc01 = b[0] * c[1] - b[1] * c[0];
-  const double bc02 = b[0] * c[2] - b[2] * c[0];
-  const double bc03 = b[0] * c[3] - b[3] * c[0];
-  const double bc12 = b[1] * c[2] - b[2] * c[1];
-  const double bc13 = b[1] * c[3] - b[3] * c[1];
-  const double bc23 = b[2] * c[3] - b[3] * c[2];
-  n[0] = 1.0 / 6.0 * (a[1] * bc23 - a[2] * bc13 + a[3] * bc12);
-  n[1] = -1.0 / 6.0 * (a[0] * bc23 - a[2] * bc03 + a[3] * bc02);
-  n[2] = 1.0 / 6.0 * (a[0] * bc13 - a[1] * bc03 + a[3] * bc01);
-  n[3] = -1.0 / 6.0 * (a[0] * bc12 - a[1] * bc02 + a[2] * bc01);
-}
-
-// Polyhedron::lines_equal
-__device__ bool lines_equal(const Line& l1, const Line& l2) {
-  const double *p11 = lstart(l1), *p12 = lend(l1), *p21 = lstart(l2);
-  double d1 = 0, d2 = 0;
-#pragma unroll
-  for (int i = 0; i < 4; i++) {
-    d1 += fabs(p11[i] - p21[i]);
-    d2 += fabs(p12[i] - p21[i]);
-    if (d1 > kEps && d2 > kEps) return false;
+// Cube::construct_polygons + check_ambiguous for 3-cube c
+// (src/cornelius.cpp:1484-1595), then its polygons' centroids.
+__device__ void cube_polygons(WarpWork& w, int c) {
+  unsigned char ids[12];
+  int nl = 0, namb = 0;
+  for (int s = 0; s < 6; s++) {
+    const int t = 6 * c + s;
+    namb += w.sqamb[t];
+    for (int j = 0; j < w.sqn[t]; j++) ids[nl++] = (unsigned char)(2 * t + j);
   }
-  return true;
+  w.nl[c] = nl;
+  w.np[c] = 0;
+  w.camb[c] = 0;
+  if (nl == 0) return;
+  int amb = namb;
+  if (amb == 0 && nl == 6) amb = 1;
+  w.camb[c] = amb;
+  int np = 0;
+  if (amb > 0) {
+    unsigned unused = (1u << nl) - 1u;
+    int used = 0;
+    do {
+      if (nl - used < 3 || np >= cn::kMaxPolyPerCube) {
+        atomicOr(&w.err, 4);
+        return;
+      }
+      Poly& pg = w.P[c][np];
+      pg.n = 0;
+      for (int i = 0; i < nl; i++) {
+        if (((unused >> i) & 1u) && pg.n < 12) {
+          if (add_line(w, pg, ids[i], false)) {
+            unused &= ~(1u << i);
+            used++;
+            i = 0;
+          }
+        }
+      }
+      np++;
+    } while (used < nl);
+  } else {
+    Poly& pg = w.P[c][0];
+    pg.n = 0;
+    for (int i = 0; i < nl; i++) add_line(w, pg, ids[i], true);
+    np = 1;
+  }
+  w.np[c] = np;
+  for (int q = 0; q < np; q++) poly_centroid(w, w.P[c][q], c >> 1);
 }
 
-// Cornelius::find_surface_4d.  hc[it*8 + jx*4 + jy*2 + jz]; dx = dt, dx, dy,
-// dz.  Writes up to kMaxElem centroids and normals (relative to the low
-// corner); returns the element count or -1.
-__device__ int find_surface_4d(Work& w, const double* hc, const double* dx, double E0,
-                               double (*cent)[4], double (*norm)[4]) {
-  int above = 0;
-#pragma unroll
-  for (int k = 0; k < 16; k++)
-    if (hc[k] >= E0) above++;
-  if (above == 0 || above == 16) return 0;
-  w.nl = w.np = w.err = 0;
+// Hypercube::check_ambiguous + construct_polyhedrons (src/cornelius.cpp:
+// 1776-1878) and the elements' centroids and normals (:761-935), one lane.
+// geo[e][8] = centroid[4], normal[4]; returns the element count or -1.
+__device__ int polyhedra(WarpWork& w, double E0, double* geo) {
   int namb = 0, nlines = 0;
-#pragma unroll 1
-  for (int i = 0; i < 4; i++)
-#pragma unroll 1
-    for (int j = 0; j < 2; j++) {
-      int ca;
-      nlines += cube3(w, hc, i, j, dx, E0, ca);
-      if (ca) namb++;
-    }
-  if (w.err) return -1;
+  unsigned char fl[64];  // polygons in the reference's order: 3-cube, then polygon
+  int nf = 0;
+  for (int c = 0; c < 8; c++) {
+    if (w.camb[c]) namb++;
+    nlines += w.nl[c];
+    for (int q = 0; q < w.np[c]; q++) fl[nf++] = (unsigned char)(8 * c + q);
+  }
   int amb = namb;
   if (amb == 0) {
     int pts = 0;
 #pragma unroll
     for (int k = 0; k < 16; k++)
-      if (hc[k] < E0) pts++;
+      if (w.hc[k] < E0) pts++;
     if (pts > 8) pts = 16 - pts;
     if (nlines == 24 && pts == 2) amb++;
   }
-  // polyhedra as lists of polygon indices
-  unsigned char ph[kMaxElem][kMaxPoly];
+  unsigned char ph[kMaxElem][64];
   int nph[kMaxElem], nel = 0;
   if (amb > 0) {
-    unsigned long long unused = w.np >= 64 ? ~0ull : ((1ull << w.np) - 1);
+    unsigned long long unused = nf >= 64 ? ~0ull : ((1ull << nf) - 1);
     int used = 0;
     do {
       if (nel >= kMaxElem) return -1;
       nph[nel] = 0;
-      for (int i = 0; i < w.np; i++) {
+      for (int i = 0; i < nf; i++) {
         if (!((unused >> i) & 1)) continue;
         bool add = nph[nel] == 0;
         if (!add) {
-          const Poly& p = w.P[i];
+          const Poly& p = w.P[fl[i] >> 3][fl[i] & 7];
           for (int q = 0; q < nph[nel] && !add; q++) {
-            const Poly& pq = w.P[ph[nel][q]];
+            const Poly& pq = w.P[ph[nel][q] >> 3][ph[nel][q] & 7];
             for (int j = 0; j < p.n && !add; j++)
               for (int k = 0; k < pq.n && !add; k++)
-                if (lines_equal(w.L[p.li[j]], w.L[pq.li[k]])) add = true;
+                if (cn::lines_equal(w.L[p.li[j]], w.L[pq.li[k]])) add = true;
           }
         }
         if (add) {
-          ph[nel][nph[nel]++] = (unsigned char)i;
+          ph[nel][nph[nel]++] = fl[i];
           unused &= ~(1ull << i);
           used++;
           i = 0;
         }
       }
       nel++;
-    } while (used < w.np);
+    } while (used < nf);
   } else {
     nph[0] = 0;
-    for (int i = 0; i < w.np; i++) ph[0][nph[0]++] = (unsigned char)i;
+    for (int i = 0; i < nf; i++) ph[0][nph[0]++] = fl[i];
     nel = 1;
   }
-  for (int i = 0; i < w.np; i++) poly_centroid(w, w.P[i]);
 #pragma unroll 1
   for (int e = 0; e < nel; e++) {
     int ntet = 0;
     double mean[4] = {0, 0, 0, 0};
     for (int q = 0; q < nph[e]; q++) {
-      const Poly& pg = w.P[ph[e][q]];
+      const Poly& pg = w.P[ph[e][q] >> 3][ph[e][q] & 7];
       ntet += pg.n;
       for (int j = 0; j < pg.n; j++) {
         const Line& l = w.L[pg.li[j]];
@@ -439,7 +446,7 @@ __device__ int find_surface_4d(Work& w, const double* hc, const double* dx, doub
     for (int k = 0; k < 4; k++) mean[k] = mean[k] / (double)(2.0 * ntet);
     double up[4] = {0, 0, 0, 0}, down = 0, a[4], b[4], c[4], n[4];
     for (int q = 0; q < nph[e]; q++) {
-      const Poly& pg = w.P[ph[e][q]];
+      const Poly& pg = w.P[ph[e][q] >> 3][ph[e][q] & 7];
       for (int j = 0; j < pg.n; j++) {
         const Line& l = w.L[pg.li[j]];
         const double *p1 = lstart(l), *p2 = lend(l);
@@ -449,7 +456,7 @@ __device__ int find_surface_4d(Work& w, const double* hc, const double* dx, doub
           b[k] = p2[k] - mean[k];
           c[k] = pg.cen[k] - mean[k];
         }
-        tetra(a, b, c, n);
+        cn::tetra(a, b, c, n);
         double V = 0;
 #pragma unroll
         for (int k = 0; k < 4; k++) V += n[k] * n[k];
@@ -459,14 +466,12 @@ __device__ int find_surface_4d(Work& w, const double* hc, const double* dx, doub
         down += V;
       }
     }
-    double* C = cent[e];
+    double C[4];
 #pragma unroll
     for (int k = 0; k < 4; k++) C[k] = up[k] / down;
-    double* Nn = norm[e];
-#pragma unroll
-    for (int k = 0; k < 4; k++) Nn[k] = 0;
+    double Nn[4] = {0, 0, 0, 0};
     for (int q = 0; q < nph[e]; q++) {
-      const Poly& pg = w.P[ph[e][q]];
+      const Poly& pg = w.P[ph[e][q] >> 3][ph[e][q] & 7];
       for (int j = 0; j < pg.n; j++) {
         const Line& l = w.L[pg.li[j]];
         const double *p1 = lstart(l), *p2 = lend(l);
@@ -476,7 +481,7 @@ __device__ int find_surface_4d(Work& w, const double* hc, const double* dx, doub
           b[k] = p2[k] - C[k];
           c[k] = pg.cen[k] - C[k];
         }
-        tetra(a, b, c, n);
+        cn::tetra(a, b, c, n);
         double dot = 0;
 #pragma unroll
         for (int k = 0; k < 4; k++) dot += (l.o[k] - C[k]) * n[k];
@@ -488,9 +493,39 @@ __device__ int find_surface_4d(Work& w, const double* hc, const double* dx, doub
         for (int k = 0; k < 4; k++) Nn[k] += n[k];
       }
     }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      geo[e * 8 + k] = C[k];
+      geo[e * 8 + 4 + k] = Nn[k];
+    }
   }
   return nel;
 }
 
-}  // namespace cn
+// The whole hypercube by the calling warp (every lane calls it, after the
+// caller has put the 16 corner values into w.hc and synchronised the warp).
+// Lane 0 gets the element count (-1 where the reference stops) and has
+// written the elements to geo.
+__device__ int find_surface_warp(WarpWork& w, const double* dx, double E0, double* geo) {
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) w.err = 0;
+  __syncwarp();
+  // Cornelius::find_surface_4d: no elements unless the iso-value straddles
+  // the corners (src/cornelius.cpp:2254-2268)
+  int above = 0;
+#pragma unroll
+  for (int k = 0; k < 16; k++)
+    if (w.hc[k] >= E0) above++;
+  if (above == 0 || above == 16) return 0;  // uniform across the warp
+  for (int t = lane; t < 48; t += 32) square_instance(w, t, dx, E0);
+  __syncwarp();
+  if (lane < 8) cube_polygons(w, lane);
+  __syncwarp();
+  int n = 0;
+  if (lane == 0) n = w.err ? -1 : polyhedra(w, E0, geo);
+  __syncwarp();
+  return n;
+}
+
+}  // namespace cnw
 }  // namespace vh

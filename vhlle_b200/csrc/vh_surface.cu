@@ -177,7 +177,7 @@ void launch_totals(const Geo& g, const EosDev& E, const Fields& f, double tau, d
 //   2. k_surf_count      straddling interior cubes per block
 //   3. k_scan_excl       block offsets (one block)
 //   4. k_surf_compact    straddling cube list in the reference's loop order
-//   5. k_surf_cornelius  Cornelius per cube -> centroids, normals, counts
+//   5. k_surf_cornelius  Cornelius, a warp per cube -> centroids, normals, counts
 //   6. k_scan_excl       element offsets
 //   7. k_surf_elements   one record per element (+ its sums' contributions)
 //   8. k_sum_cols        deterministic sums of the contributions
@@ -310,37 +310,39 @@ __global__ void __launch_bounds__(kSurfBlock) k_surf_compact(Geo g, const double
     cubes[blkoff[blockIdx.x] + woff[w] + __popc(bal & ((1u << lane) - 1u))] = (int)t;
 }
 
-constexpr int kCornBlock = 64;
 constexpr int kGeo = 8;  // centroid[4], normal[4] per element
 
-__global__ void __launch_bounds__(kCornBlock) k_surf_cornelius(
+// One warp per straddling hypercube (vh_cornelius.cuh), two per block.
+constexpr int kCornWarps = 2;
+
+__global__ void __launch_bounds__(32 * kCornWarps) k_surf_cornelius(
     Geo g, const double* __restrict__ eN, const double* __restrict__ eP, double e0, double dt4,
     const int* __restrict__ cubes, int ncubes, double* __restrict__ geo, int* __restrict__ cnt,
     unsigned* err) {
-  const int k = blockIdx.x * kCornBlock + threadIdx.x;
-  if (k >= ncubes) return;
+  __shared__ cnw::WarpWork ws[kCornWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kCornWarps + warp;
+  if (k >= ncubes) return;  // the whole warp
+  cnw::WarpWork& w = ws[warp];
   int ix, iy, iz;
-  double hc[16];
   cube_cell(g, cubes[k], ix, iy, iz);
-  load_cube(g, eN, eP, ix, iy, iz, hc);
+  if (lane < 16) {  // corner it*8 + c: Qprev layer (it = 0) or Q layer (it = 1)
+    const int c = lane & 7;
+    const long long i = cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1));
+    w.hc[lane] = (lane >> 3) ? eN[i] : eP[i];
+  }
+  __syncwarp();
   // Fluid::Fluid's Cornelius cell sizes {dt, dx, dy, dz}, src/fld.cpp:106-108
   const double dx4[4] = {dt4, g.dx, g.dy, g.dz};
-  cn::Work w;
-  double cent[cn::kMaxElem][4], norm[cn::kMaxElem][4];
-  int n = cn::find_surface_4d(w, hc, dx4, e0, cent, norm);
-  if (n < 0) {
-    atomicOr(err, ERR_SURFACE);
-    n = 0;
-  }
   double* o = geo + (long long)k * cn::kMaxElem * kGeo;
-  for (int e = 0; e < n; e++) {
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-      o[e * kGeo + d] = cent[e][d];
-      o[e * kGeo + 4 + d] = norm[e][d];
+  int n = cnw::find_surface_warp(w, dx4, e0, o);
+  if (lane == 0) {
+    if (n < 0) {
+      atomicOr(err, ERR_SURFACE);
+      n = 0;
     }
+    cnt[k] = n;
   }
-  cnt[k] = n;
 }
 
 // transformToLab, src/fld.cpp:508-513
@@ -541,7 +543,7 @@ void launch_surf_compact(const Geo& g, const double* eN, const double* eP, doubl
 void launch_surf_cornelius(const Geo& g, const double* eN, const double* eP, double e0, double dtf,
                            const int* cubes, int ncubes, double* geo, int* cnt, int* nel,
                            unsigned* err, cudaStream_t s) {
-  k_surf_cornelius<<<(ncubes + kCornBlock - 1) / kCornBlock, kCornBlock, 0, s>>>(
+  k_surf_cornelius<<<(ncubes + kCornWarps - 1) / kCornWarps, 32 * kCornWarps, 0, s>>>(
       g, eN, eP, e0, dtf, cubes, ncubes, geo, cnt, err);
   k_scan_excl<<<1, kScanBlock, 0, s>>>(cnt, ncubes, nel);
 }
@@ -561,34 +563,25 @@ void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double
 
 namespace vh {
 
-__global__ void __launch_bounds__(kCornBlock) k_cornelius_batch(const double* __restrict__ cubes,
-                                                                int n, double d0, double d1,
-                                                                double d2, double d3, double e0,
-                                                                int* __restrict__ counts,
-                                                                double* __restrict__ geo) {
-  const int k = blockIdx.x * kCornBlock + threadIdx.x;
+__global__ void __launch_bounds__(32 * kCornWarps) k_cornelius_batch(
+    const double* __restrict__ cubes, int n, double d0, double d1, double d2, double d3, double e0,
+    int* __restrict__ counts, double* __restrict__ geo) {
+  __shared__ cnw::WarpWork ws[kCornWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int k = blockIdx.x * kCornWarps + warp;
   if (k >= n) return;
-  double hc[16];
-#pragma unroll
-  for (int q = 0; q < 16; q++) hc[q] = cubes[(long long)k * 16 + q];
+  cnw::WarpWork& w = ws[warp];
+  if (lane < 16) w.hc[lane] = cubes[(long long)k * 16 + lane];
+  __syncwarp();
   const double dx4[4] = {d0, d1, d2, d3};
-  cn::Work w;
-  double cent[cn::kMaxElem][4], norm[cn::kMaxElem][4];
-  const int m = cn::find_surface_4d(w, hc, dx4, e0, cent, norm);
-  counts[k] = m;
-  double* o = geo + (long long)k * cn::kMaxElem * kGeo;
-  for (int e = 0; e < m; e++)
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-      o[e * kGeo + d] = cent[e][d];
-      o[e * kGeo + 4 + d] = norm[e][d];
-    }
+  const int m = cnw::find_surface_warp(w, dx4, e0, geo + (long long)k * cn::kMaxElem * kGeo);
+  if (lane == 0) counts[k] = m;
 }
 
 void launch_cornelius_batch(const double* cubes, int n, const double* dx, double e0, int* counts,
                             double* geo, cudaStream_t s) {
   if (n > 0)
-    k_cornelius_batch<<<(n + kCornBlock - 1) / kCornBlock, kCornBlock, 0, s>>>(
+    k_cornelius_batch<<<(n + kCornWarps - 1) / kCornWarps, 32 * kCornWarps, 0, s>>>(
         cubes, n, dx[0], dx[1], dx[2], dx[3], e0, counts, geo);
 }
 
