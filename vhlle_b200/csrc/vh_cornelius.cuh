@@ -205,7 +205,9 @@ __device__ bool lines_equal(const Line& l1, const Line& l2) {
 
 // ---------------------------------------------------------------------
 // The warp's part: 48 square instances (8 3-cubes x 6 squares) across the
-// lanes, each 3-cube's polygons in one of 8 lanes, the polyhedra in lane 0.
+// lanes, each 3-cube's polygons in one of 8 lanes, the joining into
+// polyhedra in lane 0, the tetrahedra of the centroid and normal sums across
+// the lanes.
 namespace cnw {
 
 using cn::kEps;
@@ -227,6 +229,11 @@ struct WarpWork {
   int np[8], nl[8], camb[8];
   double hc[16];
   int err;
+  // the elements as tetrahedra (one per polygon line), in the order of the
+  // reference's sums: element e owns tetrahedra es[e] .. es[e+1]-1
+  unsigned char tp[96], tl[96];  // polygon code (8 * 3-cube + polygon), line id
+  int es[kMaxElem + 1], nel;
+  double term[96][5];  // per-tetrahedron terms of the current sum
 };
 
 // Square instance t = 6 c + s: 3-cube c (constant dimension c / 2 at corner
@@ -374,9 +381,9 @@ __device__ void cube_polygons(WarpWork& w, int c) {
 }
 
 // Hypercube::check_ambiguous + construct_polyhedrons (src/cornelius.cpp:
-// 1776-1878) and the elements' centroids and normals (:761-935), one lane.
-// geo[e][8] = centroid[4], normal[4]; returns the element count or -1.
-__device__ int polyhedra(WarpWork& w, double E0, double* geo) {
+// 1776-1878), one lane: fills the tetrahedron list and w.nel (-1 where the
+// reference stops).
+__device__ void assemble(WarpWork& w, double E0) {
   int namb = 0, nlines = 0;
   unsigned char fl[64];  // polygons in the reference's order: 3-cube, then polygon
   int nf = 0;
@@ -400,7 +407,10 @@ __device__ int polyhedra(WarpWork& w, double E0, double* geo) {
     unsigned long long unused = nf >= 64 ? ~0ull : ((1ull << nf) - 1);
     int used = 0;
     do {
-      if (nel >= kMaxElem) return -1;
+      if (nel >= kMaxElem) {
+        w.nel = -1;
+        return;
+      }
       nph[nel] = 0;
       for (int i = 0; i < nf; i++) {
         if (!((unused >> i) & 1)) continue;
@@ -428,84 +438,109 @@ __device__ int polyhedra(WarpWork& w, double E0, double* geo) {
     for (int i = 0; i < nf; i++) ph[0][nph[0]++] = fl[i];
     nel = 1;
   }
-#pragma unroll 1
+  int nt = 0;
   for (int e = 0; e < nel; e++) {
-    int ntet = 0;
-    double mean[4] = {0, 0, 0, 0};
-    for (int q = 0; q < nph[e]; q++) {
-      const Poly& pg = w.P[ph[e][q] >> 3][ph[e][q] & 7];
-      ntet += pg.n;
-      for (int j = 0; j < pg.n; j++) {
-        const Line& l = w.L[pg.li[j]];
-        const double *p1 = lstart(l), *p2 = lend(l);
-#pragma unroll
-        for (int k = 0; k < 4; k++) mean[k] += p1[k] + p2[k];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < 4; k++) mean[k] = mean[k] / (double)(2.0 * ntet);
-    double up[4] = {0, 0, 0, 0}, down = 0, a[4], b[4], c[4], n[4];
+    w.es[e] = nt;
     for (int q = 0; q < nph[e]; q++) {
       const Poly& pg = w.P[ph[e][q] >> 3][ph[e][q] & 7];
       for (int j = 0; j < pg.n; j++) {
-        const Line& l = w.L[pg.li[j]];
-        const double *p1 = lstart(l), *p2 = lend(l);
-#pragma unroll
-        for (int k = 0; k < 4; k++) {
-          a[k] = p1[k] - mean[k];
-          b[k] = p2[k] - mean[k];
-          c[k] = pg.cen[k] - mean[k];
-        }
-        cn::tetra(a, b, c, n);
-        double V = 0;
-#pragma unroll
-        for (int k = 0; k < 4; k++) V += n[k] * n[k];
-        V = sqrt(V);
-#pragma unroll
-        for (int k = 0; k < 4; k++) up[k] += (p1[k] + p2[k] + pg.cen[k] + mean[k]) / 4.0 * V;
-        down += V;
+        w.tp[nt] = ph[e][q];
+        w.tl[nt] = pg.li[j];
+        nt++;
       }
     }
-    double C[4];
+  }
+  w.es[nel] = nt;
+  w.nel = nel;
+}
+
+// Polyhedron::calculate_centroid and calculate_normal (src/cornelius.cpp:
+// 790-935) of element e, all lanes: each lane forms the terms of its
+// tetrahedra, then every lane adds them in the reference's order (the same
+// uniform sums in every lane).  Lane 0 writes geo[e][8].
+__device__ void element(WarpWork& w, int e, double* geo) {
+  const int lane = threadIdx.x & 31, t0 = w.es[e], t1 = w.es[e + 1];
+  double mean[4] = {0, 0, 0, 0};
+  for (int t = t0; t < t1; t++) {
+    const Line& l = w.L[w.tl[t]];
+    const double *p1 = lstart(l), *p2 = lend(l);
 #pragma unroll
-    for (int k = 0; k < 4; k++) C[k] = up[k] / down;
-    double Nn[4] = {0, 0, 0, 0};
-    for (int q = 0; q < nph[e]; q++) {
-      const Poly& pg = w.P[ph[e][q] >> 3][ph[e][q] & 7];
-      for (int j = 0; j < pg.n; j++) {
-        const Line& l = w.L[pg.li[j]];
-        const double *p1 = lstart(l), *p2 = lend(l);
+    for (int k = 0; k < 4; k++) mean[k] += p1[k] + p2[k];
+  }
 #pragma unroll
-        for (int k = 0; k < 4; k++) {
-          a[k] = p1[k] - C[k];
-          b[k] = p2[k] - C[k];
-          c[k] = pg.cen[k] - C[k];
-        }
-        cn::tetra(a, b, c, n);
-        double dot = 0;
+  for (int k = 0; k < 4; k++) mean[k] = mean[k] / (double)(2.0 * (t1 - t0));
+  double a[4], b[4], c[4], n[4];
+  for (int t = t0 + lane; t < t1; t += 32) {
+    const Line& l = w.L[w.tl[t]];
+    const Poly& pg = w.P[w.tp[t] >> 3][w.tp[t] & 7];
+    const double *p1 = lstart(l), *p2 = lend(l);
 #pragma unroll
-        for (int k = 0; k < 4; k++) dot += (l.o[k] - C[k]) * n[k];
-        if (dot < 0) {
-#pragma unroll
-          for (int k = 0; k < 4; k++) n[k] = -n[k];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; k++) Nn[k] += n[k];
-      }
+    for (int k = 0; k < 4; k++) {
+      a[k] = p1[k] - mean[k];
+      b[k] = p2[k] - mean[k];
+      c[k] = pg.cen[k] - mean[k];
     }
+    cn::tetra(a, b, c, n);
+    double V = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) V += n[k] * n[k];
+    V = sqrt(V);
+#pragma unroll
+    for (int k = 0; k < 4; k++) w.term[t][k] = (p1[k] + p2[k] + pg.cen[k] + mean[k]) / 4.0 * V;
+    w.term[t][4] = V;
+  }
+  __syncwarp();
+  double up[4] = {0, 0, 0, 0}, down = 0;
+  for (int t = t0; t < t1; t++) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) up[k] += w.term[t][k];
+    down += w.term[t][4];
+  }
+  double C[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) C[k] = up[k] / down;
+  __syncwarp();
+  for (int t = t0 + lane; t < t1; t += 32) {
+    const Line& l = w.L[w.tl[t]];
+    const Poly& pg = w.P[w.tp[t] >> 3][w.tp[t] & 7];
+    const double *p1 = lstart(l), *p2 = lend(l);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      a[k] = p1[k] - C[k];
+      b[k] = p2[k] - C[k];
+      c[k] = pg.cen[k] - C[k];
+    }
+    cn::tetra(a, b, c, n);
+    double dot = 0;
+#pragma unroll
+    for (int k = 0; k < 4; k++) dot += (l.o[k] - C[k]) * n[k];
+    if (dot < 0) {
+#pragma unroll
+      for (int k = 0; k < 4; k++) n[k] = -n[k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) w.term[t][k] = n[k];
+  }
+  __syncwarp();
+  double Nn[4] = {0, 0, 0, 0};
+  for (int t = t0; t < t1; t++) {
+#pragma unroll
+    for (int k = 0; k < 4; k++) Nn[k] += w.term[t][k];
+  }
+  if (lane == 0) {
 #pragma unroll
     for (int k = 0; k < 4; k++) {
       geo[e * 8 + k] = C[k];
       geo[e * 8 + 4 + k] = Nn[k];
     }
   }
-  return nel;
+  __syncwarp();
 }
 
 // The whole hypercube by the calling warp (every lane calls it, after the
 // caller has put the 16 corner values into w.hc and synchronised the warp).
-// Lane 0 gets the element count (-1 where the reference stops) and has
-// written the elements to geo.
+// Every lane gets the element count (-1 where the reference stops); lane 0
+// has written the elements to geo.
 __device__ int find_surface_warp(WarpWork& w, const double* dx, double E0, double* geo) {
   const int lane = threadIdx.x & 31;
   if (lane == 0) w.err = 0;
@@ -521,10 +556,16 @@ __device__ int find_surface_warp(WarpWork& w, const double* dx, double E0, doubl
   __syncwarp();
   if (lane < 8) cube_polygons(w, lane);
   __syncwarp();
-  int n = 0;
-  if (lane == 0) n = w.err ? -1 : polyhedra(w, E0, geo);
+  if (lane == 0) {
+    if (w.err)
+      w.nel = -1;
+    else
+      assemble(w, E0);
+  }
   __syncwarp();
-  return n;
+  const int nel = w.nel;
+  for (int e = 0; e < nel; e++) element(w, e, geo);
+  return nel;
 }
 
 }  // namespace cnw
