@@ -415,6 +415,17 @@ class Hydro {
     check(vh_totals(ctx_, f_->geteCrit(), &t.E), ctx_);
     return t;
   }
+  // The freeze-out elements of Fluid::outputSurface (src/fld.cpp:606-842)
+  // at the current tau, kept on the device; writeSurface appends them to a
+  // freezeout.dat-format file (extended records with e and nb if asked).
+  vh_surface_info surface() {
+    vh_surface_info si{};
+    check(vh_surface(ctx_, f_->geteCrit(), &si), ctx_);
+    return si;
+  }
+  void writeSurface(const char* path, bool extendFO) {
+    check(vh_surface_write(ctx_, path, extendFO ? 1 : 0), ctx_);
+  }
   // The driver's substep block (src/main.cpp:405-419); returns the count.
   int advance(double dtau, double etamin, double etamax, int nz) {
     if (!uploaded_) upload();

@@ -92,9 +92,11 @@ def test_gpu_resize_keeps_asymmetric_grid():
 
 def test_cpp_driver_loop_equals_oracle(tmp_path):
     """vhlle_run (C++ host layer over the C ABI) runs the reference driver
-    loop -- substeps at small tau, the x2 resize at tauGridResize, stop at
-    tauMax -- from a snapshot; its final grid equals the oracle driven
-    through the same loop, bit-for-bit."""
+    loop -- substeps at small tau, outputSurface every iteration, the x2
+    resize at tauGridResize, stop at tauMax or on an empty surface -- from a
+    snapshot.  Its final grid equals the oracle driven through the same loop
+    bit-for-bit; its printed element counts equal the oracle's and its
+    freezeout.dat records match to 1e-12 (15 printed digits)."""
     import subprocess
     from vhlle_b200 import build as B
     drv = B.build_driver()
@@ -107,20 +109,28 @@ def test_cpp_driver_loop_equals_oracle(tmp_path):
         tmp_path / "eos.dat"))
     setup.eos.write_eos1f(str(tmp_path / "eos.dat"))
     out = tmp_path / "out"
-    r = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", str(out)],
-                       capture_output=True, text=True, timeout=300)
-    assert r.returncode == 0, r.stdout[-2000:] + r.stderr
-    assert "grid resize" in r.stdout and "timestep reduced by 2" in r.stdout
+    run = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", str(out)],
+                         capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr
+    proc_out = run.stdout
+    assert "grid resize" in proc_out and "timestep reduced by 2" in proc_out
 
     o = P.OracleRun(setup)
     g = setup.grid
     resized = False
+    recs, counts, nsusp = [], [], []
     while True:
         o.advance(setup.dt, g.etamin, g.etamax, g.nz)
+        # Fluid::outputSurface; the Fluid's step is the full dtau (doubled
+        # by the resize), which is what the oracle's step is between advances
+        r, acc = o.surface(dtf=o.dt)
+        recs.append(r)
+        counts.append(len(r))
+        nsusp.append(int(acc["nsusp"]))
         if o.tau_now >= tau_resize and not resized:
             assert o.resize2x() == 1
             resized = True
-        if not o.tau_now < tau_max + 0.0001:
+        if not (o.tau_now < tau_max + 0.0001 and len(r) > 0):
             break
     nx, ny, nz, b, tau, dt, st = W.read_snapshot(str(out / "final.vhb"))
     assert tau == o.tau_now and dt == o.dt
@@ -129,3 +139,16 @@ def test_cpp_driver_loop_equals_oracle(tmp_path):
     exp = o.get_state()
     bad = compare_states(st, exp)
     assert not bad, bad
+    # the printed surface lines and the freezeout.dat records
+    printed = []
+    for line in proc_out.splitlines():
+        w = line.split()
+        if len(w) == 9 and w[6].isdigit() and w[7].isdigit():
+            printed.append((int(w[6]), int(w[7])))
+    assert printed == list(zip(counts, nsusp)), (printed, counts, nsusp)
+    assert sum(counts) > 0
+    fz = P.read_freezeout(str(out / "freezeout.dat"))
+    ref = np.concatenate(recs)[:, :27]
+    assert fz.shape == ref.shape
+    ok = np.abs(fz - ref) <= 1e-12 * np.maximum(np.abs(fz), np.abs(ref)) + 1e-300
+    assert ok.all(), np.argwhere(~ok)[:5]

@@ -9,11 +9,16 @@
 // Parameters are read exactly as the reference reads them (same keys,
 // defaults, "CCC"/"UUU" echo).  The hydro EoS is the EoS1f table named by
 // the extra key eos1fFile, else the conformal gas of 47.5 degrees of
-// freedom.  Each loop iteration prints tau and the interior totals of
-// Fluid::outputSurface; the final grid is written to DIR/final.vhb.
+// freedom.  Each loop iteration does what Fluid::outputSurface does: it
+// appends the freeze-out elements to DIR/freezeout.dat.unfinished (renamed
+// freezeout.dat at the end) and prints the same line (tau, E, Efull,
+// nbSurf, S, EtotSurf, elements, suspicious elements, cut-cell fraction);
+// the loop stops at tauMax or when an iteration finds no element, as the
+// reference's does.  The final grid is written to DIR/final.vhb.
 #include <sys/stat.h>
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <iomanip>
 #include <iostream>
@@ -107,28 +112,41 @@ int run(int argc, char** argv) {
   std::cout << "fluid allocation done\nIC done (tau0 = " << tau0 << ")\n";
 
   vhb::Hydro* h = new vhb::Hydro(f, eos, trcoeff, tau0, P.dtau);
+  // Fluid::initOutput (src/fld.cpp:119-129): the output directory and a
+  // fresh freezeout.dat.unfinished
+  mkdir(cl.outputDir.c_str(), 0755);
+  const std::string fo = cl.outputDir + "/freezeout.dat";
+  const std::string fo_unf = fo + ".unfinished";
+  std::remove(fo.c_str());
+  std::remove(fo_unf.c_str());
   bool resized = false;
   int nloops = 0;
+  long nelements = 0;
   std::cout << std::setprecision(6);
   do {
     const int nSubSteps = h->advance(P.dtau, P.etamin, P.etamax, P.nz);
     if (nSubSteps > 1) std::cout << "timestep reduced by " << nSubSteps << std::endl;
     const vhb::Totals t = h->totals();
+    const vh_surface_info si = h->surface();
+    h->writeSurface(fo_unf.c_str(), P.freezeoutExtend);
+    nelements = si.nelements;
+    // the line Fluid::outputSurface prints (src/fld.cpp:854-857)
     std::cout << std::setw(10) << h->getTau() << std::setw(13) << t.E << std::setw(13) << t.Efull
-              << std::setw(13) << t.Nb2 << std::setw(13) << t.S << std::setw(13)
-              << (float)t.nCoreCutCells / (float)t.nCoreCells << std::endl;
+              << std::setw(13) << si.nbSurf << std::setw(13) << t.S << std::setw(13)
+              << si.EtotSurf << std::setw(10) << si.nelements << std::setw(10) << si.nsusp
+              << std::setw(13) << (float)t.nCoreCutCells / (float)t.nCoreCells << std::endl;
     nloops++;
     if (h->getTau() >= P.tauResize && !resized) {
       std::cout << "grid resize\n";
       f = vhb::expandGrid2x(h, eos, eosH, trcoeff);
       resized = true;
     }
-  } while (h->getTau() < P.tauMax + 0.0001);
+  } while (h->getTau() < P.tauMax + 0.0001 && nelements > 0);
+  std::rename(fo_unf.c_str(), fo.c_str());  // Fluid::renameOutput
 
   h->sync();
   unsigned bits = 0;
   vhb::check(vh_error_bits(h->context(), &bits), h->context());
-  mkdir(cl.outputDir.c_str(), 0755);
   const std::string out = cl.outputDir + "/final.vhb";
   f->saveSnapshot(out.c_str(), h->getTau(), h->getDtau());
   std::cout << "loops " << nloops << " error_bits " << bits << " final " << out << std::endl;
