@@ -64,8 +64,13 @@ __global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restri
 // Cell::getPrimVarRight / getPrimVarLeft or their H variants,
 // src/cll.cpp:106-204).  F[c*N + i] holds the flux of the face on the +DIR
 // side of cell i (0 where the reference adds nothing).
+// Occupancy (measured over 100 steps of the 101x101x51 event): 8 blocks of
+// 128 threads per SM (64 registers, a few spills) are 11 % faster than the
+// unbounded build (80 registers, 6 blocks); 10 blocks are slower.  The
+// same sweep set k_update to 12 blocks (-14 %), k_visc_prims to 8 (-14 %),
+// k_visc_update to 8 (-10 %); k_is_advect stays unbounded (8 blocks: +52 %).
 template <int DIR, bool PRED>
-__global__ void __launch_bounds__(128) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
+__global__ void __launch_bounds__(128, 8) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
                                               const double* __restrict__ m,
                                               double* __restrict__ F, const double* __restrict__ clk,
                                               unsigned* err) {
@@ -119,7 +124,7 @@ __global__ void __launch_bounds__(128) k_face(Geo g, EosDev E, const double* __r
 // src/hdo.cpp:307-353), then Cell::updateQtoQhByFlux (predictor) or
 // Cell::updateByFlux (corrector), src/cll.cpp:70-88.
 template <bool PRED>
-__global__ void __launch_bounds__(128) k_update(Geo g, EosDev E, double* __restrict__ Q,
+__global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __restrict__ Q,
                                                 double* __restrict__ Qh,
                                                 double* __restrict__ Qprev,
                                                 const double* __restrict__ Fx,
@@ -246,7 +251,7 @@ __global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char*
 __device__ __forceinline__ double maxM_at(const Geo& g, const double* __restrict__ m, int ix,
                                           int iy, int iz);
 
-__global__ void __launch_bounds__(128) k_visc_prims(Geo g, EosDev E, TrDev tr,
+__global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr,
                                                     const double* __restrict__ Q,
                                                     const double* __restrict__ Qprev,
                                                     const double* __restrict__ Qh,
@@ -826,7 +831,7 @@ __device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const 
   return true;
 }
 
-__global__ void __launch_bounds__(128) k_visc_update(Geo g, const double* __restrict__ pA,
+__global__ void __launch_bounds__(128, 8) k_visc_update(Geo g, const double* __restrict__ pA,
                                                      const double* __restrict__ piH,
                                                      const double* __restrict__ PiH,
                                                      const double* __restrict__ m,
