@@ -237,13 +237,13 @@ def _reset(h, setup):
     h.set_dtau(setup.dt)
 
 
-def batch_measure(capi, W, n_events, steps, device):
+def batch_measure(capi, W, n_events, steps, device, nz=None):
     """Event-by-event batch (the 256-event configuration's generator, its
     first n_events): every event stepped alone through vh_advance, one after
     another on the default stream, against the same events advanced by one
     vh_batch graph per iteration after the online tuning.  Device time with
     CUDA events; the same states are reset between the two runs."""
-    evs = W.batch_events(n_events)
+    evs = W.batch_events(n_events, nz=nz)
     cells = sum(s.grid.ncells for s in evs)
     hs = [capi.GpuHydro(s, device=device) for s in evs]
     drv = [(s.dt, s.grid.etamin, s.grid.etamax, s.grid.nz) for s in evs]
@@ -285,8 +285,9 @@ def batch_measure(capi, W, n_events, steps, device):
     for h in hs:
         h.close()
     return {"events": n_events, "steps": steps, "cells": cells,
-            "grids": "%d..%d cells (61x61x1 .. 121x121x61 family)" % (
-                min(s.grid.ncells for s in evs), max(s.grid.ncells for s in evs)),
+            "grids": "%d..%d cells (%s)" % (
+                min(s.grid.ncells for s in evs), max(s.grid.ncells for s in evs),
+                "61x61x1 .. 121x121x61 family" if nz is None else "nz = %d" % nz),
             "plain_per_event": cells * steps / (plain_ms / 1e3),
             "batched_graph": cells * steps / (batch_ms / 1e3),
             "speedup": plain_ms / batch_ms, "unit": UNIT, "error_bits": bits,
@@ -491,9 +492,10 @@ def main():
                "note": "state uploaded and downloaded every step, surface records every %d"
                        % SURF_EVERY}
 
-    batch = None
+    batch = batch2d = None
     if args.batch_events > 0:
         batch = batch_measure(capi, W, args.batch_events, args.batch_steps, local)
+        batch2d = batch_measure(capi, W, 2 * args.batch_events, 2 * args.batch_steps, local, nz=1)
     learned = None
     if not args.no_learned_guess:
         learned = learned_guess_measure(capi, W, setup, 30, local)
@@ -514,7 +516,7 @@ def main():
                        "l2": "inputs larger than L2 (%.0f MB of resident fields)" % (
                            cells * 8 * 127 / 1e6)},
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
-            "e2e": e2e, "cpu_baseline": cpu, "batch": batch, "learned_guess": learned,
+            "e2e": e2e, "cpu_baseline": cpu, "batch": batch, "batch_2d": batch2d, "learned_guess": learned,
             "gpu_launches": lps * args.steps + 9 * (args.steps // SURF_EVERY), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

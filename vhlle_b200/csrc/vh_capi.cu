@@ -702,43 +702,48 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
         (st = dalloc(ctx, &S.partial, (size_t)(kSurfPartials + 1) * vh::kSurfAcc)))
       return st;
   }
+  // Every stage reads the counts from device memory, so the call waits for
+  // the GPU once, at the end.  The buffers start at 64k cubes and twice as
+  // many elements; a call that finds more grows them and runs again (the
+  // fields it reads are unchanged in between, so the result is the same).
+  const long long ninterior = std::max(1LL, vh::surf_ncube(g));
+  size_t want_c = std::max<size_t>(S.cap_cubes, (size_t)std::min(ninterior, 65536LL));
+  size_t want_e = std::max<size_t>(S.cap_rec / vh::kSurfRec, 2 * want_c);
   cudaStream_t s = ctx->stream;
   const double taup = ctx->tau - ctx->fluid_dt;
-  vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, taup, S.eN, S.eP, s);
-  vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
-  VH_CUDA(ctx, cudaGetLastError());
-  int ncubes = 0, nel = 0;
-  VH_CUDA(ctx, cudaMemcpyAsync(&ncubes, S.counters, sizeof(int), cudaMemcpyDeviceToHost, s));
-  VH_CUDA(ctx, cudaStreamSynchronize(s));
-  if (ncubes > 0) {
-    if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, (size_t)ncubes)) ||
-        (st = dgrow(ctx, &S.geo, &S.cap_geo,
-                    (size_t)ncubes * vh::kSurfMaxElemPerCube * vh::kSurfGeo)) ||
-        (st = dgrow(ctx, &S.cnt, &S.cap_cnt, (size_t)ncubes + 1)))
-      return st;
-    vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, s);
-    vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, ncubes, S.geo, S.cnt,
-                              S.counters + 1, ctx->f.err, s);
-    VH_CUDA(ctx, cudaGetLastError());
-    VH_CUDA(ctx, cudaMemcpyAsync(&nel, S.counters + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
-    VH_CUDA(ctx, cudaStreamSynchronize(s));
-  }
+  int cnts[2] = {0, 0};
   double acc[vh::kSurfAcc] = {0., 0., 0., 0., 0.};
-  if (nel > 0) {
-    if ((st = dgrow(ctx, &S.rec, &S.cap_rec, (size_t)nel * vh::kSurfRec)) ||
-        (st = dgrow(ctx, &S.contrib, &S.cap_contrib, (size_t)nel * vh::kSurfAcc)))
-      return st;
-    const int npart = std::max(1, std::min(kSurfPartials, (nel + 255) / 256));
-    vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
-                             ctx->grid.ymin, ctx->grid.etamin, S.cubes, ncubes, S.geo, S.cnt, nel,
-                             S.rec, S.contrib, S.partial, npart, s);
-    VH_CUDA(ctx, cudaGetLastError());
-    VH_CUDA(ctx, cudaMemcpyAsync(acc, S.partial + (size_t)npart * vh::kSurfAcc, sizeof acc,
-                                 cudaMemcpyDeviceToHost, s));
-  }
   unsigned bits = 0;
-  VH_CUDA(ctx, cudaMemcpyAsync(&bits, ctx->f.err, sizeof bits, cudaMemcpyDeviceToHost, s));
-  VH_CUDA(ctx, cudaStreamSynchronize(s));
+  for (int pass = 0; pass < 2; pass++) {
+    if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, want_c)) ||
+        (st = dgrow(ctx, &S.geo, &S.cap_geo, want_c * vh::kSurfMaxElemPerCube * vh::kSurfGeo)) ||
+        (st = dgrow(ctx, &S.cnt, &S.cap_cnt, want_c + 1)) ||
+        (st = dgrow(ctx, &S.rec, &S.cap_rec, want_e * vh::kSurfRec)) ||
+        (st = dgrow(ctx, &S.contrib, &S.cap_contrib, want_e * vh::kSurfAcc)))
+      return st;
+    const int cap_c = (int)std::min<size_t>(want_c, INT32_MAX / 16);
+    const int cap_e = (int)std::min<size_t>(want_e, INT32_MAX / 32);
+    vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, taup, S.eN, S.eP, s);
+    vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
+    vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, cap_c, s);
+    vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, S.counters, cap_c,
+                              S.geo, S.cnt, ctx->f.err, s);
+    vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
+                             ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
+                             S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
+    VH_CUDA(ctx, cudaGetLastError());
+    VH_CUDA(ctx, cudaMemcpyAsync(cnts, S.counters, sizeof cnts, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaMemcpyAsync(acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
+                                 sizeof acc, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaMemcpyAsync(&bits, ctx->f.err, sizeof bits, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaStreamSynchronize(s));
+    if ((size_t)cnts[0] <= (size_t)cap_c && (size_t)cnts[1] <= (size_t)cap_e) break;
+    if (pass == 1) return fail(ctx, VH_ERR_STATE, "vh_surface: element buffers did not grow");
+    want_c = std::max(want_c, (size_t)cnts[0] + (size_t)cnts[0] / 4 + 1);
+    // a cube holds at most kSurfMaxElemPerCube elements
+    want_e = std::max(want_e, (size_t)cnts[0] * vh::kSurfMaxElemPerCube);
+  }
+  const int nel = cnts[1];
   S.nel = nel;
   ctx->EtotSurf += acc[1];
   ctx->nbSurf += acc[2];

@@ -253,9 +253,13 @@ __global__ void __launch_bounds__(kSurfBlock) k_surf_count(Geo g, const double* 
 
 // Exclusive prefix sum of a[0..n) in place by one block; *total = the sum.
 constexpr int kScanBlock = 1024;
+// With n_dev set, n = min(*n_dev, cap) is read on the device.
 __global__ void __launch_bounds__(kScanBlock) k_scan_excl(int* __restrict__ a, int n,
-                                                          int* __restrict__ total) {
+                                                          int* __restrict__ total,
+                                                          const int* __restrict__ n_dev,
+                                                          int cap) {
   __shared__ long long part[kScanBlock];
+  if (n_dev) n = min(*n_dev, cap);
   const int per = (n + kScanBlock - 1) / kScanBlock;
   const int b = threadIdx.x * per, e = min(n, b + per);
   long long s = 0;
@@ -282,7 +286,7 @@ __global__ void __launch_bounds__(kSurfBlock) k_surf_compact(Geo g, const double
                                                              const double* __restrict__ eP,
                                                              double e0, long long ncube,
                                                              const int* __restrict__ blkoff,
-                                                             int* __restrict__ cubes) {
+                                                             int* __restrict__ cubes, int cap) {
   __shared__ int woff[kSurfBlock / 32];
   const long long t = (long long)blockIdx.x * kSurfBlock + threadIdx.x;
   bool flag = false;
@@ -306,8 +310,8 @@ __global__ void __launch_bounds__(kSurfBlock) k_surf_compact(Geo g, const double
     }
   }
   __syncthreads();
-  if (flag)
-    cubes[blkoff[blockIdx.x] + woff[w] + __popc(bal & ((1u << lane) - 1u))] = (int)t;
+  const int slot = blkoff[blockIdx.x] + woff[w] + __popc(bal & ((1u << lane) - 1u));
+  if (flag && slot < cap) cubes[slot] = (int)t;  // past cap: the host grows and reruns
 }
 
 constexpr int kGeo = 8;  // centroid[4], normal[4] per element
@@ -317,31 +321,33 @@ constexpr int kCornWarps = 2;
 
 __global__ void __launch_bounds__(32 * kCornWarps) k_surf_cornelius(
     Geo g, const double* __restrict__ eN, const double* __restrict__ eP, double e0, double dt4,
-    const int* __restrict__ cubes, int ncubes, double* __restrict__ geo, int* __restrict__ cnt,
-    unsigned* err) {
+    const int* __restrict__ cubes, const int* __restrict__ ncubes_dev, int cap,
+    double* __restrict__ geo, int* __restrict__ cnt, unsigned* err) {
   __shared__ cnw::WarpWork ws[kCornWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int k = blockIdx.x * kCornWarps + warp;
-  if (k >= ncubes) return;  // the whole warp
+  const int ncubes = min(*ncubes_dev, cap);
   cnw::WarpWork& w = ws[warp];
-  int ix, iy, iz;
-  cube_cell(g, cubes[k], ix, iy, iz);
-  if (lane < 16) {  // corner it*8 + c: Qprev layer (it = 0) or Q layer (it = 1)
-    const int c = lane & 7;
-    const long long i = cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1));
-    w.hc[lane] = (lane >> 3) ? eN[i] : eP[i];
-  }
-  __syncwarp();
-  // Fluid::Fluid's Cornelius cell sizes {dt, dx, dy, dz}, src/fld.cpp:106-108
-  const double dx4[4] = {dt4, g.dx, g.dy, g.dz};
-  double* o = geo + (long long)k * cn::kMaxElem * kGeo;
-  int n = cnw::find_surface_warp(w, dx4, e0, o);
-  if (lane == 0) {
-    if (n < 0) {
-      atomicOr(err, ERR_SURFACE);
-      n = 0;
+  for (int k = blockIdx.x * kCornWarps + warp; k < ncubes; k += gridDim.x * kCornWarps) {
+    int ix, iy, iz;
+    cube_cell(g, cubes[k], ix, iy, iz);
+    if (lane < 16) {  // corner it*8 + c: Qprev layer (it = 0) or Q layer (it = 1)
+      const int c = lane & 7;
+      const long long i = cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1));
+      w.hc[lane] = (lane >> 3) ? eN[i] : eP[i];
     }
-    cnt[k] = n;
+    __syncwarp();
+    // Fluid::Fluid's Cornelius cell sizes {dt, dx, dy, dz}, src/fld.cpp:106-108
+    const double dx4[4] = {dt4, g.dx, g.dy, g.dz};
+    double* o = geo + (long long)k * cn::kMaxElem * kGeo;
+    int n = cnw::find_surface_warp(w, dx4, e0, o);
+    if (lane == 0) {
+      if (n < 0) {
+        atomicOr(err, ERR_SURFACE);
+        n = 0;
+      }
+      cnt[k] = n;
+    }
+    __syncwarp();
   }
 }
 
@@ -359,19 +365,25 @@ struct SurfArgs {
   const double *Q, *Qprev, *pi, *Pi;
   double tau, dtf, ecrit, xmin, ymin, zmin;
   const int* cubes;
-  int ncubes;
+  const int* counters;  // [0] straddling cubes, [1] elements (device)
+  int cap_cubes, cap_el;
   const double* geo;
   const int* off;
-  int nel;
   double* rec;
   double* contrib;
 };
 
+__device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncubes);
+
 __global__ void __launch_bounds__(128) k_surf_elements(SurfArgs a) {
-  const int el = blockIdx.x * blockDim.x + threadIdx.x;
-  if (el >= a.nel) return;
+  const int ncubes = min(a.counters[0], a.cap_cubes), nel = min(a.counters[1], a.cap_el);
+  for (int el = blockIdx.x * blockDim.x + threadIdx.x; el < nel; el += gridDim.x * blockDim.x)
+    surf_element(a, el, ncubes);
+}
+
+__device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncubes) {
   // the cube whose element range holds el: the last k with off[k] <= el
-  int lo = 0, hi = a.ncubes;
+  int lo = 0, hi = ncubes;
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
     if (a.off[mid] <= el)
@@ -488,9 +500,12 @@ __global__ void __launch_bounds__(128) k_surf_elements(SurfArgs a) {
 
 // Column sums of x[n][kSurfAcc] in a fixed tree: block partials, then one
 // block over the partials in index order.
+// With n_dev set, n = min(*n_dev, cap) rows are read on the device.
 __global__ void __launch_bounds__(kTotBlock) k_sum_cols(const double* __restrict__ x, int n,
-                                                        int ncol, double* __restrict__ out) {
+                                                        int ncol, double* __restrict__ out,
+                                                        const int* __restrict__ n_dev, int cap) {
   __shared__ double red[kTotBlock / 32];
+  if (n_dev) n = min(*n_dev, cap);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int c = 0; c < ncol; c++) {
     double s = 0.;
@@ -531,32 +546,40 @@ void launch_surf_count(const Geo& g, const double* eN, const double* eP, double 
     return;
   }
   k_surf_count<<<nb, kSurfBlock, 0, s>>>(g, eN, eP, e0, surf_ncube(g), blk);
-  k_scan_excl<<<1, kScanBlock, 0, s>>>(blk, nb, total);
+  k_scan_excl<<<1, kScanBlock, 0, s>>>(blk, nb, total, nullptr, 0);
 }
 
 void launch_surf_compact(const Geo& g, const double* eN, const double* eP, double e0,
-                         const int* blkoff, int* cubes, cudaStream_t s) {
+                         const int* blkoff, int* cubes, int cap, cudaStream_t s) {
   const int nb = surf_count_blocks(g);
-  if (nb) k_surf_compact<<<nb, kSurfBlock, 0, s>>>(g, eN, eP, e0, surf_ncube(g), blkoff, cubes);
+  if (nb)
+    k_surf_compact<<<nb, kSurfBlock, 0, s>>>(g, eN, eP, e0, surf_ncube(g), blkoff, cubes, cap);
 }
 
+// Grid-stride launches over the device-side counts (no host round trip):
+// 6 two-warp blocks per SM for Cornelius (its shared-memory limit), 8
+// blocks of 128 threads per SM for the elements.
+constexpr int kCornGrid = 148 * 6, kElemGrid = 148 * 8;
+
 void launch_surf_cornelius(const Geo& g, const double* eN, const double* eP, double e0, double dtf,
-                           const int* cubes, int ncubes, double* geo, int* cnt, int* nel,
+                           const int* cubes, int* counters, int cap_cubes, double* geo, int* cnt,
                            unsigned* err, cudaStream_t s) {
-  k_surf_cornelius<<<(ncubes + kCornWarps - 1) / kCornWarps, 32 * kCornWarps, 0, s>>>(
-      g, eN, eP, e0, dtf, cubes, ncubes, geo, cnt, err);
-  k_scan_excl<<<1, kScanBlock, 0, s>>>(cnt, ncubes, nel);
+  k_surf_cornelius<<<kCornGrid, 32 * kCornWarps, 0, s>>>(g, eN, eP, e0, dtf, cubes, counters,
+                                                         cap_cubes, geo, cnt, err);
+  k_scan_excl<<<1, kScanBlock, 0, s>>>(cnt, 0, counters + 1, counters, cap_cubes);
 }
 
 void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double tau, double dtf,
                           double ecrit, double xmin, double ymin, double zmin, const int* cubes,
-                          int ncubes, const double* geo, const int* off, int nel, double* rec,
-                          double* contrib, double* partial, int npartial, cudaStream_t s) {
-  SurfArgs a{g,     E,    f.Q,  f.Qprev, f.pi,  f.Pi, tau, dtf,     ecrit,   xmin, ymin,
-             zmin,  cubes, ncubes, geo,  off,   nel,  rec, contrib};
-  k_surf_elements<<<(nel + 127) / 128, 128, 0, s>>>(a);
-  k_sum_cols<<<npartial, kTotBlock, 0, s>>>(contrib, nel, kSurfAcc, partial);
-  k_sum_cols<<<1, kTotBlock, 0, s>>>(partial, npartial, kSurfAcc, partial + npartial * kSurfAcc);
+                          const int* counters, int cap_cubes, int cap_el, const double* geo,
+                          const int* off, double* rec, double* contrib, double* partial,
+                          int npartial, cudaStream_t s) {
+  SurfArgs a{g,    E,    f.Q,      f.Qprev,   f.pi,   f.Pi, tau, dtf, ecrit,  xmin, ymin, zmin,
+             cubes, counters, cap_cubes, cap_el, geo, off, rec, contrib};
+  k_surf_elements<<<kElemGrid, 128, 0, s>>>(a);
+  k_sum_cols<<<npartial, kTotBlock, 0, s>>>(contrib, 0, kSurfAcc, partial, counters + 1, cap_el);
+  k_sum_cols<<<1, kTotBlock, 0, s>>>(partial, npartial, kSurfAcc, partial + npartial * kSurfAcc,
+                                     nullptr, 0);
 }
 
 }  // namespace vh

@@ -30,17 +30,21 @@ void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double t
 // per-block counts into blk[], exclusive offsets in place, the sum to *total
 void launch_surf_count(const Geo& g, const double* eN, const double* eP, double e0, int* blk,
                        int* total, cudaStream_t s);
+// the first min(count, cap) straddling cubes in loop order
 void launch_surf_compact(const Geo& g, const double* eN, const double* eP, double e0,
-                         const int* blkoff, int* cubes, cudaStream_t s);
-// Cornelius on ncubes cubes; cnt[] becomes the element offsets, *nel the total
+                         const int* blkoff, int* cubes, int cap, cudaStream_t s);
+// Cornelius on the counters[0] (at most cap_cubes) listed cubes; cnt[]
+// becomes the element offsets and counters[1] the element total
 void launch_surf_cornelius(const Geo& g, const double* eN, const double* eP, double e0, double dtf,
-                           const int* cubes, int ncubes, double* geo, int* cnt, int* nel,
+                           const int* cubes, int* counters, int cap_cubes, double* geo, int* cnt,
                            unsigned* err, cudaStream_t s);
-// records and per-element sums; the sums land in partial[npartial*kSurfAcc ..]
+// records and per-element sums of the counters[1] (at most cap_el) elements;
+// the sums land in partial[npartial*kSurfAcc ..]
 void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double tau, double dtf,
                           double ecrit, double xmin, double ymin, double zmin, const int* cubes,
-                          int ncubes, const double* geo, const int* off, int nel, double* rec,
-                          double* contrib, double* partial, int npartial, cudaStream_t s);
+                          const int* counters, int cap_cubes, int cap_el, const double* geo,
+                          const int* off, double* rec, double* contrib, double* partial,
+                          int npartial, cudaStream_t s);
 
 // Cornelius on n independent hypercubes (16 corner values each): counts[k]
 // elements (-1 where the reference stops), geo[k][10][8] centroid + normal
