@@ -297,10 +297,11 @@ def batch_measure(capi, W, n_events, steps, device, nz=None):
 
 
 def learned_guess_measure(capi, W, setup, steps, device):
-    """The learned con2prim start point on the same event: root-find
-    iterations and throughput at the tight tolerance (1e-13, where results
-    are start-point independent) without and with the trained network, and
-    at the reference tolerance for context."""
+    """The learned con2prim start point on the event with baryon charge (the
+    3D event plus nb, 2000 x 200 (e, nb) table): root-find iterations and
+    throughput at the tight tolerance (1e-13, where results are start-point
+    independent) without and with the trained network, and at the reference
+    tolerance for context."""
     import torch
     tight = 1e-13
     cells = setup.grid.ncells
@@ -353,6 +354,9 @@ def learned_guess_measure(capi, W, setup, steps, device):
     out["iters_per_root_find"] = iters
     out["speedup_mlp_vs_tight"] = out["tight_mlp"] / out["tight"]
     out["unit"] = UNIT
+    out["workload"] = "%s %dx%dx%d, nb peak %.1f fm^-3, %dx%d (e, nb) table" % (
+        setup.name, setup.grid.nx, setup.grid.ny, setup.grid.nz, W.NB_PEAK,
+        len(setup.eos.egrid), len(setup.eos.ngrid))
     h.close()
     m.close()
     return out
@@ -498,7 +502,8 @@ def main():
         batch2d = batch_measure(capi, W, 2 * args.batch_events, 2 * args.batch_steps, local, nz=1)
     learned = None
     if not args.no_learned_guess:
-        learned = learned_guess_measure(capi, W, setup, 30, local)
+        learned = learned_guess_measure(capi, W, W.glauber3d_nb_setup(nx, ny, nz, seed=20260001 + rank),
+                                        30, local)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

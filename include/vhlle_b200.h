@@ -330,6 +330,13 @@ int vh_abi_version(void);
 vh_status vh_transform_pv(vh_ctx *ctx, const double *Q_dev, long n,
                           double *prim_dev);
 
+/* Batched transport coefficients on device arrays (TransportCoeff::getEta
+ * and getTau, src/trancoeff.cpp:68-100) with the context's parameters:
+ * in[6][n] = e, nb, T, muB, s, p -> out[4][n] = eta/s, zeta/s, tau_pi,
+ * tau_Pi.  Uses the context's stream. */
+vh_status vh_transport_eval(vh_ctx *ctx, const double *in_dev, long n,
+                            double *out_dev);
+
 /* Allocation-free step.  No counterpart in the reference: this entry point
  * exists for callers that cannot let a library allocate -- host codes whose
  * device memory is reserved up front by their own pool or by another

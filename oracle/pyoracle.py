@@ -71,6 +71,7 @@ def oracle_lib():
         lib.or_step.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_Trc),
                                 ctypes.POINTER(_State), _dp, ctypes.c_double]
         lib.or_transform_pv.argtypes = [ctypes.POINTER(_Eos), _dp, ctypes.c_int, _dp]
+        lib.or_transport_eval.argtypes = [ctypes.POINTER(_Trc), _dp, ctypes.c_int, _dp]
         lib.or_eos_eval.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_eos_s.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_update_m.argtypes = [ctypes.POINTER(_Grid), _dp, ctypes.c_double, ctypes.c_double]
@@ -115,6 +116,7 @@ def ref_lib():
         lib.ref_set_dtau.argtypes = [ctypes.c_void_p, ctypes.c_double]
         lib.ref_get_state.argtypes = [ctypes.c_void_p] + [_dp] * 9
         lib.ref_transform_pv.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_transport_eval.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
@@ -344,6 +346,14 @@ class OracleRun:
         self.lib.or_transform_pv(ctypes.byref(self.eos.s), _ptr(Q), len(Q), _ptr(out))
         return out
 
+    def transport_eval(self, inp):
+        """TransportCoeff::getEta + getTau: inp[n][6] = e, nb, T, muB, s, p
+        -> [n][4] = eta/s, zeta/s, tau_pi, tau_Pi."""
+        inp = np.ascontiguousarray(inp, dtype=np.float64).reshape(-1, 6)
+        out = np.zeros((len(inp), 4))
+        self.lib.or_transport_eval(ctypes.byref(self.trc), _ptr(inp), len(inp), _ptr(out))
+        return out
+
     def eos_eval(self, e, nb):
         e = np.ascontiguousarray(e, dtype=np.float64)
         nb = np.ascontiguousarray(nb, dtype=np.float64)
@@ -359,6 +369,14 @@ class RefRun:
 
     def __init__(self, setup, eos_file=None):
         self.setup = setup
+        self.h = None
+        self._tmp = None
+        # TransportCoeff::zetaS (src/trancoeff.cpp:19-70) has branches for
+        # zetaSparam 0..4 only and returns no value for any other; the
+        # Gaussian bump (5) exists in the oracle alone
+        if not 0 <= setup.zetaSparam <= 4 or not 0 <= setup.etaSparam <= 3:
+            raise ValueError("the reference has no etaSparam %d / zetaSparam %d"
+                             % (setup.etaSparam, setup.zetaSparam))
         self.lib = ref_lib()
         g = setup.grid
         self._tmp = None
@@ -423,6 +441,12 @@ class RefRun:
         Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
         out = np.zeros((len(Q), 8))
         self.lib.ref_transform_pv(self.h, _ptr(Q), len(Q), _ptr(out))
+        return out
+
+    def transport_eval(self, inp):
+        inp = np.ascontiguousarray(inp, dtype=np.float64).reshape(-1, 6)
+        out = np.zeros((len(inp), 4))
+        self.lib.ref_transport_eval(self.h, _ptr(inp), len(inp), _ptr(out))
         return out
 
     def totals(self):

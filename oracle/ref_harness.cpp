@@ -277,6 +277,18 @@ void ref_transform_pv(void *p, const double *Q, int n, double *out) {
   }
 }
 
+// TransportCoeff::getEta + getTau: in[n][6] = e, nb, T, muB, s, p ->
+// out[n][4] = eta/s, zeta/s, tau_pi, tau_Pi
+void ref_transport_eval(void *p, const double *in, int n, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  for (int i = 0; i < n; i++) {
+    const double *a = in + 6 * i;
+    double *o = out + 4 * i;
+    r->tr->getEta(a[0], a[1], a[2], a[3], a[4], a[5], o[0], o[1]);
+    r->tr->getTau(a[0], a[1], a[2], a[3], a[4], a[5], o[2], o[3]);
+  }
+}
+
 // EoS::eos -> out[n][3] = p, T, mub ; s_out[n] = EoS::s
 void ref_eos(void *p, const double *e, const double *nb, int n, double *out,
              double *s_out) {

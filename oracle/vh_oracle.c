@@ -1337,6 +1337,16 @@ void or_transform_pv(const or_eos *eos, const double *Q, int n, double *out) {
   }
 }
 
+void or_transport_eval(const or_trc *tr, const double *in, int n, double *out) {
+  for (int i = 0; i < n; i++) {
+    const double *a = in + 6 * i;
+    double *o = out + 4 * i;
+    o[0] = tr_etaS(tr, a[0], a[1], a[2], a[3], a[4], a[5]);
+    o[1] = tr_zetaS(tr, a[0], a[2], a[4], a[5]);
+    tr_getTau(tr, a[0], a[1], a[2], a[3], a[4], a[5], &o[2], &o[3]);
+  }
+}
+
 void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
                  double *out) {
   for (int i = 0; i < n; i++) {

@@ -80,6 +80,11 @@ int or_step(const or_grid *g, const or_eos *eos, const or_trc *tr,
  * out[n][8] = e, p, nb, nq, ns, vx, vy, vz.  Q is not modified. */
 void or_transform_pv(const or_eos *eos, const double *Q, int n, double *out);
 
+/* TransportCoeff::getEta + getTau (src/trancoeff.cpp:68-100) for n points:
+ * in[n][6] = e, nb, T, muB, s, p -> out[n][4] = eta/s, zeta/s, tau_pi,
+ * tau_Pi. */
+void or_transport_eval(const or_trc *tr, const double *in, int n, double *out);
+
 /* EoS::eos for n points; out[n][3] = p, T, mub. */
 void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
                  double *out);

@@ -33,7 +33,18 @@ CASES = {
     "gubser_21x21": (lambda: W.gubser_setup(nx=21, ny=21), 5),
     "glauber_17x17x9": (lambda: W.small_glauber3d(17, 9), 4),
     "glauber_13x13x7_b3": (lambda: W.small_glauber3d(13, 7, b=3.0, seed=5, etaS=0.2), 6),
+    # baryon charge on a 200 x 20 (e, nb) table
+    "glauber_nb_17x17x9": (lambda: W.glauber3d_nb_setup(17, 17, 9, eos=W.nb_table(200, 20)), 5),
+    # the large event's physics (shear + bulk + cross terms + nb) on a coarse
+    # grid, with the reference's own zeta/s form 2 in place of the bump
+    "large_21x21x11_zeta2": (lambda: large_with_zeta(21, 11, 2), 5),
 }
+
+
+def large_with_zeta(n, nz, zetaSparam):
+    s = W.large_event_setup(0, n, n, nz, eos=W.nb_table(200, 20))
+    s.zetaSparam = zetaSparam
+    return s
 
 
 def save_case(name, setup, nsteps):
@@ -202,13 +213,19 @@ def load_totals(path):
 if __name__ == "__main__":
     if not P.ref_available():
         sys.exit("oracle/_ref/libvhlle_ref.so missing: run `make -C oracle` first")
+    # with arguments, only the named fixtures are (re)written
+    only = set(sys.argv[1:])
     for name, (fac, n) in CASES.items():
-        save_case(name, fac(), n)
-        print("wrote", name)
+        if not only or name in only:
+            save_case(name, fac(), n)
+            print("wrote", name)
     for name, (fac, n) in SURFACE_CASES.items():
-        save_surface_case(name, fac(), n)
-        print("wrote", name)
-    cornelius_cubes()
-    print("wrote cornelius_cubes")
-    known_answers()
-    print("wrote known_answers")
+        if not only or name in only:
+            save_surface_case(name, fac(), n)
+            print("wrote", name)
+    if not only or "cornelius_cubes" in only:
+        cornelius_cubes()
+        print("wrote cornelius_cubes")
+    if not only or "known_answers" in only:
+        known_answers()
+        print("wrote known_answers")

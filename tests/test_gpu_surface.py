@@ -137,3 +137,38 @@ def test_gpu_surface_writer_matches_reference_text(tmp_path):
         first = f.readline()
     assert len(first.rstrip("\n")) == 24 * 29
     d.close()
+
+
+def _ripple_setup(n=81, nz=41, lam=4.0):
+    """A smooth triply periodic level set e = e_f crossing most hypercubes of
+    an 81x81x41 grid (about 200k elements), so that one surface call holds
+    more straddling cubes than vh_surface's first buffers (64k cubes)."""
+    g = W.Grid(n, n, nz, -15, 15, -15, 15, -7.5, 7.5)
+    x, y, eta = g.coords()
+    Z, Y, X = np.meshgrid(eta, y, x, indexing="ij")
+    k = 2 * np.pi / lam
+    e = 0.5 * (0.97 + 0.2 * (np.sin(k * X / g.dx) + np.sin(k * Y / g.dy) + np.sin(k * Z / g.dz + 0.3)))
+    zero = np.zeros_like(e)
+    Q = W.conserved_from_primitive(0.5, e, zero, zero, zero, zero, zero).reshape(7, -1)
+    tr = dict(W.TR_DEFAULTS, etaS0=0.08, zetaS0=0.0)
+    return W.Setup("ripple", g, W.make_cs2_table(), tr, 0, 0, 0.5, 0.05, 0.5, Q,
+                   np.ones(g.ncells))
+
+
+def test_gpu_surface_grows_past_first_capacity():
+    """A call with more straddling cubes than the first buffers hold grows
+    them and runs again; that call and the next (on the grown buffers) give
+    the oracle's elements."""
+    from vhlle_b200.capi import GpuHydro
+    setup = _ripple_setup()
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    for s in range(2):
+        o.step(1)
+        d.step(1)
+        ro, acc = o.surface(cap=4000000)
+        rd, info = d.surface()
+        assert len(ro) == info["nelements"] > 150000, s
+        ok = rec_close(rd, ro)
+        assert ok.all(), (s, np.argwhere(~ok)[:5])
+        assert int(acc["nsusp"]) == info["nsusp"]
+    d.close()

@@ -25,7 +25,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_upload_async", "vh_download_async", "vh_device_state", "vh_step", "vh_steps",
            "vh_set_dtau", "vh_get_dtau", "vh_get_tau", "vh_set_tau", "vh_sync",
            "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
-           "vh_abi_version", "vh_transform_pv", "vh_timer_start", "vh_timer_stop",
+           "vh_abi_version", "vh_transform_pv", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_records",
@@ -272,6 +272,7 @@ def lib():
     L.vh_last_error.restype = ctypes.c_char_p
     L.vh_abi_version.restype = ctypes.c_int
     L.vh_transform_pv.argtypes = [vp, vp, ctypes.c_long, vp]
+    L.vh_transport_eval.argtypes = [vp, vp, ctypes.c_long, vp]
     L.vh_timer_start.argtypes = [vp]
     L.vh_timer_stop.argtypes = [vp, _dp]
     L.vh_profile_enable.argtypes = [vp, ctypes.c_int]
@@ -370,6 +371,7 @@ class GpuHydro:
         if st != VH_OK:
             raise VhError(st, self.L.vh_last_error(None).decode())
         self.h = h
+        self.device = device
         if upload:
             self.upload_initial()
 
@@ -482,6 +484,22 @@ class GpuHydro:
 
     def set_con2prim_guess(self, mlp):
         self._check(self.L.vh_set_con2prim_guess(self.h, mlp.h if mlp is not None else None))
+
+    def transport_eval(self, inp):
+        """TransportCoeff::getEta + getTau on the device with this grid's
+        transport parameters: inp[n][6] = e, nb, T, muB, s, p -> [n][4] =
+        eta/s, zeta/s, tau_pi, tau_Pi (vh_transport_eval)."""
+        import torch
+        a = np.ascontiguousarray(np.asarray(inp, dtype=np.float64).reshape(-1, 6).T)
+        n = a.shape[1]
+        dev = "cuda:%d" % self.device
+        din = torch.from_numpy(a).to(dev)
+        dout = torch.empty((4, n), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        self._check(self.L.vh_transport_eval(self.h, ctypes.c_void_p(din.data_ptr()), n,
+                                             ctypes.c_void_p(dout.data_ptr())))
+        self.sync()
+        return dout.cpu().numpy().T.copy()
 
     def surface_only(self, ecrit=None):
         """vh_surface without copying the records: the info dict."""

@@ -177,6 +177,7 @@ vh_status vh_destroy(vh_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (void* p : ctx->allocs) cudaFree(p);
+  if (ctx->surf.host) cudaFreeHost(ctx->surf.host);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
   if (ctx->t0) cudaEventDestroy(ctx->t0);
   if (ctx->t1) cudaEventDestroy(ctx->t1);
@@ -702,6 +703,10 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
         (st = dalloc(ctx, &S.partial, (size_t)(kSurfPartials + 1) * vh::kSurfAcc)))
       return st;
   }
+  if (!S.host) {
+    static_assert(vh::kSurfAcc == 5, "vh_ctx::Surf::Host::acc");
+    VH_CUDA(ctx, cudaHostAlloc((void**)&S.host, sizeof(vh_ctx::Surf::Host), cudaHostAllocDefault));
+  }
   // Every stage reads the counts from device memory, so the call waits for
   // the GPU once, at the end.  The buffers start at 64k cubes and twice as
   // many elements; a call that finds more grows them and runs again (the
@@ -711,9 +716,7 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   size_t want_e = std::max<size_t>(S.cap_rec / vh::kSurfRec, 2 * want_c);
   cudaStream_t s = ctx->stream;
   const double taup = ctx->tau - ctx->fluid_dt;
-  int cnts[2] = {0, 0};
-  double acc[vh::kSurfAcc] = {0., 0., 0., 0., 0.};
-  unsigned bits = 0;
+  vh_ctx::Surf::Host& H = *S.host;
   for (int pass = 0; pass < 2; pass++) {
     if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, want_c)) ||
         (st = dgrow(ctx, &S.geo, &S.cap_geo, want_c * vh::kSurfMaxElemPerCube * vh::kSurfGeo)) ||
@@ -732,18 +735,20 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
                              ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
                              S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
     VH_CUDA(ctx, cudaGetLastError());
-    VH_CUDA(ctx, cudaMemcpyAsync(cnts, S.counters, sizeof cnts, cudaMemcpyDeviceToHost, s));
-    VH_CUDA(ctx, cudaMemcpyAsync(acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
-                                 sizeof acc, cudaMemcpyDeviceToHost, s));
-    VH_CUDA(ctx, cudaMemcpyAsync(&bits, ctx->f.err, sizeof bits, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaMemcpyAsync(H.cnt, S.counters, sizeof H.cnt, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaMemcpyAsync(H.acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
+                                 sizeof H.acc, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaMemcpyAsync(&H.bits, ctx->f.err, sizeof H.bits, cudaMemcpyDeviceToHost, s));
     VH_CUDA(ctx, cudaStreamSynchronize(s));
-    if ((size_t)cnts[0] <= (size_t)cap_c && (size_t)cnts[1] <= (size_t)cap_e) break;
+    if ((size_t)H.cnt[0] <= (size_t)cap_c && (size_t)H.cnt[1] <= (size_t)cap_e) break;
     if (pass == 1) return fail(ctx, VH_ERR_STATE, "vh_surface: element buffers did not grow");
-    want_c = std::max(want_c, (size_t)cnts[0] + (size_t)cnts[0] / 4 + 1);
+    want_c = std::max(want_c, (size_t)H.cnt[0] + (size_t)H.cnt[0] / 4 + 1);
     // a cube holds at most kSurfMaxElemPerCube elements
-    want_e = std::max(want_e, (size_t)cnts[0] * vh::kSurfMaxElemPerCube);
+    want_e = std::max(want_e, (size_t)H.cnt[0] * vh::kSurfMaxElemPerCube);
   }
-  const int nel = cnts[1];
+  const int nel = H.cnt[1];
+  const unsigned bits = H.bits;
+  const double* acc = H.acc;
   S.nel = nel;
   ctx->EtotSurf += acc[1];
   ctx->nbSurf += acc[2];
@@ -902,6 +907,15 @@ vh_status vh_transform_pv(vh_ctx* ctx, const double* Q_dev, long n, double* prim
   if (n == 0) return VH_OK;
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
   vh::launch_transform_pv(ctx->eos, Q_dev, (long long)n, prim_dev, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
+  return VH_OK;
+}
+
+vh_status vh_transport_eval(vh_ctx* ctx, const double* in_dev, long n, double* out_dev) {
+  if (!ctx || !in_dev || !out_dev || n < 0) return VH_ERR_ARG;
+  if (n == 0) return VH_OK;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::launch_transport(ctx->tr, in_dev, (long long)n, out_dev, ctx->stream);
   VH_CUDA(ctx, cudaGetLastError());
   return VH_OK;
 }

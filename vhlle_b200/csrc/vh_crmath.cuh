@@ -1,0 +1,166 @@
+// Correctly rounded exp(x) and x^(1/4) in FP64, for the transport
+// coefficients (zeta/s forms 1-5, src/trancoeff.cpp:19-70).  The reference
+// evaluates them with the host C library, whose exp and pow are accurate to
+// about half an ulp; returning the correctly rounded value reproduces the
+// library's result except where the exact value lies within ~1e-3 ulp of a
+// rounding boundary, while a faithfully rounded device exp (up to 1 ulp)
+// differs from it in a sizeable fraction of calls.  Bulk viscosity amplifies
+// a last-bit difference by ~1e6 within ten steps near the limiter and the
+// vacuum edge, so the last bit matters for parity.
+//
+// Method (own implementation from the mathematics, double-double arithmetic
+// after Dekker (1971) and Knuth's two-sum; constants from
+// gen_crmath_consts.py, exact rational arithmetic):
+//   exp: k = rint(x / ln 2); r = x - k ln 2 with ln 2 split into three
+//        doubles (Cody & Waite 1980); s = r / 2^8; expm1(s) by its Taylor
+//        series to s^11 / 11! in double-double (|s| < 1.4e-3, truncation
+//        < 2^-125); eight doublings expm1(2a) = 2 expm1(a) + expm1(a)^2;
+//        1 + expm1 rounded to nearest once; scaled by 2^k, with the
+//        subnormal range rounded to integer multiples of 2^-1074 from the
+//        double-double.  Relative error before the final rounding < 2^-98.
+//   x^(1/4): sqrt(x) as a double-double (the correctly rounded square root
+//        and its exact residual by fma), its square root the same way, and
+//        one rounding of the sum.
+// Every operation is an IEEE add, multiply, divide, sqrt or an explicit fma,
+// none contracted (the library builds with -fmad=false), so host and device
+// compilations of this header give the same bits.
+#pragma once
+
+#include <math.h>
+
+#ifdef __CUDACC__
+#define VH_CRM __host__ __device__ __forceinline__
+#else
+#define VH_CRM static inline
+#endif
+
+namespace vh {
+namespace crm {
+
+struct dd {
+  double hi, lo;
+};
+
+VH_CRM dd two_sum(double a, double b) {
+  const double s = a + b;
+  const double bb = s - a;
+  const double e = (a - (s - bb)) + (b - bb);
+  return {s, e};
+}
+
+VH_CRM dd fast_two_sum(double a, double b) {  // |a| >= |b|
+  const double s = a + b;
+  return {s, b - (s - a)};
+}
+
+VH_CRM dd two_prod(double a, double b) {
+  const double p = a * b;
+  return {p, fma(a, b, -p)};
+}
+
+VH_CRM dd add(dd a, dd b) {
+  dd s = two_sum(a.hi, b.hi);
+  const dd t = two_sum(a.lo, b.lo);
+  s.lo += t.hi;
+  s = fast_two_sum(s.hi, s.lo);
+  s.lo += t.lo;
+  return fast_two_sum(s.hi, s.lo);
+}
+
+VH_CRM dd mul(dd a, dd b) {
+  dd p = two_prod(a.hi, b.hi);
+  const double c = a.hi * b.lo;
+  const double d = a.lo * b.hi;
+  p.lo += c + d;
+  return fast_two_sum(p.hi, p.lo);
+}
+
+// 2^k for -1022 <= k <= 1023, built from its bit pattern
+VH_CRM double pow2i(int k) {
+  const long long bits = (long long)(k + 1023) << 52;
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(bits);
+#else
+  double d;
+  __builtin_memcpy(&d, &bits, sizeof d);
+  return d;
+#endif
+}
+
+// y * 2^k rounded once, y = hi + lo in [0.7, 1.5), |k| <= 1100
+VH_CRM double scale_round(dd y, int k) {
+  if (k > 1023) return y.hi * pow2i(1023) * pow2i(k - 1023);  // may overflow to inf
+  if (k > -1022) return y.hi * pow2i(k);                        // exact
+  // subnormal range: count units of 2^-1074
+  const int sh = k + 1074;
+  if (sh < -1) return 0.0;  // y 2^k < 2^-1075.4, below half the smallest subnormal
+  const double f = sh >= 0 ? pow2i(sh) : 0.5;
+  const double zh = y.hi * f, zl = y.lo * f;  // exact
+  double n = rint(zh);
+  const double rem = (zh - n) + zl;
+  if (rem > 0.5) {
+    n += 1.0;
+  } else if (rem < -0.5) {
+    n -= 1.0;
+  } else if (rem == 0.5 || rem == -0.5) {  // tie: to even
+    const double m = n + (rem > 0 ? 1.0 : -1.0);
+    if (fmod(m, 2.0) == 0.0) n = m;
+  }
+  return n * pow2i(-1022) * pow2i(-52);  // exact: n < 2^53
+}
+
+VH_CRM double exp_cr(double x) {
+  if (!(x == x)) return x;  // NaN
+  if (x > 709.8) return (double)INFINITY;
+  if (x < -746.0) return 0.0;
+  const double LN2_1 = 0x1.62e42fef00000p-1;   // 33 significant bits
+  const double LN2_2 = 0x1.473de6af278edp-34;
+  const double LN2_3 = -0x1.9ff0342542fc3p-90;
+  const double INV_LN2 = 0x1.71547652b82fep+0;
+  const double k = rint(x * INV_LN2);
+  // r = x - k ln2 as a double-double
+  dd r = two_sum(x, -(k * LN2_1));  // k * LN2_1 exact
+  r = add(r, {-two_prod(k, LN2_2).hi, -two_prod(k, LN2_2).lo});
+  r = add(r, {-(k * LN2_3), 0.0});
+  // s = r / 2^8
+  const dd s = {r.hi * 0x1p-8, r.lo * 0x1p-8};
+  // expm1(s) = s (1 + s/2! + s^2/3! + ... + s^10/11!) by Horner
+  const dd c[12] = {{0., 0.},
+                    {0x1.0000000000000p+0, 0.},
+                    {0x1.0000000000000p-1, 0.},
+                    {0x1.5555555555555p-3, 0x1.5555555555555p-57},
+                    {0x1.5555555555555p-5, 0x1.5555555555555p-59},
+                    {0x1.1111111111111p-7, 0x1.1111111111111p-63},
+                    {0x1.6c16c16c16c17p-10, -0x1.f49f49f49f49fp-65},
+                    {0x1.a01a01a01a01ap-13, 0x1.a01a01a01a01ap-73},
+                    {0x1.a01a01a01a01ap-16, 0x1.a01a01a01a01ap-76},
+                    {0x1.71de3a556c734p-19, -0x1.c154f8ddc6c00p-73},
+                    {0x1.27e4fb7789f5cp-22, 0x1.cbbc05b4fa99ap-76},
+                    {0x1.ae64567f544e4p-26, -0x1.c062e06d1f209p-80}};
+  dd p = c[11];
+#pragma unroll
+  for (int n = 10; n >= 1; n--) p = add(mul(p, s), c[n]);
+  dd e = mul(p, s);
+  // expm1(2a) = 2 expm1(a) + expm1(a)^2, eight times
+#pragma unroll
+  for (int j = 0; j < 8; j++) e = add({2. * e.hi, 2. * e.lo}, mul(e, e));
+  const dd y = add({1.0, 0.0}, e);
+  return scale_round(y, (int)k);
+}
+
+// x^(1/4) for x >= 0 (x = +0 gives +0, x = inf gives inf)
+VH_CRM double root4_cr(double x) {
+  if (!(x > 0.) || x == (double)INFINITY) return x < 0. ? (double)NAN : x;
+  // a + al = sqrt(x): a correctly rounded, fma(-a, a, x) exact
+  const double a = sqrt(x);
+  const double al = fma(-a, a, x) / (2. * a);
+  // b + bl = sqrt(a + al)
+  const double b = sqrt(a);
+  const double bl = (fma(-b, b, a) + al) / (2. * b);
+  return b + bl;
+}
+
+}  // namespace crm
+}  // namespace vh
+
+#undef VH_CRM

@@ -44,6 +44,12 @@ struct vh_ctx {
     int *blk = nullptr, *cubes = nullptr, *cnt = nullptr, *counters = nullptr;
     size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
     long long nel = 0;
+    // pinned landing place of a call's counts, sums and error bits
+    struct Host {
+      int cnt[2];
+      unsigned bits;
+      double acc[5];
+    }* host = nullptr;
   } surf;
   std::string err;
   std::vector<void*> allocs;

@@ -9,6 +9,8 @@
 
 #include <cstdint>
 
+#include "vh_crmath.cuh"
+
 namespace vh {
 
 enum { T_ = 0, X_ = 1, Y_ = 2, Z_ = 3, NB_ = 4, NQ_ = 5, NS_ = 6 };
@@ -324,44 +326,49 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
 }
 
 // ------------------------------------------------- transport coefficients
-// TransportCoeff::zetaS, src/trancoeff.cpp:19-66; cs2(e) = 1/3 (src/eos.h:37)
+// TransportCoeff::zetaS, src/trancoeff.cpp:19-66; cs2(e) = 1/3 (src/eos.h:37).
+// exp and pow(x, 0.25) are correctly rounded (vh_crmath.cuh), the value the
+// host library's half-ulp functions return in all but ~1e-3 of the calls.
 __device__ __forceinline__ double tr_zetaS(const TrDev& t, double e, double T,
                                            double s, double P) {
   const double cs2e = 1. / 3.;
   const double T_p = 0.180, T_peak = 0.165, T_width = 0.010, B_norm = 0.24,
                B_width = 1.5, T_peak2 = 0.160, B_norm2 = 0.13, B1 = 0.01, B2 = 0.12;
   if (t.zetaSparam == 0) {
-    return t.zetaS0 * (1. / 3. - cs2e) / (exp((0.16 - T) / 0.001) + 1.);
+    // the denominator is >= 1, so a zero (or NaN) numerator is the result
+    const double num = t.zetaS0 * (1. / 3. - cs2e);
+    if (num == 0. || num != num) return num;
+    return num / (crm::exp_cr((0.16 - T) / 0.001) + 1.);
   } else if (t.zetaSparam == 1) {
     if (T < 0.180)
-      return 0.03 + (0.08 * exp(((T / T_p) - 1.) / (0.0025))) +
-             (0.22 * exp(((T / T_p) - 1) / (0.022)));
+      return 0.03 + (0.08 * crm::exp_cr(((T / T_p) - 1.) / (0.0025))) +
+             (0.22 * crm::exp_cr(((T / T_p) - 1) / (0.022)));
     else if (T >= 0.180 && T < 0.200)
       return 27.55 * (T / T_p) - 13.45 - (13.77 * (T / T_p) * (T / T_p));
     else if (T >= 0.200)
-      return 0.001 + (0.9 * exp(-((T / T_p) - 1.) / (0.0025))) +
-             (0.25 * exp(-((T / T_p) - 1.) / (0.13)));
+      return 0.001 + (0.9 * crm::exp_cr(-((T / T_p) - 1.) / (0.0025))) +
+             (0.25 * crm::exp_cr(-((T / T_p) - 1.) / (0.13)));
   } else if (t.zetaSparam == 2) {
     if (T > T_peak)
       return B_norm * ((B_width * B_width) /
                        ((((T / T_peak) - 1.) * ((T / T_peak) - 1.)) + (B_width * B_width)));
     else if (T <= T_peak)
-      return B_norm * (exp(-((T - T_peak) / T_width) * ((T - T_peak) / T_width)));
+      return B_norm * (crm::exp_cr(-((T - T_peak) / T_width) * ((T - T_peak) / T_width)));
   } else if (t.zetaSparam == 3) {
     if (T < T_peak2)
-      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B1 * B1)));
+      return B_norm2 * crm::exp_cr(-((T - T_peak2) * (T - T_peak2) / (B1 * B1)));
     else if (T >= T_peak2)
-      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B2 * B2)));
+      return B_norm2 * crm::exp_cr(-((T - T_peak2) * (T - T_peak2) / (B2 * B2)));
   } else if (t.zetaSparam == 4) {
     // abs(s) binds to int abs(int) in the reference: |s| < 1 reads as 0
     if (!(fabs(s) >= 1.0) || T < 1e-1) return 0;
-    const double d = t.zetaSScaleBeta * (pow(e, 0.25) - pow(t.zetaSPeakEpsilon, 0.25));
+    const double d = t.zetaSScaleBeta * (crm::root4_cr(e) - crm::root4_cr(t.zetaSPeakEpsilon));
     const double sig = e < t.zetaSPeakEpsilon ? t.zetaSSigmaMinus : t.zetaSSigmaPlus;
-    return ((e + P) / (s * T)) * t.zetaS0 * exp(d * d / 2.0 * (sig * sig));
+    return ((e + P) / (s * T)) * t.zetaS0 * crm::exp_cr(d * d / 2.0 * (sig * sig));
   } else if (t.zetaSparam == 5) {
     // a Gaussian bump in T (this build's addition; not in the reference)
     const double x = T - t.zetaSPeakT;
-    return t.zetaS0 * exp(-x * x / (2. * t.zetaSWidthT * t.zetaSWidthT));
+    return t.zetaS0 * crm::exp_cr(-x * x / (2. * t.zetaSWidthT * t.zetaSWidthT));
   }
   return 0.;
 }
@@ -389,15 +396,24 @@ __device__ __forceinline__ double tr_etaS(const TrDev& t, double e, double rho,
 
 // TransportCoeff::getTau, src/trancoeff.cpp:92-100.  abs(e + P) binds to
 // int abs(int) in the reference: the test is trunc(e + P) != 0.
-__device__ __forceinline__ void tr_getTau(const TrDev& t, double e, double rho,
-                                          double T, double muB, double s, double P,
-                                          double& taupi, double& tauPi) {
+// etaS and zetaS are tr_etaS and tr_zetaS at the same point (pure
+// functions, evaluated once by the caller).
+__device__ __forceinline__ void tr_getTau_from(double e, double T, double s, double P,
+                                               double etaS, double zetaS, double& taupi,
+                                               double& tauPi) {
   if (T > 1e-1 && !(fabs(e + P) < 1.0)) {
-    taupi = ddiv((5. / 5.068) * s * tr_etaS(t, e, rho, T, muB, s, P), e + P);
-    tauPi = ddiv((6. / 5.068) * tr_zetaS(t, e, T, s, P) * s, e + P);
+    taupi = ddiv((5. / 5.068) * s * etaS, e + P);
+    tauPi = ddiv((6. / 5.068) * zetaS * s, e + P);
   } else {
     taupi = tauPi = 0.;
   }
+}
+
+__device__ __forceinline__ void tr_getTau(const TrDev& t, double e, double rho,
+                                          double T, double muB, double s, double P,
+                                          double& taupi, double& tauPi) {
+  tr_getTau_from(e, T, s, P, tr_etaS(t, e, rho, T, muB, s, P), tr_zetaS(t, e, T, s, P), taupi,
+                 tauPi);
 }
 
 // ---------------------------------------------------------- HLLE face flux

@@ -293,14 +293,16 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     double T, mub, p;
     eos_eval(E, a.e, a.nb, T, mub, p);
     const double s = eos_s(E, a.e, a.nb, a.nq, a.ns);
+    const double etaS = tr_etaS(tr, a.e, a.nb, T, mub, s, p);
+    const double zetaS = tr_zetaS(tr, a.e, T, s, p);
     double taupi, tauPi;
-    tr_getTau(tr, a.e, a.nb, T, mub, s, p, taupi, tauPi);
+    tr_getTau_from(a.e, T, s, p, etaS, zetaS, taupi, tauPi);
     pTh[0 * N + i] = T;
     pTh[1 * N + i] = mub;
     pTh[2 * N + i] = p;
     pTh[3 * N + i] = s;
-    pTh[4 * N + i] = tr_etaS(tr, a.e, a.nb, T, mub, s, p);
-    pTh[5 * N + i] = tr_zetaS(tr, a.e, T, s, p);
+    pTh[4 * N + i] = etaS;
+    pTh[5 * N + i] = zetaS;
     pTh[6 * N + i] = taupi;
     pTh[7 * N + i] = tauPi;
     pTh[8 * N + i] = 9. / 70. / eos_p(E, a.e, a.nb);
@@ -986,6 +988,27 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
                          cudaStream_t s) {
   k_transform_pv<<<nblk(n, 128), 128, 0, s>>>(E, Q, n, out);
+}
+
+// TransportCoeff::getEta + getTau (src/trancoeff.cpp:68-100) on arrays:
+// in[6][n] = e, nb, T, muB, s, p -> out[4][n] = eta/s, zeta/s, tau_pi, tau_Pi
+__global__ void k_transport(TrDev tr, const double* __restrict__ in, long long n,
+                            double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double e = in[i], nb = in[n + i], T = in[2 * n + i], mub = in[3 * n + i],
+               s = in[4 * n + i], p = in[5 * n + i];
+  double taupi, tauPi;
+  tr_getTau(tr, e, nb, T, mub, s, p, taupi, tauPi);
+  out[i] = tr_etaS(tr, e, nb, T, mub, s, p);
+  out[n + i] = tr_zetaS(tr, e, T, s, p);
+  out[2 * n + i] = taupi;
+  out[3 * n + i] = tauPi;
+}
+
+void launch_transport(const TrDev& tr, const double* in, long long n, double* out,
+                      cudaStream_t s) {
+  k_transport<<<nblk(n, 128), 128, 0, s>>>(tr, in, n, out);
 }
 
 // ------------------------------------------------------------ clock

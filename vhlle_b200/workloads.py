@@ -16,7 +16,15 @@ Workloads (sizes and physics as the benchmark configurations state them):
                  Monte-Carlo Glauber Pb+Pb (WS R = 6.62, a = 0.546, b = 7,
                  sigma_NN = 6.4 fm^2, 0.4 fm smearing, peak e = 50 GeV/fm^3,
                  plateau |eta_s| < 2.5 with Gaussian tails of width 1.0).
-  Smaller grids of the same physics are produced with ``scale_grid``.
+  * ``glauber3d_nb`` the same event with baryon charge: nb = 0.3 fm^-3 x
+                 the same Glauber profile, a 2000 x 200 (e, nb) table over
+                 nb in [0, 1] fm^-3 with mu_B = 1 GeV fm^3 x nb.
+  * ``large_event`` 201x201x101 on [-20,20]^2 x [-10,10], tau0 = 0.4,
+                 dtau = 0.02, b = 3 fm, peak e = 80 GeV/fm^3, eta/s = 0.08,
+                 the zeta/s bump of the batch, baryon charge and the e x nb
+                 table; a batch of 8 with seeds 20265000 + k.
+  Smaller grids of the same physics come from the same functions with
+  smaller nx, ny, nz.
 
 The reference publishes no input files for these workloads (its data
 repository is separate), so seeded synthetic inputs stand in for them.
@@ -466,3 +474,55 @@ def batch_events(n: int = 256, seed0: int = BATCH_SEED0, **kw):
     """The first n events of the batch (one EoS table shared by all)."""
     eos = kw.pop("eos", None) or make_cs2_table()
     return [batch_event(k, seed0, eos=eos, **kw) for k in range(n)]
+
+
+# ------------------------------------------------- baryon charge, large events
+NB_PEAK = 0.3        # fm^-3, peak of the initial nb profile
+NB_TABLE_MAX = 1.0   # fm^-3, top of the table's nb axis
+MUB_SLOPE = 1.0      # GeV fm^3: mu_B = MUB_SLOPE * nb
+LARGE_SEED0 = 20265000
+
+
+def nb_table(ne: int = 2000, nn: int = 200) -> EosTable:
+    """The e x nb table of the baryon-charge workloads: ``ne`` log e-points
+    (1e-4 .. 1e3 GeV/fm^3, the same c_s^2(e) form) x ``nn`` nb-points on
+    [0, 1] fm^-3, mu_B linear in nb."""
+    return make_cs2_table(ne=ne, nn=nn, nbmax=NB_TABLE_MAX, mub_slope=MUB_SLOPE)
+
+
+def glauber3d_nb_setup(nx: int = 101, ny: int = 101, nz: int = 51,
+                       eos: Optional[EosTable] = None, **kw) -> Setup:
+    """The 3D viscous event plus baryon charge: initial nb is the Glauber
+    profile scaled to a peak of 0.3 fm^-3; the (e, nb) table is
+    ``nb_table()`` unless ``eos`` is given."""
+    kw.setdefault("nb_peak", NB_PEAK)
+    s = glauber3d_setup(nx, ny, nz, eos=eos if eos is not None else nb_table(), **kw)
+    s.name = "glauber3d_nb"
+    return s
+
+
+def with_zeta_bump(s: Setup, height: float = 0.05, peak_T: float = 0.175,
+                   width_T: float = 0.02) -> Setup:
+    """zeta/s = height exp(-(T - peak_T)^2 / (2 width_T^2)) (zetaSparam 5)."""
+    s.tr = dict(s.tr, zetaS0=height, zetaSPeakT=peak_T, zetaSWidthT=width_T)
+    s.zetaSparam = 5
+    return s
+
+
+def large_event_setup(k: int = 0, nx: int = 201, ny: int = 201, nz: int = 101,
+                      eos: Optional[EosTable] = None, seed0: int = LARGE_SEED0,
+                      **kw) -> Setup:
+    """Event k of the large-event batch: 201x201x101 on [-20,20]^2 x
+    [-10,10], tau0 = 0.4, dtau = 0.02, seed seed0 + k, b = 3 fm, peak
+    e = 80 GeV/fm^3, eta/s = 0.08 plus the zeta/s bump (shear, bulk and their
+    cross terms), baryon charge and the e x nb table.  Smaller nx, ny, nz
+    keep the physical extent (coarser cells)."""
+    kw.setdefault("xmax", 20.0)
+    kw.setdefault("etamax", 10.0)
+    kw.setdefault("tau0", 0.4)
+    kw.setdefault("dt", 0.02)
+    kw.setdefault("b", 3.0)
+    kw.setdefault("epeak", 80.0)
+    s = glauber3d_nb_setup(nx, ny, nz, eos=eos, seed=seed0 + k, **kw)
+    s.name = "large_event_%d" % k
+    return with_zeta_bump(s)
