@@ -248,6 +248,19 @@ typedef struct vh_surface_info {
 } vh_surface_info;
 vh_status vh_surface(vh_ctx *ctx, double ecrit, vh_surface_info *info);
 
+/* The corona of Fluid::outputCorona (src/fld.cpp:876-1089), which the
+ * reference driver writes once at tau0, before the first step
+ * (src/main.cpp:390): every interior cube whose eight corners have
+ * e <= e_crit at the current tau and whose corner-averaged Q / tau gives
+ * e >= 0.01 becomes one element at the cube centre with dSigma_mu =
+ * tau dx dy deta (cosh eta, 0, 0, -sinh eta) and the corner-averaged state.
+ * Its records replace the last vh_surface call's (vh_surface_records,
+ * _device and _write return them).  EtotSurf and vEff add to the grid's
+ * sums; info->nbSurf is the corona's own running sum (a separate function
+ * static in the reference); nsusp is 0; high_T counts T > 0.4 or
+ * |muB| > 0.99.  Waits for the result. */
+vh_status vh_corona(vh_ctx *ctx, double ecrit, vh_surface_info *info);
+
 /* Element records of the last vh_surface call, VH_SURF_REC doubles each:
  * tau, x, y, eta, dSigma_0..3, u^0..3, T, muB, muQ, muS, pi^{mu nu}
  * (10, index44 order: 00 01 11 02 12 22 03 13 23 33), Pi, e, nb.

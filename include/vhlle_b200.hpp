@@ -423,6 +423,15 @@ class Hydro {
     check(vh_surface(ctx_, f_->geteCrit(), &si), ctx_);
     return si;
   }
+  // The corona of Fluid::outputCorona (src/fld.cpp:876-1089) at the current
+  // tau (the reference driver writes it once at tau0); writeSurface then
+  // appends its records.
+  vh_surface_info corona() {
+    if (!uploaded_) upload();
+    vh_surface_info si{};
+    check(vh_corona(ctx_, f_->geteCrit(), &si), ctx_);
+    return si;
+  }
   void writeSurface(const char* path, bool extendFO) {
     check(vh_surface_write(ctx_, path, extendFO ? 1 : 0), ctx_);
   }

@@ -82,6 +82,9 @@ def oracle_lib():
         lib.or_surface.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_State),
                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_long,
                                    _dp]
+        lib.or_corona.restype = ctypes.c_long
+        lib.or_corona.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_State),
+                                  ctypes.c_double, ctypes.c_double, _dp, ctypes.c_long, _dp]
         lib.or_cornelius4d.restype = ctypes.c_int
         lib.or_cornelius4d.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp]
         lib.or_substeps.restype = ctypes.c_int
@@ -117,6 +120,9 @@ def ref_lib():
         lib.ref_get_state.argtypes = [ctypes.c_void_p] + [_dp] * 9
         lib.ref_transform_pv.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_transport_eval.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_output_corona.restype = ctypes.c_int
+        lib.ref_output_corona.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
+                                          ctypes.c_char_p, ctypes.c_int]
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
@@ -340,6 +346,17 @@ class OracleRun:
         assert n <= cap
         return rec[:n].copy(), dict(zip(SURF_ACC, acc))
 
+    def corona(self, cap=2000000):
+        """Fluid::outputCorona's elements at the current tau: (records
+        [n][29], acc dict)."""
+        rec = np.zeros((cap, SURF_REC))
+        acc = np.zeros(5)
+        sv = self._sview()
+        n = self.lib.or_corona(ctypes.byref(self.grid), ctypes.byref(self.eos.s), ctypes.byref(sv),
+                               self.tau.value, self.setup.ecrit, _ptr(rec), cap, _ptr(acc))
+        assert n <= cap
+        return rec[:n].copy(), dict(zip(SURF_ACC, acc))
+
     def transform_pv(self, Q):
         Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
         out = np.zeros((len(Q), 8))
@@ -459,6 +476,13 @@ class RefRun:
         Element lines go to outdir/freezeout.dat.unfinished."""
         buf = ctypes.create_string_buffer(512)
         n = self.lib.ref_output_surface(self.h, outdir.encode(), int(extend), buf, 512)
+        return n, buf.value.decode()
+
+    def output_corona(self, outdir, extend=False):
+        """Fluid::outputCorona: returns (nelements, printed totals line).
+        Element lines go to outdir/freezeout.dat.unfinished."""
+        buf = ctypes.create_string_buffer(512)
+        n = self.lib.ref_output_corona(self.h, outdir.encode(), int(extend), buf, 512)
         return n, buf.value.decode()
 
     def eos_eval(self, e, nb):

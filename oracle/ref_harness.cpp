@@ -22,6 +22,7 @@
 #include <iostream>
 #include <sstream>
 #include <string>
+#include <vector>
 
 #include "eos.h"  // must precede eo1.h, which only forward-declares EoS
 #include "cll.h"
@@ -409,6 +410,40 @@ int ref_output_surface(void *p, const char *dir, int extendFO, char *line, int l
     if (!l.empty()) last = l;
   if (line && linelen > 0) {
     strncpy(line, last.c_str(), linelen - 1);
+    line[linelen - 1] = 0;
+  }
+  return n;
+}
+
+// Fluid::outputCorona at the current tau into the same freeze-out stream;
+// returns the number of corona elements (the "corona elements : n" line)
+// and copies the totals line it prints (the second-to-last line).
+int ref_output_corona(void *p, const char *dir, int extendFO, char *line, int linelen) {
+  RefRun *r = static_cast<RefRun *>(p);
+  std::streambuf *old = std::cout.rdbuf();
+  std::ostringstream cap;
+  std::cout.rdbuf(cap.rdbuf());
+  if (!r->output_open) {
+    if (output::ffreeze.is_open()) output::ffreeze.close();
+    r->f->initOutput(dir, r->tau0, true);
+    r->output_open = true;
+  }
+  r->f->outputCorona(r->h->getTau(), extendFO != 0);
+  output::ffreeze.flush();
+  std::cout.rdbuf(old);
+  std::vector<std::string> lines;
+  std::istringstream in(cap.str());
+  for (std::string l; std::getline(in, l);)
+    if (!l.empty()) lines.push_back(l);
+  int n = -1;
+  if (!lines.empty()) {
+    const std::string &last = lines.back();
+    const size_t k = last.find(':');
+    if (k != std::string::npos) n = atoi(last.c_str() + k + 1);
+  }
+  if (line && linelen > 0) {
+    const std::string t = lines.size() >= 2 ? lines[lines.size() - 2] : std::string();
+    strncpy(line, t.c_str(), linelen - 1);
     line[linelen - 1] = 0;
   }
   return n;

@@ -2003,6 +2003,21 @@ int or_cornelius4d(const double cube[16], const double dx[4], double E0, double 
   return nel;
 }
 
+/* Cartesian components of pi^{mu nu} at space-time rapidity eta (the OUTPI
+ * block of src/fld.cpp:766-790 and :1028-1053), index44 order. */
+static void pi_to_cartesian(double ch, double sh, const double *piC, double *pc) {
+  pc[0] = ch * ch * piC[0] + 2. * ch * sh * piC[6] + sh * sh * piC[9];
+  pc[1] = ch * piC[1] + sh * piC[7];
+  pc[3] = ch * piC[3] + sh * piC[8];
+  pc[6] = ch * sh * (piC[0] + piC[9]) + (ch * ch + sh * sh) * piC[6];
+  pc[2] = piC[2];
+  pc[4] = piC[4];
+  pc[7] = sh * piC[1] + ch * piC[7];
+  pc[5] = piC[5];
+  pc[8] = sh * piC[3] + ch * piC[8];
+  pc[9] = sh * sh * piC[0] + ch * ch * piC[9] + 2. * sh * ch * piC[6];
+}
+
 /* transformToLab, src/fld.cpp:508-513 */
 static void to_lab(double eta, double *vx, double *vy, double *vz) {
   const double Y = eta + 1. / 2. * log((1. + *vz) / (1. - *vz));
@@ -2146,6 +2161,104 @@ long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau
           }
           nel++;
         }
+      }
+  return nel;
+}
+
+/* Fluid::outputCorona, src/fld.cpp:876-1089 (the element part; the totals
+ * it prints are or_totals').  Loop order ix, iy, iz (iz fastest) over
+ * [2, n-2). */
+long or_corona(const or_grid *g, const or_eos *E, const or_state *s, double tau,
+               double ecrit, double *rec, long cap, double *acc) {
+  const int nx = g->nx, ny = g->ny, nz = g->nz;
+  const long N = (long)nx * ny * nz;
+  const double dx = (g->xmax - g->xmin) / (nx - 1);
+  const double dy = (g->ymax - g->ymin) / (ny - 1);
+  const double dz = (g->zmax - g->zmin) / (nz - 1);
+  long nel = 0;
+  for (int ix = 2; ix < nx - 2; ix++)
+    for (int iy = 2; iy < ny - 2; iy++)
+      for (int iz = 2; iz < nz - 2; iz++) {
+        int isCorona = 1;
+        double QCube[8][7], piS[8][10], PiS[8];
+        for (int jx = 0; jx < 2; jx++)
+          for (int jy = 0; jy < 2; jy++)
+            for (int jz = 0; jz < 2; jz++) {
+              const int c = jx * 4 + jy * 2 + jz;
+              const long i = (ix + jx) + (long)nx * (iy + jy) + (long)nx * ny * (iz + jz);
+              double q[7], e, p, nb, nq, ns, vx, vy, vz;
+              /* Cell::getPrimVar, src/cll.cpp:90-95 */
+              for (int k = 0; k < 7; k++) q[k] = s->Q[(long)k * N + i] / tau;
+              transform_pv(E, q, &e, &p, &nb, &nq, &ns, &vx, &vy, &vz);
+              for (int k = 0; k < 7; k++) QCube[c][k] = s->Q[(long)k * N + i];
+              if (e > ecrit) isCorona = 0;
+              for (int k = 0; k < 10; k++) piS[c][k] = s->pi[(long)k * N + i];
+              PiS[c] = s->Pi[i];
+            }
+        double QC[7] = {0., 0., 0., 0., 0., 0., 0.};
+        for (int c = 0; c < 8; c++)
+          for (int k = 0; k < 7; k++) QC[k] += QCube[c][k] * 0.125;
+        for (int k = 0; k < 7; k++) QC[k] = QC[k] / tau;
+        double eC, pC, nbC, nqC, nsC = 0.0, vxC, vyC, vzC, TC, mubC;
+        transform_pv(E, QC, &eC, &pC, &nbC, &nqC, &nsC, &vxC, &vyC, &vzC);
+        const int isTail = !(eC >= 0.01);
+        if (!isCorona || isTail) continue;
+        eos_eval(E, eC, nbC, &TC, &mubC, &pC);
+        const double muqC = 0., musC = 0.;
+        if (TC > 0.4 || fabs(mubC) > 0.99) acc[4] += 1.;
+        double piC[10], PiC = 0.;
+        for (int k = 0; k < 10; k++) piC[k] = 0.;
+        for (int c = 0; c < 8; c++) {
+          for (int k = 0; k < 10; k++) piC[k] += piS[c][k] * 0.125;
+          PiC += PiS[c] * 0.125;
+        }
+        double v2C = vxC * vxC + vyC * vyC + vzC * vzC;
+        if (v2C > 1.) {
+          vxC *= sqrt(0.99 / v2C);
+          vyC *= sqrt(0.99 / v2C);
+          vzC *= sqrt(0.99 / v2C);
+          v2C = 0.99;
+        }
+        const double etaC = (g->zmin + iz * dz) + 0.5 * dz;
+        to_lab(etaC, &vxC, &vyC, &vzC);
+        const double gammaC = 1. / sqrt(1. - vxC * vxC - vyC * vyC - vzC * vzC);
+        const double uC[4] = {gammaC, gammaC * vxC, gammaC * vyC, gammaC * vzC};
+        const double ch = cosh(etaC), sh = sinh(etaC);
+        double ds[4];
+        ds[0] = tau * (ch * dx * dy * dz);
+        ds[3] = tau * (-sh * dx * dy * dz);
+        ds[1] = 0.0;
+        ds[2] = 0.0;
+        double dVEff = 0.0;
+        for (int k = 0; k < 4; k++) dVEff += ds[k] * uC[k];
+        double pc[10];
+        pi_to_cartesian(ch, sh, piC, pc);
+        const int i0k[4] = {0, 1, 3, 6}; /* index44(0, k) */
+        double dEsurfVisc = 0.;
+        for (int k = 0; k < 4; k++) dEsurfVisc += pc[i0k[k]] * ds[k];
+        acc[1] += (eC + pC) * uC[0] * dVEff - pC * ds[0] + dEsurfVisc;
+        acc[2] += nbC * dVEff;
+        acc[3] += dVEff;
+        if (nel < cap) {
+          double *r = rec + nel * OR_SURF_REC;
+          r[0] = tau;
+          r[1] = (g->xmin + ix * dx) + 0.5 * dx;
+          r[2] = (g->ymin + iy * dy) + 0.5 * dy;
+          r[3] = (g->zmin + iz * dz) + 0.5 * dz;
+          for (int k = 0; k < 4; k++) {
+            r[4 + k] = ds[k];
+            r[8 + k] = uC[k];
+          }
+          r[12] = TC;
+          r[13] = mubC;
+          r[14] = muqC;
+          r[15] = musC;
+          for (int k = 0; k < 10; k++) r[16 + k] = pc[k];
+          r[26] = PiC;
+          r[27] = eC;
+          r[28] = nbC;
+        }
+        nel++;
       }
   return nel;
 }

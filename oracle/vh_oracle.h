@@ -133,6 +133,18 @@ long or_surface(const or_grid *g, const or_eos *eos, const or_state *s,
                 double tau, double dtf, double ecrit, double *rec, long cap,
                 double *acc);
 
+/* The corona part of Fluid::outputCorona (src/fld.cpp:876-1089), called
+ * once at tau0: every interior cell [ix, ix+1] x [iy, iy+1] x [iz, iz+1]
+ * whose eight corners all have e <= ecrit (getPrimVar of Q at tau) and whose
+ * corner-averaged Q gives e >= 0.01 becomes one time-like element at the
+ * cube centre with dSigma = tau dx dy dz (cosh eta, 0, 0, -sinh eta).
+ * Records as or_surface's; acc[OR_SURF_ACC] += 0 (no nsusp), EtotSurf,
+ * nbSurf, vEff increments and the count of elements with T > 0.4 or
+ * |muB| > 0.99.  Returns the number of elements (records beyond cap are
+ * counted, not written). */
+long or_corona(const or_grid *g, const or_eos *eos, const or_state *s, double tau,
+               double ecrit, double *rec, long cap, double *acc);
+
 int or_abi_version(void);
 
 #ifdef __cplusplus

@@ -109,6 +109,55 @@ def save_surface_case(name, setup, nsteps):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
 
 
+CORONA_CASES = {
+    # name: setup factory; Fluid::outputCorona at tau0
+    "corona_glauber_41x41x21": lambda: W.small_glauber3d(41, 21),
+    "corona_glauber_nb_25x25x13": lambda: W.glauber3d_nb_setup(25, 25, 13, eos=W.nb_table(200, 20)),
+}
+
+
+def _setup_arrays(setup):
+    g = setup.grid
+    eos = setup.eos
+    arrays = dict(
+        grid_n=np.array([g.nx, g.ny, g.nz]), grid_b=np.array(g.bounds()),
+        eos_kind=np.array(eos.kind), eos_cnst=np.array(eos.conf_cnst),
+        tr=np.array(setup.tr_vector()), tr_params=np.array([setup.etaSparam, setup.zetaSparam]),
+        clock=np.array([setup.tau0, setup.dt, setup.ecrit]), Q0=setup.Q, m0=setup.m)
+    if eos.kind == 1:
+        arrays.update(eos_egrid=eos.egrid, eos_ngrid=eos.ngrid, eos_p=eos.p, eos_T=eos.T,
+                      eos_mub=eos.mub)
+    return arrays
+
+
+def save_corona_case(name, setup):
+    """The corona elements the reference writes at tau0 (freezeout.dat,
+    extended records with e and nb), its element count and printed line."""
+    r = P.RefRun(setup)
+    with tempfile.TemporaryDirectory() as d:
+        n, line = r.output_corona(d, extend=True)
+        r.close()
+        rec = P.read_freezeout(os.path.join(d, "freezeout.dat.unfinished"), extend=True)
+    assert n == len(rec)
+    arrays = _setup_arrays(setup)
+    arrays.update(corona_count=np.array(n), corona_rec=rec, corona_line=np.array(line))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+
+
+def load_corona_case(path):
+    """(Setup, element count, records [n][29], printed line)."""
+    z = np.load(path)
+    nx, ny, nz = (int(v) for v in z["grid_n"])
+    g = W.Grid(nx, ny, nz, *(float(v) for v in z["grid_b"]))
+    eos = W.EosTable(kind=1, egrid=z["eos_egrid"], ngrid=z["eos_ngrid"], p=z["eos_p"],
+                     T=z["eos_T"], mub=z["eos_mub"])
+    tr = dict(zip(W.TR_FIELDS, (float(v) for v in z["tr"])))
+    tau0, dt, ecrit = (float(v) for v in z["clock"])
+    setup = W.Setup(os.path.basename(path), g, eos, tr, int(z["tr_params"][0]),
+                    int(z["tr_params"][1]), tau0, dt, ecrit, z["Q0"], z["m0"])
+    return setup, int(z["corona_count"]), z["corona_rec"], str(z["corona_line"])
+
+
 def cornelius_cubes():
     """Hypercubes (random, near-binary and exact hits of the iso-value) with
     the reference Cornelius' elements."""
@@ -222,6 +271,10 @@ if __name__ == "__main__":
     for name, (fac, n) in SURFACE_CASES.items():
         if not only or name in only:
             save_surface_case(name, fac(), n)
+            print("wrote", name)
+    for name, fac in CORONA_CASES.items():
+        if not only or name in only:
+            save_corona_case(name, fac())
             print("wrote", name)
     if not only or "cornelius_cubes" in only:
         cornelius_cubes()

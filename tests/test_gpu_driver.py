@@ -96,7 +96,8 @@ def test_cpp_driver_loop_equals_oracle(tmp_path):
     resize at tauGridResize, stop at tauMax or on an empty surface -- from a
     snapshot.  Its final grid equals the oracle driven through the same loop
     bit-for-bit; its printed element counts equal the oracle's and its
-    freezeout.dat records match to 1e-12 (15 printed digits)."""
+    freezeout.dat records (the corona at tau0, then every surface) match to
+    1e-12 (15 printed digits)."""
     import subprocess
     from vhlle_b200 import build as B
     drv = B.build_driver()
@@ -118,7 +119,10 @@ def test_cpp_driver_loop_equals_oracle(tmp_path):
     o = P.OracleRun(setup)
     g = setup.grid
     resized = False
-    recs, counts, nsusp = [], [], []
+    # Fluid::outputCorona at tau0 opens the freeze-out file
+    corona, _ = o.corona()
+    assert "corona elements : %d" % len(corona) in proc_out
+    recs, counts, nsusp = [corona], [], []
     while True:
         o.advance(setup.dt, g.etamin, g.etamax, g.nz)
         # Fluid::outputSurface; the Fluid's step is the full dtau (doubled

@@ -172,3 +172,72 @@ def test_gpu_surface_grows_past_first_capacity():
         assert ok.all(), (s, np.argwhere(~ok)[:5])
         assert int(acc["nsusp"]) == info["nsusp"]
     d.close()
+
+
+@pytest.mark.parametrize("name", ["corona_glauber_41x41x21", "corona_glauber_nb_25x25x13"])
+def test_gpu_corona_equals_reference_fixture(name, tmp_path):
+    """vh_corona at tau0 against the reference's outputCorona: element
+    count, records (15 printed digits, device cosh/sinh/log/tanh within the
+    last bit) and EtotSurf; vh_surface_write then writes those records."""
+    from make_golden import load_corona_case
+    from vhlle_b200.capi import GpuHydro
+    setup, n, rec, line = load_corona_case(os.path.join(GOLDEN, name + ".npz"))
+    d = GpuHydro(setup)
+    got, info = d.corona()
+    assert info["nelements"] == n > 0 and info["nsusp"] == 0
+    ok = rec_close(got, rec)
+    assert ok.all(), np.argwhere(~ok)[:5]
+    assert abs(info["EtotSurf"] - float(line.split()[5])) <= 5e-6 * abs(info["EtotSurf"])
+    path = str(tmp_path / "freezeout.dat")
+    d.surface_write(path, extend=True)
+    assert rec_close(P.read_freezeout(path, extend=True), rec, 1e-13).all()
+    d.close()
+
+
+def rec_close_scaled(a, b, rtol=REC_RTOL, floor=1e-13):
+    """rec_close with two allowances for the amplification of a last-bit
+    difference between the device's cosh/sinh/log/tanh and the host
+    library's (transformToLab, pi^{mu nu} to Cartesian components):
+    an absolute floor of `floor` x the column's largest magnitude, for
+    results that cancel near zero (e.g. Y = eta + ln((1+v)/(1-v))/2 close
+    to 0), and a relative 1e-15 gamma^2 per element (gamma = u^0), since
+    gamma = 1/sqrt(1 - v^2) multiplies a relative change of v by gamma^2
+    (gamma ~ 160 in the corona's vacuum-edge cells after a few steps)."""
+    scale = np.maximum(np.abs(a).max(axis=0), np.abs(b).max(axis=0))
+    g2 = np.maximum(np.abs(a[:, 8]), np.abs(b[:, 8]))[:, None] ** 2
+    tol = (rtol + 1e-15 * g2) * np.maximum(np.abs(a), np.abs(b)) + floor * scale + 1e-300
+    return np.abs(a - b) <= tol
+
+
+def _bad(a, b, ok):
+    idx = np.argwhere(~ok)[:5]
+    return [(int(i), int(j), float(a[i, j]), float(b[i, j])) for i, j in idx]
+
+
+def test_gpu_corona_full_size_event_equals_oracle():
+    """The 101x101x51 event's corona at tau0 and after 3 steps: every
+    record, the sums, and EtotSurf / vEff carried into the next vh_surface."""
+    from vhlle_b200.capi import GpuHydro
+    setup = W.glauber3d_setup()
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    ro, acc = o.corona()
+    rd, info = d.corona()
+    assert len(ro) == info["nelements"] > 1000
+    ok = rec_close(rd, ro)
+    assert ok.all(), _bad(rd, ro, ok)
+    for k in ("EtotSurf", "vEff"):
+        assert abs(info[k] - acc[k]) <= 1e-10 * abs(acc[k]), k
+    etot, veff = acc["EtotSurf"], acc["vEff"]
+    o.step(3)
+    d.step(3)
+    ro, acc = o.corona()
+    rd, info = d.corona()
+    assert len(ro) == info["nelements"]
+    ok = rec_close_scaled(rd, ro)
+    assert ok.all(), _bad(rd, ro, ok)
+    etot += acc["EtotSurf"]
+    rs, accs = o.surface(cap=2000000)
+    _, infos = d.surface()
+    assert infos["nelements"] == len(rs)
+    assert abs(infos["EtotSurf"] - (etot + accs["EtotSurf"])) <= 1e-10 * abs(etot) + 1e-8
+    d.close()

@@ -72,3 +72,40 @@ def test_oracle_surface_equals_reference_fixture():
     ok = rec_close(got, rec)
     assert ok.all(), (np.argwhere(~ok)[:5], got[~ok][:5], rec[~ok][:5])
     assert sum(counts) > 500
+
+
+CORONA_FIXTURES = ("corona_glauber_41x41x21", "corona_glauber_nb_25x25x13")
+
+
+@pytest.mark.parametrize("name", CORONA_FIXTURES)
+def test_oracle_corona_equals_reference_fixture(name):
+    """Fluid::outputCorona at tau0 (src/fld.cpp:876-1089): element count,
+    records (15 printed digits) and the printed EtotSurf."""
+    from make_golden import load_corona_case
+    setup, n, rec, line = load_corona_case(os.path.join(GOLDEN, name + ".npz"))
+    ro, acc = P.OracleRun(setup).corona()
+    assert len(ro) == n > 0
+    ok = rec_close(ro, rec)
+    assert ok.all(), np.argwhere(~ok)[:5]
+    words = line.split()  # tau E Efull nbSurf S EtotSurf
+    assert abs(acc["EtotSurf"] - float(words[5])) <= 5e-6 * abs(acc["EtotSurf"])
+    assert acc["nsusp"] == 0
+
+
+@pytest.mark.skipif(not P.ref_available(), reason="oracle/_ref not built here")
+def test_oracle_corona_equals_reference_live():
+    """The corona of a fresh event with baryon charge, after some steps (the
+    reference calls it at tau0 only, but it is defined at any tau)."""
+    import tempfile
+    from vhlle_b200 import workloads as W
+    setup = W.glauber3d_nb_setup(33, 33, 17, eos=W.nb_table(200, 20), seed=77, b=10.0)
+    o, r = P.OracleRun(setup), P.RefRun(setup)
+    o.step(3)
+    r.step(3)
+    ro, _ = o.corona()
+    with tempfile.TemporaryDirectory() as d:
+        n, _ = r.output_corona(d, extend=True)
+        rr = P.read_freezeout(os.path.join(d, "freezeout.dat.unfinished"), extend=True)
+    r.close()
+    assert len(ro) == n == len(rr) > 0
+    assert rec_close(ro, rr).all()

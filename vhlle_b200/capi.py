@@ -29,7 +29,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_records",
-           "vh_surface_device", "vh_surface_write", "vh_cornelius4d", "vh_set_con2prim",
+           "vh_surface_device", "vh_surface_write", "vh_corona", "vh_cornelius4d", "vh_set_con2prim",
            "vh_con2prim_stats", "vh_mlp_create", "vh_mlp_destroy", "vh_mlp_set_params",
            "vh_mlp_get_params", "vh_mlp_forward", "vh_mlp_grad", "vh_mlp_train",
            "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
@@ -291,6 +291,7 @@ def lib():
                              ctypes.POINTER(ctypes.c_int)]
     L.vh_resize2x.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.vh_surface.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
+    L.vh_corona.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
     L.vh_surface_records.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
@@ -500,6 +501,20 @@ class GpuHydro:
                                              ctypes.c_void_p(dout.data_ptr())))
         self.sync()
         return dout.cpu().numpy().T.copy()
+
+    def corona(self, ecrit=None):
+        """Fluid::outputCorona's elements at the current tau (vh_corona):
+        (records [n][29], info dict)."""
+        info = VhSurfaceInfo()
+        ec = self.setup.ecrit if ecrit is None else ecrit
+        self._check(self.L.vh_corona(self.h, ec, ctypes.byref(info)))
+        n = info.nelements
+        rec = np.zeros((n, SURF_REC))
+        if n:
+            got = ctypes.c_long()
+            self._check(self.L.vh_surface_records(self.h, rec.ctypes.data_as(_dp), n,
+                                                  ctypes.byref(got)))
+        return rec, {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
 
     def surface_only(self, ecrit=None):
         """vh_surface without copying the records: the info dict."""

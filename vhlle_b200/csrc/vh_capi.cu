@@ -689,10 +689,8 @@ vh_status vh_totals(vh_ctx* ctx, double ecrit, double* out) {
 // block partials of the surface sums (a fixed count keeps them deterministic)
 static const int kSurfPartials = 296;
 
-vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
-  if (!ctx) return VH_ERR_ARG;
-  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_surface: no state uploaded");
-  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+// the buffers every surface or corona call uses, allocated on first use
+static vh_status surf_common(vh_ctx* ctx) {
   const vh::Geo& g = ctx->g;
   vh_ctx::Surf& S = ctx->surf;
   vh_status st;
@@ -707,6 +705,17 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
     static_assert(vh::kSurfAcc == 5, "vh_ctx::Surf::Host::acc");
     VH_CUDA(ctx, cudaHostAlloc((void**)&S.host, sizeof(vh_ctx::Surf::Host), cudaHostAllocDefault));
   }
+  return VH_OK;
+}
+
+vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_surface: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  const vh::Geo& g = ctx->g;
+  vh_ctx::Surf& S = ctx->surf;
+  vh_status st;
+  if ((st = surf_common(ctx))) return st;
   // Every stage reads the counts from device memory, so the call waits for
   // the GPU once, at the end.  The buffers start at 64k cubes and twice as
   // many elements; a call that finds more grows them and runs again (the
@@ -763,6 +772,58 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   }
   if (bits & vh::ERR_SURFACE)
     return fail(ctx, VH_ERR_NUMERIC, "vh_surface: a hypercube on which the reference stops");
+  return VH_OK;
+}
+
+vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_corona: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  const vh::Geo& g = ctx->g;
+  vh_ctx::Surf& S = ctx->surf;
+  vh_status st;
+  if ((st = surf_common(ctx))) return st;
+  const long long ninterior = std::max(1LL, vh::surf_ncube(g));
+  if (!S.cflag && (st = dalloc(ctx, &S.cflag, (size_t)ninterior))) return st;
+  // one element per cube at most: the buffers start at 64k elements and a
+  // call that finds more grows them and runs again, as vh_surface does
+  size_t want = std::max<size_t>(std::min<size_t>(S.cap_cubes, S.cap_rec / vh::kSurfRec),
+                                 (size_t)std::min(ninterior, 65536LL));
+  cudaStream_t s = ctx->stream;
+  vh_ctx::Surf::Host& H = *S.host;
+  for (int pass = 0; pass < 2; pass++) {
+    if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, want)) ||
+        (st = dgrow(ctx, &S.rec, &S.cap_rec, want * vh::kSurfRec)) ||
+        (st = dgrow(ctx, &S.contrib, &S.cap_contrib, want * vh::kSurfAcc)))
+      return st;
+    const int cap = (int)std::min<size_t>(want, INT32_MAX / 32);
+    vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, ctx->tau - ctx->fluid_dt, S.eN, S.eP,
+                           s);
+    vh::launch_corona(g, ctx->eos, ctx->f, ctx->tau, ecrit, ctx->grid.xmin, ctx->grid.ymin,
+                      ctx->grid.etamin, S.eN, S.cflag, S.blk, S.counters, S.cubes, cap, S.rec,
+                      S.contrib, S.partial, kSurfPartials, s);
+    VH_CUDA(ctx, cudaGetLastError());
+    VH_CUDA(ctx, cudaMemcpyAsync(H.cnt, S.counters, sizeof(int), cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaMemcpyAsync(H.acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
+                                 sizeof H.acc, cudaMemcpyDeviceToHost, s));
+    VH_CUDA(ctx, cudaStreamSynchronize(s));
+    if ((size_t)H.cnt[0] <= (size_t)cap) break;
+    if (pass == 1) return fail(ctx, VH_ERR_STATE, "vh_corona: element buffers did not grow");
+    want = (size_t)H.cnt[0] + (size_t)H.cnt[0] / 8 + 1;
+  }
+  const double* acc = H.acc;
+  S.nel = H.cnt[0];
+  ctx->EtotSurf += acc[1];
+  ctx->nbCorona += acc[2];
+  ctx->vEff += acc[3];
+  if (info) {
+    info->nelements = H.cnt[0];
+    info->nsusp = 0;
+    info->high_T = (long)acc[4];
+    info->EtotSurf = ctx->EtotSurf;
+    info->nbSurf = ctx->nbCorona;
+    info->vEff = ctx->vEff;
+  }
   return VH_OK;
 }
 

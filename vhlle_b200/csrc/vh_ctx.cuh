@@ -38,10 +38,12 @@ struct vh_ctx {
   // surface sums: EtotSurf and vEff are Fluid members (reset by the resize's
   // new Fluid), nbSurf is a function static in the reference (never reset)
   double EtotSurf = 0., vEff = 0., nbSurf = 0.;
+  double nbCorona = 0.;  // outputCorona's own function static (src/fld.cpp:877)
   struct Surf {
     double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
            *partial = nullptr;
     int *blk = nullptr, *cubes = nullptr, *cnt = nullptr, *counters = nullptr;
+    unsigned char* cflag = nullptr;  // [interior cubes] corona flags
     size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
     long long nel = 0;
     // pinned landing place of a call's counts, sums and error bits

@@ -359,6 +359,23 @@ __device__ __forceinline__ void to_lab(double eta, double& vx, double& vy, doubl
   vz = tanh(Y);
 }
 
+// pi^{mu nu} to Cartesian components at space-time rapidity eta with
+// ch = cosh(eta), sh = sinh(eta), src/fld.cpp:767-786 and :1029-1048
+// (index44 order)
+__device__ __forceinline__ void pi_to_cartesian(double ch, double sh, const double* piC,
+                                                double* pc) {
+  pc[0] = ch * ch * piC[0] + 2. * ch * sh * piC[6] + sh * sh * piC[9];
+  pc[1] = ch * piC[1] + sh * piC[7];
+  pc[3] = ch * piC[3] + sh * piC[8];
+  pc[6] = ch * sh * (piC[0] + piC[9]) + (ch * ch + sh * sh) * piC[6];
+  pc[2] = piC[2];
+  pc[4] = piC[4];
+  pc[7] = sh * piC[1] + ch * piC[7];
+  pc[5] = piC[5];
+  pc[8] = sh * piC[3] + ch * piC[8];
+  pc[9] = sh * sh * piC[0] + ch * ch * piC[9] + 2. * sh * ch * piC[6];
+}
+
 struct SurfArgs {
   Geo g;
   EosDev E;
@@ -457,18 +474,8 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
   double dVEff = 0.0;
 #pragma unroll
   for (int q = 0; q < 4; q++) dVEff += ds[q] * uC[q];
-  // pi^{mu nu} to Cartesian components, src/fld.cpp:767-786 (index44 order)
   double pc[10];
-  pc[0] = ch * ch * piC[0] + 2. * ch * sh * piC[6] + sh * sh * piC[9];
-  pc[1] = ch * piC[1] + sh * piC[7];
-  pc[3] = ch * piC[3] + sh * piC[8];
-  pc[6] = ch * sh * (piC[0] + piC[9]) + (ch * ch + sh * sh) * piC[6];
-  pc[2] = piC[2];
-  pc[4] = piC[4];
-  pc[7] = sh * piC[1] + ch * piC[7];
-  pc[5] = piC[5];
-  pc[8] = sh * piC[3] + ch * piC[8];
-  pc[9] = sh * sh * piC[0] + ch * ch * piC[9] + 2. * sh * ch * piC[6];
+  pi_to_cartesian(ch, sh, piC, pc);
   double dEsurfVisc = 0.;
   dEsurfVisc += pc[0] * ds[0];
   dEsurfVisc += pc[1] * ds[1];
@@ -496,6 +503,167 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
   r[26] = PiC;
   r[27] = eC;
   r[28] = nbC;
+}
+
+// ===================================================================
+// Corona: the element part of Fluid::outputCorona (src/fld.cpp:876-1089),
+// called once at tau0.  Stages:
+//   1. k_surf_energy      e at tau per corner cell (eP unused)
+//   2. k_corona_flag      per interior cube: all eight corners e <= ecrit
+//                         and e(corner-averaged Q / tau) >= 0.01; per-block
+//                         counts
+//   3. k_scan_excl        block offsets (total = element count)
+//   4. k_corona_compact   element cubes in the reference's loop order
+//   5. k_corona_elements  one record per element (+ its sums' contributions)
+//   6. k_sum_cols         deterministic sums
+// ===================================================================
+
+// the corner-averaged Q / tau of cube (ix, iy, iz), src/fld.cpp:960-974
+__device__ __forceinline__ void corona_qc(const Geo& g, const double* __restrict__ Q, int ix,
+                                          int iy, int iz, double tau, double* QC) {
+#pragma unroll
+  for (int k = 0; k < 7; k++) QC[k] = 0.;
+#pragma unroll 1
+  for (int c = 0; c < 8; c++) {
+    const long long i = cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1));
+#pragma unroll
+    for (int k = 0; k < 7; k++) QC[k] += Q[k * g.N + i] * 0.125;
+  }
+#pragma unroll
+  for (int k = 0; k < 7; k++) QC[k] = ddivp(QC[k], tau);
+}
+
+__global__ void __launch_bounds__(kSurfBlock) k_corona_flag(Geo g, EosDev E,
+                                                            const double* __restrict__ Q,
+                                                            const double* __restrict__ eN,
+                                                            double tau, double ecrit,
+                                                            long long ncube,
+                                                            unsigned char* __restrict__ flag,
+                                                            int* __restrict__ blk) {
+  const long long t = (long long)blockIdx.x * kSurfBlock + threadIdx.x;
+  int f = 0;
+  if (t < ncube) {
+    int ix, iy, iz;
+    cube_cell(g, t, ix, iy, iz);
+    bool corona = true;
+#pragma unroll
+    for (int c = 0; c < 8; c++)
+      if (eN[cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1))] > ecrit) corona = false;
+    if (corona) {
+      double QC[7];
+      corona_qc(g, Q, ix, iy, iz, tau, QC);
+      Prim P;
+      transform_pv(E, QC, P);
+      f = P.e >= 0.01;  // not the tail
+    }
+    flag[t] = (unsigned char)f;
+  }
+  const int c = __syncthreads_count(f);
+  if (threadIdx.x == 0) blk[blockIdx.x] = c;
+}
+
+__global__ void __launch_bounds__(kSurfBlock) k_corona_compact(long long ncube,
+                                                               const unsigned char* __restrict__ flag,
+                                                               const int* __restrict__ blkoff,
+                                                               int* __restrict__ cubes, int cap) {
+  __shared__ int woff[kSurfBlock / 32];
+  const long long t = (long long)blockIdx.x * kSurfBlock + threadIdx.x;
+  const bool f = t < ncube && flag[t];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(0xffffffffu, f);
+  if (lane == 0) woff[w] = __popc(bal);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int k = 0; k < kSurfBlock / 32; k++) {
+      const int v = woff[k];
+      woff[k] = s;
+      s += v;
+    }
+  }
+  __syncthreads();
+  const int slot = blkoff[blockIdx.x] + woff[w] + __popc(bal & ((1u << lane) - 1u));
+  if (f && slot < cap) cubes[slot] = (int)t;  // past cap: the host grows and reruns
+}
+
+__global__ void __launch_bounds__(128) k_corona_elements(SurfArgs a) {
+  const int nel = min(a.counters[0], a.cap_el);
+  const Geo& g = a.g;
+  const long long N = g.N;
+  const double dx = g.dx, dy = g.dy, dz = g.dz, tau = a.tau;
+  for (int el = blockIdx.x * blockDim.x + threadIdx.x; el < nel; el += gridDim.x * blockDim.x) {
+    int ix, iy, iz;
+    cube_cell(g, a.cubes[el], ix, iy, iz);
+    double QC[7];
+    corona_qc(g, a.Q, ix, iy, iz, tau, QC);
+    Prim P;
+    transform_pv(a.E, QC, P);
+    double TC, mubC, pC;
+    eos_eval(a.E, P.e, P.nb, TC, mubC, pC);
+    const double eC = P.e, nbC = P.nb;
+    double vxC = P.vx, vyC = P.vy, vzC = P.vz;
+    double* ct = a.contrib + (long long)el * 5;
+    ct[0] = 0.;
+    ct[4] = (TC > 0.4 || fabs(mubC) > 0.99) ? 1. : 0.;
+    double piC[10], PiC = 0.;
+#pragma unroll
+    for (int q = 0; q < 10; q++) piC[q] = 0.;
+#pragma unroll 1
+    for (int c = 0; c < 8; c++) {
+      const long long i = cidx(g, ix + (c >> 2), iy + ((c >> 1) & 1), iz + (c & 1));
+#pragma unroll
+      for (int q = 0; q < 10; q++) piC[q] += a.pi[q * N + i] * 0.125;
+      PiC += a.Pi[i] * 0.125;
+    }
+    const double v2C = vxC * vxC + vyC * vyC + vzC * vzC;
+    if (v2C > 1.) {
+      vxC *= sqrt(0.99 / v2C);
+      vyC *= sqrt(0.99 / v2C);
+      vzC *= sqrt(0.99 / v2C);
+    }
+    const double etaC = (a.zmin + iz * dz) + 0.5 * dz;
+    to_lab(etaC, vxC, vyC, vzC);
+    const double gammaC = 1. / sqrt(1. - vxC * vxC - vyC * vyC - vzC * vzC);
+    const double uC[4] = {gammaC, gammaC * vxC, gammaC * vyC, gammaC * vzC};
+    const double ch = cosh(etaC), sh = sinh(etaC);
+    double ds[4];
+    ds[0] = tau * (ch * dx * dy * dz);
+    ds[3] = tau * (-sh * dx * dy * dz);
+    ds[1] = 0.0;
+    ds[2] = 0.0;
+    double dVEff = 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; q++) dVEff += ds[q] * uC[q];
+    double pc[10];
+    pi_to_cartesian(ch, sh, piC, pc);
+    double dEsurfVisc = 0.;
+    dEsurfVisc += pc[0] * ds[0];
+    dEsurfVisc += pc[1] * ds[1];
+    dEsurfVisc += pc[3] * ds[2];
+    dEsurfVisc += pc[6] * ds[3];
+    ct[1] = (eC + pC) * uC[0] * dVEff - pC * ds[0] + dEsurfVisc;
+    ct[2] = nbC * dVEff;
+    ct[3] = dVEff;
+    double* r = a.rec + (long long)el * kSurfRec;
+    r[0] = tau;
+    r[1] = (a.xmin + ix * dx) + 0.5 * dx;
+    r[2] = (a.ymin + iy * dy) + 0.5 * dy;
+    r[3] = (a.zmin + iz * dz) + 0.5 * dz;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      r[4 + q] = ds[q];
+      r[8 + q] = uC[q];
+    }
+    r[12] = TC;
+    r[13] = mubC;
+    r[14] = 0.;
+    r[15] = 0.;
+#pragma unroll
+    for (int q = 0; q < 10; q++) r[16 + q] = pc[q];
+    r[26] = PiC;
+    r[27] = eC;
+    r[28] = nbC;
+  }
 }
 
 // Column sums of x[n][kSurfAcc] in a fixed tree: block partials, then one
@@ -606,6 +774,27 @@ void launch_cornelius_batch(const double* cubes, int n, const double* dx, double
   if (n > 0)
     k_cornelius_batch<<<(n + kCornWarps - 1) / kCornWarps, 32 * kCornWarps, 0, s>>>(
         cubes, n, dx[0], dx[1], dx[2], dx[3], e0, counts, geo);
+}
+
+void launch_corona(const Geo& g, const EosDev& E, const Fields& f, double tau, double ecrit,
+                   double xmin, double ymin, double zmin, const double* eN, unsigned char* flag,
+                   int* blk, int* counters, int* cubes, int cap, double* rec, double* contrib,
+                   double* partial, int npartial, cudaStream_t s) {
+  const int nb = surf_count_blocks(g);
+  if (nb == 0) {
+    cudaMemsetAsync(counters, 0, sizeof(int), s);
+  } else {
+    const long long ncube = surf_ncube(g);
+    k_corona_flag<<<nb, kSurfBlock, 0, s>>>(g, E, f.Q, eN, tau, ecrit, ncube, flag, blk);
+    k_scan_excl<<<1, kScanBlock, 0, s>>>(blk, nb, counters, nullptr, 0);
+    k_corona_compact<<<nb, kSurfBlock, 0, s>>>(ncube, flag, blk, cubes, cap);
+  }
+  SurfArgs a{g,    E,   f.Q, f.Qprev, f.pi, f.Pi, tau, 0., ecrit, xmin, ymin, zmin,
+             cubes, counters, cap, cap, nullptr, nullptr, rec, contrib};
+  k_corona_elements<<<kElemGrid, 128, 0, s>>>(a);
+  k_sum_cols<<<npartial, kTotBlock, 0, s>>>(contrib, 0, kSurfAcc, partial, counters, cap);
+  k_sum_cols<<<1, kTotBlock, 0, s>>>(partial, npartial, kSurfAcc, partial + npartial * kSurfAcc,
+                                     nullptr, 0);
 }
 
 }  // namespace vh

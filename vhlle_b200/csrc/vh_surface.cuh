@@ -46,6 +46,14 @@ void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double
                           const int* off, double* rec, double* contrib, double* partial,
                           int npartial, cudaStream_t s);
 
+// Fluid::outputCorona's elements (eN from launch_surf_energy at tau):
+// counters[0] = the element count; the first min(count, cap) records and
+// contributions are written, their sums land in partial[npartial*kSurfAcc ..]
+void launch_corona(const Geo& g, const EosDev& E, const Fields& f, double tau, double ecrit,
+                   double xmin, double ymin, double zmin, const double* eN, unsigned char* flag,
+                   int* blk, int* counters, int* cubes, int cap, double* rec, double* contrib,
+                   double* partial, int npartial, cudaStream_t s);
+
 // Cornelius on n independent hypercubes (16 corner values each): counts[k]
 // elements (-1 where the reference stops), geo[k][10][8] centroid + normal
 void launch_cornelius_batch(const double* cubes, int n, const double* dx, double e0, int* counts,

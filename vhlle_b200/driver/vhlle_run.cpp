@@ -9,7 +9,8 @@
 // Parameters are read exactly as the reference reads them (same keys,
 // defaults, "CCC"/"UUU" echo).  The hydro EoS is the EoS1f table named by
 // the extra key eos1fFile, else the conformal gas of 47.5 degrees of
-// freedom.  Each loop iteration does what Fluid::outputSurface does: it
+// freedom.  Before the loop the corona of Fluid::outputCorona opens the
+// freeze-out file.  Each loop iteration does what Fluid::outputSurface does: it
 // appends the freeze-out elements to DIR/freezeout.dat.unfinished (renamed
 // freezeout.dat at the end) and prints the same line (tau, E, Efull,
 // nbSurf, S, EtotSurf, elements, suspicious elements, cut-cell fraction);
@@ -123,6 +124,22 @@ int run(int argc, char** argv) {
   int nloops = 0;
   long nelements = 0;
   std::cout << std::setprecision(6);
+  {
+    // Fluid::outputCorona at tau0 (src/main.cpp:390, src/fld.cpp:876-1089):
+    // the corona elements go first into the freeze-out file; the lines it
+    // prints (src/fld.cpp:1075-1088)
+    const vh_surface_info ci = h->corona();
+    h->writeSurface(fo_unf.c_str(), P.freezeoutExtend);
+    const vhb::Totals t = h->totals();
+    std::cout << std::setw(10) << "tau" << std::setw(13) << "E" << std::setw(13) << "Efull"
+              << std::setw(13) << "Nb" << std::setw(13) << "Sfull" << std::setw(13) << "EtotSurf"
+              << std::setw(13) << "elements" << std::setw(10) << "susp." << std::setw(13)
+              << "%cut" << std::endl;
+    std::cout << std::setw(10) << h->getTau() << std::setw(13) << t.E << std::setw(13) << t.Efull
+              << std::setw(13) << ci.nbSurf << std::setw(13) << t.S << std::setw(13)
+              << ci.EtotSurf << std::endl;
+    std::cout << "corona elements : " << ci.nelements << std::endl;
+  }
   do {
     const int nSubSteps = h->advance(P.dtau, P.etamin, P.etamax, P.nz);
     if (nSubSteps > 1) std::cout << "timestep reduced by " << nSubSteps << std::endl;
