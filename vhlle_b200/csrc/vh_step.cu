@@ -363,8 +363,11 @@ __device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N
 // latency better than fewer, spill-free ones (measured: 3 and 2 blocks per SM
 // are 7 % and 35 % slower, 5 and 6 are 9 % and 3 % slower).
 constexpr int kRelaxMinBlocks = 4;
+constexpr int kRelaxBlock = 128;
+// shared-memory rows of k_is_relax's relaxation loops: pi, sigma, u, h0, f0
+constexpr int kSmPI = 0, kSmSIG = 10, kSmU = 20, kSmH = 24, kSmF = 34, kSmRows = 44;
 
-__global__ void __launch_bounds__(128, kRelaxMinBlocks) k_is_relax(
+__global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
     Geo g, EosDev E, TrDev tr, const double* __restrict__ Q, const double* __restrict__ Qprev,
     const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
     const double* __restrict__ pTh, const double* __restrict__ pBC,
@@ -587,31 +590,54 @@ __global__ void __launch_bounds__(128, kRelaxMinBlocks) k_is_relax(
   h0[index44(2, 0)] += ddivp(-vz, tau1) * PI(2, 3) * dt / 2.;
   h0[index44(3, 1)] += -(ddivp(vz, tau1) * PI(0, 1)) * dt / 2.;
   h0[index44(3, 2)] += -(ddivp(vz, tau1) * PI(0, 2)) * dt / 2.;
+  // The relaxation sums over (a, b) run as a loop with (a, b) known only at
+  // run time, so that its body (36 divisions by gamma) is fetched once per
+  // warp instead of ten times unrolled: the unrolled kernel's instruction
+  // stream outgrew the instruction caches.  Operands indexed by a or b come
+  // from shared memory ([component][thread]); the arithmetic of every term
+  // is the reference's, in its order.
+  __shared__ double sm[kSmRows][kRelaxBlock];
+  const int t = threadIdx.x;
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int k = 0; k < 10; k++) {
+    sm[kSmPI + k][t] = cpi[k];
+    sm[kSmSIG + k][t] = sig[k];
+    sm[kSmH + k][t] = h0[k];
+  }
 #pragma unroll
-    for (int b = 0; b <= a; b++) {
-      double acc = h0[index44(a, b)];
-      acc += ddivp(-deltapipi * PI(a, b) * du + lambdapiPi * cPi * SIG(a, b), gamma) * 0.5 * dt;
+  for (int k = 0; k < 4; k++) sm[kSmU + k][t] = u[k];
+#pragma unroll 1
+  for (int ab = 0; ab < 10; ab++) {
+    const int a = ab >= 6 ? 3 : ab >= 3 ? 2 : ab >= 1 ? 1 : 0;
+    const int b = ab - a * (a + 1) / 2;
+    const double ua = sm[kSmU + a][t], ub = sm[kSmU + b][t];
+    double dab = -ua * ub;  // Delta[index44(a, b)]
+    if (a == b) dab += a == 0 ? 1. : -1.;
+    double acc = sm[kSmH + ab][t];
+    acc += ddivp(-deltapipi * sm[kSmPI + ab][t] * du + lambdapiPi * cPi * sm[kSmSIG + ab][t],
+                 gamma) *
+           0.5 * dt;
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        acc += ddivp(phi7 * PI(a, k) * PI(b, k) * gmumu[k] -
-                         taupipi * 0.5 *
-                             (PI(a, k) * SIG(b, k) * gmumu[k] + PI(b, k) * SIG(a, k) * gmumu[k]),
+    for (int k = 0; k < 4; k++) {
+      const double gk = gmumu[k];
+      const double pak = sm[kSmPI + index44(a, k)][t], pbk = sm[kSmPI + index44(b, k)][t];
+      const double sak = sm[kSmSIG + index44(a, k)][t], sbk = sm[kSmSIG + index44(b, k)][t];
+      acc += ddivp(phi7 * pak * pbk * gk - taupipi * 0.5 * (pak * sbk * gk + pbk * sak * gk),
+                   gamma) *
+             0.5 * dt;
+#pragma unroll
+      for (int l = 0; l < 4; l++) {
+        acc += ddivp((-pak * ub - pbk * ua) * u[l] * dmu[l][k] * gk, gamma) * 0.5 * dt -
+               ddivp(1. / 3. * dab * PI(k, l) * (phi7 * PI(k, l) - taupipi * SIG(k, l)) * gk *
+                         gmumu[l],
                      gamma) *
-               0.5 * dt;
-#pragma unroll
-        for (int l = 0; l < 4; l++) {
-          acc += ddivp((-PI(a, k) * u[b] - PI(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k], gamma) *
-                     0.5 * dt -
-                 ddivp(1. / 3. * Delta[index44(a, b)] * PI(k, l) *
-                           (phi7 * PI(k, l) - taupipi * SIG(k, l)) * gmumu[k] * gmumu[l],
-                       gamma) *
-                     0.5 * dt;
-        }
+                   0.5 * dt;
       }
-      h0[index44(a, b)] = acc;
     }
+    sm[kSmH + ab][t] = acc;
+  }
+#pragma unroll
+  for (int k = 0; k < 10; k++) h0[k] = sm[kSmH + k][t];
 #pragma unroll
   for (int k = 0; k < 4; k++)
 #pragma unroll
@@ -643,29 +669,40 @@ __global__ void __launch_bounds__(128, kRelaxMinBlocks) k_is_relax(
   f0[index44(3, 1)] += -(ddivp(vz, tau1) * H(0, 1)) * dt;
   f0[index44(3, 2)] += -(ddivp(vz, tau1) * H(0, 2)) * dt;
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int k = 0; k < 10; k++) sm[kSmF + k][t] = f0[k];
+#pragma unroll 1
+  for (int ab = 0; ab < 10; ab++) {
+    const int a = ab >= 6 ? 3 : ab >= 3 ? 2 : ab >= 1 ? 1 : 0;
+    const int b = ab - a * (a + 1) / 2;
+    const double ua = sm[kSmU + a][t], ub = sm[kSmU + b][t];
+    double dab = -ua * ub;  // Delta[index44(a, b)]
+    if (a == b) dab += a == 0 ? 1. : -1.;
+    double acc = sm[kSmF + ab][t];
+    acc += ddivp(-deltapipi * sm[kSmH + ab][t] * du + lambdapiPi * H0 * sm[kSmSIG + ab][t],
+                 gamma) *
+           dt;
 #pragma unroll
-    for (int b = 0; b <= a; b++) {
-      double acc = f0[index44(a, b)];
-      acc += ddivp(-deltapipi * H(a, b) * du + lambdapiPi * H0 * SIG(a, b), gamma) * dt;
+    for (int k = 0; k < 4; k++) {
+      const double gk = gmumu[k];
+      const double pak = sm[kSmPI + index44(a, k)][t];
+      const double hak = sm[kSmH + index44(a, k)][t], hbk = sm[kSmH + index44(b, k)][t];
+      const double sak = sm[kSmSIG + index44(a, k)][t], sbk = sm[kSmSIG + index44(b, k)][t];
+      acc += ddivp(phi7 * pak * hbk * gk - taupipi * 0.5 * (hak * sbk * gk + hbk * sak * gk),
+                   gamma) *
+             dt;
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        acc += ddivp(phi7 * PI(a, k) * H(b, k) * gmumu[k] -
-                         taupipi * 0.5 *
-                             (H(a, k) * SIG(b, k) * gmumu[k] + H(b, k) * SIG(a, k) * gmumu[k]),
+      for (int l = 0; l < 4; l++) {
+        acc += ddivp((-hak * ub - hbk * ua) * u[l] * dmu[l][k] * gk -
+                         1. / 3. * dab * H(k, l) * (phi7 * H(k, l) - taupipi * SIG(k, l)) * gk *
+                             gmumu[l],
                      gamma) *
                dt;
-#pragma unroll
-        for (int l = 0; l < 4; l++) {
-          acc += ddivp((-H(a, k) * u[b] - H(b, k) * u[a]) * u[l] * dmu[l][k] * gmumu[k] -
-                           1. / 3. * Delta[index44(a, b)] * H(k, l) *
-                               (phi7 * H(k, l) - taupipi * SIG(k, l)) * gmumu[k] * gmumu[l],
-                       gamma) *
-                 dt;
-        }
       }
-      f0[index44(a, b)] = acc;
     }
+    sm[kSmF + ab][t] = acc;
+  }
+#pragma unroll
+  for (int k = 0; k < 10; k++) f0[k] = sm[kSmF + k][t];
 #pragma unroll
   for (int k = 0; k < 4; k++)
 #pragma unroll
@@ -971,7 +1008,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
     k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
                                    F.pBC, a.clk);
     done(KK_VISC_PRIMS);
-    k_is_relax<<<nb128, 128, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh, F.pBC, F.pi,
+    k_is_relax<<<nb128, kRelaxBlock, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh, F.pBC, F.pi,
                                  F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0, F.flux, a.clk, F.err);
     done(KK_IS_RELAX);
     k_is_advect<<<nb, bs, 0, s>>>(g, F.pA, F.pi0, F.piH0, F.Pi0, F.PiH0, F.pi, F.piH, F.Pi, F.PiH,
