@@ -1,4 +1,5 @@
 """The correctly rounded exp and x^(1/4) of vhlle_b200/csrc/vh_crmath.cuh,
+and its divide-free division (Markstein),
 compiled for the host from the same header (IEEE operations and explicit
 fma only, no contraction, so the host build gives the device's bits):
 every result equals the exact value rounded to nearest (60-digit decimal
@@ -17,16 +18,39 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "vhlle_b200", "csrc", "vh_crmath.cuh")
 
 PROGRAM = r"""
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include "vh_crmath.cuh"
 int main() {
   char f[8];
   double x;
-  while (std::scanf("%1s %la", f, &x) == 2) {
+  if (std::scanf("%1s", f) == 1 && f[0] == 'm') {
+    // Markstein division against the divide: n random pairs from a seed
+    long n, seed;
+    if (std::scanf("%ld %ld", &n, &seed) != 2) return 1;
+    unsigned long long s = (unsigned long long)seed * 2654435761ull + 1;
+    auto next = [&]() {  // xorshift64*
+      s ^= s >> 12; s ^= s << 25; s ^= s >> 27;
+      return s * 2685821657736338717ull;
+    };
+    auto unit = [&]() { return (double)(next() >> 11) * 0x1p-53; };
+    long bad = 0, used = 0;
+    for (long i = 0; i < n; i++) {
+      const double b = std::ldexp(1.0 + unit(), (int)(unit() * 200) - 100);
+      const double y = (unit() < 0.5 ? -1 : 1) * std::ldexp(1.0 + unit(), (int)(unit() * 1800) - 900);
+      if (!vh::crm::mk_num_ok(y) || !vh::crm::mk_den_ok(b)) continue;
+      used++;
+      if (vh::crm::mk_div(y, b, 1.0 / b) != y / b) bad++;
+    }
+    std::printf("%ld %ld\n", used, bad);
+    return 0;
+  }
+  do {
+    if (std::scanf("%la", &x) != 1) break;
     const double y = f[0] == 'e' ? vh::crm::exp_cr(x) : vh::crm::root4_cr(x);
     std::printf("%a\n", y);
-  }
+  } while (std::scanf("%1s", f) == 1);
   return 0;
 }
 """
@@ -42,6 +66,10 @@ def crm(tmp_path_factory):
                     os.path.dirname(HEADER), str(src), "-o", str(exe)], check=True)
 
     def run(kind, xs):
+        if kind == "m":
+            out = subprocess.run([str(exe)], input="m %d %d\n" % tuple(xs), capture_output=True,
+                                 text=True, check=True)
+            return [int(t) for t in out.stdout.split()]
         inp = "".join("%s %s\n" % (kind, float(x).hex()) for x in xs)
         out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True)
         return [float.fromhex(t) for t in out.stdout.split()]
@@ -87,3 +115,10 @@ def test_fourth_root_is_correctly_rounded(crm):
            if not correctly_rounded(y, decimal.Decimal(x).sqrt().sqrt())]
     assert not bad, bad[:5]
     assert crm("r", [0.0, float("inf")]) == [0.0, float("inf")]
+
+
+def test_markstein_division_equals_the_divide(crm):
+    """crm::mk_div(y, b, RN(1/b)) == y / b over 2e6 random pairs spanning its
+    whole range (|y| in [2^-900, 2^900], b in [2^-100, 2^100])."""
+    used, bad = crm("m", (2000000, 11))
+    assert used > 1900000 and bad == 0

@@ -160,6 +160,28 @@ VH_CRM double root4_cr(double x) {
   return b + bl;
 }
 
+// y / b correctly rounded, from r = RN(1/b), without a divide: the
+// quotient q0 = RN(y r) is faithful, the remainder y - b q0 is exact in an
+// fma, and RN(q0 + r (y - b q0)) = RN(y / b) (Markstein's theorem, IBM J.
+// Res. Dev. 34 (1990); Muller et al., Handbook of Floating-Point
+// Arithmetic, the Newton-Raphson division chapter).  It needs nothing to
+// underflow or overflow: mk_num_ok(y) (2^-900 <= |y| <= 2^900, or y = 0,
+// which is returned as is, as the zero-safe divisions return it) and
+// mk_den_ok(b) (2^-100 <= b <= 2^100).  Callers test a batch of numerators
+// once and divide the IEEE way otherwise, so that a batch of quotients is
+// free of branches (a divide is an instruction sequence with a branch to a
+// slow path, which keeps independent divides from overlapping).
+VH_CRM bool mk_num_ok(double y) {
+  const double a = fabs(y);
+  return (a >= 0x1p-900 && a <= 0x1p900) || y == 0.;
+}
+VH_CRM bool mk_den_ok(double b) { return b >= 0x1p-100 && b <= 0x1p100; }
+VH_CRM double mk_div(double y, double b, double r) {
+  const double q0 = y * r;
+  const double rem = fma(-q0, b, y);
+  return y == 0. ? y : fma(rem, r, q0);
+}
+
 }  // namespace crm
 }  // namespace vh
 

@@ -363,6 +363,23 @@ __device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N
 // latency better than fewer, spill-free ones (measured: 3 and 2 blocks per SM
 // are 7 % and 35 % slower, 5 and 6 are 9 % and 3 % slower).
 constexpr int kRelaxMinBlocks = 4;
+
+// n[j] <- ddivp(n[j], b) for j < K, r = RN(1/b): through crm::mk_div when
+// every numerator and b are in its range (bit-identical, no divide), else
+// with the divide.
+template <int K>
+__device__ __forceinline__ void div_batch(double* n, double b, double r, bool bfast) {
+  bool ok = bfast;
+#pragma unroll
+  for (int j = 0; j < K; j++) ok = ok && crm::mk_num_ok(n[j]);
+  if (ok) {
+#pragma unroll
+    for (int j = 0; j < K; j++) n[j] = crm::mk_div(n[j], b, r);
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; j++) n[j] = ddivp(n[j], b);
+  }
+}
 constexpr int kRelaxBlock = 128;
 // shared-memory rows of k_is_relax's relaxation loops: pi, sigma, u, h0, f0
 constexpr int kSmPI = 0, kSmSIG = 10, kSmU = 20, kSmH = 24, kSmF = 34, kSmRows = 44;
@@ -401,6 +418,10 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
 #define PI(a, b) cpi[index44(a, b)]
   const double vx = pA[5 * N + i], vy = pA[6 * N + i], vz = pA[7 * N + i];
   const double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
+  // the ~600 divisions by gamma go through crm::mk_div (bit-identical to
+  // the divide) in batches whose numerators are all in its range
+  const double rg = 1.0 / gamma;
+  const bool gfast = crm::mk_den_ok(gamma);
   double u[4];
   u[0] = gamma;
   u[1] = u[0] * vx;
@@ -516,11 +537,12 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
     dmu[3][0] += ddivp(uuu[3], tau - 0.5 * dt);
     dmu[3][3] += ddivp(uuu[0], tau - 0.5 * dt);
     const double gdiag[4] = {1., -1., -1., -1.};
+    const double r5068 = 1.0 / 5.068;
 #pragma unroll
     for (int a = 0; a < 4; a++)
 #pragma unroll
       for (int b = 0; b <= a; b++) {
-        double acc = 0.0;
+        double n[16];  // the (k, l) terms, divided by 5.068 as a batch
 #pragma unroll
         for (int k = 0; k < 4; k++)
 #pragma unroll
@@ -532,8 +554,12 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
             if (b == l) Z += 0.5 * (gak - uuu[a] * uuu[k]);
             if (a == l) Z += 0.5 * (gbk - uuu[b] * uuu[k]);
             if (k == l) Z -= ddivp(gab - uuu[a] * uuu[b], 3.0);
-            acc += ddivp(Z * dmu[k][l] * 2.0 * etaS * s, 5.068);
+            n[4 * k + l] = Z * dmu[k][l] * 2.0 * etaS * s;
           }
+        div_batch<16>(n, 5.068, r5068, true);
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 0; j < 16; j++) acc += n[j];
         piNS[index44(a, b)] = acc;
       }
     PiNS = ddivp(-zetaS * s * (dmu[0][0] + dmu[1][1] + dmu[2][2] + dmu[3][3]), 5.068);
@@ -572,11 +598,19 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
       const int k = index44(a, b);
       Delta[k] = -u[a] * u[b];
       if (a == b) Delta[k] += gmumu[a];
-      if (taupi > 0.5 * dt)
-        h0[k] = PI(a, b) - ddivp(ddivp((PI(a, b) - PINS(a, b)) * dt / 2.0, gamma), taupi);
-      else
-        h0[k] = PINS(a, b);
     }
+  if (taupi > 0.5 * dt) {
+    double n[10];
+#pragma unroll
+    for (int k = 0; k < 10; k++) n[k] = (cpi[k] - piNS[k]) * dt / 2.0;
+    div_batch<10>(n, gamma, rg, gfast);
+    div_batch<10>(n, taupi, 1.0 / taupi, crm::mk_den_ok(taupi));
+#pragma unroll
+    for (int k = 0; k < 10; k++) h0[k] = cpi[k] - n[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 10; k++) h0[k] = piNS[k];
+  }
   double H0;
   if (tauPi > 0.5 * dt)
     H0 = cPi - ddivp(ddivp((cPi - PiNS) * dt / 2.0, gamma), tauPi);
@@ -622,39 +656,48 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
       const double gk = gmumu[k];
       const double pak = sm[kSmPI + index44(a, k)][t], pbk = sm[kSmPI + index44(b, k)][t];
       const double sak = sm[kSmSIG + index44(a, k)][t], sbk = sm[kSmSIG + index44(b, k)][t];
-      acc += ddivp(phi7 * pak * pbk * gk - taupipi * 0.5 * (pak * sbk * gk + pbk * sak * gk),
-                   gamma) *
-             0.5 * dt;
+      double n[9];  // numerators of the k term and of its four (x, y) l terms
+      n[0] = phi7 * pak * pbk * gk - taupipi * 0.5 * (pak * sbk * gk + pbk * sak * gk);
 #pragma unroll
       for (int l = 0; l < 4; l++) {
-        acc += ddivp((-pak * ub - pbk * ua) * u[l] * dmu[l][k] * gk, gamma) * 0.5 * dt -
-               ddivp(1. / 3. * dab * PI(k, l) * (phi7 * PI(k, l) - taupipi * SIG(k, l)) * gk *
-                         gmumu[l],
-                     gamma) *
-                   0.5 * dt;
+        n[1 + 2 * l] = (-pak * ub - pbk * ua) * u[l] * dmu[l][k] * gk;
+        n[2 + 2 * l] =
+            1. / 3. * dab * PI(k, l) * (phi7 * PI(k, l) - taupipi * SIG(k, l)) * gk * gmumu[l];
       }
+      div_batch<9>(n, gamma, rg, gfast);
+      acc += n[0] * 0.5 * dt;
+#pragma unroll
+      for (int l = 0; l < 4; l++) acc += n[1 + 2 * l] * 0.5 * dt - n[2 + 2 * l] * 0.5 * dt;
     }
     sm[kSmH + ab][t] = acc;
   }
 #pragma unroll
   for (int k = 0; k < 10; k++) h0[k] = sm[kSmH + k][t];
+  {
+    double n[16];
 #pragma unroll
-  for (int k = 0; k < 4; k++)
+    for (int k = 0; k < 4; k++)
 #pragma unroll
-    for (int l = 0; l < 4; l++)
-      H0 += ddivp(lamPipi * PI(k, l) * SIG(k, l) * gmumu[k] * gmumu[l], gamma) * 0.5 * dt;
+      for (int l = 0; l < 4; l++) n[4 * k + l] = lamPipi * PI(k, l) * SIG(k, l) * gmumu[k] * gmumu[l];
+    div_batch<16>(n, gamma, rg, gfast);
+#pragma unroll
+    for (int j = 0; j < 16; j++) H0 += n[j] * 0.5 * dt;
+  }
   H0 += ddivp(-delPiPi * cPi * du, gamma) * 0.5 * dt;
 #define H(a, b) h0[index44(a, b)]
   double f0[10];
+  if (taupi > 0.5 * dt) {
+    double n[10];
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+    for (int k = 0; k < 10; k++) n[k] = (h0[k] - piNS[k]) * dt;
+    div_batch<10>(n, gamma, rg, gfast);
+    div_batch<10>(n, taupi, 1.0 / taupi, crm::mk_den_ok(taupi));
 #pragma unroll
-    for (int b = 0; b <= a; b++) {
-      if (taupi > 0.5 * dt)
-        f0[index44(a, b)] = PI(a, b) - ddivp(ddivp((H(a, b) - PINS(a, b)) * dt, gamma), taupi);
-      else
-        f0[index44(a, b)] = PINS(a, b);
-    }
+    for (int k = 0; k < 10; k++) f0[k] = cpi[k] - n[k];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 10; k++) f0[k] = piNS[k];
+  }
   double F0;
   if (tauPi > 0.5 * dt)
     F0 = cPi - ddivp(ddivp((H0 - PiNS) * dt, gamma), tauPi);
@@ -687,27 +730,31 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
       const double pak = sm[kSmPI + index44(a, k)][t];
       const double hak = sm[kSmH + index44(a, k)][t], hbk = sm[kSmH + index44(b, k)][t];
       const double sak = sm[kSmSIG + index44(a, k)][t], sbk = sm[kSmSIG + index44(b, k)][t];
-      acc += ddivp(phi7 * pak * hbk * gk - taupipi * 0.5 * (hak * sbk * gk + hbk * sak * gk),
-                   gamma) *
-             dt;
+      double n[5];  // numerators of the k term and of its four l terms
+      n[0] = phi7 * pak * hbk * gk - taupipi * 0.5 * (hak * sbk * gk + hbk * sak * gk);
 #pragma unroll
-      for (int l = 0; l < 4; l++) {
-        acc += ddivp((-hak * ub - hbk * ua) * u[l] * dmu[l][k] * gk -
-                         1. / 3. * dab * H(k, l) * (phi7 * H(k, l) - taupipi * SIG(k, l)) * gk *
-                             gmumu[l],
-                     gamma) *
-               dt;
-      }
+      for (int l = 0; l < 4; l++)
+        n[1 + l] = (-hak * ub - hbk * ua) * u[l] * dmu[l][k] * gk -
+                   1. / 3. * dab * H(k, l) * (phi7 * H(k, l) - taupipi * SIG(k, l)) * gk * gmumu[l];
+      div_batch<5>(n, gamma, rg, gfast);
+      acc += n[0] * dt;
+#pragma unroll
+      for (int l = 0; l < 4; l++) acc += n[1 + l] * dt;
     }
     sm[kSmF + ab][t] = acc;
   }
 #pragma unroll
   for (int k = 0; k < 10; k++) f0[k] = sm[kSmF + k][t];
+  {
+    double n[16];
 #pragma unroll
-  for (int k = 0; k < 4; k++)
+    for (int k = 0; k < 4; k++)
 #pragma unroll
-    for (int l = 0; l < 4; l++)
-      F0 += ddivp(lamPipi * H(k, l) * SIG(k, l) * gmumu[k] * gmumu[l], gamma) * dt;
+      for (int l = 0; l < 4; l++) n[4 * k + l] = lamPipi * H(k, l) * SIG(k, l) * gmumu[k] * gmumu[l];
+    div_batch<16>(n, gamma, rg, gfast);
+#pragma unroll
+    for (int j = 0; j < 16; j++) F0 += n[j] * dt;
+  }
   F0 += ddivp(-delPiPi * H0 * du, gamma) * dt;
 #pragma unroll
   for (int k = 0; k < 10; k++) {
