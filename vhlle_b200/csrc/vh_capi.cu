@@ -304,7 +304,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   if (eos->kind == VH_EOS_TABLE) {
     const int ne = eos->ne, nn = eos->nn;
     double* buf = nullptr;
-    ALLOC(buf, (size_t)ne + nn + 3 * (size_t)ne * nn);
+    ALLOC(buf, (size_t)ne + nn + 3 * (size_t)ne * nn + (size_t)(ne - 1) + (nn - 1));
     c->eos.ne = ne;
     c->eos.nn = nn;
     choose_axis_mode(eos->egrid, ne, &c->eos.emode, &c->eos.e0, &c->eos.einv);
@@ -322,6 +322,30 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
         (e = cudaMemcpy((void*)c->eos.mub, eos->mub, tb, cudaMemcpyHostToDevice))) {
       cuda_fail(c, e, "vh_create: EoS upload");
       return bail(VH_ERR_CUDA);
+    }
+    // reciprocals of the axis intervals for the interpolation weights
+    // (vh::interp_weight); an axis with an interval out of crm::mk_div's
+    // range keeps the divide
+    double* rdev = buf + ne + nn + 3 * (size_t)ne * nn;
+    const double* axes[2] = {eos->egrid, eos->ngrid};
+    const int lens[2] = {ne, nn};
+    c->eos.erinv = c->eos.nrinv = nullptr;
+    for (int a = 0; a < 2; a++) {
+      std::vector<double> r((size_t)lens[a] - 1);
+      bool ok = true;
+      for (int k = 0; k + 1 < lens[a]; k++) {
+        const double den = axes[a][k + 1] - axes[a][k];
+        ok = ok && vh::crm::mk_den_ok(den);
+        r[k] = 1.0 / den;
+      }
+      if (ok) {
+        if ((e = cudaMemcpy(rdev, r.data(), r.size() * sizeof(double), cudaMemcpyHostToDevice))) {
+          cuda_fail(c, e, "vh_create: EoS upload");
+          return bail(VH_ERR_CUDA);
+        }
+        (a == 0 ? c->eos.erinv : c->eos.nrinv) = rdev;
+      }
+      rdev += r.size();
     }
   }
 #undef ALLOC

@@ -162,6 +162,7 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.eos.mub = eos_dev->mub;
   a.eos.emode = a.eos.nmode = vh::GRID_BSEARCH;  // the table stays on the device
   a.eos.e0 = a.eos.einv = a.eos.n0 = a.eos.ninv = 0.f;
+  a.eos.erinv = a.eos.nrinv = nullptr;  // interpolation weights by division
   a.eos.tol = 0.00001;  // src/rmn.cpp:96
   a.eos.vguess = nullptr;
   a.eos.stats = nullptr;

@@ -41,6 +41,10 @@ struct EosDev {
   int emode, nmode;    // GRID_* per axis
   float e0, einv;      // guess: (f(x) - e0) * einv, f = log2 or identity
   float n0, ninv;
+  // RN(1 / (g[k+1] - g[k])) per interval of each axis, or null: the
+  // interpolation weights then take crm::mk_div instead of a divide
+  const double* __restrict__ erinv;
+  const double* __restrict__ nrinv;
   // con2prim policy (not part of the EoS proper, but passed everywhere with
   // it): stop when |dv| < tol (the reference's 0.00001 by default); vguess,
   // when set, holds a start point in (0, 1) per cell for the root find; stats,
@@ -161,6 +165,17 @@ __device__ __forceinline__ void bracket_guess(const double* __restrict__ g, int 
   k2 = k + 1;
 }
 
+// (x - g[k1]) / (g[k2] - g[k1]), k2 = k1 + 1: with the interval's
+// reciprocal rinv[k1] (computed on the host by the same subtraction and a
+// divide) through crm::mk_div, bit-identical to the divide, when x - g[k1]
+// is in its range; otherwise divided.
+__device__ __forceinline__ double interp_weight(double x, const double* __restrict__ g,
+                                                const double* __restrict__ rinv, int k1, int k2) {
+  const double num = x - __ldg(g + k1), den = __ldg(g + k2) - __ldg(g + k1);
+  if (rinv && crm::mk_num_ok(num)) return crm::mk_div(num, den, __ldg(rinv + k1));
+  return ddiv(num, den);
+}
+
 // EoS1f::eos, src/eo1.cpp:100-123
 template <bool WANT_T>
 __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
@@ -169,12 +184,12 @@ __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
   bracket_guess(E.egrid, E.ne, e, E.emode, E.e0, E.einv, k1, k2);
   int ixe = k1;
   if (ixe > E.ne - 2) ixe = E.ne - 2;
-  const double ue = ddiv(e - __ldg(E.egrid + k1), __ldg(E.egrid + k2) - __ldg(E.egrid + k1));
+  const double ue = interp_weight(e, E.egrid, E.erinv, k1, k2);
   bracket_guess(E.ngrid, E.nn, nb, E.nmode, E.n0, E.ninv, k1, k2);
   int ixn = k1;
   if (ixn > E.nn - 2) ixn = E.nn - 2;
   if (ixn < 0) ixn = 0;
-  const double un = ddiv(nb - __ldg(E.ngrid + k1), __ldg(E.ngrid + k2) - __ldg(E.ngrid + k1));
+  const double un = interp_weight(nb, E.ngrid, E.nrinv, k1, k2);
   const double we0 = 1. - ue, we1 = ue;
   const double wn0 = 1. - un, wn1 = un;
   const int b00 = ixe + E.ne * ixn, b01 = ixe + E.ne * (ixn + 1);
@@ -314,9 +329,21 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     atomicAdd(&E.stats[0], 1ull);
     atomicAdd(&E.stats[1], (unsigned long long)it);
   }
-  o.vx = ddivp(v * Q[X_], M);
-  o.vy = ddivp(v * Q[Y_], M);
-  o.vz = ddivp(v * Q[Z_], M);
+  {
+    // v Q_i / M, i = x, y, z: one divide for RN(1/M) and crm::mk_div
+    // (bit-identical) when all three are in its range
+    const double nx = v * Q[X_], ny = v * Q[Y_], nz = v * Q[Z_];
+    if (crm::mk_den_ok(M) && crm::mk_num_ok(nx) && crm::mk_num_ok(ny) && crm::mk_num_ok(nz)) {
+      const double rM = 1.0 / M;
+      o.vx = crm::mk_div(nx, M, rM);
+      o.vy = crm::mk_div(ny, M, rM);
+      o.vz = crm::mk_div(nz, M, rM);
+    } else {
+      o.vx = ddivp(nx, M);
+      o.vy = ddivp(ny, M);
+      o.vz = ddivp(nz, M);
+    }
+  }
   o.e = Q[T_] - M * v;
   o.p = eos_p(E, o.e, nb);  // the last iterate's nb, as the reference
   const double sq = sqrt(1 - o.vx * o.vx - o.vy * o.vy - o.vz * o.vz);
