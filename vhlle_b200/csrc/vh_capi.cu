@@ -275,6 +275,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     ALLOC(f.piH0, 10 * N);
     ALLOC(f.Pi0, N);
     ALLOC(f.PiH0, N);
+    ALLOC(f.active, N);
+    ALLOC(f.nactive, 1);
   }
   ALLOC(c->clk, 2);
   ALLOC(c->tot_partial, (size_t)vh::totals_blocks(g) * vh::kTotals);

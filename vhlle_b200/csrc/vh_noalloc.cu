@@ -31,8 +31,9 @@ namespace {
 
 constexpr long long kMaxCells = VH_NOALLOC_MAX_CELLS;
 constexpr int kMaxDim = VH_NOALLOC_MAX_DIM;
-constexpr long long kDoublesPerCell = 80;  // m2 3, Fx/Fy/Fz 21, flux 4, pA 8, pD 4,
-                                           // pTh 9, pBC 9, pi0/piH0 20, Pi0/PiH0 2
+constexpr long long kDoublesPerCell = 81;  // m2 3, Fx/Fy/Fz 21, flux 4, pA 8, pD 4,
+                                           // pTh 9, pBC 9, pi0/piH0 20, Pi0/PiH0 2,
+                                           // the active-cell list (ints) 1
 constexpr size_t kHeaderBytes = 256 + 3 * kMaxDim * sizeof(int) + 3 * kMaxDim;  // err, maps
 constexpr size_t kHeaderAligned = (kHeaderBytes + 255) / 256 * 256;
 constexpr size_t kScratchBytes = kHeaderAligned + (size_t)kDoublesPerCell * kMaxCells * sizeof(double);
@@ -173,9 +174,11 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
                    tr->zetaSWidthT};
   a.viscous = tr->etaS0 > 0. || tr->zetaS0 > 0. || tr->etaSparam > 0 || tr->zetaSparam > 0;
 
-  // scratch layout: [err, clock | ghost src maps | ghost dst flags | pad][doubles...]
+  // scratch layout: [err, clock, active count | ghost src maps | ghost dst
+  // flags | pad][doubles...]
   vh::Fields& f = a.f;
   f.err = reinterpret_cast<unsigned*>(base);
+  f.nactive = reinterpret_cast<int*>(base + 32);
   double* clk = reinterpret_cast<double*>(base + 16);
   a.clk = clk;
   f.gsrc = reinterpret_cast<int*>(base + 256);
@@ -206,6 +209,8 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   f.Pi0 = d;
   d += N;
   f.PiH0 = d;
+  d += N;
+  f.active = reinterpret_cast<int*>(d);
   f.Q = s->Q;
   f.Qh = s->Qh;
   f.Qprev = s->Qprev;

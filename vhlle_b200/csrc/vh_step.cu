@@ -384,19 +384,30 @@ constexpr int kRelaxBlock = 128;
 // shared-memory rows of k_is_relax's relaxation loops: pi, sigma, u, h0, f0
 constexpr int kSmPI = 0, kSmSIG = 10, kSmU = 20, kSmH = 24, kSmF = 34, kSmRows = 44;
 
-__global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
-    Geo g, EosDev E, TrDev tr, const double* __restrict__ Q, const double* __restrict__ Qprev,
-    const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
-    const double* __restrict__ pTh, const double* __restrict__ pBC,
-    const double* __restrict__ pi, const double* __restrict__ Pi, double* __restrict__ pi0,
-    double* __restrict__ piH0, double* __restrict__ Pi0, double* __restrict__ PiH0,
-    double* __restrict__ flux, const double* __restrict__ clk, unsigned* err) {
-  const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
+// The empty cells' share of ISformal loop 1 (src/hdo.cpp:697-708: zero
+// pi0/piH0/Pi0/PiH0) and the list of the other cells, so that k_is_relax
+// runs full warps: cells with matter are packed in warp order (one atomic
+// per warp; the list's order between warps varies, and every cell's result
+// depends on that cell alone).  *nactive is zero on entry.
+__global__ void __launch_bounds__(128) k_relax_list(Geo g, const double* __restrict__ pA,
+                                                    int* __restrict__ active,
+                                                    int* __restrict__ nactive,
+                                                    double* __restrict__ pi0,
+                                                    double* __restrict__ piH0,
+                                                    double* __restrict__ Pi0,
+                                                    double* __restrict__ PiH0,
+                                                    double* __restrict__ flux) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.N) return;
   const long long N = g.N;
-  const double e = pA[i];
-  if (e <= 0.) {
+  const bool in = i < N;
+  const bool act = in && !(pA[i] <= 0.);
+  const int lane = threadIdx.x & 31;
+  const unsigned bal = __ballot_sync(0xffffffffu, act);
+  int base = 0;
+  if (lane == 0 && bal) base = atomicAdd(nactive, __popc(bal));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (act) active[base + __popc(bal & ((1u << lane) - 1u))] = (int)i;
+  if (in && !act) {
 #pragma unroll
     for (int k = 0; k < 10; k++) {
       piH0[k * N + i] = 0.0;
@@ -406,8 +417,23 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
     Pi0[i] = 0.0;
 #pragma unroll
     for (int k = 0; k < 4; k++) flux[k * N + i] = 0.;
-    return;
   }
+}
+
+__global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
+    Geo g, EosDev E, TrDev tr, const double* __restrict__ Q, const double* __restrict__ Qprev,
+    const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
+    const double* __restrict__ pTh, const double* __restrict__ pBC,
+    const double* __restrict__ pi, const double* __restrict__ Pi, double* __restrict__ pi0,
+    double* __restrict__ piH0, double* __restrict__ Pi0, double* __restrict__ PiH0,
+    double* __restrict__ flux, const double* __restrict__ clk, unsigned* err,
+    const int* __restrict__ active, const int* __restrict__ nactive) {
+  const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= *nactive) return;
+  const long long i = active[idx];  // a cell with matter (k_relax_list)
+  const long long N = g.N;
+  const double e = pA[i];
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
   const double gmumu[4] = {1., -1., -1., -1.};
@@ -1055,8 +1081,15 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
     k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
                                    F.pBC, a.clk);
     done(KK_VISC_PRIMS);
-    k_is_relax<<<nb128, kRelaxBlock, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh, F.pBC, F.pi,
-                                 F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0, F.flux, a.clk, F.err);
+    // the relaxation on full warps of cells with matter (the list kernel's
+    // time is counted with the relaxation's)
+    cudaMemsetAsync(F.nactive, 0, sizeof(int), s);
+    k_relax_list<<<nb128, 128, 0, s>>>(g, F.pA, F.active, F.nactive, F.pi0, F.piH0, F.Pi0,
+                                       F.PiH0, F.flux);
+    launches++;
+    k_is_relax<<<nb128, kRelaxBlock, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh,
+                                             F.pBC, F.pi, F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0,
+                                             F.flux, a.clk, F.err, F.active, F.nactive);
     done(KK_IS_RELAX);
     k_is_advect<<<nb, bs, 0, s>>>(g, F.pA, F.pi0, F.piH0, F.Pi0, F.PiH0, F.pi, F.piH, F.Pi, F.PiH,
                                   F.vcc, F.flux, a.clk);

@@ -50,6 +50,8 @@ struct Fields {
   double *pBC;                   // [9][N] four-velocities for NSquant's d/dtau
   double *pi0, *piH0;            // [10][N] IS relaxation results
   double *Pi0, *PiH0;            // [N]
+  int *active, *nactive;         // [N] cells with matter (e > 0) for the
+                                 // relaxation, and their count ([1])
   int *gsrc;                     // [nx+ny+nz] ghost-cell source map
   unsigned char *gdst;           // [nx+ny+nz] ghost-cell destination flags
   unsigned *err;                 // device error word
