@@ -141,58 +141,71 @@ __device__ __forceinline__ void bsearch_grid(const double* __restrict__ g, int n
 }
 
 // The bracket the binary search above returns, found from an index guess.
-// For a strictly increasing axis g[0..n-1] the search yields the unique k in
-// [0, n-2] with (k == 0 or g[k] <= x) and (k == n-2 or x < g[k+1]) (and
-// n-2 for NaN); the two walks below stop exactly there, from any start, so
-// the guess only decides how many steps they take (usually none or one).
-__device__ __forceinline__ void bracket_guess(const double* __restrict__ g, int n, double x,
-                                              int mode, float x0, float inv, int& k1, int& k2) {
-  if (mode == GRID_BSEARCH || n <= 2) {
-    bsearch_grid(g, n, x, k1, k2);
-    return;
-  }
-  int k;
-  if (x != x) {
-    k = n - 2;
-  } else {
-    const float fx = (float)x;
-    const float t = (mode == GRID_LOG ? __log2f(fx) - x0 : fx - x0) * inv;
-    k = !(t > 0.f) ? 0 : (t >= (float)(n - 2) ? n - 2 : (int)t);
-    while (k > 0 && x < __ldg(g + k)) k--;
-    while (k < n - 2 && !(x < __ldg(g + k + 1))) k++;
-  }
-  k1 = k;
-  k2 = k + 1;
-}
-
-// (x - g[k1]) / (g[k2] - g[k1]), k2 = k1 + 1: with the interval's
-// reciprocal rinv[k1] (computed on the host by the same subtraction and a
-// divide) through crm::mk_div, bit-identical to the divide, when x - g[k1]
-// is in its range; otherwise divided.
-__device__ __forceinline__ double interp_weight(double x, const double* __restrict__ g,
-                                                const double* __restrict__ rinv, int k1, int k2) {
-  const double num = x - __ldg(g + k1), den = __ldg(g + k2) - __ldg(g + k1);
-  if (rinv && crm::mk_num_ok(num)) return crm::mk_div(num, den, __ldg(rinv + k1));
+// (x - g0) / (g1 - g0) for the bracket [g0, g1] of an axis: with the
+// interval's reciprocal r (computed on the host by the same subtraction and
+// a divide; has_r false without a table) through crm::mk_div,
+// bit-identical to the divide, when x - g0 is in its range; else divided.
+__device__ __forceinline__ double interp_weight(double x, double g0, double g1, bool has_r,
+                                                double r) {
+  const double num = x - g0, den = g1 - g0;
+  if (has_r && crm::mk_num_ok(num)) return crm::mk_div(num, den, r);
   return ddiv(num, den);
 }
 
-// EoS1f::eos, src/eo1.cpp:100-123
+// The float guess of a GRID_LOG / GRID_LIN axis position, in [0, n-2].
+__device__ __forceinline__ int axis_guess(int n, double x, int mode, float x0, float inv) {
+  if (x != x) return n - 2;
+  const float fx = (float)x;
+  const float t = (mode == GRID_LOG ? __log2f(fx) - x0 : fx - x0) * inv;
+  return !(t > 0.f) ? 0 : (t >= (float)(n - 2) ? n - 2 : (int)t);
+}
+
+// k is bsearch_grid's bracket of x when (k == 0 or g[k] <= x) and
+// (k == n-2 or x < g[k+1]) (NaN: k == n-2).
+__device__ __forceinline__ bool is_bracket(int k, int n, double x, double gk, double gk1) {
+  return (k == 0 || !(x < gk)) && (k == n - 2 || x < gk1);
+}
+
+// EoS1f::eos, src/eo1.cpp:100-123.  Both axes' brackets are guessed
+// without loads (or searched, for an axis without a guess), and the bracket
+// ends, the interval reciprocals and the four table corners are loaded
+// together for the guess; a wrong guess (a step or two off, rare) walks to
+// the bracket that the binary search finds and loads again.
 template <bool WANT_T>
 __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
                                       double& T, double& mub, double& p) {
-  int k1, k2;
-  bracket_guess(E.egrid, E.ne, e, E.emode, E.e0, E.einv, k1, k2);
-  int ixe = k1;
-  if (ixe > E.ne - 2) ixe = E.ne - 2;
-  const double ue = interp_weight(e, E.egrid, E.erinv, k1, k2);
-  bracket_guess(E.ngrid, E.nn, nb, E.nmode, E.n0, E.ninv, k1, k2);
-  int ixn = k1;
-  if (ixn > E.nn - 2) ixn = E.nn - 2;
-  if (ixn < 0) ixn = 0;
-  const double un = interp_weight(nb, E.ngrid, E.nrinv, k1, k2);
+  const int ne = E.ne, nn = E.nn;
+  int ke, kn, k2;
+  if (E.emode == GRID_BSEARCH || ne <= 2)
+    bsearch_grid(E.egrid, ne, e, ke, k2);
+  else
+    ke = axis_guess(ne, e, E.emode, E.e0, E.einv);
+  if (nn <= 2)
+    kn = 0;
+  else if (E.nmode == GRID_BSEARCH)
+    bsearch_grid(E.ngrid, nn, nb, kn, k2);
+  else
+    kn = axis_guess(nn, nb, E.nmode, E.n0, E.ninv);
+  double ge0 = __ldg(E.egrid + ke), ge1 = __ldg(E.egrid + ke + 1);
+  double gn0 = __ldg(E.ngrid + kn), gn1 = __ldg(E.ngrid + kn + 1);
+  double re = E.erinv ? __ldg(E.erinv + ke) : 0., rn = E.nrinv ? __ldg(E.nrinv + kn) : 0.;
+  if (!is_bracket(ke, ne, e, ge0, ge1) || !is_bracket(kn, nn, nb, gn0, gn1)) {
+    while (ke > 0 && e < __ldg(E.egrid + ke)) ke--;
+    while (ke < ne - 2 && !(e < __ldg(E.egrid + ke + 1))) ke++;
+    while (kn > 0 && nb < __ldg(E.ngrid + kn)) kn--;
+    while (kn < nn - 2 && !(nb < __ldg(E.ngrid + kn + 1))) kn++;
+    ge0 = __ldg(E.egrid + ke);
+    ge1 = __ldg(E.egrid + ke + 1);
+    gn0 = __ldg(E.ngrid + kn);
+    gn1 = __ldg(E.ngrid + kn + 1);
+    re = E.erinv ? __ldg(E.erinv + ke) : 0.;
+    rn = E.nrinv ? __ldg(E.nrinv + kn) : 0.;
+  }
+  const int b00 = ke + ne * kn, b01 = ke + ne * (kn + 1);
+  const double ue = interp_weight(e, ge0, ge1, E.erinv != nullptr, re);
+  const double un = interp_weight(nb, gn0, gn1, E.nrinv != nullptr, rn);
   const double we0 = 1. - ue, we1 = ue;
   const double wn0 = 1. - un, wn1 = un;
-  const int b00 = ixe + E.ne * ixn, b01 = ixe + E.ne * (ixn + 1);
   double sp = 0.;
   sp += we0 * wn0 * __ldg(E.p + b00);
   sp += we0 * wn1 * __ldg(E.p + b01);

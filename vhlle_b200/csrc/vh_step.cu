@@ -813,15 +813,19 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
                                                    double* __restrict__ pi, double* __restrict__ piH,
                                                    double* __restrict__ Pi, double* __restrict__ PiH,
                                                    double* __restrict__ vcc,
-                                                   double* __restrict__ flux, const double* __restrict__ clk) {
+                                                   double* __restrict__ flux, const double* __restrict__ clk,
+                                                   const int* __restrict__ active,
+                                                   const int* __restrict__ nactive) {
   const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= g.N) return;
+  // the cells with matter only (k_relax_list); the empty ones are left as
+  // they are, as the reference's loop 2 leaves them (e <= 0)
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= *nactive) return;
+  const long long i = active[idx];
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
   const long long N = g.N;
   const Prim A = loadA(pA, N, i);
-  if (A.e <= 0.) return;
   const double e = A.e, p = A.p, vx = A.vx, vy = A.vy, vz = A.vz;
   const double xm = ddivp(-vx * dt, g.dx);
   const double ym = ddivp(-vy * dt, g.dy);
@@ -1092,7 +1096,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
                                              F.flux, a.clk, F.err, F.active, F.nactive);
     done(KK_IS_RELAX);
     k_is_advect<<<nb, bs, 0, s>>>(g, F.pA, F.pi0, F.piH0, F.Pi0, F.PiH0, F.pi, F.piH, F.Pi, F.PiH,
-                                  F.vcc, F.flux, a.clk);
+                                  F.vcc, F.flux, a.clk, F.active, F.nactive);
     done(KK_IS_ADVECT);
     k_visc_update<<<nb, bs, 0, s>>>(g, F.pA, F.piH, F.PiH, m, F.flux, F.Q, a.clk);
     done(KK_VISC_UPDATE);
