@@ -402,24 +402,24 @@ def main():
     sampler = ClockSampler(gpu_index_for(local))
     time.sleep(0.3)
     dist.barrier()
-    h.profile(True)
     h.timer_start()
     nel = 0
     for k in range(1, args.steps + 1):
-        h.step(1)
+        h.step(1)  # one captured graph per step (vh_step)
         if k % SURF_EVERY == 0:
             nel += h.surface_only()["nelements"]
     ms = h.timer_stop()
     dist.barrier()
     clocks = sampler.stop()
     h.sync()
-    prof = h.profile_read()
-    h.profile(False)
-    # the surface calls' own share: the same loop again with a CUDA-event
-    # pair around every surface call (vh_surface waits for its result, so
-    # the pair spans the call's kernels and its host round trips)
+    # the kernels' and the surface calls' own times: the same loop again,
+    # the step's kernels launched one by one with CUDA events between them
+    # (vh_profile) and a CUDA-event pair around every surface call
+    # (vh_surface waits for its result, so the pair spans the call's kernels
+    # and its host round trip)
     h.upload_initial()
     h.L.vh_set_tau(h.h, setup.tau0)
+    h.profile(True)
     surf_ms_tot = 0.0
     for k in range(1, args.steps + 1):
         h.step(1)
@@ -427,6 +427,9 @@ def main():
             h.timer_start()
             h.surface_only()
             surf_ms_tot += h.timer_stop()
+    h.sync()
+    prof = h.profile_read()
+    h.profile(False)
     ms_max = dist.max(ms)
     value = ws * cells * args.steps / (ms_max / 1e3)
 

@@ -257,3 +257,24 @@ def test_gubser_against_analytic_solution():
         assert np.abs(e[inner] / ea[inner] - 1).max() < 0.08, tau
         assert np.abs(vr[inner] - va[inner]).max() < 0.015, tau
     h.close()
+
+
+def test_graph_replay_equals_direct_launches():
+    """vh_step replays a captured graph per step; with per-kernel profiling
+    on it launches the kernels one by one.  Both give the same bits, also
+    across a change that makes the graph be captured again (the con2prim
+    tolerance) and across both fill-fraction buffer orders."""
+    s = W.small_glauber3d(41, 21)
+    g, d = capi.GpuHydro(s), capi.GpuHydro(s)
+    d.profile(True)
+    for n in (3, 4):
+        g.step(n)
+        d.step(n)
+        g.sync()
+        d.sync()
+        assert not compare_states(g.get_state(), d.get_state())
+        g.set_con2prim(1e-9)
+        d.set_con2prim(1e-9)
+    d.profile(False)
+    g.close()
+    d.close()

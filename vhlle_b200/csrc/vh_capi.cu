@@ -176,6 +176,9 @@ vh_status vh_destroy(vh_ctx* ctx) {
   if (!ctx) return VH_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  for (cudaGraphExec_t& x : ctx->step_exec)
+    if (x) cudaGraphExecDestroy(x);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->surf.host) cudaFreeHost(ctx->surf.host);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
@@ -262,6 +265,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   ALLOC(f.vcc, N);
   ALLOC(f.m, 3 * N);
   ALLOC(f.m2, 3 * N);
+  c->m_first = f.m;
   ALLOC(f.Fx, 7 * N);
   ALLOC(f.Fy, 7 * N);
   ALLOC(f.Fz, 7 * N);
@@ -437,22 +441,72 @@ vh_status vh_device_state(vh_ctx* ctx, vh_state_view* d) {
   return VH_OK;
 }
 
-vh_status vh_step(vh_ctx* ctx) {
-  if (!ctx) return VH_ERR_ARG;
-  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_step: no state uploaded");
-  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+static vh::StepArgs step_args(vh_ctx* ctx) {
   vh::StepArgs a;
   a.g = ctx->g;
   a.eos = ctx->eos;
-  a.eos.vguess = nullptr;
-  if (ctx->mlp) {  // start points for this step's root finds from Q at tau
-    vh::launch_mlp_guess(ctx->mlp->packed, ctx->f.Q, ctx->g.N, ctx->clk, ctx->vguess, ctx->stream);
-    a.eos.vguess = ctx->vguess;
-  }
+  a.eos.vguess = ctx->mlp ? ctx->vguess : nullptr;
   a.tr = ctx->tr;
   a.f = ctx->f;
   a.clk = ctx->clk;  // holds (tau, dt): set when the host changes them, advanced per step
   a.viscous = ctx->viscous;
+  return a;
+}
+
+// One step (the learned guess, performStep, tau += dt on the device clock)
+// captured into ctx->step_exec[par]; false if the capture is refused.
+static bool capture_step(vh_ctx* ctx, int par) {
+  if (!ctx->cap_stream &&
+      cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (ctx->step_exec[par]) {
+    cudaGraphExecDestroy(ctx->step_exec[par]);
+    ctx->step_exec[par] = nullptr;
+  }
+  const vh::StepArgs a = step_args(ctx);
+  cudaStream_t s = ctx->cap_stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (ctx->mlp) vh::launch_mlp_guess(ctx->mlp->packed, ctx->f.Q, ctx->g.N, ctx->clk, ctx->vguess, s);
+  const int n = vh::launch_step(a, s);
+  vh::launch_clock_op(ctx->clk, 0, 0, s);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &graph);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->step_exec[par], graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->step_exec[par] = nullptr;
+    return false;
+  }
+  ctx->step_version[par] = ctx->version;
+  ctx->step_launches[par] = n;
+  return true;
+}
+
+vh_status vh_step(vh_ctx* ctx) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_step: no state uploaded");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (!ctx->prof && ctx->step_graphs) {
+    const int par = ctx->f.m == ctx->m_first ? 0 : 1;
+    if ((ctx->step_exec[par] && ctx->step_version[par] == ctx->version) ||
+        capture_step(ctx, par)) {
+      VH_CUDA(ctx, cudaGraphLaunch(ctx->step_exec[par], ctx->stream));
+      ctx->launches = ctx->step_launches[par];
+      std::swap(ctx->f.m, ctx->f.m2);
+      ctx->tau += ctx->dt;  // src/hdo.cpp:1095
+      return VH_OK;
+    }
+    ctx->step_graphs = false;  // launch directly from now on
+  }
+  const vh::StepArgs a = step_args(ctx);
+  if (ctx->mlp)  // start points for this step's root finds from Q at tau
+    vh::launch_mlp_guess(ctx->mlp->packed, ctx->f.Q, ctx->g.N, ctx->clk, ctx->vguess, ctx->stream);
   if (ctx->prof) {
     EventMarker mk(ctx, 0);
     mk.after(-1);  // start event of this step

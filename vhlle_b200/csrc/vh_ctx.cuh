@@ -29,6 +29,17 @@ struct vh_ctx {
   double* clk = nullptr;          // [2] device clock (tau, dt) the step kernels read
   unsigned long long* c2p_stats = nullptr;  // [2] con2prim calls, iterations
   int version = 0;  // bumped by every change a captured step bakes in
+  // vh_step replays one captured step per fill-fraction buffer order
+  // (f.m == m_first or not) while `version` is unchanged: one graph launch
+  // per step instead of ~20 kernel launches (captured on a private stream,
+  // launched on `stream`); steps with per-kernel profiling launch directly
+  cudaStream_t cap_stream = nullptr;
+  cudaGraphExec_t step_exec[2] = {nullptr, nullptr};
+  int step_version[2] = {-1, -1};
+  int step_launches[2] = {0, 0};
+  bool step_graphs = true;  // false after a capture was refused (e.g. inside
+                            // a caller's own global-mode capture)
+  double* m_first = nullptr;
   vh_mlp* mlp = nullptr;           // learned con2prim start point (not owned)
   float* vguess = nullptr;         // [N] per-cell start points of the step
   unsigned long long* ucount = nullptr;
