@@ -118,7 +118,11 @@ vh_status vh_download_async(vh_ctx *ctx, const vh_state_view *host);
 vh_status vh_device_state(vh_ctx *ctx, vh_state_view *dev);
 
 /* Hydro::performStep (src/hdo.cpp:1016-1134): one timestep of the whole
- * grid; tau advances by dt.  Asynchronous. */
+ * grid; tau advances by dt.  Asynchronous.  The step is captured once
+ * (per fill-fraction buffer order, and again after a call that changes
+ * what it bakes in) on a private stream and replayed as one CUDA graph
+ * launch on the context's stream; with per-kernel profiling on, or if the
+ * capture is refused, the kernels are launched one by one. */
 vh_status vh_step(vh_ctx *ctx);
 /* n successive performStep calls. */
 vh_status vh_steps(vh_ctx *ctx, int n);
