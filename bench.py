@@ -494,10 +494,13 @@ def main():
         for p, _ in bufs.values():
             L.vh_free_pinned(p)
         L.vh_free_pinned(rec_p)
+        link = (2 * nbytes + rec_bytes / nE) * nE / (ems / 1e3) / 1e9
         e2e = {"value": ws * cells * nE / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
                "d2h_bytes_per_step": nbytes + rec_bytes // nE, "steps": nE,
-               "note": "state uploaded and downloaded every step, surface records every %d"
-                       % SURF_EVERY}
+               "host_link_gbs": link,
+               "note": "state uploaded and downloaded every step, surface records every %d; "
+                       "host_link_gbs: both directions' bytes over the whole time (copies and "
+                       "kernels serialised by the step's data dependence)" % SURF_EVERY}
 
     batch = batch2d = None
     if args.batch_events > 0:
