@@ -129,7 +129,8 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
                                                 double* __restrict__ Qprev,
                                                 const double* __restrict__ Fx,
                                                 const double* __restrict__ Fy,
-                                                const double* __restrict__ Fz, const double* __restrict__ clk, unsigned* err) {
+                                                const double* __restrict__ Fz, const double* __restrict__ clk, unsigned* err,
+                                                double* __restrict__ pB) {
   const double tau = clk[0], dt = clk[1];  // the step's clock (device)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
@@ -160,6 +161,17 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
   }
   Prim pp;
   transform_pv(E, q, pp, c2p_guess(E, i));
+  if (PRED && pB) {
+    // con2prim(Q_n / tau_n) is the viscous stage's B = con2prim(Qprev /
+    // (tau_{n+1} - dt)) whenever (tau_n + dt) - dt == tau_n: kept for it
+    // as its four-velocity and e (the same arithmetic as k_visc_prims)
+    const double ut = 1.0 / sqrt(1.0 - pp.vx * pp.vx - pp.vy * pp.vy - pp.vz * pp.vz);
+    pB[0 * N + i] = ut;
+    pB[1 * N + i] = ut * pp.vx;
+    pB[2 * N + i] = ut * pp.vy;
+    pB[3 * N + i] = ut * pp.vz;
+    pB[4 * N + i] = pp.e;
+  }
   double kk[7];
   kk[T_] = -q[T_] * pp.vz * pp.vz - pp.p * (1. + pp.vz * pp.vz);
   kk[X_] = 0.;
@@ -316,8 +328,11 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
                    maxM_at(g, m, ix - 1, iy + 1, iz) <= 0.9 ||
                    maxM_at(g, m, ix - 1, iy - 1, iz) <= 0.9;
   if (vac) return;
+  // B is the predictor's con2prim when the divisors agree bit for bit
+  // (k_update<true> stored it in pBC); otherwise computed here
+  const bool haveB = (clk[0] + dt) - dt == clk[0];
 #pragma unroll 1
-  for (int w = 0; w < 2; w++) {
+  for (int w = haveB ? 1 : 0; w < 2; w++) {
     const double* src = w == 0 ? Qprev : Q;
     const double tt = w == 0 ? tau - dt : tau;
 #pragma unroll
@@ -1064,7 +1079,8 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
         k_face<Z_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
         done(KK_FACE_Z);
       }
-      k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err);
+      k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
+                                       a.viscous ? F.pBC : nullptr);
       done(KK_UPDATE);
     } else {
       k_face<X_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
@@ -1075,7 +1091,8 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
         k_face<Z_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
         done(KK_FACE_Z);
       }
-      k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err);
+      k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
+                                        nullptr);
       done(KK_UPDATE);
     }
   }
