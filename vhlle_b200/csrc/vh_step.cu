@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
                                                 const double* __restrict__ Fx,
                                                 const double* __restrict__ Fy,
                                                 const double* __restrict__ Fz, const double* __restrict__ clk, unsigned* err,
-                                                double* __restrict__ pB) {
+                                                double* __restrict__ pB, double* __restrict__ pA) {
   const double tau = clk[0], dt = clk[1];  // the step's clock (device)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
@@ -161,6 +161,19 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
   }
   Prim pp;
   transform_pv(E, q, pp, c2p_guess(E, i));
+  if (!PRED && pA) {
+    // con2prim(Qh / (tau_n + dt/2)) is the viscous stage's A =
+    // con2prim(Qh / (tau_{n+1} - dt/2)) for every cell that the ghost copy
+    // does not overwrite, whenever the divisors agree bit for bit
+    pA[0 * N + i] = pp.e;
+    pA[1 * N + i] = pp.p;
+    pA[2 * N + i] = pp.nb;
+    pA[3 * N + i] = pp.nq;
+    pA[4 * N + i] = pp.ns;
+    pA[5 * N + i] = pp.vx;
+    pA[6 * N + i] = pp.vy;
+    pA[7 * N + i] = pp.vz;
+  }
   if (PRED && pB) {
     // con2prim(Q_n / tau_n) is the viscous stage's B = con2prim(Qprev /
     // (tau_{n+1} - dt)) whenever (tau_n + dt) - dt == tau_n: kept for it
@@ -271,7 +284,8 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
                                                     double* __restrict__ pA,
                                                     double* __restrict__ pD,
                                                     double* __restrict__ pTh,
-                                                    double* __restrict__ pBC, const double* __restrict__ clk) {
+                                                    double* __restrict__ pBC, const double* __restrict__ clk,
+                                                    const unsigned char* __restrict__ isdst) {
   const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
@@ -280,18 +294,34 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
 #pragma unroll
   for (int k = 0; k < 7; k++) qh[k] = Qh[k * N + i];
   const double tA = tau - dt / 2.;
-#pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tA);
   Prim a;
-  transform_pv(E, q, a, c2p_guess(E, i));
-  pA[0 * N + i] = a.e;
-  pA[1 * N + i] = a.p;
-  pA[2 * N + i] = a.nb;
-  pA[3 * N + i] = a.nq;
-  pA[4 * N + i] = a.ns;
-  pA[5 * N + i] = a.vx;
-  pA[6 * N + i] = a.vy;
-  pA[7 * N + i] = a.vz;
+  int gx, gy, gz;
+  coords(g, i, gx, gy, gz);
+  // A is the corrector's con2prim (k_update<false> stored it in pA) when
+  // its divisor tau_n + dt/2 equals tA bit for bit and the ghost copy has
+  // not changed this cell's Qh since
+  if (tA == clk[0] + 0.5 * dt && !(isdst[gx] | isdst[g.nx + gy] | isdst[g.nx + g.ny + gz])) {
+    a.e = pA[0 * N + i];
+    a.p = pA[1 * N + i];
+    a.nb = pA[2 * N + i];
+    a.nq = pA[3 * N + i];
+    a.ns = pA[4 * N + i];
+    a.vx = pA[5 * N + i];
+    a.vy = pA[6 * N + i];
+    a.vz = pA[7 * N + i];
+  } else {
+#pragma unroll
+    for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tA);
+    transform_pv(E, q, a, c2p_guess(E, i));
+    pA[0 * N + i] = a.e;
+    pA[1 * N + i] = a.p;
+    pA[2 * N + i] = a.nb;
+    pA[3 * N + i] = a.nq;
+    pA[4 * N + i] = a.ns;
+    pA[5 * N + i] = a.vx;
+    pA[6 * N + i] = a.vy;
+    pA[7 * N + i] = a.vz;
+  }
 #pragma unroll
   for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tau);
   Prim d;
@@ -1080,7 +1110,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
         done(KK_FACE_Z);
       }
       k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
-                                       a.viscous ? F.pBC : nullptr);
+                                       a.viscous ? F.pBC : nullptr, nullptr);
       done(KK_UPDATE);
     } else {
       k_face<X_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
@@ -1092,7 +1122,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
         done(KK_FACE_Z);
       }
       k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
-                                        nullptr);
+                                        nullptr, a.viscous ? F.pA : nullptr);
       done(KK_UPDATE);
     }
   }
@@ -1100,7 +1130,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   done(KK_GHOST);
   if (a.viscous) {
     k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
-                                   F.pBC, a.clk);
+                                   F.pBC, a.clk, F.gdst);
     done(KK_VISC_PRIMS);
     // the relaxation on full warps of cells with matter (the list kernel's
     // time is counted with the relaxation's)
