@@ -117,6 +117,30 @@ __device__ __forceinline__ double ddivp(double y, double b) {
   return z ? y : q;
 }
 
+// n[j] <- ddivp(n[j], b) for j < K, r = RN(1/b): through crm::mk_div when
+// every numerator and b are in its range (bit-identical, no divide), else
+// with the divide.
+template <int K>
+__device__ __forceinline__ void div_batch(double* n, double b, double r, bool bfast) {
+  bool ok = bfast;
+#pragma unroll
+  for (int j = 0; j < K; j++) ok = ok && crm::mk_num_ok(n[j]);
+  if (ok) {
+#pragma unroll
+    for (int j = 0; j < K; j++) n[j] = crm::mk_div(n[j], b, r);
+  } else {
+#pragma unroll
+    for (int j = 0; j < K; j++) n[j] = ddivp(n[j], b);
+  }
+}
+
+// the 7 components of Q / t (t > 0) into q, through div_batch
+__device__ __forceinline__ void q_over(const double* qin, double t, double* q) {
+#pragma unroll
+  for (int k = 0; k < 7; k++) q[k] = qin[k];
+  div_batch<7>(q, t, 1.0 / t, crm::mk_den_ok(t));
+}
+
 // sqrt(x) (sqrt(+-0) = +-0)
 __device__ __forceinline__ double sqrtz(double x) {
   const bool z = (x == 0.);

@@ -99,14 +99,21 @@ __global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* 
     R = cidx(g, ix, iy, iz + 1);
     Rp = cidx(g, ix, iy, iz + 2);
   }
-  double ql[7], qr[7];
+  double qlr[14];  // the two reconstructed states, then divided by tau as one batch
 #pragma unroll
   for (int k = 0; k < 7; k++) {
     const double a = QQ[k * N + Lm], b = QQ[k * N + L], c = QQ[k * N + R], d = QQ[k * N + Rp];
     const double dQl = minmod((c - b) / 2., (b - a) / 2.);
-    ql[k] = ddivp(b + dQl, tau);
+    qlr[k] = b + dQl;
     const double dQr = minmod((d - c) / 2., (c - b) / 2.);
-    qr[k] = ddivp(c - dQr, tau);
+    qlr[7 + k] = c - dQr;
+  }
+  div_batch<14>(qlr, tau, 1.0 / tau, crm::mk_den_ok(tau));
+  double ql[7], qr[7];
+#pragma unroll
+  for (int k = 0; k < 7; k++) {
+    ql[k] = qlr[k];
+    qr[k] = qlr[7 + k];
   }
   Prim pl, pr;
   transform_pv(E, ql, pl, c2p_guess(E, L));
@@ -157,10 +164,8 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
   const double _dt = PRED ? dt / 2. : dt;
   double q[7], qin[7];
 #pragma unroll
-  for (int k = 0; k < 7; k++) {
-    qin[k] = field[k * N + i];
-    q[k] = ddivp(qin[k], tau1);
-  }
+  for (int k = 0; k < 7; k++) qin[k] = field[k * N + i];
+  q_over(qin, tau1, q);
   Prim pp;
   transform_pv(E, q, pp, c2p_guess(E, i));
   if (!PRED && pA) {
@@ -312,8 +317,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     a.vy = pA[6 * N + i];
     a.vz = pA[7 * N + i];
   } else {
-#pragma unroll
-    for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tA);
+    q_over(qh, tA, q);
     transform_pv(E, q, a, c2p_guess(E, i));
     pA[0 * N + i] = a.e;
     pA[1 * N + i] = a.p;
@@ -324,8 +328,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     pA[6 * N + i] = a.vy;
     pA[7 * N + i] = a.vz;
   }
-#pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = ddivp(qh[k], tau);
+  q_over(qh, tau, q);
   Prim d;
   transform_pv(E, q, d, c2p_guess(E, i));
   pD[0 * N + i] = d.e;
@@ -367,8 +370,10 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
   for (int w = haveB ? 1 : 0; w < 2; w++) {
     const double* src = w == 0 ? Qprev : Q;
     const double tt = w == 0 ? tau - dt : tau;
+    double qs[7];
 #pragma unroll
-    for (int k = 0; k < 7; k++) q[k] = ddivp(src[k * N + i], tt);
+    for (int k = 0; k < 7; k++) qs[k] = src[k * N + i];
+    q_over(qs, tt, q);
     Prim P;
     transform_pv(E, q, P, c2p_guess(E, i));
     const double ut = 1.0 / sqrt(1.0 - P.vx * P.vx - P.vy * P.vy - P.vz * P.vz);
@@ -411,22 +416,6 @@ __device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N
 // are 7 % and 35 % slower, 5 and 6 are 9 % and 3 % slower).
 constexpr int kRelaxMinBlocks = 4;
 
-// n[j] <- ddivp(n[j], b) for j < K, r = RN(1/b): through crm::mk_div when
-// every numerator and b are in its range (bit-identical, no divide), else
-// with the divide.
-template <int K>
-__device__ __forceinline__ void div_batch(double* n, double b, double r, bool bfast) {
-  bool ok = bfast;
-#pragma unroll
-  for (int j = 0; j < K; j++) ok = ok && crm::mk_num_ok(n[j]);
-  if (ok) {
-#pragma unroll
-    for (int j = 0; j < K; j++) n[j] = crm::mk_div(n[j], b, r);
-  } else {
-#pragma unroll
-    for (int j = 0; j < K; j++) n[j] = ddivp(n[j], b);
-  }
-}
 constexpr int kRelaxBlock = 128;
 // shared-memory rows of k_is_relax's relaxation loops: pi, sigma, u, h0, f0
 constexpr int kSmPI = 0, kSmSIG = 10, kSmU = 20, kSmH = 24, kSmF = 34, kSmRows = 44;

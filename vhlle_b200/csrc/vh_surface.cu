@@ -23,9 +23,10 @@ namespace vh {
 __device__ __forceinline__ void cmf_variables(const EosDev& E, const double* __restrict__ Q,
                                               long long N, long long i, double eta, double tau,
                                               Prim& P, double& Y) {
-  double q[7];
+  double q[7], qs[7];
 #pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = ddivp(Q[k * N + i], tau);
+  for (int k = 0; k < 7; k++) qs[k] = Q[k * N + i];
+  q_over(qs, tau, q);
   transform_pv(E, q, P);
   Y = eta + 1. / 2. * log((1. + P.vz) / (1. - P.vz));
   P.vx = P.vx * cosh(Y - eta) / cosh(Y);
@@ -194,15 +195,17 @@ __global__ void k_surf_energy(Geo g, EosDev E, const double* __restrict__ Q,
   // only corners of interior cubes: [2, n-2] on every axis
   if (ix < 2 || iy < 2 || iz < 2 || ix > g.nx - 2 || iy > g.ny - 2 || iz > g.nz - 2) return;
   const long long N = g.N;
-  double q[7];
+  double q[7], qs[7];
   Prim P;
   // Cell::getPrimVar / getPrimVarPrev, src/cll.cpp:90-95,214-220
 #pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = ddivp(Q[k * N + i], tau);
+  for (int k = 0; k < 7; k++) qs[k] = Q[k * N + i];
+  q_over(qs, tau, q);
   transform_pv(E, q, P);
   eN[i] = P.e;
 #pragma unroll
-  for (int k = 0; k < 7; k++) q[k] = ddivp(Qprev[k * N + i], taup);
+  for (int k = 0; k < 7; k++) qs[k] = Qprev[k * N + i];
+  q_over(qs, taup, q);
   transform_pv(E, q, P);
   eP[i] = P.e;
 }
