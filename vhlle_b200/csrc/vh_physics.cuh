@@ -117,10 +117,11 @@ __device__ __forceinline__ double ddivp(double y, double b) {
   return z ? y : q;
 }
 
-// n[j] <- ddivp(n[j], b) for j < K, r = RN(1/b): through crm::mk_div when
-// every numerator and b are in its range (bit-identical, no divide), else
-// with the divide.
-template <int K>
+// n[j] <- ddivp(n[j], b) (ddiv with GENERAL) for j < K, r = RN(1/b):
+// through crm::mk_div when every numerator and b are in its range
+// (bit-identical to either, b being positive there; no divide), else with
+// the divide.
+template <int K, bool GENERAL = false>
 __device__ __forceinline__ void div_batch(double* n, double b, double r, bool bfast) {
   bool ok = bfast;
 #pragma unroll
@@ -130,7 +131,7 @@ __device__ __forceinline__ void div_batch(double* n, double b, double r, bool bf
     for (int j = 0; j < K; j++) n[j] = crm::mk_div(n[j], b, r);
   } else {
 #pragma unroll
-    for (int j = 0; j < K; j++) n[j] = ddivp(n[j], b);
+    for (int j = 0; j < K; j++) n[j] = GENERAL ? ddiv(n[j], b) : ddivp(n[j], b);
   }
 }
 
@@ -531,16 +532,22 @@ __device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, dou
     else { Fyl = Fyl + l.p; Fyr = Fyr + r.p; }
   } else {
     const double tau1 = tauFactor;
-    Ftl = ddivp(U4l * vnl, tau1) + ddivp(l.p * vnl, tau1);
-    Fxl = ddivp(U1l * vnl, tau1);
-    Fyl = ddivp(U2l * vnl, tau1);
-    Fzl = ddivp(U3l * vnl, tau1) + ddivp(l.p, tau1);
-    Fbl = ddivp(Ubl * vnl, tau1); Fql = ddivp(Uql * vnl, tau1); Fsl = ddivp(Usl * vnl, tau1);
-    Ftr = ddivp(U4r * vnr, tau1) + ddivp(r.p * vnr, tau1);
-    Fxr = ddivp(U1r * vnr, tau1);
-    Fyr = ddivp(U2r * vnr, tau1);
-    Fzr = ddivp(U3r * vnr, tau1) + ddivp(r.p, tau1);
-    Fbr = ddivp(Ubr * vnr, tau1); Fqr = ddivp(Uqr * vnr, tau1); Fsr = ddivp(Usr * vnr, tau1);
+    // the 18 quotients by tau1 as one divide-free batch (div_batch)
+    double n[18] = {U4l * vnl, l.p * vnl, U1l * vnl, U2l * vnl, U3l * vnl, l.p,
+                    Ubl * vnl, Uql * vnl, Usl * vnl,
+                    U4r * vnr, r.p * vnr, U1r * vnr, U2r * vnr, U3r * vnr, r.p,
+                    Ubr * vnr, Uqr * vnr, Usr * vnr};
+    div_batch<18>(n, tau1, 1.0 / tau1, crm::mk_den_ok(tau1));
+    Ftl = n[0] + n[1];
+    Fxl = n[2];
+    Fyl = n[3];
+    Fzl = n[4] + n[5];
+    Fbl = n[6]; Fql = n[7]; Fsl = n[8];
+    Ftr = n[9] + n[10];
+    Fxr = n[11];
+    Fyr = n[12];
+    Fzr = n[13] + n[14];
+    Fbr = n[15]; Fqr = n[16]; Fsr = n[17];
   }
   {
     const double ss = sEl + sEr, dv = vnl - vnr;
@@ -561,13 +568,15 @@ __device__ __forceinline__ bool hlle_face(int dir, bool predict, double tau, dou
   if (bl == 0. && br == 0.) return false;
   const double pre = tauFactor * dta / dxdir;
   const double den = -bl + br;
-  flux[T_] = ddiv(pre * (-bl * br * (U4l - U4r) + br * Ftl - bl * Ftr), den);
-  flux[X_] = ddiv(pre * (-bl * br * (U1l - U1r) + br * Fxl - bl * Fxr), den);
-  flux[Y_] = ddiv(pre * (-bl * br * (U2l - U2r) + br * Fyl - bl * Fyr), den);
-  flux[Z_] = ddiv(pre * (-bl * br * (U3l - U3r) + br * Fzl - bl * Fzr), den);
-  flux[NB_] = ddiv(pre * (-bl * br * (Ubl - Ubr) + br * Fbl - bl * Fbr), den);
-  flux[NQ_] = ddiv(pre * (-bl * br * (Uql - Uqr) + br * Fql - bl * Fqr), den);
-  flux[NS_] = ddiv(pre * (-bl * br * (Usl - Usr) + br * Fsl - bl * Fsr), den);
+  flux[T_] = pre * (-bl * br * (U4l - U4r) + br * Ftl - bl * Ftr);
+  flux[X_] = pre * (-bl * br * (U1l - U1r) + br * Fxl - bl * Fxr);
+  flux[Y_] = pre * (-bl * br * (U2l - U2r) + br * Fyl - bl * Fyr);
+  flux[Z_] = pre * (-bl * br * (U3l - U3r) + br * Fzl - bl * Fzr);
+  flux[NB_] = pre * (-bl * br * (Ubl - Ubr) + br * Fbl - bl * Fbr);
+  flux[NQ_] = pre * (-bl * br * (Uql - Uqr) + br * Fql - bl * Fqr);
+  flux[NS_] = pre * (-bl * br * (Usl - Usr) + br * Fsl - bl * Fsr);
+  // divided by den as one divide-free batch (ddiv's results)
+  div_batch<7, true>(flux, den, 1.0 / den, crm::mk_den_ok(den));
   if (flux[NB_] != flux[NB_]) { err |= ERR_FLUX_NAN; return false; }
   return true;
 }
