@@ -637,8 +637,11 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
   const double eta = etaS * s;
   double sig[10];
 #pragma unroll
+  for (int k = 0; k < 10; k++) sig[k] = 0.5 * piNS[k];
+  div_batch<10, true>(sig, eta, 1.0 / eta, crm::mk_den_ok(eta));  // ddiv's quotients
+#pragma unroll
   for (int k = 0; k < 10; k++) {
-    sig[k] = ddiv(0.5 * piNS[k], eta) * 5.068;
+    sig[k] = sig[k] * 5.068;
     if (eta <= 0.0) sig[k] = 0.0;
   }
 #define SIG(a, b) sig[index44(a, b)]
@@ -942,21 +945,22 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
 // Hydro::visc_flux (src/hdo.cpp:966-1014) for the six faces of the cell,
 // visc_source_step (src/hdo.cpp:355-375) and Cell::updateByViscFlux
 // (src/cll.cpp:76-84).
+// the face's cell size along dir (eta: dz (tau + dt/2), src/hdo.cpp:971-976)
+__device__ __forceinline__ double visc_dxa(int dir, double tau, double dt, const Geo& g) {
+  if (dir == X_) return g.dx;
+  if (dir == Y_) return g.dy;
+  return g.dz * (tau + 0.5 * dt);
+}
+
+// rdxa = RN(1 / dxa): the four quotients by dxa go through div_batch
 __device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const Geo& g,
                                           const double* __restrict__ pA,
                                           const double* __restrict__ piH,
                                           const double* __restrict__ PiH,
                                           const double* __restrict__ m, long long L, long long R,
-                                          double f[4]) {
+                                          double dxa, double rdxa, double f[4]) {
   const long long N = g.N;
   if (m[(dir - 1) * N + L] < 1. && m[(dir - 1) * N + R] < 1.) return false;
-  double dxa;
-  if (dir == X_)
-    dxa = g.dx;
-  else if (dir == Y_)
-    dxa = g.dy;
-  else
-    dxa = g.dz * (tau + 0.5 * dt);
   double vxl = pA[5 * N + L], vyl = pA[6 * N + L], vzl = pA[7 * N + L];
   const double vxr = pA[5 * N + R], vyr = pA[6 * N + R], vzr = pA[7 * N + R];
   vxl = 0.5 * (vxl + vxr);
@@ -978,8 +982,9 @@ __device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const 
     double x = 0.5 * (piH[k * N + L] + piH[k * N + R]);
     if (a == dir) x += -0.5 * (PL + PR) * gmumu[a];
     x += 0.5 * (PL + PR) * uuu[a] * uuu[dir];
-    f[a] = ddivp(x * (tau - 0.5 * dt) * dt, dxa);
+    f[a] = x * (tau - 0.5 * dt) * dt;
   }
+  div_batch<4>(f, dxa, rdxa, crm::mk_den_ok(dxa));
   return true;
 }
 
@@ -1004,11 +1009,13 @@ __global__ void __launch_bounds__(128, 8) k_visc_update(Geo g, const double* __r
   const int nn[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
   for (int d = 0; d < 3; d++) {
-    if (cc[d] > 0 && visc_face(d + 1, tau, dt, g, pA, piH, PiH, m, i - st[d], i, f)) {
+    const double dxa = visc_dxa(d + 1, tau, dt, g), rdxa = 1.0 / dxa;
+    if (cc[d] > 0 && visc_face(d + 1, tau, dt, g, pA, piH, PiH, m, i - st[d], i, dxa, rdxa, f)) {
 #pragma unroll
       for (int k = 0; k < 4; k++) fl[k] += f[k];
     }
-    if (cc[d] < nn[d] - 1 && visc_face(d + 1, tau, dt, g, pA, piH, PiH, m, i, i + st[d], f)) {
+    if (cc[d] < nn[d] - 1 &&
+        visc_face(d + 1, tau, dt, g, pA, piH, PiH, m, i, i + st[d], dxa, rdxa, f)) {
 #pragma unroll
       for (int k = 0; k < 4; k++) fl[k] += -f[k];
     }
