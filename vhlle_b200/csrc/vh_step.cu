@@ -339,7 +339,8 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
   {
     double T, mub, p;
     eos_eval(E, a.e, a.nb, T, mub, p);
-    const double s = eos_s(E, a.e, a.nb, a.nq, a.ns);
+    // EoS::s at the same point (eos_s, muq = mus = 0) from this lookup
+    const double s = T > 0.0 ? ddivp(a.e + p - mub * a.nb - 0. * a.nq - 0. * a.ns, T) : 0.;
     const double etaS = tr_etaS(tr, a.e, a.nb, T, mub, s, p);
     const double zetaS = tr_zetaS(tr, a.e, T, s, p);
     double taupi, tauPi;
@@ -352,7 +353,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     pTh[5 * N + i] = zetaS;
     pTh[6 * N + i] = taupi;
     pTh[7 * N + i] = tauPi;
-    pTh[8 * N + i] = 9. / 70. / eos_p(E, a.e, a.nb);
+    pTh[8 * N + i] = 9. / 70. / p;  // eos_p at the same point is this p
   }
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
