@@ -21,6 +21,7 @@ PROGRAM = r"""
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include "vh_crmath.cuh"
 int main() {
   char f[8];
@@ -36,14 +37,20 @@ int main() {
     };
     auto unit = [&]() { return (double)(next() >> 11) * 0x1p-53; };
     long bad = 0, used = 0;
+    auto same = [](double a, double c) { return std::memcmp(&a, &c, sizeof a) == 0; };
     for (long i = 0; i < n; i++) {
       const double b = std::ldexp(1.0 + unit(), (int)(unit() * 200) - 100);
-      const double y = (unit() < 0.5 ? -1 : 1) * std::ldexp(1.0 + unit(), (int)(unit() * 1800) - 900);
+      double y = (unit() < 0.5 ? -1 : 1) * std::ldexp(1.0 + unit(), (int)(unit() * 1800) - 900);
+      if (i % 1000 == 0) y = (i % 2000 == 0) ? 0.0 : -0.0;  // signed zeros
       if (!vh::crm::mk_num_ok(y) || !vh::crm::mk_den_ok(b)) continue;
       used++;
-      if (vh::crm::mk_div(y, b, 1.0 / b) != y / b) bad++;
+      if (!same(vh::crm::mk_div(y, b, 1.0 / b), y / b)) bad++;
     }
     std::printf("%ld %ld\n", used, bad);
+    return 0;
+  }
+  if (f[0] == 'k') {  // mk_num_ok of each argument
+    while (std::scanf("%la", &x) == 1) std::printf("%d\n", (int)vh::crm::mk_num_ok(x));
     return 0;
   }
   do {
@@ -70,6 +77,10 @@ def crm(tmp_path_factory):
             out = subprocess.run([str(exe)], input="m %d %d\n" % tuple(xs), capture_output=True,
                                  text=True, check=True)
             return [int(t) for t in out.stdout.split()]
+        if kind == "k":
+            inp = "k\n" + "".join("%s\n" % float(x).hex() for x in xs)
+            out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True)
+            return [bool(int(t)) for t in out.stdout.split()]
         inp = "".join("%s %s\n" % (kind, float(x).hex()) for x in xs)
         out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True)
         return [float.fromhex(t) for t in out.stdout.split()]
@@ -122,3 +133,17 @@ def test_markstein_division_equals_the_divide(crm):
     whole range (|y| in [2^-900, 2^900], b in [2^-100, 2^100])."""
     used, bad = crm("m", (2000000, 11))
     assert used > 1900000 and bad == 0
+
+
+def test_markstein_numerator_range(crm):
+    """crm::mk_num_ok (exponent bits) accepts exactly 2^-900 <= |y| < 2^900
+    and the two zeros: not subnormals, infinities or NaN."""
+    lo, hi = math.ldexp(1.0, -900), math.ldexp(1.0, 900)
+    xs = [lo, -lo, math.nextafter(lo, 0), math.nextafter(-lo, 0), hi, -hi,
+          math.nextafter(hi, 0), -math.nextafter(hi, 0), 0.0, -0.0, 5e-324, -5e-324,
+          2.2250738585072014e-308, 1e-310, float("inf"), -float("inf"), float("nan"), 1.0,
+          -3.5, 1.7976931348623157e308]
+    rng = np.random.default_rng(5)
+    xs += list(rng.choice([-1, 1], 2000) * 2.0 ** rng.uniform(-1074, 1023, 2000))
+    want = [x == 0.0 or lo <= abs(x) < hi for x in xs]
+    assert crm("k", xs) == want

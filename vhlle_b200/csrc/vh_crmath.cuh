@@ -165,21 +165,43 @@ VH_CRM double root4_cr(double x) {
 // fma, and RN(q0 + r (y - b q0)) = RN(y / b) (Markstein's theorem, IBM J.
 // Res. Dev. 34 (1990); Muller et al., Handbook of Floating-Point
 // Arithmetic, the Newton-Raphson division chapter).  It needs nothing to
-// underflow or overflow: mk_num_ok(y) (2^-900 <= |y| <= 2^900, or y = 0,
-// which is returned as is, as the zero-safe divisions return it) and
-// mk_den_ok(b) (2^-100 <= b <= 2^100).  Callers test a batch of numerators
-// once and divide the IEEE way otherwise, so that a batch of quotients is
-// free of branches (a divide is an instruction sequence with a branch to a
-// slow path, which keeps independent divides from overlapping).
+// underflow or overflow: mk_num_ok(y) (2^-900 <= |y| < 2^900, or y = +-0)
+// and mk_den_ok(b) (2^-100 <= b <= 2^100, so b > 0).  Callers test a batch
+// of numerators once and divide the IEEE way otherwise, so that a batch of
+// quotients is free of branches (a divide is an instruction sequence with a
+// branch to a slow path, which keeps independent divides from overlapping).
+// Both tests and the sign fix below are bit operations, off the FP64 pipe.
+VH_CRM unsigned mk_hi(double y) {
+#ifdef __CUDA_ARCH__
+  return (unsigned)__double2hiint(y);
+#else
+  unsigned long long u;
+  __builtin_memcpy(&u, &y, sizeof u);
+  return (unsigned)(u >> 32);
+#endif
+}
+VH_CRM unsigned mk_lo(double y) {
+#ifdef __CUDA_ARCH__
+  return (unsigned)__double2loint(y);
+#else
+  unsigned long long u;
+  __builtin_memcpy(&u, &y, sizeof u);
+  return (unsigned)u;
+#endif
+}
+// |y| in [2^-900, 2^900): biased exponent in [123, 1922]; or y = +-0
 VH_CRM bool mk_num_ok(double y) {
-  const double a = fabs(y);
-  return (a >= 0x1p-900 && a <= 0x1p900) || y == 0.;
+  const unsigned h = mk_hi(y) & 0x7fffffffu;
+  return h - (123u << 20) < (1800u << 20) || (h | mk_lo(y)) == 0u;
 }
 VH_CRM bool mk_den_ok(double b) { return b >= 0x1p-100 && b <= 0x1p100; }
+// For y != 0 the quotient has the sign of q0; for y = +-0 (b > 0) the
+// divide returns y, which q0 = y r also is, so the sign of q0 is the sign
+// of the result in both cases.
 VH_CRM double mk_div(double y, double b, double r) {
   const double q0 = y * r;
   const double rem = fma(-q0, b, y);
-  return y == 0. ? y : fma(rem, r, q0);
+  return copysign(fma(rem, r, q0), q0);
 }
 
 }  // namespace crm
