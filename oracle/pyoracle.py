@@ -54,7 +54,8 @@ class _Trc(ctypes.Structure):
 
 
 class _State(ctypes.Structure):
-    _fields_ = [(n, _dp) for n in ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")]
+    _fields_ = [(n, _dp) for n in ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc",
+                                   "dbeta")]
 
 
 _lib_oracle = None
@@ -82,6 +83,8 @@ def oracle_lib():
         lib.or_surface.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_State),
                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, _dp, ctypes.c_long,
                                    _dp]
+        lib.or_surface_beta.restype = ctypes.c_long
+        lib.or_surface_beta.argtypes = lib.or_surface.argtypes + [_dp]
         lib.or_corona.restype = ctypes.c_long
         lib.or_corona.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_State),
                                   ctypes.c_double, ctypes.c_double, _dp, ctypes.c_long, _dp]
@@ -128,6 +131,10 @@ def ref_lib():
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
         lib.ref_cornelius4d.restype = ctypes.c_int
         lib.ref_cornelius4d.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp]
+        lib.ref_enable_vorticity.argtypes = [ctypes.c_void_p]
+        lib.ref_get_dbeta.argtypes = [ctypes.c_void_p, _dp]
+        lib.ref_print_dbeta_header.restype = ctypes.c_int
+        lib.ref_print_dbeta_header.argtypes = [ctypes.c_void_p]
         lib.ref_resize2x.restype = ctypes.c_int
         lib.ref_resize2x.argtypes = [ctypes.c_void_p]
         lib.ref_advance.restype = ctypes.c_int
@@ -233,9 +240,10 @@ def _trc(setup):
 class OracleRun:
     """The C restatement driven like Hydro: step() == performStep()."""
 
-    def __init__(self, setup, tol=None):
+    def __init__(self, setup, tol=None, vorticity=False):
         """tol: the transformPV stopping tolerance (None: the reference's
-        1e-5; a smaller value gives the tight-tolerance oracle)."""
+        1e-5; a smaller value gives the tight-tolerance oracle).  vorticity:
+        Hydro::enableVorticity, d_mu beta_nu per cell in self.dbeta."""
         self.setup = setup
         g = setup.grid
         self.grid = _Grid(g.nx, g.ny, g.nz, *g.bounds())
@@ -247,11 +255,14 @@ class OracleRun:
         self.dt = setup.dt
         self.lib = oracle_lib()
         self.errors = 0
+        self.dbeta = np.zeros(16 * g.ncells) if vorticity else None
 
     def _sview(self):
         s = _State()
         for k in FIELDS:
             setattr(s, k, _ptr(self.state[k]))
+        if self.dbeta is not None:
+            s.dbeta = _ptr(self.dbeta)
         return s
 
     def step(self, n=1):
@@ -309,6 +320,8 @@ class OracleRun:
         self.grid = gout
         self.state = out
         self.dt = dt2
+        if self.dbeta is not None:  # the new fluid's cells start at zero
+            self.dbeta = np.zeros_like(self.dbeta)
         return 1
 
     def grid_coords(self):
@@ -345,6 +358,24 @@ class OracleRun:
             raise RuntimeError("Cornelius stopped (the reference would exit)")
         assert n <= cap
         return rec[:n].copy(), dict(zip(SURF_ACC, acc))
+
+    def surface_beta(self, dtf=None, cap=200000):
+        """surface() plus each element's 16 Cartesian d_mu beta_nu of the
+        beta.dat line: (records, acc dict, beta [n][16])."""
+        if self.dbeta is None:
+            raise RuntimeError("vorticity is off")
+        dtf = self.setup.dt if dtf is None else dtf
+        rec = np.zeros((cap, SURF_REC))
+        beta = np.zeros((cap, 16))
+        acc = np.zeros(5)
+        sv = self._sview()
+        n = self.lib.or_surface_beta(ctypes.byref(self.grid), ctypes.byref(self.eos.s),
+                                     ctypes.byref(sv), self.tau.value, dtf, self.setup.ecrit,
+                                     _ptr(rec), cap, _ptr(acc), _ptr(beta))
+        if n < 0:
+            raise RuntimeError("Cornelius stopped (the reference would exit)")
+        assert n <= cap
+        return rec[:n].copy(), dict(zip(SURF_ACC, acc)), beta[:n].copy()
 
     def corona(self, cap=2000000):
         """Fluid::outputCorona's elements at the current tau: (records
@@ -428,6 +459,20 @@ class RefRun:
     def step(self, n=1):
         self.lib.ref_step(self.h, n)
         return 0
+
+    def enable_vorticity(self):
+        """Hydro::enableVorticity; before the first output_surface call."""
+        self.lib.ref_enable_vorticity(self.h)
+
+    def get_dbeta(self):
+        """Cell::getDbeta of every cell, [16][N] flattened (4 mu + nu)."""
+        out = np.zeros(16 * self.setup.grid.ncells)
+        self.lib.ref_get_dbeta(self.h, _ptr(out))
+        return out
+
+    def print_dbeta_header(self):
+        """Fluid::printDbetaHeader into beta.dat; False when it throws."""
+        return self.lib.ref_print_dbeta_header(self.h) == 0
 
     @property
     def tau_now(self):

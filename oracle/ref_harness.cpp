@@ -36,7 +36,7 @@
 
 // the freeze-out stream Fluid::outputSurface writes to (src/fld.cpp:43-46)
 namespace output {
-extern std::ofstream ffreeze;
+extern std::ofstream ffreeze, fbeta;
 }
 
 namespace {
@@ -73,6 +73,7 @@ struct RefRun {
   double dx = 0, dy = 0;
   double tau0 = 0, ecrit = 0;
   bool output_open = false;
+  bool vorticity = false;
 };
 
 }  // namespace
@@ -112,6 +113,7 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
 void ref_destroy(void *p) {
   RefRun *r = static_cast<RefRun *>(p);
   if (r->output_open && output::ffreeze.is_open()) output::ffreeze.close();
+  if (r->output_open && output::fbeta.is_open()) output::fbeta.close();
   delete r->h;
   delete r->f;
   delete r->tr;
@@ -178,6 +180,8 @@ int ref_resize2x(void *p) {
       for (int iz = 0; iz < f->getNZ(); iz++)
         fnew->getCell(ix, iy, iz)->importVars(f->getCell(2 * (ix - f->getNX() / 2) + f->getNX() / 2,
                                                          2 * (iy - f->getNY() / 2) + f->getNY() / 2, iz));
+  // src/main.cpp:257,264-265: the new fluid's cells get zero dbeta
+  if (r->vorticity) fnew->enableVorticity();
   r->h->setFluid(fnew);
   r->h->setDtau(dt2);
   delete f;
@@ -396,11 +400,13 @@ int ref_output_surface(void *p, const char *dir, int extendFO, char *line, int l
   if (!r->output_open) {
     // the freeze-out stream is a process-wide global: one run at a time
     if (output::ffreeze.is_open()) output::ffreeze.close();
+    if (output::fbeta.is_open()) output::fbeta.close();
     r->f->initOutput(dir, r->tau0, true);
     r->output_open = true;
   }
   const int n = r->f->outputSurface(r->h->getTau(), extendFO != 0);
   output::ffreeze.flush();
+  if (output::fbeta.is_open()) output::fbeta.flush();
   std::cout.rdbuf(old);
   const std::string all = cap.str();
   // the totals line is the last non-empty line
@@ -447,6 +453,43 @@ int ref_output_corona(void *p, const char *dir, int extendFO, char *line, int li
     line[linelen - 1] = 0;
   }
   return n;
+}
+
+// Hydro::enableVorticity (src/hdo.cpp:60-64): dbeta in every cell, written
+// by ISformal from the next step on, and beta.dat lines from outputSurface
+// (the file opens with the freeze-out output, so call this before the first
+// ref_output_surface).
+void ref_enable_vorticity(void *p) {
+  RefRun *r = static_cast<RefRun *>(p);
+  r->h->enableVorticity();
+  r->vorticity = true;
+}
+
+// Cell::getDbeta of every cell: out[(4 mu + nu) * N + i], i x-fastest.
+void ref_get_dbeta(void *p, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  const long N = (long)r->nx * r->ny * r->nz;
+  for (int iz = 0; iz < r->nz; iz++)
+    for (int iy = 0; iy < r->ny; iy++)
+      for (int ix = 0; ix < r->nx; ix++) {
+        const long i = ix + (long)r->nx * (iy + (long)r->ny * iz);
+        Cell *c = r->f->getCell(ix, iy, iz);
+        for (int a = 0; a < 4; a++)
+          for (int b = 0; b < 4; b++) out[(4 * a + b) * N + i] = c->getDbeta(a, b);
+      }
+}
+
+// Fluid::printDbetaHeader (src/fld.cpp:174-188) into beta.dat: 0, or -1
+// when the reference throws (no corona count yet).
+int ref_print_dbeta_header(void *p) {
+  RefRun *r = static_cast<RefRun *>(p);
+  try {
+    r->f->printDbetaHeader();
+  } catch (const std::exception &) {
+    return -1;
+  }
+  if (output::fbeta.is_open()) output::fbeta.flush();
+  return 0;
 }
 
 // The reference's Cornelius class on one hypercube: cube[it*8+jx*4+jy*2+jz],

@@ -737,14 +737,17 @@ static double getpi(const Ctx *c, const double *a, long i, int mu, int nu) {
   return a[(long)index44(mu, nu) * c->N + i];
 }
 
-/* Hydro::NSquant, src/hdo.cpp:381-652 (vorticity off) */
+/* Hydro::NSquant, src/hdo.cpp:381-652.  M is ISformal's one dbeta matrix
+ * (NULL with vorticity off): rows are written only where the reference
+ * writes them, and nothing next to vacuum, so the rest keeps the values of
+ * earlier cells. */
 static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
-                    double *Pi, double dmu[4][4], double *du) {
+                    double *Pi, double dmu[4][4], double (*M)[4], double *du) {
   const double VMIN = 1e-2;
   const double UDIFF = 3.0;
   const double tau = c->tau, dt = c->dt;
   double e0, e1, p, nb, nq, ns, vx1, vy1, vz1, vx0, vy0, vz0, vxH, vyH, vzH;
-  double T, mub;
+  double T, mub, T0 = 0., T1 = 0.;
   double ut0, ux0, uy0, uz0, ut1, ux1, uy1, uz1;
   double uuu[4];
   const double gmunu[4][4] = {
@@ -769,7 +772,9 @@ static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
   }
   primCenter(c, c->s->Qprev, ic, tau - dt, &e0, &p, &nb, &nq, &ns, &vx0, &vy0,
              &vz0);
+  if (M) eos_eval(c->E, e0, nb, &T0, &mub, &p);
   primCenter(c, c->s->Q, ic, tau, &e1, &p, &nb, &nq, &ns, &vx1, &vy1, &vz1);
+  if (M) eos_eval(c->E, e1, nb, &T1, &mub, &p);
   primCenter(c, c->s->Qh, ic, tau - 0.5 * dt, &e1, &p, &nb, &nq, &ns, &vxH,
              &vyH, &vzH);
   double etaS, zetaS;
@@ -794,6 +799,14 @@ static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
   dmu[0][1] = (ux1 * ux1 - ux0 * ux0) / 2. / uuu[1] / dt;
   dmu[0][2] = (uy1 * uy1 - uy0 * uy0) / 2. / uuu[2] / dt;
   dmu[0][3] = (uz1 * uz1 - uz0 * uz0) / 2. / uuu[3] / dt;
+  if (M) { /* src/hdo.cpp:450-459; e1 is the half-step centre's here */
+    M[0][0] = (ut1 / T1 - ut0 / T0) / dt;
+    M[0][1] = (ux1 / T1 - ux0 / T0) / dt;
+    M[0][2] = (uy1 / T1 - uy0 / T0) / dt;
+    M[0][3] = (uz1 / T1 - uz0 / T0) / dt;
+    if (e1 <= 0. || e0 <= 0. || T1 <= 0. || T0 <= 0.)
+      M[0][0] = M[0][1] = M[0][2] = M[0][3] = 0.;
+  }
   if (fabs(0.5 * (ut1 + ut0) / ut1) > UDIFF) dmu[0][0] = (ut1 - ut0) / dt;
   if (fabs(uuu[1]) < VMIN || fabs(0.5 * (ux1 + ux0) / ux1) > UDIFF)
     dmu[0][1] = (ux1 - ux0) / dt;
@@ -818,7 +831,9 @@ static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
       im = cell(c, ix, iy, iz - 1);
     }
     primCenter(c, c->s->Qh, ip, tau, &e1, &p, &nb, &nq, &ns, &vx1, &vy1, &vz1);
+    if (M) eos_eval(c->E, e1, nb, &T1, &mub, &p);
     primCenter(c, c->s->Qh, im, tau, &e0, &p, &nb, &nq, &ns, &vx0, &vy0, &vz0);
+    if (M) eos_eval(c->E, e0, nb, &T0, &mub, &p);
     if (e1 > 0. && e0 > 0.) {
       ut0 = 1.0 / sqrt(1.0 - vx0 * vx0 - vy0 * vy0 - vz0 * vz0);
       ux0 = ut0 * vx0;
@@ -828,6 +843,15 @@ static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
       ux1 = ut1 * vx1;
       uy1 = ut1 * vy1;
       uz1 = ut1 * vz1;
+      if (M) { /* src/hdo.cpp:491-500, 537-546, 583-592 */
+        const double h = d == 1 ? dx : d == 2 ? dy : dz * (tau + 0.5 * dt);
+        M[d][0] = 0.5 * (ut1 / T1 - ut0 / T0) / h;
+        M[d][1] = 0.5 * (ux1 / T1 - ux0 / T0) / h;
+        M[d][2] = 0.5 * (uy1 / T1 - uy0 / T0) / h;
+        M[d][3] = 0.5 * (uz1 / T1 - uz0 / T0) / h;
+        if (e1 <= 0. || e0 <= 0. || T1 <= 0. || T0 <= 0.)
+          M[d][0] = M[d][1] = M[d][2] = M[d][3] = 0.;
+      }
       if (d == 1 || d == 2) {
         const double h = (d == 1) ? dx : dy;
         dmu[d][0] = 0.25 * (ut1 * ut1 - ut0 * ut0) / uuu[0] / h;
@@ -863,6 +887,10 @@ static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
   }
   dmu[3][0] += uuu[3] / (tau - 0.5 * dt);
   dmu[3][3] += uuu[0] / (tau - 0.5 * dt);
+  if (M && T > 0.) { /* src/hdo.cpp:608-611 */
+    M[3][0] += uuu[3] / (T * (tau - 0.5 * dt));
+    M[3][3] += uuu[0] / (T * (tau - 0.5 * dt));
+  }
   /* Z^{mu nu lambda rho} contraction, element by element */
   for (int i = 0; i < 4; i++)
     for (int j = 0; j < 4; j++) {
@@ -885,11 +913,17 @@ static void NSquant(Ctx *c, int ix, int iy, int iz, double pi[4][4],
 }
 
 /* Hydro::ISformal, src/hdo.cpp:682-963 (first-order relaxation, no
- * FORMAL_SOLUTION, vorticity off) */
+ * FORMAL_SOLUTION).  With vorticity (s->dbeta set) one dbeta matrix, zero
+ * at the start of the call, goes through NSquant cell after cell in loop
+ * order; each cell with matter stores it clamped (Cell::setDbeta,
+ * src/cll.h:173-183), each empty cell stores zeros (Cell::resetDbeta). */
 static void ISformal(Ctx *c) {
   const double tau = c->tau, dt = c->dt;
   const double gmumu[4] = {1., -1., -1., -1.};
   const long N = c->N;
+  double *dbeta = c->s->dbeta;
+  double Mb[4][4] = {{0.}};
+  double (*M)[4] = dbeta ? Mb : NULL;
   double *pi0 = c->pi0, *piH0 = c->piH0, *Pi0 = c->Pi0, *PiH0 = c->PiH0;
   const double *cpi = c->s->pi;
   const double *cPi = c->s->Pi;
@@ -913,6 +947,8 @@ static void ISformal(Ctx *c) {
             }
           PiH0[ic] = 0.0;
           Pi0[ic] = 0.0;
+          if (dbeta)
+            for (int k = 0; k < 16; k++) dbeta[(long)k * N + ic] = 0.0;
           continue;
         }
         double gamma = 1.0 / sqrt(1.0 - vx * vx - vy * vy - vz * vz);
@@ -926,7 +962,11 @@ static void ISformal(Ctx *c) {
           flux[i] = (tau - dt) * (PI(0, i) + cPi[ic] * u[0] * u[i]);
         flux[0] += -(tau - dt) * cPi[ic];
         addFlux(c, ic, flux);
-        NSquant(c, ix, iy, iz, piNS, &PiNS, dmu, &du);
+        NSquant(c, ix, iy, iz, piNS, &PiNS, dmu, M, &du);
+        if (dbeta)
+          for (int a = 0; a < 4; a++)
+            for (int b = 0; b < 4; b++)
+              dbeta[(long)(4 * a + b) * N + ic] = smax(smin(M[a][b], 100.), -100.);
         eos_eval(c->E, e, nb, &T, &mub, &p);
         double etaS, zetaS;
         const double s = eos_s(c->E, e, nb, nq, ns);
@@ -2039,8 +2079,9 @@ static void to_lab(double eta, double *vx, double *vy, double *vz) {
  * count of elements with T > 0.4 or |muB| > 0.85.  Returns the number of
  * elements (records beyond cap are counted but not written), or -1 when
  * Cornelius would have stopped the reference. */
-long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau,
-                double dtf, double ecrit, double *rec, long cap, double *acc) {
+static long surface_impl(const or_grid *g, const or_eos *E, const or_state *s, double tau,
+                         double dtf, double ecrit, double *rec, long cap, double *acc,
+                         double *beta) {
   const int nx = g->nx, ny = g->ny, nz = g->nz;
   const long N = (long)nx * ny * nz;
   const double dx = (g->xmax - g->xmin) / (nx - 1);
@@ -2051,7 +2092,7 @@ long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau
   for (int ix = 2; ix < nx - 2; ix++)
     for (int iy = 2; iy < ny - 2; iy++)
       for (int iz = 2; iz < nz - 2; iz++) {
-        double cube[16], QCube[2][8][7], piS[8][10], PiS[8];
+        double cube[16], QCube[2][8][7], piS[8][10], PiS[8], dbS[8][16];
         for (int jx = 0; jx < 2; jx++)
           for (int jy = 0; jy < 2; jy++)
             for (int jz = 0; jz < 2; jz++) {
@@ -2070,6 +2111,8 @@ long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau
               }
               for (int k = 0; k < 10; k++) piS[c][k] = s->pi[(long)k * N + i];
               PiS[c] = s->Pi[i];
+              if (beta)
+                for (int k = 0; k < 16; k++) dbS[c][k] = s->dbeta[(long)k * N + i];
             }
         double cen[CN_MAX_ELEM][4], nrm[CN_MAX_ELEM][4];
         const int ne = or_cornelius4d(cube, arrayDx, ecrit, cen, nrm);
@@ -2095,12 +2138,16 @@ long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau
           const double muqC = 0., musC = 0.;
           if (TC > 0.4 || fabs(mubC) > 0.85) acc[4] += 1.;
           if (eC > ecrit * 2.0 || eC < ecrit * 0.5) acc[0] += 1.;
+          double dbI[16];
+          for (int k = 0; k < 16; k++) dbI[k] = 0.0;
           for (int jx = 0; jx < 2; jx++)
             for (int jy = 0; jy < 2; jy++)
               for (int jz = 0; jz < 2; jz++) {
                 const int c = jx * 4 + jy * 2 + jz;
                 for (int k = 0; k < 10; k++) piC[k] += piS[c][k] * wX[jx] * wY[jy] * wZ[jz];
                 PiC += PiS[c] * wX[jx] * wY[jy] * wZ[jz];
+                if (beta) /* src/fld.cpp:716-727 */
+                  for (int k = 0; k < 16; k++) dbI[k] += dbS[c][k] * wX[jx] * wY[jy] * wZ[jz];
               }
           double v2C = vxC * vxC + vyC * vyC + vzC * vzC;
           if (v2C > 1.) {
@@ -2158,11 +2205,38 @@ long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau
             r[26] = PiC;
             r[27] = eC;
             r[28] = nbC;
+            if (beta) {
+              /* d_i beta_j in Cartesian components: J_ik J_jl dbeta_kl g_ll
+               * with the Milne-to-Cartesian Jacobian, src/fld.cpp:798-831 */
+              const double J[4][4] = {
+                  {ch, 0., 0., -sh}, {0., 1., 0., 0.}, {0., 0., 1., 0.}, {-sh, 0., 0., ch}};
+              const double gl[4] = {1., -1., -1., -1.};
+              double *b = beta + nel * 16;
+              for (int a = 0; a < 4; a++)
+                for (int bb = 0; bb < 4; bb++) {
+                  double v = 0.0;
+                  for (int k = 0; k < 4; k++)
+                    for (int l = 0; l < 4; l++) v += J[a][k] * J[bb][l] * dbI[4 * k + l] * gl[l];
+                  b[4 * a + bb] = v;
+                }
+            }
           }
           nel++;
         }
       }
   return nel;
+}
+
+long or_surface(const or_grid *g, const or_eos *E, const or_state *s, double tau,
+                double dtf, double ecrit, double *rec, long cap, double *acc) {
+  return surface_impl(g, E, s, tau, dtf, ecrit, rec, cap, acc, NULL);
+}
+
+long or_surface_beta(const or_grid *g, const or_eos *E, const or_state *s, double tau,
+                     double dtf, double ecrit, double *rec, long cap, double *acc,
+                     double *beta) {
+  if (!s->dbeta) return -2;
+  return surface_impl(g, E, s, tau, dtf, ecrit, rec, cap, acc, beta);
 }
 
 /* Fluid::outputCorona, src/fld.cpp:876-1089 (the element part; the totals

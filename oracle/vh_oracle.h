@@ -64,6 +64,10 @@ typedef struct or_state {
   double *PiH;   /* [N]                                          */
   double *m;     /* [3][N]  matter fill fraction per direction   */
   double *vcc;   /* [N]     viscCorrCut flag                      */
+  /* [16][N] d_mu beta_nu of every cell, row-major (4 mu + nu), as
+   * Cell::setDbeta stores it (clamped to [-100, 100]); NULL = vorticity
+   * off.  Written by the viscous step only (ISformal). */
+  double *dbeta;
 } or_state;
 
 /* error bits returned by or_step (the reference calls exit() on these) */
@@ -142,6 +146,12 @@ long or_surface(const or_grid *g, const or_eos *eos, const or_state *s,
  * nbSurf, vEff increments and the count of elements with T > 0.4 or
  * |muB| > 0.99.  Returns the number of elements (records beyond cap are
  * counted, not written). */
+/* or_surface plus, per element, the 16 Cartesian d_mu beta_nu of the
+ * beta.dat line (row-major) into beta[cap][16]; s->dbeta must be set. */
+long or_surface_beta(const or_grid *g, const or_eos *eos, const or_state *s,
+                     double tau, double dtf, double ecrit, double *rec, long cap,
+                     double *acc, double *beta);
+
 long or_corona(const or_grid *g, const or_eos *eos, const or_state *s, double tau,
                double ecrit, double *rec, long cap, double *acc);
 

@@ -109,6 +109,68 @@ def save_surface_case(name, setup, nsteps):
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
 
 
+VORTICITY_CASES = {
+    # name: (setup factory, steps); vorticity on, Fluid::outputSurface after
+    # every step (beta.dat lines), the cells' dbeta after the first and the
+    # last step
+    "vorticity_glauber_21x21x11_b9": (lambda: W.small_glauber3d(21, 11, b=9.0, seed=5), 6),
+    "vorticity_glauber_nb_17x17x9": (
+        lambda: W.glauber3d_nb_setup(17, 17, 9, eos=W.nb_table(200, 20)), 4),
+}
+
+
+def read_beta(path):
+    """beta.dat element lines (src/fld.cpp:665-669,741-745,826-830): position,
+    dSigma_mu, u^mu, T, muB, muQ, muS, the 16 Cartesian d_mu beta_nu, e."""
+    rows = []
+    with open(path) as f:
+        for line in f:
+            v = line.split()
+            if v and not v[0].startswith("#"):
+                rows.append([float(x) for x in v])
+    return np.array(rows, dtype=np.float64).reshape(-1, 33)
+
+
+def save_vorticity_case(name, setup, nsteps):
+    r = P.RefRun(setup)
+    r.enable_vorticity()
+    counts, dbeta = [], []
+    with tempfile.TemporaryDirectory() as d:
+        for k in range(nsteps):
+            r.step(1)
+            if k in (0, nsteps - 1):
+                dbeta.append(r.get_dbeta())
+            n, _ = r.output_surface(d, extend=True)
+            counts.append(n)
+        r.close()
+        beta = read_beta(os.path.join(d, "beta.dat"))
+    assert beta.shape[0] == sum(counts)
+    arrays = _setup_arrays(setup)
+    arrays.update(nsteps=np.array(nsteps), surf_counts=np.array(counts), beta_rec=beta,
+                  dbeta_first=dbeta[0], dbeta_last=dbeta[1])
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+
+
+def load_vorticity_case(path):
+    """(Setup, steps, per-step element counts, beta.dat records [n][33],
+    dbeta [16 N] after the first step, dbeta after the last step)."""
+    z = np.load(path)
+    setup = _setup_from(z, os.path.basename(path))
+    return (setup, int(z["nsteps"]), z["surf_counts"], z["beta_rec"], z["dbeta_first"],
+            z["dbeta_last"])
+
+
+def _setup_from(z, name):
+    nx, ny, nz = (int(v) for v in z["grid_n"])
+    g = W.Grid(nx, ny, nz, *(float(v) for v in z["grid_b"]))
+    eos = W.EosTable(kind=1, egrid=z["eos_egrid"], ngrid=z["eos_ngrid"], p=z["eos_p"],
+                     T=z["eos_T"], mub=z["eos_mub"])
+    tr = dict(zip(W.TR_FIELDS, (float(v) for v in z["tr"])))
+    tau0, dt, ecrit = (float(v) for v in z["clock"])
+    return W.Setup(name, g, eos, tr, int(z["tr_params"][0]), int(z["tr_params"][1]), tau0, dt,
+                   ecrit, z["Q0"], z["m0"])
+
+
 CORONA_CASES = {
     # name: setup factory; Fluid::outputCorona at tau0
     "corona_glauber_41x41x21": lambda: W.small_glauber3d(41, 21),
@@ -271,6 +333,10 @@ if __name__ == "__main__":
     for name, (fac, n) in SURFACE_CASES.items():
         if not only or name in only:
             save_surface_case(name, fac(), n)
+            print("wrote", name)
+    for name, (fac, n) in VORTICITY_CASES.items():
+        if not only or name in only:
+            save_vorticity_case(name, fac(), n)
             print("wrote", name)
     for name, fac in CORONA_CASES.items():
         if not only or name in only:
