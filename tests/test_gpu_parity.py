@@ -29,10 +29,10 @@ from vhlle_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-# end-state fixtures (the surface_* and corona_* fixtures hold freeze-out
-# records instead)
+# end-state fixtures (the surface_*, corona_* and vorticity_* fixtures hold
+# freeze-out and beta.dat records instead)
 CASES = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*_*x*.npz"))
-               if not os.path.basename(p).startswith(("surface_", "corona_")))
+               if not os.path.basename(p).startswith(("surface_", "corona_", "vorticity_")))
 FIELDS = ("Q", "Qh", "Qprev", "pi", "piH", "Pi", "PiH", "m", "vcc")
 
 

@@ -11,10 +11,10 @@ from helpers import compare_states
 from make_golden import load_case
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-# end-state fixtures (the surface_* and corona_* fixtures hold freeze-out
-# records instead)
+# end-state fixtures (the surface_*, corona_* and vorticity_* fixtures hold
+# freeze-out and beta.dat records instead)
 CASES = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*_*x*.npz"))
-               if not os.path.basename(p).startswith(("surface_", "corona_")))
+               if not os.path.basename(p).startswith(("surface_", "corona_", "vorticity_")))
 
 
 @pytest.mark.parametrize("path", CASES, ids=[os.path.basename(p) for p in CASES])
