@@ -279,6 +279,28 @@ vh_status vh_surface_device(vh_ctx *ctx, const double **rec, long *n);
  * when extendFO). */
 vh_status vh_surface_write(vh_ctx *ctx, const char *path, int extendFO);
 
+/* Vorticity.  Replaces Hydro::enableVorticity (src/hdo.cpp:60-64, with
+ * Fluid::enableVorticity, src/fld.h:44-52): from the next viscous step on,
+ * every step stores d_mu beta_nu (beta = u / T) per cell as ISformal does
+ * (src/hdo.cpp:381-611, 682-727), and vh_surface also computes the beta.dat
+ * values of its elements.  on = 0 stops the per-step work (the stored
+ * values stay).  Cells start at zero, and again after vh_resize2x. */
+vh_status vh_enable_vorticity(vh_ctx *ctx, int on);
+/* Cell::getDbeta of every cell (src/cll.h:199-204): out[(4 mu + nu) * N +
+ * i], clamped to [-100, 100] as Cell::setDbeta stores it.  Synchronous. */
+vh_status vh_get_dbeta(vh_ctx *ctx, double *out);
+/* The last vh_surface call's 16 Cartesian d_i beta_j per element (the
+ * beta.dat columns 17-32, src/fld.cpp:798-831), out[min(n, max)][16];
+ * *n = the element count.  Synchronous. */
+vh_status vh_surface_beta(vh_ctx *ctx, double *out, long max, long *n);
+/* Appends the last vh_surface call's elements (none after a vh_corona call)
+ * to a text file as beta.dat lines (src/fld.cpp:663-669, 741-745, 826-830:
+ * position, dSigma, u, T, muB, muQ, muS, the 16 d_i beta_j, e; 15
+ * significant digits, width 24); header != 0
+ * first writes Fluid::printDbetaHeader's three lines (src/fld.cpp:174-188),
+ * which need a vh_corona call before (its element count is in them). */
+vh_status vh_surface_write_beta(vh_ctx *ctx, const char *path, int header);
+
 /* Cornelius::find_surface_4d (src/cornelius.cpp:2247-2285) on n independent
  * hypercubes, on the device: cubes[k][16] corner values (index it*8 + jx*4 +
  * jy*2 + jz, dimension 0 is time), cell sizes dx[4], iso-value e0.

@@ -136,6 +136,10 @@ def save_vorticity_case(name, setup, nsteps):
     r.enable_vorticity()
     counts, dbeta = [], []
     with tempfile.TemporaryDirectory() as d:
+        # the driver's order (src/main.cpp:385-391): outputCorona at tau0,
+        # then the beta.dat header with its element count
+        ncorona, _ = r.output_corona(d)
+        assert r.print_dbeta_header()
         for k in range(nsteps):
             r.step(1)
             if k in (0, nsteps - 1):
@@ -144,10 +148,13 @@ def save_vorticity_case(name, setup, nsteps):
             counts.append(n)
         r.close()
         beta = read_beta(os.path.join(d, "beta.dat"))
+        with open(os.path.join(d, "beta.dat"), "rb") as f:
+            header = b"".join(f.readline() for _ in range(3))
     assert beta.shape[0] == sum(counts)
     arrays = _setup_arrays(setup)
     arrays.update(nsteps=np.array(nsteps), surf_counts=np.array(counts), beta_rec=beta,
-                  dbeta_first=dbeta[0], dbeta_last=dbeta[1])
+                  dbeta_first=dbeta[0], dbeta_last=dbeta[1], corona_count=np.array(ncorona),
+                  beta_header=np.frombuffer(header, dtype=np.uint8))
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
 
 
@@ -158,6 +165,12 @@ def load_vorticity_case(path):
     setup = _setup_from(z, os.path.basename(path))
     return (setup, int(z["nsteps"]), z["surf_counts"], z["beta_rec"], z["dbeta_first"],
             z["dbeta_last"])
+
+
+def load_beta_header(path):
+    """(outputCorona's element count at tau0, the beta.dat header bytes)."""
+    z = np.load(path)
+    return int(z["corona_count"]), z["beta_header"].tobytes()
 
 
 def _setup_from(z, name):

@@ -29,7 +29,8 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_records",
-           "vh_surface_device", "vh_surface_write", "vh_corona", "vh_cornelius4d", "vh_set_con2prim",
+           "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_get_dbeta",
+           "vh_surface_beta", "vh_surface_write_beta", "vh_corona", "vh_cornelius4d", "vh_set_con2prim",
            "vh_con2prim_stats", "vh_mlp_create", "vh_mlp_destroy", "vh_mlp_set_params",
            "vh_mlp_get_params", "vh_mlp_forward", "vh_mlp_grad", "vh_mlp_train",
            "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
@@ -295,6 +296,10 @@ def lib():
     L.vh_surface_records.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
+    L.vh_enable_vorticity.argtypes = [vp, ctypes.c_int]
+    L.vh_get_dbeta.argtypes = [vp, _dp]
+    L.vh_surface_beta.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
+    L.vh_surface_write_beta.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.vh_set_con2prim.argtypes = [vp, ctypes.c_double]
     L.vh_con2prim_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_ulonglong),
                                     ctypes.POINTER(ctypes.c_ulonglong)]
@@ -464,6 +469,31 @@ class GpuHydro:
             self._check(self.L.vh_surface_records(self.h, rec.ctypes.data_as(_dp), n,
                                                   ctypes.byref(got)))
         return rec, {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+
+    def enable_vorticity(self, on=True):
+        """Hydro::enableVorticity: dbeta per cell from the next viscous step."""
+        self._check(self.L.vh_enable_vorticity(self.h, int(on)))
+
+    def get_dbeta(self):
+        """Cell::getDbeta of every cell, [16][N] flattened (4 mu + nu)."""
+        out = np.zeros(16 * self.setup.grid.ncells)
+        self._check(self.L.vh_get_dbeta(self.h, out.ctypes.data_as(_dp)))
+        return out
+
+    def surface_beta(self, ecrit=None):
+        """surface() plus the elements' 16 Cartesian d_mu beta_nu of the
+        beta.dat lines: (records [n][29], info dict, beta [n][16])."""
+        rec, info = self.surface(ecrit)
+        n = len(rec)
+        beta = np.zeros((n, 16))
+        if n:
+            got = ctypes.c_long()
+            self._check(self.L.vh_surface_beta(self.h, beta.ctypes.data_as(_dp), n,
+                                               ctypes.byref(got)))
+        return rec, info, beta
+
+    def surface_write_beta(self, path, header=False):
+        self._check(self.L.vh_surface_write_beta(self.h, path.encode(), int(header)))
 
     def set_con2prim(self, tol):
         self._check(self.L.vh_set_con2prim(self.h, tol))

@@ -450,6 +450,7 @@ static vh::StepArgs step_args(vh_ctx* ctx) {
   a.f = ctx->f;
   a.clk = ctx->clk;  // holds (tau, dt): set when the host changes them, advanced per step
   a.viscous = ctx->viscous;
+  a.vort = ctx->vort_on && ctx->viscous ? &ctx->vort : nullptr;
   return a;
 }
 
@@ -701,6 +702,8 @@ vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
   VH_CUDA(ctx, cudaGetLastError());
   ctx->fluid_dt = dt2;  // the new Fluid's step, src/main.cpp:254-256
   ctx->EtotSurf = ctx->vEff = 0.;  // members of the new Fluid, src/fld.cpp:110-111
+  if (ctx->vort.dbeta)  // the new Fluid's cells start from zero (src/main.cpp:257,264-265)
+    VH_CUDA(ctx, cudaMemsetAsync(ctx->vort.dbeta, 0, sizeof(double) * 16 * g.N, ctx->stream));
   ctx->version++;
   if (resized) *resized = 1;
   return VH_OK;
@@ -826,6 +829,11 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
     vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
                              ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
                              S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
+    if (ctx->vort_on) {  // beta.dat lines (src/fld.cpp:663-669, 798-831)
+      if ((st = dgrow(ctx, &ctx->surf_beta, &ctx->cap_beta, want_e * 16))) return st;
+      vh::launch_surf_beta(g, ctx->vort.dbeta, ctx->grid.etamin, S.cubes, S.counters, cap_c,
+                           cap_e, S.geo, S.cnt, ctx->surf_beta, s);
+    }
     VH_CUDA(ctx, cudaGetLastError());
     VH_CUDA(ctx, cudaMemcpyAsync(H.cnt, S.counters, sizeof H.cnt, cudaMemcpyDeviceToHost, s));
     VH_CUDA(ctx, cudaMemcpyAsync(H.acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
@@ -842,6 +850,7 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   const unsigned bits = H.bits;
   const double* acc = H.acc;
   S.nel = nel;
+  ctx->beta_nel = ctx->vort_on ? nel : 0;
   ctx->EtotSurf += acc[1];
   ctx->nbSurf += acc[2];
   ctx->vEff += acc[3];
@@ -896,6 +905,8 @@ vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   }
   const double* acc = H.acc;
   S.nel = H.cnt[0];
+  ctx->corona_cells = H.cnt[0];  // Fluid::num_corona_cells, src/fld.cpp:1071
+  ctx->beta_nel = 0;             // the corona writes no beta.dat lines
   ctx->EtotSurf += acc[1];
   ctx->nbCorona += acc[2];
   ctx->vEff += acc[3];
@@ -947,6 +958,97 @@ vh_status vh_surface_write(vh_ctx* ctx, const char* path, int extendFO) {
     out << std::endl;
   }
   return out ? VH_OK : fail(ctx, VH_ERR_ARG, "vh_surface_write: write failed");
+}
+
+vh_status vh_enable_vorticity(vh_ctx* ctx, int on) {
+  if (!ctx) return VH_ERR_ARG;
+  const long long N = ctx->g.N;
+  if (N > INT32_MAX) return fail(ctx, VH_ERR_ARG, "vh_enable_vorticity: grid too large");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::VortDev& v = ctx->vort;
+  if (on && !v.dbeta) {
+    vh_status st;
+    if ((st = dalloc(ctx, &v.dbeta, (size_t)16 * N)) || (st = dalloc(ctx, &v.TD, (size_t)N)) ||
+        (st = dalloc(ctx, &v.val, (size_t)18 * N)) || (st = dalloc(ctx, &v.R, (size_t)2 * N)) ||
+        (st = dalloc(ctx, &v.flag, (size_t)N)) || (st = dalloc(ctx, &v.last, (size_t)5 * N)) ||
+        (st = dalloc(ctx, &v.agg, (size_t)5 * vh::vort_scan_blocks(N))))
+      return st;
+    // Cell::enableVorticity, src/cll.h:167-170: dbeta starts at zero
+    VH_CUDA(ctx, cudaMemsetAsync(v.dbeta, 0, sizeof(double) * 16 * N, ctx->stream));
+  }
+  if ((on != 0) != ctx->vort_on) {
+    ctx->vort_on = on != 0;
+    ctx->version++;  // the captured step changes
+  }
+  return VH_OK;
+}
+
+vh_status vh_get_dbeta(vh_ctx* ctx, double* out) {
+  if (!ctx || !out) return VH_ERR_ARG;
+  if (!ctx->vort.dbeta) return fail(ctx, VH_ERR_STATE, "vh_get_dbeta: vorticity never enabled");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  VH_CUDA(ctx, cudaMemcpyAsync(out, ctx->vort.dbeta, sizeof(double) * 16 * ctx->g.N,
+                               cudaMemcpyDeviceToHost, ctx->stream));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return VH_OK;
+}
+
+vh_status vh_surface_beta(vh_ctx* ctx, double* out, long max, long* n) {
+  if (!ctx || (!out && max > 0)) return VH_ERR_ARG;
+  if (!ctx->vort_on) return fail(ctx, VH_ERR_STATE, "vh_surface_beta: vorticity is off");
+  const long k = (long)std::min<long long>(ctx->beta_nel, std::max(0L, max));
+  if (n) *n = (long)ctx->beta_nel;
+  if (k > 0) {
+    if (!ctx->surf_beta || ctx->cap_beta < (size_t)k * 16)
+      return fail(ctx, VH_ERR_STATE, "vh_surface_beta: no vh_surface call with vorticity on");
+    VH_CUDA(ctx, cudaSetDevice(ctx->device));
+    VH_CUDA(ctx, cudaMemcpyAsync(out, ctx->surf_beta, sizeof(double) * 16 * k,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return VH_OK;
+}
+
+vh_status vh_surface_write_beta(vh_ctx* ctx, const char* path, int header) {
+  if (!ctx || !path) return VH_ERR_ARG;
+  std::ofstream out(path, std::ios::app);
+  if (!out) return fail(ctx, VH_ERR_ARG, std::string("vh_surface_write_beta: cannot open ") + path);
+  if (header) {
+    // Fluid::printDbetaHeader, src/fld.cpp:174-188 (the reference throws
+    // before outputCorona has counted the corona cells)
+    if (ctx->corona_cells < 0)
+      return fail(ctx, VH_ERR_STATE, "vh_surface_write_beta: no vh_corona call yet (header)");
+    out << "# The derivatives of \u03b2 are given in Cartesian coordinates and include a "
+           "factor of 1/2, such that \u2202\u2098\u03b2\u2099=1/2 * "
+           "\u2202\u2098(u\u2099/T)"
+        << std::endl;
+    out << "# Number of corona cells: " << ctx->corona_cells << std::endl;
+    out << "#  \u03c4  x  y  \u03b7  d\u03a3[0]  d\u03a3[1]  d\u03a3[2]  d\u03a3[3]  "
+        << "u[0]  u[1]  u[2]  u[3]  T  \u03bcB  \u03bcQ  \u03bcS  "
+        << "\u2202\u2080\u03b2\u2080  \u2202\u2080\u03b2\u2081  \u2202\u2080\u03b2\u2082  "
+           "\u2202\u2080\u03b2\u2083  \u2202\u2081\u03b2\u2080  \u2202\u2081\u03b2\u2081  "
+           "\u2202\u2081\u03b2\u2082  \u2202\u2081\u03b2\u2083  "
+        << "\u2202\u2082\u03b2\u2080  \u2202\u2082\u03b2\u2081  \u2202\u2082\u03b2\u2082  "
+           "\u2202\u2082\u03b2\u2083  \u2202\u2083\u03b2\u2080  \u2202\u2083\u03b2\u2081  "
+           "\u2202\u2083\u03b2\u2082  \u2202\u2083\u03b2\u2083  \u03f5"
+        << std::endl;
+  }
+  const long n = (long)ctx->beta_nel;
+  if (n > 0) {
+    std::vector<double> rec((size_t)n * vh::kSurfRec), beta((size_t)n * 16);
+    vh_status st = vh_surface_records(ctx, rec.data(), n, nullptr);
+    if (st == VH_OK) st = vh_surface_beta(ctx, beta.data(), n, nullptr);
+    if (st != VH_OK) return st;
+    // src/fld.cpp:663-669, 741-745, 826-830: precision 15, width 24
+    out.precision(15);
+    for (long i = 0; i < n; i++) {
+      const double* r = rec.data() + (size_t)i * vh::kSurfRec;
+      for (int c = 0; c < 16; c++) out << std::setw(24) << r[c];
+      for (int c = 0; c < 16; c++) out << std::setw(24) << beta[(size_t)i * 16 + c];
+      out << std::setw(24) << r[27] << std::endl;
+    }
+  }
+  return out ? VH_OK : fail(ctx, VH_ERR_ARG, "vh_surface_write_beta: write failed");
 }
 
 vh_status vh_cornelius4d(const double* cubes, long n, const double* dx, double e0, int device,

@@ -50,6 +50,13 @@ struct vh_ctx {
   // new Fluid), nbSurf is a function static in the reference (never reset)
   double EtotSurf = 0., vEff = 0., nbSurf = 0.;
   double nbCorona = 0.;  // outputCorona's own function static (src/fld.cpp:877)
+  // vorticity (Hydro::enableVorticity): buffers allocated on the first enable
+  bool vort_on = false;
+  vh::VortDev vort{};
+  double* surf_beta = nullptr;  // [cap][16] beta.dat values of the last vh_surface
+  size_t cap_beta = 0;
+  long long beta_nel = 0;       // its element count (0 after vh_corona)
+  long long corona_cells = -1;  // elements of the last vh_corona (the beta.dat header)
   struct Surf {
     double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
            *partial = nullptr;

@@ -1079,7 +1079,8 @@ static inline unsigned nblk(long long n, int bs) { return (unsigned)((n + bs - 1
 
 const char* const kKernelNames[KK_COUNT] = {
     "k_update_m", "k_face_x", "k_face_y", "k_face_z", "k_update", "k_ghost",
-    "k_visc_prims", "k_is_relax", "k_is_advect", "k_visc_update"};
+    "k_visc_prims", "k_is_relax", "k_is_advect", "k_visc_update",
+    "vorticity (k_vort_*, 6 kernels)"};
 
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   const Geo& g = a.g;
@@ -1131,6 +1132,10 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
     k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
                                    F.pBC, a.clk, F.gdst);
     done(KK_VISC_PRIMS);
+    if (a.vort) {
+      launches += launch_vorticity(a, s) - 1;
+      done(KK_VORT);
+    }
     // the relaxation on full warps of cells with matter (the list kernel's
     // time is counted with the relaxation's)
     cudaMemsetAsync(F.nactive, 0, sizeof(int), s);

@@ -57,6 +57,18 @@ struct Fields {
   unsigned *err;                 // device error word
 };
 
+// Device buffers of the vorticity output (Hydro::enableVorticity).
+struct VortDev {
+  double* dbeta;        // [16][N] d_mu beta_nu per cell (4 mu + nu), clamped
+  double* TD;           // [N] T at the prims of Qh at tau_{n+1}
+  double* val;          // [18][N] the 16 values NSquant writes, the 2 increments
+  double* R;            // [2][N] running M[3][0], M[3][3] at lone increments
+  unsigned char* flag;  // [N] VF_* bits
+  int* last;            // [5][N] per loop position: last writer positions
+  int* agg;             // [5][blocks] block maxima, then their prefixes
+};
+int vort_scan_blocks(long long N);
+
 struct StepArgs {
   Geo g;
   EosDev eos;
@@ -66,12 +78,17 @@ struct StepArgs {
   bool viscous;
   int block = 128;    // threads per block of the step kernels (64 or 128; the
                       // relaxation kernel always uses 128)
+  const VortDev* vort = nullptr;  // vorticity on (viscous steps only)
 };
+
+// ISformal's dbeta for every cell (after k_visc_prims, before the viscous
+// update changes Q); returns the number of launches
+int launch_vorticity(const StepArgs& a, cudaStream_t s);
 
 // Kernel kinds, for per-kernel timing.
 enum KernelKind {
   KK_UPDATE_M = 0, KK_FACE_X, KK_FACE_Y, KK_FACE_Z, KK_UPDATE, KK_GHOST, KK_VISC_PRIMS,
-  KK_IS_RELAX, KK_IS_ADVECT, KK_VISC_UPDATE, KK_COUNT
+  KK_IS_RELAX, KK_IS_ADVECT, KK_VISC_UPDATE, KK_VORT, KK_COUNT
 };
 extern const char* const kKernelNames[KK_COUNT];
 

@@ -210,13 +210,6 @@ __global__ void k_surf_energy(Geo g, EosDev E, const double* __restrict__ Q,
   eP[i] = P.e;
 }
 
-__device__ __forceinline__ void cube_cell(const Geo& g, long long t, int& ix, int& iy, int& iz) {
-  const int niz = g.nz - 4, niy = g.ny - 4;
-  iz = 2 + (int)(t % niz);
-  iy = 2 + (int)((t / niz) % niy);
-  ix = 2 + (int)(t / ((long long)niz * niy));
-}
-
 __device__ __forceinline__ void load_cube(const Geo& g, const double* __restrict__ eN,
                                           const double* __restrict__ eP, int ix, int iy, int iz,
                                           double* hc) {

@@ -19,6 +19,14 @@ constexpr int kSurfAcc = 5;
 constexpr int kSurfMaxElemPerCube = 10;
 constexpr int kSurfGeo = 8;
 
+// interior cube t (loop order, iz fastest) -> its lowest corner cell
+__device__ __forceinline__ void cube_cell(const Geo& g, long long t, int& ix, int& iy, int& iz) {
+  const int niz = g.nz - 4, niy = g.ny - 4;
+  iz = 2 + (int)(t % niz);
+  iy = 2 + (int)((t / niz) % niy);
+  ix = 2 + (int)(t / ((long long)niz * niy));
+}
+
 int totals_blocks(const Geo& g);
 void launch_totals(const Geo& g, const EosDev& E, const Fields& f, double tau, double ecrit,
                    double etamin, bool viscous, double* partial, double* out, cudaStream_t s);
@@ -53,6 +61,13 @@ void launch_corona(const Geo& g, const EosDev& E, const Fields& f, double tau, d
                    double xmin, double ymin, double zmin, const double* eN, unsigned char* flag,
                    int* blk, int* counters, int* cubes, int cap, double* rec, double* contrib,
                    double* partial, int npartial, cudaStream_t s);
+
+// beta.dat's 16 Cartesian d_mu beta_nu of each element of the last
+// launch_surf_elements call (same cubes, counters, geo and offsets), from
+// the cells' dbeta[16][N], into beta[cap_el][16]
+void launch_surf_beta(const Geo& g, const double* dbeta, double zmin, const int* cubes,
+                      const int* counters, int cap_cubes, int cap_el, const double* geo,
+                      const int* off, double* beta, cudaStream_t s);
 
 // Cornelius on n independent hypercubes (16 corner values each): counts[k]
 // elements (-1 where the reference stops), geo[k][10][8] centroid + normal
