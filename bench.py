@@ -375,6 +375,9 @@ def main():
                     help="events of the batched-vs-plain measurement (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--no-learned-guess", action="store_true")
+    ap.add_argument("--vorticity", action="store_true",
+                    help="the event with Hydro::enableVorticity (dbeta every step, beta.dat "
+                         "values at every surface)")
     ap.add_argument("--grid", default="101,101,51",
                     help="nx,ny,nz of the event (smaller grids only for profiler captures)")
     args = ap.parse_args()
@@ -391,6 +394,8 @@ def main():
     setup = W.glauber3d_setup(nx, ny, nz, seed=20260001 + rank)
     cells = setup.grid.ncells
     h = capi.GpuHydro(setup, device=local)
+    if args.vorticity:
+        h.enable_vorticity()
     lps = h.launches_per_step()
 
     # warm-up on the event itself, then restart the event for the timed run
@@ -524,6 +529,7 @@ def main():
                        "path": "plain FP64 step + device freeze-out surface every %d steps "
                                "(no MLP guess, single event per GPU)" % SURF_EVERY,
                        "parallelism": "events%d" % ws,
+                       "vorticity": bool(args.vorticity),
                        "l2": "inputs larger than L2 (%.0f MB of resident fields)" % (
                            cells * 8 * 127 / 1e6)},
             "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,

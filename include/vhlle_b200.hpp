@@ -352,12 +352,14 @@ class Hydro {
   int device_;
   double t0_, dt0_;
   bool uploaded_ = false;
+  bool vorticity_ = false;
 
   void create() {
     const vh_grid g = f_->grid();
     const vh_eos e = eos_->descriptor();
     const vh_trcoeff t = tr_->descriptor();
     check(vh_create(&g, &e, &t, t0_, dt0_, device_, &ctx_), nullptr);
+    if (vorticity_) check(vh_enable_vorticity(ctx_, 1), ctx_);  // new cells: zero dbeta
   }
 
  public:
@@ -434,6 +436,19 @@ class Hydro {
   }
   void writeSurface(const char* path, bool extendFO) {
     check(vh_surface_write(ctx_, path, extendFO ? 1 : 0), ctx_);
+  }
+  // Hydro::enableVorticity (src/hdo.cpp:60-64): every later viscous step
+  // stores d_mu beta_nu per cell, and surface() computes the beta.dat values.
+  void enableVorticity() {
+    vorticity_ = true;
+    check(vh_enable_vorticity(ctx_, 1), ctx_);
+  }
+  // Cell::getDbeta of every cell: out[(4 mu + nu) * N + i] (16 N doubles).
+  void getDbeta(double* out) { check(vh_get_dbeta(ctx_, out), ctx_); }
+  // Appends the last surface() call's beta.dat lines to `path`; with header,
+  // Fluid::printDbetaHeader's lines first (after corona(), src/main.cpp:391).
+  void writeBeta(const char* path, bool header) {
+    check(vh_surface_write_beta(ctx_, path, header ? 1 : 0), ctx_);
   }
   // The driver's substep block (src/main.cpp:405-419); returns the count.
   int advance(double dtau, double etamin, double etamax, int nz) {

@@ -156,3 +156,52 @@ def test_cpp_driver_loop_equals_oracle(tmp_path):
     assert fz.shape == ref.shape
     ok = np.abs(fz - ref) <= 1e-12 * np.maximum(np.abs(fz), np.abs(ref)) + 1e-300
     assert ok.all(), np.argwhere(~ok)[:5]
+
+
+def test_cpp_driver_vorticity_equals_oracle(tmp_path):
+    """vhlle_run with the params key `vorticity 1` (src/main.cpp:135,
+    379-391): DIR/beta.dat holds Fluid::printDbetaHeader's lines after the
+    corona, then every iteration's beta.dat lines, through the substeps and
+    the x2 resize; they match the oracle's to 1e-12 (15 printed digits,
+    plus a floor for the Jacobian's cosh/sinh cancellation)."""
+    import subprocess
+    from vhlle_b200 import build as B
+    drv = B.build_driver()
+    setup = W.small_glauber3d(17, 9, tau0=0.05, dt=0.1)
+    ic = str(tmp_path / "ic.vhb")
+    W.write_snapshot(ic, setup.grid, setup.tau0, setup.dt, W.initial_snapshot_state(setup))
+    params = str(tmp_path / "params.txt")
+    tau_max, tau_resize = 0.55, 0.3
+    W.write_params(params, setup, tauMax=tau_max, tauGridResize=tau_resize, vorticity=1,
+                   eos1fFile=str(tmp_path / "eos.dat"))
+    setup.eos.write_eos1f(str(tmp_path / "eos.dat"))
+    out = tmp_path / "out"
+    run = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", str(out)],
+                         capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr
+    assert "grid resize" in run.stdout
+
+    o = P.OracleRun(setup, vorticity=True)
+    g = setup.grid
+    corona, _ = o.corona()
+    rows, resized = [], False
+    while True:
+        o.advance(setup.dt, g.etamin, g.etamax, g.nz)
+        r, _, beta = o.surface_beta(dtf=o.dt)
+        rows.append(np.concatenate([r[:, :16], beta, r[:, 27:28]], axis=1))
+        if o.tau_now >= tau_resize and not resized:
+            assert o.resize2x() == 1
+            resized = True
+        if not (o.tau_now < tau_max + 0.0001 and len(r) > 0):
+            break
+    with open(out / "beta.dat") as f:
+        head = [f.readline() for _ in range(3)]
+    assert head[0].startswith("# The derivatives of") and all(h.startswith("#") for h in head)
+    assert head[1].strip() == "# Number of corona cells: %d" % len(corona)
+    from make_golden import read_beta
+    got = read_beta(str(out / "beta.dat"))
+    exp = np.concatenate(rows)
+    assert got.shape == exp.shape and len(exp) > 0
+    scale = np.maximum(np.abs(got[:, 16:32]).max(axis=1), np.abs(exp[:, 16:32]).max(axis=1))[:, None]
+    ok = np.abs(got - exp) <= 1e-12 * np.maximum(np.abs(got), np.abs(exp)) + 1e-13 * scale + 1e-300
+    assert ok.all(), np.argwhere(~ok)[:5]

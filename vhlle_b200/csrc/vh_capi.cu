@@ -743,10 +743,10 @@ vh_status vh_sync(vh_ctx* ctx) {
 vh_status vh_launches_per_step(vh_ctx* ctx, int* n) {
   if (!ctx || !n) return VH_ERR_ARG;
   // update_m, 2 x (faces + update), 2 ghost, the viscous five (prims, the
-  // relaxation's list and relaxation, advection, update), the MLP guess,
-  // the clock
+  // relaxation's list and relaxation, advection, update) and the six of the
+  // vorticity, the MLP guess, the clock
   int k = 1 + 2 * (2 + (ctx->g.nz > 1 ? 1 : 0) + 1) + 1 + (ctx->viscous ? 5 : 0) + 1 +
-          (ctx->mlp ? 1 : 0) + 1;
+          (ctx->viscous && ctx->vort_on ? 6 : 0) + (ctx->mlp ? 1 : 0) + 1;
   *n = k;
   return VH_OK;
 }

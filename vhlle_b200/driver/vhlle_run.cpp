@@ -15,7 +15,9 @@
 // freezeout.dat at the end) and prints the same line (tau, E, Efull,
 // nbSurf, S, EtotSurf, elements, suspicious elements, cut-cell fraction);
 // the loop stops at tauMax or when an iteration finds no element, as the
-// reference's does.  The final grid is written to DIR/final.vhb.
+// reference's does.  With the key vorticity set, DIR/beta.dat gets the
+// header after the corona and each iteration's beta.dat lines.  The final
+// grid is written to DIR/final.vhb.
 #include <sys/stat.h>
 
 #include <cmath>
@@ -113,6 +115,7 @@ int run(int argc, char** argv) {
   std::cout << "fluid allocation done\nIC done (tau0 = " << tau0 << ")\n";
 
   vhb::Hydro* h = new vhb::Hydro(f, eos, trcoeff, tau0, P.dtau);
+  if (P.vorticityOn) h->enableVorticity();  // src/main.cpp:379-382
   // Fluid::initOutput (src/fld.cpp:119-129): the output directory and a
   // fresh freezeout.dat.unfinished
   mkdir(cl.outputDir.c_str(), 0755);
@@ -120,6 +123,8 @@ int run(int argc, char** argv) {
   const std::string fo_unf = fo + ".unfinished";
   std::remove(fo.c_str());
   std::remove(fo_unf.c_str());
+  const std::string beta = cl.outputDir + "/beta.dat";  // src/fld.cpp:131-136
+  if (P.vorticityOn) std::remove(beta.c_str());
   bool resized = false;
   int nloops = 0;
   long nelements = 0;
@@ -139,6 +144,7 @@ int run(int argc, char** argv) {
               << std::setw(13) << ci.nbSurf << std::setw(13) << t.S << std::setw(13)
               << ci.EtotSurf << std::endl;
     std::cout << "corona elements : " << ci.nelements << std::endl;
+    if (P.vorticityOn) h->writeBeta(beta.c_str(), true);  // src/main.cpp:391
   }
   do {
     const int nSubSteps = h->advance(P.dtau, P.etamin, P.etamax, P.nz);
@@ -146,6 +152,7 @@ int run(int argc, char** argv) {
     const vhb::Totals t = h->totals();
     const vh_surface_info si = h->surface();
     h->writeSurface(fo_unf.c_str(), P.freezeoutExtend);
+    if (P.vorticityOn) h->writeBeta(beta.c_str(), false);
     nelements = si.nelements;
     // the line Fluid::outputSurface prints (src/fld.cpp:854-857)
     std::cout << std::setw(10) << h->getTau() << std::setw(13) << t.E << std::setw(13) << t.Efull
