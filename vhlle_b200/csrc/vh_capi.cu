@@ -230,6 +230,10 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     vh_destroy(c);
     return st;
   };
+  if ((e = vh::step_kernels_setup()) != cudaSuccess) {
+    cuda_fail(c, e, "vh_create: kernel attributes");
+    return bail(VH_ERR_CUDA);
+  }
   vh::Geo& g = c->g;
   g.nx = grid->nx;
   g.ny = grid->ny;

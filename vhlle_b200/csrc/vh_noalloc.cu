@@ -47,9 +47,10 @@ constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 void* g_scratch[kMaxDevices] = {nullptr};
 
-// Looks up the scratch array's device address for the current device, once
-// per device.  The first vh_step_noalloc call on a device does this, so that
-// first call should come before any stream capture on that device.
+// Looks up the scratch array's device address for the current device and
+// sets the step kernels' attributes, once per device.  The first
+// vh_step_noalloc call on a device does this, so that first call should
+// come before any stream capture on that device.
 cudaError_t scratch_for_current_device(unsigned char** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -60,6 +61,7 @@ cudaError_t scratch_for_current_device(unsigned char** out) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, vh_noalloc_scratch);
     if (e != cudaSuccess) return e;
+    if ((e = vh::step_kernels_setup()) != cudaSuccess) return e;
     g_scratch[dev] = p;
   }
   *out = static_cast<unsigned char*>(g_scratch[dev]);

@@ -418,8 +418,11 @@ __device__ __forceinline__ Prim loadA(const double* __restrict__ pA, long long N
 constexpr int kRelaxMinBlocks = 4;
 
 constexpr int kRelaxBlock = 128;
-// shared-memory rows of k_is_relax's relaxation loops: pi, sigma, u, h0, f0
-constexpr int kSmPI = 0, kSmSIG = 10, kSmU = 20, kSmH = 24, kSmF = 34, kSmRows = 44;
+// shared-memory rows of k_is_relax's relaxation loops: pi, sigma, u, h0, f0,
+// and phi7 h0^{kl} - tau_pipi sigma^{kl} of the second loop (dynamic shared
+// memory: 55 KB per block, four blocks per SM)
+constexpr int kSmPI = 0, kSmSIG = 10, kSmU = 20, kSmH = 24, kSmF = 34, kSmY = 44, kSmRows = 54;
+constexpr size_t kRelaxSmem = sizeof(double) * kSmRows * kRelaxBlock;
 
 // The empty cells' share of ISformal loop 1 (src/hdo.cpp:697-708: zero
 // pi0/piH0/Pi0/PiH0) and the list of the other cells, so that k_is_relax
@@ -696,7 +699,8 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
   // stream outgrew the instruction caches.  Operands indexed by a or b come
   // from shared memory ([component][thread]); the arithmetic of every term
   // is the reference's, in its order.
-  __shared__ double sm[kSmRows][kRelaxBlock];
+  extern __shared__ double relax_smem[];
+  double(*sm)[kRelaxBlock] = reinterpret_cast<double(*)[kRelaxBlock]>(relax_smem);
   const int t = threadIdx.x;
 #pragma unroll
   for (int k = 0; k < 10; k++) {
@@ -706,6 +710,10 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
   }
 #pragma unroll
   for (int k = 0; k < 4; k++) sm[kSmU + k][t] = u[k];
+  // phi7 pi^{kl} - tau_pipi sigma^{kl}, the same for every (a, b): in the
+  // rows loop 2 uses for f0 later
+#pragma unroll
+  for (int k = 0; k < 10; k++) sm[kSmF + k][t] = phi7 * cpi[k] - taupipi * sig[k];
 #pragma unroll 1
   for (int ab = 0; ab < 10; ab++) {
     const int a = ab >= 6 ? 3 : ab >= 3 ? 2 : ab >= 1 ? 1 : 0;
@@ -727,8 +735,7 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
 #pragma unroll
       for (int l = 0; l < 4; l++) {
         n[1 + 2 * l] = (-pak * ub - pbk * ua) * u[l] * dmu[l][k] * gk;
-        n[2 + 2 * l] =
-            1. / 3. * dab * PI(k, l) * (phi7 * PI(k, l) - taupipi * SIG(k, l)) * gk * gmumu[l];
+        n[2 + 2 * l] = 1. / 3. * dab * PI(k, l) * sm[kSmF + index44(k, l)][t] * gk * gmumu[l];
       }
       div_batch<9>(n, gamma, rg, gfast);
       acc += n[0] * 0.5 * dt;
@@ -779,6 +786,8 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
   f0[index44(3, 2)] += -(ddivp(vz, tau1) * H(0, 2)) * dt;
 #pragma unroll
   for (int k = 0; k < 10; k++) sm[kSmF + k][t] = f0[k];
+#pragma unroll
+  for (int k = 0; k < 10; k++) sm[kSmY + k][t] = phi7 * h0[k] - taupipi * sig[k];
 #pragma unroll 1
   for (int ab = 0; ab < 10; ab++) {
     const int a = ab >= 6 ? 3 : ab >= 3 ? 2 : ab >= 1 ? 1 : 0;
@@ -801,7 +810,7 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
 #pragma unroll
       for (int l = 0; l < 4; l++)
         n[1 + l] = (-hak * ub - hbk * ua) * u[l] * dmu[l][k] * gk -
-                   1. / 3. * dab * H(k, l) * (phi7 * H(k, l) - taupipi * SIG(k, l)) * gk * gmumu[l];
+                   1. / 3. * dab * H(k, l) * sm[kSmY + index44(k, l)][t] * gk * gmumu[l];
       div_batch<5>(n, gamma, rg, gfast);
       acc += n[0] * dt;
 #pragma unroll
@@ -1082,6 +1091,11 @@ const char* const kKernelNames[KK_COUNT] = {
     "k_visc_prims", "k_is_relax", "k_is_advect", "k_visc_update",
     "vorticity (k_vort_*, 6 kernels)"};
 
+cudaError_t step_kernels_setup() {
+  return cudaFuncSetAttribute(k_is_relax, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kRelaxSmem);
+}
+
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   const Geo& g = a.g;
   const int bs = a.block == 64 ? 64 : 128;
@@ -1142,7 +1156,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
     k_relax_list<<<nb128, 128, 0, s>>>(g, F.pA, F.active, F.nactive, F.pi0, F.piH0, F.Pi0,
                                        F.PiH0, F.flux);
     launches++;
-    k_is_relax<<<nb128, kRelaxBlock, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh,
+    k_is_relax<<<nb128, kRelaxBlock, kRelaxSmem, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, m, F.pA, F.pD, F.pTh,
                                              F.pBC, F.pi, F.Pi, F.pi0, F.piH0, F.Pi0, F.PiH0,
                                              F.flux, a.clk, F.err, F.active, F.nactive);
     done(KK_IS_RELAX);

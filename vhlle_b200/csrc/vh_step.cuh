@@ -98,6 +98,11 @@ struct LaunchMarker {
   virtual ~LaunchMarker() {}
 };
 
+// Function attributes the step kernels need (the relaxation's 55 KB of
+// dynamic shared memory), on the current device; before the first launch
+// there and outside any stream capture.
+cudaError_t step_kernels_setup();
+
 // Enqueues one performStep on stream s; returns the number of launches.
 // Leaves the updated fill fractions in f.m2 (the caller swaps m and m2).
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk = nullptr);
