@@ -274,6 +274,19 @@ vh_status vh_corona(vh_ctx *ctx, double ecrit, vh_surface_info *info);
 #define VH_SURF_REC 29
 vh_status vh_surface_records(vh_ctx *ctx, double *out, long max, long *n);
 vh_status vh_surface_device(vh_ctx *ctx, const double **rec, long *n);
+/* vh_surface in two halves, so that a caller can enqueue the next steps
+ * before it waits: vh_surface_begin enqueues the call's kernels and the copy
+ * of its counts and sums on the context stream and returns; vh_surface_end
+ * waits for them and fills `info` as vh_surface would (the records stay on
+ * the device until the next surface or corona call).  One call in flight per
+ * context; vh_surface, vh_corona and the record getters refuse while one is.
+ * The call runs with the buffers earlier calls left (64k hypercubes and
+ * twice as many elements at first, grown by any call that found more); if
+ * it finds more than they hold, vh_surface_end grows them and returns
+ * VH_ERR_STATE without results, since the fields have moved on by then
+ * (vh_surface, which re-runs on the same fields, has no such case). */
+vh_status vh_surface_begin(vh_ctx *ctx, double ecrit);
+vh_status vh_surface_end(vh_ctx *ctx, vh_surface_info *info);
 /* Appends the last call's elements to a text file as freezeout.dat lines
  * (src/fld.cpp:658-797: 15 significant digits, width 24; e and nb only
  * when extendFO). */

@@ -241,3 +241,74 @@ def test_gpu_corona_full_size_event_equals_oracle():
     assert infos["nelements"] == len(rs)
     assert abs(infos["EtotSurf"] - (etot + accs["EtotSurf"])) <= 1e-10 * abs(etot) + 1e-8
     d.close()
+
+
+def _records(d, n):
+    import ctypes
+    from vhlle_b200 import capi
+    rec = np.zeros((n, capi.SURF_REC))
+    if n:
+        got = ctypes.c_long()
+        d._check(d.L.vh_surface_records(d.h, rec.ctypes.data_as(capi._dp), n, ctypes.byref(got)))
+    return rec
+
+
+def test_gpu_surface_pipelined_equals_synchronous():
+    """vh_surface_begin / vh_surface_end, with the next step enqueued
+    between them, give what vh_surface gives on the same state: counts,
+    nsusp, the carried EtotSurf / nbSurf / vEff and every record, bit for
+    bit.  Out-of-order calls are refused."""
+    from vhlle_b200.capi import GpuHydro, VhError
+    setup = W.small_glauber3d(33, 17, seed=11, b=6.0)
+    a, b = GpuHydro(setup), GpuHydro(setup)
+    with pytest.raises(VhError):
+        b.surface_end()
+    expect = None
+    n_checked = 0
+    for k in range(1, 10):
+        a.step(1)
+        b.step(1)
+        if expect is not None:
+            info = b.surface_end()
+            assert info == expect[1], (k, info, expect[1])
+            assert np.array_equal(_records(b, info["nelements"]), expect[0])
+            n_checked += info["nelements"]
+            expect = None
+        if k % 2 == 0:
+            expect = a.surface()
+            b.surface_begin()
+            with pytest.raises(VhError):
+                b.surface_begin()
+            with pytest.raises(VhError):
+                b.surface()
+    with pytest.raises(VhError):  # the last call was collected in the loop
+        b.surface_end()
+    assert n_checked > 500
+    a.close()
+    b.close()
+
+
+def test_gpu_surface_pipelined_overflow_is_reported():
+    """A pipelined call that finds more than the buffers hold reports it
+    (VH_ERR_STATE, buffers grown); vh_surface then gives the full result,
+    and the next pipelined call fits."""
+    from vhlle_b200.capi import GpuHydro, VhError
+    setup = _ripple_setup()
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    o.step(1)
+    d.step(1)
+    d.surface_begin()
+    with pytest.raises(VhError):
+        d.surface_end()
+    rd, info = d.surface()
+    ro, _ = o.surface(cap=4000000)
+    assert len(ro) == info["nelements"] > 150000
+    assert rec_close(rd, ro).all()
+    o.step(1)
+    d.step(1)
+    d.surface_begin()
+    info = d.surface_end()
+    ro, _ = o.surface(cap=4000000)
+    assert len(ro) == info["nelements"]
+    assert rec_close(_records(d, info["nelements"]), ro).all()
+    d.close()

@@ -28,7 +28,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_abi_version", "vh_transform_pv", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
-           "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_records",
+           "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
            "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_get_dbeta",
            "vh_surface_beta", "vh_surface_write_beta", "vh_corona", "vh_cornelius4d", "vh_set_con2prim",
            "vh_con2prim_stats", "vh_mlp_create", "vh_mlp_destroy", "vh_mlp_set_params",
@@ -293,6 +293,8 @@ def lib():
     L.vh_resize2x.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.vh_surface.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
     L.vh_corona.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
+    L.vh_surface_begin.argtypes = [vp, ctypes.c_double]
+    L.vh_surface_end.argtypes = [vp, ctypes.POINTER(VhSurfaceInfo)]
     L.vh_surface_records.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_device.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
@@ -551,6 +553,17 @@ class GpuHydro:
         info = VhSurfaceInfo()
         ec = self.setup.ecrit if ecrit is None else ecrit
         self._check(self.L.vh_surface(self.h, ec, ctypes.byref(info)))
+        return {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+
+    def surface_begin(self, ecrit=None):
+        """vh_surface_begin: enqueue a surface call; results at surface_end()."""
+        ec = self.setup.ecrit if ecrit is None else ecrit
+        self._check(self.L.vh_surface_begin(self.h, ec))
+
+    def surface_end(self):
+        """vh_surface_end: the info dict of the pending surface call."""
+        info = VhSurfaceInfo()
+        self._check(self.L.vh_surface_end(self.h, ctypes.byref(info)))
         return {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
 
     def surface_write(self, path, extend=False):

@@ -182,6 +182,7 @@ vh_status vh_destroy(vh_ctx* ctx) {
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->surf.host) cudaFreeHost(ctx->surf.host);
   for (cudaEvent_t e : ctx->evpool) cudaEventDestroy(e);
+  if (ctx->surf_ev) cudaEventDestroy(ctx->surf_ev);
   if (ctx->t0) cudaEventDestroy(ctx->t0);
   if (ctx->t1) cudaEventDestroy(ctx->t1);
   delete ctx;
@@ -798,58 +799,73 @@ static vh_status surf_common(vh_ctx* ctx) {
   return VH_OK;
 }
 
-vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
-  if (!ctx) return VH_ERR_ARG;
-  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_surface: no state uploaded");
-  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+// One pass of outputSurface's element search on the context stream with
+// buffers for want_c hypercubes and want_e elements: the nine kernels, the
+// beta.dat values when vorticity is on, and the copies of the counts, sums
+// and error bits into the pinned host block.  Nothing waits.
+static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t want_e) {
   const vh::Geo& g = ctx->g;
   vh_ctx::Surf& S = ctx->surf;
   vh_status st;
-  if ((st = surf_common(ctx))) return st;
-  // Every stage reads the counts from device memory, so the call waits for
-  // the GPU once, at the end.  The buffers start at 64k cubes and twice as
-  // many elements; a call that finds more grows them and runs again (the
-  // fields it reads are unchanged in between, so the result is the same).
-  const long long ninterior = std::max(1LL, vh::surf_ncube(g));
-  size_t want_c = std::max<size_t>(S.cap_cubes, (size_t)std::min(ninterior, 65536LL));
-  size_t want_e = std::max<size_t>(S.cap_rec / vh::kSurfRec, 2 * want_c);
+  if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, want_c)) ||
+      (st = dgrow(ctx, &S.geo, &S.cap_geo, want_c * vh::kSurfMaxElemPerCube * vh::kSurfGeo)) ||
+      (st = dgrow(ctx, &S.cnt, &S.cap_cnt, want_c + 1)) ||
+      (st = dgrow(ctx, &S.rec, &S.cap_rec, want_e * vh::kSurfRec)) ||
+      (st = dgrow(ctx, &S.contrib, &S.cap_contrib, want_e * vh::kSurfAcc)))
+    return st;
+  if (ctx->vort_on && (st = dgrow(ctx, &ctx->surf_beta, &ctx->cap_beta, want_e * 16))) return st;
+  const int cap_c = (int)std::min<size_t>(want_c, INT32_MAX / 16);
+  const int cap_e = (int)std::min<size_t>(want_e, INT32_MAX / 32);
+  S.pass_cap_c = cap_c;
+  S.pass_cap_e = cap_e;
   cudaStream_t s = ctx->stream;
   const double taup = ctx->tau - ctx->fluid_dt;
   vh_ctx::Surf::Host& H = *S.host;
-  for (int pass = 0; pass < 2; pass++) {
-    if ((st = dgrow(ctx, &S.cubes, &S.cap_cubes, want_c)) ||
-        (st = dgrow(ctx, &S.geo, &S.cap_geo, want_c * vh::kSurfMaxElemPerCube * vh::kSurfGeo)) ||
-        (st = dgrow(ctx, &S.cnt, &S.cap_cnt, want_c + 1)) ||
-        (st = dgrow(ctx, &S.rec, &S.cap_rec, want_e * vh::kSurfRec)) ||
-        (st = dgrow(ctx, &S.contrib, &S.cap_contrib, want_e * vh::kSurfAcc)))
-      return st;
-    const int cap_c = (int)std::min<size_t>(want_c, INT32_MAX / 16);
-    const int cap_e = (int)std::min<size_t>(want_e, INT32_MAX / 32);
-    vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, taup, S.eN, S.eP, s);
-    vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
-    vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, cap_c, s);
-    vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, S.counters, cap_c,
-                              S.geo, S.cnt, ctx->f.err, s);
-    vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
-                             ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
-                             S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
-    if (ctx->vort_on) {  // beta.dat lines (src/fld.cpp:663-669, 798-831)
-      if ((st = dgrow(ctx, &ctx->surf_beta, &ctx->cap_beta, want_e * 16))) return st;
-      vh::launch_surf_beta(g, ctx->vort.dbeta, ctx->grid.etamin, S.cubes, S.counters, cap_c,
-                           cap_e, S.geo, S.cnt, ctx->surf_beta, s);
-    }
-    VH_CUDA(ctx, cudaGetLastError());
-    VH_CUDA(ctx, cudaMemcpyAsync(H.cnt, S.counters, sizeof H.cnt, cudaMemcpyDeviceToHost, s));
-    VH_CUDA(ctx, cudaMemcpyAsync(H.acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
-                                 sizeof H.acc, cudaMemcpyDeviceToHost, s));
-    VH_CUDA(ctx, cudaMemcpyAsync(&H.bits, ctx->f.err, sizeof H.bits, cudaMemcpyDeviceToHost, s));
-    VH_CUDA(ctx, cudaStreamSynchronize(s));
-    if ((size_t)H.cnt[0] <= (size_t)cap_c && (size_t)H.cnt[1] <= (size_t)cap_e) break;
-    if (pass == 1) return fail(ctx, VH_ERR_STATE, "vh_surface: element buffers did not grow");
-    want_c = std::max(want_c, (size_t)H.cnt[0] + (size_t)H.cnt[0] / 4 + 1);
-    // a cube holds at most kSurfMaxElemPerCube elements
-    want_e = std::max(want_e, (size_t)H.cnt[0] * vh::kSurfMaxElemPerCube);
-  }
+  vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, taup, S.eN, S.eP, s);
+  vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
+  vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, cap_c, s);
+  vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, S.counters, cap_c,
+                            S.geo, S.cnt, ctx->f.err, s);
+  vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
+                           ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
+                           S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
+  if (ctx->vort_on)  // beta.dat lines (src/fld.cpp:663-669, 798-831)
+    vh::launch_surf_beta(g, ctx->vort.dbeta, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
+                         S.geo, S.cnt, ctx->surf_beta, s);
+  VH_CUDA(ctx, cudaGetLastError());
+  VH_CUDA(ctx, cudaMemcpyAsync(H.cnt, S.counters, sizeof H.cnt, cudaMemcpyDeviceToHost, s));
+  VH_CUDA(ctx, cudaMemcpyAsync(H.acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
+                               sizeof H.acc, cudaMemcpyDeviceToHost, s));
+  VH_CUDA(ctx, cudaMemcpyAsync(&H.bits, ctx->f.err, sizeof H.bits, cudaMemcpyDeviceToHost, s));
+  return VH_OK;
+}
+
+// The buffers a pass starts with: what earlier calls left, at least 64k
+// hypercubes (or all of them) and twice as many elements.
+static void surf_want(vh_ctx* ctx, size_t* want_c, size_t* want_e) {
+  const long long ninterior = std::max(1LL, vh::surf_ncube(ctx->g));
+  *want_c = std::max<size_t>(ctx->surf.cap_cubes, (size_t)std::min(ninterior, 65536LL));
+  *want_e = std::max<size_t>(ctx->surf.cap_rec / vh::kSurfRec, 2 * *want_c);
+}
+
+// After a pass's copies landed: false when it found more hypercubes or
+// elements than its buffers held (then want_c / want_e hold what a pass
+// over the same fields needs).
+static bool surf_fits(vh_ctx* ctx, size_t* want_c, size_t* want_e) {
+  const vh_ctx::Surf& S = ctx->surf;
+  const vh_ctx::Surf::Host& H = *S.host;
+  if ((size_t)H.cnt[0] <= (size_t)S.pass_cap_c && (size_t)H.cnt[1] <= (size_t)S.pass_cap_e)
+    return true;
+  *want_c = std::max(*want_c, (size_t)H.cnt[0] + (size_t)H.cnt[0] / 4 + 1);
+  // a cube holds at most kSurfMaxElemPerCube elements
+  *want_e = std::max(*want_e, (size_t)H.cnt[0] * vh::kSurfMaxElemPerCube);
+  return false;
+}
+
+// The results of a pass that fit: element count, the carried sums, info.
+static vh_status surf_finish(vh_ctx* ctx, vh_surface_info* info) {
+  vh_ctx::Surf& S = ctx->surf;
+  const vh_ctx::Surf::Host& H = *S.host;
   const int nel = H.cnt[1];
   const unsigned bits = H.bits;
   const double* acc = H.acc;
@@ -871,9 +887,71 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   return VH_OK;
 }
 
+vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_surface: no state uploaded");
+  if (ctx->surf_pending) return fail(ctx, VH_ERR_STATE, "vh_surface: a vh_surface_begin is pending");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh_status st;
+  if ((st = surf_common(ctx))) return st;
+  // Every stage reads the counts from device memory, so the call waits for
+  // the GPU once, at the end.  A call that finds more than the buffers hold
+  // grows them and runs again (the fields it reads are unchanged in
+  // between, so the result is the same).
+  size_t want_c, want_e;
+  surf_want(ctx, &want_c, &want_e);
+  for (int pass = 0; pass < 2; pass++) {
+    if ((st = surf_enqueue(ctx, ecrit, want_c, want_e))) return st;
+    VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (surf_fits(ctx, &want_c, &want_e)) return surf_finish(ctx, info);
+  }
+  return fail(ctx, VH_ERR_STATE, "vh_surface: element buffers did not grow");
+}
+
+vh_status vh_surface_begin(vh_ctx* ctx, double ecrit) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_surface_begin: no state uploaded");
+  if (ctx->surf_pending)
+    return fail(ctx, VH_ERR_STATE, "vh_surface_begin: the previous call has not ended");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh_status st;
+  if ((st = surf_common(ctx))) return st;
+  if (!ctx->surf_ev) VH_CUDA(ctx, cudaEventCreateWithFlags(&ctx->surf_ev, cudaEventDisableTiming));
+  size_t want_c, want_e;
+  surf_want(ctx, &want_c, &want_e);
+  if ((st = surf_enqueue(ctx, ecrit, want_c, want_e))) return st;
+  VH_CUDA(ctx, cudaEventRecord(ctx->surf_ev, ctx->stream));
+  ctx->surf_pending = true;
+  return VH_OK;
+}
+
+vh_status vh_surface_end(vh_ctx* ctx, vh_surface_info* info) {
+  if (!ctx) return VH_ERR_ARG;
+  if (!ctx->surf_pending) return fail(ctx, VH_ERR_STATE, "vh_surface_end: no vh_surface_begin");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  ctx->surf_pending = false;
+  VH_CUDA(ctx, cudaEventSynchronize(ctx->surf_ev));
+  size_t want_c, want_e;
+  surf_want(ctx, &want_c, &want_e);
+  if (!surf_fits(ctx, &want_c, &want_e)) {
+    // the fields have moved on: grow for the next call, report this one lost
+    ctx->surf.nel = 0;
+    ctx->beta_nel = 0;
+    vh_status st;
+    if ((st = dgrow(ctx, &ctx->surf.cubes, &ctx->surf.cap_cubes, want_c)) ||
+        (st = dgrow(ctx, &ctx->surf.rec, &ctx->surf.cap_rec, want_e * vh::kSurfRec)))
+      return st;
+    return fail(ctx, VH_ERR_STATE,
+                "vh_surface_end: more elements than the buffers held; buffers grown, "
+                "this call's elements are lost (use vh_surface for it)");
+  }
+  return surf_finish(ctx, info);
+}
+
 vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   if (!ctx) return VH_ERR_ARG;
   if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_corona: no state uploaded");
+  if (ctx->surf_pending) return fail(ctx, VH_ERR_STATE, "vh_corona: a vh_surface_begin is pending");
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
   const vh::Geo& g = ctx->g;
   vh_ctx::Surf& S = ctx->surf;
@@ -927,6 +1005,8 @@ vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
 
 vh_status vh_surface_records(vh_ctx* ctx, double* out, long max, long* n) {
   if (!ctx || (!out && max > 0)) return VH_ERR_ARG;
+  if (ctx->surf_pending)
+    return fail(ctx, VH_ERR_STATE, "vh_surface_records: a vh_surface_begin is pending");
   const long k = (long)std::min<long long>(ctx->surf.nel, std::max(0L, max));
   if (n) *n = (long)ctx->surf.nel;
   if (k > 0) {
@@ -999,6 +1079,8 @@ vh_status vh_get_dbeta(vh_ctx* ctx, double* out) {
 
 vh_status vh_surface_beta(vh_ctx* ctx, double* out, long max, long* n) {
   if (!ctx || (!out && max > 0)) return VH_ERR_ARG;
+  if (ctx->surf_pending)
+    return fail(ctx, VH_ERR_STATE, "vh_surface_beta: a vh_surface_begin is pending");
   if (!ctx->vort_on) return fail(ctx, VH_ERR_STATE, "vh_surface_beta: vorticity is off");
   const long k = (long)std::min<long long>(ctx->beta_nel, std::max(0L, max));
   if (n) *n = (long)ctx->beta_nel;

@@ -57,12 +57,16 @@ struct vh_ctx {
   size_t cap_beta = 0;
   long long beta_nel = 0;       // its element count (0 after vh_corona)
   long long corona_cells = -1;  // elements of the last vh_corona (the beta.dat header)
+  // vh_surface_begin / vh_surface_end: one call in flight, its completion event
+  bool surf_pending = false;
+  cudaEvent_t surf_ev = nullptr;
   struct Surf {
     double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
            *partial = nullptr;
     int *blk = nullptr, *cubes = nullptr, *cnt = nullptr, *counters = nullptr;
     unsigned char* cflag = nullptr;  // [interior cubes] corona flags
     size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
+    int pass_cap_c = 0, pass_cap_e = 0;  // the buffers the last pass ran with
     long long nel = 0;
     // pinned landing place of a call's counts, sums and error bits
     struct Host {
