@@ -60,15 +60,30 @@ typedef struct vh_grid {
  * (src/eos.h:21-38), so the EoS is lowered to data:
  *  kind VH_EOS_CONFORMAL: p = e/3, T = (e/conf_cnst)^(1/4), muB = 0;
  *  kind VH_EOS_TABLE:     EoS1f (e, nb) table (src/eo1.cpp:21-123): sorted
- *                         egrid[ne], ngrid[nn] (nn >= 2), p/T/mub[ie + ne*inb].
+ *                         egrid[ne], ngrid[nn] (nn >= 2), p/T/mub[ie + ne*inb];
+ *  kind VH_EOS_CHIRAL:    EoSChiral (src/eoChiral.cpp:99-178): aux[0] the
+ *                         chiralsmall table (used for e < 1.46, nb < 0.3),
+ *                         aux[1] the chiraleos table (e < 146, nb < 6), and
+ *                         p = 0.2964 e, T = 0.15120476935 e^(1/4) above.
  * Host arrays are copied at vh_create. */
 #define VH_EOS_CONFORMAL 0
 #define VH_EOS_TABLE 1
+#define VH_EOS_CHIRAL 2
+/* One EoSaux table (src/eoChiral.cpp:33-97) after its constructor's unit
+ * conversions: the e and nb grids are uniform from emin to emax (GeV/fm^3)
+ * and nmin to nmax (fm^-3) with ne, nn >= 2 points; p (GeV/fm^3), T, muB,
+ * muS (GeV) at [in * ne + ie]. */
+typedef struct vh_eos_aux {
+  int ne, nn;
+  double emin, emax, nmin, nmax;
+  const double *p, *T, *mub, *mus;
+} vh_eos_aux;
 typedef struct vh_eos {
   int kind;
   double conf_cnst;
   int ne, nn;
   const double *egrid, *ngrid, *p, *T, *mub;
+  vh_eos_aux aux[2]; /* VH_EOS_CHIRAL only */
 } vh_eos;
 
 /* TransportCoeff public constants (src/trancoeff.h:8-11, ctor :14-20). */
@@ -381,6 +396,13 @@ int vh_abi_version(void);
  * Uses the context's EoS and stream. */
 vh_status vh_transform_pv(vh_ctx *ctx, const double *Q_dev, long n,
                           double *prim_dev);
+
+/* The context's EoS on device arrays (EoS::eos with muS, EoS::p and
+ * EoS::s with nq = ns = 0; src/eos.h:21-38, src/eos.cpp:18-25):
+ * e[n], nb[n] -> out[6][n] = p, T, muB, muS, p(), s.  Uses the context's
+ * stream. */
+vh_status vh_eos_eval(vh_ctx *ctx, const double *e_dev, const double *nb_dev, long n,
+                      double *out_dev);
 
 /* Batched transport coefficients on device arrays (TransportCoeff::getEta
  * and getTau, src/trancoeff.cpp:68-100) with the context's parameters:

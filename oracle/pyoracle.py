@@ -37,11 +37,17 @@ class _Grid(ctypes.Structure):
                 ("zmin", ctypes.c_double), ("zmax", ctypes.c_double)]
 
 
+class _Aux(ctypes.Structure):
+    _fields_ = [("ne", ctypes.c_int), ("nn", ctypes.c_int), ("emin", ctypes.c_double),
+                ("emax", ctypes.c_double), ("nmin", ctypes.c_double), ("nmax", ctypes.c_double),
+                ("p", _dp), ("T", _dp), ("mub", _dp), ("mus", _dp)]
+
+
 class _Eos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
-                ("tol", ctypes.c_double)]
+                ("tol", ctypes.c_double), ("aux", _Aux * 2)]
 
 
 class _Trc(ctypes.Structure):
@@ -74,6 +80,7 @@ def oracle_lib():
         lib.or_transform_pv.argtypes = [ctypes.POINTER(_Eos), _dp, ctypes.c_int, _dp]
         lib.or_transport_eval.argtypes = [ctypes.POINTER(_Trc), _dp, ctypes.c_int, _dp]
         lib.or_eos_eval.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
+        lib.or_eos6.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_eos_s.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_update_m.argtypes = [ctypes.POINTER(_Grid), _dp, ctypes.c_double, ctypes.c_double]
         lib.or_resize2x.restype = ctypes.c_int
@@ -127,6 +134,7 @@ def ref_lib():
         lib.ref_output_corona.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                           ctypes.c_char_p, ctypes.c_int]
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
+        lib.ref_eos6.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
         lib.ref_cornelius4d.restype = ctypes.c_int
@@ -226,6 +234,13 @@ class _EosHolder:
             self.s.ne = len(arrs[0])
             self.s.nn = len(arrs[1])
             self.s.egrid, self.s.ngrid, self.s.p, self.s.T, self.s.mub = (_ptr(a) for a in arrs)
+        if eos.kind == 2:
+            for k, a in enumerate(eos.aux):
+                arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
+                self.keep += arrs
+                x = self.s.aux[k]
+                x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax = a.ne, a.nn, a.emin, a.emax, a.nmin, a.nmax
+                x.p, x.T, x.mub, x.mus = (_ptr(v) for v in arrs)
 
 
 def _trc(setup):
@@ -402,6 +417,10 @@ class OracleRun:
         self.lib.or_transport_eval(ctypes.byref(self.trc), _ptr(inp), len(inp), _ptr(out))
         return out
 
+    def eos6(self, e, nb):
+        """[n][6] = p, T, muB, muS, EoS::p, EoS::s (nq = ns = 0)."""
+        return _eos6(self.lib.or_eos6, ctypes.byref(self.eos.s), e, nb)
+
     def eos_eval(self, e, nb):
         e = np.ascontiguousarray(e, dtype=np.float64)
         nb = np.ascontiguousarray(nb, dtype=np.float64)
@@ -410,6 +429,14 @@ class OracleRun:
         self.lib.or_eos_eval(ctypes.byref(self.eos.s), _ptr(e), _ptr(nb), len(e), _ptr(out))
         self.lib.or_eos_s(ctypes.byref(self.eos.s), _ptr(e), _ptr(nb), len(e), _ptr(s))
         return out, s
+
+
+def _eos6(fn, h, e, nb):
+    e = np.ascontiguousarray(e, dtype=np.float64)
+    nb = np.ascontiguousarray(nb, dtype=np.float64)
+    out = np.zeros((len(e), 6))
+    fn(h, _ptr(e), _ptr(nb), len(e), _ptr(out))
+    return out
 
 
 class RefRun:
@@ -432,6 +459,10 @@ class RefRun:
             self._tmp = tempfile.TemporaryDirectory()
             eos_file = os.path.join(self._tmp.name, "eos1f.dat")
             setup.eos.write_eos1f(eos_file)
+        if setup.eos.kind == 2 and eos_file is None:  # the directory that holds eos/
+            self._tmp = tempfile.TemporaryDirectory()
+            eos_file = self._tmp.name
+            setup.eos.write_chiral(eos_file)
         bounds = np.array(g.bounds(), dtype=np.float64)
         tr = np.array(setup.tr_vector(), dtype=np.float64)
         self.h = self.lib.ref_create(g.nx, g.ny, g.nz, _ptr(bounds), setup.tau0, setup.dt,
@@ -529,6 +560,10 @@ class RefRun:
         buf = ctypes.create_string_buffer(512)
         n = self.lib.ref_output_corona(self.h, outdir.encode(), int(extend), buf, 512)
         return n, buf.value.decode()
+
+    def eos6(self, e, nb):
+        """[n][6] = p, T, muB, muS, EoS::p, EoS::s (nq = ns = 0)."""
+        return _eos6(self.lib.ref_eos6, self.h, e, nb)
 
     def eos_eval(self, e, nb):
         e = np.ascontiguousarray(e, dtype=np.float64)

@@ -15,6 +15,8 @@
 //  * The initial state is uploaded as conserved Q arrays through Cell::setQ
 //    + saveQprev + setAllM, the pattern every reference IC ends with
 //    (e.g. src/icGubser.cpp:50-57).
+#include <unistd.h>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -28,6 +30,7 @@
 #include "cll.h"
 #include "cornelius.h"
 #include "eo1.h"
+#include "eoChiral.h"
 #include "fld.h"
 #include "hdo.h"
 #include "inc.h"
@@ -90,10 +93,30 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
                  double conf_cnst, const char *eos_file, const double *tr,
                  int etaSparam, int zetaSparam) {
   RefRun *r = new RefRun;
-  if (eos_kind == 0)
+  if (eos_kind == 0) {
     r->eos = new ConformalEoS(conf_cnst);
-  else
+  } else if (eos_kind == 2) {
+    // EoSChiral reads eos/chiraleos.dat and eos/chiralsmall.dat relative to
+    // the working directory (src/eoChiral.cpp:153-156): eos_file names the
+    // directory that holds eos/
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof cwd) || chdir(eos_file) != 0) {
+      delete r;
+      return nullptr;
+    }
+    std::streambuf *old = std::cout.rdbuf();
+    std::ostringstream quiet;
+    std::cout.rdbuf(quiet.rdbuf());
+    r->eos = new EoSChiral();
+    std::cout.rdbuf(old);
+    if (chdir(cwd) != 0) {
+      delete r->eos;
+      delete r;
+      return nullptr;
+    }
+  } else {
     r->eos = new EoS1f(const_cast<char *>(eos_file));
+  }
   r->tr = new TransportCoeff(tr[0], tr[1], tr[2], tr[3], tr[4], tr[5], tr[6],
                              tr[7], tr[8], tr[9], tr[10], tr[11], tr[12],
                              tr[13], r->eos, etaSparam, zetaSparam);
@@ -305,6 +328,23 @@ void ref_eos(void *p, const double *e, const double *nb, int n, double *out,
     out[3 * i + 1] = T;
     out[3 * i + 2] = mub;
     if (s_out) s_out[i] = r->eos->s(e[i], nb[i], 0., 0.);
+  }
+}
+
+// EoS::eos with muS, EoS::p and EoS::s (nq = ns = 0) on arrays:
+// out[n][6] = p, T, muB, muS, p(), s
+void ref_eos6(void *p, const double *e, const double *nb, int n, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  for (int i = 0; i < n; i++) {
+    double T, mub, muq, mus, pp;
+    r->eos->eos(e[i], nb[i], 0., 0., T, mub, muq, mus, pp);
+    double *o = out + 6 * i;
+    o[0] = pp;
+    o[1] = T;
+    o[2] = mub;
+    o[3] = mus;
+    o[4] = r->eos->p(e[i], nb[i], 0., 0.);
+    o[5] = r->eos->s(e[i], nb[i], 0., 0.);
   }
 }
 

@@ -101,21 +101,84 @@ static void eos1f(const or_eos *E, double e, double nb, double *T, double *mub,
   *mub = smu;
 }
 
-/* EoS::eos(); muq = mus = 0 for both supported kinds */
-static void eos_eval(const or_eos *E, double e, double nb, double *T,
-                     double *mub, double *p) {
+/* EoSaux::get, src/eoChiral.cpp:99-130 (EoSaux::p, :132-151, is its p) */
+static void chiral_aux(const or_aux *A, double e, double nb, double *p,
+                       double *T, double *mub, double *mus) {
+  if (e < 0.) {
+    *T = *mub = *mus = *p = 0.;
+    return;
+  }
+  const double de = (A->emax - A->emin) / (A->ne - 1);
+  const double dn = (A->nmax - A->nmin) / (A->nn - 1);
+  int ie = (int)((e - A->emin) / de);
+  int in = (int)((nb - A->nmin) / dn);
+  if (ie < 0) ie = 0;
+  if (in < 0) in = 0;
+  if (ie > A->ne - 2) ie = A->ne - 2;
+  if (in > A->nn - 2) in = A->nn - 2;
+  const double em = e - A->emin - ie * de;
+  const double nm = nb - A->nmin - in * dn;
+  const double we[2] = {1. - em / de, em / de};
+  const double wn[2] = {1. - nm / dn, nm / dn};
+  double sp = 0., sT = 0., sb = 0., ss = 0.;
+  for (int je = 0; je < 2; je++)
+    for (int jn = 0; jn < 2; jn++) {
+      const long k = (long)(in + jn) * A->ne + (ie + je);
+      sp += we[je] * wn[jn] * A->p[k];
+      sT += we[je] * wn[jn] * A->T[k];
+      sb += we[je] * wn[jn] * A->mub[k];
+      ss += we[je] * wn[jn] * A->mus[k];
+    }
+  if (sp < 0.0) sp = 0.0;
+  *p = sp;
+  *T = sT;
+  *mub = sb;
+  *mus = ss;
+}
+
+/* EoSChiral::eos, src/eoChiral.cpp:159-170 (muq = 0) */
+static void eos_chiral(const or_eos *E, double e, double nb, double *T,
+                       double *mub, double *mus, double *p) {
+  if (e < 1.46 && nb < 0.3)
+    chiral_aux(&E->aux[0], e, nb, p, T, mub, mus);
+  else if (e < 146. && nb < 6.)
+    chiral_aux(&E->aux[1], e, nb, p, T, mub, mus);
+  else {
+    *p = 0.2964 * e;
+    *T = 0.15120476935 * pow(e, 0.25);
+    *mub = *mus = 0.0;
+  }
+}
+
+/* EoS::eos(); muq = 0 for every supported kind, mus = 0 but for kind 2 */
+static void eos_eval4(const or_eos *E, double e, double nb, double *T,
+                      double *mub, double *mus, double *p) {
+  *mus = 0.;
   if (E->kind == 0) {
     *p = e / 3.;
     *T = e > 0. ? sqrt(sqrt(e / E->conf_cnst)) : 0.;
     *mub = 0.;
+  } else if (E->kind == 2) {
+    eos_chiral(E, e, nb, T, mub, mus, p);
   } else {
     eos1f(E, e, nb, T, mub, p);
   }
 }
 
+static void eos_eval(const or_eos *E, double e, double nb, double *T,
+                     double *mub, double *p) {
+  double mus;
+  eos_eval4(E, e, nb, T, mub, &mus, p);
+}
+
+/* EoS::p; EoSChiral::p (src/eoChiral.cpp:172-178) is its eos's p */
 static double eos_p(const or_eos *E, double e, double nb) {
-  double T, mub, p;
+  double T, mub, mus, p;
   if (E->kind == 0) return e / 3.;
+  if (E->kind == 2) {
+    eos_chiral(E, e, nb, &T, &mub, &mus, &p);
+    return p;
+  }
   eos1f(E, e, nb, &T, &mub, &p);
   return p;
 }
@@ -123,9 +186,9 @@ static double eos_p(const or_eos *E, double e, double nb) {
 /* EoS::s, src/eos.cpp:18-25 */
 static double eos_s(const or_eos *E, double e, double nb, double nq,
                     double ns) {
-  double T, mub, p;
-  const double muq = 0., mus = 0.;
-  eos_eval(E, e, nb, &T, &mub, &p);
+  double T, mub, mus, p;
+  const double muq = 0.;
+  eos_eval4(E, e, nb, &T, &mub, &mus, &p);
   if (T > 0.0)
     return (e + p - mub * nb - muq * nq - mus * ns) / T;
   else
@@ -1387,6 +1450,16 @@ void or_transport_eval(const or_trc *tr, const double *in, int n, double *out) {
   }
 }
 
+/* out[n][6] = p, T, muB, muS, EoS::p, EoS::s (nq = ns = 0) */
+void or_eos6(const or_eos *eos, const double *e, const double *nb, int n, double *out) {
+  for (int i = 0; i < n; i++) {
+    double *o = out + 6 * i;
+    eos_eval4(eos, e[i], nb[i], &o[1], &o[2], &o[3], &o[0]);
+    o[4] = eos_p(eos, e[i], nb[i]);
+    o[5] = eos_s(eos, e[i], nb[i], 0., 0.);
+  }
+}
+
 void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
                  double *out) {
   for (int i = 0; i < n; i++) {
@@ -2132,10 +2205,10 @@ static long surface_impl(const or_grid *g, const or_eos *E, const or_state *s, d
                   for (int k = 0; k < 7; k++)
                     QC[k] += QCube[jt][jx * 4 + jy * 2 + jz][k] * wT[jt] * wX[jx] * wY[jy] * wZ[jz];
           for (int k = 0; k < 7; k++) QC[k] = QC[k] / (tau + C[0]);
-          double eC, pC, nbC, nqC, nsC = 0.0, vxC, vyC, vzC, TC, mubC;
+          double eC, pC, nbC, nqC, nsC = 0.0, vxC, vyC, vzC, TC, mubC, musC;
           transform_pv(E, QC, &eC, &pC, &nbC, &nqC, &nsC, &vxC, &vyC, &vzC);
-          eos_eval(E, eC, nbC, &TC, &mubC, &pC);
-          const double muqC = 0., musC = 0.;
+          eos_eval4(E, eC, nbC, &TC, &mubC, &musC, &pC);
+          const double muqC = 0.;
           if (TC > 0.4 || fabs(mubC) > 0.85) acc[4] += 1.;
           if (eC > ecrit * 2.0 || eC < ecrit * 0.5) acc[0] += 1.;
           double dbI[16];
@@ -2277,8 +2350,9 @@ long or_corona(const or_grid *g, const or_eos *E, const or_state *s, double tau,
         transform_pv(E, QC, &eC, &pC, &nbC, &nqC, &nsC, &vxC, &vyC, &vzC);
         const int isTail = !(eC >= 0.01);
         if (!isCorona || isTail) continue;
-        eos_eval(E, eC, nbC, &TC, &mubC, &pC);
-        const double muqC = 0., musC = 0.;
+        double musC;
+        eos_eval4(E, eC, nbC, &TC, &mubC, &musC, &pC);
+        const double muqC = 0.;
         if (TC > 0.4 || fabs(mubC) > 0.99) acc[4] += 1.;
         double piC[10], PiC = 0.;
         for (int k = 0; k < 10; k++) piC[k] = 0.;

@@ -31,8 +31,17 @@ typedef struct or_grid {
 
 /* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)
  * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb] */
+/* One EoSaux table of EoSChiral (src/eoChiral.cpp:33-97), converted to
+ * GeV/fm^3, fm^-3 and GeV as its constructor does: uniform grids from emin
+ * to emax and nmin to nmax, p/T/mub/mus[in * ne + ie]. */
+typedef struct or_aux {
+  int ne, nn;
+  double emin, emax, nmin, nmax;
+  const double *p, *T, *mub, *mus;
+} or_aux;
+
 typedef struct or_eos {
-  int kind;
+  int kind; /* 0 conformal gas, 1 EoS1f table, 2 EoSChiral */
   double conf_cnst;
   int ne, nn;
   const double *egrid, *ngrid, *p, *T, *mub;
@@ -40,6 +49,7 @@ typedef struct or_eos {
    * (src/rmn.cpp:96).  A smaller value gives the tight-tolerance oracle the
    * learned-guess path is checked against. */
   double tol;
+  or_aux aux[2]; /* kind 2: chiralsmall, chiraleos */
 } or_eos;
 
 /* TransportCoeff (src/trancoeff.h:6-45) public constants */
@@ -96,6 +106,9 @@ void or_eos_eval(const or_eos *eos, const double *e, const double *nb, int n,
 /* EoS::s for n points (nq = ns = 0). */
 void or_eos_s(const or_eos *eos, const double *e, const double *nb, int n,
               double *out);
+
+void or_eos6(const or_eos *eos, const double *e, const double *nb, int n,
+             double *out);
 
 /* The grid totals Fluid::outputSurface accumulates over the interior cells
  * [2, n-2)^3 (src/fld.cpp:544-604, scaled at :846-851).  out[OR_TOT_N]:

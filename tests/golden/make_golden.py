@@ -38,7 +38,22 @@ CASES = {
     # the large event's physics (shear + bulk + cross terms + nb) on a coarse
     # grid, with the reference's own zeta/s form 2 in place of the bump
     "large_21x21x11_zeta2": (lambda: large_with_zeta(21, 11, 2), 5),
+    # baryon charge on the reference's default EoS, EoSChiral (its two
+    # tables from workloads.chiral_eos)
+    "glauber_nb_chiral_17x17x9": (lambda: W.glauber3d_nb_setup(17, 17, 9, eos=W.chiral_eos()), 5),
 }
+
+
+def chiral_digest(eos):
+    """A fingerprint of a chiral EoS's tables (the fixtures hold it instead
+    of the 26 MB of tables, which workloads.chiral_eos regenerates)."""
+    import hashlib
+    h = hashlib.sha256()
+    for a in eos.aux:
+        h.update(np.array([a.ne, a.nn, a.emin, a.emax, a.nmin, a.nmax]).tobytes())
+        for x in (a.p, a.T, a.mub, a.mus):
+            h.update(np.ascontiguousarray(x, dtype=np.float64).tobytes())
+    return h.hexdigest()
 
 
 def large_with_zeta(n, nz, zetaSparam):
@@ -68,6 +83,8 @@ def save_case(name, setup, nsteps):
     if eos.kind == 1:
         arrays.update(eos_egrid=eos.egrid, eos_ngrid=eos.ngrid, eos_p=eos.p, eos_T=eos.T,
                       eos_mub=eos.mub)
+    if eos.kind == 2:
+        arrays.update(eos_digest=np.array(chiral_digest(eos)))
     for k, v in st.items():
         arrays["out_" + k] = v
     r.close()
@@ -276,6 +293,32 @@ def load_surface_case(path):
     return setup, int(z["nsteps"]), z["surf_counts"], z["surf_rec"], [str(v) for v in z["surf_lines"]]
 
 
+def chiral_points():
+    """(e, nb) points over EoSChiral's three regions, their borders, the
+    clamped table edges, negative e and nb, and the power law above."""
+    rng = np.random.default_rng(12)
+    e = np.concatenate([rng.uniform(-0.1, 1.6, 3000), rng.uniform(0, 160, 3000),
+                        10 ** rng.uniform(-6, 5, 2000),
+                        [0., -0., 1.46, 1.4599999999, 146., 145.99999999, 1e300, 0.146, 0.073,
+                         np.inf, 1e-300]])
+    nb = np.concatenate([rng.uniform(-0.05, 0.35, 3000), rng.uniform(-0.1, 6.5, 3000),
+                         rng.uniform(0, 7, 2000),
+                         [0., 0.3, 0.2999999999, 0., 5.999999, 6., 0., 0.15, -1e300, 0., 0.]])
+    return e, nb
+
+
+def chiral_known_answers():
+    """EoSChiral (the reference's own class on workloads.chiral_eos's files)
+    at chiral_points(): p, T, muB, muS, EoS::p, EoS::s."""
+    e, nb = chiral_points()
+    setup = W.glauber3d_nb_setup(17, 17, 9, eos=W.chiral_eos())
+    r = P.RefRun(setup)
+    out = r.eos6(e, nb)
+    r.close()
+    np.savez_compressed(os.path.join(HERE, "chiral_known_answers.npz"), e=e, nb=nb, out=out,
+                        eos_digest=np.array(chiral_digest(setup.eos)))
+
+
 def known_answers():
     """transformPV / EoS known answers over regimes the step meets: empty
     (Q_t <= 0), at rest (M = 0), superluminal (M > Q_t), dilute, dense."""
@@ -317,6 +360,10 @@ def load_case(path):
     if int(z["eos_kind"]) == 1:
         eos = W.EosTable(kind=1, egrid=z["eos_egrid"], ngrid=z["eos_ngrid"], p=z["eos_p"],
                          T=z["eos_T"], mub=z["eos_mub"])
+    elif int(z["eos_kind"]) == 2:
+        eos = W.chiral_eos()
+        if chiral_digest(eos) != str(z["eos_digest"]):
+            raise RuntimeError("workloads.chiral_eos no longer gives the fixture's tables")
     else:
         eos = W.EosTable(kind=0, conf_cnst=float(z["eos_cnst"]))
     tr = dict(zip(W.TR_FIELDS, (float(v) for v in z["tr"])))
@@ -358,6 +405,9 @@ if __name__ == "__main__":
     if not only or "cornelius_cubes" in only:
         cornelius_cubes()
         print("wrote cornelius_cubes")
+    if not only or "chiral_known_answers" in only:
+        chiral_known_answers()
+        print("wrote chiral_known_answers")
     if not only or "known_answers" in only:
         known_answers()
         print("wrote known_answers")

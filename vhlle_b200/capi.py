@@ -25,7 +25,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_upload_async", "vh_download_async", "vh_device_state", "vh_step", "vh_steps",
            "vh_set_dtau", "vh_get_dtau", "vh_get_tau", "vh_set_tau", "vh_sync",
            "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
-           "vh_abi_version", "vh_transform_pv", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
+           "vh_abi_version", "vh_transform_pv", "vh_eos_eval", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
@@ -213,10 +213,17 @@ class VhGrid(ctypes.Structure):
                 ("etamin", ctypes.c_double), ("etamax", ctypes.c_double)]
 
 
+class VhEosAux(ctypes.Structure):
+    _fields_ = [("ne", ctypes.c_int), ("nn", ctypes.c_int), ("emin", ctypes.c_double),
+                ("emax", ctypes.c_double), ("nmin", ctypes.c_double), ("nmax", ctypes.c_double),
+                ("p", _dp), ("T", _dp), ("mub", _dp), ("mus", _dp)]
+
+
 class VhEos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
-                ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp)]
+                ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
+                ("aux", VhEosAux * 2)]
 
 
 class VhTrcoeff(ctypes.Structure):
@@ -293,6 +300,7 @@ def lib():
     L.vh_resize2x.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.vh_surface.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
     L.vh_corona.argtypes = [vp, ctypes.c_double, ctypes.POINTER(VhSurfaceInfo)]
+    L.vh_eos_eval.argtypes = [vp, vp, vp, ctypes.c_long, vp]
     L.vh_surface_begin.argtypes = [vp, ctypes.c_double]
     L.vh_surface_end.argtypes = [vp, ctypes.POINTER(VhSurfaceInfo)]
     L.vh_surface_records.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
@@ -350,6 +358,13 @@ def make_eos(eos):
                 for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub)]
         d.ne, d.nn = len(keep[0]), len(keep[1])
         d.egrid, d.ngrid, d.p, d.T, d.mub = (_ptr(a) for a in keep)
+    if eos.kind == 2:
+        for k, a in enumerate(eos.aux):
+            arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
+            keep += arrs
+            x = d.aux[k]
+            x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax = a.ne, a.nn, a.emin, a.emax, a.nmin, a.nmax
+            x.p, x.T, x.mub, x.mus = (_ptr(v) for v in arrs)
     return d, keep
 
 
@@ -531,6 +546,23 @@ class GpuHydro:
         torch.cuda.synchronize(dev)
         self._check(self.L.vh_transport_eval(self.h, ctypes.c_void_p(din.data_ptr()), n,
                                              ctypes.c_void_p(dout.data_ptr())))
+        self.sync()
+        return dout.cpu().numpy().T.copy()
+
+    def eos6(self, e, nb):
+        """The context's EoS on the device (vh_eos_eval): [n][6] = p, T,
+        muB, muS, EoS::p, EoS::s (nq = ns = 0)."""
+        import torch
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        nb = np.ascontiguousarray(nb, dtype=np.float64)
+        n = len(e)
+        dev = "cuda:%d" % self.device
+        de, dn = torch.from_numpy(e).to(dev), torch.from_numpy(nb).to(dev)
+        dout = torch.empty((6, n), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        self._check(self.L.vh_eos_eval(self.h, ctypes.c_void_p(de.data_ptr()),
+                                       ctypes.c_void_p(dn.data_ptr()), n,
+                                       ctypes.c_void_p(dout.data_ptr())))
         self.sync()
         return dout.cpu().numpy().T.copy()
 

@@ -200,8 +200,13 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   if (!(grid->xmin < grid->xmax) || !(grid->ymin < grid->ymax) || !(grid->etamin < grid->etamax))
     return fail(nullptr, VH_ERR_ARG, "vh_create: the grid needs min < max on every axis");
   if (!(tau0 > 0.)) return fail(nullptr, VH_ERR_ARG, "vh_create: tau0 must be positive");
-  if (eos->kind != VH_EOS_CONFORMAL && eos->kind != VH_EOS_TABLE)
+  if (eos->kind != VH_EOS_CONFORMAL && eos->kind != VH_EOS_TABLE && eos->kind != VH_EOS_CHIRAL)
     return fail(nullptr, VH_ERR_ARG, "vh_create: unsupported EoS kind (no device lowering)");
+  if (eos->kind == VH_EOS_CHIRAL)
+    for (const vh_eos_aux& x : eos->aux)
+      if (x.ne < 2 || x.nn < 2 || !x.p || !x.T || !x.mub || !x.mus ||
+          (long long)x.ne * x.nn > (1LL << 30))
+        return fail(nullptr, VH_ERR_ARG, "vh_create: chiral EoS table missing or too small");
   if (eos->kind == VH_EOS_TABLE) {
     if (eos->ne < 2 || eos->nn < 2 || !eos->egrid || !eos->ngrid || !eos->p || !eos->T || !eos->mub)
       return fail(nullptr, VH_ERR_ARG,
@@ -357,6 +362,22 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
         (a == 0 ? c->eos.erinv : c->eos.nrinv) = rdev;
       }
       rdev += r.size();
+    }
+  }
+  if (eos->kind == VH_EOS_CHIRAL) {
+    for (int k = 0; k < 2; k++) {
+      const vh_eos_aux& x = eos->aux[k];
+      const size_t n = (size_t)x.ne * x.nn;
+      double* buf = nullptr;
+      ALLOC(buf, 4 * n);
+      const double* src[4] = {x.p, x.T, x.mub, x.mus};
+      for (int q = 0; q < 4; q++)
+        if ((e = cudaMemcpy(buf + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice))) {
+          cuda_fail(c, e, "vh_create: EoS upload");
+          return bail(VH_ERR_CUDA);
+        }
+      c->eos.ch[k] = vh::ChiralAux{x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax,
+                                   buf, buf + n, buf + 2 * n, buf + 3 * n};
     }
   }
 #undef ALLOC
@@ -1248,6 +1269,16 @@ vh_status vh_transport_eval(vh_ctx* ctx, const double* in_dev, long n, double* o
   if (n == 0) return VH_OK;
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
   vh::launch_transport(ctx->tr, in_dev, (long long)n, out_dev, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
+  return VH_OK;
+}
+
+vh_status vh_eos_eval(vh_ctx* ctx, const double* e_dev, const double* nb_dev, long n,
+                      double* out_dev) {
+  if (!ctx || !e_dev || !nb_dev || !out_dev || n < 0) return VH_ERR_ARG;
+  if (n == 0) return VH_OK;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::launch_eos_eval(ctx->eos, e_dev, nb_dev, (long long)n, out_dev, ctx->stream);
   VH_CUDA(ctx, cudaGetLastError());
   return VH_OK;
 }

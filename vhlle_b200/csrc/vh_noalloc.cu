@@ -129,8 +129,13 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
     return nfail(VH_ERR_ARG,
                  "vh_step_noalloc: grid exceeds VH_NOALLOC_MAX_CELLS (32768 cells); "
                  "use vh_create/vh_step for larger grids");
-  if (eos_dev->kind != VH_EOS_CONFORMAL && eos_dev->kind != VH_EOS_TABLE)
+  if (eos_dev->kind != VH_EOS_CONFORMAL && eos_dev->kind != VH_EOS_TABLE &&
+      eos_dev->kind != VH_EOS_CHIRAL)
     return nfail(VH_ERR_ARG, "vh_step_noalloc: unsupported EoS kind");
+  if (eos_dev->kind == VH_EOS_CHIRAL)
+    for (const vh_eos_aux& x : eos_dev->aux)
+      if (x.ne < 2 || x.nn < 2 || !x.p || !x.T || !x.mub || !x.mus)
+        return nfail(VH_ERR_ARG, "vh_step_noalloc: chiral EoS table missing or too small");
   if (eos_dev->kind == VH_EOS_TABLE &&
       (eos_dev->ne < 2 || eos_dev->nn < 2 || !eos_dev->egrid || !eos_dev->ngrid ||
        !eos_dev->p || !eos_dev->T || !eos_dev->mub))
@@ -163,6 +168,11 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.eos.p = eos_dev->p;
   a.eos.T = eos_dev->T;
   a.eos.mub = eos_dev->mub;
+  if (eos_dev->kind == VH_EOS_CHIRAL)
+    for (int k = 0; k < 2; k++) {
+      const vh_eos_aux& x = eos_dev->aux[k];
+      a.eos.ch[k] = vh::ChiralAux{x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax, x.p, x.T, x.mub, x.mus};
+    }
   a.eos.emode = a.eos.nmode = vh::GRID_BSEARCH;  // the table stays on the device
   a.eos.e0 = a.eos.einv = a.eos.n0 = a.eos.ninv = 0.f;
   a.eos.erinv = a.eos.nrinv = nullptr;  // interpolation weights by division

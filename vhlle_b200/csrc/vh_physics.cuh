@@ -29,8 +29,15 @@ enum : unsigned {
 // the same bracket (GRID_LOG / GRID_LIN need a strictly increasing axis).
 enum : int { GRID_BSEARCH = 0, GRID_LOG = 1, GRID_LIN = 2 };
 
+// One EoSChiral sub-table (EoSaux): uniform grids, p/T/mub/mus[in*ne + ie]
+struct ChiralAux {
+  int ne, nn;
+  double emin, emax, nmin, nmax;
+  const double *__restrict__ p, *__restrict__ T, *__restrict__ mub, *__restrict__ mus;
+};
+
 struct EosDev {
-  int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table
+  int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table, 2 EoSChiral
   double conf_cnst;  // e = cnst T^4 for kind 0
   int ne, nn;
   const double* __restrict__ egrid;
@@ -52,6 +59,7 @@ struct EosDev {
   double tol;
   const float* __restrict__ vguess;
   unsigned long long* stats;
+  ChiralAux ch[2];  // kind 2: chiralsmall, chiraleos
 };
 
 __device__ __forceinline__ float c2p_guess(const EosDev& E, long long i) {
@@ -253,30 +261,113 @@ __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
   }
 }
 
+// EoSaux::get / EoSaux::p, src/eoChiral.cpp:99-151: the bracket is the
+// truncated (x - min) / step, clamped; the weights are (x - min - i step) /
+// step.  (int) of a double saturates here and gives INT_MIN on the host
+// for a large negative quotient alike; the region tests of eos_chiral keep
+// positive quotients below the table size.
+template <bool WANT_T>
+__device__ __forceinline__ void chiral_aux(const ChiralAux& A, double e, double nb, double& p,
+                                           double& T, double& mub, double& mus) {
+  if (e < 0.) {
+    T = mub = mus = p = 0.;
+    return;
+  }
+  const double de = (A.emax - A.emin) / (A.ne - 1);
+  const double dn = (A.nmax - A.nmin) / (A.nn - 1);
+  int ie = (int)((e - A.emin) / de);
+  int in = (int)((nb - A.nmin) / dn);
+  if (ie < 0) ie = 0;
+  if (in < 0) in = 0;
+  if (ie > A.ne - 2) ie = A.ne - 2;
+  if (in > A.nn - 2) in = A.nn - 2;
+  const double em = e - A.emin - ie * de;
+  const double nm = nb - A.nmin - in * dn;
+  const double we0 = 1. - em / de, we1 = em / de;
+  const double wn0 = 1. - nm / dn, wn1 = nm / dn;
+  const int b00 = in * A.ne + ie, b01 = b00 + A.ne;  // [ie][in], [ie][in + 1]
+  double sp = 0.;
+  sp += we0 * wn0 * __ldg(A.p + b00);
+  sp += we0 * wn1 * __ldg(A.p + b01);
+  sp += we1 * wn0 * __ldg(A.p + b00 + 1);
+  sp += we1 * wn1 * __ldg(A.p + b01 + 1);
+  if (WANT_T) {
+    double sT = 0., sb = 0., ss = 0.;
+    sT += we0 * wn0 * __ldg(A.T + b00);
+    sb += we0 * wn0 * __ldg(A.mub + b00);
+    ss += we0 * wn0 * __ldg(A.mus + b00);
+    sT += we0 * wn1 * __ldg(A.T + b01);
+    sb += we0 * wn1 * __ldg(A.mub + b01);
+    ss += we0 * wn1 * __ldg(A.mus + b01);
+    sT += we1 * wn0 * __ldg(A.T + b00 + 1);
+    sb += we1 * wn0 * __ldg(A.mub + b00 + 1);
+    ss += we1 * wn0 * __ldg(A.mus + b00 + 1);
+    sT += we1 * wn1 * __ldg(A.T + b01 + 1);
+    sb += we1 * wn1 * __ldg(A.mub + b01 + 1);
+    ss += we1 * wn1 * __ldg(A.mus + b01 + 1);
+    T = sT;
+    mub = sb;
+    mus = ss;
+  }
+  if (sp < 0.0) sp = 0.0;
+  p = sp;
+}
+
+// EoSChiral::eos / EoSChiral::p, src/eoChiral.cpp:159-178 (muq = 0); the
+// 1/4 power of the region above the tables is the correctly rounded one
+template <bool WANT_T>
+__device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb, double& T,
+                                           double& mub, double& mus, double& p) {
+  if (e < 1.46 && nb < 0.3) {
+    chiral_aux<WANT_T>(E.ch[0], e, nb, p, T, mub, mus);
+  } else if (e < 146. && nb < 6.) {
+    chiral_aux<WANT_T>(E.ch[1], e, nb, p, T, mub, mus);
+  } else {
+    p = 0.2964 * e;
+    if (WANT_T) {
+      T = 0.15120476935 * crm::root4_cr(e);
+      mub = mus = 0.0;
+    }
+  }
+}
+
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
   if (E.kind == 0) return ddivp(e, 3.);
-  double T, mub, p;
-  eos1f<false>(E, e, nb, T, mub, p);
+  double T, mub, mus, p;
+  if (E.kind == 2)
+    eos_chiral<false>(E, e, nb, T, mub, mus, p);
+  else
+    eos1f<false>(E, e, nb, T, mub, p);
   return p;
 }
 
-__device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
-                                         double& T, double& mub, double& p) {
+// EoS::eos with muS (muQ is 0 for every kind here; muS only for kind 2)
+__device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
+                                         double& mub, double& mus, double& p) {
+  mus = 0.;
   if (E.kind == 0) {
     p = ddivp(e, 3.);
     T = e > 0. ? sqrt(sqrt(e / E.conf_cnst)) : 0.;
     mub = 0.;
+  } else if (E.kind == 2) {
+    eos_chiral<true>(E, e, nb, T, mub, mus, p);
   } else {
     eos1f<true>(E, e, nb, T, mub, p);
   }
 }
 
-// EoS::s, src/eos.cpp:18-25 (muq = mus = 0)
+__device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
+                                         double& T, double& mub, double& p) {
+  double mus;
+  eos_eval(E, e, nb, T, mub, mus, p);
+}
+
+// EoS::s, src/eos.cpp:18-25 (muq = 0)
 __device__ __forceinline__ double eos_s(const EosDev& E, double e, double nb,
                                         double nq, double ns) {
-  double T, mub, p;
-  const double muq = 0., mus = 0.;
-  eos_eval(E, e, nb, T, mub, p);
+  double T, mub, mus, p;
+  const double muq = 0.;
+  eos_eval(E, e, nb, T, mub, mus, p);
   if (T > 0.0) return ddivp(e + p - mub * nb - muq * nq - mus * ns, T);
   return 0.;
 }

@@ -337,10 +337,10 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
   pD[3 * N + i] = d.vz;
   if (a.e <= 0.) return;
   {
-    double T, mub, p;
-    eos_eval(E, a.e, a.nb, T, mub, p);
-    // EoS::s at the same point (eos_s, muq = mus = 0) from this lookup
-    const double s = T > 0.0 ? ddivp(a.e + p - mub * a.nb - 0. * a.nq - 0. * a.ns, T) : 0.;
+    double T, mub, mus, p;
+    eos_eval(E, a.e, a.nb, T, mub, mus, p);
+    // EoS::s at the same point (eos_s, muq = 0) from this lookup
+    const double s = T > 0.0 ? ddivp(a.e + p - mub * a.nb - 0. * a.nq - mus * a.ns, T) : 0.;
     const double etaS = tr_etaS(tr, a.e, a.nb, T, mub, s, p);
     const double zetaS = tr_zetaS(tr, a.e, T, s, p);
     double taupi, tauPi;
@@ -1195,6 +1195,27 @@ __global__ void k_transport(TrDev tr, const double* __restrict__ in, long long n
 void launch_transport(const TrDev& tr, const double* in, long long n, double* out,
                       cudaStream_t s) {
   k_transport<<<nblk(n, 128), 128, 0, s>>>(tr, in, n, out);
+}
+
+// EoS::eos with muS, EoS::p and EoS::s (nq = ns = 0) on arrays:
+// e[n], nb[n] -> out[6][n] = p, T, muB, muS, p(), s
+__global__ void k_eos_eval(EosDev E, const double* __restrict__ e, const double* __restrict__ nb,
+                           long long n, double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double T, mub, mus, p;
+  eos_eval(E, e[i], nb[i], T, mub, mus, p);
+  out[i] = p;
+  out[n + i] = T;
+  out[2 * n + i] = mub;
+  out[3 * n + i] = mus;
+  out[4 * n + i] = eos_p(E, e[i], nb[i]);
+  out[5 * n + i] = eos_s(E, e[i], nb[i], 0., 0.);
+}
+
+void launch_eos_eval(const EosDev& E, const double* e, const double* nb, long long n, double* out,
+                     cudaStream_t s) {
+  k_eos_eval<<<nblk(n, 128), 128, 0, s>>>(E, e, nb, n, out);
 }
 
 // ------------------------------------------------------------ clock

@@ -115,6 +115,8 @@ void launch_resize_gather(const Geo& g, const double* src, double* dst, int ncom
 
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
                          cudaStream_t s);
+void launch_eos_eval(const EosDev& E, const double* e, const double* nb, long long n, double* out,
+                     cudaStream_t s);
 void launch_transport(const TrDev& tr, const double* in, long long n, double* out,
                       cudaStream_t s);
 

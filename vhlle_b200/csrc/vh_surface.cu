@@ -432,8 +432,8 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
   for (int q = 0; q < 7; q++) QC[q] = QC[q] / (tau + C[0]);
   Prim P;
   transform_pv(a.E, QC, P);
-  double TC, mubC, pC;
-  eos_eval(a.E, P.e, P.nb, TC, mubC, pC);
+  double TC, mubC, musC, pC;
+  eos_eval(a.E, P.e, P.nb, TC, mubC, musC, pC);
   const double eC = P.e, nbC = P.nb;
   double vxC = P.vx, vyC = P.vy, vzC = P.vz;
   double* ct = a.contrib + (long long)el * 5;
@@ -493,7 +493,7 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
   r[12] = TC;
   r[13] = mubC;
   r[14] = 0.;
-  r[15] = 0.;
+  r[15] = musC;
 #pragma unroll
   for (int q = 0; q < 10; q++) r[16 + q] = pc[q];
   r[26] = PiC;
@@ -594,8 +594,8 @@ __global__ void __launch_bounds__(128) k_corona_elements(SurfArgs a) {
     corona_qc(g, a.Q, ix, iy, iz, tau, QC);
     Prim P;
     transform_pv(a.E, QC, P);
-    double TC, mubC, pC;
-    eos_eval(a.E, P.e, P.nb, TC, mubC, pC);
+    double TC, mubC, musC, pC;
+    eos_eval(a.E, P.e, P.nb, TC, mubC, musC, pC);
     const double eC = P.e, nbC = P.nb;
     double vxC = P.vx, vyC = P.vy, vzC = P.vz;
     double* ct = a.contrib + (long long)el * 5;
@@ -653,7 +653,7 @@ __global__ void __launch_bounds__(128) k_corona_elements(SurfArgs a) {
     r[12] = TC;
     r[13] = mubC;
     r[14] = 0.;
-    r[15] = 0.;
+    r[15] = musC;
 #pragma unroll
     for (int q = 0; q < 10; q++) r[16 + q] = pc[q];
     r[26] = PiC;

@@ -33,6 +33,7 @@ from __future__ import annotations
 
 import dataclasses
 import math
+import os
 from typing import Optional
 
 import numpy as np
@@ -105,7 +106,8 @@ class Grid:
 @dataclasses.dataclass
 class EosTable:
     """EoS descriptor.  kind 0: conformal gas; kind 1: EoS1f (e, nb) table
-    with p/T/mub stored [ie + ne*inb] (src/eo1.cpp:21-45)."""
+    with p/T/mub stored [ie + ne*inb] (src/eo1.cpp:21-45); kind 2: EoSChiral
+    (src/eoChiral.cpp), `aux` = (chiralsmall, chiraleos) ChiralAux tables."""
     kind: int
     conf_cnst: float = CONF_CNST
     egrid: Optional[np.ndarray] = None
@@ -113,6 +115,17 @@ class EosTable:
     p: Optional[np.ndarray] = None
     T: Optional[np.ndarray] = None
     mub: Optional[np.ndarray] = None
+    aux: Optional[tuple] = None
+
+    def write_chiral(self, directory: str) -> None:
+        """directory/eos/chiralsmall.dat and chiraleos.dat, the files
+        EoSChiral reads from its working directory (src/eoChiral.cpp:153-156):
+        8 columns (T, mu_q, e, p, n, s, mu_S, unused) with n outer and e
+        inner, every value exact in 10 decimals."""
+        assert self.kind == 2
+        os.makedirs(os.path.join(directory, "eos"), exist_ok=True)
+        for name, cols, _ in _chiral_tables():
+            np.savetxt(os.path.join(directory, "eos", name), cols, fmt="%.10f")
 
     @property
     def ne(self) -> int:
@@ -159,6 +172,67 @@ class EosTable:
                     p[k] = 0.0
                 pos += 3
         return EosTable(kind=1, egrid=egrid, ngrid=ngrid, p=p, T=T, mub=mub)
+
+
+@dataclasses.dataclass
+class ChiralAux:
+    """One EoSaux table as its constructor leaves it (src/eoChiral.cpp:48-80):
+    uniform grids [emin, emax] x [nmin, nmax] (GeV/fm^3, fm^-3), p/T/mub/mus
+    (GeV/fm^3, GeV) at [in * ne + ie]."""
+    ne: int
+    nn: int
+    emin: float
+    emax: float
+    nmin: float
+    nmax: float
+    p: np.ndarray
+    T: np.ndarray
+    mub: np.ndarray
+    mus: np.ndarray
+
+
+# EoSChiral's table sizes and this generator's ranges in the files' units
+# (e in e0 = 0.146 GeV/fm^3, n in n0 = 0.15 fm^-3): the small table covers
+# e < 1.46 GeV/fm^3, nb < 0.3 fm^-3 and the big one e < 146, nb < 6, the
+# regions EoSChiral::eos sends to them (src/eoChiral.cpp:153-170)
+CHIRAL_TABLES = (("chiralsmall.dat", 201, 201, 10.0, 2.0), ("chiraleos.dat", 2001, 401, 1000.0, 40.0))
+
+
+def _q(x):
+    """Rounded to a multiple of 2^-10: exact in binary and in short decimal."""
+    return np.round(np.asarray(x, dtype=np.float64) * 1024.0) / 1024.0
+
+
+def _chiral_tables():
+    """(file name, the file's 8 columns, ChiralAux) per EoSChiral table."""
+    out = []
+    for name, ne, nn, emax_f, nmax_f in CHIRAL_TABLES:
+        e_f = _q(np.arange(ne) * (emax_f / (ne - 1)))
+        n_f = _q(np.arange(nn) * (nmax_f / (nn - 1)))
+        E, Nb = np.meshgrid(e_f, n_f)  # [in][ie]
+        T_f = _q(20.0 + 140.0 * (E + 0.05) ** 0.25 * (1.0 - 0.1 * Nb / nmax_f))
+        muq_f = _q(60.0 * Nb / (1.0 + 0.02 * E) + 0.5 * Nb ** 2)
+        p_f = _q(E / 3.0 * (1.0 - 0.3 * np.exp(-E)) - 0.02 + 0.01 * Nb)
+        s_f = _q((E + p_f) * 146.0 / T_f)
+        mus_f = _q(15.0 * Nb / (1.0 + E))
+        cols = np.stack([T_f, muq_f, E, p_f, Nb, s_f, mus_f, np.zeros_like(E)],
+                        axis=-1).reshape(-1, 8)
+        aux = ChiralAux(ne=ne, nn=nn, emin=e_f[0] * 0.146, emax=e_f[-1] * 0.146,
+                        nmin=n_f[0] * 0.15, nmax=n_f[-1] * 0.15,
+                        p=(p_f * 0.146).ravel(), T=(T_f / 1000.0).ravel(),
+                        mub=(muq_f * (3.0 / 1000.0)).ravel(), mus=(mus_f / 1000.0).ravel())
+        out.append((name, cols, aux))
+    return out
+
+
+def chiral_eos() -> EosTable:
+    """A synthetic EoSChiral (the chiral model's tables are not in the
+    reference tree): smooth T, mu_q, p, s, mu_S over each table's (e, n)
+    grid in the file units (MeV, e0, n0), every value a multiple of 2^-10,
+    converted as the reference's EoSaux constructor converts them (T / 1000,
+    mu_q * (3 / 1000), mu_S / 1000, p * 0.146, grid ends * 0.146 and * 0.15),
+    so that the files (write_chiral) and these arrays hold the same doubles."""
+    return EosTable(kind=2, aux=tuple(t[2] for t in _chiral_tables()))
 
 
 def cs2_model(e):
