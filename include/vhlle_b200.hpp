@@ -160,6 +160,93 @@ class EoS1f : public EoS {
   }
 };
 
+// EoSChiral (src/eoChiral.cpp): the reference's default EoS (eosType 1).
+// Reads dir/eos/chiraleos.dat (2001 x 401) and dir/eos/chiralsmall.dat
+// (201 x 201) in the EoSaux format (8 columns, nb outer, e inner) with its
+// unit conversions; the device evaluates the same tables.
+class EoSChiral : public EoS {
+  struct Aux {
+    int ne, nn;
+    double emin = 0., emax = 0., nmin = 0., nmax = 0.;
+    std::vector<double> p, T, mub, mus;  // [in * ne + ie]
+    Aux(const std::string& path, int Ne, int Nn) : ne(Ne), nn(Nn) {
+      std::ifstream fin(path);
+      if (!fin.good()) throw Error(VH_ERR_ARG, "EoSChiral: I/O error with " + path);
+      const size_t n = (size_t)ne * nn;
+      p.resize(n);
+      T.resize(n);
+      mub.resize(n);
+      mus.resize(n);
+      std::vector<double> e(ne), nb(nn);
+      double s, a;
+      for (int in = 0; in < nn; in++)
+        for (int ie = 0; ie < ne; ie++) {
+          const size_t k = (size_t)in * ne + ie;
+          fin >> T[k] >> mub[k] >> e[ie] >> p[k] >> nb[in] >> s >> mus[k] >> a;
+          T[k] /= 1000.0;
+          mub[k] *= 3.0 / 1000.0;
+          mus[k] /= 1000.0;
+          p[k] *= 0.146;
+        }
+      if (!fin) throw Error(VH_ERR_ARG, "EoSChiral: truncated table " + path);
+      emin = e[0] * 0.146;
+      emax = e[ne - 1] * 0.146;
+      nmin = nb[0] * 0.15;
+      nmax = nb[nn - 1] * 0.15;
+    }
+    void get(double e, double n, double& pp, double& TT, double& mb, double& ms) const {
+      if (e < 0.) {
+        TT = mb = ms = pp = 0.;
+        return;
+      }
+      const double de = (emax - emin) / (ne - 1), dn = (nmax - nmin) / (nn - 1);
+      int ie = (int)((e - emin) / de), in = (int)((n - nmin) / dn);
+      ie = std::min(std::max(ie, 0), ne - 2);
+      in = std::min(std::max(in, 0), nn - 2);
+      const double em = e - emin - ie * de, nm = n - nmin - in * dn;
+      const double we[2] = {1. - em / de, em / de}, wn[2] = {1. - nm / dn, nm / dn};
+      TT = mb = ms = pp = 0.0;
+      for (int je = 0; je < 2; je++)
+        for (int jn = 0; jn < 2; jn++) {
+          const size_t k = (size_t)(in + jn) * ne + ie + je;
+          pp += we[je] * wn[jn] * p[k];
+          TT += we[je] * wn[jn] * T[k];
+          mb += we[je] * wn[jn] * mub[k];
+          ms += we[je] * wn[jn] * mus[k];
+        }
+      if (pp < 0.0) pp = 0.0;
+    }
+    vh_eos_aux view() const {
+      return vh_eos_aux{ne, nn, emin, emax, nmin, nmax, p.data(), T.data(), mub.data(), mus.data()};
+    }
+  };
+  Aux small_, big_;
+
+ public:
+  explicit EoSChiral(const std::string& dir = ".")
+      : small_(dir + "/eos/chiralsmall.dat", 201, 201), big_(dir + "/eos/chiraleos.dat", 2001, 401) {}
+  void eos(double e, double nb, double, double, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    if (e < 1.46 && nb < 0.3)
+      small_.get(e, nb, p, T, mub, mus);
+    else if (e < 146. && nb < 6.)
+      big_.get(e, nb, p, T, mub, mus);
+    else {
+      p = 0.2964 * e;
+      T = 0.15120476935 * std::pow(e, 0.25);
+      mub = mus = 0.0;
+    }
+    muq = 0.0;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_CHIRAL;
+    d.aux[0] = small_.view();
+    d.aux[1] = big_.view();
+    return d;
+  }
+};
+
 // -------------------------------------------------------- TransportCoeff
 // src/trancoeff.h:6-45: the same public constants and constructor.
 class TransportCoeff {

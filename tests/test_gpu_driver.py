@@ -205,3 +205,34 @@ def test_cpp_driver_vorticity_equals_oracle(tmp_path):
     scale = np.maximum(np.abs(got[:, 16:32]).max(axis=1), np.abs(exp[:, 16:32]).max(axis=1))[:, None]
     ok = np.abs(got - exp) <= 1e-12 * np.maximum(np.abs(got), np.abs(exp)) + 1e-13 * scale + 1e-300
     assert ok.all(), np.argwhere(~ok)[:5]
+
+
+def test_cpp_driver_chiral_eos_equals_oracle(tmp_path):
+    """vhlle_run with the reference's default eosType 1 and its EoSChiral
+    tables under ./eos (src/main.cpp:291-292, src/eoChiral.cpp:153-156)
+    ends on the oracle's grid, bit for bit."""
+    import subprocess
+    from vhlle_b200 import build as B
+    drv = B.build_driver()
+    setup = W.glauber3d_nb_setup(17, 17, 9, eos=W.chiral_eos())
+    setup.eos.write_chiral(str(tmp_path))
+    ic = str(tmp_path / "ic.vhb")
+    W.write_snapshot(ic, setup.grid, setup.tau0, setup.dt, W.initial_snapshot_state(setup))
+    params = str(tmp_path / "params.txt")
+    tau_max = setup.tau0 + 3.5 * setup.dt
+    W.write_params(params, setup, tauMax=tau_max, tauGridResize=100.0, eosType=1)
+    run = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", "out"],
+                         capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr
+    assert "hydro EoS: EoSChiral" in run.stdout
+    o = P.OracleRun(setup)
+    g = setup.grid
+    while True:
+        o.advance(setup.dt, g.etamin, g.etamax, g.nz)
+        r, _ = o.surface(dtf=o.dt)
+        if not (o.tau_now < tau_max + 0.0001 and len(r) > 0):
+            break
+    nx, ny, nz, b, tau, dt, st = W.read_snapshot(str(tmp_path / "out" / "final.vhb"))
+    assert tau == o.tau_now
+    bad = compare_states(st, o.get_state())
+    assert not bad, bad

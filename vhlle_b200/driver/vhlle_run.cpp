@@ -8,8 +8,10 @@
 //
 // Parameters are read exactly as the reference reads them (same keys,
 // defaults, "CCC"/"UUU" echo).  The hydro EoS is the EoS1f table named by
-// the extra key eos1fFile, else the conformal gas of 47.5 degrees of
-// freedom.  Before the loop the corona of Fluid::outputCorona opens the
+// the extra key eos1fFile; else, for eosType 1 (the default), EoSChiral from
+// ./eos/chiraleos.dat and ./eos/chiralsmall.dat as the reference reads them;
+// else (those files absent, or another eosType) the conformal gas of 47.5
+// degrees of freedom.  Before the loop the corona of Fluid::outputCorona opens the
 // freeze-out file.  Each loop iteration does what Fluid::outputSurface does: it
 // appends the freeze-out elements to DIR/freezeout.dat.unfinished (renamed
 // freezeout.dat at the end) and prints the same line (tau, E, Efull,
@@ -93,10 +95,21 @@ int run(int argc, char** argv) {
   if (cl.isInputFile.empty()) throw vhb::Error(VH_ERR_ARG, "no -ISinput snapshot given");
 
   const double hbarc = 0.1973269804, deg = 16.0 + 3.0 * 12.0 * (7.0 / 8.0);
-  vhb::EoS* eos = P.eos1fFile.empty()
-                      ? static_cast<vhb::EoS*>(new vhb::EoSConformal(3.0 * deg * M_PI * M_PI / 90.0 /
-                                                                     (hbarc * hbarc * hbarc)))
-                      : static_cast<vhb::EoS*>(new vhb::EoS1f(P.eos1fFile.c_str()));
+  struct stat sb;
+  const bool chiral = P.eos1fFile.empty() && P.eosType == 1 &&
+                      stat("eos/chiraleos.dat", &sb) == 0 && stat("eos/chiralsmall.dat", &sb) == 0;
+  vhb::EoS* eos;
+  if (!P.eos1fFile.empty())
+    eos = new vhb::EoS1f(P.eos1fFile.c_str());
+  else if (chiral)  // src/main.cpp:291-292, the tables under ./eos as there
+    eos = new vhb::EoSChiral(".");
+  else
+    eos = new vhb::EoSConformal(3.0 * deg * M_PI * M_PI / 90.0 / (hbarc * hbarc * hbarc));
+  std::cout << "hydro EoS: "
+            << (!P.eos1fFile.empty() ? "EoS1f " + P.eos1fFile
+                                     : chiral ? std::string("EoSChiral (eos/chiraleos.dat, eos/chiralsmall.dat)")
+                                              : std::string("conformal gas"))
+            << std::endl;
   vhb::EoS* eosH = eos;
   vhb::TransportCoeff* trcoeff = new vhb::TransportCoeff(
       P.etaS, P.zetaS, P.ah, P.al, P.aRho, P.T0, P.etaSMin, P.etaSEpsilonMin, P.etaSShiftMuB,
