@@ -331,35 +331,46 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
   }
 }
 
+// EK selects the EoS kinds compiled in: EK_ANY (every kind, chosen at run
+// time), EK_TABLE (kinds 0 and 1) or EK_CHIRAL (kind 2).  The step's
+// con2prim kernels are instantiated per class: compiled into every
+// con2prim iteration next to the table lookup, the chiral lookup made those
+// kernels spill more (face kernels 25 % slower on the table kind).
+enum { EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2 };
+
+template <int EK = EK_ANY>
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
-  if (E.kind == 0) return ddivp(e, 3.);
   double T, mub, mus, p;
-  if (E.kind == 2)
+  if (EK == EK_CHIRAL || (EK == EK_ANY && E.kind == 2)) {
     eos_chiral<false>(E, e, nb, T, mub, mus, p);
-  else
-    eos1f<false>(E, e, nb, T, mub, p);
+    return p;
+  }
+  if (E.kind == 0) return ddivp(e, 3.);
+  eos1f<false>(E, e, nb, T, mub, p);
   return p;
 }
 
 // EoS::eos with muS (muQ is 0 for every kind here; muS only for kind 2)
+template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
                                          double& mub, double& mus, double& p) {
   mus = 0.;
-  if (E.kind == 0) {
+  if (EK == EK_CHIRAL || (EK == EK_ANY && E.kind == 2)) {
+    eos_chiral<true>(E, e, nb, T, mub, mus, p);
+  } else if (E.kind == 0) {
     p = ddivp(e, 3.);
     T = e > 0. ? sqrt(sqrt(e / E.conf_cnst)) : 0.;
     mub = 0.;
-  } else if (E.kind == 2) {
-    eos_chiral<true>(E, e, nb, T, mub, mus, p);
   } else {
     eos1f<true>(E, e, nb, T, mub, p);
   }
 }
 
+template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
                                          double& T, double& mub, double& p) {
   double mus;
-  eos_eval(E, e, nb, T, mub, mus, p);
+  eos_eval<EK>(E, e, nb, T, mub, mus, p);
 }
 
 // EoS::s, src/eos.cpp:18-25 (muq = 0)
@@ -378,6 +389,7 @@ __device__ __forceinline__ double eos_s(const EosDev& E, double e, double nb,
 // (a learned guess) the iteration starts there instead of at 0.5 and the
 // bracket is narrowed by the sign of f at g; the safeguarded Newton /
 // bisection then runs as in the reference until |dv| < E.tol.
+template <int EK = EK_ANY>
 __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim& o,
                                              float g = -1.f) {
   const int MAXIT = 100;
@@ -395,7 +407,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     o.e = Q[T_];
     o.vx = 0.; o.vy = 0.; o.vz = 0.;
     o.nb = Q[NB_]; o.nq = Q[NQ_]; o.ns = Q[NS_];
-    o.p = eos_p(E, o.e, o.nb);
+    o.p = eos_p<EK>(E, o.e, o.nb);
     return;
   }
   if (M > Q[T_]) {
@@ -415,7 +427,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     nq = Q[NQ_] * sq;
     ns = Q[NS_] * sq;
   }
-  p = eos_p(E, e, nb);
+  p = eos_p<EK>(E, e, nb);
   f = (Q[T_] + p) * v - M;
   df = (Q[T_] + p) - M * v * dpe;
   if (guessed) {
@@ -446,7 +458,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     nb = Q[NB_] * sq;
     nq = Q[NQ_] * sq;
     ns = Q[NS_] * sq;
-    p = eos_p(E, e, nb);
+    p = eos_p<EK>(E, e, nb);
     f = (Q[T_] + p) * v - M;
     df = (Q[T_] + p) - M * v * dpe;
     if (f > 0.)
@@ -474,7 +486,7 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     }
   }
   o.e = Q[T_] - M * v;
-  o.p = eos_p(E, o.e, nb);  // the last iterate's nb, as the reference
+  o.p = eos_p<EK>(E, o.e, nb);  // the last iterate's nb, as the reference
   const double sq = sqrt(1 - o.vx * o.vx - o.vy * o.vy - o.vz * o.vz);
   o.nb = Q[NB_] * sq;
   o.nq = Q[NQ_] * sq;

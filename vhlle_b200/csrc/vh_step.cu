@@ -69,7 +69,7 @@ __global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restri
 // unbounded build (80 registers, 6 blocks); 10 blocks are slower.  The
 // same sweep set k_update to 12 blocks (-14 %), k_visc_prims to 8 (-14 %),
 // k_visc_update to 8 (-10 %); k_is_advect stays unbounded (8 blocks: +52 %).
-template <int DIR, bool PRED>
+template <int DIR, bool PRED, int EK>
 // 7 blocks of 128 per SM (72 registers): measured against 6 and 8 blocks on
 // the 300-step event, 3 % faster than 8 (64 registers, more spills)
 __global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
@@ -116,8 +116,8 @@ __global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* 
     qr[k] = qlr[7 + k];
   }
   Prim pl, pr;
-  transform_pv(E, ql, pl, c2p_guess(E, L));
-  transform_pv(E, qr, pr, c2p_guess(E, R));
+  transform_pv<EK>(E, ql, pl, c2p_guess(E, L));
+  transform_pv<EK>(E, qr, pr, c2p_guess(E, R));
   const double dxdir = DIR == X_ ? g.dx : (DIR == Y_ ? g.dy : g.dz);
   double fl[7];
   unsigned e = 0;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* 
 // Gathers the six face fluxes and the Milne source (Hydro::source_step,
 // src/hdo.cpp:307-353), then Cell::updateQtoQhByFlux (predictor) or
 // Cell::updateByFlux (corrector), src/cll.cpp:70-88.
-template <bool PRED>
+template <bool PRED, int EK>
 __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __restrict__ Q,
                                                 double* __restrict__ Qh,
                                                 double* __restrict__ Qprev,
@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
   for (int k = 0; k < 7; k++) qin[k] = field[k * N + i];
   q_over(qin, tau1, q);
   Prim pp;
-  transform_pv(E, q, pp, c2p_guess(E, i));
+  transform_pv<EK>(E, q, pp, c2p_guess(E, i));
   if (!PRED && pA) {
     // con2prim(Qh / (tau_n + dt/2)) is the viscous stage's A =
     // con2prim(Qh / (tau_{n+1} - dt/2)) for every cell that the ghost copy
@@ -283,6 +283,7 @@ __global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char*
 __device__ __forceinline__ double maxM_at(const Geo& g, const double* __restrict__ m, int ix,
                                           int iy, int iz);
 
+template <int EK>
 __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr,
                                                     const double* __restrict__ Q,
                                                     const double* __restrict__ Qprev,
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     a.vz = pA[7 * N + i];
   } else {
     q_over(qh, tA, q);
-    transform_pv(E, q, a, c2p_guess(E, i));
+    transform_pv<EK>(E, q, a, c2p_guess(E, i));
     pA[0 * N + i] = a.e;
     pA[1 * N + i] = a.p;
     pA[2 * N + i] = a.nb;
@@ -330,7 +331,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
   }
   q_over(qh, tau, q);
   Prim d;
-  transform_pv(E, q, d, c2p_guess(E, i));
+  transform_pv<EK>(E, q, d, c2p_guess(E, i));
   pD[0 * N + i] = d.e;
   pD[1 * N + i] = d.vx;
   pD[2 * N + i] = d.vy;
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
   if (a.e <= 0.) return;
   {
     double T, mub, mus, p;
-    eos_eval(E, a.e, a.nb, T, mub, mus, p);
+    eos_eval<EK>(E, a.e, a.nb, T, mub, mus, p);
     // EoS::s at the same point (eos_s, muq = 0) from this lookup
     const double s = T > 0.0 ? ddivp(a.e + p - mub * a.nb - 0. * a.nq - mus * a.ns, T) : 0.;
     const double etaS = tr_etaS(tr, a.e, a.nb, T, mub, s, p);
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     for (int k = 0; k < 7; k++) qs[k] = src[k * N + i];
     q_over(qs, tt, q);
     Prim P;
-    transform_pv(E, q, P, c2p_guess(E, i));
+    transform_pv<EK>(E, q, P, c2p_guess(E, i));
     const double ut = 1.0 / sqrt(1.0 - P.vx * P.vx - P.vy * P.vy - P.vz * P.vz);
     const int o = w == 0 ? 0 : 5;
     pBC[(o + 0) * N + i] = ut;
@@ -1096,7 +1097,8 @@ cudaError_t step_kernels_setup() {
                               (int)kRelaxSmem);
 }
 
-int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
+template <int EK>
+static int launch_step_ek(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   const Geo& g = a.g;
   const int bs = a.block == 64 ? 64 : 128;
   const unsigned nb = nblk(g.N, bs);
@@ -1115,27 +1117,27 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
     const bool pred = pass == 0;
     const double* QQ = pred ? F.Q : F.Qh;
     if (pred) {
-      k_face<X_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
+      k_face<X_, true, EK><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
       done(KK_FACE_X);
-      k_face<Y_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.clk, F.err);
+      k_face<Y_, true, EK><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.clk, F.err);
       done(KK_FACE_Y);
       if (g.nz > 1) {
-        k_face<Z_, true><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
+        k_face<Z_, true, EK><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
         done(KK_FACE_Z);
       }
-      k_update<true><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
+      k_update<true, EK><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
                                        a.viscous ? F.pBC : nullptr, nullptr);
       done(KK_UPDATE);
     } else {
-      k_face<X_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
+      k_face<X_, false, EK><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fx, a.clk, F.err);
       done(KK_FACE_X);
-      k_face<Y_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.clk, F.err);
+      k_face<Y_, false, EK><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fy, a.clk, F.err);
       done(KK_FACE_Y);
       if (g.nz > 1) {
-        k_face<Z_, false><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
+        k_face<Z_, false, EK><<<nb, bs, 0, s>>>(g, a.eos, QQ, m, F.Fz, a.clk, F.err);
         done(KK_FACE_Z);
       }
-      k_update<false><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
+      k_update<false, EK><<<nb, bs, 0, s>>>(g, a.eos, F.Q, F.Qh, F.Qprev, F.Fx, F.Fy, F.Fz, a.clk, F.err,
                                         nullptr, a.viscous ? F.pA : nullptr);
       done(KK_UPDATE);
     }
@@ -1143,7 +1145,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   k_ghost<false><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
   done(KK_GHOST);
   if (a.viscous) {
-    k_visc_prims<<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
+    k_visc_prims<EK><<<nb, bs, 0, s>>>(g, a.eos, a.tr, F.Q, F.Qprev, F.Qh, m, F.pA, F.pD, F.pTh,
                                    F.pBC, a.clk, F.gdst);
     done(KK_VISC_PRIMS);
     if (a.vort) {
@@ -1169,6 +1171,10 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   k_ghost<true><<<nb, bs, 0, s>>>(g, F.gsrc, F.gdst, F.Q, F.Qh, F.pi, F.Pi);
   done(KK_GHOST);
   return launches;
+}
+
+int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
+  return a.eos.kind == 2 ? launch_step_ek<EK_CHIRAL>(a, s, mk) : launch_step_ek<EK_TABLE>(a, s, mk);
 }
 
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,

@@ -185,6 +185,7 @@ void launch_totals(const Geo& g, const EosDev& E, const Fields& f, double tau, d
 // ===================================================================
 namespace vh {
 
+template <int EK>
 __global__ void k_surf_energy(Geo g, EosDev E, const double* __restrict__ Q,
                               const double* __restrict__ Qprev, double tau, double taup,
                               double* __restrict__ eN, double* __restrict__ eP) {
@@ -201,12 +202,12 @@ __global__ void k_surf_energy(Geo g, EosDev E, const double* __restrict__ Q,
 #pragma unroll
   for (int k = 0; k < 7; k++) qs[k] = Q[k * N + i];
   q_over(qs, tau, q);
-  transform_pv(E, q, P);
+  transform_pv<EK>(E, q, P);
   eN[i] = P.e;
 #pragma unroll
   for (int k = 0; k < 7; k++) qs[k] = Qprev[k * N + i];
   q_over(qs, taup, q);
-  transform_pv(E, q, P);
+  transform_pv<EK>(E, q, P);
   eP[i] = P.e;
 }
 
@@ -386,14 +387,18 @@ struct SurfArgs {
   double* contrib;
 };
 
+template <int EK>
 __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncubes);
 
+// instantiated per EoS class, as the step's con2prim kernels are
+template <int EK>
 __global__ void __launch_bounds__(128) k_surf_elements(SurfArgs a) {
   const int ncubes = min(a.counters[0], a.cap_cubes), nel = min(a.counters[1], a.cap_el);
   for (int el = blockIdx.x * blockDim.x + threadIdx.x; el < nel; el += gridDim.x * blockDim.x)
-    surf_element(a, el, ncubes);
+    surf_element<EK>(a, el, ncubes);
 }
 
+template <int EK>
 __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncubes) {
   // the cube whose element range holds el: the last k with off[k] <= el
   int lo = 0, hi = ncubes;
@@ -431,9 +436,9 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
 #pragma unroll
   for (int q = 0; q < 7; q++) QC[q] = QC[q] / (tau + C[0]);
   Prim P;
-  transform_pv(a.E, QC, P);
+  transform_pv<EK>(a.E, QC, P);
   double TC, mubC, musC, pC;
-  eos_eval(a.E, P.e, P.nb, TC, mubC, musC, pC);
+  eos_eval<EK>(a.E, P.e, P.nb, TC, mubC, musC, pC);
   const double eC = P.e, nbC = P.nb;
   double vxC = P.vx, vyC = P.vy, vzC = P.vz;
   double* ct = a.contrib + (long long)el * 5;
@@ -689,7 +694,11 @@ __global__ void __launch_bounds__(kTotBlock) k_sum_cols(const double* __restrict
 
 void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double tau, double taup,
                         double* eN, double* eP, cudaStream_t s) {
-  k_surf_energy<<<(unsigned)((g.N + 127) / 128), 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN,
+  const unsigned nb = (unsigned)((g.N + 127) / 128);
+  if (E.kind == 2)
+    k_surf_energy<EK_CHIRAL><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
+  else
+    k_surf_energy<EK_TABLE><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN,
                                                                eP);
 }
 
@@ -740,7 +749,10 @@ void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double
                           int npartial, cudaStream_t s) {
   SurfArgs a{g,    E,    f.Q,      f.Qprev,   f.pi,   f.Pi, tau, dtf, ecrit,  xmin, ymin, zmin,
              cubes, counters, cap_cubes, cap_el, geo, off, rec, contrib};
-  k_surf_elements<<<kElemGrid, 128, 0, s>>>(a);
+  if (E.kind == 2)
+    k_surf_elements<EK_CHIRAL><<<kElemGrid, 128, 0, s>>>(a);
+  else
+    k_surf_elements<EK_TABLE><<<kElemGrid, 128, 0, s>>>(a);
   k_sum_cols<<<npartial, kTotBlock, 0, s>>>(contrib, 0, kSurfAcc, partial, counters + 1, cap_el);
   k_sum_cols<<<1, kTotBlock, 0, s>>>(partial, npartial, kSurfAcc, partial + npartial * kSurfAcc,
                                      nullptr, 0);
