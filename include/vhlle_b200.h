@@ -31,7 +31,9 @@
 extern "C" {
 #endif
 
-#define VH_ABI_VERSION 1
+/* 2: vh_eos gained the aux tables of VH_EOS_CHIRAL (a caller built against
+ * version 1 passes a shorter vh_eos) */
+#define VH_ABI_VERSION 2
 
 typedef int vh_status;
 #define VH_OK 0
