@@ -34,6 +34,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -86,7 +87,10 @@ class ClockSampler:
 
     def __init__(self, gpu_index):
         self.p = None
-        self.out = os.path.join(ROOT, "gpurun_out", "clocks_rank%s.csv" % os.environ.get("RANK", "0"))
+        # the raw samples go to $VH_CLOCKS_DIR (default: a temporary
+        # directory); the JSON line carries their summary
+        d = os.environ.get("VH_CLOCKS_DIR") or tempfile.mkdtemp(prefix="vh_clocks_")
+        self.out = os.path.join(d, "clocks_rank%s.csv" % os.environ.get("RANK", "0"))
         try:
             os.makedirs(os.path.dirname(self.out), exist_ok=True)
             self.f = open(self.out, "w")
