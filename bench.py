@@ -34,8 +34,8 @@ import json
 import os
 import statistics
 import subprocess
-import tempfile
 import sys
+import tempfile
 import time
 
 import numpy as np
