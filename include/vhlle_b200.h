@@ -316,6 +316,11 @@ vh_status vh_surface_write(vh_ctx *ctx, const char *path, int extendFO);
  * values of its elements.  on = 0 stops the per-step work (the stored
  * values stay).  Cells start at zero, and again after vh_resize2x. */
 vh_status vh_enable_vorticity(vh_ctx *ctx, int on);
+/* How many earlier lone increments of M[3][0] / M[3][3] (no row-3 write
+ * at their cell) one cell follows back before it folds its run by walking
+ * the loop positions in order instead (0-32, default 32).  The result is the
+ * same either way; for tests of both paths. */
+vh_status vh_vorticity_chain(vh_ctx *ctx, int n);
 /* Cell::getDbeta of every cell (src/cll.h:199-204): out[(4 mu + nu) * N +
  * i], clamped to [-100, 100] as Cell::setDbeta stores it.  Synchronous. */
 vh_status vh_get_dbeta(vh_ctx *ctx, double *out);

@@ -82,6 +82,24 @@ def test_gpu_dbeta_equals_oracle(case):
     d.close()
 
 
+@pytest.mark.parametrize("chain", [0, 1])
+def test_gpu_dbeta_ordered_walk_equals_oracle(chain):
+    """With the chain limit at 0 or 1 every run of lone increments is folded
+    by the ordered walk over loop positions: the same bits as the oracle."""
+    from vhlle_b200.capi import GpuHydro
+    setup = W.small_glauber3d(33, 17, seed=5, b=8.0)
+    o, d = P.OracleRun(setup, vorticity=True), GpuHydro(setup)
+    d.enable_vorticity()
+    d._check(d.L.vh_vorticity_chain(d.h, chain))
+    for k in range(4):
+        o.step(1)
+        d.step(1)
+        db = d.get_dbeta()
+        bad = (db != o.dbeta) & ~(np.isnan(db) & np.isnan(o.dbeta))
+        assert not bad.any(), (k, np.argwhere(bad)[:5])
+    d.close()
+
+
 def test_gpu_vorticity_resize_and_toggle():
     """Zero dbeta after a x2 resize, as the reference's new Fluid; turning
     vorticity off keeps the stored values and the step's results."""

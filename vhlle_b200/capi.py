@@ -29,7 +29,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
-           "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_get_dbeta",
+           "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_vorticity_chain", "vh_get_dbeta",
            "vh_surface_beta", "vh_surface_write_beta", "vh_corona", "vh_cornelius4d", "vh_set_con2prim",
            "vh_con2prim_stats", "vh_mlp_create", "vh_mlp_destroy", "vh_mlp_set_params",
            "vh_mlp_get_params", "vh_mlp_forward", "vh_mlp_grad", "vh_mlp_train",
@@ -308,6 +308,7 @@ def lib():
     L.vh_surface_write.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.vh_enable_vorticity.argtypes = [vp, ctypes.c_int]
     L.vh_get_dbeta.argtypes = [vp, _dp]
+    L.vh_vorticity_chain.argtypes = [vp, ctypes.c_int]
     L.vh_surface_beta.argtypes = [vp, _dp, ctypes.c_long, ctypes.POINTER(ctypes.c_long)]
     L.vh_surface_write_beta.argtypes = [vp, ctypes.c_char_p, ctypes.c_int]
     L.vh_set_con2prim.argtypes = [vp, ctypes.c_double]

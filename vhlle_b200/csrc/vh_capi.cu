@@ -1088,6 +1088,13 @@ vh_status vh_enable_vorticity(vh_ctx* ctx, int on) {
   return VH_OK;
 }
 
+vh_status vh_vorticity_chain(vh_ctx* ctx, int n) {
+  if (!ctx || n < 0 || n > 32) return VH_ERR_ARG;
+  ctx->vort.chain = n;
+  ctx->version++;  // the captured step holds the value
+  return VH_OK;
+}
+
 vh_status vh_get_dbeta(vh_ctx* ctx, double* out) {
   if (!ctx || !out) return VH_ERR_ARG;
   if (!ctx->vort.dbeta) return fail(ctx, VH_ERR_STATE, "vh_get_dbeta: vorticity never enabled");

@@ -66,6 +66,7 @@ struct VortDev {
   unsigned char* flag;  // [N] VF_* bits
   int* last;            // [5][N] per loop position: last writer positions
   int* agg;             // [5][blocks] block maxima, then their prefixes
+  int chain = 32;       // lone increments followed back before the ordered walk
 };
 int vort_scan_blocks(long long N);
 

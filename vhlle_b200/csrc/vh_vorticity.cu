@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(kVortBlock) k_vort_orphan(Geo g, VortDev v, in
   bool walk = false;
   for (long long c = p > 0 ? vort_last(v, N, nsb, 4, p - 1) : -1; c > L;
        c = c > 0 ? vort_last(v, N, nsb, 4, c - 1) : -1) {
-    if (n == kVortChain) {
+    if (n == min(v.chain, kVortChain)) {
       walk = true;
       break;
     }
