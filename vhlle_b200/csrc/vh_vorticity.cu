@@ -84,6 +84,7 @@ __device__ __forceinline__ void four_velocity(double vx, double vy, double vz, d
 
 // T at the prims of Qh at tau_{n+1} (Cell::getPrimVarHCenter(tau) then
 // EoS::eos, src/hdo.cpp:471-480): the same con2prim as k_visc_prims' pD
+template <int EK>
 __global__ void __launch_bounds__(kVortBlock) k_vort_T(Geo g, EosDev E,
                                                        const double* __restrict__ Qh,
                                                        const double* __restrict__ clk,
@@ -97,14 +98,15 @@ __global__ void __launch_bounds__(kVortBlock) k_vort_T(Geo g, EosDev E,
   for (int k = 0; k < 7; k++) qs[k] = Qh[k * N + i];
   q_over(qs, tau, q);
   Prim d;
-  transform_pv(E, q, d, c2p_guess(E, i));
+  transform_pv<EK>(E, q, d, c2p_guess(E, i));
   double T, mub, p;
-  eos_eval(E, d.e, d.nb, T, mub, p);
+  eos_eval<EK>(E, d.e, d.nb, T, mub, p);
   TD[i] = T;
 }
 
 // What NSquant does to M at cell i (src/hdo.cpp:397-414, 418-459, 466-500,
 // 512-546, 558-592, 606-611)
+template <int EK>
 __global__ void __launch_bounds__(kVortBlock) k_vort_ops(
     Geo g, EosDev E, const double* __restrict__ Q, const double* __restrict__ Qprev,
     const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
@@ -138,14 +140,14 @@ __global__ void __launch_bounds__(kVortBlock) k_vort_ops(
 #pragma unroll
     for (int k = 0; k < 7; k++) qs[k] = Qprev[k * N + i];
     q_over(qs, tau - dt, q);
-    transform_pv(E, q, P0, c2p_guess(E, i));
+    transform_pv<EK>(E, q, P0, c2p_guess(E, i));
 #pragma unroll
     for (int k = 0; k < 7; k++) qs[k] = Q[k * N + i];
     q_over(qs, tau, q);
-    transform_pv(E, q, P1, c2p_guess(E, i));
+    transform_pv<EK>(E, q, P1, c2p_guess(E, i));
     double T0, T1, mub, p;
-    eos_eval(E, P0.e, P0.nb, T0, mub, p);
-    eos_eval(E, P1.e, P1.nb, T1, mub, p);
+    eos_eval<EK>(E, P0.e, P0.nb, T0, mub, p);
+    eos_eval<EK>(E, P1.e, P1.nb, T1, mub, p);
     double u0[4], u1[4];
     four_velocity(P0.vx, P0.vy, P0.vz, u0);
     four_velocity(P1.vx, P1.vy, P1.vz, u1);
@@ -374,8 +376,15 @@ int launch_vorticity(const StepArgs& a, cudaStream_t s) {
   const VortDev& v = *a.vort;
   const unsigned nb = vblk(g.N, kVortBlock);
   const int nsb = vort_scan_blocks(g.N);
-  k_vort_T<<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
-  k_vort_ops<<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD, F.pTh, a.clk, v);
+  if (a.eos.kind == 2) {  // per EoS class, as the step's con2prim kernels
+    k_vort_T<EK_CHIRAL><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
+    k_vort_ops<EK_CHIRAL><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,
+                                                    F.pTh, a.clk, v);
+  } else {
+    k_vort_T<EK_TABLE><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
+    k_vort_ops<EK_TABLE><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,
+                                                   F.pTh, a.clk, v);
+  }
   k_vort_scan_blocks<<<nsb, kVortScan, 0, s>>>(g, v, nsb);
   k_vort_scan_aggs<<<1, 1024, 0, s>>>(v.agg, nsb);
   k_vort_orphan<<<nb, kVortBlock, 0, s>>>(g, v, nsb);
