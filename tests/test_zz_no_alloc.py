@@ -47,6 +47,15 @@ def _device_eos(torch, eos):
         d.ne, d.nn = len(eos.egrid), len(eos.ngrid)
         dp = ctypes.POINTER(ctypes.c_double)
         d.egrid, d.ngrid, d.p, d.T, d.mub = (ctypes.cast(t.data_ptr(), dp) for t in keep)
+    if eos.kind == 2:  # EoSChiral: both tables' planes on the device
+        dp = ctypes.POINTER(ctypes.c_double)
+        for k, a in enumerate(eos.aux):
+            ts = [torch.from_numpy(np.ascontiguousarray(x, dtype=np.float64)).cuda()
+                  for x in (a.p, a.T, a.mub, a.mus)]
+            keep += ts
+            x = d.aux[k]
+            x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax = a.ne, a.nn, a.emin, a.emax, a.nmin, a.nmax
+            x.p, x.T, x.mub, x.mus = (ctypes.cast(t.data_ptr(), dp) for t in ts)
     return d, keep
 
 
@@ -64,8 +73,9 @@ def _noalloc_step(L, setup, eos_d, dev, tau):
 
 
 @pytest.mark.parametrize("make", [lambda: W.small_glauber3d(21, 11),
-                                  lambda: W.gubser_setup(nx=31, ny=31)],
-                         ids=["viscous_21x21x11", "gubser_31x31"])
+                                  lambda: W.gubser_setup(nx=31, ny=31),
+                                  lambda: W.glauber3d_nb_setup(17, 17, 9, eos=W.chiral_eos())],
+                         ids=["viscous_21x21x11", "gubser_31x31", "chiral_nb_17x17x9"])
 def test_noalloc_step_matches_the_context_step_twice(make):
     torch = pytest.importorskip("torch")
     setup = make()
