@@ -52,10 +52,13 @@ WORKLOAD = ("3D viscous single event %s (x,y in [-15,15] fm, eta_s in [-7.5,7.5]
             "seeded MC-Glauber Pb+Pb b=7 fm, peak e=50 GeV/fm^3, Cornelius surface at "
             "e_f=0.5 GeV/fm^3 every 2 steps")
 SURF_EVERY = 2
+EVENT_SEED = 20260001  # the Glauber event of the timed run (rank r: EVENT_SEED + r)
 COMPULSORY_B = 288  # bytes per cell-update: Q[7] + pi[10] + Pi, read + write
 
-# Algorithmic bytes per cell per launch of each kernel (fields each launch
-# must read and write once; stencil neighbours come from cache).
+# Algorithmic bytes of each kernel: the fields a launch must read and write
+# once (stencil neighbours come from cache), per grid cell, or for the
+# relaxation and the advection per cell on the packed list of cells with
+# matter (nactive, read from the device every step).
 KERNEL_BYTES = {
     "k_update_m": 48,       # m[3] in, m[3] out
     "k_face_x": 120,        # Q or Qh [7] + m in, face flux [7] out
@@ -64,11 +67,38 @@ KERNEL_BYTES = {
     "k_update": 336,        # 3 face fluxes [21] + Q/Qh [7] in, 2 x [7] out
     "k_ghost": 0,           # boundary planes only
     "k_visc_prims": 152,    # Qh [7] in, prims [8] + [4] out
-    "k_is_relax": 528,      # Q, Qprev [14], m [3], prims [12], pi, Pi [11] in; pi0, piH0, Pi0, PiH0 [22], flux [4] out
-    "k_is_advect": 496,     # prims [5], pi0, piH0, Pi0, PiH0 [22], flux [4] in; pi, piH, Pi, PiH, vcc [23], flux [4] out
     "k_visc_update": 288,   # prims [4], piH [10], PiH, m [3], flux [4], Q [7] in; Q [7] out
 }
+RELAX_ACTIVE_B = 528  # per listed cell: Q, Qprev [14], m [3], prims [12], pi, Pi [11] in;
+                      # pi0, piH0, Pi0, PiH0 [22], flux [4] out
+RELAX_VACUUM_B = 208  # per empty cell, by the list kernel: pi0, piH0, Pi0, PiH0, flux [26] out
+RELAX_LIST_B = 12     # per cell: e of the half-step prims in, per listed cell its index out
+ADVECT_ACTIVE_B = 496  # per listed cell: prims [5], pi0, piH0, Pi0, PiH0 [22], flux [4] in;
+                       # pi, piH, Pi, PiH, vcc [23], flux [4] out
+KERNEL_BYTES_RULE = {
+    "k_is_relax": "%d B x listed cells + %d B x empty cells + %d B x cells (k_relax_list + k_is_relax)"
+                  % (RELAX_ACTIVE_B, RELAX_VACUUM_B, RELAX_LIST_B),
+    "k_is_advect": "%d B x listed cells" % ADVECT_ACTIVE_B,
+}
+for _k, _b in KERNEL_BYTES.items():
+    KERNEL_BYTES_RULE[_k] = "%d B x cells" % _b
 
+
+def kernel_alg_bytes(prof, cells, nactive):
+    """Algorithmic bytes of every profiled kernel summed over its launches;
+    nactive is the listed-cell count summed over the profiled steps."""
+    out = {}
+    for k, (n, _) in prof.items():
+        if k in KERNEL_BYTES:
+            out[k] = float(KERNEL_BYTES[k]) * cells * n
+    if "k_is_relax" in prof:
+        n = prof["k_is_relax"][0]
+        out["k_is_relax"] = (RELAX_ACTIVE_B * nactive + RELAX_VACUUM_B * (n * cells - nactive)
+                             + RELAX_LIST_B * n * cells)
+    if "k_is_advect" in prof:
+        out["k_is_advect"] = float(ADVECT_ACTIVE_B) * nactive
+    return out
+STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")  # persistent per-cell state
 STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")  # persistent per-cell state
 
 
@@ -78,6 +108,29 @@ def measured_peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def fp64_peak_tflops(device, n=8192, reps=6):
+    """FP64 throughput of a cuBLAS DGEMM (n x n x n, through torch) on this
+    GPU, measured now: the denominator of the FP64 co-roofline (the B200's
+    FP64 rate is the same on its tensor and CUDA-core paths)."""
+    import torch
+    dev = "cuda:%d" % device
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = torch.mm(a, b)
+    torch.cuda.synchronize(dev)
+    s = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        torch.mm(a, b, out=c)
+    e1.record(s)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (ms / 1e3) / 1e12
 
 
 class ClockSampler:
@@ -129,6 +182,16 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def gpu_index_for(local_rank):
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     if vis:
@@ -138,15 +201,19 @@ def gpu_index_for(local_rank):
     return str(local_rank)
 
 
-def traffic_per_cell(kernel):
-    """DRAM bytes per cell of one launch of `kernel` from the committed ncu
-    summary (profiles/traffic.json), or None."""
+def traffic_per_launch(kernel, grid, steps, launches):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed
+    ncu summary of the same workload and steps (profiles/traffic.json:
+    per grid, per kernel, the bytes of each launch in step order), averaged
+    over this run's launches; None if no capture covers them."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
+    d = json.load(open(p)).get("x".join(map(str, grid)), {})
     v = d.get(kernel)
-    return None if v is None else float(v["bytes_per_cell"])
+    if not v or len(v["bytes_per_launch"]) < launches:
+        return None
+    return float(sum(v["bytes_per_launch"][:launches]) / launches)
 
 
 def cpu_baseline_sample(setup, steps=2):
@@ -169,19 +236,20 @@ def cpu_baseline_sample(setup, steps=2):
         run.close()
     cells = setup.grid.ncells
     return {"value": cells * steps / dt, "unit": UNIT, "cores": 1, "kind": kind,
+            "cpu_model": cpu_model(),
             "sample": "%d performStep calls of the %dx%dx%d event with the freeze-out "
                       "surface after every %d, after 1 warm-up step, one thread, %.1f s"
                       % (steps, setup.grid.nx, setup.grid.ny, setup.grid.nz, SURF_EVERY, dt)}
 
 
 def _ref_worker(args):
-    seed, steps, budget = args
+    seed, steps, budget, grid = args
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from vhlle_b200 import workloads as W
     import pyoracle as P
     import tempfile
-    setup = W.glauber3d_setup(seed=seed)
+    setup = W.glauber3d_setup(*grid, seed=seed)
     ref = P.ref_available()
     run = P.RefRun(setup) if ref else P.OracleRun(setup)
     done = 0
@@ -211,8 +279,9 @@ def run_reference_arm(args):
     steps = max(1, args.steps)
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
+    # every process steps its own copy of the event the GPU arm times
     with ctx.Pool(nproc) as pool:
-        res = pool.map(_ref_worker, [(20260001 + k, steps, budget) for k in range(nproc)])
+        res = pool.map(_ref_worker, [(EVENT_SEED, steps, budget, args.grid)] * nproc)
     wall = time.perf_counter() - t0
     total = sum(r[0] for r in res)
     slowest = max(r[1] for r in res)
@@ -222,13 +291,14 @@ def run_reference_arm(args):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD % "101x101x51",
+        "config": {"workload": WORKLOAD % ("x".join(map(str, args.grid))),
                    "path": "reference C++ Hydro::performStep + Fluid::outputSurface every %d steps"
                            % SURF_EVERY},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": nproc, "kind": kind,
-                         "sample": "%d processes, each stepping its own copy of the event (surface every "
-                                   "%d steps) for up to %d steps or %.0f s; %.1f s wall"
-                                   % (nproc, SURF_EVERY, steps, budget, wall)},
+                         "cpu_model": cpu_model(),
+                         "sample": "%d processes, each stepping its own copy of the event (seed %d, "
+                                   "surface every %d steps) for up to %d steps or %.0f s; %.1f s wall"
+                                   % (nproc, EVENT_SEED, SURF_EVERY, steps, budget, wall)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -402,8 +472,14 @@ def main():
         h.enable_vorticity()
     lps = h.launches_per_step()
 
-    # warm-up on the event itself, then restart the event for the timed run
-    h.step(args.warmup)
+    # warm-up on the event itself (steps and pipelined surface calls, so
+    # that the surface buffers and the step graphs exist before the timed
+    # loop), then restart the event for the timed run
+    for k in range(1, max(args.warmup, SURF_EVERY) + 1):
+        h.step(1)
+        if k % SURF_EVERY == 0:
+            h.surface_begin()
+            h.surface_end()
     h.sync()
     h.upload_initial()
     h.L.vh_set_tau(h.h, setup.tau0)
@@ -439,8 +515,10 @@ def main():
     h.L.vh_set_tau(h.h, setup.tau0)
     h.profile(True)
     surf_ms_tot = 0.0
+    nactive = 0  # cells the relaxation and the advection ran on, summed over the steps
     for k in range(1, args.steps + 1):
         h.step(1)
+        nactive += h.active_cells()
         if k % SURF_EVERY == 0:
             h.timer_start()
             h.surface_only()
@@ -451,22 +529,29 @@ def main():
     ms_max = dist.max(ms)
     value = ws * cells * args.steps / (ms_max / 1e3)
 
-    # dominant kernel roofline
+    # per-kernel algorithmic bytes over the timed steps and the dominant
+    # kernel's roofline
     peak, peak_kind = measured_peaks()
+    alg_total = kernel_alg_bytes(prof, cells, nactive)
     dom = max(prof.items(), key=lambda kv: kv[1][1])
     dname, (dn, dms) = dom
     avg_s = dms / dn / 1e3
-    alg = KERNEL_BYTES.get(dname, 0) * cells
+    alg = alg_total.get(dname, 0.0) / dn
     achieved = alg / avg_s / 1e9
-    tpc = traffic_per_cell(dname)
     roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": None if tpc is None else tpc * cells,
-                "alg_bytes_per_launch": alg, "avg_launch_ms": avg_s * 1e3}
+                "traffic": traffic_per_launch(dname, args.grid, args.steps, dn),
+                "alg_bytes_per_launch": alg, "avg_launch_ms": avg_s * 1e3,
+                "active_cells_per_step": nactive / args.steps,
+                "alg_bytes_rule": KERNEL_BYTES_RULE.get(dname, "")}
     step_bw = COMPULSORY_B * cells * args.steps / (ms / 1e3) / 1e9
     step_roofline = {"bound": "hbm", "achieved": step_bw, "peak": peak, "unit": "GB/s",
                      "frac": step_bw / peak, "bytes_per_cell_update": COMPULSORY_B}
-    kernels = {k: {"launches": n, "total_ms": t, "share": t / ms} for k, (n, t) in prof.items()}
+    kernels = {}
+    for k, (n, t) in prof.items():
+        kernels[k] = {"launches": n, "total_ms": t, "share": t / ms}
+        if k in alg_total and t > 0:
+            kernels[k]["alg_gbs"] = alg_total[k] / (t / 1e3) / 1e9
     nsurf = args.steps // SURF_EVERY
     kernels["surface (vh_surface, 9 kernels)"] = {"launches": nsurf, "total_ms": surf_ms_tot,
                                                    "share": surf_ms_tot / ms, "elements": nel}

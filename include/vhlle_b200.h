@@ -158,6 +158,20 @@ vh_status vh_set_tau(vh_ctx *ctx, double tau);
  * No counterpart in the reference (its tolerance is a literal). */
 vh_status vh_set_con2prim(vh_ctx *ctx, double tol);
 
+/* The con2prim root find's Newton slope.  VH_C2P_REFERENCE (the default):
+ * the reference's constant dp/de = 1/3 (src/rmn.cpp:36,96), which converges
+ * linearly wherever c_s^2 differs from 1/3.  VH_C2P_TABLE_SLOPE: the EoS's
+ * own local derivatives, f'(v) = Q_t + p - v (M dp/de + dp/dnb Q_nb v /
+ * sqrt(1 - v^2)), quadratic inside a table cell, with the same bisection
+ * safeguard and a stop on an exactly zero residual (the reference's bracket
+ * test would send an exact root into bisection).  Only with a tight
+ * tolerance (tol <= 1e-10, where the root does not depend on the path to
+ * it); it is not the reference's iteration.  Applies to the step's root
+ * finds.  No counterpart in the reference. */
+#define VH_C2P_REFERENCE 0
+#define VH_C2P_TABLE_SLOPE 1
+vh_status vh_set_con2prim_method(vh_ctx *ctx, int method);
+
 /* The learned con2prim start point.  A vh_mlp is a 4 -> 64 -> 64 -> 3
  * network (SiLU; BF16 weights and activations, FP32 accumulation) from the
  * features x = (0.1 ln T^00, min(|T^0i|/T^00, 1.5), J^0/T^00,
@@ -224,6 +238,12 @@ vh_status vh_advance(vh_ctx *ctx, double dtau, double etamin, double etamax,
  * the new cell size returns VH_ERR_ARG with nothing changed (the reference
  * exits).  *resized may be NULL. */
 vh_status vh_resize2x(vh_ctx *ctx, int *resized);
+
+/* The number of cells the last viscous step relaxed and advected: those
+ * with e > 0 at the half step, the cells ISformal does not zero
+ * (src/hdo.cpp:694-708); 0 for an ideal context.  Waits for the stream.
+ * For measurements (the relaxation's bytes per launch scale with it). */
+vh_status vh_active_cells(vh_ctx *ctx, long long *n);
 
 /* Waits for the context's work; returns VH_ERR_NUMERIC if a step set the
  * device error word (then vh_error_bits tells which check fired). */
@@ -298,10 +318,14 @@ vh_status vh_surface_device(vh_ctx *ctx, const double **rec, long *n);
  * the device until the next surface or corona call).  One call in flight per
  * context; vh_surface, vh_corona and the record getters refuse while one is.
  * The call runs with the buffers earlier calls left (64k hypercubes and
- * twice as many elements at first, grown by any call that found more); if
- * it finds more than they hold, vh_surface_end grows them and returns
- * VH_ERR_STATE without results, since the fields have moved on by then
- * (vh_surface, which re-runs on the same fields, has no such case). */
+ * twice as many elements at first, grown by any call that found more).  If
+ * it finds more than they hold, its pass copies the fields it reads (Q,
+ * Qprev, pi, Pi, and dbeta with vorticity on: 25 or 41 doubles per cell,
+ * allocated by the first vh_surface_begin) on the device, and
+ * vh_surface_end grows the buffers and runs the pass again on that copy,
+ * after whatever the caller queued in between: no call loses elements.
+ * While a call is pending, vh_upload_state, vh_upload_async, vh_resize2x,
+ * vh_enable_vorticity and vh_set_stream return VH_ERR_STATE. */
 vh_status vh_surface_begin(vh_ctx *ctx, double ecrit);
 vh_status vh_surface_end(vh_ctx *ctx, vh_surface_info *info);
 /* Appends the last call's elements to a text file as freezeout.dat lines
@@ -430,9 +454,15 @@ vh_status vh_transport_eval(vh_ctx *ctx, const double *in_dev, long n,
  * VH_NOALLOC_MAX_CELLS cells and VH_NOALLOC_MAX_DIM cells per dimension
  * (about 21 MB held on every GPU that loads the library until exit); larger
  * grids are rejected with VH_ERR_ARG.  Nothing is allocated: no cudaMalloc,
- * cudaFree, host malloc or library allocator is called.  The first call on a
- * device looks up the array's device address (cudaGetSymbolAddress), so make
- * that first call before any stream capture on the device.  Every call on a
+ * cudaFree, host malloc or library allocator is called.  The array is a
+ * module variable: the CUDA runtime maps it (and loads the step kernels)
+ * when the library's module is first used on a device, which with lazy
+ * module loading (the default) is the first look-up of its address.  Call
+ * vh_noalloc_prepare(device) once per device before reserving your own
+ * device memory pool and before any stream capture: it does that look-up
+ * and the kernels' set-up, so that later calls take no device memory at
+ * all.  Without it, the first vh_step_noalloc call on a device does the
+ * same set-up (and may then fail for lack of memory).  Every call on a
  * device shares the array: calls whose GPU work overlaps race, so serialise
  * them.  The call waits for `stream`, writes the device error word to
  * *error_bits (if not NULL) and returns VH_ERR_NUMERIC when it is nonzero;
@@ -444,6 +474,10 @@ vh_status vh_step_noalloc(const vh_grid *grid, const vh_eos *eos_dev,
                           const vh_state_view *state, void *stream,
                           unsigned *error_bits);
 const char *vh_noalloc_last_error(void);
+/* The set-up of vh_step_noalloc on CUDA device `device` (made current for
+ * the call and restored after): maps the scratch array, looks up its
+ * address and sets the step kernels' attributes.  Idempotent. */
+vh_status vh_noalloc_prepare(int device);
 
 #ifdef __cplusplus
 }

@@ -47,7 +47,7 @@ class _Eos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
-                ("tol", ctypes.c_double), ("aux", _Aux * 2)]
+                ("tol", ctypes.c_double), ("aux", _Aux * 2), ("crmath", ctypes.c_int)]
 
 
 class _Trc(ctypes.Structure):
@@ -56,7 +56,8 @@ class _Trc(ctypes.Structure):
         "etaSShiftMuB", "etaSScaleMuB", "zetaSPeakEpsilon", "zetaSScaleBeta",
         "zetaSSigmaMinus", "zetaSSigmaPlus")] + [
         ("etaSparam", ctypes.c_int), ("zetaSparam", ctypes.c_int),
-        ("zetaSPeakT", ctypes.c_double), ("zetaSWidthT", ctypes.c_double)]
+        ("zetaSPeakT", ctypes.c_double), ("zetaSWidthT", ctypes.c_double),
+        ("crmath", ctypes.c_int)]
 
 
 class _State(ctypes.Structure):
@@ -130,6 +131,7 @@ def ref_lib():
         lib.ref_get_state.argtypes = [ctypes.c_void_p] + [_dp] * 9
         lib.ref_transform_pv.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_transport_eval.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_set_prim_var.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_output_corona.restype = ctypes.c_int
         lib.ref_output_corona.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                           ctypes.c_char_p, ctypes.c_int]
@@ -243,28 +245,33 @@ class _EosHolder:
                 x.p, x.T, x.mub, x.mus = (_ptr(v) for v in arrs)
 
 
-def _trc(setup):
+def _trc(setup, crmath=False):
     t = _Trc()
     for k, v in setup.tr.items():
         setattr(t, k, float(v))
     t.etaSparam = setup.etaSparam
     t.zetaSparam = setup.zetaSparam
+    t.crmath = int(crmath)
     return t
 
 
 class OracleRun:
     """The C restatement driven like Hydro: step() == performStep()."""
 
-    def __init__(self, setup, tol=None, vorticity=False):
+    def __init__(self, setup, tol=None, vorticity=False, crmath=False):
         """tol: the transformPV stopping tolerance (None: the reference's
         1e-5; a smaller value gives the tight-tolerance oracle).  vorticity:
-        Hydro::enableVorticity, d_mu beta_nu per cell in self.dbeta."""
+        Hydro::enableVorticity, d_mu beta_nu per cell in self.dbeta.
+        crmath: exp and x^(1/4) in the transport coefficients and EoSChiral's
+        power law correctly rounded, as the CUDA path evaluates them (False:
+        the C library's, as the reference does)."""
         self.setup = setup
         g = setup.grid
         self.grid = _Grid(g.nx, g.ny, g.nz, *g.bounds())
         self.eos = _EosHolder(setup.eos)
         self.eos.s.tol = 0.0 if tol is None else float(tol)
-        self.trc = _trc(setup)
+        self.eos.s.crmath = int(crmath)
+        self.trc = _trc(setup, crmath)
         self.state = initial_state(setup)
         self.tau = ctypes.c_double(setup.tau0)
         self.dt = setup.dt
@@ -534,6 +541,14 @@ class RefRun:
         Q = np.ascontiguousarray(Q, dtype=np.float64).reshape(-1, 7)
         out = np.zeros((len(Q), 8))
         self.lib.ref_transform_pv(self.h, _ptr(Q), len(Q), _ptr(out))
+        return out
+
+    def set_prim_var(self, inp):
+        """Cell::setPrimVar on n points: inp[n][8] = tau, e, nb, nq, ns, vx,
+        vy, vz -> the stored Q [n][7]."""
+        inp = np.ascontiguousarray(inp, dtype=np.float64).reshape(-1, 8)
+        out = np.zeros((len(inp), 7))
+        self.lib.ref_set_prim_var(self.h, _ptr(inp), len(inp), _ptr(out))
         return out
 
     def transport_eval(self, inp):

@@ -305,6 +305,19 @@ void ref_transform_pv(void *p, const double *Q, int n, double *out) {
   }
 }
 
+// Cell::setPrimVar (src/cll.cpp:222-241) with the run's EoS, through a
+// scratch Cell: in[n][8] = tau, e, nb, nq, ns, vx, vy, vz -> out[n][7] = the
+// Q it stores.  The IC modules end with this call for every cell.
+void ref_set_prim_var(void *p, const double *in, int n, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  Cell c;
+  for (int i = 0; i < n; i++) {
+    const double *a = in + 8 * i;
+    c.setPrimVar(r->eos, a[0], a[1], a[2], a[3], a[4], a[5], a[6], a[7]);
+    c.getQ(out + 7 * i);
+  }
+}
+
 // TransportCoeff::getEta + getTau: in[n][6] = e, nb, T, muB, s, p ->
 // out[n][4] = eta/s, zeta/s, tau_pi, tau_Pi
 void ref_transport_eval(void *p, const double *in, int n, double *out) {

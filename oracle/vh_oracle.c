@@ -145,7 +145,7 @@ static void eos_chiral(const or_eos *E, double e, double nb, double *T,
     chiral_aux(&E->aux[1], e, nb, p, T, mub, mus);
   else {
     *p = 0.2964 * e;
-    *T = 0.15120476935 * pow(e, 0.25);
+    *T = 0.15120476935 * (E->crmath ? or_root4_cr(e) : pow(e, 0.25));
     *mub = *mus = 0.0;
   }
 }
@@ -281,6 +281,8 @@ static void transform_pv(const or_eos *E, double Q[7], double *e, double *p,
 
 /* TransportCoeff::zetaS, src/trancoeff.cpp:19-66.  cs2(e) is the EoS base
  * class value 1/3 for both supported EoS kinds (src/eos.h:37). */
+#define TR_EXP(x) (t->crmath ? or_exp_cr(x) : exp(x))
+#define TR_ROOT4(x) (t->crmath ? or_root4_cr(x) : pow((x), 0.25))
 static double tr_zetaS(const or_trc *t, double e, double T, double s,
                        double P) {
   const double cs2e = 1. / 3.;
@@ -288,16 +290,16 @@ static double tr_zetaS(const or_trc *t, double e, double T, double s,
                B_width = 1.5, T_peak2 = 0.160, B_norm2 = 0.13, B1 = 0.01,
                B2 = 0.12;
   if (t->zetaSparam == 0)
-    return t->zetaS0 * (1. / 3. - cs2e) / (exp((0.16 - T) / 0.001) + 1.);
+    return t->zetaS0 * (1. / 3. - cs2e) / (TR_EXP((0.16 - T) / 0.001) + 1.);
   else if (t->zetaSparam == 1) {
     if (T < 0.180)
-      return 0.03 + (0.08 * exp(((T / T_p) - 1.) / (0.0025))) +
-             (0.22 * exp(((T / T_p) - 1) / (0.022)));
+      return 0.03 + (0.08 * TR_EXP(((T / T_p) - 1.) / (0.0025))) +
+             (0.22 * TR_EXP(((T / T_p) - 1) / (0.022)));
     else if (T >= 0.180 && T < 0.200)
       return 27.55 * (T / T_p) - 13.45 - (13.77 * (T / T_p) * (T / T_p));
     else if (T >= 0.200)
-      return 0.001 + (0.9 * exp(-((T / T_p) - 1.) / (0.0025))) +
-             (0.25 * exp(-((T / T_p) - 1.) / (0.13)));
+      return 0.001 + (0.9 * TR_EXP(-((T / T_p) - 1.) / (0.0025))) +
+             (0.25 * TR_EXP(-((T / T_p) - 1.) / (0.13)));
   } else if (t->zetaSparam == 2) {
     if (T > T_peak)
       return B_norm * ((B_width * B_width) /
@@ -305,24 +307,24 @@ static double tr_zetaS(const or_trc *t, double e, double T, double s,
                         (B_width * B_width)));
     else if (T <= T_peak)
       return B_norm *
-             (exp(-((T - T_peak) / T_width) * ((T - T_peak) / T_width)));
+             (TR_EXP(-((T - T_peak) / T_width) * ((T - T_peak) / T_width)));
   } else if (t->zetaSparam == 3) {
     if (T < T_peak2)
-      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B1 * B1)));
+      return B_norm2 * TR_EXP(-((T - T_peak2) * (T - T_peak2) / (B1 * B1)));
     else if (T >= T_peak2)
-      return B_norm2 * exp(-((T - T_peak2) * (T - T_peak2) / (B2 * B2)));
+      return B_norm2 * TR_EXP(-((T - T_peak2) * (T - T_peak2) / (B2 * B2)));
   } else if (t->zetaSparam == 4) {
     /* abs() binds to int abs(int) in the reference: |s| < 1 reads as 0 */
     if (!(fabs(s) >= 1.0) || T < 1e-1) return 0;
     const double d =
-        t->zetaSScaleBeta * (pow(e, 0.25) - pow(t->zetaSPeakEpsilon, 0.25));
+        t->zetaSScaleBeta * (TR_ROOT4(e) - TR_ROOT4(t->zetaSPeakEpsilon));
     const double sig =
         e < t->zetaSPeakEpsilon ? t->zetaSSigmaMinus : t->zetaSSigmaPlus;
-    return ((e + P) / (s * T)) * t->zetaS0 * exp(d * d / 2.0 * (sig * sig));
+    return ((e + P) / (s * T)) * t->zetaS0 * TR_EXP(d * d / 2.0 * (sig * sig));
   } else if (t->zetaSparam == 5) {
     /* a Gaussian bump in T: this build's addition, not in the reference */
     const double x = T - t->zetaSPeakT;
-    return t->zetaS0 * exp(-x * x / (2. * t->zetaSWidthT * t->zetaSWidthT));
+    return t->zetaS0 * TR_EXP(-x * x / (2. * t->zetaSWidthT * t->zetaSWidthT));
   }
   return 0.;
 }

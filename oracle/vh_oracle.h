@@ -50,7 +50,12 @@ typedef struct or_eos {
    * learned-guess path is checked against. */
   double tol;
   or_aux aux[2]; /* kind 2: chiralsmall, chiraleos */
+  int crmath; /* as or_trc.crmath, for EoSChiral's power law */
 } or_eos;
+
+/* Correctly rounded exp(x) and x^(1/4) (oracle/crm_shim.cpp). */
+double or_exp_cr(double x);
+double or_root4_cr(double x);
 
 /* TransportCoeff (src/trancoeff.h:6-45) public constants */
 typedef struct or_trc {
@@ -61,6 +66,12 @@ typedef struct or_trc {
   /* zetaSparam 5, an addition of this build (no reference counterpart):
    * zeta/s = zetaS0 exp(-(T - zetaSPeakT)^2 / (2 zetaSWidthT^2)) */
   double zetaSPeakT, zetaSWidthT;
+  /* 0: exp and pow(x, 0.25) from the C library, as the reference computes
+   * them; 1: their correctly rounded values (or_exp_cr, or_root4_cr), as
+   * the CUDA path computes them.  The library's results differ from the
+   * correctly rounded ones in about one call in 1,300, so this switch
+   * separates that last-bit difference from everything else. */
+  int crmath;
 } or_trc;
 
 /* Persistent + inspected cell fields (all caller-owned, component-major). */

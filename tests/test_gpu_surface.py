@@ -174,6 +174,54 @@ def test_gpu_surface_grows_past_first_capacity():
     d.close()
 
 
+def test_gpu_pipelined_surface_past_capacity_loses_nothing():
+    """A pipelined call (vh_surface_begin, the next step queued, then
+    vh_surface_end) that finds more straddling cubes than the first buffers
+    hold keeps its inputs on the device and runs again at surface_end: its
+    elements are the oracle's at the call's tau, although the grid has
+    moved on by then; the next pipelined call runs on the grown buffers."""
+    from vhlle_b200.capi import GpuHydro
+    setup = _ripple_setup()
+    o, d = P.OracleRun(setup), GpuHydro(setup)
+    for s in range(2):
+        o.step(1)
+        d.step(1)
+        ro, acc = o.surface(cap=4000000)
+        d.surface_begin()
+        d.step(1)  # queued behind the call's pass; runs before surface_end waits
+        info = d.surface_end()
+        rd = d.surface_records()
+        assert len(ro) == info["nelements"] > 150000, s
+        ok = rec_close(rd, ro)
+        assert ok.all(), (s, np.argwhere(~ok)[:5])
+        assert int(acc["nsusp"]) == info["nsusp"]
+        o.step(1)
+    d.close()
+
+
+def test_gpu_grid_changes_refused_while_surface_pending():
+    """vh_resize2x, vh_upload_state and vh_enable_vorticity return
+    VH_ERR_STATE between vh_surface_begin and vh_surface_end (the reference
+    takes the old Fluid's surface before a resize replaces it); after the
+    call ends they run."""
+    from vhlle_b200.capi import GpuHydro, VhError
+    setup = W.small_glauber3d(21, 11, b=9.0, seed=5)
+    d = GpuHydro(setup)
+    d.step(2)
+    d.surface_begin()
+    for call in (d.resize2x, d.upload_initial, lambda: d.enable_vorticity(True)):
+        with pytest.raises(VhError) as e:
+            call()
+        assert e.value.status == 4 and "has not ended" in str(e.value)
+    info = d.surface_end()
+    o = P.OracleRun(setup)
+    o.step(2)
+    ro, _ = o.surface()
+    assert info["nelements"] == len(ro)
+    assert d.resize2x() == 1
+    d.close()
+
+
 @pytest.mark.parametrize("name", ["corona_glauber_41x41x21", "corona_glauber_nb_25x25x13"])
 def test_gpu_corona_equals_reference_fixture(name, tmp_path):
     """vh_corona at tau0 against the reference's outputCorona: element

@@ -16,7 +16,8 @@ from vhlle_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-CASES = ("vorticity_glauber_21x21x11_b9", "vorticity_glauber_nb_17x17x9")
+CASES = ("vorticity_glauber_21x21x11_b9", "vorticity_glauber_nb_17x17x9",
+         "vorticity_glauber_nb_chiral_17x17x9")
 
 
 def beta_columns(rec, beta):
@@ -58,6 +59,8 @@ def test_gpu_dbeta_equals_reference_fixture(name):
 @pytest.mark.parametrize("case", [
     ("glauber_41x41x21", lambda: W.small_glauber3d(41, 21, seed=3, b=6.0), 5),
     ("glauber_nb_33x33x17", lambda: W.glauber3d_nb_setup(33, 33, 17, eos=W.nb_table(200, 20)), 4),
+    # EoSChiral: the k_vort_T / k_vort_ops instantiations of the chiral class
+    ("glauber_nb_chiral_25x25x13", lambda: W.glauber3d_nb_setup(25, 25, 13, eos=W.chiral_eos()), 4),
 ], ids=lambda c: c[0])
 def test_gpu_dbeta_equals_oracle(case):
     """Every step's stored dbeta bit for bit, on events whose surface and

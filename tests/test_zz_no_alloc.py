@@ -80,6 +80,8 @@ def test_noalloc_step_matches_the_context_step_twice(make):
     torch = pytest.importorskip("torch")
     setup = make()
     L = capi.lib()
+    # the set-up a caller does before reserving its own memory pool
+    assert L.vh_noalloc_prepare(0) == capi.VH_OK, L.vh_noalloc_last_error().decode()
     ref = capi.GpuHydro(setup)
     dev = _device_state(torch, setup)
     eos_d, keep = _device_eos(torch, setup.eos)
@@ -89,8 +91,12 @@ def test_noalloc_step_matches_the_context_step_twice(make):
         ref.step(1)
         ref.sync()
         expect = ref.get_state()
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         st, bits = _noalloc_step(L, setup, eos_d, dev, tau)
         assert st == capi.VH_OK, L.vh_noalloc_last_error().decode()
+        # after vh_noalloc_prepare the call takes no device memory at all
+        assert torch.cuda.mem_get_info()[0] == free_before, call
         assert bits == 0
         tau = tau + setup.dt
         assert ref.tau == tau

@@ -27,7 +27,9 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_error_bits", "vh_clear_errors", "vh_launches_per_step", "vh_last_error",
            "vh_abi_version", "vh_transform_pv", "vh_eos_eval", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
-           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_totals",
+           "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_noalloc_prepare",
+           "vh_active_cells", "vh_set_con2prim_method",
+           "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
            "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_vorticity_chain", "vh_get_dbeta",
            "vh_surface_beta", "vh_surface_write_beta", "vh_corona", "vh_cornelius4d", "vh_set_con2prim",
@@ -293,6 +295,9 @@ def lib():
                                   ctypes.POINTER(VhTrcoeff), ctypes.c_double, ctypes.c_double,
                                   ctypes.POINTER(VhStateView), vp, ctypes.POINTER(ctypes.c_uint)]
     L.vh_noalloc_last_error.restype = ctypes.c_char_p
+    L.vh_noalloc_prepare.argtypes = [ctypes.c_int]
+    L.vh_active_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    L.vh_set_con2prim_method.argtypes = [vp, ctypes.c_int]
     L.vh_totals.argtypes = [vp, ctypes.c_double, _dp]
     L.vh_get_grid.argtypes = [vp, ctypes.POINTER(VhGrid)]
     L.vh_advance.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -480,13 +485,18 @@ class GpuHydro:
         info = VhSurfaceInfo()
         ec = self.setup.ecrit if ecrit is None else ecrit
         self._check(self.L.vh_surface(self.h, ec, ctypes.byref(info)))
-        n = info.nelements
-        rec = np.zeros((n, SURF_REC))
-        if n:
+        return self.surface_records(), {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+
+    def surface_records(self):
+        """The element records [n][29] of the last surface call."""
+        n = ctypes.c_long()
+        self._check(self.L.vh_surface_records(self.h, None, 0, ctypes.byref(n)))
+        rec = np.zeros((n.value, SURF_REC))
+        if n.value:
             got = ctypes.c_long()
-            self._check(self.L.vh_surface_records(self.h, rec.ctypes.data_as(_dp), n,
+            self._check(self.L.vh_surface_records(self.h, rec.ctypes.data_as(_dp), n.value,
                                                   ctypes.byref(got)))
-        return rec, {k: getattr(info, k) for k, _ in VhSurfaceInfo._fields_}
+        return rec
 
     def enable_vorticity(self, on=True):
         """Hydro::enableVorticity: dbeta per cell from the next viscous step."""
@@ -512,6 +522,11 @@ class GpuHydro:
 
     def surface_write_beta(self, path, header=False):
         self._check(self.L.vh_surface_write_beta(self.h, path.encode(), int(header)))
+
+    def set_con2prim_method(self, method):
+        """vh_set_con2prim_method: 0 the reference's constant slope, 1 the
+        EoS's own slope (tight tolerance only)."""
+        self._check(self.L.vh_set_con2prim_method(self.h, int(method)))
 
     def set_con2prim(self, tol):
         self._check(self.L.vh_set_con2prim(self.h, tol))
@@ -617,6 +632,12 @@ class GpuHydro:
             return np.array([a[0] + 0 * d[0], a[0] + n[0] * d[0], a[2] + 0 * d[1],
                              a[2] + n[1] * d[1], a[4] + 0 * d[2], a[4] + n[2] * d[2],
                              d[0], d[1], d[2]])
+
+    def active_cells(self) -> int:
+        """Cells the last viscous step relaxed (e > 0 at the half step)."""
+        n = ctypes.c_longlong()
+        self._check(self.L.vh_active_cells(self.h, ctypes.byref(n)))
+        return n.value
 
     def launches_per_step(self) -> int:
         n = ctypes.c_int()

@@ -64,6 +64,16 @@ static vh_status fail(vh_ctx* c, vh_status st, const std::string& msg) {
   return st;
 }
 
+// Calls that change the grid, its fields' meaning or the stream are refused
+// while a vh_surface_begin has not ended: its pass reads the grid and may
+// run again at vh_surface_end (the reference takes the surface of the old
+// Fluid before a resize replaces it, src/main.cpp:246-271,420-427).
+#define VH_NOT_PENDING(ctx, who)                                                   \
+  do {                                                                             \
+    if ((ctx)->surf_pending)                                                       \
+      return fail((ctx), VH_ERR_STATE, who ": a vh_surface_begin has not ended"); \
+  } while (0)
+
 static vh_status cuda_fail(vh_ctx* c, cudaError_t e, const char* where) {
   return fail(c, VH_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
@@ -164,6 +174,33 @@ static void choose_axis_mode(const double* g, int n, int* mode, float* x0, float
   }
 }
 
+namespace vh {
+const char* eos_problem(const vh_eos& e) {
+  auto size_ok = [](int ne, int nn) { return ne >= 2 && nn >= 2 && (long long)ne * nn <= (1LL << 30); };
+  switch (e.kind) {
+    case VH_EOS_CONFORMAL:
+      return nullptr;
+    case VH_EOS_TABLE:
+      if (!size_ok(e.ne, e.nn))
+        return "EoS table needs ne >= 2, nn >= 2 and at most 2^30 points";
+      if (!e.egrid || !e.ngrid || !e.p || !e.T || !e.mub) return "EoS table needs all five arrays";
+      return nullptr;
+    case VH_EOS_CHIRAL:
+      for (const vh_eos_aux& x : e.aux) {
+        if (!size_ok(x.ne, x.nn) || !x.p || !x.T || !x.mub || !x.mus)
+          return "chiral EoS table missing, smaller than 2 x 2 or above 2^30 points";
+        // the uniform grids' steps (emax - emin) / (ne - 1) divide the lookups
+        if (!(x.emin < x.emax) || !(x.nmin < x.nmax) || !std::isfinite(x.emax - x.emin) ||
+            !std::isfinite(x.nmax - x.nmin))
+          return "chiral EoS table needs finite emin < emax and nmin < nmax";
+      }
+      return nullptr;
+    default:
+      return "unsupported EoS kind (no device lowering)";
+  }
+}
+}  // namespace vh
+
 extern "C" {
 
 int vh_abi_version(void) { return VH_ABI_VERSION; }
@@ -200,18 +237,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   if (!(grid->xmin < grid->xmax) || !(grid->ymin < grid->ymax) || !(grid->etamin < grid->etamax))
     return fail(nullptr, VH_ERR_ARG, "vh_create: the grid needs min < max on every axis");
   if (!(tau0 > 0.)) return fail(nullptr, VH_ERR_ARG, "vh_create: tau0 must be positive");
-  if (eos->kind != VH_EOS_CONFORMAL && eos->kind != VH_EOS_TABLE && eos->kind != VH_EOS_CHIRAL)
-    return fail(nullptr, VH_ERR_ARG, "vh_create: unsupported EoS kind (no device lowering)");
-  if (eos->kind == VH_EOS_CHIRAL)
-    for (const vh_eos_aux& x : eos->aux)
-      if (x.ne < 2 || x.nn < 2 || !x.p || !x.T || !x.mub || !x.mus ||
-          (long long)x.ne * x.nn > (1LL << 30))
-        return fail(nullptr, VH_ERR_ARG, "vh_create: chiral EoS table missing or too small");
-  if (eos->kind == VH_EOS_TABLE) {
-    if (eos->ne < 2 || eos->nn < 2 || !eos->egrid || !eos->ngrid || !eos->p || !eos->T || !eos->mub)
-      return fail(nullptr, VH_ERR_ARG,
-                  "vh_create: EoS table needs ne >= 2, nn >= 2 and all five arrays");
-  }
+  if (const char* why = vh::eos_problem(*eos))
+    return fail(nullptr, VH_ERR_ARG, std::string("vh_create: ") + why);
   const double dx = (grid->xmax - grid->xmin) / (grid->nx - 1);
   const double dy = (grid->ymax - grid->ymin) / (grid->ny - 1);
   if (!(dt > 0.) || dt > dx / 2. || dt > dy / 2.)
@@ -317,6 +344,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   c->eos.tol = 0.00001;  // src/rmn.cpp:96
   c->eos.vguess = nullptr;
   c->eos.stats = nullptr;
+  c->eos.slope = 0;  // the reference's constant dp/de (src/rmn.cpp:36)
   if (eos->kind == VH_EOS_TABLE) {
     const int ne = eos->ne, nn = eos->nn;
     double* buf = nullptr;
@@ -387,6 +415,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
 
 vh_status vh_set_stream(vh_ctx* ctx, void* stream) {
   if (!ctx) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_set_stream");
   ctx->stream = static_cast<cudaStream_t>(stream);
   return VH_OK;
 }
@@ -407,6 +436,7 @@ static const FieldSpec kFields[] = {
 
 vh_status vh_upload_async(vh_ctx* ctx, const vh_state_view* h) {
   if (!ctx || !h) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_upload_async");
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
   for (const FieldSpec& fs : kFields) {
     const double* src = h->*(fs.host);
@@ -432,6 +462,7 @@ vh_status vh_download_async(vh_ctx* ctx, const vh_state_view* h) {
 
 vh_status vh_upload_state(vh_ctx* ctx, const vh_state_view* h) {
   if (!ctx || !h) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_upload_state");
   if (!h->Q) return fail(ctx, VH_ERR_ARG, "vh_upload_state: Q is required");
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
   const long long N = ctx->g.N;
@@ -595,7 +626,24 @@ vh_status vh_set_con2prim(vh_ctx* ctx, double tol) {
   if (!ctx) return VH_ERR_ARG;
   if (!(tol > 0.) || !(tol <= 0.00001))
     return fail(ctx, VH_ERR_ARG, "vh_set_con2prim: tol must be in (0, 1e-5]");
+  if (ctx->eos.slope && !(tol <= 1e-10))
+    return fail(ctx, VH_ERR_ARG,
+                "vh_set_con2prim: the table-slope method needs tol <= 1e-10 (set the method "
+                "back to VH_C2P_REFERENCE first)");
   ctx->eos.tol = tol;
+  ctx->version++;
+  return VH_OK;
+}
+
+vh_status vh_set_con2prim_method(vh_ctx* ctx, int method) {
+  if (!ctx) return VH_ERR_ARG;
+  if (method != VH_C2P_REFERENCE && method != VH_C2P_TABLE_SLOPE)
+    return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_method: unknown method");
+  if (method == VH_C2P_TABLE_SLOPE && !(ctx->eos.tol <= 1e-10))
+    return fail(ctx, VH_ERR_ARG,
+                "vh_set_con2prim_method: the table slope needs a tight tolerance "
+                "(vh_set_con2prim with tol <= 1e-10 first)");
+  ctx->eos.slope = method;
   ctx->version++;
   return VH_OK;
 }
@@ -626,6 +674,7 @@ vh_status vh_mlp_samples(vh_ctx* ctx, float* X, float* Y, long cap, long* n) {
   vh::EosDev E = ctx->eos;
   E.tol = 1e-13;  // labels from the root converged to round-off
   E.vguess = nullptr;
+  E.slope = 0;
   E.stats = nullptr;
   vh::launch_mlp_samples(E, ctx->f.Q, ctx->g.N, ctx->tau, X, Y, cap, ctx->ucount, ctx->stream);
   VH_CUDA(ctx, cudaGetLastError());
@@ -682,6 +731,7 @@ vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
   if (resized) *resized = 0;
   if (!ctx) return VH_ERR_ARG;
   if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_resize2x: no state uploaded");
+  VH_NOT_PENDING(ctx, "vh_resize2x");
   const vh_grid& gr = ctx->grid;
   vh::Geo& g = ctx->g;
   // Fluid::getX / getY / getZ, src/fld.h:62-64
@@ -732,6 +782,18 @@ vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
     VH_CUDA(ctx, cudaMemsetAsync(ctx->vort.dbeta, 0, sizeof(double) * 16 * g.N, ctx->stream));
   ctx->version++;
   if (resized) *resized = 1;
+  return VH_OK;
+}
+
+vh_status vh_active_cells(vh_ctx* ctx, long long* n) {
+  if (!ctx || !n) return VH_ERR_ARG;
+  *n = 0;
+  if (!ctx->f.nactive) return VH_OK;  // an ideal context has no relaxation
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  int h = 0;
+  VH_CUDA(ctx, cudaMemcpyAsync(&h, ctx->f.nactive, sizeof h, cudaMemcpyDeviceToHost, ctx->stream));
+  VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *n = h;
   return VH_OK;
 }
 
@@ -824,7 +886,8 @@ static vh_status surf_common(vh_ctx* ctx) {
 // buffers for want_c hypercubes and want_e elements: the nine kernels, the
 // beta.dat values when vorticity is on, and the copies of the counts, sums
 // and error bits into the pinned host block.  Nothing waits.
-static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t want_e) {
+static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t want_e,
+                              const vh::Fields& f, double tau, const double* dbeta) {
   const vh::Geo& g = ctx->g;
   vh_ctx::Surf& S = ctx->surf;
   vh_status st;
@@ -840,19 +903,19 @@ static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t w
   S.pass_cap_c = cap_c;
   S.pass_cap_e = cap_e;
   cudaStream_t s = ctx->stream;
-  const double taup = ctx->tau - ctx->fluid_dt;
+  const double taup = tau - ctx->fluid_dt;
   vh_ctx::Surf::Host& H = *S.host;
-  vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, taup, S.eN, S.eP, s);
+  vh::launch_surf_energy(g, ctx->eos, f, tau, taup, S.eN, S.eP, s);
   vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
   vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, cap_c, s);
   vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, S.counters, cap_c,
-                            S.geo, S.cnt, ctx->f.err, s);
-  vh::launch_surf_elements(g, ctx->eos, ctx->f, ctx->tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
+                            S.geo, S.cnt, f.err, s);
+  vh::launch_surf_elements(g, ctx->eos, f, tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
                            ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
                            S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
   if (ctx->vort_on)  // beta.dat lines (src/fld.cpp:663-669, 798-831)
-    vh::launch_surf_beta(g, ctx->vort.dbeta, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
-                         S.geo, S.cnt, ctx->surf_beta, s);
+    vh::launch_surf_beta(g, dbeta, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e, S.geo,
+                         S.cnt, ctx->surf_beta, s);
   VH_CUDA(ctx, cudaGetLastError());
   VH_CUDA(ctx, cudaMemcpyAsync(H.cnt, S.counters, sizeof H.cnt, cudaMemcpyDeviceToHost, s));
   VH_CUDA(ctx, cudaMemcpyAsync(H.acc, S.partial + (size_t)kSurfPartials * vh::kSurfAcc,
@@ -922,7 +985,8 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   size_t want_c, want_e;
   surf_want(ctx, &want_c, &want_e);
   for (int pass = 0; pass < 2; pass++) {
-    if ((st = surf_enqueue(ctx, ecrit, want_c, want_e))) return st;
+    if ((st = surf_enqueue(ctx, ecrit, want_c, want_e, ctx->f, ctx->tau, ctx->vort.dbeta)))
+      return st;
     VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (surf_fits(ctx, &want_c, &want_e)) return surf_finish(ctx, info);
   }
@@ -938,10 +1002,23 @@ vh_status vh_surface_begin(vh_ctx* ctx, double ecrit) {
   vh_status st;
   if ((st = surf_common(ctx))) return st;
   if (!ctx->surf_ev) VH_CUDA(ctx, cudaEventCreateWithFlags(&ctx->surf_ev, cudaEventDisableTiming));
+  // the copy an overflowing pass leaves for vh_surface_end (allocated here,
+  // on the first call, so that no later call allocates unless it grows)
+  vh_ctx::Surf& S = ctx->surf;
+  const bool beta = ctx->vort_on;
+  const size_t keep = (size_t)(beta ? 41 : 25) * ctx->g.N;
+  if ((st = dgrow(ctx, &S.keep, &S.cap_keep, keep))) return st;
   size_t want_c, want_e;
   surf_want(ctx, &want_c, &want_e);
-  if ((st = surf_enqueue(ctx, ecrit, want_c, want_e))) return st;
+  if ((st = surf_enqueue(ctx, ecrit, want_c, want_e, ctx->f, ctx->tau, ctx->vort.dbeta))) return st;
+  const vh::Fields& f = ctx->f;
+  vh::SurfKeepSrc src{{f.Q, f.Qprev, f.pi, f.Pi, ctx->vort.dbeta}, {7, 7, 10, 1, 16}, beta ? 5 : 4};
+  vh::launch_surf_keep(S.counters, S.pass_cap_c, S.pass_cap_e, src, S.keep, ctx->g.N, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
   VH_CUDA(ctx, cudaEventRecord(ctx->surf_ev, ctx->stream));
+  S.keep_tau = ctx->tau;
+  S.keep_ecrit = ecrit;
+  S.keep_beta = beta;
   ctx->surf_pending = true;
   return VH_OK;
 }
@@ -955,16 +1032,22 @@ vh_status vh_surface_end(vh_ctx* ctx, vh_surface_info* info) {
   size_t want_c, want_e;
   surf_want(ctx, &want_c, &want_e);
   if (!surf_fits(ctx, &want_c, &want_e)) {
-    // the fields have moved on: grow for the next call, report this one lost
-    ctx->surf.nel = 0;
-    ctx->beta_nel = 0;
+    // The fields have moved on, but the pass kept its inputs (k_surf_keep):
+    // grow the buffers and run it again on that copy, behind whatever the
+    // caller queued since, then wait for it.
+    vh_ctx::Surf& S = ctx->surf;
+    const long long N = ctx->g.N;
+    vh::Fields kf = ctx->f;
+    kf.Q = S.keep;
+    kf.Qprev = S.keep + 7 * N;
+    kf.pi = S.keep + 14 * N;
+    kf.Pi = S.keep + 24 * N;
+    const double* kbeta = S.keep_beta ? S.keep + 25 * N : nullptr;
     vh_status st;
-    if ((st = dgrow(ctx, &ctx->surf.cubes, &ctx->surf.cap_cubes, want_c)) ||
-        (st = dgrow(ctx, &ctx->surf.rec, &ctx->surf.cap_rec, want_e * vh::kSurfRec)))
-      return st;
-    return fail(ctx, VH_ERR_STATE,
-                "vh_surface_end: more elements than the buffers held; buffers grown, "
-                "this call's elements are lost (use vh_surface for it)");
+    if ((st = surf_enqueue(ctx, S.keep_ecrit, want_c, want_e, kf, S.keep_tau, kbeta))) return st;
+    VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!surf_fits(ctx, &want_c, &want_e))
+      return fail(ctx, VH_ERR_STATE, "vh_surface_end: element buffers did not grow");
   }
   return surf_finish(ctx, info);
 }
@@ -1067,6 +1150,7 @@ vh_status vh_surface_write(vh_ctx* ctx, const char* path, int extendFO) {
 
 vh_status vh_enable_vorticity(vh_ctx* ctx, int on) {
   if (!ctx) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_enable_vorticity");
   const long long N = ctx->g.N;
   if (N > INT32_MAX) return fail(ctx, VH_ERR_ARG, "vh_enable_vorticity: grid too large");
   VH_CUDA(ctx, cudaSetDevice(ctx->device));

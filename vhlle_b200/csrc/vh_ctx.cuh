@@ -68,6 +68,13 @@ struct vh_ctx {
     size_t cap_cubes = 0, cap_geo = 0, cap_cnt = 0, cap_rec = 0, cap_contrib = 0;
     int pass_cap_c = 0, pass_cap_e = 0;  // the buffers the last pass ran with
     long long nel = 0;
+    // a pipelined call's copy of Q, Qprev, pi, Pi (and dbeta with vorticity
+    // on), written on the device only when its pass overflowed, and the
+    // call's tau and e_crit: vh_surface_end runs the pass again from them
+    double* keep = nullptr;
+    size_t cap_keep = 0;
+    double keep_tau = 0., keep_ecrit = 0.;
+    bool keep_beta = false;
     // pinned landing place of a call's counts, sums and error bits
     struct Host {
       int cnt[2];

@@ -48,9 +48,11 @@ std::mutex g_setup_mutex;
 void* g_scratch[kMaxDevices] = {nullptr};
 
 // Looks up the scratch array's device address for the current device and
-// sets the step kernels' attributes, once per device.  The first
-// vh_step_noalloc call on a device does this, so that first call should
-// come before any stream capture on that device.
+// sets the step kernels' attributes, once per device.  With lazy module
+// loading the look-up is also what maps the array on the device, so it
+// takes device memory once: vh_noalloc_prepare does it ahead of the caller's
+// pool reservation; otherwise the first vh_step_noalloc call on a device
+// does it, and that first call should come before any stream capture.
 cudaError_t scratch_for_current_device(unsigned char** out) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
@@ -106,6 +108,20 @@ void ghost_map_fixed(int n, int* src, unsigned char* dst) {
 
 extern "C" const char* vh_noalloc_last_error(void) { return g_msg; }
 
+extern "C" vh_status vh_noalloc_prepare(int device) {
+  g_msg[0] = 0;
+  int prev = -1;
+  cudaError_t e = cudaGetDevice(&prev);
+  if (e != cudaSuccess) return cfail(e, "cudaGetDevice");
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return cfail(e, "cudaSetDevice");
+  unsigned char* base = nullptr;
+  e = scratch_for_current_device(&base);
+  const cudaError_t e2 = cudaSetDevice(prev);
+  if (e != cudaSuccess) return cfail(e, "scratch set-up");
+  if (e2 != cudaSuccess) return cfail(e2, "cudaSetDevice (restore)");
+  return VH_OK;
+}
+
 extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
                                      const vh_trcoeff* tr, double tau, double dt,
                                      const vh_state_view* s, void* stream,
@@ -129,18 +145,10 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
     return nfail(VH_ERR_ARG,
                  "vh_step_noalloc: grid exceeds VH_NOALLOC_MAX_CELLS (32768 cells); "
                  "use vh_create/vh_step for larger grids");
-  if (eos_dev->kind != VH_EOS_CONFORMAL && eos_dev->kind != VH_EOS_TABLE &&
-      eos_dev->kind != VH_EOS_CHIRAL)
-    return nfail(VH_ERR_ARG, "vh_step_noalloc: unsupported EoS kind");
-  if (eos_dev->kind == VH_EOS_CHIRAL)
-    for (const vh_eos_aux& x : eos_dev->aux)
-      if (x.ne < 2 || x.nn < 2 || !x.p || !x.T || !x.mub || !x.mus)
-        return nfail(VH_ERR_ARG, "vh_step_noalloc: chiral EoS table missing or too small");
-  if (eos_dev->kind == VH_EOS_TABLE &&
-      (eos_dev->ne < 2 || eos_dev->nn < 2 || !eos_dev->egrid || !eos_dev->ngrid ||
-       !eos_dev->p || !eos_dev->T || !eos_dev->mub))
-    return nfail(VH_ERR_ARG,
-                 "vh_step_noalloc: EoS table needs ne >= 2, nn >= 2 and five device arrays");
+  if (const char* why = vh::eos_problem(*eos_dev)) {
+    snprintf(g_msg, sizeof g_msg, "vh_step_noalloc: %s", why);
+    return VH_ERR_ARG;
+  }
   const double dx = (grid->xmax - grid->xmin) / (grid->nx - 1);
   const double dy = (grid->ymax - grid->ymin) / (grid->ny - 1);
   if (!(dt > 0.) || dt > dx / 2. || dt > dy / 2.)
@@ -179,6 +187,7 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.eos.tol = 0.00001;  // src/rmn.cpp:96
   a.eos.vguess = nullptr;
   a.eos.stats = nullptr;
+  a.eos.slope = 0;
   a.tr = vh::TrDev{tr->etaS0, tr->zetaS0, tr->ah, tr->al, tr->aRho, tr->T0, tr->etaSMin,
                    tr->etaSEpsilonMin, tr->etaSShiftMuB, tr->etaSScaleMuB,
                    tr->zetaSPeakEpsilon, tr->zetaSScaleBeta, tr->zetaSSigmaMinus,

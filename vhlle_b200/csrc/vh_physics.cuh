@@ -59,6 +59,10 @@ struct EosDev {
   double tol;
   const float* __restrict__ vguess;
   unsigned long long* stats;
+  // the Newton slope of the root find: 0 the reference's constant
+  // dp/de = 1/3; 1 the EoS's own local dp/de and dp/dnb (the step kernels
+  // take it through the EK_*_SL instantiations)
+  int slope;
   ChiralAux ch[2];  // kind 2: chiralsmall, chiraleos
 };
 
@@ -204,9 +208,13 @@ __device__ __forceinline__ bool is_bracket(int k, int n, double x, double gk, do
 // ends, the interval reciprocals and the four table corners are loaded
 // together for the guess; a wrong guess (a step or two off, rare) walks to
 // the bracket that the binary search finds and loads again.
-template <bool WANT_T>
+// With WANT_D also the interpolant's partial derivatives dp/de and dp/dnb
+// in the bracket (0 where p is clamped at 0): the Newton slope of the
+// table-slope root find.
+template <bool WANT_T, bool WANT_D = false>
 __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
-                                      double& T, double& mub, double& p) {
+                                      double& T, double& mub, double& p, double* dpde = nullptr,
+                                      double* dpdn = nullptr) {
   const int ne = E.ne, nn = E.nn;
   int ke, kn, k2;
   if (E.emode == GRID_BSEARCH || ne <= 2)
@@ -239,11 +247,19 @@ __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
   const double un = interp_weight(nb, gn0, gn1, E.nrinv != nullptr, rn);
   const double we0 = 1. - ue, we1 = ue;
   const double wn0 = 1. - un, wn1 = un;
+  const double p00 = __ldg(E.p + b00), p01 = __ldg(E.p + b01);
+  const double p10 = __ldg(E.p + b00 + 1), p11 = __ldg(E.p + b01 + 1);
   double sp = 0.;
-  sp += we0 * wn0 * __ldg(E.p + b00);
-  sp += we0 * wn1 * __ldg(E.p + b01);
-  sp += we1 * wn0 * __ldg(E.p + b00 + 1);
-  sp += we1 * wn1 * __ldg(E.p + b01 + 1);
+  sp += we0 * wn0 * p00;
+  sp += we0 * wn1 * p01;
+  sp += we1 * wn0 * p10;
+  sp += we1 * wn1 * p11;
+  if (WANT_D) {
+    const double se = wn0 * (p10 - p00) + wn1 * (p11 - p01);
+    const double sn = we0 * (p01 - p00) + we1 * (p11 - p10);
+    *dpde = sp < 0. ? 0. : (E.erinv ? se * re : ddiv(se, ge1 - ge0));
+    *dpdn = sp < 0. ? 0. : (E.nrinv ? sn * rn : ddiv(sn, gn1 - gn0));
+  }
   if (sp < 0.) sp = 0.;
   p = sp;
   if (WANT_T) {
@@ -266,11 +282,13 @@ __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
 // step.  (int) of a double saturates here and gives INT_MIN on the host
 // for a large negative quotient alike; the region tests of eos_chiral keep
 // positive quotients below the table size.
-template <bool WANT_T>
+template <bool WANT_T, bool WANT_D = false>
 __device__ __forceinline__ void chiral_aux(const ChiralAux& A, double e, double nb, double& p,
-                                           double& T, double& mub, double& mus) {
+                                           double& T, double& mub, double& mus,
+                                           double* dpde = nullptr, double* dpdn = nullptr) {
   if (e < 0.) {
     T = mub = mus = p = 0.;
+    if (WANT_D) *dpde = *dpdn = 0.;
     return;
   }
   const double de = (A.emax - A.emin) / (A.ne - 1);
@@ -286,11 +304,17 @@ __device__ __forceinline__ void chiral_aux(const ChiralAux& A, double e, double 
   const double we0 = 1. - em / de, we1 = em / de;
   const double wn0 = 1. - nm / dn, wn1 = nm / dn;
   const int b00 = in * A.ne + ie, b01 = b00 + A.ne;  // [ie][in], [ie][in + 1]
+  const double p00 = __ldg(A.p + b00), p01 = __ldg(A.p + b01);
+  const double p10 = __ldg(A.p + b00 + 1), p11 = __ldg(A.p + b01 + 1);
   double sp = 0.;
-  sp += we0 * wn0 * __ldg(A.p + b00);
-  sp += we0 * wn1 * __ldg(A.p + b01);
-  sp += we1 * wn0 * __ldg(A.p + b00 + 1);
-  sp += we1 * wn1 * __ldg(A.p + b01 + 1);
+  sp += we0 * wn0 * p00;
+  sp += we0 * wn1 * p01;
+  sp += we1 * wn0 * p10;
+  sp += we1 * wn1 * p11;
+  if (WANT_D) {
+    *dpde = sp < 0. ? 0. : (wn0 * (p10 - p00) + wn1 * (p11 - p01)) / de;
+    *dpdn = sp < 0. ? 0. : (we0 * (p01 - p00) + we1 * (p11 - p10)) / dn;
+  }
   if (WANT_T) {
     double sT = 0., sb = 0., ss = 0.;
     sT += we0 * wn0 * __ldg(A.T + b00);
@@ -315,15 +339,20 @@ __device__ __forceinline__ void chiral_aux(const ChiralAux& A, double e, double 
 
 // EoSChiral::eos / EoSChiral::p, src/eoChiral.cpp:159-178 (muq = 0); the
 // 1/4 power of the region above the tables is the correctly rounded one
-template <bool WANT_T>
+template <bool WANT_T, bool WANT_D = false>
 __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb, double& T,
-                                           double& mub, double& mus, double& p) {
+                                           double& mub, double& mus, double& p,
+                                           double* dpde = nullptr, double* dpdn = nullptr) {
   if (e < 1.46 && nb < 0.3) {
-    chiral_aux<WANT_T>(E.ch[0], e, nb, p, T, mub, mus);
+    chiral_aux<WANT_T, WANT_D>(E.ch[0], e, nb, p, T, mub, mus, dpde, dpdn);
   } else if (e < 146. && nb < 6.) {
-    chiral_aux<WANT_T>(E.ch[1], e, nb, p, T, mub, mus);
+    chiral_aux<WANT_T, WANT_D>(E.ch[1], e, nb, p, T, mub, mus, dpde, dpdn);
   } else {
     p = 0.2964 * e;
+    if (WANT_D) {
+      *dpde = 0.2964;
+      *dpdn = 0.;
+    }
     if (WANT_T) {
       T = 0.15120476935 * crm::root4_cr(e);
       mub = mus = 0.0;
@@ -336,12 +365,34 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
 // con2prim kernels are instantiated per class: compiled into every
 // con2prim iteration next to the table lookup, the chiral lookup made those
 // kernels spill more (face kernels 25 % slower on the table kind).
-enum { EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2 };
+// EK_TABLE_SL / EK_CHIRAL_SL: the same classes with the table-slope root
+// find (EosDev::slope = 1).
+enum { EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4 };
+__host__ __device__ constexpr bool ek_chiral(int ek) { return ek == EK_CHIRAL || ek == EK_CHIRAL_SL; }
+__host__ __device__ constexpr bool ek_slope(int ek) { return ek == EK_TABLE_SL || ek == EK_CHIRAL_SL; }
+
+// p and its partial derivatives (the table-slope root find)
+template <int EK = EK_ANY>
+__device__ __forceinline__ double eos_p_d(const EosDev& E, double e, double nb, double& dpde,
+                                          double& dpdn) {
+  double T, mub, mus, p;
+  if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
+    eos_chiral<false, true>(E, e, nb, T, mub, mus, p, &dpde, &dpdn);
+    return p;
+  }
+  if (E.kind == 0) {
+    dpde = 1. / 3.;
+    dpdn = 0.;
+    return ddivp(e, 3.);
+  }
+  eos1f<false, true>(E, e, nb, T, mub, p, &dpde, &dpdn);
+  return p;
+}
 
 template <int EK = EK_ANY>
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
   double T, mub, mus, p;
-  if (EK == EK_CHIRAL || (EK == EK_ANY && E.kind == 2)) {
+  if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
     eos_chiral<false>(E, e, nb, T, mub, mus, p);
     return p;
   }
@@ -355,7 +406,7 @@ template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
                                          double& mub, double& mus, double& p) {
   mus = 0.;
-  if (EK == EK_CHIRAL || (EK == EK_ANY && E.kind == 2)) {
+  if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
     eos_chiral<true>(E, e, nb, T, mub, mus, p);
   } else if (E.kind == 0) {
     p = ddivp(e, 3.);
@@ -427,9 +478,26 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     nq = Q[NQ_] * sq;
     ns = Q[NS_] * sq;
   }
-  p = eos_p<EK>(E, e, nb);
+  // The table-slope variant (ek_slope) takes f' = (Q_t + p) - v (M dp/de +
+  // dp/dnb Q_nb v / sqrt(1 - v^2)) with the EoS's own derivatives, so the
+  // Newton steps converge quadratically inside a table cell, and stops when
+  // f is exactly 0 (the reference's bracket test would send an exact root
+  // into bisection).  Not the reference's iteration: for a tight tolerance
+  // only, where the result does not depend on the path to the root.
+  constexpr bool SL = ek_slope(EK);
+  double dpde = 0., dpdn = 0.;
+  auto slope = [&](double vv, double sq) {
+    const double dn = sq > 0. ? dpdn * Q[NB_] * vv / sq : 0.;
+    return (Q[T_] + p) - vv * (M * dpde + dn);
+  };
+  double sq0 = sqrt(1 - v * v);
+  if (SL) {
+    p = eos_p_d<EK>(E, e, nb, dpde, dpdn);
+  } else {
+    p = eos_p<EK>(E, e, nb);
+  }
   f = (Q[T_] + p) * v - M;
-  df = (Q[T_] + p) - M * v * dpe;
+  df = SL ? slope(v, sq0) : (Q[T_] + p) - M * v * dpe;
   if (guessed) {
     if (f > 0.)
       vh = v;
@@ -439,7 +507,8 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
   dvold = vh - vl;
   dv = dvold;
   int it = 0;
-  for (int i = 0; i < MAXIT; i++) {
+  const bool at_root = SL && f == 0.;  // a start point that is the root
+  for (int i = 0; i < MAXIT && !at_root; i++) {
     it = i + 1;
     if ((f + df * (vh - v)) * (f + df * (vl - v)) >= 0. ||
         fabs(2. * f) > fabs(dvold * df)) {
@@ -458,9 +527,14 @@ __device__ __forceinline__ void transform_pv(const EosDev& E, double Q[7], Prim&
     nb = Q[NB_] * sq;
     nq = Q[NQ_] * sq;
     ns = Q[NS_] * sq;
-    p = eos_p<EK>(E, e, nb);
+    if (SL) {
+      p = eos_p_d<EK>(E, e, nb, dpde, dpdn);
+    } else {
+      p = eos_p<EK>(E, e, nb);
+    }
     f = (Q[T_] + p) * v - M;
-    df = (Q[T_] + p) - M * v * dpe;
+    if (SL && f == 0.) break;
+    df = SL ? slope(v, sq) : (Q[T_] + p) - M * v * dpe;
     if (f > 0.)
       vh = v;
     else

@@ -1174,7 +1174,10 @@ static int launch_step_ek(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
 }
 
 int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
-  return a.eos.kind == 2 ? launch_step_ek<EK_CHIRAL>(a, s, mk) : launch_step_ek<EK_TABLE>(a, s, mk);
+  const bool chiral = a.eos.kind == 2;
+  if (a.eos.slope)
+    return chiral ? launch_step_ek<EK_CHIRAL_SL>(a, s, mk) : launch_step_ek<EK_TABLE_SL>(a, s, mk);
+  return chiral ? launch_step_ek<EK_CHIRAL>(a, s, mk) : launch_step_ek<EK_TABLE>(a, s, mk);
 }
 
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/vhlle_b200.h"
 #include "vh_physics.cuh"
 
 namespace vh {
@@ -120,5 +121,11 @@ void launch_eos_eval(const EosDev& E, const double* e, const double* nb, long lo
                      cudaStream_t s);
 void launch_transport(const TrDev& tr, const double* in, long long n, double* out,
                       cudaStream_t s);
+
+// What is wrong with an EoS descriptor the device cannot evaluate (unknown
+// kind, a table smaller than 2 x 2 or larger than 2^30 points, missing
+// arrays, a chiral table whose range is empty or not finite), or NULL.
+// Shared by vh_create and vh_step_noalloc (vh_capi.cu).
+const char* eos_problem(const vh_eos& e);
 
 }  // namespace vh
