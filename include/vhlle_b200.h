@@ -239,6 +239,28 @@ vh_status vh_advance(vh_ctx *ctx, double dtau, double etamin, double etamax,
  * exits).  *resized may be NULL. */
 vh_status vh_resize2x(vh_ctx *ctx, int *resized);
 
+/* The initial state of a Monte-Carlo Glauber event, built on the device at
+ * the context's tau: the participants' density prof(x, y) = sum_p
+ * exp(-((x - x_p)^2 + (y - y_p)^2) / (2 smear^2)) on the transverse grid
+ * (summed in participant order), normalised to its maximum, e = (epeak
+ * H[iz]) prof, cells with e < ecut set to vacuum, nb = (nb_peak H[iz]) prof
+ * where e > 0, and every cell set at rest as Cell::setPrimVar + saveQprev +
+ * setAllM(e > 0) leave it (src/cll.cpp:222-241, the ending of every IC module
+ * such as src/icGlauber.cpp:147-166); the viscous fields start at zero.
+ * Replaces the host IC generation plus vh_upload_state.  parts and H are
+ * host arrays.  No counterpart in the reference (its Glauber IC is an
+ * optical one through GSL). */
+typedef struct vh_glauber_ic {
+  const double *parts; /* [nparts][2]: x, y of each participant (fm) */
+  int nparts;
+  double smear;        /* Gaussian width (fm) */
+  double epeak;        /* e at the profile's maximum (GeV/fm^3) */
+  const double *H;     /* [nz] longitudinal profile of each eta cell */
+  double ecut;         /* e below which a cell starts as vacuum */
+  double nb_peak;      /* nb at the maximum (fm^-3) */
+} vh_glauber_ic;
+vh_status vh_init_glauber(vh_ctx *ctx, const vh_glauber_ic *ic);
+
 /* The number of cells the last viscous step relaxed and advected: those
  * with e > 0 at the half step, the cells ISformal does not zero
  * (src/hdo.cpp:694-708); 0 for an ideal context.  Waits for the stream.

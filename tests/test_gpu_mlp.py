@@ -70,10 +70,11 @@ def test_gpu_mlp_forward_matches_cpu_restatement():
     m.close()
 
 
-def _iters_per_call(setup, mlp, nsteps):
+def _iters_per_call(setup, mlp, nsteps, method=0):
     from vhlle_b200.capi import GpuHydro
     d = GpuHydro(setup)
     d.set_con2prim(TIGHT)
+    d.set_con2prim_method(method)
     if mlp is not None:
         d.set_con2prim_guess(mlp)
     d.step(2)
@@ -112,18 +113,65 @@ def test_gpu_mlp_trained_guess_saves_iterations_within_tolerance():
     untrained = Mlp(seed=8)
     raw, _ = _iters_per_call(setup, untrained, 4)
     guided, st = _iters_per_call(setup, m, 4)
-    print("iterations per root find: start 0.5 %.3f, untrained %.3f, trained %.3f"
-          % (base, raw, guided))
+    slope, st_s = _iters_per_call(setup, None, 4, method=1)
+    guided_slope, st_gs = _iters_per_call(setup, m, 4, method=1)
+    print("iterations per root find: start 0.5 %.3f, untrained %.3f, trained %.3f; "
+          "table slope: start 0.5 %.3f, trained %.3f" % (base, raw, guided, slope, guided_slope))
     assert guided < base
-    # the guided step against the tight oracle after the same 6 steps
+    # the EoS's own slope converges quadratically inside a table cell; the
+    # trained start point saves iterations on top of it
+    assert slope < 0.7 * base and guided_slope < slope
+    # every guided / table-slope step against the tight oracle after the
+    # same 6 steps
     o = P.OracleRun(setup, tol=TIGHT)
     o.step(6)
-    got, exp = gpu_state_as_oracle(st), o.get_state()
+    exp = o.get_state()
+    for state in (st, st_s, st_gs):
+        _within_tight(gpu_state_as_oracle(state), exp)
+    m.close()
+    untrained.close()
+
+
+def _within_tight(got, exp):
     for k in exp:
         a = np.asarray(got[k], dtype=np.float64).reshape(-1)
         b = np.asarray(exp[k], dtype=np.float64).reshape(-1)
         scale = np.abs(b).max()
         ok = np.abs(a - b) <= 1e-8 * np.maximum(np.abs(a), np.abs(b)) + 1e-12 * scale
         assert ok.all(), (k, np.argwhere(~ok)[:5])
-    m.close()
-    untrained.close()
+
+
+@pytest.mark.parametrize("case", [
+    ("glauber_nb_25x25x13", lambda: W.glauber3d_nb_setup(25, 25, 13, eos=W.nb_table(200, 20)), 8),
+    ("glauber_nb_chiral_17x17x9", lambda: W.glauber3d_nb_setup(17, 17, 9, eos=W.chiral_eos()), 6),
+    ("gubser_31x31", lambda: W.gubser_setup(nx=31, ny=31), 10),
+], ids=lambda c: c[0])
+def test_gpu_table_slope_within_tight_oracle(case):
+    """VH_C2P_TABLE_SLOPE on the (e, nb) table, the chiral EoS and the
+    conformal gas: the step stays within 1e-8 of the tight oracle and takes
+    no more iterations than the reference's constant slope."""
+    from vhlle_b200.capi import GpuHydro, VhError
+    _, fac, n = case
+    setup = fac()
+    d = GpuHydro(setup)
+    with pytest.raises(VhError):
+        d.set_con2prim_method(1)  # needs a tight tolerance first
+    d.set_con2prim(TIGHT)
+    d.set_con2prim_method(1)
+    with pytest.raises(VhError):
+        d.set_con2prim(1e-5)  # and keeps it
+    d.con2prim_stats(True)
+    d.step(n)
+    c, it = d.con2prim_stats(False)
+    o = P.OracleRun(setup, tol=TIGHT)
+    o.step(n)
+    _within_tight(gpu_state_as_oracle(d.get_state()), o.get_state())
+    d.close()
+    r = GpuHydro(setup)
+    r.set_con2prim(TIGHT)
+    r.con2prim_stats(True)
+    r.step(n)
+    c0, it0 = r.con2prim_stats(False)
+    r.close()
+    print("iterations per root find: constant slope %.3f, table slope %.3f" % (it0 / c0, it / c))
+    assert it / c <= it0 / c0 + 1e-9

@@ -191,7 +191,8 @@ def test_gpu_pipelined_surface_past_capacity_loses_nothing():
         d.step(1)  # queued behind the call's pass; runs before surface_end waits
         info = d.surface_end()
         rd = d.surface_records()
-        assert len(ro) == info["nelements"] > 150000, s
+        # the first call finds more than the first buffers' 128k elements
+        assert len(ro) == info["nelements"] > (150000 if s == 0 else 100000), s
         ok = rec_close(rd, ro)
         assert ok.all(), (s, np.argwhere(~ok)[:5])
         assert int(acc["nsusp"]) == info["nsusp"]
@@ -334,29 +335,3 @@ def test_gpu_surface_pipelined_equals_synchronous():
     assert n_checked > 500
     a.close()
     b.close()
-
-
-def test_gpu_surface_pipelined_overflow_is_reported():
-    """A pipelined call that finds more than the buffers hold reports it
-    (VH_ERR_STATE, buffers grown); vh_surface then gives the full result,
-    and the next pipelined call fits."""
-    from vhlle_b200.capi import GpuHydro, VhError
-    setup = _ripple_setup()
-    o, d = P.OracleRun(setup), GpuHydro(setup)
-    o.step(1)
-    d.step(1)
-    d.surface_begin()
-    with pytest.raises(VhError):
-        d.surface_end()
-    rd, info = d.surface()
-    ro, _ = o.surface(cap=4000000)
-    assert len(ro) == info["nelements"] > 150000
-    assert rec_close(rd, ro).all()
-    o.step(1)
-    d.step(1)
-    d.surface_begin()
-    info = d.surface_end()
-    ro, _ = o.surface(cap=4000000)
-    assert len(ro) == info["nelements"]
-    assert rec_close(_records(d, info["nelements"]), ro).all()
-    d.close()

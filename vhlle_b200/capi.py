@@ -28,7 +28,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_abi_version", "vh_transform_pv", "vh_eos_eval", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_noalloc_prepare",
-           "vh_active_cells", "vh_set_con2prim_method",
+           "vh_active_cells", "vh_set_con2prim_method", "vh_init_glauber",
            "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
            "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_vorticity_chain", "vh_get_dbeta",
@@ -228,6 +228,12 @@ class VhEos(ctypes.Structure):
                 ("aux", VhEosAux * 2)]
 
 
+class VhGlauberIc(ctypes.Structure):
+    _fields_ = [("parts", _dp), ("nparts", ctypes.c_int), ("smear", ctypes.c_double),
+                ("epeak", ctypes.c_double), ("H", _dp), ("ecut", ctypes.c_double),
+                ("nb_peak", ctypes.c_double)]
+
+
 class VhTrcoeff(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin",
@@ -298,6 +304,7 @@ def lib():
     L.vh_noalloc_prepare.argtypes = [ctypes.c_int]
     L.vh_active_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.vh_set_con2prim_method.argtypes = [vp, ctypes.c_int]
+    L.vh_init_glauber.argtypes = [vp, ctypes.POINTER(VhGlauberIc)]
     L.vh_totals.argtypes = [vp, ctypes.c_double, _dp]
     L.vh_get_grid.argtypes = [vp, ctypes.POINTER(VhGrid)]
     L.vh_advance.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -431,6 +438,18 @@ class GpuHydro:
         if s.Pi is not None:
             fields["Pi"] = np.ascontiguousarray(s.Pi, dtype=np.float64)
         self.upload(fields)
+
+    def init_glauber(self, parts, H, smear=0.4, epeak=50.0, ecut=1e-3, nb_peak=0.0):
+        """vh_init_glauber: the Glauber initial state built on the device from
+        the participants' positions parts[n][2] and the longitudinal profile
+        H[nz] (workloads.glauber_participants / eta_profile)."""
+        parts = np.ascontiguousarray(parts, dtype=np.float64).reshape(-1, 2)
+        H = np.ascontiguousarray(H, dtype=np.float64).reshape(-1)
+        if len(H) != self.setup.grid.nz:
+            raise ValueError("H needs one value per eta cell")
+        ic = VhGlauberIc(parts.ctypes.data_as(_dp), len(parts), smear, epeak, H.ctypes.data_as(_dp),
+                         ecut, nb_peak)
+        self._check(self.L.vh_init_glauber(self.h, ctypes.byref(ic)))
 
     def upload(self, fields: dict):
         v = VhStateView()

@@ -364,11 +364,12 @@ def _woods_saxon(rng, A, R, a):
     return out
 
 
-def glauber_profile(seed: int, b: float, x: np.ndarray, y: np.ndarray,
-                    A: int = 208, R: float = 6.62, a: float = 0.546,
-                    sigma_nn: float = 6.4, smear: float = 0.4):
-    """Participant density of one seeded MC-Glauber event on the (x, y) grid,
-    normalised to a maximum of 1; returns (profile[iy][ix], n_participants)."""
+def glauber_participants(seed: int, b: float, A: int = 208, R: float = 6.62,
+                         a: float = 0.546, sigma_nn: float = 6.4) -> np.ndarray:
+    """Transverse positions [n][2] (fm) of the participants of one seeded
+    MC-Glauber event: two Woods-Saxon nuclei at x = +-b/2, a nucleon
+    participates when it comes within sqrt(sigma_NN / pi) of one of the
+    other nucleus (nucleus A's participants first, in sampling order)."""
     rng = np.random.default_rng(seed)
     na = _woods_saxon(rng, A, R, a)
     nbn = _woods_saxon(rng, A, R, a)
@@ -376,7 +377,15 @@ def glauber_profile(seed: int, b: float, x: np.ndarray, y: np.ndarray,
     nbn[:, 0] -= b / 2
     d2 = ((na[:, None, 0] - nbn[None, :, 0]) ** 2 + (na[:, None, 1] - nbn[None, :, 1]) ** 2)
     hit = d2 < sigma_nn / math.pi
-    parts = np.concatenate([na[hit.any(1), :2], nbn[hit.any(0), :2]], 0)
+    return np.ascontiguousarray(np.concatenate([na[hit.any(1), :2], nbn[hit.any(0), :2]], 0))
+
+
+def glauber_profile(seed: int, b: float, x: np.ndarray, y: np.ndarray,
+                    A: int = 208, R: float = 6.62, a: float = 0.546,
+                    sigma_nn: float = 6.4, smear: float = 0.4):
+    """Participant density of one seeded MC-Glauber event on the (x, y) grid,
+    normalised to a maximum of 1; returns (profile[iy][ix], n_participants)."""
+    parts = glauber_participants(seed, b, A, R, a, sigma_nn)
     X, Y = np.meshgrid(x, y, indexing="xy")
     prof = np.zeros_like(X)
     for px, py in parts:
