@@ -201,7 +201,35 @@ def gpu_index_for(local_rank):
     return str(local_rank)
 
 
-def traffic_per_launch(kernel, grid, steps, launches):
+def fp64_per_launch(kernel, grid, launches):
+    """FP64 operations (DADD + DMUL + 2 DFMA, ncu's
+    sm__sass_thread_inst_executed_op_d{add,mul,fma}_pred_on) per launch of
+    `kernel` from the committed ncu summary of the same workload's timed
+    steps (profiles/fp64.json: per grid, per kernel, each launch's count in
+    step order), averaged over this run's launches; None if no capture
+    covers them."""
+    p = os.path.join(ROOT, "profiles", "fp64.json")
+    if not os.path.exists(p):
+        return None
+    v = json.load(open(p)).get("x".join(map(str, grid)), {}).get(kernel)
+    if not v or len(v["flops_per_launch"]) < launches:
+        return None
+    return float(sum(v["flops_per_launch"][:launches]) / launches)
+
+
+def nvtx(name=None):
+    """Marks the timed region for profiler captures (ncu --nvtx-include)."""
+    try:
+        import torch
+        if name is None:
+            torch.cuda.nvtx.range_pop()
+        else:
+            torch.cuda.nvtx.range_push(name)
+    except Exception:
+        pass
+
+
+def traffic_per_launch(kernel, grid, launches):
     """DRAM bytes (read + write) per launch of `kernel` from the committed
     ncu summary of the same workload and steps (profiles/traffic.json:
     per grid, per kernel, the bytes of each launch in step order), averaged
@@ -370,69 +398,221 @@ def batch_measure(capi, W, n_events, steps, device, nz=None):
             "physics": "eta/s=0.12, zeta/s Gaussian bump 0.05 at T=0.175 GeV (width 0.02)"}
 
 
-def learned_guess_measure(capi, W, setup, steps, device):
-    """The learned con2prim start point on the event with baryon charge (the
-    3D event plus nb, 2000 x 200 (e, nb) table): root-find iterations and
-    throughput at the tight tolerance (1e-13, where results are start-point
-    independent) without and with the trained network, and at the reference
-    tolerance for context."""
+TIGHT = 1e-13  # con2prim stop at which the root does not depend on the path to it
+
+
+def train_guess_network(capi, W, device, target=10_000_000):
+    """The start-point network trained on about `target` (features, label)
+    pairs that transformPV at the tight tolerance gives on the cells of
+    runs of the 3D event, the event with baryon charge and eight events of
+    the event-by-event set (every cell with matter, every 5th step)."""
     import torch
-    tight = 1e-13
-    cells = setup.grid.ncells
-    h = capi.GpuHydro(setup, device=device)
-    out = {"tolerance": tight}
-    # iterations per root find
-    iters = {}
-    for name, tol in (("reference_tol", None), ("tight", tight)):
-        _reset(h, setup)
-        if tol:
-            h.set_con2prim(tol)
-        h.con2prim_stats(True)
-        h.step(10)
-        c, it = h.con2prim_stats(False)
-        iters[name] = it / c
-    # training data from the event itself, then training
     t0 = time.perf_counter()
-    _reset(h, setup)
-    cap = 24 * cells
-    X = torch.empty((cap, 4), dtype=torch.float32, device="cuda:%d" % device)
-    Y = torch.empty((cap, 3), dtype=torch.float32, device="cuda:%d" % device)
+    sources = [W.glauber3d_setup(seed=EVENT_SEED), W.glauber3d_nb_setup(seed=EVENT_SEED)]
+    sources += W.batch_events(8)
+    per = target // len(sources)
+    dev = "cuda:%d" % device
+    X = torch.empty((target, 4), dtype=torch.float32, device=dev)
+    Y = torch.empty((target, 3), dtype=torch.float32, device=dev)
     n = 0
-    for _ in range(20):
-        h.step(5)
-        n += h.mlp_samples(X[n:], Y[n:])
+    for s in sources:
+        h = capi.GpuHydro(s, device=device)
+        got = 0
+        for _ in range(60):
+            room = min(per - got, target - n)
+            if room <= 0:
+                break
+            h.step(5)
+            k = h.mlp_samples(X[n:n + room], Y[n:n + room])
+            got += k
+            n += k
+        h.close()
     X, Y = X[:n].contiguous(), Y[:n].contiguous()
     m = capi.Mlp(device=device, seed=17)
-    losses = m.train(X, Y, batch=16384, epochs=8, lr=3e-3, seed=5)
+    epochs = 6
+    losses = m.train(X, Y, batch=16384, epochs=epochs, lr=3e-3, seed=5)
     torch.cuda.synchronize()
-    out["train"] = {"samples": n, "epochs": 8, "first_loss": float(losses[0]),
-                    "final_loss": float(losses[-1]), "seconds": time.perf_counter() - t0}
-    for name, guess in (("tight", None), ("tight_mlp", m)):
+    info = {"samples": n, "epochs": epochs, "first_loss": float(losses[0]),
+            "final_loss": float(losses[-1]), "seconds": time.perf_counter() - t0,
+            "sources": "101x101x51 event, the same with nb, 8 events of the event-by-event set"}
+    del X, Y
+    torch.cuda.empty_cache()
+    return m, info
+
+
+def _c2p_mode(h, mode, mlp):
+    """mode: 'reference' (tol 1e-5, constant slope), 'tight' (1e-13,
+    constant slope), 'tight_mlp' (1e-13, constant slope, learned start),
+    'tight_slope' (1e-13, the EoS's slope), 'tight_slope_mlp'."""
+    h.set_con2prim_guess(None)
+    h.set_con2prim_method(0)
+    h.set_con2prim(1e-5 if mode == "reference" else TIGHT)
+    if "slope" in mode:
+        h.set_con2prim_method(1)
+    if "mlp" in mode:
+        h.set_con2prim_guess(mlp)
+
+
+LG_MODES = ("reference", "tight", "tight_mlp", "tight_slope", "tight_slope_mlp")
+
+
+def learned_guess_measure(capi, W, setup, steps, device, mlp):
+    """The learned con2prim start point on one event: root-find iterations
+    and device throughput for each con2prim mode (LG_MODES); what the trained
+    network gains is tight_slope_mlp over tight_slope (same method) and over
+    tight (the reference's method at the same tolerance)."""
+    cells = setup.grid.ncells
+    h = capi.GpuHydro(setup, device=device)
+    out = {"tolerance": TIGHT}
+    iters = {}
+    for mode in LG_MODES:
+        _c2p_mode(h, mode, mlp)
         _reset(h, setup)
-        h.set_con2prim(tight)
-        h.set_con2prim_guess(guess)
-        h.step(3)
+        h.step(3)  # captures this mode's step graph
         h.sync()
         _reset(h, setup)
-        h.set_con2prim(tight)
         h.timer_start()
         h.step(steps)
         ms = h.timer_stop()
-        out[name] = cells * steps / (ms / 1e3)
+        out[mode] = cells * steps / (ms / 1e3)
+        _reset(h, setup)
         h.con2prim_stats(True)
-        h.step(5)
+        h.step(steps)
         c, it = h.con2prim_stats(False)
-        if guess is not None:
-            iters["tight_mlp"] = it / c
-    h.set_con2prim_guess(None)
+        iters[mode] = it / c
+    _c2p_mode(h, "reference", None)
     out["iters_per_root_find"] = iters
-    out["speedup_mlp_vs_tight"] = out["tight_mlp"] / out["tight"]
+    out["speedup_mlp_vs_tight"] = out["tight_slope_mlp"] / out["tight"]
+    out["speedup_mlp_vs_tight_slope"] = out["tight_slope_mlp"] / out["tight_slope"]
+    out["speedup_slope_vs_tight"] = out["tight_slope"] / out["tight"]
     out["unit"] = UNIT
-    out["workload"] = "%s %dx%dx%d, nb peak %.1f fm^-3, %dx%d (e, nb) table" % (
-        setup.name, setup.grid.nx, setup.grid.ny, setup.grid.nz, W.NB_PEAK,
-        len(setup.eos.egrid), len(setup.eos.ngrid))
+    out["steps"] = steps
+    out["workload"] = "%s %dx%dx%d" % (setup.name, setup.grid.nx, setup.grid.ny, setup.grid.nz)
     h.close()
-    m.close()
+    return out
+
+
+def state_error(a, b, fields=("Q", "pi", "Pi")):
+    """Per field: the largest relative difference and the fraction of
+    values beyond 1e-8 relative (each difference less 1e-12 of the field's
+    largest magnitude, for values near zero), and the relative 2-norm of the
+    difference."""
+    out = {}
+    for k in fields:
+        x, y = np.asarray(a[k]).reshape(-1), np.asarray(b[k]).reshape(-1)
+        scale = float(np.abs(y).max()) if y.size else 0.0
+        d = np.abs(x - y) - 1e-12 * scale
+        r = np.where(d > 0, d / np.maximum(np.maximum(np.abs(x), np.abs(y)), 1e-300), 0.0)
+        ny = float(np.linalg.norm(y))
+        out[k] = {"max_rel": float(r.max()) if r.size else 0.0,
+                  "frac_beyond_1e-8": float((r > 1e-8).mean()) if r.size else 0.0,
+                  "norm_rel": float(np.linalg.norm(x - y)) / ny if ny > 0 else 0.0}
+    return out
+
+
+def batched_mlp_measure(capi, W, n_events, steps, device, mlp, tau_resize=4.0, nsample=8):
+    """The benchmark metric's numerator and denominator on the
+    event-by-event set (the first n_events seeded events: 61x61x1 ..
+    121x121x61, eta/s = 0.12, the zeta/s bump, the one-shot x2 resize at
+    tau_resize): every event of the set stepped alone (one vh_advance per
+    driver-loop iteration, event after event) at the reference tolerance and
+    at the tight one, against the same events advanced together by one
+    vh_batch graph per iteration at the tight tolerance, without and with
+    the learned start point (with the EoS's own Newton slope).  Device time
+    with CUDA events over `steps` iterations; every arm starts from fresh
+    contexts with the initial states (a resize changes a context's grid).
+    errors: the batched + learned path against the plain tight path
+    (bit-identical to the tight oracle, tests/test_gpu_con2prim_tight.py)
+    over nsample events (the smallest and the largest)."""
+    evs = W.batch_events(n_events)
+    cells = sum(s.grid.ncells for s in evs)
+    drv = [(s.dt, s.grid.etamin, s.grid.etamax, s.grid.nz) for s in evs]
+    by_size = sorted(range(n_events), key=lambda k: evs[k].grid.ncells)
+    sample = sorted(set(by_size[:nsample // 2] + by_size[-(nsample - nsample // 2):]))
+
+    def fresh(mode):
+        hs = [capi.GpuHydro(s, device=device) for s in evs]
+        for h in hs:
+            _c2p_mode(h, mode, mlp)
+        return hs
+
+    def plain(mode):
+        hs = fresh(mode)
+        for h, d in zip(hs, drv):  # captures each event's step graph for this mode
+            h.advance(*d)
+        for h, s in zip(hs, evs):
+            _reset(h, s)
+        for h in hs:
+            h.sync()
+        resized = [False] * n_events
+        hs[0].timer_start()
+        for _ in range(steps):
+            for k, (h, d) in enumerate(zip(hs, drv)):
+                h.advance(*d)
+                if not resized[k] and h.tau >= tau_resize:  # src/main.cpp:423-427
+                    h.resize2x()
+                    resized[k] = True
+        ms = hs[0].timer_stop()
+        for h in hs:
+            h.sync()
+        return ms, hs
+
+    def batched(mode):
+        hs = fresh(mode)
+        b = capi.Batch(hs)
+        for k, d in enumerate(drv):
+            b.set_driver(k, *d, tau_resize)
+        b.tune(True)
+        b.advance(16)  # the tuner's configurations (16 iterations stay below tau_resize)
+        b.sync()
+        for h, s in zip(hs, evs):
+            _reset(h, s)
+        for h in hs:
+            h.sync()
+        b.advance(2)  # the graphs of the reset state's buffer parity
+        b.sync()
+        for h, s in zip(hs, evs):
+            _reset(h, s)
+        for h in hs:
+            h.sync()
+        b.timer_start()
+        b.advance(steps)
+        ms = b.timer_stop()
+        bits = b.sync()
+        info = b.info()
+        b.close()
+        return ms, hs, bits, info
+
+    out = {"events": n_events, "steps": steps, "cells": cells, "unit": UNIT,
+           "grids": "%d..%d cells" % (min(s.grid.ncells for s in evs), max(s.grid.ncells for s in evs)),
+           "tau_resize": tau_resize, "tolerance": TIGHT,
+           "physics": "eta/s=0.12, zeta/s Gaussian bump 0.05 at T=0.175 GeV (width 0.02)"}
+    ms = {}
+    ms["plain_reference_tol"], hs = plain("reference")
+    for h in hs:
+        h.close()
+    ms["plain_tight"], hs = plain("tight")
+    ref_states = {k: hs[k].get_state(("Q", "pi", "Pi")) for k in sample}
+    for h in hs:
+        h.close()
+    for mode in ("tight", "tight_slope_mlp"):
+        ms["batched_" + mode], hs, bits, info = batched(mode)
+        out["error_bits_" + mode] = bits
+        out["tuned_" + mode] = {"nstreams": info["nstreams"], "block": info["block"]}
+        errs = {k: state_error(hs[k].get_state(("Q", "pi", "Pi")), ref_states[k]) for k in sample}
+        out["errors_" + mode] = {
+            f: {"max_rel": max(e[f]["max_rel"] for e in errs.values()),
+                "frac_beyond_1e-8": max(e[f]["frac_beyond_1e-8"] for e in errs.values()),
+                "norm_rel": max(e[f]["norm_rel"] for e in errs.values())} for f in ("Q", "pi", "Pi")}
+        for h in hs:
+            h.close()
+    for k, v in ms.items():
+        out[k] = cells * steps / (v / 1e3)
+    out["error_max"] = max(v["max_rel"] for v in out["errors_tight_slope_mlp"].values())
+    out["speedup"] = ms["plain_tight"] / ms["batched_tight_slope_mlp"]
+    out["speedup_vs_plain_reference_tol"] = ms["plain_reference_tol"] / ms["batched_tight_slope_mlp"]
+    out["speedup_batching_alone"] = ms["plain_tight"] / ms["batched_tight"]
+    out["error_sample"] = "%d events (the smallest and the largest)" % len(sample)
     return out
 
 
@@ -445,8 +625,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--batch-events", type=int, default=32,
-                    help="events of the batched-vs-plain measurement (0: skip)")
+    ap.add_argument("--batch-events", type=int, default=256,
+                    help="events of the batched + learned-guess measurement (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=20)
     ap.add_argument("--no-learned-guess", action="store_true")
     ap.add_argument("--vorticity", action="store_true",
@@ -465,7 +645,7 @@ def main():
     ws, rank, local = dist_env()
     dist = Ranks(ws)
     nx, ny, nz = args.grid
-    setup = W.glauber3d_setup(nx, ny, nz, seed=20260001 + rank)
+    setup = W.glauber3d_setup(nx, ny, nz, seed=EVENT_SEED + rank)
     cells = setup.grid.ncells
     h = capi.GpuHydro(setup, device=local)
     if args.vorticity:
@@ -487,6 +667,7 @@ def main():
     sampler = ClockSampler(gpu_index_for(local))
     time.sleep(0.3)
     dist.barrier()
+    nvtx("timed")
     h.timer_start()
     nel = 0
     pending = False
@@ -503,6 +684,7 @@ def main():
     if pending:
         nel += h.surface_end()["nelements"]
     ms = h.timer_stop()
+    nvtx()
     dist.barrier()
     clocks = sampler.stop()
     h.sync()
@@ -540,10 +722,33 @@ def main():
     achieved = alg / avg_s / 1e9
     roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic_per_launch(dname, args.grid, args.steps, dn),
+                "traffic": traffic_per_launch(dname, args.grid, dn),
                 "alg_bytes_per_launch": alg, "avg_launch_ms": avg_s * 1e3,
                 "active_cells_per_step": nactive / args.steps,
                 "alg_bytes_rule": KERNEL_BYTES_RULE.get(dname, "")}
+    # FP64 co-roofline: the dominant kernel's and the whole step's FP64
+    # operations (ncu counts of the same launches) over their CUDA-event
+    # time, against a cuBLAS DGEMM measured now
+    fp64_peak = fp64_peak_tflops(local)
+    fl = fp64_per_launch(dname, args.grid, dn)
+    step_fl = 0.0
+    for k, (n, _) in prof.items():
+        f = fp64_per_launch(k, args.grid, n)
+        step_fl = None if (f is None or step_fl is None) else step_fl + f * n
+    kern_s = sum(t for _, t in prof.values()) / 1e3
+    fp64_roofline = {
+        "kernel": dname, "unit": "TFLOP/s", "peak": fp64_peak,
+        "peak_source": "measured now: cuBLAS DGEMM 8192^3 (torch.mm, float64)",
+        "achieved": None if fl is None else fl / avg_s / 1e12,
+        "flops_per_launch": fl,
+        "step_achieved": None if step_fl is None else step_fl / kern_s / 1e12,
+        "step_flops_per_cell_update": None if step_fl is None else step_fl / (cells * args.steps),
+        "source": "profiles/fp64.json (ncu sm__sass_thread_inst_executed_op_d{add,mul,fma}_pred_on "
+                  "of the same workload's timed launches; flops = add + mul + 2 fma)"}
+    if fl is not None:
+        fp64_roofline["frac"] = fp64_roofline["achieved"] / fp64_peak
+    if step_fl is not None:
+        fp64_roofline["step_frac"] = fp64_roofline["step_achieved"] / fp64_peak
     step_bw = COMPULSORY_B * cells * args.steps / (ms / 1e3) / 1e9
     step_roofline = {"bound": "hbm", "achieved": step_bw, "peak": peak, "unit": "GB/s",
                      "frac": step_bw / peak, "bytes_per_cell_update": COMPULSORY_B}
@@ -605,18 +810,23 @@ def main():
                        "host_link_gbs: both directions' bytes over the whole time (copies and "
                        "kernels serialised by the step's data dependence)" % SURF_EVERY}
 
-    batch = batch2d = None
-    if args.batch_events > 0:
-        batch = batch_measure(capi, W, args.batch_events, args.batch_steps, local)
-        batch2d = batch_measure(capi, W, 2 * args.batch_events, 2 * args.batch_steps, local, nz=1)
-    learned = None
+    batch2d = learned = bmlp = None
+    mlp = None
     if not args.no_learned_guess:
-        learned = learned_guess_measure(capi, W, W.glauber3d_nb_setup(nx, ny, nz, seed=20260001 + rank),
-                                        30, local)
+        mlp, mlp_info = train_guess_network(capi, W, local)
+        learned = learned_guess_measure(capi, W, W.glauber3d_nb_setup(nx, ny, nz, seed=EVENT_SEED + rank),
+                                        30, local, mlp)
+        learned["train"] = mlp_info
+    if args.batch_events > 0:
+        if mlp is not None:
+            bmlp = batched_mlp_measure(capi, W, args.batch_events, args.batch_steps, local, mlp)
+        batch2d = batch_measure(capi, W, 64, 2 * args.batch_steps, local, nz=1)
+    if mlp is not None:
+        mlp.close()
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(W.glauber3d_setup(nx, ny, nz, seed=20260001))
+        cpu = cpu_baseline_sample(W.glauber3d_setup(nx, ny, nz, seed=EVENT_SEED))
 
     if rank == 0:
         line = {
@@ -630,9 +840,13 @@ def main():
                        "vorticity": bool(args.vorticity),
                        "l2": "inputs larger than L2 (%.0f MB of resident fields)" % (
                            cells * 8 * 127 / 1e6)},
-            "roofline": roofline, "step_roofline": step_roofline, "kernels": kernels,
-            "e2e": e2e, "cpu_baseline": cpu, "batch": batch, "batch_2d": batch2d, "learned_guess": learned,
-            "gpu_launches": lps * args.steps + 9 * (args.steps // SURF_EVERY), "clocks": clocks,
+            "roofline": roofline, "step_roofline": step_roofline, "fp64_roofline": fp64_roofline,
+            "kernels": kernels,
+            "e2e": e2e, "cpu_baseline": cpu, "batched_mlp": bmlp, "batch_2d": batch2d,
+            "learned_guess": learned,
+            # the step graph's kernels, and per pipelined surface call its
+            # nine kernels plus the overflow check (k_surf_keep)
+            "gpu_launches": lps * args.steps + 10 * (args.steps // SURF_EVERY), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     h.close()
