@@ -446,7 +446,7 @@ def _c2p_mode(h, mode, mlp):
     'tight_slope' (1e-13, the EoS's slope), 'tight_slope_mlp'."""
     h.set_con2prim_guess(None)
     h.set_con2prim_method(0)
-    h.set_con2prim(1e-5 if mode == "reference" else TIGHT)
+    h.set_con2prim(1e-5 if mode == "reference" else (1e-14 if mode == "tight14" else TIGHT))
     if "slope" in mode:
         h.set_con2prim_method(1)
     if "mlp" in mode:
@@ -595,6 +595,27 @@ def batched_mlp_measure(capi, W, n_events, steps, device, mlp, tau_resize=4.0, n
     ref_states = {k: hs[k].get_state(("Q", "pi", "Pi")) for k in sample}
     for h in hs:
         h.close()
+    # the noise floor: the same sample events stepped alone with the stop
+    # tightened to 1e-14 (the reference's method and start point).  Any
+    # change of the root find's path (start point, slope, stop) moves each
+    # root by ~1e-14 and the limiter and vacuum-edge branches amplify that
+    # to O(1) in some cells within ~10-20 steps, the oracle included.
+    floor = {}
+    for k in sample:
+        h = capi.GpuHydro(evs[k], device=device)
+        _c2p_mode(h, "tight14", mlp)
+        resized = False
+        for _ in range(steps):
+            h.advance(*drv[k])
+            if not resized and h.tau >= tau_resize:
+                h.resize2x()
+                resized = True
+        floor[k] = state_error(h.get_state(("Q", "pi", "Pi")), ref_states[k])
+        h.close()
+    out["errors_floor_tight_1e-14"] = {
+        f: {"max_rel": max(e[f]["max_rel"] for e in floor.values()),
+            "frac_beyond_1e-8": max(e[f]["frac_beyond_1e-8"] for e in floor.values()),
+            "norm_rel": max(e[f]["norm_rel"] for e in floor.values())} for f in ("Q", "pi", "Pi")}
     for mode in ("tight", "tight_slope_mlp"):
         ms["batched_" + mode], hs, bits, info = batched(mode)
         out["error_bits_" + mode] = bits

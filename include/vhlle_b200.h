@@ -56,6 +56,11 @@ typedef struct vh_ctx vh_ctx;
 typedef struct vh_grid {
   int nx, ny, nz;
   double xmin, xmax, ymin, ymax, etamin, etamax;
+  /* eta cell size: 0 derives it from the bounds as the Fluid constructor
+   * does (src/fld.cpp:79); a slab of a larger grid (vh_pack_planes) passes
+   * the whole grid's, so that its cells are the whole grid's bit for bit
+   * (its bounds then place its planes' coordinates). */
+  double dz;
 } vh_grid;
 
 /* EoS descriptor.  Device code cannot call the host EoS virtuals
@@ -260,6 +265,22 @@ typedef struct vh_glauber_ic {
   double nb_peak;      /* nb at the maximum (fm^-3) */
 } vh_glauber_ic;
 vh_status vh_init_glauber(vh_ctx *ctx, const vh_glauber_ic *ic);
+
+/* One event split into slabs along eta (one context per slab, a GPU each):
+ * every persistent field (Q, Qh, Qprev, pi, piH, Pi, PiH, m, viscCorrCut:
+ * VH_PLANE_DOUBLES doubles per cell) of the z-planes [z0, z0 + nplanes)
+ * into (pack) or out of (unpack) a contiguous DEVICE buffer laid out
+ * [field][component][plane][nx * ny], on the context's stream (no wait).
+ * A step reaches at most 6 cells along eta (the fill fractions 1, each ideal
+ * stage 2, NSquant's neighbours 1, the advection's upwind cell 1, the
+ * viscous face flux 1), so slabs that carry 6 halo planes on each inner
+ * side and receive them from their neighbours' owned planes once per step
+ * evolve their owned planes exactly as the whole grid does.  The slab
+ * contexts take the global cell size dz bit for bit (their eta bounds are
+ * chosen so).  No counterpart in the reference (it runs on one CPU core). */
+#define VH_PLANE_DOUBLES 47
+vh_status vh_pack_planes(vh_ctx *ctx, int z0, int nplanes, double *buf_dev);
+vh_status vh_unpack_planes(vh_ctx *ctx, int z0, int nplanes, const double *buf_dev);
 
 /* The number of cells the last viscous step relaxed and advected: those
  * with e > 0 at the half step, the cells ISformal does not zero

@@ -34,7 +34,7 @@ class _Grid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
                 ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
-                ("zmin", ctypes.c_double), ("zmax", ctypes.c_double)]
+                ("zmin", ctypes.c_double), ("zmax", ctypes.c_double), ("dz", ctypes.c_double)]
 
 
 class _Aux(ctypes.Structure):
@@ -267,7 +267,7 @@ class OracleRun:
         the C library's, as the reference does)."""
         self.setup = setup
         g = setup.grid
-        self.grid = _Grid(g.nx, g.ny, g.nz, *g.bounds())
+        self.grid = _Grid(g.nx, g.ny, g.nz, *g.bounds(), g.cell_dz or 0.0)
         self.eos = _EosHolder(setup.eos)
         self.eos.s.tol = 0.0 if tol is None else float(tol)
         self.eos.s.crmath = int(crmath)

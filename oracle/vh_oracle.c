@@ -23,6 +23,11 @@ int or_abi_version(void) { return 1; }
 /* ---------------------------------------------------------------- helpers */
 
 /* minmod slope limiter, src/cll.cpp:12-19 */
+/* Fluid's dz (src/fld.cpp:79), or the whole grid's for a slab of it */
+static double grid_dz(const or_grid *g) {
+  return g->dz > 0. ? g->dz : (g->zmax - g->zmin) / (g->nz - 1);
+}
+
 static double minmod(double a, double b) {
   if (a * b <= 0.) return 0.;
   if (fabs(a) > fabs(b))
@@ -1345,7 +1350,7 @@ int or_step(const or_grid *g, const or_eos *eos, const or_trc *tr,
   c->N = (long)g->nx * g->ny * g->nz;
   c->dx = (g->xmax - g->xmin) / (g->nx - 1);
   c->dy = (g->ymax - g->ymin) / (g->ny - 1);
-  c->dz = (g->zmax - g->zmin) / (g->nz - 1);
+  c->dz = grid_dz(g);
   c->tau = *tau;
   c->dt = dt;
   const long N = c->N;
@@ -1492,7 +1497,7 @@ void or_update_m(const or_grid *g, double *m, double tau, double dt) {
   cx.N = (long)g->nx * g->ny * g->nz;
   cx.dx = (g->xmax - g->xmin) / (g->nx - 1);
   cx.dy = (g->ymax - g->ymin) / (g->ny - 1);
-  cx.dz = (g->zmax - g->zmin) / (g->nz - 1);
+  cx.dz = grid_dz(g);
   cx.dm = (double *)calloc((size_t)(3 * cx.N), sizeof(double));
   updateM(&cx, tau, dt);
   free(cx.dm);
@@ -1520,7 +1525,7 @@ void or_totals(const or_grid *g, const or_eos *E, const or_trc *tr,
   const long N = (long)nx * ny * nz;
   const double dx = (g->xmax - g->xmin) / (nx - 1);
   const double dy = (g->ymax - g->ymin) / (ny - 1);
-  const double dz = (g->zmax - g->zmin) / (nz - 1);
+  const double dz = grid_dz(g);
   const int visc = tr_isViscous(tr);
   double E_ = 0., Efull = 0., S = 0., Px = 0., vt_num = 0., vt_den = 0.,
          vxvy_num = 0., vxvy_den = 0., pi0x_num = 0., pi0x_den = 0.,
@@ -1611,7 +1616,7 @@ int or_resize2x(const or_grid *g, const or_state *in, or_grid *gout,
                 or_state *out) {
   const double dx = (g->xmax - g->xmin) / (g->nx - 1);
   const double dy = (g->ymax - g->ymin) / (g->ny - 1);
-  const double dz = (g->zmax - g->zmin) / (g->nz - 1);
+  const double dz = grid_dz(g);
   const double x0 = g->xmin + 0 * dx, x1 = g->xmin + (g->nx - 1) * dx;
   const double y0 = g->ymin + 0 * dy, y1 = g->ymin + (g->ny - 1) * dy;
   if (x0 + x1 > 0.001 || y0 + y1 > 0.001) return 0;
@@ -2161,7 +2166,7 @@ static long surface_impl(const or_grid *g, const or_eos *E, const or_state *s, d
   const long N = (long)nx * ny * nz;
   const double dx = (g->xmax - g->xmin) / (nx - 1);
   const double dy = (g->ymax - g->ymin) / (ny - 1);
-  const double dz = (g->zmax - g->zmin) / (nz - 1);
+  const double dz = grid_dz(g);
   const double arrayDx[4] = {dtf, dx, dy, dz};
   long nel = 0;
   for (int ix = 2; ix < nx - 2; ix++)
@@ -2323,7 +2328,7 @@ long or_corona(const or_grid *g, const or_eos *E, const or_state *s, double tau,
   const long N = (long)nx * ny * nz;
   const double dx = (g->xmax - g->xmin) / (nx - 1);
   const double dy = (g->ymax - g->ymin) / (ny - 1);
-  const double dz = (g->zmax - g->zmin) / (nz - 1);
+  const double dz = grid_dz(g);
   long nel = 0;
   for (int ix = 2; ix < nx - 2; ix++)
     for (int iy = 2; iy < ny - 2; iy++)

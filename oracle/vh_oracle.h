@@ -27,6 +27,8 @@ extern "C" {
 typedef struct or_grid {
   int nx, ny, nz;
   double xmin, xmax, ymin, ymax, zmin, zmax; /* zmin/zmax = eta range */
+  double dz; /* 0: (zmax - zmin) / (nz - 1); else the cell size of a larger
+                grid this one is a slab of */
 } or_grid;
 
 /* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)

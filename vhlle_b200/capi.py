@@ -28,7 +28,8 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_abi_version", "vh_transform_pv", "vh_eos_eval", "vh_transport_eval", "vh_timer_start", "vh_timer_stop",
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_noalloc_prepare",
-           "vh_active_cells", "vh_set_con2prim_method", "vh_init_glauber",
+           "vh_active_cells", "vh_set_con2prim_method", "vh_init_glauber", "vh_pack_planes",
+           "vh_unpack_planes",
            "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
            "vh_surface_device", "vh_surface_write", "vh_enable_vorticity", "vh_vorticity_chain", "vh_get_dbeta",
@@ -54,6 +55,7 @@ class VhSurfaceInfo(ctypes.Structure):
 
 
 SURF_REC = 29
+VH_PLANE_DOUBLES = 47  # doubles per cell moved by vh_pack_planes / vh_unpack_planes
 
 
 def cornelius4d(cubes, dx, e0, device=0):
@@ -212,7 +214,7 @@ class VhGrid(ctypes.Structure):
     _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("xmin", ctypes.c_double), ("xmax", ctypes.c_double),
                 ("ymin", ctypes.c_double), ("ymax", ctypes.c_double),
-                ("etamin", ctypes.c_double), ("etamax", ctypes.c_double)]
+                ("etamin", ctypes.c_double), ("etamax", ctypes.c_double), ("dz", ctypes.c_double)]
 
 
 class VhEosAux(ctypes.Structure):
@@ -305,6 +307,8 @@ def lib():
     L.vh_active_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.vh_set_con2prim_method.argtypes = [vp, ctypes.c_int]
     L.vh_init_glauber.argtypes = [vp, ctypes.POINTER(VhGlauberIc)]
+    L.vh_pack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+    L.vh_unpack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
     L.vh_totals.argtypes = [vp, ctypes.c_double, _dp]
     L.vh_get_grid.argtypes = [vp, ctypes.POINTER(VhGrid)]
     L.vh_advance.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -398,7 +402,7 @@ class GpuHydro:
         self.setup = setup
         g = setup.grid
         self.N = g.ncells
-        grid = VhGrid(g.nx, g.ny, g.nz, *g.bounds())
+        grid = VhGrid(g.nx, g.ny, g.nz, *g.bounds(), g.cell_dz or 0.0)
         eos, self._eos_keep = make_eos(setup.eos)
         tr = make_trcoeff(setup)
         h = ctypes.c_void_p()
@@ -450,6 +454,15 @@ class GpuHydro:
         ic = VhGlauberIc(parts.ctypes.data_as(_dp), len(parts), smear, epeak, H.ctypes.data_as(_dp),
                          ecut, nb_peak)
         self._check(self.L.vh_init_glauber(self.h, ctypes.byref(ic)))
+
+    def pack_planes(self, z0, nplanes, buf_ptr):
+        """vh_pack_planes into the device buffer at buf_ptr (47 doubles per
+        cell of the planes)."""
+        self._check(self.L.vh_pack_planes(self.h, z0, nplanes, ctypes.c_void_p(buf_ptr)))
+
+    def unpack_planes(self, z0, nplanes, buf_ptr):
+        """vh_unpack_planes from the device buffer at buf_ptr."""
+        self._check(self.L.vh_unpack_planes(self.h, z0, nplanes, ctypes.c_void_p(buf_ptr)))
 
     def upload(self, fields: dict):
         v = VhStateView()

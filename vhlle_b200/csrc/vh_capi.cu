@@ -274,7 +274,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   g.N = (long long)grid->nx * grid->ny * grid->nz;
   g.dx = dx;
   g.dy = dy;
-  g.dz = (grid->etamax - grid->etamin) / (grid->nz - 1);
+  g.dz = grid->dz > 0. ? grid->dz : (grid->etamax - grid->etamin) / (grid->nz - 1);
   c->grid = *grid;
   c->tau = tau0;
   c->dt = dt;
@@ -490,6 +490,36 @@ vh_status vh_download_state(vh_ctx* ctx, const vh_state_view* h) {
   if (st != VH_OK) return st;
   VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return VH_OK;
+}
+
+static vh_status planes(vh_ctx* ctx, int z0, int nplanes, double* buf, bool pack,
+                        const char* who) {
+  if (!ctx || !buf || nplanes < 0) return VH_ERR_ARG;
+  if (z0 < 0 || (long long)z0 + nplanes > ctx->g.nz)
+    return fail(ctx, VH_ERR_ARG, std::string(who) + ": planes outside the grid's z range");
+  if (!pack) VH_NOT_PENDING(ctx, "vh_unpack_planes");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::PlaneFields pf{};
+  int k = 0;
+  for (const FieldSpec& fs : kFields) {
+    pf.p[k] = ctx->f.*(fs.dev);
+    pf.ncomp[k] = fs.ncomp;
+    pf.ncomp_total += fs.ncomp;
+    k++;
+  }
+  pf.nfield = k;
+  const long long nxy = (long long)ctx->g.nx * ctx->g.ny;
+  vh::launch_planes(pf, ctx->g.N, nxy, z0, nplanes, buf, pack, ctx->stream);
+  VH_CUDA(ctx, cudaGetLastError());
+  return VH_OK;
+}
+
+vh_status vh_pack_planes(vh_ctx* ctx, int z0, int nplanes, double* buf_dev) {
+  return planes(ctx, z0, nplanes, buf_dev, true, "vh_pack_planes");
+}
+
+vh_status vh_unpack_planes(vh_ctx* ctx, int z0, int nplanes, const double* buf_dev) {
+  return planes(ctx, z0, nplanes, const_cast<double*>(buf_dev), false, "vh_unpack_planes");
 }
 
 vh_status vh_device_state(vh_ctx* ctx, vh_state_view* d) {
@@ -739,6 +769,7 @@ vh_status vh_resize2x(vh_ctx* ctx, int* resized) {
   const double y0 = gr.ymin + 0 * g.dy, y1 = gr.ymin + (g.ny - 1) * g.dy;
   if (x0 + x1 > 0.001 || y0 + y1 > 0.001) return VH_OK;
   vh_grid ng = gr;
+  ng.dz = 0.;  // the new Fluid derives its cell size from its bounds
   ng.xmin = 2.0 * x0;
   ng.xmax = 2.0 * x1;
   ng.ymin = 2.0 * y0;

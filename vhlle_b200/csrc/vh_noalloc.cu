@@ -166,7 +166,7 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.g.N = N;
   a.g.dx = dx;
   a.g.dy = dy;
-  a.g.dz = (grid->etamax - grid->etamin) / (grid->nz - 1);
+  a.g.dz = grid->dz > 0. ? grid->dz : (grid->etamax - grid->etamin) / (grid->nz - 1);
   a.eos.kind = eos_dev->kind;
   a.eos.conf_cnst = eos_dev->conf_cnst;
   a.eos.ne = eos_dev->ne;

@@ -14,6 +14,8 @@
 //    the host from the reference's copy sequence (z, then y, then x).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "vh_physics.cuh"
 #include "vh_step.cuh"
 
@@ -1297,6 +1299,37 @@ __global__ void k_resize_gather(Geo g, const double* __restrict__ src, double* _
 void launch_resize_gather(const Geo& g, const double* src, double* dst, int ncomp,
                           cudaStream_t s) {
   if (g.N > 0) k_resize_gather<<<nblk(g.N, 256), 256, 0, s>>>(g, src, dst, ncomp);
+}
+
+// Planes z0 .. z0 + nz - 1 of every listed field to or from one contiguous
+// buffer laid out [field][component][plane][nx*ny] (pack = 1: fields ->
+// buffer).  A z-plane of a component is contiguous (x fastest, then y),
+// so a thread moves one double and consecutive threads move consecutive
+// doubles of one plane.
+__global__ void k_planes(PlaneFields pf, long long N, long long nxy, int z0, int nz,
+                         double* __restrict__ buf, int pack) {
+  const long long per = (long long)nz * nxy;  // doubles per component
+  const long long total = per * pf.ncomp_total;
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    long long c = t / per;
+    const long long r = t - c * per;
+    int f = 0;
+    while (c >= pf.ncomp[f]) c -= pf.ncomp[f++];
+    double* p = pf.p[f] + c * N + (long long)z0 * nxy + r;
+    if (pack)
+      buf[t] = *p;
+    else
+      *p = buf[t];
+  }
+}
+
+void launch_planes(const PlaneFields& pf, long long N, long long nxy, int z0, int nz,
+                   double* buf, bool pack, cudaStream_t s) {
+  const long long total = (long long)nz * nxy * pf.ncomp_total;
+  if (total <= 0) return;
+  const long long blocks = std::min<long long>((total + 255) / 256, 148LL * 16);
+  k_planes<<<(unsigned)blocks, 256, 0, s>>>(pf, N, nxy, z0, nz, buf, pack ? 1 : 0);
 }
 
 }  // namespace vh

@@ -114,6 +114,16 @@ void launch_clock_op(double* clk, int op, int n, cudaStream_t s);
 // gathers ncomp planes of the x2 resized grid from src into dst
 void launch_resize_gather(const Geo& g, const double* src, double* dst, int ncomp,
                           cudaStream_t s);
+// Up to nine fields (pointer, components) for launch_planes.
+struct PlaneFields {
+  double* p[9];
+  int ncomp[9];
+  int nfield, ncomp_total;
+};
+// z-planes [z0, z0 + nz) of every field to (pack) or from a contiguous
+// buffer [field][component][plane][nx*ny]
+void launch_planes(const PlaneFields& pf, long long N, long long nxy, int z0, int nz,
+                   double* buf, bool pack, cudaStream_t s);
 
 void launch_transform_pv(const EosDev& E, const double* Q, long long n, double* out,
                          cudaStream_t s);

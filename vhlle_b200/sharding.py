@@ -84,3 +84,94 @@ class Ranks:
         if self.dist and self.dist.is_initialized():
             self.dist.destroy_process_group()
         self.dist = None
+
+
+# --------------------------------------------------------------- one event, many GPUs
+# A single event split along eta into one slab per rank.  A step reaches at
+# most HALO cells along eta, so a slab that stores HALO extra planes beyond
+# each inner edge, refreshed from its neighbours' owned planes once per
+# step, evolves its owned planes bit for bit as the whole grid does (its own
+# ghost-cell copies at an inner edge touch only halo planes that the next
+# exchange overwrites).  The exchange is one send and one receive per inner
+# edge of HALO planes x every persistent field (vh_pack_planes /
+# vh_unpack_planes on the device; NCCL send/recv between the GPUs).
+HALO = 6
+
+
+def slab_ranges(nz: int, world: int, halo: int = HALO) -> List[Tuple[int, int, int, int]]:
+    """Per rank (owned z0, owned z1, stored z0, stored z1): owned planes
+    split as evenly as possible, each slab stored with `halo` more planes on
+    every side that has a neighbour."""
+    if world < 1 or nz < world * max(halo, 1):
+        raise ValueError("cannot split %d eta cells among %d ranks with %d halo planes "
+                         "(every slab must own at least as many planes as a halo)"
+                         % (nz, world, halo))
+    bounds = [nz * r // world for r in range(world + 1)]
+    out = []
+    for r in range(world):
+        a, b = bounds[r], bounds[r + 1]
+        out.append((a, b, max(0, a - halo), min(nz, b + halo)))
+    return out
+
+
+def slab_grid(grid, z0: int, z1: int):
+    """The Grid of planes [z0, z1) of `grid`: its eta bounds are the planes'
+    coordinates (Fluid::getZ of the whole grid) and its cell size is the
+    whole grid's, bit for bit."""
+    from . import workloads as W
+    dz = grid.dz
+    return W.Grid(grid.nx, grid.ny, z1 - z0, grid.xmin, grid.xmax, grid.ymin, grid.ymax,
+                  grid.etamin + z0 * dz, grid.etamin + (z1 - 1) * dz, cell_dz=dz)
+
+
+def slab_setup(setup, z0: int, z1: int):
+    """The Setup of planes [z0, z1) of an event (initial Q and m sliced)."""
+    import copy
+    g = setup.grid
+    nxy = g.nx * g.ny
+    s = copy.copy(setup)
+    s.grid = slab_grid(g, z0, z1)
+    s.Q = setup.Q.reshape(7, g.nz, nxy)[:, z0:z1].reshape(7, -1).copy()
+    s.m = setup.m.reshape(g.nz, nxy)[z0:z1].reshape(-1).copy()
+    if setup.pi is not None:
+        s.pi = setup.pi.reshape(10, g.nz, nxy)[:, z0:z1].reshape(10, -1).copy()
+    if setup.Pi is not None:
+        s.Pi = setup.Pi.reshape(g.nz, nxy)[z0:z1].reshape(-1).copy()
+    s.name = "%s_slab_%d_%d" % (setup.name, z0, z1)
+    return s
+
+
+def halo_plan(ranges, rank: int):
+    """The exchanges of `rank`, lower neighbour first: (peer, send z0 and
+    planes (local), receive z0 and planes (local)).  What a rank sends is
+    the part of its owned planes its neighbour stores as halo; what it
+    receives fills its own halo."""
+    a, b, c, d = ranges[rank]
+    plan = []
+    if rank > 0:
+        dp = ranges[rank - 1][3]
+        plan.append((rank - 1, a - c, dp - a, 0, a - c))
+    if rank < len(ranges) - 1:
+        an, _, cn, _ = ranges[rank + 1]
+        plan.append((rank + 1, cn - c, an - cn, b - c, d - b))
+    return plan
+
+
+def exchange_halos(dist, ranges, rank: int, pack, unpack, new_buffer) -> None:
+    """One halo exchange of `rank` with its neighbours through torch
+    distributed point-to-point calls (NCCL between GPUs, gloo on the host):
+    pack(z0, n, buf) / unpack(z0, n, buf) move planes between the slab and a
+    buffer from new_buffer(n).  Every send and receive is posted before any
+    is waited on, so the ranks cannot deadlock."""
+    ops, recvs = [], []
+    for peer, z_send, n_send, z_recv, n_recv in halo_plan(ranges, rank):
+        sbuf, rbuf = new_buffer(n_send), new_buffer(n_recv)
+        pack(z_send, n_send, sbuf)
+        ops.append(dist.P2POp(dist.isend, sbuf, peer))
+        ops.append(dist.P2POp(dist.irecv, rbuf, peer))
+        recvs.append((z_recv, n_recv, rbuf))
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+    for z, n, buf in recvs:
+        unpack(z, n, buf)

@@ -68,6 +68,9 @@ class Grid:
     ymax: float
     etamin: float
     etamax: float
+    # the eta cell size of a larger grid this one is a slab of (None: from
+    # the bounds, as Fluid does)
+    cell_dz: Optional[float] = None
 
     @property
     def ncells(self) -> int:
@@ -83,6 +86,8 @@ class Grid:
 
     @property
     def dz(self) -> float:
+        if self.cell_dz:
+            return self.cell_dz
         # nz = 1 gives an infinite cell, as the reference's FP64 division does
         span = self.etamax - self.etamin
         if self.nz == 1:
