@@ -71,11 +71,20 @@ typedef struct vh_grid {
  *  kind VH_EOS_CHIRAL:    EoSChiral (src/eoChiral.cpp:99-178): aux[0] the
  *                         chiralsmall table (used for e < 1.46, nb < 0.3),
  *                         aux[1] the chiraleos table (e < 146, nb < 6), and
- *                         p = 0.2964 e, T = 0.15120476935 e^(1/4) above.
+ *                         p = 0.2964 e, T = 0.15120476935 e^(1/4) above;
+ *  kind VH_EOS_TABLE3:    EoS3f (e, nb, nq, ns) table (src/eo3.cpp:21-175):
+ *                         sorted egrid[ne] and ngrid[nn] (one grid for the
+ *                         three charges), p/T/mub and muq/mus at
+ *                         [ie + ne*ib + ne*nn*iq + ne*nn*nn*is].  The states
+ *                         evolved here carry no electric or strange charge
+ *                         (no IC sets them and the fluxes keep them zero),
+ *                         so the lookups take nq = ns = 0 as the reference's
+ *                         transformPV then does.
  * Host arrays are copied at vh_create. */
 #define VH_EOS_CONFORMAL 0
 #define VH_EOS_TABLE 1
 #define VH_EOS_CHIRAL 2
+#define VH_EOS_TABLE3 3
 /* One EoSaux table (src/eoChiral.cpp:33-97) after its constructor's unit
  * conversions: the e and nb grids are uniform from emin to emax (GeV/fm^3)
  * and nmin to nmax (fm^-3) with ne, nn >= 2 points; p (GeV/fm^3), T, muB,
@@ -91,6 +100,7 @@ typedef struct vh_eos {
   int ne, nn;
   const double *egrid, *ngrid, *p, *T, *mub;
   vh_eos_aux aux[2]; /* VH_EOS_CHIRAL only */
+  const double *muq, *mus; /* VH_EOS_TABLE3 only */
 } vh_eos;
 
 /* TransportCoeff public constants (src/trancoeff.h:8-11, ctor :14-20). */

@@ -47,7 +47,8 @@ class _Eos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
-                ("tol", ctypes.c_double), ("aux", _Aux * 2), ("crmath", ctypes.c_int)]
+                ("tol", ctypes.c_double), ("aux", _Aux * 2), ("crmath", ctypes.c_int),
+                ("muq", _dp), ("mus", _dp)]
 
 
 class _Trc(ctypes.Structure):
@@ -82,6 +83,7 @@ def oracle_lib():
         lib.or_transport_eval.argtypes = [ctypes.POINTER(_Trc), _dp, ctypes.c_int, _dp]
         lib.or_eos_eval.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_eos6.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
+        lib.or_eos_full.argtypes = [ctypes.POINTER(_Eos), _dp, ctypes.c_int, _dp]
         lib.or_eos_s.argtypes = [ctypes.POINTER(_Eos), _dp, _dp, ctypes.c_int, _dp]
         lib.or_update_m.argtypes = [ctypes.POINTER(_Grid), _dp, ctypes.c_double, ctypes.c_double]
         lib.or_resize2x.restype = ctypes.c_int
@@ -132,6 +134,7 @@ def ref_lib():
         lib.ref_transform_pv.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_transport_eval.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_set_prim_var.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_eos_full.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_output_corona.restype = ctypes.c_int
         lib.ref_output_corona.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                           ctypes.c_char_p, ctypes.c_int]
@@ -236,6 +239,14 @@ class _EosHolder:
             self.s.ne = len(arrs[0])
             self.s.nn = len(arrs[1])
             self.s.egrid, self.s.ngrid, self.s.p, self.s.T, self.s.mub = (_ptr(a) for a in arrs)
+        if eos.kind == 3:
+            arrs = [np.ascontiguousarray(a, dtype=np.float64)
+                    for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
+            self.keep = arrs
+            self.s.ne = len(arrs[0])
+            self.s.nn = len(arrs[1])
+            (self.s.egrid, self.s.ngrid, self.s.p, self.s.T, self.s.mub, self.s.muq,
+             self.s.mus) = (_ptr(a) for a in arrs)
         if eos.kind == 2:
             for k, a in enumerate(eos.aux):
                 arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
@@ -424,6 +435,13 @@ class OracleRun:
         self.lib.or_transport_eval(ctypes.byref(self.trc), _ptr(inp), len(inp), _ptr(out))
         return out
 
+    def eos_full(self, pts):
+        """EoS::eos at pts[n][4] = e, nb, nq, ns -> [n][5] = p, T, muB, muQ, muS."""
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 4)
+        out = np.zeros((len(pts), 5))
+        self.lib.or_eos_full(ctypes.byref(self.eos.s), _ptr(pts), len(pts), _ptr(out))
+        return out
+
     def eos6(self, e, nb):
         """[n][6] = p, T, muB, muS, EoS::p, EoS::s (nq = ns = 0)."""
         return _eos6(self.lib.or_eos6, ctypes.byref(self.eos.s), e, nb)
@@ -466,6 +484,10 @@ class RefRun:
             self._tmp = tempfile.TemporaryDirectory()
             eos_file = os.path.join(self._tmp.name, "eos1f.dat")
             setup.eos.write_eos1f(eos_file)
+        if setup.eos.kind == 3 and eos_file is None:
+            self._tmp = tempfile.TemporaryDirectory()
+            eos_file = os.path.join(self._tmp.name, "eos3f.dat")
+            setup.eos.write_eos3f(eos_file)
         if setup.eos.kind == 2 and eos_file is None:  # the directory that holds eos/
             self._tmp = tempfile.TemporaryDirectory()
             eos_file = self._tmp.name
@@ -579,6 +601,13 @@ class RefRun:
     def eos6(self, e, nb):
         """[n][6] = p, T, muB, muS, EoS::p, EoS::s (nq = ns = 0)."""
         return _eos6(self.lib.ref_eos6, self.h, e, nb)
+
+    def eos_full(self, pts):
+        """EoS::eos at pts[n][4] = e, nb, nq, ns -> [n][5] = p, T, muB, muQ, muS."""
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 4)
+        out = np.zeros((len(pts), 5))
+        self.lib.ref_eos_full(self.h, _ptr(pts), len(pts), _ptr(out))
+        return out
 
     def eos_eval(self, e, nb):
         e = np.ascontiguousarray(e, dtype=np.float64)

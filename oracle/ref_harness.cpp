@@ -30,6 +30,7 @@
 #include "cll.h"
 #include "cornelius.h"
 #include "eo1.h"
+#include "eo3.h"
 #include "eoChiral.h"
 #include "fld.h"
 #include "hdo.h"
@@ -114,6 +115,10 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
       delete r;
       return nullptr;
     }
+  } else if (eos_kind == 3) {
+    // EoS3f: the header's B is 0 in the files used here, so the
+    // constructor's own arguments are not compared with it
+    r->eos = new EoS3f(const_cast<char *>(eos_file), 0., 0., 0., 0., 0.);
   } else {
     r->eos = new EoS1f(const_cast<char *>(eos_file));
   }
@@ -341,6 +346,17 @@ void ref_eos(void *p, const double *e, const double *nb, int n, double *out,
     out[3 * i + 1] = T;
     out[3 * i + 2] = mub;
     if (s_out) s_out[i] = r->eos->s(e[i], nb[i], 0., 0.);
+  }
+}
+
+// EoS::eos at general charges: in[n][4] = e, nb, nq, ns -> out[n][5] = p,
+// T, muB, muQ, muS
+void ref_eos_full(void *p, const double *in, int n, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  for (int i = 0; i < n; i++) {
+    const double *a = in + 4 * i;
+    double *o = out + 5 * i;
+    r->eos->eos(a[0], a[1], a[2], a[3], o[1], o[2], o[3], o[4], o[0]);
   }
 }
 

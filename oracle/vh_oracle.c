@@ -155,9 +155,71 @@ static void eos_chiral(const or_eos *E, double e, double nb, double *T,
   }
 }
 
-/* EoS::eos(); muq = 0 for every supported kind, mus = 0 but for kind 2 */
-static void eos_eval4(const or_eos *E, double e, double nb, double *T,
-                      double *mub, double *mus, double *p) {
+/* EoS3f::getue / getun (src/eo3.cpp:98-130): the bracket of the binary
+ * search, clamped (the e index only from above), and the weight from the
+ * unclamped bracket */
+static void eo3_bracket(const double *g, int n, double x, int clamp_low,
+                        int *ix, double *u) {
+  int k, k1 = 0, k2 = n - 1;
+  while (k2 - k1 > 1) {
+    k = (k1 + k2) / 2;
+    if (x < g[k])
+      k2 = k;
+    else
+      k1 = k;
+  }
+  *ix = k1;
+  if (*ix > n - 2) *ix = n - 2;
+  if (clamp_low && *ix < 0) *ix = 0;
+  *u = (x - g[k1]) / (g[k2] - g[k1]);
+}
+
+/* EoS3f::eos, src/eo3.cpp:132-175.  For e < 0 the reference sets the
+ * outputs to 0 and then interpolates anyway (there is no return), so the
+ * extrapolated values it computes are what it returns. */
+static void eos3f(const or_eos *E, double e, double nb, double nq, double ns,
+                  double *T, double *mub, double *muq, double *mus,
+                  double *p) {
+  const int ne = E->ne, nn = E->nn;
+  int ixe, ixnb, ixnq, ixns;
+  double ue, ub, uq, us;
+  eo3_bracket(E->egrid, ne, e, 0, &ixe, &ue);
+  eo3_bracket(E->ngrid, nn, nb, 1, &ixnb, &ub);
+  eo3_bracket(E->ngrid, nn, nq, 1, &ixnq, &uq);
+  eo3_bracket(E->ngrid, nn, ns, 1, &ixns, &us);
+  const double we[2] = {1. - ue, ue}, wnb[2] = {1. - ub, ub};
+  const double wnq[2] = {1. - uq, uq}, wns[2] = {1. - us, us};
+  double sp = 0., sT = 0., sb = 0., sq = 0., ss = 0.;
+  for (int je = 0; je < 2; je++)
+    for (int jnb = 0; jnb < 2; jnb++)
+      for (int jnq = 0; jnq < 2; jnq++)
+        for (int jns = 0; jns < 2; jns++) {
+          const long k = (long)(ixe + je) + (long)ne * (ixnb + jnb) +
+                         (long)ne * nn * (ixnq + jnq) +
+                         (long)ne * nn * nn * (ixns + jns);
+          const double w = we[je] * wnb[jnb] * wnq[jnq] * wns[jns];
+          sp += w * E->p[k];
+          sT += w * E->T[k];
+          sb += w * E->mub[k];
+          sq += w * E->muq[k];
+          ss += w * E->mus[k];
+        }
+  if (sp < 0.) sp = 0.;
+  *p = sp;
+  *T = sT;
+  *mub = sb;
+  *muq = sq;
+  *mus = ss;
+}
+
+/* EoS::eos() with muq; muq = 0 but for kind 3, mus = 0 but for kinds 2, 3 */
+static void eos_eval5(const or_eos *E, double e, double nb, double *T,
+                      double *mub, double *muq, double *mus, double *p) {
+  *muq = 0.;
+  if (E->kind == 3) {
+    eos3f(E, e, nb, 0., 0., T, mub, muq, mus, p);
+    return;
+  }
   *mus = 0.;
   if (E->kind == 0) {
     *p = e / 3.;
@@ -170,6 +232,12 @@ static void eos_eval4(const or_eos *E, double e, double nb, double *T,
   }
 }
 
+static void eos_eval4(const or_eos *E, double e, double nb, double *T,
+                      double *mub, double *mus, double *p) {
+  double muq;
+  eos_eval5(E, e, nb, T, mub, &muq, mus, p);
+}
+
 static void eos_eval(const or_eos *E, double e, double nb, double *T,
                      double *mub, double *p) {
   double mus;
@@ -180,6 +248,11 @@ static void eos_eval(const or_eos *E, double e, double nb, double *T,
 static double eos_p(const or_eos *E, double e, double nb) {
   double T, mub, mus, p;
   if (E->kind == 0) return e / 3.;
+  if (E->kind == 3) {
+    double muq;
+    eos3f(E, e, nb, 0., 0., &T, &mub, &muq, &mus, &p);
+    return p;
+  }
   if (E->kind == 2) {
     eos_chiral(E, e, nb, &T, &mub, &mus, &p);
     return p;
@@ -191,9 +264,8 @@ static double eos_p(const or_eos *E, double e, double nb) {
 /* EoS::s, src/eos.cpp:18-25 */
 static double eos_s(const or_eos *E, double e, double nb, double nq,
                     double ns) {
-  double T, mub, mus, p;
-  const double muq = 0.;
-  eos_eval4(E, e, nb, &T, &mub, &mus, &p);
+  double T, mub, mus, p, muq;
+  eos_eval5(E, e, nb, &T, &mub, &muq, &mus, &p);
   if (T > 0.0)
     return (e + p - mub * nb - muq * nq - mus * ns) / T;
   else
@@ -1458,6 +1530,18 @@ void or_transport_eval(const or_trc *tr, const double *in, int n, double *out) {
 }
 
 /* out[n][6] = p, T, muB, muS, EoS::p, EoS::s (nq = ns = 0) */
+void or_eos_full(const or_eos *E, const double *in, int n, double *out) {
+  for (int i = 0; i < n; i++) {
+    const double *a = in + 4 * i;
+    double *o = out + 5 * i;
+    if (E->kind == 3) {
+      eos3f(E, a[0], a[1], a[2], a[3], &o[1], &o[2], &o[3], &o[4], &o[0]);
+    } else {
+      eos_eval5(E, a[0], a[1], &o[1], &o[2], &o[3], &o[4], &o[0]);
+    }
+  }
+}
+
 void or_eos6(const or_eos *eos, const double *e, const double *nb, int n, double *out) {
   for (int i = 0; i < n; i++) {
     double *o = out + 6 * i;
@@ -2214,8 +2298,8 @@ static long surface_impl(const or_grid *g, const or_eos *E, const or_state *s, d
           for (int k = 0; k < 7; k++) QC[k] = QC[k] / (tau + C[0]);
           double eC, pC, nbC, nqC, nsC = 0.0, vxC, vyC, vzC, TC, mubC, musC;
           transform_pv(E, QC, &eC, &pC, &nbC, &nqC, &nsC, &vxC, &vyC, &vzC);
-          eos_eval4(E, eC, nbC, &TC, &mubC, &musC, &pC);
-          const double muqC = 0.;
+          double muqC;
+          eos_eval5(E, eC, nbC, &TC, &mubC, &muqC, &musC, &pC);
           if (TC > 0.4 || fabs(mubC) > 0.85) acc[4] += 1.;
           if (eC > ecrit * 2.0 || eC < ecrit * 0.5) acc[0] += 1.;
           double dbI[16];
@@ -2358,8 +2442,8 @@ long or_corona(const or_grid *g, const or_eos *E, const or_state *s, double tau,
         const int isTail = !(eC >= 0.01);
         if (!isCorona || isTail) continue;
         double musC;
-        eos_eval4(E, eC, nbC, &TC, &mubC, &musC, &pC);
-        const double muqC = 0.;
+        double muqC;
+        eos_eval5(E, eC, nbC, &TC, &mubC, &muqC, &musC, &pC);
         if (TC > 0.4 || fabs(mubC) > 0.99) acc[4] += 1.;
         double piC[10], PiC = 0.;
         for (int k = 0; k < 10; k++) piC[k] = 0.;

@@ -32,7 +32,8 @@ typedef struct or_grid {
 } or_grid;
 
 /* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)
- * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb] */
+ * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb]
+ * kind 2: EoSChiral (aux below); kind 3: EoS3f (muq, mus below) */
 /* One EoSaux table of EoSChiral (src/eoChiral.cpp:33-97), converted to
  * GeV/fm^3, fm^-3 and GeV as its constructor does: uniform grids from emin
  * to emax and nmin to nmax, p/T/mub/mus[in * ne + ie]. */
@@ -53,6 +54,10 @@ typedef struct or_eos {
   double tol;
   or_aux aux[2]; /* kind 2: chiralsmall, chiraleos */
   int crmath; /* as or_trc.crmath, for EoSChiral's power law */
+  /* kind 3 (EoS3f, src/eo3.cpp): egrid[ne], ngrid[nn] (one grid for nb, nq,
+   * ns) and p, T, mub above plus muq, mus, all at
+   * [ie + ne*ib + ne*nn*iq + ne*nn*nn*is] */
+  const double *muq, *mus;
 } or_eos;
 
 /* Correctly rounded exp(x) and x^(1/4) (oracle/crm_shim.cpp). */
@@ -106,6 +111,10 @@ int or_step(const or_grid *g, const or_eos *eos, const or_trc *tr,
 /* transformPV (src/rmn.cpp:28-139) on n states Q[n][7] (row-major);
  * out[n][8] = e, p, nb, nq, ns, vx, vy, vz.  Q is not modified. */
 void or_transform_pv(const or_eos *eos, const double *Q, int n, double *out);
+
+/* EoS::eos at general charges: in[n][4] = e, nb, nq, ns -> out[n][5] =
+ * p, T, muB, muQ, muS (EoS3f::eos for kind 3, src/eo3.cpp:132-175). */
+void or_eos_full(const or_eos *eos, const double *in, int n, double *out);
 
 /* TransportCoeff::getEta + getTau (src/trancoeff.cpp:68-100) for n points:
  * in[n][6] = e, nb, T, muB, s, p -> out[n][4] = eta/s, zeta/s, tau_pi,

@@ -227,7 +227,7 @@ class VhEos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
-                ("aux", VhEosAux * 2)]
+                ("aux", VhEosAux * 2), ("muq", _dp), ("mus", _dp)]
 
 
 class VhGlauberIc(ctypes.Structure):
@@ -375,6 +375,11 @@ def make_eos(eos):
                 for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub)]
         d.ne, d.nn = len(keep[0]), len(keep[1])
         d.egrid, d.ngrid, d.p, d.T, d.mub = (_ptr(a) for a in keep)
+    if eos.kind == 3:
+        keep = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
+        d.ne, d.nn = len(keep[0]), len(keep[1])
+        d.egrid, d.ngrid, d.p, d.T, d.mub, d.muq, d.mus = (_ptr(a) for a in keep)
     if eos.kind == 2:
         for k, a in enumerate(eos.aux):
             arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]

@@ -185,6 +185,12 @@ const char* eos_problem(const vh_eos& e) {
         return "EoS table needs ne >= 2, nn >= 2 and at most 2^30 points";
       if (!e.egrid || !e.ngrid || !e.p || !e.T || !e.mub) return "EoS table needs all five arrays";
       return nullptr;
+    case VH_EOS_TABLE3:
+      if (e.ne < 2 || e.nn < 2 || (long long)e.ne * e.nn * e.nn * e.nn > (1LL << 31))
+        return "EoS3f table needs ne >= 2, nn >= 2 and at most 2^31 points";
+      if (!e.egrid || !e.ngrid || !e.p || !e.T || !e.mub || !e.muq || !e.mus)
+        return "EoS3f table needs all seven arrays";
+      return nullptr;
     case VH_EOS_CHIRAL:
       for (const vh_eos_aux& x : e.aux) {
         if (!size_ok(x.ne, x.nn) || !x.p || !x.T || !x.mub || !x.mus)
@@ -391,6 +397,48 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
       }
       rdev += r.size();
     }
+  }
+  if (eos->kind == VH_EOS_TABLE3) {
+    const int ne = eos->ne, nn = eos->nn;
+    const size_t n = (size_t)ne * nn * nn * nn;
+    double* buf = nullptr;
+    ALLOC(buf, (size_t)ne + nn + 5 * n);
+    c->eos.ne = ne;
+    c->eos.nn = nn;
+    c->eos.emode = c->eos.nmode = vh::GRID_BSEARCH;
+    c->eos.erinv = c->eos.nrinv = nullptr;
+    c->eos.egrid = buf;
+    c->eos.ngrid = buf + ne;
+    double* t = buf + ne + nn;
+    const double* src[5] = {eos->p, eos->T, eos->mub, eos->muq, eos->mus};
+    e = cudaMemcpy(buf, eos->egrid, ne * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(buf + ne, eos->ngrid, nn * sizeof(double), cudaMemcpyHostToDevice);
+    for (int q = 0; q < 5 && e == cudaSuccess; q++)
+      e = cudaMemcpy(t + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cuda_fail(c, e, "vh_create: EoS upload");
+      return bail(VH_ERR_CUDA);
+    }
+    c->eos.p = t;
+    c->eos.T = t + n;
+    c->eos.mub = t + 2 * n;
+    c->eos.muq = t + 3 * n;
+    c->eos.mus = t + 4 * n;
+    // EoS3f::getun (src/eo3.cpp:115-130) of a zero charge: every lookup's
+    // nq and ns
+    int k1 = 0, k2 = nn - 1;
+    while (k2 - k1 > 1) {
+      const int k = (k1 + k2) / 2;
+      if (0. < eos->ngrid[k])
+        k2 = k;
+      else
+        k1 = k;
+    }
+    int ix = k1 > nn - 2 ? nn - 2 : k1;
+    if (ix < 0) ix = 0;
+    c->eos.iq0 = ix;
+    c->eos.uq0 = (0. - eos->ngrid[k1]) / (eos->ngrid[k2] - eos->ngrid[k1]);
   }
   if (eos->kind == VH_EOS_CHIRAL) {
     for (int k = 0; k < 2; k++) {
@@ -669,6 +717,8 @@ vh_status vh_set_con2prim_method(vh_ctx* ctx, int method) {
   if (!ctx) return VH_ERR_ARG;
   if (method != VH_C2P_REFERENCE && method != VH_C2P_TABLE_SLOPE)
     return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_method: unknown method");
+  if (method == VH_C2P_TABLE_SLOPE && ctx->eos.kind == VH_EOS_TABLE3)
+    return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_method: no table slope for the EoS3f kind");
   if (method == VH_C2P_TABLE_SLOPE && !(ctx->eos.tol <= 1e-10))
     return fail(ctx, VH_ERR_ARG,
                 "vh_set_con2prim_method: the table slope needs a tight tolerance "

@@ -64,6 +64,13 @@ struct EosDev {
   // take it through the EK_*_SL instantiations)
   int slope;
   ChiralAux ch[2];  // kind 2: chiralsmall, chiraleos
+  // kind 3 (EoS3f): muQ and muS tables beside p, T, muB (the 4-D layout
+  // [ie + ne*ib + ne*nn*iq + ne*nn*nn*is]); iq0 and uq0 are the n-grid
+  // bracket and weight of a zero charge, the nq and ns of every lookup
+  const double* __restrict__ muq;
+  const double* __restrict__ mus;
+  int iq0;
+  double uq0;
 };
 
 __device__ __forceinline__ float c2p_guess(const EosDev& E, long long i) {
@@ -366,8 +373,8 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
 // con2prim iteration next to the table lookup, the chiral lookup made those
 // kernels spill more (face kernels 25 % slower on the table kind).
 // EK_TABLE_SL / EK_CHIRAL_SL: the same classes with the table-slope root
-// find (EosDev::slope = 1).
-enum { EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4 };
+// find (EosDev::slope = 1); EK_TABLE3: EoS3f (kind 3).
+enum { EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4, EK_TABLE3 = 5 };
 __host__ __device__ constexpr bool ek_chiral(int ek) { return ek == EK_CHIRAL || ek == EK_CHIRAL_SL; }
 __host__ __device__ constexpr bool ek_slope(int ek) { return ek == EK_TABLE_SL || ek == EK_CHIRAL_SL; }
 
@@ -389,9 +396,64 @@ __device__ __forceinline__ double eos_p_d(const EosDev& E, double e, double nb, 
   return p;
 }
 
+// EoS3f::eos, src/eo3.cpp:132-175, at nq = ns = 0 (their bracket iq0 and
+// weight uq0 are fixed): the binary searches of getue / getun (the e index
+// clamped from above only; the weights from the unclamped bracket), then
+// the 16 corners in the reference's order with the weight product
+// ((w_e w_nb) w_nq) w_ns.  For e < 0 the reference zeroes its outputs and
+// interpolates anyway (no return), which is what this does.
+template <bool WANT_T>
+__device__ __forceinline__ void eos3f(const EosDev& E, double e, double nb, double& T,
+                                      double& mub, double& muq, double& mus, double& p) {
+  const int ne = E.ne, nn = E.nn;
+  int k1, k2;
+  bsearch_grid(E.egrid, ne, e, k1, k2);
+  const int ixe = k1 > ne - 2 ? ne - 2 : k1;
+  const double ue = (e - __ldg(E.egrid + k1)) / (__ldg(E.egrid + k2) - __ldg(E.egrid + k1));
+  bsearch_grid(E.ngrid, nn, nb, k1, k2);
+  int ixb = k1 > nn - 2 ? nn - 2 : k1;
+  if (ixb < 0) ixb = 0;
+  const double ub = (nb - __ldg(E.ngrid + k1)) / (__ldg(E.ngrid + k2) - __ldg(E.ngrid + k1));
+  const double we[2] = {1. - ue, ue}, wb[2] = {1. - ub, ub};
+  const double wq[2] = {1. - E.uq0, E.uq0};
+  const long long sb = ne, sq = (long long)ne * nn, ss = (long long)ne * nn * nn;
+  double sp = 0., sT = 0., smb = 0., smq = 0., sms = 0.;
+#pragma unroll
+  for (int je = 0; je < 2; je++)
+#pragma unroll
+    for (int jb = 0; jb < 2; jb++)
+#pragma unroll
+      for (int jq = 0; jq < 2; jq++)
+#pragma unroll
+        for (int js = 0; js < 2; js++) {
+          const long long k = (ixe + je) + sb * (ixb + jb) + sq * (E.iq0 + jq) + ss * (E.iq0 + js);
+          const double w = we[je] * wb[jb] * wq[jq] * wq[js];
+          sp += w * __ldg(E.p + k);
+          if (WANT_T) {
+            sT += w * __ldg(E.T + k);
+            smb += w * __ldg(E.mub + k);
+            smq += w * __ldg(E.muq + k);
+            sms += w * __ldg(E.mus + k);
+          }
+        }
+  if (sp < 0.) sp = 0.;
+  p = sp;
+  if (WANT_T) {
+    T = sT;
+    mub = smb;
+    muq = smq;
+    mus = sms;
+  }
+}
+
 template <int EK = EK_ANY>
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
   double T, mub, mus, p;
+  if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
+    double muq;
+    eos3f<false>(E, e, nb, T, mub, muq, mus, p);
+    return p;
+  }
   if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
     eos_chiral<false>(E, e, nb, T, mub, mus, p);
     return p;
@@ -406,7 +468,10 @@ template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
                                          double& mub, double& mus, double& p) {
   mus = 0.;
-  if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
+  if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
+    double muq;
+    eos3f<true>(E, e, nb, T, mub, muq, mus, p);
+  } else if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
     eos_chiral<true>(E, e, nb, T, mub, mus, p);
   } else if (E.kind == 0) {
     p = ddivp(e, 3.);
@@ -424,12 +489,23 @@ __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
   eos_eval<EK>(E, e, nb, T, mub, mus, p);
 }
 
-// EoS::s, src/eos.cpp:18-25 (muq = 0)
+// EoS::eos with muQ, which only EoS3f has (0 for the other kinds)
+template <int EK = EK_ANY>
+__device__ __forceinline__ void eos_eval_q(const EosDev& E, double e, double nb, double& T,
+                                           double& mub, double& muq, double& mus, double& p) {
+  if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
+    eos3f<true>(E, e, nb, T, mub, muq, mus, p);
+    return;
+  }
+  muq = 0.;
+  eos_eval<EK>(E, e, nb, T, mub, mus, p);
+}
+
+// EoS::s, src/eos.cpp:18-25
 __device__ __forceinline__ double eos_s(const EosDev& E, double e, double nb,
                                         double nq, double ns) {
-  double T, mub, mus, p;
-  const double muq = 0.;
-  eos_eval(E, e, nb, T, mub, mus, p);
+  double T, mub, mus, p, muq;
+  eos_eval_q(E, e, nb, T, mub, muq, mus, p);
   if (T > 0.0) return ddivp(e + p - mub * nb - muq * nq - mus * ns, T);
   return 0.;
 }

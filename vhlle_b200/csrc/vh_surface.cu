@@ -437,8 +437,8 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
   for (int q = 0; q < 7; q++) QC[q] = QC[q] / (tau + C[0]);
   Prim P;
   transform_pv<EK>(a.E, QC, P);
-  double TC, mubC, musC, pC;
-  eos_eval<EK>(a.E, P.e, P.nb, TC, mubC, musC, pC);
+  double TC, mubC, muqC, musC, pC;
+  eos_eval_q<EK>(a.E, P.e, P.nb, TC, mubC, muqC, musC, pC);
   const double eC = P.e, nbC = P.nb;
   double vxC = P.vx, vyC = P.vy, vzC = P.vz;
   double* ct = a.contrib + (long long)el * 5;
@@ -497,7 +497,7 @@ __device__ __forceinline__ void surf_element(const SurfArgs& a, int el, int ncub
   }
   r[12] = TC;
   r[13] = mubC;
-  r[14] = 0.;
+  r[14] = muqC;
   r[15] = musC;
 #pragma unroll
   for (int q = 0; q < 10; q++) r[16 + q] = pc[q];
@@ -599,8 +599,8 @@ __global__ void __launch_bounds__(128) k_corona_elements(SurfArgs a) {
     corona_qc(g, a.Q, ix, iy, iz, tau, QC);
     Prim P;
     transform_pv(a.E, QC, P);
-    double TC, mubC, musC, pC;
-    eos_eval(a.E, P.e, P.nb, TC, mubC, musC, pC);
+    double TC, mubC, muqC, musC, pC;
+    eos_eval_q(a.E, P.e, P.nb, TC, mubC, muqC, musC, pC);
     const double eC = P.e, nbC = P.nb;
     double vxC = P.vx, vyC = P.vy, vzC = P.vz;
     double* ct = a.contrib + (long long)el * 5;
@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(128) k_corona_elements(SurfArgs a) {
     }
     r[12] = TC;
     r[13] = mubC;
-    r[14] = 0.;
+    r[14] = muqC;
     r[15] = musC;
 #pragma unroll
     for (int q = 0; q < 10; q++) r[16 + q] = pc[q];
@@ -695,7 +695,9 @@ __global__ void __launch_bounds__(kTotBlock) k_sum_cols(const double* __restrict
 void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double tau, double taup,
                         double* eN, double* eP, cudaStream_t s) {
   const unsigned nb = (unsigned)((g.N + 127) / 128);
-  if (E.kind == 2)
+  if (E.kind == 3)
+    k_surf_energy<EK_TABLE3><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
+  else if (E.kind == 2)
     k_surf_energy<EK_CHIRAL><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
   else
     k_surf_energy<EK_TABLE><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN,
@@ -749,7 +751,9 @@ void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double
                           int npartial, cudaStream_t s) {
   SurfArgs a{g,    E,    f.Q,      f.Qprev,   f.pi,   f.Pi, tau, dtf, ecrit,  xmin, ymin, zmin,
              cubes, counters, cap_cubes, cap_el, geo, off, rec, contrib};
-  if (E.kind == 2)
+  if (E.kind == 3)
+    k_surf_elements<EK_TABLE3><<<kElemGrid, 128, 0, s>>>(a);
+  else if (E.kind == 2)
     k_surf_elements<EK_CHIRAL><<<kElemGrid, 128, 0, s>>>(a);
   else
     k_surf_elements<EK_TABLE><<<kElemGrid, 128, 0, s>>>(a);

@@ -376,7 +376,11 @@ int launch_vorticity(const StepArgs& a, cudaStream_t s) {
   const VortDev& v = *a.vort;
   const unsigned nb = vblk(g.N, kVortBlock);
   const int nsb = vort_scan_blocks(g.N);
-  if (a.eos.kind == 2) {  // per EoS class, as the step's con2prim kernels
+  if (a.eos.kind == 3) {  // per EoS class, as the step's con2prim kernels
+    k_vort_T<EK_TABLE3><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
+    k_vort_ops<EK_TABLE3><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,
+                                                    F.pTh, a.clk, v);
+  } else if (a.eos.kind == 2) {
     k_vort_T<EK_CHIRAL><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
     k_vort_ops<EK_CHIRAL><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,
                                                     F.pTh, a.clk, v);

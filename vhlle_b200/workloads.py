@@ -112,7 +112,9 @@ class Grid:
 class EosTable:
     """EoS descriptor.  kind 0: conformal gas; kind 1: EoS1f (e, nb) table
     with p/T/mub stored [ie + ne*inb] (src/eo1.cpp:21-45); kind 2: EoSChiral
-    (src/eoChiral.cpp), `aux` = (chiralsmall, chiraleos) ChiralAux tables."""
+    (src/eoChiral.cpp), `aux` = (chiralsmall, chiraleos) ChiralAux tables;
+    kind 3: EoS3f (e, nb, nq, ns) table, one n grid for the three charges
+    (src/eo3.cpp:21-91)."""
     kind: int
     conf_cnst: float = CONF_CNST
     egrid: Optional[np.ndarray] = None
@@ -121,6 +123,12 @@ class EosTable:
     T: Optional[np.ndarray] = None
     mub: Optional[np.ndarray] = None
     aux: Optional[tuple] = None
+    # kind 3 (EoS3f): muQ and muS tables beside p, T, muB, all
+    # [ie + ne*inb + ne*nn*inq + ne*nn*nn*ins], and the file's header
+    # constants B, volex0, delta0, aaa, bbb
+    muq: Optional[np.ndarray] = None
+    mus: Optional[np.ndarray] = None
+    header3: tuple = (0.0, 0.0, 0.0, 0.0, 0.0)
 
     def write_chiral(self, directory: str) -> None:
         """directory/eos/chiralsmall.dat and chiraleos.dat, the files
@@ -156,6 +164,25 @@ class EosTable:
                 for inb in range(nn):
                     k = ie + ne * inb
                     f.write("%r %r %r\n" % (float(self.p[k]), float(self.T[k]), float(self.mub[k])))
+
+    def write_eos3f(self, path: str) -> None:
+        """Write the table in the reference's EoS3f text format: the header
+        constants ``B volex0 delta0 aaa bbb``, ``emax e0 nmax n0 ne nn``, the
+        e grid, the n grid, then ``p T mub muq mus`` rows with ie, inb, inq,
+        ins nested outer to inner (src/eo3.cpp:24-85); 17 significant digits."""
+        assert self.kind == 3
+        ne, nn = self.ne, self.nn
+        with open(path, "w") as f:
+            f.write(" ".join(repr(float(v)) for v in self.header3) + "\n")
+            f.write("%r %r %r %r %d %d\n" % (float(self.egrid[-1]), float(self.egrid[0]),
+                                            float(self.ngrid[-1]), float(self.ngrid[0]), ne, nn))
+            f.write(" ".join(repr(float(v)) for v in self.egrid) + "\n")
+            f.write(" ".join(repr(float(v)) for v in self.ngrid) + "\n")
+            idx = np.arange(ne * nn ** 3).reshape(nn, nn, nn, ne)  # [is][iq][ib][ie]
+            order = idx.transpose(3, 2, 1, 0).reshape(-1)           # ie, ib, iq, is nesting
+            cols = np.stack([self.p[order], self.T[order], self.mub[order], self.muq[order],
+                             self.mus[order]], 1)
+            f.write("\n".join(" ".join(repr(float(v)) for v in row) for row in cols) + "\n")
 
     @staticmethod
     def read_eos1f(path: str) -> "EosTable":
@@ -238,6 +265,32 @@ def chiral_eos() -> EosTable:
     mu_q * (3 / 1000), mu_S / 1000, p * 0.146, grid ends * 0.146 and * 0.15),
     so that the files (write_chiral) and these arrays hold the same doubles."""
     return EosTable(kind=2, aux=tuple(t[2] for t in _chiral_tables()))
+
+
+def eos3f_table(ne: int = 120, emin: float = 1e-4, emax: float = 1e3) -> EosTable:
+    """A synthetic EoS3f table: ``ne`` log e-points (1e-4 .. 1e3 GeV/fm^3)
+    and one n grid of 9 points on [-0.4, 0.4] fm^-3 (0 a node) for nb, nq
+    and ns; p = c_s^2(e) e + 0.5 nb^2 + 0.25 nq^2 + 0.15 ns^2 with the
+    c_s^2(e) of the other tables, T from the conformal-gas form, mu_B =
+    1 GeV fm^3 nb, mu_Q = 0.5 GeV fm^3 nq + 0.05 GeV fm^3 nb, mu_S = 0.3 GeV fm^3 ns + 0.1 GeV
+    fm^3 nb.  The header's B is 0, so the reference reads it without checking
+    its constructor's arguments against it (src/eo3.cpp:26-51)."""
+    egrid = np.exp(np.linspace(np.log(emin), np.log(emax), ne))
+    ngrid = np.array([-0.4, -0.3, -0.2, -0.1, 0.0, 0.1, 0.2, 0.3, 0.4])
+    nn = len(ngrid)
+    E = egrid[None, None, None, :]
+    nb = ngrid[None, None, :, None]
+    nq = ngrid[None, :, None, None]
+    ns = ngrid[:, None, None, None]
+    p = cs2_model(E) * E + 0.5 * nb * nb + 0.25 * nq * nq + 0.15 * ns * ns
+    T = 0.15120476935 * np.sqrt(np.sqrt(E)) + 0.0 * nb
+    shape = (nn, nn, nn, ne)
+    return EosTable(kind=3, egrid=egrid, ngrid=ngrid,
+                    p=np.broadcast_to(p, shape).reshape(-1).copy(),
+                    T=np.broadcast_to(T, shape).reshape(-1).copy(),
+                    mub=np.broadcast_to(1.0 * nb + 0 * E, shape).reshape(-1).copy(),
+                    muq=np.broadcast_to(0.5 * nq + 0.05 * nb + 0 * E, shape).reshape(-1).copy(),
+                    mus=np.broadcast_to(0.3 * ns + 0.1 * nb + 0 * E, shape).reshape(-1).copy())
 
 
 def cs2_model(e):
