@@ -160,6 +160,106 @@ class EoS1f : public EoS {
   }
 };
 
+// EoS3f (src/eo3.cpp:21-175): the (e, nb, nq, ns) table with one n grid
+// for the three charges.  Reads the reference's file (the header constants
+// B, volex0, delta0, aaa, bbb are compared with the constructor's when the
+// file's B is positive, as the reference does, with an exception in place
+// of its exit); eos() interpolates the 16 corners in the reference's order.
+class EoS3f : public EoS {
+  int ne_ = 0, nn_ = 0;
+  std::vector<double> eg_, ng_, p_, T_, mub_, muq_, mus_;
+
+  // getue / getun (src/eo3.cpp:98-130): the e index is clamped from above
+  // only, the weight comes from the unclamped bracket
+  static void bracket(const std::vector<double>& g, double x, bool clamp_low, int& ix,
+                      double& u) {
+    int n = (int)g.size(), k1 = 0, k2 = n - 1;
+    while (k2 - k1 > 1) {
+      const int k = (k1 + k2) / 2;
+      if (x < g[k])
+        k2 = k;
+      else
+        k1 = k;
+    }
+    ix = k1 > n - 2 ? n - 2 : k1;
+    if (clamp_low && ix < 0) ix = 0;
+    u = (x - g[k1]) / (g[k2] - g[k1]);
+  }
+  size_t index(int ie, int ib, int iq, int is) const {
+    return ie + (size_t)ne_ * ib + (size_t)ne_ * nn_ * iq + (size_t)ne_ * nn_ * nn_ * is;
+  }
+
+ public:
+  EoS3f(const char* filename, double B, double volex0, double delta0, double aaa, double bbb) {
+    std::ifstream fin(filename);
+    if (!fin) throw Error(VH_ERR_ARG, std::string("EoS3f: cannot open ") + filename);
+    double h[5];
+    for (double& v : h) fin >> v;
+    const double want[5] = {B, volex0, delta0, aaa, bbb};
+    if (h[0] > 0)
+      for (int k = 0; k < 5; k++)
+        if (std::fabs(h[k] - want[k]) > 1e-5)
+          throw Error(VH_ERR_ARG, "EoS3f: the table's header constants differ from the arguments");
+    double emax, e0, nmax, n0;
+    fin >> emax >> e0 >> nmax >> n0 >> ne_ >> nn_;
+    if (!fin || ne_ < 2 || nn_ < 2) throw Error(VH_ERR_ARG, "EoS3f: bad table header");
+    eg_.resize(ne_);
+    ng_.resize(nn_);
+    for (double& v : eg_) fin >> v;
+    for (double& v : ng_) fin >> v;
+    const size_t n = (size_t)ne_ * nn_ * nn_ * nn_;
+    for (auto* t : {&p_, &T_, &mub_, &muq_, &mus_}) t->resize(n);
+    for (int ie = 0; ie < ne_; ie++)
+      for (int ib = 0; ib < nn_; ib++)
+        for (int iq = 0; iq < nn_; iq++)
+          for (int is = 0; is < nn_; is++) {
+            const size_t k = index(ie, ib, iq, is);
+            fin >> p_[k] >> T_[k] >> mub_[k] >> muq_[k] >> mus_[k];
+            if (p_[k] < 1e-18) p_[k] = 0.;
+          }
+    if (!fin) throw Error(VH_ERR_ARG, "EoS3f: truncated table");
+  }
+  void eos(double e, double nb, double nq, double ns, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    int ie, ib, iq, is;
+    double ue, ub, uq, us;
+    bracket(eg_, e, false, ie, ue);
+    bracket(ng_, nb, true, ib, ub);
+    bracket(ng_, nq, true, iq, uq);
+    bracket(ng_, ns, true, is, us);
+    const double we[2] = {1. - ue, ue}, wb[2] = {1. - ub, ub};
+    const double wq[2] = {1. - uq, uq}, ws[2] = {1. - us, us};
+    T = mub = muq = mus = p = 0.;
+    for (int je = 0; je < 2; je++)
+      for (int jb = 0; jb < 2; jb++)
+        for (int jq = 0; jq < 2; jq++)
+          for (int js = 0; js < 2; js++) {
+            const size_t k = index(ie + je, ib + jb, iq + jq, is + js);
+            const double w = we[je] * wb[jb] * wq[jq] * ws[js];
+            p += w * p_[k];
+            T += w * T_[k];
+            mub += w * mub_[k];
+            muq += w * muq_[k];
+            mus += w * mus_[k];
+          }
+    if (p < 0.) p = 0.;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_TABLE3;
+    d.ne = ne_;
+    d.nn = nn_;
+    d.egrid = eg_.data();
+    d.ngrid = ng_.data();
+    d.p = p_.data();
+    d.T = T_.data();
+    d.mub = mub_.data();
+    d.muq = muq_.data();
+    d.mus = mus_.data();
+    return d;
+  }
+};
+
 // EoSChiral (src/eoChiral.cpp): the reference's default EoS (eosType 1).
 // Reads dir/eos/chiraleos.dat (2001 x 401) and dir/eos/chiralsmall.dat
 // (201 x 201) in the EoSaux format (8 columns, nb outer, e inner) with its

@@ -6,6 +6,7 @@
 //   host_setprimvar table <eos1f file> <in> <out>
 //   host_setprimvar chiral <dir holding eos/> <in> <out>
 //   host_setprimvar conformal <cnst> <in> <out>
+//   host_setprimvar table3 <eos3f file> <in> <out>
 //
 // <in>: raw float64 [n][8] = tau, e, nb, nq, ns, vx, vy, vz;
 // <out>: raw float64 [n][7], the Q each call stores.
@@ -28,6 +29,8 @@ int main(int argc, char** argv) {
     eos.reset(new vhb::EoS1f(argv[2]));
   else if (kind == "chiral")
     eos.reset(new vhb::EoSChiral(argv[2]));
+  else if (kind == "table3")
+    eos.reset(new vhb::EoS3f(argv[2], 0., 0., 0., 0., 0.));
   else if (kind == "conformal")
     eos.reset(new vhb::EoSConformal(std::atof(argv[2])));
   else

@@ -48,11 +48,12 @@ def _setups():
         "table_cs2": W.small_glauber3d(9, 5),
         "conformal": W.gubser_setup(nx=9, ny=9),
         "chiral": W.glauber3d_nb_setup(9, 9, 5, eos=W.chiral_eos()),
+        "table3": W.glauber3d_nb_setup(9, 9, 5, eos=W.eos3f_table()),
     }
 
 
 @needs_ref
-@pytest.mark.parametrize("name", ["table_nb", "table_cs2", "conformal", "chiral"])
+@pytest.mark.parametrize("name", ["table_nb", "table_cs2", "conformal", "chiral", "table3"])
 def test_conserved_from_primitive_equals_reference(name):
     setup = _setups()[name]
     pts = _points()
@@ -67,7 +68,7 @@ def test_conserved_from_primitive_equals_reference(name):
 
 @needs_ref
 @pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
-@pytest.mark.parametrize("name", ["table_nb", "table_cs2", "conformal", "chiral"])
+@pytest.mark.parametrize("name", ["table_nb", "table_cs2", "conformal", "chiral", "table3"])
 def test_host_layer_set_prim_var_equals_reference(name, tmp_path):
     exe = str(tmp_path / "host_setprimvar")
     src = os.path.join(ROOT, "tests", "cpp", "host_setprimvar.cpp")
@@ -85,6 +86,10 @@ def test_host_layer_set_prim_var_equals_reference(name, tmp_path):
         arg = str(tmp_path)
         eos.write_chiral(arg)
         kind = "chiral"
+    elif eos.kind == 3:
+        arg = str(tmp_path / "eos3f.dat")
+        eos.write_eos3f(arg)
+        kind = "table3"
     else:
         arg = repr(float(eos.conf_cnst))
         kind = "conformal"
