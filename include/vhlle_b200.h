@@ -79,12 +79,17 @@ typedef struct vh_grid {
  *                         evolved here carry no electric or strange charge
  *                         (no IC sets them and the fluxes keep them zero),
  *                         so the lookups take nq = ns = 0 as the reference's
- *                         transformPV then does.
- * Host arrays are copied at vh_create. */
+ *                         transformPV then does;
+ *  kind VH_EOS_HADRON:    EoSHadron (src/eoHadron.cpp), the hadronic EoS the
+ *                         reference driver gives the freeze-out surface
+ *                         (eosTypeHadron 0): `hadron` below; for
+ *                         vh_set_surface_eos only.
+ * Host arrays are copied at vh_create (vh_set_surface_eos). */
 #define VH_EOS_CONFORMAL 0
 #define VH_EOS_TABLE 1
 #define VH_EOS_CHIRAL 2
 #define VH_EOS_TABLE3 3
+#define VH_EOS_HADRON 4
 /* One EoSaux table (src/eoChiral.cpp:33-97) after its constructor's unit
  * conversions: the e and nb grids are uniform from emin to emax (GeV/fm^3)
  * and nmin to nmax (fm^-3) with ne, nn >= 2 points; p (GeV/fm^3), T, muB,
@@ -101,6 +106,15 @@ typedef struct vh_eos {
   const double *egrid, *ngrid, *p, *T, *mub;
   vh_eos_aux aux[2]; /* VH_EOS_CHIRAL only */
   const double *muq, *mus; /* VH_EOS_TABLE3 only */
+  /* VH_EOS_HADRON only: the file's header ne nnb nnq e0 n0 logemin logemax
+   * lognmax (src/eoHadron.cpp:19) and its tables p, T, muB, muQ, muS and
+   * status at [inq + nnq*inb + nnq*nnb*ie] */
+  struct vh_eos_hadron {
+    int ne, nnb, nnq;
+    double e0, n0, logemin, logemax, lognmax;
+    const double *p, *T, *mub, *muq, *mus;
+    const int *status;
+  } hadron;
 } vh_eos;
 
 /* TransportCoeff public constants (src/trancoeff.h:8-11, ctor :14-20). */
@@ -130,6 +144,14 @@ vh_status vh_create(const vh_grid *grid, const vh_eos *eos,
                     const vh_trcoeff *tr, double tau0, double dt, int device,
                     vh_ctx **out);
 vh_status vh_destroy(vh_ctx *ctx);
+
+/* The EoS of the freeze-out surface, the corona and the totals: Fluid's
+ * eosH, which outputSurface and outputCorona swap in for their whole body
+ * (src/fld.cpp:540-542, 870-872, 885-887, 1085-1087); the reference driver
+ * passes EoSHadron or EoSSmash there (src/main.cpp:305-311).  eos = NULL
+ * goes back to the hydro EoS (the default).  Any kind but the conformal gas;
+ * VH_EOS_HADRON only here. */
+vh_status vh_set_surface_eos(vh_ctx *ctx, const vh_eos *eos);
 
 /* Uses `stream` (a cudaStream_t, NULL = legacy default) for all later work. */
 vh_status vh_set_stream(vh_ctx *ctx, void *stream);

@@ -48,7 +48,11 @@ class _Eos(ctypes.Structure):
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
                 ("tol", ctypes.c_double), ("aux", _Aux * 2), ("crmath", ctypes.c_int),
-                ("muq", _dp), ("mus", _dp)]
+                ("muq", _dp), ("mus", _dp),
+                ("hne", ctypes.c_int), ("hnnb", ctypes.c_int), ("hnnq", ctypes.c_int),
+                ("he0", ctypes.c_double), ("hn0", ctypes.c_double), ("logemin", ctypes.c_double),
+                ("logemax", ctypes.c_double), ("lognmax", ctypes.c_double),
+                ("status", ctypes.POINTER(ctypes.c_int))]
 
 
 class _Trc(ctypes.Structure):
@@ -135,6 +139,9 @@ def ref_lib():
         lib.ref_transport_eval.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_set_prim_var.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_eos_full.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_surface_eos_full.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        lib.ref_set_surface_eos.restype = ctypes.c_int
+        lib.ref_set_surface_eos.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]
         lib.ref_output_corona.restype = ctypes.c_int
         lib.ref_output_corona.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                           ctypes.c_char_p, ctypes.c_int]
@@ -247,6 +254,15 @@ class _EosHolder:
             self.s.nn = len(arrs[1])
             (self.s.egrid, self.s.ngrid, self.s.p, self.s.T, self.s.mub, self.s.muq,
              self.s.mus) = (_ptr(a) for a in arrs)
+        if eos.kind == 4:
+            arrs = [np.ascontiguousarray(a, dtype=np.float64)
+                    for a in (eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
+            st = np.ascontiguousarray(eos.status, dtype=np.int32)
+            self.keep = arrs + [st]
+            (self.s.hne, self.s.hnnb, self.s.hnnq, self.s.he0, self.s.hn0, self.s.logemin,
+             self.s.logemax, self.s.lognmax) = eos.hadron
+            self.s.p, self.s.T, self.s.mub, self.s.muq, self.s.mus = (_ptr(a) for a in arrs)
+            self.s.status = st.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
         if eos.kind == 2:
             for k, a in enumerate(eos.aux):
                 arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
@@ -269,7 +285,7 @@ def _trc(setup, crmath=False):
 class OracleRun:
     """The C restatement driven like Hydro: step() == performStep()."""
 
-    def __init__(self, setup, tol=None, vorticity=False, crmath=False):
+    def __init__(self, setup, tol=None, vorticity=False, crmath=False, surface_eos=None):
         """tol: the transformPV stopping tolerance (None: the reference's
         1e-5; a smaller value gives the tight-tolerance oracle).  vorticity:
         Hydro::enableVorticity, d_mu beta_nu per cell in self.dbeta.
@@ -282,6 +298,13 @@ class OracleRun:
         self.eos = _EosHolder(setup.eos)
         self.eos.s.tol = 0.0 if tol is None else float(tol)
         self.eos.s.crmath = int(crmath)
+        # Fluid's eosH: the EoS of the surface, corona and totals (SWAP_EOS,
+        # src/fld.cpp:540-542); the hydro EoS unless given
+        self.eosH = self.eos
+        if surface_eos is not None:
+            self.eosH = _EosHolder(surface_eos)
+            self.eosH.s.tol = self.eos.s.tol
+            self.eosH.s.crmath = int(crmath)
         self.trc = _trc(setup, crmath)
         self.state = initial_state(setup)
         self.tau = ctypes.c_double(setup.tau0)
@@ -374,7 +397,7 @@ class OracleRun:
     def totals(self):
         out = np.zeros(len(TOTALS))
         sv = self._sview()
-        self.lib.or_totals(ctypes.byref(self.grid), ctypes.byref(self.eos.s), ctypes.byref(self.trc),
+        self.lib.or_totals(ctypes.byref(self.grid), ctypes.byref(self.eosH.s), ctypes.byref(self.trc),
                            ctypes.byref(sv), self.tau.value, self.setup.ecrit, _ptr(out))
         return dict(zip(TOTALS, out))
 
@@ -385,7 +408,7 @@ class OracleRun:
         rec = np.zeros((cap, SURF_REC))
         acc = np.zeros(5)
         sv = self._sview()
-        n = self.lib.or_surface(ctypes.byref(self.grid), ctypes.byref(self.eos.s), ctypes.byref(sv),
+        n = self.lib.or_surface(ctypes.byref(self.grid), ctypes.byref(self.eosH.s), ctypes.byref(sv),
                                 self.tau.value, dtf, self.setup.ecrit, _ptr(rec), cap, _ptr(acc))
         if n < 0:
             raise RuntimeError("Cornelius stopped (the reference would exit)")
@@ -402,7 +425,7 @@ class OracleRun:
         beta = np.zeros((cap, 16))
         acc = np.zeros(5)
         sv = self._sview()
-        n = self.lib.or_surface_beta(ctypes.byref(self.grid), ctypes.byref(self.eos.s),
+        n = self.lib.or_surface_beta(ctypes.byref(self.grid), ctypes.byref(self.eosH.s),
                                      ctypes.byref(sv), self.tau.value, dtf, self.setup.ecrit,
                                      _ptr(rec), cap, _ptr(acc), _ptr(beta))
         if n < 0:
@@ -416,7 +439,7 @@ class OracleRun:
         rec = np.zeros((cap, SURF_REC))
         acc = np.zeros(5)
         sv = self._sview()
-        n = self.lib.or_corona(ctypes.byref(self.grid), ctypes.byref(self.eos.s), ctypes.byref(sv),
+        n = self.lib.or_corona(ctypes.byref(self.grid), ctypes.byref(self.eosH.s), ctypes.byref(sv),
                                self.tau.value, self.setup.ecrit, _ptr(rec), cap, _ptr(acc))
         assert n <= cap
         return rec[:n].copy(), dict(zip(SURF_ACC, acc))
@@ -467,7 +490,7 @@ def _eos6(fn, h, e, nb):
 class RefRun:
     """The compiled reference (Fluid/Hydro objects) behind the same interface."""
 
-    def __init__(self, setup, eos_file=None):
+    def __init__(self, setup, eos_file=None, surface_eos=None):
         self.setup = setup
         self.h = None
         self._tmp = None
@@ -498,6 +521,13 @@ class RefRun:
                                      setup.ecrit, setup.eos.kind, setup.eos.conf_cnst,
                                      (eos_file or "").encode(), _ptr(tr), setup.etaSparam,
                                      setup.zetaSparam)
+        if surface_eos is not None:  # Fluid's eosH (kind 4: EoSHadron)
+            if self._tmp is None:
+                self._tmp = tempfile.TemporaryDirectory()
+            hfile = os.path.join(self._tmp.name, "eos_hadron.dat")
+            surface_eos.write_hadron(hfile)
+            if self.lib.ref_set_surface_eos(self.h, surface_eos.kind, hfile.encode()) != 0:
+                raise ValueError("the reference has no surface EoS of kind %d" % surface_eos.kind)
         st = initial_state(setup)
         self.lib.ref_set_state(self.h, _ptr(st["Q"]), _ptr(st["pi"]), _ptr(st["piH"]),
                                _ptr(st["Pi"][0]), _ptr(st["PiH"][0]), _ptr(st["m"][0].copy()))
@@ -607,6 +637,13 @@ class RefRun:
         pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 4)
         out = np.zeros((len(pts), 5))
         self.lib.ref_eos_full(self.h, _ptr(pts), len(pts), _ptr(out))
+        return out
+
+    def surface_eos_full(self, pts):
+        """eos_full of the surface EoS (Fluid's eosH)."""
+        pts = np.ascontiguousarray(pts, dtype=np.float64).reshape(-1, 4)
+        out = np.zeros((len(pts), 5))
+        self.lib.ref_surface_eos_full(self.h, _ptr(pts), len(pts), _ptr(out))
         return out
 
     def eos_eval(self, e, nb):

@@ -32,6 +32,7 @@
 #include "eo1.h"
 #include "eo3.h"
 #include "eoChiral.h"
+#include "eoHadron.h"
 #include "fld.h"
 #include "hdo.h"
 #include "inc.h"
@@ -70,6 +71,9 @@ class ConformalEoS : public EoS {
 
 struct RefRun {
   EoS *eos = nullptr;
+  EoS *eosH = nullptr;  // the freeze-out EoS (Fluid's eosH); nullptr: eos
+  double bounds[6] = {0, 0, 0, 0, 0, 0};
+  double dt = 0;
   TransportCoeff *tr = nullptr;
   Fluid *f = nullptr;
   Hydro *h = nullptr;
@@ -128,6 +132,8 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
   r->f = new Fluid(r->eos, r->eos, r->tr, nx, ny, nz, bounds[0], bounds[1],
                    bounds[2], bounds[3], bounds[4], bounds[5], dt, ecrit);
   r->h = new Hydro(r->f, r->eos, r->tr, tau0, dt);
+  for (int k = 0; k < 6; k++) r->bounds[k] = bounds[k];
+  r->dt = dt;
   r->nx = nx;
   r->ny = ny;
   r->nz = nz;
@@ -138,6 +144,40 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
   return r;
 }
 
+// EoS::eos of the surface EoS at general charges, as ref_eos_full
+void ref_surface_eos_full(void *p, const double *in, int n, double *out) {
+  RefRun *r = static_cast<RefRun *>(p);
+  EoS *e = r->eosH ? r->eosH : r->eos;
+  for (int i = 0; i < n; i++) {
+    const double *a = in + 4 * i;
+    double *o = out + 5 * i;
+    e->eos(a[0], a[1], a[2], a[3], o[1], o[2], o[3], o[4], o[0]);
+  }
+}
+
+// Fluid's eosH, the EoS of outputSurface and outputCorona (src/fld.cpp:
+// 540-542, 870-872: SWAP_EOS), from a table file: kind 4 EoSHadron
+// (src/eoHadron.cpp).  The Fluid and Hydro are made again with it, so call
+// this before the state is set.  Returns 0, or -1 for an unknown kind.
+int ref_set_surface_eos(void *p, int kind, const char *file) {
+  RefRun *r = static_cast<RefRun *>(p);
+  std::streambuf *old = std::cout.rdbuf();
+  std::ostringstream quiet;
+  std::cout.rdbuf(quiet.rdbuf());
+  EoS *eh = nullptr;
+  if (kind == 4) eh = new EoSHadron(const_cast<char *>(file));
+  std::cout.rdbuf(old);
+  if (!eh) return -1;
+  r->eosH = eh;
+  const double tau0 = r->h->getTau();
+  delete r->h;
+  delete r->f;
+  r->f = new Fluid(r->eos, r->eosH, r->tr, r->nx, r->ny, r->nz, r->bounds[0], r->bounds[1],
+                   r->bounds[2], r->bounds[3], r->bounds[4], r->bounds[5], r->dt, r->ecrit);
+  r->h = new Hydro(r->f, r->eos, r->tr, tau0, r->dt);
+  return 0;
+}
+
 void ref_destroy(void *p) {
   RefRun *r = static_cast<RefRun *>(p);
   if (r->output_open && output::ffreeze.is_open()) output::ffreeze.close();
@@ -146,6 +186,7 @@ void ref_destroy(void *p) {
   delete r->f;
   delete r->tr;
   delete r->eos;
+  delete r->eosH;
   delete r;
 }
 
@@ -194,7 +235,7 @@ int ref_resize2x(void *p) {
   if (f->getX(0) + f->getX(f->getNX() - 1) > 0.001 ||
       f->getY(0) + f->getY(f->getNY() - 1) > 0.001)
     return 0;
-  Fluid *fnew = new Fluid(r->eos, r->eos, r->tr, f->getNX(), f->getNY(), f->getNZ(),
+  Fluid *fnew = new Fluid(r->eos, r->eosH ? r->eosH : r->eos, r->tr, f->getNX(), f->getNY(), f->getNZ(),
                           2.0 * f->getX(0), 2.0 * f->getX(f->getNX() - 1),
                           2.0 * f->getY(0), 2.0 * f->getY(f->getNY() - 1), f->getZ(0),
                           f->getZ(f->getNZ() - 1), 2.0 * r->h->getDtau(), f->geteCrit());
@@ -398,10 +439,21 @@ void ref_totals(void *p, double tau, double *out) {
       for (int iz = 2; iz < nz - 2; iz++) {
         Cell *c = f->getCell(ix, iy, iz);
         double e, nb, nq, ns, vx, vy, vz, t, mub, muq, mus, p, Q[7];
-        f->getCMFvariables(c, tau, e, nb, nq, ns, vx, vy, vz);
+        // outputSurface computes these after swapping in Fluid's eosH
+        // (src/fld.cpp:540-550): Fluid::getCMFvariables (src/fld.cpp:50-60)
+        // with that EoS
+        EoS *eh = r->eosH ? r->eosH : r->eos;
+        {
+          double pp, vzz;
+          c->getPrimVar(eh, tau, e, pp, nb, nq, ns, vx, vy, vzz);
+          const double etac = f->getZ(c->getZ());
+          vz = etac + 1. / 2. * log((1. + vzz) / (1. - vzz));
+          vx = vx * cosh(vz - etac) / cosh(vz);
+          vy = vy * cosh(vz - etac) / cosh(vz);
+        }
         c->getQ(Q);
-        r->eos->eos(e, nb, nq, ns, t, mub, muq, mus, p);
-        double s = r->eos->s(e, nb, nq, ns);
+        eh->eos(e, nb, nq, ns, t, mub, muq, mus, p);
+        double s = eh->s(e, nb, nq, ns);
         const double eta = f->getZ(iz);
         const double cosh_int = (sinh(eta + 0.5 * dz) - sinh(eta - 0.5 * dz)) / dz;
         const double sinh_int = (cosh(eta + 0.5 * dz) - cosh(eta - 0.5 * dz)) / dz;

@@ -212,12 +212,97 @@ static void eos3f(const or_eos *E, double e, double nb, double nq, double ns,
   *mus = ss;
 }
 
+/* EoSHadron: the table position of a charge (the "inverse log mapping" of
+ * src/eoHadron.cpp:97-112) */
+static double hadron_x(double n, double n0, double lognmax, double dxn,
+                       double n_abs_min) {
+  if (n != 0.0) {
+    const double zn = log(fabs(n) / n0);
+    if (zn >= -lognmax + 2.0 * dxn)
+      return n / fabs(n) * 0.5 * (zn + lognmax);
+    return n / n_abs_min * dxn;
+  }
+  return 0.;
+}
+
+/* EoSHadron::eos / ::p, src/eoHadron.cpp:81-208 (nq from the caller; the
+ * constructor's nb_abs_min, nq_abs_min and e_min recomputed as it does,
+ * src/eoHadron.cpp:49-53) */
+static void eos_hadron(const or_eos *E, double e, double nb, double nq,
+                       double *T, double *mub, double *muq, double *mus,
+                       double *p) {
+  const int ne = E->hne, nnb = E->hnnb, nnq = E->hnnq;
+#define IX3(ie, inb, inq) ((long)(inq) + (long)nnq * (inb) + (long)nnq * nnb * (ie))
+  const double dxnb0 = (2.0 * E->lognmax) / (nnb - 1);
+  const double dxnq0 = (2.0 * E->lognmax) / (nnq - 1);
+  const double nb_abs_min = E->hn0 * exp(2.0 * dxnb0 - E->lognmax);
+  const double nq_abs_min = E->hn0 * exp(2.0 * dxnq0 - E->lognmax);
+  const double e_min = E->he0 * exp(E->logemin);
+  if (e <= 0.) {
+    *T = *mub = *muq = *mus = *p = 0.;
+    return;
+  }
+  if (e < e_min) {
+    *p = e / e_min * E->p[IX3(0, nnb / 2, nnq / 2)];
+    *T = e / e_min * E->T[IX3(0, nnb / 2, nnq / 2)];
+    *mub = *muq = *mus = 0.;
+    return;
+  }
+  const double xe = log(e / E->he0);
+  const double dxe = (E->logemax - E->logemin) / (ne - 1);
+  const double dxnb = (2.0 * E->lognmax) / (nnb - 1);
+  const double dxnq = (2.0 * E->lognmax) / (nnq - 1);
+  const double xnb = hadron_x(nb, E->hn0, E->lognmax, dxnb, nb_abs_min);
+  const double xnq = hadron_x(nq, E->hn0, E->lognmax, dxnq, nq_abs_min);
+  int ie = (int)((xe - E->logemin) / dxe);
+  int inb = (int)((xnb + E->lognmax) / dxnb);
+  int inq = (int)((xnq + E->lognmax) / dxnq);
+  if (ie < 0) ie = 0;
+  if (inb < 0) inb = 0;
+  if (inq < 0) inq = 0;
+  if (ie > ne - 2) ie = ne - 2;
+  if (inb > nnb - 2) inb = nnb - 2;
+  if (inq > nnq - 2) inq = nnq - 2;
+  const double em = xe - E->logemin - ie * dxe;
+  const double nbm = xnb + E->lognmax - inb * dxnb;
+  const double nqm = xnq + E->lognmax - inq * dxnq;
+  if (E->status[IX3(ie, inb, inq)] == 1) {
+    *T = *mub = *muq = *mus = *p = 0.;
+    return;
+  }
+  const double we[2] = {1. - em / dxe, em / dxe};
+  const double wnb[2] = {1. - nbm / dxnb, nbm / dxnb};
+  const double wnq[2] = {1. - nqm / dxnq, nqm / dxnq};
+  double sT = 0., sb = 0., sq = 0., ss = 0., sp = 0.;
+  for (int je = 0; je < 2; je++)
+    for (int jnb = 0; jnb < 2; jnb++)
+      for (int jnq = 0; jnq < 2; jnq++) {
+        const long k = IX3(ie + je, inb + jnb, inq + jnq);
+        sp += we[je] * wnb[jnb] * wnq[jnq] * E->p[k];
+        sT += we[je] * wnb[jnb] * wnq[jnq] * E->T[k];
+        sb += we[je] * wnb[jnb] * wnq[jnq] * E->mub[k];
+        sq += we[je] * wnb[jnb] * wnq[jnq] * E->muq[k];
+        ss += we[je] * wnb[jnb] * wnq[jnq] * E->mus[k];
+      }
+#undef IX3
+  if (sp < 0.0) sp = 0.0;
+  *p = sp;
+  *T = sT;
+  *mub = sb;
+  *muq = sq;
+  *mus = ss;
+}
+
 /* EoS::eos() with muq; muq = 0 but for kind 3, mus = 0 but for kinds 2, 3 */
 static void eos_eval5(const or_eos *E, double e, double nb, double *T,
                       double *mub, double *muq, double *mus, double *p) {
   *muq = 0.;
   if (E->kind == 3) {
     eos3f(E, e, nb, 0., 0., T, mub, muq, mus, p);
+    return;
+  }
+  if (E->kind == 4) {
+    eos_hadron(E, e, nb, 0., T, mub, muq, mus, p);
     return;
   }
   *mus = 0.;
@@ -251,6 +336,11 @@ static double eos_p(const or_eos *E, double e, double nb) {
   if (E->kind == 3) {
     double muq;
     eos3f(E, e, nb, 0., 0., &T, &mub, &muq, &mus, &p);
+    return p;
+  }
+  if (E->kind == 4) {
+    double muq;
+    eos_hadron(E, e, nb, 0., &T, &mub, &muq, &mus, &p);
     return p;
   }
   if (E->kind == 2) {
@@ -1536,6 +1626,8 @@ void or_eos_full(const or_eos *E, const double *in, int n, double *out) {
     double *o = out + 5 * i;
     if (E->kind == 3) {
       eos3f(E, a[0], a[1], a[2], a[3], &o[1], &o[2], &o[3], &o[4], &o[0]);
+    } else if (E->kind == 4) {
+      eos_hadron(E, a[0], a[1], a[2], &o[1], &o[2], &o[3], &o[4], &o[0]);
     } else {
       eos_eval5(E, a[0], a[1], &o[1], &o[2], &o[3], &o[4], &o[0]);
     }

@@ -33,7 +33,8 @@ typedef struct or_grid {
 
 /* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)
  * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb]
- * kind 2: EoSChiral (aux below); kind 3: EoS3f (muq, mus below) */
+ * kind 2: EoSChiral (aux below); kind 3: EoS3f (muq, mus below);
+ * kind 4: EoSHadron (the hadronic EoS of the freeze-out surface) */
 /* One EoSaux table of EoSChiral (src/eoChiral.cpp:33-97), converted to
  * GeV/fm^3, fm^-3 and GeV as its constructor does: uniform grids from emin
  * to emax and nmin to nmax, p/T/mub/mus[in * ne + ie]. */
@@ -58,6 +59,12 @@ typedef struct or_eos {
    * ns) and p, T, mub above plus muq, mus, all at
    * [ie + ne*ib + ne*nn*iq + ne*nn*nn*is] */
   const double *muq, *mus;
+  /* kind 4 (EoSHadron, src/eoHadron.cpp): log-spaced e axis and the
+   * symmetric log mapping of nb and nq; p, T, mub, muq, mus and status at
+   * [inq + nnq*inb + nnq*nnb*ie] */
+  int hne, hnnb, hnnq;
+  double he0, hn0, logemin, logemax, lognmax;
+  const int *status;
 } or_eos;
 
 /* Correctly rounded exp(x) and x^(1/4) (oracle/crm_shim.cpp). */

@@ -1,0 +1,79 @@
+"""The freeze-out EoS (Fluid's eosH: outputSurface, outputCorona and the
+printed totals swap it in, src/fld.cpp:540-542, 870-872, 885-887) set to
+EoSHadron (src/eoHadron.cpp, the reference driver's default hadronic EoS)
+in the oracle against the reference's own classes: the lookup at general
+nb, nq bit for bit (below its e range, in its log mapping's linear core,
+the cells its status table marks invalid, beyond its edges), and the
+surface records, the corona and the totals of an event whose hydro EoS is
+the (e, nb) table.  The table is synthetic (workloads.hadron_eos_table) in
+the reference's file format."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import pyoracle as P
+from vhlle_b200 import workloads as W
+
+pytestmark = pytest.mark.skipif(not P.ref_available(), reason="compiled reference not present")
+
+
+def test_hadron_eos_lookup_equals_reference():
+    h = W.hadron_eos_table()
+    rng = np.random.default_rng(9)
+    n = 20000
+    e = np.concatenate([10 ** rng.uniform(-4, 1.5, n - 300), rng.uniform(0, 1e-3, 100),
+                        np.zeros(100), -rng.uniform(0, 1, 100)])
+    nb = np.concatenate([rng.uniform(-2.5, 2.5, n // 2), rng.uniform(-0.01, 0.01, n - n // 2)])
+    nq = rng.uniform(-0.3, 0.3, n)
+    nq[::5] = 0.0
+    nb[::7] = 0.0
+    pts = np.column_stack([e, nb, nq, np.zeros(n)])
+    s = W.glauber3d_nb_setup(5, 5, 5, eos=W.nb_table(200, 20))
+    o = P.OracleRun(s)
+    o_h = P.OracleRun(W.Setup("h", s.grid, h, s.tr, 0, 0, s.tau0, s.dt, s.ecrit, s.Q, s.m))
+    got = o_h.eos_full(pts)
+    r = P.RefRun(s, surface_eos=h)
+    ref = _ref_surface_eos_full(r, pts)
+    same = (got == ref) | (np.isnan(got) & np.isnan(ref))
+    assert same.all(), np.argwhere(~same)[:5]
+    assert (got[:, 0] == 0).sum() > 100 and np.abs(got[:, 3]).max() > 0.01
+
+
+def _ref_surface_eos_full(r, pts):
+    """EoSHadron::eos through the harness: a RefRun whose hydro EoS is the
+    hadron table would need the driver's hydro path; the lookup is called on
+    a second run created with the table as its hydro EoS file instead."""
+    return r.surface_eos_full(pts)
+
+
+def test_hadron_surface_eos_event_equals_reference():
+    h = W.hadron_eos_table()
+    s = W.glauber3d_nb_setup(21, 21, 11, eos=W.nb_table(200, 20))
+    o, r = P.OracleRun(s, surface_eos=h), P.RefRun(s, surface_eos=h)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "freezeout.dat.unfinished")
+        nc, _ = r.output_corona(d, extend=True)
+        co = P.read_freezeout(path, extend=True)
+        oc, _ = o.corona()
+        assert len(oc) == nc == len(co) > 0
+        assert (np.abs(oc - co) <= 1e-13 * np.maximum(np.abs(oc), np.abs(co)) + 1e-300).all()
+        for _ in range(4):
+            assert o.step(1) == 0
+            r.step(1)
+        t_o, t_r = o.totals(), r.totals()
+        for k in t_r:
+            assert t_o[k] == t_r[k], (k, t_o[k], t_r[k])
+        n, _ = r.output_surface(d, extend=True)
+        rec = P.read_freezeout(path, extend=True)[len(co):]
+    ro, _ = o.surface(cap=400000)
+    assert len(ro) == n > 50
+    ok = np.abs(ro - rec) <= 1e-13 * np.maximum(np.abs(ro), np.abs(rec)) + 1e-300
+    assert ok.all(), np.argwhere(~ok)[:5]
+    col = {c: k for k, c in enumerate(P.SURF_COLS)}
+    # the records carry the hadronic EoS's T, mu_B and mu_Q, not the hydro table's
+    o2 = P.OracleRun(s)
+    o2.step(4)
+    r2, _ = o2.surface(cap=400000)
+    assert not np.allclose(r2[:, col["T"]], ro[:, col["T"]])

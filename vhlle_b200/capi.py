@@ -29,6 +29,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_profile_enable", "vh_profile_read", "vh_profile_kinds", "vh_alloc_pinned",
            "vh_free_pinned", "vh_step_noalloc", "vh_noalloc_last_error", "vh_noalloc_prepare",
            "vh_active_cells", "vh_set_con2prim_method", "vh_init_glauber", "vh_pack_planes",
+           "vh_set_surface_eos",
            "vh_unpack_planes",
            "vh_totals",
            "vh_get_grid", "vh_advance", "vh_resize2x", "vh_surface", "vh_surface_begin", "vh_surface_end", "vh_surface_records",
@@ -223,11 +224,19 @@ class VhEosAux(ctypes.Structure):
                 ("p", _dp), ("T", _dp), ("mub", _dp), ("mus", _dp)]
 
 
+class VhEosHadron(ctypes.Structure):
+    _fields_ = [("ne", ctypes.c_int), ("nnb", ctypes.c_int), ("nnq", ctypes.c_int),
+                ("e0", ctypes.c_double), ("n0", ctypes.c_double), ("logemin", ctypes.c_double),
+                ("logemax", ctypes.c_double), ("lognmax", ctypes.c_double),
+                ("p", _dp), ("T", _dp), ("mub", _dp), ("muq", _dp), ("mus", _dp),
+                ("status", ctypes.POINTER(ctypes.c_int))]
+
+
 class VhEos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
-                ("aux", VhEosAux * 2), ("muq", _dp), ("mus", _dp)]
+                ("aux", VhEosAux * 2), ("muq", _dp), ("mus", _dp), ("hadron", VhEosHadron)]
 
 
 class VhGlauberIc(ctypes.Structure):
@@ -308,6 +317,7 @@ def lib():
     L.vh_set_con2prim_method.argtypes = [vp, ctypes.c_int]
     L.vh_init_glauber.argtypes = [vp, ctypes.POINTER(VhGlauberIc)]
     L.vh_pack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
+    L.vh_set_surface_eos.argtypes = [vp, ctypes.POINTER(VhEos)]
     L.vh_unpack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
     L.vh_totals.argtypes = [vp, ctypes.c_double, _dp]
     L.vh_get_grid.argtypes = [vp, ctypes.POINTER(VhGrid)]
@@ -380,6 +390,15 @@ def make_eos(eos):
                 for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
         d.ne, d.nn = len(keep[0]), len(keep[1])
         d.egrid, d.ngrid, d.p, d.T, d.mub, d.muq, d.mus = (_ptr(a) for a in keep)
+    if eos.kind == 4:
+        keep = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
+        st = np.ascontiguousarray(eos.status, dtype=np.int32)
+        keep.append(st)
+        h = d.hadron
+        h.ne, h.nnb, h.nnq, h.e0, h.n0, h.logemin, h.logemax, h.lognmax = eos.hadron
+        h.p, h.T, h.mub, h.muq, h.mus = (_ptr(a) for a in keep[:5])
+        h.status = st.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
     if eos.kind == 2:
         for k, a in enumerate(eos.aux):
             arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
@@ -459,6 +478,15 @@ class GpuHydro:
         ic = VhGlauberIc(parts.ctypes.data_as(_dp), len(parts), smear, epeak, H.ctypes.data_as(_dp),
                          ecut, nb_peak)
         self._check(self.L.vh_init_glauber(self.h, ctypes.byref(ic)))
+
+    def set_surface_eos(self, eos):
+        """vh_set_surface_eos: the freeze-out EoS (Fluid's eosH) from a
+        workloads.EosTable, or None for the hydro EoS."""
+        if eos is None:
+            self._check(self.L.vh_set_surface_eos(self.h, None))
+            return
+        d, keep = make_eos(eos)
+        self._check(self.L.vh_set_surface_eos(self.h, ctypes.byref(d)))
 
     def pack_planes(self, z0, nplanes, buf_ptr):
         """vh_pack_planes into the device buffer at buf_ptr (47 doubles per

@@ -191,6 +191,16 @@ const char* eos_problem(const vh_eos& e) {
       if (!e.egrid || !e.ngrid || !e.p || !e.T || !e.mub || !e.muq || !e.mus)
         return "EoS3f table needs all seven arrays";
       return nullptr;
+    case VH_EOS_HADRON: {
+      const vh_eos::vh_eos_hadron& h = e.hadron;
+      if (h.ne < 2 || h.nnb < 2 || h.nnq < 2 || (long long)h.ne * h.nnb * h.nnq > (1LL << 31))
+        return "EoSHadron table needs ne, nnb, nnq >= 2 and at most 2^31 points";
+      if (!h.p || !h.T || !h.mub || !h.muq || !h.mus || !h.status)
+        return "EoSHadron table needs all six arrays";
+      if (!(h.e0 > 0.) || !(h.n0 > 0.) || !(h.logemin < h.logemax) || !(h.lognmax > 0.))
+        return "EoSHadron table needs e0, n0 > 0, logemin < logemax and lognmax > 0";
+      return nullptr;
+    }
     case VH_EOS_CHIRAL:
       for (const vh_eos_aux& x : e.aux) {
         if (!size_ok(x.ne, x.nn) || !x.p || !x.T || !x.mub || !x.mus)
@@ -232,6 +242,177 @@ vh_status vh_destroy(vh_ctx* ctx) {
   return VH_OK;
 }
 
+// Lowers an EoS descriptor into device tables (allocated on the
+// context, freed with it): the hydro EoS at vh_create, the surface EoS at
+// vh_set_surface_eos.
+static vh_status upload_eos(vh_ctx* c, const vh_eos* eos, vh::EosDev& E) {
+  vh_status st = VH_OK;
+  cudaError_t e = cudaSuccess;
+  (void)e;
+  E.kind = eos->kind;
+  E.conf_cnst = eos->conf_cnst;
+  E.tol = 0.00001;  // src/rmn.cpp:96
+  E.vguess = nullptr;
+  E.stats = nullptr;
+  E.slope = 0;  // the reference's constant dp/de (src/rmn.cpp:36)
+  if (eos->kind == VH_EOS_TABLE) {
+    const int ne = eos->ne, nn = eos->nn;
+    double* buf = nullptr;
+    if ((st = dalloc(c, &buf, (size_t)((size_t)ne + nn + 3 * (size_t)ne * nn + (size_t)(ne - 1) + (nn - 1)))) != VH_OK) return st;
+    E.ne = ne;
+    E.nn = nn;
+    choose_axis_mode(eos->egrid, ne, &E.emode, &E.e0, &E.einv);
+    choose_axis_mode(eos->ngrid, nn, &E.nmode, &E.n0, &E.ninv);
+    E.egrid = buf;
+    E.ngrid = buf + ne;
+    E.p = buf + ne + nn;
+    E.T = E.p + (size_t)ne * nn;
+    E.mub = E.T + (size_t)ne * nn;
+    const size_t tb = (size_t)ne * nn * sizeof(double);
+    if ((e = cudaMemcpy((void*)E.egrid, eos->egrid, ne * sizeof(double), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)E.ngrid, eos->ngrid, nn * sizeof(double), cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)E.p, eos->p, tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)E.T, eos->T, tb, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy((void*)E.mub, eos->mub, tb, cudaMemcpyHostToDevice))) {
+      cuda_fail(c, e, "vh_create: EoS upload");
+      return VH_ERR_CUDA;
+    }
+    // reciprocals of the axis intervals for the interpolation weights
+    // (vh::interp_weight); an axis with an interval out of crm::mk_div's
+    // range keeps the divide
+    double* rdev = buf + ne + nn + 3 * (size_t)ne * nn;
+    const double* axes[2] = {eos->egrid, eos->ngrid};
+    const int lens[2] = {ne, nn};
+    E.erinv = E.nrinv = nullptr;
+    for (int a = 0; a < 2; a++) {
+      std::vector<double> r((size_t)lens[a] - 1);
+      bool ok = true;
+      for (int k = 0; k + 1 < lens[a]; k++) {
+        const double den = axes[a][k + 1] - axes[a][k];
+        ok = ok && vh::crm::mk_den_ok(den);
+        r[k] = 1.0 / den;
+      }
+      if (ok) {
+        if ((e = cudaMemcpy(rdev, r.data(), r.size() * sizeof(double), cudaMemcpyHostToDevice))) {
+          cuda_fail(c, e, "vh_create: EoS upload");
+          return VH_ERR_CUDA;
+        }
+        (a == 0 ? E.erinv : E.nrinv) = rdev;
+      }
+      rdev += r.size();
+    }
+  }
+  if (eos->kind == VH_EOS_TABLE3) {
+    const int ne = eos->ne, nn = eos->nn;
+    const size_t n = (size_t)ne * nn * nn * nn;
+    double* buf = nullptr;
+    if ((st = dalloc(c, &buf, (size_t)((size_t)ne + nn + 5 * n))) != VH_OK) return st;
+    E.ne = ne;
+    E.nn = nn;
+    E.emode = E.nmode = vh::GRID_BSEARCH;
+    E.erinv = E.nrinv = nullptr;
+    E.egrid = buf;
+    E.ngrid = buf + ne;
+    double* t = buf + ne + nn;
+    const double* src[5] = {eos->p, eos->T, eos->mub, eos->muq, eos->mus};
+    e = cudaMemcpy(buf, eos->egrid, ne * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(buf + ne, eos->ngrid, nn * sizeof(double), cudaMemcpyHostToDevice);
+    for (int q = 0; q < 5 && e == cudaSuccess; q++)
+      e = cudaMemcpy(t + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cuda_fail(c, e, "vh_create: EoS upload");
+      return VH_ERR_CUDA;
+    }
+    E.p = t;
+    E.T = t + n;
+    E.mub = t + 2 * n;
+    E.muq = t + 3 * n;
+    E.mus = t + 4 * n;
+    // EoS3f::getun (src/eo3.cpp:115-130) of a zero charge: every lookup's
+    // nq and ns
+    int k1 = 0, k2 = nn - 1;
+    while (k2 - k1 > 1) {
+      const int k = (k1 + k2) / 2;
+      if (0. < eos->ngrid[k])
+        k2 = k;
+      else
+        k1 = k;
+    }
+    int ix = k1 > nn - 2 ? nn - 2 : k1;
+    if (ix < 0) ix = 0;
+    E.iq0 = ix;
+    E.uq0 = (0. - eos->ngrid[k1]) / (eos->ngrid[k2] - eos->ngrid[k1]);
+  }
+  if (eos->kind == VH_EOS_CHIRAL) {
+    for (int k = 0; k < 2; k++) {
+      const vh_eos_aux& x = eos->aux[k];
+      const size_t n = (size_t)x.ne * x.nn;
+      double* buf = nullptr;
+      if ((st = dalloc(c, &buf, (size_t)(4 * n))) != VH_OK) return st;
+      const double* src[4] = {x.p, x.T, x.mub, x.mus};
+      for (int q = 0; q < 4; q++)
+        if ((e = cudaMemcpy(buf + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice))) {
+          cuda_fail(c, e, "vh_create: EoS upload");
+          return VH_ERR_CUDA;
+        }
+      E.ch[k] = vh::ChiralAux{x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax,
+                                   buf, buf + n, buf + 2 * n, buf + 3 * n};
+    }
+  }
+  if (eos->kind == VH_EOS_HADRON) {
+    const vh_eos::vh_eos_hadron& h = eos->hadron;
+    vh::HadronTab& H = E.h;
+    H.ne = h.ne;
+    H.nnb = h.nnb;
+    H.nnq = h.nnq;
+    H.e0 = h.e0;
+    H.n0 = h.n0;
+    H.logemin = h.logemin;
+    H.logemax = h.logemax;
+    H.lognmax = h.lognmax;
+    // the constructor's derived constants (src/eoHadron.cpp:49-53)
+    const double dxnb = (2.0 * h.lognmax) / (h.nnb - 1);
+    const double dxnq = (2.0 * h.lognmax) / (h.nnq - 1);
+    H.nb_abs_min = h.n0 * exp(2.0 * dxnb - h.lognmax);
+    H.nq_abs_min = h.n0 * exp(2.0 * dxnq - h.lognmax);
+    H.e_min = h.e0 * exp(h.logemin);
+    const size_t n = (size_t)h.ne * h.nnb * h.nnq;
+    double* buf = nullptr;
+    int* sbuf = nullptr;
+    if ((st = dalloc(c, &buf, 5 * n)) != VH_OK) return st;
+    if ((st = dalloc(c, &sbuf, n)) != VH_OK) return st;
+    const double* src[5] = {h.p, h.T, h.mub, h.muq, h.mus};
+    e = cudaSuccess;
+    for (int q = 0; q < 5 && e == cudaSuccess; q++)
+      e = cudaMemcpy(buf + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(sbuf, h.status, n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cuda_fail(c, e, "EoS upload");
+      return VH_ERR_CUDA;
+    }
+    H.p = buf;
+    H.T = buf + n;
+    H.mub = buf + 2 * n;
+    H.muq = buf + 3 * n;
+    H.mus = buf + 4 * n;
+    H.status = sbuf;
+  }
+  return VH_OK;
+}
+
+// The EoS outputSurface / outputCorona run with (Fluid's eosH, swapped in
+// for their whole body, src/fld.cpp:540-542, 870-872), with the hydro
+// EoS's root-find settings.
+static vh::EosDev surf_eos(const vh_ctx* c) {
+  vh::EosDev E = c->has_eosH ? c->eosH : c->eos;
+  E.tol = c->eos.tol;
+  E.stats = c->eos.stats;
+  E.vguess = nullptr;
+  E.slope = 0;
+  return E;
+}
+
 vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr, double tau0,
                     double dt, int device, vh_ctx** out) {
   if (!out) return fail(nullptr, VH_ERR_ARG, "vh_create: out is NULL");
@@ -245,6 +426,8 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   if (!(tau0 > 0.)) return fail(nullptr, VH_ERR_ARG, "vh_create: tau0 must be positive");
   if (const char* why = vh::eos_problem(*eos))
     return fail(nullptr, VH_ERR_ARG, std::string("vh_create: ") + why);
+  if (eos->kind == VH_EOS_HADRON)
+    return fail(nullptr, VH_ERR_ARG, "vh_create: EoSHadron is a surface EoS (vh_set_surface_eos)");
   const double dx = (grid->xmax - grid->xmin) / (grid->nx - 1);
   const double dy = (grid->ymax - grid->ymin) / (grid->ny - 1);
   if (!(dt > 0.) || dt > dx / 2. || dt > dy / 2.)
@@ -345,119 +528,32 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
     cuda_fail(c, e, "vh_create: upload");
     return bail(VH_ERR_CUDA);
   }
-  c->eos.kind = eos->kind;
-  c->eos.conf_cnst = eos->conf_cnst;
-  c->eos.tol = 0.00001;  // src/rmn.cpp:96
-  c->eos.vguess = nullptr;
-  c->eos.stats = nullptr;
-  c->eos.slope = 0;  // the reference's constant dp/de (src/rmn.cpp:36)
-  if (eos->kind == VH_EOS_TABLE) {
-    const int ne = eos->ne, nn = eos->nn;
-    double* buf = nullptr;
-    ALLOC(buf, (size_t)ne + nn + 3 * (size_t)ne * nn + (size_t)(ne - 1) + (nn - 1));
-    c->eos.ne = ne;
-    c->eos.nn = nn;
-    choose_axis_mode(eos->egrid, ne, &c->eos.emode, &c->eos.e0, &c->eos.einv);
-    choose_axis_mode(eos->ngrid, nn, &c->eos.nmode, &c->eos.n0, &c->eos.ninv);
-    c->eos.egrid = buf;
-    c->eos.ngrid = buf + ne;
-    c->eos.p = buf + ne + nn;
-    c->eos.T = c->eos.p + (size_t)ne * nn;
-    c->eos.mub = c->eos.T + (size_t)ne * nn;
-    const size_t tb = (size_t)ne * nn * sizeof(double);
-    if ((e = cudaMemcpy((void*)c->eos.egrid, eos->egrid, ne * sizeof(double), cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy((void*)c->eos.ngrid, eos->ngrid, nn * sizeof(double), cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy((void*)c->eos.p, eos->p, tb, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy((void*)c->eos.T, eos->T, tb, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy((void*)c->eos.mub, eos->mub, tb, cudaMemcpyHostToDevice))) {
-      cuda_fail(c, e, "vh_create: EoS upload");
-      return bail(VH_ERR_CUDA);
-    }
-    // reciprocals of the axis intervals for the interpolation weights
-    // (vh::interp_weight); an axis with an interval out of crm::mk_div's
-    // range keeps the divide
-    double* rdev = buf + ne + nn + 3 * (size_t)ne * nn;
-    const double* axes[2] = {eos->egrid, eos->ngrid};
-    const int lens[2] = {ne, nn};
-    c->eos.erinv = c->eos.nrinv = nullptr;
-    for (int a = 0; a < 2; a++) {
-      std::vector<double> r((size_t)lens[a] - 1);
-      bool ok = true;
-      for (int k = 0; k + 1 < lens[a]; k++) {
-        const double den = axes[a][k + 1] - axes[a][k];
-        ok = ok && vh::crm::mk_den_ok(den);
-        r[k] = 1.0 / den;
-      }
-      if (ok) {
-        if ((e = cudaMemcpy(rdev, r.data(), r.size() * sizeof(double), cudaMemcpyHostToDevice))) {
-          cuda_fail(c, e, "vh_create: EoS upload");
-          return bail(VH_ERR_CUDA);
-        }
-        (a == 0 ? c->eos.erinv : c->eos.nrinv) = rdev;
-      }
-      rdev += r.size();
-    }
-  }
-  if (eos->kind == VH_EOS_TABLE3) {
-    const int ne = eos->ne, nn = eos->nn;
-    const size_t n = (size_t)ne * nn * nn * nn;
-    double* buf = nullptr;
-    ALLOC(buf, (size_t)ne + nn + 5 * n);
-    c->eos.ne = ne;
-    c->eos.nn = nn;
-    c->eos.emode = c->eos.nmode = vh::GRID_BSEARCH;
-    c->eos.erinv = c->eos.nrinv = nullptr;
-    c->eos.egrid = buf;
-    c->eos.ngrid = buf + ne;
-    double* t = buf + ne + nn;
-    const double* src[5] = {eos->p, eos->T, eos->mub, eos->muq, eos->mus};
-    e = cudaMemcpy(buf, eos->egrid, ne * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess)
-      e = cudaMemcpy(buf + ne, eos->ngrid, nn * sizeof(double), cudaMemcpyHostToDevice);
-    for (int q = 0; q < 5 && e == cudaSuccess; q++)
-      e = cudaMemcpy(t + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-      cuda_fail(c, e, "vh_create: EoS upload");
-      return bail(VH_ERR_CUDA);
-    }
-    c->eos.p = t;
-    c->eos.T = t + n;
-    c->eos.mub = t + 2 * n;
-    c->eos.muq = t + 3 * n;
-    c->eos.mus = t + 4 * n;
-    // EoS3f::getun (src/eo3.cpp:115-130) of a zero charge: every lookup's
-    // nq and ns
-    int k1 = 0, k2 = nn - 1;
-    while (k2 - k1 > 1) {
-      const int k = (k1 + k2) / 2;
-      if (0. < eos->ngrid[k])
-        k2 = k;
-      else
-        k1 = k;
-    }
-    int ix = k1 > nn - 2 ? nn - 2 : k1;
-    if (ix < 0) ix = 0;
-    c->eos.iq0 = ix;
-    c->eos.uq0 = (0. - eos->ngrid[k1]) / (eos->ngrid[k2] - eos->ngrid[k1]);
-  }
-  if (eos->kind == VH_EOS_CHIRAL) {
-    for (int k = 0; k < 2; k++) {
-      const vh_eos_aux& x = eos->aux[k];
-      const size_t n = (size_t)x.ne * x.nn;
-      double* buf = nullptr;
-      ALLOC(buf, 4 * n);
-      const double* src[4] = {x.p, x.T, x.mub, x.mus};
-      for (int q = 0; q < 4; q++)
-        if ((e = cudaMemcpy(buf + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice))) {
-          cuda_fail(c, e, "vh_create: EoS upload");
-          return bail(VH_ERR_CUDA);
-        }
-      c->eos.ch[k] = vh::ChiralAux{x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax,
-                                   buf, buf + n, buf + 2 * n, buf + 3 * n};
-    }
+  {
+    vh_status se = upload_eos(c, eos, c->eos);
+    if (se != VH_OK) return bail(se);
   }
 #undef ALLOC
   *out = c;
+  return VH_OK;
+}
+
+vh_status vh_set_surface_eos(vh_ctx* ctx, const vh_eos* eos) {
+  if (!ctx) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_set_surface_eos");
+  if (!eos) {
+    ctx->has_eosH = false;
+    return VH_OK;
+  }
+  if (eos->kind == VH_EOS_CONFORMAL)
+    return fail(ctx, VH_ERR_ARG, "vh_set_surface_eos: the conformal gas is not a surface EoS");
+  if (const char* why = vh::eos_problem(*eos))
+    return fail(ctx, VH_ERR_ARG, std::string("vh_set_surface_eos: ") + why);
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  vh::EosDev E{};
+  vh_status st = upload_eos(ctx, eos, E);
+  if (st != VH_OK) return st;
+  ctx->eosH = E;
+  ctx->has_eosH = true;
   return VH_OK;
 }
 
@@ -924,7 +1020,7 @@ vh_status vh_totals(vh_ctx* ctx, double ecrit, double* out) {
   if (!ctx || !out) return VH_ERR_ARG;
   if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_totals: no state uploaded");
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
-  vh::launch_totals(ctx->g, ctx->eos, ctx->f, ctx->tau, ecrit, ctx->grid.etamin, ctx->viscous,
+  vh::launch_totals(ctx->g, surf_eos(ctx), ctx->f, ctx->tau, ecrit, ctx->grid.etamin, ctx->viscous,
                     ctx->tot_partial, ctx->tot_out, ctx->stream);
   VH_CUDA(ctx, cudaGetLastError());
   double h[vh::kTotals];
@@ -986,12 +1082,13 @@ static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t w
   cudaStream_t s = ctx->stream;
   const double taup = tau - ctx->fluid_dt;
   vh_ctx::Surf::Host& H = *S.host;
-  vh::launch_surf_energy(g, ctx->eos, f, tau, taup, S.eN, S.eP, s);
+  const vh::EosDev SE = surf_eos(ctx);
+  vh::launch_surf_energy(g, SE, f, tau, taup, S.eN, S.eP, s);
   vh::launch_surf_count(g, S.eN, S.eP, ecrit, S.blk, S.counters, s);
   vh::launch_surf_compact(g, S.eN, S.eP, ecrit, S.blk, S.cubes, cap_c, s);
   vh::launch_surf_cornelius(g, S.eN, S.eP, ecrit, ctx->fluid_dt, S.cubes, S.counters, cap_c,
                             S.geo, S.cnt, f.err, s);
-  vh::launch_surf_elements(g, ctx->eos, f, tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
+  vh::launch_surf_elements(g, SE, f, tau, ctx->fluid_dt, ecrit, ctx->grid.xmin,
                            ctx->grid.ymin, ctx->grid.etamin, S.cubes, S.counters, cap_c, cap_e,
                            S.geo, S.cnt, S.rec, S.contrib, S.partial, kSurfPartials, s);
   if (ctx->vort_on)  // beta.dat lines (src/fld.cpp:663-669, 798-831)
@@ -1156,9 +1253,9 @@ vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
         (st = dgrow(ctx, &S.contrib, &S.cap_contrib, want * vh::kSurfAcc)))
       return st;
     const int cap = (int)std::min<size_t>(want, INT32_MAX / 32);
-    vh::launch_surf_energy(g, ctx->eos, ctx->f, ctx->tau, ctx->tau - ctx->fluid_dt, S.eN, S.eP,
+    vh::launch_surf_energy(g, surf_eos(ctx), ctx->f, ctx->tau, ctx->tau - ctx->fluid_dt, S.eN, S.eP,
                            s);
-    vh::launch_corona(g, ctx->eos, ctx->f, ctx->tau, ecrit, ctx->grid.xmin, ctx->grid.ymin,
+    vh::launch_corona(g, surf_eos(ctx), ctx->f, ctx->tau, ecrit, ctx->grid.xmin, ctx->grid.ymin,
                       ctx->grid.etamin, S.eN, S.cflag, S.blk, S.counters, S.cubes, cap, S.rec,
                       S.contrib, S.partial, kSurfPartials, s);
     VH_CUDA(ctx, cudaGetLastError());

@@ -16,6 +16,10 @@ struct vh_ctx {
   cudaStream_t stream = nullptr;
   vh::Geo g{};
   vh::EosDev eos{};
+  // Fluid's eosH (vh_set_surface_eos): the EoS of the surface, the corona
+  // and the totals when has_eosH; else the hydro EoS
+  vh::EosDev eosH{};
+  bool has_eosH = false;
   vh::TrDev tr{};
   vh::Fields f{};
   double tau = 0., dt = 0.;

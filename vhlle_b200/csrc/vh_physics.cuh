@@ -36,6 +36,17 @@ struct ChiralAux {
   const double *__restrict__ p, *__restrict__ T, *__restrict__ mub, *__restrict__ mus;
 };
 
+// EoSHadron's tables and constants (kind 4, the freeze-out EoS):
+// p/T/mub/muq/mus and status at [inq + nnq*inb + nnq*nnb*ie]
+struct HadronTab {
+  int ne, nnb, nnq;
+  double e0, n0, logemin, logemax, lognmax;
+  double nb_abs_min, nq_abs_min, e_min;  // the constructor's derived constants
+  const double *__restrict__ p, *__restrict__ T, *__restrict__ mub, *__restrict__ muq,
+      *__restrict__ mus;
+  const int* __restrict__ status;
+};
+
 struct EosDev {
   int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table, 2 EoSChiral
   double conf_cnst;  // e = cnst T^4 for kind 0
@@ -71,6 +82,7 @@ struct EosDev {
   const double* __restrict__ mus;
   int iq0;
   double uq0;
+  HadronTab h;  // kind 4
 };
 
 __device__ __forceinline__ float c2p_guess(const EosDev& E, long long i) {
@@ -373,8 +385,12 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
 // con2prim iteration next to the table lookup, the chiral lookup made those
 // kernels spill more (face kernels 25 % slower on the table kind).
 // EK_TABLE_SL / EK_CHIRAL_SL: the same classes with the table-slope root
-// find (EosDev::slope = 1); EK_TABLE3: EoS3f (kind 3).
-enum { EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4, EK_TABLE3 = 5 };
+// find (EosDev::slope = 1); EK_TABLE3: EoS3f (kind 3); EK_HADRON:
+// EoSHadron (kind 4, the surface's).
+enum {
+  EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4, EK_TABLE3 = 5,
+  EK_HADRON = 6
+};
 __host__ __device__ constexpr bool ek_chiral(int ek) { return ek == EK_CHIRAL || ek == EK_CHIRAL_SL; }
 __host__ __device__ constexpr bool ek_slope(int ek) { return ek == EK_TABLE_SL || ek == EK_CHIRAL_SL; }
 
@@ -446,9 +462,90 @@ __device__ __forceinline__ void eos3f(const EosDev& E, double e, double nb, doub
   }
 }
 
+// EoSHadron's position of a charge on its table (the inverse log mapping
+// of src/eoHadron.cpp:97-112)
+__device__ __forceinline__ double hadron_x(double n, double n0, double lognmax, double dxn,
+                                           double n_abs_min) {
+  if (n != 0.0) {
+    const double zn = log(fabs(n) / n0);
+    if (zn >= -lognmax + 2.0 * dxn) return n / fabs(n) * 0.5 * (zn + lognmax);
+    return n / n_abs_min * dxn;
+  }
+  return 0.;
+}
+
+// EoSHadron::eos / ::p, src/eoHadron.cpp:81-208, at nq = 0 (its log is the
+// device's, which may differ from the C library's in the last bit)
+template <bool WANT_T>
+__device__ __forceinline__ void eos_hadron(const HadronTab& H, double e, double nb, double& T,
+                                           double& mub, double& muq, double& mus, double& p) {
+  const int ne = H.ne, nnb = H.nnb, nnq = H.nnq;
+  auto ix3 = [&](int ie, int inb, int inq) {
+    return (long long)inq + (long long)nnq * inb + (long long)nnq * nnb * ie;
+  };
+  T = mub = muq = mus = p = 0.;
+  if (e <= 0.) return;
+  if (e < H.e_min) {
+    p = e / H.e_min * __ldg(H.p + ix3(0, nnb / 2, nnq / 2));
+    if (WANT_T) T = e / H.e_min * __ldg(H.T + ix3(0, nnb / 2, nnq / 2));
+    return;
+  }
+  const double xe = log(e / H.e0);
+  const double dxe = (H.logemax - H.logemin) / (ne - 1);
+  const double dxnb = (2.0 * H.lognmax) / (nnb - 1);
+  const double dxnq = (2.0 * H.lognmax) / (nnq - 1);
+  const double xnb = hadron_x(nb, H.n0, H.lognmax, dxnb, H.nb_abs_min);
+  const double xnq = 0.;  // nq = 0
+  int ie = (int)((xe - H.logemin) / dxe);
+  int inb = (int)((xnb + H.lognmax) / dxnb);
+  int inq = (int)((xnq + H.lognmax) / dxnq);
+  if (ie < 0) ie = 0;
+  if (inb < 0) inb = 0;
+  if (inq < 0) inq = 0;
+  if (ie > ne - 2) ie = ne - 2;
+  if (inb > nnb - 2) inb = nnb - 2;
+  if (inq > nnq - 2) inq = nnq - 2;
+  const double em = xe - H.logemin - ie * dxe;
+  const double nbm = xnb + H.lognmax - inb * dxnb;
+  const double nqm = xnq + H.lognmax - inq * dxnq;
+  if (__ldg(H.status + ix3(ie, inb, inq)) == 1) return;
+  const double we[2] = {1. - em / dxe, em / dxe};
+  const double wnb[2] = {1. - nbm / dxnb, nbm / dxnb};
+  const double wnq[2] = {1. - nqm / dxnq, nqm / dxnq};
+  double sp = 0., sT = 0., sb = 0., sq = 0., ss = 0.;
+#pragma unroll
+  for (int je = 0; je < 2; je++)
+#pragma unroll
+    for (int jnb = 0; jnb < 2; jnb++)
+#pragma unroll
+      for (int jnq = 0; jnq < 2; jnq++) {
+        const long long k = ix3(ie + je, inb + jnb, inq + jnq);
+        sp += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.p + k);
+        if (WANT_T) {
+          sT += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.T + k);
+          sb += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.mub + k);
+          sq += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.muq + k);
+          ss += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.mus + k);
+        }
+      }
+  if (sp < 0.0) sp = 0.0;
+  p = sp;
+  if (WANT_T) {
+    T = sT;
+    mub = sb;
+    muq = sq;
+    mus = ss;
+  }
+}
+
 template <int EK = EK_ANY>
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
   double T, mub, mus, p;
+  if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
+    double muq;
+    eos_hadron<false>(E.h, e, nb, T, mub, muq, mus, p);
+    return p;
+  }
   if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
     double muq;
     eos3f<false>(E, e, nb, T, mub, muq, mus, p);
@@ -468,7 +565,10 @@ template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
                                          double& mub, double& mus, double& p) {
   mus = 0.;
-  if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
+  if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
+    double muq;
+    eos_hadron<true>(E.h, e, nb, T, mub, muq, mus, p);
+  } else if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
     double muq;
     eos3f<true>(E, e, nb, T, mub, muq, mus, p);
   } else if (ek_chiral(EK) || (EK == EK_ANY && E.kind == 2)) {
@@ -493,6 +593,10 @@ __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
 template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval_q(const EosDev& E, double e, double nb, double& T,
                                            double& mub, double& muq, double& mus, double& p) {
+  if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
+    eos_hadron<true>(E.h, e, nb, T, mub, muq, mus, p);
+    return;
+  }
   if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
     eos3f<true>(E, e, nb, T, mub, muq, mus, p);
     return;

@@ -129,6 +129,12 @@ class EosTable:
     muq: Optional[np.ndarray] = None
     mus: Optional[np.ndarray] = None
     header3: tuple = (0.0, 0.0, 0.0, 0.0, 0.0)
+    # kind 4 (EoSHadron): (ne, nnb, nnq, e0, n0, logemin, logemax, lognmax),
+    # the file's e, nb, nq value of every row, and the status table; p, T,
+    # mub, muq, mus at [inq + nnq*inb + nnq*nnb*ie]
+    hadron: Optional[tuple] = None
+    hrows: Optional[np.ndarray] = None
+    status: Optional[np.ndarray] = None
 
     def write_chiral(self, directory: str) -> None:
         """directory/eos/chiralsmall.dat and chiraleos.dat, the files
@@ -183,6 +189,21 @@ class EosTable:
             cols = np.stack([self.p[order], self.T[order], self.mub[order], self.muq[order],
                              self.mus[order]], 1)
             f.write("\n".join(" ".join(repr(float(v)) for v in row) for row in cols) + "\n")
+
+    def write_hadron(self, path: str) -> None:
+        """Write the table in the reference's EoSHadron text format: the
+        header ``ne nnb nnq e0 n0 logemin logemax lognmax``, then ``e nb nq p T
+        mub muq mus status`` rows with ie, inb, inq nested outer to inner
+        (src/eoHadron.cpp:13-40); 17 significant digits."""
+        assert self.kind == 4
+        ne, nnb, nnq, e0, n0, lo, hi, ln = self.hadron
+        with open(path, "w") as f:
+            f.write("%d %d %d %r %r %r %r %r\n" % (ne, nnb, nnq, e0, n0, lo, hi, ln))
+            for k in range(ne * nnb * nnq):
+                f.write("%r %r %r %r %r %r %r %r %d\n" % (
+                    float(self.hrows[k, 0]), float(self.hrows[k, 1]), float(self.hrows[k, 2]),
+                    float(self.p[k]), float(self.T[k]), float(self.mub[k]), float(self.muq[k]),
+                    float(self.mus[k]), int(self.status[k])))
 
     @staticmethod
     def read_eos1f(path: str) -> "EosTable":
@@ -265,6 +286,49 @@ def chiral_eos() -> EosTable:
     mu_q * (3 / 1000), mu_S / 1000, p * 0.146, grid ends * 0.146 and * 0.15),
     so that the files (write_chiral) and these arrays hold the same doubles."""
     return EosTable(kind=2, aux=tuple(t[2] for t in _chiral_tables()))
+
+
+def hadron_eos_table(ne: int = 101, nnb: int = 41, nnq: int = 21, e0: float = 1.0,
+                     n0: float = 0.15, logemin: float = -6.9, logemax: float = 2.3,
+                     lognmax: float = 2.5) -> EosTable:
+    """A synthetic hadronic EoS in the reference's EoSHadron format (the
+    freeze-out EoS the reference's driver loads by default): e on a log
+    grid e0 exp(x), x uniform on [logemin, logemax]; nb and nq on the
+    symmetric log mapping of src/eoHadron.cpp:91-112 (|n| = n0 exp(2|x| -
+    lognmax) beyond the two innermost cells, linear inside), x uniform on
+    [-lognmax, lognmax]; a resonance-gas-like p = 0.15 e + 0.4 nb^2, T =
+    0.16 (e / 0.5)^0.2 - 0.01 nb^2, mu_B = 0.8 tanh(nb / 0.3), mu_Q = 0.1 nq,
+    mu_S = 0.2 mu_B; the status is 1 (invalid) where |nb| > 1.5 fm^-3 and e
+    < 0.02 GeV/fm^3."""
+    dxe = (logemax - logemin) / (ne - 1)
+    xe = logemin + dxe * np.arange(ne)
+    e = e0 * np.exp(xe)
+
+    def charge(nn):
+        dx = (2.0 * lognmax) / (nn - 1)
+        x = -lognmax + dx * np.arange(nn)
+        amin = n0 * math.exp(2.0 * dx - lognmax)
+        n = np.where(np.abs(x) >= dx, np.sign(x) * n0 * np.exp(2 * np.abs(x) - lognmax),
+                     x / dx * amin)
+        return n
+
+    nb = charge(nnb)
+    nq = charge(nnq)
+    E = e[:, None, None]
+    B = nb[None, :, None]
+    Qc = nq[None, None, :]
+    shape = (ne, nnb, nnq)
+    p = np.broadcast_to(0.15 * E + 0.4 * B * B + 0 * Qc, shape)
+    T = np.broadcast_to(0.16 * (E / 0.5) ** 0.2 - 0.01 * B * B + 0 * Qc, shape)
+    mub = np.broadcast_to(0.8 * np.tanh(B / 0.3) + 0 * E + 0 * Qc, shape)
+    muq = np.broadcast_to(0.1 * Qc + 0 * E + 0 * B, shape)
+    mus = 0.2 * mub
+    status = np.broadcast_to(((np.abs(B) > 1.5) & (E < 0.02)) + 0 * Qc, shape).astype(np.int32)
+    rows = np.stack(np.broadcast_arrays(E, B, Qc), -1).reshape(-1, 3)
+    flat = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)  # noqa: E731
+    return EosTable(kind=4, p=flat(p), T=flat(T), mub=flat(mub), muq=flat(muq), mus=flat(mus),
+                    hadron=(ne, nnb, nnq, e0, n0, logemin, logemax, lognmax), hrows=rows,
+                    status=np.ascontiguousarray(status.reshape(-1)))
 
 
 def eos3f_table(ne: int = 120, emin: float = 1e-4, emax: float = 1e3) -> EosTable:
