@@ -260,6 +260,102 @@ class EoS3f : public EoS {
   }
 };
 
+// EoSHadron (src/eoHadron.cpp): the hadronic EoS the reference driver gives
+// the freeze-out surface (eosTypeHadron 0, src/main.cpp:305-307).  Reads the
+// reference's file (header ne nnb nnq e0 n0 logemin logemax lognmax, then
+// e nb nq p T mub muq mus status rows, inq fastest) and checks its ranges as
+// the constructor does (an exception in place of exit).  As a Fluid's eosH
+// it becomes the device's surface EoS (vh_set_surface_eos).
+class EoSHadron : public EoS {
+  int ne_ = 0, nnb_ = 0, nnq_ = 0;
+  double e0_ = 0, n0_ = 0, logemin_ = 0, logemax_ = 0, lognmax_ = 0;
+  double nb_abs_min_ = 0, nq_abs_min_ = 0, e_min_ = 0;
+  std::vector<double> p_, T_, mub_, muq_, mus_;
+  std::vector<int> status_;
+  size_t ix3(int ie, int inb, int inq) const {
+    return inq + (size_t)nnq_ * inb + (size_t)nnq_ * nnb_ * ie;
+  }
+  // the position of a charge on the table (src/eoHadron.cpp:97-112)
+  static double xpos(double n, double n0, double lognmax, double dxn, double n_abs_min) {
+    if (n == 0.0) return 0.;
+    const double zn = std::log(std::fabs(n) / n0);
+    if (zn >= -lognmax + 2.0 * dxn) return n / std::fabs(n) * 0.5 * (zn + lognmax);
+    return n / n_abs_min * dxn;
+  }
+
+ public:
+  explicit EoSHadron(const char* filename) {
+    std::ifstream fin(filename);
+    if (!fin) throw Error(VH_ERR_ARG, std::string("EoSHadron: I/O error with ") + filename);
+    fin >> ne_ >> nnb_ >> nnq_ >> e0_ >> n0_ >> logemin_ >> logemax_ >> lognmax_;
+    if (!fin || ne_ < 2 || nnb_ < 2 || nnq_ < 2) throw Error(VH_ERR_ARG, "EoSHadron: bad header");
+    const size_t n = (size_t)ne_ * nnb_ * nnq_;
+    for (auto* t : {&p_, &T_, &mub_, &muq_, &mus_}) t->resize(n);
+    status_.resize(n);
+    std::vector<double> e(ne_), nb(nnb_), nq(nnq_);
+    for (int ie = 0; ie < ne_; ie++)
+      for (int inb = 0; inb < nnb_; inb++)
+        for (int inq = 0; inq < nnq_; inq++) {
+          const size_t k = ix3(ie, inb, inq);
+          fin >> e[ie] >> nb[inb] >> nq[inq] >> p_[k] >> T_[k] >> mub_[k] >> muq_[k] >> mus_[k] >>
+              status_[k];
+        }
+    if (!fin) throw Error(VH_ERR_ARG, "EoSHadron: truncated table");
+    const double dxnb = (2.0 * lognmax_) / (nnb_ - 1), dxnq = (2.0 * lognmax_) / (nnq_ - 1);
+    nb_abs_min_ = n0_ * std::exp(2.0 * dxnb - lognmax_);
+    nq_abs_min_ = n0_ * std::exp(2.0 * dxnq - lognmax_);
+    e_min_ = e0_ * std::exp(logemin_);
+    if (std::fabs((e0_ * std::exp(logemin_) - e[0]) / e[0]) > 1e-5 ||
+        std::fabs((e0_ * std::exp(logemax_) - e[ne_ - 1]) / e[ne_ - 1]) > 1e-5 ||
+        std::fabs(n0_ * std::exp(lognmax_) - nb[nnb_ - 1]) > 1e-4)
+      throw Error(VH_ERR_ARG, "EoSHadron: wrong eps or nb range");
+  }
+  void eos(double e, double nb, double nq, double, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    T = mub = muq = mus = p = 0.;
+    if (e <= 0.) return;
+    if (e < e_min_) {
+      p = e / e_min_ * p_[ix3(0, nnb_ / 2, nnq_ / 2)];
+      T = e / e_min_ * T_[ix3(0, nnb_ / 2, nnq_ / 2)];
+      return;
+    }
+    const double xe = std::log(e / e0_);
+    const double dxe = (logemax_ - logemin_) / (ne_ - 1);
+    const double dxnb = (2.0 * lognmax_) / (nnb_ - 1), dxnq = (2.0 * lognmax_) / (nnq_ - 1);
+    const double xnb = xpos(nb, n0_, lognmax_, dxnb, nb_abs_min_);
+    const double xnq = xpos(nq, n0_, lognmax_, dxnq, nq_abs_min_);
+    int ie = (int)((xe - logemin_) / dxe), inb = (int)((xnb + lognmax_) / dxnb),
+        inq = (int)((xnq + lognmax_) / dxnq);
+    ie = std::min(std::max(ie, 0), ne_ - 2);
+    inb = std::min(std::max(inb, 0), nnb_ - 2);
+    inq = std::min(std::max(inq, 0), nnq_ - 2);
+    const double em = xe - logemin_ - ie * dxe, nbm = xnb + lognmax_ - inb * dxnb,
+                 nqm = xnq + lognmax_ - inq * dxnq;
+    if (status_[ix3(ie, inb, inq)] == 1) return;
+    const double we[2] = {1. - em / dxe, em / dxe}, wnb[2] = {1. - nbm / dxnb, nbm / dxnb},
+                 wnq[2] = {1. - nqm / dxnq, nqm / dxnq};
+    for (int je = 0; je < 2; je++)
+      for (int jnb = 0; jnb < 2; jnb++)
+        for (int jnq = 0; jnq < 2; jnq++) {
+          const size_t k = ix3(ie + je, inb + jnb, inq + jnq);
+          p += we[je] * wnb[jnb] * wnq[jnq] * p_[k];
+          T += we[je] * wnb[jnb] * wnq[jnq] * T_[k];
+          mub += we[je] * wnb[jnb] * wnq[jnq] * mub_[k];
+          muq += we[je] * wnb[jnb] * wnq[jnq] * muq_[k];
+          mus += we[je] * wnb[jnb] * wnq[jnq] * mus_[k];
+        }
+    if (p < 0.0) p = 0.0;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_HADRON;
+    d.hadron = vh_eos::vh_eos_hadron{ne_,        nnb_,        nnq_,       e0_,        n0_,
+                                     logemin_,   logemax_,    lognmax_,   p_.data(),  T_.data(),
+                                     mub_.data(), muq_.data(), mus_.data(), status_.data()};
+    return d;
+  }
+};
+
 // EoSChiral (src/eoChiral.cpp): the reference's default EoS (eosType 1).
 // Reads dir/eos/chiraleos.dat (2001 x 401) and dir/eos/chiralsmall.dat
 // (201 x 201) in the EoSaux format (8 columns, nb outer, e inner) with its
@@ -392,6 +488,8 @@ class Fluid {
  public:
   std::vector<double> Q, Qh, Qprev, pi, piH, Pi, PiH, m, vcc;
 
+  EoS* eos() const { return eos_; }
+  EoS* eosH() const { return eosH_; }
   Fluid(EoS* eos, EoS* eosH, TransportCoeff* tr, int nx, int ny, int nz, double minx,
         double maxx, double miny, double maxy, double minz, double maxz, double dt, double eCrit)
       : eos_(eos), eosH_(eosH), tr_(tr), nx_(nx), ny_(ny), nz_(nz), minx_(minx), maxx_(maxx),
@@ -422,7 +520,7 @@ class Fluid {
   double geteCrit() const { return ecrit_; }
   EoS* getEoS() const { return eos_; }
   long long ncells() const { return N_; }
-  vh_grid grid() const { return vh_grid{nx_, ny_, nz_, minx_, maxx_, miny_, maxy_, minz_, maxz_}; }
+  vh_grid grid() const { return vh_grid{nx_, ny_, nz_, minx_, maxx_, miny_, maxy_, minz_, maxz_, 0.}; }
   // Fluid::getCell clamping (src/fld.h:70-78)
   long long index(int ix, int iy, int iz) const {
     ix = std::min(std::max(ix, 0), nx_ - 1);
@@ -492,7 +590,7 @@ class Fluid {
     in.read(reinterpret_cast<char*>(b), sizeof b);
     if (!in || std::memcmp(tag, "VHBSNAP1", 8) != 0)
       throw Error(VH_ERR_ARG, std::string("not a grid snapshot: ") + path);
-    return SnapshotHeader{vh_grid{n[0], n[1], n[2], b[0], b[1], b[2], b[3], b[4], b[5]}, b[6],
+    return SnapshotHeader{vh_grid{n[0], n[1], n[2], b[0], b[1], b[2], b[3], b[4], b[5], 0.}, b[6],
                           b[7]};
   }
   void loadSnapshot(const char* path) {
@@ -547,6 +645,12 @@ class Hydro {
     const vh_trcoeff t = tr_->descriptor();
     check(vh_create(&g, &e, &t, t0_, dt0_, device_, &ctx_), nullptr);
     if (vorticity_) check(vh_enable_vorticity(ctx_, 1), ctx_);  // new cells: zero dbeta
+    // the Fluid's eosH is the EoS of outputSurface / outputCorona
+    // (src/fld.cpp:540-542, 885-887)
+    if (f_->eosH() && f_->eosH() != eos_) {
+      const vh_eos h = f_->eosH()->descriptor();
+      check(vh_set_surface_eos(ctx_, &h), ctx_);
+    }
   }
 
  public:
