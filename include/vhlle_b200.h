@@ -82,14 +82,16 @@ typedef struct vh_grid {
  *                         transformPV then does;
  *  kind VH_EOS_HADRON:    EoSHadron (src/eoHadron.cpp), the hadronic EoS the
  *                         reference driver gives the freeze-out surface
- *                         (eosTypeHadron 0): `hadron` below; for
- *                         vh_set_surface_eos only.
+ *                         (eosTypeHadron 0): `hadron` below;
+ *  kind VH_EOS_SMASH:     EoSSmash (src/eoSmash.cpp, eosTypeHadron 1):
+ *                         `smash` below; both for vh_set_surface_eos only.
  * Host arrays are copied at vh_create (vh_set_surface_eos). */
 #define VH_EOS_CONFORMAL 0
 #define VH_EOS_TABLE 1
 #define VH_EOS_CHIRAL 2
 #define VH_EOS_TABLE3 3
 #define VH_EOS_HADRON 4
+#define VH_EOS_SMASH 5
 /* One EoSaux table (src/eoChiral.cpp:33-97) after its constructor's unit
  * conversions: the e and nb grids are uniform from emin to emax (GeV/fm^3)
  * and nmin to nmax (fm^-3) with ne, nn >= 2 points; p (GeV/fm^3), T, muB,
@@ -115,6 +117,15 @@ typedef struct vh_eos {
     const double *p, *T, *mub, *muq, *mus;
     const int *status;
   } hadron;
+  /* VH_EOS_SMASH only: ne x nnb x nnq points on uniform grids from emin to
+   * emax, nbmin to nbmax, nqmin to nqmax (the first and last rows' values,
+   * src/eoSmash.cpp:45-51); p, T, muB, muQ, muS at [inq + nnq*inb +
+   * nnq*nnb*ie] */
+  struct vh_eos_smash {
+    int ne, nnb, nnq;
+    double emin, emax, nbmin, nbmax, nqmin, nqmax;
+    const double *p, *T, *mub, *muq, *mus;
+  } smash;
 } vh_eos;
 
 /* TransportCoeff public constants (src/trancoeff.h:8-11, ctor :14-20). */
@@ -150,7 +161,7 @@ vh_status vh_destroy(vh_ctx *ctx);
  * (src/fld.cpp:540-542, 870-872, 885-887, 1085-1087); the reference driver
  * passes EoSHadron or EoSSmash there (src/main.cpp:305-311).  eos = NULL
  * goes back to the hydro EoS (the default).  Any kind but the conformal gas;
- * VH_EOS_HADRON only here. */
+ * VH_EOS_HADRON and VH_EOS_SMASH only here. */
 vh_status vh_set_surface_eos(vh_ctx *ctx, const vh_eos *eos);
 
 /* Uses `stream` (a cudaStream_t, NULL = legacy default) for all later work. */

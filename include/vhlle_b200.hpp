@@ -451,7 +451,7 @@ class TransportCoeff {
       etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta, zetaSSigmaMinus, zetaSSigmaPlus;
   EoS* eos;
   const int etaSparam, zetaSparam;
-  // zetaSparam 5 (this build's Gaussian bump in T; not in the reference)
+  // zetaSparam 5 (a Gaussian bump in T; not in the reference)
   double zetaSPeakT = 0.175, zetaSWidthT = 0.02;
   TransportCoeff(double _etaS0, double _zetaS0, double _ah, double _al, double _aRho, double _T0,
                  double _etaSMin, double _etaSEpsilonMin, double _etaSShiftMuB,
@@ -791,7 +791,7 @@ struct Params {
          Rgt = 1.0, Rgz = 1.0, impactPar = 0., s0ScaleFactor = 0.;
   std::string collSystem, outputDir = "data", isInputFile, vtk_values;
   int icModel = 1, glauberVariable = 1, smoothingType = 0;
-  // extension of this build: an EoS1f table for the hydro EoS (the
+  // not a reference parameter: an EoS1f table for the hydro EoS (the
   // reference selects compiled-in EoS classes with eosType instead)
   std::string eos1fFile;
 

@@ -11,3 +11,4 @@
 
 extern "C" double or_exp_cr(double x) { return vh::crm::exp_cr(x); }
 extern "C" double or_root4_cr(double x) { return vh::crm::root4_cr(x); }
+extern "C" double or_log_cr(double x) { return vh::crm::log_cr(x); }

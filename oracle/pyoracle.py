@@ -52,7 +52,9 @@ class _Eos(ctypes.Structure):
                 ("hne", ctypes.c_int), ("hnnb", ctypes.c_int), ("hnnq", ctypes.c_int),
                 ("he0", ctypes.c_double), ("hn0", ctypes.c_double), ("logemin", ctypes.c_double),
                 ("logemax", ctypes.c_double), ("lognmax", ctypes.c_double),
-                ("status", ctypes.POINTER(ctypes.c_int))]
+                ("status", ctypes.POINTER(ctypes.c_int)),
+                ("semin", ctypes.c_double), ("semax", ctypes.c_double), ("snbmin", ctypes.c_double),
+                ("snbmax", ctypes.c_double), ("snqmin", ctypes.c_double), ("snqmax", ctypes.c_double)]
 
 
 class _Trc(ctypes.Structure):
@@ -141,7 +143,8 @@ def ref_lib():
         lib.ref_eos_full.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_surface_eos_full.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         lib.ref_set_surface_eos.restype = ctypes.c_int
-        lib.ref_set_surface_eos.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p]
+        lib.ref_set_surface_eos.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p,
+                                            ctypes.c_int, ctypes.c_int, ctypes.c_int]
         lib.ref_output_corona.restype = ctypes.c_int
         lib.ref_output_corona.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int,
                                           ctypes.c_char_p, ctypes.c_int]
@@ -254,6 +257,15 @@ class _EosHolder:
             self.s.nn = len(arrs[1])
             (self.s.egrid, self.s.ngrid, self.s.p, self.s.T, self.s.mub, self.s.muq,
              self.s.mus) = (_ptr(a) for a in arrs)
+        if eos.kind == 5:
+            arrs = [np.ascontiguousarray(a, dtype=np.float64)
+                    for a in (eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
+            self.keep = arrs
+            (self.s.hne, self.s.hnnb, self.s.hnnq), (eg, bg, qg) = eos.smash
+            self.s.semin, self.s.semax = float(eg[0]), float(eg[-1])
+            self.s.snbmin, self.s.snbmax = float(bg[0]), float(bg[-1])
+            self.s.snqmin, self.s.snqmax = float(qg[0]), float(qg[-1])
+            self.s.p, self.s.T, self.s.mub, self.s.muq, self.s.mus = (_ptr(a) for a in arrs)
         if eos.kind == 4:
             arrs = [np.ascontiguousarray(a, dtype=np.float64)
                     for a in (eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
@@ -525,8 +537,13 @@ class RefRun:
             if self._tmp is None:
                 self._tmp = tempfile.TemporaryDirectory()
             hfile = os.path.join(self._tmp.name, "eos_hadron.dat")
-            surface_eos.write_hadron(hfile)
-            if self.lib.ref_set_surface_eos(self.h, surface_eos.kind, hfile.encode()) != 0:
+            dims = (0, 0, 0)
+            if surface_eos.kind == 5:
+                surface_eos.write_smash(hfile)
+                dims = surface_eos.smash[0]
+            else:
+                surface_eos.write_hadron(hfile)
+            if self.lib.ref_set_surface_eos(self.h, surface_eos.kind, hfile.encode(), *dims) != 0:
                 raise ValueError("the reference has no surface EoS of kind %d" % surface_eos.kind)
         st = initial_state(setup)
         self.lib.ref_set_state(self.h, _ptr(st["Q"]), _ptr(st["pi"]), _ptr(st["piH"]),

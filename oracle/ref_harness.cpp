@@ -33,6 +33,7 @@
 #include "eo3.h"
 #include "eoChiral.h"
 #include "eoHadron.h"
+#include "eoSmash.h"
 #include "fld.h"
 #include "hdo.h"
 #include "inc.h"
@@ -158,14 +159,17 @@ void ref_surface_eos_full(void *p, const double *in, int n, double *out) {
 // Fluid's eosH, the EoS of outputSurface and outputCorona (src/fld.cpp:
 // 540-542, 870-872: SWAP_EOS), from a table file: kind 4 EoSHadron
 // (src/eoHadron.cpp).  The Fluid and Hydro are made again with it, so call
-// this before the state is set.  Returns 0, or -1 for an unknown kind.
-int ref_set_surface_eos(void *p, int kind, const char *file) {
+// this before the state is set; kind 5 EoSSmash (src/eoSmash.cpp) takes its
+// table's ne, nnb, nnq as the driver passes them (src/main.cpp:308).
+// Returns 0, or -1 for an unknown kind.
+int ref_set_surface_eos(void *p, int kind, const char *file, int ne, int nnb, int nnq) {
   RefRun *r = static_cast<RefRun *>(p);
   std::streambuf *old = std::cout.rdbuf();
   std::ostringstream quiet;
   std::cout.rdbuf(quiet.rdbuf());
   EoS *eh = nullptr;
   if (kind == 4) eh = new EoSHadron(const_cast<char *>(file));
+  if (kind == 5) eh = new EoSSmash(const_cast<char *>(file), ne, nnb, nnq);
   std::cout.rdbuf(old);
   if (!eh) return -1;
   r->eosH = eh;

@@ -214,10 +214,10 @@ static void eos3f(const or_eos *E, double e, double nb, double nq, double ns,
 
 /* EoSHadron: the table position of a charge (the "inverse log mapping" of
  * src/eoHadron.cpp:97-112) */
-static double hadron_x(double n, double n0, double lognmax, double dxn,
-                       double n_abs_min) {
+static double hadron_x(int crmath, double n, double n0, double lognmax,
+                       double dxn, double n_abs_min) {
   if (n != 0.0) {
-    const double zn = log(fabs(n) / n0);
+    const double zn = crmath ? or_log_cr(fabs(n) / n0) : log(fabs(n) / n0);
     if (zn >= -lognmax + 2.0 * dxn)
       return n / fabs(n) * 0.5 * (zn + lognmax);
     return n / n_abs_min * dxn;
@@ -248,12 +248,12 @@ static void eos_hadron(const or_eos *E, double e, double nb, double nq,
     *mub = *muq = *mus = 0.;
     return;
   }
-  const double xe = log(e / E->he0);
+  const double xe = E->crmath ? or_log_cr(e / E->he0) : log(e / E->he0);
   const double dxe = (E->logemax - E->logemin) / (ne - 1);
   const double dxnb = (2.0 * E->lognmax) / (nnb - 1);
   const double dxnq = (2.0 * E->lognmax) / (nnq - 1);
-  const double xnb = hadron_x(nb, E->hn0, E->lognmax, dxnb, nb_abs_min);
-  const double xnq = hadron_x(nq, E->hn0, E->lognmax, dxnq, nq_abs_min);
+  const double xnb = hadron_x(E->crmath, nb, E->hn0, E->lognmax, dxnb, nb_abs_min);
+  const double xnq = hadron_x(E->crmath, nq, E->hn0, E->lognmax, dxnq, nq_abs_min);
   int ie = (int)((xe - E->logemin) / dxe);
   int inb = (int)((xnb + E->lognmax) / dxnb);
   int inq = (int)((xnq + E->lognmax) / dxnq);
@@ -293,6 +293,60 @@ static void eos_hadron(const or_eos *E, double e, double nb, double nq,
   *mus = ss;
 }
 
+/* EoSSmash::eos / ::p, src/eoSmash.cpp:70-177 */
+static void eos_smash(const or_eos *E, double e, double nb, double nq,
+                      double *T, double *mub, double *muq, double *mus,
+                      double *p) {
+  const int ne = E->hne, nnb = E->hnnb, nnq = E->hnnq;
+#define IX3(ie, inb, inq) ((long)(inq) + (long)nnq * (inb) + (long)nnq * nnb * (ie))
+  if (e <= 0.) {
+    *T = *mub = *muq = *mus = *p = 0.;
+    return;
+  }
+  if (e < E->semin) {
+    *p = e / E->semin * E->p[IX3(0, nnb / 2, nnq / 2)];
+    *T = e / E->semin * E->T[IX3(0, nnb / 2, nnq / 2)];
+    *mub = *muq = *mus = 0.;
+    return;
+  }
+  const double de = (E->semax - E->semin) / (ne - 1);
+  const double dnb = (E->snbmax - E->snbmin) / (nnb - 1);
+  const double dnq = (E->snqmax - E->snqmin) / (nnq - 1);
+  int ie = (int)((e - E->semin) / de);
+  int inb = (int)((nb - E->snbmin) / dnb);
+  int inq = (int)((nq - E->snqmin) / dnq);
+  if (ie < 0) ie = 0;
+  if (inb < 0) inb = 0;
+  if (inq < 0) inq = 0;
+  if (ie > ne - 2) ie = ne - 2;
+  if (inb > nnb - 2) inb = nnb - 2;
+  if (inq > nnq - 2) inq = nnq - 2;
+  const double em = e - E->semin - ie * de;
+  const double nbm = nb - E->snbmin - inb * dnb;
+  const double nqm = nq - E->snqmin - inq * dnq;
+  const double we[2] = {1. - em / de, em / de};
+  const double wnb[2] = {1. - nbm / dnb, nbm / dnb};
+  const double wnq[2] = {1. - nqm / dnq, nqm / dnq};
+  double sT = 0., sb = 0., sq = 0., ss = 0., sp = 0.;
+  for (int je = 0; je < 2; je++)
+    for (int jnb = 0; jnb < 2; jnb++)
+      for (int jnq = 0; jnq < 2; jnq++) {
+        const long k = IX3(ie + je, inb + jnb, inq + jnq);
+        sp += we[je] * wnb[jnb] * wnq[jnq] * E->p[k];
+        sT += we[je] * wnb[jnb] * wnq[jnq] * E->T[k];
+        sb += we[je] * wnb[jnb] * wnq[jnq] * E->mub[k];
+        sq += we[je] * wnb[jnb] * wnq[jnq] * E->muq[k];
+        ss += we[je] * wnb[jnb] * wnq[jnq] * E->mus[k];
+      }
+#undef IX3
+  if (sp < 0.0) sp = 0.0;
+  *p = sp;
+  *T = sT;
+  *mub = sb;
+  *muq = sq;
+  *mus = ss;
+}
+
 /* EoS::eos() with muq; muq = 0 but for kind 3, mus = 0 but for kinds 2, 3 */
 static void eos_eval5(const or_eos *E, double e, double nb, double *T,
                       double *mub, double *muq, double *mus, double *p) {
@@ -303,6 +357,10 @@ static void eos_eval5(const or_eos *E, double e, double nb, double *T,
   }
   if (E->kind == 4) {
     eos_hadron(E, e, nb, 0., T, mub, muq, mus, p);
+    return;
+  }
+  if (E->kind == 5) {
+    eos_smash(E, e, nb, 0., T, mub, muq, mus, p);
     return;
   }
   *mus = 0.;
@@ -341,6 +399,11 @@ static double eos_p(const or_eos *E, double e, double nb) {
   if (E->kind == 4) {
     double muq;
     eos_hadron(E, e, nb, 0., &T, &mub, &muq, &mus, &p);
+    return p;
+  }
+  if (E->kind == 5) {
+    double muq;
+    eos_smash(E, e, nb, 0., &T, &mub, &muq, &mus, &p);
     return p;
   }
   if (E->kind == 2) {
@@ -489,7 +552,7 @@ static double tr_zetaS(const or_trc *t, double e, double T, double s,
         e < t->zetaSPeakEpsilon ? t->zetaSSigmaMinus : t->zetaSSigmaPlus;
     return ((e + P) / (s * T)) * t->zetaS0 * TR_EXP(d * d / 2.0 * (sig * sig));
   } else if (t->zetaSparam == 5) {
-    /* a Gaussian bump in T: this build's addition, not in the reference */
+    /* a Gaussian bump in T: not in the reference */
     const double x = T - t->zetaSPeakT;
     return t->zetaS0 * TR_EXP(-x * x / (2. * t->zetaSWidthT * t->zetaSWidthT));
   }
@@ -1628,6 +1691,8 @@ void or_eos_full(const or_eos *E, const double *in, int n, double *out) {
       eos3f(E, a[0], a[1], a[2], a[3], &o[1], &o[2], &o[3], &o[4], &o[0]);
     } else if (E->kind == 4) {
       eos_hadron(E, a[0], a[1], a[2], &o[1], &o[2], &o[3], &o[4], &o[0]);
+    } else if (E->kind == 5) {
+      eos_smash(E, a[0], a[1], a[2], &o[1], &o[2], &o[3], &o[4], &o[0]);
     } else {
       eos_eval5(E, a[0], a[1], &o[1], &o[2], &o[3], &o[4], &o[0]);
     }

@@ -34,7 +34,7 @@ typedef struct or_grid {
 /* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)
  * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb]
  * kind 2: EoSChiral (aux below); kind 3: EoS3f (muq, mus below);
- * kind 4: EoSHadron (the hadronic EoS of the freeze-out surface) */
+ * kind 4: EoSHadron, kind 5: EoSSmash (hadronic EoS of the freeze-out surface) */
 /* One EoSaux table of EoSChiral (src/eoChiral.cpp:33-97), converted to
  * GeV/fm^3, fm^-3 and GeV as its constructor does: uniform grids from emin
  * to emax and nmin to nmax, p/T/mub/mus[in * ne + ie]. */
@@ -54,7 +54,8 @@ typedef struct or_eos {
    * learned-guess path is checked against. */
   double tol;
   or_aux aux[2]; /* kind 2: chiralsmall, chiraleos */
-  int crmath; /* as or_trc.crmath, for EoSChiral's power law */
+  int crmath; /* as or_trc.crmath, for EoSChiral's power law and
+               * EoSHadron's logarithms (or_log_cr) */
   /* kind 3 (EoS3f, src/eo3.cpp): egrid[ne], ngrid[nn] (one grid for nb, nq,
    * ns) and p, T, mub above plus muq, mus, all at
    * [ie + ne*ib + ne*nn*iq + ne*nn*nn*is] */
@@ -65,11 +66,16 @@ typedef struct or_eos {
   int hne, hnnb, hnnq;
   double he0, hn0, logemin, logemax, lognmax;
   const int *status;
+  /* kind 5 (EoSSmash, src/eoSmash.cpp): hne x hnnb x hnnq points on uniform
+   * grids from the first to the last row's e, nb, nq; p, T, mub, muq, mus as
+   * kind 4 */
+  double semin, semax, snbmin, snbmax, snqmin, snqmax;
 } or_eos;
 
 /* Correctly rounded exp(x) and x^(1/4) (oracle/crm_shim.cpp). */
 double or_exp_cr(double x);
 double or_root4_cr(double x);
+double or_log_cr(double x);
 
 /* TransportCoeff (src/trancoeff.h:6-45) public constants */
 typedef struct or_trc {
@@ -77,7 +83,7 @@ typedef struct or_trc {
       etaSShiftMuB, etaSScaleMuB, zetaSPeakEpsilon, zetaSScaleBeta,
       zetaSSigmaMinus, zetaSSigmaPlus;
   int etaSparam, zetaSparam;
-  /* zetaSparam 5, an addition of this build (no reference counterpart):
+  /* zetaSparam 5, with no reference counterpart:
    * zeta/s = zetaS0 exp(-(T - zetaSPeakT)^2 / (2 zetaSWidthT^2)) */
   double zetaSPeakT, zetaSWidthT;
   /* 0: exp and pow(x, 0.25) from the C library, as the reference computes

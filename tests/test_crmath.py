@@ -1,4 +1,4 @@
-"""The correctly rounded exp and x^(1/4) of vhlle_b200/csrc/vh_crmath.cuh,
+"""The correctly rounded exp, log and x^(1/4) of vhlle_b200/csrc/vh_crmath.cuh,
 and its divide-free division (Markstein),
 compiled for the host from the same header (IEEE operations and explicit
 fma only, no contraction, so the host build gives the device's bits):
@@ -55,7 +55,9 @@ int main() {
   }
   do {
     if (std::scanf("%la", &x) != 1) break;
-    const double y = f[0] == 'e' ? vh::crm::exp_cr(x) : vh::crm::root4_cr(x);
+    const double y = f[0] == 'e'   ? vh::crm::exp_cr(x)
+                     : f[0] == 'l' ? vh::crm::log_cr(x)
+                                   : vh::crm::root4_cr(x);
     std::printf("%a\n", y);
   } while (std::scanf("%1s", f) == 1);
   return 0;
@@ -115,6 +117,22 @@ def test_exp_is_correctly_rounded(crm):
     assert not bad, bad[:5]
     assert crm("e", [float("nan")])[0] != crm("e", [float("nan")])[0]  # NaN
     assert crm("e", [800.0, -800.0]) == [float("inf"), 0.0]
+
+
+def test_log_is_correctly_rounded(crm):
+    rng = np.random.default_rng(6)
+    xs = list(10 ** rng.uniform(-300, 300, 1500)) + list(10 ** rng.uniform(-3, 3, 2000)) + \
+        list(1 + rng.uniform(-1e-3, 1e-3, 500)) + list(1 + rng.uniform(-1e-12, 1e-12, 200)) + \
+        list(rng.uniform(0.70, 0.72, 200)) + list(rng.uniform(1.40, 1.43, 200)) + \
+        [1.0, 2.0, 0.5, 1.41421356, math.nextafter(1.41421356, 2), math.nextafter(1.0, 2),
+         math.nextafter(1.0, 0), 5e-324, 1e-310, 2.2250738585072014e-308,
+         1.7976931348623157e308, 10.0, 0.1, math.e]
+    ys = crm("l", xs)
+    bad = [(x, y) for x, y in zip(xs, ys) if x != 1.0 and
+           not correctly_rounded(y, decimal.Decimal(x).ln())]
+    assert not bad, bad[:5]
+    assert crm("l", [1.0, 0.0, float("inf")]) == [0.0, -float("inf"), float("inf")]
+    assert math.isnan(crm("l", [-1.0])[0]) and math.isnan(crm("l", [float("nan")])[0])
 
 
 def test_fourth_root_is_correctly_rounded(crm):

@@ -1,7 +1,8 @@
 """The freeze-out EoS on the device (vh_set_surface_eos: Fluid's eosH, which
 outputSurface and outputCorona swap in, src/fld.cpp:540-542, 885-887) set to
-EoSHadron (VH_EOS_HADRON, src/eoHadron.cpp) against the oracle, itself equal
-bit for bit to the reference's classes (tests/test_oracle_hadron_eos.py):
+EoSHadron (VH_EOS_HADRON, src/eoHadron.cpp) or EoSSmash (VH_EOS_SMASH,
+src/eoSmash.cpp) against the oracle, itself equal bit for bit to the
+reference's classes (tests/test_oracle_hadron_eos.py):
 the corona and the surface records within 1e-12 relative (EoSHadron takes
 logarithms, which the device may round differently from the C library in
 the last bit), the totals within 1e-10; the hydro evolution is untouched."""
@@ -20,8 +21,9 @@ def _close(a, b, rtol):
     return np.abs(a - b) <= rtol * np.maximum(np.abs(a), np.abs(b)) + 1e-300
 
 
-def test_gpu_hadron_surface_eos_equals_oracle():
-    h = W.hadron_eos_table()
+@pytest.mark.parametrize("name", ["hadron", "smash"])
+def test_gpu_surface_eos_equals_oracle(name):
+    h = {"hadron": W.hadron_eos_table, "smash": W.smash_eos_table}[name]()
     s = W.glauber3d_nb_setup(33, 33, 17, eos=W.nb_table(200, 20))
     o, d = P.OracleRun(s, surface_eos=h), capi.GpuHydro(s)
     d.set_surface_eos(h)
@@ -51,8 +53,9 @@ def test_gpu_hadron_surface_eos_equals_oracle():
     d.close()
 
 
-def test_gpu_hadron_eos_is_only_a_surface_eos():
-    h = W.hadron_eos_table()
+@pytest.mark.parametrize("name", ["hadron", "smash"])
+def test_gpu_hadron_eos_is_only_a_surface_eos(name):
+    h = {"hadron": W.hadron_eos_table, "smash": W.smash_eos_table}[name]()
     s = W.glauber3d_nb_setup(9, 9, 5, eos=h)
     with pytest.raises(capi.VhError):
         capi.GpuHydro(s)

@@ -1,12 +1,13 @@
 """The freeze-out EoS (Fluid's eosH: outputSurface, outputCorona and the
 printed totals swap it in, src/fld.cpp:540-542, 870-872, 885-887) set to
 EoSHadron (src/eoHadron.cpp, the reference driver's default hadronic EoS)
-in the oracle against the reference's own classes: the lookup at general
-nb, nq bit for bit (below its e range, in its log mapping's linear core,
-the cells its status table marks invalid, beyond its edges), and the
-surface records, the corona and the totals of an event whose hydro EoS is
-the (e, nb) table.  The table is synthetic (workloads.hadron_eos_table) in
-the reference's file format."""
+or EoSSmash (src/eoSmash.cpp, its eosTypeHadron 1) in the oracle against
+the reference's own classes: the lookup at general nb, nq bit for bit
+(below the e range, in EoSHadron's log mapping's linear core, the cells its
+status table marks invalid, beyond the edges), and the surface records,
+the corona and the totals of an event whose hydro EoS is the (e, nb)
+table.  The tables are synthetic (workloads.hadron_eos_table,
+smash_eos_table) in the reference's file formats."""
 import os
 import tempfile
 
@@ -19,8 +20,12 @@ from vhlle_b200 import workloads as W
 pytestmark = pytest.mark.skipif(not P.ref_available(), reason="compiled reference not present")
 
 
-def test_hadron_eos_lookup_equals_reference():
-    h = W.hadron_eos_table()
+TABLES = {"hadron": W.hadron_eos_table, "smash": W.smash_eos_table}
+
+
+@pytest.mark.parametrize("name", sorted(TABLES))
+def test_surface_eos_lookup_equals_reference(name):
+    h = TABLES[name]()
     rng = np.random.default_rng(9)
     n = 20000
     e = np.concatenate([10 ** rng.uniform(-4, 1.5, n - 300), rng.uniform(0, 1e-3, 100),
@@ -39,6 +44,7 @@ def test_hadron_eos_lookup_equals_reference():
     same = (got == ref) | (np.isnan(got) & np.isnan(ref))
     assert same.all(), np.argwhere(~same)[:5]
     assert (got[:, 0] == 0).sum() > 100 and np.abs(got[:, 3]).max() > 0.01
+    assert (got[:, 0] > 0).sum() > n // 2
 
 
 def _ref_surface_eos_full(r, pts):
@@ -48,8 +54,9 @@ def _ref_surface_eos_full(r, pts):
     return r.surface_eos_full(pts)
 
 
-def test_hadron_surface_eos_event_equals_reference():
-    h = W.hadron_eos_table()
+@pytest.mark.parametrize("name", sorted(TABLES))
+def test_surface_eos_event_equals_reference(name):
+    h = TABLES[name]()
     s = W.glauber3d_nb_setup(21, 21, 11, eos=W.nb_table(200, 20))
     o, r = P.OracleRun(s, surface_eos=h), P.RefRun(s, surface_eos=h)
     with tempfile.TemporaryDirectory() as d:

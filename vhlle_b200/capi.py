@@ -232,11 +232,19 @@ class VhEosHadron(ctypes.Structure):
                 ("status", ctypes.POINTER(ctypes.c_int))]
 
 
+class VhEosSmash(ctypes.Structure):
+    _fields_ = [("ne", ctypes.c_int), ("nnb", ctypes.c_int), ("nnq", ctypes.c_int),
+                ("emin", ctypes.c_double), ("emax", ctypes.c_double), ("nbmin", ctypes.c_double),
+                ("nbmax", ctypes.c_double), ("nqmin", ctypes.c_double), ("nqmax", ctypes.c_double),
+                ("p", _dp), ("T", _dp), ("mub", _dp), ("muq", _dp), ("mus", _dp)]
+
+
 class VhEos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
-                ("aux", VhEosAux * 2), ("muq", _dp), ("mus", _dp), ("hadron", VhEosHadron)]
+                ("aux", VhEosAux * 2), ("muq", _dp), ("mus", _dp), ("hadron", VhEosHadron),
+                ("smash", VhEosSmash)]
 
 
 class VhGlauberIc(ctypes.Structure):
@@ -390,6 +398,14 @@ def make_eos(eos):
                 for a in (eos.egrid, eos.ngrid, eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
         d.ne, d.nn = len(keep[0]), len(keep[1])
         d.egrid, d.ngrid, d.p, d.T, d.mub, d.muq, d.mus = (_ptr(a) for a in keep)
+    if eos.kind == 5:
+        keep = [np.ascontiguousarray(a, dtype=np.float64)
+                for a in (eos.p, eos.T, eos.mub, eos.muq, eos.mus)]
+        h = d.smash
+        (h.ne, h.nnb, h.nnq), (eg, bg, qg) = eos.smash
+        h.emin, h.emax, h.nbmin, h.nbmax, h.nqmin, h.nqmax = (
+            float(eg[0]), float(eg[-1]), float(bg[0]), float(bg[-1]), float(qg[0]), float(qg[-1]))
+        h.p, h.T, h.mub, h.muq, h.mus = (_ptr(a) for a in keep)
     if eos.kind == 4:
         keep = [np.ascontiguousarray(a, dtype=np.float64)
                 for a in (eos.p, eos.T, eos.mub, eos.muq, eos.mus)]

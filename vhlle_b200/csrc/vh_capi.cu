@@ -191,6 +191,15 @@ const char* eos_problem(const vh_eos& e) {
       if (!e.egrid || !e.ngrid || !e.p || !e.T || !e.mub || !e.muq || !e.mus)
         return "EoS3f table needs all seven arrays";
       return nullptr;
+    case VH_EOS_SMASH: {
+      const vh_eos::vh_eos_smash& h = e.smash;
+      if (h.ne < 2 || h.nnb < 2 || h.nnq < 2 || (long long)h.ne * h.nnb * h.nnq > (1LL << 31))
+        return "EoSSmash table needs ne, nnb, nnq >= 2 and at most 2^31 points";
+      if (!h.p || !h.T || !h.mub || !h.muq || !h.mus) return "EoSSmash table needs all five arrays";
+      if (!(h.emin < h.emax) || !(h.nbmin < h.nbmax) || !(h.nqmin < h.nqmax))
+        return "EoSSmash table needs emin < emax, nbmin < nbmax, nqmin < nqmax";
+      return nullptr;
+    }
     case VH_EOS_HADRON: {
       const vh_eos::vh_eos_hadron& h = e.hadron;
       if (h.ne < 2 || h.nnb < 2 || h.nnq < 2 || (long long)h.ne * h.nnb * h.nnq > (1LL << 31))
@@ -360,6 +369,35 @@ static vh_status upload_eos(vh_ctx* c, const vh_eos* eos, vh::EosDev& E) {
                                    buf, buf + n, buf + 2 * n, buf + 3 * n};
     }
   }
+  if (eos->kind == VH_EOS_SMASH) {
+    const vh_eos::vh_eos_smash& h = eos->smash;
+    vh::SmashTab& H = E.sm;
+    H.ne = h.ne;
+    H.nnb = h.nnb;
+    H.nnq = h.nnq;
+    H.emin = h.emin;
+    H.emax = h.emax;
+    H.nbmin = h.nbmin;
+    H.nbmax = h.nbmax;
+    H.nqmin = h.nqmin;
+    H.nqmax = h.nqmax;
+    const size_t n = (size_t)h.ne * h.nnb * h.nnq;
+    double* buf = nullptr;
+    if ((st = dalloc(c, &buf, 5 * n)) != VH_OK) return st;
+    const double* src[5] = {h.p, h.T, h.mub, h.muq, h.mus};
+    e = cudaSuccess;
+    for (int q = 0; q < 5 && e == cudaSuccess; q++)
+      e = cudaMemcpy(buf + q * n, src[q], n * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      cuda_fail(c, e, "EoS upload");
+      return VH_ERR_CUDA;
+    }
+    H.p = buf;
+    H.T = buf + n;
+    H.mub = buf + 2 * n;
+    H.muq = buf + 3 * n;
+    H.mus = buf + 4 * n;
+  }
   if (eos->kind == VH_EOS_HADRON) {
     const vh_eos::vh_eos_hadron& h = eos->hadron;
     vh::HadronTab& H = E.h;
@@ -426,8 +464,9 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   if (!(tau0 > 0.)) return fail(nullptr, VH_ERR_ARG, "vh_create: tau0 must be positive");
   if (const char* why = vh::eos_problem(*eos))
     return fail(nullptr, VH_ERR_ARG, std::string("vh_create: ") + why);
-  if (eos->kind == VH_EOS_HADRON)
-    return fail(nullptr, VH_ERR_ARG, "vh_create: EoSHadron is a surface EoS (vh_set_surface_eos)");
+  if (eos->kind == VH_EOS_HADRON || eos->kind == VH_EOS_SMASH)
+    return fail(nullptr, VH_ERR_ARG,
+                "vh_create: EoSHadron / EoSSmash are surface EoS (vh_set_surface_eos)");
   const double dx = (grid->xmax - grid->xmin) / (grid->nx - 1);
   const double dy = (grid->ymax - grid->ymin) / (grid->ny - 1);
   if (!(dt > 0.) || dt > dx / 2. || dt > dy / 2.)

@@ -1,5 +1,6 @@
-// Correctly rounded exp(x) and x^(1/4) in FP64, for the transport
-// coefficients (zeta/s forms 1-5, src/trancoeff.cpp:19-70).  The reference
+// Correctly rounded exp(x), log(x) and x^(1/4) in FP64, for the transport
+// coefficients (zeta/s forms 1-5, src/trancoeff.cpp:19-70), EoSChiral's
+// power law and EoSHadron's logarithmic table coordinates.  The reference
 // evaluates them with the host C library, whose exp and pow are accurate to
 // about half an ulp; returning the correctly rounded value reproduces the
 // library's result except where the exact value lies within ~1e-3 ulp of a
@@ -18,6 +19,7 @@
 //        1 + expm1 rounded to nearest once; scaled by 2^k, with the
 //        subnormal range rounded to integer multiples of 2^-1074 from the
 //        double-double.  Relative error before the final rounding < 2^-98.
+//   log: a Newton step on the exp above from a faithful seed (log_cr).
 //   x^(1/4): sqrt(x) as a double-double (the correctly rounded square root
 //        and its exact residual by fma), its square root the same way, and
 //        one rounding of the sum.
@@ -109,19 +111,14 @@ VH_CRM double scale_round(dd y, int k) {
   return n * pow2i(-1022) * pow2i(-52);  // exact: n < 2^53
 }
 
-VH_CRM double exp_cr(double x) {
-  if (!(x == x)) return x;  // NaN
-  if (x > 709.8) return (double)INFINITY;
-  if (x < -746.0) return 0.0;
-  const double LN2_1 = 0x1.62e42fef00000p-1;   // 33 significant bits
-  const double LN2_2 = 0x1.473de6af278edp-34;
-  const double LN2_3 = -0x1.9ff0342542fc3p-90;
-  const double INV_LN2 = 0x1.71547652b82fep+0;
-  const double k = rint(x * INV_LN2);
-  // r = x - k ln2 as a double-double
-  dd r = two_sum(x, -(k * LN2_1));  // k * LN2_1 exact
-  r = add(r, {-two_prod(k, LN2_2).hi, -two_prod(k, LN2_2).lo});
-  r = add(r, {-(k * LN2_3), 0.0});
+// ln 2 = LN2_1 + LN2_2 + LN2_3 (LN2_1 has 33 significant bits, so k LN2_1
+// is exact for |k| < 2^20)
+#define VH_CRM_LN2_1 0x1.62e42fef00000p-1
+#define VH_CRM_LN2_2 0x1.473de6af278edp-34
+#define VH_CRM_LN2_3 -0x1.9ff0342542fc3p-90
+
+// expm1(r) for |r| <= 0.36 as a double-double
+VH_CRM dd expm1_dd(dd r) {
   // s = r / 2^8
   const dd s = {r.hi * 0x1p-8, r.lo * 0x1p-8};
   // expm1(s) = s (1 + s/2! + s^2/3! + ... + s^10/11!) by Horner
@@ -144,8 +141,74 @@ VH_CRM double exp_cr(double x) {
   // expm1(2a) = 2 expm1(a) + expm1(a)^2, eight times
 #pragma unroll
   for (int j = 0; j < 8; j++) e = add({2. * e.hi, 2. * e.lo}, mul(e, e));
-  const dd y = add({1.0, 0.0}, e);
+  return e;
+}
+
+VH_CRM double exp_cr(double x) {
+  if (!(x == x)) return x;  // NaN
+  if (x > 709.8) return (double)INFINITY;
+  if (x < -746.0) return 0.0;
+  const double INV_LN2 = 0x1.71547652b82fep+0;
+  const double k = rint(x * INV_LN2);
+  // r = x - k ln2 as a double-double
+  dd r = two_sum(x, -(k * VH_CRM_LN2_1));  // k * LN2_1 exact
+  r = add(r, {-two_prod(k, VH_CRM_LN2_2).hi, -two_prod(k, VH_CRM_LN2_2).lo});
+  r = add(r, {-(k * VH_CRM_LN2_3), 0.0});
+  const dd y = add({1.0, 0.0}, expm1_dd(r));
   return scale_round(y, (int)k);
+}
+
+VH_CRM double from_bits(unsigned long long u) {
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double((long long)u);
+#else
+  double d;
+  __builtin_memcpy(&d, &u, sizeof d);
+  return d;
+#endif
+}
+
+VH_CRM unsigned long long to_bits(double d) {
+#ifdef __CUDA_ARCH__
+  return (unsigned long long)__double_as_longlong(d);
+#else
+  unsigned long long u;
+  __builtin_memcpy(&u, &d, sizeof u);
+  return u;
+#endif
+}
+
+// log(x), correctly rounded.  x = m 2^k with m in [0.707, 1.415); the
+// platform's log(m) (faithful, on the host or the device) is a seed y0;
+// one Newton step on exp, y = y0 + ((m - 1) - expm1(y0)) / exp(y0), with
+// m - 1 exact and expm1(y0) a double-double, removes the seed's error (the
+// step's own error is of the order of the seed error squared, ~2^-104 |y|);
+// then k ln 2 + y in double-double and one rounding.  Seeds that differ by
+// an ulp give the same result, so host and device agree.
+VH_CRM double log_cr(double x) {
+  if (!(x > 0.)) return x == 0. ? -(double)INFINITY : (double)NAN;
+  if (x == (double)INFINITY) return x;
+  int k = 0;
+  if (x < 0x1p-1022) {  // subnormal: scale into the normal range (exact)
+    x *= 0x1p54;
+    k = -54;
+  }
+  const unsigned long long u = to_bits(x);
+  k += (int)(u >> 52) - 1023;
+  double m = from_bits((u & 0x000fffffffffffffull) | 0x3ff0000000000000ull);  // [1, 2)
+  if (m > 1.41421356) {
+    m *= 0.5;
+    k += 1;
+  }
+  const double y0 = log(m);
+  const dd em1 = expm1_dd({y0, 0.});
+  const dd d = add({m - 1., 0.}, {-em1.hi, -em1.lo});  // m - 1 exact (Sterbenz)
+  const double c = d.hi / (1. + em1.hi);
+  const dd y = two_sum(y0, c);
+  const double kd = (double)k;
+  dd L = add(two_prod(kd, VH_CRM_LN2_2), {kd * VH_CRM_LN2_3, 0.});
+  L = add({kd * VH_CRM_LN2_1, 0.}, L);
+  return add(L, y).hi;
 }
 
 // x^(1/4) for x >= 0 (x = +0 gives +0, x = inf gives inf)
@@ -208,3 +271,6 @@ VH_CRM double mk_div(double y, double b, double r) {
 }  // namespace vh
 
 #undef VH_CRM
+#undef VH_CRM_LN2_1
+#undef VH_CRM_LN2_2
+#undef VH_CRM_LN2_3

@@ -47,6 +47,14 @@ struct HadronTab {
   const int* __restrict__ status;
 };
 
+// EoSSmash's tables and grids (kind 5, a freeze-out EoS)
+struct SmashTab {
+  int ne, nnb, nnq;
+  double emin, emax, nbmin, nbmax, nqmin, nqmax;
+  const double *__restrict__ p, *__restrict__ T, *__restrict__ mub, *__restrict__ muq,
+      *__restrict__ mus;
+};
+
 struct EosDev {
   int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table, 2 EoSChiral
   double conf_cnst;  // e = cnst T^4 for kind 0
@@ -83,6 +91,7 @@ struct EosDev {
   int iq0;
   double uq0;
   HadronTab h;  // kind 4
+  SmashTab sm;  // kind 5
 };
 
 __device__ __forceinline__ float c2p_guess(const EosDev& E, long long i) {
@@ -389,7 +398,7 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
 // EoSHadron (kind 4, the surface's).
 enum {
   EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4, EK_TABLE3 = 5,
-  EK_HADRON = 6
+  EK_HADRON = 6, EK_SMASH = 7
 };
 __host__ __device__ constexpr bool ek_chiral(int ek) { return ek == EK_CHIRAL || ek == EK_CHIRAL_SL; }
 __host__ __device__ constexpr bool ek_slope(int ek) { return ek == EK_TABLE_SL || ek == EK_CHIRAL_SL; }
@@ -467,15 +476,18 @@ __device__ __forceinline__ void eos3f(const EosDev& E, double e, double nb, doub
 __device__ __forceinline__ double hadron_x(double n, double n0, double lognmax, double dxn,
                                            double n_abs_min) {
   if (n != 0.0) {
-    const double zn = log(fabs(n) / n0);
+    const double zn = crm::log_cr(fabs(n) / n0);
     if (zn >= -lognmax + 2.0 * dxn) return n / fabs(n) * 0.5 * (zn + lognmax);
     return n / n_abs_min * dxn;
   }
   return 0.;
 }
 
-// EoSHadron::eos / ::p, src/eoHadron.cpp:81-208, at nq = 0 (its log is the
-// device's, which may differ from the C library's in the last bit)
+// EoSHadron::eos / ::p, src/eoHadron.cpp:81-208, at nq = 0; its logarithms
+// correctly rounded (crm::log_cr), the C library's value bar the rare
+// arguments where the library itself misrounds: the pressure feeds
+// transformPV's root search at the freeze-out surface, whose iteration count
+// follows the last bit
 template <bool WANT_T>
 __device__ __forceinline__ void eos_hadron(const HadronTab& H, double e, double nb, double& T,
                                            double& mub, double& muq, double& mus, double& p) {
@@ -490,7 +502,7 @@ __device__ __forceinline__ void eos_hadron(const HadronTab& H, double e, double 
     if (WANT_T) T = e / H.e_min * __ldg(H.T + ix3(0, nnb / 2, nnq / 2));
     return;
   }
-  const double xe = log(e / H.e0);
+  const double xe = crm::log_cr(e / H.e0);
   const double dxe = (H.logemax - H.logemin) / (ne - 1);
   const double dxnb = (2.0 * H.lognmax) / (nnb - 1);
   const double dxnq = (2.0 * H.lognmax) / (nnq - 1);
@@ -538,9 +550,74 @@ __device__ __forceinline__ void eos_hadron(const HadronTab& H, double e, double 
   }
 }
 
+// EoSSmash::eos / ::p, src/eoSmash.cpp:70-177, at nq = 0
+template <bool WANT_T>
+__device__ __forceinline__ void eos_smash(const SmashTab& H, double e, double nb, double& T,
+                                          double& mub, double& muq, double& mus, double& p) {
+  const int ne = H.ne, nnb = H.nnb, nnq = H.nnq;
+  auto ix3 = [&](int ie, int inb, int inq) {
+    return (long long)inq + (long long)nnq * inb + (long long)nnq * nnb * ie;
+  };
+  T = mub = muq = mus = p = 0.;
+  if (e <= 0.) return;
+  if (e < H.emin) {
+    p = e / H.emin * __ldg(H.p + ix3(0, nnb / 2, nnq / 2));
+    if (WANT_T) T = e / H.emin * __ldg(H.T + ix3(0, nnb / 2, nnq / 2));
+    return;
+  }
+  const double nq = 0.;
+  const double de = (H.emax - H.emin) / (ne - 1);
+  const double dnb = (H.nbmax - H.nbmin) / (nnb - 1);
+  const double dnq = (H.nqmax - H.nqmin) / (nnq - 1);
+  int ie = (int)((e - H.emin) / de);
+  int inb = (int)((nb - H.nbmin) / dnb);
+  int inq = (int)((nq - H.nqmin) / dnq);
+  if (ie < 0) ie = 0;
+  if (inb < 0) inb = 0;
+  if (inq < 0) inq = 0;
+  if (ie > ne - 2) ie = ne - 2;
+  if (inb > nnb - 2) inb = nnb - 2;
+  if (inq > nnq - 2) inq = nnq - 2;
+  const double em = e - H.emin - ie * de;
+  const double nbm = nb - H.nbmin - inb * dnb;
+  const double nqm = nq - H.nqmin - inq * dnq;
+  const double we[2] = {1. - em / de, em / de};
+  const double wnb[2] = {1. - nbm / dnb, nbm / dnb};
+  const double wnq[2] = {1. - nqm / dnq, nqm / dnq};
+  double sp = 0., sT = 0., sb = 0., sq = 0., ss = 0.;
+#pragma unroll
+  for (int je = 0; je < 2; je++)
+#pragma unroll
+    for (int jnb = 0; jnb < 2; jnb++)
+#pragma unroll
+      for (int jnq = 0; jnq < 2; jnq++) {
+        const long long k = ix3(ie + je, inb + jnb, inq + jnq);
+        sp += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.p + k);
+        if (WANT_T) {
+          sT += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.T + k);
+          sb += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.mub + k);
+          sq += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.muq + k);
+          ss += we[je] * wnb[jnb] * wnq[jnq] * __ldg(H.mus + k);
+        }
+      }
+  if (sp < 0.0) sp = 0.0;
+  p = sp;
+  if (WANT_T) {
+    T = sT;
+    mub = sb;
+    muq = sq;
+    mus = ss;
+  }
+}
+
 template <int EK = EK_ANY>
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
   double T, mub, mus, p;
+  if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
+    double muq;
+    eos_smash<false>(E.sm, e, nb, T, mub, muq, mus, p);
+    return p;
+  }
   if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
     double muq;
     eos_hadron<false>(E.h, e, nb, T, mub, muq, mus, p);
@@ -565,7 +642,10 @@ template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
                                          double& mub, double& mus, double& p) {
   mus = 0.;
-  if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
+  if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
+    double muq;
+    eos_smash<true>(E.sm, e, nb, T, mub, muq, mus, p);
+  } else if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
     double muq;
     eos_hadron<true>(E.h, e, nb, T, mub, muq, mus, p);
   } else if (EK == EK_TABLE3 || (EK == EK_ANY && E.kind == 3)) {
@@ -593,6 +673,10 @@ __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb,
 template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval_q(const EosDev& E, double e, double nb, double& T,
                                            double& mub, double& muq, double& mus, double& p) {
+  if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
+    eos_smash<true>(E.sm, e, nb, T, mub, muq, mus, p);
+    return;
+  }
   if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {
     eos_hadron<true>(E.h, e, nb, T, mub, muq, mus, p);
     return;
@@ -788,7 +872,7 @@ __device__ __forceinline__ double tr_zetaS(const TrDev& t, double e, double T,
     const double sig = e < t.zetaSPeakEpsilon ? t.zetaSSigmaMinus : t.zetaSSigmaPlus;
     return ((e + P) / (s * T)) * t.zetaS0 * crm::exp_cr(d * d / 2.0 * (sig * sig));
   } else if (t.zetaSparam == 5) {
-    // a Gaussian bump in T (this build's addition; not in the reference)
+    // a Gaussian bump in T (not in the reference)
     const double x = T - t.zetaSPeakT;
     return t.zetaS0 * crm::exp_cr(-x * x / (2. * t.zetaSWidthT * t.zetaSWidthT));
   }

@@ -695,7 +695,9 @@ __global__ void __launch_bounds__(kTotBlock) k_sum_cols(const double* __restrict
 void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double tau, double taup,
                         double* eN, double* eP, cudaStream_t s) {
   const unsigned nb = (unsigned)((g.N + 127) / 128);
-  if (E.kind == 4)
+  if (E.kind == 5)
+    k_surf_energy<EK_SMASH><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
+  else if (E.kind == 4)
     k_surf_energy<EK_HADRON><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
   else if (E.kind == 3)
     k_surf_energy<EK_TABLE3><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
@@ -753,7 +755,9 @@ void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double
                           int npartial, cudaStream_t s) {
   SurfArgs a{g,    E,    f.Q,      f.Qprev,   f.pi,   f.Pi, tau, dtf, ecrit,  xmin, ymin, zmin,
              cubes, counters, cap_cubes, cap_el, geo, off, rec, contrib};
-  if (E.kind == 4)
+  if (E.kind == 5)
+    k_surf_elements<EK_SMASH><<<kElemGrid, 128, 0, s>>>(a);
+  else if (E.kind == 4)
     k_surf_elements<EK_HADRON><<<kElemGrid, 128, 0, s>>>(a);
   else if (E.kind == 3)
     k_surf_elements<EK_TABLE3><<<kElemGrid, 128, 0, s>>>(a);

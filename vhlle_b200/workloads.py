@@ -135,6 +135,9 @@ class EosTable:
     hadron: Optional[tuple] = None
     hrows: Optional[np.ndarray] = None
     status: Optional[np.ndarray] = None
+    # kind 5 (EoSSmash): (ne, nnb, nnq) and the uniform grids' values; p, T,
+    # mub, muq, mus at [inq + nnq*inb + nnq*nnb*ie]
+    smash: Optional[tuple] = None
 
     def write_chiral(self, directory: str) -> None:
         """directory/eos/chiralsmall.dat and chiraleos.dat, the files
@@ -204,6 +207,23 @@ class EosTable:
                     float(self.hrows[k, 0]), float(self.hrows[k, 1]), float(self.hrows[k, 2]),
                     float(self.p[k]), float(self.T[k]), float(self.mub[k]), float(self.muq[k]),
                     float(self.mus[k]), int(self.status[k])))
+
+    def write_smash(self, path: str) -> None:
+        """Write the table in the reference's EoSSmash text format: one header
+        line, then ``e nb nq T p mub mus muq`` rows with ie, inb, inq nested
+        outer to inner (src/eoSmash.cpp:30-43); 17 significant digits."""
+        assert self.kind == 5
+        (ne, nnb, nnq), (eg, bg, qg) = self.smash
+        with open(path, "w") as f:
+            f.write("# e nb nq T p muB muS muQ\n")
+            for ie in range(ne):
+                for inb in range(nnb):
+                    for inq in range(nnq):
+                        k = inq + nnq * inb + nnq * nnb * ie
+                        f.write("%r %r %r %r %r %r %r %r\n" % (
+                            float(eg[ie]), float(bg[inb]), float(qg[inq]), float(self.T[k]),
+                            float(self.p[k]), float(self.mub[k]), float(self.mus[k]),
+                            float(self.muq[k])))
 
     @staticmethod
     def read_eos1f(path: str) -> "EosTable":
@@ -329,6 +349,22 @@ def hadron_eos_table(ne: int = 101, nnb: int = 41, nnq: int = 21, e0: float = 1.
     return EosTable(kind=4, p=flat(p), T=flat(T), mub=flat(mub), muq=flat(muq), mus=flat(mus),
                     hadron=(ne, nnb, nnq, e0, n0, logemin, logemax, lognmax), hrows=rows,
                     status=np.ascontiguousarray(status.reshape(-1)))
+
+
+def smash_eos_table(ne: int = 101, nnb: int = 51, nnq: int = 51) -> EosTable:
+    """A synthetic hadron-gas EoS in the reference's EoSSmash format (the
+    driver's eosTypeHadron 1, read with ne x nnb x nnq = 101 x 51 x 51,
+    src/main.cpp:308): uniform grids e in [0.01, 1.01] GeV/fm^3, nb and nq in
+    [-0.5, 0.5] fm^-3; p = 0.14 e + 0.3 nb^2 + 0.05 nq^2, T = 0.12 + 0.05 e
+    - 0.02 nb^2, mu_B = 0.9 nb, mu_Q = 0.2 nq, mu_S = 0.25 nb."""
+    eg = 0.01 + 0.01 * np.arange(ne)
+    bg = -0.5 + (1.0 / (nnb - 1)) * np.arange(nnb)
+    qg = -0.5 + (1.0 / (nnq - 1)) * np.arange(nnq)
+    E, B, Qc = np.meshgrid(eg, bg, qg, indexing="ij")
+    flat = lambda a: np.ascontiguousarray(a, dtype=np.float64).reshape(-1)  # noqa: E731
+    return EosTable(kind=5, p=flat(0.14 * E + 0.3 * B * B + 0.05 * Qc * Qc),
+                    T=flat(0.12 + 0.05 * E - 0.02 * B * B), mub=flat(0.9 * B),
+                    muq=flat(0.2 * Qc), mus=flat(0.25 * B), smash=((ne, nnb, nnq), (eg, bg, qg)))
 
 
 def eos3f_table(ne: int = 120, emin: float = 1e-4, emax: float = 1e3) -> EosTable:
