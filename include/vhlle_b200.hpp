@@ -356,6 +356,91 @@ class EoSHadron : public EoS {
   }
 };
 
+// EoSSmash (src/eoSmash.cpp): the SMASH hadron-gas EoS the reference driver
+// gives the freeze-out surface for eosTypeHadron 1 (src/main.cpp:308-309,
+// eos/hadgas_eos_SMASH.dat with 101 x 51 x 51 points).  Reads the table (a
+// header line, then "e nb nq T p muB muS muQ" rows, ie outer, inq inner);
+// the grids are uniform from the first to the last row's e, nb, nq, and the
+// lookup is trilinear; the device evaluates the same table.
+class EoSSmash : public EoS {
+  int ne_ = 0, nnb_ = 0, nnq_ = 0;
+  double emin_ = 0, emax_ = 0, nbmin_ = 0, nbmax_ = 0, nqmin_ = 0, nqmax_ = 0;
+  std::vector<double> p_, T_, mub_, muq_, mus_;
+  size_t ix3(int ie, int inb, int inq) const {
+    return inq + (size_t)nnq_ * inb + (size_t)nnq_ * nnb_ * ie;
+  }
+
+ public:
+  EoSSmash(const char* filename, int ne, int nnb, int nnq) : ne_(ne), nnb_(nnb), nnq_(nnq) {
+    std::ifstream fin(filename);
+    if (!fin) throw Error(VH_ERR_ARG, std::string("EoSSmash: I/O error with ") + filename);
+    if (ne < 2 || nnb < 2 || nnq < 2) throw Error(VH_ERR_ARG, "EoSSmash: bad table dimensions");
+    std::string header;
+    std::getline(fin, header);
+    const size_t n = (size_t)ne_ * nnb_ * nnq_;
+    for (auto* t : {&p_, &T_, &mub_, &muq_, &mus_}) t->resize(n);
+    double e = 0, nb = 0, nq = 0;
+    for (int ie = 0; ie < ne_; ie++)
+      for (int inb = 0; inb < nnb_; inb++)
+        for (int inq = 0; inq < nnq_; inq++) {
+          const size_t k = ix3(ie, inb, inq);
+          fin >> e >> nb >> nq >> T_[k] >> p_[k] >> mub_[k] >> mus_[k] >> muq_[k];
+          if (k == 0) {
+            emin_ = e;
+            nbmin_ = nb;
+            nqmin_ = nq;
+          }
+        }
+    if (!fin) throw Error(VH_ERR_ARG, "EoSSmash: truncated table");
+    emax_ = e;
+    nbmax_ = nb;
+    nqmax_ = nq;
+    if (!(emin_ < emax_) || !(nbmin_ < nbmax_) || !(nqmin_ < nqmax_))
+      throw Error(VH_ERR_ARG, "EoSSmash: the table's e, nb, nq ranges are empty");
+  }
+  void eos(double e, double nb, double nq, double, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    T = mub = muq = mus = p = 0.;
+    if (e <= 0.) return;
+    if (e < emin_) {
+      p = e / emin_ * p_[ix3(0, nnb_ / 2, nnq_ / 2)];
+      T = e / emin_ * T_[ix3(0, nnb_ / 2, nnq_ / 2)];
+      return;
+    }
+    const double de = (emax_ - emin_) / (ne_ - 1), dnb = (nbmax_ - nbmin_) / (nnb_ - 1),
+                 dnq = (nqmax_ - nqmin_) / (nnq_ - 1);
+    int ie = (int)((e - emin_) / de), inb = (int)((nb - nbmin_) / dnb),
+        inq = (int)((nq - nqmin_) / dnq);
+    ie = std::min(std::max(ie, 0), ne_ - 2);
+    inb = std::min(std::max(inb, 0), nnb_ - 2);
+    inq = std::min(std::max(inq, 0), nnq_ - 2);
+    const double em = e - emin_ - ie * de, nbm = nb - nbmin_ - inb * dnb,
+                 nqm = nq - nqmin_ - inq * dnq;
+    const double we[2] = {1. - em / de, em / de}, wnb[2] = {1. - nbm / dnb, nbm / dnb},
+                 wnq[2] = {1. - nqm / dnq, nqm / dnq};
+    for (int je = 0; je < 2; je++)
+      for (int jnb = 0; jnb < 2; jnb++)
+        for (int jnq = 0; jnq < 2; jnq++) {
+          const size_t k = ix3(ie + je, inb + jnb, inq + jnq);
+          const double w = we[je] * wnb[jnb] * wnq[jnq];
+          p += w * p_[k];
+          T += w * T_[k];
+          mub += w * mub_[k];
+          muq += w * muq_[k];
+          mus += w * mus_[k];
+        }
+    if (p < 0.0) p = 0.0;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_SMASH;
+    d.smash = vh_eos::vh_eos_smash{ne_,    nnb_,   nnq_,      emin_,     emax_,
+                                   nbmin_, nbmax_, nqmin_,    nqmax_,    p_.data(),
+                                   T_.data(), mub_.data(), muq_.data(), mus_.data()};
+    return d;
+  }
+};
+
 // EoSChiral (src/eoChiral.cpp): the reference's default EoS (eosType 1).
 // Reads dir/eos/chiraleos.dat (2001 x 401) and dir/eos/chiralsmall.dat
 // (201 x 201) in the EoSaux format (8 columns, nb outer, e inner) with its

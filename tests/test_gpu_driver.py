@@ -236,3 +236,54 @@ def test_cpp_driver_chiral_eos_equals_oracle(tmp_path):
     assert tau == o.tau_now
     bad = compare_states(st, o.get_state())
     assert not bad, bad
+
+
+@pytest.mark.parametrize("kind", [0, 1], ids=["EoSHadron", "EoSSmash"])
+def test_cpp_driver_freezeout_eos_equals_oracle(tmp_path, kind):
+    """vhlle_run with eosTypeHadron 0 / 1 and the reference's table under
+    ./eos (eos/eosHadronLog.dat, eos/hadgas_eos_SMASH.dat at 101 x 51 x 51,
+    src/main.cpp:304-309): the corona and every surface of freezeout.dat
+    are those of the oracle with that freeze-out EoS (1e-12, 15 printed
+    digits), and the final grid, which the freeze-out EoS does not touch,
+    is the oracle's bit for bit."""
+    import os
+    import subprocess
+    from vhlle_b200 import build as B
+    drv = B.build_driver()
+    h = W.hadron_eos_table() if kind == 0 else W.smash_eos_table(101, 51, 51)
+    os.makedirs(tmp_path / "eos")
+    if kind == 0:
+        h.write_hadron(str(tmp_path / "eos" / "eosHadronLog.dat"))
+    else:
+        h.write_smash(str(tmp_path / "eos" / "hadgas_eos_SMASH.dat"))
+    setup = W.glauber3d_nb_setup(17, 17, 9, eos=W.nb_table(200, 20))
+    setup.eos.write_eos1f(str(tmp_path / "eos.dat"))
+    ic = str(tmp_path / "ic.vhb")
+    W.write_snapshot(ic, setup.grid, setup.tau0, setup.dt, W.initial_snapshot_state(setup))
+    params = str(tmp_path / "params.txt")
+    tau_max = setup.tau0 + 4.5 * setup.dt
+    W.write_params(params, setup, tauMax=tau_max, tauGridResize=100.0, eosTypeHadron=kind,
+                   eos1fFile=str(tmp_path / "eos.dat"))
+    run = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", "out"],
+                         capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr
+    assert ("freeze-out EoS: " + ("EoSHadron" if kind == 0 else "EoSSmash")) in run.stdout
+    o = P.OracleRun(setup, surface_eos=h)
+    g = setup.grid
+    corona, _ = o.corona()
+    recs = [corona]
+    while True:
+        o.advance(setup.dt, g.etamin, g.etamax, g.nz)
+        r, _ = o.surface(dtf=o.dt)
+        recs.append(r)
+        if not (o.tau_now < tau_max + 0.0001 and len(r) > 0):
+            break
+    fz = P.read_freezeout(str(tmp_path / "out" / "freezeout.dat"))
+    ref = np.concatenate(recs)[:, :27]
+    assert fz.shape == ref.shape and len(ref) > len(corona)
+    ok = np.abs(fz - ref) <= 1e-12 * np.maximum(np.abs(fz), np.abs(ref)) + 1e-300
+    assert ok.all(), np.argwhere(~ok)[:5]
+    nx, ny, nz, b, tau, dt, st = W.read_snapshot(str(tmp_path / "out" / "final.vhb"))
+    assert tau == o.tau_now
+    bad = compare_states(st, o.get_state())
+    assert not bad, bad

@@ -11,7 +11,10 @@
 // the extra key eos1fFile; else, for eosType 1 (the default), EoSChiral from
 // ./eos/chiraleos.dat and ./eos/chiralsmall.dat as the reference reads them;
 // else (those files absent, or another eosType) the conformal gas of 47.5
-// degrees of freedom.  Before the loop the corona of Fluid::outputCorona opens the
+// degrees of freedom.  The freeze-out EoS (src/main.cpp:304-314) is, for
+// eosTypeHadron 0, EoSHadron from ./eos/eosHadronLog.dat, for eosTypeHadron
+// 1, EoSSmash from ./eos/hadgas_eos_SMASH.dat (101 x 51 x 51), where those
+// files exist; otherwise the hydro EoS.  Before the loop the corona of Fluid::outputCorona opens the
 // freeze-out file.  Each loop iteration does what Fluid::outputSurface does: it
 // appends the freeze-out elements to DIR/freezeout.dat.unfinished (renamed
 // freezeout.dat at the end) and prints the same line (tau, E, Efull,
@@ -111,6 +114,22 @@ int run(int argc, char** argv) {
                                               : std::string("conformal gas"))
             << std::endl;
   vhb::EoS* eosH = eos;
+  if (P.eosTypeHadron == 0 && stat("eos/eosHadronLog.dat", &sb) == 0)
+    eosH = new vhb::EoSHadron("eos/eosHadronLog.dat");
+  else if (P.eosTypeHadron == 1 && stat("eos/hadgas_eos_SMASH.dat", &sb) == 0)
+    eosH = new vhb::EoSSmash("eos/hadgas_eos_SMASH.dat", 101, 51, 51);
+  else if (P.eosTypeHadron != 0 && P.eosTypeHadron != 1) {  // src/main.cpp:310-314
+    std::cout << "Unknown hadronic EoS type for hypersurface creation.\n"
+              << "eosTypeHadron should be either \"0\" (PDG hadronic EoS) or \"1\" (SMASH "
+                 "hadronic EoS).\n";
+    delete eos;
+    return 0;
+  }
+  std::cout << "freeze-out EoS: "
+            << (eosH == eos ? std::string("the hydro EoS")
+                            : P.eosTypeHadron == 0 ? std::string("EoSHadron (eos/eosHadronLog.dat)")
+                                                   : std::string("EoSSmash (eos/hadgas_eos_SMASH.dat)"))
+            << std::endl;
   vhb::TransportCoeff* trcoeff = new vhb::TransportCoeff(
       P.etaS, P.zetaS, P.ah, P.al, P.aRho, P.T0, P.etaSMin, P.etaSEpsilonMin, P.etaSShiftMuB,
       P.etaSScaleMuB, P.zetaSPeakEpsilon, P.zetaSScaleBeta, P.zetaSSigmaMinus,
@@ -190,6 +209,7 @@ int run(int argc, char** argv) {
   delete h;
   delete f;
   delete trcoeff;
+  if (eosH != eos) delete eosH;
   delete eos;
   return bits ? 3 : 0;
 }
