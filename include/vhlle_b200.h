@@ -32,8 +32,10 @@ extern "C" {
 #endif
 
 /* 2: vh_eos gained the aux tables of VH_EOS_CHIRAL (a caller built against
- * version 1 passes a shorter vh_eos) */
-#define VH_ABI_VERSION 2
+ * version 1 passes a shorter vh_eos);
+ * 3: vh_grid gained dz, vh_eos the EoS3f, EoSHadron, EoSSmash and EoSAZH
+ * members (kinds 3-6) */
+#define VH_ABI_VERSION 3
 
 typedef int vh_status;
 #define VH_OK 0
@@ -84,7 +86,9 @@ typedef struct vh_grid {
  *                         reference driver gives the freeze-out surface
  *                         (eosTypeHadron 0): `hadron` below;
  *  kind VH_EOS_SMASH:     EoSSmash (src/eoSmash.cpp, eosTypeHadron 1):
- *                         `smash` below; both for vh_set_surface_eos only.
+ *                         `smash` below; both for vh_set_surface_eos only;
+ *  kind VH_EOS_AZH:       EoSAZH (src/eoAZH.cpp, eosType 2): six uniform
+ *                         (e, nb) tables, `azh` below.
  * Host arrays are copied at vh_create (vh_set_surface_eos). */
 #define VH_EOS_CONFORMAL 0
 #define VH_EOS_TABLE 1
@@ -92,6 +96,7 @@ typedef struct vh_grid {
 #define VH_EOS_TABLE3 3
 #define VH_EOS_HADRON 4
 #define VH_EOS_SMASH 5
+#define VH_EOS_AZH 6
 /* One EoSaux table (src/eoChiral.cpp:33-97) after its constructor's unit
  * conversions: the e and nb grids are uniform from emin to emax (GeV/fm^3)
  * and nmin to nmax (fm^-3) with ne, nn >= 2 points; p (GeV/fm^3), T, muB,
@@ -126,6 +131,17 @@ typedef struct vh_eos {
     double emin, emax, nbmin, nbmax, nqmin, nqmax;
     const double *p, *T, *mub, *muq, *mus;
   } smash;
+  /* VH_EOS_AZH only: EoSAZH's six EoSAZHaux tables (src/eoAZH.cpp:15-56),
+   * p, T and muB below (1) and above (2) the first table's e range.  Each
+   * has ne x nn points on the uniform grids e = emin + ie de, nb = nmin +
+   * in dn (ne and nn the file's counts plus one), values at [ie * nn + in]. */
+  struct vh_eos_azh {
+    struct vh_eos_azh_table {
+      int ne, nn;
+      double emin, nmin, de, dn;
+      const double *v;
+    } p1, p2, T1, T2, mu1, mu2;
+  } azh;
 } vh_eos;
 
 /* TransportCoeff public constants (src/trancoeff.h:8-11, ctor :14-20). */

@@ -441,6 +441,87 @@ class EoSSmash : public EoS {
   }
 };
 
+// EoSAZH (src/eoAZH.cpp): the reference driver's eosType 2.  Reads
+// dir/eos/azhydro0p2/aa{1,2}_{p,t,mb}.dat in the EoSAZHaux format (header
+// "nmin emin", "dn de nn ne" with one point fewer than stored on each axis,
+// then the values with e outer); p, T and muB come from the first table set
+// inside its e range, from the second above it and from the first set's
+// first row scaled by e / emin below it; the device evaluates the same tables.
+class EoSAZH : public EoS {
+  struct Tab {
+    int ne = 0, nn = 0;
+    double emin = 0, nmin = 0, de = 0, dn = 0;
+    std::vector<double> v;  // [ie * nn + in]
+    explicit Tab(const std::string& path) {
+      std::ifstream fin(path);
+      if (!fin.good()) throw Error(VH_ERR_ARG, "EoSAZH: I/O error with " + path);
+      fin >> nmin >> emin >> dn >> de >> nn >> ne;
+      nn++;
+      ne++;
+      if (!fin || ne < 2 || nn < 2 || !(de > 0.) || !(dn > 0.) || !(emin > 0.))
+        throw Error(VH_ERR_ARG, "EoSAZH: bad header in " + path);
+      v.resize((size_t)ne * nn);
+      for (double& x : v) fin >> x;
+      if (!fin) throw Error(VH_ERR_ARG, "EoSAZH: truncated table " + path);
+    }
+    double get(double e, double nb) const {  // EoSAZHaux::get
+      if (e <= 0.) return 0.0;
+      int ie = (int)((e - emin) / de), in = (int)((nb - nmin) / dn);
+      ie = std::min(std::max(ie, 0), ne - 2);
+      in = std::min(std::max(in, 0), nn - 2);
+      const double em = (e - emin - ie * de) / de, nm = (nb - nmin - in * dn) / dn;
+      const double we[2] = {1. - em, em}, wn[2] = {1. - nm, nm};
+      double value = 0.0;
+      for (int je = 0; je < 2; je++)
+        for (int jn = 0; jn < 2; jn++) value += we[je] * wn[jn] * v[(size_t)(ie + je) * nn + in + jn];
+      return value;
+    }
+    double getLow(double e, double nb) const {  // EoSAZHaux::getLow
+      if (e <= 0.) return 0.0;
+      int in = (int)((nb - nmin) / dn);
+      in = std::min(std::max(in, 0), nn - 2);
+      const double nm = (nb - nmin - in * dn) / dn;
+      const double value = (1. - nm) * v[in] + nm * v[in + 1];
+      return value * e / emin;
+    }
+    vh_eos::vh_eos_azh::vh_eos_azh_table desc() const {
+      return {ne, nn, emin, nmin, de, dn, v.data()};
+    }
+  };
+  std::vector<Tab> t_;  // p1, p2, T1, T2, mu1, mu2
+
+ public:
+  explicit EoSAZH(const std::string& dir) {
+    for (const char* f : {"aa1_p", "aa2_p", "aa1_t", "aa2_t", "aa1_mb", "aa2_mb"})
+      t_.emplace_back(dir + "/eos/azhydro0p2/" + f + ".dat");
+  }
+  void eos(double e, double nb, double, double, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    const double anb = std::fabs(nb);
+    const Tab& p1 = t_[0];
+    if (e > p1.emin + p1.de * (p1.ne - 1)) {
+      p = t_[1].get(e, anb);
+      T = t_[3].get(e, anb);
+      mub = t_[5].get(e, nb);
+    } else if (e > p1.emin) {
+      p = t_[0].get(e, anb);
+      T = t_[2].get(e, anb);
+      mub = t_[4].get(e, nb);
+    } else {
+      p = t_[0].getLow(e, anb);
+      T = t_[2].getLow(e, anb);
+      mub = t_[4].getLow(e, nb);
+    }
+    muq = mus = 0.0;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_AZH;
+    d.azh = {t_[0].desc(), t_[1].desc(), t_[2].desc(), t_[3].desc(), t_[4].desc(), t_[5].desc()};
+    return d;
+  }
+};
+
 // EoSChiral (src/eoChiral.cpp): the reference's default EoS (eosType 1).
 // Reads dir/eos/chiraleos.dat (2001 x 401) and dir/eos/chiralsmall.dat
 // (201 x 201) in the EoSaux format (8 columns, nb outer, e inner) with its

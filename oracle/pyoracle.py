@@ -43,6 +43,12 @@ class _Aux(ctypes.Structure):
                 ("p", _dp), ("T", _dp), ("mub", _dp), ("mus", _dp)]
 
 
+class _Azh(ctypes.Structure):
+    _fields_ = [("ne", ctypes.c_int), ("nn", ctypes.c_int), ("emin", ctypes.c_double),
+                ("nmin", ctypes.c_double), ("de", ctypes.c_double), ("dn", ctypes.c_double),
+                ("v", _dp)]
+
+
 class _Eos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
@@ -54,7 +60,8 @@ class _Eos(ctypes.Structure):
                 ("logemax", ctypes.c_double), ("lognmax", ctypes.c_double),
                 ("status", ctypes.POINTER(ctypes.c_int)),
                 ("semin", ctypes.c_double), ("semax", ctypes.c_double), ("snbmin", ctypes.c_double),
-                ("snbmax", ctypes.c_double), ("snqmin", ctypes.c_double), ("snqmax", ctypes.c_double)]
+                ("snbmax", ctypes.c_double), ("snqmin", ctypes.c_double), ("snqmax", ctypes.c_double),
+                ("az", _Azh * 6)]
 
 
 class _Trc(ctypes.Structure):
@@ -275,6 +282,14 @@ class _EosHolder:
              self.s.logemax, self.s.lognmax) = eos.hadron
             self.s.p, self.s.T, self.s.mub, self.s.muq, self.s.mus = (_ptr(a) for a in arrs)
             self.s.status = st.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        if eos.kind == 6:
+            for k, (ne, nn, emin, nmin, de, dn, v) in enumerate(eos.azh):
+                arr = np.ascontiguousarray(v, dtype=np.float64)
+                assert arr.size == ne * nn
+                self.keep.append(arr)
+                x = self.s.az[k]
+                x.ne, x.nn, x.emin, x.nmin, x.de, x.dn = ne, nn, emin, nmin, de, dn
+                x.v = _ptr(arr)
         if eos.kind == 2:
             for k, a in enumerate(eos.aux):
                 arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
@@ -527,6 +542,10 @@ class RefRun:
             self._tmp = tempfile.TemporaryDirectory()
             eos_file = self._tmp.name
             setup.eos.write_chiral(eos_file)
+        if setup.eos.kind == 6 and eos_file is None:  # the directory that holds eos/
+            self._tmp = tempfile.TemporaryDirectory()
+            eos_file = self._tmp.name
+            setup.eos.write_azh(eos_file)
         bounds = np.array(g.bounds(), dtype=np.float64)
         tr = np.array(setup.tr_vector(), dtype=np.float64)
         self.h = self.lib.ref_create(g.nx, g.ny, g.nz, _ptr(bounds), setup.tau0, setup.dt,

@@ -34,6 +34,7 @@
 #include "eoChiral.h"
 #include "eoHadron.h"
 #include "eoSmash.h"
+#include "eoAZH.h"
 #include "fld.h"
 #include "hdo.h"
 #include "inc.h"
@@ -114,6 +115,24 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
     std::ostringstream quiet;
     std::cout.rdbuf(quiet.rdbuf());
     r->eos = new EoSChiral();
+    std::cout.rdbuf(old);
+    if (chdir(cwd) != 0) {
+      delete r->eos;
+      delete r;
+      return nullptr;
+    }
+  } else if (eos_kind == 6) {
+    // EoSAZH reads eos/azhydro0p2/aa{1,2}_{p,t,mb}.dat relative to the
+    // working directory (src/eoAZH.cpp:110-117), as EoSChiral does
+    char cwd[4096];
+    if (!getcwd(cwd, sizeof cwd) || chdir(eos_file) != 0) {
+      delete r;
+      return nullptr;
+    }
+    std::streambuf *old = std::cout.rdbuf();
+    std::ostringstream quiet;
+    std::cout.rdbuf(quiet.rdbuf());
+    r->eos = new EoSAZH();
     std::cout.rdbuf(old);
     if (chdir(cwd) != 0) {
       delete r->eos;

@@ -347,6 +347,59 @@ static void eos_smash(const or_eos *E, double e, double nb, double nq,
   *mus = ss;
 }
 
+/* EoSAZHaux::get, src/eoAZH.cpp:58-83 */
+static double azh_get(const struct or_azh *t, double e, double nb) {
+  if (e <= 0.) return 0.0;
+  int ie = (int)((e - t->emin) / t->de);
+  int in = (int)((nb - t->nmin) / t->dn);
+  if (ie < 0) ie = 0;
+  if (in < 0) in = 0;
+  if (ie > t->ne - 2) ie = t->ne - 2;
+  if (in > t->nn - 2) in = t->nn - 2;
+  const double em = (e - t->emin - ie * t->de) / t->de;
+  const double nm = (nb - t->nmin - in * t->dn) / t->dn;
+  const double we[2] = {1. - em, em};
+  const double wn[2] = {1. - nm, nm};
+  double value = 0.0;
+  for (int je = 0; je < 2; je++)
+    for (int jn = 0; jn < 2; jn++)
+      value += we[je] * wn[jn] * t->v[(long)(ie + je) * t->nn + (in + jn)];
+  return value;
+}
+
+/* EoSAZHaux::getLow, src/eoAZH.cpp:85-102 (its exit for nb beyond 10000
+ * cells left out: the clamped cell extrapolates) */
+static double azh_low(const struct or_azh *t, double e, double nb) {
+  if (e <= 0.) return 0.0;
+  int in = (int)((nb - t->nmin) / t->dn);
+  if (in < 0) in = 0;
+  if (in > t->nn - 2) in = t->nn - 2;
+  const double nm = (nb - t->nmin - in * t->dn) / t->dn;
+  const double wn[2] = {1. - nm, nm};
+  const double value = wn[0] * t->v[in] + wn[1] * t->v[in + 1];
+  return value * e / t->emin;
+}
+
+/* EoSAZH::eos, src/eoAZH.cpp:123-140 (p, T at |nb|, muB at nb) */
+static void eos_azh(const or_eos *E, double e, double nb, double *T,
+                    double *mub, double *p) {
+  const struct or_azh *a = E->az;
+  const double anb = fabs(nb);
+  if (e > a[0].emin + a[0].de * (a[0].ne - 1)) {
+    *p = azh_get(&a[1], e, anb);
+    *T = azh_get(&a[3], e, anb);
+    *mub = azh_get(&a[5], e, nb);
+  } else if (e > a[0].emin) {
+    *p = azh_get(&a[0], e, anb);
+    *T = azh_get(&a[2], e, anb);
+    *mub = azh_get(&a[4], e, nb);
+  } else {
+    *p = azh_low(&a[0], e, anb);
+    *T = azh_low(&a[2], e, anb);
+    *mub = azh_low(&a[4], e, nb);
+  }
+}
+
 /* EoS::eos() with muq; muq = 0 but for kind 3, mus = 0 but for kinds 2, 3 */
 static void eos_eval5(const or_eos *E, double e, double nb, double *T,
                       double *mub, double *muq, double *mus, double *p) {
@@ -370,6 +423,8 @@ static void eos_eval5(const or_eos *E, double e, double nb, double *T,
     *mub = 0.;
   } else if (E->kind == 2) {
     eos_chiral(E, e, nb, T, mub, mus, p);
+  } else if (E->kind == 6) {
+    eos_azh(E, e, nb, T, mub, p);
   } else {
     eos1f(E, e, nb, T, mub, p);
   }
@@ -408,6 +463,10 @@ static double eos_p(const or_eos *E, double e, double nb) {
   }
   if (E->kind == 2) {
     eos_chiral(E, e, nb, &T, &mub, &mus, &p);
+    return p;
+  }
+  if (E->kind == 6) {  /* EoSAZH::p, src/eoAZH.cpp:142-150: eos's p */
+    eos_azh(E, e, nb, &T, &mub, &p);
     return p;
   }
   eos1f(E, e, nb, &T, &mub, &p);

@@ -34,7 +34,8 @@ typedef struct or_grid {
 /* kind 0: conformal gas p = e/3, T = (e/cnst)^(1/4) (harness EoS)
  * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb]
  * kind 2: EoSChiral (aux below); kind 3: EoS3f (muq, mus below);
- * kind 4: EoSHadron, kind 5: EoSSmash (hadronic EoS of the freeze-out surface) */
+ * kind 4: EoSHadron, kind 5: EoSSmash (hadronic EoS of the freeze-out surface)
+ * kind 6: EoSAZH (six uniform (e, nb) tables, az below) */
 /* One EoSaux table of EoSChiral (src/eoChiral.cpp:33-97), converted to
  * GeV/fm^3, fm^-3 and GeV as its constructor does: uniform grids from emin
  * to emax and nmin to nmax, p/T/mub/mus[in * ne + ie]. */
@@ -70,6 +71,14 @@ typedef struct or_eos {
    * grids from the first to the last row's e, nb, nq; p, T, mub, muq, mus as
    * kind 4 */
   double semin, semax, snbmin, snbmax, snqmin, snqmax;
+  /* kind 6 (EoSAZH, src/eoAZH.cpp): p1, p2, T1, T2, mu1, mu2, each an
+   * EoSAZHaux table of ne x nn values at [ie * nn + in] on the grids
+   * emin + ie de, nmin + in dn (ne, nn the file's counts plus one) */
+  struct or_azh {
+    int ne, nn;
+    double emin, nmin, de, dn;
+    const double *v;
+  } az[6];
 } or_eos;
 
 /* Correctly rounded exp(x) and x^(1/4) (oracle/crm_shim.cpp). */

@@ -33,7 +33,7 @@ def test_header_declares_the_binding_list():
 def test_library_exports_every_declared_symbol(lib):
     for name in declared_symbols():
         assert hasattr(lib, name), name
-    assert lib.vh_abi_version() == 2
+    assert lib.vh_abi_version() == 3
 
 
 def _create(setup, dt=None):

@@ -238,6 +238,37 @@ def test_cpp_driver_chiral_eos_equals_oracle(tmp_path):
     assert not bad, bad
 
 
+def test_cpp_driver_azh_eos_equals_oracle(tmp_path):
+    """vhlle_run with eosType 2 and the EoSAZH tables under ./eos/azhydro0p2
+    (src/main.cpp:293-294, src/eoAZH.cpp:110-117) ends on the oracle's grid,
+    bit for bit."""
+    import subprocess
+    from vhlle_b200 import build as B
+    drv = B.build_driver()
+    setup = W.glauber3d_nb_setup(17, 17, 9, eos=W.azh_eos_table())
+    setup.eos.write_azh(str(tmp_path))
+    ic = str(tmp_path / "ic.vhb")
+    W.write_snapshot(ic, setup.grid, setup.tau0, setup.dt, W.initial_snapshot_state(setup))
+    params = str(tmp_path / "params.txt")
+    tau_max = setup.tau0 + 3.5 * setup.dt
+    W.write_params(params, setup, tauMax=tau_max, tauGridResize=100.0, eosType=2)
+    run = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", "out"],
+                         capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr
+    assert "hydro EoS: EoSAZH" in run.stdout
+    o = P.OracleRun(setup)
+    g = setup.grid
+    while True:
+        o.advance(setup.dt, g.etamin, g.etamax, g.nz)
+        r, _ = o.surface(dtf=o.dt)
+        if not (o.tau_now < tau_max + 0.0001 and len(r) > 0):
+            break
+    nx, ny, nz, b, tau, dt, st = W.read_snapshot(str(tmp_path / "out" / "final.vhb"))
+    assert tau == o.tau_now
+    bad = compare_states(st, o.get_state())
+    assert not bad, bad
+
+
 @pytest.mark.parametrize("kind", [0, 1], ids=["EoSHadron", "EoSSmash"])
 def test_cpp_driver_freezeout_eos_equals_oracle(tmp_path, kind):
     """vhlle_run with eosTypeHadron 0 / 1 and the reference's table under

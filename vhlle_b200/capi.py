@@ -239,12 +239,22 @@ class VhEosSmash(ctypes.Structure):
                 ("p", _dp), ("T", _dp), ("mub", _dp), ("muq", _dp), ("mus", _dp)]
 
 
+class VhEosAzhTable(ctypes.Structure):
+    _fields_ = [("ne", ctypes.c_int), ("nn", ctypes.c_int), ("emin", ctypes.c_double),
+                ("nmin", ctypes.c_double), ("de", ctypes.c_double), ("dn", ctypes.c_double),
+                ("v", _dp)]
+
+
+class VhEosAzh(ctypes.Structure):
+    _fields_ = [(n, VhEosAzhTable) for n in ("p1", "p2", "T1", "T2", "mu1", "mu2")]
+
+
 class VhEos(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int), ("conf_cnst", ctypes.c_double),
                 ("ne", ctypes.c_int), ("nn", ctypes.c_int),
                 ("egrid", _dp), ("ngrid", _dp), ("p", _dp), ("T", _dp), ("mub", _dp),
                 ("aux", VhEosAux * 2), ("muq", _dp), ("mus", _dp), ("hadron", VhEosHadron),
-                ("smash", VhEosSmash)]
+                ("smash", VhEosSmash), ("azh", VhEosAzh)]
 
 
 class VhGlauberIc(ctypes.Structure):
@@ -415,6 +425,15 @@ def make_eos(eos):
         h.ne, h.nnb, h.nnq, h.e0, h.n0, h.logemin, h.logemax, h.lognmax = eos.hadron
         h.p, h.T, h.mub, h.muq, h.mus = (_ptr(a) for a in keep[:5])
         h.status = st.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    if eos.kind == 6:
+        for name, (ne, nn, emin, nmin, de, dn, v) in zip(
+                ("p1", "p2", "T1", "T2", "mu1", "mu2"), eos.azh):
+            arr = np.ascontiguousarray(v, dtype=np.float64)
+            assert arr.size == ne * nn
+            keep.append(arr)
+            x = getattr(d.azh, name)
+            x.ne, x.nn, x.emin, x.nmin, x.de, x.dn = ne, nn, emin, nmin, de, dn
+            x.v = _ptr(arr)
     if eos.kind == 2:
         for k, a in enumerate(eos.aux):
             arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]

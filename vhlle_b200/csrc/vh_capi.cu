@@ -191,6 +191,17 @@ const char* eos_problem(const vh_eos& e) {
       if (!e.egrid || !e.ngrid || !e.p || !e.T || !e.mub || !e.muq || !e.mus)
         return "EoS3f table needs all seven arrays";
       return nullptr;
+    case VH_EOS_AZH: {
+      const vh_eos::vh_eos_azh::vh_eos_azh_table* t[6] = {&e.azh.p1, &e.azh.p2, &e.azh.T1,
+                                                          &e.azh.T2, &e.azh.mu1, &e.azh.mu2};
+      for (auto* x : t) {
+        if (!size_ok(x->ne, x->nn) || !x->v)
+          return "EoSAZH tables need ne >= 2, nn >= 2, at most 2^30 points and their values";
+        if (!(x->de > 0.) || !(x->dn > 0.) || !(x->emin > 0.))
+          return "EoSAZH tables need de > 0, dn > 0 and emin > 0";
+      }
+      return nullptr;
+    }
     case VH_EOS_SMASH: {
       const vh_eos::vh_eos_smash& h = e.smash;
       if (h.ne < 2 || h.nnb < 2 || h.nnq < 2 || (long long)h.ne * h.nnb * h.nnq > (1LL << 31))
@@ -367,6 +378,27 @@ static vh_status upload_eos(vh_ctx* c, const vh_eos* eos, vh::EosDev& E) {
         }
       E.ch[k] = vh::ChiralAux{x.ne, x.nn, x.emin, x.emax, x.nmin, x.nmax,
                                    buf, buf + n, buf + 2 * n, buf + 3 * n};
+    }
+  }
+  if (eos->kind == VH_EOS_AZH) {
+    const vh_eos::vh_eos_azh::vh_eos_azh_table* t[6] = {
+        &eos->azh.p1, &eos->azh.p2, &eos->azh.T1, &eos->azh.T2, &eos->azh.mu1, &eos->azh.mu2};
+    size_t n = 0;
+    for (auto* x : t) n += (size_t)x->ne * x->nn;
+    double* buf = nullptr;
+    if ((st = dalloc(c, &buf, n)) != VH_OK) return st;
+    e = cudaSuccess;
+    size_t off = 0;
+    for (int q = 0; q < 6; q++) {
+      const size_t m = (size_t)t[q]->ne * t[q]->nn;
+      if (e == cudaSuccess)
+        e = cudaMemcpy(buf + off, t[q]->v, m * sizeof(double), cudaMemcpyHostToDevice);
+      E.az[q] = vh::AzhTab{t[q]->ne, t[q]->nn, t[q]->emin, t[q]->nmin, t[q]->de, t[q]->dn, buf + off};
+      off += m;
+    }
+    if (e != cudaSuccess) {
+      cuda_fail(c, e, "EoS upload");
+      return VH_ERR_CUDA;
     }
   }
   if (eos->kind == VH_EOS_SMASH) {
@@ -852,8 +884,9 @@ vh_status vh_set_con2prim_method(vh_ctx* ctx, int method) {
   if (!ctx) return VH_ERR_ARG;
   if (method != VH_C2P_REFERENCE && method != VH_C2P_TABLE_SLOPE)
     return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_method: unknown method");
-  if (method == VH_C2P_TABLE_SLOPE && ctx->eos.kind == VH_EOS_TABLE3)
-    return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_method: no table slope for the EoS3f kind");
+  if (method == VH_C2P_TABLE_SLOPE && (ctx->eos.kind == VH_EOS_TABLE3 || ctx->eos.kind == VH_EOS_AZH))
+    return fail(ctx, VH_ERR_ARG,
+                "vh_set_con2prim_method: no table slope for the EoS3f and EoSAZH kinds");
   if (method == VH_C2P_TABLE_SLOPE && !(ctx->eos.tol <= 1e-10))
     return fail(ctx, VH_ERR_ARG,
                 "vh_set_con2prim_method: the table slope needs a tight tolerance "

@@ -55,6 +55,14 @@ struct SmashTab {
       *__restrict__ mus;
 };
 
+// one of EoSAZH's six tables (EoSAZHaux, src/eoAZH.cpp:15-56): ne x nn
+// values at [ie * nn + in] on the uniform grids emin + ie de, nmin + in dn
+struct AzhTab {
+  int ne, nn;
+  double emin, nmin, de, dn;
+  const double* __restrict__ v;
+};
+
 struct EosDev {
   int kind;          // 0 conformal gas, 1 EoS1f (e, nb) table, 2 EoSChiral
   double conf_cnst;  // e = cnst T^4 for kind 0
@@ -92,6 +100,7 @@ struct EosDev {
   double uq0;
   HadronTab h;  // kind 4
   SmashTab sm;  // kind 5
+  AzhTab az[6];  // kind 6: p1, p2, T1, T2, mu1, mu2
 };
 
 __device__ __forceinline__ float c2p_guess(const EosDev& E, long long i) {
@@ -395,10 +404,11 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
 // kernels spill more (face kernels 25 % slower on the table kind).
 // EK_TABLE_SL / EK_CHIRAL_SL: the same classes with the table-slope root
 // find (EosDev::slope = 1); EK_TABLE3: EoS3f (kind 3); EK_HADRON:
-// EoSHadron (kind 4, the surface's).
+// EoSHadron (kind 4, the surface's); EK_SMASH: EoSSmash (kind 5, the
+// surface's); EK_AZH: EoSAZH (kind 6).
 enum {
   EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4, EK_TABLE3 = 5,
-  EK_HADRON = 6, EK_SMASH = 7
+  EK_HADRON = 6, EK_SMASH = 7, EK_AZH = 8
 };
 __host__ __device__ constexpr bool ek_chiral(int ek) { return ek == EK_CHIRAL || ek == EK_CHIRAL_SL; }
 __host__ __device__ constexpr bool ek_slope(int ek) { return ek == EK_TABLE_SL || ek == EK_CHIRAL_SL; }
@@ -610,9 +620,80 @@ __device__ __forceinline__ void eos_smash(const SmashTab& H, double e, double nb
   }
 }
 
+// EoSAZHaux::get, src/eoAZH.cpp:58-83: bilinear in the cell of (e, nb),
+// the cell clamped to the table (outside it the edge cell extrapolates)
+__device__ __forceinline__ double azh_get(const AzhTab& t, double e, double nb) {
+  if (e <= 0.) return 0.0;
+  int ie = (int)((e - t.emin) / t.de);
+  int in = (int)((nb - t.nmin) / t.dn);
+  if (ie < 0) ie = 0;
+  if (in < 0) in = 0;
+  if (ie > t.ne - 2) ie = t.ne - 2;
+  if (in > t.nn - 2) in = t.nn - 2;
+  const double em = (e - t.emin - ie * t.de) / t.de;
+  const double nm = (nb - t.nmin - in * t.dn) / t.dn;
+  const double we[2] = {1. - em, em};
+  const double wn[2] = {1. - nm, nm};
+  double value = 0.0;
+#pragma unroll
+  for (int je = 0; je < 2; je++)
+#pragma unroll
+    for (int jn = 0; jn < 2; jn++)
+      value += we[je] * wn[jn] * __ldg(t.v + (long long)(ie + je) * t.nn + (in + jn));
+  return value;
+}
+
+// EoSAZHaux::getLow, src/eoAZH.cpp:85-102: below the table's e range, the
+// first row linear in nb, scaled by e / emin.  (The reference exits when
+// (nb - nmin) / dn > 10000; here the clamped first-row cell extrapolates.)
+__device__ __forceinline__ double azh_low(const AzhTab& t, double e, double nb) {
+  if (e <= 0.) return 0.0;
+  int in = (int)((nb - t.nmin) / t.dn);
+  if (in < 0) in = 0;
+  if (in > t.nn - 2) in = t.nn - 2;
+  const double nm = (nb - t.nmin - in * t.dn) / t.dn;
+  const double wn[2] = {1. - nm, nm};
+  const double value = wn[0] * __ldg(t.v + in) + wn[1] * __ldg(t.v + in + 1);
+  return value * e / t.emin;
+}
+
+// EoSAZH::eos / ::p, src/eoAZH.cpp:123-150: the second table set above the
+// first p table's e range, the first inside it, getLow below; p and T at
+// |nb|, muB at nb; muQ = muS = 0
+template <bool WANT_T>
+__device__ __forceinline__ void eos_azh(const EosDev& E, double e, double nb, double& T,
+                                        double& mub, double& p) {
+  const AzhTab* a = E.az;
+  const double anb = fabs(nb);
+  T = mub = 0.;
+  if (e > a[0].emin + a[0].de * (a[0].ne - 1)) {
+    p = azh_get(a[1], e, anb);
+    if (WANT_T) {
+      T = azh_get(a[3], e, anb);
+      mub = azh_get(a[5], e, nb);
+    }
+  } else if (e > a[0].emin) {
+    p = azh_get(a[0], e, anb);
+    if (WANT_T) {
+      T = azh_get(a[2], e, anb);
+      mub = azh_get(a[4], e, nb);
+    }
+  } else {
+    p = azh_low(a[0], e, anb);
+    if (WANT_T) {
+      T = azh_low(a[2], e, anb);
+      mub = azh_low(a[4], e, nb);
+    }
+  }
+}
+
 template <int EK = EK_ANY>
 __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
   double T, mub, mus, p;
+  if (EK == EK_AZH || (EK == EK_ANY && E.kind == 6)) {
+    eos_azh<false>(E, e, nb, T, mub, p);
+    return p;
+  }
   if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
     double muq;
     eos_smash<false>(E.sm, e, nb, T, mub, muq, mus, p);
@@ -642,7 +723,9 @@ template <int EK = EK_ANY>
 __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, double& T,
                                          double& mub, double& mus, double& p) {
   mus = 0.;
-  if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
+  if (EK == EK_AZH || (EK == EK_ANY && E.kind == 6)) {
+    eos_azh<true>(E, e, nb, T, mub, p);
+  } else if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
     double muq;
     eos_smash<true>(E.sm, e, nb, T, mub, muq, mus, p);
   } else if (EK == EK_HADRON || (EK == EK_ANY && E.kind == 4)) {

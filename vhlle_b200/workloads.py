@@ -138,6 +138,26 @@ class EosTable:
     # kind 5 (EoSSmash): (ne, nnb, nnq) and the uniform grids' values; p, T,
     # mub, muq, mus at [inq + nnq*inb + nnq*nnb*ie]
     smash: Optional[tuple] = None
+    # kind 6 (EoSAZH): six tables p1, p2, T1, T2, mu1, mu2, each
+    # (ne, nn, emin, nmin, de, dn, values[ie * nn + in])
+    azh: Optional[tuple] = None
+
+    def write_azh(self, directory: str) -> None:
+        """directory/eos/azhydro0p2/aa{1,2}_{p,t,mb}.dat, the files EoSAZH
+        reads from its working directory (src/eoAZH.cpp:110-117), in the
+        EoSAZHaux format: ``nmin emin``, ``dn de nn-1 ne-1``, then the values
+        with e outer and nb inner (src/eoAZH.cpp:31-50); 17 significant
+        digits."""
+        assert self.kind == 6
+        d = os.path.join(directory, "eos", "azhydro0p2")
+        os.makedirs(d, exist_ok=True)
+        names = ("aa1_p", "aa2_p", "aa1_t", "aa2_t", "aa1_mb", "aa2_mb")
+        for name, (ne, nn, emin, nmin, de, dn, v) in zip(names, self.azh):
+            with open(os.path.join(d, name + ".dat"), "w") as f:
+                f.write("%r %r\n%r %r %d %d\n" % (nmin, emin, dn, de, nn - 1, ne - 1))
+                v = np.asarray(v, dtype=np.float64).reshape(ne, nn)
+                for row in v:
+                    f.write(" ".join("%r" % float(x) for x in row) + "\n")
 
     def write_chiral(self, directory: str) -> None:
         """directory/eos/chiralsmall.dat and chiraleos.dat, the files
@@ -365,6 +385,27 @@ def smash_eos_table(ne: int = 101, nnb: int = 51, nnq: int = 51) -> EosTable:
     return EosTable(kind=5, p=flat(0.14 * E + 0.3 * B * B + 0.05 * Qc * Qc),
                     T=flat(0.12 + 0.05 * E - 0.02 * B * B), mub=flat(0.9 * B),
                     muq=flat(0.2 * Qc), mus=flat(0.25 * B), smash=((ne, nnb, nnq), (eg, bg, qg)))
+
+
+def azh_eos_table(ne1: int = 401, ne2: int = 301, nn: int = 51) -> EosTable:
+    """A synthetic EoS in the reference's EoSAZH format (eosType 2, six
+    EoSAZHaux tables): the first set on e = 0.01 + 0.005 ie GeV/fm^3 (up to
+    2.01), the second on e = 2 + 0.5 ie (up to 152), both on nb = 0.01 in
+    fm^-3 (0 .. 0.5); p = e/3 - 0.15 e / (1 + e) + 0.05 nb^2 / (1 + e),
+    T = 0.16 e^(1/4) (1 - 0.2 nb), mu_B = 0.8 nb / sqrt(0.3 + e).  Below the
+    first set (e < 0.01) EoSAZH scales its first row by e / emin."""
+    def fill(f, ne, emin, de):
+        E, B = np.meshgrid(emin + de * np.arange(ne), 0.01 * np.arange(nn), indexing="ij")
+        return np.ascontiguousarray(f(E, B), dtype=np.float64).reshape(-1)
+    fp = lambda E, B: E / 3.0 - 0.15 * E / (1.0 + E) + 0.05 * B * B / (1.0 + E)  # noqa: E731
+    fT = lambda E, B: 0.16 * E ** 0.25 * (1.0 - 0.2 * B)  # noqa: E731
+    fm = lambda E, B: 0.8 * B / np.sqrt(0.3 + E)  # noqa: E731
+    sets = ((ne1, 0.01, 0.005), (ne2, 2.0, 0.5))
+    tabs = []
+    for f in (fp, fT, fm):
+        for ne, emin, de in sets:
+            tabs.append((ne, nn, emin, 0.0, de, 0.01, fill(f, ne, emin, de)))
+    return EosTable(kind=6, azh=tuple(tabs))
 
 
 def eos3f_table(ne: int = 120, emin: float = 1e-4, emax: float = 1e3) -> EosTable:
