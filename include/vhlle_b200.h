@@ -34,7 +34,7 @@ extern "C" {
 /* 2: vh_eos gained the aux tables of VH_EOS_CHIRAL (a caller built against
  * version 1 passes a shorter vh_eos);
  * 3: vh_grid gained dz, vh_eos the EoS3f, EoSHadron, EoSSmash and EoSAZH
- * members (kinds 3-6) */
+ * members (kinds 3-6); kind 7 (EoSCMFe) uses aux */
 #define VH_ABI_VERSION 3
 
 typedef int vh_status;
@@ -88,7 +88,13 @@ typedef struct vh_grid {
  *  kind VH_EOS_SMASH:     EoSSmash (src/eoSmash.cpp, eosTypeHadron 1):
  *                         `smash` below; both for vh_set_surface_eos only;
  *  kind VH_EOS_AZH:       EoSAZH (src/eoAZH.cpp, eosType 2): six uniform
- *                         (e, nb) tables, `azh` below.
+ *                         (e, nb) tables, `azh` below;
+ *  kind VH_EOS_CMFE:      EoSCMFe (src/eoCMFe.cpp, eosType 4): aux[0] the
+ *                         small table (eos/cmfe_small.dat), aux[1] the big
+ *                         one (eos/cmfe.dat), converted to GeV/fm^3, fm^-3
+ *                         and GeV as its constructor does, in the aux layout
+ *                         [in * ne + ie]; a NaN entry is allowed (the
+ *                         reference then returns zeros).
  * Host arrays are copied at vh_create (vh_set_surface_eos). */
 #define VH_EOS_CONFORMAL 0
 #define VH_EOS_TABLE 1
@@ -97,6 +103,7 @@ typedef struct vh_grid {
 #define VH_EOS_HADRON 4
 #define VH_EOS_SMASH 5
 #define VH_EOS_AZH 6
+#define VH_EOS_CMFE 7
 /* One EoSaux table (src/eoChiral.cpp:33-97) after its constructor's unit
  * conversions: the e and nb grids are uniform from emin to emax (GeV/fm^3)
  * and nmin to nmax (fm^-3) with ne, nn >= 2 points; p (GeV/fm^3), T, muB,
@@ -111,7 +118,7 @@ typedef struct vh_eos {
   double conf_cnst;
   int ne, nn;
   const double *egrid, *ngrid, *p, *T, *mub;
-  vh_eos_aux aux[2]; /* VH_EOS_CHIRAL only */
+  vh_eos_aux aux[2]; /* VH_EOS_CHIRAL and VH_EOS_CMFE only */
   const double *muq, *mus; /* VH_EOS_TABLE3 only */
   /* VH_EOS_HADRON only: the file's header ne nnb nnq e0 n0 logemin logemax
    * lognmax (src/eoHadron.cpp:19) and its tables p, T, muB, muQ, muS and

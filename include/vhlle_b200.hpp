@@ -15,6 +15,7 @@
 #pragma once
 
 #include <algorithm>
+#include <limits>
 #include <cmath>
 #include <cstdint>
 #include <cstdlib>
@@ -518,6 +519,113 @@ class EoSAZH : public EoS {
     vh_eos d{};
     d.kind = VH_EOS_AZH;
     d.azh = {t_[0].desc(), t_[1].desc(), t_[2].desc(), t_[3].desc(), t_[4].desc(), t_[5].desc()};
+    return d;
+  }
+};
+
+// EoSCMFe (src/eoCMFe.cpp): the reference driver's eosType 4.  Reads
+// dir/eos/cmfe_small.dat (1501 x 501) and dir/eos/cmfe.dat (4001 x 401): a
+// header line, then e n T p s muB muS rows with e outer (NAN allowed),
+// converted to GeV/fm^3, fm^-3 and GeV as its constructor does; the
+// lookup is EoSChiral's with a cutoff at e = 2e-2 and a NaN pressure
+// replaced; the device evaluates the same tables.
+class EoSCMFe : public EoS {
+  static constexpr double kEps0 = 146.51751415742 * 0.87326281;
+  static constexpr double kN0 = 0.15891 * 0.87272727;
+  struct Aux {
+    int ne, nn;
+    double emin = 0., emax = 0., nmin = 0., nmax = 0.;
+    std::vector<double> p, T, mub, mus;  // [in * ne + ie]
+    Aux(const std::string& path, int Ne, int Nn) : ne(Ne), nn(Nn) {
+      std::ifstream fin(path);
+      if (!fin.good()) throw Error(VH_ERR_ARG, "EoSCMFe: I/O error with " + path);
+      fin.ignore(1000, '\n');
+      const size_t n = (size_t)ne * nn;
+      for (auto* t : {&p, &T, &mub, &mus}) t->resize(n);
+      auto num = [&fin]() {
+        std::string w;
+        fin >> w;
+        return w == "NAN" ? std::numeric_limits<double>::quiet_NaN() : std::atof(w.c_str());
+      };
+      double e0 = 0., e1 = 0., n0 = 0., n1 = 0.;
+      for (int ie = 0; ie < ne; ie++)
+        for (int in = 0; in < nn; in++) {
+          const size_t k = (size_t)in * ne + ie;
+          const double e = num() * kEps0 / 1000.0, nb = num() * kN0;
+          T[k] = num() / 1000.0;
+          p[k] = num() * kEps0 / 1000.0;
+          num();  // s
+          mub[k] = num() / 1000.0;
+          mus[k] = num() / 1000.0;
+          if (ie == 0) e0 = e;
+          if (ie == ne - 1) e1 = e;
+          if (in == 0) n0 = nb;
+          if (in == nn - 1) n1 = nb;
+        }
+      if (!fin) throw Error(VH_ERR_ARG, "EoSCMFe: truncated table " + path);
+      emin = e0;
+      emax = e1;
+      nmin = n0;
+      nmax = n1;
+    }
+    void get(double e, double nb, double& pp, double& TT, double& mb, double& ms) const {
+      if (e < 2e-2) {
+        TT = mb = ms = pp = 0.;
+        return;
+      }
+      const double de = (emax - emin) / (ne - 1), dn = (nmax - nmin) / (nn - 1);
+      int ie = (int)((e - emin) / de), in = (int)((nb - nmin) / dn);
+      ie = std::min(std::max(ie, 0), ne - 2);
+      in = std::min(std::max(in, 0), nn - 2);
+      const double em = e - emin - ie * de, nm = nb - nmin - in * dn;
+      const double we[2] = {1. - em / de, em / de}, wn[2] = {1. - nm / dn, nm / dn};
+      TT = mb = ms = pp = 0.0;
+      for (int je = 0; je < 2; je++)
+        for (int jn = 0; jn < 2; jn++) {
+          const size_t k = (size_t)(in + jn) * ne + (ie + je);
+          pp += we[je] * wn[jn] * p[k];
+          TT += we[je] * wn[jn] * T[k];
+          mb += we[je] * wn[jn] * mub[k];
+          ms += we[je] * wn[jn] * mus[k];
+        }
+      if (std::isnan(pp)) {
+        if (e > 0.8 * kEps0 || nb > 40. * kN0) {
+          pp = 0.2964 * e;
+          TT = 0.15120476935 * std::pow(e, 0.25);
+          mb = ms = 0.0;
+        } else {
+          TT = mb = ms = pp = 0.;
+        }
+      }
+      if (pp < 0.0) pp = 0.0;
+    }
+    vh_eos_aux desc() const {
+      return {ne, nn, emin, emax, nmin, nmax, p.data(), T.data(), mub.data(), mus.data()};
+    }
+  };
+  Aux small_, big_;
+
+ public:
+  explicit EoSCMFe(const std::string& dir)
+      : small_(dir + "/eos/cmfe_small.dat", 1501, 501), big_(dir + "/eos/cmfe.dat", 4001, 401) {}
+  void eos(double e, double nb, double, double, double& T, double& mub, double& muq,
+           double& mus, double& p) const override {
+    if (e < 15 * kEps0 / 1000.0 && nb < 5 * kN0)
+      small_.get(e, nb, p, T, mub, mus);
+    else if (e < 0.8 * kEps0 && nb < 40. * kN0)
+      big_.get(e, nb, p, T, mub, mus);
+    else {
+      p = 0.2964 * e;
+      T = 0.15120476935 * std::pow(e, 0.25);
+      mub = mus = 0.0;
+    }
+    muq = 0.0;
+  }
+  vh_eos descriptor() const override {
+    vh_eos d{};
+    d.kind = VH_EOS_CMFE;
+    d.aux[0] = small_.desc();
+    d.aux[1] = big_.desc();
     return d;
   }
 };

@@ -290,7 +290,7 @@ class _EosHolder:
                 x = self.s.az[k]
                 x.ne, x.nn, x.emin, x.nmin, x.de, x.dn = ne, nn, emin, nmin, de, dn
                 x.v = _ptr(arr)
-        if eos.kind == 2:
+        if eos.kind in (2, 7):
             for k, a in enumerate(eos.aux):
                 arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
                 self.keep += arrs
@@ -546,6 +546,10 @@ class RefRun:
             self._tmp = tempfile.TemporaryDirectory()
             eos_file = self._tmp.name
             setup.eos.write_azh(eos_file)
+        if setup.eos.kind == 7 and eos_file is None:  # the directory that holds eos/
+            self._tmp = tempfile.TemporaryDirectory()
+            eos_file = self._tmp.name
+            setup.eos.write_cmfe(eos_file)
         bounds = np.array(g.bounds(), dtype=np.float64)
         tr = np.array(setup.tr_vector(), dtype=np.float64)
         self.h = self.lib.ref_create(g.nx, g.ny, g.nz, _ptr(bounds), setup.tau0, setup.dt,

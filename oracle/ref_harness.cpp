@@ -35,6 +35,7 @@
 #include "eoHadron.h"
 #include "eoSmash.h"
 #include "eoAZH.h"
+#include "eoCMFe.h"
 #include "fld.h"
 #include "hdo.h"
 #include "inc.h"
@@ -121,9 +122,10 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
       delete r;
       return nullptr;
     }
-  } else if (eos_kind == 6) {
-    // EoSAZH reads eos/azhydro0p2/aa{1,2}_{p,t,mb}.dat relative to the
-    // working directory (src/eoAZH.cpp:110-117), as EoSChiral does
+  } else if (eos_kind == 6 || eos_kind == 7) {
+    // EoSAZH reads eos/azhydro0p2/aa{1,2}_{p,t,mb}.dat, EoSCMFe
+    // eos/cmfe.dat and eos/cmfe_small.dat, relative to the working directory
+    // (src/eoAZH.cpp:110-117, src/eoCMFe.cpp:194-197), as EoSChiral does
     char cwd[4096];
     if (!getcwd(cwd, sizeof cwd) || chdir(eos_file) != 0) {
       delete r;
@@ -132,7 +134,10 @@ void *ref_create(int nx, int ny, int nz, const double *bounds /*6*/,
     std::streambuf *old = std::cout.rdbuf();
     std::ostringstream quiet;
     std::cout.rdbuf(quiet.rdbuf());
-    r->eos = new EoSAZH();
+    if (eos_kind == 6)
+      r->eos = new EoSAZH();
+    else
+      r->eos = new EoSCMFe();
     std::cout.rdbuf(old);
     if (chdir(cwd) != 0) {
       delete r->eos;

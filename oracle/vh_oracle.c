@@ -106,10 +106,17 @@ static void eos1f(const or_eos *E, double e, double nb, double *T, double *mub,
   *mub = smu;
 }
 
-/* EoSaux::get, src/eoChiral.cpp:99-130 (EoSaux::p, :132-151, is its p) */
-static void chiral_aux(const or_aux *A, double e, double nb, double *p,
-                       double *T, double *mub, double *mus) {
-  if (e < 0.) {
+/* EoSCMFe's constants, src/eoCMFe.h:10-11 */
+#define CMFE_EPS0 (146.51751415742 * 0.87326281)
+#define CMFE_N0 (0.15891 * 0.87272727)
+
+/* EoSaux::get, src/eoChiral.cpp:99-130 (EoSaux::p, :132-151, is its p);
+ * with cmfe, EoSCMFeaux::get / ::p (src/eoCMFe.cpp:121-189): zeros below
+ * EPS_CUTOFF = 2e-2 and a NaN pressure replaced after the interpolation */
+static void chiral_aux_x(const or_aux *A, int cmfe, int crmath, double e,
+                         double nb, double *p, double *T, double *mub,
+                         double *mus) {
+  if (cmfe ? e < 2e-2 : e < 0.) {
     *T = *mub = *mus = *p = 0.;
     return;
   }
@@ -134,11 +141,39 @@ static void chiral_aux(const or_aux *A, double e, double nb, double *p,
       sb += we[je] * wn[jn] * A->mub[k];
       ss += we[je] * wn[jn] * A->mus[k];
     }
+  if (cmfe && isnan(sp)) {
+    if (e > 0.8 * CMFE_EPS0 || nb > 40. * CMFE_N0) {
+      sp = 0.2964 * e;
+      sT = 0.15120476935 * (crmath ? or_root4_cr(e) : pow(e, 0.25));
+      sb = ss = 0.0;
+    } else {
+      sT = sb = ss = sp = 0.;
+    }
+  }
   if (sp < 0.0) sp = 0.0;
   *p = sp;
   *T = sT;
   *mub = sb;
   *mus = ss;
+}
+
+static void chiral_aux(const or_aux *A, double e, double nb, double *p,
+                       double *T, double *mub, double *mus) {
+  chiral_aux_x(A, 0, 0, e, nb, p, T, mub, mus);
+}
+
+/* EoSCMFe::eos, src/eoCMFe.cpp:204-217 (muq = 0; ::p, :219-226, is its p) */
+static void eos_cmfe(const or_eos *E, double e, double nb, double *T,
+                     double *mub, double *mus, double *p) {
+  if (e < 15 * CMFE_EPS0 / 1000.0 && nb < 5 * CMFE_N0)
+    chiral_aux_x(&E->aux[0], 1, E->crmath, e, nb, p, T, mub, mus);
+  else if (e < 0.8 * CMFE_EPS0 && nb < 40. * CMFE_N0)
+    chiral_aux_x(&E->aux[1], 1, E->crmath, e, nb, p, T, mub, mus);
+  else {
+    *p = 0.2964 * e;
+    *T = 0.15120476935 * (E->crmath ? or_root4_cr(e) : pow(e, 0.25));
+    *mub = *mus = 0.0;
+  }
 }
 
 /* EoSChiral::eos, src/eoChiral.cpp:159-170 (muq = 0) */
@@ -425,6 +460,8 @@ static void eos_eval5(const or_eos *E, double e, double nb, double *T,
     eos_chiral(E, e, nb, T, mub, mus, p);
   } else if (E->kind == 6) {
     eos_azh(E, e, nb, T, mub, p);
+  } else if (E->kind == 7) {
+    eos_cmfe(E, e, nb, T, mub, mus, p);
   } else {
     eos1f(E, e, nb, T, mub, p);
   }
@@ -463,6 +500,10 @@ static double eos_p(const or_eos *E, double e, double nb) {
   }
   if (E->kind == 2) {
     eos_chiral(E, e, nb, &T, &mub, &mus, &p);
+    return p;
+  }
+  if (E->kind == 7) {
+    eos_cmfe(E, e, nb, &T, &mub, &mus, &p);
     return p;
   }
   if (E->kind == 6) {  /* EoSAZH::p, src/eoAZH.cpp:142-150: eos's p */

@@ -35,7 +35,8 @@ typedef struct or_grid {
  * kind 1: EoS1f (e, nb) table, src/eo1.cpp:21-123, p/T/mub[ie + ne*inb]
  * kind 2: EoSChiral (aux below); kind 3: EoS3f (muq, mus below);
  * kind 4: EoSHadron, kind 5: EoSSmash (hadronic EoS of the freeze-out surface)
- * kind 6: EoSAZH (six uniform (e, nb) tables, az below) */
+ * kind 6: EoSAZH (six uniform (e, nb) tables, az below)
+ * kind 7: EoSCMFe (aux below: cmfe_small, cmfe) */
 /* One EoSaux table of EoSChiral (src/eoChiral.cpp:33-97), converted to
  * GeV/fm^3, fm^-3 and GeV as its constructor does: uniform grids from emin
  * to emax and nmin to nmax, p/T/mub/mus[in * ne + ie]. */
@@ -54,7 +55,7 @@ typedef struct or_eos {
    * (src/rmn.cpp:96).  A smaller value gives the tight-tolerance oracle the
    * learned-guess path is checked against. */
   double tol;
-  or_aux aux[2]; /* kind 2: chiralsmall, chiraleos */
+  or_aux aux[2]; /* kind 2: chiralsmall, chiraleos; kind 7: cmfe_small, cmfe */
   int crmath; /* as or_trc.crmath, for EoSChiral's power law and
                * EoSHadron's logarithms (or_log_cr) */
   /* kind 3 (EoS3f, src/eo3.cpp): egrid[ne], ngrid[nn] (one grid for nb, nq,

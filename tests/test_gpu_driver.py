@@ -238,24 +238,27 @@ def test_cpp_driver_chiral_eos_equals_oracle(tmp_path):
     assert not bad, bad
 
 
-def test_cpp_driver_azh_eos_equals_oracle(tmp_path):
-    """vhlle_run with eosType 2 and the EoSAZH tables under ./eos/azhydro0p2
-    (src/main.cpp:293-294, src/eoAZH.cpp:110-117) ends on the oracle's grid,
-    bit for bit."""
+@pytest.mark.parametrize("eos_type", [2, 4], ids=["EoSAZH", "EoSCMFe"])
+def test_cpp_driver_table_eos_equals_oracle(tmp_path, eos_type):
+    """vhlle_run with eosType 2 (EoSAZH, tables under ./eos/azhydro0p2,
+    src/main.cpp:293-294, src/eoAZH.cpp:110-117) or 4 (EoSCMFe, ./eos/cmfe.dat
+    and ./eos/cmfe_small.dat, src/main.cpp:297-298, src/eoCMFe.cpp:194-197)
+    ends on the oracle's grid, bit for bit."""
     import subprocess
     from vhlle_b200 import build as B
     drv = B.build_driver()
-    setup = W.glauber3d_nb_setup(17, 17, 9, eos=W.azh_eos_table())
-    setup.eos.write_azh(str(tmp_path))
+    eos = W.azh_eos_table() if eos_type == 2 else W.cmfe_eos_table()
+    setup = W.glauber3d_nb_setup(17, 17, 9, eos=eos)
+    (eos.write_azh if eos_type == 2 else eos.write_cmfe)(str(tmp_path))
     ic = str(tmp_path / "ic.vhb")
     W.write_snapshot(ic, setup.grid, setup.tau0, setup.dt, W.initial_snapshot_state(setup))
     params = str(tmp_path / "params.txt")
     tau_max = setup.tau0 + 3.5 * setup.dt
-    W.write_params(params, setup, tauMax=tau_max, tauGridResize=100.0, eosType=2)
+    W.write_params(params, setup, tauMax=tau_max, tauGridResize=100.0, eosType=eos_type)
     run = subprocess.run([drv, "-params", params, "-ISinput", ic, "-outputDir", "out"],
                          capture_output=True, text=True, timeout=300, cwd=str(tmp_path))
     assert run.returncode == 0, run.stdout[-2000:] + run.stderr
-    assert "hydro EoS: EoSAZH" in run.stdout
+    assert ("hydro EoS: " + ("EoSAZH" if eos_type == 2 else "EoSCMFe")) in run.stdout
     o = P.OracleRun(setup)
     g = setup.grid
     while True:

@@ -434,7 +434,7 @@ def make_eos(eos):
             x = getattr(d.azh, name)
             x.ne, x.nn, x.emin, x.nmin, x.de, x.dn = ne, nn, emin, nmin, de, dn
             x.v = _ptr(arr)
-    if eos.kind == 2:
+    if eos.kind in (2, 7):
         for k, a in enumerate(eos.aux):
             arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (a.p, a.T, a.mub, a.mus)]
             keep += arrs

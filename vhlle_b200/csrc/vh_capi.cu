@@ -222,6 +222,7 @@ const char* eos_problem(const vh_eos& e) {
       return nullptr;
     }
     case VH_EOS_CHIRAL:
+    case VH_EOS_CMFE:
       for (const vh_eos_aux& x : e.aux) {
         if (!size_ok(x.ne, x.nn) || !x.p || !x.T || !x.mub || !x.mus)
           return "chiral EoS table missing, smaller than 2 x 2 or above 2^30 points";
@@ -364,7 +365,7 @@ static vh_status upload_eos(vh_ctx* c, const vh_eos* eos, vh::EosDev& E) {
     E.iq0 = ix;
     E.uq0 = (0. - eos->ngrid[k1]) / (eos->ngrid[k2] - eos->ngrid[k1]);
   }
-  if (eos->kind == VH_EOS_CHIRAL) {
+  if (eos->kind == VH_EOS_CHIRAL || eos->kind == VH_EOS_CMFE) {
     for (int k = 0; k < 2; k++) {
       const vh_eos_aux& x = eos->aux[k];
       const size_t n = (size_t)x.ne * x.nn;
@@ -884,9 +885,10 @@ vh_status vh_set_con2prim_method(vh_ctx* ctx, int method) {
   if (!ctx) return VH_ERR_ARG;
   if (method != VH_C2P_REFERENCE && method != VH_C2P_TABLE_SLOPE)
     return fail(ctx, VH_ERR_ARG, "vh_set_con2prim_method: unknown method");
-  if (method == VH_C2P_TABLE_SLOPE && (ctx->eos.kind == VH_EOS_TABLE3 || ctx->eos.kind == VH_EOS_AZH))
+  if (method == VH_C2P_TABLE_SLOPE && (ctx->eos.kind == VH_EOS_TABLE3 || ctx->eos.kind == VH_EOS_AZH ||
+                                       ctx->eos.kind == VH_EOS_CMFE))
     return fail(ctx, VH_ERR_ARG,
-                "vh_set_con2prim_method: no table slope for the EoS3f and EoSAZH kinds");
+                "vh_set_con2prim_method: no table slope for the EoS3f, EoSAZH and EoSCMFe kinds");
   if (method == VH_C2P_TABLE_SLOPE && !(ctx->eos.tol <= 1e-10))
     return fail(ctx, VH_ERR_ARG,
                 "vh_set_con2prim_method: the table slope needs a tight tolerance "

@@ -146,7 +146,7 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
                  "vh_step_noalloc: grid exceeds VH_NOALLOC_MAX_CELLS (32768 cells); "
                  "use vh_create/vh_step for larger grids");
   if (eos_dev->kind == VH_EOS_TABLE3 || eos_dev->kind == VH_EOS_HADRON ||
-      eos_dev->kind == VH_EOS_SMASH || eos_dev->kind == VH_EOS_AZH)
+      eos_dev->kind == VH_EOS_SMASH || eos_dev->kind == VH_EOS_AZH || eos_dev->kind == VH_EOS_CMFE)
     return nfail(VH_ERR_ARG, "vh_step_noalloc: this EoS kind needs vh_create");
   if (const char* why = vh::eos_problem(*eos_dev)) {
     snprintf(g_msg, sizeof g_msg, "vh_step_noalloc: %s", why);

@@ -319,11 +319,19 @@ __device__ __forceinline__ void eos1f(const EosDev& E, double e, double nb,
 // step.  (int) of a double saturates here and gives INT_MIN on the host
 // for a large negative quotient alike; the region tests of eos_chiral keep
 // positive quotients below the table size.
-template <bool WANT_T, bool WANT_D = false>
+// EoSCMFe's constants (src/eoCMFe.h:10-11, src/eoCMFe.cpp:34-37)
+#define VH_CMFE_EPS0 (146.51751415742 * 0.87326281)
+#define VH_CMFE_N0 (0.15891 * 0.87272727)
+
+// CMFE: EoSCMFeaux::get / ::p (src/eoCMFe.cpp:121-189), the same lookup
+// with e below EPS_CUTOFF = 2e-2 giving zeros and a NaN pressure (a NaN
+// table entry) replaced: zeros inside the tables' region, the conformal
+// fallback outside it.
+template <bool WANT_T, bool WANT_D = false, bool CMFE = false>
 __device__ __forceinline__ void chiral_aux(const ChiralAux& A, double e, double nb, double& p,
                                            double& T, double& mub, double& mus,
                                            double* dpde = nullptr, double* dpdn = nullptr) {
-  if (e < 0.) {
+  if (CMFE ? e < 2e-2 : e < 0.) {
     T = mub = mus = p = 0.;
     if (WANT_D) *dpde = *dpdn = 0.;
     return;
@@ -370,6 +378,18 @@ __device__ __forceinline__ void chiral_aux(const ChiralAux& A, double e, double 
     mub = sb;
     mus = ss;
   }
+  if (CMFE && isnan(sp)) {
+    if (e > 0.8 * VH_CMFE_EPS0 || nb > 40. * VH_CMFE_N0) {
+      sp = 0.2964 * e;
+      if (WANT_T) {
+        T = 0.15120476935 * crm::root4_cr(e);
+        mub = mus = 0.0;
+      }
+    } else {
+      sp = 0.;
+      if (WANT_T) T = mub = mus = 0.;
+    }
+  }
   if (sp < 0.0) sp = 0.0;
   p = sp;
 }
@@ -397,6 +417,25 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
   }
 }
 
+// EoSCMFe::eos / ::p, src/eoCMFe.cpp:204-226 (muq = 0): the small table
+// below 15 EPS_0 / 1000 and 5 N_0, the big one below 0.8 EPS_0 and 40 N_0,
+// the conformal fallback (correctly rounded 1/4 power) above
+template <bool WANT_T>
+__device__ __forceinline__ void eos_cmfe(const EosDev& E, double e, double nb, double& T,
+                                         double& mub, double& mus, double& p) {
+  if (e < 15 * VH_CMFE_EPS0 / 1000.0 && nb < 5 * VH_CMFE_N0) {
+    chiral_aux<WANT_T, false, true>(E.ch[0], e, nb, p, T, mub, mus);
+  } else if (e < 0.8 * VH_CMFE_EPS0 && nb < 40. * VH_CMFE_N0) {
+    chiral_aux<WANT_T, false, true>(E.ch[1], e, nb, p, T, mub, mus);
+  } else {
+    p = 0.2964 * e;
+    if (WANT_T) {
+      T = 0.15120476935 * crm::root4_cr(e);
+      mub = mus = 0.0;
+    }
+  }
+}
+
 // EK selects the EoS kinds compiled in: EK_ANY (every kind, chosen at run
 // time), EK_TABLE (kinds 0 and 1) or EK_CHIRAL (kind 2).  The step's
 // con2prim kernels are instantiated per class: compiled into every
@@ -405,10 +444,10 @@ __device__ __forceinline__ void eos_chiral(const EosDev& E, double e, double nb,
 // EK_TABLE_SL / EK_CHIRAL_SL: the same classes with the table-slope root
 // find (EosDev::slope = 1); EK_TABLE3: EoS3f (kind 3); EK_HADRON:
 // EoSHadron (kind 4, the surface's); EK_SMASH: EoSSmash (kind 5, the
-// surface's); EK_AZH: EoSAZH (kind 6).
+// surface's); EK_AZH: EoSAZH (kind 6); EK_CMFE: EoSCMFe (kind 7).
 enum {
   EK_ANY = -1, EK_TABLE = 1, EK_CHIRAL = 2, EK_TABLE_SL = 3, EK_CHIRAL_SL = 4, EK_TABLE3 = 5,
-  EK_HADRON = 6, EK_SMASH = 7, EK_AZH = 8
+  EK_HADRON = 6, EK_SMASH = 7, EK_AZH = 8, EK_CMFE = 9
 };
 __host__ __device__ constexpr bool ek_chiral(int ek) { return ek == EK_CHIRAL || ek == EK_CHIRAL_SL; }
 __host__ __device__ constexpr bool ek_slope(int ek) { return ek == EK_TABLE_SL || ek == EK_CHIRAL_SL; }
@@ -694,6 +733,10 @@ __device__ __forceinline__ double eos_p(const EosDev& E, double e, double nb) {
     eos_azh<false>(E, e, nb, T, mub, p);
     return p;
   }
+  if (EK == EK_CMFE || (EK == EK_ANY && E.kind == 7)) {
+    eos_cmfe<false>(E, e, nb, T, mub, mus, p);
+    return p;
+  }
   if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
     double muq;
     eos_smash<false>(E.sm, e, nb, T, mub, muq, mus, p);
@@ -725,6 +768,8 @@ __device__ __forceinline__ void eos_eval(const EosDev& E, double e, double nb, d
   mus = 0.;
   if (EK == EK_AZH || (EK == EK_ANY && E.kind == 6)) {
     eos_azh<true>(E, e, nb, T, mub, p);
+  } else if (EK == EK_CMFE || (EK == EK_ANY && E.kind == 7)) {
+    eos_cmfe<true>(E, e, nb, T, mub, mus, p);
   } else if (EK == EK_SMASH || (EK == EK_ANY && E.kind == 5)) {
     double muq;
     eos_smash<true>(E.sm, e, nb, T, mub, muq, mus, p);

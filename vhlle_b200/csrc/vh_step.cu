@@ -1179,6 +1179,7 @@ int launch_step(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
   const bool chiral = a.eos.kind == 2;
   if (a.eos.kind == 3) return launch_step_ek<EK_TABLE3>(a, s, mk);  // EoS3f (no slope method)
   if (a.eos.kind == 6) return launch_step_ek<EK_AZH>(a, s, mk);     // EoSAZH (no slope method)
+  if (a.eos.kind == 7) return launch_step_ek<EK_CMFE>(a, s, mk);    // EoSCMFe (no slope method)
   if (a.eos.slope)
     return chiral ? launch_step_ek<EK_CHIRAL_SL>(a, s, mk) : launch_step_ek<EK_TABLE_SL>(a, s, mk);
   return chiral ? launch_step_ek<EK_CHIRAL>(a, s, mk) : launch_step_ek<EK_TABLE>(a, s, mk);

@@ -703,6 +703,8 @@ void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double t
     k_surf_energy<EK_TABLE3><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
   else if (E.kind == 6)
     k_surf_energy<EK_AZH><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
+  else if (E.kind == 7)
+    k_surf_energy<EK_CMFE><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
   else if (E.kind == 2)
     k_surf_energy<EK_CHIRAL><<<nb, 128, 0, s>>>(g, E, f.Q, f.Qprev, tau, taup, eN, eP);
   else
@@ -765,6 +767,8 @@ void launch_surf_elements(const Geo& g, const EosDev& E, const Fields& f, double
     k_surf_elements<EK_TABLE3><<<kElemGrid, 128, 0, s>>>(a);
   else if (E.kind == 6)
     k_surf_elements<EK_AZH><<<kElemGrid, 128, 0, s>>>(a);
+  else if (E.kind == 7)
+    k_surf_elements<EK_CMFE><<<kElemGrid, 128, 0, s>>>(a);
   else if (E.kind == 2)
     k_surf_elements<EK_CHIRAL><<<kElemGrid, 128, 0, s>>>(a);
   else

@@ -380,6 +380,10 @@ int launch_vorticity(const StepArgs& a, cudaStream_t s) {
     k_vort_T<EK_TABLE3><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
     k_vort_ops<EK_TABLE3><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,
                                                     F.pTh, a.clk, v);
+  } else if (a.eos.kind == 7) {
+    k_vort_T<EK_CMFE><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
+    k_vort_ops<EK_CMFE><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,
+                                                  F.pTh, a.clk, v);
   } else if (a.eos.kind == 6) {
     k_vort_T<EK_AZH><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Qh, a.clk, v.TD);
     k_vort_ops<EK_AZH><<<nb, kVortBlock, 0, s>>>(g, a.eos, F.Q, F.Qprev, F.m2, F.pA, F.pD,

@@ -10,7 +10,8 @@
 // defaults, "CCC"/"UUU" echo).  The hydro EoS is the EoS1f table named by
 // the extra key eos1fFile; else, for eosType 1 (the default), EoSChiral from
 // ./eos/chiraleos.dat and ./eos/chiralsmall.dat as the reference reads them;
-// for eosType 2, EoSAZH from ./eos/azhydro0p2;
+// for eosType 2, EoSAZH from ./eos/azhydro0p2; for eosType 4, EoSCMFe from
+// ./eos/cmfe.dat and ./eos/cmfe_small.dat;
 // else (those files absent, or another eosType) the conformal gas of 47.5
 // degrees of freedom.  The freeze-out EoS (src/main.cpp:304-314) is, for
 // eosTypeHadron 0, EoSHadron from ./eos/eosHadronLog.dat, for eosTypeHadron
@@ -104,6 +105,8 @@ int run(int argc, char** argv) {
                       stat("eos/chiraleos.dat", &sb) == 0 && stat("eos/chiralsmall.dat", &sb) == 0;
   const bool azh = P.eos1fFile.empty() && P.eosType == 2 &&
                    stat("eos/azhydro0p2/aa1_p.dat", &sb) == 0;
+  const bool cmfe = P.eos1fFile.empty() && P.eosType == 4 && stat("eos/cmfe.dat", &sb) == 0 &&
+                    stat("eos/cmfe_small.dat", &sb) == 0;
   vhb::EoS* eos;
   if (!P.eos1fFile.empty())
     eos = new vhb::EoS1f(P.eos1fFile.c_str());
@@ -111,12 +114,15 @@ int run(int argc, char** argv) {
     eos = new vhb::EoSChiral(".");
   else if (azh)  // src/main.cpp:293-294
     eos = new vhb::EoSAZH(".");
+  else if (cmfe)  // src/main.cpp:297-298
+    eos = new vhb::EoSCMFe(".");
   else
     eos = new vhb::EoSConformal(3.0 * deg * M_PI * M_PI / 90.0 / (hbarc * hbarc * hbarc));
   std::cout << "hydro EoS: "
             << (!P.eos1fFile.empty() ? "EoS1f " + P.eos1fFile
                 : chiral ? std::string("EoSChiral (eos/chiraleos.dat, eos/chiralsmall.dat)")
                 : azh    ? std::string("EoSAZH (eos/azhydro0p2)")
+                : cmfe   ? std::string("EoSCMFe (eos/cmfe.dat, eos/cmfe_small.dat)")
                          : std::string("conformal gas"))
             << std::endl;
   vhb::EoS* eosH = eos;

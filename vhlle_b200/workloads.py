@@ -159,6 +159,18 @@ class EosTable:
                 for row in v:
                     f.write(" ".join("%r" % float(x) for x in row) + "\n")
 
+    def write_cmfe(self, directory: str) -> None:
+        """directory/eos/cmfe_small.dat and cmfe.dat, the files EoSCMFe reads
+        from its working directory (src/eoCMFe.cpp:194-197): a header line,
+        then 7 columns (e, n, T, p, s, mu_B, mu_S in the files' units) with e
+        outer and n inner (src/eoCMFe.cpp:83-94), every value exact in 10
+        decimals (a NaN written as nan)."""
+        assert self.kind == 7
+        os.makedirs(os.path.join(directory, "eos"), exist_ok=True)
+        for name, cols, _ in _cmfe_tables():
+            np.savetxt(os.path.join(directory, "eos", name), cols, fmt="%.10f",
+                       header="e n T p s muB muS", comments="# ")
+
     def write_chiral(self, directory: str) -> None:
         """directory/eos/chiralsmall.dat and chiraleos.dat, the files
         EoSChiral reads from its working directory (src/eoChiral.cpp:153-156):
@@ -326,6 +338,54 @@ def chiral_eos() -> EosTable:
     mu_q * (3 / 1000), mu_S / 1000, p * 0.146, grid ends * 0.146 and * 0.15),
     so that the files (write_chiral) and these arrays hold the same doubles."""
     return EosTable(kind=2, aux=tuple(t[2] for t in _chiral_tables()))
+
+
+# EoSCMFe's table sizes (src/eoCMFe.cpp:194-197) and this generator's
+# ranges in the files' units (e in EPS_0 / 1000 GeV/fm^3, n in N_0): the
+# small table covers the region EoSCMFe::eos sends to it (e < 15, n < 5),
+# the big one e < 800, n < 40
+CMFE_TABLES = (("cmfe_small.dat", 1501, 501, 15.0, 5.0), ("cmfe.dat", 4001, 401, 800.0, 40.0))
+CMFE_EPS0 = 146.51751415742 * 0.87326281
+CMFE_N0 = 0.15891 * 0.87272727
+
+
+def _cmfe_tables():
+    """(file name, the file's 7 columns, ChiralAux) per EoSCMFe table; the
+    big table has no model solution (NaN) where n > 36 N_0 and e < 40."""
+    out = []
+    for name, ne, nn, emax_f, nmax_f in CMFE_TABLES:
+        e_f = _q(np.arange(ne) * (emax_f / (ne - 1)))
+        n_f = _q(np.arange(nn) * (nmax_f / (nn - 1)))
+        E, Nb = np.meshgrid(e_f, n_f, indexing="ij")  # [ie][in]
+        T_f = _q(20.0 + 140.0 * (E / 10.0 + 0.05) ** 0.25 * (1.0 - 0.1 * Nb / nmax_f))
+        p_f = _q(E / 3.0 * (1.0 - 0.3 * np.exp(-E / 10.0)) - 0.02 + 0.01 * Nb)
+        s_f = _q((E + p_f) * 7.0 / T_f)
+        mub_f = _q(300.0 * Nb / (1.0 + 0.02 * E))
+        mus_f = _q(15.0 * Nb / (1.0 + E / 10.0))
+        if nmax_f > 5.0:
+            hole = (Nb > 36.0) & (E < 40.0)
+            for a in (T_f, p_f, s_f, mub_f, mus_f):
+                a[hole] = np.nan
+        cols = np.stack([E, Nb, T_f, p_f, s_f, mub_f, mus_f], axis=-1).reshape(-1, 7)
+        # EoSCMFeaux's conversions (src/eoCMFe.cpp:85-92), in the aux layout
+        aux = ChiralAux(ne=ne, nn=nn, emin=e_f[0] * CMFE_EPS0 / 1000.0,
+                        emax=e_f[-1] * CMFE_EPS0 / 1000.0, nmin=n_f[0] * CMFE_N0,
+                        nmax=n_f[-1] * CMFE_N0,
+                        p=np.ascontiguousarray((p_f * CMFE_EPS0 / 1000.0).T).ravel(),
+                        T=np.ascontiguousarray((T_f / 1000.0).T).ravel(),
+                        mub=np.ascontiguousarray((mub_f / 1000.0).T).ravel(),
+                        mus=np.ascontiguousarray((mus_f / 1000.0).T).ravel())
+        out.append((name, cols, aux))
+    return out
+
+
+def cmfe_eos_table() -> EosTable:
+    """A synthetic EoSCMFe (the CMF model's tables are not in the reference
+    tree): smooth T, p, s, mu_B, mu_S over each table's (e, n) grid in the
+    file units (MeV, EPS_0 / 1000, N_0), every value a multiple of 2^-10,
+    converted as the reference's EoSCMFeaux constructor converts them, so
+    that the files (write_cmfe) and these arrays hold the same doubles."""
+    return EosTable(kind=7, aux=tuple(t[2] for t in _cmfe_tables()))
 
 
 def hadron_eos_table(ne: int = 101, nnb: int = 41, nnq: int = 21, e0: float = 1.0,
