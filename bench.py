@@ -201,20 +201,37 @@ def gpu_index_for(local_rank):
     return str(local_rank)
 
 
-def fp64_per_launch(kernel, grid, launches):
-    """FP64 operations (DADD + DMUL + 2 DFMA, ncu's
-    sm__sass_thread_inst_executed_op_d{add,mul,fma}_pred_on) per launch of
-    `kernel` from the committed ncu summary of the same workload's timed
-    steps (profiles/fp64.json: per grid, per kernel, each launch's count in
-    step order), averaged over this run's launches; None if no capture
-    covers them."""
-    p = os.path.join(ROOT, "profiles", "fp64.json")
+# kernels whose work is the listed cells with matter (k_relax_list's list)
+ACTIVE_KERNELS = ("k_is_relax", "k_is_advect")
+
+
+def ncu_per_launch(fname, field, kernel, grid, launches, warmup, active_per_step):
+    """A per-launch ncu figure of `kernel` from a committed summary of the
+    same workload's timed steps (profiles/<fname>: per grid, per kernel,
+    each launch's value in step order; "_capture" holds the capture's
+    warm-up and step counts and its listed cells per step).  Returns
+    (value, basis): the mean over this run's launches when the run starts
+    where the capture did and the capture covers them; otherwise the
+    capture's mean, per listed cell for the kernels that work on the list
+    (times this run's listed cells per step) and per launch for the others;
+    (None, None) without a capture of the grid."""
+    p = os.path.join(ROOT, "profiles", fname)
     if not os.path.exists(p):
-        return None
-    v = json.load(open(p)).get("x".join(map(str, grid)), {}).get(kernel)
-    if not v or len(v["flops_per_launch"]) < launches:
-        return None
-    return float(sum(v["flops_per_launch"][:launches]) / launches)
+        return None, None
+    d = json.load(open(p))
+    key = "x".join(map(str, grid))
+    v = d.get(key, {}).get(kernel)
+    cap = d.get("_capture", {}).get(key)
+    if not v or not v[field] or not cap:
+        return None, None
+    vals = v[field]
+    if cap["warmup"] == warmup and len(vals) >= launches:
+        return float(sum(vals[:launches]) / launches), "ncu, the same launches"
+    m = float(sum(vals) / len(vals))
+    what = "ncu of steps %d-%d" % (cap["warmup"] + 1, cap["warmup"] + cap["steps"])
+    if kernel in ACTIVE_KERNELS:
+        return m / cap["active_cells_per_step"] * active_per_step, what + ", per listed cell"
+    return m, what + ", per launch"
 
 
 def nvtx(name=None):
@@ -227,21 +244,6 @@ def nvtx(name=None):
             torch.cuda.nvtx.range_push(name)
     except Exception:
         pass
-
-
-def traffic_per_launch(kernel, grid, launches):
-    """DRAM bytes (read + write) per launch of `kernel` from the committed
-    ncu summary of the same workload and steps (profiles/traffic.json:
-    per grid, per kernel, the bytes of each launch in step order), averaged
-    over this run's launches; None if no capture covers them."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if not os.path.exists(p):
-        return None
-    d = json.load(open(p)).get("x".join(map(str, grid)), {})
-    v = d.get(kernel)
-    if not v or len(v["bytes_per_launch"]) < launches:
-        return None
-    return float(sum(v["bytes_per_launch"][:launches]) / launches)
 
 
 def cpu_baseline_sample(setup, steps=2):
@@ -743,18 +745,22 @@ def main():
     achieved = alg / avg_s / 1e9
     roofline = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": peak,
                 "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
-                "traffic": traffic_per_launch(dname, args.grid, dn),
+                "traffic": None,
                 "alg_bytes_per_launch": alg, "avg_launch_ms": avg_s * 1e3,
                 "active_cells_per_step": nactive / args.steps,
                 "alg_bytes_rule": KERNEL_BYTES_RULE.get(dname, "")}
     # FP64 co-roofline: the dominant kernel's and the whole step's FP64
     # operations (ncu counts of the same launches) over their CUDA-event
     # time, against a cuBLAS DGEMM measured now
+    act = nactive / args.steps
+    roofline["traffic"], roofline["traffic_basis"] = ncu_per_launch(
+        "traffic.json", "bytes_per_launch", dname, args.grid, dn, args.warmup, act)
     fp64_peak = fp64_peak_tflops(local)
-    fl = fp64_per_launch(dname, args.grid, dn)
+    fl, fl_basis = ncu_per_launch("fp64.json", "flops_per_launch", dname, args.grid, dn,
+                                  args.warmup, act)
     step_fl = 0.0
     for k, (n, _) in prof.items():
-        f = fp64_per_launch(k, args.grid, n)
+        f, _ = ncu_per_launch("fp64.json", "flops_per_launch", k, args.grid, n, args.warmup, act)
         step_fl = None if (f is None or step_fl is None) else step_fl + f * n
     kern_s = sum(t for _, t in prof.values()) / 1e3
     fp64_roofline = {
@@ -765,7 +771,8 @@ def main():
         "step_achieved": None if step_fl is None else step_fl / kern_s / 1e12,
         "step_flops_per_cell_update": None if step_fl is None else step_fl / (cells * args.steps),
         "source": "profiles/fp64.json (ncu sm__sass_thread_inst_executed_op_d{add,mul,fma}_pred_on "
-                  "of the same workload's timed launches; flops = add + mul + 2 fma)"}
+                  "of the same workload's timed launches; flops = add + mul + 2 fma)",
+        "basis": fl_basis}
     if fl is not None:
         fp64_roofline["frac"] = fp64_roofline["achieved"] / fp64_peak
     if step_fl is not None:
