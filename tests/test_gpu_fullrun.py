@@ -15,7 +15,9 @@ the canonical float64 values, so -0.0 == +0.0); the interior totals within
 1e-10 relative; every surface call's element count and nsusp exactly, its
 records' per-column sums within 1e-9 of their magnitude sums (elements
 within 1e-12 of the reference's 15-digit text, see test_gpu_surface) and
-the printed EtotSurf to its 6 digits.
+the printed EtotSurf to its 6 digits.  The totals are summed in another
+order on the device, so the sums that cancel (Px and the flow numerators)
+get an absolute allowance of 1e-12 of the total energy.
 
 zeta/s form 2 evaluates exp(), which the C library rounds correctly in all
 but about one call in 1,300 while the device's exp is always correctly
@@ -75,7 +77,11 @@ def test_gpu_full_run_equals_reference(case):
                               if step == z["nsteps"] else "")
             tot = d.totals()
             t = np.array([tot[n] for n in P.TOTALS])
-            assert _close(t, totals[k], 1e-10).all(), (step, t, totals[k])
+            # 1e-10 relative, and 1e-12 of the total energy for the sums that
+            # cancel (Px, the flow numerators): the device sums in another order
+            ok = np.abs(t - totals[k]) <= (1e-10 * np.maximum(np.abs(t), np.abs(totals[k])) +
+                                           1e-12 * abs(totals[k][0]))
+            assert ok.all(), (step, [n for n, o in zip(P.TOTALS, ok) if not o], t, totals[k])
             assert abs(d.tau - z["tau"][k]) <= 1e-12 * z["tau"][k]
     d.close()
     if arm:

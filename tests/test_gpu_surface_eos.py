@@ -3,14 +3,17 @@ outputSurface and outputCorona swap in, src/fld.cpp:540-542, 885-887) set to
 EoSHadron (VH_EOS_HADRON, src/eoHadron.cpp) or EoSSmash (VH_EOS_SMASH,
 src/eoSmash.cpp) against the oracle, itself equal bit for bit to the
 reference's classes (tests/test_oracle_hadron_eos.py):
-the corona and the surface records within 1e-12 relative (EoSHadron takes
-logarithms, which the device may round differently from the C library in
-the last bit), the totals within 1e-10; the hydro evolution is untouched."""
+the corona and the surface records within 1e-12 relative, with the
+allowances of test_gpu_surface.rec_close_scaled after steps (a near-zero
+dSigma component cancels, and gamma^2 multiplies a last-bit difference of
+the device's cosh/sinh/log/tanh in transformToLab), the totals within
+1e-10; the hydro evolution is untouched."""
 import numpy as np
 import pytest
 
 import pyoracle as P
 from helpers import compare_states, gpu_state_as_oracle
+from test_gpu_surface import rec_close_scaled
 from vhlle_b200 import capi
 from vhlle_b200 import workloads as W
 
@@ -19,6 +22,12 @@ pytestmark = pytest.mark.gpu
 
 def _close(a, b, rtol):
     return np.abs(a - b) <= rtol * np.maximum(np.abs(a), np.abs(b)) + 1e-300
+
+
+def _report(a, b, ok):
+    """The failing records: index, column, both values, u^0."""
+    bad = np.argwhere(~ok)[:6]
+    return [(int(i), int(c), float(a[i, c]), float(b[i, c]), float(a[i, 8])) for i, c in bad]
 
 
 @pytest.mark.parametrize("name", ["hadron", "smash"])
@@ -37,8 +46,8 @@ def test_gpu_surface_eos_equals_oracle(name):
         ro, acc = o.surface(cap=400000)
         rd, info = d.surface()
         assert len(ro) == info["nelements"] > 0 and int(acc["nsusp"]) == info["nsusp"], step
-        ok = _close(rd, ro, 1e-12)
-        assert ok.all(), (step, np.argwhere(~ok)[:5])
+        ok = rec_close_scaled(rd, ro)
+        assert ok.all(), (step, _report(rd, ro, ok))
     t_o, t_d = o.totals(), d.totals()
     for k in t_o:
         assert _close(np.array(t_d[k]), np.array(t_o[k]), 1e-10), (k, t_d[k], t_o[k])
@@ -49,7 +58,8 @@ def test_gpu_surface_eos_equals_oracle(name):
     o2.step(4)
     r2, _ = o2.surface(cap=400000)
     rd2, _ = d.surface()
-    assert _close(rd2, r2, 1e-12).all()
+    ok = rec_close_scaled(rd2, r2)
+    assert ok.all(), _report(rd2, r2, ok)
     d.close()
 
 
