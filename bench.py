@@ -484,9 +484,12 @@ def learned_guess_measure(capi, W, setup, steps, device, mlp):
         iters[mode] = it / c
     _c2p_mode(h, "reference", None)
     out["iters_per_root_find"] = iters
-    out["speedup_mlp_vs_tight"] = out["tight_slope_mlp"] / out["tight"]
-    out["speedup_mlp_vs_tight_slope"] = out["tight_slope_mlp"] / out["tight_slope"]
+    # the network with the reference's Newton, the table slope alone, both
+    # together against the tight path, and what the network adds to the slope
+    out["speedup_mlp_vs_tight"] = out["tight_mlp"] / out["tight"]
     out["speedup_slope_vs_tight"] = out["tight_slope"] / out["tight"]
+    out["speedup_slope_mlp_vs_tight"] = out["tight_slope_mlp"] / out["tight"]
+    out["speedup_mlp_vs_tight_slope"] = out["tight_slope_mlp"] / out["tight_slope"]
     out["unit"] = UNIT
     out["steps"] = steps
     out["workload"] = "%s %dx%dx%d" % (setup.name, setup.grid.nx, setup.grid.ny, setup.grid.nz)
