@@ -515,11 +515,17 @@ def state_error(a, b, fields=("Q", "pi", "Pi")):
     return out
 
 
-def batched_mlp_measure(capi, W, n_events, steps, device, mlp, tau_resize=4.0, nsample=8):
-    """The benchmark metric's numerator and denominator on the
-    event-by-event set (the first n_events seeded events: 61x61x1 ..
+BUMP = "eta/s=0.12, zeta/s Gaussian bump 0.05 at T=0.175 GeV (width 0.02)"
+LARGE = ("201x201x101 on [-20,20]^2 x [-10,10], tau0=0.4, dtau=0.02, eta/s=0.08 + the zeta/s "
+         "bump, shear + bulk + cross terms, nb on the (e, nb) table")
+
+
+def batched_mlp_measure(capi, W, evs, steps, device, mlp, tau_resize=4.0, nsample=8,
+                        physics=BUMP):
+    """The benchmark metric's numerator and denominator on a set of events
+    `evs` (the event-by-event set's first seeded events: 61x61x1 ..
     121x121x61, eta/s = 0.12, the zeta/s bump, the one-shot x2 resize at
-    tau_resize): every event of the set stepped alone (one vh_advance per
+    tau_resize; or the large events): every event of the set stepped alone (one vh_advance per
     driver-loop iteration, event after event) at the reference tolerance and
     at the tight one, against the same events advanced together by one
     vh_batch graph per iteration at the tight tolerance, without and with
@@ -529,7 +535,7 @@ def batched_mlp_measure(capi, W, n_events, steps, device, mlp, tau_resize=4.0, n
     errors: the batched + learned path against the plain tight path
     (bit-identical to the tight oracle, tests/test_gpu_con2prim_tight.py)
     over nsample events (the smallest and the largest)."""
-    evs = W.batch_events(n_events)
+    n_events = len(evs)
     cells = sum(s.grid.ncells for s in evs)
     drv = [(s.dt, s.grid.etamin, s.grid.etamax, s.grid.nz) for s in evs]
     by_size = sorted(range(n_events), key=lambda k: evs[k].grid.ncells)
@@ -590,8 +596,7 @@ def batched_mlp_measure(capi, W, n_events, steps, device, mlp, tau_resize=4.0, n
 
     out = {"events": n_events, "steps": steps, "cells": cells, "unit": UNIT,
            "grids": "%d..%d cells" % (min(s.grid.ncells for s in evs), max(s.grid.ncells for s in evs)),
-           "tau_resize": tau_resize, "tolerance": TIGHT,
-           "physics": "eta/s=0.12, zeta/s Gaussian bump 0.05 at T=0.175 GeV (width 0.02)"}
+           "tau_resize": tau_resize, "tolerance": TIGHT, "physics": physics}
     ms = {}
     ms["plain_reference_tol"], hs = plain("reference")
     for h in hs:
@@ -654,6 +659,8 @@ def main():
     ap.add_argument("--batch-events", type=int, default=256,
                     help="events of the batched + learned-guess measurement (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=20)
+    ap.add_argument("--large-steps", type=int, default=10,
+                    help="steps of the 8 large events' batched leg")
     ap.add_argument("--no-learned-guess", action="store_true")
     ap.add_argument("--vorticity", action="store_true",
                     help="the event with Hydro::enableVorticity (dbeta every step, beta.dat "
@@ -841,7 +848,7 @@ def main():
                        "host_link_gbs: both directions' bytes over the whole time (copies and "
                        "kernels serialised by the step's data dependence)" % SURF_EVERY}
 
-    batch2d = learned = bmlp = None
+    batch2d = learned = bmlp = large = None
     mlp = None
     if not args.no_learned_guess:
         mlp, mlp_info = train_guess_network(capi, W, local)
@@ -850,7 +857,11 @@ def main():
         learned["train"] = mlp_info
     if args.batch_events > 0:
         if mlp is not None:
-            bmlp = batched_mlp_measure(capi, W, args.batch_events, args.batch_steps, local, mlp)
+            bmlp = batched_mlp_measure(capi, W, W.batch_events(args.batch_events),
+                                       args.batch_steps, local, mlp)
+            # the large events (8 of them, 4.1 M cells each: 33 GB resident)
+            large = batched_mlp_measure(capi, W, [W.large_event_setup(k) for k in range(8)],
+                                        args.large_steps, local, mlp, nsample=2, physics=LARGE)
         batch2d = batch_measure(capi, W, 64, 2 * args.batch_steps, local, nz=1)
     if mlp is not None:
         mlp.close()
@@ -874,6 +885,7 @@ def main():
             "roofline": roofline, "step_roofline": step_roofline, "fp64_roofline": fp64_roofline,
             "kernels": kernels,
             "e2e": e2e, "cpu_baseline": cpu, "batched_mlp": bmlp, "batch_2d": batch2d,
+            "batched_mlp_large": large,
             "learned_guess": learned,
             # the step graph's kernels, and per pipelined surface call its
             # nine kernels plus the overflow check (k_surf_keep)
