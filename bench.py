@@ -24,7 +24,17 @@ The JSON line carries, besides the contract keys:
                 every step uploads the state from pinned host memory, steps,
                 and reads the updated state back;
   cpu_baseline  the reference's own C++ step (compiled from its sources,
-                single-threaded) timed on this host over a bounded sample.
+                single-threaded) timed on this host over a bounded sample;
+  fp64_roofline the dominant kernel's and the step's FP64 operations (ncu
+                counts, profiles/fp64.json) over their CUDA-event time,
+                against a cuBLAS DGEMM measured in the same run;
+  batched_mlp   the metric's numerator and denominator on the 256-event
+                set: batched + table slope + learned start point against
+                every event alone, at the tight tolerance, with errors and
+                their noise floor;
+  batched_mlp_large  the same on 8 large events (201x201x101);
+  batch_2d      the batched graph on 64 2+1D events against each alone;
+  learned_guess the con2prim modes on one event with baryon charge.
 """
 from __future__ import annotations
 
