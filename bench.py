@@ -33,7 +33,8 @@ The JSON line carries, besides the contract keys:
                 every event alone, at the tight tolerance, with errors and
                 their noise floor;
   batched_mlp_large  the same on 8 large events (201x201x101);
-  batch_2d      the batched graph on 64 2+1D events against each alone;
+  batch_2d      64 2+1D events batched (the tuner's form, the stage-batched
+                form and a branch per event) against each alone;
   learned_guess the con2prim modes on one event with baryon charge.
 """
 from __future__ import annotations
@@ -108,7 +109,8 @@ def kernel_alg_bytes(prof, cells, nactive):
     if "k_is_advect" in prof:
         out["k_is_advect"] = float(ADVECT_ACTIVE_B) * nactive
     return out
-STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")  # persistent per-cell state
+
+
 STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")  # persistent per-cell state
 
 
@@ -378,22 +380,33 @@ def batch_measure(capi, W, n_events, steps, device, nz=None):
     for k, d in enumerate(drv):
         b.set_driver(k, *d, 4.0)
     b.tune(True)
-    b.advance(16)  # 7 configurations x 2 timed iterations, then the chosen one
+    b.advance(16)  # 8 configurations x 2 timed iterations, then the chosen one
     b.sync()
-    for h, s in zip(hs, evs):
-        _reset(h, s)
-    for h in hs:
-        h.sync()
-    b.advance(2)  # graphs of the reset parity
-    b.sync()
-    for h, s in zip(hs, evs):
-        _reset(h, s)
-    for h in hs:
-        h.sync()
-    b.timer_start()
-    b.advance(steps)
-    batch_ms = b.timer_stop()
-    bits = b.sync()
+    tuned = b.info()
+
+    def timed():
+        for h, s in zip(hs, evs):
+            _reset(h, s)
+        for h in hs:
+            h.sync()
+        b.advance(2)  # graphs of the reset parity
+        b.sync()
+        for h, s in zip(hs, evs):
+            _reset(h, s)
+        for h in hs:
+            h.sync()
+        b.timer_start()
+        b.advance(steps)
+        ms = b.timer_stop()
+        return ms, b.sync()
+
+    tuned_ms, bits = timed()
+    # each form on its own: stage-batched, and a branch per event (8 streams
+    # when the tuner chose the stage-batched form)
+    b.set_mode(True)
+    stage_ms, bits_s = timed()
+    b.set_mode(False)
+    graph_ms, bits_g = timed()
     info = b.info()
     b.close()
     for h in hs:
@@ -403,10 +416,16 @@ def batch_measure(capi, W, n_events, steps, device, nz=None):
                 min(s.grid.ncells for s in evs), max(s.grid.ncells for s in evs),
                 "61x61x1 .. 121x121x61 family" if nz is None else "nz = %d" % nz),
             "plain_per_event": cells * steps / (plain_ms / 1e3),
-            "batched_graph": cells * steps / (batch_ms / 1e3),
-            "speedup": plain_ms / batch_ms, "unit": UNIT, "error_bits": bits,
-            "tuned": {"nstreams": info["nstreams"], "block": info["block"],
+            "batched_tuned": cells * steps / (tuned_ms / 1e3),
+            "batched_stage": cells * steps / (stage_ms / 1e3),
+            "batched_graph": cells * steps / (graph_ms / 1e3),
+            "speedup": plain_ms / tuned_ms, "speedup_stage": plain_ms / stage_ms,
+            "speedup_graph": plain_ms / graph_ms, "unit": UNIT,
+            "error_bits": bits | bits_s | bits_g,
+            "tuned": {"form": "stage-batched" if tuned["nstreams"] == 0 else "branch per event",
+                      "nstreams": tuned["nstreams"], "block": tuned["block"],
                       "captures": info["captures"]},
+            "graph": {"nstreams": info["nstreams"], "block": info["block"]},
             "physics": "eta/s=0.12, zeta/s Gaussian bump 0.05 at T=0.175 GeV (width 0.02)"}
 
 
@@ -584,7 +603,7 @@ def batched_mlp_measure(capi, W, evs, steps, device, mlp, tau_resize=4.0, nsampl
         for k, d in enumerate(drv):
             b.set_driver(k, *d, tau_resize)
         b.tune(True)
-        b.advance(16)  # the tuner's configurations (16 iterations stay below tau_resize)
+        b.advance(16)  # the tuner's 8 configurations x 2 (16 iterations stay below tau_resize)
         b.sync()
         for h, s in zip(hs, evs):
             _reset(h, s)
@@ -639,7 +658,9 @@ def batched_mlp_measure(capi, W, evs, steps, device, mlp, tau_resize=4.0, nsampl
     for mode in ("tight", "tight_slope_mlp"):
         ms["batched_" + mode], hs, bits, info = batched(mode)
         out["error_bits_" + mode] = bits
-        out["tuned_" + mode] = {"nstreams": info["nstreams"], "block": info["block"]}
+        out["tuned_" + mode] = {"form": "stage-batched" if info["nstreams"] == 0 else
+                                "branch per event", "nstreams": info["nstreams"],
+                                "block": info["block"]}
         errs = {k: state_error(hs[k].get_state(("Q", "pi", "Pi")), ref_states[k]) for k in sample}
         out["errors_" + mode] = {
             f: {"max_rel": max(e[f]["max_rel"] for e in errs.values()),

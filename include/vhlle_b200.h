@@ -490,8 +490,17 @@ vh_status vh_cornelius4d(const double *cubes, long n, const double *dx, double e
  * to advancing each context alone with vh_advance / vh_resize2x.
  * vh_batch_set_driver sets an event's (k >= 0) or every event's (k < 0)
  * dtau, eta range, nz and tau_resize (defaults: the context's step and grid,
- * no resize).  vh_batch_tune(b, 1) times the next iterations under each
- * launch configuration (capture streams, block size) and keeps the fastest.
+ * no resize).  A batch has two forms of the iteration: a branch per event
+ * over capture streams, or stage-batched: one launch per stage of the step
+ * (faces, updates, relaxation, ...) over a work table of every event's
+ * blocks, so that hundreds of small grids run as one grid per stage (only
+ * when every event has the same EoS class and viscosity and none has
+ * vorticity on).  vh_batch_tune(b, 1) times the next iterations under each
+ * launch configuration (capture streams and block size of the branch form,
+ * and the stage-batched form) and keeps the fastest; vh_batch_set_mode(b,
+ * 1) selects the stage-batched form, 0 the tuner's choice (VH_ERR_ARG where
+ * the stage-batched form is unavailable); vh_batch_info reports nstreams = 0
+ * for it.
  * Set every context (tolerance, network, stream counters) before advancing;
  * a change is picked up by re-capturing.  vh_batch_sync waits and ORs the
  * events' device error words (VH_ERR_NUMERIC if any is set).  Errors of
@@ -505,6 +514,7 @@ vh_status vh_batch_tune(vh_batch *batch, int enable);
 vh_status vh_batch_advance(vh_batch *batch, int *nsub_max);
 vh_status vh_batch_sync(vh_batch *batch, unsigned *error_bits);
 vh_status vh_batch_info(vh_batch *batch, int *captures, int *nstreams, int *block);
+vh_status vh_batch_set_mode(vh_batch *batch, int stage_batched);
 /* CUDA-event timing of the batch's stream (stop waits for the stop event). */
 vh_status vh_batch_timer_start(vh_batch *batch);
 vh_status vh_batch_timer_stop(vh_batch *batch, double *ms);

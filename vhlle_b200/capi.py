@@ -40,7 +40,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
            "vh_batch_destroy", "vh_batch_set_driver", "vh_batch_tune", "vh_batch_advance",
            "vh_batch_sync", "vh_batch_info", "vh_batch_last_error", "vh_batch_timer_start",
-           "vh_batch_timer_stop")
+           "vh_batch_timer_stop", "vh_batch_set_mode")
 
 
 class VhError(RuntimeError):
@@ -174,6 +174,11 @@ class Batch:
 
     def tune(self, enable=True):
         self._check(self.L.vh_batch_tune(self.b, int(enable)))
+
+    def set_mode(self, stage_batched):
+        """True: one launch per stage over every event's blocks; False: the
+        tuner's configuration (vh_batch_set_mode)."""
+        self._check(self.L.vh_batch_set_mode(self.b, int(bool(stage_batched))))
 
     def advance(self, n=1):
         m = ctypes.c_int()
@@ -375,6 +380,7 @@ def lib():
     L.vh_batch_set_driver.argtypes = [vp, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_int, ctypes.c_double]
     L.vh_batch_tune.argtypes = [vp, ctypes.c_int]
+    L.vh_batch_set_mode.argtypes = [vp, ctypes.c_int]
     L.vh_batch_advance.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.vh_batch_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
     L.vh_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3

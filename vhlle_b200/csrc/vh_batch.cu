@@ -11,14 +11,22 @@
 // (src/main.cpp:405-419), the parity of its double-buffered fill fractions,
 // a grid resize (src/main.cpp:423-427), or the launch configuration.
 //
+// The stage-batched form captures instead, per substep index, one launch
+// per stage of the step over a work table of every event's blocks (events
+// with fewer substeps drop out of the later tables), with the events'
+// clock operations batched too: a few dozen launches per iteration
+// whatever the number of events.
+//
 // The launch configuration (capture streams, block size of the step
-// kernels) is picked by an online autotuner: with tuning on, successive
-// iterations run under each candidate and are timed with CUDA events, and
-// the fastest is kept.  Every configuration runs the same kernels on the
-// same data in the same per-event order, so results do not depend on it.
+// kernels, or the stage-batched form) is picked by an online autotuner:
+// with tuning on, successive iterations run under each candidate and are
+// timed with CUDA events, and the fastest is kept.  Every configuration runs
+// the same per-cell operations on the same data in the same per-event
+// order, so results do not depend on it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <map>
 #include <numeric>
 #include <string>
@@ -32,11 +40,12 @@
 namespace {
 
 struct Config {
-  int nstreams, block;
+  int nstreams, block;  // nstreams 0: the stage-batched form
 };
 const Config kConfigs[] = {{4, 128}, {8, 128}, {16, 128}, {32, 128},
-                           {8, 64},  {16, 64}, {32, 64}};
+                           {8, 64},  {16, 64}, {32, 64},  {0, 128}};
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
+constexpr int kStageConfig = kNumConfigs - 1;
 constexpr int kTuneReps = 2;  // iterations timed per candidate
 
 thread_local std::string g_batch_error;
@@ -62,17 +71,34 @@ struct vh_batch {
   cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr, ts = nullptr, te = nullptr;
   std::vector<cudaEvent_t> join;
   std::map<std::vector<int>, cudaGraphExec_t> graphs;
+  // the device work tables a stage-batched graph reads, per graph key
+  std::map<std::vector<int>, std::vector<void*>> tables;
   int captures = 0;
   int config = 1;  // index into kConfigs
+  // the stage-batched form: the events' common EoS class (-1: unavailable)
+  // and viscosity
+  int stage_ek = -1;
+  bool stage_viscous = false;
+  std::vector<int> cands;  // the tuner's candidates (indices into kConfigs)
   // online tuning state
   bool tuning = false;
   int tune_cand = 0, tune_rep = 0;
   std::vector<float> tune_ms;
   double last_ms = 0.;
 
+  void drop_graph(const std::vector<int>& key) {
+    auto t = tables.find(key);
+    if (t != tables.end()) {
+      for (void* p : t->second) cudaFree(p);
+      tables.erase(t);
+    }
+  }
   void clear_graphs() {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     graphs.clear();
+    for (auto& kv : tables)
+      for (void* p : kv.second) cudaFree(p);
+    tables.clear();
   }
 };
 
@@ -154,6 +180,98 @@ vh_status capture(vh_batch* b, const std::vector<int>& nsub, const Config& cfg,
   return VH_OK;
 }
 
+// The stage-batched form of one iteration: per substep index j a work
+// table of every event with more than j substeps (its StepDev with the
+// fill-fraction buffers of that substep's parity, and its blocks), the
+// learned start points per event, the stage launches and the clocks'
+// tau += dt over the table's events; dt / n before and dt * n after over all
+// events (n = 1 leaves dt as it is).  The tables are device arrays written
+// before the capture and kept with the graph.
+vh_status capture_stages(vh_batch* b, const std::vector<int>& nsub, cudaGraphExec_t* out,
+                         std::vector<void*>* keep) {
+  const int n = (int)b->ev.size();
+  int nmax = 1;
+  for (int k = 0; k < n; k++) nmax = std::max(nmax, nsub[k]);
+  std::vector<vh::StepDev> devs;
+  std::vector<vh::BItem> items;
+  std::vector<int> ns;
+  struct Part {
+    int dev0, nev, item0, nitems;
+  };
+  std::vector<Part> parts;
+  for (int j = 0; j < nmax; j++) {
+    Part pt{(int)devs.size(), 0, (int)items.size(), 0};
+    for (int r = 0; r < n; r++) {
+      const int ei = b->order[r];
+      if (nsub[ei] <= j) continue;
+      const vh_ctx* c = b->ev[ei];
+      vh::StepDev d;
+      d.g = c->g;
+      d.eos = c->eos;
+      d.eos.vguess = c->mlp ? c->vguess : nullptr;
+      d.tr = c->tr;
+      d.f = c->f;
+      if (j & 1) std::swap(d.f.m, d.f.m2);
+      d.clk = c->clk;
+      d.viscous = c->viscous;
+      const int idx = (int)devs.size() - pt.dev0;
+      devs.push_back(d);
+      if (j == 0) ns.push_back(nsub[ei]);
+      const long long nb = (c->g.N + vh::kBatchBlock - 1) / vh::kBatchBlock;
+      for (long long k = 0; k < nb; k++) items.push_back(vh::BItem{idx, (int)k});
+      pt.nev++;
+    }
+    pt.nitems = (int)items.size() - pt.item0;
+    parts.push_back(pt);
+  }
+  if (items.size() > (size_t)INT32_MAX)
+    return bfail(VH_ERR_ARG, "vh_batch_advance: the stage-batched work table is too large");
+  vh::StepDev* ddev = nullptr;
+  vh::BItem* idev = nullptr;
+  int* ndev = nullptr;
+  cudaError_t e = cudaMalloc(&ddev, devs.size() * sizeof(vh::StepDev));
+  if (e == cudaSuccess) e = cudaMalloc(&idev, items.size() * sizeof(vh::BItem));
+  if (e == cudaSuccess) e = cudaMalloc(&ndev, ns.size() * sizeof(int));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ddev, devs.data(), devs.size() * sizeof(vh::StepDev), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(idev, items.data(), items.size() * sizeof(vh::BItem), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(ndev, ns.data(), ns.size() * sizeof(int), cudaMemcpyHostToDevice);
+  keep->push_back(ddev);
+  keep->push_back(idev);
+  keep->push_back(ndev);
+  if (e != cudaSuccess)
+    return bfail(VH_ERR_CUDA, std::string("stage-batched tables: ") + cudaGetErrorString(e));
+  e = cudaStreamBeginCapture(b->origin, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess)
+    return bfail(VH_ERR_CUDA, std::string("cudaStreamBeginCapture: ") + cudaGetErrorString(e));
+  vh::launch_clock_op_batched(ddev, parts[0].nev, 1, ndev, b->origin);  // dt / n
+  for (int j = 0; j < nmax; j++) {
+    const Part& pt = parts[j];
+    for (int r = 0; r < n; r++) {
+      const int ei = b->order[r];
+      const vh_ctx* c = b->ev[ei];
+      if (nsub[ei] > j && c->mlp)
+        vh::launch_mlp_guess(c->mlp->packed, c->f.Q, c->g.N, c->clk, c->vguess, b->origin);
+    }
+    vh::launch_step_batched(b->stage_ek, b->stage_viscous, ddev + pt.dev0, pt.nev,
+                            idev + pt.item0, pt.nitems, b->origin);
+    vh::launch_clock_op_batched(ddev + pt.dev0, pt.nev, 0, nullptr, b->origin);  // tau += dt
+  }
+  vh::launch_clock_op_batched(ddev, parts[0].nev, 2, ndev, b->origin);  // dt * n
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(b->origin, &graph);
+  if (e != cudaSuccess)
+    return bfail(VH_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(out, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess)
+    return bfail(VH_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  b->captures++;
+  return VH_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -216,6 +334,15 @@ vh_status vh_batch_create(vh_ctx* const* ctxs, int n, vh_batch** out) {
     vh_batch_destroy(b);
     return bfail(VH_ERR_CUDA, cudaGetErrorString(e));
   }
+  // the stage-batched form: one EoS class and viscosity, no vorticity
+  b->stage_ek = vh::step_ek(ctxs[0]->eos);
+  b->stage_viscous = ctxs[0]->viscous;
+  for (int k = 0; k < n; k++)
+    if (vh::step_ek(ctxs[k]->eos) != b->stage_ek || ctxs[k]->viscous != b->stage_viscous ||
+        ctxs[k]->vort_on)
+      b->stage_ek = -1;
+  for (int k = 0; k < kNumConfigs; k++)
+    if (k != kStageConfig || b->stage_ek >= 0) b->cands.push_back(k);
   // the contexts' queued work comes first
   for (vh_ctx* c : b->ev) cudaStreamSynchronize(c->stream);
   *out = b;
@@ -242,7 +369,22 @@ vh_status vh_batch_tune(vh_batch* b, int enable) {
   b->tuning = enable != 0;
   b->tune_cand = 0;
   b->tune_rep = 0;
-  b->tune_ms.assign(kNumConfigs, 0.f);
+  b->tune_ms.assign(b->cands.size(), 0.f);
+  return VH_OK;
+}
+
+vh_status vh_batch_set_mode(vh_batch* b, int stage_batched) {
+  if (!b) return VH_ERR_ARG;
+  if (stage_batched) {
+    if (b->stage_ek < 0)
+      return bfail(VH_ERR_ARG,
+                   "vh_batch_set_mode: the events differ in EoS class or viscosity, or one has "
+                   "vorticity on");
+    b->config = kStageConfig;
+  } else if (b->config == kStageConfig) {
+    b->config = 1;
+  }
+  b->tuning = false;
   return VH_OK;
 }
 
@@ -258,7 +400,13 @@ vh_status vh_batch_advance(vh_batch* b, int* nsub_max) {
     if (nsub[k] < 0) return bfail(VH_ERR_ARG, "vh_batch_advance: substep count overflow");
     nmax = std::max(nmax, nsub[k]);
   }
-  const int cfg_idx = b->tuning ? b->tune_cand : b->config;
+  // vorticity switched on after the batch was made rules the form out
+  if (b->stage_ek >= 0)
+    for (const vh_ctx* c : b->ev)
+      if (c->vort_on)
+        return bfail(VH_ERR_STATE,
+                     "vh_batch_advance: an event turned vorticity on; make a new batch");
+  const int cfg_idx = b->tuning ? b->cands[b->tune_cand] : b->config;
   const Config cfg = kConfigs[cfg_idx];
   key.reserve(3 * n + 1);
   key.push_back(cfg_idx);
@@ -272,8 +420,19 @@ vh_status vh_batch_advance(vh_batch* b, int* nsub_max) {
   if (it != b->graphs.end()) {
     exec = it->second;
   } else {
-    vh_status st = capture(b, nsub, cfg, &exec);
-    if (st != VH_OK) return st;
+    vh_status st;
+    if (cfg.nstreams == 0) {
+      std::vector<void*> keep;
+      st = capture_stages(b, nsub, &exec, &keep);
+      if (st != VH_OK) {
+        for (void* p : keep) cudaFree(p);
+        return st;
+      }
+      b->tables[key] = keep;
+    } else {
+      st = capture(b, nsub, cfg, &exec);
+      if (st != VH_OK) return st;
+    }
     b->graphs[key] = exec;
   }
   cudaEventRecord(b->t0, b->origin);
@@ -298,14 +457,15 @@ vh_status vh_batch_advance(vh_batch* b, int* nsub_max) {
     b->tune_ms[b->tune_cand] += ms;
     if (++b->tune_rep == kTuneReps) {
       b->tune_rep = 0;
-      if (++b->tune_cand == kNumConfigs) {
+      if (++b->tune_cand == (int)b->cands.size()) {
         b->tuning = false;
-        b->config = (int)(std::min_element(b->tune_ms.begin(), b->tune_ms.end()) -
-                          b->tune_ms.begin());
+        b->config = b->cands[std::min_element(b->tune_ms.begin(), b->tune_ms.end()) -
+                             b->tune_ms.begin()];
         // keep only the chosen configuration's graphs
         for (auto g = b->graphs.begin(); g != b->graphs.end();) {
           if (g->first[0] != b->config) {
             cudaGraphExecDestroy(g->second);
+            b->drop_graph(g->first);
             g = b->graphs.erase(g);
           } else {
             ++g;

@@ -23,10 +23,11 @@ namespace vh {
 
 // -------------------------------------------------------------- updateM
 // Fluid::updateM, src/fld.cpp:384-423 (both passes; out of place).
-__global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restrict__ mo,
-                           const double* __restrict__ clk) {
+__device__ __forceinline__ void d_update_m(const Geo& g, const double* __restrict__ m,
+                                           double* __restrict__ mo, const double* __restrict__ clk,
+                                           long long blk) {
   const double tau = clk[0], dt = clk[1];  // the step's clock (device)
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = blk * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
@@ -60,6 +61,11 @@ __global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restri
   mo[N + i] = a1;
   mo[2 * N + i] = a2;
 }
+__global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restrict__ mo,
+                           const double* __restrict__ clk) {
+  d_update_m(g, m, mo, clk, blockIdx.x);
+}
+
 
 // ------------------------------------------------------------ face flux
 // One HLLE face between cell i and its +DIR neighbour (Hydro::hlle_flux with
@@ -74,12 +80,13 @@ __global__ void k_update_m(Geo g, const double* __restrict__ m, double* __restri
 template <int DIR, bool PRED, int EK>
 // 7 blocks of 128 per SM (72 registers): measured against 6 and 8 blocks on
 // the 300-step event, 3 % faster than 8 (64 registers, more spills)
-__global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
-                                              const double* __restrict__ m,
-                                              double* __restrict__ F, const double* __restrict__ clk,
-                                              unsigned* err) {
+__device__ __forceinline__ void d_face(const Geo& g, const EosDev& E,
+                                       const double* __restrict__ QQ,
+                                       const double* __restrict__ m, double* __restrict__ F,
+                                       const double* __restrict__ clk, unsigned* err,
+                                       long long blk) {
   const double tau = clk[0], dt = clk[1];  // the step's clock (device)
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = blk * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
@@ -129,21 +136,30 @@ __global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* 
 #pragma unroll
   for (int k = 0; k < 7; k++) F[k * N + i] = ok ? fl[k] : 0.;
 }
+template <int DIR, bool PRED, int EK>
+__global__ void __launch_bounds__(128, 7) k_face(Geo g, EosDev E, const double* __restrict__ QQ,
+                                              const double* __restrict__ m,
+                                              double* __restrict__ F, const double* __restrict__ clk,
+                                              unsigned* err) {
+  d_face<DIR, PRED, EK>(g, E, QQ, m, F, clk, err, blockIdx.x);
+}
+
 
 // --------------------------------------------------- ideal cell update
 // Gathers the six face fluxes and the Milne source (Hydro::source_step,
 // src/hdo.cpp:307-353), then Cell::updateQtoQhByFlux (predictor) or
 // Cell::updateByFlux (corrector), src/cll.cpp:70-88.
 template <bool PRED, int EK>
-__global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __restrict__ Q,
-                                                double* __restrict__ Qh,
-                                                double* __restrict__ Qprev,
-                                                const double* __restrict__ Fx,
-                                                const double* __restrict__ Fy,
-                                                const double* __restrict__ Fz, const double* __restrict__ clk, unsigned* err,
-                                                double* __restrict__ pB, double* __restrict__ pA) {
+__device__ __forceinline__ void d_update(const Geo& g, const EosDev& E, double* __restrict__ Q,
+                                         double* __restrict__ Qh, double* __restrict__ Qprev,
+                                         const double* __restrict__ Fx,
+                                         const double* __restrict__ Fy,
+                                         const double* __restrict__ Fz,
+                                         const double* __restrict__ clk, unsigned* err,
+                                         double* __restrict__ pB, double* __restrict__ pA,
+                                         long long blk) {
   const double tau = clk[0], dt = clk[1];  // the step's clock (device)
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = blk * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
@@ -224,6 +240,17 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
     }
   }
 }
+template <bool PRED, int EK>
+__global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __restrict__ Q,
+                                                double* __restrict__ Qh,
+                                                double* __restrict__ Qprev,
+                                                const double* __restrict__ Fx,
+                                                const double* __restrict__ Fy,
+                                                const double* __restrict__ Fz, const double* __restrict__ clk, unsigned* err,
+                                                double* __restrict__ pB, double* __restrict__ pA) {
+  d_update<PRED, EK>(g, E, Q, Qh, Qprev, Fx, Fy, Fz, clk, err, pB, pA, blockIdx.x);
+}
+
 
 // ------------------------------------------------------------- ghosts
 // Fluid::correctImagCells (FULL = false: Q and Qh) and correctImagCellsFull
@@ -231,10 +258,12 @@ __global__ void __launch_bounds__(128, 12) k_update(Geo g, EosDev E, double* __r
 // per-dimension source maps; copies into a ghost zero the row when Q_t < 0
 // (Cell::setQ / setQh).
 template <bool FULL>
-__global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char* __restrict__ isdst,
-                        double* __restrict__ Q, double* __restrict__ Qh,
-                        double* __restrict__ pi, double* __restrict__ Pi) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void d_ghost(const Geo& g, const int* __restrict__ src,
+                                        const unsigned char* __restrict__ isdst,
+                                        double* __restrict__ Q, double* __restrict__ Qh,
+                                        double* __restrict__ pi, double* __restrict__ Pi,
+                                        long long blk) {
+  const long long i = blk * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
@@ -269,6 +298,13 @@ __global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char*
     Pi[i] = P;
   }
 }
+template <bool FULL>
+__global__ void k_ghost(Geo g, const int* __restrict__ src, const unsigned char* __restrict__ isdst,
+                        double* __restrict__ Q, double* __restrict__ Qh,
+                        double* __restrict__ pi, double* __restrict__ Pi) {
+  d_ghost<FULL>(g, src, isdst, Q, Qh, pi, Pi, blockIdx.x);
+}
+
 
 // ------------------------------------------------ viscous cell prims
 // Per-cell inputs of the viscous stages, one thread per cell:
@@ -286,18 +322,18 @@ __device__ __forceinline__ double maxM_at(const Geo& g, const double* __restrict
                                           int iy, int iz);
 
 template <int EK>
-__global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr,
-                                                    const double* __restrict__ Q,
-                                                    const double* __restrict__ Qprev,
-                                                    const double* __restrict__ Qh,
-                                                    const double* __restrict__ m,
-                                                    double* __restrict__ pA,
-                                                    double* __restrict__ pD,
-                                                    double* __restrict__ pTh,
-                                                    double* __restrict__ pBC, const double* __restrict__ clk,
-                                                    const unsigned char* __restrict__ isdst) {
+__device__ __forceinline__ void d_visc_prims(const Geo& g, const EosDev& E, const TrDev& tr,
+                                             const double* __restrict__ Q,
+                                             const double* __restrict__ Qprev,
+                                             const double* __restrict__ Qh,
+                                             const double* __restrict__ m, double* __restrict__ pA,
+                                             double* __restrict__ pD, double* __restrict__ pTh,
+                                             double* __restrict__ pBC,
+                                             const double* __restrict__ clk,
+                                             const unsigned char* __restrict__ isdst,
+                                             long long blk) {
   const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = blk * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   const long long N = g.N;
   double q[7], qh[7];
@@ -389,6 +425,20 @@ __global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr
     if (w == 0) pBC[4 * N + i] = P.e;
   }
 }
+template <int EK>
+__global__ void __launch_bounds__(128, 8) k_visc_prims(Geo g, EosDev E, TrDev tr,
+                                                    const double* __restrict__ Q,
+                                                    const double* __restrict__ Qprev,
+                                                    const double* __restrict__ Qh,
+                                                    const double* __restrict__ m,
+                                                    double* __restrict__ pA,
+                                                    double* __restrict__ pD,
+                                                    double* __restrict__ pTh,
+                                                    double* __restrict__ pBC, const double* __restrict__ clk,
+                                                    const unsigned char* __restrict__ isdst) {
+  d_visc_prims<EK>(g, E, tr, Q, Qprev, Qh, m, pA, pD, pTh, pBC, clk, isdst, blockIdx.x);
+}
+
 
 __device__ __forceinline__ double maxM_at(const Geo& g, const double* __restrict__ m, int ix,
                                           int iy, int iz) {
@@ -432,15 +482,12 @@ constexpr size_t kRelaxSmem = sizeof(double) * kSmRows * kRelaxBlock;
 // runs full warps: cells with matter are packed in warp order (one atomic
 // per warp; the list's order between warps varies, and every cell's result
 // depends on that cell alone).  *nactive is zero on entry.
-__global__ void __launch_bounds__(128) k_relax_list(Geo g, const double* __restrict__ pA,
-                                                    int* __restrict__ active,
-                                                    int* __restrict__ nactive,
-                                                    double* __restrict__ pi0,
-                                                    double* __restrict__ piH0,
-                                                    double* __restrict__ Pi0,
-                                                    double* __restrict__ PiH0,
-                                                    double* __restrict__ flux) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void d_relax_list(const Geo& g, const double* __restrict__ pA,
+                                             int* __restrict__ active, int* __restrict__ nactive,
+                                             double* __restrict__ pi0, double* __restrict__ piH0,
+                                             double* __restrict__ Pi0, double* __restrict__ PiH0,
+                                             double* __restrict__ flux, long long blk) {
+  const long long i = blk * blockDim.x + threadIdx.x;
   const long long N = g.N;
   const bool in = i < N;
   const bool act = in && !(pA[i] <= 0.);
@@ -462,17 +509,29 @@ __global__ void __launch_bounds__(128) k_relax_list(Geo g, const double* __restr
     for (int k = 0; k < 4; k++) flux[k * N + i] = 0.;
   }
 }
+__global__ void __launch_bounds__(128) k_relax_list(Geo g, const double* __restrict__ pA,
+                                                    int* __restrict__ active,
+                                                    int* __restrict__ nactive,
+                                                    double* __restrict__ pi0,
+                                                    double* __restrict__ piH0,
+                                                    double* __restrict__ Pi0,
+                                                    double* __restrict__ PiH0,
+                                                    double* __restrict__ flux) {
+  d_relax_list(g, pA, active, nactive, pi0, piH0, Pi0, PiH0, flux, blockIdx.x);
+}
 
-__global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
-    Geo g, EosDev E, TrDev tr, const double* __restrict__ Q, const double* __restrict__ Qprev,
-    const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
-    const double* __restrict__ pTh, const double* __restrict__ pBC,
-    const double* __restrict__ pi, const double* __restrict__ Pi, double* __restrict__ pi0,
-    double* __restrict__ piH0, double* __restrict__ Pi0, double* __restrict__ PiH0,
-    double* __restrict__ flux, const double* __restrict__ clk, unsigned* err,
-    const int* __restrict__ active, const int* __restrict__ nactive) {
+
+__device__ __forceinline__ void d_is_relax(
+    const Geo& g, const EosDev& E, const TrDev& tr, const double* __restrict__ Q,
+    const double* __restrict__ Qprev, const double* __restrict__ m, const double* __restrict__ pA,
+    const double* __restrict__ pD, const double* __restrict__ pTh,
+    const double* __restrict__ pBC, const double* __restrict__ pi, const double* __restrict__ Pi,
+    double* __restrict__ pi0, double* __restrict__ piH0, double* __restrict__ Pi0,
+    double* __restrict__ PiH0, double* __restrict__ flux, const double* __restrict__ clk,
+    unsigned* err, const int* __restrict__ active, const int* __restrict__ nactive,
+    long long blk) {
   const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = (int)(blk * blockDim.x + threadIdx.x);
   if (idx >= *nactive) return;
   const long long i = active[idx];  // a cell with matter (k_relax_list)
   const long long N = g.N;
@@ -846,6 +905,18 @@ __global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
 #undef SIG
 #undef H
 }
+__global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) k_is_relax(
+    Geo g, EosDev E, TrDev tr, const double* __restrict__ Q, const double* __restrict__ Qprev,
+    const double* __restrict__ m, const double* __restrict__ pA, const double* __restrict__ pD,
+    const double* __restrict__ pTh, const double* __restrict__ pBC,
+    const double* __restrict__ pi, const double* __restrict__ Pi, double* __restrict__ pi0,
+    double* __restrict__ piH0, double* __restrict__ Pi0, double* __restrict__ PiH0,
+    double* __restrict__ flux, const double* __restrict__ clk, unsigned* err,
+    const int* __restrict__ active, const int* __restrict__ nactive) {
+  d_is_relax(g, E, tr, Q, Qprev, m, pA, pD, pTh, pBC, pi, Pi, pi0, piH0, Pi0, PiH0, flux, clk,
+             err, active, nactive, blockIdx.x);
+}
+
 
 // ------------------------------------------------ ISformal, loop #2
 // Semi-Lagrangian advection of pi0/piH0 from the 2x2x2 upwind cells, the
@@ -857,21 +928,21 @@ __device__ __forceinline__ double sgn(double x) {
   return 0.;
 }
 
-__global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restrict__ pA,
-                                                   const double* __restrict__ pi0,
-                                                   const double* __restrict__ piH0,
-                                                   const double* __restrict__ Pi0,
-                                                   const double* __restrict__ PiH0,
-                                                   double* __restrict__ pi, double* __restrict__ piH,
-                                                   double* __restrict__ Pi, double* __restrict__ PiH,
-                                                   double* __restrict__ vcc,
-                                                   double* __restrict__ flux, const double* __restrict__ clk,
-                                                   const int* __restrict__ active,
-                                                   const int* __restrict__ nactive) {
+__device__ __forceinline__ void d_is_advect(const Geo& g, const double* __restrict__ pA,
+                                            const double* __restrict__ pi0,
+                                            const double* __restrict__ piH0,
+                                            const double* __restrict__ Pi0,
+                                            const double* __restrict__ PiH0,
+                                            double* __restrict__ pi, double* __restrict__ piH,
+                                            double* __restrict__ Pi, double* __restrict__ PiH,
+                                            double* __restrict__ vcc, double* __restrict__ flux,
+                                            const double* __restrict__ clk,
+                                            const int* __restrict__ active,
+                                            const int* __restrict__ nactive, long long blk) {
   const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
   // the cells with matter only (k_relax_list); the empty ones are left as
   // they are, as the reference's loop 2 leaves them (e <= 0)
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = (int)(blk * blockDim.x + threadIdx.x);
   if (idx >= *nactive) return;
   const long long i = active[idx];
   int ix, iy, iz;
@@ -953,6 +1024,21 @@ __global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restri
 #pragma unroll
   for (int k = 0; k < 4; k++) flux[k * N + i] += f[k];
 }
+__global__ void __launch_bounds__(128) k_is_advect(Geo g, const double* __restrict__ pA,
+                                                   const double* __restrict__ pi0,
+                                                   const double* __restrict__ piH0,
+                                                   const double* __restrict__ Pi0,
+                                                   const double* __restrict__ PiH0,
+                                                   double* __restrict__ pi, double* __restrict__ piH,
+                                                   double* __restrict__ Pi, double* __restrict__ PiH,
+                                                   double* __restrict__ vcc,
+                                                   double* __restrict__ flux, const double* __restrict__ clk,
+                                                   const int* __restrict__ active,
+                                                   const int* __restrict__ nactive) {
+  d_is_advect(g, pA, pi0, piH0, Pi0, PiH0, pi, piH, Pi, PiH, vcc, flux, clk, active, nactive,
+              blockIdx.x);
+}
+
 
 // --------------------------------------------- viscous flux + update
 // Hydro::visc_flux (src/hdo.cpp:966-1014) for the six faces of the cell,
@@ -1001,14 +1087,15 @@ __device__ __forceinline__ bool visc_face(int dir, double tau, double dt, const 
   return true;
 }
 
-__global__ void __launch_bounds__(128, 8) k_visc_update(Geo g, const double* __restrict__ pA,
-                                                     const double* __restrict__ piH,
-                                                     const double* __restrict__ PiH,
-                                                     const double* __restrict__ m,
-                                                     const double* __restrict__ flux,
-                                                     double* __restrict__ Q, const double* __restrict__ clk) {
+__device__ __forceinline__ void d_visc_update(const Geo& g, const double* __restrict__ pA,
+                                              const double* __restrict__ piH,
+                                              const double* __restrict__ PiH,
+                                              const double* __restrict__ m,
+                                              const double* __restrict__ flux,
+                                              double* __restrict__ Q,
+                                              const double* __restrict__ clk, long long blk) {
   const double dt = clk[1], tau = clk[0] + dt;  // tau_{n+1} (src/hdo.cpp:1095)
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = blk * blockDim.x + threadIdx.x;
   if (i >= g.N) return;
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
@@ -1065,6 +1152,15 @@ __global__ void __launch_bounds__(128, 8) k_visc_update(Geo g, const double* __r
     for (int k = 4; k < 7; k++) Q[k * N + i] += fac * 0.;
   }
 }
+__global__ void __launch_bounds__(128, 8) k_visc_update(Geo g, const double* __restrict__ pA,
+                                                     const double* __restrict__ piH,
+                                                     const double* __restrict__ PiH,
+                                                     const double* __restrict__ m,
+                                                     const double* __restrict__ flux,
+                                                     double* __restrict__ Q, const double* __restrict__ clk) {
+  d_visc_update(g, pA, piH, PiH, m, flux, Q, clk, blockIdx.x);
+}
+
 
 // --------------------------------------------------- batched transformPV
 __global__ void k_transform_pv(EosDev E, const double* __restrict__ Q, long long n,
@@ -1094,10 +1190,6 @@ const char* const kKernelNames[KK_COUNT] = {
     "k_visc_prims", "k_is_relax", "k_is_advect", "k_visc_update",
     "vorticity (k_vort_*, 6 kernels)"};
 
-cudaError_t step_kernels_setup() {
-  return cudaFuncSetAttribute(k_is_relax, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)kRelaxSmem);
-}
 
 template <int EK>
 static int launch_step_ek(const StepArgs& a, cudaStream_t s, LaunchMarker* mk) {
@@ -1248,6 +1340,178 @@ __global__ void k_clock_op(double* clk, int op, int n) {
     clk[1] = clk[1] / n;
   else
     clk[1] = clk[1] * n;
+}
+
+// ------------------------------------------------- stage-batched step
+// The step kernels' bodies over a work table: block b of the launch is
+// block items[b].blk of event items[b].ev, whose arguments come from
+// evs[items[b].ev] (the small structures copied into registers, the
+// field pointers loaded once).  Each event's cells see exactly the
+// operations of its own launch_step; events are independent, so the order
+// of blocks across events does not matter.
+#define VH_ITEM                              \
+  const BItem it = items[blockIdx.x];        \
+  const StepDev& A = evs[it.ev];             \
+  const Geo g = A.g;                         \
+  const long long blk = it.blk;
+
+__global__ void kb_update_m(const StepDev* __restrict__ evs, const BItem* __restrict__ items) {
+  VH_ITEM
+  d_update_m(g, A.f.m, A.f.m2, A.clk, blk);
+}
+
+template <int DIR, bool PRED, int EK>
+__global__ void __launch_bounds__(128, 7) kb_face(const StepDev* __restrict__ evs,
+                                               const BItem* __restrict__ items) {
+  VH_ITEM
+  const EosDev E = A.eos;
+  double* F = DIR == X_ ? A.f.Fx : (DIR == Y_ ? A.f.Fy : A.f.Fz);
+  d_face<DIR, PRED, EK>(g, E, PRED ? A.f.Q : A.f.Qh, A.f.m2, F, A.clk, A.f.err, blk);
+}
+
+template <bool PRED, int EK>
+__global__ void __launch_bounds__(128, 12) kb_update(const StepDev* __restrict__ evs,
+                                                 const BItem* __restrict__ items) {
+  VH_ITEM
+  const EosDev E = A.eos;
+  double* pB = PRED && A.viscous ? A.f.pBC : nullptr;
+  double* pA = !PRED && A.viscous ? A.f.pA : nullptr;
+  d_update<PRED, EK>(g, E, A.f.Q, A.f.Qh, A.f.Qprev, A.f.Fx, A.f.Fy, A.f.Fz, A.clk, A.f.err, pB,
+                     pA, blk);
+}
+
+template <bool FULL>
+__global__ void kb_ghost(const StepDev* __restrict__ evs, const BItem* __restrict__ items) {
+  VH_ITEM
+  d_ghost<FULL>(g, A.f.gsrc, A.f.gdst, A.f.Q, A.f.Qh, A.f.pi, A.f.Pi, blk);
+}
+
+template <int EK>
+__global__ void __launch_bounds__(128, 8) kb_visc_prims(const StepDev* __restrict__ evs,
+                                                     const BItem* __restrict__ items) {
+  VH_ITEM
+  const EosDev E = A.eos;
+  const TrDev tr = A.tr;
+  d_visc_prims<EK>(g, E, tr, A.f.Q, A.f.Qprev, A.f.Qh, A.f.m2, A.f.pA, A.f.pD, A.f.pTh,
+                   A.f.pBC, A.clk, A.f.gdst, blk);
+}
+
+__global__ void kb_nactive_zero(const StepDev* __restrict__ evs, int nev) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < nev) *evs[e].f.nactive = 0;
+}
+
+__global__ void __launch_bounds__(128) kb_relax_list(const StepDev* __restrict__ evs,
+                                                     const BItem* __restrict__ items) {
+  VH_ITEM
+  d_relax_list(g, A.f.pA, A.f.active, A.f.nactive, A.f.pi0, A.f.piH0, A.f.Pi0, A.f.PiH0,
+               A.f.flux, blk);
+}
+
+__global__ void __launch_bounds__(kRelaxBlock, kRelaxMinBlocks) kb_is_relax(
+    const StepDev* __restrict__ evs, const BItem* __restrict__ items) {
+  VH_ITEM
+  const EosDev E = A.eos;
+  const TrDev tr = A.tr;
+  d_is_relax(g, E, tr, A.f.Q, A.f.Qprev, A.f.m2, A.f.pA, A.f.pD, A.f.pTh, A.f.pBC, A.f.pi,
+             A.f.Pi, A.f.pi0, A.f.piH0, A.f.Pi0, A.f.PiH0, A.f.flux, A.clk, A.f.err, A.f.active,
+             A.f.nactive, blk);
+}
+
+__global__ void __launch_bounds__(128) kb_is_advect(const StepDev* __restrict__ evs,
+                                                    const BItem* __restrict__ items) {
+  VH_ITEM
+  d_is_advect(g, A.f.pA, A.f.pi0, A.f.piH0, A.f.Pi0, A.f.PiH0, A.f.pi, A.f.piH, A.f.Pi,
+              A.f.PiH, A.f.vcc, A.f.flux, A.clk, A.f.active, A.f.nactive, blk);
+}
+
+__global__ void __launch_bounds__(128, 8) kb_visc_update(const StepDev* __restrict__ evs,
+                                                      const BItem* __restrict__ items) {
+  VH_ITEM
+  d_visc_update(g, A.f.pA, A.f.piH, A.f.PiH, A.f.m2, A.f.flux, A.f.Q, A.clk, blk);
+}
+#undef VH_ITEM
+
+__global__ void kb_clock_op(const StepDev* __restrict__ evs, int nev, int op,
+                            const int* __restrict__ ns) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nev) return;
+  double* clk = evs[e].clk;
+  const int n = ns ? ns[e] : 1;
+  if (op == 0)
+    clk[0] += clk[1];
+  else if (op == 1)
+    clk[1] = clk[1] / n;
+  else
+    clk[1] = clk[1] * n;
+}
+
+// launch_step_ek's stages in its order, over the work table
+template <int EK>
+static int launch_step_batched_ek(bool viscous, const StepDev* evs, int nev, const BItem* items,
+                                  int nitems, cudaStream_t s) {
+  const unsigned nb = (unsigned)nitems, ne = nblk(nev, 128);
+  int launches = 0;
+  kb_update_m<<<nb, kBatchBlock, 0, s>>>(evs, items);
+  launches++;
+  // predictor and corrector; z faces of 2+1D events return at once
+  kb_face<X_, true, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_face<Y_, true, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_face<Z_, true, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_update<true, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_face<X_, false, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_face<Y_, false, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_face<Z_, false, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_update<false, EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  kb_ghost<false><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  launches += 9;
+  if (viscous) {
+    kb_visc_prims<EK><<<nb, kBatchBlock, 0, s>>>(evs, items);
+    kb_nactive_zero<<<ne, 128, 0, s>>>(evs, nev);
+    kb_relax_list<<<nb, kBatchBlock, 0, s>>>(evs, items);
+    kb_is_relax<<<nb, kRelaxBlock, kRelaxSmem, s>>>(evs, items);
+    kb_is_advect<<<nb, kBatchBlock, 0, s>>>(evs, items);
+    kb_visc_update<<<nb, kBatchBlock, 0, s>>>(evs, items);
+    launches += 6;
+  }
+  kb_ghost<true><<<nb, kBatchBlock, 0, s>>>(evs, items);
+  return launches + 1;
+}
+
+int step_ek(const EosDev& E) {
+  if (E.kind == 3) return EK_TABLE3;
+  if (E.kind == 6) return EK_AZH;
+  if (E.kind == 7) return EK_CMFE;
+  const bool chiral = E.kind == 2;
+  if (E.slope) return chiral ? EK_CHIRAL_SL : EK_TABLE_SL;
+  return chiral ? EK_CHIRAL : EK_TABLE;
+}
+
+int launch_step_batched(int ek, bool viscous, const StepDev* evs, int nev, const BItem* items,
+                        int nitems, cudaStream_t s) {
+  switch (ek) {
+    case EK_TABLE3: return launch_step_batched_ek<EK_TABLE3>(viscous, evs, nev, items, nitems, s);
+    case EK_AZH: return launch_step_batched_ek<EK_AZH>(viscous, evs, nev, items, nitems, s);
+    case EK_CMFE: return launch_step_batched_ek<EK_CMFE>(viscous, evs, nev, items, nitems, s);
+    case EK_CHIRAL_SL:
+      return launch_step_batched_ek<EK_CHIRAL_SL>(viscous, evs, nev, items, nitems, s);
+    case EK_TABLE_SL:
+      return launch_step_batched_ek<EK_TABLE_SL>(viscous, evs, nev, items, nitems, s);
+    case EK_CHIRAL: return launch_step_batched_ek<EK_CHIRAL>(viscous, evs, nev, items, nitems, s);
+    default: return launch_step_batched_ek<EK_TABLE>(viscous, evs, nev, items, nitems, s);
+  }
+}
+
+void launch_clock_op_batched(const StepDev* evs, int nev, int op, const int* ns, cudaStream_t s) {
+  kb_clock_op<<<nblk(nev, 128), 128, 0, s>>>(evs, nev, op, ns);
+}
+
+cudaError_t step_kernels_setup() {
+  cudaError_t e = cudaFuncSetAttribute(k_is_relax, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)kRelaxSmem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kb_is_relax, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)kRelaxSmem);
 }
 
 void launch_clock_set(double* clk, double tau, double dt, cudaStream_t s) {

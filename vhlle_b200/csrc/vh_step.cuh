@@ -83,6 +83,35 @@ struct StepArgs {
   const VortDev* vort = nullptr;  // vorticity on (viscous steps only)
 };
 
+// A batch's stage-batched step (vh_batch.cu): one launch per stage over
+// the blocks of every event.  StepDev is one event's step arguments in
+// device memory (f.m the current fill fractions, f.m2 the updated ones, as
+// launch_step leaves them); a work item is one block of one event.
+struct StepDev {
+  Geo g;
+  EosDev eos;
+  TrDev tr;
+  Fields f;
+  double* clk;
+  int viscous;
+};
+struct BItem {
+  int ev;   // index into the StepDev array
+  int blk;  // block of that event's grid (128 cells each)
+};
+constexpr int kBatchBlock = 128;
+
+// The EoS class instantiation launch_step picks for an EoS descriptor.
+int step_ek(const EosDev& E);
+// One step of nev events (evs: device), work items covering every event's
+// nblk(N, kBatchBlock) blocks (items: device); every event with EoS class
+// ek and the same viscous flag.  Returns the number of launches.
+int launch_step_batched(int ek, bool viscous, const StepDev* evs, int nev, const BItem* items,
+                        int nitems, cudaStream_t s);
+// launch_clock_op on the clocks of nev events at once (ns: device, each
+// event's n for ops 1 and 2)
+void launch_clock_op_batched(const StepDev* evs, int nev, int op, const int* ns, cudaStream_t s);
+
 // ISformal's dbeta for every cell (after k_visc_prims, before the viscous
 // update changes Q); returns the number of launches
 int launch_vorticity(const StepArgs& a, cudaStream_t s);
