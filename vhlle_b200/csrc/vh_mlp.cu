@@ -51,6 +51,17 @@ __device__ __forceinline__ float bf16r(float x) {
   return __bfloat162float(__float2bfloat16_rn(x));
 }
 __device__ __forceinline__ float silu(float z) { return z / (1.f + __expf(-z)); }
+// SiLU for inference: z sigmoid(z) = z (1 + tanh(z / 2)) / 2 with the
+// hardware tanh (one transcendental-unit operation instead of an exp and a
+// reciprocal; relative error ~2^-11, below the BF16 rounding of the
+// activations that follows).  The exp and the divide of silu() kept the
+// transcendental unit of the inference kernel 58 % busy.
+__device__ __forceinline__ float tanh_hw(float x) {
+  float r;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float silu_fast(float z) { return 0.5f * z * (1.f + tanh_hw(0.5f * z)); }
 __device__ __forceinline__ float silu_grad(float z) {
   const float s = 1.f / (1.f + __expf(-z));
   return s * (1.f + z * (1.f - s));
@@ -126,7 +137,7 @@ __device__ __forceinline__ void mlp_warp(const uint32_t* __restrict__ W, const f
     c[1] = c[3] = bias[8 * j + 2 * t + 1];
     const uint32_t* wr = W + kP1 + (8 * j + g) * kP1Stride;
     mma_bf16(c, a, wr[t], wr[t + 4]);
-    const uint32_t lo = pack2(silu(c[0]), silu(c[1])), hi = pack2(silu(c[2]), silu(c[3]));
+    const uint32_t lo = pack2(silu_fast(c[0]), silu_fast(c[1])), hi = pack2(silu_fast(c[2]), silu_fast(c[3]));
     if (j & 1) {
       h[j >> 1][2] = lo;
       h[j >> 1][3] = hi;
@@ -145,7 +156,7 @@ __device__ __forceinline__ void mlp_warp(const uint32_t* __restrict__ W, const f
     const uint32_t* wr = W + kP2 + (8 * j + g) * kP2Stride;
 #pragma unroll
     for (int kt = 0; kt < 4; kt++) mma_bf16(c, h[kt], wr[8 * kt + t], wr[8 * kt + t + 4]);
-    const uint32_t lo = pack2(silu(c[0]), silu(c[1])), hi = pack2(silu(c[2]), silu(c[3]));
+    const uint32_t lo = pack2(silu_fast(c[0]), silu_fast(c[1])), hi = pack2(silu_fast(c[2]), silu_fast(c[3]));
     if (j & 1) {
       h2[j >> 1][2] = lo;
       h2[j >> 1][3] = hi;
@@ -227,8 +238,11 @@ __global__ void __launch_bounds__(kMlpBlock) k_mlp_guess(const uint32_t* __restr
       bool ok = false;
       if (i < N) {
         double q[7];
+        // the features are ratios and a float log: Q times RN(1/tau) is
+        // as good as Q / tau for them, and takes no divide per component
+        const double rtau = 1.0 / tau;
 #pragma unroll
-        for (int k = 0; k < 7; k++) q[k] = Q[k * N + i] / tau;
+        for (int k = 0; k < 7; k++) q[k] = Q[k * N + i] * rtau;
         ok = mlp_features(q, x);
       }
       okv[warp][lane] = ok;
