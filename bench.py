@@ -380,7 +380,7 @@ def batch_measure(capi, W, n_events, steps, device, nz=None):
     for k, d in enumerate(drv):
         b.set_driver(k, *d, 4.0)
     b.tune(True)
-    b.advance(16)  # 8 configurations x 2 timed iterations, then the chosen one
+    b.advance(18)  # 9 configurations x 2 timed iterations, then the chosen one
     b.sync()
     tuned = b.info()
 
@@ -603,7 +603,7 @@ def batched_mlp_measure(capi, W, evs, steps, device, mlp, tau_resize=4.0, nsampl
         for k, d in enumerate(drv):
             b.set_driver(k, *d, tau_resize)
         b.tune(True)
-        b.advance(16)  # the tuner's 8 configurations x 2 (16 iterations stay below tau_resize)
+        b.advance(18)  # the tuner's 9 configurations x 2 (18 iterations stay below tau_resize)
         b.sync()
         for h, s in zip(hs, evs):
             _reset(h, s)

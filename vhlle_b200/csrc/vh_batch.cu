@@ -42,8 +42,9 @@ namespace {
 struct Config {
   int nstreams, block;  // nstreams 0: the stage-batched form
 };
-const Config kConfigs[] = {{4, 128}, {8, 128}, {16, 128}, {32, 128},
+const Config kConfigs[] = {{1, 128}, {4, 128}, {8, 128}, {16, 128}, {32, 128},
                            {8, 64},  {16, 64}, {32, 64},  {0, 128}};
+constexpr int kDefaultConfig = 2;  // {8, 128}
 constexpr int kNumConfigs = sizeof(kConfigs) / sizeof(kConfigs[0]);
 constexpr int kStageConfig = kNumConfigs - 1;
 constexpr int kTuneReps = 2;  // iterations timed per candidate
@@ -74,7 +75,7 @@ struct vh_batch {
   // the device work tables a stage-batched graph reads, per graph key
   std::map<std::vector<int>, std::vector<void*>> tables;
   int captures = 0;
-  int config = 1;  // index into kConfigs
+  int config = kDefaultConfig;  // index into kConfigs
   // the stage-batched form: the events' common EoS class (-1: unavailable)
   // and viscosity
   int stage_ek = -1;
@@ -382,7 +383,7 @@ vh_status vh_batch_set_mode(vh_batch* b, int stage_batched) {
                    "vorticity on");
     b->config = kStageConfig;
   } else if (b->config == kStageConfig) {
-    b->config = 1;
+    b->config = kDefaultConfig;
   }
   b->tuning = false;
   return VH_OK;
