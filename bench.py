@@ -13,7 +13,8 @@ copy) and include those surface calls.
 
 Multi-GPU (torchrun, N ranks): events are independent, so every rank runs
 its own event (seed + rank) with no collective on the data path; the time is
-the max over ranks (weak scaling).
+the max over ranks (weak scaling).  The per-GPU legs below (batched_mlp,
+batched_mlp_large, batch_2d, learned_guess) run at N = 1 only.
 
 The JSON line carries, besides the contract keys:
   roofline      the dominant kernel's algorithmic bytes per launch over its
@@ -881,12 +882,15 @@ def main():
 
     batch2d = learned = bmlp = large = None
     mlp = None
-    if not args.no_learned_guess:
+    # the per-GPU legs run on one GPU only (the multi-GPU line reports the
+    # sharded step, which the legs do not change)
+    legs = ws == 1
+    if legs and not args.no_learned_guess:
         mlp, mlp_info = train_guess_network(capi, W, local)
         learned = learned_guess_measure(capi, W, W.glauber3d_nb_setup(nx, ny, nz, seed=EVENT_SEED + rank),
                                         30, local, mlp)
         learned["train"] = mlp_info
-    if args.batch_events > 0:
+    if legs and args.batch_events > 0:
         if mlp is not None:
             bmlp = batched_mlp_measure(capi, W, W.batch_events(args.batch_events),
                                        args.batch_steps, local, mlp)
