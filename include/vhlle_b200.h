@@ -347,6 +347,21 @@ vh_status vh_init_glauber(vh_ctx *ctx, const vh_glauber_ic *ic);
 #define VH_PLANE_DOUBLES 47
 vh_status vh_pack_planes(vh_ctx *ctx, int z0, int nplanes, double *buf_dev);
 vh_status vh_unpack_planes(vh_ctx *ctx, int z0, int nplanes, const double *buf_dev);
+/* A slab's share of the freeze-out output: its planes [own0, own1) are the
+ * ones it owns, and its plane 0 is plane z_global0 of a whole grid of
+ * nz_global planes.  vh_surface and vh_corona then take only the
+ * hypercubes whose lowest corner is an owned plane (and interior in the
+ * whole grid: [2, nz_global - 2)), and vh_totals only the owned interior
+ * cells, with Fluid::outputSurface's mid-rapidity window at the whole
+ * grid's centre; the slabs' elements are then the whole grid's, and their
+ * sums add up to its.  vh_set_slab(ctx, 0, nz, 0, nz) is the whole grid
+ * again.  vh_surface_cells gives, for each element of the last vh_surface
+ * or vh_corona, the lowest corner (ix, iy, iz of the whole grid) of its
+ * hypercube (cap elements at most, *n their number): the slabs' records in
+ * order of that cell (iz fastest, a cube's elements in their order) are the
+ * whole grid's in its order. */
+vh_status vh_set_slab(vh_ctx *ctx, int own0, int own1, int z_global0, int nz_global);
+vh_status vh_surface_cells(vh_ctx *ctx, int *ixyz, long cap, long *n);
 
 /* The number of cells the last viscous step relaxed and advected: those
  * with e > 0 at the half step, the cells ISformal does not zero

@@ -58,3 +58,55 @@ def test_gpu_slabs_equal_the_whole_grid(case):
     assert all(h.tau == whole.tau for h in hs)
     for h in hs + [whole]:
         h.close()
+
+
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_gpu_slab_surfaces_and_totals_equal_the_whole_grid(nslabs):
+    """Each slab's freeze-out output of its owned planes (vh_set_slab): the
+    corona at tau0 and the surface after the steps, merged in the order of
+    the elements' hypercubes (sharding.merge_slab_surfaces), are the whole
+    grid's elements in its order, within the record tolerance (a slab's eta
+    coordinates start from its own first plane); nsusp adds up exactly and
+    the totals within 1e-10 (1e-12 of E for the sums that cancel)."""
+    torch = pytest.importorskip("torch")
+    from test_gpu_surface import rec_close_scaled
+    setup = W.glauber3d_setup(61, 61, 41)
+    g = setup.grid
+    nxy = g.nx * g.ny
+    ranges = S.slab_ranges(g.nz, nslabs)
+    hs = [capi.GpuHydro(S.slab_setup(setup, c, d)) for a, b, c, d in ranges]
+    for r, h in enumerate(hs):
+        h.set_slab(*S.slab_window(ranges, r, g.nz))
+    whole = capi.GpuHydro(setup)
+
+    def check(kind):
+        if kind == "corona":
+            rw, iw = whole.corona()
+            parts = [(h.corona()[0], h.surface_cells()) for h in hs]
+        else:
+            rw, iw = whole.surface()
+            parts = []
+            nsusp = 0
+            for h in hs:
+                r, info = h.surface()
+                parts.append((r, h.surface_cells()))
+                nsusp += info["nsusp"]
+            assert nsusp == iw["nsusp"]
+        rm = S.merge_slab_surfaces(parts)
+        assert rm.shape == rw.shape and len(rw) > 100, (kind, rm.shape, rw.shape)
+        ok = rec_close_scaled(rm, rw)
+        assert ok.all(), (kind, np.argwhere(~ok)[:5])
+        tw = whole.totals()
+        ts = S.merge_slab_totals([h.totals() for h in hs])
+        for k, v in tw.items():
+            assert abs(ts[k] - v) <= 1e-10 * abs(v) + 1e-12 * abs(tw["E"]), (kind, k, ts[k], v)
+
+    check("corona")
+    for step in range(8):
+        for h in hs:
+            h.step(1)
+        whole.step(1)
+        _exchange(hs, ranges, nxy, torch)
+    check("surface")
+    for h in hs + [whole]:
+        h.close()

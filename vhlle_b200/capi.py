@@ -40,7 +40,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
            "vh_batch_destroy", "vh_batch_set_driver", "vh_batch_tune", "vh_batch_advance",
            "vh_batch_sync", "vh_batch_info", "vh_batch_last_error", "vh_batch_timer_start",
-           "vh_batch_timer_stop", "vh_batch_set_mode")
+           "vh_batch_timer_stop", "vh_batch_set_mode", "vh_set_slab", "vh_surface_cells")
 
 
 class VhError(RuntimeError):
@@ -381,6 +381,9 @@ def lib():
                                       ctypes.c_double, ctypes.c_int, ctypes.c_double]
     L.vh_batch_tune.argtypes = [vp, ctypes.c_int]
     L.vh_batch_set_mode.argtypes = [vp, ctypes.c_int]
+    L.vh_set_slab.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    L.vh_surface_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_long,
+                                   ctypes.POINTER(ctypes.c_long)]
     L.vh_batch_advance.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     L.vh_batch_sync.argtypes = [vp, ctypes.POINTER(ctypes.c_uint)]
     L.vh_batch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3
@@ -537,6 +540,24 @@ class GpuHydro:
     def unpack_planes(self, z0, nplanes, buf_ptr):
         """vh_unpack_planes from the device buffer at buf_ptr."""
         self._check(self.L.vh_unpack_planes(self.h, z0, nplanes, ctypes.c_void_p(buf_ptr)))
+
+    def set_slab(self, own0, own1, z_global0, nz_global):
+        """vh_set_slab: the freeze-out output and the totals of this slab's
+        owned planes [own0, own1), its plane 0 being plane z_global0 of a
+        grid of nz_global planes."""
+        self._check(self.L.vh_set_slab(self.h, own0, own1, z_global0, nz_global))
+
+    def surface_cells(self) -> np.ndarray:
+        """[n][3]: the lowest corner (ix, iy, iz of the whole grid) of each
+        element's hypercube, for the last vh_surface or vh_corona."""
+        n = ctypes.c_long()
+        self._check(self.L.vh_surface_cells(self.h, None, 0, ctypes.byref(n)))
+        out = np.zeros((n.value, 3), dtype=np.int32)
+        if n.value:
+            self._check(self.L.vh_surface_cells(
+                self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), n.value,
+                ctypes.byref(n)))
+        return out
 
     def upload(self, fields: dict):
         v = VhStateView()

@@ -536,6 +536,7 @@ vh_status vh_create(const vh_grid* grid, const vh_eos* eos, const vh_trcoeff* tr
   g.dx = dx;
   g.dy = dy;
   g.dz = grid->dz > 0. ? grid->dz : (grid->etamax - grid->etamin) / (grid->nz - 1);
+  vh::geo_whole(g);
   c->grid = *grid;
   c->tau = tau0;
   c->dt = dt;
@@ -1206,6 +1207,7 @@ static vh_status surf_finish(vh_ctx* ctx, vh_surface_info* info) {
   const unsigned bits = H.bits;
   const double* acc = H.acc;
   S.nel = nel;
+  ctx->cells_kind = 1;
   ctx->beta_nel = ctx->vort_on ? nel : 0;
   ctx->EtotSurf += acc[1];
   ctx->nbSurf += acc[2];
@@ -1343,6 +1345,7 @@ vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   }
   const double* acc = H.acc;
   S.nel = H.cnt[0];
+  ctx->cells_kind = 2;
   ctx->corona_cells = H.cnt[0];  // Fluid::num_corona_cells, src/fld.cpp:1071
   ctx->beta_nel = 0;             // the corona writes no beta.dat lines
   ctx->EtotSurf += acc[1];
@@ -1355,6 +1358,66 @@ vh_status vh_corona(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
     info->EtotSurf = ctx->EtotSurf;
     info->nbSurf = ctx->nbCorona;
     info->vEff = ctx->vEff;
+  }
+  return VH_OK;
+}
+
+vh_status vh_set_slab(vh_ctx* ctx, int own0, int own1, int z_global0, int nz_global) {
+  if (!ctx) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_set_slab");
+  vh::Geo& g = ctx->g;
+  if (own0 < 0 || own1 <= own0 || own1 > g.nz || z_global0 < 0 ||
+      (long long)z_global0 + g.nz > nz_global)
+    return fail(ctx, VH_ERR_ARG, "vh_set_slab: the owned planes or the slab's place are out of range");
+  g.zoff = z_global0;
+  g.nzg = nz_global;
+  // the whole grid's interior [2, nz_global - 2) in this slab's planes
+  const int lo = 2 - z_global0, hi = nz_global - 2 - z_global0;
+  g.zc0 = g.zt0 = std::max(own0, lo);
+  g.zc1 = g.zt1 = std::max(g.zc0, std::min(own1, hi));
+  // a cube's upper corner plane must exist here
+  if (g.zc1 > g.nz - 1)
+    return fail(ctx, VH_ERR_ARG, "vh_set_slab: an owned cube's upper plane is not in the slab");
+  return VH_OK;
+}
+
+vh_status vh_surface_cells(vh_ctx* ctx, int* ixyz, long cap, long* n) {
+  if (!ctx || (!ixyz && cap > 0)) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_surface_cells");
+  if (ctx->cells_kind == 0) return fail(ctx, VH_ERR_STATE, "vh_surface_cells: no freeze-out call yet");
+  const vh_ctx::Surf& S = ctx->surf;
+  const long long nel = S.nel;
+  if (n) *n = (long)nel;
+  const long k = (long)std::min<long long>(nel, std::max(0L, cap));
+  if (k == 0) return VH_OK;
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  const vh::Geo& g = ctx->g;
+  const long long niz = g.zc1 - g.zc0, niy = g.ny - 4;
+  auto put = [&](long e, int t) {
+    ixyz[3 * e + 0] = 2 + (int)(t / (niz * niy));  // cube_cell (vh_surface.cuh)
+    ixyz[3 * e + 1] = 2 + (int)((t / niz) % niy);
+    ixyz[3 * e + 2] = g.zc0 + (int)(t % niz) + g.zoff;
+  };
+  if (ctx->cells_kind == 2) {  // a corona element per cube
+    std::vector<int> cubes((size_t)k);
+    VH_CUDA(ctx, cudaMemcpyAsync(cubes.data(), S.cubes, sizeof(int) * k, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (long e = 0; e < k; e++) put(e, cubes[(size_t)e]);
+    return VH_OK;
+  }
+  const int ncubes = S.host->cnt[0];
+  std::vector<int> cubes((size_t)ncubes), off((size_t)ncubes);
+  if (ncubes > 0) {
+    VH_CUDA(ctx, cudaMemcpyAsync(cubes.data(), S.cubes, sizeof(int) * ncubes,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    VH_CUDA(ctx, cudaMemcpyAsync(off.data(), S.cnt, sizeof(int) * ncubes, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  for (int c = 0; c < ncubes; c++) {
+    const long e1 = c + 1 < ncubes ? off[(size_t)c + 1] : (long)nel;
+    for (long e = off[(size_t)c]; e < e1 && e < k; e++) put(e, cubes[(size_t)c]);
   }
   return VH_OK;
 }

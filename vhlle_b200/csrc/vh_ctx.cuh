@@ -60,6 +60,7 @@ struct vh_ctx {
   double* surf_beta = nullptr;  // [cap][16] beta.dat values of the last vh_surface
   size_t cap_beta = 0;
   long long beta_nel = 0;       // its element count (0 after vh_corona)
+  int cells_kind = 0;           // the last freeze-out call: 1 vh_surface, 2 vh_corona
   long long corona_cells = -1;  // elements of the last vh_corona (the beta.dat header)
   // vh_surface_begin / vh_surface_end: one call in flight, its completion event
   bool surf_pending = false;

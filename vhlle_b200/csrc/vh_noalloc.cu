@@ -170,6 +170,7 @@ extern "C" vh_status vh_step_noalloc(const vh_grid* grid, const vh_eos* eos_dev,
   a.g.dx = dx;
   a.g.dy = dy;
   a.g.dz = grid->dz > 0. ? grid->dz : (grid->etamax - grid->etamin) / (grid->nz - 1);
+  vh::geo_whole(a.g);
   a.eos.kind = eos_dev->kind;
   a.eos.conf_cnst = eos_dev->conf_cnst;
   a.eos.ne = eos_dev->ne;

@@ -13,7 +13,20 @@ struct Geo {
   int nx, ny, nz;
   long long N;
   double dx, dy, dz;
+  // the freeze-out surface's and the totals' window in eta (vh_set_slab):
+  // hypercubes whose lowest corner plane is in [zc0, zc1), interior cells
+  // in [zt0, zt1), and where these planes sit in the whole grid (plane 0 is
+  // plane zoff of nzg); the whole grid by default ([2, nz - 2), 0, nz)
+  int zc0, zc1, zt0, zt1, zoff, nzg;
 };
+
+// the default window of a whole grid
+inline void geo_whole(Geo& g) {
+  g.zc0 = g.zt0 = 2;
+  g.zc1 = g.zt1 = g.nz - 2;
+  g.zoff = 0;
+  g.nzg = g.nz;
+}
 
 // Fluid::getCell index with clamping (src/fld.h:70-78)
 __device__ __forceinline__ long long cidx(const Geo& g, int ix, int iy, int iz) {

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kTotBlock) k_totals(Geo g, EosDev E, const dou
                                                       double ecrit, double etamin, bool visc,
                                                       double* __restrict__ partial) {
   __shared__ double red[kTotBlock / 32][kTotals];
-  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.nz - 4;
+  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.zt1 - g.zt0;
   const long long nint = (nix > 0 && niy > 0 && niz > 0) ? (long long)nix * niy * niz : 0;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double c[kTotals];
@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(kTotBlock) k_totals(Geo g, EosDev E, const dou
   for (int k = 0; k < kTotals; k++) c[k] = 0.;
   if (t < nint) {
     // interior cell, z fastest like the reference loop (ix, iy outer)
-    const int iz = 2 + (int)(t % niz);
+    const int iz = g.zt0 + (int)(t % niz);
     const int iy = 2 + (int)((t / niz) % niy);
     const int ix = 2 + (int)(t / ((long long)niz * niy));
     const long long N = g.N;
@@ -100,7 +100,8 @@ __global__ void __launch_bounds__(kTotBlock) k_totals(Geo g, EosDev E, const dou
       c[4] = tau * s * (cosh_int - th * sinh_int) / sqrt(den);
     }
     c[5] = tau * (e + p) * vx / den;
-    if (iz > g.nz / 2 - 3 && iz < g.nz / 2 + 3) {
+    const int izg = iz + g.zoff;  // the plane in the whole grid (Fluid's nz)
+    if (izg > g.nzg / 2 - 3 && izg < g.nzg / 2 + 3) {
       c[8] = e * (fabs(vx) - fabs(vy));
       c[9] = e;
       c[7] = e / sqrt(1. - vx * vx - vy * vy);
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(kTotBlock) k_totals_final(const double* __rest
 }
 
 int totals_blocks(const Geo& g) {
-  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.nz - 4;
+  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.zt1 - g.zt0;
   const long long nint = (nix > 0 && niy > 0 && niz > 0) ? (long long)nix * niy * niz : 0;
   const long long nb = (nint + kTotBlock - 1) / kTotBlock;
   return nb > 0 ? (int)nb : 1;
@@ -194,7 +195,7 @@ __global__ void k_surf_energy(Geo g, EosDev E, const double* __restrict__ Q,
   int ix, iy, iz;
   coords(g, i, ix, iy, iz);
   // only corners of interior cubes: [2, n-2] on every axis
-  if (ix < 2 || iy < 2 || iz < 2 || ix > g.nx - 2 || iy > g.ny - 2 || iz > g.nz - 2) return;
+  if (ix < 2 || iy < 2 || iz < g.zc0 || ix > g.nx - 2 || iy > g.ny - 2 || iz > g.zc1) return;
   const long long N = g.N;
   double q[7], qs[7];
   Prim P;
@@ -713,7 +714,7 @@ void launch_surf_energy(const Geo& g, const EosDev& E, const Fields& f, double t
 }
 
 long long surf_ncube(const Geo& g) {
-  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.nz - 4;
+  const int nix = g.nx - 4, niy = g.ny - 4, niz = g.zc1 - g.zc0;
   return (nix > 0 && niy > 0 && niz > 0) ? (long long)nix * niy * niz : 0;
 }
 

@@ -19,10 +19,11 @@ constexpr int kSurfAcc = 5;
 constexpr int kSurfMaxElemPerCube = 10;
 constexpr int kSurfGeo = 8;
 
-// interior cube t (loop order, iz fastest) -> its lowest corner cell
+// interior cube t (loop order, iz fastest) -> its lowest corner cell; in
+// eta the cubes of the window [zc0, zc1)
 __device__ __forceinline__ void cube_cell(const Geo& g, long long t, int& ix, int& iy, int& iz) {
-  const int niz = g.nz - 4, niy = g.ny - 4;
-  iz = 2 + (int)(t % niz);
+  const int niz = g.zc1 - g.zc0, niy = g.ny - 4;
+  iz = g.zc0 + (int)(t % niz);
   iy = 2 + (int)((t / niz) % niy);
   ix = 2 + (int)(t / ((long long)niz * niy));
 }

@@ -175,3 +175,35 @@ def exchange_halos(dist, ranges, rank: int, pack, unpack, new_buffer) -> None:
             w.wait()
     for z, n, buf in recvs:
         unpack(z, n, buf)
+
+
+def slab_window(ranges, rank: int, nz: int):
+    """vh_set_slab's arguments for `rank`'s slab of a grid of nz planes:
+    (owned z0, owned z1 in its own planes, its first plane in the grid, nz)."""
+    a, b, c, _ = ranges[rank]
+    return a - c, b - c, c, nz
+
+
+def merge_slab_surfaces(parts):
+    """The whole grid's freeze-out records from its slabs' (records [n][29],
+    cells [n][3]) pairs, in slab order: Fluid::outputSurface visits the
+    hypercubes ix-, iy-, then iz-ordered (iz fastest) and writes each cube's
+    elements in turn, so a stable sort of the concatenated records by their
+    cube's (ix, iy, iz) restores its order."""
+    import numpy as np
+    if not parts:
+        return np.zeros((0, 29))
+    rec = np.concatenate([p[0] for p in parts])
+    cells = np.concatenate([np.asarray(p[1]).reshape(-1, 3) for p in parts])
+    order = np.lexsort((cells[:, 2], cells[:, 1], cells[:, 0]))  # stable
+    return rec[order]
+
+
+def merge_slab_totals(parts):
+    """The whole grid's totals from its slabs' (vh_totals dicts): every
+    entry is a sum over the owned interior cells."""
+    out = {}
+    for t in parts:
+        for k, v in t.items():
+            out[k] = out.get(k, 0.0) + v
+    return out
