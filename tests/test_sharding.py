@@ -116,3 +116,36 @@ def test_two_gloo_ranks_slab_decomposed_event_equals_whole_grid(tmp_path):
     for k in slab_worker.FIELDS:
         want = o.state[k].reshape(slab_worker.NCOMP[k], g.nz, g.nx * g.ny)
         assert np.array_equal(z[k], want, equal_nan=True), k
+
+
+def test_merge_slab_surfaces_restores_the_cube_order():
+    """Elements of two slabs (iz 2-4 and 5-7), each in its own cube order,
+    merge into the whole grid's order: (ix, iy, iz) with iz fastest, a
+    cube's elements in their order."""
+    import numpy as np
+    from vhlle_b200 import sharding as S
+    whole = []
+    for ix in (2, 3):
+        for iy in (2, 3):
+            for iz in range(2, 8):
+                for k in range(1 + (ix + iy + iz) % 3):  # 1-3 elements per cube
+                    whole.append((ix, iy, iz, k))
+    whole = np.array(whole)
+    rec = np.zeros((len(whole), 29))
+    rec[:, 0] = np.arange(len(whole))  # the whole grid's element index
+    parts = []
+    for lo, hi in ((2, 5), (5, 8)):
+        sel = (whole[:, 2] >= lo) & (whole[:, 2] < hi)
+        parts.append((rec[sel], whole[sel, :3].astype(np.int32)))
+    merged = S.merge_slab_surfaces(parts)
+    assert np.array_equal(merged[:, 0], np.arange(len(whole)))
+    t = S.merge_slab_totals([{"E": 1.0, "S": 2.0}, {"E": 0.5, "S": 1.0}])
+    assert t == {"E": 1.5, "S": 3.0}
+
+
+def test_slab_window_covers_the_owned_planes():
+    from vhlle_b200 import sharding as S
+    ranges = S.slab_ranges(41, 3)
+    got = [S.slab_window(ranges, r, 41) for r in range(3)]
+    for (a, b, c, d), (o0, o1, z0, nz) in zip(ranges, got):
+        assert (o0 + z0, o1 + z0, nz) == (a, b, 41) and o1 <= d - c
