@@ -436,18 +436,20 @@ vh_status vh_corona(vh_ctx *ctx, double ecrit, vh_surface_info *info);
 vh_status vh_surface_records(vh_ctx *ctx, double *out, long max, long *n);
 vh_status vh_surface_device(vh_ctx *ctx, const double **rec, long *n);
 /* vh_surface in two halves, so that a caller can enqueue the next steps
- * before it waits: vh_surface_begin enqueues the call's kernels and the copy
- * of its counts and sums on the context stream and returns; vh_surface_end
- * waits for them and fills `info` as vh_surface would (the records stay on
- * the device until the next surface or corona call).  One call in flight per
+ * before it waits: vh_surface_begin copies the fields the pass reads (Q,
+ * Qprev, pi, Pi, and dbeta with vorticity on: 25 or 41 doubles per cell,
+ * allocated by the first call) in order on the context stream, then runs
+ * the call's kernels and the copy of its counts and sums from that copy on
+ * a stream of its own, beside the steps the caller queues next, and
+ * returns; vh_surface_end waits for them, orders the context stream after
+ * them and fills `info` as vh_surface would (the records stay on the
+ * device until the next surface or corona call).  One call in flight per
  * context; vh_surface, vh_corona and the record getters refuse while one is.
  * The call runs with the buffers earlier calls left (64k hypercubes and
  * twice as many elements at first, grown by any call that found more).  If
- * it finds more than they hold, its pass copies the fields it reads (Q,
- * Qprev, pi, Pi, and dbeta with vorticity on: 25 or 41 doubles per cell,
- * allocated by the first vh_surface_begin) on the device, and
- * vh_surface_end grows the buffers and runs the pass again on that copy,
- * after whatever the caller queued in between: no call loses elements.
+ * it finds more than they hold, vh_surface_end grows the buffers and runs
+ * the pass again on the copy, on the context stream: no call loses
+ * elements.
  * While a call is pending, vh_upload_state, vh_upload_async, vh_resize2x,
  * vh_enable_vorticity and vh_set_stream return VH_ERR_STATE. */
 vh_status vh_surface_begin(vh_ctx *ctx, double ecrit);

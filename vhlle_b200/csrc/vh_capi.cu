@@ -250,6 +250,11 @@ vh_status vh_destroy(vh_ctx* ctx) {
   if (!ctx) return VH_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  if (ctx->surf_stream) {
+    cudaStreamSynchronize(ctx->surf_stream);
+    cudaStreamDestroy(ctx->surf_stream);
+  }
+  if (ctx->snap_ev) cudaEventDestroy(ctx->snap_ev);
   for (cudaGraphExec_t& x : ctx->step_exec)
     if (x) cudaGraphExecDestroy(x);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
@@ -758,6 +763,27 @@ static vh::StepArgs step_args(vh_ctx* ctx) {
   return a;
 }
 
+// Gives every kernel node of a captured step the device's highest stream
+// priority, so that a pipelined surface pass on its own stream (priority 0)
+// takes only the SM room the step's kernels leave between them.
+static cudaError_t graph_high_priority(cudaGraph_t graph) {
+  int least = 0, greatest = 0;
+  cudaError_t e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  size_t n = 0;
+  if (e == cudaSuccess) e = cudaGraphGetNodes(graph, nullptr, &n);
+  std::vector<cudaGraphNode_t> nodes(n);
+  if (e == cudaSuccess && n) e = cudaGraphGetNodes(graph, nodes.data(), &n);
+  for (size_t i = 0; e == cudaSuccess && i < n; i++) {
+    cudaGraphNodeType t;
+    if ((e = cudaGraphNodeGetType(nodes[i], &t)) != cudaSuccess || t != cudaGraphNodeTypeKernel)
+      continue;
+    cudaLaunchAttributeValue v = {};
+    v.priority = greatest;
+    e = cudaGraphKernelNodeSetAttribute(nodes[i], cudaLaunchAttributePriority, &v);
+  }
+  return e;
+}
+
 // One step (the learned guess, performStep, tau += dt on the device clock)
 // captured into ctx->step_exec[par]; false if the capture is refused.
 static bool capture_step(vh_ctx* ctx, int par) {
@@ -781,7 +807,12 @@ static bool capture_step(vh_ctx* ctx, int par) {
   vh::launch_clock_op(ctx->clk, 0, 0, s);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(s, &graph);
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->step_exec[par], graph, 0);
+  unsigned long long flags = cudaGraphInstantiateFlagUseNodePriority;
+  if (e == cudaSuccess && graph_high_priority(graph) != cudaSuccess) {
+    cudaGetLastError();  // the step runs at its stream's priority then
+    flags = 0;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->step_exec[par], graph, flags);
   if (graph) cudaGraphDestroy(graph);
   if (e != cudaSuccess) {
     cudaGetLastError();
@@ -1061,6 +1092,8 @@ vh_status vh_error_bits(vh_ctx* ctx, unsigned* bits) {
 vh_status vh_clear_errors(vh_ctx* ctx) {
   if (!ctx) return VH_ERR_ARG;
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  // a pending surface pass reports into the same word from its own stream
+  if (ctx->surf_pending) VH_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->surf_ev, 0));
   VH_CUDA(ctx, cudaMemsetAsync(ctx->f.err, 0, sizeof(unsigned), ctx->stream));
   return VH_OK;
 }
@@ -1139,7 +1172,8 @@ static vh_status surf_common(vh_ctx* ctx) {
 // beta.dat values when vorticity is on, and the copies of the counts, sums
 // and error bits into the pinned host block.  Nothing waits.
 static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t want_e,
-                              const vh::Fields& f, double tau, const double* dbeta) {
+                              const vh::Fields& f, double tau, const double* dbeta,
+                              cudaStream_t s) {
   const vh::Geo& g = ctx->g;
   vh_ctx::Surf& S = ctx->surf;
   vh_status st;
@@ -1154,7 +1188,6 @@ static vh_status surf_enqueue(vh_ctx* ctx, double ecrit, size_t want_c, size_t w
   const int cap_e = (int)std::min<size_t>(want_e, INT32_MAX / 32);
   S.pass_cap_c = cap_c;
   S.pass_cap_e = cap_e;
-  cudaStream_t s = ctx->stream;
   const double taup = tau - ctx->fluid_dt;
   vh_ctx::Surf::Host& H = *S.host;
   const vh::EosDev SE = surf_eos(ctx);
@@ -1239,7 +1272,8 @@ vh_status vh_surface(vh_ctx* ctx, double ecrit, vh_surface_info* info) {
   size_t want_c, want_e;
   surf_want(ctx, &want_c, &want_e);
   for (int pass = 0; pass < 2; pass++) {
-    if ((st = surf_enqueue(ctx, ecrit, want_c, want_e, ctx->f, ctx->tau, ctx->vort.dbeta)))
+    if ((st = surf_enqueue(ctx, ecrit, want_c, want_e, ctx->f, ctx->tau, ctx->vort.dbeta,
+                           ctx->stream)))
       return st;
     VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (surf_fits(ctx, &want_c, &want_e)) return surf_finish(ctx, info);
@@ -1256,20 +1290,40 @@ vh_status vh_surface_begin(vh_ctx* ctx, double ecrit) {
   vh_status st;
   if ((st = surf_common(ctx))) return st;
   if (!ctx->surf_ev) VH_CUDA(ctx, cudaEventCreateWithFlags(&ctx->surf_ev, cudaEventDisableTiming));
-  // the copy an overflowing pass leaves for vh_surface_end (allocated here,
-  // on the first call, so that no later call allocates unless it grows)
+  if (!ctx->snap_ev) VH_CUDA(ctx, cudaEventCreateWithFlags(&ctx->snap_ev, cudaEventDisableTiming));
+  if (!ctx->surf_stream)
+    VH_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->surf_stream, cudaStreamNonBlocking));
+  // The call's inputs (Q, Qprev, pi, Pi and, with vorticity, dbeta) are
+  // copied in stream order (allocated on the first call), and the pass runs
+  // on its own stream from that copy, beside the steps the caller queues
+  // next; the copy also serves vh_surface_end when the pass overflows.
   vh_ctx::Surf& S = ctx->surf;
   const bool beta = ctx->vort_on;
-  const size_t keep = (size_t)(beta ? 41 : 25) * ctx->g.N;
+  const long long N = ctx->g.N;
+  const size_t keep = (size_t)(beta ? 41 : 25) * N;
   if ((st = dgrow(ctx, &S.keep, &S.cap_keep, keep))) return st;
+  const vh::Fields& f = ctx->f;
+  const double* src[5] = {f.Q, f.Qprev, f.pi, f.Pi, ctx->vort.dbeta};
+  const int ncomp[5] = {7, 7, 10, 1, 16};
+  size_t off = 0;
+  for (int k = 0; k < (beta ? 5 : 4); k++) {
+    VH_CUDA(ctx, cudaMemcpyAsync(S.keep + off, src[k], sizeof(double) * ncomp[k] * N,
+                                 cudaMemcpyDeviceToDevice, ctx->stream));
+    off += (size_t)ncomp[k] * N;
+  }
+  VH_CUDA(ctx, cudaEventRecord(ctx->snap_ev, ctx->stream));
+  VH_CUDA(ctx, cudaStreamWaitEvent(ctx->surf_stream, ctx->snap_ev, 0));
+  vh::Fields kf = ctx->f;
+  kf.Q = S.keep;
+  kf.Qprev = S.keep + 7 * N;
+  kf.pi = S.keep + 14 * N;
+  kf.Pi = S.keep + 24 * N;
+  const double* kbeta = beta ? S.keep + 25 * N : nullptr;
   size_t want_c, want_e;
   surf_want(ctx, &want_c, &want_e);
-  if ((st = surf_enqueue(ctx, ecrit, want_c, want_e, ctx->f, ctx->tau, ctx->vort.dbeta))) return st;
-  const vh::Fields& f = ctx->f;
-  vh::SurfKeepSrc src{{f.Q, f.Qprev, f.pi, f.Pi, ctx->vort.dbeta}, {7, 7, 10, 1, 16}, beta ? 5 : 4};
-  vh::launch_surf_keep(S.counters, S.pass_cap_c, S.pass_cap_e, src, S.keep, ctx->g.N, ctx->stream);
-  VH_CUDA(ctx, cudaGetLastError());
-  VH_CUDA(ctx, cudaEventRecord(ctx->surf_ev, ctx->stream));
+  if ((st = surf_enqueue(ctx, ecrit, want_c, want_e, kf, ctx->tau, kbeta, ctx->surf_stream)))
+    return st;
+  VH_CUDA(ctx, cudaEventRecord(ctx->surf_ev, ctx->surf_stream));
   S.keep_tau = ctx->tau;
   S.keep_ecrit = ecrit;
   S.keep_beta = beta;
@@ -1283,10 +1337,12 @@ vh_status vh_surface_end(vh_ctx* ctx, vh_surface_info* info) {
   VH_CUDA(ctx, cudaSetDevice(ctx->device));
   ctx->surf_pending = false;
   VH_CUDA(ctx, cudaEventSynchronize(ctx->surf_ev));
+  // what the caller queues next on its stream comes after the pass
+  VH_CUDA(ctx, cudaStreamWaitEvent(ctx->stream, ctx->surf_ev, 0));
   size_t want_c, want_e;
   surf_want(ctx, &want_c, &want_e);
   if (!surf_fits(ctx, &want_c, &want_e)) {
-    // The fields have moved on, but the pass kept its inputs (k_surf_keep):
+    // The fields have moved on, but the pass ran from a copy of its inputs:
     // grow the buffers and run it again on that copy, behind whatever the
     // caller queued since, then wait for it.
     vh_ctx::Surf& S = ctx->surf;
@@ -1298,7 +1354,8 @@ vh_status vh_surface_end(vh_ctx* ctx, vh_surface_info* info) {
     kf.Pi = S.keep + 24 * N;
     const double* kbeta = S.keep_beta ? S.keep + 25 * N : nullptr;
     vh_status st;
-    if ((st = surf_enqueue(ctx, S.keep_ecrit, want_c, want_e, kf, S.keep_tau, kbeta))) return st;
+    if ((st = surf_enqueue(ctx, S.keep_ecrit, want_c, want_e, kf, S.keep_tau, kbeta, ctx->stream)))
+      return st;
     VH_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (!surf_fits(ctx, &want_c, &want_e))
       return fail(ctx, VH_ERR_STATE, "vh_surface_end: element buffers did not grow");

@@ -65,6 +65,10 @@ struct vh_ctx {
   // vh_surface_begin / vh_surface_end: one call in flight, its completion event
   bool surf_pending = false;
   cudaEvent_t surf_ev = nullptr;
+  // a pipelined surface call runs on its own stream from a snapshot of its
+  // inputs, beside the steps that follow it
+  cudaStream_t surf_stream = nullptr;
+  cudaEvent_t snap_ev = nullptr;
   struct Surf {
     double *eN = nullptr, *eP = nullptr, *geo = nullptr, *rec = nullptr, *contrib = nullptr,
            *partial = nullptr;

@@ -826,29 +826,4 @@ void launch_corona(const Geo& g, const EosDev& E, const Fields& f, double tau, d
                                      nullptr, 0);
 }
 
-// A pipelined surface call (vh_surface_begin) whose pass found more
-// straddling cubes or elements than its buffers held keeps a copy of the
-// fields the element pass reads, so that vh_surface_end can grow the
-// buffers and run the pass again after the caller's next steps have moved
-// the grid on.  The copy happens on the device, only on overflow; otherwise
-// every block returns after reading the two counts.
-__global__ void k_surf_keep(const int* __restrict__ counters, int cap_c, int cap_e,
-                            SurfKeepSrc src, double* __restrict__ dst, long long N) {
-  if (counters[0] <= cap_c && counters[1] <= cap_e) return;
-  long long off = 0;
-  for (int k = 0; k < src.n; k++) {
-    const long long len = (long long)src.ncomp[k] * N;
-    const double* __restrict__ p = src.p[k];
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
-         i += (long long)gridDim.x * blockDim.x)
-      dst[off + i] = p[i];
-    off += len;
-  }
-}
-
-void launch_surf_keep(const int* counters, int cap_c, int cap_e, const SurfKeepSrc& src,
-                      double* dst, long long N, cudaStream_t s) {
-  k_surf_keep<<<4 * 148, 256, 0, s>>>(counters, cap_c, cap_e, src, dst, N);
-}
-
 }  // namespace vh

@@ -70,18 +70,6 @@ void launch_surf_beta(const Geo& g, const double* dbeta, double zmin, const int*
                       const int* counters, int cap_cubes, int cap_el, const double* geo,
                       const int* off, double* beta, cudaStream_t s);
 
-// Up to five field arrays (pointer, components) copied back to back by
-// launch_surf_keep.
-struct SurfKeepSrc {
-  const double* p[5];
-  int ncomp[5];
-  int n;
-};
-// dst <- the fields of src when counters[0] > cap_c or counters[1] > cap_e
-// (the pass that wrote the counters overflowed its buffers); nothing else
-void launch_surf_keep(const int* counters, int cap_c, int cap_e, const SurfKeepSrc& src,
-                      double* dst, long long N, cudaStream_t s);
-
 // Cornelius on n independent hypercubes (16 corner values each): counts[k]
 // elements (-1 where the reference stops), geo[k][10][8] centroid + normal
 void launch_cornelius_batch(const double* cubes, int n, const double* dx, double e0, int* counts,
