@@ -332,6 +332,94 @@ typedef struct vh_glauber_ic {
 } vh_glauber_ic;
 vh_status vh_init_glauber(vh_ctx *ctx, const vh_glauber_ic *ic);
 
+/* ---- the reference's initial-state modules, built on the device ----
+ * Each call replaces the host IC module plus vh_upload_state: it leaves
+ * every cell as a fresh Fluid's cell (Cell::Cell, src/cll.cpp:33-52) after
+ * the module's setIC, at the context's tau (the driver's tau0).  Per-source
+ * and per-cell work (smearing, interpolation, the s95p inversion, the
+ * normalisation sums in the reference's loop order, setPrimVar) runs on the
+ * device; per-axis factors (nz or nx*nz values of exp, cosh, tanh, sinh)
+ * are evaluated once on the host with the C library, as the reference
+ * evaluates them.  The modules' console summaries (total energy, angular
+ * momentum) are not printed.  A slab context (vh_set_slab) is refused with
+ * VH_ERR_STATE: the normalisation sums run over the whole grid. */
+
+/* The collision setup constants of IcGlissando (icModel 5) and IcTrento
+ * (icModel 7): src/icGlissando.cpp:33-123, src/icTrento.cpp:33-88.  A setup
+ * leaves unset what it does not use (0 here). */
+typedef struct vh_ic_setup {
+  double sNN;      /* sqrt(s_NN) (GeV): < 100 adds the baryon density, 27
+                      recomputes eta0, sigEta, neta0, nsigma per event */
+  double eta0;     /* midrapidity plateau */
+  double sigEta;   /* diffuseness of the rapidity profile */
+  double etaM;     /* tilt of the sources' rapidity profile (IcGlissando) */
+  double ybeam;    /* beam rapidity */
+  double alphaMix; /* WN / binary mixing */
+  double Rg;       /* transverse Gaussian smearing (fm, IcGlissando) */
+  double A;        /* initial shear flow (0 in every setup) */
+  double nsigma;   /* width of the baryon Gaussian */
+  double neta0;    /* centre of the baryon Gaussian */
+} vh_ic_setup;
+/* The constants of a named setup ("LHC276", "RHIC200", "LHC5020",
+ * "RHIC62", "RHIC27", and for IcGlissando "AFTER72") of model 5 or 7;
+ * VH_ERR_ARG for another name (where the reference exits). */
+vh_status vh_ic_setup_named(int model, const char *name, vh_ic_setup *out);
+
+/* IcGlissando (src/icGlissando.cpp): Gaussian-smeared sources of nevents
+ * GLISSANDO events, each spread over +-(int)(3 Rg / dx) cells (cells with
+ * ix > 0, iy > 0 only, as the reference's loop) with a tilted, plateau
+ * rapidity profile; the entropy normalisation sNorm (and, below 100 GeV,
+ * the baryon normalisation nNorm) iterated to a change of at most 1e-4
+ * against npart = (all sources) / nevents (integer division); then
+ * e = s95p_e(sNorm rho / nevents / dx / dy), nb, nq = 0.4 nb, setPrimVar
+ * and setAllM(1) where e > 0; Qprev stays zero.  Host arrays. */
+typedef struct vh_glissando_ic {
+  vh_ic_setup setup;
+  const double *x, *y; /* [nsrc] source positions (fm), every event in file order */
+  const int *c;        /* [nsrc] the source's code (non-zero; binary-collision
+                          lines, code 0, are dropped by the reader) */
+  const int *npart;    /* [nevents] sources of each event (>= 1) */
+  int nevents;
+} vh_glissando_ic;
+/* norms (may be NULL) <- sNorm, nNorm (nNorm 0 above 100 GeV) */
+vh_status vh_init_glissando(vh_ctx *ctx, const vh_glissando_ic *ic, double *norms);
+
+/* IcTrento (src/icTrento.cpp): the bilinear interpolation of each TRENTO
+ * event's n x n entropy grid over [-grid_max, grid_max]^2 times the plateau
+ * rapidity profile, summed over the events; below 2760 GeV sNorm (and below
+ * 100 GeV nNorm) iterated against the last event's npart; then
+ * e = s95p_e(sNorm rho / nevents) and setPrimVar as IcGlissando.  Host
+ * arrays. */
+typedef struct vh_trento_ic {
+  vh_ic_setup setup;
+  const double *grid;   /* every event's n^2 values in file order (row iy, then ix) */
+  const int *ngrid;     /* [nevents] n (grid-nsteps, >= 2) */
+  const double *gmax;   /* [nevents] grid-max (fm) */
+  const int *npart;     /* [nevents] npart of the header */
+  int nevents;
+} vh_trento_ic;
+vh_status vh_init_trento(vh_ctx *ctx, const vh_trento_ic *ic, double *norms);
+
+/* ICGubser (src/icGubser.cpp, icModel 4): the Gubser flow at t = q = 1,
+ * e = (4 / (1 + 2 (1 + r^2) + (1 - r^2)^2))^(4/3), transverse velocity
+ * 2 r / (2 + r^2) radially, setPrimVar + saveQprev + setAllM. */
+vh_status vh_init_gubser(vh_ctx *ctx);
+
+/* IC (src/ic.cpp, icModel 2) over the table of s95p::loadSongIC
+ * (src/s95p.cpp:43-88): values val[ix * ny + iy] on the axes x[nx], y[ny]
+ * (the first and last entries set the range), times factor and, for
+ * glauber_var 1, turned from entropy to energy by s95p_e; bilinear
+ * interpolation (zero off the table) times the plateau rapidity factor,
+ * cells below e = 0.5 set to vacuum, setPrimVar at rest + saveQprev +
+ * setAllM.  Host arrays. */
+typedef struct vh_table_ic {
+  int nx, ny;
+  const double *x, *y, *val;
+  double factor;    /* s0ScaleFactor */
+  int glauber_var;  /* glauberVar: 1 entropy density, else energy density */
+} vh_table_ic;
+vh_status vh_init_table(vh_ctx *ctx, const vh_table_ic *ic);
+
 /* One event split into slabs along eta (one context per slab, a GPU each):
  * every persistent field (Q, Qh, Qprev, pi, piH, Pi, PiH, m, viscCorrCut:
  * VH_PLANE_DOUBLES doubles per cell) of the z-planes [z0, z0 + nplanes)

@@ -79,6 +79,12 @@ class _State(ctypes.Structure):
                                    "dbeta")]
 
 
+class _IcSetup(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("sNN", "eta0", "sigEta", "etaM", "ybeam",
+                                                "alphaMix", "Rg", "A", "nsigma", "neta0")]
+
+
+_ip = ctypes.POINTER(ctypes.c_int)
 _lib_oracle = None
 _lib_ref = None
 
@@ -118,6 +124,23 @@ def oracle_lib():
                                     ctypes.c_double, ctypes.c_int]
         lib.or_totals.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.POINTER(_Trc),
                                   ctypes.POINTER(_State), ctypes.c_double, ctypes.c_double, _dp]
+        lib.or_pow_cr.restype = ctypes.c_double
+        lib.or_pow_cr.argtypes = [ctypes.c_double, ctypes.c_double]
+        lib.or_s95p_e.restype = ctypes.c_double
+        lib.or_s95p_e.argtypes = [ctypes.c_double, ctypes.c_int]
+        lib.or_ic_glissando.restype = ctypes.c_int
+        lib.or_ic_glissando.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos),
+                                        ctypes.POINTER(_IcSetup), ctypes.c_double, _dp, _dp, _ip,
+                                        _ip, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_State), _dp]
+        lib.or_ic_trento.restype = ctypes.c_int
+        lib.or_ic_trento.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos),
+                                     ctypes.POINTER(_IcSetup), ctypes.c_double, _dp, _ip, _dp, _ip,
+                                     ctypes.c_int, ctypes.c_int, ctypes.POINTER(_State), _dp]
+        lib.or_ic_gubser.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.c_double,
+                                     ctypes.c_int, ctypes.POINTER(_State)]
+        lib.or_ic_table.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
+                                    ctypes.c_int, ctypes.c_int, ctypes.POINTER(_State)]
         _lib_oracle = lib
     return _lib_oracle
 
@@ -158,6 +181,10 @@ def ref_lib():
         lib.ref_eos.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp, _dp]
         lib.ref_eos6.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int, _dp]
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        lib.ref_ic.restype = ctypes.c_int
+        lib.ref_ic.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
+                               ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+        lib.ref_s95p_e.argtypes = [_dp, ctypes.c_int, _dp]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
         lib.ref_cornelius4d.restype = ctypes.c_int
         lib.ref_cornelius4d.argtypes = [_dp, _dp, ctypes.c_double, _dp, _dp]
@@ -307,6 +334,60 @@ def _trc(setup, crmath=False):
     t.zetaSparam = setup.zetaSparam
     t.crmath = int(crmath)
     return t
+
+
+def oracle_ic(setup, model, data=None, ic_setup=None, crmath=False, factor=1.0, glauber_var=1):
+    """The C restatement of an IC module (vh_oracle_ic.c) on setup's grid and
+    EoS at setup.tau0: model 5 IcGlissando (data: ic_files.GlissandoEvents),
+    7 IcTrento (ic_files.TrentoEvents), 4 ICGubser, 2 IC over a table
+    (ic_files.SongTable, factor, glauber_var).  ic_setup: the setup dict of
+    models 5 and 7.  Returns (state dict, (sNorm, nNorm))."""
+    lib = oracle_lib()
+    g = setup.grid
+    grid = _Grid(g.nx, g.ny, g.nz, *g.bounds(), g.cell_dz or 0.0)
+    eos = _EosHolder(setup.eos)
+    eos.s.crmath = int(crmath)
+    st = empty_state(g.ncells)
+    sv = _State()
+    for k in FIELDS:
+        setattr(sv, k, _ptr(st[k]))
+    norms = np.zeros(2)
+    if model in (5, 7):
+        su = _IcSetup(*[float(ic_setup[n]) for n, _ in _IcSetup._fields_])
+    if model == 5:
+        x = np.ascontiguousarray(data.x, dtype=np.float64)
+        y = np.ascontiguousarray(data.y, dtype=np.float64)
+        c = np.ascontiguousarray(data.c, dtype=np.int32)
+        npart = np.ascontiguousarray(data.npart, dtype=np.int32)
+        rc = lib.or_ic_glissando(ctypes.byref(grid), ctypes.byref(eos.s), ctypes.byref(su),
+                                 setup.tau0, _ptr(x), _ptr(y), c.ctypes.data_as(_ip),
+                                 npart.ctypes.data_as(_ip), len(npart), int(crmath),
+                                 ctypes.byref(sv), _ptr(norms))
+        assert rc == 0
+    elif model == 7:
+        src = np.ascontiguousarray(np.concatenate([np.asarray(a, dtype=np.float64).reshape(-1)
+                                                   for a in data.grids]))
+        ngrid = np.array([a.shape[0] for a in data.grids], dtype=np.int32)
+        gmax = np.ascontiguousarray(data.gmax, dtype=np.float64)
+        npart = np.ascontiguousarray(data.npart, dtype=np.int32)
+        rc = lib.or_ic_trento(ctypes.byref(grid), ctypes.byref(eos.s), ctypes.byref(su),
+                              setup.tau0, _ptr(src), ngrid.ctypes.data_as(_ip), _ptr(gmax),
+                              npart.ctypes.data_as(_ip), len(ngrid), int(crmath), ctypes.byref(sv),
+                              _ptr(norms))
+        assert rc == 0
+    elif model == 4:
+        lib.or_ic_gubser(ctypes.byref(grid), ctypes.byref(eos.s), setup.tau0, int(crmath),
+                         ctypes.byref(sv))
+    elif model == 2:
+        x = np.ascontiguousarray(data.x, dtype=np.float64)
+        y = np.ascontiguousarray(data.y, dtype=np.float64)
+        val = np.ascontiguousarray(data.val, dtype=np.float64)
+        lib.or_ic_table(ctypes.byref(grid), ctypes.byref(eos.s), setup.tau0, len(x), len(y),
+                        _ptr(x), _ptr(y), _ptr(val), float(factor), int(glauber_var), int(crmath),
+                        ctypes.byref(sv))
+    else:
+        raise ValueError("no IC model %d" % model)
+    return st, (float(norms[0]), float(norms[1]))
 
 
 class OracleRun:
@@ -589,6 +670,24 @@ class RefRun:
     def step(self, n=1):
         self.lib.ref_step(self.h, n)
         return 0
+
+    def ic(self, model, path="", setup_name="", s0scale=1.0, glauber_var=1):
+        """The reference's IC module `model` (2, 4, 5 or 7: src/main.cpp:324-366)
+        on a fresh Fluid of this run's grid, from the file at path with the
+        named setup; returns Q, Qprev [7][N] and m [N] of every cell."""
+        N = self.setup.grid.ncells
+        Q, Qp, m = np.zeros((7, N)), np.zeros((7, N)), np.zeros(N)
+        rc = self.lib.ref_ic(self.h, model, path.encode(), setup_name.encode(), s0scale,
+                             glauber_var, _ptr(Q), _ptr(Qp), _ptr(m))
+        if rc != 0:
+            raise ValueError("the reference has no IC model %d here" % model)
+        return {"Q": Q, "Qprev": Qp, "m": m}
+
+    def s95p_e(self, s):
+        s = np.ascontiguousarray(s, dtype=np.float64)
+        out = np.zeros_like(s)
+        self.lib.ref_s95p_e(_ptr(s), len(s), _ptr(out))
+        return out
 
     def enable_vorticity(self):
         """Hydro::enableVorticity; before the first output_surface call."""

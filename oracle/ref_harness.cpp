@@ -38,7 +38,12 @@
 #include "eoCMFe.h"
 #include "fld.h"
 #include "hdo.h"
+#include "ic.h"
+#include "icGlissando.h"
+#include "icGubser.h"
+#include "icTrento.h"
 #include "inc.h"
+#include "s95p.h"
 #include "rmn.h"
 #include "trancoeff.h"
 
@@ -46,6 +51,9 @@
 namespace output {
 extern std::ofstream ffreeze, fbeta;
 }
+
+// the params key glauberVar (oracle/ref_globals.cpp)
+extern int glauberVariable;
 
 namespace {
 
@@ -676,6 +684,65 @@ int ref_cornelius4d(const double *cube, const double *dx, double E0, double *cen
   }
   delete[] c;
   return n;
+}
+
+// One of the reference's IC modules run on a fresh Fluid of the run's grid,
+// as the driver does (src/main.cpp:320-366): model 2 IC (the entropy or energy
+// table of file, scaled by s0scale; glauber_var sets glauberVar), 4
+// ICGubser, 5 IcGlissando, 7 IcTrento (file and the setup name).  Returns
+// every cell's Q and Qprev [7][N] and m [N] (its three directions are
+// equal), in the grid order (ix fastest), or -1 for another model.  The
+// modules' console output is discarded.
+int ref_ic(void *p, int model, const char *file, const char *setup, double s0scale,
+           int glauber_var, double *Q, double *Qprev, double *m) {
+  RefRun *r = static_cast<RefRun *>(p);
+  if (model != 2 && model != 4 && model != 5 && model != 7) return -1;
+  // a fresh Fluid (and its Hydro), as the driver builds before the IC
+  delete r->h;
+  delete r->f;
+  r->f = new Fluid(r->eos, r->eosH ? r->eosH : r->eos, r->tr, r->nx, r->ny, r->nz, r->bounds[0],
+                   r->bounds[1], r->bounds[2], r->bounds[3], r->bounds[4], r->bounds[5], r->dt,
+                   r->ecrit);
+  r->h = new Hydro(r->f, r->eos, r->tr, r->tau0, r->dt);
+  std::streambuf *old = std::cout.rdbuf();
+  std::ostringstream quiet;
+  std::cout.rdbuf(quiet.rdbuf());
+  if (model == 2) {
+    glauberVariable = glauber_var;
+    IC ic(file, s0scale);
+    ic.setIC(r->f, r->eos, r->tau0);
+  } else if (model == 4) {
+    ICGubser ic;
+    ic.setIC(r->f, r->eos, r->tau0);
+  } else if (model == 5) {
+    IcGlissando ic(r->f, file, r->tau0, setup);
+    ic.setIC(r->f, r->eos);
+  } else {
+    IcTrento ic(r->f, file, r->tau0, setup);
+    ic.setIC(r->f, r->eos);
+  }
+  std::cout.rdbuf(old);
+  const long N = (long)r->nx * r->ny * r->nz;
+  for (int iz = 0; iz < r->nz; iz++)
+    for (int iy = 0; iy < r->ny; iy++)
+      for (int ix = 0; ix < r->nx; ix++) {
+        const long i = ix + (long)r->nx * (iy + (long)r->ny * iz);
+        Cell *c = r->f->getCell(ix, iy, iz);
+        double q[7], qp[7];
+        c->getQ(q);
+        c->getQprev(qp);
+        for (int k = 0; k < 7; k++) {
+          Q[k * N + i] = q[k];
+          Qprev[k * N + i] = qp[k];
+        }
+        m[i] = c->getM(X_);
+      }
+  return 0;
+}
+
+// s95p::s95p_e (src/s95p.cpp:34-41) of n entropy densities
+void ref_s95p_e(const double *s, int n, double *out) {
+  for (int i = 0; i < n; i++) out[i] = s95p::s95p_e(s[i]);
 }
 
 // Fluid::updateM alone (test of the vacuum-front rule)

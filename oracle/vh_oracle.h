@@ -215,6 +215,38 @@ long or_corona(const or_grid *g, const or_eos *eos, const or_state *s, double ta
 
 int or_abi_version(void);
 
+/* ---- initial states (vh_oracle_ic.c) ---- */
+/* x^y correctly rounded (oracle/crm_shim.cpp) */
+double or_pow_cr(double x, double y);
+/* s95p::s95p_s / s95p_e (src/s95p.cpp:14-41); cr as or_trc.crmath */
+double or_s95p_s(double e, int cr);
+double or_s95p_e(double s, int cr);
+/* The setup constants of IcGlissando / IcTrento (src/icGlissando.cpp:33-123,
+ * src/icTrento.cpp:33-88) */
+typedef struct or_ic_setup {
+  double sNN, eta0, sigEta, etaM, ybeam, alphaMix, Rg, A, nsigma, neta0;
+} or_ic_setup;
+/* IcGlissando (src/icGlissando.cpp): the sources X, Y, C of every event in
+ * file order (C != 0: binary-collision lines already dropped), npart[ev]
+ * per event; norms (may be NULL) <- sNorm, nNorm.  s is overwritten with a
+ * fresh Fluid's cells, then setIC's.  Returns 0, or -1 if out of memory. */
+int or_ic_glissando(const or_grid *g, const or_eos *E, const or_ic_setup *setup, double tau0,
+                    const double *X, const double *Y, const int *C, const int *npart,
+                    int nevents, int cr, or_state *s, double *norms);
+/* IcTrento (src/icTrento.cpp): every event's ngrid[ev]^2 source values in
+ * file order (row iy, then ix), its grid-max and npart */
+int or_ic_trento(const or_grid *g, const or_eos *E, const or_ic_setup *setup, double tau0,
+                 const double *src, const int *ngrid, const double *gmax, const int *npart,
+                 int nevents, int cr, or_state *s, double *norms);
+/* ICGubser (src/icGubser.cpp) at tau */
+void or_ic_gubser(const or_grid *g, const or_eos *E, double tau, int cr, or_state *s);
+/* IC with the table of s95p::loadSongIC (src/ic.cpp, src/s95p.cpp:43-88):
+ * xs[NX], ys[NY] as the loader keeps them, val[ix * NY + iy] as read,
+ * scaled by factor and, for glauber_var 1, turned from entropy to energy */
+void or_ic_table(const or_grid *g, const or_eos *E, double tau, int NX, int NY,
+                 const double *xs, const double *ys, const double *val, double factor,
+                 int glauber_var, int cr, or_state *s);
+
 #ifdef __cplusplus
 }
 #endif

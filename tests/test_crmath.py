@@ -1,4 +1,4 @@
-"""The correctly rounded exp, log and x^(1/4) of vhlle_b200/csrc/vh_crmath.cuh,
+"""The correctly rounded exp, log, x^y and x^(1/4) of vhlle_b200/csrc/vh_crmath.cuh,
 and its divide-free division (Markstein),
 compiled for the host from the same header (IEEE operations and explicit
 fma only, no contraction, so the host build gives the device's bits):
@@ -55,6 +55,12 @@ int main() {
   }
   do {
     if (std::scanf("%la", &x) != 1) break;
+    if (f[0] == 'p' || f[0] == 'q') {  // x^y: pow_cr, or the C library's pow
+      double e;
+      if (std::scanf("%la", &e) != 1) break;
+      std::printf("%a\n", f[0] == 'p' ? vh::crm::pow_cr(x, e) : std::pow(x, e));
+      continue;
+    }
     const double y = f[0] == 'e'   ? vh::crm::exp_cr(x)
                      : f[0] == 'l' ? vh::crm::log_cr(x)
                                    : vh::crm::root4_cr(x);
@@ -83,7 +89,10 @@ def crm(tmp_path_factory):
             inp = "k\n" + "".join("%s\n" % float(x).hex() for x in xs)
             out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True)
             return [bool(int(t)) for t in out.stdout.split()]
-        inp = "".join("%s %s\n" % (kind, float(x).hex()) for x in xs)
+        if kind in "pq":
+            inp = "".join("%s %s %s\n" % (kind, float(x).hex(), float(e).hex()) for x, e in xs)
+        else:
+            inp = "".join("%s %s\n" % (kind, float(x).hex()) for x in xs)
         out = subprocess.run([str(exe)], input=inp, capture_output=True, text=True, check=True)
         return [float.fromhex(t) for t in out.stdout.split()]
     return run
@@ -133,6 +142,45 @@ def test_log_is_correctly_rounded(crm):
     assert not bad, bad[:5]
     assert crm("l", [1.0, 0.0, float("inf")]) == [0.0, -float("inf"), float("inf")]
     assert math.isnan(crm("l", [-1.0])[0]) and math.isnan(crm("l", [float("nan")])[0])
+
+
+def test_pow_is_correctly_rounded(crm):
+    """x^y over the arguments of the initial states' entropy inversion
+    (src/s95p.cpp:14-40: exponents 1.15-4.55, 3/4, 4/3, -1/4, -0.128, -1.18
+    on 1e-6 .. 1e3) and random ones; and how often the C library's pow (the
+    reference's) differs from it."""
+    rng = np.random.default_rng(11)
+    exps = [1.16849, 1.15635, 1.16187, 4.54886, -0.128012, 1.18735, -1.18423, 0.75,
+            4.0 / 3.0, -0.25, 3.0 / 4.0]
+    xs = [(x, e) for e in exps for x in 10 ** rng.uniform(-6, 3, 300)]
+    xs += list(zip(10 ** rng.uniform(-30, 30, 1500), rng.uniform(-8, 8, 1500)))
+    xs += list(zip(rng.uniform(0.5, 2, 500), rng.uniform(-300, 300, 500)))
+    xs += [(2.0, 10.0), (10.0, -3.0), (3.0, 0.5), (1e-300, 0.5), (1.5, 1700.0), (0.5, 1074.0),
+           (0.5, 1075.5), (7.0, 2.0), (1.0000000001, 1e10)]
+    ys = crm("p", xs)
+    ctx = decimal.getcontext()
+    bad = []
+    for (x, e), y in zip(xs, ys):
+        exact = (decimal.Decimal(e) * decimal.Decimal(x).ln()).exp(ctx)
+        if not correctly_rounded(y, exact):
+            bad.append((x, e, y))
+    assert not bad, bad[:5]
+    lib = crm("q", xs)
+    diff = [(x, e, a, b) for (x, e), a, b in zip(xs, ys, lib)
+            if not (a == b or (math.isnan(a) and math.isnan(b)))]
+    # the library's pow (max error ~0.52 ulp) misrounds about 1 call in 1000
+    # here, always by one ulp; pow_cr is the correctly rounded neighbour
+    assert len(diff) <= len(xs) // 200, diff
+    assert all(abs(a - b) <= math.ulp(max(abs(a), abs(b))) for x, e, a, b in diff), diff
+    specials = [(0.0, 2.5), (0.0, -1.5), (-0.0, 3.0), (-0.0, -3.0), (-2.0, 3.0), (-2.0, 2.0),
+                (-2.0, 0.5), (float("inf"), 2.0), (float("inf"), -1.0), (5.0, 0.0),
+                (1.0, float("nan")), (float("nan"), 1.0), (2.0, 1e6), (2.0, -1e6)]
+    got = crm("p", specials)
+    inf, nan = float("inf"), float("nan")
+    want = [0.0, inf, -0.0, -inf, -8.0, 4.0, nan, inf, 0.0, 1.0, 1.0, nan, inf, 0.0]
+    for (x, e), a, b in zip(specials, got, want):
+        assert (math.isnan(a) and math.isnan(b)) or (a == b and math.copysign(1, a) ==
+                                                      math.copysign(1, b)), (x, e, a, b)
 
 
 def test_fourth_root_is_correctly_rounded(crm):

@@ -19,7 +19,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libvhlle_b200.so")
 SOURCES = ["vh_step.cu", "vh_capi.cu", "vh_noalloc.cu", "vh_surface.cu", "vh_vorticity.cu", "vh_mlp.cu",
-           "vh_batch.cu", "vh_ic.cu"]
+           "vh_batch.cu", "vh_ic.cu", "vh_ic_ref.cu"]
 HEADERS = ["vh_physics.cuh", "vh_step.cuh", "vh_surface.cuh", "vh_cornelius.cuh", "vh_mlp.cuh",
            "vh_ctx.cuh"]
 DRIVER_SRC = os.path.join(HERE, "driver", "vhlle_run.cpp")

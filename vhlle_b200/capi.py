@@ -40,7 +40,9 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_mlp_last_error", "vh_mlp_samples", "vh_set_con2prim_guess", "vh_batch_create",
            "vh_batch_destroy", "vh_batch_set_driver", "vh_batch_tune", "vh_batch_advance",
            "vh_batch_sync", "vh_batch_info", "vh_batch_last_error", "vh_batch_timer_start",
-           "vh_batch_timer_stop", "vh_batch_set_mode", "vh_set_slab", "vh_surface_cells")
+           "vh_batch_timer_stop", "vh_batch_set_mode", "vh_set_slab", "vh_surface_cells",
+           "vh_ic_setup_named", "vh_init_glissando", "vh_init_trento", "vh_init_gubser",
+           "vh_init_table")
 
 
 class VhError(RuntimeError):
@@ -268,6 +270,47 @@ class VhGlauberIc(ctypes.Structure):
                 ("nb_peak", ctypes.c_double)]
 
 
+IC_SETUP_FIELDS = ("sNN", "eta0", "sigEta", "etaM", "ybeam", "alphaMix", "Rg", "A", "nsigma",
+                   "neta0")
+
+
+class VhIcSetup(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in IC_SETUP_FIELDS]
+
+
+class VhGlissandoIc(ctypes.Structure):
+    _fields_ = [("setup", VhIcSetup), ("x", _dp), ("y", _dp), ("c", ctypes.POINTER(ctypes.c_int)),
+                ("npart", ctypes.POINTER(ctypes.c_int)), ("nevents", ctypes.c_int)]
+
+
+class VhTrentoIc(ctypes.Structure):
+    _fields_ = [("setup", VhIcSetup), ("grid", _dp), ("ngrid", ctypes.POINTER(ctypes.c_int)),
+                ("gmax", _dp), ("npart", ctypes.POINTER(ctypes.c_int)), ("nevents", ctypes.c_int)]
+
+
+class VhTableIc(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("x", _dp), ("y", _dp), ("val", _dp),
+                ("factor", ctypes.c_double), ("glauber_var", ctypes.c_int)]
+
+
+# icModel of the two readers with named setups (src/main.cpp:342-358)
+IC_GLISSANDO, IC_TRENTO = 5, 7
+
+
+def ic_setup(model: int, name: str) -> dict:
+    """vh_ic_setup_named: the constants of IcGlissando's (model 5) or
+    IcTrento's (model 7) setup `name`, as a dict (ValueError for an unknown
+    name, where the reference exits).  Host-only: needs no GPU."""
+    out = VhIcSetup()
+    if lib().vh_ic_setup_named(model, name.encode(), ctypes.byref(out)) != VH_OK:
+        raise ValueError("no setup %r for icModel %d" % (name, model))
+    return {n: getattr(out, n) for n in IC_SETUP_FIELDS}
+
+
+def _ic_setup_struct(d: dict) -> VhIcSetup:
+    return VhIcSetup(*[float(d[n]) for n in IC_SETUP_FIELDS])
+
+
 class VhTrcoeff(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in (
         "etaS0", "zetaS0", "ah", "al", "aRho", "T0", "etaSMin", "etaSEpsilonMin",
@@ -339,6 +382,11 @@ def lib():
     L.vh_active_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.vh_set_con2prim_method.argtypes = [vp, ctypes.c_int]
     L.vh_init_glauber.argtypes = [vp, ctypes.POINTER(VhGlauberIc)]
+    L.vh_ic_setup_named.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(VhIcSetup)]
+    L.vh_init_glissando.argtypes = [vp, ctypes.POINTER(VhGlissandoIc), _dp]
+    L.vh_init_trento.argtypes = [vp, ctypes.POINTER(VhTrentoIc), _dp]
+    L.vh_init_gubser.argtypes = [vp]
+    L.vh_init_table.argtypes = [vp, ctypes.POINTER(VhTableIc)]
     L.vh_pack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
     L.vh_set_surface_eos.argtypes = [vp, ctypes.POINTER(VhEos)]
     L.vh_unpack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
@@ -522,6 +570,50 @@ class GpuHydro:
         ic = VhGlauberIc(parts.ctypes.data_as(_dp), len(parts), smear, epeak, H.ctypes.data_as(_dp),
                          ecut, nb_peak)
         self._check(self.L.vh_init_glauber(self.h, ctypes.byref(ic)))
+
+    def init_glissando(self, ev, setup: dict):
+        """vh_init_glissando: IcGlissando's initial state (icModel 5) from
+        ic_files.GlissandoEvents and a setup dict (ic_setup(IC_GLISSANDO,
+        name)); returns (sNorm, nNorm)."""
+        x = np.ascontiguousarray(ev.x, dtype=np.float64)
+        y = np.ascontiguousarray(ev.y, dtype=np.float64)
+        c = np.ascontiguousarray(ev.c, dtype=np.int32)
+        npart = np.ascontiguousarray(ev.npart, dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        ic = VhGlissandoIc(_ic_setup_struct(setup), x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
+                           c.ctypes.data_as(ip), npart.ctypes.data_as(ip), len(npart))
+        norms = np.zeros(2)
+        self._check(self.L.vh_init_glissando(self.h, ctypes.byref(ic), norms.ctypes.data_as(_dp)))
+        return float(norms[0]), float(norms[1])
+
+    def init_trento(self, ev, setup: dict):
+        """vh_init_trento: IcTrento's initial state (icModel 7) from
+        ic_files.TrentoEvents and a setup dict; returns (sNorm, nNorm)."""
+        grid = np.ascontiguousarray(np.concatenate([np.asarray(g, dtype=np.float64).reshape(-1)
+                                                    for g in ev.grids]))
+        ngrid = np.array([g.shape[0] for g in ev.grids], dtype=np.int32)
+        gmax = np.ascontiguousarray(ev.gmax, dtype=np.float64)
+        npart = np.ascontiguousarray(ev.npart, dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        ic = VhTrentoIc(_ic_setup_struct(setup), grid.ctypes.data_as(_dp), ngrid.ctypes.data_as(ip),
+                        gmax.ctypes.data_as(_dp), npart.ctypes.data_as(ip), len(ngrid))
+        norms = np.zeros(2)
+        self._check(self.L.vh_init_trento(self.h, ctypes.byref(ic), norms.ctypes.data_as(_dp)))
+        return float(norms[0]), float(norms[1])
+
+    def init_gubser(self):
+        """vh_init_gubser: ICGubser's initial state (icModel 4)."""
+        self._check(self.L.vh_init_gubser(self.h))
+
+    def init_table(self, table, factor=1.0, glauber_var=1):
+        """vh_init_table: IC over the s95p table (icModel 2) from an
+        ic_files.SongTable."""
+        x = np.ascontiguousarray(table.x, dtype=np.float64)
+        y = np.ascontiguousarray(table.y, dtype=np.float64)
+        val = np.ascontiguousarray(table.val, dtype=np.float64)
+        ic = VhTableIc(len(x), len(y), x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
+                       val.ctypes.data_as(_dp), factor, glauber_var)
+        self._check(self.L.vh_init_table(self.h, ctypes.byref(ic)))
 
     def set_surface_eos(self, eos):
         """vh_set_surface_eos: the freeze-out EoS (Fluid's eosH) from a

@@ -1,6 +1,7 @@
-// Correctly rounded exp(x), log(x) and x^(1/4) in FP64, for the transport
-// coefficients (zeta/s forms 1-5, src/trancoeff.cpp:19-70), EoSChiral's
-// power law and EoSHadron's logarithmic table coordinates.  The reference
+// Correctly rounded exp(x), log(x), x^y and x^(1/4) in FP64, for the
+// transport coefficients (zeta/s forms 1-5, src/trancoeff.cpp:19-70),
+// EoSChiral's power law, EoSHadron's logarithmic table coordinates and the
+// entropy-to-energy inversion of the initial states (src/s95p.cpp:14-40).  The reference
 // evaluates them with the host C library, whose exp and pow are accurate to
 // about half an ulp; returning the correctly rounded value reproduces the
 // library's result except where the exact value lies within ~1e-3 ulp of a
@@ -20,6 +21,7 @@
 //        subnormal range rounded to integer multiples of 2^-1074 from the
 //        double-double.  Relative error before the final rounding < 2^-98.
 //   log: a Newton step on the exp above from a faithful seed (log_cr).
+//   x^y: exp of y log(x), both in double-double (pow_cr).
 //   x^(1/4): sqrt(x) as a double-double (the correctly rounded square root
 //        and its exact residual by fma), its square root the same way, and
 //        one rounding of the sum.
@@ -185,9 +187,17 @@ VH_CRM unsigned long long to_bits(double d) {
 // step's own error is of the order of the seed error squared, ~2^-104 |y|);
 // then k ln 2 + y in double-double and one rounding.  Seeds that differ by
 // an ulp give the same result, so host and device agree.
+VH_CRM dd log_dd(double x);
+
 VH_CRM double log_cr(double x) {
   if (!(x > 0.)) return x == 0. ? -(double)INFINITY : (double)NAN;
   if (x == (double)INFINITY) return x;
+  return log_dd(x).hi;
+}
+
+// log(x) as a double-double for finite x > 0 (relative error ~2^-102):
+// the steps of log_cr before its one rounding
+VH_CRM dd log_dd(double x) {
   int k = 0;
   if (x < 0x1p-1022) {  // subnormal: scale into the normal range (exact)
     x *= 0x1p54;
@@ -208,7 +218,55 @@ VH_CRM double log_cr(double x) {
   const double kd = (double)k;
   dd L = add(two_prod(kd, VH_CRM_LN2_2), {kd * VH_CRM_LN2_3, 0.});
   L = add({kd * VH_CRM_LN2_1, 0.}, L);
-  return add(L, y).hi;
+  return add(L, y);
+}
+
+// exp(t.hi + t.lo) for a double-double argument (|t.lo| <= ulp(t.hi)), as
+// exp_cr: the low part joins the reduced argument before expm1
+VH_CRM double exp_dd_cr(dd t) {
+  const double x = t.hi;
+  if (!(x == x)) return x;  // NaN
+  if (x > 709.8) return (double)INFINITY;
+  if (x < -746.0) return 0.0;
+  const double INV_LN2 = 0x1.71547652b82fep+0;
+  const double k = rint(x * INV_LN2);
+  dd r = two_sum(x, -(k * VH_CRM_LN2_1));
+  r = add(r, {-two_prod(k, VH_CRM_LN2_2).hi, -two_prod(k, VH_CRM_LN2_2).lo});
+  r = add(r, {-(k * VH_CRM_LN2_3), t.lo});
+  const dd y = add({1.0, 0.0}, expm1_dd(r));
+  return scale_round(y, (int)k);
+}
+
+// x^y, correctly rounded but where the exact value lies within ~2^-38 ulp
+// of a rounding boundary: exp(y log x) with log x a double-double
+// (log_dd), the product y log x a double-double (absolute error below
+// 2^-92 while it is in exp's range) and exp_dd_cr.  y = 2 is x * x (one
+// rounding of the exact square, which can be a tie).  The C library's
+// special values: x^0 = 1 and 1^y = 1 (NaN included), NaN otherwise
+// propagates; 0^y = +0 (y > 0) or +inf (y < 0), with -0 kept for odd
+// integers y; inf^y = inf or 0; negative x for integer y only (NaN else).
+VH_CRM double pow_cr(double x, double y) {
+  if (y == 0. || x == 1.) return 1.;
+  if (!(x == x) || !(y == y)) return x + y;
+  if (y == 2.) return x * x;
+  const bool yint = rint(y) == y;
+  const bool yodd = yint && fabs(y) < 0x1p53 && fmod(y, 2.0) != 0.;
+  if (x == 0.) {
+    const double r = y > 0. ? 0. : (double)INFINITY;
+    return (yodd && to_bits(x) >> 63) ? -r : r;
+  }
+  double sgn = 1.;
+  if (x < 0.) {
+    if (!yint) return (double)NAN;
+    if (yodd) sgn = -1.;
+    x = -x;
+  }
+  if (x == (double)INFINITY) return sgn * (y > 0. ? (double)INFINITY : 0.);
+  const dd L = log_dd(x);
+  const dd t = mul({y, 0.}, L);
+  if (t.hi > 709.8) return sgn * (double)INFINITY;
+  if (t.hi < -746.0) return sgn * 0.;
+  return sgn * exp_dd_cr(t);
 }
 
 // x^(1/4) for x >= 0 (x = +0 gives +0, x = inf gives inf)
