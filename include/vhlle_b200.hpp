@@ -27,6 +27,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "vhlle_b200.h"
@@ -1023,6 +1024,9 @@ class Hydro {
     return n;
   }
   vh_ctx* context() const { return ctx_; }
+  // The device cells were set by a device builder (IcGlissando::setIC and
+  // the like below): the first step must not upload the host Fluid's.
+  void adoptDeviceState() { uploaded_ = true; }
 
   // expandGrid2x (src/main.cpp:246-271): the device grid doubles its
   // transverse range and the step doubles.  Returns the new host Fluid (its
@@ -1047,6 +1051,149 @@ inline Fluid* expandGrid2x(Hydro* h, EoS* eos, EoS* eosH, TransportCoeff* tr) {
   delete f;
   return fnew;
 }
+
+// ------------------------------------------------------ initial states
+// The reference's IC modules (src/icGlissando.h, src/icTrento.h,
+// src/icGubser.h, src/ic.h) with their constructors' file reading, built on
+// the device: setIC fills the Hydro's device cells (vh_init_glissando,
+// vh_init_trento, vh_init_gubser, vh_init_table) at the Hydro's tau, where
+// the reference's setIC(Fluid*, EoS*) fills host cells; call sync() for a
+// host copy.  An unknown setup name throws (the reference exits).
+
+// IcGlissando (icModel 5): "x y c w" lines, c != 0 kept, a line that does
+// not parse ending an event that holds sources (src/icGlissando.cpp:130-160)
+class IcGlissando {
+  vh_ic_setup setup_{};
+  std::vector<double> x_, y_;
+  std::vector<int> c_, npart_;
+
+ public:
+  IcGlissando(Fluid*, const char* filename, double /*tau0: the Hydro's*/, const char* setup) {
+    check(vh_ic_setup_named(5, setup, &setup_), nullptr);
+    std::ifstream fin(filename);
+    if (!fin.good()) throw Error(VH_ERR_ARG, std::string("I/O error with ") + filename);
+    std::string line;
+    int np = 0;
+    // line by line until end of file: a file that ends with a newline gives
+    // a last, empty line, which ends the last event (without the newline the
+    // last event is not counted, as in the reference)
+    while (!fin.eof()) {
+      std::getline(fin, line);
+      std::istringstream in(line);
+      double x, y, w;
+      int c;
+      if (in >> x >> y >> c >> w) {
+        if (c != 0) {
+          x_.push_back(x);
+          y_.push_back(y);
+          c_.push_back(c);
+          if (++np > 9999) throw Error(VH_ERR_ARG, "IcGlissando: more sources in an event than NP");
+        }
+      } else if (np > 0) {
+        npart_.push_back(np);
+        np = 0;
+      }
+    }
+    if (npart_.empty()) throw Error(VH_ERR_ARG, std::string("no GLISSANDO events in ") + filename);
+  }
+  int nevents() const { return (int)npart_.size(); }
+  // returns sNorm, nNorm
+  std::pair<double, double> setIC(Hydro* h) {
+    vh_glissando_ic ic{setup_, x_.data(), y_.data(), c_.data(), npart_.data(), nevents()};
+    double norms[2];
+    check(vh_init_glissando(h->context(), &ic, norms), h->context());
+    h->adoptDeviceState();
+    return {norms[0], norms[1]};
+  }
+};
+
+// IcTrento (icModel 7): per event the header's npart (line 3, column 9),
+// grid-nsteps (line 10, column 15) and grid-max (line 11, column 12), then
+// n rows of n values; an empty third header line ends the file
+// (src/icTrento.cpp:115-179)
+class IcTrento {
+  vh_ic_setup setup_{};
+  std::vector<double> grid_, gmax_;
+  std::vector<int> ngrid_, npart_;
+
+ public:
+  IcTrento(Fluid*, const char* filename, double /*tau0: the Hydro's*/, const char* setup) {
+    check(vh_ic_setup_named(7, setup, &setup_), nullptr);
+    std::ifstream fin(filename);
+    if (!fin.good()) throw Error(VH_ERR_ARG, std::string("I/O error with ") + filename);
+    auto field = [](const std::string& l, size_t col) {
+      return l.size() > col ? l.substr(col) : std::string();
+    };
+    for (;;) {
+      std::string l[11];
+      for (int k = 0; k < 3; k++) std::getline(fin, l[k]);
+      if (l[2].empty()) break;
+      for (int k = 3; k < 11; k++) std::getline(fin, l[k]);
+      int npart = 0, n = 0;
+      double gmax = 0.;
+      std::istringstream(field(l[2], 9)) >> npart;
+      std::istringstream(field(l[9], 15)) >> n;
+      std::istringstream(field(l[10], 12)) >> gmax;
+      if (n < 2) throw Error(VH_ERR_ARG, std::string("bad grid-nsteps in ") + filename);
+      for (long long k = 0; k < (long long)n * n; k++) {
+        double v = 0.;
+        fin >> v;
+        grid_.push_back(v);
+      }
+      std::string rest;
+      std::getline(fin, rest);
+      npart_.push_back(npart);
+      ngrid_.push_back(n);
+      gmax_.push_back(gmax);
+    }
+    if (npart_.empty()) throw Error(VH_ERR_ARG, std::string("no TRENTO events in ") + filename);
+  }
+  int nevents() const { return (int)npart_.size(); }
+  std::pair<double, double> setIC(Hydro* h) {
+    vh_trento_ic ic{setup_, grid_.data(), ngrid_.data(), gmax_.data(), npart_.data(), nevents()};
+    double norms[2];
+    check(vh_init_trento(h->context(), &ic, norms), h->context());
+    h->adoptDeviceState();
+    return {norms[0], norms[1]};
+  }
+};
+
+// ICGubser (icModel 4)
+class ICGubser {
+ public:
+  void setIC(Hydro* h) {
+    check(vh_init_gubser(h->context()), h->context());
+    h->adoptDeviceState();
+  }
+};
+
+// IC (icModel 2) over the table of s95p::loadSongIC: "NX NY" then NX*NY
+// lines "x y value" (src/s95p.cpp:43-66); glauberVar 1 reads entropy
+class IC {
+  std::vector<double> x_, y_, val_;
+  int nx_ = 0, ny_ = 0;
+  double factor_;
+  int glauberVar_;
+
+ public:
+  IC(const char* icInputFile, double s0ScaleFactor, int glauberVar = 1)
+      : factor_(s0ScaleFactor), glauberVar_(glauberVar) {
+    std::ifstream fin(icInputFile);
+    if (!fin) throw Error(VH_ERR_ARG, std::string("cannot open ") + icInputFile);
+    fin >> nx_ >> ny_;
+    if (nx_ < 2 || ny_ < 2) throw Error(VH_ERR_ARG, std::string("bad table size in ") + icInputFile);
+    x_.assign(nx_, 0.);
+    y_.assign(ny_, 0.);
+    val_.assign((size_t)nx_ * ny_, 0.);
+    for (int ix = 0; ix < nx_; ix++)
+      for (int iy = 0; iy < ny_; iy++) fin >> x_[ix] >> y_[iy] >> val_[(size_t)ix * ny_ + iy];
+  }
+  void setIC(Hydro* h) {
+    vh_table_ic ic{nx_, ny_, x_.data(), y_.data(), val_.data(), factor_, glauberVar_};
+    check(vh_init_table(h->context(), &ic), h->context());
+    h->adoptDeviceState();
+  }
+};
 
 // ------------------------------------------------------------- parameters
 // The reference driver's parameters with their defaults (src/main.cpp:70-81)

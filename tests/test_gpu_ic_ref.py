@@ -167,3 +167,43 @@ def test_gpu_ic_refused_on_a_slab(grid_setup):
         assert e.value.args[0].startswith("vhlle_b200 status %d" % capi.VH_ERR_STATE)
     finally:
         h.close()
+
+
+@pytest.mark.parametrize("model", [5, 7, 4])
+def test_gpu_driver_builds_the_reference_ic(model, grid_setup, tmp_path):
+    """vhlle_run with icModel 5 (IcGlissando), 7 (IcTrento) or 4 (ICGubser):
+    the initial state built on the device (the printed sNorm is the
+    oracle's), then the corona at tau0 equals the oracle's on that state."""
+    import dataclasses
+    import subprocess
+    from vhlle_b200 import build as B
+    drv = B.build_driver()
+    setup = grid_setup
+    extra = dict(icModel=model, tauMax=setup.tau0 + setup.dt, eos1fFile=str(tmp_path / "eos.dat"))
+    setup.eos.write_eos1f(str(tmp_path / "eos.dat"))
+    args = []
+    if model == 5:
+        path = str(tmp_path / "sources.txt")
+        F.write_glissando(path, F.synthetic_glissando_events(3, seed=5))
+        o, norms = P.oracle_ic(setup, 5, F.read_glissando(path),
+                               capi.ic_setup(capi.IC_GLISSANDO, "RHIC200"), crmath=True)
+        args = ["-ISinput", path, "-system", "RHIC200"]
+    elif model == 7:
+        path = str(tmp_path / "trento.dat")
+        F.write_trento(path, F.synthetic_trento_events(2, seed=7, n=60))
+        o, norms = P.oracle_ic(setup, 7, F.read_trento(path),
+                               capi.ic_setup(capi.IC_TRENTO, "RHIC62"), crmath=True)
+        args = ["-ISinput", path, "-system", "RHIC62"]
+    else:
+        o, norms = P.oracle_ic(setup, 4, crmath=True)
+    params = str(tmp_path / "params.txt")
+    W.write_params(params, setup, **extra)
+    out = tmp_path / "out"
+    run = subprocess.run([drv, "-params", params, *args, "-outputDir", str(out)],
+                         capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout[-2000:] + run.stderr
+    if model in (5, 7):
+        assert "sNorm set to %.17g" % norms[0] in run.stdout, run.stdout[-1500:]
+    ic_setup = dataclasses.replace(setup, Q=o["Q"], m=o["m"][0].copy())
+    corona, _ = P.OracleRun(ic_setup).corona()
+    assert "corona elements : %d" % len(corona) in run.stdout, run.stdout[-1500:]

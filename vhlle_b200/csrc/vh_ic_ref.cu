@@ -327,7 +327,10 @@ __global__ void __launch_bounds__(kTpb) k_ic_terms(TermArgs a) {
 }
 
 // sum of t[0..n) from 0.0 in index order, rounded after every addition as
-// the host loop: the warp loads 32 terms at a time, lane 0 adds them in turn
+// the host loop: the warp loads 32 terms at a time, lane 0 adds the non-zero
+// ones in turn.  Skipping zeros changes nothing: the running sum starts at
+// +0 and is never -0 (an exact cancellation rounds to +0), and s + (+-0) = s
+// for every other s; the vacuum cells' terms are exactly zero.
 __global__ void __launch_bounds__(32) k_seq_sum(const double* __restrict__ t, long long n,
                                                 double* __restrict__ out) {
   const int lane = threadIdx.x;
@@ -335,8 +338,10 @@ __global__ void __launch_bounds__(32) k_seq_sum(const double* __restrict__ t, lo
   for (long long base = 0; base < n; base += 32) {
     const long long k = base + lane;
     const double v = k < n ? t[k] : 0.0;
-    const int m = (int)min(32LL, n - base);
-    for (int j = 0; j < m; j++) {
+    unsigned live = __ballot_sync(0xffffffffu, v != 0.0);  // NaN counts
+    while (live) {
+      const int j = __ffs(live) - 1;
+      live &= live - 1;
       const double x = __shfl_sync(0xffffffffu, v, j);
       if (lane == 0) s += x;
     }

@@ -1,10 +1,16 @@
 // vhlle_run -- the reference driver's evolution loop (src/main.cpp:273-441)
 // over the device hydro: parameters file, substeps, one-shot x2 resize,
-// termination at tauMax, with the initial grid read from a snapshot instead
-// of the reference's initial-state models.
+// termination at tauMax.  The initial state (src/main.cpp:320-366) is built
+// on the device by the reference's modules for icModel 2 (IC over the s95p
+// table of -ISinput, s0ScaleFactor, glauberVar), 4 (ICGubser), 5
+// (IcGlissando) and 7 (IcTrento), the last two reading -ISinput with the
+// setup named by -system, at tau0; or, whatever icModel says, it is read
+// from -ISinput when that file is a grid snapshot (VHBSNAP1, which fixes
+// tau0).  The other models (the GSL optical Glauber, the UrQMD and SMASH
+// particle lists, TRENTO 3D, SuperMC) are refused.
 //
-//   vhlle_run -params FILE -ISinput SNAPSHOT [-outputDir DIR] [-system S]
-//             [-printParams]
+//   vhlle_run -params FILE [-ISinput SNAPSHOT|ICFILE] [-outputDir DIR]
+//             [-system S] [-printParams]
 //
 // Parameters are read exactly as the reference reads them (same keys,
 // defaults, "CCC"/"UUU" echo).  The hydro EoS is the EoS1f table named by
@@ -30,6 +36,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <iomanip>
 #include <iostream>
 #include <string>
@@ -97,7 +104,18 @@ int run(int argc, char** argv) {
   const CommandLine cl = readCommandLine(argc, argv, P);
   printParameters(P);
   if (cl.printParams) return 0;
-  if (cl.isInputFile.empty()) throw vhb::Error(VH_ERR_ARG, "no -ISinput snapshot given");
+  bool snapshot = false;
+  if (!cl.isInputFile.empty()) {
+    std::ifstream in(cl.isInputFile, std::ios::binary);
+    char tag[8] = {};
+    in.read(tag, 8);
+    snapshot = in && std::memcmp(tag, "VHBSNAP1", 8) == 0;
+  }
+  if (!snapshot && P.icModel != 2 && P.icModel != 4 && P.icModel != 5 && P.icModel != 7)
+    throw vhb::Error(VH_ERR_ARG, "icModel " + std::to_string(P.icModel) +
+                                     " is not built here: give a grid snapshot as -ISinput");
+  if (!snapshot && P.icModel != 4 && cl.isInputFile.empty())
+    throw vhb::Error(VH_ERR_ARG, "no -ISinput given");
 
   const double hbarc = 0.1973269804, deg = 16.0 + 3.0 * 12.0 * (7.0 / 8.0);
   struct stat sb;
@@ -147,18 +165,41 @@ int run(int argc, char** argv) {
       P.etaSScaleMuB, P.zetaSPeakEpsilon, P.zetaSScaleBeta, P.zetaSSigmaMinus,
       P.zetaSSigmaPlus, eos, P.etaSparam, P.zetaSparam);
 
-  const auto hdr = vhb::Fluid::readSnapshotHeader(cl.isInputFile.c_str());
-  if (hdr.grid.nx != P.nx || hdr.grid.ny != P.ny || hdr.grid.nz != P.nz ||
-      hdr.grid.xmin != P.xmin || hdr.grid.xmax != P.xmax || hdr.grid.ymin != P.ymin ||
-      hdr.grid.ymax != P.ymax || hdr.grid.etamin != P.etamin || hdr.grid.etamax != P.etamax)
-    throw vhb::Error(VH_ERR_ARG, "the snapshot's grid differs from the parameters' grid");
   vhb::Fluid* f = new vhb::Fluid(eos, eosH, trcoeff, P.nx, P.ny, P.nz, P.xmin, P.xmax, P.ymin,
                                  P.ymax, P.etamin, P.etamax, P.dtau, P.eCrit);
-  f->loadSnapshot(cl.isInputFile.c_str());
-  const double tau0 = hdr.tau;  // the snapshot fixes the start time
-  std::cout << "fluid allocation done\nIC done (tau0 = " << tau0 << ")\n";
+  double tau0 = P.tau0;
+  if (snapshot) {
+    const auto hdr = vhb::Fluid::readSnapshotHeader(cl.isInputFile.c_str());
+    if (hdr.grid.nx != P.nx || hdr.grid.ny != P.ny || hdr.grid.nz != P.nz ||
+        hdr.grid.xmin != P.xmin || hdr.grid.xmax != P.xmax || hdr.grid.ymin != P.ymin ||
+        hdr.grid.ymax != P.ymax || hdr.grid.etamin != P.etamin || hdr.grid.etamax != P.etamax)
+      throw vhb::Error(VH_ERR_ARG, "the snapshot's grid differs from the parameters' grid");
+    f->loadSnapshot(cl.isInputFile.c_str());
+    tau0 = hdr.tau;  // the snapshot fixes the start time
+  }
+  std::cout << "fluid allocation done\n";
 
   vhb::Hydro* h = new vhb::Hydro(f, eos, trcoeff, tau0, P.dtau);
+  if (!snapshot) {  // src/main.cpp:324-366, the modules built on the device
+    const char* file = cl.isInputFile.c_str();
+    const char* sys = cl.collSystem.c_str();
+    if (P.icModel == 2) {
+      vhb::IC(file, P.s0ScaleFactor, P.glauberVariable).setIC(h);
+    } else if (P.icModel == 4) {
+      vhb::ICGubser().setIC(h);
+    } else if (P.icModel == 5) {
+      vhb::IcGlissando ic(f, file, tau0, sys);
+      const auto n = ic.setIC(h);
+      std::cout << "IcGlissando: loaded " << ic.nevents() << " events, sNorm set to " << n.first
+                << "\n";
+    } else {
+      vhb::IcTrento ic(f, file, tau0, sys);
+      const auto n = ic.setIC(h);
+      std::cout << "IcTrento: loaded " << ic.nevents() << " events, sNorm set to " << n.first
+                << "\n";
+    }
+  }
+  std::cout << "IC done (tau0 = " << tau0 << ")\n";
   if (P.vorticityOn) h->enableVorticity();  // src/main.cpp:379-382
   // Fluid::initOutput (src/fld.cpp:119-129): the output directory and a
   // fresh freezeout.dat.unfinished
