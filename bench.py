@@ -14,7 +14,7 @@ copy) and include those surface calls.
 Multi-GPU (torchrun, N ranks): events are independent, so every rank runs
 its own event (seed + rank) with no collective on the data path; the time is
 the max over ranks (weak scaling).  The per-GPU legs below (batched_mlp,
-batched_mlp_large, batch_2d, learned_guess) run at N = 1 only.
+batched_mlp_large, batch_2d, learned_guess, ic_build) run at N = 1 only.
 
 The JSON line carries, besides the contract keys:
   roofline      the dominant kernel's algorithmic bytes per launch over its
@@ -36,7 +36,13 @@ The JSON line carries, besides the contract keys:
   batched_mlp_large  the same on 8 large events (201x201x101);
   batch_2d      64 2+1D events batched (the tuner's form, the stage-batched
                 form and a branch per event) against each alone;
-  learned_guess the con2prim modes on one event with baryon charge.
+  learned_guess the con2prim modes on one event with baryon charge;
+  ic_build      the reference's IcGlissando initial state (10 seeded
+                GLISSANDO events, setup RHIC62) built on the device
+                (vh_init_glissando) on the benchmark grid, beside the
+                reference's own module on one host thread (the reference
+                time also sits in cpu_baseline.ic_build_reference_s).
+`--ic-only` times the ic_build leg alone (for profiler captures).
 """
 from __future__ import annotations
 
@@ -257,6 +263,64 @@ def nvtx(name=None):
             torch.cuda.nvtx.range_push(name)
     except Exception:
         pass
+
+
+# the initial-state leg: IcGlissando (icModel 5) of IC_EVENTS seeded
+# GLISSANDO events, collision setup IC_SETUP (baryon density on), on the
+# benchmark grid
+IC_EVENTS, IC_SEED, IC_SETUP = 10, 11, "RHIC62"
+
+
+def ic_events(path):
+    from vhlle_b200 import ic_files as F
+    F.write_glissando(path, F.synthetic_glissando_events(IC_EVENTS, seed=IC_SEED))
+    return F.read_glissando(path)
+
+
+def ic_build_measure(capi, W, grid, device, reps=3):
+    """vh_init_glissando on the device: the best of `reps` calls after one
+    warm-up call, host wall clock around the call (it returns after its last
+    copy), input file parsed beforehand."""
+    import tempfile
+    setup = W.glauber3d_setup(*grid, seed=EVENT_SEED)
+    su = capi.ic_setup(capi.IC_GLISSANDO, IC_SETUP)
+    with tempfile.TemporaryDirectory() as d:
+        ev = ic_events(os.path.join(d, "sources.txt"))
+    h = capi.GpuHydro(setup, device=device, upload=False)
+    try:
+        norms = h.init_glissando(ev, su)
+        best = float("inf")
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            h.init_glissando(ev, su)
+            best = min(best, time.perf_counter() - t0)
+    finally:
+        h.close()
+    return {"module": "IcGlissando (icModel 5)", "setup": IC_SETUP, "events": IC_EVENTS,
+            "sources": int(len(ev.x)), "grid": "x".join(map(str, grid)), "device_s": best,
+            "sNorm": norms[0], "nNorm": norms[1]}
+
+
+def ic_reference_sample(grid):
+    """The reference's IcGlissando constructor + setIC (oracle/_ref) on the
+    same input, one thread; None where the reference is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as P
+    import tempfile
+    from vhlle_b200 import workloads as W
+    if not P.ref_available():
+        return None
+    setup = W.glauber3d_setup(*grid, seed=EVENT_SEED)
+    run = P.RefRun(setup)
+    try:
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "sources.txt")
+            ic_events(path)
+            t0 = time.perf_counter()
+            run.ic(5, path, IC_SETUP)
+            return time.perf_counter() - t0
+    finally:
+        run.close()
 
 
 def cpu_baseline_sample(setup, steps=2):
@@ -697,6 +761,10 @@ def main():
     ap.add_argument("--vorticity", action="store_true",
                     help="the event with Hydro::enableVorticity (dbeta every step, beta.dat "
                          "values at every surface)")
+    ap.add_argument("--no-ic", action="store_true",
+                    help="skip the initial-state leg (IcGlissando on the device)")
+    ap.add_argument("--ic-only", action="store_true",
+                    help="time the initial-state leg alone and print it (profiler captures)")
     ap.add_argument("--grid", default="101,101,51",
                     help="nx,ny,nz of the event (smaller grids only for profiler captures)")
     args = ap.parse_args()
@@ -706,6 +774,10 @@ def main():
 
     from vhlle_b200 import capi
     from vhlle_b200 import workloads as W
+
+    if args.ic_only:
+        print(json.dumps({"ic_build": ic_build_measure(capi, W, args.grid, 0)}), flush=True)
+        return 0
 
     ws, rank, local = dist_env()
     dist = Ranks(ws)
@@ -901,9 +973,19 @@ def main():
     if mlp is not None:
         mlp.close()
 
+    ic = None
+    if legs and not args.no_ic:
+        ic = ic_build_measure(capi, W, args.grid, local)
+
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(W.glauber3d_setup(nx, ny, nz, seed=EVENT_SEED))
+        if ic is not None:
+            ref_s = ic_reference_sample(args.grid)
+            cpu["ic_build_reference_s"] = ref_s
+            if ref_s is not None:
+                ic["reference_s"] = ref_s
+                ic["speedup"] = ref_s / ic["device_s"]
 
     if rank == 0:
         line = {
@@ -921,10 +1003,10 @@ def main():
             "kernels": kernels,
             "e2e": e2e, "cpu_baseline": cpu, "batched_mlp": bmlp, "batch_2d": batch2d,
             "batched_mlp_large": large,
-            "learned_guess": learned,
+            "learned_guess": learned, "ic_build": ic,
             # the step graph's kernels, and per pipelined surface call its
-            # nine kernels plus the overflow check (k_surf_keep)
-            "gpu_launches": lps * args.steps + 10 * (args.steps // SURF_EVERY), "clocks": clocks,
+            # nine kernels
+            "gpu_launches": lps * args.steps + 9 * (args.steps // SURF_EVERY), "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     h.close()

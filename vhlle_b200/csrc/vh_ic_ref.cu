@@ -20,8 +20,9 @@
 //   k_ic_terms    a normalisation pass's per-cell terms (s95p_e and the
 //                 cell's energy, or its baryon number), written in the
 //                 reference's loop order (ix, iy, iz)
-//   k_seq_sum     their sum in that order, one lane adding what the warp
-//                 loads: the same rounded sum as the host loop
+//   k_seq_sum     their sum in that order, one thread adding tiles that
+//                 the block's other warps stage in shared memory: the same
+//                 rounded sum as the host loop
 //   k_ic_set      e = s95p_e(..), nb, setPrimVar, setAllM for every cell
 //   k_ic_gubser, k_table_prep, k_ic_table   the other two modules
 //
@@ -57,33 +58,39 @@ constexpr int kKz = 8;             // eta cells per thread in the source sums
 constexpr int kS95pMaxIt = 200;    // the reference iterates without a bound
 constexpr int kNormMaxIt = 10000;  // likewise its normalisation loops
 
+// x^y and e^x kept out of line: s95p_s holds up to six powers and two
+// exponentials, each ~800 FP64 operations inlined, and the Newton loop
+// around it would otherwise be tens of KB of straight-line code per kernel
+__device__ __noinline__ double pw(double x, double y) { return crm::pow_cr(x, y); }
+__device__ __noinline__ double ex(double x) { return crm::exp_cr(x); }
+
 // s95p::s95p_s, src/s95p.cpp:14-32 (the s95p-PCE fit of s(e))
 __device__ double s95p_s(double e) {
   double val;
   if (e < 0.1270769021427449)
-    val = 12.2304 * crm::pow_cr(e, 1.16849);
+    val = 12.2304 * pw(e, 1.16849);
   else if (e < 0.4467079524674040)
-    val = 11.9279 * crm::pow_cr(e, 1.15635);
+    val = 11.9279 * pw(e, 1.15635);
   else if (e < 1.9402832534193788)
-    val = 0.0580578 + 11.833 * crm::pow_cr(e, 1.16187);
+    val = 0.0580578 + 11.833 * pw(e, 1.16187);
   else if (e < 3.7292474570977285)
-    val = 18.202 * e - 62.021814 - 4.85479 * crm::exp_cr(-2.72407e-11 * crm::pow_cr(e, 4.54886)) +
-          65.1272 * crm::pow_cr(e, -0.128012) * crm::exp_cr(-0.00369624 * crm::pow_cr(e, 1.18735)) -
-          4.75253 * crm::pow_cr(e, -1.18423);
+    val = 18.202 * e - 62.021814 - 4.85479 * ex(-2.72407e-11 * pw(e, 4.54886)) +
+          65.1272 * pw(e, -0.128012) * ex(-0.00369624 * pw(e, 1.18735)) -
+          4.75253 * pw(e, -1.18423);
   else
-    val = 18.202 * e - 63.0218 - 4.85479 * crm::exp_cr(-2.72407e-11 * crm::pow_cr(e, 4.54886)) +
-          65.1272 * crm::pow_cr(e, -0.128012) * crm::exp_cr(-0.00369624 * crm::pow_cr(e, 1.18735));
-  return crm::pow_cr(val, 3. / 4.);
+    val = 18.202 * e - 63.0218 - 4.85479 * ex(-2.72407e-11 * pw(e, 4.54886)) +
+          65.1272 * pw(e, -0.128012) * ex(-0.00369624 * pw(e, 1.18735));
+  return pw(val, 3. / 4.);
 }
 
 // s95p::s95p_e, src/s95p.cpp:34-41; *bad gets bit 1 if kS95pMaxIt steps
 // did not converge (the reference would not return)
 __device__ double s95p_e(double s, unsigned* bad) {
-  double e = crm::pow_cr(s, 4. / 3.) / 18.2, e0;
+  double e = pw(s, 4. / 3.) / 18.2, e0;
   int it = 0;
   do {
     e0 = e;
-    e = e0 - (s95p_s(e0) - s) / (6.608681233 * crm::pow_cr(e0, -0.25));
+    e = e0 - (s95p_s(e0) - s) / (6.608681233 * pw(e0, -0.25));
     if (++it > kS95pMaxIt) {
       atomicOr(bad, 1u);
       break;
@@ -327,26 +334,37 @@ __global__ void __launch_bounds__(kTpb) k_ic_terms(TermArgs a) {
 }
 
 // sum of t[0..n) from 0.0 in index order, rounded after every addition as
-// the host loop: the warp loads 32 terms at a time, lane 0 adds the non-zero
-// ones in turn.  Skipping zeros changes nothing: the running sum starts at
-// +0 and is never -0 (an exact cancellation rounds to +0), and s + (+-0) = s
-// for every other s; the vacuum cells' terms are exactly zero.
-__global__ void __launch_bounds__(32) k_seq_sum(const double* __restrict__ t, long long n,
-                                                double* __restrict__ out) {
-  const int lane = threadIdx.x;
+// the host loop (zeros included, as there): thread 0 adds a tile of terms
+// from shared memory while warps 1.. load the next tile, so the running sum
+// waits only on its own additions, not on memory
+constexpr int kSumThreads = 256;
+constexpr int kSumTile = 2048;  // two tiles: 32 KB of shared memory
+
+__global__ void __launch_bounds__(kSumThreads) k_seq_sum(const double* __restrict__ t, long long n,
+                                                         double* __restrict__ out) {
+  __shared__ double buf[2][kSumTile];
+  const int tid = threadIdx.x;
+  const long long ntile = (n + kSumTile - 1) / kSumTile;
+  if (tid >= 32 && ntile > 0)
+    for (int j = tid - 32; j < kSumTile; j += kSumThreads - 32) buf[0][j] = j < n ? t[j] : 0.0;
+  __syncthreads();
   double s = 0.0;
-  for (long long base = 0; base < n; base += 32) {
-    const long long k = base + lane;
-    const double v = k < n ? t[k] : 0.0;
-    unsigned live = __ballot_sync(0xffffffffu, v != 0.0);  // NaN counts
-    while (live) {
-      const int j = __ffs(live) - 1;
-      live &= live - 1;
-      const double x = __shfl_sync(0xffffffffu, v, j);
-      if (lane == 0) s += x;
+  for (long long tile = 0; tile < ntile; tile++) {
+    const int b = (int)(tile & 1);
+    if (tid >= 32 && tile + 1 < ntile) {
+      const long long base = (tile + 1) * kSumTile;
+      for (int j = tid - 32; j < kSumTile; j += kSumThreads - 32)
+        buf[b ^ 1][j] = base + j < n ? t[base + j] : 0.0;
     }
+    if (tid == 0) {
+      const double* p = buf[b];
+      const int m = (int)min((long long)kSumTile, n - tile * kSumTile);
+#pragma unroll 8
+      for (int j = 0; j < m; j++) s += p[j];
+    }
+    __syncthreads();
   }
-  if (lane == 0) out[0] = s;
+  if (tid == 0) out[0] = s;
 }
 
 struct SetArgs {
@@ -584,7 +602,7 @@ vh_status norm_loop(vh_ctx* ctx, vh::icr::TermArgs ta, double* d_sum, double* h_
     old = nrm;
     ta.norm = nrm;
     vh::icr::k_ic_terms<<<blocks(ta.N), kTpb, 0, s>>>(ta);
-    vh::icr::k_seq_sum<<<1, 32, 0, s>>>(ta.terms, ta.N, d_sum);
+    vh::icr::k_seq_sum<<<1, vh::icr::kSumThreads, 0, s>>>(ta.terms, ta.N, d_sum);
     cudaError_t e = cudaMemcpyAsync(h_sum, d_sum, sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return ic_cuda(ctx, e, who);
