@@ -334,34 +334,53 @@ __global__ void __launch_bounds__(kTpb) k_ic_terms(TermArgs a) {
 }
 
 // sum of t[0..n) from 0.0 in index order, rounded after every addition as
-// the host loop (zeros included, as there): thread 0 adds a tile of terms
-// from shared memory while warps 1.. load the next tile, so the running sum
-// waits only on its own additions, not on memory
-constexpr int kSumThreads = 256;
-constexpr int kSumTile = 2048;  // two tiles: 32 KB of shared memory
+// the host loop: thread 0 adds a tile of terms from shared memory while the
+// block's loader warps stage the next tile, so the running sum waits only on
+// its own additions.  Each loader warp keeps its 256 terms of the tile with
+// the zeros squeezed out, in order (ballot and prefix count), and thread 0
+// adds the warps' runs in warp order: the same sequence of non-zero
+// additions as the host loop, whose zero terms change nothing (the running
+// sum starts at +0 and is never -0, and s + (+-0) = s for every other s; the
+// vacuum cells' terms are exactly zero).
+constexpr int kSumLoaders = 8;                     // loader warps
+constexpr int kSumThreads = 32 * (1 + kSumLoaders);
+constexpr int kSumRun = 256;                       // terms per loader warp and tile
+constexpr int kSumTile = kSumLoaders * kSumRun;    // 2 x 16 KB of shared memory
 
 __global__ void __launch_bounds__(kSumThreads) k_seq_sum(const double* __restrict__ t, long long n,
                                                          double* __restrict__ out) {
   __shared__ double buf[2][kSumTile];
-  const int tid = threadIdx.x;
+  __shared__ int cnt[2][kSumLoaders];
+  const int tid = threadIdx.x, warp = tid / 32, lane = tid % 32;
   const long long ntile = (n + kSumTile - 1) / kSumTile;
-  if (tid >= 32 && ntile > 0)
-    for (int j = tid - 32; j < kSumTile; j += kSumThreads - 32) buf[0][j] = j < n ? t[j] : 0.0;
+  // loader warp w stages terms [w * kSumRun, (w + 1) * kSumRun) of a tile
+  auto stage = [&](long long tile, int b) {
+    const int w = warp - 1;
+    const long long base = tile * kSumTile + (long long)w * kSumRun;
+    double* dst = buf[b] + w * kSumRun;
+    int c = 0;
+    for (int r = 0; r < kSumRun; r += 32) {
+      const long long k = base + r + lane;
+      const double v = k < n ? t[k] : 0.0;
+      const unsigned live = __ballot_sync(0xffffffffu, v != 0.0);  // NaN counts
+      if (v != 0.0) dst[c + __popc(live & ((1u << lane) - 1u))] = v;
+      c += __popc(live);
+    }
+    if (lane == 0) cnt[b][w] = c;
+  };
+  if (warp > 0 && ntile > 0) stage(0, 0);
   __syncthreads();
   double s = 0.0;
   for (long long tile = 0; tile < ntile; tile++) {
     const int b = (int)(tile & 1);
-    if (tid >= 32 && tile + 1 < ntile) {
-      const long long base = (tile + 1) * kSumTile;
-      for (int j = tid - 32; j < kSumTile; j += kSumThreads - 32)
-        buf[b ^ 1][j] = base + j < n ? t[base + j] : 0.0;
-    }
-    if (tid == 0) {
-      const double* p = buf[b];
-      const int m = (int)min((long long)kSumTile, n - tile * kSumTile);
-#pragma unroll 8
-      for (int j = 0; j < m; j++) s += p[j];
-    }
+    if (warp > 0 && tile + 1 < ntile) stage(tile + 1, b ^ 1);
+    if (tid == 0)
+      for (int w = 0; w < kSumLoaders; w++) {
+        const double* p = buf[b] + w * kSumRun;
+        const int m = cnt[b][w];
+#pragma unroll 4
+        for (int j = 0; j < m; j++) s += p[j];
+      }
     __syncthreads();
   }
   if (tid == 0) out[0] = s;
