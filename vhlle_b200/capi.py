@@ -293,7 +293,7 @@ class VhTableIc(ctypes.Structure):
                 ("factor", ctypes.c_double), ("glauber_var", ctypes.c_int)]
 
 
-# icModel of the two readers with named setups (src/main.cpp:342-358)
+# icModel of the two readers with named setups (src/main.cpp:341-354)
 IC_GLISSANDO, IC_TRENTO = 5, 7
 
 
