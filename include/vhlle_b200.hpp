@@ -1097,6 +1097,10 @@ class IcGlissando {
     if (npart_.empty()) throw Error(VH_ERR_ARG, std::string("no GLISSANDO events in ") + filename);
   }
   int nevents() const { return (int)npart_.size(); }
+  const std::vector<double>& x() const { return x_; }
+  const std::vector<double>& y() const { return y_; }
+  const std::vector<int>& c() const { return c_; }
+  const std::vector<int>& npart() const { return npart_; }
   // returns sNorm, nNorm
   std::pair<double, double> setIC(Hydro* h) {
     vh_glissando_ic ic{setup_, x_.data(), y_.data(), c_.data(), npart_.data(), nevents()};
@@ -1149,6 +1153,10 @@ class IcTrento {
     if (npart_.empty()) throw Error(VH_ERR_ARG, std::string("no TRENTO events in ") + filename);
   }
   int nevents() const { return (int)npart_.size(); }
+  const std::vector<double>& grid() const { return grid_; }
+  const std::vector<int>& ngrid() const { return ngrid_; }
+  const std::vector<double>& gmax() const { return gmax_; }
+  const std::vector<int>& npart() const { return npart_; }
   std::pair<double, double> setIC(Hydro* h) {
     vh_trento_ic ic{setup_, grid_.data(), ngrid_.data(), gmax_.data(), npart_.data(), nevents()};
     double norms[2];
@@ -1188,6 +1196,9 @@ class IC {
     for (int ix = 0; ix < nx_; ix++)
       for (int iy = 0; iy < ny_; iy++) fin >> x_[ix] >> y_[iy] >> val_[(size_t)ix * ny_ + iy];
   }
+  const std::vector<double>& x() const { return x_; }
+  const std::vector<double>& y() const { return y_; }
+  const std::vector<double>& val() const { return val_; }
   void setIC(Hydro* h) {
     vh_table_ic ic{nx_, ny_, x_.data(), y_.data(), val_.data(), factor_, glauberVar_};
     check(vh_init_table(h->context(), &ic), h->context());

@@ -166,3 +166,63 @@ def test_ic_setup_names():
         capi.ic_setup(capi.IC_TRENTO, "AFTER72")
     with pytest.raises(ValueError):
         capi.ic_setup(3, "LHC276")
+
+
+def _cpp_readers(tmp_path):
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "vhlle_b200")
+    if not os.path.exists(os.path.join(libdir, "libvhlle_b200.so")):
+        pytest.skip("library not built")
+    exe = str(tmp_path / "ic_readers")
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "ic_readers.cpp"), "-L", libdir,
+                    "-lvhlle_b200", "-Wl,-rpath," + libdir, "-o", exe], check=True)
+
+    def run(*args):
+        out = subprocess.run([exe, *args], capture_output=True, text=True, check=True).stdout
+        res, lines, i = {}, out.split("\n"), 0
+        while i < len(lines) and lines[i]:
+            tag, n = lines[i].split()
+            res[tag] = np.array([float(v) for v in lines[i + 1:i + 1 + int(n)]])
+            i += 1 + int(n)
+        return res
+    return run
+
+
+def test_cpp_readers_equal_the_python_readers(tmp_path):
+    """vhb::IcGlissando / IcTrento / IC parse the files as the Python readers
+    (and so as the reference's constructors, whose loops both follow),
+    including a GLISSANDO file that ends without a newline, whose last event
+    the reference does not count."""
+    run = _cpp_readers(tmp_path)
+    g = str(tmp_path / "g.txt")
+    F.write_glissando(g, F.synthetic_glissando_events(3, seed=2))
+    ev = F.read_glissando(g)
+    got = run("glissando", g, "RHIC200")
+    assert np.array_equal(got["npart"], ev.npart) and np.array_equal(got["c"], ev.c)
+    assert np.array_equal(got["x"], ev.x) and np.array_equal(got["y"], ev.y)
+    cut = str(tmp_path / "g2.txt")
+    with open(g) as f:
+        text = f.read()
+    with open(cut, "w") as f:
+        f.write(text.rstrip("\n"))
+    assert len(F.read_glissando(cut).npart) == 2
+    assert list(run("glissando", cut, "RHIC200")["npart"]) == list(ev.npart[:2])
+    t = str(tmp_path / "t.dat")
+    F.write_trento(t, F.synthetic_trento_events(2, seed=3, n=17))
+    tev = F.read_trento(t)
+    got = run("trento", t, "LHC276")
+    assert np.array_equal(got["npart"], tev.npart) and list(got["ngrid"]) == [17, 17]
+    assert np.array_equal(got["gmax"], tev.gmax)
+    assert np.array_equal(got["grid"], np.concatenate([a.reshape(-1) for a in tev.grids]))
+    s = str(tmp_path / "s.dat")
+    F.synthetic_song_table(nx=9, ny=5).write(s)
+    tab = F.read_song_table(s)
+    got = run("table", s)
+    assert np.array_equal(got["x"], tab.x) and np.array_equal(got["y"], tab.y)
+    assert np.array_equal(got["val"], tab.val.reshape(-1))
