@@ -118,19 +118,15 @@ __device__ __forceinline__ void d_face(const Geo& g, const EosDev& E,
     qlr[7 + k] = c - dQr;
   }
   div_batch<14>(qlr, tau, 1.0 / tau, crm::mk_den_ok(tau));
-  // the two root finds through one copy of transform_pv's code (a loop kept
-  // rolled): the kernel's instruction footprint was its second stall
-  Prim pp[2];
-  const long long at[2] = {L, R};
-#pragma unroll 1
-  for (int sd = 0; sd < 2; sd++) {
-    double q[7];
+  double ql[7], qr[7];
 #pragma unroll
-    for (int k = 0; k < 7; k++) q[k] = qlr[7 * sd + k];
-    transform_pv<EK>(E, q, pp[sd], c2p_guess(E, at[sd]));
+  for (int k = 0; k < 7; k++) {
+    ql[k] = qlr[k];
+    qr[k] = qlr[7 + k];
   }
-  const Prim& pl = pp[0];
-  const Prim& pr = pp[1];
+  Prim pl, pr;
+  transform_pv<EK>(E, ql, pl, c2p_guess(E, L));
+  transform_pv<EK>(E, qr, pr, c2p_guess(E, R));
   const double dxdir = DIR == X_ ? g.dx : (DIR == Y_ ? g.dy : g.dz);
   double fl[7];
   unsigned e = 0;
