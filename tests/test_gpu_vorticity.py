@@ -152,3 +152,39 @@ def test_gpu_beta_writer_matches_reference_text(tmp_path):
         lines = f.read().splitlines()
     assert len(lines[3]) == 24 * 33
     d.close()
+
+
+def test_gpu_pipelined_surface_with_vorticity_equals_blocking():
+    """With vorticity on, the pipelined surface call (on its own stream, from
+    the copy of Q, Qprev, pi, Pi and dbeta it takes in stream order) gives
+    the blocking call's records and beta.dat values bit for bit while the
+    next step runs beside it."""
+    import ctypes
+    from vhlle_b200.capi import GpuHydro
+    setup = W.small_glauber3d(33, 17, seed=11, b=6.0)
+    a, b = GpuHydro(setup), GpuHydro(setup)
+    a.enable_vorticity()
+    b.enable_vorticity()
+    pending, checked = None, 0
+    for k in range(1, 10):
+        a.step(1)
+        b.step(1)
+        if pending is not None:
+            info = b.surface_end()
+            rec0, info0, beta0 = pending
+            assert info == info0, (k, info, info0)
+            assert np.array_equal(b.surface_records(), rec0)
+            n = info["nelements"]
+            beta = np.zeros((n, 16))
+            got = ctypes.c_long()
+            b._check(b.L.vh_surface_beta(b.h, beta.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                         n, ctypes.byref(got)))
+            assert got.value == n and np.array_equal(beta, beta0)
+            checked += n
+            pending = None
+        if k % 2 == 0:
+            pending = a.surface_beta()
+            b.surface_begin()
+    assert checked > 500
+    a.close()
+    b.close()
