@@ -212,6 +212,22 @@ vh_status vh_device_state(vh_ctx *ctx, vh_state_view *dev);
  * launch on the context's stream; with per-kernel profiling on, or if the
  * capture is refused, the kernels are launched one by one. */
 vh_status vh_step(vh_ctx *ctx);
+/* One performStep with the state in host memory: copies the non-NULL
+ * fields of `in` to the device, steps as vh_step, and copies the fields
+ * named in `out` back (in and out may be the same view), as one CUDA graph
+ * launch on the context's stream whose copies overlap the step's kernels
+ * where its data flow allows: Q, m, Qh and Qprev go up first; pi, piH, Pi,
+ * PiH and viscCorrCut go up beside the ideal predictor and corrector, which
+ * do not read them; m comes back once the step's updateM has run, piH, PiH
+ * and viscCorrCut once the relaxation's advection has, the rest at the
+ * end.  Asynchronous: the host buffers must stay valid and unread until
+ * the work is done (vh_sync), and must be pinned (vh_alloc_pinned) for the
+ * copies to overlap anything.  The graph is captured per buffer set (and
+ * fill-fraction buffer order) and replayed while they repeat; with
+ * profiling on, or if the capture is refused, it is the sequence
+ * vh_upload_async, vh_step, vh_download_async.  No defaults are applied to
+ * NULL input fields (they keep their device values). */
+vh_status vh_step_host(vh_ctx *ctx, const vh_state_view *in, const vh_state_view *out);
 /* n successive performStep calls. */
 vh_status vh_steps(vh_ctx *ctx, int n);
 

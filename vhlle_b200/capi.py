@@ -42,7 +42,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_batch_sync", "vh_batch_info", "vh_batch_last_error", "vh_batch_timer_start",
            "vh_batch_timer_stop", "vh_batch_set_mode", "vh_set_slab", "vh_surface_cells",
            "vh_ic_setup_named", "vh_init_glissando", "vh_init_trento", "vh_init_gubser",
-           "vh_init_table")
+           "vh_init_table", "vh_step_host")
 
 
 class VhError(RuntimeError):
@@ -382,6 +382,7 @@ def lib():
     L.vh_active_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     L.vh_set_con2prim_method.argtypes = [vp, ctypes.c_int]
     L.vh_init_glauber.argtypes = [vp, ctypes.POINTER(VhGlauberIc)]
+    L.vh_step_host.argtypes = [vp, ctypes.POINTER(VhStateView), ctypes.POINTER(VhStateView)]
     L.vh_ic_setup_named.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.POINTER(VhIcSetup)]
     L.vh_init_glissando.argtypes = [vp, ctypes.POINTER(VhGlissandoIc), _dp]
     L.vh_init_trento.argtypes = [vp, ctypes.POINTER(VhTrentoIc), _dp]
@@ -528,6 +529,7 @@ class GpuHydro:
             raise VhError(st, self.L.vh_last_error(None).decode())
         self.h = h
         self.device = device
+        self._pinned = []
         if upload:
             self.upload_initial()
 
@@ -539,6 +541,9 @@ class GpuHydro:
         if getattr(self, "h", None):
             self.L.vh_destroy(self.h)
             self.h = None
+        for p in getattr(self, "_pinned", []):
+            self.L.vh_free_pinned(p)
+        self._pinned = []
 
     def __del__(self):
         try:
@@ -862,6 +867,32 @@ class GpuHydro:
         n = ctypes.c_int()
         self._check(self.L.vh_launches_per_step(self.h, ctypes.byref(n)))
         return n.value
+
+    def step_host(self, fields: dict, sync=True):
+        """vh_step_host: one step with the state in the host arrays
+        `fields` (name -> float64 array [ncomp][N], uploaded before and
+        overwritten after the step); pinned arrays (pinned_state) let the
+        copies overlap the kernels."""
+        v = VhStateView()
+        for k, a in fields.items():
+            assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"] and a.size == STATE_NCOMP[k] * self.N
+            setattr(v, k, a.ctypes.data)
+        self._check(self.L.vh_step_host(self.h, ctypes.byref(v), ctypes.byref(v)))
+        if sync:
+            self.sync()
+
+    def pinned_state(self, fields=STATE_FIELDS) -> dict:
+        """Page-locked host arrays (vh_alloc_pinned) for the named fields,
+        [ncomp][N] float64; released by close()."""
+        out = {}
+        for k in fields:
+            n = STATE_NCOMP[k] * self.N
+            p = ctypes.c_void_p()
+            self._check(self.L.vh_alloc_pinned(n * 8, ctypes.byref(p)))
+            self._pinned.append(p)
+            out[k] = np.ctypeslib.as_array((ctypes.c_double * n).from_address(p.value)).reshape(
+                STATE_NCOMP[k], self.N)
+        return out
 
     def get_state(self, fields=STATE_FIELDS) -> dict:
         v = VhStateView()

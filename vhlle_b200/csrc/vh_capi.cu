@@ -257,6 +257,12 @@ vh_status vh_destroy(vh_ctx* ctx) {
   if (ctx->snap_ev) cudaEventDestroy(ctx->snap_ev);
   for (cudaGraphExec_t& x : ctx->step_exec)
     if (x) cudaGraphExecDestroy(x);
+  for (cudaGraphExec_t& x : ctx->host_exec)
+    if (x) cudaGraphExecDestroy(x);
+  if (ctx->copy_up) cudaStreamDestroy(ctx->copy_up);
+  if (ctx->copy_down) cudaStreamDestroy(ctx->copy_down);
+  for (cudaEvent_t e : ctx->host_ev)
+    if (e) cudaEventDestroy(e);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   for (void* p : ctx->allocs) cudaFree(p);
   if (ctx->surf.host) cudaFreeHost(ctx->surf.host);
@@ -858,6 +864,172 @@ vh_status vh_step(vh_ctx* ctx) {
   std::swap(ctx->f.m, ctx->f.m2);
   ctx->tau += ctx->dt;  // src/hdo.cpp:1095
   return VH_OK;
+}
+
+// vh_step_host's copies hung on the step's kernels: m back once updateM
+// has run, the viscous inputs awaited before the first kernel after the
+// corrector's update (the ghost copy, which reads pi and Pi), piH, PiH and
+// viscCorrCut back once the relaxation's advection (their last writer) ran
+struct HostCopyMarker : vh::LaunchMarker {
+  vh_ctx* ctx;
+  cudaStream_t s;
+  const vh_state_view* out;
+  int nupdate = 0;
+  bool advected = false;
+  cudaError_t err = cudaSuccess;
+  HostCopyMarker(vh_ctx* c, cudaStream_t st, const vh_state_view* o) : ctx(c), s(st), out(o) {}
+  void down(double* dst, const double* src, int ncomp) {
+    if (dst && err == cudaSuccess)
+      err = cudaMemcpyAsync(dst, src, sizeof(double) * ncomp * ctx->g.N, cudaMemcpyDeviceToHost,
+                            ctx->copy_down);
+  }
+  void fork_down(cudaEvent_t ev) {
+    if (err == cudaSuccess) err = cudaEventRecord(ev, s);
+    if (err == cudaSuccess) err = cudaStreamWaitEvent(ctx->copy_down, ev, 0);
+  }
+  void after(int kind) override {
+    if (err != cudaSuccess) return;
+    if (kind == vh::KK_UPDATE_M) {
+      if (out->m) {
+        fork_down(ctx->host_ev[2]);
+        down(out->m, ctx->f.m2, 3);  // the next step's fill fractions
+      }
+    } else if (kind == vh::KK_UPDATE && ++nupdate == 2) {
+      err = cudaStreamWaitEvent(s, ctx->host_ev[1], 0);
+    } else if (kind == vh::KK_IS_ADVECT) {
+      advected = true;
+      if (out->piH || out->PiH || out->viscCorrCut) {
+        fork_down(ctx->host_ev[3]);
+        down(out->piH, ctx->f.piH, 10);
+        down(out->PiH, ctx->f.PiH, 1);
+        down(out->viscCorrCut, ctx->f.vcc, 1);
+      }
+    }
+  }
+};
+
+static std::vector<const void*> host_key(const vh_state_view* in, const vh_state_view* out) {
+  std::vector<const void*> k;
+  for (const FieldSpec& fs : kFields) {
+    k.push_back(in->*(fs.host));
+    k.push_back(out->*(fs.host));
+  }
+  return k;
+}
+
+// The step with its host copies captured into ctx->host_exec[par]; false if
+// the capture is refused (pageable host memory may be, for one).
+static bool capture_host_step(vh_ctx* ctx, int par, const vh_state_view* in,
+                              const vh_state_view* out) {
+  cudaError_t e = cudaSuccess;
+  if (!ctx->cap_stream) e = cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !ctx->copy_up)
+    e = cudaStreamCreateWithFlags(&ctx->copy_up, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !ctx->copy_down)
+    e = cudaStreamCreateWithFlags(&ctx->copy_down, cudaStreamNonBlocking);
+  for (cudaEvent_t& ev : ctx->host_ev)
+    if (e == cudaSuccess && !ev) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (ctx->host_exec[par]) {
+    cudaGraphExecDestroy(ctx->host_exec[par]);
+    ctx->host_exec[par] = nullptr;
+  }
+  const vh::StepArgs a = step_args(ctx);
+  const vh::Fields& F = ctx->f;
+  const long long N = ctx->g.N;
+  cudaStream_t s = ctx->cap_stream;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  auto copy = [&](double* dst, const double* src, int ncomp, cudaMemcpyKind kind, cudaStream_t st) {
+    if (src && dst && e == cudaSuccess)
+      e = cudaMemcpyAsync(dst, src, sizeof(double) * ncomp * N, kind, st);
+  };
+  // what the ideal stages read goes up first, on the step's stream
+  copy(F.Q, in->Q, 7, cudaMemcpyHostToDevice, s);
+  copy(F.m, in->m, 3, cudaMemcpyHostToDevice, s);
+  copy(F.Qh, in->Qh, 7, cudaMemcpyHostToDevice, s);
+  copy(F.Qprev, in->Qprev, 7, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->host_ev[0], s);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_up, ctx->host_ev[0], 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_down, ctx->host_ev[0], 0);
+  // the viscous inputs beside the ideal stages
+  copy(F.pi, in->pi, 10, cudaMemcpyHostToDevice, ctx->copy_up);
+  copy(F.piH, in->piH, 10, cudaMemcpyHostToDevice, ctx->copy_up);
+  copy(F.Pi, in->Pi, 1, cudaMemcpyHostToDevice, ctx->copy_up);
+  copy(F.PiH, in->PiH, 1, cudaMemcpyHostToDevice, ctx->copy_up);
+  copy(F.vcc, in->viscCorrCut, 1, cudaMemcpyHostToDevice, ctx->copy_up);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->host_ev[1], ctx->copy_up);
+  HostCopyMarker mk(ctx, s, out);
+  int n = 0;
+  if (e == cudaSuccess) {
+    if (ctx->mlp) vh::launch_mlp_guess(ctx->mlp->packed, F.Q, N, ctx->clk, ctx->vguess, s);
+    n = vh::launch_step(a, s, &mk);
+    vh::launch_clock_op(ctx->clk, 0, 0, s);
+    e = mk.err;
+  }
+  // the rest comes back at the end
+  copy(out->Q, F.Q, 7, cudaMemcpyDeviceToHost, s);
+  copy(out->Qh, F.Qh, 7, cudaMemcpyDeviceToHost, s);
+  copy(out->Qprev, F.Qprev, 7, cudaMemcpyDeviceToHost, s);
+  copy(out->pi, F.pi, 10, cudaMemcpyDeviceToHost, s);
+  copy(out->Pi, F.Pi, 1, cudaMemcpyDeviceToHost, s);
+  if (!mk.advected) {
+    copy(out->piH, F.piH, 10, cudaMemcpyDeviceToHost, s);
+    copy(out->PiH, F.PiH, 1, cudaMemcpyDeviceToHost, s);
+    copy(out->viscCorrCut, F.vcc, 1, cudaMemcpyDeviceToHost, s);
+  }
+  // join the copy streams
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->host_ev[4], ctx->copy_down);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->host_ev[4], 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ctx->host_ev[1], 0);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(s, &graph);
+  if (e == cudaSuccess) e = ec;
+  unsigned long long flags = cudaGraphInstantiateFlagUseNodePriority;
+  if (e == cudaSuccess && graph_high_priority(graph) != cudaSuccess) {
+    cudaGetLastError();
+    flags = 0;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&ctx->host_exec[par], graph, flags);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    ctx->host_exec[par] = nullptr;
+    return false;
+  }
+  ctx->host_version[par] = ctx->version;
+  ctx->host_key[par] = host_key(in, out);
+  ctx->step_launches[par] = n;
+  return true;
+}
+
+vh_status vh_step_host(vh_ctx* ctx, const vh_state_view* in, const vh_state_view* out) {
+  if (!ctx || !in || !out) return VH_ERR_ARG;
+  VH_NOT_PENDING(ctx, "vh_step_host");
+  VH_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (in->Q) ctx->uploaded = true;
+  if (!ctx->uploaded) return fail(ctx, VH_ERR_STATE, "vh_step_host: no state uploaded");
+  if (!ctx->prof && ctx->step_graphs) {
+    const int par = ctx->f.m == ctx->m_first ? 0 : 1;
+    if ((ctx->host_exec[par] && ctx->host_version[par] == ctx->version &&
+         ctx->host_key[par] == host_key(in, out)) ||
+        capture_host_step(ctx, par, in, out)) {
+      VH_CUDA(ctx, cudaGraphLaunch(ctx->host_exec[par], ctx->stream));
+      ctx->launches = ctx->step_launches[par];
+      std::swap(ctx->f.m, ctx->f.m2);
+      ctx->tau += ctx->dt;  // src/hdo.cpp:1095
+      return VH_OK;
+    }
+  }
+  vh_status st = vh_upload_async(ctx, in);
+  if (st == VH_OK) st = vh_step(ctx);
+  if (st == VH_OK) st = vh_download_async(ctx, out);
+  return st;
 }
 
 vh_status vh_steps(vh_ctx* ctx, int n) {

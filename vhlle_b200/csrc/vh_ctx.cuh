@@ -38,6 +38,13 @@ struct vh_ctx {
   // per step instead of ~20 kernel launches (captured on a private stream,
   // launched on `stream`); steps with per-kernel profiling launch directly
   cudaStream_t cap_stream = nullptr;
+  // vh_step_host: the step with its host copies, per fill-fraction buffer
+  // order, for one buffer set (host_key) at the version it was captured at
+  cudaGraphExec_t host_exec[2] = {nullptr, nullptr};
+  int host_version[2] = {-1, -1};
+  std::vector<const void*> host_key[2];
+  cudaStream_t copy_up = nullptr, copy_down = nullptr;
+  cudaEvent_t host_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   cudaGraphExec_t step_exec[2] = {nullptr, nullptr};
   int step_version[2] = {-1, -1};
   int step_launches[2] = {0, 0};
