@@ -118,7 +118,10 @@ def kernel_alg_bytes(prof, cells, nactive):
     return out
 
 
-STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")  # persistent per-cell state
+# the persistent per-cell state a step reads or leaves for the next one (the
+# empty cells keep their piH, PiH and viscCorrCut, which the viscous fluxes
+# and the surface read)
+STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m", "viscCorrCut")
 
 
 def measured_peaks():

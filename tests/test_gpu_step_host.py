@@ -12,7 +12,7 @@ from vhlle_b200 import capi
 from vhlle_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
-STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m")
+STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m", "viscCorrCut")
 
 
 @pytest.mark.parametrize("pinned", [True, False])
