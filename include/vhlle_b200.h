@@ -436,6 +436,27 @@ typedef struct vh_table_ic {
 } vh_table_ic;
 vh_status vh_init_table(vh_ctx *ctx, const vh_table_ic *ic);
 
+/* IcPartUrqmd (src/icPartUrqmd.cpp, icModel 3): every particle's
+ * energy-momentum (mt cosh and sinh of rap - eta + zdiff, px, py), baryon
+ * number (+-1 for |id| < 56) and charge smeared over a Gaussian in x, y and
+ * eta (widths Rgt, Rgt, Rgz; the eta term dropped for Rgz < 1e-5) on the
+ * stencil +-(int)(6 Rgt / dx), +-(int)(6 Rgt / dy), +-(int)(1.5 Rgz / dz)
+ * around its rounded cell (cells with ix, iy, iz > 0), normalised to the
+ * stencil's own sum, averaged over the events; then per cell transformPV
+ * (the reference's Newton at its 1e-5 tolerance), the module's cut (e <
+ * 1e-7 or |x| > 10, |y| > 10, |eta| > 5 fm: vacuum), setPrimVar and
+ * setAllM; Qprev stays zero.  Host arrays. */
+typedef struct vh_urqmd_ic {
+  const double *p;     /* [n][8]: tau, x, y, eta, mt, px, py, rap of every event's
+                          particles in file order */
+  const int *id;       /* [n] particle id */
+  const int *charge;   /* [n] */
+  const int *npart;    /* [nevents] particles of each event (>= 1) */
+  int nevents;
+  double Rgt, Rgz;     /* the params keys Rgt and Rgz */
+} vh_urqmd_ic;
+vh_status vh_init_urqmd(vh_ctx *ctx, const vh_urqmd_ic *ic);
+
 /* One event split into slabs along eta (one context per slab, a GPU each):
  * every persistent field (Q, Qh, Qprev, pi, piH, Pi, PiH, m, viscCorrCut:
  * VH_PLANE_DOUBLES doubles per cell) of the z-planes [z0, z0 + nplanes)

@@ -1206,6 +1206,47 @@ class IC {
   }
 };
 
+// IcPartUrqmd (icModel 3): "tau x y eta mt px py rap id charge" lines, a
+// line that does not parse ending an event that holds particles
+// (src/icPartUrqmd.cpp:79-103)
+class IcPartUrqmd {
+  std::vector<double> p_;
+  std::vector<int> id_, charge_, npart_;
+  double Rgt_, Rgz_;
+
+ public:
+  IcPartUrqmd(Fluid*, const char* filename, double Rgt, double Rgz, double /*tau0: the Hydro's*/)
+      : Rgt_(Rgt), Rgz_(Rgz) {
+    std::ifstream fin(filename);
+    if (!fin.good()) throw Error(VH_ERR_ARG, std::string("I/O error with ") + filename);
+    std::string line;
+    int np = 0;
+    while (!fin.eof()) {  // as IcGlissando's reader: see there for the last line
+      std::getline(fin, line);
+      std::istringstream in(line);
+      double v[8];
+      int id, ch;
+      if (in >> v[0] >> v[1] >> v[2] >> v[3] >> v[4] >> v[5] >> v[6] >> v[7] >> id >> ch) {
+        p_.insert(p_.end(), v, v + 8);
+        id_.push_back(id);
+        charge_.push_back(ch);
+        if (++np > 9999) throw Error(VH_ERR_ARG, "IcPartUrqmd: more particles in an event than NP");
+      } else if (np > 0) {
+        npart_.push_back(np);
+        np = 0;
+      }
+    }
+    if (npart_.empty()) throw Error(VH_ERR_ARG, std::string("no particle events in ") + filename);
+  }
+  int nevents() const { return (int)npart_.size(); }
+  const std::vector<int>& npart() const { return npart_; }
+  void setIC(Hydro* h) {
+    vh_urqmd_ic ic{p_.data(), id_.data(), charge_.data(), npart_.data(), nevents(), Rgt_, Rgz_};
+    check(vh_init_urqmd(h->context(), &ic), h->context());
+    h->adoptDeviceState();
+  }
+};
+
 // ------------------------------------------------------------- parameters
 // The reference driver's parameters with their defaults (src/main.cpp:70-81)
 // and its params-file reader (src/main.cpp:83-156): "name value" lines;

@@ -138,6 +138,9 @@ def oracle_lib():
                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(_State), _dp]
         lib.or_ic_gubser.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.c_double,
                                      ctypes.c_int, ctypes.POINTER(_State)]
+        lib.or_ic_urqmd.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.c_double,
+                                    _dp, _ip, _ip, _ip, ctypes.c_int, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_int, ctypes.POINTER(_State)]
         lib.or_ic_table.argtypes = [ctypes.POINTER(_Grid), ctypes.POINTER(_Eos), ctypes.c_double,
                                     ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, ctypes.c_double,
                                     ctypes.c_int, ctypes.c_int, ctypes.POINTER(_State)]
@@ -183,7 +186,8 @@ def ref_lib():
         lib.ref_update_m.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
         lib.ref_ic.restype = ctypes.c_int
         lib.ref_ic.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p,
-                               ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+                               ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                               _dp, _dp, _dp]
         lib.ref_s95p_e.argtypes = [_dp, ctypes.c_int, _dp]
         lib.ref_totals.argtypes = [ctypes.c_void_p, ctypes.c_double, _dp]
         lib.ref_cornelius4d.restype = ctypes.c_int
@@ -336,11 +340,13 @@ def _trc(setup, crmath=False):
     return t
 
 
-def oracle_ic(setup, model, data=None, ic_setup=None, crmath=False, factor=1.0, glauber_var=1):
+def oracle_ic(setup, model, data=None, ic_setup=None, crmath=False, factor=1.0, glauber_var=1,
+              Rgt=1.0, Rgz=1.0):
     """The C restatement of an IC module (vh_oracle_ic.c) on setup's grid and
     EoS at setup.tau0: model 5 IcGlissando (data: ic_files.GlissandoEvents),
     7 IcTrento (ic_files.TrentoEvents), 4 ICGubser, 2 IC over a table
-    (ic_files.SongTable, factor, glauber_var).  ic_setup: the setup dict of
+    (ic_files.SongTable, factor, glauber_var), 3 IcPartUrqmd
+    (ic_files.UrqmdEvents, Rgt, Rgz).  ic_setup: the setup dict of
     models 5 and 7.  Returns (state dict, (sNorm, nNorm))."""
     lib = oracle_lib()
     g = setup.grid
@@ -375,6 +381,14 @@ def oracle_ic(setup, model, data=None, ic_setup=None, crmath=False, factor=1.0, 
                               npart.ctypes.data_as(_ip), len(ngrid), int(crmath), ctypes.byref(sv),
                               _ptr(norms))
         assert rc == 0
+    elif model == 3:
+        pp = np.ascontiguousarray(data.p, dtype=np.float64)
+        pid = np.ascontiguousarray(data.id, dtype=np.int32)
+        ch = np.ascontiguousarray(data.charge, dtype=np.int32)
+        npart = np.ascontiguousarray(data.npart, dtype=np.int32)
+        lib.or_ic_urqmd(ctypes.byref(grid), ctypes.byref(eos.s), setup.tau0, _ptr(pp),
+                        pid.ctypes.data_as(_ip), ch.ctypes.data_as(_ip), npart.ctypes.data_as(_ip),
+                        len(npart), float(Rgt), float(Rgz), int(crmath), ctypes.byref(sv))
     elif model == 4:
         lib.or_ic_gubser(ctypes.byref(grid), ctypes.byref(eos.s), setup.tau0, int(crmath),
                          ctypes.byref(sv))
@@ -671,14 +685,15 @@ class RefRun:
         self.lib.ref_step(self.h, n)
         return 0
 
-    def ic(self, model, path="", setup_name="", s0scale=1.0, glauber_var=1):
-        """The reference's IC module `model` (2, 4, 5 or 7: src/main.cpp:324-366)
-        on a fresh Fluid of this run's grid, from the file at path with the
-        named setup; returns Q, Qprev [7][N] and m [N] of every cell."""
+    def ic(self, model, path="", setup_name="", s0scale=1.0, glauber_var=1, Rgt=1.0, Rgz=1.0):
+        """The reference's IC module `model` (2, 3, 4, 5 or 7:
+        src/main.cpp:324-366) on a fresh Fluid of this run's grid, from the
+        file at path with the named setup (or the smearing widths Rgt, Rgz);
+        returns Q, Qprev [7][N] and m [N] of every cell."""
         N = self.setup.grid.ncells
         Q, Qp, m = np.zeros((7, N)), np.zeros((7, N)), np.zeros(N)
         rc = self.lib.ref_ic(self.h, model, path.encode(), setup_name.encode(), s0scale,
-                             glauber_var, _ptr(Q), _ptr(Qp), _ptr(m))
+                             glauber_var, Rgt, Rgz, _ptr(Q), _ptr(Qp), _ptr(m))
         if rc != 0:
             raise ValueError("the reference has no IC model %d here" % model)
         return {"Q": Q, "Qprev": Qp, "m": m}

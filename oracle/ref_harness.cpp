@@ -41,6 +41,7 @@
 #include "ic.h"
 #include "icGlissando.h"
 #include "icGubser.h"
+#include "icPartUrqmd.h"
 #include "icTrento.h"
 #include "inc.h"
 #include "s95p.h"
@@ -688,15 +689,16 @@ int ref_cornelius4d(const double *cube, const double *dx, double E0, double *cen
 
 // One of the reference's IC modules run on a fresh Fluid of the run's grid,
 // as the driver does (src/main.cpp:320-366): model 2 IC (the entropy or energy
-// table of file, scaled by s0scale; glauber_var sets glauberVar), 4
-// ICGubser, 5 IcGlissando, 7 IcTrento (file and the setup name).  Returns
+// table of file, scaled by s0scale; glauber_var sets glauberVar), 3
+// IcPartUrqmd (file, the widths Rgt and Rgz), 4 ICGubser, 5 IcGlissando, 7
+// IcTrento (file and the setup name).  Returns
 // every cell's Q and Qprev [7][N] and m [N] (its three directions are
 // equal), in the grid order (ix fastest), or -1 for another model.  The
 // modules' console output is discarded.
 int ref_ic(void *p, int model, const char *file, const char *setup, double s0scale,
-           int glauber_var, double *Q, double *Qprev, double *m) {
+           int glauber_var, double Rgt, double Rgz, double *Q, double *Qprev, double *m) {
   RefRun *r = static_cast<RefRun *>(p);
-  if (model != 2 && model != 4 && model != 5 && model != 7) return -1;
+  if (model != 2 && model != 3 && model != 4 && model != 5 && model != 7) return -1;
   // a fresh Fluid (and its Hydro), as the driver builds before the IC
   delete r->h;
   delete r->f;
@@ -711,6 +713,9 @@ int ref_ic(void *p, int model, const char *file, const char *setup, double s0sca
     glauberVariable = glauber_var;
     IC ic(file, s0scale);
     ic.setIC(r->f, r->eos, r->tau0);
+  } else if (model == 3) {
+    IcPartUrqmd ic(r->f, file, Rgt, Rgz, r->tau0);
+    ic.setIC(r->f, r->eos);
   } else if (model == 4) {
     ICGubser ic;
     ic.setIC(r->f, r->eos, r->tau0);

@@ -247,6 +247,13 @@ void or_ic_table(const or_grid *g, const or_eos *E, double tau, int NX, int NY,
                  const double *xs, const double *ys, const double *val, double factor,
                  int glauber_var, int cr, or_state *s);
 
+/* IcPartUrqmd (src/icPartUrqmd.cpp): p[n][8] = tau, x, y, eta, mt, px, py,
+ * rap of every event's particles in file order, their id and charge,
+ * npart[ev]; the smearing widths Rgt (transverse) and Rgz (eta) */
+void or_ic_urqmd(const or_grid *g, const or_eos *E, double tau0, const double *p,
+                 const int *id, const int *charge, const int *npart, int nevents, double Rgt,
+                 double Rgz, int cr, or_state *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -9,6 +9,7 @@
  *   or_ic_gubser     ICGubser (src/icGubser.cpp), icModel 4
  *   or_ic_table      IC + s95p::loadSongIC / getSongEps (src/ic.cpp,
  *                    src/s95p.cpp:43-88), icModel 2
+ *   or_ic_urqmd      IcPartUrqmd (src/icPartUrqmd.cpp), icModel 3
  * over the structure-of-arrays state of vh_oracle.h.  It checks the CUDA
  * builders (vh_init_glissando, vh_init_trento, vh_init_gubser,
  * vh_init_table); the product never links, loads or calls it.
@@ -400,4 +401,82 @@ void or_ic_table(const or_grid *g, const or_eos *E, double tau, int NX, int NY,
         if (e > 0.) set_all_m(s, N, i, 1.);
       }
   free(t);
+}
+
+/* IcPartUrqmd (src/icPartUrqmd.cpp:17-253), icModel 3: each particle's
+ * energy-momentum, baryon number and charge smeared over a 3D Gaussian
+ * stencil normalised to its own sum (makeSmoothTable, :105-175), summed over
+ * the events; then per cell transformPV of the averaged Q, a cut, setPrimVar
+ * and setAllM (setIC, :202-227).  p[n][8] = tau, x, y, eta, mt, px, py, rap.
+ * The per-particle cosh / sinh of (rap - eta + zdiff) and gamma_z use the C
+ * library in both arms (the CUDA path's host side computes them). */
+void or_ic_urqmd(const or_grid *g, const or_eos *E, double tau0, const double *p,
+                 const int *id, const int *charge, const int *npart, int nevents, double Rgt,
+                 double Rgz, int cr, or_state *s) {
+  const long N = (long)g->nx * g->ny * g->nz;
+  const double dx = gdx(g), dy = gdy(g), dz = gdz(g);
+  const double Rgx = Rgt, Rgy = Rgt;
+  const int nsx = (int)(6.0 * Rgx / dx), nsy = (int)(6.0 * Rgy / dy);
+  const int nsz = (int)(1.5 * Rgz / dz);
+  double *T = calloc(6 * (size_t)N, sizeof(double)); /* T00, T0x, T0y, T0z, QB, QE */
+  if (!T) return;
+  fresh_cells(g, s);
+  long np = 0;
+  for (int ev = 0; ev < nevents; ev++) np += npart[ev];
+  for (long ip = 0; ip < np; ip++) {
+    const double *q = p + 8 * ip;
+    const double X = q[1], Y = q[2], Eta = q[3], Mt = q[4], Px = q[5], Py = q[6], Rap = q[7];
+    const int ixc = (int)round((X - g->xmin) / dx);
+    const int iyc = (int)round((Y - g->ymin) / dy);
+    const int izc = (int)round((Eta - g->zmin) / dz);
+    const double gammaz = cosh(Rap - Eta);
+    double norm_gauss = 0.0;
+    for (int pass = 0; pass < 2; pass++)
+      for (int ix = ixc - nsx; ix < ixc + nsx + 1; ix++)
+        for (int iy = iyc - nsy; iy < iyc + nsy + 1; iy++)
+          for (int iz = izc - nsz; iz < izc + nsz + 1; iz++)
+            if (ix > 0 && ix < g->nx && iy > 0 && iy < g->ny && iz > 0 && iz < g->nz) {
+              const double xdiff = X - (g->xmin + ix * dx);
+              const double ydiff = Y - (g->ymin + iy * dy);
+              const double zdiff = Eta - (g->zmin + iz * dz);
+              double a;
+              if (fabs(Rgz) < 1e-5)
+                a = -xdiff * xdiff / Rgx / Rgx - ydiff * ydiff / Rgy / Rgy;
+              else
+                a = -xdiff * xdiff / Rgx / Rgx - ydiff * ydiff / Rgy / Rgy -
+                    zdiff * zdiff / Rgz / Rgz * gammaz * gammaz * tau0 * tau0;
+              if (pass == 0) {
+                norm_gauss += xexp(a, cr);
+                continue;
+              }
+              double weight = 1.0 / norm_gauss * xexp(a, cr);
+              if (weight != weight || fabs(weight) > DBL_MAX) weight = 0.0;
+              const long i = ix + (long)g->nx * (iy + (long)g->ny * iz);
+              T[0 * N + i] += weight * Mt * cosh(Rap - Eta + zdiff);
+              T[1 * N + i] += weight * Px;
+              T[2 * N + i] += weight * Py;
+              T[3 * N + i] += weight * Mt * sinh(Rap - Eta + zdiff);
+              if (id[ip] > 0 && id[ip] < 56) T[4 * N + i] += weight;
+              if (id[ip] < 0 && id[ip] > -56) T[4 * N + i] -= weight;
+              T[5 * N + i] += charge[ip] * weight;
+            }
+  }
+  for (int ix = 0; ix < g->nx; ix++)
+    for (int iy = 0; iy < g->ny; iy++)
+      for (int iz = 0; iz < g->nz; iz++) {
+        const long i = ix + (long)g->nx * (iy + (long)g->ny * iz);
+        double Q[7], o[8];
+        for (int k = 0; k < 6; k++) Q[k] = T[k * N + i] / nevents / dx / dy / dz / tau0;
+        Q[6] = 0.0;
+        or_transform_pv(E, Q, 1, o);
+        double e = o[0], nb = o[2], nq = o[3], ns = o[4], vx = o[5], vy = o[6], vz = o[7];
+        const double x = g->xmin + ix * dx, y = g->ymin + iy * dy, eta = g->zmin + iz * dz;
+        if (e < 1e-7 || fabs(x) > 10. || fabs(y) > 10. || fabs(eta) > 5.) {
+          e = nb = nq = 0.0;
+          vx = vy = vz = 0.0;
+        }
+        set_prim_var(E, s->Q, N, i, tau0, e, nb, nq, ns, vx, vy, vz);
+        if (e > 0.) set_all_m(s, N, i, 1.);
+      }
+  free(T);
 }

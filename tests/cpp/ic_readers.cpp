@@ -8,6 +8,7 @@
 //   ic_readers glissando <file> <setup>
 //   ic_readers trento <file> <setup>
 //   ic_readers table <file>
+//   ic_readers urqmd <file>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -36,6 +37,9 @@ int main(int argc, char** argv) {
       put("ngrid", ic.ngrid());
       put("gmax", ic.gmax());
       put("grid", ic.grid());
+    } else if (kind == "urqmd") {
+      vhb::IcPartUrqmd ic(nullptr, argv[2], 1.0, 1.0, 0.5);
+      put("npart", ic.npart());
     } else if (kind == "table") {
       vhb::IC ic(argv[2], 1.0, 1);
       put("x", ic.x());

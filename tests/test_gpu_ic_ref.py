@@ -1,8 +1,9 @@
 """The device builders of the reference's initial-state modules
-(vh_init_glissando, vh_init_trento, vh_init_gubser, vh_init_table) against
-the C restatement and the compiled reference modules (IcGlissando, IcTrento,
-ICGubser, IC: src/icGlissando.cpp, src/icTrento.cpp, src/icGubser.cpp,
-src/ic.cpp), on seeded synthetic inputs in the modules' file formats.
+(vh_init_glissando, vh_init_trento, vh_init_gubser, vh_init_table,
+vh_init_urqmd) against the C restatement and the compiled reference modules
+(IcGlissando, IcTrento, ICGubser, IC, IcPartUrqmd: src/icGlissando.cpp,
+src/icTrento.cpp, src/icGubser.cpp, src/ic.cpp, src/icPartUrqmd.cpp), on
+seeded synthetic inputs in the modules' file formats.
 
 The device evaluates exp and pow correctly rounded (crm::exp_cr, pow_cr):
 against the oracle's crmath arm every cell is bit-identical (Q, Qprev, m, the
@@ -121,6 +122,25 @@ def test_gpu_table_equals_oracle_and_reference(gv, grid_setup, tmp_path):
             ref.close()
 
 
+@pytest.mark.parametrize("Rgt,Rgz", [(1.0, 1.0), (0.8, 0.0)])
+def test_gpu_urqmd_equals_oracle_and_reference(Rgt, Rgz, grid_setup, tmp_path):
+    """IcPartUrqmd (icModel 3): the per-cell transformPV amplifies the
+    smearing's last-bit exp differences, hence 1e-13 against the
+    reference."""
+    path = str(tmp_path / "particles.txt")
+    F.write_urqmd(path, F.synthetic_urqmd_events(3, seed=5, nmean=300))
+    ev = F.read_urqmd(path)
+    st, _ = _device(grid_setup, lambda h: h.init_urqmd(ev, Rgt, Rgz))
+    o, _ = P.oracle_ic(grid_setup, 3, ev, Rgt=Rgt, Rgz=Rgz, crmath=True)
+    _equal_oracle(st, o)
+    if P.ref_available():
+        ref = P.RefRun(grid_setup)
+        try:
+            _close_ref(st, ref.ic(3, path, Rgt=Rgt, Rgz=Rgz), rtol=1e-13)
+        finally:
+            ref.close()
+
+
 def test_gpu_glissando_full_grid_equals_oracle(tmp_path):
     """The 101x101x51 grid with 10 RHIC62 events (baryon density on): bit
     for bit the oracle's crmath arm; the device and reference times are
@@ -169,9 +189,10 @@ def test_gpu_ic_refused_on_a_slab(grid_setup):
         h.close()
 
 
-@pytest.mark.parametrize("model", [5, 7, 4])
+@pytest.mark.parametrize("model", [5, 7, 4, 3])
 def test_gpu_driver_builds_the_reference_ic(model, grid_setup, tmp_path):
-    """vhlle_run with icModel 5 (IcGlissando), 7 (IcTrento) or 4 (ICGubser):
+    """vhlle_run with icModel 5 (IcGlissando), 7 (IcTrento), 4 (ICGubser) or
+    3 (IcPartUrqmd, Rgt = Rgz = 1 by default):
     the initial state built on the device (the printed sNorm is the
     oracle's), then the corona at tau0 equals the oracle's on that state."""
     import dataclasses
@@ -194,6 +215,11 @@ def test_gpu_driver_builds_the_reference_ic(model, grid_setup, tmp_path):
         o, norms = P.oracle_ic(setup, 7, F.read_trento(path),
                                capi.ic_setup(capi.IC_TRENTO, "RHIC62"), crmath=True)
         args = ["-ISinput", path, "-system", "RHIC62"]
+    elif model == 3:
+        path = str(tmp_path / "particles.txt")
+        F.write_urqmd(path, F.synthetic_urqmd_events(3, seed=5, nmean=300))
+        o, norms = P.oracle_ic(setup, 3, F.read_urqmd(path), Rgt=1.0, Rgz=1.0, crmath=True)
+        args = ["-ISinput", path]
     else:
         o, norms = P.oracle_ic(setup, 4, crmath=True)
     params = str(tmp_path / "params.txt")

@@ -1,7 +1,7 @@
 """The C restatement of the reference's initial-state modules
 (oracle/vh_oracle_ic.c) against the modules themselves, compiled unmodified
-into oracle/_ref: IcGlissando, IcTrento, ICGubser and IC over the s95p table
-(icModel 5, 7, 4, 2: src/main.cpp:324-366), on seeded synthetic inputs in
+into oracle/_ref: IcGlissando, IcTrento, ICGubser, IC over the s95p table and
+IcPartUrqmd (icModel 5, 7, 4, 2, 3: src/main.cpp:324-366), on seeded synthetic inputs in
 the modules' file formats (vhlle_b200/ic_files.py), every named setup.
 
 With the C library's exp and pow (the reference's) the restatement is bit
@@ -123,6 +123,22 @@ def test_table_oracle_equals_reference(gv, grid_setup, ref, tmp_path):
     _close(o1["Q"], r["Q"], 1e-14)
 
 
+@needs_ref
+@pytest.mark.parametrize("Rgt,Rgz", [(1.0, 1.0), (0.8, 0.0)])
+def test_urqmd_oracle_equals_reference(Rgt, Rgz, grid_setup, ref, tmp_path):
+    """IcPartUrqmd (icModel 3), with the eta smearing and without it."""
+    path = str(tmp_path / "particles.txt")
+    F.write_urqmd(path, F.synthetic_urqmd_events(3, seed=5, nmean=300))
+    ev = F.read_urqmd(path)
+    r = ref.ic(3, path, Rgt=Rgt, Rgz=Rgz)
+    o, _ = P.oracle_ic(grid_setup, 3, ev, Rgt=Rgt, Rgz=Rgz)
+    _same(o, r)
+    assert (r["Q"][0] > 0).sum() > 1000 and np.abs(r["Q"][1]).max() > 0
+    assert (r["Q"][4] != 0).any() and (r["Q"][5] != 0).any()
+    o1, _ = P.oracle_ic(grid_setup, 3, ev, Rgt=Rgt, Rgz=Rgz, crmath=True)
+    _close(o1["Q"], r["Q"], 1e-13)
+
+
 def test_glissando_reader_follows_the_reference_loop(tmp_path):
     """Binary-collision lines (c = 0) are dropped, a line that does not parse
     ends an event that holds sources, and the last event ends at the end of
@@ -220,6 +236,10 @@ def test_cpp_readers_equal_the_python_readers(tmp_path):
     assert np.array_equal(got["npart"], tev.npart) and list(got["ngrid"]) == [17, 17]
     assert np.array_equal(got["gmax"], tev.gmax)
     assert np.array_equal(got["grid"], np.concatenate([a.reshape(-1) for a in tev.grids]))
+    u = str(tmp_path / "u.txt")
+    F.write_urqmd(u, F.synthetic_urqmd_events(2, seed=4, nmean=50))
+    uev = F.read_urqmd(u)
+    assert list(run("urqmd", u)["npart"]) == list(uev.npart)
     s = str(tmp_path / "s.dat")
     F.synthetic_song_table(nx=9, ny=5).write(s)
     tab = F.read_song_table(s)

@@ -42,7 +42,7 @@ EXPORTS = ("vh_create", "vh_destroy", "vh_set_stream", "vh_upload_state", "vh_do
            "vh_batch_sync", "vh_batch_info", "vh_batch_last_error", "vh_batch_timer_start",
            "vh_batch_timer_stop", "vh_batch_set_mode", "vh_set_slab", "vh_surface_cells",
            "vh_ic_setup_named", "vh_init_glissando", "vh_init_trento", "vh_init_gubser",
-           "vh_init_table", "vh_step_host")
+           "vh_init_table", "vh_step_host", "vh_init_urqmd")
 
 
 class VhError(RuntimeError):
@@ -293,6 +293,12 @@ class VhTableIc(ctypes.Structure):
                 ("factor", ctypes.c_double), ("glauber_var", ctypes.c_int)]
 
 
+class VhUrqmdIc(ctypes.Structure):
+    _fields_ = [("p", _dp), ("id", ctypes.POINTER(ctypes.c_int)),
+                ("charge", ctypes.POINTER(ctypes.c_int)), ("npart", ctypes.POINTER(ctypes.c_int)),
+                ("nevents", ctypes.c_int), ("Rgt", ctypes.c_double), ("Rgz", ctypes.c_double)]
+
+
 # icModel of the two readers with named setups (src/main.cpp:341-354)
 IC_GLISSANDO, IC_TRENTO = 5, 7
 
@@ -388,6 +394,7 @@ def lib():
     L.vh_init_trento.argtypes = [vp, ctypes.POINTER(VhTrentoIc), _dp]
     L.vh_init_gubser.argtypes = [vp]
     L.vh_init_table.argtypes = [vp, ctypes.POINTER(VhTableIc)]
+    L.vh_init_urqmd.argtypes = [vp, ctypes.POINTER(VhUrqmdIc)]
     L.vh_pack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
     L.vh_set_surface_eos.argtypes = [vp, ctypes.POINTER(VhEos)]
     L.vh_unpack_planes.argtypes = [vp, ctypes.c_int, ctypes.c_int, vp]
@@ -619,6 +626,18 @@ class GpuHydro:
         ic = VhTableIc(len(x), len(y), x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
                        val.ctypes.data_as(_dp), factor, glauber_var)
         self._check(self.L.vh_init_table(self.h, ctypes.byref(ic)))
+
+    def init_urqmd(self, ev, Rgt=1.0, Rgz=1.0):
+        """vh_init_urqmd: IcPartUrqmd's initial state (icModel 3) from
+        ic_files.UrqmdEvents with the smearing widths Rgt, Rgz."""
+        p = np.ascontiguousarray(ev.p, dtype=np.float64)
+        pid = np.ascontiguousarray(ev.id, dtype=np.int32)
+        ch = np.ascontiguousarray(ev.charge, dtype=np.int32)
+        npart = np.ascontiguousarray(ev.npart, dtype=np.int32)
+        ip = ctypes.POINTER(ctypes.c_int)
+        ic = VhUrqmdIc(p.ctypes.data_as(_dp), pid.ctypes.data_as(ip), ch.ctypes.data_as(ip),
+                       npart.ctypes.data_as(ip), len(npart), Rgt, Rgz)
+        self._check(self.L.vh_init_urqmd(self.h, ctypes.byref(ic)))
 
     def set_surface_eos(self, eos):
         """vh_set_surface_eos: the freeze-out EoS (Fluid's eosH) from a

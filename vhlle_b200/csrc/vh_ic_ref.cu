@@ -484,6 +484,126 @@ __global__ void __launch_bounds__(kTpb) k_ic_table(TableArgs a) {
   put_cell(a.f, g.N, i, qv, true, e > 0. ? 1. : 0.);
 }
 
+// ---- IcPartUrqmd (src/icPartUrqmd.cpp:105-175, 202-227)
+constexpr int kUqTx = 32, kUqTy = 4;  // transverse tile of one block (one eta cell)
+
+struct UrqmdArgs {
+  Geo g;
+  double xmin, ymin, zmin, tau0, Rgx, Rgy, Rgz, nev;
+  int nsx, nsy, nsz;
+  const double* p;    // [n][8] tau, x, y, eta, mt, px, py, rap
+  const int* id;
+  const int* charge;
+  const int* c3;      // [n][3] ixc, iyc, izc
+  const double* gz;   // [n] gamma_z = cosh(rap - eta)
+  const double* csh;  // [n][2 nsz + 1][2] cosh, sinh of (rap - eta + zdiff) per stencil plane
+  double* norm;       // [n]
+  int n;
+  const int* toff;    // [ntiles + 1] CSR of the particles whose stencil meets a tile
+  const int* tlist;
+  int ntx;
+  double* T;          // [6][N] T00, T0x, T0y, T0z, QB, QE
+};
+
+// the Gaussian's exponent, as both of the module's stencil loops write it
+__device__ __forceinline__ double uq_arg(const UrqmdArgs& a, double xdiff, double ydiff,
+                                         double zdiff, double gammaz) {
+  if (fabs(a.Rgz) < 1e-5) return -xdiff * xdiff / a.Rgx / a.Rgx - ydiff * ydiff / a.Rgy / a.Rgy;
+  return -xdiff * xdiff / a.Rgx / a.Rgx - ydiff * ydiff / a.Rgy / a.Rgy -
+         zdiff * zdiff / a.Rgz / a.Rgz * gammaz * gammaz * a.tau0 * a.tau0;
+}
+
+// norm_gauss of every particle: its stencil in the module's loop order
+__global__ void __launch_bounds__(kTpb) k_urqmd_norm(UrqmdArgs a) {
+  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ip >= a.n) return;
+  const Geo& g = a.g;
+  const double X = a.p[8 * ip + 1], Y = a.p[8 * ip + 2], Eta = a.p[8 * ip + 3];
+  const int ixc = a.c3[3 * ip], iyc = a.c3[3 * ip + 1], izc = a.c3[3 * ip + 2];
+  const double gammaz = a.gz[ip];
+  double s = 0.0;
+  for (int ix = ixc - a.nsx; ix < ixc + a.nsx + 1; ix++)
+    for (int iy = iyc - a.nsy; iy < iyc + a.nsy + 1; iy++)
+      for (int iz = izc - a.nsz; iz < izc + a.nsz + 1; iz++)
+        if (ix > 0 && ix < g.nx && iy > 0 && iy < g.ny && iz > 0 && iz < g.nz) {
+          const double xdiff = X - (a.xmin + ix * g.dx);
+          const double ydiff = Y - (a.ymin + iy * g.dy);
+          const double zdiff = Eta - (a.zmin + iz * g.dz);
+          s += ex(uq_arg(a, xdiff, ydiff, zdiff, gammaz));
+        }
+  a.norm[ip] = s;
+}
+
+// every cell's sums over the particles whose stencil covers it, in file
+// order (the tile's list is in that order)
+__global__ void __launch_bounds__(kUqTx * kUqTy) k_urqmd_T(UrqmdArgs a) {
+  const Geo& g = a.g;
+  const int tile = blockIdx.x, iz = blockIdx.y;
+  const int ix = (tile % a.ntx) * kUqTx + threadIdx.x % kUqTx;
+  const int iy = (tile / a.ntx) * kUqTy + threadIdx.x / kUqTx;
+  const bool in = ix < g.nx && iy < g.ny;
+  const bool open = in && ix > 0 && iy > 0 && iz > 0;  // the loops' ix, iy, iz > 0
+  double t00 = 0., t0x = 0., t0y = 0., t0z = 0., qb = 0., qe = 0.;
+  if (open) {
+    const double xc = a.xmin + ix * g.dx, yc = a.ymin + iy * g.dy, zc = a.zmin + iz * g.dz;
+    for (int k = a.toff[tile]; k < a.toff[tile + 1]; k++) {
+      const int ip = a.tlist[k];
+      const int ixc = a.c3[3 * ip], iyc = a.c3[3 * ip + 1], izc = a.c3[3 * ip + 2];
+      if (ix < ixc - a.nsx || ix > ixc + a.nsx || iy < iyc - a.nsy || iy > iyc + a.nsy ||
+          iz < izc - a.nsz || iz > izc + a.nsz)
+        continue;
+      const double* q = a.p + 8 * ip;
+      const double xdiff = q[1] - xc, ydiff = q[2] - yc, zdiff = q[3] - zc;
+      double w = 1.0 / a.norm[ip] * ex(uq_arg(a, xdiff, ydiff, zdiff, a.gz[ip]));
+      if (w != w || fabs(w) > DBL_MAX) w = 0.0;
+      const double* cs = a.csh + ((long long)ip * (2 * a.nsz + 1) + (iz - (izc - a.nsz))) * 2;
+      t00 += w * q[4] * cs[0];
+      t0x += w * q[5];
+      t0y += w * q[6];
+      t0z += w * q[4] * cs[1];
+      const int id = a.id[ip];
+      if (id > 0 && id < 56) qb += w;
+      if (id < 0 && id > -56) qb -= w;
+      qe += a.charge[ip] * w;
+    }
+  }
+  if (!in) return;
+  const long long N = g.N, i = ix + (long long)g.nx * (iy + (long long)g.ny * iz);
+  a.T[0 * N + i] = t00;
+  a.T[1 * N + i] = t0x;
+  a.T[2 * N + i] = t0y;
+  a.T[3 * N + i] = t0z;
+  a.T[4 * N + i] = qb;
+  a.T[5 * N + i] = qe;
+}
+
+// IcPartUrqmd::setIC: transformPV of the averaged Q, the module's cut,
+// setPrimVar, setAllM; no saveQprev
+__global__ void __launch_bounds__(kTpb) k_urqmd_set(UrqmdArgs a, EosDev E, Fields f) {
+  const Geo& g = a.g;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= g.N) return;
+  const long long N = g.N;
+  const int nxy = g.nx * g.ny;
+  const int iz = (int)(i / nxy), it = (int)(i % nxy);
+  const int ix = it % g.nx, iy = it / g.nx;
+  double Q[7];
+#pragma unroll
+  for (int k = 0; k < 6; k++) Q[k] = a.T[k * N + i] / a.nev / g.dx / g.dy / g.dz / a.tau0;
+  Q[6] = 0.0;
+  Prim o;
+  transform_pv<EK_ANY>(E, Q, o);
+  double e = o.e, nb = o.nb, nq = o.nq, vx = o.vx, vy = o.vy, vz = o.vz;
+  const double x = a.xmin + ix * g.dx, y = a.ymin + iy * g.dy, eta = a.zmin + iz * g.dz;
+  if (e < 1e-7 || fabs(x) > 10. || fabs(y) > 10. || fabs(eta) > 5.) {
+    e = nb = nq = 0.0;
+    vx = vy = vz = 0.0;
+  }
+  double q[7];
+  set_prim(E, a.tau0, e, nb, nq, o.ns, vx, vy, vz, q);
+  put_cell(f, N, i, q, false, e > 0. ? 1. : 0.);
+}
+
 }  // namespace icr
 }  // namespace vh
 
@@ -937,5 +1057,99 @@ extern "C" vh_status vh_init_table(vh_ctx* ctx, const vh_table_ic* ic) {
   a.E = ctx->eos;
   a.f = ctx->f;
   vh::icr::k_ic_table<<<blocks(g.N), kTpb, 0, s>>>(a);
+  return ic_finish(ctx, sc, d_bad, who);
+}
+
+extern "C" vh_status vh_init_urqmd(vh_ctx* ctx, const vh_urqmd_ic* ic) {
+  static const char* who = "vh_init_urqmd";
+  if (!ctx || !ic || ic->nevents < 1 || !ic->npart || !ic->p || !ic->id || !ic->charge)
+    return VH_ERR_ARG;
+  long long n = 0;
+  for (int ev = 0; ev < ic->nevents; ev++) {
+    if (ic->npart[ev] < 1) return ic_err(ctx, VH_ERR_ARG, std::string(who) + ": an event without particles");
+    n += ic->npart[ev];
+  }
+  if (n > INT32_MAX / 64 || !(ic->Rgt > 0.) || !(ic->Rgz >= 0.))
+    return ic_err(ctx, VH_ERR_ARG, std::string(who) + ": need Rgt > 0, Rgz >= 0");
+  vh_status st = ic_begin(ctx, who);
+  if (st) return st;
+  const vh::Geo& g = ctx->g;
+  cudaStream_t s = ctx->stream;
+  vh::icr::UrqmdArgs a{};
+  a.g = g;
+  a.xmin = ctx->grid.xmin;
+  a.ymin = ctx->grid.ymin;
+  a.zmin = ctx->grid.etamin;
+  a.tau0 = ctx->tau;
+  a.Rgx = a.Rgy = ic->Rgt;
+  a.Rgz = ic->Rgz;
+  a.nev = ic->nevents;
+  // the stencil half-widths (src/icPartUrqmd.cpp:36-38)
+  a.nsx = (int)(6.0 * a.Rgx / g.dx);
+  a.nsy = (int)(6.0 * a.Rgy / g.dy);
+  a.nsz = (int)(1.5 * a.Rgz / g.dz);
+  a.n = (int)n;
+  const int nzs = 2 * a.nsz + 1;
+  // per particle: the stencil centre (rounded as the module rounds), gamma_z
+  // and the cosh / sinh of every stencil plane's rapidity offset, with the C
+  // library; the tiles each stencil meets, in particle order
+  std::vector<int> c3(3 * (size_t)n);
+  std::vector<double> gz(n), csh((size_t)n * nzs * 2);
+  a.ntx = (g.nx + vh::icr::kUqTx - 1) / vh::icr::kUqTx;
+  const int nty = (g.ny + vh::icr::kUqTy - 1) / vh::icr::kUqTy;
+  std::vector<std::vector<int>> tiles((size_t)a.ntx * nty);
+  for (long long ip = 0; ip < n; ip++) {
+    const double* q = ic->p + 8 * ip;
+    const int ixc = (int)std::round((q[1] - a.xmin) / g.dx);
+    const int iyc = (int)std::round((q[2] - a.ymin) / g.dy);
+    const int izc = (int)std::round((q[3] - a.zmin) / g.dz);
+    c3[3 * ip] = ixc;
+    c3[3 * ip + 1] = iyc;
+    c3[3 * ip + 2] = izc;
+    gz[ip] = std::cosh(q[7] - q[3]);
+    for (int k = 0; k < nzs; k++) {
+      const int iz = izc - a.nsz + k;
+      const double zdiff = q[3] - (a.zmin + iz * g.dz);
+      csh[((size_t)ip * nzs + k) * 2] = std::cosh(q[7] - q[3] + zdiff);
+      csh[((size_t)ip * nzs + k) * 2 + 1] = std::sinh(q[7] - q[3] + zdiff);
+    }
+    const int x0 = std::max(1, ixc - a.nsx), x1 = std::min(g.nx - 1, ixc + a.nsx);
+    const int y0 = std::max(1, iyc - a.nsy), y1 = std::min(g.ny - 1, iyc + a.nsy);
+    const int z0 = std::max(1, izc - a.nsz), z1 = std::min(g.nz - 1, izc + a.nsz);
+    if (x0 > x1 || y0 > y1 || z0 > z1) continue;  // the stencil misses the grid
+    for (int ty = y0 / vh::icr::kUqTy; ty <= y1 / vh::icr::kUqTy; ty++)
+      for (int tx = x0 / vh::icr::kUqTx; tx <= x1 / vh::icr::kUqTx; tx++)
+        tiles[(size_t)ty * a.ntx + tx].push_back((int)ip);
+  }
+  std::vector<int> toff(tiles.size() + 1, 0), tlist;
+  for (size_t t = 0; t < tiles.size(); t++) {
+    toff[t + 1] = toff[t] + (int)tiles[t].size();
+    tlist.insert(tlist.end(), tiles[t].begin(), tiles[t].end());
+  }
+  Scratch sc;
+  a.p = sc.upload(ic->p, 8 * (size_t)n, s);
+  a.id = sc.upload(ic->id, (size_t)n, s);
+  a.charge = sc.upload(ic->charge, (size_t)n, s);
+  a.c3 = sc.upload(c3.data(), c3.size(), s);
+  a.gz = sc.upload(gz.data(), gz.size(), s);
+  a.csh = sc.upload(csh.data(), csh.size(), s);
+  a.norm = sc.alloc<double>((size_t)n);
+  a.toff = sc.upload(toff.data(), toff.size(), s);
+  a.tlist = sc.upload(tlist.data(), tlist.size(), s);
+  a.T = sc.alloc<double>(6 * (size_t)g.N);
+  unsigned* d_bad = sc.alloc<unsigned>(1);
+  if (sc.err == cudaSuccess) sc.err = cudaMemsetAsync(d_bad, 0, sizeof(unsigned), s);
+  if (sc.err != cudaSuccess) return ic_cuda(ctx, sc.err, who);
+  vh::icr::k_urqmd_norm<<<blocks(n), kTpb, 0, s>>>(a);
+  vh::icr::k_urqmd_T<<<dim3((unsigned)tiles.size(), (unsigned)g.nz), vh::icr::kUqTx * vh::icr::kUqTy,
+                       0, s>>>(a);
+  // the module's transformPV: the reference's Newton at its own tolerance,
+  // whatever the context's steps use
+  vh::EosDev E = ctx->eos;
+  E.tol = 0.00001;
+  E.slope = 0;
+  E.vguess = nullptr;
+  E.stats = nullptr;
+  vh::icr::k_urqmd_set<<<blocks(g.N), kTpb, 0, s>>>(a, E, ctx->f);
   return ic_finish(ctx, sc, d_bad, who);
 }

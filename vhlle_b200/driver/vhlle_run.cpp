@@ -2,12 +2,13 @@
 // over the device hydro: parameters file, substeps, one-shot x2 resize,
 // termination at tauMax.  The initial state (src/main.cpp:320-366) is built
 // on the device by the reference's modules for icModel 2 (IC over the s95p
-// table of -ISinput, s0ScaleFactor, glauberVar), 4 (ICGubser), 5
+// table of -ISinput, s0ScaleFactor, glauberVar), 3 (IcPartUrqmd, the
+// particle list of -ISinput smeared with Rgt, Rgz), 4 (ICGubser), 5
 // (IcGlissando) and 7 (IcTrento), the last two reading -ISinput with the
 // setup named by -system, at tau0; or, whatever icModel says, it is read
 // from -ISinput when that file is a grid snapshot (VHBSNAP1, which fixes
-// tau0).  The other models (the GSL optical Glauber, the UrQMD and SMASH
-// particle lists, TRENTO 3D, SuperMC) are refused.
+// tau0).  The other models (the GSL optical Glauber, the SMASH particle
+// lists, TRENTO 3D, SuperMC) are refused.
 //
 //   vhlle_run -params FILE [-ISinput SNAPSHOT|ICFILE] [-outputDir DIR]
 //             [-system S] [-printParams]
@@ -111,7 +112,8 @@ int run(int argc, char** argv) {
     in.read(tag, 8);
     snapshot = in && std::memcmp(tag, "VHBSNAP1", 8) == 0;
   }
-  if (!snapshot && P.icModel != 2 && P.icModel != 4 && P.icModel != 5 && P.icModel != 7)
+  if (!snapshot && P.icModel != 2 && P.icModel != 3 && P.icModel != 4 && P.icModel != 5 &&
+      P.icModel != 7)
     throw vhb::Error(VH_ERR_ARG, "icModel " + std::to_string(P.icModel) +
                                      " is not built here: give a grid snapshot as -ISinput");
   if (!snapshot && P.icModel != 4 && cl.isInputFile.empty())
@@ -185,6 +187,10 @@ int run(int argc, char** argv) {
     const char* sys = cl.collSystem.c_str();
     if (P.icModel == 2) {
       vhb::IC(file, P.s0ScaleFactor, P.glauberVariable).setIC(h);
+    } else if (P.icModel == 3) {
+      vhb::IcPartUrqmd ic(f, file, P.Rgt, P.Rgz, tau0);
+      ic.setIC(h);
+      std::cout << "IcPartUrqmd: loaded " << ic.nevents() << " events\n";
     } else if (P.icModel == 4) {
       vhb::ICGubser().setIC(h);
     } else if (P.icModel == 5) {

@@ -9,9 +9,13 @@ tree):
     line 10, grid-max on line 11) and n rows of n entropy values
     (IcTrento, src/icTrento.cpp:115-179)
   * the (x, y, value) table of s95p::loadSongIC (src/s95p.cpp:43-66)
+  * UrQMD particle lists, one "tau x y eta mt px py rap id charge" line per
+    particle, events separated as GLISSANDO's (IcPartUrqmd,
+    src/icPartUrqmd.cpp:79-103)
 
-The parsed forms feed vh_init_glissando, vh_init_trento and vh_init_table
-(capi.GpuHydro.init_glissando / init_trento / init_table)."""
+The parsed forms feed vh_init_glissando, vh_init_trento, vh_init_table and
+vh_init_urqmd (capi.GpuHydro.init_glissando / init_trento / init_table /
+init_urqmd)."""
 from __future__ import annotations
 
 import math
@@ -247,3 +251,100 @@ def synthetic_song_table(nx: int = 101, ny: int = 101, xmax: float = 12.0,
     X, Y = np.meshgrid(x, y, indexing="ij")
     r = np.sqrt((X / 0.8) ** 2 + Y ** 2)
     return SongTable(x, y, s0 / (1 + np.exp((r - r0) / 0.6)))
+
+
+# ------------------------------------------------------ UrQMD particle lists
+URQMD_MAX_PARTICLES = 10000  # IcPartUrqmd::NP (src/icPartUrqmd.h:11)
+
+
+@dataclass
+class UrqmdEvents:
+    p: np.ndarray       # [n][8] tau, x, y, eta, mt, px, py, rap; every event in file order
+    id: np.ndarray      # int32 [n] particle id
+    charge: np.ndarray  # int32 [n]
+    npart: np.ndarray   # int32 [nevents]
+
+    @property
+    def nevents(self) -> int:
+        return len(self.npart)
+
+
+def _parse_particle(line: str):
+    """`istringstream >> Tau >> X >> Y >> Eta >> Mt >> Px >> Py >> Rap >> Id
+    >> Charge` on one line, or None where it fails."""
+    t = line.split()
+    if len(t) < 10:
+        return None
+    try:
+        v = [float(x) for x in t[:8]]
+        return v, int(t[8]), int(t[9])
+    except ValueError:
+        return None
+
+
+def read_urqmd(path: str) -> UrqmdEvents:
+    """IcPartUrqmd's reading loop (src/icPartUrqmd.cpp:79-103): a line that
+    parses is a particle, a line that does not ends an event that holds
+    particles (the end of the file, after a last newline, too)."""
+    rows, ids, ch, npart = [], [], [], []
+    n = 0
+    with open(path) as f:
+        lines = f.read().split("\n")
+    for line in lines:
+        v = _parse_particle(line)
+        if v is not None:
+            rows.append(v[0])
+            ids.append(v[1])
+            ch.append(v[2])
+            n += 1
+            if n >= URQMD_MAX_PARTICLES:
+                raise ValueError("an event with more particles than the reader's arrays hold")
+        elif n > 0:
+            npart.append(n)
+            n = 0
+    if not npart:
+        raise ValueError("no particle events in %s" % path)
+    return UrqmdEvents(np.array(rows).reshape(-1, 8), np.array(ids, dtype=np.int32),
+                       np.array(ch, dtype=np.int32), np.array(npart, dtype=np.int32))
+
+
+def write_urqmd(path: str, ev: UrqmdEvents) -> None:
+    """One "tau x y eta mt px py rap id charge" line per particle, each
+    event after a "# event k" line (which ends the one before)."""
+    with open(path, "w") as f:
+        base = 0
+        for k, n in enumerate(ev.npart):
+            f.write("# event %d\n" % k)
+            for j in range(base, base + n):
+                f.write(" ".join("%.10g" % v for v in ev.p[j]) + " %d %d\n" % (ev.id[j], ev.charge[j]))
+            base += n
+
+
+def synthetic_urqmd_events(nevents: int, seed: int, nmean: int = 400, tau0: float = 0.5,
+                           R: float = 4.0) -> UrqmdEvents:
+    """Seeded particle lists on the tau0 hypersurface: positions Gaussian in
+    x, y (width R) and in eta (width 1.5), thermal-like transverse momenta,
+    rapidities near eta, a nucleon / pion / kaon mix of ids and charges (a
+    few baryons with |id| < 56 and charged mesons)."""
+    rng = np.random.default_rng(seed)
+    rows, ids, ch, npart = [], [], [], []
+    for _ in range(nevents):
+        n = int(rng.integers(nmean // 2, nmean + nmean // 2))
+        x, y = rng.normal(0, R, n), rng.normal(0, R, n)
+        eta = rng.normal(0, 1.5, n)
+        m = rng.choice([0.938, 0.138, 0.494], n, p=[0.25, 0.6, 0.15])
+        pt = rng.exponential(0.45, n)
+        phi = rng.uniform(0, 2 * np.pi, n)
+        px, py = pt * np.cos(phi), pt * np.sin(phi)
+        mt = np.sqrt(m * m + pt * pt)
+        rap = eta + rng.normal(0, 0.3, n)
+        pid = np.where(m > 0.9, rng.choice([1, 17, -1], n, p=[0.7, 0.2, 0.1]),
+                       np.where(m > 0.3, 106, 101))
+        c = np.where(m > 0.9, np.where(pid > 0, 1, -1) * (rng.uniform(0, 1, n) < 0.4),
+                     rng.choice([-1, 0, 1], n))
+        rows.append(np.stack([np.full(n, tau0), x, y, eta, mt, px, py, rap], 1))
+        ids.append(pid)
+        ch.append(c)
+        npart.append(n)
+    return UrqmdEvents(np.concatenate(rows), np.concatenate(ids).astype(np.int32),
+                       np.concatenate(ch).astype(np.int32), np.array(npart, dtype=np.int32))
