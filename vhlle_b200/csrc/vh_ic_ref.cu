@@ -1121,7 +1121,12 @@ extern "C" vh_status vh_init_urqmd(vh_ctx* ctx, const vh_urqmd_ic* ic) {
       for (int tx = x0 / vh::icr::kUqTx; tx <= x1 / vh::icr::kUqTx; tx++)
         tiles[(size_t)ty * a.ntx + tx].push_back((int)ip);
   }
+  size_t nlist = 0;
+  for (const std::vector<int>& t : tiles) nlist += t.size();
+  if (nlist > (size_t)INT32_MAX)
+    return ic_err(ctx, VH_ERR_ARG, std::string(who) + ": too many particle-tile pairs");
   std::vector<int> toff(tiles.size() + 1, 0), tlist;
+  tlist.reserve(nlist);
   for (size_t t = 0; t < tiles.size(); t++) {
     toff[t + 1] = toff[t] + (int)tiles[t].size();
     tlist.insert(tlist.end(), tiles[t].begin(), tiles[t].end());
