@@ -178,6 +178,38 @@ def test_gpu_glissando_full_grid_equals_oracle(tmp_path):
     print(msg)
 
 
+def test_gpu_urqmd_full_grid_equals_oracle(tmp_path):
+    """IcPartUrqmd on the 101x101x51 grid, 10 events of ~400 particles,
+    Rgt = Rgz = 1 (a 41 x 41 x 11 stencil per particle): bit for bit the
+    oracle's crmath arm; the device and reference times are printed."""
+    setup = W.glauber3d_setup()
+    path = str(tmp_path / "particles.txt")
+    F.write_urqmd(path, F.synthetic_urqmd_events(10, seed=13))
+    ev = F.read_urqmd(path)
+    h = capi.GpuHydro(setup, upload=False)
+    try:
+        h.init_urqmd(ev, 1.0, 1.0)  # first call: module load
+        t0 = time.perf_counter()
+        h.init_urqmd(ev, 1.0, 1.0)
+        t_dev = time.perf_counter() - t0
+        st = h.get_state()
+    finally:
+        h.close()
+    o, _ = P.oracle_ic(setup, 3, ev, Rgt=1.0, Rgz=1.0, crmath=True)
+    _equal_oracle(st, o)
+    msg = "IcPartUrqmd 101x101x51, %d particles: device %.4f s" % (len(ev.id), t_dev)
+    if P.ref_available():
+        ref = P.RefRun(setup)
+        try:
+            t0 = time.perf_counter()
+            r = ref.ic(3, path, Rgt=1.0, Rgz=1.0)
+            msg += ", reference %.2f s" % (time.perf_counter() - t0)
+            _close_ref(st, r, rtol=1e-13)
+        finally:
+            ref.close()
+    print(msg)
+
+
 def test_gpu_ic_refused_on_a_slab(grid_setup):
     h = capi.GpuHydro(grid_setup, upload=False)
     try:
