@@ -3,8 +3,9 @@ overlapping the kernels) against vh_step with the state resident on the
 device: after every step the host arrays hold what the resident run
 downloads, bit for bit, with page-locked arrays (the captured graph with its
 copy branches) and with ordinary ones (the upload / step / download
-sequence), on a viscous event (the relaxation-stage copies) and an ideal one
-(every copy at the end), with surface calls between the steps."""
+sequence), on a viscous event (the relaxation-stage copies), the same with
+vorticity on, and an ideal one (every copy at the end), with surface calls
+between the steps."""
 import numpy as np
 import pytest
 
@@ -16,11 +17,14 @@ STATE_IO = ("Q", "pi", "piH", "Pi", "PiH", "m", "viscCorrCut")
 
 
 @pytest.mark.parametrize("pinned", [True, False])
-@pytest.mark.parametrize("case", ["viscous", "ideal"])
+@pytest.mark.parametrize("case", ["viscous", "ideal", "vorticity"])
 def test_gpu_step_host_equals_resident(case, pinned):
-    setup = (W.small_glauber3d(33, 17, seed=11, b=6.0) if case == "viscous"
-             else W.gubser_setup(nx=41, ny=41))
+    setup = (W.gubser_setup(nx=41, ny=41) if case == "ideal"
+             else W.small_glauber3d(33, 17, seed=11, b=6.0))
     a, b = capi.GpuHydro(setup), capi.GpuHydro(setup)
+    if case == "vorticity":
+        a.enable_vorticity()
+        b.enable_vorticity()
     try:
         host = (b.pinned_state(STATE_IO) if pinned else
                 {k: np.zeros((capi.STATE_NCOMP[k], b.N)) for k in STATE_IO})
@@ -37,8 +41,10 @@ def test_gpu_step_host_equals_resident(case, pinned):
             if n % 3 == 0:
                 assert a.surface()[1] == b.surface()[1]
         assert (host["Q"][0] > 0).any() and (host["m"] > 0).any()
-        if case == "viscous":
+        if case != "ideal":
             assert np.abs(host["pi"]).max() > 0
+        if case == "vorticity":
+            assert np.array_equal(a.get_dbeta(), b.get_dbeta())
     finally:
         a.close()
         b.close()
